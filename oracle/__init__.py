@@ -1,0 +1,343 @@
+"""ctypes bindings for the CPU oracle (test infrastructure only).
+
+The oracle is a plain FP64 C++ restatement of the reference's Monte Carlo sweep
+(glotzerlab/hoomd-rs v1.4.0, ``hoomd-mc``), built by ``oracle/Makefile`` into
+``oracle/liboracle.so``. Only ``tests/``, ``__graft_entry__.smoke()`` and the
+CPU-baseline leg of ``bench.py`` load it; it is the checker, never the product.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboracle.so")
+
+HARD_SPHERE = 0
+HARD_CONVEX_POLYGON = 1
+HARD_CONVEX_POLYHEDRON = 2
+LENNARD_JONES = 3
+TRANSLATE = 0
+ROTATE = 1
+
+_dp = C.POINTER(C.c_double)
+_u64p = C.POINTER(C.c_uint64)
+_u8p = C.POINTER(C.c_uint8)
+_u32p = C.POINTER(C.c_uint32)
+
+
+def build() -> str:
+    """Compile the oracle with its Makefile (idempotent)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = C.CDLL(_LIB_PATH)
+        L.oracle_sfc64_outputs.argtypes = [C.c_uint64] * 6 + [_u64p]
+        L.oracle_sfc64_seed_from_u64.argtypes = [C.c_uint64] * 3 + [_u64p]
+        L.oracle_counter_outputs.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint64, _u64p]
+        L.oracle_counter_uniforms.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint64, _dp]
+        L.oracle_counter_normals.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint64, _dp]
+        L.oracle_counter_ball.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint32,
+                                          C.c_double, C.c_uint64, _dp]
+        L.oracle_counter_choose.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint32]
+        L.oracle_counter_choose.restype = C.c_uint32
+        L.oracle_cbrt.argtypes = [C.c_double]
+        L.oracle_cbrt.restype = C.c_double
+        L.oracle_sincos_half.argtypes = [C.c_double, _dp, _dp]
+        L.oracle_ziggurat_tables.argtypes = [_dp, _dp]
+        L.oracle_wrap.argtypes = [C.c_uint32, _dp, _dp]
+        L.oracle_generate_ghosts.argtypes = [C.c_uint32, _dp, C.c_double, _dp, _dp]
+        L.oracle_generate_ghosts.restype = C.c_uint32
+        L.oracle_checkerboard_dimensions.argtypes = [C.c_uint32, _dp, C.c_double, C.c_int, _dp, _u64p]
+        L.oracle_checkerboard_dimensions.restype = C.c_int
+        L.oracle_point_to_space_index.argtypes = [C.c_uint32, _dp, _dp, _u64p, C.c_int, _dp]
+        L.oracle_point_to_space_index.restype = C.c_int64
+        L.oracle_space_indices_by_color.argtypes = [C.c_uint32, _u64p, _u64p]
+        L.oracle_checkerboard_for_counter.argtypes = [C.c_uint32, _dp, C.c_double, C.c_uint64, C.c_uint32,
+                                                      C.c_uint32, _dp, _dp, _u64p]
+        L.oracle_checkerboard_for_counter.restype = C.c_int
+        L.oracle_convex_intersects_at_3d.argtypes = [_dp, C.c_uint32, _dp, C.c_uint32, _dp, _dp]
+        L.oracle_convex_intersects_at_2d.argtypes = [_dp, C.c_uint32, _dp, C.c_uint32, _dp, C.c_double]
+        L.oracle_convex_intersects_at_global_3d.argtypes = [_dp, C.c_uint32, _dp, _dp, _dp, _dp]
+        L.oracle_versor_from_axis_angle.argtypes = [_dp, C.c_double, _dp]
+        L.oracle_versor_combine.argtypes = [_dp, _dp, _dp]
+        L.oracle_versor_rotate.argtypes = [_dp, _dp, _dp]
+        L.oracle_lj_energy.argtypes = [C.c_double] * 3
+        L.oracle_lj_energy.restype = C.c_double
+        L.oracle_shifted_lj_pair.argtypes = [C.c_double] * 5
+        L.oracle_shifted_lj_pair.restype = C.c_double
+        L.oracle_system_create.argtypes = [C.c_uint32, _dp, C.c_uint64, _dp, _dp, C.c_uint64, C.c_uint32,
+                                           C.c_uint32, C.c_uint32, C.c_double, _dp, C.c_uint32, C.c_double,
+                                           C.c_double, C.c_double, C.c_double, C.c_double]
+        L.oracle_system_create.restype = C.c_void_p
+        L.oracle_system_destroy.argtypes = [C.c_void_p]
+        L.oracle_get_state.argtypes = [C.c_void_p, _dp, _dp, _u64p, _u32p]
+        L.oracle_set_counter.argtypes = [C.c_void_p, C.c_uint64, C.c_uint32]
+        L.oracle_increment_step.argtypes = [C.c_void_p]
+        L.oracle_parallel_sweep.argtypes = [C.c_void_p, C.c_uint32, C.c_double, C.c_double, C.c_double,
+                                            _u64p, _u64p]
+        L.oracle_parallel_sweep.restype = C.c_int
+        L.oracle_serial_sweep.argtypes = [C.c_void_p, C.c_uint32, C.c_double, C.c_double, _u64p, _u64p]
+        L.oracle_serial_sweep.restype = C.c_int
+        L.oracle_overlap_count.argtypes = [C.c_void_p]
+        L.oracle_overlap_count.restype = C.c_uint64
+        L.oracle_total_energy.argtypes = [C.c_void_p]
+        L.oracle_total_energy.restype = C.c_double
+        L.oracle_delta_energy_one.argtypes = [C.c_void_p, C.c_uint64, _dp, _dp]
+        L.oracle_delta_energy_one.restype = C.c_double
+        L.oracle_eval_moves.argtypes = [C.c_void_p, C.c_uint64, _u64p, _dp, _dp, _dp, C.c_double, _u8p, _dp]
+        _lib = L
+    return _lib
+
+
+def _d(a):
+    return a.ctypes.data_as(_dp) if a is not None else None
+
+
+def _f64(a, shape=None):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    return a if shape is None else a.reshape(shape)
+
+
+# ---- random numbers ---------------------------------------------------------------
+def sfc64_seed_from_u64(state: int, n: int, skip: int = 0) -> np.ndarray:
+    out = np.zeros(n, dtype=np.uint64)
+    lib().oracle_sfc64_seed_from_u64(state, skip, n, out.ctypes.data_as(_u64p))
+    return out
+
+
+def counter_outputs(step, substep, seed, index, n):
+    out = np.zeros(n, dtype=np.uint64)
+    lib().oracle_counter_outputs(step, substep, seed, index, n, out.ctypes.data_as(_u64p))
+    return out
+
+
+def counter_uniforms(step, substep, seed, index, n):
+    out = np.zeros(n)
+    lib().oracle_counter_uniforms(step, substep, seed, index, n, _d(out))
+    return out
+
+
+def counter_normals(step, substep, seed, index, n):
+    out = np.zeros(n)
+    lib().oracle_counter_normals(step, substep, seed, index, n, _d(out))
+    return out
+
+
+def counter_ball(step, substep, seed, index, dim, radius, n):
+    out = np.zeros((n, dim))
+    lib().oracle_counter_ball(step, substep, seed, index, dim, radius, n, _d(out))
+    return out
+
+
+def cbrt(x: float) -> float:
+    return lib().oracle_cbrt(x)
+
+
+def ziggurat_tables():
+    x = np.zeros(257)
+    f = np.zeros(257)
+    lib().oracle_ziggurat_tables(_d(x), _d(f))
+    return x, f
+
+
+# ---- boundary / checkerboard ------------------------------------------------------
+def wrap(point, edge_lengths):
+    p = _f64(point).copy()
+    L = _f64(edge_lengths)
+    lib().oracle_wrap(len(L), _d(L), _d(p))
+    return p
+
+
+def generate_ghosts(point, edge_lengths, rng):
+    L = _f64(edge_lengths)
+    p = _f64(point)
+    out = np.zeros(7 * len(L))
+    n = lib().oracle_generate_ghosts(len(L), _d(L), rng, _d(p), _d(out))
+    return out[: n * len(L)].reshape(n, len(L))
+
+
+def checkerboard_dimensions(edge_lengths, rng, periodic):
+    L = _f64(edge_lengths)
+    w = np.zeros(len(L))
+    s = np.zeros(len(L), dtype=np.uint64)
+    rc = lib().oracle_checkerboard_dimensions(len(L), _d(L), rng, int(periodic), _d(w), s.ctypes.data_as(_u64p))
+    if rc:
+        raise ValueError("interaction range too large for the boundary")
+    return w, s
+
+
+def point_to_space_index(origin, width, shape, periodic, point):
+    o = _f64(origin)
+    w = _f64(width)
+    s = np.ascontiguousarray(shape, dtype=np.uint64)
+    p = _f64(point)
+    r = lib().oracle_point_to_space_index(len(o), _d(o), _d(w), s.ctypes.data_as(_u64p), int(periodic), _d(p))
+    return None if r < 0 else int(r)
+
+
+def space_indices_by_color(shape):
+    s = np.ascontiguousarray(shape, dtype=np.uint64)
+    total = int(np.prod(s))
+    out = np.zeros(total, dtype=np.uint64)
+    lib().oracle_space_indices_by_color(len(s), s.ctypes.data_as(_u64p), out.ctypes.data_as(_u64p))
+    return out.reshape(2 ** len(s), -1)
+
+
+def checkerboard_for_counter(edge_lengths, rng, step, substep, seed):
+    L = _f64(edge_lengths)
+    o = np.zeros(len(L))
+    w = np.zeros(len(L))
+    s = np.zeros(len(L), dtype=np.uint64)
+    rc = lib().oracle_checkerboard_for_counter(len(L), _d(L), rng, step, substep, seed, _d(o), _d(w),
+                                               s.ctypes.data_as(_u64p))
+    if rc:
+        raise ValueError("interaction range too large for the boundary")
+    return o, w, s
+
+
+# ---- geometry / potentials --------------------------------------------------------
+def convex_intersects_at_3d(verts_a, verts_b, v_ij, q_ij) -> bool:
+    a = _f64(verts_a)
+    b = _f64(verts_b)
+    v = _f64(v_ij)
+    q = _f64(q_ij)
+    return bool(lib().oracle_convex_intersects_at_3d(_d(a), len(a) // 3 if a.ndim == 1 else a.shape[0], _d(b),
+                                                     len(b) // 3 if b.ndim == 1 else b.shape[0], _d(v), _d(q)))
+
+
+def convex_intersects_at_2d(verts_a, verts_b, v_ij, theta) -> bool:
+    a = _f64(verts_a)
+    b = _f64(verts_b)
+    v = _f64(v_ij)
+    return bool(lib().oracle_convex_intersects_at_2d(_d(a), a.shape[0], _d(b), b.shape[0], _d(v), theta))
+
+
+def versor_from_axis_angle(axis, angle):
+    a = _f64(axis)
+    q = np.zeros(4)
+    lib().oracle_versor_from_axis_angle(_d(a), angle, _d(q))
+    return q
+
+
+def versor_combine(a, b):
+    a = _f64(a)
+    b = _f64(b)
+    o = np.zeros(4)
+    lib().oracle_versor_combine(_d(a), _d(b), _d(o))
+    return o
+
+
+def versor_rotate(q, v):
+    q = _f64(q)
+    v = _f64(v)
+    o = np.zeros(3)
+    lib().oracle_versor_rotate(_d(q), _d(v), _d(o))
+    return o
+
+
+def lj_energy(epsilon, sigma, r):
+    return lib().oracle_lj_energy(epsilon, sigma, r)
+
+
+def shifted_lj_pair(epsilon, sigma, r_cut, r_shift, r_squared):
+    return lib().oracle_shifted_lj_pair(epsilon, sigma, r_cut, r_shift, r_squared)
+
+
+# ---- systems -------------------------------------------------------------------
+class System:
+    """An oracle microstate: bodies in a periodic box with one pair interaction."""
+
+    def __init__(self, dim, edge_lengths, positions, orientations=None, *, step=0, substep=0, seed=0,
+                 interaction=HARD_SPHERE, diameter=1.0, vertices=None, lj_epsilon=1.0, lj_sigma=1.0,
+                 lj_r_cut=2.5, lj_r_shift=2.5, boundary_range=None):
+        self.dim = dim
+        self.L = _f64(edge_lengths)
+        pos = _f64(positions, (-1,))
+        self.n = pos.size // dim
+        self.interaction = interaction
+        ori = None if orientations is None else _f64(orientations, (-1,))
+        verts = None if vertices is None else _f64(vertices, (-1,))
+        nv = 0 if verts is None else verts.size // dim
+        if boundary_range is None:
+            if interaction == HARD_SPHERE:
+                boundary_range = diameter
+            elif interaction == LENNARD_JONES:
+                boundary_range = lj_r_cut
+            else:
+                boundary_range = 2.0 * float(np.sqrt(np.max(np.sum(verts.reshape(nv, dim) ** 2, axis=1))))
+        self.boundary_range = boundary_range
+        self._h = lib().oracle_system_create(dim, _d(self.L), self.n, _d(pos), _d(ori), step, substep, seed,
+                                             interaction, diameter, _d(verts), nv, lj_epsilon, lj_sigma,
+                                             lj_r_cut, lj_r_shift, boundary_range)
+        self.ori_len = 0 if interaction in (HARD_SPHERE, LENNARD_JONES) else (4 if dim == 3 else 1)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib().oracle_system_destroy(h)
+            self._h = None
+
+    def state(self):
+        pos = np.zeros((self.n, self.dim))
+        ori = np.zeros((self.n, self.ori_len)) if self.ori_len else None
+        step = C.c_uint64()
+        sub = C.c_uint32()
+        lib().oracle_get_state(self._h, _d(pos), _d(ori), C.byref(step), C.byref(sub))
+        return pos, ori, step.value, sub.value
+
+    def set_counter(self, step, substep):
+        lib().oracle_set_counter(self._h, step, substep)
+
+    def increment_step(self):
+        lib().oracle_increment_step(self._h)
+
+    def parallel_sweep(self, move, maximum, kt, body_interaction_range):
+        a = C.c_uint64()
+        r = C.c_uint64()
+        rc = lib().oracle_parallel_sweep(self._h, move, maximum, kt, body_interaction_range, C.byref(a),
+                                         C.byref(r))
+        if rc:
+            raise RuntimeError(f"oracle parallel sweep failed ({rc})")
+        return a.value, r.value
+
+    def serial_sweep(self, move, maximum, kt):
+        a = C.c_uint64()
+        r = C.c_uint64()
+        lib().oracle_serial_sweep(self._h, move, maximum, kt, C.byref(a), C.byref(r))
+        return a.value, r.value
+
+    def overlap_count(self) -> int:
+        return int(lib().oracle_overlap_count(self._h))
+
+    def total_energy(self) -> float:
+        return float(lib().oracle_total_energy(self._h))
+
+    def delta_energy_one(self, body, position, orientation=None):
+        p = _f64(position)
+        o = None if orientation is None else _f64(orientation)
+        return lib().oracle_delta_energy_one(self._h, body, _d(p), _d(o))
+
+    def eval_moves(self, bodies, positions, orientations, u, kt):
+        b = np.ascontiguousarray(bodies, dtype=np.uint64)
+        n = b.size
+        p = _f64(positions, (-1,))
+        o = None if orientations is None else _f64(orientations, (-1,))
+        uu = _f64(u)
+        dec = np.zeros(n, dtype=np.uint8)
+        dh = np.zeros(n)
+        lib().oracle_eval_moves(self._h, n, b.ctypes.data_as(_u64p), _d(p), _d(o), _d(uu), kt,
+                                dec.ctypes.data_as(_u8p), _d(dh))
+        return dec.astype(bool), dh

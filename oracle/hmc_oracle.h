@@ -1,0 +1,120 @@
+// CPU oracle for the hoomd-mc local-move sweep.
+//
+// TEST INFRASTRUCTURE ONLY. This is a plain FP64 C++ restatement of the
+// reference's sweep path (glotzerlab/hoomd-rs v1.4.0, hoomd-mc and the crates it
+// calls), used as the checker for the CUDA library in tests/, by
+// __graft_entry__.smoke() and as the timed CPU baseline in bench.py. Nothing in
+// the shipped library links, loads or calls it.
+//
+// It is compiled with -ffp-contract=off so that every product and sum rounds
+// exactly where the reference's Rust code rounds; std::fma is called exactly
+// where the reference calls f64::mul_add.
+//
+// All entry points use plain C types so that Python's ctypes can drive them.
+#ifndef HMC_ORACLE_H
+#define HMC_ORACLE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+// ---- random numbers (hoomd-rand/src/sfc.rs, counter.rs) -----------------------
+void oracle_sfc64_outputs(uint64_t a, uint64_t b, uint64_t c, uint64_t counter, uint64_t n_skip,
+                          uint64_t n, uint64_t* out);
+void oracle_sfc64_seed_from_u64(uint64_t state, uint64_t n_skip, uint64_t n, uint64_t* out);
+void oracle_counter_outputs(uint64_t step, uint32_t substep, uint32_t seed, uint64_t index,
+                            uint64_t n, uint64_t* out);
+// Uniform f64 in [0, 1), standard normals and ball displacements from a counter stream.
+void oracle_counter_uniforms(uint64_t step, uint32_t substep, uint32_t seed, uint64_t index,
+                             uint64_t n, double* out);
+void oracle_counter_normals(uint64_t step, uint32_t substep, uint32_t seed, uint64_t index,
+                            uint64_t n, double* out);
+void oracle_counter_ball(uint64_t step, uint32_t substep, uint32_t seed, uint64_t index,
+                         uint32_t dim, double radius, uint64_t n, double* out);
+uint32_t oracle_counter_choose(uint64_t step, uint32_t substep, uint32_t seed, uint64_t index,
+                               uint32_t len);
+double oracle_cbrt(double x);
+void oracle_sincos_half(double theta, double* s, double* c);
+void oracle_ziggurat_tables(double* x_out /*257*/, double* f_out /*257*/);
+
+// ---- boundary and checkerboard (hoomd-microstate boundary, hoomd-mc hypercuboid.rs) ----
+void oracle_wrap(uint32_t dim, const double* edge_lengths, double* point);
+// Returns the number of ghosts written (<= 7); ghosts holds dim doubles each.
+uint32_t oracle_generate_ghosts(uint32_t dim, const double* edge_lengths, double range,
+                                const double* point, double* ghosts);
+// Returns 0 on success, 1 when the range is too large (the reference panics).
+int oracle_checkerboard_dimensions(uint32_t dim, const double* edge_lengths, double range,
+                                   int periodic, double* space_width, uint64_t* shape);
+int64_t oracle_point_to_space_index(uint32_t dim, const double* origin, const double* space_width,
+                                    const uint64_t* shape, int periodic, const double* point);
+// Writes 2^dim colours x (num_spaces / 2^dim) indices.
+void oracle_space_indices_by_color(uint32_t dim, const uint64_t* shape, uint64_t* out);
+// Checkerboard used by ParallelSweep for the counter (step, substep, seed).
+int oracle_checkerboard_for_counter(uint32_t dim, const double* edge_lengths, double range,
+                                    uint64_t step, uint32_t substep, uint32_t seed,
+                                    double* origin, double* space_width, uint64_t* shape);
+
+// ---- geometry (hoomd-geometry) -----------------------------------------------------
+// Convex::intersects_at in the local frame (v_ij, o_ij); q = (s, x, y, z) in 3-D,
+// o_ij = theta in 2-D.
+int oracle_convex_intersects_at_3d(const double* verts_a, uint32_t nv_a, const double* verts_b,
+                                   uint32_t nv_b, const double* v_ij, const double* q_ij);
+int oracle_convex_intersects_at_2d(const double* verts_a, uint32_t nv_a, const double* verts_b,
+                                   uint32_t nv_b, const double* v_ij, double theta_ij);
+int oracle_convex_intersects_at_global_3d(const double* verts, uint32_t nv, const double* r_i,
+                                          const double* q_i, const double* r_j,
+                                          const double* q_j);
+void oracle_versor_from_axis_angle(const double* axis, double angle, double* q);
+void oracle_versor_combine(const double* a, const double* b, double* out);
+void oracle_versor_rotate(const double* q, const double* v, double* out);
+double oracle_lj_energy(double epsilon, double sigma, double r);
+double oracle_shifted_lj_pair(double epsilon, double sigma, double r_cut, double r_shift,
+                              double r_squared);
+
+// ---- systems --------------------------------------------------------------------
+enum { ORACLE_HARD_SPHERE = 0, ORACLE_HARD_CONVEX_POLYGON = 1, ORACLE_HARD_CONVEX_POLYHEDRON = 2,
+       ORACLE_LENNARD_JONES = 3 };
+enum { ORACLE_TRANSLATE = 0, ORACLE_ROTATE = 1 };
+
+typedef struct oracle_system oracle_system;
+
+// positions: n*dim doubles; orientations: n*4 (3-D versor s,x,y,z) or n (2-D angle) or NULL.
+oracle_system* oracle_system_create(uint32_t dim, const double* edge_lengths, uint64_t n,
+                                    const double* positions, const double* orientations,
+                                    uint64_t step, uint32_t substep, uint32_t seed,
+                                    uint32_t interaction, double diameter,
+                                    const double* vertices, uint32_t n_vertices, double lj_epsilon,
+                                    double lj_sigma, double lj_r_cut, double lj_r_shift,
+                                    double boundary_range);
+void oracle_system_destroy(oracle_system* s);
+void oracle_get_state(const oracle_system* s, double* positions, double* orientations,
+                      uint64_t* step, uint32_t* substep);
+void oracle_set_counter(oracle_system* s, uint64_t step, uint32_t substep);
+void oracle_increment_step(oracle_system* s);
+
+// ParallelSweep::apply (parallel_sweep.rs:390-421). Returns 0, or 1 on a checkerboard error.
+int oracle_parallel_sweep(oracle_system* s, uint32_t move, double maximum, double kt,
+                          double body_interaction_range, uint64_t* accepted, uint64_t* rejected);
+// Sweep::apply (sweep.rs:159-224).
+int oracle_serial_sweep(oracle_system* s, uint32_t move, double maximum, double kt,
+                        uint64_t* accepted, uint64_t* rejected);
+// Number of overlapping pairs (hard) / total energy (LJ), pairs with tag_i < tag_j
+// (pairwise_cutoff.rs:720-745).
+uint64_t oracle_overlap_count(const oracle_system* s);
+double oracle_total_energy(const oracle_system* s);
+// delta_energy_one for one trial body (pairwise_cutoff.rs:919-941).
+double oracle_delta_energy_one(const oracle_system* s, uint64_t body, const double* position,
+                               const double* orientation);
+// Metropolis decisions for injected moves: (body, trial properties, u). u < 0 means the
+// decision needs no uniform (hard shapes). Returns decisions in out (0/1) and delta_h.
+void oracle_eval_moves(const oracle_system* s, uint64_t n, const uint64_t* bodies,
+                       const double* positions, const double* orientations, const double* u,
+                       double kt, uint8_t* decisions, double* delta_h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
