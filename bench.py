@@ -1,0 +1,327 @@
+#!/usr/bin/env python
+"""Throughput of the hoomd-mc hard-sphere sweep on B200: trial moves per second.
+
+Workload (one step = one ParallelSweep::apply, i.e. at least N trial moves):
+3-D hard spheres (sigma = 1), N = 2^20, periodic cubic box at packing fraction 0.50,
+FCC start with seeded jitter 0.01 sigma, translation moves with the maximum distance
+tuned to ~30 % acceptance. The headline runs the FP32 pair test with FP64 recheck; the
+plain FP64 sweep runs on an identical copy of the state and must end bit-identical
+(mismatches = 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (torchrun), every rank runs an independent replica (different seed) on its
+own GPU; there is no data-path collective. Prints one JSON line on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "trial moves/s, 1 B200: FP32+FP64-recheck vs plain FP64, 0 mismatches; CPU ref"
+UNIT = "trial moves/s"
+N_BODIES = 1 << 20
+PHI = 0.50
+SEED = 0x5EED0002
+TARGET_ACCEPTANCE = 0.30
+
+
+def workload_config(d, extra=None):
+    cfg = {"workload": "3-D hard spheres, N=2^20, packing fraction 0.50, periodic cube, FCC start + 0.01 jitter, "
+                       "translation moves tuned to ~30% acceptance, one ParallelSweep per step",
+           "n_bodies": N_BODIES, "packing_fraction": PHI, "box_length": None, "move_size": d,
+           "seed": SEED, "l2": "flushed before every timed step (256 MiB device write)"}
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+def tune_move(micro, d, precision, rounds=12):
+    """tune_by_scaling (hoomd-mc/src/lib.rs:514-524) applied to whole-sweep counts."""
+    from hoomd_rs_b200 import TRANSLATE
+    for _ in range(rounds):
+        c = micro.sweep(TRANSLATE, d, 1.0, precision, n_sweeps=1, increment_step=False)
+        d *= (c.acceptance_ratio() + 1.5) / (TARGET_ACCEPTANCE + 1.5)
+    return d
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak_hbm():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def cpu_baseline(pos, L, d, seconds=12.0):
+    """The oracle's ParallelSweep (a C++ port of the reference) on one host core."""
+    import oracle
+    o = oracle.System(3, [L] * 3, pos, diameter=1.0, seed=SEED)
+    trials, t0, sweeps = 0, time.perf_counter(), 0
+    while True:
+        a, r = o.parallel_sweep(oracle.TRANSLATE, d, 1.0, 1.0)
+        o.increment_step()
+        trials += a + r
+        sweeps += 1
+        el = time.perf_counter() - t0
+        if el >= seconds or sweeps >= 8:
+            break
+    return {"value": trials / el, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{sweeps} ParallelSweep sweeps of the same 2^20-sphere state ({trials} trial moves, "
+                      f"{el:.1f} s)"}
+
+
+def run_reference(args, rank):
+    """--impl reference: the CPU restatement of ParallelSweep (oracle/), timed on host cores."""
+    if rank != 0:
+        return
+    import oracle
+    from hoomd_rs_b200 import lattice
+    pos, L = lattice.hard_sphere_box(N_BODIES, PHI, 3, SEED)
+    d = 0.26  # the tuned move size of the GPU arm at this state (~30 % acceptance)
+    o = oracle.System(3, [L] * 3, pos, diameter=1.0, seed=SEED)
+    for _ in range(args.warmup):
+        o.parallel_sweep(oracle.TRANSLATE, d, 1.0, 1.0)
+        o.increment_step()
+    times, trials = [], 0
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        a, r = o.parallel_sweep(oracle.TRANSLATE, d, 1.0, 1.0)
+        times.append(time.perf_counter() - t0)
+        o.increment_step()
+        trials += a + r
+    total = sum(times)
+    v = trials / total
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config(d, {"box_length": L, "precision": "fp64 (CPU)"}),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
+                             "sample": f"{args.steps} full ParallelSweep sweeps of 2^20 spheres on one host thread"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import torch
+    import torch.distributed as dist
+    from hoomd_rs_b200 import FP32_RECHECK, FP64, TRANSLATE, Context, HardSphere, Microstate, PairwiseCutoff, Periodic
+    from hoomd_rs_b200 import lattice
+
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    ctx = Context(local_rank)
+    seed = SEED + rank
+    pos, L = lattice.hard_sphere_box(N_BODIES, PHI, 3, seed)
+    h = PairwiseCutoff(HardSphere(1.0))
+    tuner = Microstate(ctx, Periodic(1.0, [L] * 3), pos, h, seed=seed)
+    d = tune_move(tuner, 0.13, FP32_RECHECK)
+    start_pos, step0, _ = tuner.state()
+    tuner.close()
+
+    stream = torch.cuda.Stream()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def make_system():
+        m = Microstate(ctx, Periodic(1.0, [L] * 3), pos, h, seed=seed)
+        m.set_state(start_pos, step0, 0)
+        m.set_stream(stream.cuda_stream)
+        return m
+
+    def timed(m, precision, steps, warmup, profile=False):
+        for _ in range(warmup):
+            m.sweep(TRANSLATE, d, 1.0, precision, n_sweeps=1, increment_step=True)
+        if profile:
+            m.profile(enable=True, reset=True)
+        launches0 = m.profile()["kernel_launches"]
+        ms, acc, trials, rech, checks, maxerr = 0.0, 0, 0, 0, 0, 0.0
+        for _ in range(steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+            c = m.sweep(TRANSLATE, d, 1.0, precision, n_sweeps=1, increment_step=True)
+            e1.record(stream)
+            e1.synchronize()
+            ms += e0.elapsed_time(e1)
+            acc += c.accepted
+            trials += c.total()
+            rech += c.rechecks
+            checks += c.pair_checks
+            maxerr = max(maxerr, c.max_fp32_error)
+        prof = m.profile(enable=False)
+        return {"ms": ms, "trials": trials, "accepted": acc, "rechecks": rech, "pair_checks": checks,
+                "max_err": maxerr, "launches": prof["kernel_launches"] - launches0, "profile": prof}
+
+    a = make_system()
+    b = make_system()
+    sampler = ClockSampler(local_rank)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    ra = timed(a, FP32_RECHECK, args.steps, args.warmup, profile=True)
+    clocks = sampler.stop()
+    rb = timed(b, FP64, args.steps, args.warmup)
+    torch.cuda.synchronize()
+    pa, pb = a.positions(), b.positions()
+    mismatches = int(np.count_nonzero(np.any(pa != pb, axis=1)))
+    overlaps = a.overlap_count()
+
+    # whole-job aggregate: units of all ranks over the slowest rank's device time
+    t_max = ra["ms"]
+    trials_all = ra["trials"]
+    if world > 1:
+        t = torch.tensor([ra["ms"]], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max = float(t.item())
+        n = torch.tensor([ra["trials"]], dtype=torch.float64, device="cuda")
+        dist.all_reduce(n, op=dist.ReduceOp.SUM)
+        trials_all = int(n.item())
+    value = trials_all / (t_max / 1e3)
+    fp64_value = rb["trials"] / (rb["ms"] / 1e3)
+
+    # roofline of the dominant kernel (the colour-pass sweep), algorithmic bytes per launch
+    prof = ra["profile"]
+    launches = max(prof["sweep_launches"], 1)
+    t_launch = prof["sweep_ms"] / 1e3 / launches
+    shape = math.floor(L / 1.0)
+    shape -= shape % 2  # compute_dimensions (hoomd-mc/src/hypercuboid.rs:188-228)
+    cells = shape ** 3
+    trials_per_launch = ra["trials"] / launches
+    acc_per_launch = ra["accepted"] / launches
+    bytes_per_launch = N_BODIES * 12 + (cells + 1) * 4 + trials_per_launch * 24 + acc_per_launch * 84
+    peak, peak_kind = measured_peak_hbm()
+    achieved = bytes_per_launch / t_launch / 1e9
+
+    # end to end through the C ABI with host buffers: upload, sweep, download every step
+    e2e_steps = max(3, min(args.steps, 10))
+    host = np.ascontiguousarray(pa)
+    e2e_trials, t_e2e = 0, 0.0
+    for _ in range(e2e_steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        a.set_state(host, a.step(), 0)
+        c = a.sweep(TRANSLATE, d, 1.0, FP32_RECHECK, n_sweeps=1, increment_step=True)
+        host = a.positions()
+        t_e2e += time.perf_counter() - t0
+        e2e_trials += c.total()
+    e2e_value = e2e_trials / t_e2e
+    if world > 1:
+        t = torch.tensor([t_e2e], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_value = e2e_trials * world / float(t.item())
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "fp32 pair test + fp64 recheck (fp64 state)", "data": "synthetic",
+        "config": workload_config(d, {"box_length": L, "precision": "fp32_recheck", "replicas": world}),
+        "fp64": {"value": fp64_value, "ms_per_step": rb["ms"] / args.steps,
+                 "speedup_fp32_recheck_over_fp64": value / world / fp64_value if world == 1 else None},
+        "mismatches": mismatches, "overlaps_after": overlaps,
+        "acceptance": ra["accepted"] / max(ra["trials"], 1),
+        "recheck_fraction": ra["rechecks"] / max(ra["pair_checks"], 1), "max_fp32_error": ra["max_err"],
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "kernel": "k_sweep_sphere<3,fp32>",
+                     "bytes_per_launch": bytes_per_launch, "launch_ms": t_launch * 1e3,
+                     "peak_source": f"{peak_kind} hbm_gbs"},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": N_BODIES * 3 * 8,
+                "d2h_bytes_per_step": N_BODIES * 3 * 8},
+        "gpu_launches": ra["launches"],
+        "clocks": clocks,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(start_pos, L, d)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    a.close()
+    b.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

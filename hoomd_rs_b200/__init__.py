@@ -1,0 +1,343 @@
+"""B200-native Monte Carlo sweep for hoomd-rs's hoomd-mc, driven through its C ABI.
+
+The compute lives in ``libhmc_b200.so`` (CUDA kernels for sm_100a behind the C ABI in
+``include/hmc.h``). This module loads that library with ctypes and mirrors the
+reference's Rust API on the sweep path so that a caller reads like hoomd-rs code::
+
+    from hoomd_rs_b200 import (Context, HardSphere, Isothermal, Microstate, PairwiseCutoff,
+                               ParallelSweep, Periodic, Translate)
+
+    ctx = Context()
+    hamiltonian = PairwiseCutoff(HardSphere(diameter=1.0))
+    microstate = Microstate(ctx, Periodic(1.0, [L, L, L]), positions, hamiltonian, seed=1)
+    sweep = ParallelSweep(1.0, Translate.with_maximum_distance(0.1))
+    count = sweep.apply(microstate, hamiltonian, Isothermal(temperature=1.0))
+    microstate.increment_step()
+
+There is no CPU fallback: if the library cannot be loaded, importing the module raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+from typing import Optional, Sequence
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libhmc_b200.so")
+
+# hmc_status
+OK, INVALID_ARGUMENT, RANGE_TOO_LARGE, OVERLAP_IN_INPUT, CELL_OVERFLOW, NAN_STATE, ITERATION_CAP, TIMEOUT, \
+    CUDA_ERROR, OUT_OF_MEMORY, NOT_SUPPORTED, OUTSIDE_CHECKERBOARD = range(12)
+# hmc_interaction / hmc_move / hmc_precision
+HARD_SPHERE, HARD_CONVEX_POLYGON, HARD_CONVEX_POLYHEDRON, LENNARD_JONES = range(4)
+TRANSLATE, ROTATE = range(2)
+FP64, FP32_RECHECK = range(2)
+
+
+class HmcError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"hmc status {status}: {message}")
+        self.status = status
+
+
+class hmc_device_opts(C.Structure):
+    _fields_ = [("struct_size", C.c_uint32), ("device", C.c_int32)]
+
+
+class hmc_system_desc(C.Structure):
+    _fields_ = [("struct_size", C.c_uint32), ("dim", C.c_uint32), ("edge_lengths", C.c_double * 3),
+                ("n_bodies", C.c_uint64), ("step", C.c_uint64), ("substep", C.c_uint32), ("seed", C.c_uint32),
+                ("interaction", C.c_uint32), ("n_vertices", C.c_uint32), ("vertices", C.POINTER(C.c_double)),
+                ("diameter", C.c_double), ("lj_epsilon", C.c_double), ("lj_sigma", C.c_double),
+                ("lj_r_cut", C.c_double), ("lj_r_shift", C.c_double), ("boundary_range", C.c_double),
+                ("body_interaction_range", C.c_double)]
+
+
+class hmc_sweep_params(C.Structure):
+    _fields_ = [("struct_size", C.c_uint32), ("move", C.c_uint32), ("maximum", C.c_double),
+                ("temperature", C.c_double), ("precision", C.c_uint32), ("n_sweeps", C.c_uint32),
+                ("increment_step", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+class hmc_count(C.Structure):
+    _fields_ = [("accepted", C.c_uint64), ("rejected", C.c_uint64), ("rechecks", C.c_uint64),
+                ("pair_checks", C.c_uint64), ("max_fp32_error", C.c_double)]
+
+
+class hmc_injected_move(C.Structure):
+    _fields_ = [("body", C.c_uint64), ("position", C.c_double * 3), ("orientation", C.c_double * 4),
+                ("u", C.c_double)]
+
+
+class hmc_profile(C.Structure):
+    _fields_ = [("kernel_launches", C.c_uint64), ("sweep_launches", C.c_uint64), ("sweep_ms", C.c_double),
+                ("rebuild_launches", C.c_uint64), ("rebuild_ms", C.c_double), ("sweeps", C.c_uint64)]
+
+
+# Every function that include/hmc.h declares: name -> (restype, argtypes).
+_vp = C.c_void_p
+_dp = C.POINTER(C.c_double)
+_u8p = C.POINTER(C.c_uint8)
+SIGNATURES = {
+    "hmc_abi_version": (C.c_uint32, []),
+    "hmc_status_string": (C.c_char_p, [C.c_int]),
+    "hmc_last_error_message": (C.c_char_p, []),
+    "hmc_context_create": (C.c_int, [C.POINTER(hmc_device_opts), C.POINTER(_vp)]),
+    "hmc_context_destroy": (None, [_vp]),
+    "hmc_system_create": (C.c_int, [_vp, C.POINTER(hmc_system_desc), _dp, _dp, C.POINTER(_vp)]),
+    "hmc_system_destroy": (None, [_vp]),
+    "hmc_system_set_stream": (C.c_int, [_vp, _vp]),
+    "hmc_system_stream": (_vp, [_vp]),
+    "hmc_set_state": (C.c_int, [_vp, _dp, _dp, C.c_uint64, C.c_uint32]),
+    "hmc_get_state": (C.c_int, [_vp, _dp, _dp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32)]),
+    "hmc_sweep": (C.c_int, [_vp, C.POINTER(hmc_sweep_params), C.POINTER(hmc_count)]),
+    "hmc_tune": (C.c_int, [_vp, C.POINTER(hmc_sweep_params), C.c_double, C.c_uint32, C.c_uint32]),
+    "hmc_overlap_check": (C.c_int, [_vp, C.POINTER(C.c_uint64)]),
+    "hmc_eval_moves": (C.c_int, [_vp, C.POINTER(hmc_injected_move), C.c_uint64, C.c_double, C.c_uint32, _u8p,
+                                 _u8p]),
+    "hmc_profile_enable": (C.c_int, [_vp, C.c_int]),
+    "hmc_profile_read": (C.c_int, [_vp, C.POINTER(hmc_profile), C.c_int]),
+}
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Load libhmc_b200.so and bind every C-ABI symbol. Raises if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(f"{path} is missing: build it with `python -m hoomd_rs_b200.build` "
+                          "(there is no CPU fallback)")
+    lib = C.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _check(status: int):
+    if status != OK:
+        msg = _lib.hmc_last_error_message().decode()
+        raise HmcError(status, msg)
+
+
+class Context:
+    """A CUDA device context (hmc_context)."""
+
+    def __init__(self, device: int = 0):
+        lib = load_library()
+        opts = hmc_device_opts(C.sizeof(hmc_device_opts), device)
+        h = _vp()
+        _check(lib.hmc_context_create(C.byref(opts), C.byref(h)))
+        self._h = h
+        self.device = device
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.hmc_context_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+
+# ---- mirrors of the reference's types ---------------------------------------------------------
+@dataclass
+class HardSphere:
+    """hoomd_interaction::pairwise::HardSphere (hard_shape.rs:128-175)."""
+    diameter: float = 1.0
+
+    @property
+    def maximum_interaction_range(self) -> float:
+        return self.diameter
+
+
+@dataclass
+class PairwiseCutoff:
+    """hoomd_interaction::PairwiseCutoff (pairwise_cutoff.rs:140)."""
+    pair: HardSphere
+
+
+@dataclass
+class Periodic:
+    """hoomd_microstate::boundary::Periodic<Hypercuboid<N>> (boundary/periodic.rs:65-107)."""
+    maximum_interaction_range: float
+    edge_lengths: Sequence[float]
+
+
+@dataclass
+class Isothermal:
+    """hoomd_simulation::macrostate::Isothermal (macrostate.rs:109)."""
+    temperature: float = 1.0
+
+
+@dataclass
+class Count:
+    """hoomd_mc::Count (lib.rs:206-294), plus the FP32 recheck statistics."""
+    accepted: int = 0
+    rejected: int = 0
+    rechecks: int = 0
+    pair_checks: int = 0
+    max_fp32_error: float = 0.0
+
+    def total(self) -> int:
+        return self.accepted + self.rejected
+
+    def acceptance_ratio(self) -> Optional[float]:
+        t = self.total()
+        return self.accepted / t if t > 0 else None
+
+
+@dataclass
+class Translate:
+    """hoomd_mc::Translate (translate.rs:41, translate/cartesian.rs:40-51)."""
+    maximum_distance: float
+
+    @classmethod
+    def with_maximum_distance(cls, d: float) -> "Translate":
+        return cls(float(d))
+
+
+class Microstate:
+    """Bodies in a periodic box, resident on the GPU (one hmc_system)."""
+
+    def __init__(self, ctx: Context, boundary: Periodic, positions, hamiltonian: PairwiseCutoff, *,
+                 step: int = 0, substep: int = 0, seed: int = 0, body_interaction_range: float = 0.0):
+        lib = load_library()
+        L = [float(x) for x in boundary.edge_lengths]
+        self.dim = len(L)
+        pos = np.ascontiguousarray(positions, dtype=np.float64).reshape(-1, self.dim)
+        self.n = pos.shape[0]
+        d = hmc_system_desc()
+        d.struct_size = C.sizeof(hmc_system_desc)
+        d.dim = self.dim
+        for a, x in enumerate(L):
+            d.edge_lengths[a] = x
+        d.n_bodies = self.n
+        d.step, d.substep, d.seed = step, substep, seed
+        pair = hamiltonian.pair
+        if isinstance(pair, HardSphere):
+            d.interaction = HARD_SPHERE
+            d.diameter = pair.diameter
+        else:
+            raise HmcError(NOT_SUPPORTED, f"{type(pair).__name__}")
+        d.boundary_range = boundary.maximum_interaction_range
+        d.body_interaction_range = body_interaction_range
+        h = _vp()
+        _check(lib.hmc_system_create(ctx._h, C.byref(d), pos.ctypes.data_as(_dp), None, C.byref(h)))
+        self._h = h
+        self._ctx = ctx  # keep the context alive
+        self.edge_lengths = L
+        self.hamiltonian = hamiltonian
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.hmc_system_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    # microstate.rs:412-455
+    def state(self):
+        pos = np.zeros((self.n, self.dim))
+        step = C.c_uint64()
+        sub = C.c_uint32()
+        _check(_lib.hmc_get_state(self._h, pos.ctypes.data_as(_dp), None, C.byref(step), C.byref(sub)))
+        return pos, step.value, sub.value
+
+    def positions(self) -> np.ndarray:
+        return self.state()[0]
+
+    def step(self) -> int:
+        return self.state()[1]
+
+    def substep(self) -> int:
+        return self.state()[2]
+
+    def set_state(self, positions, step: int, substep: int):
+        pos = np.ascontiguousarray(positions, dtype=np.float64).reshape(self.n, self.dim)
+        _check(_lib.hmc_set_state(self._h, pos.ctypes.data_as(_dp), None, step, substep))
+
+    def increment_step(self):
+        pos, step, _ = self.state()
+        _check(_lib.hmc_set_state(self._h, pos.ctypes.data_as(_dp), None, step + 1, 0))
+
+    def overlap_count(self) -> int:
+        n = C.c_uint64()
+        _check(_lib.hmc_overlap_check(self._h, C.byref(n)))
+        return n.value
+
+    def stream(self) -> int:
+        return _lib.hmc_system_stream(self._h) or 0
+
+    def profile(self, enable: Optional[bool] = None, reset: bool = False) -> dict:
+        if enable is not None:
+            _check(_lib.hmc_profile_enable(self._h, int(enable)))
+        p = hmc_profile()
+        _check(_lib.hmc_profile_read(self._h, C.byref(p), int(reset)))
+        return {f: getattr(p, f) for f, _ in hmc_profile._fields_}
+
+    def set_stream(self, stream_ptr: int):
+        _check(_lib.hmc_system_set_stream(self._h, C.c_void_p(stream_ptr)))
+
+    def sweep(self, move: int, maximum: float, temperature: float, precision: int, n_sweeps: int = 1,
+              increment_step: bool = False) -> Count:
+        p = hmc_sweep_params(C.sizeof(hmc_sweep_params), move, maximum, temperature, precision, n_sweeps,
+                             int(increment_step), 0)
+        c = hmc_count()
+        _check(_lib.hmc_sweep(self._h, C.byref(p), C.byref(c)))
+        return Count(c.accepted, c.rejected, c.rechecks, c.pair_checks, c.max_fp32_error)
+
+    def eval_moves(self, bodies, positions, u=None, temperature: float = 1.0, precision: int = FP64):
+        bodies = np.asarray(bodies, dtype=np.uint64)
+        pos = np.asarray(positions, dtype=np.float64).reshape(len(bodies), self.dim)
+        n = len(bodies)
+        moves = (hmc_injected_move * n)()
+        for i in range(n):
+            moves[i].body = int(bodies[i])
+            for a in range(self.dim):
+                moves[i].position[a] = pos[i, a]
+            moves[i].u = -1.0 if u is None else float(u[i])
+        dec = np.zeros(n, dtype=np.uint8)
+        rech = np.zeros(n, dtype=np.uint8)
+        _check(_lib.hmc_eval_moves(self._h, moves, n, temperature, precision, dec.ctypes.data_as(_u8p),
+                                   rech.ctypes.data_as(_u8p)))
+        return dec.astype(bool), rech.astype(bool)
+
+
+class ParallelSweep:
+    """hoomd_mc::ParallelSweep (parallel_sweep.rs:83-421) executed on the GPU.
+
+    ``precision`` selects the plain FP64 pair test (``FP64``) or the FP32 test with FP64
+    recheck inside the forward-error bound (``FP32_RECHECK``); both give the same decisions.
+    """
+
+    def __init__(self, body_interaction_range: float, local_trial: Translate, precision: int = FP32_RECHECK):
+        self.body_interaction_range = float(body_interaction_range)
+        self.local_trial = local_trial
+        self.precision = precision
+        self.last_count: Optional[Count] = None
+
+    def apply(self, microstate: Microstate, hamiltonian: PairwiseCutoff, macrostate: Isothermal) -> Count:
+        if hamiltonian is not microstate.hamiltonian and hamiltonian != microstate.hamiltonian:
+            raise HmcError(INVALID_ARGUMENT, "the hamiltonian differs from the one the microstate was built with")
+        if isinstance(self.local_trial, Translate):
+            move, maximum = TRANSLATE, self.local_trial.maximum_distance
+        else:
+            raise HmcError(NOT_SUPPORTED, type(self.local_trial).__name__)
+        c = microstate.sweep(move, maximum, macrostate.temperature, self.precision)
+        self.last_count = c
+        return c
+
+
+__all__ = ["Context", "Count", "HardSphere", "HmcError", "Isothermal", "Microstate", "PairwiseCutoff",
+           "ParallelSweep", "Periodic", "Translate", "load_library", "SIGNATURES", "FP64", "FP32_RECHECK",
+           "TRANSLATE", "ROTATE"]

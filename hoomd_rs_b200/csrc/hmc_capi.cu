@@ -1,0 +1,551 @@
+// C ABI of libhmc_b200.so (declared in include/hmc.h): contexts, systems, state transfer
+// and the host side of ParallelSweep::apply (hoomd-mc/src/parallel_sweep.rs:390-421).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/hmc.h"
+#include "hmc_internal.cuh"
+
+using namespace hmc;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+hmc_status fail(hmc_status st, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return st;
+}
+
+#define HMC_CUDA(call)                                                                                \
+    do {                                                                                              \
+        cudaError_t e_ = (call);                                                                      \
+        if (e_ != cudaSuccess)                                                                        \
+            return fail(e_ == cudaErrorMemoryAllocation ? HMC_OUT_OF_MEMORY : HMC_CUDA_ERROR, "%s: %s (%s:%d)", \
+                        #call, cudaGetErrorString(e_), __FILE__, __LINE__);                           \
+    } while (0)
+
+// HypercuboidCheckerboard::compute_dimensions for periodic axes (hypercuboid.rs:188-228).
+bool compute_dimensions(int dim, const double* L, double range, double* width, uint32_t* shape) {
+    for (int a = 0; a < dim; ++a) {
+        double f = std::floor(L[a] / range);
+        if (!(f >= 2.0) || f > 2.0e9) return false;
+        uint64_t inside = (uint64_t)f;
+        if (inside % 2 != 0) inside -= 1;
+        width[a] = L[a] / (double)inside;
+        shape[a] = (uint32_t)inside;
+    }
+    return true;
+}
+
+}  // namespace
+
+struct hmc_context {
+    int device = 0;
+    double* zig = nullptr;  // 2 x 257 doubles: x then f
+};
+
+struct hmc_system {
+    hmc_context* ctx = nullptr;
+    int dim = 3;
+    uint64_t n = 0;
+    uint64_t step = 0;
+    uint32_t substep = 0;
+    uint32_t seed = 0;
+    uint32_t interaction = HMC_HARD_SPHERE;
+    double pair_range = 1.0;
+    double boundary_range = 1.0;
+    double body_range = 1.0;
+    Geometry geom{};
+    Pair pair{};
+    Arrays arr{};
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    DeviceStats* host_stats = nullptr;  // pinned
+    std::vector<void*> allocations;
+    // profiling
+    bool profiling = false;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    hmc_profile prof{};
+};
+
+namespace {
+
+template <typename T>
+hmc_status dalloc(hmc_system* s, T** p, size_t count) {
+    *p = nullptr;
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMalloc((void**)p, sizeof(T) * count);
+    if (e != cudaSuccess)
+        return fail(e == cudaErrorMemoryAllocation ? HMC_OUT_OF_MEMORY : HMC_CUDA_ERROR, "cudaMalloc(%zu bytes): %s",
+                    sizeof(T) * count, cudaGetErrorString(e));
+    s->allocations.push_back((void*)*p);
+    return HMC_OK;
+}
+
+// The forward-error bound of the FP32 pair test for hard spheres. With u32 = 2^-24 and
+// u64 = 2^-53, a stored FP32 offset differs from the exact offset of the FP64 site by at
+// most u32*w + 4*u64*(L + w); the FP32 displacement of two offsets plus a cell shift
+// then differs from the exact displacement by E <= 8*u32*w + 16*u64*(L + w) per axis.
+// Near contact (d ~ sigma) the FP32 d^2 is within 2*E*sqrt(dim)*d + dim*E^2 + dim*u32*d^2
+// of the exact d^2, and the reference FP64 d^2 is within 6*u64*(L+w)*sqrt(dim)*d +
+// dim*u64*d^2 of it. A factor of two covers both and the rounding of the thresholds.
+void sphere_bound(hmc_system* s) {
+    const double u32 = std::ldexp(1.0, -24), u64 = std::ldexp(1.0, -53);
+    double wmax = 0, Lmax = 0;
+    for (int a = 0; a < s->dim; ++a) {
+        wmax = std::max(wmax, s->geom.width[a]);
+        Lmax = std::max(Lmax, s->geom.L[a]);
+    }
+    double sigma2 = s->pair.sigma2;
+    double sigma = std::sqrt(sigma2);
+    double E = 8.0 * u32 * wmax + 16.0 * u64 * (Lmax + wmax);
+    double rd = std::sqrt((double)s->dim);
+    double dmax = sigma * 1.01 + 1e-3;
+    double b32 = 2.0 * E * rd * dmax + s->dim * E * E + s->dim * u32 * dmax * dmax;
+    double b64 = 6.0 * u64 * (Lmax + wmax) * rd * dmax + s->dim * u64 * dmax * dmax;
+    double B = 2.0 * (b32 + b64);
+    s->pair.sig2_lo32 = std::nextafter((float)(sigma2 - B), -INFINITY);
+    s->pair.sig2_hi32 = std::nextafter((float)(sigma2 + B), INFINITY);
+}
+
+hmc_status read_stats(hmc_system* s) {
+    HMC_CUDA(cudaMemcpyAsync(s->host_stats, s->arr.stats, sizeof(DeviceStats), cudaMemcpyDeviceToHost, s->stream));
+    HMC_CUDA(cudaStreamSynchronize(s->stream));
+    return HMC_OK;
+}
+
+hmc_status check_flags(hmc_system* s) {
+    uint32_t f = s->host_stats->error_flags;
+    if (f & kErrNonFinite) return fail(HMC_NAN_STATE, "a body position is not finite");
+    if (f & kErrOutsideCheckerboard) return fail(HMC_OUTSIDE_CHECKERBOARD, "a body maps to no checkerboard space");
+    return HMC_OK;
+}
+
+// update_checkerboard (parallel_sweep.rs:176-201): origin shift from the counter's
+// index u64::MAX stream, then the device counting sort into cell order.
+hmc_status rebuild(hmc_system* s) {
+    Sfc64 rng = make_rng(s->step, s->substep, s->seed, UINT64_MAX);
+    for (int a = 0; a < s->dim; ++a) {
+        double off = uniform01(rng);
+        s->geom.origin[a] = -s->geom.L[a] / 2.0 - off * s->geom.width[a];
+    }
+    HMC_CUDA(cudaMemsetAsync(s->arr.stats, 0, sizeof(DeviceStats), s->stream));
+    HMC_CUDA(launch_rebuild(s->dim, s->geom, s->arr, (uint32_t)s->n, s->stream));
+    s->prof.kernel_launches += s->n > 0 ? 6 : 4;  // bin, 3 scan passes, scatter, finalize
+    return HMC_OK;
+}
+
+hmc_status validate_positions(const hmc_system* s, const double* pos) {
+    for (uint64_t i = 0; i < s->n * (uint64_t)s->dim; ++i)
+        if (!std::isfinite(pos[i])) return fail(HMC_NAN_STATE, "position %llu is not finite", (unsigned long long)(i / s->dim));
+    return HMC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+uint32_t hmc_abi_version(void) { return HMC_ABI_VERSION; }
+
+const char* hmc_status_string(hmc_status st) {
+    switch (st) {
+        case HMC_OK: return "ok";
+        case HMC_INVALID_ARGUMENT: return "invalid argument";
+        case HMC_RANGE_TOO_LARGE: return "interaction range too large for the box";
+        case HMC_OVERLAP_IN_INPUT: return "overlap in input";
+        case HMC_CELL_OVERFLOW: return "cell overflow";
+        case HMC_NAN_STATE: return "non-finite state";
+        case HMC_ITERATION_CAP: return "iteration cap reached";
+        case HMC_TIMEOUT: return "timeout";
+        case HMC_CUDA_ERROR: return "CUDA error";
+        case HMC_OUT_OF_MEMORY: return "out of device memory";
+        case HMC_NOT_SUPPORTED: return "not supported";
+        case HMC_OUTSIDE_CHECKERBOARD: return "body outside the checkerboard";
+    }
+    return "unknown status";
+}
+
+const char* hmc_last_error_message(void) { return g_last_error.c_str(); }
+
+hmc_status hmc_context_create(const hmc_device_opts* opts, hmc_context** out) {
+    if (!out) return fail(HMC_INVALID_ARGUMENT, "out is NULL");
+    *out = nullptr;
+    int device = 0;
+    if (opts) {
+        if (opts->struct_size < sizeof(hmc_device_opts)) return fail(HMC_INVALID_ARGUMENT, "hmc_device_opts.struct_size");
+        device = opts->device;
+    }
+    int count = 0;
+    HMC_CUDA(cudaGetDeviceCount(&count));
+    if (device < 0 || device >= count) return fail(HMC_INVALID_ARGUMENT, "device %d of %d", device, count);
+    HMC_CUDA(cudaSetDevice(device));
+    hmc_context* c = new hmc_context();
+    c->device = device;
+    ZigTables t;
+    zig_tables(t);
+    cudaError_t e = cudaMalloc((void**)&c->zig, sizeof(double) * 2 * (kZigLayers + 1));
+    if (e == cudaSuccess) e = cudaMemcpy(c->zig, t.x, sizeof(t.x), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(c->zig + kZigLayers + 1, t.f, sizeof(t.f), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        if (c->zig) cudaFree(c->zig);
+        delete c;
+        return fail(HMC_CUDA_ERROR, "context setup: %s", cudaGetErrorString(e));
+    }
+    *out = c;
+    return HMC_OK;
+}
+
+void hmc_context_destroy(hmc_context* c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->zig) cudaFree(c->zig);
+    delete c;
+}
+
+void hmc_system_destroy(hmc_system* s) {
+    if (!s) return;
+    cudaSetDevice(s->ctx->device);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    for (void* p : s->allocations) cudaFree(p);
+    for (cudaEvent_t e : s->ev)
+        if (e) cudaEventDestroy(e);
+    if (s->host_stats) cudaFreeHost(s->host_stats);
+    if (s->own_stream) cudaStreamDestroy(s->own_stream);
+    delete s;
+}
+
+hmc_status hmc_system_create(hmc_context* ctx, const hmc_system_desc* d, const double* positions,
+                             const double* orientations, hmc_system** out) {
+    if (!ctx || !d || !out) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
+    *out = nullptr;
+    if (d->struct_size < sizeof(hmc_system_desc)) return fail(HMC_INVALID_ARGUMENT, "hmc_system_desc.struct_size");
+    if (d->dim != 2 && d->dim != 3) return fail(HMC_INVALID_ARGUMENT, "dim must be 2 or 3 (got %u)", d->dim);
+    if (d->n_bodies > 0 && !positions) return fail(HMC_INVALID_ARGUMENT, "positions is NULL");
+    if (d->n_bodies >= (1ull << 31)) return fail(HMC_INVALID_ARGUMENT, "too many bodies");
+    for (uint32_t a = 0; a < d->dim; ++a)
+        if (!(d->edge_lengths[a] > 0.0) || !std::isfinite(d->edge_lengths[a]))
+            return fail(HMC_INVALID_ARGUMENT, "edge length %u must be positive", a);
+    if (d->interaction != HMC_HARD_SPHERE)
+        return fail(HMC_NOT_SUPPORTED, "interaction %u is not available in this build", d->interaction);
+    if (!(d->diameter > 0.0)) return fail(HMC_INVALID_ARGUMENT, "diameter must be positive");
+
+    HMC_CUDA(cudaSetDevice(ctx->device));
+    hmc_system* s = new hmc_system();
+    s->ctx = ctx;
+    s->dim = (int)d->dim;
+    s->n = d->n_bodies;
+    s->step = d->step;
+    s->substep = d->substep;
+    s->seed = d->seed;
+    s->interaction = d->interaction;
+    s->pair_range = d->diameter;  // HardSphere::maximum_interaction_range (hard_shape.rs:171-175)
+    s->boundary_range = d->boundary_range > 0.0 ? d->boundary_range : s->pair_range;
+    s->body_range = d->body_interaction_range > 0.0 ? d->body_interaction_range : s->pair_range;
+    for (int a = 0; a < 3; ++a) s->geom.L[a] = a < s->dim ? d->edge_lengths[a] : 1.0;
+    double min_l = s->geom.L[0];
+    for (int a = 0; a < s->dim; ++a) min_l = std::min(min_l, s->geom.L[a]);
+    auto destroy_fail = [&](hmc_status st) {
+        std::string msg = g_last_error;
+        hmc_system_destroy(s);
+        g_last_error = msg;
+        return st;
+    };
+    if (s->boundary_range > min_l / 2.0) {
+        fail(HMC_RANGE_TOO_LARGE, "boundary interaction range %g exceeds L/2 = %g", s->boundary_range, min_l / 2.0);
+        return destroy_fail(HMC_RANGE_TOO_LARGE);
+    }
+    if (s->body_range < s->pair_range) {
+        fail(HMC_INVALID_ARGUMENT, "body interaction range %g is below the pair range %g", s->body_range, s->pair_range);
+        return destroy_fail(HMC_INVALID_ARGUMENT);
+    }
+    if (!compute_dimensions(s->dim, s->geom.L, s->body_range, s->geom.width, s->geom.shape)) {
+        fail(HMC_RANGE_TOO_LARGE, "body interaction range %g leaves fewer than 2 spaces per axis", s->body_range);
+        return destroy_fail(HMC_RANGE_TOO_LARGE);
+    }
+    uint64_t cells = 1;
+    for (int a = 0; a < s->dim; ++a) {
+        s->geom.half[a] = s->geom.L[a] / 2.0;
+        s->geom.ghost_hi[a] = s->geom.half[a] - s->boundary_range;
+        s->geom.ghost_lo[a] = -s->geom.half[a] + s->boundary_range;
+        s->geom.w32[a] = (float)s->geom.width[a];
+        s->geom.half_shape[a] = s->geom.shape[a] / 2;
+        cells *= s->geom.shape[a];
+    }
+    if (cells > 16000000ull) {
+        fail(HMC_NOT_SUPPORTED, "%llu checkerboard spaces exceed the supported 16M", (unsigned long long)cells);
+        return destroy_fail(HMC_NOT_SUPPORTED);
+    }
+    s->geom.n_cells = (uint32_t)cells;
+    s->pair.sigma2 = d->diameter * d->diameter;  // diameter.powi(2)
+    sphere_bound(s);
+
+    cudaError_t e = cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        fail(HMC_CUDA_ERROR, "cudaStreamCreate: %s", cudaGetErrorString(e));
+        return destroy_fail(HMC_CUDA_ERROR);
+    }
+    s->stream = s->own_stream;
+    e = cudaMallocHost((void**)&s->host_stats, sizeof(DeviceStats));
+    if (e != cudaSuccess) {
+        fail(HMC_CUDA_ERROR, "cudaMallocHost: %s", cudaGetErrorString(e));
+        return destroy_fail(HMC_CUDA_ERROR);
+    }
+    uint64_t n = s->n;
+    hmc_status st = HMC_OK;
+    Arrays& A = s->arr;
+    uint32_t scan_blocks = (uint32_t)((cells + 2047) / 2048);
+    if ((st = dalloc(s, &A.body_pos, n)) || (st = dalloc(s, &A.sorted_b, n)) || (st = dalloc(s, &A.sorted_s, n)) ||
+        (st = dalloc(s, &A.sorted_off, n)) || (st = dalloc(s, &A.sorted_body, n)) ||
+        (st = dalloc(s, &A.slot_of_body, n)) || (st = dalloc(s, &A.body_cell, n)) ||
+        (st = dalloc(s, &A.body_rank, n)) || (st = dalloc(s, &A.cell_count, cells)) ||
+        (st = dalloc(s, &A.cell_start, cells + 1)) || (st = dalloc(s, &A.block_sums, scan_blocks)) ||
+        (st = dalloc(s, &A.stats, 1)))
+        return destroy_fail(st);
+    A.body_ori = nullptr;
+    A.sorted_q = nullptr;
+    A.zig_x = ctx->zig;
+    A.zig_f = ctx->zig + kZigLayers + 1;
+    if (n > 0) {
+        if ((st = validate_positions(s, positions))) return destroy_fail(st);
+        // Microstate::add_body (microstate.rs:777-835): the body keeps wrap(input).
+        std::vector<double4> host(n);
+        for (uint64_t i = 0; i < n; ++i) {
+            double p[3] = {0.0, 0.0, 0.0};
+            for (int a = 0; a < s->dim; ++a) p[a] = positions[i * s->dim + a];
+            if (s->dim == 2)
+                wrap<2>(s->geom.L, p);
+            else
+                wrap<3>(s->geom.L, p);
+            host[i] = make_double4(p[0], p[1], p[2], 0.0);
+        }
+        e = cudaMemcpy(A.body_pos, host.data(), sizeof(double4) * n, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) {
+            fail(HMC_CUDA_ERROR, "upload: %s", cudaGetErrorString(e));
+            return destroy_fail(HMC_CUDA_ERROR);
+        }
+    }
+    (void)orientations;
+    *out = s;
+    return HMC_OK;
+}
+
+hmc_status hmc_system_set_stream(hmc_system* s, void* stream) {
+    if (!s) return fail(HMC_INVALID_ARGUMENT, "NULL system");
+    HMC_CUDA(cudaStreamSynchronize(s->stream));
+    s->stream = stream ? (cudaStream_t)stream : s->own_stream;
+    return HMC_OK;
+}
+
+void* hmc_system_stream(hmc_system* s) { return s ? (void*)s->stream : nullptr; }
+
+hmc_status hmc_set_state(hmc_system* s, const double* positions, const double* orientations, uint64_t step,
+                         uint32_t substep) {
+    if (!s || (s->n > 0 && !positions)) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
+    hmc_status st = validate_positions(s, positions);
+    if (st) return st;
+    (void)orientations;
+    HMC_CUDA(cudaSetDevice(s->ctx->device));
+    // Positions are body positions as returned by hmc_get_state (already wrapped).
+    std::vector<double4> host(s->n);
+    for (uint64_t i = 0; i < s->n; ++i)
+        host[i] = make_double4(positions[i * s->dim], positions[i * s->dim + 1],
+                               s->dim == 3 ? positions[i * s->dim + 2] : 0.0, 0.0);
+    if (s->n) HMC_CUDA(cudaMemcpyAsync(s->arr.body_pos, host.data(), sizeof(double4) * s->n, cudaMemcpyHostToDevice, s->stream));
+    HMC_CUDA(cudaStreamSynchronize(s->stream));
+    s->step = step;
+    s->substep = substep;
+    return HMC_OK;
+}
+
+hmc_status hmc_get_state(hmc_system* s, double* positions, double* orientations, uint64_t* step,
+                         uint32_t* substep) {
+    if (!s) return fail(HMC_INVALID_ARGUMENT, "NULL system");
+    (void)orientations;
+    HMC_CUDA(cudaSetDevice(s->ctx->device));
+    if (positions && s->n) {
+        std::vector<double4> host(s->n);
+        HMC_CUDA(cudaMemcpyAsync(host.data(), s->arr.body_pos, sizeof(double4) * s->n, cudaMemcpyDeviceToHost, s->stream));
+        HMC_CUDA(cudaStreamSynchronize(s->stream));
+        for (uint64_t i = 0; i < s->n; ++i) {
+            positions[i * s->dim] = host[i].x;
+            positions[i * s->dim + 1] = host[i].y;
+            if (s->dim == 3) positions[i * s->dim + 2] = host[i].z;
+        }
+    }
+    if (step) *step = s->step;
+    if (substep) *substep = s->substep;
+    return HMC_OK;
+}
+
+hmc_status hmc_sweep(hmc_system* s, const hmc_sweep_params* p, hmc_count* out) {
+    if (!s || !p) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
+    if (p->struct_size < sizeof(hmc_sweep_params)) return fail(HMC_INVALID_ARGUMENT, "hmc_sweep_params.struct_size");
+    if (p->move != HMC_TRANSLATE) return fail(HMC_NOT_SUPPORTED, "hard spheres take translation moves only");
+    if (!(p->maximum > 0.0) || !std::isfinite(p->maximum)) return fail(HMC_INVALID_ARGUMENT, "maximum must be positive");
+    // The 2-D ball sampler squares the radius; keep it far from overflow. Moves longer
+    // than the box are equivalent modulo wrapping, so this rejects no useful input.
+    double lmax = 0.0;
+    for (int a = 0; a < s->dim; ++a) lmax = std::max(lmax, s->geom.L[a]);
+    if (p->maximum > 4.0 * lmax) return fail(HMC_INVALID_ARGUMENT, "maximum %g exceeds 4 box lengths", p->maximum);
+    if (!(p->temperature > 0.0)) return fail(HMC_INVALID_ARGUMENT, "temperature must be positive");
+    if (p->precision > HMC_FP32_RECHECK) return fail(HMC_INVALID_ARGUMENT, "precision");
+    HMC_CUDA(cudaSetDevice(s->ctx->device));
+    hmc_count total{};
+    const bool fp32 = p->precision == HMC_FP32_RECHECK;
+    const uint32_t colors = 1u << s->dim;
+    uint32_t n_active = 1;
+    for (int a = 0; a < s->dim; ++a) n_active *= s->geom.half_shape[a];
+    for (uint32_t sweep = 0; sweep < p->n_sweeps; ++sweep) {
+        if (s->profiling) HMC_CUDA(cudaEventRecord(s->ev[0], s->stream));
+        hmc_status st = rebuild(s);
+        if (st) return st;
+        if (s->profiling) HMC_CUDA(cudaEventRecord(s->ev[1], s->stream));
+        if ((st = read_stats(s))) return st;
+        if ((st = check_flags(s))) return st;
+        uint64_t nonempty = s->host_stats->nonempty;
+        // while count.total() < N: one trial per non-empty space per colour (:402-418)
+        uint64_t rounds = (s->n == 0) ? 0 : (s->n + nonempty - 1) / nonempty;
+        Launch L{};
+        L.step = s->step;
+        L.seed = s->seed;
+        L.max_move = p->maximum;
+        L.n_active = n_active;
+        L.n_bodies = (uint32_t)s->n;
+        if (s->profiling) HMC_CUDA(cudaEventRecord(s->ev[2], s->stream));
+        for (uint64_t r = 0; r < rounds; ++r) {
+            L.substep = s->substep;
+            for (uint32_t c = 0; c < colors; ++c) {
+                L.color = c;
+                HMC_CUDA(launch_sweep_sphere(s->dim, fp32, s->geom, s->arr, s->pair, L, s->stream));
+                s->prof.kernel_launches += 1;
+            }
+            s->substep += 1;  // increment_substep after every full colour set
+        }
+        if (s->profiling) HMC_CUDA(cudaEventRecord(s->ev[3], s->stream));
+        if ((st = read_stats(s))) return st;
+        if (s->profiling) {
+            float t_rebuild = 0.f, t_sweep = 0.f;
+            HMC_CUDA(cudaEventElapsedTime(&t_rebuild, s->ev[0], s->ev[1]));
+            HMC_CUDA(cudaEventElapsedTime(&t_sweep, s->ev[2], s->ev[3]));
+            s->prof.rebuild_ms += t_rebuild;
+            s->prof.rebuild_launches += s->n > 0 ? 6 : 4;
+            s->prof.sweep_ms += t_sweep;
+            s->prof.sweep_launches += rounds * colors;
+            s->prof.sweeps += 1;
+        }
+        total.accepted += s->host_stats->accepted;
+        total.rejected += rounds * nonempty - s->host_stats->accepted;
+        total.rechecks += s->host_stats->rechecks;
+        total.pair_checks += s->host_stats->pair_checks;
+        double me;
+        unsigned long long bits = s->host_stats->max_err_bits;
+        std::memcpy(&me, &bits, 8);
+        total.max_fp32_error = std::max(total.max_fp32_error, me);
+        if (p->increment_step) {
+            s->step += 1;
+            s->substep = 0;
+        }
+    }
+    if (out) *out = total;
+    return HMC_OK;
+}
+
+hmc_status hmc_profile_enable(hmc_system* s, int enable) {
+    if (!s) return fail(HMC_INVALID_ARGUMENT, "NULL system");
+    HMC_CUDA(cudaSetDevice(s->ctx->device));
+    for (cudaEvent_t& e : s->ev)
+        if (!e) HMC_CUDA(cudaEventCreate(&e));
+    s->profiling = enable != 0;
+    return HMC_OK;
+}
+
+hmc_status hmc_profile_read(hmc_system* s, hmc_profile* out, int reset) {
+    if (!s || !out) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
+    *out = s->prof;
+    if (reset) s->prof = hmc_profile{};
+    return HMC_OK;
+}
+
+hmc_status hmc_tune(hmc_system* s, hmc_sweep_params* p, double target, uint32_t samples, uint32_t steps) {
+    (void)s;
+    (void)p;
+    (void)target;
+    (void)samples;
+    (void)steps;
+    return fail(HMC_NOT_SUPPORTED, "hmc_tune is not available in this build");
+}
+
+hmc_status hmc_overlap_check(hmc_system* s, uint64_t* n_overlaps) {
+    if (!s || !n_overlaps) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
+    HMC_CUDA(cudaSetDevice(s->ctx->device));
+    hmc_status st = rebuild(s);
+    if (st) return st;
+    HMC_CUDA(launch_overlap_sphere(s->dim, s->geom, s->arr, s->pair, (uint32_t)s->n, s->stream));
+    s->prof.kernel_launches += 1;
+    if ((st = read_stats(s))) return st;
+    if ((st = check_flags(s))) return st;
+    *n_overlaps = s->host_stats->overlaps;
+    return HMC_OK;
+}
+
+hmc_status hmc_eval_moves(hmc_system* s, const hmc_injected_move* moves, uint64_t n, double temperature,
+                          uint32_t precision, uint8_t* decisions, uint8_t* rechecked) {
+    if (!s || (n && (!moves || !decisions))) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
+    if (precision > HMC_FP32_RECHECK) return fail(HMC_INVALID_ARGUMENT, "precision");
+    (void)temperature;
+    if (n == 0) return HMC_OK;
+    if (n >= (1ull << 31)) return fail(HMC_INVALID_ARGUMENT, "too many moves");
+    HMC_CUDA(cudaSetDevice(s->ctx->device));
+    for (uint64_t i = 0; i < n; ++i)
+        if (moves[i].body >= s->n) return fail(HMC_INVALID_ARGUMENT, "move %llu names body %llu of %llu",
+                                                (unsigned long long)i, (unsigned long long)moves[i].body,
+                                                (unsigned long long)s->n);
+    hmc_status st = rebuild(s);
+    if (st) return st;
+    std::vector<uint64_t> hb(n);
+    std::vector<double4> ht(n);
+    for (uint64_t i = 0; i < n; ++i) {
+        hb[i] = moves[i].body;
+        ht[i] = make_double4(moves[i].position[0], moves[i].position[1], s->dim == 3 ? moves[i].position[2] : 0.0, 0.0);
+    }
+    uint64_t* db = nullptr;
+    double4* dt = nullptr;
+    uint8_t* dd = nullptr;
+    cudaError_t e = cudaMallocAsync((void**)&db, sizeof(uint64_t) * n, s->stream);
+    if (e == cudaSuccess) e = cudaMallocAsync((void**)&dt, sizeof(double4) * n, s->stream);
+    if (e == cudaSuccess) e = cudaMallocAsync((void**)&dd, 2 * n, s->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(db, hb.data(), sizeof(uint64_t) * n, cudaMemcpyHostToDevice, s->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dt, ht.data(), sizeof(double4) * n, cudaMemcpyHostToDevice, s->stream);
+    if (e == cudaSuccess)
+        e = launch_eval_sphere(s->dim, precision == HMC_FP32_RECHECK, s->geom, s->arr, s->pair, db, dt, (uint32_t)n, dd,
+                               dd + n, s->stream);
+    std::vector<uint8_t> hd(2 * n);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(hd.data(), dd, 2 * n, cudaMemcpyDeviceToHost, s->stream);
+    if (db) cudaFreeAsync(db, s->stream);
+    if (dt) cudaFreeAsync(dt, s->stream);
+    if (dd) cudaFreeAsync(dd, s->stream);
+    cudaError_t e2 = cudaStreamSynchronize(s->stream);
+    if (e == cudaSuccess) e = e2;
+    if (e != cudaSuccess) return fail(HMC_CUDA_ERROR, "eval_moves: %s", cudaGetErrorString(e));
+    if ((st = read_stats(s))) return st;
+    if ((st = check_flags(s))) return st;
+    std::memcpy(decisions, hd.data(), n);
+    if (rechecked) std::memcpy(rechecked, hd.data() + n, n);
+    return HMC_OK;
+}
+
+}  // extern "C"

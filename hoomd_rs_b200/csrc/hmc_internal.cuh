@@ -1,0 +1,92 @@
+// Internal types shared by the kernels (hmc_kernels.cu) and the C ABI (hmc_capi.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "hmc_math.cuh"
+
+namespace hmc {
+
+// Device-side error flags (DeviceStats::error_flags).
+enum : uint32_t {
+    kErrOutsideCheckerboard = 1u << 0,
+    kErrNonFinite = 1u << 1,
+};
+
+// Counters written by the kernels. Zeroed by the host before a sweep.
+struct DeviceStats {
+    unsigned long long accepted;
+    unsigned long long rechecks;
+    unsigned long long pair_checks;
+    unsigned long long max_err_bits;  // bits of the largest non-negative FP32 error
+    unsigned int nonempty;            // non-empty checkerboard spaces after a rebuild
+    unsigned int error_flags;
+    unsigned long long overlaps;      // pairs found by the overlap check
+};
+
+// The checkerboard (hoomd-mc/src/hypercuboid.rs) together with the periodic box.
+struct Geometry {
+    double L[3];        // box edge lengths
+    double half[3];     // L / 2
+    double ghost_hi[3]; // half - boundary_range: a site beyond has an image at x - L
+    double ghost_lo[3]; // -half + boundary_range: a site below has an image at x + L
+    double origin[3];   // checkerboard origin (shifted each sweep)
+    double width[3];    // space width
+    float w32[3];       // width rounded to FP32
+    uint32_t shape[3];  // spaces per axis (even)
+    uint32_t half_shape[3];
+    uint32_t n_cells;
+};
+
+// Sorted (cell-ordered) and body-ordered device arrays of one system.
+struct Arrays {
+    double4* body_pos;       // [n] body positions B, body order (x, y, z, 0)
+    double4* body_ori;       // [n] body versors (s, x, y, z), body order; may be null
+    double4* sorted_b;       // [n] body positions B in cell order (proposal source)
+    double4* sorted_s;       // [n] site positions S = wrap(B) in cell order (neighbour tests)
+    float4* sorted_off;      // [n] FP32 offsets of S from its cell corner; .w = fast-axis cell index bits
+    double4* sorted_q;       // [n] versors in cell order; may be null
+    uint32_t* sorted_body;   // [n] cell-order slot -> body index
+    uint32_t* slot_of_body;  // [n] body index -> cell-order slot
+    uint32_t* body_cell;     // [n]
+    uint32_t* body_rank;     // [n]
+    uint32_t* cell_count;    // [cells]
+    uint32_t* cell_start;    // [cells + 1]
+    uint32_t* block_sums;    // scan scratch
+    DeviceStats* stats;
+    const double* zig_x;     // ziggurat tables (257 each)
+    const double* zig_f;
+};
+
+// Pair interaction parameters.
+struct Pair {
+    double sigma2;     // HardSphere diameter^2
+    float sig2_lo32;   // FP32 certain-overlap threshold (sigma^2 - bound, rounded down)
+    float sig2_hi32;   // FP32 certain-clear threshold (sigma^2 + bound, rounded up)
+};
+
+// One sweep launch: counter, move and colour.
+struct Launch {
+    uint64_t step;
+    uint32_t substep;
+    uint32_t seed;
+    uint32_t color;       // parity offsets: bit a of color (last axis = bit 0) is the offset on axis a
+    uint32_t n_active;    // spaces of this colour
+    double max_move;      // Translate maximum distance
+    uint32_t n_bodies;
+};
+
+// Kernel launchers (hmc_kernels.cu). All return cudaGetLastError() after enqueueing.
+cudaError_t launch_rebuild(int dim, const Geometry& g, const Arrays& a, uint32_t n, cudaStream_t s);
+cudaError_t launch_sweep_sphere(int dim, bool fp32, const Geometry& g, const Arrays& a, const Pair& p,
+                                const Launch& l, cudaStream_t s);
+cudaError_t launch_overlap_sphere(int dim, const Geometry& g, const Arrays& a, const Pair& p, uint32_t n,
+                                  cudaStream_t s);
+// Injected moves: positions (n x 4 doubles), result decisions and recheck flags.
+cudaError_t launch_eval_sphere(int dim, bool fp32, const Geometry& g, const Arrays& a, const Pair& p,
+                               const uint64_t* bodies, const double4* trial, uint32_t n, uint8_t* decisions,
+                               uint8_t* rechecked, cudaStream_t s);
+
+}  // namespace hmc

@@ -1,0 +1,180 @@
+/*
+ * hmc.h -- C ABI of the B200 (sm_100a) Monte Carlo sweep library, libhmc_b200.so.
+ *
+ * The library runs the local-move Metropolis sweep of hoomd-rs's hoomd-mc crate
+ * (glotzerlab/hoomd-rs v1.4.0) on one GPU. The reference has no FFI; these entry points
+ * are the ones a Rust `GpuSweep` type would bind to replace the monomorphised generic
+ * calls on the sweep path (citations are file:line in the reference):
+ *
+ *   hmc_system_create / hmc_set_state / hmc_get_state
+ *       replace building a Microstate<B,S,VecCell,Periodic<Hypercuboid>> with
+ *       Microstate::builder()...try_build() / add_body (hoomd-microstate/src/microstate.rs:777-835)
+ *       and reading microstate.bodies() back. step/substep/seed are the Counter fields
+ *       (microstate.rs:529).
+ *   hmc_sweep
+ *       replaces Trial::apply (hoomd-mc/src/lib.rs:134-147) as implemented by
+ *       ParallelSweep::apply (hoomd-mc/src/parallel_sweep.rs:390-421), with the trial moves
+ *       Translate<Cartesian<N>> (translate/cartesian.rs:40-51), Rotate<Versor>
+ *       (rotate/versor.rs:112-123), the Hamiltonian PairwiseCutoff::delta_energy_one
+ *       (hoomd-interaction/src/pairwise_cutoff.rs:919-941) over HardSphere, HardShape<Convex<
+ *       ConvexPolyhedron>> or Isotropic<Shifted<LennardJones>>, and the Isothermal macrostate.
+ *       Returns the Count (hoomd-mc/src/lib.rs:206-294).
+ *   hmc_tune
+ *       replaces Tune::tune_with_options (hoomd-mc/src/lib.rs:430-449, tune_local.rs:21-89).
+ *   hmc_overlap_check
+ *       replaces PairwiseCutoff::total_energy (pairwise_cutoff.rs:720-745) as an overlap check.
+ *   hmc_eval_moves
+ *       evaluates injected trial moves against the current state: delta_energy_one plus the
+ *       Metropolis test of sweep.rs:207-208. It is the decision-parity probe.
+ *
+ * Conventions. Every call returns hmc_status; no call aborts. On failure,
+ * hmc_last_error_message() gives a thread-local description. Host arrays are owned by the
+ * caller and copied; no pointer is retained across calls. One hmc_system is driven by one
+ * host thread at a time. All device work of a system runs on one CUDA stream.
+ */
+#ifndef HMC_H
+#define HMC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HMC_ABI_VERSION 1u
+
+typedef enum hmc_status {
+    HMC_OK = 0,
+    HMC_INVALID_ARGUMENT = 1,     /* bad sizes, NULL pointers, non-positive lengths */
+    HMC_RANGE_TOO_LARGE = 2,      /* interaction range leaves < 2 checkerboard spaces per axis
+                                     (hypercuboid.rs:196-199 panics) or exceeds L/2
+                                     (boundary/periodic.rs:97-107) */
+    HMC_OVERLAP_IN_INPUT = 3,     /* reserved: reported by hmc_overlap_check callers */
+    HMC_CELL_OVERFLOW = 4,        /* a cell holds more bodies than a kernel supports */
+    HMC_NAN_STATE = 5,            /* a non-finite coordinate was found */
+    HMC_ITERATION_CAP = 6,        /* reserved */
+    HMC_TIMEOUT = 7,              /* reserved */
+    HMC_CUDA_ERROR = 8,           /* a CUDA runtime call failed */
+    HMC_OUT_OF_MEMORY = 9,
+    HMC_NOT_SUPPORTED = 10,       /* combination not implemented */
+    HMC_OUTSIDE_CHECKERBOARD = 11 /* a body maps to no space (parallel_sweep.rs:198 panics) */
+} hmc_status;
+
+typedef enum hmc_interaction {
+    HMC_HARD_SPHERE = 0,            /* PairwiseCutoff(HardSphere { diameter }) */
+    HMC_HARD_CONVEX_POLYGON = 1,    /* PairwiseCutoff(HardShape(Convex(ConvexPolygon))) */
+    HMC_HARD_CONVEX_POLYHEDRON = 2, /* PairwiseCutoff(HardShape(Convex(ConvexPolyhedron))) */
+    HMC_LENNARD_JONES = 3           /* PairwiseCutoff(Isotropic { Shifted { LennardJones }, r_cut }) */
+} hmc_interaction;
+
+typedef enum hmc_move {
+    HMC_TRANSLATE = 0, /* Translate::with_maximum_distance(maximum) */
+    HMC_ROTATE = 1     /* Rotate::with_maximum_rotation(maximum) */
+} hmc_move;
+
+typedef enum hmc_precision {
+    HMC_FP64 = 0,        /* every pair test in FP64, the reference's arithmetic */
+    HMC_FP32_RECHECK = 1 /* FP32 pair tests under a forward-error bound; pairs inside the
+                            bound are re-evaluated in FP64, so decisions equal HMC_FP64 */
+} hmc_precision;
+
+typedef struct hmc_context hmc_context;
+typedef struct hmc_system hmc_system;
+
+typedef struct hmc_device_opts {
+    uint32_t struct_size; /* sizeof(hmc_device_opts) */
+    int32_t device;       /* CUDA device ordinal */
+} hmc_device_opts;
+
+typedef struct hmc_system_desc {
+    uint32_t struct_size;        /* sizeof(hmc_system_desc) */
+    uint32_t dim;                /* 2 or 3 */
+    double edge_lengths[3];      /* periodic box, centred on the origin: [-L/2, L/2) */
+    uint64_t n_bodies;
+    uint64_t step;               /* Counter step */
+    uint32_t substep;            /* Counter substep */
+    uint32_t seed;               /* Counter seed */
+    uint32_t interaction;        /* hmc_interaction */
+    uint32_t n_vertices;         /* convex polytope vertex count (<= 32) */
+    const double* vertices;      /* n_vertices * dim, FP64 */
+    double diameter;             /* HardSphere */
+    double lj_epsilon, lj_sigma, lj_r_cut, lj_r_shift; /* Isotropic<Shifted<LennardJones>> */
+    double boundary_range;       /* Periodic::new maximum_interaction_range; 0 = the pair range */
+    double body_interaction_range; /* ParallelSweep::new range; 0 = the pair range */
+} hmc_system_desc;
+
+typedef struct hmc_sweep_params {
+    uint32_t struct_size;     /* sizeof(hmc_sweep_params) */
+    uint32_t move;            /* hmc_move */
+    double maximum;           /* maximum distance (translate) or rotation (rotate) */
+    double temperature;       /* Isothermal kT */
+    uint32_t precision;       /* hmc_precision */
+    uint32_t n_sweeps;        /* number of ParallelSweep::apply calls */
+    uint32_t increment_step;  /* 1: Microstate::increment_step() after every apply */
+    uint32_t reserved;
+} hmc_sweep_params;
+
+typedef struct hmc_count {
+    uint64_t accepted;
+    uint64_t rejected;
+    uint64_t rechecks;       /* FP32 pair results re-evaluated in FP64 */
+    uint64_t pair_checks;    /* pair evaluations in the FP32 path */
+    double max_fp32_error;   /* largest |FP32 - FP64| over rechecked pair quantities */
+} hmc_count;
+
+/* One injected trial move for hmc_eval_moves. */
+typedef struct hmc_injected_move {
+    uint64_t body;           /* body index */
+    double position[3];      /* trial body position as returned by wrap(propose(..)) */
+    double orientation[4];   /* trial versor (s, x, y, z) or angle in [0] */
+    double u;                /* the Metropolis uniform in [0, 1); ignored for hard shapes */
+} hmc_injected_move;
+
+/* Device-time profile of a system's kernels, collected with CUDA events on the system's
+ * stream while profiling is enabled. */
+typedef struct hmc_profile {
+    uint64_t kernel_launches;       /* every kernel this system enqueued (profiling on or off) */
+    uint64_t sweep_launches;        /* colour-pass sweep kernels timed */
+    double sweep_ms;                /* device time of the timed colour-pass kernels */
+    uint64_t rebuild_launches;      /* cell-list kernels timed */
+    double rebuild_ms;              /* device time of the timed cell-list rebuilds */
+    uint64_t sweeps;                /* ParallelSweep::apply calls timed */
+} hmc_profile;
+
+/* ---- context and errors ---- */
+uint32_t hmc_abi_version(void);
+const char* hmc_status_string(hmc_status status);
+const char* hmc_last_error_message(void);
+hmc_status hmc_context_create(const hmc_device_opts* opts, hmc_context** out);
+void hmc_context_destroy(hmc_context* ctx);
+
+/* ---- systems ---- */
+hmc_status hmc_system_create(hmc_context* ctx, const hmc_system_desc* desc, const double* positions,
+                             const double* orientations, hmc_system** out);
+void hmc_system_destroy(hmc_system* sys);
+/* Run the system's device work on an external cudaStream_t (NULL: the library's own). */
+hmc_status hmc_system_set_stream(hmc_system* sys, void* cuda_stream);
+void* hmc_system_stream(hmc_system* sys);
+/* positions: n*dim; orientations: n*4 (3-D) or n (2-D) or NULL for unoriented bodies. */
+hmc_status hmc_set_state(hmc_system* sys, const double* positions, const double* orientations, uint64_t step,
+                         uint32_t substep);
+hmc_status hmc_get_state(hmc_system* sys, double* positions, double* orientations, uint64_t* step,
+                         uint32_t* substep);
+
+/* ---- the sweep ---- */
+hmc_status hmc_sweep(hmc_system* sys, const hmc_sweep_params* params, hmc_count* out);
+hmc_status hmc_tune(hmc_system* sys, hmc_sweep_params* params, double target_acceptance, uint32_t samples,
+                    uint32_t steps);
+hmc_status hmc_overlap_check(hmc_system* sys, uint64_t* n_overlaps);
+hmc_status hmc_eval_moves(hmc_system* sys, const hmc_injected_move* moves, uint64_t n, double temperature,
+                          uint32_t precision, uint8_t* decisions, uint8_t* rechecked);
+
+/* ---- profiling ---- */
+hmc_status hmc_profile_enable(hmc_system* sys, int enable);
+hmc_status hmc_profile_read(hmc_system* sys, hmc_profile* out, int reset);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HMC_H */
