@@ -26,7 +26,8 @@ from typing import Optional, Sequence
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libhmc_b200.so")
+# HMC_B200_LIB selects another build of the library (for example a variant under test).
+LIB_PATH = os.environ.get("HMC_B200_LIB", os.path.join(_HERE, "libhmc_b200.so"))
 
 # hmc_status
 OK, INVALID_ARGUMENT, RANGE_TOO_LARGE, OVERLAP_IN_INPUT, CELL_OVERFLOW, NAN_STATE, ITERATION_CAP, TIMEOUT, \

@@ -41,12 +41,13 @@ def _stale() -> bool:
     return any(os.path.getmtime(p) > t for p in deps)
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    if not force and not _stale():
+def build(force: bool = False, verbose: bool = False, out: str = LIB, defines=()) -> str:
+    if not force and out == LIB and not _stale():
         return LIB
-    cmd = [nvcc(), *ARCH, *FLAGS, "-shared", "-o", LIB, *[os.path.join(CSRC, f) for f in SOURCES]]
+    cmd = [nvcc(), *ARCH, *FLAGS, *[f"-D{d}" for d in defines], "-shared", "-o", out,
+           *[os.path.join(CSRC, f) for f in SOURCES]]
     r = subprocess.run(cmd, capture_output=True, text=True)
-    log = os.path.join(HERE, "build.log")
+    log = out + ".build.log"
     with open(log, "w") as f:
         f.write(" ".join(cmd) + "\n" + r.stdout + r.stderr)
     if r.returncode != 0:
@@ -54,7 +55,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         raise RuntimeError(f"nvcc failed ({r.returncode}); see {log}")
     if verbose:
         sys.stdout.write(r.stderr)
-    return LIB
+    return out
 
 
 if __name__ == "__main__":

@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -76,6 +77,7 @@ struct hmc_system {
     cudaStream_t stream = nullptr;
     DeviceStats* host_stats = nullptr;  // pinned
     std::vector<void*> allocations;
+    uint32_t tile_cap[2] = {0, 0};  // staged bodies per block of the tiled pass: [fp64, fp32]
     // profiling
     bool profiling = false;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -137,14 +139,14 @@ hmc_status check_flags(hmc_system* s) {
 
 // update_checkerboard (parallel_sweep.rs:176-201): origin shift from the counter's
 // index u64::MAX stream, then the device counting sort into cell order.
-hmc_status rebuild(hmc_system* s) {
+hmc_status rebuild(hmc_system* s, bool write_s) {
     Sfc64 rng = make_rng(s->step, s->substep, s->seed, UINT64_MAX);
     for (int a = 0; a < s->dim; ++a) {
         double off = uniform01(rng);
         s->geom.origin[a] = -s->geom.L[a] / 2.0 - off * s->geom.width[a];
     }
     HMC_CUDA(cudaMemsetAsync(s->arr.stats, 0, sizeof(DeviceStats), s->stream));
-    HMC_CUDA(launch_rebuild(s->dim, s->geom, s->arr, (uint32_t)s->n, s->stream));
+    HMC_CUDA(launch_rebuild(s->dim, s->geom, s->arr, (uint32_t)s->n, write_s, s->stream));
     s->prof.kernel_launches += s->n > 0 ? 6 : 4;  // bin, 3 scan passes, scatter, finalize
     return HMC_OK;
 }
@@ -282,6 +284,8 @@ hmc_status hmc_system_create(hmc_context* ctx, const hmc_system_desc* d, const d
         s->geom.ghost_hi[a] = s->geom.half[a] - s->boundary_range;
         s->geom.ghost_lo[a] = -s->geom.half[a] + s->boundary_range;
         s->geom.w32[a] = (float)s->geom.width[a];
+        s->geom.invL[a] = 1.0 / s->geom.L[a];
+        s->geom.invW[a] = 1.0 / s->geom.width[a];
         s->geom.half_shape[a] = s->geom.shape[a] / 2;
         cells *= s->geom.shape[a];
     }
@@ -289,9 +293,34 @@ hmc_status hmc_system_create(hmc_context* ctx, const hmc_system_desc* d, const d
         fail(HMC_NOT_SUPPORTED, "%llu checkerboard spaces exceed the supported 16M", (unsigned long long)cells);
         return destroy_fail(HMC_NOT_SUPPORTED);
     }
+    // colour lists pack the multi-index: 10 bits per axis in 3-D, 16 in 2-D
+    for (int a = 0; a < s->dim; ++a) {
+        if (s->geom.shape[a] > (s->dim == 3 ? 1024u : 65535u)) {
+            fail(HMC_NOT_SUPPORTED, "%u spaces on axis %d exceed the supported %u", s->geom.shape[a], a,
+                 s->dim == 3 ? 1024u : 65535u);
+            return destroy_fail(HMC_NOT_SUPPORTED);
+        }
+        if (s->geom.shape[a] == 2) s->geom.any_two = 1;
+    }
     s->geom.n_cells = (uint32_t)cells;
+    s->geom.color_stride = (uint32_t)(cells >> s->dim);
     s->pair.sigma2 = d->diameter * d->diameter;  // diameter.powi(2)
     sphere_bound(s);
+    // Shared-memory staging capacity: 1.5x the mean body count of a 9 x 9 x 17 region plus
+    // slack, within 100 KB per block; a denser system keeps the global-memory pass.
+    // The direct (global-memory) pass measured faster than the shared-memory tiled pass on
+    // B200 for hard spheres; HMC_B200_SWEEP_KERNEL=tiled selects the tiled pass instead.
+    const char* kern = std::getenv("HMC_B200_SWEEP_KERNEL");
+    const bool tiled = kern && std::strcmp(kern, "tiled") == 0;
+    if (tiled && tile_kernel_applies(s->dim, s->geom)) {
+        double mean = 9.0 * 9.0 * 17.0 * (double)s->n / (double)cells;
+        uint32_t want = (uint32_t)(1.5 * mean + 64.0);
+        for (int f = 0; f < 2; ++f) {
+            uint32_t cap = want;
+            while (cap > 64 && tile_smem_bytes(f == 1, cap) > 100u * 1024u) cap -= 32;
+            s->tile_cap[f] = cap >= want ? cap : 0u;
+        }
+    }
 
     cudaError_t e = cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
@@ -312,7 +341,8 @@ hmc_status hmc_system_create(hmc_context* ctx, const hmc_system_desc* d, const d
         (st = dalloc(s, &A.sorted_off, n)) || (st = dalloc(s, &A.sorted_body, n)) ||
         (st = dalloc(s, &A.slot_of_body, n)) || (st = dalloc(s, &A.body_cell, n)) ||
         (st = dalloc(s, &A.body_rank, n)) || (st = dalloc(s, &A.cell_count, cells)) ||
-        (st = dalloc(s, &A.cell_start, cells + 1)) || (st = dalloc(s, &A.block_sums, scan_blocks)) ||
+        (st = dalloc(s, &A.cell_start, cells + 1)) || (st = dalloc(s, &A.block_sums, (size_t)scan_blocks * 9)) ||
+        (st = dalloc(s, &A.color_cells, cells)) ||
         (st = dalloc(s, &A.stats, 1)))
         return destroy_fail(st);
     A.body_ori = nullptr;
@@ -407,11 +437,9 @@ hmc_status hmc_sweep(hmc_system* s, const hmc_sweep_params* p, hmc_count* out) {
     hmc_count total{};
     const bool fp32 = p->precision == HMC_FP32_RECHECK;
     const uint32_t colors = 1u << s->dim;
-    uint32_t n_active = 1;
-    for (int a = 0; a < s->dim; ++a) n_active *= s->geom.half_shape[a];
     for (uint32_t sweep = 0; sweep < p->n_sweeps; ++sweep) {
         if (s->profiling) HMC_CUDA(cudaEventRecord(s->ev[0], s->stream));
-        hmc_status st = rebuild(s);
+        hmc_status st = rebuild(s, !fp32);
         if (st) return st;
         if (s->profiling) HMC_CUDA(cudaEventRecord(s->ev[1], s->stream));
         if ((st = read_stats(s))) return st;
@@ -423,14 +451,16 @@ hmc_status hmc_sweep(hmc_system* s, const hmc_sweep_params* p, hmc_count* out) {
         L.step = s->step;
         L.seed = s->seed;
         L.max_move = p->maximum;
-        L.n_active = n_active;
         L.n_bodies = (uint32_t)s->n;
+        uint32_t color_count[8];
+        for (uint32_t c = 0; c < colors; ++c) color_count[c] = s->host_stats->color_count[c];
         if (s->profiling) HMC_CUDA(cudaEventRecord(s->ev[2], s->stream));
         for (uint64_t r = 0; r < rounds; ++r) {
             L.substep = s->substep;
             for (uint32_t c = 0; c < colors; ++c) {
                 L.color = c;
-                HMC_CUDA(launch_sweep_sphere(s->dim, fp32, s->geom, s->arr, s->pair, L, s->stream));
+                L.n_active = color_count[c];
+                HMC_CUDA(launch_sweep_sphere(s->dim, fp32, s->geom, s->arr, s->pair, L, s->tile_cap[fp32], s->stream));
                 s->prof.kernel_launches += 1;
             }
             s->substep += 1;  // increment_substep after every full colour set
@@ -492,7 +522,7 @@ hmc_status hmc_tune(hmc_system* s, hmc_sweep_params* p, double target, uint32_t 
 hmc_status hmc_overlap_check(hmc_system* s, uint64_t* n_overlaps) {
     if (!s || !n_overlaps) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
     HMC_CUDA(cudaSetDevice(s->ctx->device));
-    hmc_status st = rebuild(s);
+    hmc_status st = rebuild(s, true);
     if (st) return st;
     HMC_CUDA(launch_overlap_sphere(s->dim, s->geom, s->arr, s->pair, (uint32_t)s->n, s->stream));
     s->prof.kernel_launches += 1;
@@ -514,7 +544,7 @@ hmc_status hmc_eval_moves(hmc_system* s, const hmc_injected_move* moves, uint64_
         if (moves[i].body >= s->n) return fail(HMC_INVALID_ARGUMENT, "move %llu names body %llu of %llu",
                                                 (unsigned long long)i, (unsigned long long)moves[i].body,
                                                 (unsigned long long)s->n);
-    hmc_status st = rebuild(s);
+    hmc_status st = rebuild(s, true);
     if (st) return st;
     std::vector<uint64_t> hb(n);
     std::vector<double4> ht(n);

@@ -24,6 +24,7 @@ struct DeviceStats {
     unsigned int nonempty;            // non-empty checkerboard spaces after a rebuild
     unsigned int error_flags;
     unsigned long long overlaps;      // pairs found by the overlap check
+    unsigned int color_count[8];      // non-empty spaces per colour after a rebuild
 };
 
 // The checkerboard (hoomd-mc/src/hypercuboid.rs) together with the periodic box.
@@ -34,10 +35,14 @@ struct Geometry {
     double ghost_lo[3]; // -half + boundary_range: a site below has an image at x + L
     double origin[3];   // checkerboard origin (shifted each sweep)
     double width[3];    // space width
+    double invL[3];     // RN(1 / L), for div_fixed
+    double invW[3];     // RN(1 / width), for div_fixed
     float w32[3];       // width rounded to FP32
     uint32_t shape[3];  // spaces per axis (even)
     uint32_t half_shape[3];
     uint32_t n_cells;
+    uint32_t color_stride;  // capacity of one colour's list of non-empty spaces (n_cells >> dim)
+    uint32_t any_two;       // some axis has exactly two spaces (minimum-image fix-up needed)
 };
 
 // Sorted (cell-ordered) and body-ordered device arrays of one system.
@@ -55,6 +60,7 @@ struct Arrays {
     uint32_t* cell_count;    // [cells]
     uint32_t* cell_start;    // [cells + 1]
     uint32_t* block_sums;    // scan scratch
+    uint32_t* color_cells;   // [cells] per-colour lists of non-empty spaces, packed multi-indices
     DeviceStats* stats;
     const double* zig_x;     // ziggurat tables (257 each)
     const double* zig_f;
@@ -73,15 +79,22 @@ struct Launch {
     uint32_t substep;
     uint32_t seed;
     uint32_t color;       // parity offsets: bit a of color (last axis = bit 0) is the offset on axis a
-    uint32_t n_active;    // spaces of this colour
+    uint32_t n_active;    // non-empty spaces of this colour (length of its list)
     double max_move;      // Translate maximum distance
     uint32_t n_bodies;
 };
 
 // Kernel launchers (hmc_kernels.cu). All return cudaGetLastError() after enqueueing.
-cudaError_t launch_rebuild(int dim, const Geometry& g, const Arrays& a, uint32_t n, cudaStream_t s);
+// write_s: also store the FP64 site positions S = wrap(B) in cell order (needed by the
+// plain FP64 pair test, the overlap check and injected-move evaluation).
+cudaError_t launch_rebuild(int dim, const Geometry& g, const Arrays& a, uint32_t n, bool write_s, cudaStream_t s);
+// tile_cap > 0 selects the shared-memory tiled pass (3-D, at least 9 x 9 x 17 spaces) with room
+// for tile_cap staged bodies per block; a block whose region holds more falls back to
+// global-memory neighbour reads.
 cudaError_t launch_sweep_sphere(int dim, bool fp32, const Geometry& g, const Arrays& a, const Pair& p,
-                                const Launch& l, cudaStream_t s);
+                                const Launch& l, uint32_t tile_cap, cudaStream_t s);
+size_t tile_smem_bytes(bool fp32, uint32_t cap);
+bool tile_kernel_applies(int dim, const Geometry& g);
 cudaError_t launch_overlap_sphere(int dim, const Geometry& g, const Arrays& a, const Pair& p, uint32_t n,
                                   cudaStream_t s);
 // Injected moves: positions (n x 4 doubles), result decisions and recheck flags.

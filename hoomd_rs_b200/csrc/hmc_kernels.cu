@@ -16,10 +16,18 @@
 // memory and their bodies form one contiguous range of the cell-ordered arrays.
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "hmc_internal.cuh"
 
 namespace hmc {
 namespace {
+
+// Resident blocks per SM the direct pass is compiled for: 6 caps it at 80 registers,
+// which measured fastest on B200 (more resident warps beat the few spilled values).
+#ifndef HMC_SWEEP_MIN_BLOCKS
+#define HMC_SWEEP_MIN_BLOCKS 6
+#endif
 
 constexpr int kScanThreads = 256;
 constexpr int kScanItems = 8;
@@ -33,7 +41,7 @@ __device__ __forceinline__ bool point_to_space(const Geometry& g, const double* 
 #pragma unroll
     for (int a = 0; a < DIM; ++a) {
         double p = dsub(x[a], g.origin[a]);
-        double f = floor(ddiv(p, g.width[a]));
+        double f = floor(div_fixed(p, g.width[a], g.invW[a]));
         if (!(f >= 0.0)) return false;
         if (f > 4.0e9) return false;
         uint32_t idx = (uint32_t)f;
@@ -122,10 +130,17 @@ __device__ __forceinline__ void ball_sample(Sfc64& r, double radius, const doubl
             }
         }
     } else {
-        double p[3];
-        p[0] = standard_normal(r, zx, zf);
-        p[1] = standard_normal(r, zx, zf);
-        p[2] = standard_normal(r, zx, zf);
+        double p[3] = {0.0, 0.0, 0.0};
+#pragma unroll 1
+        for (int i = 0; i < 3; ++i) {
+            double z = standard_normal(r, zx, zf);
+            if (i == 0)
+                p[0] = z;
+            else if (i == 1)
+                p[1] = z;
+            else
+                p[2] = z;
+        }
         double norm = dsqrt(dot<3>(p, p));
         double u = uniform01(r);
         double scale = dmul(ddiv(radius, norm), portable_cbrt(u));
@@ -136,11 +151,65 @@ __device__ __forceinline__ void ball_sample(Sfc64& r, double radius, const doubl
 }
 
 // ---- neighbour stencil over cell-ordered rows ----------------------------------------------
-// Calls f(q, dshift) for every body slot q in the 3^DIM spaces around the space m, where
-// dshift[a] (FP32) is the displacement of the candidate's cell corner from m's corner
-// along each axis for the slow axes; the fast-axis shift is derived per candidate from
-// its stored cell index. Stops early when f returns true. Spaces are visited once even
-// when an axis has only two spaces (both neighbours are then the same space).
+__device__ __forceinline__ uint32_t wrap_index(int i, uint32_t n) {
+    return i < 0 ? (uint32_t)(i + (int)n) : ((uint32_t)i >= n ? (uint32_t)i - n : (uint32_t)i);
+}
+
+// Packed multi-index of a space in a colour list: 10 bits per axis in 3-D, 16 in 2-D.
+template <int DIM>
+__device__ __forceinline__ uint32_t pack_m(const uint32_t* m) {
+    return DIM == 3 ? (m[0] | (m[1] << 10) | (m[2] << 20)) : (m[0] | (m[1] << 16));
+}
+template <int DIM>
+__device__ __forceinline__ void unpack_m(uint32_t p, uint32_t* m) {
+    if (DIM == 3) {
+        m[0] = p & 1023u;
+        m[1] = (p >> 10) & 1023u;
+        m[2] = p >> 20;
+    } else {
+        m[0] = p & 0xffffu;
+        m[1] = p >> 16;
+    }
+}
+
+// Rows of the 3^DIM stencil around space m, as ranges of cell-ordered slots. A row is
+// the run of three spaces m[last]-1 .. m[last]+1 along the fast axis at one offset of the
+// slow axes; it is contiguous unless it wraps around the fast axis (m[last] at either end).
+// Row r (r = 3*(i0+1) + (i1+1) in 3-D, i1+1 in 2-D) has slow-axis offsets (i0, i1). When a
+// slow axis has two spaces its offset -1 names the same space as +1; that row is left empty.
+template <int DIM>
+constexpr int kRows = DIM == 3 ? 9 : 3;
+
+template <int DIM>
+__device__ __forceinline__ void load_rows(const Geometry& g, const uint32_t* __restrict__ cs, const uint32_t* m,
+                                          uint32_t* a0, uint32_t* a1) {
+    const uint32_t sf = g.shape[DIM - 1], mf = m[DIM - 1];
+    const uint32_t lo = sf == 2 ? 0u : mf - 1u;
+    const uint32_t hi = sf == 2 ? 2u : mf + 2u;
+#pragma unroll
+    for (int r = 0; r < kRows<DIM>; ++r) {
+        int i0 = DIM == 3 ? r / 3 - 1 : 0;
+        int i1 = DIM == 3 ? r % 3 - 1 : r - 1;
+        uint32_t base;
+        bool skip;
+        if (DIM == 3) {
+            uint32_t c0 = wrap_index((int)m[0] + i0, g.shape[0]);
+            uint32_t c1 = wrap_index((int)m[1] + i1, g.shape[1]);
+            skip = (i0 == -1 && g.shape[0] == 2) || (i1 == -1 && g.shape[1] == 2);
+            base = (c0 * g.shape[1] + c1) * sf;
+        } else {
+            uint32_t c0 = wrap_index((int)m[0] + i1, g.shape[0]);
+            skip = i1 == -1 && g.shape[0] == 2;
+            base = c0 * sf;
+        }
+        a0[r] = skip ? 0u : __ldg(cs + base + lo);
+        a1[r] = skip ? 0u : __ldg(cs + base + hi);
+    }
+}
+
+// Generic stencil walk (any position of m, including the fast-axis ends): calls
+// f(q, slow_shift) for every slot q of the 3^DIM spaces around m and stops when f returns
+// true. Each space is visited once, also when an axis has two spaces.
 template <int DIM, typename F>
 __device__ __forceinline__ bool for_each_neighbor(const Geometry& g, const uint32_t* __restrict__ cell_start,
                                                   const uint32_t* m, F&& f) {
@@ -155,13 +224,13 @@ __device__ __forceinline__ bool for_each_neighbor(const Geometry& g, const uint3
             uint32_t row_base;
             float slow_shift[2];
             if (DIM == 3) {
-                uint32_t c0 = (m[0] + g.shape[0] + i0) % g.shape[0];
-                uint32_t c1 = (m[1] + g.shape[1] + i1) % g.shape[1];
+                uint32_t c0 = wrap_index((int)m[0] + i0, g.shape[0]);
+                uint32_t c1 = wrap_index((int)m[1] + i1, g.shape[1]);
                 row_base = (c0 * g.shape[1] + c1) * sf;
                 slow_shift[0] = (float)i0 * g.w32[0];
                 slow_shift[1] = (float)i1 * g.w32[1];
             } else {
-                uint32_t c0 = (m[0] + g.shape[0] + i1) % g.shape[0];
+                uint32_t c0 = wrap_index((int)m[0] + i1, g.shape[0]);
                 row_base = c0 * sf;
                 slow_shift[0] = (float)i1 * g.w32[0];
                 slow_shift[1] = 0.f;
@@ -207,24 +276,76 @@ struct PairStats {
     double max_err = 0.0;
 };
 
-// Hard-sphere overlap of trial site t (FP64, FP32 offsets t32 within space m) against the
-// neighbourhood of m, skipping slot `self`. FP32=true: FP32 test under the bound, FP64
-// recheck in between; FP32=false: the reference FP64 test on every candidate.
+// The FP32 displacement (trial minus candidate) from the FP32 offsets, given the shift of
+// the candidate's space corner along the slow axes and its fast-axis space offset dm.
+template <int DIM>
+__device__ __forceinline__ float fp32_dist2(const Geometry& g, float4 t32, float4 o, float s0, float s1, int dm) {
+    float d[3];
+    if (DIM == 3) {
+        d[0] = t32.x - (o.x + s0);
+        d[1] = t32.y - (o.y + s1);
+        d[2] = t32.z - (o.z + (float)dm * g.w32[2]);
+    } else {
+        d[0] = t32.x - (o.x + s0);
+        d[1] = t32.y - (o.y + (float)dm * g.w32[1]);
+        d[2] = 0.f;
+    }
+    if (g.any_two) {
+#pragma unroll
+        for (int a = 0; a < DIM; ++a) {
+            if (g.shape[a] == 2) {
+                float w = g.w32[a];
+                if (d[a] > w)
+                    d[a] -= 2.f * w;
+                else if (d[a] < -w)
+                    d[a] += 2.f * w;
+            }
+        }
+    }
+    float dd = d[0] * d[0] + d[1] * d[1];
+    if (DIM == 3) dd += d[2] * d[2];
+    return dd;
+}
+
+// FP64 recheck of a pair whose FP32 d^2 lies inside the bound.
+// S of the candidate is wrap(B), recomputed from its body position.
+template <int DIM>
+__device__ __forceinline__ bool recheck_fp64(const Geometry& g, const Arrays& A, const Pair& P, const double* t,
+                                          float dd, uint32_t q, PairStats& st) {
+    st.rechecks++;
+    double4 b4 = ldg4(A.sorted_b + q);
+    double sv[3] = {b4.x, b4.y, b4.z};
+    wrap_inv<DIM>(g.L, g.invL, sv);
+    double r2 = ref_dist2<DIM>(g, t, sv);
+    double e = fabs((double)dd - r2);
+    st.max_err = e > st.max_err ? e : st.max_err;
+    return r2 < P.sigma2;
+}
+
+// FP32 pair decision: certain overlap below sig2_lo32, certain clearance at or above
+// sig2_hi32, the reference FP64 test in between.
+template <int DIM>
+__device__ __forceinline__ bool fp32_pair_overlaps(const Geometry& g, const Arrays& A, const Pair& P,
+                                                   const double* t, float dd, uint32_t q, PairStats& st) {
+    st.checks++;
+    if (dd < P.sig2_lo32) return true;
+    if (dd >= P.sig2_hi32) return false;
+    return recheck_fp64<DIM>(g, A, P, t, dd, q, st);
+}
+
+// Hard-sphere overlap of the trial site t against the stencil of space m, any position of
+// m (generic walk). FP32: bounded FP32 test plus FP64 recheck; else the reference FP64 test
+// on sorted S.
 template <int DIM, bool FP32>
-__device__ __forceinline__ bool sphere_overlaps(const Geometry& g, const Arrays& A, const Pair& P, const double* t,
-                                                float4 t32, const uint32_t* m, uint32_t self, PairStats& st) {
-    const uint32_t* __restrict__ cs = A.cell_start;
-    const float4* __restrict__ off = A.sorted_off;
-    const double4* __restrict__ ss = A.sorted_s;
-    constexpr int F_AX = DIM - 1;
-    const uint32_t sf = g.shape[F_AX];
-    const int mf = (int)m[F_AX];
-    const float wf = g.w32[F_AX];
-    const bool slow_two = (DIM == 3) ? (g.shape[0] == 2 || g.shape[1] == 2) : (g.shape[0] == 2);
-    return for_each_neighbor<DIM>(g, cs, m, [&](uint32_t q, const float* slow_shift) -> bool {
+__device__ __forceinline__ bool sphere_overlaps_generic(const Geometry& g, const Arrays& A, const Pair& P,
+                                                        const double* t, float4 t32, const uint32_t* m, uint32_t self,
+                                                        PairStats& st) {
+    const uint32_t sf = g.shape[DIM - 1];
+    const int mf = (int)m[DIM - 1];
+    return for_each_neighbor<DIM>(g, A.cell_start, m, [&](uint32_t q, const float* slow_shift) -> bool {
         if (q == self) return false;
         if (FP32) {
-            float4 o = __ldg(off + q);
+            float4 o = __ldg(A.sorted_off + q);
             int dm = __float_as_int(o.w) - mf;
             if (sf >= 4) {
                 if (dm > 1)
@@ -232,44 +353,10 @@ __device__ __forceinline__ bool sphere_overlaps(const Geometry& g, const Arrays&
                 else if (dm < -1)
                     dm += (int)sf;
             }
-            float tv[3] = {t32.x, t32.y, t32.z};
-            float ov[3] = {o.x, o.y, o.z};
-            float d[3] = {0.f, 0.f, 0.f};
-            if (DIM == 3) {
-                d[0] = tv[0] - (ov[0] + slow_shift[0]);
-                d[1] = tv[1] - (ov[1] + slow_shift[1]);
-                d[2] = tv[2] - (ov[2] + (float)dm * wf);
-            } else {
-                d[0] = tv[0] - (ov[0] + slow_shift[0]);
-                d[1] = tv[1] - (ov[1] + (float)dm * wf);
-            }
-            if (slow_two || sf == 2) {
-#pragma unroll
-                for (int a = 0; a < DIM; ++a) {
-                    if (g.shape[a] == 2) {
-                        float w = g.w32[a];
-                        if (d[a] > w)
-                            d[a] -= 2.f * w;
-                        else if (d[a] < -w)
-                            d[a] += 2.f * w;
-                    }
-                }
-            }
-            float dd = d[0] * d[0] + d[1] * d[1];
-            if (DIM == 3) dd += d[2] * d[2];
-            st.checks++;
-            if (dd < P.sig2_lo32) return true;
-            if (dd >= P.sig2_hi32) return false;
-            // inside the bound: the reference FP64 test decides
-            st.rechecks++;
-            double4 s4 = ldg4(ss + q);
-            double sv[3] = {s4.x, s4.y, s4.z};
-            double r2 = ref_dist2<DIM>(g, t, sv);
-            double e = fabs((double)dd - r2);
-            st.max_err = e > st.max_err ? e : st.max_err;
-            return r2 < P.sigma2;
+            float dd = fp32_dist2<DIM>(g, t32, o, slow_shift[0], slow_shift[1], dm);
+            return fp32_pair_overlaps<DIM>(g, A, P, t, dd, q, st);
         } else {
-            double4 s4 = ldg4(ss + q);
+            double4 s4 = ldg4(A.sorted_s + q);
             double sv[3] = {s4.x, s4.y, s4.z};
             st.checks++;
             return ref_dist2<DIM>(g, t, sv) < P.sigma2;
@@ -277,13 +364,76 @@ __device__ __forceinline__ bool sphere_overlaps(const Geometry& g, const Arrays&
     });
 }
 
-__device__ __forceinline__ void flush_stats(DeviceStats* stats, const PairStats& st, bool accepted) {
+// The same test for a space away from the fast-axis ends, over preloaded row ranges.
+// Candidates are taken one per row per step, so the loads of all rows of a step are
+// independent and in flight together. Returns kClear, kOverlap, or (FP32 only) kUncertain
+// when no pair overlaps for certain but some pair lies inside the FP32 bound; the caller
+// then decides with the generic walk, which rechecks those pairs in FP64.
+enum : int { kClear = 0, kOverlap = 1, kUncertain = 2 };
+
+template <int DIM, bool FP32>
+__device__ __forceinline__ int sphere_overlaps_rows(const Geometry& g, const Arrays& A, const Pair& P,
+                                                    const double* t, float4 t32, int mf, uint32_t self,
+                                                    const uint32_t* a0, const uint32_t* a1, PairStats& st) {
+    constexpr int R = kRows<DIM>;
+    bool uncertain = false;
+    for (uint32_t k = 0;; ++k) {
+        bool any = false;
+        if (FP32) {
+            float4 v[R];
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                uint32_t q = a0[r] + k;
+                bool ok = q < a1[r];
+                any |= ok;
+                v[r] = ok ? __ldg(A.sorted_off + q) : make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+            if (!any) return uncertain ? kUncertain : kClear;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                uint32_t q = a0[r] + k;
+                if (q < a1[r] && q != self) {
+                    int i0 = DIM == 3 ? r / 3 - 1 : 0;
+                    int i1 = DIM == 3 ? r % 3 - 1 : r - 1;
+                    float s0 = DIM == 3 ? (float)i0 * g.w32[0] : (float)i1 * g.w32[0];
+                    float s1 = DIM == 3 ? (float)i1 * g.w32[1] : 0.f;
+                    int dm = __float_as_int(v[r].w) - mf;
+                    float dd = fp32_dist2<DIM>(g, t32, v[r], s0, s1, dm);
+                    st.checks++;
+                    if (dd < P.sig2_lo32) return kOverlap;
+                    uncertain |= dd < P.sig2_hi32;
+                }
+            }
+        } else {
+            double4 v[R];
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                uint32_t q = a0[r] + k;
+                bool ok = q < a1[r];
+                any |= ok;
+                v[r] = ok ? ldg4(A.sorted_s + q) : make_double4(0.0, 0.0, 0.0, 0.0);
+            }
+            if (!any) return kClear;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                uint32_t q = a0[r] + k;
+                if (q < a1[r] && q != self) {
+                    double sv[3] = {v[r].x, v[r].y, v[r].z};
+                    st.checks++;
+                    if (ref_dist2<DIM>(g, t, sv) < P.sigma2) return kOverlap;
+                }
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ void flush_stats(DeviceStats* stats, const PairStats& st, uint32_t accepted) {
     const unsigned full = 0xffffffffu;
-    unsigned acc = __ballot_sync(full, accepted);
+    unsigned acc = __reduce_add_sync(full, accepted);
     unsigned checks = __reduce_add_sync(full, st.checks);
     unsigned rech = __reduce_add_sync(full, st.rechecks);
     if ((threadIdx.x & 31) == 0) {
-        if (acc) atomicAdd(&stats->accepted, (unsigned long long)__popc(acc));
+        if (acc) atomicAdd(&stats->accepted, (unsigned long long)acc);
         if (checks) atomicAdd(&stats->pair_checks, (unsigned long long)checks);
         if (rech) atomicAdd(&stats->rechecks, (unsigned long long)rech);
     }
@@ -291,58 +441,267 @@ __device__ __forceinline__ void flush_stats(DeviceStats* stats, const PairStats&
 }
 
 // ---- the colour pass ------------------------------------------------------------------------
-// One thread per space of the colour: ParallelSweep::generate_trial_moves for that space
-// (parallel_sweep.rs:231-278) followed by update_bodies (:283-314) for an accepted move.
+// One thread per non-empty space of the colour: ParallelSweep::generate_trial_moves for that
+// space (parallel_sweep.rs:231-278) followed by update_bodies (:283-314) for an accepted move.
 // Spaces of one colour are two spaces apart, so the in-place update of an accepted body is
 // invisible to every other trial of the colour, as in the reference.
 template <int DIM, bool FP32>
-__global__ void __launch_bounds__(128) k_sweep_sphere(Geometry g, Arrays A, Pair P, Launch L) {
-    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
-    bool accepted = false;
+__global__ void __launch_bounds__(128, HMC_SWEEP_MIN_BLOCKS) k_sweep_sphere(Geometry g, Arrays A, Pair P, Launch L) {
+    uint32_t n_accepted = 0;
     PairStats st;
-    if (tid < L.n_active) {
-        uint32_t m[3];
-        uint32_t rem = tid;
-#pragma unroll
-        for (int a = DIM - 1; a >= 0; --a) {
-            uint32_t h = rem % g.half_shape[a];
-            rem /= g.half_shape[a];
-            m[a] = 2u * h + ((L.color >> (DIM - 1 - a)) & 1u);
-        }
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x; tid < L.n_active; tid += stride) {
+        uint32_t m[3] = {0, 0, 0};
+        unpack_m<DIM>(__ldg(A.color_cells + (size_t)L.color * g.color_stride + tid), m);
         const uint32_t cell = cell_index<DIM>(g, m);
-        const uint32_t start = A.cell_start[cell];
-        const uint32_t count = A.cell_start[cell + 1] - start;
-        if (count > 0) {
-            Sfc64 rng = make_rng(L.step, L.substep, L.seed, (uint64_t)cell);
-            const uint32_t k = start + canon_range_u32(rng, count);
-            double4 b4 = A.sorted_b[k];
-            double x[3] = {b4.x, b4.y, b4.z};
-            double dv[3];
-            ball_sample<DIM>(rng, L.max_move, A.zig_x, A.zig_f, dv);
+        const uint32_t sf = g.shape[DIM - 1], mf = m[DIM - 1];
+        const bool edge = sf > 2 && (mf == 0 || mf + 1 == sf);
+        // The stencil depends only on the space: start its loads before the proposal math.
+        uint32_t a0[kRows<DIM>], a1[kRows<DIM>];
+        if (!edge) load_rows<DIM>(g, A.cell_start, m, a0, a1);
+        const uint32_t start = __ldg(A.cell_start + cell);
+        const uint32_t count = __ldg(A.cell_start + cell + 1) - start;
+        Sfc64 rng = make_rng(L.step, L.substep, L.seed, (uint64_t)cell);
+        const uint32_t k = start + canon_range_u32(rng, count);
+        double4 b4 = A.sorted_b[k];
+        double x[3] = {b4.x, b4.y, b4.z};
+        double dv[3];
+        ball_sample<DIM>(rng, L.max_move, A.zig_x, A.zig_f, dv);
 #pragma unroll
-            for (int a = 0; a < DIM; ++a) x[a] = dadd(x[a], dv[a]);
-            wrap<DIM>(g.L, x);  // W1 = wrap(propose(..))
-            uint32_t mt[3];
-            bool same = point_to_space<DIM>(g, x, mt) && cell_index<DIM>(g, mt) == cell;
-            if (same) {
-                double t[3] = {x[0], x[1], DIM == 3 ? x[2] : 0.0};
-                wrap<DIM>(g.L, t);  // delta_energy_one wraps the site again: T = wrap(W1)
-                float4 t32 = FP32 ? cell_offsets<DIM>(g, t, m) : make_float4(0.f, 0.f, 0.f, 0.f);
-                bool overlap = sphere_overlaps<DIM, FP32>(g, A, P, t, t32, m, k, st);
-                if (!overlap) {
-                    accepted = true;
-                    // update_body_properties: body = wrap(W1) = T, site = wrap(body)
-                    double s[3] = {t[0], t[1], t[2]};
-                    wrap<DIM>(g.L, s);
-                    A.sorted_b[k] = make_double4(t[0], t[1], t[2], 0.0);
-                    A.sorted_s[k] = make_double4(s[0], s[1], s[2], 0.0);
-                    A.sorted_off[k] = cell_offsets<DIM>(g, s, m);
-                    A.body_pos[A.sorted_body[k]] = make_double4(t[0], t[1], t[2], 0.0);
+        for (int a = 0; a < DIM; ++a) x[a] = dadd(x[a], dv[a]);
+        wrap_inv<DIM>(g.L, g.invL, x);  // W1 = wrap(propose(..))
+        uint32_t mt[3];
+        bool same = point_to_space<DIM>(g, x, mt) && cell_index<DIM>(g, mt) == cell;
+        if (!same) continue;
+        double t[3] = {x[0], x[1], DIM == 3 ? x[2] : 0.0};
+        wrap_inv<DIM>(g.L, g.invL, t);  // delta_energy_one wraps the site again: T = wrap(W1)
+        float4 t32 = FP32 ? cell_offsets<DIM>(g, t, m) : make_float4(0.f, 0.f, 0.f, 0.f);
+        int res = edge ? kUncertain : sphere_overlaps_rows<DIM, FP32>(g, A, P, t, t32, (int)mf, k, a0, a1, st);
+        if (res == kUncertain) {
+            PairStats st2;  // the fast path already counted its pair checks
+            res = sphere_overlaps_generic<DIM, FP32>(g, A, P, t, t32, m, k, st2) ? kOverlap : kClear;
+            st.rechecks += st2.rechecks;
+            st.max_err = st2.max_err > st.max_err ? st2.max_err : st.max_err;
+            if (edge) st.checks += st2.checks;
+        }
+        if (res == kOverlap) continue;
+        n_accepted++;
+        // update_body_properties: body = wrap(W1) = T, site = wrap(body)
+        double sv[3] = {t[0], t[1], t[2]};
+        wrap_inv<DIM>(g.L, g.invL, sv);
+        A.sorted_b[k] = make_double4(t[0], t[1], t[2], 0.0);
+        if (!FP32) A.sorted_s[k] = make_double4(sv[0], sv[1], sv[2], 0.0);
+        A.sorted_off[k] = cell_offsets<DIM>(g, sv, m);
+        A.body_pos[A.sorted_body[k]] = make_double4(t[0], t[1], t[2], 0.0);
+    }
+    flush_stats(A.stats, st, n_accepted);
+}
+
+// ---- the colour pass, staged through shared memory (3-D) ------------------------------------
+// A block owns a tile of TX x TY x TZ spaces of the colour (every second space per axis).
+// The union of their stencils is a region of (2TX+1) x (2TY+1) x (2TZ+1) spaces; the block
+// copies the bodies of the whole region into shared memory with cp.async while the threads
+// compute their FP64 trial moves, then tests every candidate pair from shared memory. Only
+// spaces of other colours lie in the region apart from the tile's own, so the staged
+// neighbours are never modified during the pass.
+constexpr int kTX = 4, kTY = 4, kTZ = 8, kTT = kTX * kTY * kTZ;
+constexpr int kRX = 2 * kTX + 1, kRY = 2 * kTY + 1, kRZ = 2 * kTZ + 1, kRC = kRX * kRY * kRZ;
+constexpr int kChunk = (kRC + kTT - 1) / kTT;
+
+template <int NT, typename T>
+__device__ __forceinline__ T block_scan_exclusive(T v, T* total, T* warp_sums) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    T x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        T y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_sums[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        T w = lane < NT / 32 ? warp_sums[lane] : T(0);
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            T y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
+        }
+        if (lane < NT / 32) warp_sums[lane] = w;
+    }
+    __syncthreads();
+    T prefix = warp > 0 ? warp_sums[warp - 1] : T(0);
+    *total = warp_sums[NT / 32 - 1];
+    return prefix + x - v;
+}
+
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
+    uint32_t d = (uint32_t)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+template <bool FP32>
+__global__ void __launch_bounds__(kTT) k_sweep_tile3(Geometry g, Arrays A, Pair P, Launch L, uint32_t cap) {
+    using Elem = typename std::conditional<FP32, float4, double4>::type;
+    extern __shared__ __align__(16) unsigned char smem[];
+    Elem* s_pos = reinterpret_cast<Elem*>(smem);
+    uint32_t* s_gstart = reinterpret_cast<uint32_t*>(smem + (size_t)cap * sizeof(Elem));
+    uint32_t* s_lstart = s_gstart + kRC;  // kRC + 1 entries
+    __shared__ uint32_t s_warp[kTT / 32];
+
+    const uint32_t tid = threadIdx.x;
+    const uint32_t sx = g.shape[0], sy = g.shape[1], sz = g.shape[2];
+    const int px = (L.color >> 2) & 1, py = (L.color >> 1) & 1, pz = L.color & 1;
+    const int hx0 = blockIdx.z * kTX, hy0 = blockIdx.y * kTY, hz0 = blockIdx.x * kTZ;
+    const int x0 = 2 * hx0 + px - 1, y0 = 2 * hy0 + py - 1, z0 = 2 * hz0 + pz - 1;
+    const uint32_t* __restrict__ cs = A.cell_start;
+
+    // 1. ranges of the region's spaces: each thread owns kChunk consecutive region spaces
+    uint32_t gs[kChunk], cnt[kChunk];
+    uint32_t sum = 0;
+#pragma unroll
+    for (int j = 0; j < kChunk; ++j) {
+        const int rc = (int)tid * kChunk + j;
+        uint32_t c0 = 0, c1 = 0;
+        if (rc < kRC) {
+            const int rz = rc % kRZ, rxy = rc / kRZ, ry = rxy % kRY, rx = rxy / kRY;
+            const uint32_t c = (wrap_index(x0 + rx, sx) * sy + wrap_index(y0 + ry, sy)) * sz + wrap_index(z0 + rz, sz);
+            c0 = __ldg(cs + c);
+            c1 = __ldg(cs + c + 1);
+        }
+        gs[j] = c0;
+        cnt[j] = c1 - c0;
+        sum += cnt[j];
+    }
+    uint32_t total;
+    uint32_t run = block_scan_exclusive<kTT>(sum, &total, s_warp);
+    const bool staged = total <= cap;
+#pragma unroll
+    for (int j = 0; j < kChunk; ++j) {
+        const int rc = (int)tid * kChunk + j;
+        if (rc < kRC) {
+            s_gstart[rc] = gs[j];
+            s_lstart[rc] = run;
+        }
+        if (staged) {
+            const Elem* src = FP32 ? reinterpret_cast<const Elem*>(A.sorted_off) : reinterpret_cast<const Elem*>(A.sorted_s);
+            for (uint32_t b = 0; b < cnt[j]; ++b) {
+                if constexpr (FP32) {
+                    cp_async16(s_pos + run + b, src + gs[j] + b);
+                } else {
+                    cp_async16(reinterpret_cast<char*>(s_pos + run + b), src + gs[j] + b);
+                    cp_async16(reinterpret_cast<char*>(s_pos + run + b) + 16,
+                               reinterpret_cast<const char*>(src + gs[j] + b) + 16);
                 }
             }
         }
+        run += cnt[j];
     }
-    flush_stats(A.stats, st, accepted);
+    cp_async_commit();
+    if (tid == kTT - 1) s_lstart[kRC] = total;
+    __syncthreads();
+
+    // 2. the trial move of this thread's space, while the copies are in flight
+    const int tx = (int)tid / (kTY * kTZ), ty = ((int)tid / kTZ) % kTY, tz = (int)tid % kTZ;
+    const bool valid = hx0 + tx < (int)g.half_shape[0] && hy0 + ty < (int)g.half_shape[1] &&
+                       hz0 + tz < (int)g.half_shape[2];
+    const int ro = ((2 * tx + 1) * kRY + (2 * ty + 1)) * kRZ + (2 * tz + 1);
+    const uint32_t own_count = valid ? s_lstart[ro + 1] - s_lstart[ro] : 0u;
+    uint32_t m[3] = {(uint32_t)(2 * (hx0 + tx) + px), (uint32_t)(2 * (hy0 + ty) + py), (uint32_t)(2 * (hz0 + tz) + pz)};
+    bool trial = false;
+    uint32_t pick = 0, k = 0;
+    double t[3] = {0.0, 0.0, 0.0};
+    float4 t32 = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (own_count > 0) {
+        const uint32_t cell = (m[0] * sy + m[1]) * sz + m[2];
+        Sfc64 rng = make_rng(L.step, L.substep, L.seed, (uint64_t)cell);
+        pick = canon_range_u32(rng, own_count);
+        k = s_gstart[ro] + pick;
+        double4 b4 = A.sorted_b[k];
+        double x[3] = {b4.x, b4.y, b4.z};
+        double dv[3];
+        ball_sample<3>(rng, L.max_move, A.zig_x, A.zig_f, dv);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) x[a] = dadd(x[a], dv[a]);
+        wrap_inv<3>(g.L, g.invL, x);
+        uint32_t mt[3];
+        trial = point_to_space<3>(g, x, mt) && mt[0] == m[0] && mt[1] == m[1] && mt[2] == m[2];
+        if (trial) {
+            t[0] = x[0];
+            t[1] = x[1];
+            t[2] = x[2];
+            wrap_inv<3>(g.L, g.invL, t);
+            if (FP32) t32 = cell_offsets<3>(g, t, m);
+        }
+    }
+    cp_async_wait_all();
+    __syncthreads();
+
+    // 3. pair tests from shared memory
+    PairStats st;
+    uint32_t n_accepted = 0;
+    if (trial) {
+        int res = kClear;
+        if (!staged) {
+            res = kUncertain;
+        } else {
+            const uint32_t self = s_lstart[ro] + pick;
+            const int mz = (int)m[2];
+            bool uncertain = false;
+#pragma unroll
+            for (int r = 0; r < 9 && res == kClear; ++r) {
+                const int dx = r / 3 - 1, dy = r % 3 - 1;
+                const int rc = ((2 * tx + 1 + dx) * kRY + (2 * ty + 1 + dy)) * kRZ + 2 * tz;
+                const uint32_t lb = s_lstart[rc], le = s_lstart[rc + 3];
+                const float s0 = (float)dx * g.w32[0], s1 = (float)dy * g.w32[1];
+                for (uint32_t q = lb; q < le; ++q) {
+                    if (q == self) continue;
+                    if constexpr (FP32) {
+                        const float4 v = s_pos[q];
+                        int dm = __float_as_int(v.w) - mz;
+                        if (dm > 1)
+                            dm -= (int)sz;
+                        else if (dm < -1)
+                            dm += (int)sz;
+                        const float dd = fp32_dist2<3>(g, t32, v, s0, s1, dm);
+                        st.checks++;
+                        if (dd < P.sig2_lo32) {
+                            res = kOverlap;
+                            break;
+                        }
+                        uncertain |= dd < P.sig2_hi32;
+                    } else {
+                        const double4 v = reinterpret_cast<const double4*>(s_pos)[q];
+                        double sv[3] = {v.x, v.y, v.z};
+                        st.checks++;
+                        if (ref_dist2<3>(g, t, sv) < P.sigma2) {
+                            res = kOverlap;
+                            break;
+                        }
+                    }
+                }
+            }
+            if (res == kClear && uncertain) res = kUncertain;
+        }
+        if (res == kUncertain) {
+            PairStats st2;
+            res = sphere_overlaps_generic<3, FP32>(g, A, P, t, t32, m, k, st2) ? kOverlap : kClear;
+            st.rechecks += st2.rechecks;
+            st.max_err = st2.max_err > st.max_err ? st2.max_err : st.max_err;
+            if (!staged) st.checks += st2.checks;
+        }
+        if (res == kClear) {
+            n_accepted = 1;
+            double sv[3] = {t[0], t[1], t[2]};
+            wrap_inv<3>(g.L, g.invL, sv);
+            A.sorted_b[k] = make_double4(t[0], t[1], t[2], 0.0);
+            if (!FP32) A.sorted_s[k] = make_double4(sv[0], sv[1], sv[2], 0.0);
+            A.sorted_off[k] = cell_offsets<3>(g, sv, m);
+            A.body_pos[A.sorted_body[k]] = make_double4(t[0], t[1], t[2], 0.0);
+        }
+    }
+    flush_stats(A.stats, st, n_accepted);
 }
 
 // ---- cell list rebuild -------------------------------------------------------------------
@@ -366,107 +725,202 @@ __global__ void k_bin(Geometry g, Arrays A, uint32_t n) {
     A.body_rank[i] = atomicAdd(&A.cell_count[cell], 1u);
 }
 
-__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* total) {
-    __shared__ uint32_t warp_sums[kScanThreads / 32];
+// Exclusive scan over a block of kScanThreads threads (T = uint32_t or packed uint64_t).
+template <typename T>
+__device__ __forceinline__ T block_exclusive_scan(T v, T* total) {
+    __shared__ T warp_sums[kScanThreads / 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    uint32_t x = v;
+    T x = v;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-        uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        T y = __shfl_up_sync(0xffffffffu, x, o);
         if (lane >= o) x += y;
     }
     if (lane == 31) warp_sums[warp] = x;
     __syncthreads();
     if (warp == 0) {
-        uint32_t w = lane < kScanThreads / 32 ? warp_sums[lane] : 0;
+        T w = lane < kScanThreads / 32 ? warp_sums[lane] : T(0);
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+            T y = __shfl_up_sync(0xffffffffu, w, o);
             if (lane >= o) w += y;
         }
         if (lane < kScanThreads / 32) warp_sums[lane] = w;
     }
     __syncthreads();
-    uint32_t warp_prefix = warp > 0 ? warp_sums[warp - 1] : 0;
+    T warp_prefix = warp > 0 ? warp_sums[warp - 1] : T(0);
     *total = warp_sums[kScanThreads / 32 - 1];
     __syncthreads();
     return warp_prefix + x - v;
 }
 
-__global__ void __launch_bounds__(kScanThreads) k_scan_reduce(Arrays A, uint32_t n_cells) {
+// Each scan thread owns kScanItems consecutive spaces. Their colours (parity bits of the
+// multi-index, last axis = bit 0, as index_to_multi_index(c, [2; N]) in hypercuboid.rs)
+// are tallied as 16-bit fields of two packed u64 words (colours 0-3 and 4-7), so one
+// 64-bit block scan per word gives every colour's exclusive prefix at once.
+template <int DIM>
+__device__ __forceinline__ void first_multi_index(const Geometry& g, uint32_t c, uint32_t* m) {
+#pragma unroll
+    for (int a = DIM - 1; a >= 0; --a) {
+        m[a] = c % g.shape[a];
+        c /= g.shape[a];
+    }
+}
+template <int DIM>
+__device__ __forceinline__ void next_multi_index(const Geometry& g, uint32_t* m) {
+#pragma unroll
+    for (int a = DIM - 1; a >= 0; --a) {
+        if (++m[a] < g.shape[a]) return;
+        m[a] = 0;
+    }
+}
+template <int DIM>
+__device__ __forceinline__ uint32_t color_of(const uint32_t* m) {
+    uint32_t color = 0;
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) color = (color << 1) | (m[a] & 1u);
+    return color;
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(kScanThreads) k_scan_reduce(Geometry g, Arrays A) {
+    const uint32_t n_cells = g.n_cells;
     uint32_t base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
-    uint32_t sum = 0, nonempty = 0;
+    uint32_t sum = 0;
+    unsigned long long lo = 0, hi = 0;
+    uint32_t m[3] = {0, 0, 0};
+    if (base < n_cells) first_multi_index<DIM>(g, base, m);
 #pragma unroll
     for (int k = 0; k < kScanItems; ++k) {
         uint32_t c = base + k;
         uint32_t v = c < n_cells ? A.cell_count[c] : 0;
         sum += v;
-        nonempty += v > 0;
+        if (v > 0) {
+            uint32_t col = color_of<DIM>(m);
+            if (col < 4)
+                lo += 1ull << (16 * col);
+            else
+                hi += 1ull << (16 * (col - 4));
+        }
+        next_multi_index<DIM>(g, m);
     }
     uint32_t total;
+    unsigned long long tlo, thi;
     block_exclusive_scan(sum, &total);
-    uint32_t ne = __reduce_add_sync(0xffffffffu, nonempty);
-    if ((threadIdx.x & 31) == 0 && ne) atomicAdd(&A.stats->nonempty, ne);
-    if (threadIdx.x == 0) A.block_sums[blockIdx.x] = total;
+    block_exclusive_scan(lo, &tlo);
+    block_exclusive_scan(hi, &thi);
+    if (threadIdx.x == 0) {
+        const uint32_t nb = gridDim.x;
+        A.block_sums[blockIdx.x] = total;
+#pragma unroll
+        for (int col = 0; col < 4; ++col) {
+            A.block_sums[(1 + col) * nb + blockIdx.x] = (uint32_t)((tlo >> (16 * col)) & 0xffffu);
+            A.block_sums[(5 + col) * nb + blockIdx.x] = (uint32_t)((thi >> (16 * col)) & 0xffffu);
+        }
+    }
 }
 
-__global__ void __launch_bounds__(1024) k_scan_block_sums(Arrays A, uint32_t n_blocks) {
-    // Single block: exclusive scan of up to 1024 * 8 block sums in place.
+// Single block: exclusive scans (in place) of the block totals of the cell counts and of
+// the nine colour tallies; writes the per-colour totals and the non-empty count.
+__global__ void __launch_bounds__(1024) k_scan_block_sums(Arrays A, uint32_t n_blocks, uint32_t n_colors) {
     __shared__ uint32_t warp_sums[32];
     constexpr int items = 8;
-    uint32_t base = threadIdx.x * items;
-    uint32_t v[items];
-    uint32_t sum = 0;
-#pragma unroll
-    for (int k = 0; k < items; ++k) {
-        v[k] = base + k < n_blocks ? A.block_sums[base + k] : 0;
-        sum += v[k];
-    }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    uint32_t x = sum;
+    uint32_t nonempty = 0;
+    for (uint32_t arr = 0; arr <= n_colors; ++arr) {
+        uint32_t* data = A.block_sums + (size_t)arr * n_blocks;
+        uint32_t b0 = threadIdx.x * items;
+        uint32_t v[items];
+        uint32_t sum = 0;
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= o) x += y;
-    }
-    if (lane == 31) warp_sums[warp] = x;
-    __syncthreads();
-    if (warp == 0) {
-        uint32_t w = warp_sums[lane];
+        for (int k = 0; k < items; ++k) {
+            v[k] = b0 + k < n_blocks ? data[b0 + k] : 0;
+            sum += v[k];
+        }
+        uint32_t x = sum;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
-            if (lane >= o) w += y;
+            uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
         }
-        warp_sums[lane] = w;
-    }
-    __syncthreads();
-    uint32_t run = (warp > 0 ? warp_sums[warp - 1] : 0) + x - sum;
+        if (lane == 31) warp_sums[warp] = x;
+        __syncthreads();
+        if (warp == 0) {
+            uint32_t w = warp_sums[lane];
 #pragma unroll
-    for (int k = 0; k < items; ++k) {
-        if (base + k < n_blocks) A.block_sums[base + k] = run;
-        run += v[k];
+            for (int o = 1; o < 32; o <<= 1) {
+                uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+                if (lane >= o) w += y;
+            }
+            warp_sums[lane] = w;
+        }
+        __syncthreads();
+        uint32_t run = (warp > 0 ? warp_sums[warp - 1] : 0) + x - sum;
+#pragma unroll
+        for (int k = 0; k < items; ++k) {
+            if (b0 + k < n_blocks) data[b0 + k] = run;
+            run += v[k];
+        }
+        if (threadIdx.x == 0 && arr > 0) {
+            A.stats->color_count[arr - 1] = warp_sums[31];
+            nonempty += warp_sums[31];
+        }
+        __syncthreads();
     }
+    if (threadIdx.x == 0) A.stats->nonempty = nonempty;
 }
 
-__global__ void __launch_bounds__(kScanThreads) k_scan_apply(Arrays A, uint32_t n_cells) {
+template <int DIM>
+__global__ void __launch_bounds__(kScanThreads) k_scan_apply(Geometry g, Arrays A) {
+    const uint32_t n_cells = g.n_cells;
+    const uint32_t nb = gridDim.x;
     uint32_t base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
     uint32_t v[kScanItems];
     uint32_t sum = 0;
+    unsigned long long lo = 0, hi = 0;
+    uint32_t m[3] = {0, 0, 0};
+    if (base < n_cells) first_multi_index<DIM>(g, base, m);
+    uint32_t m0[3] = {m[0], m[1], m[2]};
 #pragma unroll
     for (int k = 0; k < kScanItems; ++k) {
         uint32_t c = base + k;
         v[k] = c < n_cells ? A.cell_count[c] : 0;
         sum += v[k];
+        if (v[k] > 0) {
+            uint32_t col = color_of<DIM>(m);
+            if (col < 4)
+                lo += 1ull << (16 * col);
+            else
+                hi += 1ull << (16 * (col - 4));
+        }
+        next_multi_index<DIM>(g, m);
     }
     uint32_t total;
+    unsigned long long tlo, thi;
     uint32_t run = block_exclusive_scan(sum, &total) + A.block_sums[blockIdx.x];
+    unsigned long long plo = block_exclusive_scan(lo, &tlo);
+    unsigned long long phi = block_exclusive_scan(hi, &thi);
+    uint32_t pos[8];
+#pragma unroll
+    for (int col = 0; col < 8; ++col) {
+        uint32_t within = col < 4 ? (uint32_t)((plo >> (16 * col)) & 0xffffu) : (uint32_t)((phi >> (16 * (col - 4))) & 0xffffu);
+        pos[col] = (col < (1 << DIM) ? A.block_sums[(1 + col) * nb + blockIdx.x] : 0u) + within;
+    }
+    m[0] = m0[0];
+    m[1] = m0[1];
+    m[2] = m0[2];
 #pragma unroll
     for (int k = 0; k < kScanItems; ++k) {
         uint32_t c = base + k;
         if (c < n_cells) A.cell_start[c] = run;
         run += v[k];
         if (c + 1 == n_cells) A.cell_start[n_cells] = run;
+        if (v[k] > 0) {
+            uint32_t col = color_of<DIM>(m);
+            A.color_cells[(size_t)col * g.color_stride + pos[col]] = pack_m<DIM>(m);
+            pos[col] += 1;
+        }
+        next_multi_index<DIM>(g, m);
     }
 }
 
@@ -477,39 +931,44 @@ __global__ void k_scatter(Arrays A, uint32_t n) {
 }
 
 // One thread per space: order its bodies by index (the order in which update_checkerboard
-// pushes them, parallel_sweep.rs:194-200, which IndexedRandom::choose indexes) and gather
-// B, S = wrap(B), the FP32 offsets and orientations into cell order.
-template <int DIM>
-__global__ void k_finalize(Geometry g, Arrays A) {
-    uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= g.n_cells) return;
-    uint32_t s = A.cell_start[c], e = A.cell_start[c + 1];
-    for (uint32_t k = s + 1; k < e; ++k) {
-        uint32_t v = A.sorted_body[k];
-        uint32_t j = k;
-        while (j > s && A.sorted_body[j - 1] > v) {
-            A.sorted_body[j] = A.sorted_body[j - 1];
-            --j;
-        }
-        A.sorted_body[j] = v;
-    }
+// pushes them, parallel_sweep.rs:194-200, which IndexedRandom::choose indexes), gather B,
+// the FP32 offsets of S = wrap(B) (and S itself when WRITE_S) and orientations into cell
+// order.
+template <int DIM, bool WRITE_S>
+__global__ void __launch_bounds__(128) k_finalize(Geometry g, Arrays A) {
+    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = c < g.n_cells;
+    uint32_t s = 0, e = 0;
     uint32_t m[3] = {0, 0, 0};
-    uint32_t rem = c;
+    if (valid) {
+        s = A.cell_start[c];
+        e = A.cell_start[c + 1];
+        for (uint32_t k = s + 1; k < e; ++k) {
+            uint32_t v = A.sorted_body[k];
+            uint32_t j = k;
+            while (j > s && A.sorted_body[j - 1] > v) {
+                A.sorted_body[j] = A.sorted_body[j - 1];
+                --j;
+            }
+            A.sorted_body[j] = v;
+        }
+        uint32_t rem = c;
 #pragma unroll
-    for (int a = DIM - 1; a >= 0; --a) {
-        m[a] = rem % g.shape[a];
-        rem /= g.shape[a];
-    }
-    for (uint32_t k = s; k < e; ++k) {
-        uint32_t i = A.sorted_body[k];
-        A.slot_of_body[i] = k;
-        double4 b = A.body_pos[i];
-        A.sorted_b[k] = b;
-        double sv[3] = {b.x, b.y, b.z};
-        wrap<DIM>(g.L, sv);
-        A.sorted_s[k] = make_double4(sv[0], sv[1], sv[2], 0.0);
-        A.sorted_off[k] = cell_offsets<DIM>(g, sv, m);
-        if (A.sorted_q) A.sorted_q[k] = A.body_ori[i];
+        for (int a = DIM - 1; a >= 0; --a) {
+            m[a] = rem % g.shape[a];
+            rem /= g.shape[a];
+        }
+        for (uint32_t k = s; k < e; ++k) {
+            uint32_t i = A.sorted_body[k];
+            A.slot_of_body[i] = k;
+            double4 b = A.body_pos[i];
+            A.sorted_b[k] = b;
+            double sv[3] = {b.x, b.y, b.z};
+            wrap_inv<DIM>(g.L, g.invL, sv);
+            if (WRITE_S) A.sorted_s[k] = make_double4(sv[0], sv[1], sv[2], 0.0);
+            A.sorted_off[k] = cell_offsets<DIM>(g, sv, m);
+            if (A.sorted_q) A.sorted_q[k] = A.body_ori[i];
+        }
     }
 }
 
@@ -551,21 +1010,21 @@ __global__ void k_eval_sphere(Geometry g, Arrays A, Pair P, const uint64_t* bodi
     if (i < n) {
         double4 w = trial[i];
         double t[3] = {w.x, w.y, DIM == 3 ? w.z : 0.0};
-        wrap<DIM>(g.L, t);
+        wrap_inv<DIM>(g.L, g.invL, t);
         uint32_t m[3];
         bool ok = point_to_space<DIM>(g, t, m);
         uint8_t dec = 0;
         if (ok) {
             uint32_t self = A.slot_of_body[bodies[i]];
             float4 t32 = FP32 ? cell_offsets<DIM>(g, t, m) : make_float4(0.f, 0.f, 0.f, 0.f);
-            dec = sphere_overlaps<DIM, FP32>(g, A, P, t, t32, m, self, st) ? 0 : 1;
+            dec = sphere_overlaps_generic<DIM, FP32>(g, A, P, t, t32, m, self, st) ? 0 : 1;
         } else {
             atomicOr(&A.stats->error_flags, kErrOutsideCheckerboard);
         }
         decisions[i] = dec;
         rechecked[i] = st.rechecks > 0;
     }
-    flush_stats(A.stats, st, false);
+    flush_stats(A.stats, st, 0u);
 }
 
 template <typename T>
@@ -575,7 +1034,7 @@ inline uint32_t blocks_for(T n, uint32_t threads) {
 
 }  // namespace
 
-cudaError_t launch_rebuild(int dim, const Geometry& g, const Arrays& a, uint32_t n, cudaStream_t s) {
+cudaError_t launch_rebuild(int dim, const Geometry& g, const Arrays& a, uint32_t n, bool write_s, cudaStream_t s) {
     cudaError_t e = cudaMemsetAsync(a.cell_count, 0, sizeof(uint32_t) * g.n_cells, s);
     if (e != cudaSuccess) return e;
     if (n > 0) {
@@ -585,21 +1044,80 @@ cudaError_t launch_rebuild(int dim, const Geometry& g, const Arrays& a, uint32_t
             k_bin<3><<<blocks_for(n, 256), 256, 0, s>>>(g, a, n);
     }
     uint32_t nb = blocks_for(g.n_cells, kScanTile);
-    k_scan_reduce<<<nb, kScanThreads, 0, s>>>(a, g.n_cells);
-    k_scan_block_sums<<<1, 1024, 0, s>>>(a, nb);
-    k_scan_apply<<<nb, kScanThreads, 0, s>>>(a, g.n_cells);
-    if (n > 0) k_scatter<<<blocks_for(n, 256), 256, 0, s>>>(a, n);
     if (dim == 2)
-        k_finalize<2><<<blocks_for(g.n_cells, 128), 128, 0, s>>>(g, a);
+        k_scan_reduce<2><<<nb, kScanThreads, 0, s>>>(g, a);
     else
-        k_finalize<3><<<blocks_for(g.n_cells, 128), 128, 0, s>>>(g, a);
+        k_scan_reduce<3><<<nb, kScanThreads, 0, s>>>(g, a);
+    k_scan_block_sums<<<1, 1024, 0, s>>>(a, nb, 1u << dim);
+    if (dim == 2)
+        k_scan_apply<2><<<nb, kScanThreads, 0, s>>>(g, a);
+    else
+        k_scan_apply<3><<<nb, kScanThreads, 0, s>>>(g, a);
+    if (n > 0) k_scatter<<<blocks_for(n, 256), 256, 0, s>>>(a, n);
+    uint32_t fb = blocks_for(g.n_cells, 128);
+    if (dim == 2) {
+        if (write_s)
+            k_finalize<2, true><<<fb, 128, 0, s>>>(g, a);
+        else
+            k_finalize<2, false><<<fb, 128, 0, s>>>(g, a);
+    } else {
+        if (write_s)
+            k_finalize<3, true><<<fb, 128, 0, s>>>(g, a);
+        else
+            k_finalize<3, false><<<fb, 128, 0, s>>>(g, a);
+    }
     return cudaGetLastError();
 }
 
+size_t tile_smem_bytes(bool fp32, uint32_t cap) {
+    return (size_t)cap * (fp32 ? sizeof(float4) : sizeof(double4)) + sizeof(uint32_t) * (2 * kRC + 1);
+}
+
+bool tile_kernel_applies(int dim, const Geometry& g) {
+    return dim == 3 && g.shape[0] >= (uint32_t)kRX && g.shape[1] >= (uint32_t)kRY && g.shape[2] >= (uint32_t)kRZ;
+}
+
 cudaError_t launch_sweep_sphere(int dim, bool fp32, const Geometry& g, const Arrays& a, const Pair& p,
-                                const Launch& l, cudaStream_t s) {
-    if (l.n_active == 0) return cudaSuccess;
+                                const Launch& l, uint32_t tile_cap, cudaStream_t s) {
+    if (l.n_active == 0) return cudaSuccess;  // no non-empty space of this colour
+    if (tile_cap > 0 && tile_kernel_applies(dim, g)) {
+        dim3 grid((g.half_shape[2] + kTZ - 1) / kTZ, (g.half_shape[1] + kTY - 1) / kTY,
+                  (g.half_shape[0] + kTX - 1) / kTX);
+        size_t smem = tile_smem_bytes(fp32, tile_cap);
+        static size_t smem_set[2] = {0, 0};
+        if (smem > smem_set[fp32]) {
+            cudaError_t e = fp32 ? cudaFuncSetAttribute(k_sweep_tile3<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                        (int)smem)
+                                 : cudaFuncSetAttribute(k_sweep_tile3<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                        (int)smem);
+            if (e != cudaSuccess) return e;
+            smem_set[fp32] = smem;
+        }
+        if (fp32)
+            k_sweep_tile3<true><<<grid, kTT, smem, s>>>(g, a, p, l, tile_cap);
+        else
+            k_sweep_tile3<false><<<grid, kTT, smem, s>>>(g, a, p, l, tile_cap);
+        return cudaGetLastError();
+    }
+    // Grid-stride over the colour's list with at most one resident wave of blocks.
+    static int max_blocks[2][2] = {{0, 0}, {0, 0}};
+    int& mb = max_blocks[dim == 3][fp32];
+    if (mb == 0) {
+        int dev = 0, sms = 0, per_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaError_t e;
+        if (dim == 2)
+            e = fp32 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_sphere<2, true>, 128, 0)
+                     : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_sphere<2, false>, 128, 0);
+        else
+            e = fp32 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_sphere<3, true>, 128, 0)
+                     : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_sphere<3, false>, 128, 0);
+        if (e != cudaSuccess) return e;
+        mb = sms * (per_sm > 0 ? per_sm : 1);
+    }
     uint32_t grid = blocks_for(l.n_active, 128);
+    if (grid > (uint32_t)mb) grid = (uint32_t)mb;
     if (dim == 2) {
         if (fp32)
             k_sweep_sphere<2, true><<<grid, 128, 0, s>>>(g, a, p, l);

@@ -180,34 +180,41 @@ HMC_HD double standard_normal(Sfc64& r, const double* __restrict__ zx, const dou
 }
 
 // ---- deterministic cube root and half-angle sin/cos -------------------------------------
-// Exponent split, three Halley steps and one Newton step on an FMA-evaluated residual.
-// Only correctly rounded operations, so host and device results agree bit for bit.
+// Cube root without division: x = m 2^(3q + r) with m in [1, 2); y ~ m^(-1/3) from a
+// quadratic Chebyshev fit refined by three Newton steps y += y (1 - m y^3) / 3; then
+// cbrt(x) ~ m y^2 cbrt(2^r) 2^q, corrected once by a Newton step on the FMA-evaluated
+// residual c^3 - m 2^r. Only correctly rounded operations (mul, fma), so host and device
+// agree bit for bit; the result is within one ulp of the true cube root.
 HMC_HD double portable_cbrt(double x) {
     if (x == 0.0 || !(fabs(x) <= 1.79769313486231570e308)) return x;
-    bool neg = x < 0.0;
+    const bool neg = x < 0.0;
     double ax = neg ? -x : x;
     int extra = 0;
     if (ax < 2.2250738585072014e-308) {
         ax = dmul(ax, 18014398509481984.0);
         extra = -18;
     }
-    uint64_t b = as_bits(ax);
-    int e = (int)((b >> 52) & 0x7ff) - 1023;
-    double m = as_double((b & 0x000FFFFFFFFFFFFFULL) | 0x3FF0000000000000ULL);
-    int q = (e >= 0) ? e / 3 : -((-e + 2) / 3);
-    int rr = e - 3 * q;
-    double a = dmul(m, rr == 0 ? 1.0 : (rr == 1 ? 2.0 : 4.0));
-    double y = dadd(1.0, dmul(dsub(a, 1.0), 1.0 / 7.0));
+    const uint64_t b = as_bits(ax);
+    const int e = (int)((b >> 52) & 0x7ff) - 1023;
+    const double m = as_double((b & 0x000FFFFFFFFFFFFFULL) | 0x3FF0000000000000ULL);
+    const int q = (e >= 0) ? e / 3 : -((-e + 2) / 3);
+    const int rr = e - 3 * q;
+    double y = dfma(dfma(0.09303886055928341, m, -0.48224275792479104), m, 1.387389992245347);
     for (int it = 0; it < 3; ++it) {
-        double y3 = dmul(dmul(y, y), y);
-        y = ddiv(dmul(y, dadd(y3, dmul(2.0, a))), dadd(dmul(2.0, y3), a));
+        const double y3 = dmul(dmul(y, y), y);
+        const double eps = dfma(-m, y3, 1.0);
+        y = dfma(dmul(y, eps), 0.3333333333333333, y);
     }
-    double y2 = dmul(y, y);
-    double y2lo = dfma(y, y, -y2);
-    double resid = dadd(dfma(y2, y, -a), dmul(y2lo, y));
-    y = dsub(y, ddiv(resid, dmul(3.0, y2)));
-    double scale = as_double((uint64_t)(q + extra + 1023) << 52);
-    double res = dmul(y, scale);
+    const double a = dmul(m, rr == 0 ? 1.0 : (rr == 1 ? 2.0 : 4.0));
+    const double k = rr == 0 ? 1.0 : (rr == 1 ? 1.2599210498948732 : 1.5874010519681994);
+    const double ik2 = rr == 0 ? 0.3333333333333333 : (rr == 1 ? 0.20998684164914552 : 0.13228342099734997);
+    double c = dmul(dmul(dmul(m, y), y), k);
+    const double c2 = dmul(c, c);
+    const double c2lo = dfma(c, c, -c2);
+    const double resid = dadd(dfma(c2, c, -a), dmul(c2lo, c));
+    c = dsub(c, dmul(resid, dmul(dmul(y, y), ik2)));
+    const double scale = as_double((uint64_t)(q + extra + 1023) << 52);
+    const double res = dmul(c, scale);
     return neg ? -res : res;
 }
 
@@ -250,6 +257,31 @@ HMC_HD void portable_sincos(double h, double* s, double* c) {
     *c = pc;
 }
 
+// x / d, correctly rounded, for a divisor d fixed per system with precomputed rd = RN(1/d).
+// On the device: q = RN(q0 + r rd) with q0 = RN(x rd) and r = x - q0 d (exact by FMA), then
+// q is accepted only if the exact residual x - q d proves |x/d - q| below half the spacing of
+// doubles around q (a quarter ulp when q is a power of two); otherwise the IEEE division runs.
+// The result therefore always equals x / d.
+HMC_HD double div_fixed(double x, double d, double rd) {
+#ifdef __CUDA_ARCH__
+    const double q0 = __dmul_rn(x, rd);
+    const double r0 = __fma_rn(-q0, d, x);
+    const double q1 = __fma_rn(r0, rd, q0);
+    const double r1 = __fma_rn(-q1, d, x);
+    const uint64_t bits = (uint64_t)__double_as_longlong(q1);
+    const uint32_t ex = (uint32_t)((bits >> 52) & 0x7ffu);
+    if (ex > 60u && ex < 1990u) {
+        const uint32_t hex = (bits & 0x000FFFFFFFFFFFFFULL) ? ex - 53u : ex - 54u;
+        const double h = __longlong_as_double((long long)((uint64_t)hex << 52));
+        if (fabs(r1) < __dmul_rn(h, fabs(d))) return q1;
+    }
+    return __ddiv_rn(x, d);
+#else
+    (void)rd;
+    return x / d;
+#endif
+}
+
 // ---- hoomd-vector arithmetic -------------------------------------------------------------
 // InnerProduct::dot (cartesian.rs:293-296): mul_add fold from 0.0.
 template <int N>
@@ -266,6 +298,18 @@ HMC_HD void wrap(const double* L, double* x) {
 #pragma unroll
     for (int a = 0; a < N; ++a) {
         double lam = ddiv(x[a], L[a]);
+        lam = dsub(lam, round(lam));
+        if (lam == 0.5) lam = -0.5;
+        x[a] = dmul(lam, L[a]);
+    }
+}
+
+// wrap with the division by the box length done by div_fixed (same result as wrap).
+template <int N>
+HMC_HD void wrap_inv(const double* L, const double* invL, double* x) {
+#pragma unroll
+    for (int a = 0; a < N; ++a) {
+        double lam = div_fixed(x[a], L[a], invL[a]);
         lam = dsub(lam, round(lam));
         if (lam == 0.5) lam = -0.5;
         x[a] = dmul(lam, L[a]);

@@ -19,7 +19,7 @@
 //   * standard normal: the 256-layer ziggurat of Marsaglia & Tsang (2000) in the
 //     ZIGNOR form of Doornik (2005), tables computed below from R and V.
 // cbrt and the half-angle sin/cos use the deterministic algorithms in
-// portable_cbrt / portable_sincos (Halley iteration, Taylor series) so that the
+// portable_cbrt / portable_sincos (Newton iteration, Taylor series) so that the
 // CUDA library, which uses the same algorithms, proposes bit-identical moves.
 #include "hmc_oracle.h"
 
@@ -140,8 +140,10 @@ double standard_normal(Sfc64& rng) {
 }
 
 // ---- deterministic cbrt and half-angle sin/cos --------------------------------------
-// Cube root by exponent splitting and three Halley steps, y <- y (y^3 + 2a) / (2y^3 + a).
-// Uses only correctly rounded operations, so host and device agree bit for bit.
+// Cube root without division: x = m 2^(3q + r), m in [1, 2); y ~ m^(-1/3) from a quadratic
+// Chebyshev fit and three Newton steps y += y (1 - m y^3) / 3; cbrt ~ m y^2 cbrt(2^r) 2^q,
+// corrected by one Newton step on the FMA-evaluated residual. Only correctly rounded
+// operations, so the CUDA library, which uses the same algorithm, agrees bit for bit.
 double portable_cbrt(double x) {
     if (x == 0.0 || !std::isfinite(x)) return x;
     bool neg = x < 0.0;
@@ -156,19 +158,22 @@ double portable_cbrt(double x) {
     double m = bits_to_double((b & 0x000FFFFFFFFFFFFFULL) | 0x3FF0000000000000ULL);
     int q = (e >= 0) ? e / 3 : -((-e + 2) / 3);
     int r = e - 3 * q;
-    double a = m * (r == 0 ? 1.0 : (r == 1 ? 2.0 : 4.0));
-    double y = 1.0 + (a - 1.0) * (1.0 / 7.0);
+    double y = std::fma(std::fma(0.09303886055928341, m, -0.48224275792479104), m, 1.387389992245347);
     for (int it = 0; it < 3; ++it) {
-        double y3 = y * y * y;
-        y = y * (y3 + 2.0 * a) / (2.0 * y3 + a);
+        double y3 = (y * y) * y;
+        double eps = std::fma(-m, y3, 1.0);
+        y = std::fma(y * eps, 0.3333333333333333, y);
     }
-    // One Newton step on an accurately evaluated residual y^3 - a.
-    double y2 = y * y;
-    double y2lo = std::fma(y, y, -y2);
-    double resid = std::fma(y2, y, -a) + y2lo * y;
-    y = y - resid / (3.0 * y2);
+    double a = m * (r == 0 ? 1.0 : (r == 1 ? 2.0 : 4.0));
+    double k = r == 0 ? 1.0 : (r == 1 ? 1.2599210498948732 : 1.5874010519681994);
+    double ik2 = r == 0 ? 0.3333333333333333 : (r == 1 ? 0.20998684164914552 : 0.13228342099734997);
+    double c = ((m * y) * y) * k;
+    double c2 = c * c;
+    double c2lo = std::fma(c, c, -c2);
+    double resid = std::fma(c2, c, -a) + c2lo * c;
+    c = c - resid * ((y * y) * ik2);
     double scale = bits_to_double((uint64_t)(q + extra + 1023) << 52);
-    double res = y * scale;
+    double res = c * scale;
     return neg ? -res : res;
 }
 
