@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cfloat>
 #include <cmath>
 #include <cstdarg>
@@ -54,9 +55,12 @@ bool compute_dimensions(int dim, const double* L, double range, double* width, u
 
 }  // namespace
 
+// A context is shared by its systems: it is freed when hmc_context_destroy has been called
+// and the last system created from it is destroyed, in whichever order these happen.
 struct hmc_context {
     int device = 0;
     double* zig = nullptr;  // 2 x 257 doubles: x then f
+    std::atomic<int> refs{1};
 };
 
 struct hmc_system {
@@ -211,11 +215,17 @@ hmc_status hmc_context_create(const hmc_device_opts* opts, hmc_context** out) {
     return HMC_OK;
 }
 
-void hmc_context_destroy(hmc_context* c) {
-    if (!c) return;
+static void context_release(hmc_context* c) {
+    if (c->refs.fetch_sub(1) != 1) return;
     cudaSetDevice(c->device);
     if (c->zig) cudaFree(c->zig);
+    cudaGetLastError();  // a destructor reports nothing: leave no sticky error behind
     delete c;
+}
+
+void hmc_context_destroy(hmc_context* c) {
+    if (!c) return;
+    context_release(c);
 }
 
 void hmc_system_destroy(hmc_system* s) {
@@ -227,7 +237,10 @@ void hmc_system_destroy(hmc_system* s) {
         if (e) cudaEventDestroy(e);
     if (s->host_stats) cudaFreeHost(s->host_stats);
     if (s->own_stream) cudaStreamDestroy(s->own_stream);
+    cudaGetLastError();  // a destructor reports nothing: leave no sticky error behind
+    hmc_context* c = s->ctx;
     delete s;
+    context_release(c);
 }
 
 hmc_status hmc_system_create(hmc_context* ctx, const hmc_system_desc* d, const double* positions,
@@ -247,6 +260,7 @@ hmc_status hmc_system_create(hmc_context* ctx, const hmc_system_desc* d, const d
 
     HMC_CUDA(cudaSetDevice(ctx->device));
     hmc_system* s = new hmc_system();
+    ctx->refs.fetch_add(1);
     s->ctx = ctx;
     s->dim = (int)d->dim;
     s->n = d->n_bodies;

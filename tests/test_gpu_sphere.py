@@ -186,3 +186,16 @@ def test_errors_are_status_codes(ctx):
     assert e.value.status == hm.INVALID_ARGUMENT
     # the context stays usable after errors
     assert g.sweep(TRANSLATE, 0.3, 1.0, FP64).total() == 1
+
+
+def test_context_released_after_its_last_system(ctx):
+    # Destroying a context while a system still uses it defers the release to the
+    # system's destruction; nothing leaks into later calls.
+    c2 = Context(0)
+    pos, L = lattice.hard_sphere_box(512, 0.4, 3, 21)
+    g = Microstate(c2, Periodic(1.0, [L] * 3), pos, PairwiseCutoff(HardSphere(1.0)), seed=21)
+    c2.close()
+    assert g.sweep(TRANSLATE, 0.2, 1.0, FP32_RECHECK).total() >= 512
+    g.close()
+    h = Microstate(ctx, Periodic(1.0, [L] * 3), pos, PairwiseCutoff(HardSphere(1.0)), seed=21)
+    assert h.overlap_count() == 0
