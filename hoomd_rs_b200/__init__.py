@@ -99,6 +99,7 @@ SIGNATURES = {
     "hmc_overlap_check": (C.c_int, [_vp, C.POINTER(C.c_uint64)]),
     "hmc_eval_moves": (C.c_int, [_vp, C.POINTER(hmc_injected_move), C.c_uint64, C.c_double, C.c_uint32, _u8p,
                                  _u8p]),
+    "hmc_overlap_count_noalloc": (C.c_int, [_vp, C.c_uint64, C.c_uint32, _dp, C.c_double, C.c_double, _vp, _vp]),
     "hmc_profile_enable": (C.c_int, [_vp, C.c_int]),
     "hmc_profile_read": (C.c_int, [_vp, C.POINTER(hmc_profile), C.c_int]),
 }

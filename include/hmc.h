@@ -170,6 +170,33 @@ hmc_status hmc_overlap_check(hmc_system* sys, uint64_t* n_overlaps);
 hmc_status hmc_eval_moves(hmc_system* sys, const hmc_injected_move* moves, uint64_t n, double temperature,
                           uint32_t precision, uint8_t* decisions, uint8_t* rechecked);
 
+/* ---- overlap count into caller buffers, with no device allocation ----
+ * No counterpart in the reference (hoomd-rs has no GPU path); it serves callers that must
+ * not call cudaMalloc when they run the check, for example a framework that hands out all
+ * device memory from its own pre-reserved pool, or a plugin that may not grow the
+ * process's device footprint after start-up. It counts the pairs (i < j) of hard spheres
+ * of the given diameter whose sites overlap through any periodic image, with the same
+ * arithmetic as hmc_overlap_check, and needs no hmc_context or hmc_system.
+ *
+ *   positions      device pointer, n_bodies * dim FP64 body positions (as hmc_get_state
+ *                  returns them; sites are wrap(position))
+ *   edge_lengths   host pointer, dim FP64 box edge lengths
+ *   boundary_range Periodic::new maximum_interaction_range; 0 = diameter
+ *   overlaps       device pointer to one uint64_t; set to the count
+ *   cuda_stream    cudaStream_t (NULL: the default stream); runs on the current device
+ *
+ * Its cell list lives in a fixed device array inside the library (about 3.4 MB, held on
+ * every GPU that loads the library until the process exits), so n_bodies is limited to
+ * HMC_NOALLOC_MAX_BODIES (HMC_INVALID_ARGUMENT beyond). The first call on a device looks
+ * up that array's device address (cudaGetSymbolAddress) with the device current; make it
+ * before capturing any stream into a CUDA graph. All calls share the array: calls that
+ * overlap in time on the GPU race with each other. Errors are reported by status only. */
+#define HMC_NOALLOC_MAX_BODIES 65536u
+#define HMC_NOALLOC_MAX_CELLS 65536u
+hmc_status hmc_overlap_count_noalloc(const double* positions, uint64_t n_bodies, uint32_t dim,
+                                     const double* edge_lengths, double diameter, double boundary_range,
+                                     uint64_t* overlaps, void* cuda_stream);
+
 /* ---- profiling ---- */
 hmc_status hmc_profile_enable(hmc_system* sys, int enable);
 hmc_status hmc_profile_read(hmc_system* sys, hmc_profile* out, int reset);
