@@ -98,7 +98,8 @@ SIGNATURES = {
     "hmc_tune": (C.c_int, [_vp, C.POINTER(hmc_sweep_params), C.c_double, C.c_uint32, C.c_uint32]),
     "hmc_overlap_check": (C.c_int, [_vp, C.POINTER(C.c_uint64)]),
     "hmc_eval_moves": (C.c_int, [_vp, C.POINTER(hmc_injected_move), C.c_uint64, C.c_double, C.c_uint32, _u8p,
-                                 _u8p]),
+                                 _u8p, _dp]),
+    "hmc_total_energy": (C.c_int, [_vp, _dp]),
     "hmc_overlap_count_noalloc": (C.c_int, [_vp, C.c_uint64, C.c_uint32, _dp, C.c_double, C.c_double, _vp, _vp]),
     "hmc_profile_enable": (C.c_int, [_vp, C.c_int]),
     "hmc_profile_read": (C.c_int, [_vp, C.POINTER(hmc_profile), C.c_int]),
@@ -162,9 +163,34 @@ class HardSphere:
 
 
 @dataclass
+class LennardJones:
+    """hoomd_interaction::univariate::LennardJones (lennard_jones.rs:79-124)."""
+    epsilon: float = 1.0
+    sigma: float = 1.0
+
+
+@dataclass
+class Shifted:
+    """hoomd_interaction::univariate::Shifted (shifted.rs:57-102): f(r) - f(r_shift)."""
+    f: LennardJones
+    r_shift: float
+
+
+@dataclass
+class Isotropic:
+    """hoomd_interaction::pairwise::Isotropic (isotropic.rs:88-187)."""
+    interaction: Shifted
+    r_cut: float
+
+    @property
+    def maximum_interaction_range(self) -> float:
+        return self.r_cut
+
+
+@dataclass
 class PairwiseCutoff:
     """hoomd_interaction::PairwiseCutoff (pairwise_cutoff.rs:140)."""
-    pair: HardSphere
+    pair: object
 
 
 @dataclass
@@ -228,6 +254,12 @@ class Microstate:
         if isinstance(pair, HardSphere):
             d.interaction = HARD_SPHERE
             d.diameter = pair.diameter
+        elif isinstance(pair, Isotropic) and isinstance(pair.interaction, Shifted):
+            d.interaction = LENNARD_JONES
+            d.lj_epsilon = pair.interaction.f.epsilon
+            d.lj_sigma = pair.interaction.f.sigma
+            d.lj_r_cut = pair.r_cut
+            d.lj_r_shift = pair.interaction.r_shift
         else:
             raise HmcError(NOT_SUPPORTED, f"{type(pair).__name__}")
         d.boundary_range = boundary.maximum_interaction_range
@@ -298,21 +330,30 @@ class Microstate:
         _check(_lib.hmc_sweep(self._h, C.byref(p), C.byref(c)))
         return Count(c.accepted, c.rejected, c.rechecks, c.pair_checks, c.max_fp32_error)
 
-    def eval_moves(self, bodies, positions, u=None, temperature: float = 1.0, precision: int = FP64):
+    def eval_moves(self, bodies, positions, u=None, temperature: float = 1.0, precision: int = FP64,
+                   return_delta_h: bool = False):
         bodies = np.asarray(bodies, dtype=np.uint64)
         pos = np.asarray(positions, dtype=np.float64).reshape(len(bodies), self.dim)
         n = len(bodies)
-        moves = (hmc_injected_move * n)()
-        for i in range(n):
-            moves[i].body = int(bodies[i])
-            for a in range(self.dim):
-                moves[i].position[a] = pos[i, a]
-            moves[i].u = -1.0 if u is None else float(u[i])
+        arr = np.zeros(n, dtype=[("body", np.uint64), ("position", np.float64, 3), ("orientation", np.float64, 4),
+                                 ("u", np.float64)])
+        arr["body"] = bodies
+        arr["position"][:, : self.dim] = pos
+        arr["u"] = -1.0 if u is None else np.asarray(u, dtype=np.float64)
+        moves = arr.ctypes.data_as(C.POINTER(hmc_injected_move))
         dec = np.zeros(n, dtype=np.uint8)
         rech = np.zeros(n, dtype=np.uint8)
+        dh = np.zeros(n)
         _check(_lib.hmc_eval_moves(self._h, moves, n, temperature, precision, dec.ctypes.data_as(_u8p),
-                                   rech.ctypes.data_as(_u8p)))
+                                   rech.ctypes.data_as(_u8p), dh.ctypes.data_as(_dp)))
+        if return_delta_h:
+            return dec.astype(bool), rech.astype(bool), dh
         return dec.astype(bool), rech.astype(bool)
+
+    def total_energy(self) -> float:
+        e = C.c_double()
+        _check(_lib.hmc_total_energy(self._h, C.byref(e)))
+        return e.value
 
 
 class ParallelSweep:
@@ -340,6 +381,7 @@ class ParallelSweep:
         return c
 
 
-__all__ = ["Context", "Count", "HardSphere", "HmcError", "Isothermal", "Microstate", "PairwiseCutoff",
+__all__ = ["Context", "Count", "HardSphere", "HmcError", "Isothermal", "Isotropic", "LennardJones", "Microstate",
+           "PairwiseCutoff", "Shifted",
            "ParallelSweep", "Periodic", "Translate", "load_library", "SIGNATURES", "FP64", "FP32_RECHECK",
            "TRANSLATE", "ROTATE"]

@@ -128,6 +128,43 @@ void sphere_bound(hmc_system* s) {
     s->pair.sig2_hi32 = std::nextafter((float)(sigma2 + B), INFINITY);
 }
 
+// LennardJones::energy (lennard_jones.rs:107-111), the host copy of the device formula.
+double lj_energy_host(double four_eps, double sigma, double r) {
+    double sr = sigma / r;
+    double s2 = sr * sr, s4 = s2 * s2, s8 = s4 * s4;
+    return four_eps * (s4 * s8 - s2 * s4);
+}
+
+// Parameters of Isotropic<Shifted<LennardJones>> and the error bounds of its FP32 pass:
+// E bounds the per-axis FP32 displacement error (as for spheres); the cut-off band is the
+// r^2 interval in which the FP32 r^2 cannot decide r^2 < r_cut^2, and band_energy bounds the
+// energy the FP64 pass may count for a pair in it.
+void lj_setup(hmc_system* s, double eps, double sigma, double rcut, double rshift) {
+    const double u32 = std::ldexp(1.0, -24), u64 = std::ldexp(1.0, -53);
+    Pair& P = s->pair;
+    P.lj_sigma = sigma;
+    P.lj_four_eps = 4.0 * eps;
+    P.lj_rcut2 = rcut * rcut;
+    P.lj_e_shift = lj_energy_host(P.lj_four_eps, sigma, rshift);
+    P.lj_sigma2_32 = (float)(sigma * sigma);
+    P.lj_four_eps32 = (float)P.lj_four_eps;
+    P.lj_e_shift32 = (float)P.lj_e_shift;
+    double wmax = 0, Lmax = 0;
+    for (int a = 0; a < s->dim; ++a) {
+        wmax = std::max(wmax, s->geom.width[a]);
+        Lmax = std::max(Lmax, s->geom.L[a]);
+    }
+    // the FP32 sigma^2 and 4 eps carry one rounding each; fold them into E generously
+    const double E = 8.0 * u32 * wmax + 16.0 * u64 * (Lmax + wmax) + 4.0 * u32 * sigma;
+    P.lj_disp_err = (float)(E * 1.01);
+    const double band = 2.0 * (3.5 * E * (rcut + E) + 3.1 * u32 * rcut * rcut);
+    P.lj_rcut2_lo32 = std::nextafter((float)(P.lj_rcut2 - band), -INFINITY);
+    P.lj_rcut2_hi32 = std::nextafter((float)(P.lj_rcut2 + band), INFINITY);
+    double e_lo = lj_energy_host(P.lj_four_eps, sigma, std::sqrt(std::max(P.lj_rcut2 - 2.0 * band, 0.0))) - P.lj_e_shift;
+    double e_hi = lj_energy_host(P.lj_four_eps, sigma, std::sqrt(P.lj_rcut2 + 2.0 * band)) - P.lj_e_shift;
+    P.lj_band_energy = (float)(2.0 * std::max(std::fabs(e_lo), std::fabs(e_hi)) + 1e-7);
+}
+
 hmc_status read_stats(hmc_system* s) {
     HMC_CUDA(cudaMemcpyAsync(s->host_stats, s->arr.stats, sizeof(DeviceStats), cudaMemcpyDeviceToHost, s->stream));
     HMC_CUDA(cudaStreamSynchronize(s->stream));
@@ -254,9 +291,13 @@ hmc_status hmc_system_create(hmc_context* ctx, const hmc_system_desc* d, const d
     for (uint32_t a = 0; a < d->dim; ++a)
         if (!(d->edge_lengths[a] > 0.0) || !std::isfinite(d->edge_lengths[a]))
             return fail(HMC_INVALID_ARGUMENT, "edge length %u must be positive", a);
-    if (d->interaction != HMC_HARD_SPHERE)
+    if (d->interaction != HMC_HARD_SPHERE && d->interaction != HMC_LENNARD_JONES)
         return fail(HMC_NOT_SUPPORTED, "interaction %u is not available in this build", d->interaction);
-    if (!(d->diameter > 0.0)) return fail(HMC_INVALID_ARGUMENT, "diameter must be positive");
+    if (d->interaction == HMC_HARD_SPHERE && !(d->diameter > 0.0))
+        return fail(HMC_INVALID_ARGUMENT, "diameter must be positive");
+    if (d->interaction == HMC_LENNARD_JONES &&
+        (!(d->lj_sigma > 0.0) || !(d->lj_r_cut > 0.0) || !(d->lj_r_shift > 0.0) || !std::isfinite(d->lj_epsilon)))
+        return fail(HMC_INVALID_ARGUMENT, "Lennard-Jones sigma, r_cut and r_shift must be positive");
 
     HMC_CUDA(cudaSetDevice(ctx->device));
     hmc_system* s = new hmc_system();
@@ -268,7 +309,8 @@ hmc_status hmc_system_create(hmc_context* ctx, const hmc_system_desc* d, const d
     s->substep = d->substep;
     s->seed = d->seed;
     s->interaction = d->interaction;
-    s->pair_range = d->diameter;  // HardSphere::maximum_interaction_range (hard_shape.rs:171-175)
+    // maximum_interaction_range: HardSphere (hard_shape.rs:171-175) = diameter; Isotropic = r_cut
+    s->pair_range = d->interaction == HMC_LENNARD_JONES ? d->lj_r_cut : d->diameter;
     s->boundary_range = d->boundary_range > 0.0 ? d->boundary_range : s->pair_range;
     s->body_range = d->body_interaction_range > 0.0 ? d->body_interaction_range : s->pair_range;
     for (int a = 0; a < 3; ++a) s->geom.L[a] = a < s->dim ? d->edge_lengths[a] : 1.0;
@@ -318,8 +360,12 @@ hmc_status hmc_system_create(hmc_context* ctx, const hmc_system_desc* d, const d
     }
     s->geom.n_cells = (uint32_t)cells;
     s->geom.color_stride = (uint32_t)(cells >> s->dim);
-    s->pair.sigma2 = d->diameter * d->diameter;  // diameter.powi(2)
-    sphere_bound(s);
+    if (d->interaction == HMC_HARD_SPHERE) {
+        s->pair.sigma2 = d->diameter * d->diameter;  // diameter.powi(2)
+        sphere_bound(s);
+    } else {
+        lj_setup(s, d->lj_epsilon, d->lj_sigma, d->lj_r_cut, d->lj_r_shift);
+    }
     // Shared-memory staging capacity: 1.5x the mean body count of a 9 x 9 x 17 region plus
     // slack, within 100 KB per block; a denser system keeps the global-memory pass.
     // The direct (global-memory) pass measured faster than the shared-memory tiled pass on
@@ -438,7 +484,7 @@ hmc_status hmc_get_state(hmc_system* s, double* positions, double* orientations,
 hmc_status hmc_sweep(hmc_system* s, const hmc_sweep_params* p, hmc_count* out) {
     if (!s || !p) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
     if (p->struct_size < sizeof(hmc_sweep_params)) return fail(HMC_INVALID_ARGUMENT, "hmc_sweep_params.struct_size");
-    if (p->move != HMC_TRANSLATE) return fail(HMC_NOT_SUPPORTED, "hard spheres take translation moves only");
+    if (p->move != HMC_TRANSLATE) return fail(HMC_NOT_SUPPORTED, "spheres and Lennard-Jones sites take translation moves only");
     if (!(p->maximum > 0.0) || !std::isfinite(p->maximum)) return fail(HMC_INVALID_ARGUMENT, "maximum must be positive");
     // The 2-D ball sampler squares the radius; keep it far from overflow. Moves longer
     // than the box are equivalent modulo wrapping, so this rejects no useful input.
@@ -465,6 +511,7 @@ hmc_status hmc_sweep(hmc_system* s, const hmc_sweep_params* p, hmc_count* out) {
         L.step = s->step;
         L.seed = s->seed;
         L.max_move = p->maximum;
+        L.kt = p->temperature;
         L.n_bodies = (uint32_t)s->n;
         uint32_t color_count[8];
         for (uint32_t c = 0; c < colors; ++c) color_count[c] = s->host_stats->color_count[c];
@@ -474,7 +521,10 @@ hmc_status hmc_sweep(hmc_system* s, const hmc_sweep_params* p, hmc_count* out) {
             for (uint32_t c = 0; c < colors; ++c) {
                 L.color = c;
                 L.n_active = color_count[c];
-                HMC_CUDA(launch_sweep_sphere(s->dim, fp32, s->geom, s->arr, s->pair, L, s->tile_cap[fp32], s->stream));
+                if (s->interaction == HMC_LENNARD_JONES)
+                    HMC_CUDA(launch_sweep_lj(s->dim, fp32, s->geom, s->arr, s->pair, L, s->stream));
+                else
+                    HMC_CUDA(launch_sweep_sphere(s->dim, fp32, s->geom, s->arr, s->pair, L, s->tile_cap[fp32], s->stream));
                 s->prof.kernel_launches += 1;
             }
             s->substep += 1;  // increment_substep after every full colour set
@@ -535,6 +585,7 @@ hmc_status hmc_tune(hmc_system* s, hmc_sweep_params* p, double target, uint32_t 
 
 hmc_status hmc_overlap_check(hmc_system* s, uint64_t* n_overlaps) {
     if (!s || !n_overlaps) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
+    if (s->interaction != HMC_HARD_SPHERE) return fail(HMC_NOT_SUPPORTED, "overlap check of a soft potential");
     HMC_CUDA(cudaSetDevice(s->ctx->device));
     hmc_status st = rebuild(s, true);
     if (st) return st;
@@ -546,11 +597,33 @@ hmc_status hmc_overlap_check(hmc_system* s, uint64_t* n_overlaps) {
     return HMC_OK;
 }
 
+hmc_status hmc_total_energy(hmc_system* s, double* energy) {
+    if (!s || !energy) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
+    if (s->interaction == HMC_HARD_SPHERE) {
+        uint64_t n = 0;
+        hmc_status st = hmc_overlap_check(s, &n);
+        if (st) return st;
+        *energy = n > 0 ? INFINITY : 0.0;
+        return HMC_OK;
+    }
+    HMC_CUDA(cudaSetDevice(s->ctx->device));
+    hmc_status st = rebuild(s, true);
+    if (st) return st;
+    double* d = reinterpret_cast<double*>(&s->arr.stats->overlaps);  // 8 zeroed bytes after the rebuild
+    HMC_CUDA(launch_energy_lj(s->dim, s->geom, s->arr, s->pair, (uint32_t)s->n, d, s->stream));
+    s->prof.kernel_launches += 1;
+    if ((st = read_stats(s))) return st;
+    if ((st = check_flags(s))) return st;
+    std::memcpy(energy, &s->host_stats->overlaps, sizeof(double));
+    return HMC_OK;
+}
+
 hmc_status hmc_eval_moves(hmc_system* s, const hmc_injected_move* moves, uint64_t n, double temperature,
-                          uint32_t precision, uint8_t* decisions, uint8_t* rechecked) {
+                          uint32_t precision, uint8_t* decisions, uint8_t* rechecked, double* delta_h) {
     if (!s || (n && (!moves || !decisions))) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
     if (precision > HMC_FP32_RECHECK) return fail(HMC_INVALID_ARGUMENT, "precision");
-    (void)temperature;
+    if (s->interaction == HMC_LENNARD_JONES && !(temperature > 0.0))
+        return fail(HMC_INVALID_ARGUMENT, "temperature must be positive");
     if (n == 0) return HMC_OK;
     if (n >= (1ull << 31)) return fail(HMC_INVALID_ARGUMENT, "too many moves");
     HMC_CUDA(cudaSetDevice(s->ctx->device));
@@ -562,25 +635,43 @@ hmc_status hmc_eval_moves(hmc_system* s, const hmc_injected_move* moves, uint64_
     if (st) return st;
     std::vector<uint64_t> hb(n);
     std::vector<double4> ht(n);
+    std::vector<double> hu(n);
     for (uint64_t i = 0; i < n; ++i) {
         hb[i] = moves[i].body;
         ht[i] = make_double4(moves[i].position[0], moves[i].position[1], s->dim == 3 ? moves[i].position[2] : 0.0, 0.0);
+        hu[i] = moves[i].u;
     }
+    const bool lj = s->interaction == HMC_LENNARD_JONES;
     uint64_t* db = nullptr;
     double4* dt = nullptr;
+    double* du = nullptr;
+    double* dh = nullptr;
     uint8_t* dd = nullptr;
     cudaError_t e = cudaMallocAsync((void**)&db, sizeof(uint64_t) * n, s->stream);
     if (e == cudaSuccess) e = cudaMallocAsync((void**)&dt, sizeof(double4) * n, s->stream);
+    if (e == cudaSuccess) e = cudaMallocAsync((void**)&du, sizeof(double) * n, s->stream);
+    if (e == cudaSuccess) e = cudaMallocAsync((void**)&dh, sizeof(double) * n, s->stream);
     if (e == cudaSuccess) e = cudaMallocAsync((void**)&dd, 2 * n, s->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(db, hb.data(), sizeof(uint64_t) * n, cudaMemcpyHostToDevice, s->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(dt, ht.data(), sizeof(double4) * n, cudaMemcpyHostToDevice, s->stream);
-    if (e == cudaSuccess)
-        e = launch_eval_sphere(s->dim, precision == HMC_FP32_RECHECK, s->geom, s->arr, s->pair, db, dt, (uint32_t)n, dd,
-                               dd + n, s->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(du, hu.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(dh, 0, sizeof(double) * n, s->stream);
+    if (e == cudaSuccess) {
+        if (lj)
+            e = launch_eval_lj(s->dim, precision == HMC_FP32_RECHECK, s->geom, s->arr, s->pair, db, dt, du, temperature,
+                               (uint32_t)n, dd, dd + n, dh, s->stream);
+        else
+            e = launch_eval_sphere(s->dim, precision == HMC_FP32_RECHECK, s->geom, s->arr, s->pair, db, dt,
+                                   (uint32_t)n, dd, dd + n, s->stream);
+    }
     std::vector<uint8_t> hd(2 * n);
+    std::vector<double> hh(n);
     if (e == cudaSuccess) e = cudaMemcpyAsync(hd.data(), dd, 2 * n, cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(hh.data(), dh, sizeof(double) * n, cudaMemcpyDeviceToHost, s->stream);
     if (db) cudaFreeAsync(db, s->stream);
     if (dt) cudaFreeAsync(dt, s->stream);
+    if (du) cudaFreeAsync(du, s->stream);
+    if (dh) cudaFreeAsync(dh, s->stream);
     if (dd) cudaFreeAsync(dd, s->stream);
     cudaError_t e2 = cudaStreamSynchronize(s->stream);
     if (e == cudaSuccess) e = e2;
@@ -589,6 +680,13 @@ hmc_status hmc_eval_moves(hmc_system* s, const hmc_injected_move* moves, uint64_
     if ((st = check_flags(s))) return st;
     std::memcpy(decisions, hd.data(), n);
     if (rechecked) std::memcpy(rechecked, hd.data() + n, n);
+    if (delta_h) {
+        if (lj) {
+            std::memcpy(delta_h, hh.data(), sizeof(double) * n);
+        } else {
+            for (uint64_t i = 0; i < n; ++i) delta_h[i] = hd[i] ? 0.0 : INFINITY;
+        }
+    }
     return HMC_OK;
 }
 

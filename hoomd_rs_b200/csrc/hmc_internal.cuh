@@ -71,6 +71,19 @@ struct Pair {
     double sigma2;     // HardSphere diameter^2
     float sig2_lo32;   // FP32 certain-overlap threshold (sigma^2 - bound, rounded down)
     float sig2_hi32;   // FP32 certain-clear threshold (sigma^2 + bound, rounded up)
+    // Isotropic<Shifted<LennardJones>> (isotropic.rs:147-156, shifted.rs:92-94,
+    // lennard_jones.rs:107-111)
+    double lj_sigma;
+    double lj_four_eps;   // 4.0 * epsilon
+    double lj_rcut2;      // r_cut.powi(2)
+    double lj_e_shift;    // LennardJones::energy(r_shift)
+    float lj_sigma2_32;   // sigma^2 in FP32
+    float lj_four_eps32;
+    float lj_e_shift32;
+    float lj_rcut2_lo32;  // r_cut^2 minus the r^2 error bound: below, the pair is inside for certain
+    float lj_rcut2_hi32;  // r_cut^2 plus the bound: at or above, outside for certain
+    float lj_disp_err;    // per-axis FP32 displacement error bound E
+    float lj_band_energy; // bound on |pair energy| for a pair inside the cut-off band
 };
 
 // One sweep launch: counter, move and colour.
@@ -81,6 +94,7 @@ struct Launch {
     uint32_t color;       // parity offsets: bit a of color (last axis = bit 0) is the offset on axis a
     uint32_t n_active;    // non-empty spaces of this colour (length of its list)
     double max_move;      // Translate maximum distance
+    double kt;            // Isothermal temperature
     uint32_t n_bodies;
 };
 
@@ -97,6 +111,14 @@ size_t tile_smem_bytes(bool fp32, uint32_t cap);
 bool tile_kernel_applies(int dim, const Geometry& g);
 cudaError_t launch_overlap_sphere(int dim, const Geometry& g, const Arrays& a, const Pair& p, uint32_t n,
                                   cudaStream_t s);
+cudaError_t launch_sweep_lj(int dim, bool fp32, const Geometry& g, const Arrays& a, const Pair& p, const Launch& l,
+                            cudaStream_t s);
+// delta_energy_one in FP64 for injected trial positions (LJ); u < 0 means no decision needed.
+cudaError_t launch_eval_lj(int dim, bool fp32, const Geometry& g, const Arrays& a, const Pair& p,
+                           const uint64_t* bodies, const double4* trial, const double* u, double kt, uint32_t n,
+                           uint8_t* decisions, uint8_t* rechecked, double* delta_h, cudaStream_t s);
+cudaError_t launch_energy_lj(int dim, const Geometry& g, const Arrays& a, const Pair& p, uint32_t n, double* out,
+                             cudaStream_t s);
 // Injected moves: positions (n x 4 doubles), result decisions and recheck flags.
 cudaError_t launch_eval_sphere(int dim, bool fp32, const Geometry& g, const Arrays& a, const Pair& p,
                                const uint64_t* bodies, const double4* trial, uint32_t n, uint8_t* decisions,

@@ -18,7 +18,7 @@
 
 #include <type_traits>
 
-#include "hmc_internal.cuh"
+#include "hmc_device.cuh"
 
 namespace hmc {
 namespace {
@@ -32,280 +32,6 @@ namespace {
 constexpr int kScanThreads = 256;
 constexpr int kScanItems = 8;
 constexpr int kScanTile = kScanThreads * kScanItems;
-
-// ---- checkerboard maps --------------------------------------------------------------------
-// point_to_space_index for a periodic checkerboard (hypercuboid.rs:85-128). Returns false
-// for None. m receives the multi-index.
-template <int DIM>
-__device__ __forceinline__ bool point_to_space(const Geometry& g, const double* x, uint32_t* m) {
-#pragma unroll
-    for (int a = 0; a < DIM; ++a) {
-        double p = dsub(x[a], g.origin[a]);
-        double f = floor(div_fixed(p, g.width[a], g.invW[a]));
-        if (!(f >= 0.0)) return false;
-        if (f > 4.0e9) return false;
-        uint32_t idx = (uint32_t)f;
-        if (idx == g.shape[a]) idx = 0;
-        if (idx > g.shape[a]) return false;
-        m[a] = idx;
-    }
-    return true;
-}
-template <int DIM>
-__device__ __forceinline__ uint32_t cell_index(const Geometry& g, const uint32_t* m) {
-    uint32_t idx = 0;
-#pragma unroll
-    for (int a = 0; a < DIM; ++a) idx = idx * g.shape[a] + m[a];
-    return idx;
-}
-
-// FP32 offset of a site from the lower corner of its cell (multi-index m), periodic frame.
-template <int DIM>
-__device__ __forceinline__ float4 cell_offsets(const Geometry& g, const double* s, const uint32_t* m) {
-    float o[3] = {0.f, 0.f, 0.f};
-#pragma unroll
-    for (int a = 0; a < DIM; ++a) {
-        double off = dsub(dsub(s[a], g.origin[a]), dmul((double)m[a], g.width[a]));
-        if (off > 1.5 * g.width[a])
-            off = dsub(off, g.L[a]);
-        else if (off < -0.5 * g.width[a])
-            off = dadd(off, g.L[a]);
-        o[a] = __double2float_rn(off);
-    }
-    return make_float4(o[0], o[1], o[2], __int_as_float((int)m[DIM - 1]));
-}
-
-// Squared distance between a trial site t and a site s exactly as the reference computes
-// it against s's primary and ghost images: the ghost rule of generate_ghosts_in_range
-// (boundary/periodic/cuboid.rs:109-161) gives the image translations that exist, and
-// distance_squared (hoomd-vector/src/cartesian.rs:339-342) folds (t - image)^2 from 0.0.
-// Each axis keeps the image with the smaller |difference|; rounding is monotone, so this
-// is the minimum of the reference's d^2 over all images.
-template <int DIM>
-__device__ __forceinline__ double ref_dist2(const Geometry& g, const double* t, const double* s) {
-    bool inside = true;
-#pragma unroll
-    for (int a = 0; a < DIM; ++a) inside = inside && (s[a] >= -g.half[a]) && (s[a] < g.half[a]);
-    double p = 0.0;
-#pragma unroll
-    for (int a = 0; a < DIM; ++a) {
-        double d = dsub(t[a], s[a]);
-        if (inside) {
-            double tr = 0.0;
-            bool has = false;
-            if (s[a] > g.ghost_hi[a]) {
-                tr = -g.L[a];
-                has = true;
-            } else if (s[a] < g.ghost_lo[a]) {
-                tr = g.L[a];
-                has = true;
-            }
-            if (has) {
-                double d2 = dsub(t[a], dadd(s[a], tr));
-                if (fabs(d2) < fabs(d)) d = d2;
-            }
-        }
-        p = dadd(p, dmul(d, d));
-    }
-    return p;
-}
-
-// ---- trial moves --------------------------------------------------------------------------
-// Ball::sample (hoomd-vector/src/distribution.rs:41-69).
-template <int DIM>
-__device__ __forceinline__ void ball_sample(Sfc64& r, double radius, const double* zx, const double* zf,
-                                            double* out) {
-    if (DIM == 2) {
-        for (;;) {
-            double c0 = uniform01(r);
-            double c1 = uniform01(r);
-            double v0 = dmul(dsub(dmul(c0, 2.0), 1.0), radius);
-            double v1 = dmul(dsub(dmul(c1, 2.0), 1.0), radius);
-            double n2 = dfma(v1, v1, dfma(v0, v0, 0.0));
-            if (n2 < dmul(radius, radius)) {
-                out[0] = v0;
-                out[1] = v1;
-                out[2] = 0.0;
-                return;
-            }
-        }
-    } else {
-        double p[3] = {0.0, 0.0, 0.0};
-#pragma unroll 1
-        for (int i = 0; i < 3; ++i) {
-            double z = standard_normal(r, zx, zf);
-            if (i == 0)
-                p[0] = z;
-            else if (i == 1)
-                p[1] = z;
-            else
-                p[2] = z;
-        }
-        double norm = dsqrt(dot<3>(p, p));
-        double u = uniform01(r);
-        double scale = dmul(ddiv(radius, norm), portable_cbrt(u));
-        out[0] = dmul(p[0], scale);
-        out[1] = dmul(p[1], scale);
-        out[2] = dmul(p[2], scale);
-    }
-}
-
-// ---- neighbour stencil over cell-ordered rows ----------------------------------------------
-__device__ __forceinline__ uint32_t wrap_index(int i, uint32_t n) {
-    return i < 0 ? (uint32_t)(i + (int)n) : ((uint32_t)i >= n ? (uint32_t)i - n : (uint32_t)i);
-}
-
-// Packed multi-index of a space in a colour list: 10 bits per axis in 3-D, 16 in 2-D.
-template <int DIM>
-__device__ __forceinline__ uint32_t pack_m(const uint32_t* m) {
-    return DIM == 3 ? (m[0] | (m[1] << 10) | (m[2] << 20)) : (m[0] | (m[1] << 16));
-}
-template <int DIM>
-__device__ __forceinline__ void unpack_m(uint32_t p, uint32_t* m) {
-    if (DIM == 3) {
-        m[0] = p & 1023u;
-        m[1] = (p >> 10) & 1023u;
-        m[2] = p >> 20;
-    } else {
-        m[0] = p & 0xffffu;
-        m[1] = p >> 16;
-    }
-}
-
-// Rows of the 3^DIM stencil around space m, as ranges of cell-ordered slots. A row is
-// the run of three spaces m[last]-1 .. m[last]+1 along the fast axis at one offset of the
-// slow axes; it is contiguous unless it wraps around the fast axis (m[last] at either end).
-// Row r (r = 3*(i0+1) + (i1+1) in 3-D, i1+1 in 2-D) has slow-axis offsets (i0, i1). When a
-// slow axis has two spaces its offset -1 names the same space as +1; that row is left empty.
-template <int DIM>
-constexpr int kRows = DIM == 3 ? 9 : 3;
-
-template <int DIM>
-__device__ __forceinline__ void load_rows(const Geometry& g, const uint32_t* __restrict__ cs, const uint32_t* m,
-                                          uint32_t* a0, uint32_t* a1) {
-    const uint32_t sf = g.shape[DIM - 1], mf = m[DIM - 1];
-    const uint32_t lo = sf == 2 ? 0u : mf - 1u;
-    const uint32_t hi = sf == 2 ? 2u : mf + 2u;
-#pragma unroll
-    for (int r = 0; r < kRows<DIM>; ++r) {
-        int i0 = DIM == 3 ? r / 3 - 1 : 0;
-        int i1 = DIM == 3 ? r % 3 - 1 : r - 1;
-        uint32_t base;
-        bool skip;
-        if (DIM == 3) {
-            uint32_t c0 = wrap_index((int)m[0] + i0, g.shape[0]);
-            uint32_t c1 = wrap_index((int)m[1] + i1, g.shape[1]);
-            skip = (i0 == -1 && g.shape[0] == 2) || (i1 == -1 && g.shape[1] == 2);
-            base = (c0 * g.shape[1] + c1) * sf;
-        } else {
-            uint32_t c0 = wrap_index((int)m[0] + i1, g.shape[0]);
-            skip = i1 == -1 && g.shape[0] == 2;
-            base = c0 * sf;
-        }
-        a0[r] = skip ? 0u : __ldg(cs + base + lo);
-        a1[r] = skip ? 0u : __ldg(cs + base + hi);
-    }
-}
-
-// Generic stencil walk (any position of m, including the fast-axis ends): calls
-// f(q, slow_shift) for every slot q of the 3^DIM spaces around m and stops when f returns
-// true. Each space is visited once, also when an axis has two spaces.
-template <int DIM, typename F>
-__device__ __forceinline__ bool for_each_neighbor(const Geometry& g, const uint32_t* __restrict__ cell_start,
-                                                  const uint32_t* m, F&& f) {
-    constexpr int F_AX = DIM - 1;
-    const uint32_t sf = g.shape[F_AX];
-    const uint32_t mf = m[F_AX];
-    int lo0 = (DIM == 3) ? (g.shape[0] == 2 ? 0 : -1) : 0;
-    int hi0 = (DIM == 3) ? 1 : 0;
-    int lo1 = (g.shape[DIM == 3 ? 1 : 0] == 2) ? 0 : -1;
-    for (int i0 = lo0; i0 <= hi0; ++i0) {
-        for (int i1 = lo1; i1 <= 1; ++i1) {
-            uint32_t row_base;
-            float slow_shift[2];
-            if (DIM == 3) {
-                uint32_t c0 = wrap_index((int)m[0] + i0, g.shape[0]);
-                uint32_t c1 = wrap_index((int)m[1] + i1, g.shape[1]);
-                row_base = (c0 * g.shape[1] + c1) * sf;
-                slow_shift[0] = (float)i0 * g.w32[0];
-                slow_shift[1] = (float)i1 * g.w32[1];
-            } else {
-                uint32_t c0 = wrap_index((int)m[0] + i1, g.shape[0]);
-                row_base = c0 * sf;
-                slow_shift[0] = (float)i1 * g.w32[0];
-                slow_shift[1] = 0.f;
-            }
-            uint32_t a0, a1, b0 = 0, b1 = 0;
-            if (sf == 2) {
-                a0 = cell_start[row_base];
-                a1 = cell_start[row_base + 2];
-            } else if (mf >= 1 && mf + 1 < sf) {
-                a0 = cell_start[row_base + mf - 1];
-                a1 = cell_start[row_base + mf + 2];
-            } else if (mf == 0) {
-                a0 = cell_start[row_base];
-                a1 = cell_start[row_base + 2];
-                b0 = cell_start[row_base + sf - 1];
-                b1 = cell_start[row_base + sf];
-            } else {
-                a0 = cell_start[row_base + sf - 2];
-                a1 = cell_start[row_base + sf];
-                b0 = cell_start[row_base];
-                b1 = cell_start[row_base + 1];
-            }
-            for (uint32_t q = a0; q < a1; ++q)
-                if (f(q, slow_shift)) return true;
-            for (uint32_t q = b0; q < b1; ++q)
-                if (f(q, slow_shift)) return true;
-        }
-    }
-    return false;
-}
-
-// Read-only load of a double4 as two 16-byte loads through the non-coherent cache.
-__device__ __forceinline__ double4 ldg4(const double4* p) {
-    const double2* q = reinterpret_cast<const double2*>(p);
-    double2 a = __ldg(q), b = __ldg(q + 1);
-    return make_double4(a.x, a.y, b.x, b.y);
-}
-
-// Per-thread statistics of the FP32 path.
-struct PairStats {
-    uint32_t checks = 0;
-    uint32_t rechecks = 0;
-    double max_err = 0.0;
-};
-
-// The FP32 displacement (trial minus candidate) from the FP32 offsets, given the shift of
-// the candidate's space corner along the slow axes and its fast-axis space offset dm.
-template <int DIM>
-__device__ __forceinline__ float fp32_dist2(const Geometry& g, float4 t32, float4 o, float s0, float s1, int dm) {
-    float d[3];
-    if (DIM == 3) {
-        d[0] = t32.x - (o.x + s0);
-        d[1] = t32.y - (o.y + s1);
-        d[2] = t32.z - (o.z + (float)dm * g.w32[2]);
-    } else {
-        d[0] = t32.x - (o.x + s0);
-        d[1] = t32.y - (o.y + (float)dm * g.w32[1]);
-        d[2] = 0.f;
-    }
-    if (g.any_two) {
-#pragma unroll
-        for (int a = 0; a < DIM; ++a) {
-            if (g.shape[a] == 2) {
-                float w = g.w32[a];
-                if (d[a] > w)
-                    d[a] -= 2.f * w;
-                else if (d[a] < -w)
-                    d[a] += 2.f * w;
-            }
-        }
-    }
-    float dd = d[0] * d[0] + d[1] * d[1];
-    if (DIM == 3) dd += d[2] * d[2];
-    return dd;
-}
 
 // FP64 recheck of a pair whose FP32 d^2 lies inside the bound.
 // S of the candidate is wrap(B), recomputed from its body position.
@@ -369,7 +95,6 @@ __device__ __forceinline__ bool sphere_overlaps_generic(const Geometry& g, const
 // independent and in flight together. Returns kClear, kOverlap, or (FP32 only) kUncertain
 // when no pair overlaps for certain but some pair lies inside the FP32 bound; the caller
 // then decides with the generic walk, which rechecks those pairs in FP64.
-enum : int { kClear = 0, kOverlap = 1, kUncertain = 2 };
 
 template <int DIM, bool FP32>
 __device__ __forceinline__ int sphere_overlaps_rows(const Geometry& g, const Arrays& A, const Pair& P,
@@ -425,19 +150,6 @@ __device__ __forceinline__ int sphere_overlaps_rows(const Geometry& g, const Arr
             }
         }
     }
-}
-
-__device__ __forceinline__ void flush_stats(DeviceStats* stats, const PairStats& st, uint32_t accepted) {
-    const unsigned full = 0xffffffffu;
-    unsigned acc = __reduce_add_sync(full, accepted);
-    unsigned checks = __reduce_add_sync(full, st.checks);
-    unsigned rech = __reduce_add_sync(full, st.rechecks);
-    if ((threadIdx.x & 31) == 0) {
-        if (acc) atomicAdd(&stats->accepted, (unsigned long long)acc);
-        if (checks) atomicAdd(&stats->pair_checks, (unsigned long long)checks);
-        if (rech) atomicAdd(&stats->rechecks, (unsigned long long)rech);
-    }
-    if (st.max_err > 0.0) atomicMax(&stats->max_err_bits, (unsigned long long)__double_as_longlong(st.max_err));
 }
 
 // ---- the colour pass ------------------------------------------------------------------------

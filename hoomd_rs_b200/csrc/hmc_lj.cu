@@ -1,0 +1,476 @@
+// Lennard-Jones Metropolis sweep: PairwiseCutoff<Isotropic<Shifted<LennardJones>>>.
+//
+// delta_energy_one (hoomd-interaction/src/pairwise_cutoff.rs:919-941) sums the pair energy of
+// the trial site and of the current site over every other site within r_cut; the Metropolis
+// test (hoomd-mc/src/parallel_sweep.rs:267-268) accepts when dH <= 0, else draws u and accepts
+// when u < exp(-dH / kT). At the survey's LJ state (rho = 0.8, r_cut = 2.5) a space holds ~13
+// bodies, so a colour pass has few trials (~5k for 2^19 bodies) with ~360 candidates each:
+// one warp per trial, lanes striding along each stencil row (coalesced), warp reductions of
+// the sums.
+//
+// FP32 + recheck: the warp sums FP32 pair energies together with a rigorous bound B on
+// |dU32 - dU64| (r^2 error from the FP32 offsets, propagated through dE/dr^2; rounding of the
+// energy formula; summation chains; the FP64 sum's own error). A decision that B cannot
+// change is taken from the FP32 sums; otherwise the warp recomputes dU in FP64 with exactly
+// the lane assignment and reduction order of the plain FP64 pass, so decisions equal it.
+#include <cuda_runtime.h>
+
+#include "hmc_device.cuh"
+
+namespace hmc {
+namespace {
+
+constexpr float kU32 = 5.9604645e-8f;  // 2^-24
+
+// Pair energy in FP64 exactly as the reference evaluates it: Isotropic::site_pair_energy
+// (isotropic.rs:147-156: r^2 >= r_cut^2 -> 0, else energy(sqrt(r^2))), Shifted::energy
+// (shifted.rs:92-94: f(r) - f(r_shift)), LennardJones::energy (lennard_jones.rs:107-111:
+// 4 eps ((sigma/r)^12 - (sigma/r)^6) with powi by repeated squaring).
+__device__ __forceinline__ double lj_pair64(const Pair& P, double r2) {
+    if (r2 >= P.lj_rcut2) return 0.0;
+    const double r = dsqrt(r2);
+    const double sr = ddiv(P.lj_sigma, r);
+    const double s2 = dmul(sr, sr), s4 = dmul(s2, s2), s8 = dmul(s4, s4);
+    return dsub(dmul(P.lj_four_eps, dsub(dmul(s4, s8), dmul(s2, s4))), P.lj_e_shift);
+}
+
+// FP32 pair energy and a bound on its error against the exact energy of the FP64 sites.
+// dr2: bound on |r2_32 - r2_exact|.
+__device__ __forceinline__ void lj_pair32(const Pair& P, float r2, float dr2, float& e, float& err) {
+    if (r2 >= P.lj_rcut2_hi32) {
+        e = 0.f;
+        err = 0.f;
+        return;
+    }
+    if (r2 >= P.lj_rcut2_lo32) {  // the FP64 pass may or may not count this pair
+        e = 0.f;
+        err = P.lj_band_energy;
+        return;
+    }
+    const float sr2 = __fdiv_rn(P.lj_sigma2_32, r2);
+    const float sr6 = sr2 * sr2 * sr2;
+    const float b = P.lj_four_eps32 * sr6;  // 4 eps (sigma/r)^6
+    const float a = b * sr6;                // 4 eps (sigma/r)^12
+    e = (a - b) - P.lj_e_shift32;
+    // |dE/dr^2| = (6a - 3b) / r^2 at most (6a + 3b) / r^2; 1.1 covers its variation over
+    // [r2 - dr2, r2 + dr2] and the FP32 evaluation of this bound.
+    err = 1.1f * ((6.f * a + 3.f * b) * __fdiv_ru(dr2, r2) + 16.f * kU32 * (a + b + fabsf(P.lj_e_shift32)));
+}
+
+// Error bound of an FP32 r^2 formed from FP32 offsets: per-axis displacement error E,
+// sum |d_a| <= sqrt(3) r.
+__device__ __forceinline__ float r2_error(const Pair& P, float r2) {
+    const float E = P.lj_disp_err;
+    const float r = __fsqrt_ru(r2) * 1.0001f;
+    return 3.5f * E * (r + E) + 3.1f * kU32 * r2;
+}
+
+// The stencil rows of space m as at most two slot ranges each (two when the row wraps around
+// the fast axis), with the slow-axis shifts of each row.
+template <int DIM>
+struct Stencil {
+    uint32_t lo[kRows<DIM>][2], hi[kRows<DIM>][2];
+    float s0[kRows<DIM>], s1[kRows<DIM>];
+    bool used[kRows<DIM>];
+};
+
+template <int DIM>
+__device__ __forceinline__ void make_stencil(const Geometry& g, const uint32_t* __restrict__ cs, const uint32_t* m,
+                                             Stencil<DIM>& st) {
+    const uint32_t sf = g.shape[DIM - 1], mf = m[DIM - 1];
+#pragma unroll
+    for (int r = 0; r < kRows<DIM>; ++r) {
+        const int i0 = DIM == 3 ? r / 3 - 1 : 0;
+        const int i1 = DIM == 3 ? r % 3 - 1 : r - 1;
+        uint32_t base;
+        bool skip;
+        if (DIM == 3) {
+            skip = (i0 == -1 && g.shape[0] == 2) || (i1 == -1 && g.shape[1] == 2);
+            base = (wrap_index((int)m[0] + i0, g.shape[0]) * g.shape[1] + wrap_index((int)m[1] + i1, g.shape[1])) * sf;
+            st.s0[r] = (float)i0 * g.w32[0];
+            st.s1[r] = (float)i1 * g.w32[1];
+        } else {
+            skip = i1 == -1 && g.shape[0] == 2;
+            base = wrap_index((int)m[0] + i1, g.shape[0]) * sf;
+            st.s0[r] = (float)i1 * g.w32[0];
+            st.s1[r] = 0.f;
+        }
+        st.used[r] = !skip;
+        uint32_t a0 = 0, a1 = 0, b0 = 0, b1 = 0;
+        if (!skip) {
+            if (sf == 2) {
+                a0 = __ldg(cs + base);
+                a1 = __ldg(cs + base + 2);
+            } else if (mf >= 1 && mf + 1 < sf) {
+                a0 = __ldg(cs + base + mf - 1);
+                a1 = __ldg(cs + base + mf + 2);
+            } else if (mf == 0) {
+                a0 = __ldg(cs + base);
+                a1 = __ldg(cs + base + 2);
+                b0 = __ldg(cs + base + sf - 1);
+                b1 = __ldg(cs + base + sf);
+            } else {
+                a0 = __ldg(cs + base + sf - 2);
+                a1 = __ldg(cs + base + sf);
+                b0 = __ldg(cs + base);
+                b1 = __ldg(cs + base + 1);
+            }
+        }
+        st.lo[r][0] = a0;
+        st.hi[r][0] = a1;
+        st.lo[r][1] = b0;
+        st.hi[r][1] = b1;
+    }
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ float warp_sumf(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ uint32_t warp_maxu(uint32_t v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// FP64 energy of site t against the stencil of space m, skipping slot self: lane-strided over
+// the rows, then a butterfly reduction (every lane ends with the same value). S of a
+// candidate comes from sorted_s when have_s, else from wrap(sorted_b).
+template <int DIM>
+__device__ __forceinline__ double lj_energy64(const Geometry& g, const Arrays& A, const Pair& P, const double* t,
+                                              const Stencil<DIM>& st, uint32_t self, bool have_s, uint32_t lane) {
+    double e = 0.0;
+#pragma unroll
+    for (int r = 0; r < kRows<DIM>; ++r) {
+        for (int seg = 0; seg < 2; ++seg) {
+            for (uint32_t q = st.lo[r][seg] + lane; q < st.hi[r][seg]; q += 32) {
+                if (q == self) continue;
+                double sv[3];
+                if (have_s) {
+                    const double4 s4 = ldg4(A.sorted_s + q);
+                    sv[0] = s4.x;
+                    sv[1] = s4.y;
+                    sv[2] = s4.z;
+                } else {
+                    const double4 b4 = ldg4(A.sorted_b + q);
+                    sv[0] = b4.x;
+                    sv[1] = b4.y;
+                    sv[2] = b4.z;
+                    wrap_inv<DIM>(g.L, g.invL, sv);
+                }
+                e = dadd(e, lj_pair64(P, ref_dist2<DIM>(g, t, sv)));
+            }
+        }
+    }
+    return warp_sum(e);
+}
+
+struct Sums32 {
+    float e_new, e_old, err, mag;
+    uint32_t terms, pairs;
+};
+
+// FP32 energies of the trial site (offsets t32) and the current site (offsets c32) against
+// the stencil of their common space, with error bounds.
+template <int DIM>
+__device__ __forceinline__ Sums32 lj_energy32(const Geometry& g, const Arrays& A, const Pair& P, float4 t32,
+                                               float4 c32, int mf, const Stencil<DIM>& st, uint32_t self,
+                                               uint32_t lane) {
+    Sums32 s{0.f, 0.f, 0.f, 0.f, 0u, 0u};
+    const uint32_t sf = g.shape[DIM - 1];
+#pragma unroll
+    for (int r = 0; r < kRows<DIM>; ++r) {
+        for (int seg = 0; seg < 2; ++seg) {
+            for (uint32_t q = st.lo[r][seg] + lane; q < st.hi[r][seg]; q += 32) {
+                if (q == self) continue;
+                const float4 o = __ldg(A.sorted_off + q);
+                int dm = __float_as_int(o.w) - mf;
+                if (sf >= 4) {
+                    if (dm > 1)
+                        dm -= (int)sf;
+                    else if (dm < -1)
+                        dm += (int)sf;
+                }
+                const float r2n = fp32_dist2<DIM>(g, t32, o, st.s0[r], st.s1[r], dm);
+                const float r2o = fp32_dist2<DIM>(g, c32, o, st.s0[r], st.s1[r], dm);
+                float en, ern, eo, ero;
+                lj_pair32(P, r2n, r2_error(P, r2n), en, ern);
+                lj_pair32(P, r2o, r2_error(P, r2o), eo, ero);
+                s.e_new += en;
+                s.e_old += eo;
+                s.err += ern + ero;
+                s.mag += fabsf(en) + fabsf(eo);
+                s.terms += 1;
+                s.pairs += 2;
+            }
+        }
+    }
+    s.e_new = warp_sumf(s.e_new);
+    s.e_old = warp_sumf(s.e_old);
+    s.err = warp_sumf(s.err);
+    s.mag = warp_sumf(s.mag);
+    s.terms = warp_maxu(s.terms);
+    return s;
+}
+
+// Metropolis decision from the FP32 sums: 1 accept, 0 reject, -1 needs the FP64 sums. When the
+// decision needs the uniform, *u is drawn from rng here (the FP64 path draws it at the same
+// point of the stream: only when dU > 0).
+__device__ __forceinline__ int decide32(const Sums32& s, double kt, Sfc64& rng, bool& drew, double& u) {
+    const float d32 = s.e_new - s.e_old;
+    // summation chains (per lane + 5 reduction levels + the final difference), FP64's own error
+    const float b = s.err + (float)(s.terms + 7) * kU32 * s.mag * 1.01f + kU32 * fabsf(d32) + 1e-9f * (s.mag + 1.f);
+    if (!isfinite(d32) || !isfinite(b)) return -1;
+    const double lo = (double)d32 - (double)b, hi = (double)d32 + (double)b;
+    if (hi <= 0.0) return 1;  // dU64 <= 0 for certain: accepted without a uniform
+    if (lo <= 0.0) return -1;
+    u = uniform01(rng);  // dU64 > 0 for certain
+    drew = true;
+    const double t_hi = exp(-lo / kt) * (1.0 + 1e-12);
+    const double t_lo = exp(-hi / kt) * (1.0 - 1e-12);
+    if (u < t_lo) return 1;
+    if (u >= t_hi) return 0;
+    return -1;
+}
+
+template <int DIM, bool FP32>
+__global__ void __launch_bounds__(128) k_sweep_lj(Geometry g, Arrays A, Pair P, Launch L) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t n_warps = (gridDim.x * blockDim.x) >> 5;
+    uint32_t n_accepted = 0;
+    PairStats pst;
+    for (uint32_t w = warp; w < L.n_active; w += n_warps) {
+        uint32_t m[3] = {0, 0, 0};
+        unpack_m<DIM>(__ldg(A.color_cells + (size_t)L.color * g.color_stride + w), m);
+        const uint32_t cell = cell_index<DIM>(g, m);
+        Stencil<DIM> st;
+        make_stencil<DIM>(g, A.cell_start, m, st);
+        const uint32_t start = __ldg(A.cell_start + cell);
+        const uint32_t count = __ldg(A.cell_start + cell + 1) - start;
+        // every lane draws the same stream: the trial is computed redundantly, warp-uniform
+        Sfc64 rng = make_rng(L.step, L.substep, L.seed, (uint64_t)cell);
+        const uint32_t k = start + canon_range_u32(rng, count);
+        const double4 b4 = A.sorted_b[k];
+        double x[3] = {b4.x, b4.y, b4.z};
+        double dv[3];
+        ball_sample<DIM>(rng, L.max_move, A.zig_x, A.zig_f, dv);
+#pragma unroll
+        for (int a = 0; a < DIM; ++a) x[a] = dadd(x[a], dv[a]);
+        wrap_inv<DIM>(g.L, g.invL, x);
+        uint32_t mt[3];
+        if (!(point_to_space<DIM>(g, x, mt) && cell_index<DIM>(g, mt) == cell)) continue;
+        double t[3] = {x[0], x[1], DIM == 3 ? x[2] : 0.0};
+        wrap_inv<DIM>(g.L, g.invL, t);
+        int decision;
+        bool drew = false;
+        double u = 0.0;
+        if (FP32) {
+            const float4 t32 = cell_offsets<DIM>(g, t, m);
+            const float4 c32 = __ldg(A.sorted_off + k);
+            const Sums32 s = lj_energy32<DIM>(g, A, P, t32, c32, (int)m[DIM - 1], st, k, lane);
+            pst.checks += s.pairs;
+            decision = decide32(s, L.kt, rng, drew, u);
+            if (decision < 0) {
+                // FP64 recheck with the plain pass's order; the uniform, if already drawn, is
+                // the one the plain pass would draw (its draw point is the same).
+                double si[3] = {b4.x, b4.y, b4.z};
+                wrap_inv<DIM>(g.L, g.invL, si);
+                const double du = dsub(lj_energy64<DIM>(g, A, P, t, st, k, false, lane),
+                                       lj_energy64<DIM>(g, A, P, si, st, k, false, lane));
+                if (lane == 0) {
+                    pst.rechecks++;
+                    const double err = fabs((double)(s.e_new - s.e_old) - du);
+                    pst.max_err = err > pst.max_err ? err : pst.max_err;
+                }
+                if (du <= 0.0) {
+                    decision = 1;
+                } else {
+                    if (!drew) u = uniform01(rng);
+                    decision = u < exp(ddiv(-du, L.kt)) ? 1 : 0;
+                }
+            }
+        } else {
+            const double4 s4 = ldg4(A.sorted_s + k);
+            const double si[3] = {s4.x, s4.y, s4.z};
+            const double du = dsub(lj_energy64<DIM>(g, A, P, t, st, k, true, lane),
+                                   lj_energy64<DIM>(g, A, P, si, st, k, true, lane));
+            decision = (du <= 0.0 || uniform01(rng) < exp(ddiv(-du, L.kt))) ? 1 : 0;
+        }
+        if (decision == 1 && lane == 0) {
+            n_accepted++;
+            double sv[3] = {t[0], t[1], t[2]};
+            wrap_inv<DIM>(g.L, g.invL, sv);
+            A.sorted_b[k] = make_double4(t[0], t[1], t[2], 0.0);
+            if (!FP32) A.sorted_s[k] = make_double4(sv[0], sv[1], sv[2], 0.0);
+            A.sorted_off[k] = cell_offsets<DIM>(g, sv, m);
+            A.body_pos[A.sorted_body[k]] = make_double4(t[0], t[1], t[2], 0.0);
+        }
+        __syncwarp();
+    }
+    flush_stats(A.stats, pst, n_accepted);
+}
+
+// Injected moves: warp per move. delta_h gets dU64 (stencils around the trial's space for the
+// final energy and around the body's space for the initial energy); the decision follows the
+// precision mode with the given uniform.
+template <int DIM, bool FP32>
+__global__ void __launch_bounds__(128) k_eval_lj(Geometry g, Arrays A, Pair P, const uint64_t* bodies,
+                                                 const double4* trial, const double* uu, double kt, uint32_t n,
+                                                 uint8_t* decisions, uint8_t* rechecked, double* delta_h) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    PairStats pst;
+    if (i < n) {
+        const uint32_t k = A.slot_of_body[bodies[i]];
+        const double4 w4 = trial[i];
+        double t[3] = {w4.x, w4.y, DIM == 3 ? w4.z : 0.0};
+        wrap_inv<DIM>(g.L, g.invL, t);
+        const double4 s4 = ldg4(A.sorted_s + k);
+        const double si[3] = {s4.x, s4.y, s4.z};
+        uint32_t mt[3], mi[3];
+        const bool ok = point_to_space<DIM>(g, t, mt) && point_to_space<DIM>(g, si, mi);
+        uint8_t dec = 0, rech = 0;
+        double du = 0.0;
+        if (ok) {
+            Stencil<DIM> stt, sti;
+            make_stencil<DIM>(g, A.cell_start, mt, stt);
+            make_stencil<DIM>(g, A.cell_start, mi, sti);
+            du = dsub(lj_energy64<DIM>(g, A, P, t, stt, k, true, lane), lj_energy64<DIM>(g, A, P, si, sti, k, true, lane));
+            const double u = uu[i];
+            bool dec64 = du <= 0.0 || u < exp(ddiv(-du, kt));
+            dec = dec64 ? 1 : 0;
+            if (FP32) {
+                // FP32 sums need a common space for both sites: when the trial left the body's
+                // space, they are evaluated in FP64 as the sweep never sees such a trial.
+                const bool same = mt[0] == mi[0] && mt[1] == mi[1] && (DIM == 2 || mt[2] == mi[2]);
+                if (same) {
+                    const float4 t32 = cell_offsets<DIM>(g, t, mt);
+                    const float4 c32 = __ldg(A.sorted_off + k);
+                    const Sums32 s = lj_energy32<DIM>(g, A, P, t32, c32, (int)mt[DIM - 1], stt, k, lane);
+                    const float d32 = s.e_new - s.e_old;
+                    const float b = s.err + (float)(s.terms + 7) * kU32 * s.mag * 1.01f + kU32 * fabsf(d32) +
+                                    1e-9f * (s.mag + 1.f);
+                    int d = -1;
+                    if (isfinite(d32) && isfinite(b)) {
+                        const double lo = (double)d32 - b, hi = (double)d32 + b;
+                        if (hi <= 0.0) {
+                            d = 1;
+                        } else if (lo > 0.0) {
+                            const double t_hi = exp(-lo / kt) * (1.0 + 1e-12), t_lo = exp(-hi / kt) * (1.0 - 1e-12);
+                            d = u < t_lo ? 1 : (u >= t_hi ? 0 : -1);
+                        }
+                    }
+                    if (d < 0) {
+                        rech = 1;
+                        d = dec64 ? 1 : 0;  // the FP64 recheck
+                    }
+                    dec = (uint8_t)d;
+                } else {
+                    rech = 1;
+                }
+            }
+        } else if (lane == 0) {
+            atomicOr(&A.stats->error_flags, kErrOutsideCheckerboard);
+        }
+        if (lane == 0) {
+            decisions[i] = dec;
+            rechecked[i] = rech;
+            delta_h[i] = du;
+        }
+    }
+    flush_stats(A.stats, pst, 0u);
+}
+
+// Total pair energy, pairs (i < j) in FP64 (PairwiseCutoff::total_energy,
+// pairwise_cutoff.rs:720-745); one thread per body, atomically summed.
+template <int DIM>
+__global__ void k_energy_lj(Geometry g, Arrays A, Pair P, uint32_t n, double* out) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    double e = 0.0;
+    if (k < n) {
+        const uint32_t bi = A.sorted_body[k];
+        const double4 s4 = A.sorted_s[k];
+        const double t[3] = {s4.x, s4.y, s4.z};
+        uint32_t m[3];
+        uint32_t c = A.body_cell[bi];
+#pragma unroll
+        for (int a = DIM - 1; a >= 0; --a) {
+            m[a] = c % g.shape[a];
+            c /= g.shape[a];
+        }
+        for_each_neighbor<DIM>(g, A.cell_start, m, [&](uint32_t q, const float*) -> bool {
+            if (A.sorted_body[q] <= bi) return false;
+            const double4 o4 = A.sorted_s[q];
+            const double sv[3] = {o4.x, o4.y, o4.z};
+            e += lj_pair64(P, ref_dist2<DIM>(g, t, sv));
+            return false;
+        });
+        atomicAdd(out, e);
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_sweep_lj(int dim, bool fp32, const Geometry& g, const Arrays& a, const Pair& p, const Launch& l,
+                            cudaStream_t s) {
+    if (l.n_active == 0) return cudaSuccess;
+    static int max_blocks = 0;
+    if (max_blocks == 0) {
+        int dev = 0, sms = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        max_blocks = sms * 16;
+    }
+    uint32_t blocks = (l.n_active + 3) / 4;  // four warps (trials) per block
+    if (blocks > (uint32_t)max_blocks) blocks = (uint32_t)max_blocks;
+    if (dim == 2) {
+        if (fp32)
+            k_sweep_lj<2, true><<<blocks, 128, 0, s>>>(g, a, p, l);
+        else
+            k_sweep_lj<2, false><<<blocks, 128, 0, s>>>(g, a, p, l);
+    } else {
+        if (fp32)
+            k_sweep_lj<3, true><<<blocks, 128, 0, s>>>(g, a, p, l);
+        else
+            k_sweep_lj<3, false><<<blocks, 128, 0, s>>>(g, a, p, l);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_eval_lj(int dim, bool fp32, const Geometry& g, const Arrays& a, const Pair& p,
+                           const uint64_t* bodies, const double4* trial, const double* u, double kt, uint32_t n,
+                           uint8_t* decisions, uint8_t* rechecked, double* delta_h, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    const uint32_t blocks = (n + 3) / 4;
+    if (dim == 2) {
+        if (fp32)
+            k_eval_lj<2, true><<<blocks, 128, 0, s>>>(g, a, p, bodies, trial, u, kt, n, decisions, rechecked, delta_h);
+        else
+            k_eval_lj<2, false><<<blocks, 128, 0, s>>>(g, a, p, bodies, trial, u, kt, n, decisions, rechecked, delta_h);
+    } else {
+        if (fp32)
+            k_eval_lj<3, true><<<blocks, 128, 0, s>>>(g, a, p, bodies, trial, u, kt, n, decisions, rechecked, delta_h);
+        else
+            k_eval_lj<3, false><<<blocks, 128, 0, s>>>(g, a, p, bodies, trial, u, kt, n, decisions, rechecked, delta_h);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_energy_lj(int dim, const Geometry& g, const Arrays& a, const Pair& p, uint32_t n, double* out,
+                             cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    if (dim == 2)
+        k_energy_lj<2><<<(n + 127) / 128, 128, 0, s>>>(g, a, p, n, out);
+    else
+        k_energy_lj<3><<<(n + 127) / 128, 128, 0, s>>>(g, a, p, n, out);
+    return cudaGetLastError();
+}
+
+}  // namespace hmc

@@ -97,3 +97,11 @@ def hard_sphere_box(n: int, packing_fraction: float, dim: int, seed: int, lattic
     if dim == 3 and lattice in ("auto", "fcc"):
         return fcc_lattice(n, L, seed, jitter), L
     return cubic_lattice(n, L, dim, seed, jitter), L
+
+
+def lennard_jones_box(n: int, number_density: float, dim: int, seed: int, jitter: float = 0.01):
+    """(positions, L) for Lennard-Jones sites (sigma = 1) at the given number density."""
+    L = box_length(n, number_density, dim)
+    if dim == 3:
+        return fcc_lattice(n, L, seed, jitter), L
+    return cubic_lattice(n, L, dim, seed, jitter), L

@@ -167,8 +167,13 @@ hmc_status hmc_sweep(hmc_system* sys, const hmc_sweep_params* params, hmc_count*
 hmc_status hmc_tune(hmc_system* sys, hmc_sweep_params* params, double target_acceptance, uint32_t samples,
                     uint32_t steps);
 hmc_status hmc_overlap_check(hmc_system* sys, uint64_t* n_overlaps);
+/* decisions[i] = 1 when move i would be accepted; rechecked[i] = 1 when the FP32 path had to
+ * fall back to FP64 for it; delta_h[i] (may be NULL) = delta_energy_one in FP64. */
 hmc_status hmc_eval_moves(hmc_system* sys, const hmc_injected_move* moves, uint64_t n, double temperature,
-                          uint32_t precision, uint8_t* decisions, uint8_t* rechecked);
+                          uint32_t precision, uint8_t* decisions, uint8_t* rechecked, double* delta_h);
+/* PairwiseCutoff::total_energy (pairwise_cutoff.rs:720-745): the pair energy sum in FP64 for
+ * Lennard-Jones; +infinity or 0 for hard shapes (any overlap / none). */
+hmc_status hmc_total_energy(hmc_system* sys, double* energy);
 
 /* ---- overlap count into caller buffers, with no device allocation ----
  * No counterpart in the reference (hoomd-rs has no GPU path); it serves callers that must
