@@ -188,6 +188,31 @@ class Isotropic:
 
 
 @dataclass
+class ConvexPolyhedron:
+    """hoomd_geometry::shape::ConvexPolyhedron (convex_polytope.rs:120): up to 32 vertices."""
+    vertices: np.ndarray
+
+    @classmethod
+    def with_vertices(cls, vertices) -> "ConvexPolyhedron":
+        v = np.ascontiguousarray(vertices, dtype=np.float64).reshape(-1, 3)
+        return cls(v)
+
+    @property
+    def bounding_radius(self) -> float:
+        return float(np.sqrt(max(float(np.dot(v, v)) for v in self.vertices)))
+
+
+@dataclass
+class HardShape:
+    """hoomd_interaction::pairwise::HardShape(Convex(shape)) (hard_shape.rs:33-119)."""
+    shape: ConvexPolyhedron
+
+    @property
+    def maximum_interaction_range(self) -> float:
+        return self.shape.bounding_radius * 2.0
+
+
+@dataclass
 class PairwiseCutoff:
     """hoomd_interaction::PairwiseCutoff (pairwise_cutoff.rs:140)."""
     pair: object
@@ -224,6 +249,16 @@ class Count:
 
 
 @dataclass
+class Rotate:
+    """hoomd_mc::Rotate<Versor> (rotate/versor.rs:40-123): Gaussian rotation vector, sigma = maximum."""
+    maximum_rotation: float
+
+    @classmethod
+    def with_maximum_rotation(cls, a: float) -> "Rotate":
+        return cls(float(a))
+
+
+@dataclass
 class Translate:
     """hoomd_mc::Translate (translate.rs:41, translate/cartesian.rs:40-51)."""
     maximum_distance: float
@@ -237,7 +272,8 @@ class Microstate:
     """Bodies in a periodic box, resident on the GPU (one hmc_system)."""
 
     def __init__(self, ctx: Context, boundary: Periodic, positions, hamiltonian: PairwiseCutoff, *,
-                 step: int = 0, substep: int = 0, seed: int = 0, body_interaction_range: float = 0.0):
+                 step: int = 0, substep: int = 0, seed: int = 0, body_interaction_range: float = 0.0,
+                 orientations=None):
         lib = load_library()
         L = [float(x) for x in boundary.edge_lengths]
         self.dim = len(L)
@@ -254,6 +290,12 @@ class Microstate:
         if isinstance(pair, HardSphere):
             d.interaction = HARD_SPHERE
             d.diameter = pair.diameter
+        elif isinstance(pair, HardShape):
+            d.interaction = HARD_CONVEX_POLYHEDRON
+            verts = np.ascontiguousarray(pair.shape.vertices, dtype=np.float64)
+            self._verts = verts  # keep alive during the call
+            d.n_vertices = verts.shape[0]
+            d.vertices = verts.ctypes.data_as(_dp)
         elif isinstance(pair, Isotropic) and isinstance(pair.interaction, Shifted):
             d.interaction = LENNARD_JONES
             d.lj_epsilon = pair.interaction.f.epsilon
@@ -264,8 +306,15 @@ class Microstate:
             raise HmcError(NOT_SUPPORTED, f"{type(pair).__name__}")
         d.boundary_range = boundary.maximum_interaction_range
         d.body_interaction_range = body_interaction_range
+        self.oriented = d.interaction == HARD_CONVEX_POLYHEDRON
+        ori = None
+        if self.oriented:
+            if orientations is None:
+                orientations = np.tile([1.0, 0.0, 0.0, 0.0], (self.n, 1))
+            ori = np.ascontiguousarray(orientations, dtype=np.float64).reshape(self.n, 4)
         h = _vp()
-        _check(lib.hmc_system_create(ctx._h, C.byref(d), pos.ctypes.data_as(_dp), None, C.byref(h)))
+        _check(lib.hmc_system_create(ctx._h, C.byref(d), pos.ctypes.data_as(_dp),
+                                     None if ori is None else ori.ctypes.data_as(_dp), C.byref(h)))
         self._h = h
         self._ctx = ctx  # keep the context alive
         self.edge_lengths = L
@@ -287,6 +336,11 @@ class Microstate:
         _check(_lib.hmc_get_state(self._h, pos.ctypes.data_as(_dp), None, C.byref(step), C.byref(sub)))
         return pos, step.value, sub.value
 
+    def orientations(self) -> np.ndarray:
+        ori = np.zeros((self.n, 4))
+        _check(_lib.hmc_get_state(self._h, None, ori.ctypes.data_as(_dp), None, None))
+        return ori
+
     def positions(self) -> np.ndarray:
         return self.state()[0]
 
@@ -296,9 +350,11 @@ class Microstate:
     def substep(self) -> int:
         return self.state()[2]
 
-    def set_state(self, positions, step: int, substep: int):
+    def set_state(self, positions, step: int, substep: int, orientations=None):
         pos = np.ascontiguousarray(positions, dtype=np.float64).reshape(self.n, self.dim)
-        _check(_lib.hmc_set_state(self._h, pos.ctypes.data_as(_dp), None, step, substep))
+        ori = None if orientations is None else np.ascontiguousarray(orientations, dtype=np.float64).reshape(self.n, 4)
+        _check(_lib.hmc_set_state(self._h, pos.ctypes.data_as(_dp), None if ori is None else ori.ctypes.data_as(_dp),
+                                  step, substep))
 
     def increment_step(self):
         pos, step, _ = self.state()
@@ -331,7 +387,7 @@ class Microstate:
         return Count(c.accepted, c.rejected, c.rechecks, c.pair_checks, c.max_fp32_error)
 
     def eval_moves(self, bodies, positions, u=None, temperature: float = 1.0, precision: int = FP64,
-                   return_delta_h: bool = False):
+                   return_delta_h: bool = False, orientations=None):
         bodies = np.asarray(bodies, dtype=np.uint64)
         pos = np.asarray(positions, dtype=np.float64).reshape(len(bodies), self.dim)
         n = len(bodies)
@@ -340,6 +396,8 @@ class Microstate:
         arr["body"] = bodies
         arr["position"][:, : self.dim] = pos
         arr["u"] = -1.0 if u is None else np.asarray(u, dtype=np.float64)
+        if orientations is not None:
+            arr["orientation"] = np.asarray(orientations, dtype=np.float64).reshape(n, 4)
         moves = arr.ctypes.data_as(C.POINTER(hmc_injected_move))
         dec = np.zeros(n, dtype=np.uint8)
         rech = np.zeros(n, dtype=np.uint8)
@@ -363,7 +421,7 @@ class ParallelSweep:
     recheck inside the forward-error bound (``FP32_RECHECK``); both give the same decisions.
     """
 
-    def __init__(self, body_interaction_range: float, local_trial: Translate, precision: int = FP32_RECHECK):
+    def __init__(self, body_interaction_range: float, local_trial, precision: int = FP32_RECHECK):
         self.body_interaction_range = float(body_interaction_range)
         self.local_trial = local_trial
         self.precision = precision
@@ -374,6 +432,8 @@ class ParallelSweep:
             raise HmcError(INVALID_ARGUMENT, "the hamiltonian differs from the one the microstate was built with")
         if isinstance(self.local_trial, Translate):
             move, maximum = TRANSLATE, self.local_trial.maximum_distance
+        elif isinstance(self.local_trial, Rotate):
+            move, maximum = ROTATE, self.local_trial.maximum_rotation
         else:
             raise HmcError(NOT_SUPPORTED, type(self.local_trial).__name__)
         c = microstate.sweep(move, maximum, macrostate.temperature, self.precision)
@@ -381,7 +441,7 @@ class ParallelSweep:
         return c
 
 
-__all__ = ["Context", "Count", "HardSphere", "HmcError", "Isothermal", "Isotropic", "LennardJones", "Microstate",
-           "PairwiseCutoff", "Shifted",
+__all__ = ["Context", "ConvexPolyhedron", "Count", "HardShape", "HardSphere", "HmcError", "Isothermal", "Isotropic",
+           "LennardJones", "Microstate", "PairwiseCutoff", "Rotate", "Shifted",
            "ParallelSweep", "Periodic", "Translate", "load_library", "SIGNATURES", "FP64", "FP32_RECHECK",
            "TRANSLATE", "ROTATE"]

@@ -82,6 +82,12 @@ struct hmc_system {
     DeviceStats* host_stats = nullptr;  // pinned
     std::vector<void*> allocations;
     uint32_t tile_cap[2] = {0, 0};  // staged bodies per block of the tiled pass: [fp64, fp32]
+    // convex polyhedron
+    double4* verts = nullptr;
+    uint32_t n_vertices = 0;
+    double poly_rcut2 = 0.0;
+    float poly_rcut2_hi32 = 0.f;
+    bool oriented() const { return interaction == HMC_HARD_CONVEX_POLYHEDRON; }
     // profiling
     bool profiling = false;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -291,13 +297,36 @@ hmc_status hmc_system_create(hmc_context* ctx, const hmc_system_desc* d, const d
     for (uint32_t a = 0; a < d->dim; ++a)
         if (!(d->edge_lengths[a] > 0.0) || !std::isfinite(d->edge_lengths[a]))
             return fail(HMC_INVALID_ARGUMENT, "edge length %u must be positive", a);
-    if (d->interaction != HMC_HARD_SPHERE && d->interaction != HMC_LENNARD_JONES)
+    if (d->interaction != HMC_HARD_SPHERE && d->interaction != HMC_LENNARD_JONES &&
+        d->interaction != HMC_HARD_CONVEX_POLYHEDRON)
         return fail(HMC_NOT_SUPPORTED, "interaction %u is not available in this build", d->interaction);
+    if (d->interaction == HMC_HARD_CONVEX_POLYHEDRON) {
+        if (d->dim != 3) return fail(HMC_INVALID_ARGUMENT, "convex polyhedra are 3-D");
+        // ConvexPolytope::with_vertices: at least one vertex, at most 32 (ConvexPolyhedron)
+        if (d->n_vertices < 1 || d->n_vertices > 32 || !d->vertices)
+            return fail(HMC_INVALID_ARGUMENT, "a convex polyhedron needs 1 to 32 vertices");
+        for (uint32_t i = 0; i < 3 * d->n_vertices; ++i)
+            if (!std::isfinite(d->vertices[i])) return fail(HMC_INVALID_ARGUMENT, "vertex coordinates must be finite");
+    }
     if (d->interaction == HMC_HARD_SPHERE && !(d->diameter > 0.0))
         return fail(HMC_INVALID_ARGUMENT, "diameter must be positive");
     if (d->interaction == HMC_LENNARD_JONES &&
         (!(d->lj_sigma > 0.0) || !(d->lj_r_cut > 0.0) || !(d->lj_r_shift > 0.0) || !std::isfinite(d->lj_epsilon)))
         return fail(HMC_INVALID_ARGUMENT, "Lennard-Jones sigma, r_cut and r_shift must be positive");
+
+    // maximum_interaction_range: HardSphere (hard_shape.rs:171-175) = diameter; Isotropic = r_cut;
+    // HardShape (hard_shape.rs:111-118) = 2 x the bounding radius, where ConvexPolytope's
+    // bounding radius (convex_polytope.rs:199-207) is sqrt(max |v|^2) with |v|^2 by mul_add.
+    double bounding_radius = 0.0;
+    if (d->interaction == HMC_HARD_CONVEX_POLYHEDRON) {
+        double mx = 0.0;
+        for (uint32_t i = 0; i < d->n_vertices; ++i) {
+            const double* v = d->vertices + 3 * i;
+            mx = std::max(mx, std::fma(v[2], v[2], std::fma(v[1], v[1], std::fma(v[0], v[0], 0.0))));
+        }
+        bounding_radius = std::sqrt(mx);
+        if (!(bounding_radius > 0.0)) return fail(HMC_INVALID_ARGUMENT, "the polyhedron's bounding radius must be positive");
+    }
 
     HMC_CUDA(cudaSetDevice(ctx->device));
     hmc_system* s = new hmc_system();
@@ -309,8 +338,9 @@ hmc_status hmc_system_create(hmc_context* ctx, const hmc_system_desc* d, const d
     s->substep = d->substep;
     s->seed = d->seed;
     s->interaction = d->interaction;
-    // maximum_interaction_range: HardSphere (hard_shape.rs:171-175) = diameter; Isotropic = r_cut
-    s->pair_range = d->interaction == HMC_LENNARD_JONES ? d->lj_r_cut : d->diameter;
+    s->pair_range = d->interaction == HMC_LENNARD_JONES ? d->lj_r_cut
+                    : d->interaction == HMC_HARD_CONVEX_POLYHEDRON ? bounding_radius * 2.0
+                                                                  : d->diameter;
     s->boundary_range = d->boundary_range > 0.0 ? d->boundary_range : s->pair_range;
     s->body_range = d->body_interaction_range > 0.0 ? d->body_interaction_range : s->pair_range;
     for (int a = 0; a < 3; ++a) s->geom.L[a] = a < s->dim ? d->edge_lengths[a] : 1.0;
@@ -363,6 +393,14 @@ hmc_status hmc_system_create(hmc_context* ctx, const hmc_system_desc* d, const d
     if (d->interaction == HMC_HARD_SPHERE) {
         s->pair.sigma2 = d->diameter * d->diameter;  // diameter.powi(2)
         sphere_bound(s);
+    } else if (d->interaction == HMC_HARD_CONVEX_POLYHEDRON) {
+        // circumsphere rejection (convex.rs:162-165): r_cut = R + R, compared with r_cut.powi(2)
+        const double rc = bounding_radius + bounding_radius;
+        s->poly_rcut2 = rc * rc;
+        s->pair.sigma2 = s->poly_rcut2;  // the FP32 prefilter threshold reuses the sphere bound
+        sphere_bound(s);
+        s->poly_rcut2_hi32 = s->pair.sig2_hi32;
+        s->n_vertices = d->n_vertices;
     } else {
         lj_setup(s, d->lj_epsilon, d->lj_sigma, d->lj_r_cut, d->lj_r_shift);
     }
@@ -407,6 +445,27 @@ hmc_status hmc_system_create(hmc_context* ctx, const hmc_system_desc* d, const d
         return destroy_fail(st);
     A.body_ori = nullptr;
     A.sorted_q = nullptr;
+    if (s->oriented()) {
+        if ((st = dalloc(s, &A.body_ori, n)) || (st = dalloc(s, &A.sorted_q, n)) ||
+            (st = dalloc(s, &s->verts, s->n_vertices)))
+            return destroy_fail(st);
+        std::vector<double4> hv(s->n_vertices);
+        for (uint32_t i = 0; i < s->n_vertices; ++i)
+            hv[i] = make_double4(d->vertices[3 * i], d->vertices[3 * i + 1], d->vertices[3 * i + 2], 0.0);
+        e = cudaMemcpy(s->verts, hv.data(), sizeof(double4) * s->n_vertices, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess && n > 0) {
+            std::vector<double4> hq(n);
+            for (uint64_t i = 0; i < n; ++i)
+                hq[i] = orientations ? make_double4(orientations[4 * i], orientations[4 * i + 1], orientations[4 * i + 2],
+                                                    orientations[4 * i + 3])
+                                     : make_double4(1.0, 0.0, 0.0, 0.0);
+            e = cudaMemcpy(A.body_ori, hq.data(), sizeof(double4) * n, cudaMemcpyHostToDevice);
+        }
+        if (e != cudaSuccess) {
+            fail(HMC_CUDA_ERROR, "upload: %s", cudaGetErrorString(e));
+            return destroy_fail(HMC_CUDA_ERROR);
+        }
+    }
     A.zig_x = ctx->zig;
     A.zig_f = ctx->zig + kZigLayers + 1;
     if (n > 0) {
@@ -428,7 +487,6 @@ hmc_status hmc_system_create(hmc_context* ctx, const hmc_system_desc* d, const d
             return destroy_fail(HMC_CUDA_ERROR);
         }
     }
-    (void)orientations;
     *out = s;
     return HMC_OK;
 }
@@ -447,8 +505,13 @@ hmc_status hmc_set_state(hmc_system* s, const double* positions, const double* o
     if (!s || (s->n > 0 && !positions)) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
     hmc_status st = validate_positions(s, positions);
     if (st) return st;
-    (void)orientations;
     HMC_CUDA(cudaSetDevice(s->ctx->device));
+    if (s->oriented() && orientations && s->n) {
+        std::vector<double4> hq(s->n);
+        for (uint64_t i = 0; i < s->n; ++i)
+            hq[i] = make_double4(orientations[4 * i], orientations[4 * i + 1], orientations[4 * i + 2], orientations[4 * i + 3]);
+        HMC_CUDA(cudaMemcpy(s->arr.body_ori, hq.data(), sizeof(double4) * s->n, cudaMemcpyHostToDevice));
+    }
     // Positions are body positions as returned by hmc_get_state (already wrapped).
     std::vector<double4> host(s->n);
     for (uint64_t i = 0; i < s->n; ++i)
@@ -464,8 +527,18 @@ hmc_status hmc_set_state(hmc_system* s, const double* positions, const double* o
 hmc_status hmc_get_state(hmc_system* s, double* positions, double* orientations, uint64_t* step,
                          uint32_t* substep) {
     if (!s) return fail(HMC_INVALID_ARGUMENT, "NULL system");
-    (void)orientations;
     HMC_CUDA(cudaSetDevice(s->ctx->device));
+    if (s->oriented() && orientations && s->n) {
+        std::vector<double4> hq(s->n);
+        HMC_CUDA(cudaMemcpyAsync(hq.data(), s->arr.body_ori, sizeof(double4) * s->n, cudaMemcpyDeviceToHost, s->stream));
+        HMC_CUDA(cudaStreamSynchronize(s->stream));
+        for (uint64_t i = 0; i < s->n; ++i) {
+            orientations[4 * i] = hq[i].x;
+            orientations[4 * i + 1] = hq[i].y;
+            orientations[4 * i + 2] = hq[i].z;
+            orientations[4 * i + 3] = hq[i].w;
+        }
+    }
     if (positions && s->n) {
         std::vector<double4> host(s->n);
         HMC_CUDA(cudaMemcpyAsync(host.data(), s->arr.body_pos, sizeof(double4) * s->n, cudaMemcpyDeviceToHost, s->stream));
@@ -484,7 +557,8 @@ hmc_status hmc_get_state(hmc_system* s, double* positions, double* orientations,
 hmc_status hmc_sweep(hmc_system* s, const hmc_sweep_params* p, hmc_count* out) {
     if (!s || !p) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
     if (p->struct_size < sizeof(hmc_sweep_params)) return fail(HMC_INVALID_ARGUMENT, "hmc_sweep_params.struct_size");
-    if (p->move != HMC_TRANSLATE) return fail(HMC_NOT_SUPPORTED, "spheres and Lennard-Jones sites take translation moves only");
+    if (p->move != HMC_TRANSLATE && !(p->move == HMC_ROTATE && s->oriented()))
+        return fail(HMC_NOT_SUPPORTED, "rotation moves need oriented bodies (convex polyhedra)");
     if (!(p->maximum > 0.0) || !std::isfinite(p->maximum)) return fail(HMC_INVALID_ARGUMENT, "maximum must be positive");
     // The 2-D ball sampler squares the radius; keep it far from overflow. Moves longer
     // than the box are equivalent modulo wrapping, so this rejects no useful input.
@@ -523,6 +597,9 @@ hmc_status hmc_sweep(hmc_system* s, const hmc_sweep_params* p, hmc_count* out) {
                 L.n_active = color_count[c];
                 if (s->interaction == HMC_LENNARD_JONES)
                     HMC_CUDA(launch_sweep_lj(s->dim, fp32, s->geom, s->arr, s->pair, L, s->stream));
+                else if (s->interaction == HMC_HARD_CONVEX_POLYHEDRON)
+                    HMC_CUDA(launch_sweep_poly(fp32, s->geom, s->arr, s->verts, s->n_vertices, s->poly_rcut2,
+                                               s->poly_rcut2_hi32, L, p->move == HMC_ROTATE, s->stream));
                 else
                     HMC_CUDA(launch_sweep_sphere(s->dim, fp32, s->geom, s->arr, s->pair, L, s->tile_cap[fp32], s->stream));
                 s->prof.kernel_launches += 1;
@@ -585,11 +662,14 @@ hmc_status hmc_tune(hmc_system* s, hmc_sweep_params* p, double target, uint32_t 
 
 hmc_status hmc_overlap_check(hmc_system* s, uint64_t* n_overlaps) {
     if (!s || !n_overlaps) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
-    if (s->interaction != HMC_HARD_SPHERE) return fail(HMC_NOT_SUPPORTED, "overlap check of a soft potential");
+    if (s->interaction == HMC_LENNARD_JONES) return fail(HMC_NOT_SUPPORTED, "overlap check of a soft potential");
     HMC_CUDA(cudaSetDevice(s->ctx->device));
     hmc_status st = rebuild(s, true);
     if (st) return st;
-    HMC_CUDA(launch_overlap_sphere(s->dim, s->geom, s->arr, s->pair, (uint32_t)s->n, s->stream));
+    if (s->interaction == HMC_HARD_CONVEX_POLYHEDRON)
+        HMC_CUDA(launch_overlap_poly(s->geom, s->arr, s->verts, s->n_vertices, s->poly_rcut2, (uint32_t)s->n, s->stream));
+    else
+        HMC_CUDA(launch_overlap_sphere(s->dim, s->geom, s->arr, s->pair, (uint32_t)s->n, s->stream));
     s->prof.kernel_launches += 1;
     if ((st = read_stats(s))) return st;
     if ((st = check_flags(s))) return st;
@@ -599,7 +679,7 @@ hmc_status hmc_overlap_check(hmc_system* s, uint64_t* n_overlaps) {
 
 hmc_status hmc_total_energy(hmc_system* s, double* energy) {
     if (!s || !energy) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
-    if (s->interaction == HMC_HARD_SPHERE) {
+    if (s->interaction != HMC_LENNARD_JONES) {
         uint64_t n = 0;
         hmc_status st = hmc_overlap_check(s, &n);
         if (st) return st;
@@ -636,10 +716,13 @@ hmc_status hmc_eval_moves(hmc_system* s, const hmc_injected_move* moves, uint64_
     std::vector<uint64_t> hb(n);
     std::vector<double4> ht(n);
     std::vector<double> hu(n);
+    std::vector<double4> hq(n);
     for (uint64_t i = 0; i < n; ++i) {
         hb[i] = moves[i].body;
         ht[i] = make_double4(moves[i].position[0], moves[i].position[1], s->dim == 3 ? moves[i].position[2] : 0.0, 0.0);
         hu[i] = moves[i].u;
+        hq[i] = make_double4(moves[i].orientation[0], moves[i].orientation[1], moves[i].orientation[2],
+                             moves[i].orientation[3]);
     }
     const bool lj = s->interaction == HMC_LENNARD_JONES;
     uint64_t* db = nullptr;
@@ -655,11 +738,19 @@ hmc_status hmc_eval_moves(hmc_system* s, const hmc_injected_move* moves, uint64_
     if (e == cudaSuccess) e = cudaMemcpyAsync(db, hb.data(), sizeof(uint64_t) * n, cudaMemcpyHostToDevice, s->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(dt, ht.data(), sizeof(double4) * n, cudaMemcpyHostToDevice, s->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(du, hu.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s->stream);
+    double4* dq = nullptr;
+    if (e == cudaSuccess && s->oriented()) {
+        e = cudaMallocAsync((void**)&dq, sizeof(double4) * n, s->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(dq, hq.data(), sizeof(double4) * n, cudaMemcpyHostToDevice, s->stream);
+    }
     if (e == cudaSuccess) e = cudaMemsetAsync(dh, 0, sizeof(double) * n, s->stream);
     if (e == cudaSuccess) {
         if (lj)
             e = launch_eval_lj(s->dim, precision == HMC_FP32_RECHECK, s->geom, s->arr, s->pair, db, dt, du, temperature,
                                (uint32_t)n, dd, dd + n, dh, s->stream);
+        else if (s->oriented())
+            e = launch_eval_poly(precision == HMC_FP32_RECHECK, s->geom, s->arr, s->verts, s->n_vertices, s->poly_rcut2,
+                                 s->poly_rcut2_hi32, db, dt, dq, (uint32_t)n, dd, s->stream);
         else
             e = launch_eval_sphere(s->dim, precision == HMC_FP32_RECHECK, s->geom, s->arr, s->pair, db, dt,
                                    (uint32_t)n, dd, dd + n, s->stream);
@@ -673,6 +764,7 @@ hmc_status hmc_eval_moves(hmc_system* s, const hmc_injected_move* moves, uint64_
     if (du) cudaFreeAsync(du, s->stream);
     if (dh) cudaFreeAsync(dh, s->stream);
     if (dd) cudaFreeAsync(dd, s->stream);
+    if (dq) cudaFreeAsync(dq, s->stream);
     cudaError_t e2 = cudaStreamSynchronize(s->stream);
     if (e == cudaSuccess) e = e2;
     if (e != cudaSuccess) return fail(HMC_CUDA_ERROR, "eval_moves: %s", cudaGetErrorString(e));

@@ -89,6 +89,37 @@ __device__ __forceinline__ double ref_dist2(const Geometry& g, const double* t, 
     return p;
 }
 
+// ref_dist2 that also returns the per-axis difference d = t - image of the chosen image.
+template <int DIM>
+__device__ __forceinline__ double ref_disp(const Geometry& g, const double* t, const double* s, double* dout) {
+    bool inside = true;
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) inside = inside && (s[a] >= -g.half[a]) && (s[a] < g.half[a]);
+    double p = 0.0;
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) {
+        double d = dsub(t[a], s[a]);
+        if (inside) {
+            double tr = 0.0;
+            bool has = false;
+            if (s[a] > g.ghost_hi[a]) {
+                tr = -g.L[a];
+                has = true;
+            } else if (s[a] < g.ghost_lo[a]) {
+                tr = g.L[a];
+                has = true;
+            }
+            if (has) {
+                double d2 = dsub(t[a], dadd(s[a], tr));
+                if (fabs(d2) < fabs(d)) d = d2;
+            }
+        }
+        dout[a] = d;
+        p = dadd(p, dmul(d, d));
+    }
+    return p;
+}
+
 // ---- trial moves --------------------------------------------------------------------------
 // Ball::sample (hoomd-vector/src/distribution.rs:41-69).
 template <int DIM>

@@ -119,6 +119,13 @@ cudaError_t launch_eval_lj(int dim, bool fp32, const Geometry& g, const Arrays& 
                            uint8_t* decisions, uint8_t* rechecked, double* delta_h, cudaStream_t s);
 cudaError_t launch_energy_lj(int dim, const Geometry& g, const Arrays& a, const Pair& p, uint32_t n, double* out,
                              cudaStream_t s);
+cudaError_t launch_sweep_poly(bool fp32, const Geometry& g, const Arrays& a, const double4* verts, uint32_t nv,
+                              double rcut2, float rcut2_hi32, const Launch& l, bool rotate, cudaStream_t s);
+cudaError_t launch_eval_poly(bool fp32, const Geometry& g, const Arrays& a, const double4* verts, uint32_t nv,
+                             double rcut2, float rcut2_hi32, const uint64_t* bodies, const double4* trial,
+                             const double4* trial_q, uint32_t n, uint8_t* decisions, cudaStream_t s);
+cudaError_t launch_overlap_poly(const Geometry& g, const Arrays& a, const double4* verts, uint32_t nv, double rcut2,
+                                uint32_t n, cudaStream_t s);
 // Injected moves: positions (n x 4 doubles), result decisions and recheck flags.
 cudaError_t launch_eval_sphere(int dim, bool fp32, const Geometry& g, const Arrays& a, const Pair& p,
                                const uint64_t* bodies, const double4* trial, uint32_t n, uint8_t* decisions,

@@ -34,35 +34,27 @@ __device__ __forceinline__ double lj_pair64(const Pair& P, double r2) {
     return dsub(dmul(P.lj_four_eps, dsub(dmul(s4, s8), dmul(s2, s4))), P.lj_e_shift);
 }
 
-// FP32 pair energy and a bound on its error against the exact energy of the FP64 sites.
-// dr2: bound on |r2_32 - r2_exact|.
-__device__ __forceinline__ void lj_pair32(const Pair& P, float r2, float dr2, float& e, float& err) {
-    if (r2 >= P.lj_rcut2_hi32) {
-        e = 0.f;
-        err = 0.f;
-        return;
-    }
+// FP32 pair energy and a bound on its error against the exact energy of the FP64 sites, for
+// a pair with r2 below the band's upper end (the caller skips pairs outside the cut-off).
+// The r^2 error is bounded without a square root: sum |d_a| <= sqrt(3) r and
+// r <= (r^2 + 1) / 2, so |r2_32 - r2| <= 3.5 E ((r^2 + 1)/2 + E) + 3.1 u32 r^2.
+__device__ __forceinline__ void lj_pair32(const Pair& P, float r2, float& e, float& err) {
     if (r2 >= P.lj_rcut2_lo32) {  // the FP64 pass may or may not count this pair
         e = 0.f;
         err = P.lj_band_energy;
         return;
     }
-    const float sr2 = __fdiv_rn(P.lj_sigma2_32, r2);
+    const float E = P.lj_disp_err;
+    const float dr2 = 3.5f * E * (0.5f * (r2 + 1.f) + E) + 3.1f * kU32 * r2;
+    const float inv = __frcp_rn(r2);
+    const float sr2 = P.lj_sigma2_32 * inv;
     const float sr6 = sr2 * sr2 * sr2;
     const float b = P.lj_four_eps32 * sr6;  // 4 eps (sigma/r)^6
     const float a = b * sr6;                // 4 eps (sigma/r)^12
     e = (a - b) - P.lj_e_shift32;
-    // |dE/dr^2| = (6a - 3b) / r^2 at most (6a + 3b) / r^2; 1.1 covers its variation over
-    // [r2 - dr2, r2 + dr2] and the FP32 evaluation of this bound.
-    err = 1.1f * ((6.f * a + 3.f * b) * __fdiv_ru(dr2, r2) + 16.f * kU32 * (a + b + fabsf(P.lj_e_shift32)));
-}
-
-// Error bound of an FP32 r^2 formed from FP32 offsets: per-axis displacement error E,
-// sum |d_a| <= sqrt(3) r.
-__device__ __forceinline__ float r2_error(const Pair& P, float r2) {
-    const float E = P.lj_disp_err;
-    const float r = __fsqrt_ru(r2) * 1.0001f;
-    return 3.5f * E * (r + E) + 3.1f * kU32 * r2;
+    // |dE/dr^2| <= (6a + 3b) / r^2; 1.1 covers its variation over [r2 - dr2, r2 + dr2] and the
+    // FP32 evaluation of this bound; 24 u32 covers the roundings of the energy formula.
+    err = 1.1f * ((6.f * a + 3.f * b) * (dr2 * inv) + 24.f * kU32 * (a + b + fabsf(P.lj_e_shift32)));
 }
 
 // The stencil rows of space m as at most two slot ranges each (two when the row wraps around
@@ -199,15 +191,23 @@ __device__ __forceinline__ Sums32 lj_energy32(const Geometry& g, const Arrays& A
                 }
                 const float r2n = fp32_dist2<DIM>(g, t32, o, st.s0[r], st.s1[r], dm);
                 const float r2o = fp32_dist2<DIM>(g, c32, o, st.s0[r], st.s1[r], dm);
-                float en, ern, eo, ero;
-                lj_pair32(P, r2n, r2_error(P, r2n), en, ern);
-                lj_pair32(P, r2o, r2_error(P, r2o), eo, ero);
-                s.e_new += en;
-                s.e_old += eo;
-                s.err += ern + ero;
-                s.mag += fabsf(en) + fabsf(eo);
-                s.terms += 1;
                 s.pairs += 2;
+                if (r2n < P.lj_rcut2_hi32) {
+                    float e, err;
+                    lj_pair32(P, r2n, e, err);
+                    s.e_new += e;
+                    s.err += err;
+                    s.mag += fabsf(e);
+                    s.terms += 1;
+                }
+                if (r2o < P.lj_rcut2_hi32) {
+                    float e, err;
+                    lj_pair32(P, r2o, e, err);
+                    s.e_old += e;
+                    s.err += err;
+                    s.mag += fabsf(e);
+                    s.terms += 1;
+                }
             }
         }
     }

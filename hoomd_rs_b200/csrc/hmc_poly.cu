@@ -1,0 +1,455 @@
+// Hard convex polyhedra: PairwiseCutoff<HardShape<Convex<ConvexPolyhedron>>> with
+// Translate<Cartesian<3>> and Rotate<Versor> trial moves.
+//
+// The pair test is Convex::intersects_at_global (hoomd-geometry/src/convex.rs:154-170): a
+// circumsphere rejection, pair_system_to_local (hoomd-vector/src/lib.rs:878-888) and
+// XenoCollide / Minkowski portal refinement (hoomd-geometry/src/xenocollide.rs:172-414) over
+// the support function of the vertex table (shape/convex_polytope.rs:222-244). Every
+// product, sum and fused multiply-add below follows the reference's expression order, so
+// the FP64 decision is the reference's.
+//
+// One warp per trial: all lanes compute the same trial move, then stride over the stencil's
+// candidates; the first overlap found by any lane rejects the trial (early exit by vote).
+// FP32 + recheck: a candidate whose FP32 centre distance clears the circumsphere by more
+// than the FP32 error bound is skipped; every other candidate runs the FP64 test, so the
+// decisions equal the FP64 pass.
+#include <cuda_runtime.h>
+
+#include "hmc_device.cuh"
+
+namespace hmc {
+namespace {
+
+struct Q {
+    double s, x, y, z;
+};
+struct V3 {
+    double x, y, z;
+};
+
+__device__ __forceinline__ double dot3(const V3& a, const V3& b) {  // mul_add fold from 0.0
+    return dfma(a.z, b.z, dfma(a.y, b.y, dfma(a.x, b.x, 0.0)));
+}
+__device__ __forceinline__ V3 cross3(const V3& a, const V3& b) {  // cartesian.rs:604-610
+    return {dsub(dmul(a.y, b.z), dmul(a.z, b.y)), dsub(dmul(a.z, b.x), dmul(a.x, b.z)),
+            dsub(dmul(a.x, b.y), dmul(a.y, b.x))};
+}
+__device__ __forceinline__ V3 sub3(const V3& a, const V3& b) { return {dsub(a.x, b.x), dsub(a.y, b.y), dsub(a.z, b.z)}; }
+__device__ __forceinline__ V3 neg3(const V3& a) { return {-a.x, -a.y, -a.z}; }
+
+// Quaternion::mul (quaternion.rs:408-415).
+__device__ __forceinline__ Q qmul(const Q& a, const Q& b) {
+    const V3 av{a.x, a.y, a.z}, bv{b.x, b.y, b.z};
+    const double sc = dsub(dmul(a.s, b.s), dot3(av, bv));
+    const V3 c = cross3(av, bv);
+    return {sc, dadd(dadd(dmul(bv.x, a.s), dmul(av.x, b.s)), c.x), dadd(dadd(dmul(bv.y, a.s), dmul(av.y, b.s)), c.y),
+            dadd(dadd(dmul(bv.z, a.s), dmul(av.z, b.s)), c.z)};
+}
+// Versor::rotate (quaternion.rs:740-747).
+__device__ __forceinline__ V3 vrotate(const Q& q, const V3& v) {
+    const V3 qv{q.x, q.y, q.z};
+    const double k1 = dsub(dmul(q.s, q.s), dot3(qv, qv));
+    const V3 c = cross3(qv, v);
+    const double k2 = dmul(2.0, q.s);
+    const double k3 = dmul(2.0, dot3(qv, v));
+    return {dadd(dadd(dmul(v.x, k1), dmul(c.x, k2)), dmul(qv.x, k3)),
+            dadd(dadd(dmul(v.y, k1), dmul(c.y, k2)), dmul(qv.y, k3)),
+            dadd(dadd(dmul(v.z, k1), dmul(c.z, k2)), dmul(qv.z, k3))};
+}
+
+struct M3 {
+    V3 r[3];
+};
+// RotationMatrix::from(Versor) (quaternion.rs:642-690).
+__device__ __forceinline__ M3 mat_from(const Q& q) {
+    const double a = q.s, b = q.x, c = q.y, d = q.z;
+    M3 m;
+    m.r[0] = {dsub(dsub(dadd(dmul(a, a), dmul(b, b)), dmul(c, c)), dmul(d, d)),
+              dsub(dmul(dmul(2.0, b), c), dmul(dmul(2.0, a), d)), dadd(dmul(dmul(2.0, b), d), dmul(dmul(2.0, a), c))};
+    m.r[1] = {dadd(dmul(dmul(2.0, b), c), dmul(dmul(2.0, a), d)),
+              dsub(dadd(dsub(dmul(a, a), dmul(b, b)), dmul(c, c)), dmul(d, d)),
+              dsub(dmul(dmul(2.0, c), d), dmul(dmul(2.0, a), b))};
+    m.r[2] = {dsub(dmul(dmul(2.0, b), d), dmul(dmul(2.0, a), c)), dadd(dmul(dmul(2.0, c), d), dmul(dmul(2.0, a), b)),
+              dadd(dsub(dsub(dmul(a, a), dmul(b, b)), dmul(c, c)), dmul(d, d))};
+    return m;
+}
+__device__ __forceinline__ V3 mat_rotate(const M3& m, const V3& v) {
+    return {dot3(m.r[0], v), dot3(m.r[1], v), dot3(m.r[2], v)};
+}
+__device__ __forceinline__ M3 transpose(const M3& m) {
+    return {{{m.r[0].x, m.r[1].x, m.r[2].x}, {m.r[0].y, m.r[1].y, m.r[2].y}, {m.r[0].z, m.r[1].z, m.r[2].z}}};
+}
+
+// ConvexPolytope::support_mapping: argmax of ((v0 n0) + v1 n1) + v2 n2, first maximum wins.
+__device__ __forceinline__ V3 support(const double4* __restrict__ verts, uint32_t nv, const V3& n) {
+    uint32_t arg = 0;
+    double best = -INFINITY;
+    for (uint32_t i = 0; i < nv; ++i) {
+        const double4 v = ldg4(verts + i);
+        const double x = dadd(dadd(dmul(v.x, n.x), dmul(v.y, n.y)), dmul(v.z, n.z));
+        if (x > best) {
+            best = x;
+            arg = i;
+        }
+    }
+    const double4 v = ldg4(verts + arg);
+    return {v.x, v.y, v.z};
+}
+
+struct Minkowski {
+    const double4* verts;
+    uint32_t nv;
+    V3 vij;
+    M3 q, qinv;
+    // composite_support_mapping (xenocollide.rs:318-328)
+    __device__ __forceinline__ V3 operator()(const V3& n) const {
+        const V3 sb = support(verts, nv, mat_rotate(qinv, n));
+        V3 r = mat_rotate(q, sb);
+        r = {dadd(r.x, vij.x), dadd(r.y, vij.y), dadd(r.z, vij.z)};
+        const V3 sa = support(verts, nv, neg3(n));
+        return sub3(r, sa);
+    }
+};
+
+constexpr int kXenoMaxIter = 1024;  // xenocollide.rs:38
+
+// collide for N = 3 (xenocollide.rs:172-291, :361-414). The iteration caps return overlap,
+// as the reference does.
+__device__ bool collide3d(const double4* verts, uint32_t nv, const V3& vij, const Q& oij) {
+    Minkowski s;
+    s.verts = verts;
+    s.nv = nv;
+    s.vij = vij;
+    s.q = mat_from(oij);
+    s.qinv = transpose(s.q);
+    const double TOL = 2e-12;
+    const V3 v0 = vij;
+    if (fabs(v0.x) < TOL && fabs(v0.y) < TOL && fabs(v0.z) < TOL) return true;
+    V3 v1 = s(neg3(v0));
+    if (dot3(v1, v0) > 0.0) return false;
+    V3 n = cross3(v1, v0);
+    if (fabs(n.x) < TOL && fabs(n.y) < TOL && fabs(n.z) < TOL) return true;
+    V3 v2 = s(n);
+    if (dot3(v2, n) < 0.0) return false;
+    n = cross3(sub3(v1, v0), sub3(v2, v0));
+    if (dot3(n, v0) > 0.0) {
+        const V3 t = v1;
+        v1 = v2;
+        v2 = t;
+        n = neg3(n);
+    }
+    V3 v3;
+    for (int count = 1;; ++count) {
+        if (count >= kXenoMaxIter) return true;
+        v3 = s(n);
+        if (dot3(v3, n) <= 0.0) return false;
+        if (dot3(cross3(v1, v3), v0) < 0.0) {
+            v2 = v3;
+            n = cross3(sub3(v1, v0), sub3(v2, v0));
+            continue;
+        }
+        if (dot3(cross3(v3, v2), v0) < 0.0) {
+            v1 = v3;
+            n = cross3(sub3(v1, v0), sub3(v2, v0));
+            continue;
+        }
+        break;
+    }
+    V3 p0 = v1, p1 = v2, p2 = v3;
+    for (int count = 1;; ++count) {
+        V3 nn = cross3(sub3(p1, p0), sub3(p2, p0));
+        if (dot3(sub3(p0, v0), nn) < 0.0) nn = neg3(nn);
+        if (dot3(p0, nn) >= 0.0) return true;
+        const V3 vn = s(nn);
+        if (dot3(vn, nn) < 0.0) return false;
+        const double tol = dmul(TOL, dsqrt(dot3(nn, nn)));
+        if (fabs(dot3(sub3(vn, p0), nn)) < tol) return false;
+        if (fabs(dot3(p0, nn)) < tol) return true;
+        const V3 vp = cross3(vn, v0);
+        const bool t1 = dot3(vp, p0) > 0.0, t2 = dot3(vp, p1) > 0.0, t3 = dot3(vp, p2) > 0.0;
+        if (t1 && t2)
+            p0 = vn;
+        else if (t1 && !t2)
+            p2 = vn;
+        else if (!t1 && t3)
+            p1 = vn;
+        else
+            p0 = vn;
+        if (count >= kXenoMaxIter) return true;
+    }
+}
+
+// Trial site t (position) with versor qi against the site of slot q (position S via the image
+// rule, versor sorted_q[q]): HardShape::site_pair_energy -> intersects_at_global.
+__device__ __forceinline__ bool poly_overlap64(const Geometry& g, const Arrays& A, const double4* verts, uint32_t nv,
+                                               double rcut2, const double* t, const Q& qi, const double* sj, uint32_t q) {
+    double d[3];
+    const double d2 = ref_disp<3>(g, t, sj, d);
+    if (d2 >= rcut2) return false;  // r_self.distance_squared(r_other) >= r_cut^2
+    const V3 rab{-d[0], -d[1], -d[2]};  // image - t, exactly -(t - image)
+    const double4 o4 = ldg4(A.sorted_q + q);
+    const Q qj{o4.x, o4.y, o4.z, o4.w};
+    const Q ia{qi.s, -qi.x, -qi.y, -qi.z};  // Versor::inverted = conjugate
+    const V3 vij = vrotate(ia, rab);
+    const Q oij = qmul(ia, qj);
+    return collide3d(verts, nv, vij, oij);
+}
+
+// Rotate<Versor>::propose (rotate/versor.rs:40-71, 112-123): Gaussian rotation vector with
+// standard deviation sigma, rejected beyond pi, lifted by the exponential map, composed in
+// front of the current orientation.
+__device__ __forceinline__ Q versor_move(Sfc64& rng, double sigma, const double* zx, const double* zf, const Q& q) {
+    for (;;) {
+        double s0 = dadd(0.0, dmul(sigma, standard_normal(rng, zx, zf)));
+        double s1 = dadd(0.0, dmul(sigma, standard_normal(rng, zx, zf)));
+        double s2 = dadd(0.0, dmul(sigma, standard_normal(rng, zx, zf)));
+        const V3 sv{s0, s1, s2};
+        const double theta = dsqrt(dot3(sv, sv));
+        if (theta > 3.141592653589793) continue;
+        double sh, ch;
+        portable_sincos(dmul(0.5, theta), &sh, &ch);
+        double vf = ddiv(sh, theta);
+        if (!isfinite(vf)) vf = 0.5;
+        const Q dq{ch, dmul(s0, vf), dmul(s1, vf), dmul(s2, vf)};
+        return qmul(dq, q);
+    }
+}
+
+struct PolyShape {
+    const double4* verts;
+    uint32_t nv;
+    double rcut2;     // (R_a + R_b)^2
+    float rcut2_hi32; // FP32 threshold: at or above this, outside the circumsphere for certain
+};
+
+__device__ __forceinline__ bool warp_any(bool v) { return __any_sync(0xffffffffu, v); }
+
+// Overlap of the trial (t, qi; FP32 offsets t32) with any candidate of the stencil of space m,
+// skipping slot self. Lanes stride along each row; a vote after every stride step stops the
+// warp at the first overlap. FP32: the circumsphere prefilter in FP32 under the bound.
+template <bool FP32>
+__device__ __forceinline__ bool poly_overlaps(const Geometry& g, const Arrays& A, const PolyShape& sh, const double* t,
+                                              const Q& qi, float4 t32, const uint32_t* m, uint32_t self,
+                                              uint32_t lane, PairStats& st) {
+    const uint32_t sf = g.shape[2];
+    const int mf = (int)m[2];
+    for (int i0 = (g.shape[0] == 2 ? 0 : -1); i0 <= 1; ++i0) {
+        for (int i1 = (g.shape[1] == 2 ? 0 : -1); i1 <= 1; ++i1) {
+            const uint32_t base =
+                (wrap_index((int)m[0] + i0, g.shape[0]) * g.shape[1] + wrap_index((int)m[1] + i1, g.shape[1])) * sf;
+            uint32_t seg_lo[2], seg_hi[2];
+            if (sf == 2) {
+                seg_lo[0] = __ldg(A.cell_start + base);
+                seg_hi[0] = __ldg(A.cell_start + base + 2);
+                seg_lo[1] = seg_hi[1] = 0;
+            } else if (mf >= 1 && mf + 1 < (int)sf) {
+                seg_lo[0] = __ldg(A.cell_start + base + mf - 1);
+                seg_hi[0] = __ldg(A.cell_start + base + mf + 2);
+                seg_lo[1] = seg_hi[1] = 0;
+            } else if (mf == 0) {
+                seg_lo[0] = __ldg(A.cell_start + base);
+                seg_hi[0] = __ldg(A.cell_start + base + 2);
+                seg_lo[1] = __ldg(A.cell_start + base + sf - 1);
+                seg_hi[1] = __ldg(A.cell_start + base + sf);
+            } else {
+                seg_lo[0] = __ldg(A.cell_start + base + sf - 2);
+                seg_hi[0] = __ldg(A.cell_start + base + sf);
+                seg_lo[1] = __ldg(A.cell_start + base);
+                seg_hi[1] = __ldg(A.cell_start + base + 1);
+            }
+            const float s0 = (float)i0 * g.w32[0], s1 = (float)i1 * g.w32[1];
+            for (int seg = 0; seg < 2; ++seg) {
+                for (uint32_t q0 = seg_lo[seg]; q0 < seg_hi[seg]; q0 += 32) {
+                    const uint32_t q = q0 + lane;
+                    bool hit = false;
+                    if (q < seg_hi[seg] && q != self) {
+                        bool test = true;
+                        if (FP32) {
+                            const float4 o = __ldg(A.sorted_off + q);
+                            int dm = __float_as_int(o.w) - mf;
+                            if (sf >= 4) {
+                                if (dm > 1)
+                                    dm -= (int)sf;
+                                else if (dm < -1)
+                                    dm += (int)sf;
+                            }
+                            st.checks++;
+                            test = fp32_dist2<3>(g, t32, o, s0, s1, dm) < sh.rcut2_hi32;
+                            if (test) st.rechecks++;
+                        }
+                        if (test) {
+                            double sj[3];
+                            if (FP32) {
+                                const double4 b4 = ldg4(A.sorted_b + q);
+                                sj[0] = b4.x;
+                                sj[1] = b4.y;
+                                sj[2] = b4.z;
+                                wrap_inv<3>(g.L, g.invL, sj);
+                            } else {
+                                const double4 s4 = ldg4(A.sorted_s + q);
+                                sj[0] = s4.x;
+                                sj[1] = s4.y;
+                                sj[2] = s4.z;
+                                st.checks++;
+                            }
+                            hit = poly_overlap64(g, A, sh.verts, sh.nv, sh.rcut2, t, qi, sj, q);
+                        }
+                    }
+                    if (warp_any(hit)) return true;
+                }
+            }
+        }
+    }
+    return false;
+}
+
+template <bool FP32>
+__global__ void __launch_bounds__(128) k_sweep_poly3(Geometry g, Arrays A, PolyShape sh, Launch L, uint32_t rotate) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t n_warps = (gridDim.x * blockDim.x) >> 5;
+    uint32_t n_accepted = 0;
+    PairStats st;
+    for (uint32_t w = warp; w < L.n_active; w += n_warps) {
+        uint32_t m[3];
+        unpack_m<3>(__ldg(A.color_cells + (size_t)L.color * g.color_stride + w), m);
+        const uint32_t cell = cell_index<3>(g, m);
+        const uint32_t start = __ldg(A.cell_start + cell);
+        const uint32_t count = __ldg(A.cell_start + cell + 1) - start;
+        Sfc64 rng = make_rng(L.step, L.substep, L.seed, (uint64_t)cell);
+        const uint32_t k = start + canon_range_u32(rng, count);
+        const double4 b4 = A.sorted_b[k];
+        double x[3] = {b4.x, b4.y, b4.z};
+        const double4 q4 = A.sorted_q[k];
+        Q qi{q4.x, q4.y, q4.z, q4.w};
+        if (rotate) {
+            qi = versor_move(rng, L.max_move, A.zig_x, A.zig_f, qi);
+        } else {
+            double dv[3];
+            ball_sample<3>(rng, L.max_move, A.zig_x, A.zig_f, dv);
+            for (int a = 0; a < 3; ++a) x[a] = dadd(x[a], dv[a]);
+        }
+        wrap_inv<3>(g.L, g.invL, x);  // W1 = wrap(propose(..))
+        uint32_t mt[3];
+        if (!(point_to_space<3>(g, x, mt) && cell_index<3>(g, mt) == cell)) continue;
+        double t[3] = {x[0], x[1], x[2]};
+        wrap_inv<3>(g.L, g.invL, t);
+        const float4 t32 = FP32 ? cell_offsets<3>(g, t, m) : make_float4(0.f, 0.f, 0.f, 0.f);
+        if (poly_overlaps<FP32>(g, A, sh, t, qi, t32, m, k, lane, st)) continue;
+        if (lane == 0) {
+            n_accepted++;
+            double sv[3] = {t[0], t[1], t[2]};
+            wrap_inv<3>(g.L, g.invL, sv);
+            const uint32_t body = A.sorted_body[k];
+            A.sorted_b[k] = make_double4(t[0], t[1], t[2], 0.0);
+            if (!FP32) A.sorted_s[k] = make_double4(sv[0], sv[1], sv[2], 0.0);
+            A.sorted_off[k] = cell_offsets<3>(g, sv, m);
+            A.sorted_q[k] = make_double4(qi.s, qi.x, qi.y, qi.z);
+            A.body_pos[body] = make_double4(t[0], t[1], t[2], 0.0);
+            A.body_ori[body] = make_double4(qi.s, qi.x, qi.y, qi.z);
+        }
+        __syncwarp();
+    }
+    flush_stats(A.stats, st, n_accepted);
+}
+
+// Injected moves (position and versor): warp per move, decision in the requested mode.
+template <bool FP32>
+__global__ void __launch_bounds__(128) k_eval_poly3(Geometry g, Arrays A, PolyShape sh, const uint64_t* bodies,
+                                                    const double4* trial, const double4* trial_q, uint32_t n,
+                                                    uint8_t* decisions) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    PairStats st;
+    if (i < n) {
+        const uint32_t k = A.slot_of_body[bodies[i]];
+        const double4 w4 = trial[i];
+        double t[3] = {w4.x, w4.y, w4.z};
+        wrap_inv<3>(g.L, g.invL, t);
+        const double4 q4 = trial_q[i];
+        const Q qi{q4.x, q4.y, q4.z, q4.w};
+        uint32_t m[3];
+        uint8_t dec = 0;
+        if (point_to_space<3>(g, t, m)) {
+            const float4 t32 = FP32 ? cell_offsets<3>(g, t, m) : make_float4(0.f, 0.f, 0.f, 0.f);
+            dec = poly_overlaps<FP32>(g, A, sh, t, qi, t32, m, k, lane, st) ? 0 : 1;
+        } else if (lane == 0) {
+            atomicOr(&A.stats->error_flags, kErrOutsideCheckerboard);
+        }
+        if (lane == 0) decisions[i] = dec;
+    }
+    flush_stats(A.stats, st, 0u);
+}
+
+// Overlapping pairs (i < j), FP64 (the overlap check of total_energy).
+__global__ void k_overlap_poly3(Geometry g, Arrays A, PolyShape sh, uint32_t n) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t found = 0;
+    if (k < n) {
+        const uint32_t bi = A.sorted_body[k];
+        const double4 s4 = A.sorted_s[k];
+        const double t[3] = {s4.x, s4.y, s4.z};
+        const double4 q4 = A.sorted_q[k];
+        const Q qi{q4.x, q4.y, q4.z, q4.w};
+        uint32_t m[3];
+        uint32_t c = A.body_cell[bi];
+        for (int a = 2; a >= 0; --a) {
+            m[a] = c % g.shape[a];
+            c /= g.shape[a];
+        }
+        for_each_neighbor<3>(g, A.cell_start, m, [&](uint32_t q, const float*) -> bool {
+            if (A.sorted_body[q] <= bi) return false;
+            const double4 o4 = A.sorted_s[q];
+            const double sj[3] = {o4.x, o4.y, o4.z};
+            if (poly_overlap64(g, A, sh.verts, sh.nv, sh.rcut2, t, qi, sj, q)) found++;
+            return false;
+        });
+    }
+    const unsigned tot = __reduce_add_sync(0xffffffffu, found);
+    if ((threadIdx.x & 31) == 0 && tot) atomicAdd(&A.stats->overlaps, (unsigned long long)tot);
+}
+
+}  // namespace
+
+cudaError_t launch_sweep_poly(bool fp32, const Geometry& g, const Arrays& a, const double4* verts, uint32_t nv,
+                              double rcut2, float rcut2_hi32, const Launch& l, bool rotate, cudaStream_t s) {
+    if (l.n_active == 0) return cudaSuccess;
+    static int max_blocks = 0;
+    if (max_blocks == 0) {
+        int dev = 0, sms = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        max_blocks = sms * 16;
+    }
+    PolyShape sh{verts, nv, rcut2, rcut2_hi32};
+    uint32_t blocks = (l.n_active + 3) / 4;
+    if (blocks > (uint32_t)max_blocks) blocks = (uint32_t)max_blocks;
+    if (fp32)
+        k_sweep_poly3<true><<<blocks, 128, 0, s>>>(g, a, sh, l, rotate ? 1u : 0u);
+    else
+        k_sweep_poly3<false><<<blocks, 128, 0, s>>>(g, a, sh, l, rotate ? 1u : 0u);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_eval_poly(bool fp32, const Geometry& g, const Arrays& a, const double4* verts, uint32_t nv,
+                             double rcut2, float rcut2_hi32, const uint64_t* bodies, const double4* trial,
+                             const double4* trial_q, uint32_t n, uint8_t* decisions, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    PolyShape sh{verts, nv, rcut2, rcut2_hi32};
+    const uint32_t blocks = (n + 3) / 4;
+    if (fp32)
+        k_eval_poly3<true><<<blocks, 128, 0, s>>>(g, a, sh, bodies, trial, trial_q, n, decisions);
+    else
+        k_eval_poly3<false><<<blocks, 128, 0, s>>>(g, a, sh, bodies, trial, trial_q, n, decisions);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_overlap_poly(const Geometry& g, const Arrays& a, const double4* verts, uint32_t nv, double rcut2,
+                                uint32_t n, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    PolyShape sh{verts, nv, rcut2, 0.f};
+    k_overlap_poly3<<<(n + 127) / 128, 128, 0, s>>>(g, a, sh, n);
+    return cudaGetLastError();
+}
+
+}  // namespace hmc
