@@ -360,6 +360,12 @@ class Microstate:
         pos, step, _ = self.state()
         _check(_lib.hmc_set_state(self._h, pos.ctypes.data_as(_dp), None, step + 1, 0))
 
+    def tune(self, move: int, maximum: float, temperature: float, precision: int, target: float, samples: int,
+             steps: int) -> float:
+        p = hmc_sweep_params(C.sizeof(hmc_sweep_params), move, maximum, temperature, precision, 1, 0, 0)
+        _check(_lib.hmc_tune(self._h, C.byref(p), target, samples, steps))
+        return p.maximum
+
     def overlap_count(self) -> int:
         n = C.c_uint64()
         _check(_lib.hmc_overlap_check(self._h, C.byref(n)))
@@ -414,6 +420,14 @@ class Microstate:
         return e.value
 
 
+@dataclass
+class TuneOptions:
+    """hoomd_mc::TuneOptions (lib.rs:394-412)."""
+    target_acceptance: float = 0.2
+    samples: int = 8000
+    steps: int = 32
+
+
 class ParallelSweep:
     """hoomd_mc::ParallelSweep (parallel_sweep.rs:83-421) executed on the GPU.
 
@@ -440,8 +454,22 @@ class ParallelSweep:
         self.last_count = c
         return c
 
+    def tune_with_options(self, microstate: "Microstate", hamiltonian: PairwiseCutoff, macrostate: Isothermal,
+                          options: TuneOptions = TuneOptions()) -> None:
+        """Tune::tune_with_options (lib.rs:430-449): rescales the local trial's maximum."""
+        if isinstance(self.local_trial, Translate):
+            move, maximum = TRANSLATE, self.local_trial.maximum_distance
+        else:
+            move, maximum = ROTATE, self.local_trial.maximum_rotation
+        tuned = microstate.tune(move, maximum, macrostate.temperature, self.precision, options.target_acceptance,
+                                options.samples, options.steps)
+        if isinstance(self.local_trial, Translate):
+            self.local_trial.maximum_distance = tuned
+        else:
+            self.local_trial.maximum_rotation = tuned
+
 
 __all__ = ["Context", "ConvexPolyhedron", "Count", "HardShape", "HardSphere", "HmcError", "Isothermal", "Isotropic",
-           "LennardJones", "Microstate", "PairwiseCutoff", "Rotate", "Shifted",
+           "LennardJones", "Microstate", "PairwiseCutoff", "Rotate", "Shifted", "TuneOptions",
            "ParallelSweep", "Periodic", "Translate", "load_library", "SIGNATURES", "FP64", "FP32_RECHECK",
            "TRANSLATE", "ROTATE"]

@@ -651,13 +651,76 @@ hmc_status hmc_profile_read(hmc_system* s, hmc_profile* out, int reset) {
     return HMC_OK;
 }
 
+// Tune::tune_with_options for ParallelSweep (hoomd-mc/src/lib.rs:430-449, tune_local.rs:21-89):
+// `steps` rounds of `samples` trial moves of random bodies against the unchanged state, each
+// round scaling the move size by (acceptance + 1.5) / (target + 1.5) (tune_by_scaling,
+// lib.rs:514-524). The state and its counters are not modified.
 hmc_status hmc_tune(hmc_system* s, hmc_sweep_params* p, double target, uint32_t samples, uint32_t steps) {
-    (void)s;
-    (void)p;
-    (void)target;
-    (void)samples;
-    (void)steps;
-    return fail(HMC_NOT_SUPPORTED, "hmc_tune is not available in this build");
+    if (!s || !p) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
+    if (p->struct_size < sizeof(hmc_sweep_params)) return fail(HMC_INVALID_ARGUMENT, "hmc_sweep_params.struct_size");
+    if (!(target > 0.0 && target < 1.0)) return fail(HMC_INVALID_ARGUMENT, "target acceptance must be in (0, 1)");
+    if (p->move != HMC_TRANSLATE && !(p->move == HMC_ROTATE && s->oriented()))
+        return fail(HMC_NOT_SUPPORTED, "rotation moves need oriented bodies (convex polyhedra)");
+    if (!(p->maximum > 0.0) || !std::isfinite(p->maximum)) return fail(HMC_INVALID_ARGUMENT, "maximum must be positive");
+    if (!(p->temperature > 0.0)) return fail(HMC_INVALID_ARGUMENT, "temperature must be positive");
+    if (samples == 0 || samples >= (1u << 31)) return fail(HMC_INVALID_ARGUMENT, "samples must be in [1, 2^31)");
+    if (s->n == 0 || steps == 0) return HMC_OK;
+    HMC_CUDA(cudaSetDevice(s->ctx->device));
+    hmc_status st = rebuild(s, true);
+    if (st) return st;
+    double lmax = 0.0;
+    for (int a = 0; a < s->dim; ++a) lmax = std::max(lmax, s->geom.L[a]);
+    uint64_t* db = nullptr;
+    double4 *dt = nullptr, *dq = nullptr;
+    double *du = nullptr, *dh = nullptr;
+    uint8_t* dd = nullptr;
+    cudaError_t e = cudaMallocAsync((void**)&db, sizeof(uint64_t) * samples, s->stream);
+    if (e == cudaSuccess) e = cudaMallocAsync((void**)&dt, sizeof(double4) * samples, s->stream);
+    if (e == cudaSuccess) e = cudaMallocAsync((void**)&dq, sizeof(double4) * samples, s->stream);
+    if (e == cudaSuccess) e = cudaMallocAsync((void**)&du, sizeof(double) * samples, s->stream);
+    if (e == cudaSuccess) e = cudaMallocAsync((void**)&dh, sizeof(double) * samples, s->stream);
+    if (e == cudaSuccess) e = cudaMallocAsync((void**)&dd, 2 * (size_t)samples, s->stream);
+    std::vector<uint8_t> hd(samples);
+    const bool fp32 = p->precision == HMC_FP32_RECHECK;
+    for (uint32_t step = 0; step < steps && e == cudaSuccess; ++step) {
+        if (p->maximum > 4.0 * lmax) p->maximum = 4.0 * lmax;  // the samplers' bound (see hmc_sweep)
+        Launch L{};
+        L.step = s->step;
+        L.substep = s->substep;
+        L.seed = s->seed;
+        L.max_move = p->maximum;
+        L.kt = p->temperature;
+        L.n_bodies = (uint32_t)s->n;
+        e = launch_tune_moves(s->dim, s->geom, s->arr, L, step, samples, p->move == HMC_ROTATE, db, dt, dq, du, s->stream);
+        if (e != cudaSuccess) break;
+        if (s->interaction == HMC_LENNARD_JONES)
+            e = launch_eval_lj(s->dim, fp32, s->geom, s->arr, s->pair, db, dt, du, p->temperature, samples, dd,
+                               dd + samples, dh, s->stream);
+        else if (s->oriented())
+            e = launch_eval_poly(fp32, s->geom, s->arr, s->verts, s->n_vertices, s->poly_rcut2, s->poly_rcut2_hi32, db,
+                                 dt, dq, samples, dd, s->stream);
+        else
+            e = launch_eval_sphere(s->dim, fp32, s->geom, s->arr, s->pair, db, dt, samples, dd, dd + samples, s->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(hd.data(), dd, samples, cudaMemcpyDeviceToHost, s->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+        if (e != cudaSuccess) break;
+        s->prof.kernel_launches += 2;
+        uint64_t acc = 0;
+        for (uint32_t j = 0; j < samples; ++j) acc += hd[j];
+        const double ratio = (double)acc / (double)samples;
+        p->maximum *= (ratio + 1.5) / (target + 1.5);
+    }
+    if (db) cudaFreeAsync(db, s->stream);
+    if (dt) cudaFreeAsync(dt, s->stream);
+    if (dq) cudaFreeAsync(dq, s->stream);
+    if (du) cudaFreeAsync(du, s->stream);
+    if (dh) cudaFreeAsync(dh, s->stream);
+    if (dd) cudaFreeAsync(dd, s->stream);
+    cudaError_t e2 = cudaStreamSynchronize(s->stream);
+    if (e == cudaSuccess) e = e2;
+    if (e != cudaSuccess) return fail(HMC_CUDA_ERROR, "tune: %s", cudaGetErrorString(e));
+    if ((st = read_stats(s))) return st;
+    return check_flags(s);
 }
 
 hmc_status hmc_overlap_check(hmc_system* s, uint64_t* n_overlaps) {

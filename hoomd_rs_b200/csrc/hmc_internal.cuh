@@ -126,6 +126,9 @@ cudaError_t launch_eval_poly(bool fp32, const Geometry& g, const Arrays& a, cons
                              const double4* trial_q, uint32_t n, uint8_t* decisions, cudaStream_t s);
 cudaError_t launch_overlap_poly(const Geometry& g, const Arrays& a, const double4* verts, uint32_t nv, double rcut2,
                                 uint32_t n, cudaStream_t s);
+cudaError_t launch_tune_moves(int dim, const Geometry& g, const Arrays& a, const Launch& l, uint32_t tune_step,
+                              uint32_t samples, bool rotate, uint64_t* bodies, double4* trial, double4* trial_q,
+                              double* u, cudaStream_t s);
 // Injected moves: positions (n x 4 doubles), result decisions and recheck flags.
 cudaError_t launch_eval_sphere(int dim, bool fp32, const Geometry& g, const Arrays& a, const Pair& p,
                                const uint64_t* bodies, const double4* trial, uint32_t n, uint8_t* decisions,

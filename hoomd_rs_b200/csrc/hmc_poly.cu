@@ -409,6 +409,39 @@ __global__ void k_overlap_poly3(Geometry g, Arrays A, PolyShape sh, uint32_t n) 
     if ((threadIdx.x & 31) == 0 && tot) atomicAdd(&A.stats->overlaps, (unsigned long long)tot);
 }
 
+// Trial moves for the move-size tuner (tune_local.rs:21-89): sample j draws a uniformly random
+// body, proposes a move of it and its Metropolis uniform from its own counter stream
+// Counter(step, substep, seed).index(2^63 | tune_step << 32 | j). The reference draws all samples
+// from one sequential stream; per-sample streams make the samples independent of each other
+// and of the sweep's streams, with the same distribution.
+template <int DIM>
+__global__ void k_tune_moves(Geometry g, Arrays A, Launch L, uint32_t tune_step, uint32_t samples, uint32_t rotate,
+                             uint64_t* bodies, double4* trial, double4* trial_q, double* uu) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= samples) return;
+    Sfc64 rng = make_rng(L.step, L.substep, L.seed, (1ull << 63) | ((uint64_t)tune_step << 32) | (uint64_t)j);
+    const uint32_t b = canon_range_u32(rng, L.n_bodies);
+    const double4 b4 = A.body_pos[b];
+    double x[3] = {b4.x, b4.y, b4.z};
+    Q q{1.0, 0.0, 0.0, 0.0};
+    if (A.body_ori) {
+        const double4 q4 = A.body_ori[b];
+        q = Q{q4.x, q4.y, q4.z, q4.w};
+    }
+    if (rotate) {
+        q = versor_move(rng, L.max_move, A.zig_x, A.zig_f, q);
+    } else {
+        double dv[3];
+        ball_sample<DIM>(rng, L.max_move, A.zig_x, A.zig_f, dv);
+        for (int a = 0; a < DIM; ++a) x[a] = dadd(x[a], dv[a]);
+    }
+    wrap_inv<DIM>(g.L, g.invL, x);
+    bodies[j] = b;
+    trial[j] = make_double4(x[0], x[1], DIM == 3 ? x[2] : 0.0, 0.0);
+    trial_q[j] = make_double4(q.s, q.x, q.y, q.z);
+    uu[j] = uniform01(rng);
+}
+
 }  // namespace
 
 cudaError_t launch_sweep_poly(bool fp32, const Geometry& g, const Arrays& a, const double4* verts, uint32_t nv,
@@ -452,4 +485,18 @@ cudaError_t launch_overlap_poly(const Geometry& g, const Arrays& a, const double
     return cudaGetLastError();
 }
 
+}  // namespace hmc
+
+namespace hmc {
+cudaError_t launch_tune_moves(int dim, const Geometry& g, const Arrays& a, const Launch& l, uint32_t tune_step,
+                              uint32_t samples, bool rotate, uint64_t* bodies, double4* trial, double4* trial_q,
+                              double* u, cudaStream_t s) {
+    if (samples == 0) return cudaSuccess;
+    const uint32_t blocks = (samples + 127) / 128;
+    if (dim == 2)
+        k_tune_moves<2><<<blocks, 128, 0, s>>>(g, a, l, tune_step, samples, rotate ? 1u : 0u, bodies, trial, trial_q, u);
+    else
+        k_tune_moves<3><<<blocks, 128, 0, s>>>(g, a, l, tune_step, samples, rotate ? 1u : 0u, bodies, trial, trial_q, u);
+    return cudaGetLastError();
+}
 }  // namespace hmc

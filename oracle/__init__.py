@@ -91,6 +91,8 @@ def lib():
         L.oracle_parallel_sweep.restype = C.c_int
         L.oracle_serial_sweep.argtypes = [C.c_void_p, C.c_uint32, C.c_double, C.c_double, _u64p, _u64p]
         L.oracle_serial_sweep.restype = C.c_int
+        L.oracle_tune.argtypes = [C.c_void_p, C.c_uint32, C.c_double, C.c_double, C.c_double, C.c_uint32, C.c_uint32]
+        L.oracle_tune.restype = C.c_double
         L.oracle_overlap_count.argtypes = [C.c_void_p]
         L.oracle_overlap_count.restype = C.c_uint64
         L.oracle_total_energy.argtypes = [C.c_void_p]
@@ -318,6 +320,9 @@ class System:
         r = C.c_uint64()
         lib().oracle_serial_sweep(self._h, move, maximum, kt, C.byref(a), C.byref(r))
         return a.value, r.value
+
+    def tune(self, move, maximum, kt, target, samples, steps) -> float:
+        return float(lib().oracle_tune(self._h, move, maximum, kt, target, samples, steps))
 
     def overlap_count(self) -> int:
         return int(lib().oracle_overlap_count(self._h))

@@ -1264,6 +1264,30 @@ int oracle_serial_sweep(oracle_system* s, uint32_t move, double maximum, double 
     return 0;
 }
 
+// Tune::tune_with_options (tune_local.rs:21-89) with one counter stream per sample:
+// sample j of round t uses Counter(step, substep, seed).index(2^63 | t << 32 | j), draws the
+// body index, the move and the Metropolis uniform; the state is not modified.
+double oracle_tune(const oracle_system* s, uint32_t move, double maximum, double kt, double target, uint32_t samples,
+                   uint32_t steps) {
+    int ol = s->ori_len();
+    for (uint32_t t = 0; t < steps; ++t) {
+        uint64_t acc = 0;
+        for (uint32_t j = 0; j < samples; ++j) {
+            Sfc64 rng = make_rng(s->step, s->substep, s->seed, (1ull << 63) | ((uint64_t)t << 32) | (uint64_t)j);
+            uint64_t b = canon_range_u32(rng, (uint32_t)s->n);
+            double pos[3] = {0, 0, 0}, ori[4] = {0, 0, 0, 0};
+            s->propose(rng, (int)move, maximum, b, pos, ori);
+            wrap(s->dim, s->L, pos);
+            double u = uniform01(rng);
+            double dh = s->delta_energy_one(b, pos, ol ? ori : nullptr);
+            if (dh != INFINITY && (dh <= 0.0 || u < std::exp(-dh / kt))) acc += 1;
+        }
+        double ratio = (double)acc / (double)samples;
+        maximum *= (ratio + 1.5) / (target + 1.5);
+    }
+    return maximum;
+}
+
 uint64_t oracle_overlap_count(const oracle_system* s) {
     // total_energy, pairwise_cutoff.rs:720-745: pairs of sites (and ghosts) with tag_i < tag_j.
     std::vector<uint32_t> cand;

@@ -101,6 +101,9 @@ int oracle_parallel_sweep(oracle_system* s, uint32_t move, double maximum, doubl
 // Sweep::apply (sweep.rs:159-224).
 int oracle_serial_sweep(oracle_system* s, uint32_t move, double maximum, double kt,
                         uint64_t* accepted, uint64_t* rejected);
+// Move-size tuning (tune_local.rs:21-89) with per-sample counter streams; returns the tuned size.
+double oracle_tune(const oracle_system* s, uint32_t move, double maximum, double kt, double target, uint32_t samples,
+                   uint32_t steps);
 // Number of overlapping pairs (hard) / total energy (LJ), pairs with tag_i < tag_j
 // (pairwise_cutoff.rs:720-745).
 uint64_t oracle_overlap_count(const oracle_system* s);
