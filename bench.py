@@ -4,7 +4,8 @@
 Workload (one step = one ParallelSweep::apply, i.e. at least N trial moves):
 3-D hard spheres (sigma = 1), N = 2^20, periodic cubic box at packing fraction 0.50,
 FCC start with seeded jitter 0.01 sigma, translation moves with the maximum distance
-tuned to ~30 % acceptance. The headline runs the FP32 pair test with FP64 recheck; the
+tuned by Tune::tune_with_options (target acceptance 0.30, 8000 samples x 32 rounds, run on
+the device by hmc_tune). The headline runs the FP32 pair test with FP64 recheck; the
 plain FP64 sweep runs on an identical copy of the state and must end bit-identical
 (mismatches = 0).
 
@@ -20,7 +21,6 @@ import json
 import math
 import os
 import statistics
-import subprocess
 import sys
 import threading
 import time
@@ -40,7 +40,7 @@ TARGET_ACCEPTANCE = 0.30
 
 def workload_config(d, extra=None):
     cfg = {"workload": "3-D hard spheres, N=2^20, packing fraction 0.50, periodic cube, FCC start + 0.01 jitter, "
-                       "translation moves tuned to ~30% acceptance, one ParallelSweep per step",
+                       "translation moves tuned by Tune (target 0.30, hmc_tune), one ParallelSweep per step",
            "n_bodies": N_BODIES, "packing_fraction": PHI, "box_length": None, "move_size": d,
            "seed": SEED, "l2": "flushed before every timed step (256 MiB device write)"}
     if extra:
@@ -48,65 +48,74 @@ def workload_config(d, extra=None):
     return cfg
 
 
-def tune_move(micro, d, precision, rounds=12):
-    """tune_by_scaling (hoomd-mc/src/lib.rs:514-524) applied to whole-sweep counts."""
-    from hoomd_rs_b200 import TRANSLATE
-    for _ in range(rounds):
-        c = micro.sweep(TRANSLATE, d, 1.0, precision, n_sweeps=1, increment_step=False)
-        d *= (c.acceptance_ratio() + 1.5) / (TARGET_ACCEPTANCE + 1.5)
-    return d
+TUNE_SAMPLES, TUNE_STEPS, D0 = 8000, 32, 0.13
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
 
 
 class ClockSampler:
-    """nvidia-smi clock/throttle samples while the timed region runs."""
+    """SM clock and clock-event reasons sampled every 5 ms (NVML) while the timed region runs."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = {0x8: "hw_slowdown", 0x40: "hw_thermal_slowdown", 0x20: "sw_thermal_slowdown", 0x4: "sw_power_cap",
+               0x80: "hw_power_brake_slowdown"}
 
-    def __init__(self, device):
-        self.device = device
-        self.proc = None
-        self.lines = []
+    def __init__(self, local_rank):
+        self.local_rank = local_rank
+        self.samples = []
+        self.smax = None
+        self.stop_flag = threading.Event()
+        self.thread = None
+        self.error = None
+
+    def _index(self):
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+        ids = [x.strip() for x in vis.split(",") if x.strip()]
+        if ids and all(x.isdigit() for x in ids) and self.local_rank < len(ids):
+            return int(ids[self.local_rank])
+        return self.local_rank
 
     def start(self):
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
-            self.thread.start()
-        except OSError:
-            self.proc = None
+            import pynvml
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByIndex(self._index())
+            self.smax = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+        except Exception as e:  # no NVML: report it instead of clocks
+            self.error = f"nvml unavailable: {e}"
+            return
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+        def run():
+            while not self.stop_flag.is_set():
+                try:
+                    sm = pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
+                    reasons = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    self.samples.append((sm, reasons))
+                except Exception as e:
+                    self.error = str(e)
+                    return
+                self.stop_flag.wait(0.005)
+
+        self.thread = threading.Thread(target=run, daemon=True)
+        self.thread.start()
 
     def stop(self):
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        sm, smax, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
-            f = [x.strip() for x in line.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                smax = float(f[2])
-            except ValueError:
-                continue
-            for name, v in zip(names, f[5:9]):
-                if v.lower().startswith("active"):
+        if self.thread is not None:
+            self.stop_flag.set()
+            self.thread.join(timeout=5)
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.smax, "reasons": [self.error or "no samples"], "samples": 0}
+        reasons = set()
+        for _, bits in self.samples:
+            for bit, name in self.REASONS.items():
+                if bits & bit:
                     reasons.add(name)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        return {"sm_mhz": statistics.median(x for x, _ in self.samples), "sm_max_mhz": self.smax,
+                "reasons": sorted(reasons), "samples": len(self.samples), "source": "nvml, 5 ms"}
 
 
 def measured_peak_hbm():
@@ -117,22 +126,23 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
-def cpu_baseline(pos, L, d, seconds=12.0):
-    """The oracle's ParallelSweep (a C++ port of the reference) on one host core."""
+def cpu_baseline(pos, L, d, step, seconds=12.0):
+    """The oracle's ParallelSweep (a C++ port of the reference) on all host cores."""
     import oracle
-    o = oracle.System(3, [L] * 3, pos, diameter=1.0, seed=SEED)
+    threads = host_threads()
+    o = oracle.System(3, [L] * 3, pos, diameter=1.0, seed=SEED, step=step)
     trials, t0, sweeps = 0, time.perf_counter(), 0
     while True:
-        a, r = o.parallel_sweep(oracle.TRANSLATE, d, 1.0, 1.0)
+        a, r = o.parallel_sweep(oracle.TRANSLATE, d, 1.0, 1.0, threads=threads)
         o.increment_step()
         trials += a + r
         sweeps += 1
         el = time.perf_counter() - t0
-        if el >= seconds or sweeps >= 8:
+        if el >= seconds or sweeps >= 16:
             break
-    return {"value": trials / el, "unit": UNIT, "cores": 1, "kind": "port",
+    return {"value": trials / el, "unit": UNIT, "cores": threads, "kind": "port",
             "sample": f"{sweeps} ParallelSweep sweeps of the same 2^20-sphere state ({trials} trial moves, "
-                      f"{el:.1f} s)"}
+                      f"{el:.1f} s, {threads} threads)"}
 
 
 def run_reference(args, rank):
@@ -141,16 +151,18 @@ def run_reference(args, rank):
         return
     import oracle
     from hoomd_rs_b200 import lattice
+    threads = host_threads()
     pos, L = lattice.hard_sphere_box(N_BODIES, PHI, 3, SEED)
-    d = 0.26  # the tuned move size of the GPU arm at this state (~30 % acceptance)
     o = oracle.System(3, [L] * 3, pos, diameter=1.0, seed=SEED)
+    # the same tuner as the GPU arm (identical per-sample streams give the identical size)
+    d = o.tune(oracle.TRANSLATE, D0, 1.0, TARGET_ACCEPTANCE, TUNE_SAMPLES, TUNE_STEPS)
     for _ in range(args.warmup):
-        o.parallel_sweep(oracle.TRANSLATE, d, 1.0, 1.0)
+        o.parallel_sweep(oracle.TRANSLATE, d, 1.0, 1.0, threads=threads)
         o.increment_step()
     times, trials = [], 0
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        a, r = o.parallel_sweep(oracle.TRANSLATE, d, 1.0, 1.0)
+        a, r = o.parallel_sweep(oracle.TRANSLATE, d, 1.0, 1.0, threads=threads)
         times.append(time.perf_counter() - t0)
         o.increment_step()
         trials += a + r
@@ -160,8 +172,9 @@ def run_reference(args, rank):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": workload_config(d, {"box_length": L, "precision": "fp64 (CPU)"}),
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
-                             "sample": f"{args.steps} full ParallelSweep sweeps of 2^20 spheres on one host thread"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"{args.steps} full ParallelSweep sweeps of 2^20 spheres, {threads} host "
+                                       f"threads"},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -169,7 +182,7 @@ def run_reference(args, rank):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -195,7 +208,9 @@ def main():
     pos, L = lattice.hard_sphere_box(N_BODIES, PHI, 3, seed)
     h = PairwiseCutoff(HardSphere(1.0))
     tuner = Microstate(ctx, Periodic(1.0, [L] * 3), pos, h, seed=seed)
-    d = tune_move(tuner, 0.13, FP32_RECHECK)
+    d = tuner.tune(TRANSLATE, D0, 1.0, FP32_RECHECK, TARGET_ACCEPTANCE, TUNE_SAMPLES, TUNE_STEPS)
+    # a few sweeps away from the lattice before the copies start
+    tuner.sweep(TRANSLATE, d, 1.0, FP32_RECHECK, n_sweeps=4, increment_step=True)
     start_pos, step0, _ = tuner.state()
     tuner.close()
 
@@ -275,18 +290,22 @@ def main():
     peak, peak_kind = measured_peak_hbm()
     achieved = bytes_per_launch / t_launch / 1e9
 
-    # end to end through the C ABI with host buffers: upload, sweep, download every step
+    # end to end through the C ABI with pinned host buffers: every step uploads the state
+    # (hmc_set_state), sweeps, and downloads the new state (hmc_get_state)
     e2e_steps = max(3, min(args.steps, 10))
-    host = np.ascontiguousarray(pa)
+    host_in = torch.empty((N_BODIES, 3), dtype=torch.float64, pin_memory=True).numpy()
+    host_out = torch.empty((N_BODIES, 3), dtype=torch.float64, pin_memory=True).numpy()
+    host_in[:] = pa
     e2e_trials, t_e2e = 0, 0.0
     for _ in range(e2e_steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        a.set_state(host, a.step(), 0)
+        a.set_state(host_in, a.step(), 0)
         c = a.sweep(TRANSLATE, d, 1.0, FP32_RECHECK, n_sweeps=1, increment_step=True)
-        host = a.positions()
+        a.state(out=host_out)
         t_e2e += time.perf_counter() - t0
         e2e_trials += c.total()
+        host_in, host_out = host_out, host_in
     e2e_value = e2e_trials / t_e2e
     if world > 1:
         t = torch.tensor([t_e2e], dtype=torch.float64, device="cuda")
@@ -313,7 +332,7 @@ def main():
         "clocks": clocks,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(start_pos, L, d)
+        line["cpu_baseline"] = cpu_baseline(start_pos, L, d, step0)
     if rank == 0:
         print(json.dumps(line), flush=True)
     a.close()

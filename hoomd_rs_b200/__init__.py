@@ -94,6 +94,7 @@ SIGNATURES = {
     "hmc_system_stream": (_vp, [_vp]),
     "hmc_set_state": (C.c_int, [_vp, _dp, _dp, C.c_uint64, C.c_uint32]),
     "hmc_get_state": (C.c_int, [_vp, _dp, _dp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32)]),
+    "hmc_increment_step": (C.c_int, [_vp]),
     "hmc_sweep": (C.c_int, [_vp, C.POINTER(hmc_sweep_params), C.POINTER(hmc_count)]),
     "hmc_tune": (C.c_int, [_vp, C.POINTER(hmc_sweep_params), C.c_double, C.c_uint32, C.c_uint32]),
     "hmc_overlap_check": (C.c_int, [_vp, C.POINTER(C.c_uint64)]),
@@ -329,8 +330,11 @@ class Microstate:
         self.close()
 
     # microstate.rs:412-455
-    def state(self):
-        pos = np.zeros((self.n, self.dim))
+    def state(self, out: Optional[np.ndarray] = None):
+        """(positions, step, substep); `out` (n x dim float64, C-contiguous) receives the positions."""
+        pos = np.empty((self.n, self.dim)) if out is None else out
+        if pos.shape != (self.n, self.dim) or pos.dtype != np.float64 or not pos.flags.c_contiguous:
+            raise HmcError(INVALID_ARGUMENT, "out must be a C-contiguous float64 array of shape (n, dim)")
         step = C.c_uint64()
         sub = C.c_uint32()
         _check(_lib.hmc_get_state(self._h, pos.ctypes.data_as(_dp), None, C.byref(step), C.byref(sub)))
@@ -344,11 +348,17 @@ class Microstate:
     def positions(self) -> np.ndarray:
         return self.state()[0]
 
+    def _counter(self):
+        step = C.c_uint64()
+        sub = C.c_uint32()
+        _check(_lib.hmc_get_state(self._h, None, None, C.byref(step), C.byref(sub)))
+        return step.value, sub.value
+
     def step(self) -> int:
-        return self.state()[1]
+        return self._counter()[0]
 
     def substep(self) -> int:
-        return self.state()[2]
+        return self._counter()[1]
 
     def set_state(self, positions, step: int, substep: int, orientations=None):
         pos = np.ascontiguousarray(positions, dtype=np.float64).reshape(self.n, self.dim)
@@ -357,8 +367,8 @@ class Microstate:
                                   step, substep))
 
     def increment_step(self):
-        pos, step, _ = self.state()
-        _check(_lib.hmc_set_state(self._h, pos.ctypes.data_as(_dp), None, step + 1, 0))
+        """Microstate::increment_step (microstate.rs:412-430): step += 1, substep = 0."""
+        _check(_lib.hmc_increment_step(self._h))
 
     def tune(self, move: int, maximum: float, temperature: float, precision: int, target: float, samples: int,
              steps: int) -> float:

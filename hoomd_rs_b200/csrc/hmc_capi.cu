@@ -80,8 +80,12 @@ struct hmc_system {
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
     DeviceStats* host_stats = nullptr;  // pinned
+    double* stage = nullptr;            // n x dim packed positions (host layout) for set/get_state
+    unsigned long long* first_bad = nullptr;       // device word for the finiteness check
+    unsigned long long* host_first_bad = nullptr;  // pinned mirror
     std::vector<void*> allocations;
     uint32_t tile_cap[2] = {0, 0};  // staged bodies per block of the tiled pass: [fp64, fp32]
+    bool coop = false;              // warp-cooperative hard-sphere pass
     // convex polyhedron
     double4* verts = nullptr;
     uint32_t n_vertices = 0;
@@ -279,6 +283,7 @@ void hmc_system_destroy(hmc_system* s) {
     for (cudaEvent_t e : s->ev)
         if (e) cudaEventDestroy(e);
     if (s->host_stats) cudaFreeHost(s->host_stats);
+    if (s->host_first_bad) cudaFreeHost(s->host_first_bad);
     if (s->own_stream) cudaStreamDestroy(s->own_stream);
     cudaGetLastError();  // a destructor reports nothing: leave no sticky error behind
     hmc_context* c = s->ctx;
@@ -410,6 +415,7 @@ hmc_status hmc_system_create(hmc_context* ctx, const hmc_system_desc* d, const d
     // B200 for hard spheres; HMC_B200_SWEEP_KERNEL=tiled selects the tiled pass instead.
     const char* kern = std::getenv("HMC_B200_SWEEP_KERNEL");
     const bool tiled = kern && std::strcmp(kern, "tiled") == 0;
+    s->coop = kern && std::strcmp(kern, "coop") == 0;
     if (tiled && tile_kernel_applies(s->dim, s->geom)) {
         double mean = 9.0 * 9.0 * 17.0 * (double)s->n / (double)cells;
         uint32_t want = (uint32_t)(1.5 * mean + 64.0);
@@ -441,8 +447,15 @@ hmc_status hmc_system_create(hmc_context* ctx, const hmc_system_desc* d, const d
         (st = dalloc(s, &A.body_rank, n)) || (st = dalloc(s, &A.cell_count, cells)) ||
         (st = dalloc(s, &A.cell_start, cells + 1)) || (st = dalloc(s, &A.block_sums, (size_t)scan_blocks * 9)) ||
         (st = dalloc(s, &A.color_cells, cells)) ||
-        (st = dalloc(s, &A.stats, 1)))
+        (st = dalloc(s, &A.stats, 1)) || (st = dalloc(s, &s->stage, n * (uint64_t)s->dim)) ||
+        (st = dalloc(s, &s->first_bad, 1)))
         return destroy_fail(st);
+    e = cudaMallocHost((void**)&s->host_first_bad, sizeof(unsigned long long));
+    if (e != cudaSuccess) {
+        s->host_first_bad = nullptr;
+        fail(HMC_OUT_OF_MEMORY, "cudaMallocHost: %s", cudaGetErrorString(e));
+        return destroy_fail(HMC_OUT_OF_MEMORY);
+    }
     A.body_ori = nullptr;
     A.sorted_q = nullptr;
     if (s->oriented()) {
@@ -500,25 +513,31 @@ hmc_status hmc_system_set_stream(hmc_system* s, void* stream) {
 
 void* hmc_system_stream(hmc_system* s) { return s ? (void*)s->stream : nullptr; }
 
+// The host arrays are copied with one cudaMemcpyAsync each (direct DMA when the caller's
+// buffers are pinned) into the packed staging array, checked and unpacked on the device.
+// The call returns after the copies complete, so the caller may reuse its buffers; on a
+// non-finite coordinate it returns HMC_NAN_STATE and the device state is unchanged.
 hmc_status hmc_set_state(hmc_system* s, const double* positions, const double* orientations, uint64_t step,
                          uint32_t substep) {
     if (!s || (s->n > 0 && !positions)) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
-    hmc_status st = validate_positions(s, positions);
-    if (st) return st;
     HMC_CUDA(cudaSetDevice(s->ctx->device));
-    if (s->oriented() && orientations && s->n) {
-        std::vector<double4> hq(s->n);
-        for (uint64_t i = 0; i < s->n; ++i)
-            hq[i] = make_double4(orientations[4 * i], orientations[4 * i + 1], orientations[4 * i + 2], orientations[4 * i + 3]);
-        HMC_CUDA(cudaMemcpy(s->arr.body_ori, hq.data(), sizeof(double4) * s->n, cudaMemcpyHostToDevice));
+    if (s->n) {
+        const uint64_t count = s->n * (uint64_t)s->dim;
+        HMC_CUDA(cudaMemcpyAsync(s->stage, positions, sizeof(double) * count, cudaMemcpyHostToDevice, s->stream));
+        HMC_CUDA(cudaMemsetAsync(s->first_bad, 0xFF, sizeof(unsigned long long), s->stream));
+        HMC_CUDA(launch_check_finite(s->stage, count, (uint32_t)s->dim, s->first_bad, s->stream));
+        HMC_CUDA(cudaMemcpyAsync(s->host_first_bad, s->first_bad, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                                 s->stream));
+        HMC_CUDA(cudaStreamSynchronize(s->stream));
+        if (*s->host_first_bad != ~0ull)
+            return fail(HMC_NAN_STATE, "position %llu is not finite", (unsigned long long)*s->host_first_bad);
+        // Positions are body positions as returned by hmc_get_state (already wrapped).
+        HMC_CUDA(launch_unpack_positions(s->dim, s->stage, s->arr.body_pos, s->n, s->stream));
+        if (s->oriented() && orientations)  // (s, x, y, z) per body: the double4 layout
+            HMC_CUDA(cudaMemcpyAsync(s->arr.body_ori, orientations, sizeof(double4) * s->n, cudaMemcpyHostToDevice,
+                                     s->stream));
+        HMC_CUDA(cudaStreamSynchronize(s->stream));
     }
-    // Positions are body positions as returned by hmc_get_state (already wrapped).
-    std::vector<double4> host(s->n);
-    for (uint64_t i = 0; i < s->n; ++i)
-        host[i] = make_double4(positions[i * s->dim], positions[i * s->dim + 1],
-                               s->dim == 3 ? positions[i * s->dim + 2] : 0.0, 0.0);
-    if (s->n) HMC_CUDA(cudaMemcpyAsync(s->arr.body_pos, host.data(), sizeof(double4) * s->n, cudaMemcpyHostToDevice, s->stream));
-    HMC_CUDA(cudaStreamSynchronize(s->stream));
     s->step = step;
     s->substep = substep;
     return HMC_OK;
@@ -527,30 +546,27 @@ hmc_status hmc_set_state(hmc_system* s, const double* positions, const double* o
 hmc_status hmc_get_state(hmc_system* s, double* positions, double* orientations, uint64_t* step,
                          uint32_t* substep) {
     if (!s) return fail(HMC_INVALID_ARGUMENT, "NULL system");
-    HMC_CUDA(cudaSetDevice(s->ctx->device));
-    if (s->oriented() && orientations && s->n) {
-        std::vector<double4> hq(s->n);
-        HMC_CUDA(cudaMemcpyAsync(hq.data(), s->arr.body_ori, sizeof(double4) * s->n, cudaMemcpyDeviceToHost, s->stream));
-        HMC_CUDA(cudaStreamSynchronize(s->stream));
-        for (uint64_t i = 0; i < s->n; ++i) {
-            orientations[4 * i] = hq[i].x;
-            orientations[4 * i + 1] = hq[i].y;
-            orientations[4 * i + 2] = hq[i].z;
-            orientations[4 * i + 3] = hq[i].w;
+    if (s->n && (positions || (orientations && s->oriented()))) {
+        HMC_CUDA(cudaSetDevice(s->ctx->device));
+        if (positions) {
+            HMC_CUDA(launch_pack_positions(s->dim, s->arr.body_pos, s->stage, s->n, s->stream));
+            HMC_CUDA(cudaMemcpyAsync(positions, s->stage, sizeof(double) * s->n * s->dim, cudaMemcpyDeviceToHost,
+                                     s->stream));
         }
-    }
-    if (positions && s->n) {
-        std::vector<double4> host(s->n);
-        HMC_CUDA(cudaMemcpyAsync(host.data(), s->arr.body_pos, sizeof(double4) * s->n, cudaMemcpyDeviceToHost, s->stream));
+        if (s->oriented() && orientations)
+            HMC_CUDA(cudaMemcpyAsync(orientations, s->arr.body_ori, sizeof(double4) * s->n, cudaMemcpyDeviceToHost,
+                                     s->stream));
         HMC_CUDA(cudaStreamSynchronize(s->stream));
-        for (uint64_t i = 0; i < s->n; ++i) {
-            positions[i * s->dim] = host[i].x;
-            positions[i * s->dim + 1] = host[i].y;
-            if (s->dim == 3) positions[i * s->dim + 2] = host[i].z;
-        }
     }
     if (step) *step = s->step;
     if (substep) *substep = s->substep;
+    return HMC_OK;
+}
+
+hmc_status hmc_increment_step(hmc_system* s) {
+    if (!s) return fail(HMC_INVALID_ARGUMENT, "NULL system");
+    s->step += 1;
+    s->substep = 0;
     return HMC_OK;
 }
 
@@ -601,7 +617,7 @@ hmc_status hmc_sweep(hmc_system* s, const hmc_sweep_params* p, hmc_count* out) {
                     HMC_CUDA(launch_sweep_poly(fp32, s->geom, s->arr, s->verts, s->n_vertices, s->poly_rcut2,
                                                s->poly_rcut2_hi32, L, p->move == HMC_ROTATE, s->stream));
                 else
-                    HMC_CUDA(launch_sweep_sphere(s->dim, fp32, s->geom, s->arr, s->pair, L, s->tile_cap[fp32], s->stream));
+                    HMC_CUDA(launch_sweep_sphere(s->dim, fp32, s->geom, s->arr, s->pair, L, s->tile_cap[fp32], s->coop, s->stream));
                 s->prof.kernel_launches += 1;
             }
             s->substep += 1;  // increment_substep after every full colour set

@@ -190,12 +190,13 @@ __device__ __forceinline__ void unpack_m(uint32_t p, uint32_t* m) {
 template <int DIM>
 constexpr int kRows = DIM == 3 ? 9 : 3;
 
+// Row ranges of the stencil around space m: for each of the 3^(DIM-1) rows along the fast
+// (last) axis, [a0, a1) covers the contiguous spaces lo .. hi-1 of that row in cell order.
+// A slow axis with two spaces contributes each neighbour row once.
 template <int DIM>
 __device__ __forceinline__ void load_rows(const Geometry& g, const uint32_t* __restrict__ cs, const uint32_t* m,
-                                          uint32_t* a0, uint32_t* a1) {
-    const uint32_t sf = g.shape[DIM - 1], mf = m[DIM - 1];
-    const uint32_t lo = sf == 2 ? 0u : mf - 1u;
-    const uint32_t hi = sf == 2 ? 2u : mf + 2u;
+                                          uint32_t lo, uint32_t hi, uint32_t* a0, uint32_t* a1) {
+    const uint32_t sf = g.shape[DIM - 1];
 #pragma unroll
     for (int r = 0; r < kRows<DIM>; ++r) {
         int i0 = DIM == 3 ? r / 3 - 1 : 0;
@@ -215,6 +216,14 @@ __device__ __forceinline__ void load_rows(const Geometry& g, const uint32_t* __r
         a0[r] = skip ? 0u : __ldg(cs + base + lo);
         a1[r] = skip ? 0u : __ldg(cs + base + hi);
     }
+}
+
+// The fast-axis span of the row ranges: spaces mf-1 .. mf+1 when they are contiguous; at
+// the two ends of a periodic fast axis the span stops at the end and the wrapped space
+// (sf-1 for mf = 0, 0 for mf = sf-1) is covered by a second pass with `wrapped_lo`.
+__device__ __forceinline__ void row_span(uint32_t sf, uint32_t mf, uint32_t* lo, uint32_t* hi) {
+    *lo = sf == 2 ? 0u : (mf == 0 ? 0u : mf - 1u);
+    *hi = sf == 2 ? 2u : (mf + 1u == sf ? sf : mf + 2u);
 }
 
 // Generic stencil walk (any position of m, including the fast-axis ends): calls

@@ -105,8 +105,9 @@ cudaError_t launch_rebuild(int dim, const Geometry& g, const Arrays& a, uint32_t
 // tile_cap > 0 selects the shared-memory tiled pass (3-D, at least 9 x 9 x 17 spaces) with room
 // for tile_cap staged bodies per block; a block whose region holds more falls back to
 // global-memory neighbour reads.
+// coop selects the warp-cooperative pass (the per-lane pass otherwise).
 cudaError_t launch_sweep_sphere(int dim, bool fp32, const Geometry& g, const Arrays& a, const Pair& p,
-                                const Launch& l, uint32_t tile_cap, cudaStream_t s);
+                                const Launch& l, uint32_t tile_cap, bool coop, cudaStream_t s);
 size_t tile_smem_bytes(bool fp32, uint32_t cap);
 bool tile_kernel_applies(int dim, const Geometry& g);
 cudaError_t launch_overlap_sphere(int dim, const Geometry& g, const Arrays& a, const Pair& p, uint32_t n,
@@ -129,6 +130,13 @@ cudaError_t launch_overlap_poly(const Geometry& g, const Arrays& a, const double
 cudaError_t launch_tune_moves(int dim, const Geometry& g, const Arrays& a, const Launch& l, uint32_t tune_step,
                               uint32_t samples, bool rotate, uint64_t* bodies, double4* trial, double4* trial_q,
                               double* u, cudaStream_t s);
+// State transfer through a packed staging array of n x dim doubles (the host layout):
+// first_nonfinite receives the smallest body index with a non-finite coordinate (it must hold
+// ~0 before the launch); unpack writes body positions, pack reads them.
+cudaError_t launch_check_finite(const double* packed, uint64_t count, uint32_t dim,
+                                unsigned long long* first_nonfinite, cudaStream_t s);
+cudaError_t launch_unpack_positions(int dim, const double* packed, double4* body_pos, uint64_t n, cudaStream_t s);
+cudaError_t launch_pack_positions(int dim, const double4* body_pos, double* packed, uint64_t n, cudaStream_t s);
 // Injected moves: positions (n x 4 doubles), result decisions and recheck flags.
 cudaError_t launch_eval_sphere(int dim, bool fp32, const Geometry& g, const Arrays& a, const Pair& p,
                                const uint64_t* bodies, const double4* trial, uint32_t n, uint8_t* decisions,

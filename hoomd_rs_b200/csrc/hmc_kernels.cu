@@ -169,8 +169,9 @@ __global__ void __launch_bounds__(128, HMC_SWEEP_MIN_BLOCKS) k_sweep_sphere(Geom
         const uint32_t sf = g.shape[DIM - 1], mf = m[DIM - 1];
         const bool edge = sf > 2 && (mf == 0 || mf + 1 == sf);
         // The stencil depends only on the space: start its loads before the proposal math.
-        uint32_t a0[kRows<DIM>], a1[kRows<DIM>];
-        if (!edge) load_rows<DIM>(g, A.cell_start, m, a0, a1);
+        uint32_t a0[kRows<DIM>], a1[kRows<DIM>], lo, hi;
+        row_span(sf, mf, &lo, &hi);
+        load_rows<DIM>(g, A.cell_start, m, lo, hi, a0, a1);
         const uint32_t start = __ldg(A.cell_start + cell);
         const uint32_t count = __ldg(A.cell_start + cell + 1) - start;
         Sfc64 rng = make_rng(L.step, L.substep, L.seed, (uint64_t)cell);
@@ -188,15 +189,219 @@ __global__ void __launch_bounds__(128, HMC_SWEEP_MIN_BLOCKS) k_sweep_sphere(Geom
         double t[3] = {x[0], x[1], DIM == 3 ? x[2] : 0.0};
         wrap_inv<DIM>(g.L, g.invL, t);  // delta_energy_one wraps the site again: T = wrap(W1)
         float4 t32 = FP32 ? cell_offsets<DIM>(g, t, m) : make_float4(0.f, 0.f, 0.f, 0.f);
-        int res = edge ? kUncertain : sphere_overlaps_rows<DIM, FP32>(g, A, P, t, t32, (int)mf, k, a0, a1, st);
+        int res = sphere_overlaps_rows<DIM, FP32>(g, A, P, t, t32, (int)mf, k, a0, a1, st);
+        if (edge && res != kOverlap) {
+            // the wrapped space of each row; its stored fast-axis index is sf-1 (mf = 0) or 0
+            // (mf = sf-1), so a virtual mf of sf or -1 gives the cell shift -1 or +1
+            const uint32_t wlo = mf == 0 ? sf - 1u : 0u;
+            load_rows<DIM>(g, A.cell_start, m, wlo, wlo + 1u, a0, a1);
+            int r2 = sphere_overlaps_rows<DIM, FP32>(g, A, P, t, t32, mf == 0 ? (int)sf : -1, k, a0, a1, st);
+            res = r2 == kOverlap ? kOverlap : (res == kUncertain || r2 == kUncertain ? kUncertain : kClear);
+        }
         if (res == kUncertain) {
             PairStats st2;  // the fast path already counted its pair checks
             res = sphere_overlaps_generic<DIM, FP32>(g, A, P, t, t32, m, k, st2) ? kOverlap : kClear;
             st.rechecks += st2.rechecks;
             st.max_err = st2.max_err > st.max_err ? st2.max_err : st.max_err;
-            if (edge) st.checks += st2.checks;
         }
         if (res == kOverlap) continue;
+        n_accepted++;
+        // update_body_properties: body = wrap(W1) = T, site = wrap(body)
+        double sv[3] = {t[0], t[1], t[2]};
+        wrap_inv<DIM>(g.L, g.invL, sv);
+        A.sorted_b[k] = make_double4(t[0], t[1], t[2], 0.0);
+        if (!FP32) A.sorted_s[k] = make_double4(sv[0], sv[1], sv[2], 0.0);
+        A.sorted_off[k] = cell_offsets<DIM>(g, sv, m);
+        A.body_pos[A.sorted_body[k]] = make_double4(t[0], t[1], t[2], 0.0);
+    }
+    flush_stats(A.stats, st, n_accepted);
+}
+
+// ---- the colour pass, warp-cooperative -------------------------------------------------------
+// Each lane proposes the trial of its own space and walks the first kOwnSteps candidates of
+// every stencil row itself; most overlapping trials end there. The trials still undecided
+// (every accepted trial among them) then have their remaining candidates tested by the
+// whole warp, one trial at a time: lane l takes range l % nr at depth l / nr, so a trial's
+// ~27 candidates take one or two warp steps instead of a divergent per-lane loop whose
+// length is the longest row of any lane. A decision is the OR over its candidates, so the
+// order of the tests cannot change it.
+#ifndef HMC_COOP_OWN_STEPS
+#define HMC_COOP_OWN_STEPS 1
+#endif
+constexpr uint32_t kOwnSteps = HMC_COOP_OWN_STEPS;
+constexpr int kFlagOverlap = 1, kFlagUncertain = 2, kFlagMore = 4;
+
+// Candidates k < k_end of every row range; returns kFlagOverlap, or kFlagUncertain and
+// kFlagMore (some row has candidates at k >= k_end).
+template <int DIM, bool FP32>
+__device__ __forceinline__ int sphere_rows_head(const Geometry& g, const Arrays& A, const Pair& P, const double* t,
+                                                float4 t32, int mf, uint32_t self, const uint32_t* a0,
+                                                const uint32_t* a1, uint32_t k_end, PairStats& st) {
+    constexpr int R = kRows<DIM>;
+    int flags = 0;
+    for (uint32_t k = 0; k < k_end; ++k) {
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            uint32_t q = a0[r] + k;
+            if (q < a1[r] && q != self) {
+                st.checks++;
+                if (FP32) {
+                    float4 v = __ldg(A.sorted_off + q);
+                    int i0 = DIM == 3 ? r / 3 - 1 : 0;
+                    int i1 = DIM == 3 ? r % 3 - 1 : r - 1;
+                    float s0 = DIM == 3 ? (float)i0 * g.w32[0] : (float)i1 * g.w32[0];
+                    float s1 = DIM == 3 ? (float)i1 * g.w32[1] : 0.f;
+                    float dd = fp32_dist2<DIM>(g, t32, v, s0, s1, __float_as_int(v.w) - mf);
+                    if (dd < P.sig2_lo32) return kFlagOverlap;
+                    if (dd < P.sig2_hi32) flags |= kFlagUncertain;
+                } else {
+                    double4 v = ldg4(A.sorted_s + q);
+                    double sv[3] = {v.x, v.y, v.z};
+                    if (ref_dist2<DIM>(g, t, sv) < P.sigma2) return kFlagOverlap;
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+        if (a0[r] + k_end < a1[r]) flags |= kFlagMore;
+    return flags;
+}
+
+template <int DIM, bool FP32>
+__global__ void __launch_bounds__(128, HMC_SWEEP_MIN_BLOCKS) k_sweep_sphere_coop(Geometry g, Arrays A, Pair P,
+                                                                                  Launch L) {
+    constexpr int R = kRows<DIM>;
+    constexpr int NR = 2 * R;  // row ranges plus, at a fast-axis end, the wrapped spaces
+    using Site = typename std::conditional<FP32, float4, double4>::type;
+    __shared__ Site s_site[4][32];
+    __shared__ uint32_t s_lo[4][32][NR];
+    __shared__ uint32_t s_hi[4][32][NR];
+    __shared__ int s_mf[4][32][2];
+    __shared__ uint32_t s_self[4][32];
+    const unsigned full = 0xffffffffu;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // this lane's range and depth for a trial with R or 2R ranges
+    const uint32_t rA = lane % R, dA = lane / R, rB = lane % NR, dB = lane / NR;
+    uint32_t n_accepted = 0;
+    PairStats st;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x + warp * 32; base < L.n_active; base += stride) {
+        const uint32_t tid = base + lane;
+        uint32_t m[3] = {0, 0, 0}, cell = 0, k = 0, sf = g.shape[DIM - 1], mf = 0;
+        double t[3] = {0.0, 0.0, 0.0};
+        float4 t32 = make_float4(0.f, 0.f, 0.f, 0.f);
+        int res = kFlagOverlap;  // lanes without a trial in the cell count as decided
+        bool edge = false, trial = false;
+        if (tid < L.n_active) {
+            unpack_m<DIM>(__ldg(A.color_cells + (size_t)L.color * g.color_stride + tid), m);
+            cell = cell_index<DIM>(g, m);
+            mf = m[DIM - 1];
+            edge = sf > 2 && (mf == 0 || mf + 1 == sf);
+            uint32_t a0[R], a1[R], lo, hi;
+            row_span(sf, mf, &lo, &hi);
+            load_rows<DIM>(g, A.cell_start, m, lo, hi, a0, a1);
+            const uint32_t start = __ldg(A.cell_start + cell);
+            const uint32_t count = __ldg(A.cell_start + cell + 1) - start;
+            Sfc64 rng = make_rng(L.step, L.substep, L.seed, (uint64_t)cell);
+            k = start + canon_range_u32(rng, count);
+            double4 b4 = A.sorted_b[k];
+            double x[3] = {b4.x, b4.y, b4.z};
+            double dv[3];
+            ball_sample<DIM>(rng, L.max_move, A.zig_x, A.zig_f, dv);
+#pragma unroll
+            for (int a = 0; a < DIM; ++a) x[a] = dadd(x[a], dv[a]);
+            wrap_inv<DIM>(g.L, g.invL, x);  // W1 = wrap(propose(..))
+            uint32_t mt[3];
+            if (point_to_space<DIM>(g, x, mt) && cell_index<DIM>(g, mt) == cell) {
+                trial = true;
+                t[0] = x[0];
+                t[1] = x[1];
+                t[2] = DIM == 3 ? x[2] : 0.0;
+                wrap_inv<DIM>(g.L, g.invL, t);  // delta_energy_one wraps the site again: T = wrap(W1)
+                if (FP32) t32 = cell_offsets<DIM>(g, t, m);
+                res = sphere_rows_head<DIM, FP32>(g, A, P, t, t32, (int)mf, k, a0, a1, kOwnSteps, st);
+                if (res != kFlagOverlap && (res & kFlagMore || edge)) {
+                    // hand the rest to the warp: remaining row ranges, then the wrapped spaces
+#pragma unroll
+                    for (int r = 0; r < R; ++r) {
+                        s_lo[warp][lane][r] = a0[r] + kOwnSteps;
+                        s_hi[warp][lane][r] = a1[r];
+                    }
+                    if (edge) {
+                        const uint32_t wlo = mf == 0 ? sf - 1u : 0u;
+                        load_rows<DIM>(g, A.cell_start, m, wlo, wlo + 1u, a0, a1);
+#pragma unroll
+                        for (int r = 0; r < R; ++r) {
+                            s_lo[warp][lane][R + r] = a0[r];
+                            s_hi[warp][lane][R + r] = a1[r];
+                        }
+                        res |= kFlagMore;
+                    }
+                    if constexpr (FP32)
+                        s_site[warp][lane] = t32;
+                    else
+                        s_site[warp][lane] = make_double4(t[0], t[1], t[2], 0.0);
+                    s_mf[warp][lane][0] = (int)mf;
+                    s_mf[warp][lane][1] = mf == 0 ? (int)sf : -1;
+                    s_self[warp][lane] = k;
+                }
+            }
+        }
+        const unsigned pending = __ballot_sync(full, (res & kFlagMore) != 0);
+        const unsigned edges = __ballot_sync(full, edge);
+        __syncwarp();
+        for (unsigned todo = pending; todo; todo &= todo - 1) {
+            const int src = __ffs(todo) - 1;
+            const bool wide = (edges >> src) & 1u;
+            const uint32_t r = wide ? rB : rA, dep = wide ? dB : dA, per = wide ? 32u / NR : 32u / R;
+            const bool mine = dep < per;
+            const uint32_t self = s_self[warp][src];
+            const uint32_t hi = mine ? s_hi[warp][src][r] : 0u;
+            uint32_t q = mine ? s_lo[warp][src][r] + dep : 0u;
+            const int mfx = s_mf[warp][src][r < (uint32_t)R ? 0 : 1];
+            const Site site = s_site[warp][src];
+            int f = 0;
+            while (__any_sync(full, q < hi)) {
+                if (q < hi && q != self) {
+                    st.checks++;
+                    if constexpr (FP32) {
+                        const float4 t4 = site;
+                        float4 v = __ldg(A.sorted_off + q);
+                        const int rr = (int)(r % R);
+                        int i0 = DIM == 3 ? rr / 3 - 1 : 0;
+                        int i1 = DIM == 3 ? rr % 3 - 1 : rr - 1;
+                        float s0 = DIM == 3 ? (float)i0 * g.w32[0] : (float)i1 * g.w32[0];
+                        float s1 = DIM == 3 ? (float)i1 * g.w32[1] : 0.f;
+                        float dd = fp32_dist2<DIM>(g, t4, v, s0, s1, __float_as_int(v.w) - mfx);
+                        if (dd < P.sig2_lo32)
+                            f |= kFlagOverlap;
+                        else if (dd < P.sig2_hi32)
+                            f |= kFlagUncertain;
+                    } else {
+                        const double4 t4 = site;
+                        const double tv[3] = {t4.x, t4.y, t4.z};
+                        double4 v = ldg4(A.sorted_s + q);
+                        double sv[3] = {v.x, v.y, v.z};
+                        if (ref_dist2<DIM>(g, tv, sv) < P.sigma2) f |= kFlagOverlap;
+                    }
+                }
+                if (__any_sync(full, f & kFlagOverlap)) break;
+                q += per;
+            }
+            const unsigned ov = __ballot_sync(full, f & kFlagOverlap);
+            const unsigned un = __ballot_sync(full, f & kFlagUncertain);
+            if (lane == src) res = ov ? kFlagOverlap : ((res & kFlagUncertain) | (un ? kFlagUncertain : 0));
+        }
+        __syncwarp();
+        if (!trial || res == kFlagOverlap) continue;
+        if (res & kFlagUncertain) {
+            PairStats st2;  // the fast path already counted its pair checks
+            const bool ov = sphere_overlaps_generic<DIM, FP32>(g, A, P, t, t32, m, k, st2);
+            st.rechecks += st2.rechecks;
+            st.max_err = st2.max_err > st.max_err ? st2.max_err : st.max_err;
+            if (ov) continue;
+        }
         n_accepted++;
         // update_body_properties: body = wrap(W1) = T, site = wrap(body)
         double sv[3] = {t[0], t[1], t[2]};
@@ -744,7 +949,65 @@ inline uint32_t blocks_for(T n, uint32_t threads) {
     return (uint32_t)((n + threads - 1) / threads);
 }
 
+// ---- state transfer ------------------------------------------------------------------
+__global__ void k_check_finite(const double* __restrict__ packed, uint64_t count, uint32_t dim,
+                               unsigned long long* first_nonfinite) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < count;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        if (!isfinite(packed[i])) atomicMin(first_nonfinite, (unsigned long long)(i / dim));
+    }
+}
+
+template <int DIM>
+__global__ void k_unpack_positions(const double* __restrict__ packed, double4* __restrict__ body_pos, uint64_t n) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const double* p = packed + i * DIM;
+        body_pos[i] = make_double4(p[0], p[1], DIM == 3 ? p[2] : 0.0, 0.0);
+    }
+}
+
+template <int DIM>
+__global__ void k_pack_positions(const double4* __restrict__ body_pos, double* __restrict__ packed, uint64_t n) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        double4 b = body_pos[i];
+        double* p = packed + i * DIM;
+        p[0] = b.x;
+        p[1] = b.y;
+        if (DIM == 3) p[2] = b.z;
+    }
+}
+
+inline uint32_t stream_grid(uint64_t n) {
+    uint64_t b = (n + 255) / 256;
+    return (uint32_t)(b < 148ull * 16 ? (b ? b : 1) : 148ull * 16);
+}
+
 }  // namespace
+
+cudaError_t launch_check_finite(const double* packed, uint64_t count, uint32_t dim,
+                                unsigned long long* first_nonfinite, cudaStream_t s) {
+    if (count == 0) return cudaSuccess;
+    k_check_finite<<<stream_grid(count), 256, 0, s>>>(packed, count, dim, first_nonfinite);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_unpack_positions(int dim, const double* packed, double4* body_pos, uint64_t n, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    if (dim == 2)
+        k_unpack_positions<2><<<stream_grid(n), 256, 0, s>>>(packed, body_pos, n);
+    else
+        k_unpack_positions<3><<<stream_grid(n), 256, 0, s>>>(packed, body_pos, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pack_positions(int dim, const double4* body_pos, double* packed, uint64_t n, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    if (dim == 2)
+        k_pack_positions<2><<<stream_grid(n), 256, 0, s>>>(body_pos, packed, n);
+    else
+        k_pack_positions<3><<<stream_grid(n), 256, 0, s>>>(body_pos, packed, n);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_rebuild(int dim, const Geometry& g, const Arrays& a, uint32_t n, bool write_s, cudaStream_t s) {
     cudaError_t e = cudaMemsetAsync(a.cell_count, 0, sizeof(uint32_t) * g.n_cells, s);
@@ -790,8 +1053,40 @@ bool tile_kernel_applies(int dim, const Geometry& g) {
 }
 
 cudaError_t launch_sweep_sphere(int dim, bool fp32, const Geometry& g, const Arrays& a, const Pair& p,
-                                const Launch& l, uint32_t tile_cap, cudaStream_t s) {
+                                const Launch& l, uint32_t tile_cap, bool coop, cudaStream_t s) {
     if (l.n_active == 0) return cudaSuccess;  // no non-empty space of this colour
+    if (coop) {
+        static int coop_blocks[2][2] = {{0, 0}, {0, 0}};
+        int& cb = coop_blocks[dim == 3][fp32];
+        if (cb == 0) {
+            int dev = 0, sms = 0, per_sm = 0;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            cudaError_t e;
+            if (dim == 2)
+                e = fp32 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_sphere_coop<2, true>, 128, 0)
+                         : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_sphere_coop<2, false>, 128, 0);
+            else
+                e = fp32 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_sphere_coop<3, true>, 128, 0)
+                         : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_sphere_coop<3, false>, 128, 0);
+            if (e != cudaSuccess) return e;
+            cb = sms * (per_sm > 0 ? per_sm : 1);
+        }
+        uint32_t grid = blocks_for(l.n_active, 128);
+        if (grid > (uint32_t)cb) grid = (uint32_t)cb;
+        if (dim == 2) {
+            if (fp32)
+                k_sweep_sphere_coop<2, true><<<grid, 128, 0, s>>>(g, a, p, l);
+            else
+                k_sweep_sphere_coop<2, false><<<grid, 128, 0, s>>>(g, a, p, l);
+        } else {
+            if (fp32)
+                k_sweep_sphere_coop<3, true><<<grid, 128, 0, s>>>(g, a, p, l);
+            else
+                k_sweep_sphere_coop<3, false><<<grid, 128, 0, s>>>(g, a, p, l);
+        }
+        return cudaGetLastError();
+    }
     if (tile_cap > 0 && tile_kernel_applies(dim, g)) {
         dim3 grid((g.half_shape[2] + kTZ - 1) / kTZ, (g.half_shape[1] + kTY - 1) / kTY,
                   (g.half_shape[0] + kTX - 1) / kTX);

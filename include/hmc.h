@@ -156,11 +156,16 @@ void hmc_system_destroy(hmc_system* sys);
 /* Run the system's device work on an external cudaStream_t (NULL: the library's own). */
 hmc_status hmc_system_set_stream(hmc_system* sys, void* cuda_stream);
 void* hmc_system_stream(hmc_system* sys);
-/* positions: n*dim; orientations: n*4 (3-D) or n (2-D) or NULL for unoriented bodies. */
+/* positions: n*dim; orientations: n*4 (3-D) or n (2-D) or NULL for unoriented bodies.
+ * Each host array moves with one copy (direct DMA from pinned buffers); both calls return
+ * after their copies complete. set_state returns HMC_NAN_STATE, leaving the device state
+ * unchanged, when a coordinate is not finite. */
 hmc_status hmc_set_state(hmc_system* sys, const double* positions, const double* orientations, uint64_t step,
                          uint32_t substep);
 hmc_status hmc_get_state(hmc_system* sys, double* positions, double* orientations, uint64_t* step,
                          uint32_t* substep);
+/* Microstate::increment_step (hoomd-microstate/src/microstate.rs:412-415): step += 1, substep = 0. */
+hmc_status hmc_increment_step(hmc_system* sys);
 
 /* ---- the sweep ---- */
 hmc_status hmc_sweep(hmc_system* sys, const hmc_sweep_params* params, hmc_count* out);

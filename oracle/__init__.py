@@ -89,6 +89,9 @@ def lib():
         L.oracle_parallel_sweep.argtypes = [C.c_void_p, C.c_uint32, C.c_double, C.c_double, C.c_double,
                                             _u64p, _u64p]
         L.oracle_parallel_sweep.restype = C.c_int
+        L.oracle_parallel_sweep_threads.argtypes = [C.c_void_p, C.c_uint32, C.c_double, C.c_double, C.c_double,
+                                                    C.c_uint32, _u64p, _u64p]
+        L.oracle_parallel_sweep_threads.restype = C.c_int
         L.oracle_serial_sweep.argtypes = [C.c_void_p, C.c_uint32, C.c_double, C.c_double, _u64p, _u64p]
         L.oracle_serial_sweep.restype = C.c_int
         L.oracle_tune.argtypes = [C.c_void_p, C.c_uint32, C.c_double, C.c_double, C.c_double, C.c_uint32, C.c_uint32]
@@ -306,11 +309,11 @@ class System:
     def increment_step(self):
         lib().oracle_increment_step(self._h)
 
-    def parallel_sweep(self, move, maximum, kt, body_interaction_range):
+    def parallel_sweep(self, move, maximum, kt, body_interaction_range, threads=1):
         a = C.c_uint64()
         r = C.c_uint64()
-        rc = lib().oracle_parallel_sweep(self._h, move, maximum, kt, body_interaction_range, C.byref(a),
-                                         C.byref(r))
+        rc = lib().oracle_parallel_sweep_threads(self._h, move, maximum, kt, body_interaction_range, threads,
+                                                 C.byref(a), C.byref(r))
         if rc:
             raise RuntimeError(f"oracle parallel sweep failed ({rc})")
         return a.value, r.value

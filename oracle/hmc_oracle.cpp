@@ -26,6 +26,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 namespace {
@@ -1178,8 +1179,13 @@ void oracle_increment_step(oracle_system* s) {
     s->substep = 0;
 }
 
-int oracle_parallel_sweep(oracle_system* s, uint32_t move, double maximum, double kt, double range,
-                          uint64_t* accepted, uint64_t* rejected) {
+// ParallelSweep::apply (parallel_sweep.rs:390-421). The trials of one colour pass only read
+// the pre-colour state, so `threads` workers evaluate contiguous slices of the colour's
+// space list (the reference does this with rayon); the accepted moves are then applied in
+// space-list order, so the cell lists, and with them every later sum, do not depend on the
+// thread count.
+static int parallel_sweep_impl(oracle_system* s, uint32_t move, double maximum, double kt, double range,
+                               unsigned threads, uint64_t* accepted, uint64_t* rejected) {
     // update_checkerboard, parallel_sweep.rs:176-201
     Checkerboard cb;
     if (!checkerboard_for_counter(s->dim, s->L, range, s->step, s->substep, s->seed, cb)) return 1;
@@ -1197,40 +1203,56 @@ int oracle_parallel_sweep(oracle_system* s, uint32_t move, double maximum, doubl
         uint64_t body;
         double pos[3];
         double ori[4];
+        int outcome;  // 0 empty space, 1 rejected, 2 accepted
     };
-    std::vector<Trial> accepted_trials;
+    std::vector<Trial> trials;
     int ol = s->ori_len();
+    if (threads == 0) threads = 1;
+    // generate_trial_moves, :209-279 (every trial sees the pre-colour state)
+    auto generate = [&](const std::vector<uint64_t>& space_indices, size_t lo, size_t hi) {
+        for (size_t k = lo; k < hi; ++k) {
+            uint64_t sp = space_indices[k];
+            Trial& t = trials[k];
+            t.outcome = 0;
+            const auto& members = spaces[sp];
+            Sfc64 rng = make_rng(s->step, s->substep, s->seed, sp);
+            if (members.empty()) continue;  // EmptySpace: not counted (:299)
+            uint32_t pick = canon_range_u32(rng, (uint32_t)members.size());
+            uint64_t b = members[pick];
+            t.body = b;
+            for (int q = 0; q < 4; ++q) t.ori[q] = 0.0;
+            s->propose(rng, (int)move, maximum, b, t.pos, t.ori);
+            wrap(s->dim, s->L, t.pos);
+            t.outcome = 1;
+            if (point_to_space(cb, t.pos) != (int64_t)sp) continue;
+            double dh = s->delta_energy_one(b, t.pos, t.ori);
+            if (dh != INFINITY && (dh <= 0.0 || uniform01(rng) < std::exp(-dh / kt))) t.outcome = 2;
+        }
+    };
     // apply, :390-421
     while (acc + rej < s->n) {
         for (auto& space_indices : by_color) {
-            accepted_trials.clear();
-            // generate_trial_moves, :209-279 (every trial sees the pre-colour state)
-            for (uint64_t sp : space_indices) {
-                const auto& members = spaces[sp];
-                Sfc64 rng = make_rng(s->step, s->substep, s->seed, sp);
-                if (members.empty()) continue;  // EmptySpace: not counted (:299)
-                uint32_t pick = canon_range_u32(rng, (uint32_t)members.size());
-                uint64_t b = members[pick];
-                Trial t;
-                t.body = b;
-                for (int k = 0; k < 4; ++k) t.ori[k] = 0.0;
-                s->propose(rng, (int)move, maximum, b, t.pos, t.ori);
-                wrap(s->dim, s->L, t.pos);
-                if (point_to_space(cb, t.pos) != (int64_t)sp) {
-                    rej += 1;
-                    continue;
+            size_t m = space_indices.size();
+            trials.resize(m);
+            if (threads == 1 || m < 4 * (size_t)threads) {
+                generate(space_indices, 0, m);
+            } else {
+                std::vector<std::thread> pool;
+                size_t chunk = (m + threads - 1) / threads;
+                for (unsigned w = 0; w < threads; ++w) {
+                    size_t lo = std::min(m, w * chunk), hi = std::min(m, lo + chunk);
+                    pool.emplace_back(generate, std::cref(space_indices), lo, hi);
                 }
-                double dh = s->delta_energy_one(b, t.pos, t.ori);
-                bool ok = dh != INFINITY && (dh <= 0.0 || uniform01(rng) < std::exp(-dh / kt));
-                if (ok)
-                    accepted_trials.push_back(t);
-                else
-                    rej += 1;
+                for (auto& th : pool) th.join();
             }
             // update_bodies, :283-314
-            for (auto& t : accepted_trials) {
-                s->update_body(t.body, t.pos, ol ? t.ori : nullptr);
-                acc += 1;
+            for (auto& t : trials) {
+                if (t.outcome == 2) {
+                    s->update_body(t.body, t.pos, ol ? t.ori : nullptr);
+                    acc += 1;
+                } else if (t.outcome == 1) {
+                    rej += 1;
+                }
             }
         }
         s->substep += 1;
@@ -1238,6 +1260,16 @@ int oracle_parallel_sweep(oracle_system* s, uint32_t move, double maximum, doubl
     *accepted = acc;
     *rejected = rej;
     return 0;
+}
+
+int oracle_parallel_sweep(oracle_system* s, uint32_t move, double maximum, double kt, double range,
+                          uint64_t* accepted, uint64_t* rejected) {
+    return parallel_sweep_impl(s, move, maximum, kt, range, 1, accepted, rejected);
+}
+
+int oracle_parallel_sweep_threads(oracle_system* s, uint32_t move, double maximum, double kt, double range,
+                                  uint32_t threads, uint64_t* accepted, uint64_t* rejected) {
+    return parallel_sweep_impl(s, move, maximum, kt, range, threads, accepted, rejected);
 }
 
 int oracle_serial_sweep(oracle_system* s, uint32_t move, double maximum, double kt, uint64_t* accepted,

@@ -98,6 +98,11 @@ void oracle_increment_step(oracle_system* s);
 // ParallelSweep::apply (parallel_sweep.rs:390-421). Returns 0, or 1 on a checkerboard error.
 int oracle_parallel_sweep(oracle_system* s, uint32_t move, double maximum, double kt,
                           double body_interaction_range, uint64_t* accepted, uint64_t* rejected);
+// The same sweep with the trials of each colour pass split over `threads` host threads;
+// results are identical for every thread count.
+int oracle_parallel_sweep_threads(oracle_system* s, uint32_t move, double maximum, double kt,
+                                  double body_interaction_range, uint32_t threads, uint64_t* accepted,
+                                  uint64_t* rejected);
 // Sweep::apply (sweep.rs:159-224).
 int oracle_serial_sweep(oracle_system* s, uint32_t move, double maximum, double kt,
                         uint64_t* accepted, uint64_t* rejected);

@@ -41,8 +41,14 @@ def test_tune_reaches_target_and_sweep_api(ctx):
     micro = Microstate(ctx, Periodic(1.0, [L] * 3), pos, h, seed=5)
     sweep = ParallelSweep(1.0, Translate.with_maximum_distance(0.13))
     sweep.tune_with_options(micro, h, Isothermal(1.0), TuneOptions(target_acceptance=0.3, samples=8000, steps=32))
+    tuned = sweep.local_trial.maximum_distance
+    # one more tuning round at the tuned size: its scale factor (r + 1.5) / (t + 1.5) gives the
+    # single-body acceptance r the tuner measures (tune_local.rs samples bodies one at a time)
+    r = micro.tune(TRANSLATE, tuned, 1.0, FP64, 0.3, 20000, 1) / tuned * 1.8 - 1.5
+    assert abs(r - 0.3) < 0.02
+    # the checkerboard sweep also rejects moves that leave their space, so its ratio is lower
     c = sweep.apply(micro, h, Isothermal(1.0))
-    assert abs(c.acceptance_ratio() - 0.3) < 0.05
+    assert 0.2 < c.acceptance_ratio() < 0.3
 
 
 def test_tune_cube_rotation_matches_oracle(ctx):
