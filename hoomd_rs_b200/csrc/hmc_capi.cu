@@ -84,8 +84,7 @@ struct hmc_system {
     unsigned long long* first_bad = nullptr;       // device word for the finiteness check
     unsigned long long* host_first_bad = nullptr;  // pinned mirror
     std::vector<void*> allocations;
-    uint32_t tile_cap[2] = {0, 0};  // staged bodies per block of the tiled pass: [fp64, fp32]
-    bool coop = false;              // warp-cooperative hard-sphere pass
+    bool coop[2] = {true, false};  // warp-cooperative hard-sphere pass: [fp64, fp32]
     // convex polyhedron
     double4* verts = nullptr;
     uint32_t n_vertices = 0;
@@ -134,6 +133,12 @@ void sphere_bound(hmc_system* s) {
     double b32 = 2.0 * E * rd * dmax + s->dim * E * E + s->dim * u32 * dmax * dmax;
     double b64 = 6.0 * u64 * (Lmax + wmax) * rd * dmax + s->dim * u64 * dmax * dmax;
     double B = 2.0 * (b32 + b64);
+    // HMC_B200_FP32_BAND_SCALE (>= 1) widens the band of FP32 distances that are decided in
+    // FP64. Decisions do not change; it makes the recheck path common enough to test.
+    if (const char* e = std::getenv("HMC_B200_FP32_BAND_SCALE")) {
+        double f = std::atof(e);
+        if (f > 1.0 && f < 1e12) B *= f;
+    }
     s->pair.sig2_lo32 = std::nextafter((float)(sigma2 - B), -INFINITY);
     s->pair.sig2_hi32 = std::nextafter((float)(sigma2 + B), INFINITY);
 }
@@ -409,21 +414,12 @@ hmc_status hmc_system_create(hmc_context* ctx, const hmc_system_desc* d, const d
     } else {
         lj_setup(s, d->lj_epsilon, d->lj_sigma, d->lj_r_cut, d->lj_r_shift);
     }
-    // Shared-memory staging capacity: 1.5x the mean body count of a 9 x 9 x 17 region plus
-    // slack, within 100 KB per block; a denser system keeps the global-memory pass.
-    // The direct (global-memory) pass measured faster than the shared-memory tiled pass on
-    // B200 for hard spheres; HMC_B200_SWEEP_KERNEL=tiled selects the tiled pass instead.
-    const char* kern = std::getenv("HMC_B200_SWEEP_KERNEL");
-    const bool tiled = kern && std::strcmp(kern, "tiled") == 0;
-    s->coop = kern && std::strcmp(kern, "coop") == 0;
-    if (tiled && tile_kernel_applies(s->dim, s->geom)) {
-        double mean = 9.0 * 9.0 * 17.0 * (double)s->n / (double)cells;
-        uint32_t want = (uint32_t)(1.5 * mean + 64.0);
-        for (int f = 0; f < 2; ++f) {
-            uint32_t cap = want;
-            while (cap > 64 && tile_smem_bytes(f == 1, cap) > 100u * 1024u) cap -= 32;
-            s->tile_cap[f] = cap >= want ? cap : 0u;
-        }
+    // The hard-sphere colour pass: per lane for FP32 (cheap pair tests), warp-cooperative for
+    // FP64 (each pair test costs more than the coordination), as measured on B200;
+    // HMC_B200_SWEEP_KERNEL=direct or =coop forces one of them for both precisions.
+    if (const char* kern = std::getenv("HMC_B200_SWEEP_KERNEL")) {
+        if (std::strcmp(kern, "direct") == 0) s->coop[0] = s->coop[1] = false;
+        if (std::strcmp(kern, "coop") == 0) s->coop[0] = s->coop[1] = true;
     }
 
     cudaError_t e = cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking);
@@ -617,7 +613,7 @@ hmc_status hmc_sweep(hmc_system* s, const hmc_sweep_params* p, hmc_count* out) {
                     HMC_CUDA(launch_sweep_poly(fp32, s->geom, s->arr, s->verts, s->n_vertices, s->poly_rcut2,
                                                s->poly_rcut2_hi32, L, p->move == HMC_ROTATE, s->stream));
                 else
-                    HMC_CUDA(launch_sweep_sphere(s->dim, fp32, s->geom, s->arr, s->pair, L, s->tile_cap[fp32], s->coop, s->stream));
+                    HMC_CUDA(launch_sweep_sphere(s->dim, fp32, s->geom, s->arr, s->pair, L, s->coop[fp32], s->stream));
                 s->prof.kernel_launches += 1;
             }
             s->substep += 1;  // increment_substep after every full colour set

@@ -102,14 +102,9 @@ struct Launch {
 // write_s: also store the FP64 site positions S = wrap(B) in cell order (needed by the
 // plain FP64 pair test, the overlap check and injected-move evaluation).
 cudaError_t launch_rebuild(int dim, const Geometry& g, const Arrays& a, uint32_t n, bool write_s, cudaStream_t s);
-// tile_cap > 0 selects the shared-memory tiled pass (3-D, at least 9 x 9 x 17 spaces) with room
-// for tile_cap staged bodies per block; a block whose region holds more falls back to
-// global-memory neighbour reads.
 // coop selects the warp-cooperative pass (the per-lane pass otherwise).
 cudaError_t launch_sweep_sphere(int dim, bool fp32, const Geometry& g, const Arrays& a, const Pair& p,
-                                const Launch& l, uint32_t tile_cap, bool coop, cudaStream_t s);
-size_t tile_smem_bytes(bool fp32, uint32_t cap);
-bool tile_kernel_applies(int dim, const Geometry& g);
+                                const Launch& l, bool coop, cudaStream_t s);
 cudaError_t launch_overlap_sphere(int dim, const Geometry& g, const Arrays& a, const Pair& p, uint32_t n,
                                   cudaStream_t s);
 cudaError_t launch_sweep_lj(int dim, bool fp32, const Geometry& g, const Arrays& a, const Pair& p, const Launch& l,

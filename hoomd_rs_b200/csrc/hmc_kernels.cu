@@ -226,7 +226,7 @@ __global__ void __launch_bounds__(128, HMC_SWEEP_MIN_BLOCKS) k_sweep_sphere(Geom
 // length is the longest row of any lane. A decision is the OR over its candidates, so the
 // order of the tests cannot change it.
 #ifndef HMC_COOP_OWN_STEPS
-#define HMC_COOP_OWN_STEPS 1
+#define HMC_COOP_OWN_STEPS 2
 #endif
 constexpr uint32_t kOwnSteps = HMC_COOP_OWN_STEPS;
 constexpr int kFlagOverlap = 1, kFlagUncertain = 2, kFlagMore = 4;
@@ -410,213 +410,6 @@ __global__ void __launch_bounds__(128, HMC_SWEEP_MIN_BLOCKS) k_sweep_sphere_coop
         if (!FP32) A.sorted_s[k] = make_double4(sv[0], sv[1], sv[2], 0.0);
         A.sorted_off[k] = cell_offsets<DIM>(g, sv, m);
         A.body_pos[A.sorted_body[k]] = make_double4(t[0], t[1], t[2], 0.0);
-    }
-    flush_stats(A.stats, st, n_accepted);
-}
-
-// ---- the colour pass, staged through shared memory (3-D) ------------------------------------
-// A block owns a tile of TX x TY x TZ spaces of the colour (every second space per axis).
-// The union of their stencils is a region of (2TX+1) x (2TY+1) x (2TZ+1) spaces; the block
-// copies the bodies of the whole region into shared memory with cp.async while the threads
-// compute their FP64 trial moves, then tests every candidate pair from shared memory. Only
-// spaces of other colours lie in the region apart from the tile's own, so the staged
-// neighbours are never modified during the pass.
-constexpr int kTX = 4, kTY = 4, kTZ = 8, kTT = kTX * kTY * kTZ;
-constexpr int kRX = 2 * kTX + 1, kRY = 2 * kTY + 1, kRZ = 2 * kTZ + 1, kRC = kRX * kRY * kRZ;
-constexpr int kChunk = (kRC + kTT - 1) / kTT;
-
-template <int NT, typename T>
-__device__ __forceinline__ T block_scan_exclusive(T v, T* total, T* warp_sums) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    T x = v;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        T y = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= o) x += y;
-    }
-    if (lane == 31) warp_sums[warp] = x;
-    __syncthreads();
-    if (warp == 0) {
-        T w = lane < NT / 32 ? warp_sums[lane] : T(0);
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            T y = __shfl_up_sync(0xffffffffu, w, o);
-            if (lane >= o) w += y;
-        }
-        if (lane < NT / 32) warp_sums[lane] = w;
-    }
-    __syncthreads();
-    T prefix = warp > 0 ? warp_sums[warp - 1] : T(0);
-    *total = warp_sums[NT / 32 - 1];
-    return prefix + x - v;
-}
-
-__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
-    uint32_t d = (uint32_t)__cvta_generic_to_shared(smem_dst);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gsrc) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
-
-template <bool FP32>
-__global__ void __launch_bounds__(kTT) k_sweep_tile3(Geometry g, Arrays A, Pair P, Launch L, uint32_t cap) {
-    using Elem = typename std::conditional<FP32, float4, double4>::type;
-    extern __shared__ __align__(16) unsigned char smem[];
-    Elem* s_pos = reinterpret_cast<Elem*>(smem);
-    uint32_t* s_gstart = reinterpret_cast<uint32_t*>(smem + (size_t)cap * sizeof(Elem));
-    uint32_t* s_lstart = s_gstart + kRC;  // kRC + 1 entries
-    __shared__ uint32_t s_warp[kTT / 32];
-
-    const uint32_t tid = threadIdx.x;
-    const uint32_t sx = g.shape[0], sy = g.shape[1], sz = g.shape[2];
-    const int px = (L.color >> 2) & 1, py = (L.color >> 1) & 1, pz = L.color & 1;
-    const int hx0 = blockIdx.z * kTX, hy0 = blockIdx.y * kTY, hz0 = blockIdx.x * kTZ;
-    const int x0 = 2 * hx0 + px - 1, y0 = 2 * hy0 + py - 1, z0 = 2 * hz0 + pz - 1;
-    const uint32_t* __restrict__ cs = A.cell_start;
-
-    // 1. ranges of the region's spaces: each thread owns kChunk consecutive region spaces
-    uint32_t gs[kChunk], cnt[kChunk];
-    uint32_t sum = 0;
-#pragma unroll
-    for (int j = 0; j < kChunk; ++j) {
-        const int rc = (int)tid * kChunk + j;
-        uint32_t c0 = 0, c1 = 0;
-        if (rc < kRC) {
-            const int rz = rc % kRZ, rxy = rc / kRZ, ry = rxy % kRY, rx = rxy / kRY;
-            const uint32_t c = (wrap_index(x0 + rx, sx) * sy + wrap_index(y0 + ry, sy)) * sz + wrap_index(z0 + rz, sz);
-            c0 = __ldg(cs + c);
-            c1 = __ldg(cs + c + 1);
-        }
-        gs[j] = c0;
-        cnt[j] = c1 - c0;
-        sum += cnt[j];
-    }
-    uint32_t total;
-    uint32_t run = block_scan_exclusive<kTT>(sum, &total, s_warp);
-    const bool staged = total <= cap;
-#pragma unroll
-    for (int j = 0; j < kChunk; ++j) {
-        const int rc = (int)tid * kChunk + j;
-        if (rc < kRC) {
-            s_gstart[rc] = gs[j];
-            s_lstart[rc] = run;
-        }
-        if (staged) {
-            const Elem* src = FP32 ? reinterpret_cast<const Elem*>(A.sorted_off) : reinterpret_cast<const Elem*>(A.sorted_s);
-            for (uint32_t b = 0; b < cnt[j]; ++b) {
-                if constexpr (FP32) {
-                    cp_async16(s_pos + run + b, src + gs[j] + b);
-                } else {
-                    cp_async16(reinterpret_cast<char*>(s_pos + run + b), src + gs[j] + b);
-                    cp_async16(reinterpret_cast<char*>(s_pos + run + b) + 16,
-                               reinterpret_cast<const char*>(src + gs[j] + b) + 16);
-                }
-            }
-        }
-        run += cnt[j];
-    }
-    cp_async_commit();
-    if (tid == kTT - 1) s_lstart[kRC] = total;
-    __syncthreads();
-
-    // 2. the trial move of this thread's space, while the copies are in flight
-    const int tx = (int)tid / (kTY * kTZ), ty = ((int)tid / kTZ) % kTY, tz = (int)tid % kTZ;
-    const bool valid = hx0 + tx < (int)g.half_shape[0] && hy0 + ty < (int)g.half_shape[1] &&
-                       hz0 + tz < (int)g.half_shape[2];
-    const int ro = ((2 * tx + 1) * kRY + (2 * ty + 1)) * kRZ + (2 * tz + 1);
-    const uint32_t own_count = valid ? s_lstart[ro + 1] - s_lstart[ro] : 0u;
-    uint32_t m[3] = {(uint32_t)(2 * (hx0 + tx) + px), (uint32_t)(2 * (hy0 + ty) + py), (uint32_t)(2 * (hz0 + tz) + pz)};
-    bool trial = false;
-    uint32_t pick = 0, k = 0;
-    double t[3] = {0.0, 0.0, 0.0};
-    float4 t32 = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (own_count > 0) {
-        const uint32_t cell = (m[0] * sy + m[1]) * sz + m[2];
-        Sfc64 rng = make_rng(L.step, L.substep, L.seed, (uint64_t)cell);
-        pick = canon_range_u32(rng, own_count);
-        k = s_gstart[ro] + pick;
-        double4 b4 = A.sorted_b[k];
-        double x[3] = {b4.x, b4.y, b4.z};
-        double dv[3];
-        ball_sample<3>(rng, L.max_move, A.zig_x, A.zig_f, dv);
-#pragma unroll
-        for (int a = 0; a < 3; ++a) x[a] = dadd(x[a], dv[a]);
-        wrap_inv<3>(g.L, g.invL, x);
-        uint32_t mt[3];
-        trial = point_to_space<3>(g, x, mt) && mt[0] == m[0] && mt[1] == m[1] && mt[2] == m[2];
-        if (trial) {
-            t[0] = x[0];
-            t[1] = x[1];
-            t[2] = x[2];
-            wrap_inv<3>(g.L, g.invL, t);
-            if (FP32) t32 = cell_offsets<3>(g, t, m);
-        }
-    }
-    cp_async_wait_all();
-    __syncthreads();
-
-    // 3. pair tests from shared memory
-    PairStats st;
-    uint32_t n_accepted = 0;
-    if (trial) {
-        int res = kClear;
-        if (!staged) {
-            res = kUncertain;
-        } else {
-            const uint32_t self = s_lstart[ro] + pick;
-            const int mz = (int)m[2];
-            bool uncertain = false;
-#pragma unroll
-            for (int r = 0; r < 9 && res == kClear; ++r) {
-                const int dx = r / 3 - 1, dy = r % 3 - 1;
-                const int rc = ((2 * tx + 1 + dx) * kRY + (2 * ty + 1 + dy)) * kRZ + 2 * tz;
-                const uint32_t lb = s_lstart[rc], le = s_lstart[rc + 3];
-                const float s0 = (float)dx * g.w32[0], s1 = (float)dy * g.w32[1];
-                for (uint32_t q = lb; q < le; ++q) {
-                    if (q == self) continue;
-                    if constexpr (FP32) {
-                        const float4 v = s_pos[q];
-                        int dm = __float_as_int(v.w) - mz;
-                        if (dm > 1)
-                            dm -= (int)sz;
-                        else if (dm < -1)
-                            dm += (int)sz;
-                        const float dd = fp32_dist2<3>(g, t32, v, s0, s1, dm);
-                        st.checks++;
-                        if (dd < P.sig2_lo32) {
-                            res = kOverlap;
-                            break;
-                        }
-                        uncertain |= dd < P.sig2_hi32;
-                    } else {
-                        const double4 v = reinterpret_cast<const double4*>(s_pos)[q];
-                        double sv[3] = {v.x, v.y, v.z};
-                        st.checks++;
-                        if (ref_dist2<3>(g, t, sv) < P.sigma2) {
-                            res = kOverlap;
-                            break;
-                        }
-                    }
-                }
-            }
-            if (res == kClear && uncertain) res = kUncertain;
-        }
-        if (res == kUncertain) {
-            PairStats st2;
-            res = sphere_overlaps_generic<3, FP32>(g, A, P, t, t32, m, k, st2) ? kOverlap : kClear;
-            st.rechecks += st2.rechecks;
-            st.max_err = st2.max_err > st.max_err ? st2.max_err : st.max_err;
-            if (!staged) st.checks += st2.checks;
-        }
-        if (res == kClear) {
-            n_accepted = 1;
-            double sv[3] = {t[0], t[1], t[2]};
-            wrap_inv<3>(g.L, g.invL, sv);
-            A.sorted_b[k] = make_double4(t[0], t[1], t[2], 0.0);
-            if (!FP32) A.sorted_s[k] = make_double4(sv[0], sv[1], sv[2], 0.0);
-            A.sorted_off[k] = cell_offsets<3>(g, sv, m);
-            A.body_pos[A.sorted_body[k]] = make_double4(t[0], t[1], t[2], 0.0);
-        }
     }
     flush_stats(A.stats, st, n_accepted);
 }
@@ -1044,16 +837,8 @@ cudaError_t launch_rebuild(int dim, const Geometry& g, const Arrays& a, uint32_t
     return cudaGetLastError();
 }
 
-size_t tile_smem_bytes(bool fp32, uint32_t cap) {
-    return (size_t)cap * (fp32 ? sizeof(float4) : sizeof(double4)) + sizeof(uint32_t) * (2 * kRC + 1);
-}
-
-bool tile_kernel_applies(int dim, const Geometry& g) {
-    return dim == 3 && g.shape[0] >= (uint32_t)kRX && g.shape[1] >= (uint32_t)kRY && g.shape[2] >= (uint32_t)kRZ;
-}
-
 cudaError_t launch_sweep_sphere(int dim, bool fp32, const Geometry& g, const Arrays& a, const Pair& p,
-                                const Launch& l, uint32_t tile_cap, bool coop, cudaStream_t s) {
+                                const Launch& l, bool coop, cudaStream_t s) {
     if (l.n_active == 0) return cudaSuccess;  // no non-empty space of this colour
     if (coop) {
         static int coop_blocks[2][2] = {{0, 0}, {0, 0}};
@@ -1085,25 +870,6 @@ cudaError_t launch_sweep_sphere(int dim, bool fp32, const Geometry& g, const Arr
             else
                 k_sweep_sphere_coop<3, false><<<grid, 128, 0, s>>>(g, a, p, l);
         }
-        return cudaGetLastError();
-    }
-    if (tile_cap > 0 && tile_kernel_applies(dim, g)) {
-        dim3 grid((g.half_shape[2] + kTZ - 1) / kTZ, (g.half_shape[1] + kTY - 1) / kTY,
-                  (g.half_shape[0] + kTX - 1) / kTX);
-        size_t smem = tile_smem_bytes(fp32, tile_cap);
-        static size_t smem_set[2] = {0, 0};
-        if (smem > smem_set[fp32]) {
-            cudaError_t e = fp32 ? cudaFuncSetAttribute(k_sweep_tile3<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                        (int)smem)
-                                 : cudaFuncSetAttribute(k_sweep_tile3<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                        (int)smem);
-            if (e != cudaSuccess) return e;
-            smem_set[fp32] = smem;
-        }
-        if (fp32)
-            k_sweep_tile3<true><<<grid, kTT, smem, s>>>(g, a, p, l, tile_cap);
-        else
-            k_sweep_tile3<false><<<grid, kTT, smem, s>>>(g, a, p, l, tile_cap);
         return cudaGetLastError();
     }
     // Grid-stride over the colour's list with at most one resident wave of blocks.

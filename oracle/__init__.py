@@ -20,6 +20,7 @@ HARD_SPHERE = 0
 HARD_CONVEX_POLYGON = 1
 HARD_CONVEX_POLYHEDRON = 2
 LENNARD_JONES = 3
+HARD_CONVEX_SURFACE_MESH_2D = 4
 TRANSLATE = 0
 ROTATE = 1
 
@@ -70,6 +71,9 @@ def lib():
         L.oracle_checkerboard_for_counter.restype = C.c_int
         L.oracle_convex_intersects_at_3d.argtypes = [_dp, C.c_uint32, _dp, C.c_uint32, _dp, _dp]
         L.oracle_convex_intersects_at_2d.argtypes = [_dp, C.c_uint32, _dp, C.c_uint32, _dp, C.c_double]
+        L.oracle_surface_mesh_intersects_at_2d.argtypes = [_dp, C.c_uint32, _dp, C.c_uint32, _dp, C.c_double]
+        L.oracle_cr_sincos.argtypes = [C.c_double, _dp, _dp]
+        L.oracle_cr_sincos.restype = C.c_int
         L.oracle_convex_intersects_at_global_3d.argtypes = [_dp, C.c_uint32, _dp, _dp, _dp, _dp]
         L.oracle_versor_from_axis_angle.argtypes = [_dp, C.c_double, _dp]
         L.oracle_versor_combine.argtypes = [_dp, _dp, _dp]
@@ -228,6 +232,22 @@ def convex_intersects_at_2d(verts_a, verts_b, v_ij, theta) -> bool:
     b = _f64(verts_b)
     v = _f64(v_ij)
     return bool(lib().oracle_convex_intersects_at_2d(_d(a), a.shape[0], _d(b), b.shape[0], _d(v), theta))
+
+
+def surface_mesh_intersects_at_2d(verts_a, verts_b, v_ij, theta) -> bool:
+    a = _f64(verts_a, (-1, 2))
+    b = _f64(verts_b, (-1, 2))
+    v = _f64(v_ij)
+    return bool(lib().oracle_surface_mesh_intersects_at_2d(_d(a), a.shape[0], _d(b), b.shape[0], _d(v), theta))
+
+
+def cr_sincos(x: float):
+    """Correctly rounded (sin x, cos x); raises for |x| >= 2^20."""
+    s = C.c_double()
+    c = C.c_double()
+    if lib().oracle_cr_sincos(x, C.byref(s), C.byref(c)):
+        raise ValueError("|x| >= 2^20")
+    return s.value, c.value
 
 
 def versor_from_axis_angle(axis, angle):

@@ -216,6 +216,148 @@ void portable_sincos(double h, double* s, double* c) {
     *c = pc;
 }
 
+// ---- correctly rounded sin and cos ----------------------------------------------
+// The reference turns an Angle into a rotation with f64::sin / f64::cos (hoomd-vector
+// angle.rs:120-150), i.e. the platform libm. The oracle and the device both use this
+// deterministic method instead, which returns the correctly rounded values (what an exact
+// libm returns) built only from correctly rounded +, -, *, fma:
+//  * Cody-Waite reduction x = k pi/2 + r with pi/2 split into 33+33+33+53 bits (about 160
+//    bits, the products k*C1..k*C3 exact for |k| < 2^20), r kept as a double-double;
+//  * Taylor series of sin r and cos r, |r| <= pi/4: the leading terms in double-double,
+//    the rest in double (relative error below 2^-66), then Ziv's rounding test against a
+//    2^-62 bound; if the rounding is not decided, the whole series in double-double
+//    (error below 2^-95) decides it. Ambiguous after that only when the exact value lies
+//    within 2^-95 of a rounding boundary, where the double-double result is returned.
+// Inputs with |x| >= 2^20 are outside the supported range (return 1).
+struct DD {
+    double h, l;
+};
+static inline DD dd_two_sum(double a, double b) {
+    double s = a + b;
+    double bb = s - a;
+    return {s, (a - (s - bb)) + (b - bb)};
+}
+static inline DD dd_fast(double a, double b) {  // |a| >= |b|
+    double s = a + b;
+    return {s, b - (s - a)};
+}
+static inline DD dd_mul(DD a, DD b) {
+    double p = a.h * b.h;
+    double e = std::fma(a.h, b.h, -p);
+    e = std::fma(a.h, b.l, e);
+    e = std::fma(a.l, b.h, e);
+    return dd_fast(p, e);
+}
+static inline DD dd_add(DD a, DD b) {
+    DD s = dd_two_sum(a.h, b.h);
+    return dd_fast(s.h, s.l + (a.l + b.l));
+}
+// (-1)^(k/2) / k! as double-doubles, k = 2..27 (exact rationals rounded twice).
+static const double kInvFact[26][2] = {
+    {-0x1.0000000000000p-1, 0x0.0p+0},
+    {-0x1.5555555555555p-3, -0x1.5555555555555p-57},
+    {0x1.5555555555555p-5, 0x1.5555555555555p-59},
+    {0x1.1111111111111p-7, 0x1.1111111111111p-63},
+    {-0x1.6c16c16c16c17p-10, 0x1.f49f49f49f49fp-65},
+    {-0x1.a01a01a01a01ap-13, -0x1.a01a01a01a01ap-73},
+    {0x1.a01a01a01a01ap-16, 0x1.a01a01a01a01ap-76},
+    {0x1.71de3a556c734p-19, -0x1.c154f8ddc6c00p-73},
+    {-0x1.27e4fb7789f5cp-22, -0x1.cbbc05b4fa99ap-76},
+    {-0x1.ae64567f544e4p-26, 0x1.c062e06d1f209p-80},
+    {0x1.1eed8eff8d898p-29, -0x1.2aec959e14c06p-83},
+    {0x1.6124613a86d09p-33, 0x1.f28e0cc748ebep-87},
+    {-0x1.93974a8c07c9dp-37, -0x1.05d6f8a2efd1fp-92},
+    {-0x1.ae7f3e733b81fp-41, -0x1.1d8656b0ee8cbp-97},
+    {0x1.ae7f3e733b81fp-45, 0x1.1d8656b0ee8cbp-101},
+    {0x1.952c77030ad4ap-49, 0x1.ac981465ddc6cp-103},
+    {-0x1.6827863b97d97p-53, -0x1.eec01221a8b0bp-107},
+    {-0x1.2f49b46814157p-57, -0x1.2650f61dbdcb4p-112},
+    {0x1.e542ba4020225p-62, 0x1.ea72b4afe3c2fp-120},
+    {0x1.71b8ef6dcf572p-66, -0x1.d043ae40c4647p-120},
+    {-0x1.0ce396db7f853p-70, 0x1.aebcdbd20331cp-124},
+    {-0x1.761b41316381ap-75, 0x1.3423c7d91404fp-130},
+    {0x1.f2cf01972f578p-80, -0x1.9ada5fcc1ab14p-135},
+    {0x1.3f3ccdd165fa9p-84, -0x1.58ddadf344487p-139},
+    {-0x1.88e85fc6a4e5ap-89, 0x1.71c37ebd16540p-143},
+    {-0x1.d1ab1c2dccea3p-94, -0x1.054d0c78aea14p-149}};
+static inline DD inv_fact(int k) { return {kInvFact[k - 2][0], kInvFact[k - 2][1]}; }
+
+// sum_{j>=0} c_{first+2j} z^j with the first n_dd coefficients in double-double and the
+// rest (up to k = 27) in double.
+static DD series(int first, DD z, int n_dd) {
+    int last = first;
+    while (last + 2 <= 27) last += 2;
+    int split = first + 2 * n_dd;  // first coefficient evaluated in double
+    double t = 0.0;
+    for (int k = last; k >= split; k -= 2) t = std::fma(t, z.h, kInvFact[k - 2][0]);
+    DD p{t, 0.0};
+    if (split <= last) p = dd_mul(p, z);
+    for (int k = split - 2; k >= first; k -= 2) {
+        p = dd_add(inv_fact(k), p);
+        if (k > first) p = dd_mul(p, z);
+    }
+    return p;
+}
+static inline double next_up(double x) {
+    uint64_t b = double_to_bits(x);
+    if (x == 0.0) return 4.9406564584124654e-324;
+    return bits_to_double(x > 0 ? b + 1 : b - 1);
+}
+static inline double next_down(double x) { return -next_up(-x); }
+// Ziv's test: the exact value lies within err of h + l; returns true when it rounds to h.
+static inline bool rounds_to_h(DD v, double err) {
+    double up = (next_up(v.h) - v.h) * 0.5, down = (v.h - next_down(v.h)) * 0.5;
+    return v.l + err < up && v.l - err > -down;
+}
+// sin r and cos r for r = rh + rl, |r| <= pi/4 (slightly above, after reduction).
+static void sincos_reduced(DD r, int tier2, DD* s, DD* c) {
+    DD z = dd_mul(r, r);
+    int n = tier2 ? 13 : 3;
+    DD ps = series(3, z, n);  // -1/6 + z/120 - ...
+    DD pc = series(2, z, n);  // -1/2 + z/24 - ...
+    *s = dd_add(r, dd_mul(dd_mul(r, z), ps));
+    *c = dd_add(DD{1.0, 0.0}, dd_mul(z, pc));
+}
+int cr_sincos(double x, double* sn, double* cs) {
+    if (!std::isfinite(x)) {
+        *sn = *cs = x - x;
+        return 0;
+    }
+    double ax = std::fabs(x);
+    if (ax < 0x1p-27) {
+        *sn = x;
+        *cs = 1.0;
+        return 0;
+    }
+    if (ax >= 0x1p20) {
+        *sn = *cs = NAN;
+        return 1;
+    }
+    double k = std::nearbyint(x * 0x1.45f306dc9c883p-1);
+    DD r{x, 0.0};
+    if (k != 0.0) {
+        double t = x - k * 0x1.921fb54400000p+0;  // exact
+        r = dd_two_sum(t, -(k * 0x1.0b4611a600000p-34));
+        r = dd_add(r, DD{-(k * 0x1.3198a2e000000p-69), 0.0});
+        double p = k * 0x1.b839a252049c1p-104;
+        r = dd_add(r, DD{-p, -std::fma(k, 0x1.b839a252049c1p-104, -p)});
+    }
+    int q = (int)(((long long)k) & 3);
+    DD s, c;
+    sincos_reduced(r, 0, &s, &c);
+    const double tol1 = 0x1p-62;
+    if (!rounds_to_h(s, tol1 * std::fabs(s.h)) || !rounds_to_h(c, tol1 * std::fabs(c.h)))
+        sincos_reduced(r, 1, &s, &c);
+    double sv = s.h, cv = c.h;
+    switch (q) {
+        case 0: *sn = sv; *cs = cv; break;
+        case 1: *sn = cv; *cs = -sv; break;
+        case 2: *sn = -sv; *cs = -cv; break;
+        default: *sn = -cv; *cs = sv; break;
+    }
+    return 0;
+}
+
 // ============================================================================
 // hoomd-vector arithmetic with the reference's rounding
 // ============================================================================
@@ -519,7 +661,8 @@ bool collide2d(const Polytope& a, const Polytope& b, const double* vij, const do
 
 // Angle -> RotationMatrix<2>, angle.rs:130-138.
 void mat2_from_angle(double theta, double (&m)[2][2]) {
-    double s = std::sin(theta), c = std::cos(theta);
+    double s, c;
+    cr_sincos(theta, &s, &c);
     m[0][0] = c;
     m[0][1] = -s;
     m[1][0] = s;
@@ -544,12 +687,64 @@ bool convex_global_2d(const Polytope& p, const double* ri, double ti, const doub
     if (distance_squared(ri, rj, 2) >= rcut * rcut) return false;
     double rab[2] = {rj[0] - ri[0], rj[1] - ri[1]};
     double inv = -ti;
-    double s = std::sin(inv), c = std::cos(inv);
+    double s, c;
+    cr_sincos(inv, &s, &c);
     double vij[2] = {rab[0] * c - rab[1] * s, rab[0] * s + rab[1] * c};
     double oij = inv + tj;
     double m[2][2];
     mat2_from_angle(oij, m);
     return collide2d(p, p, vij, m);
+}
+
+// ConvexSurfaceMesh2d separating-axis test (convex_surface_mesh_2d.rs:578-640): a and b
+// hold counter-clockwise hull vertices; o_b rotates b into a's frame.
+static void mat2_rotate(const double (&m)[2][2], const double* v, double* out) {  // rows dot v
+    out[0] = dot(m[0], v, 2);
+    out[1] = dot(m[1], v, 2);
+}
+// is_separating, :625-640: every vertex of a strictly outside the plane (p, n).
+static bool is_separating(const Polytope& a, const double* p, const double* n) {
+    double n_dot_p = dot(n, p, 2);
+    for (int i = 0; i < a.nv; ++i)
+        if (dot(n, &a.verts[2 * i], 2) - n_dot_p <= 0.0) return false;
+    return true;
+}
+// b_edge_separates, :597-623.
+static bool b_edge_separates(const Polytope& a, const Polytope& b, const double* v_ab, const double (&o_b)[2][2]) {
+    int previous = b.nv - 1;
+    for (int current = 0; current < b.nv; ++current) {
+        const double* p = &b.verts[2 * current];
+        double edge[2] = {p[0] - b.verts[2 * previous], p[1] - b.verts[2 * previous + 1]};
+        double n[2] = {edge[1], -edge[0]};  // -edge.perpendicular(), perpendicular = (-y, x)
+        double pa[2], na[2];
+        mat2_rotate(o_b, p, pa);
+        pa[0] = pa[0] + v_ab[0];
+        pa[1] = pa[1] + v_ab[1];
+        mat2_rotate(o_b, n, na);
+        if (is_separating(a, pa, na)) return true;
+        previous = current;
+    }
+    return false;
+}
+bool sat_intersects_at(const Polytope& a, const Polytope& b, const double* v_ij, const double (&o_j)[2][2]) {
+    if (b_edge_separates(a, b, v_ij, o_j)) return false;
+    double inv[2][2] = {{o_j[0][0], o_j[1][0]}, {o_j[0][1], o_j[1][1]}};
+    double mv[2] = {-v_ij[0], -v_ij[1]}, v_ji[2];
+    mat2_rotate(inv, mv, v_ji);
+    return !b_edge_separates(b, a, v_ji, inv);
+}
+// IntersectsAtGlobal for ConvexSurfaceMesh2d, :514-536.
+bool sat_global_2d(const Polytope& p, const double* ri, double ti, const double* rj, double tj) {
+    double rcut = p.bounding_radius + p.bounding_radius;
+    if (distance_squared(ri, rj, 2) >= rcut * rcut) return false;
+    double rab[2] = {rj[0] - ri[0], rj[1] - ri[1]};
+    double inv = -ti;
+    double s, c;
+    cr_sincos(inv, &s, &c);
+    double vij[2] = {rab[0] * c - rab[1] * s, rab[0] * s + rab[1] * c};
+    double m[2][2];
+    mat2_from_angle(inv + tj, m);
+    return sat_intersects_at(p, p, vij, m);
 }
 
 // ============================================================================
@@ -807,7 +1002,8 @@ struct oracle_system {
 
     bool hard() const { return interaction != ORACLE_LENNARD_JONES; }
     bool oriented() const {
-        return interaction == ORACLE_HARD_CONVEX_POLYGON || interaction == ORACLE_HARD_CONVEX_POLYHEDRON;
+        return interaction == ORACLE_HARD_CONVEX_POLYGON || interaction == ORACLE_HARD_CONVEX_POLYHEDRON ||
+               interaction == ORACLE_HARD_CONVEX_SURFACE_MESH_2D;
     }
 
     void build_grid() {
@@ -887,6 +1083,8 @@ struct oracle_system {
             }
             case ORACLE_HARD_CONVEX_POLYGON:
                 return convex_global_2d(poly, x, o[0], y, orient[j]) ? INFINITY : 0.0;
+            case ORACLE_HARD_CONVEX_SURFACE_MESH_2D:
+                return sat_global_2d(poly, x, o[0], y, orient[j]) ? INFINITY : 0.0;
             default:
                 return shifted_lj_pair(eps, sigma, rcut, rshift, distance_squared(x, y, dim));
         }
@@ -1007,6 +1205,7 @@ uint32_t oracle_counter_choose(uint64_t step, uint32_t substep, uint32_t seed, u
 }
 double oracle_cbrt(double x) { return portable_cbrt(x); }
 void oracle_sincos_half(double theta, double* s, double* c) { portable_sincos(theta, s, c); }
+int oracle_cr_sincos(double x, double* s, double* c) { return cr_sincos(x, s, c); }
 void oracle_ziggurat_tables(double* x_out, double* f_out) {
     for (int i = 0; i <= ZIG_LAYERS; ++i) {
         x_out[i] = zig().x[i];
@@ -1082,6 +1281,13 @@ int oracle_convex_intersects_at_2d(const double* va, uint32_t na, const double* 
     mat2_from_angle(theta, m);
     return collide2d(a, b, vij, m) ? 1 : 0;
 }
+int oracle_surface_mesh_intersects_at_2d(const double* va, uint32_t na, const double* vb, uint32_t nb,
+                                         const double* vij, double theta) {
+    Polytope a = make_poly(va, na, 2), b = make_poly(vb, nb, 2);
+    double m[2][2];
+    mat2_from_angle(theta, m);
+    return sat_intersects_at(a, b, vij, m) ? 1 : 0;
+}
 int oracle_convex_intersects_at_global_3d(const double* verts, uint32_t nv, const double* ri, const double* qi,
                                           const double* rj, const double* qj) {
     Polytope p = make_poly(verts, nv, 3);
@@ -1130,7 +1336,8 @@ oracle_system* oracle_system_create(uint32_t dim, const double* L, uint64_t n, c
     s->rcut = rcut;
     s->rshift = rshift;
     s->boundary_range = boundary_range;
-    if (interaction == ORACLE_HARD_CONVEX_POLYGON || interaction == ORACLE_HARD_CONVEX_POLYHEDRON)
+    if (interaction == ORACLE_HARD_CONVEX_POLYGON || interaction == ORACLE_HARD_CONVEX_POLYHEDRON ||
+        interaction == ORACLE_HARD_CONVEX_SURFACE_MESH_2D)
         s->poly = make_poly(vertices, n_vertices, (int)dim);
     switch (interaction) {
         case ORACLE_HARD_SPHERE:

@@ -38,6 +38,8 @@ uint32_t oracle_counter_choose(uint64_t step, uint32_t substep, uint32_t seed, u
                                uint32_t len);
 double oracle_cbrt(double x);
 void oracle_sincos_half(double theta, double* s, double* c);
+// Correctly rounded sin and cos (the 2-D rotation path); returns 1 for |x| >= 2^20.
+int oracle_cr_sincos(double x, double* s, double* c);
 void oracle_ziggurat_tables(double* x_out /*257*/, double* f_out /*257*/);
 
 // ---- boundary and checkerboard (hoomd-microstate boundary, hoomd-mc hypercuboid.rs) ----
@@ -64,6 +66,9 @@ int oracle_convex_intersects_at_3d(const double* verts_a, uint32_t nv_a, const d
                                    uint32_t nv_b, const double* v_ij, const double* q_ij);
 int oracle_convex_intersects_at_2d(const double* verts_a, uint32_t nv_a, const double* verts_b,
                                    uint32_t nv_b, const double* v_ij, double theta_ij);
+// ConvexSurfaceMesh2d::intersects_at (separating axes) with theta_ij; CCW hull vertices.
+int oracle_surface_mesh_intersects_at_2d(const double* verts_a, uint32_t nv_a, const double* verts_b,
+                                         uint32_t nv_b, const double* v_ij, double theta_ij);
 int oracle_convex_intersects_at_global_3d(const double* verts, uint32_t nv, const double* r_i,
                                           const double* q_i, const double* r_j,
                                           const double* q_j);
@@ -76,7 +81,7 @@ double oracle_shifted_lj_pair(double epsilon, double sigma, double r_cut, double
 
 // ---- systems --------------------------------------------------------------------
 enum { ORACLE_HARD_SPHERE = 0, ORACLE_HARD_CONVEX_POLYGON = 1, ORACLE_HARD_CONVEX_POLYHEDRON = 2,
-       ORACLE_LENNARD_JONES = 3 };
+       ORACLE_LENNARD_JONES = 3, ORACLE_HARD_CONVEX_SURFACE_MESH_2D = 4 };
 enum { ORACLE_TRANSLATE = 0, ORACLE_ROTATE = 1 };
 
 typedef struct oracle_system oracle_system;

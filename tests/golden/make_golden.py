@@ -191,6 +191,32 @@ def convex(root):
     return shapes, cases2d, cases3d
 
 
+def surface_mesh_2d(root):
+    """Separating-axis cases of ConvexSurfaceMesh2d (hoomd-blue's polygon cases, restated there)."""
+    rel = "hoomd-geometry/src/shape/convex_surface_mesh_2d.rs"
+    t = _read(root, rel)
+    shapes = {}
+    for name in ("square", "triangle"):
+        m = re.search(r"fn " + name + r"\(\) -> ConvexSurfaceMesh2d \{.*?from_point_set\(\[(.*?)\]\)", t, re.S)
+        shapes[name] = [[_num(x) for x in v.split(",")] for v in re.findall(r"\[([^\[\]]+)\]\.into\(\)", m.group(1))]
+    cases = []
+    for name, s, e in _fn_blocks(t):
+        body = t[s:e]
+        if name in ("square_no_rot", "square_rot"):
+            ang = 0.0 if name == "square_no_rot" else math.pi / 4
+            for c in re.finditer(r"assert!\((!?)square\.intersects_at\(&square, &\[([^\]]+)\]\.into\(\), &a\)\);", body):
+                cases.append({"a": "square", "b": "square", "v_ij": [_num(x) for x in c.group(2).split(",")],
+                              "theta_ij": ang, "expected": c.group(1) != "!", "symmetric": False,
+                              "src": f"{rel}:{_line_of(t, s + c.start())}"})
+        elif name == "square_triangle":
+            for c in re.finditer(r"assert_symmetric_overlap\(\s*\[([^\]]+)\]\.into\(\),\s*&square,\s*&triangle,\s*"
+                                 r"r_square,\s*r_triangle,\s*(true|false),?\s*\)", body):
+                cases.append({"a": "square", "b": "triangle", "r_ab": [_num(x) for x in c.group(1).split(",")],
+                              "theta_a": -math.pi / 4, "theta_b": math.pi, "expected": c.group(2) == "true",
+                              "symmetric": True, "src": f"{rel}:{_line_of(t, s + c.start())}"})
+    return {"shapes": shapes, "cases": cases}
+
+
 def spheres(root):
     rel = "hoomd-geometry/src/shape/sphere.rs"
     t = _read(root, rel)
@@ -256,6 +282,7 @@ def main(root):
         "convex_shapes": shapes,
         "convex_2d": c2,
         "convex_3d": c3,
+        "surface_mesh_2d": surface_mesh_2d(root),
         "spheres": spheres(root),
         "lennard_jones": lj(root),
         "pairwise_doc": pairwise_doc(root),

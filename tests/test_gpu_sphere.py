@@ -63,6 +63,24 @@ def test_trajectory_bit_identical_to_oracle(ctx, dim, n, phi, d, sweeps, precisi
     assert o.overlap_count() == 0
 
 
+@pytest.mark.parametrize("dim,n,phi,d", [(3, 4000, 0.50, 0.15), (2, 4096, 0.70, 0.1)])
+def test_wide_fp32_band_rechecks_in_fp64(ctx, monkeypatch, dim, n, phi, d):
+    # Widening the FP32 band 10^5 times sends every pair within ~10 % of contact to the FP64
+    # recheck inside the sweep; the trajectory must still equal the oracle's.
+    monkeypatch.setenv("HMC_B200_FP32_BAND_SCALE", "1e5")
+    g, o, _ = make(ctx, dim, n, phi, seed=0x5EED0011)
+    monkeypatch.delenv("HMC_B200_FP32_BAND_SCALE")
+    rechecks = 0
+    for _ in range(6):
+        c = g.sweep(TRANSLATE, d, 1.0, FP32_RECHECK, n_sweeps=1, increment_step=True)
+        a, r = o.parallel_sweep(oracle.TRANSLATE, d, 1.0, 1.0)
+        o.increment_step()
+        assert (c.accepted, c.rejected) == (a, r)
+        rechecks += c.rechecks
+    assert rechecks > 100
+    assert np.array_equal(g.positions(), o.state()[0])
+
+
 @pytest.mark.parametrize("precision", [FP64, FP32_RECHECK])
 def test_large_spaces_choose_among_several_bodies(ctx, precision):
     # body_interaction_range 2.5: ~5-15 bodies per space, exercising choose() and the

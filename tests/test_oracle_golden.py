@@ -116,9 +116,93 @@ def test_convex_polygon_overlaps(golden):
         for r_ab, sa, sb, ta, tb in ((np.array(c["r_ab"]), a, b, c["theta_a"], c["theta_b"]),
                                      (-np.array(c["r_ab"]), b, a, c["theta_b"], c["theta_a"])):
             inv = -ta
-            s, co = math.sin(inv), math.cos(inv)
+            s, co = oracle.cr_sincos(inv)
             v_ij = [r_ab[0] * co - r_ab[1] * s, r_ab[0] * s + r_ab[1] * co]
             assert oracle.convex_intersects_at_2d(sa, sb, v_ij, tb + inv) == c["expected"], c["src"]
+
+
+def test_surface_mesh_separating_axes(golden):
+    # ConvexSurfaceMesh2d::intersects_at (convex_surface_mesh_2d.rs:578-640) on the
+    # reference's own cases (square_no_rot, square_rot, square_triangle).
+    g = golden["surface_mesh_2d"]
+    assert len(g["cases"]) == 34
+    shapes = {k: np.array(v) for k, v in g["shapes"].items()}
+    for c in g["cases"]:
+        a, b = shapes[c["a"]], shapes[c["b"]]
+        if not c["symmetric"]:
+            assert oracle.surface_mesh_intersects_at_2d(a, b, c["v_ij"], c["theta_ij"]) == c["expected"], c["src"]
+            continue
+        for r_ab, sa, sb, ta, tb in ((np.array(c["r_ab"]), a, b, c["theta_a"], c["theta_b"]),
+                                     (-np.array(c["r_ab"]), b, a, c["theta_b"], c["theta_a"])):
+            inv = -ta
+            s, co = oracle.cr_sincos(inv)
+            v_ij = [r_ab[0] * co - r_ab[1] * s, r_ab[0] * s + r_ab[1] * co]
+            assert oracle.surface_mesh_intersects_at_2d(sa, sb, v_ij, tb + inv) == c["expected"], c["src"]
+
+
+def _exact_sincos(x):
+    """sin x, cos x of the binary64 x to ~75 digits (Machin pi, Taylor series), then rounded."""
+    from decimal import Decimal, localcontext
+    with localcontext() as ctx:
+        ctx.prec = 90
+
+        def arctan_inv(n):
+            n = Decimal(n)
+            s, t, k, sign = Decimal(0), 1 / n, 1, 1
+            while True:
+                term = t / k
+                if term < Decimal(10) ** -88:
+                    return s
+                s += sign * term
+                t /= n * n
+                k += 2
+                sign = -sign
+
+        half_pi = (16 * arctan_inv(5) - 4 * arctan_inv(239)) / 2
+        X = Decimal(x)
+        k = (X / half_pi).to_integral_value()
+        r = X - k * half_pi
+        sn, cs = Decimal(0), Decimal(0)
+        term, n = r, 1
+        while abs(term) > Decimal(10) ** -85:
+            sn += term
+            term = -term * r * r / ((n + 1) * (n + 2))
+            n += 2
+        term, n = Decimal(1), 0
+        while abs(term) > Decimal(10) ** -85:
+            cs += term
+            term = -term * r * r / ((n + 1) * (n + 2))
+            n += 2
+        sn, cs = [(sn, cs), (cs, -sn), (-sn, -cs), (-cs, sn)][int(k) % 4]
+        return float(sn), float(cs)
+
+
+def test_cr_sincos_is_correctly_rounded():
+    # The 2-D rotation path (Angle -> RotationMatrix, angle.rs:120-150) uses these values on
+    # the device and in the oracle: check them against a 90-digit evaluation.
+    rng = np.random.default_rng(17)
+    xs = list(rng.uniform(-7.0, 7.0, 300)) + list(rng.uniform(-1e5, 1e5, 100))
+    xs += [math.pi / 4, -math.pi / 4, math.pi / 2, math.pi, 3 * math.pi / 2, 1e-9, -3e-8, 2.0 ** -26, 1e6,
+           355.0, 103993.0, float(2 ** 20 - 1)]
+    for x in xs:
+        assert oracle.cr_sincos(float(x)) == _exact_sincos(float(x)), x
+    with pytest.raises(ValueError):
+        oracle.cr_sincos(2.0 ** 20)
+
+
+def test_cr_sincos_against_platform_libm():
+    # The reference calls the platform libm; this platform's sin/cos are not always
+    # correctly rounded. The two agree on almost every argument and never by more than 1 ulp.
+    rng = np.random.default_rng(18)
+    xs = rng.uniform(-4.0, 4.0, 20000)
+    diff = 0
+    for x in xs:
+        s, c = oracle.cr_sincos(float(x))
+        for got, ref in ((s, math.sin(x)), (c, math.cos(x))):
+            if got != ref:
+                diff += 1
+                assert abs(got - ref) <= np.spacing(abs(ref))
+    assert diff < 0.01 * 2 * len(xs)
 
 
 def test_sphere_overlaps_through_hard_sphere_pair(golden):
