@@ -33,7 +33,7 @@ LIB_PATH = os.environ.get("HMC_B200_LIB", os.path.join(_HERE, "libhmc_b200.so"))
 OK, INVALID_ARGUMENT, RANGE_TOO_LARGE, OVERLAP_IN_INPUT, CELL_OVERFLOW, NAN_STATE, ITERATION_CAP, TIMEOUT, \
     CUDA_ERROR, OUT_OF_MEMORY, NOT_SUPPORTED, OUTSIDE_CHECKERBOARD = range(12)
 # hmc_interaction / hmc_move / hmc_precision
-HARD_SPHERE, HARD_CONVEX_POLYGON, HARD_CONVEX_POLYHEDRON, LENNARD_JONES = range(4)
+HARD_SPHERE, HARD_CONVEX_POLYGON, HARD_CONVEX_POLYHEDRON, LENNARD_JONES, HARD_CONVEX_SURFACE_MESH_2D = range(5)
 TRANSLATE, ROTATE = range(2)
 FP64, FP32_RECHECK = range(2)
 
@@ -95,6 +95,7 @@ SIGNATURES = {
     "hmc_set_state": (C.c_int, [_vp, _dp, _dp, C.c_uint64, C.c_uint32]),
     "hmc_get_state": (C.c_int, [_vp, _dp, _dp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32)]),
     "hmc_increment_step": (C.c_int, [_vp]),
+    "hmc_math_sincos": (C.c_int, [_vp, _dp, C.c_uint64, _dp, _dp]),
     "hmc_sweep": (C.c_int, [_vp, C.POINTER(hmc_sweep_params), C.POINTER(hmc_count)]),
     "hmc_tune": (C.c_int, [_vp, C.POINTER(hmc_sweep_params), C.c_double, C.c_uint32, C.c_uint32]),
     "hmc_overlap_check": (C.c_int, [_vp, C.POINTER(C.c_uint64)]),
@@ -142,6 +143,15 @@ class Context:
         _check(lib.hmc_context_create(C.byref(opts), C.byref(h)))
         self._h = h
         self.device = device
+
+    def sincos(self, x) -> "tuple[np.ndarray, np.ndarray]":
+        """The correctly rounded sin and cos of the 2-D rotation path, evaluated on the device."""
+        x = np.ascontiguousarray(x, dtype=np.float64).reshape(-1)
+        sn = np.empty_like(x)
+        cs = np.empty_like(x)
+        _check(_lib.hmc_math_sincos(self._h, x.ctypes.data_as(_dp), x.size, sn.ctypes.data_as(_dp),
+                                    cs.ctypes.data_as(_dp)))
+        return sn, cs
 
     def close(self):
         if getattr(self, "_h", None):
@@ -204,9 +214,70 @@ class ConvexPolyhedron:
 
 
 @dataclass
+class ConvexPolygon:
+    """hoomd_geometry::shape::ConvexPolygon (convex_polytope.rs:100): 3 to 32 vertices, any order
+    (the support function's first maximum follows the given order); XenoCollide overlaps."""
+    vertices: np.ndarray
+
+    @classmethod
+    def with_vertices(cls, vertices) -> "ConvexPolygon":
+        return cls(np.ascontiguousarray(vertices, dtype=np.float64).reshape(-1, 2))
+
+    @classmethod
+    def regular(cls, n: int) -> "ConvexPolygon":
+        """Regular n-gon of unit circumradius (a vertex at angle 0)."""
+        k = np.arange(n)
+        return cls(np.stack([np.cos(2 * np.pi * k / n), np.sin(2 * np.pi * k / n)], axis=1))
+
+    @property
+    def bounding_radius(self) -> float:
+        return float(np.sqrt(max(float(np.dot(v, v)) for v in self.vertices)))
+
+
+def convex_hull_2d(points) -> np.ndarray:
+    """Counter-clockwise hull without collinear points, starting at the lowest (then leftmost)
+    point, as ConvexSurfaceMesh2d::construct_convex_hull keeps it (convex_surface_mesh_2d.rs:166-260)."""
+    pts = sorted({(float(x), float(y)) for x, y in np.asarray(points, dtype=np.float64).reshape(-1, 2)})
+
+    def cross(o, a, b):
+        return (a[0] - o[0]) * (b[1] - o[1]) - (a[1] - o[1]) * (b[0] - o[0])
+
+    lower, upper = [], []
+    for p in pts:
+        while len(lower) >= 2 and cross(lower[-2], lower[-1], p) <= 0:
+            lower.pop()
+        lower.append(p)
+    for p in reversed(pts):
+        while len(upper) >= 2 and cross(upper[-2], upper[-1], p) <= 0:
+            upper.pop()
+        upper.append(p)
+    hull = lower[:-1] + upper[:-1]
+    if len(hull) < 3:
+        raise HmcError(INVALID_ARGUMENT, "fewer than 3 non-collinear points")
+    start = min(range(len(hull)), key=lambda i: (hull[i][1], hull[i][0]))
+    return np.array(hull[start:] + hull[:start])
+
+
+@dataclass
+class ConvexSurfaceMesh2d:
+    """hoomd_geometry::shape::ConvexSurfaceMesh2d (convex_surface_mesh_2d.rs): a convex polygon
+    held as its counter-clockwise hull; separating-axis overlaps."""
+    vertices: np.ndarray
+
+    @classmethod
+    def from_point_set(cls, points) -> "ConvexSurfaceMesh2d":
+        return cls(convex_hull_2d(points))
+
+    @property
+    def bounding_radius(self) -> float:
+        return float(np.sqrt(max(float(np.dot(v, v)) for v in self.vertices)))
+
+
+@dataclass
 class HardShape:
-    """hoomd_interaction::pairwise::HardShape(Convex(shape)) (hard_shape.rs:33-119)."""
-    shape: ConvexPolyhedron
+    """hoomd_interaction::pairwise::HardShape(Convex(shape)) or HardShape(ConvexSurfaceMesh2d)
+    (hard_shape.rs:33-119)."""
+    shape: object
 
     @property
     def maximum_interaction_range(self) -> float:
@@ -292,7 +363,8 @@ class Microstate:
             d.interaction = HARD_SPHERE
             d.diameter = pair.diameter
         elif isinstance(pair, HardShape):
-            d.interaction = HARD_CONVEX_POLYHEDRON
+            d.interaction = {ConvexPolyhedron: HARD_CONVEX_POLYHEDRON, ConvexPolygon: HARD_CONVEX_POLYGON,
+                             ConvexSurfaceMesh2d: HARD_CONVEX_SURFACE_MESH_2D}[type(pair.shape)]
             verts = np.ascontiguousarray(pair.shape.vertices, dtype=np.float64)
             self._verts = verts  # keep alive during the call
             d.n_vertices = verts.shape[0]
@@ -307,12 +379,13 @@ class Microstate:
             raise HmcError(NOT_SUPPORTED, f"{type(pair).__name__}")
         d.boundary_range = boundary.maximum_interaction_range
         d.body_interaction_range = body_interaction_range
-        self.oriented = d.interaction == HARD_CONVEX_POLYHEDRON
+        self.oriented = d.interaction in (HARD_CONVEX_POLYHEDRON, HARD_CONVEX_POLYGON, HARD_CONVEX_SURFACE_MESH_2D)
+        self.ori_len = (4 if self.dim == 3 else 1) if self.oriented else 0
         ori = None
         if self.oriented:
             if orientations is None:
-                orientations = np.tile([1.0, 0.0, 0.0, 0.0], (self.n, 1))
-            ori = np.ascontiguousarray(orientations, dtype=np.float64).reshape(self.n, 4)
+                orientations = np.tile([1.0, 0.0, 0.0, 0.0], (self.n, 1)) if self.dim == 3 else np.zeros(self.n)
+            ori = np.ascontiguousarray(orientations, dtype=np.float64).reshape(self.n * self.ori_len)
         h = _vp()
         _check(lib.hmc_system_create(ctx._h, C.byref(d), pos.ctypes.data_as(_dp),
                                      None if ori is None else ori.ctypes.data_as(_dp), C.byref(h)))
@@ -341,7 +414,8 @@ class Microstate:
         return pos, step.value, sub.value
 
     def orientations(self) -> np.ndarray:
-        ori = np.zeros((self.n, 4))
+        """Versors (n x 4: s, x, y, z) in 3-D, angles (n) in 2-D."""
+        ori = np.zeros((self.n, 4)) if self.dim == 3 else np.zeros(self.n)
         _check(_lib.hmc_get_state(self._h, None, ori.ctypes.data_as(_dp), None, None))
         return ori
 
@@ -362,7 +436,8 @@ class Microstate:
 
     def set_state(self, positions, step: int, substep: int, orientations=None):
         pos = np.ascontiguousarray(positions, dtype=np.float64).reshape(self.n, self.dim)
-        ori = None if orientations is None else np.ascontiguousarray(orientations, dtype=np.float64).reshape(self.n, 4)
+        ori = None if orientations is None else np.ascontiguousarray(orientations, dtype=np.float64).reshape(
+            self.n * (4 if self.dim == 3 else 1))
         _check(_lib.hmc_set_state(self._h, pos.ctypes.data_as(_dp), None if ori is None else ori.ctypes.data_as(_dp),
                                   step, substep))
 
@@ -413,7 +488,10 @@ class Microstate:
         arr["position"][:, : self.dim] = pos
         arr["u"] = -1.0 if u is None else np.asarray(u, dtype=np.float64)
         if orientations is not None:
-            arr["orientation"] = np.asarray(orientations, dtype=np.float64).reshape(n, 4)
+            if self.dim == 3:
+                arr["orientation"] = np.asarray(orientations, dtype=np.float64).reshape(n, 4)
+            else:
+                arr["orientation"][:, 0] = np.asarray(orientations, dtype=np.float64).reshape(n)
         moves = arr.ctypes.data_as(C.POINTER(hmc_injected_move))
         dec = np.zeros(n, dtype=np.uint8)
         rech = np.zeros(n, dtype=np.uint8)
@@ -479,7 +557,8 @@ class ParallelSweep:
             self.local_trial.maximum_rotation = tuned
 
 
-__all__ = ["Context", "ConvexPolyhedron", "Count", "HardShape", "HardSphere", "HmcError", "Isothermal", "Isotropic",
+__all__ = ["Context", "ConvexPolygon", "ConvexPolyhedron", "ConvexSurfaceMesh2d", "Count", "convex_hull_2d", "HardShape", "HardSphere", "HmcError", "Isothermal", "Isotropic",
            "LennardJones", "Microstate", "PairwiseCutoff", "Rotate", "Shifted", "TuneOptions",
            "ParallelSweep", "Periodic", "Translate", "load_library", "SIGNATURES", "FP64", "FP32_RECHECK",
-           "TRANSLATE", "ROTATE"]
+           "TRANSLATE", "ROTATE", "HARD_SPHERE", "HARD_CONVEX_POLYGON", "HARD_CONVEX_POLYHEDRON", "LENNARD_JONES",
+           "HARD_CONVEX_SURFACE_MESH_2D"]

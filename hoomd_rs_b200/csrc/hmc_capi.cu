@@ -90,7 +90,11 @@ struct hmc_system {
     uint32_t n_vertices = 0;
     double poly_rcut2 = 0.0;
     float poly_rcut2_hi32 = 0.f;
-    bool oriented() const { return interaction == HMC_HARD_CONVEX_POLYHEDRON; }
+    bool polygon() const {
+        return interaction == HMC_HARD_CONVEX_POLYGON || interaction == HMC_HARD_CONVEX_SURFACE_MESH_2D;
+    }
+    bool oriented() const { return interaction == HMC_HARD_CONVEX_POLYHEDRON || polygon(); }
+    bool sat() const { return interaction == HMC_HARD_CONVEX_SURFACE_MESH_2D; }
     // profiling
     bool profiling = false;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -190,6 +194,7 @@ hmc_status check_flags(hmc_system* s) {
     uint32_t f = s->host_stats->error_flags;
     if (f & kErrNonFinite) return fail(HMC_NAN_STATE, "a body position is not finite");
     if (f & kErrOutsideCheckerboard) return fail(HMC_OUTSIDE_CHECKERBOARD, "a body maps to no checkerboard space");
+    if (f & kErrAngleRange) return fail(HMC_INVALID_ARGUMENT, "a 2-D orientation angle reached 2^19 rad");
     return HMC_OK;
 }
 
@@ -308,8 +313,37 @@ hmc_status hmc_system_create(hmc_context* ctx, const hmc_system_desc* d, const d
         if (!(d->edge_lengths[a] > 0.0) || !std::isfinite(d->edge_lengths[a]))
             return fail(HMC_INVALID_ARGUMENT, "edge length %u must be positive", a);
     if (d->interaction != HMC_HARD_SPHERE && d->interaction != HMC_LENNARD_JONES &&
-        d->interaction != HMC_HARD_CONVEX_POLYHEDRON)
+        d->interaction != HMC_HARD_CONVEX_POLYHEDRON && d->interaction != HMC_HARD_CONVEX_POLYGON &&
+        d->interaction != HMC_HARD_CONVEX_SURFACE_MESH_2D)
         return fail(HMC_NOT_SUPPORTED, "interaction %u is not available in this build", d->interaction);
+    const bool polygon = d->interaction == HMC_HARD_CONVEX_POLYGON || d->interaction == HMC_HARD_CONVEX_SURFACE_MESH_2D;
+    if (polygon) {
+        if (d->dim != 2) return fail(HMC_INVALID_ARGUMENT, "convex polygons are 2-D");
+        // ConvexPolygon = ConvexPolytope<2, 32>; the separating-axis test needs a hull of >= 3
+        if (d->n_vertices < 3 || d->n_vertices > 32 || !d->vertices)
+            return fail(HMC_INVALID_ARGUMENT, "a convex polygon needs 3 to 32 vertices");
+        for (uint32_t i = 0; i < 2 * d->n_vertices; ++i)
+            if (!std::isfinite(d->vertices[i])) return fail(HMC_INVALID_ARGUMENT, "vertex coordinates must be finite");
+        if (d->interaction == HMC_HARD_CONVEX_SURFACE_MESH_2D) {
+            // ConvexSurfaceMesh2d keeps its hull counter-clockwise without collinear points
+            // (convex_surface_mesh_2d.rs:166-260); its edge normals rely on that order.
+            const uint32_t nv = d->n_vertices;
+            for (uint32_t i = 0; i < nv; ++i) {
+                const double* a = d->vertices + 2 * i;
+                const double* b = d->vertices + 2 * ((i + 1) % nv);
+                const double* c = d->vertices + 2 * ((i + 2) % nv);
+                const double cross = (b[0] - a[0]) * (c[1] - b[1]) - (b[1] - a[1]) * (c[0] - b[0]);
+                if (!(cross > 0.0))
+                    return fail(HMC_INVALID_ARGUMENT,
+                                "surface-mesh vertices must be a strictly convex counter-clockwise hull");
+            }
+        }
+        if (d->n_bodies > 0 && orientations)
+            for (uint64_t i = 0; i < d->n_bodies; ++i)
+                if (!(std::fabs(orientations[i]) < 524288.0))
+                    return fail(HMC_INVALID_ARGUMENT, "orientation angle %llu must be finite with |theta| < 2^19",
+                                (unsigned long long)i);
+    }
     if (d->interaction == HMC_HARD_CONVEX_POLYHEDRON) {
         if (d->dim != 3) return fail(HMC_INVALID_ARGUMENT, "convex polyhedra are 3-D");
         // ConvexPolytope::with_vertices: at least one vertex, at most 32 (ConvexPolyhedron)
@@ -328,14 +362,16 @@ hmc_status hmc_system_create(hmc_context* ctx, const hmc_system_desc* d, const d
     // HardShape (hard_shape.rs:111-118) = 2 x the bounding radius, where ConvexPolytope's
     // bounding radius (convex_polytope.rs:199-207) is sqrt(max |v|^2) with |v|^2 by mul_add.
     double bounding_radius = 0.0;
-    if (d->interaction == HMC_HARD_CONVEX_POLYHEDRON) {
+    if (d->interaction == HMC_HARD_CONVEX_POLYHEDRON || polygon) {
         double mx = 0.0;
         for (uint32_t i = 0; i < d->n_vertices; ++i) {
-            const double* v = d->vertices + 3 * i;
-            mx = std::max(mx, std::fma(v[2], v[2], std::fma(v[1], v[1], std::fma(v[0], v[0], 0.0))));
+            const double* v = d->vertices + d->dim * i;
+            double n2 = std::fma(v[1], v[1], std::fma(v[0], v[0], 0.0));
+            if (d->dim == 3) n2 = std::fma(v[2], v[2], n2);
+            mx = std::max(mx, n2);
         }
         bounding_radius = std::sqrt(mx);
-        if (!(bounding_radius > 0.0)) return fail(HMC_INVALID_ARGUMENT, "the polyhedron's bounding radius must be positive");
+        if (!(bounding_radius > 0.0)) return fail(HMC_INVALID_ARGUMENT, "the shape's bounding radius must be positive");
     }
 
     HMC_CUDA(cudaSetDevice(ctx->device));
@@ -349,7 +385,7 @@ hmc_status hmc_system_create(hmc_context* ctx, const hmc_system_desc* d, const d
     s->seed = d->seed;
     s->interaction = d->interaction;
     s->pair_range = d->interaction == HMC_LENNARD_JONES ? d->lj_r_cut
-                    : d->interaction == HMC_HARD_CONVEX_POLYHEDRON ? bounding_radius * 2.0
+                    : (d->interaction == HMC_HARD_CONVEX_POLYHEDRON || polygon) ? bounding_radius * 2.0
                                                                   : d->diameter;
     s->boundary_range = d->boundary_range > 0.0 ? d->boundary_range : s->pair_range;
     s->body_range = d->body_interaction_range > 0.0 ? d->body_interaction_range : s->pair_range;
@@ -403,7 +439,7 @@ hmc_status hmc_system_create(hmc_context* ctx, const hmc_system_desc* d, const d
     if (d->interaction == HMC_HARD_SPHERE) {
         s->pair.sigma2 = d->diameter * d->diameter;  // diameter.powi(2)
         sphere_bound(s);
-    } else if (d->interaction == HMC_HARD_CONVEX_POLYHEDRON) {
+    } else if (d->interaction == HMC_HARD_CONVEX_POLYHEDRON || polygon) {
         // circumsphere rejection (convex.rs:162-165): r_cut = R + R, compared with r_cut.powi(2)
         const double rc = bounding_radius + bounding_radius;
         s->poly_rcut2 = rc * rc;
@@ -459,15 +495,22 @@ hmc_status hmc_system_create(hmc_context* ctx, const hmc_system_desc* d, const d
             (st = dalloc(s, &s->verts, s->n_vertices)))
             return destroy_fail(st);
         std::vector<double4> hv(s->n_vertices);
+        const uint32_t dv = (uint32_t)s->dim;
         for (uint32_t i = 0; i < s->n_vertices; ++i)
-            hv[i] = make_double4(d->vertices[3 * i], d->vertices[3 * i + 1], d->vertices[3 * i + 2], 0.0);
+            hv[i] = make_double4(d->vertices[dv * i], d->vertices[dv * i + 1], dv == 3 ? d->vertices[dv * i + 2] : 0.0,
+                                 0.0);
         e = cudaMemcpy(s->verts, hv.data(), sizeof(double4) * s->n_vertices, cudaMemcpyHostToDevice);
         if (e == cudaSuccess && n > 0) {
+            // versors (s, x, y, z) in 3-D, identity by default; angles in .x in 2-D, 0 by default
             std::vector<double4> hq(n);
-            for (uint64_t i = 0; i < n; ++i)
-                hq[i] = orientations ? make_double4(orientations[4 * i], orientations[4 * i + 1], orientations[4 * i + 2],
-                                                    orientations[4 * i + 3])
-                                     : make_double4(1.0, 0.0, 0.0, 0.0);
+            for (uint64_t i = 0; i < n; ++i) {
+                if (s->dim == 3)
+                    hq[i] = orientations ? make_double4(orientations[4 * i], orientations[4 * i + 1],
+                                                        orientations[4 * i + 2], orientations[4 * i + 3])
+                                         : make_double4(1.0, 0.0, 0.0, 0.0);
+                else
+                    hq[i] = make_double4(orientations ? orientations[i] : 0.0, 0.0, 0.0, 0.0);
+            }
             e = cudaMemcpy(A.body_ori, hq.data(), sizeof(double4) * n, cudaMemcpyHostToDevice);
         }
         if (e != cudaSuccess) {
@@ -529,10 +572,23 @@ hmc_status hmc_set_state(hmc_system* s, const double* positions, const double* o
             return fail(HMC_NAN_STATE, "position %llu is not finite", (unsigned long long)*s->host_first_bad);
         // Positions are body positions as returned by hmc_get_state (already wrapped).
         HMC_CUDA(launch_unpack_positions(s->dim, s->stage, s->arr.body_pos, s->n, s->stream));
-        if (s->oriented() && orientations)  // (s, x, y, z) per body: the double4 layout
+        if (s->oriented() && orientations && s->dim == 3)  // (s, x, y, z) per body: the double4 layout
             HMC_CUDA(cudaMemcpyAsync(s->arr.body_ori, orientations, sizeof(double4) * s->n, cudaMemcpyHostToDevice,
                                      s->stream));
         HMC_CUDA(cudaStreamSynchronize(s->stream));
+        if (s->oriented() && orientations && s->dim == 2) {  // one angle per body, through the staging array
+            HMC_CUDA(cudaMemcpyAsync(s->stage, orientations, sizeof(double) * s->n, cudaMemcpyHostToDevice, s->stream));
+            HMC_CUDA(cudaMemsetAsync(s->first_bad, 0xFF, sizeof(unsigned long long), s->stream));
+            HMC_CUDA(launch_check_angles(s->stage, s->n, s->first_bad, s->stream));
+            HMC_CUDA(cudaMemcpyAsync(s->host_first_bad, s->first_bad, sizeof(unsigned long long),
+                                     cudaMemcpyDeviceToHost, s->stream));
+            HMC_CUDA(cudaStreamSynchronize(s->stream));
+            if (*s->host_first_bad != ~0ull)
+                return fail(HMC_INVALID_ARGUMENT, "orientation angle %llu must be finite with |theta| < 2^19 "
+                            "(positions were set)", (unsigned long long)*s->host_first_bad);
+            HMC_CUDA(launch_unpack_angles(s->stage, s->arr.body_ori, s->n, s->stream));
+            HMC_CUDA(cudaStreamSynchronize(s->stream));
+        }
     }
     s->step = step;
     s->substep = substep;
@@ -549,10 +605,15 @@ hmc_status hmc_get_state(hmc_system* s, double* positions, double* orientations,
             HMC_CUDA(cudaMemcpyAsync(positions, s->stage, sizeof(double) * s->n * s->dim, cudaMemcpyDeviceToHost,
                                      s->stream));
         }
-        if (s->oriented() && orientations)
+        if (s->oriented() && orientations && s->dim == 3)
             HMC_CUDA(cudaMemcpyAsync(orientations, s->arr.body_ori, sizeof(double4) * s->n, cudaMemcpyDeviceToHost,
                                      s->stream));
         HMC_CUDA(cudaStreamSynchronize(s->stream));
+        if (s->oriented() && orientations && s->dim == 2) {
+            HMC_CUDA(launch_pack_angles(s->arr.body_ori, s->stage, s->n, s->stream));
+            HMC_CUDA(cudaMemcpyAsync(orientations, s->stage, sizeof(double) * s->n, cudaMemcpyDeviceToHost, s->stream));
+            HMC_CUDA(cudaStreamSynchronize(s->stream));
+        }
     }
     if (step) *step = s->step;
     if (substep) *substep = s->substep;
@@ -612,6 +673,9 @@ hmc_status hmc_sweep(hmc_system* s, const hmc_sweep_params* p, hmc_count* out) {
                 else if (s->interaction == HMC_HARD_CONVEX_POLYHEDRON)
                     HMC_CUDA(launch_sweep_poly(fp32, s->geom, s->arr, s->verts, s->n_vertices, s->poly_rcut2,
                                                s->poly_rcut2_hi32, L, p->move == HMC_ROTATE, s->stream));
+                else if (s->polygon())
+                    HMC_CUDA(launch_sweep_poly2(fp32, s->sat(), s->geom, s->arr, s->verts, s->n_vertices, s->poly_rcut2,
+                                                s->poly_rcut2_hi32, L, p->move == HMC_ROTATE, s->stream));
                 else
                     HMC_CUDA(launch_sweep_sphere(s->dim, fp32, s->geom, s->arr, s->pair, L, s->coop[fp32], s->stream));
                 s->prof.kernel_launches += 1;
@@ -644,6 +708,28 @@ hmc_status hmc_sweep(hmc_system* s, const hmc_sweep_params* p, hmc_count* out) {
         }
     }
     if (out) *out = total;
+    return HMC_OK;
+}
+
+hmc_status hmc_math_sincos(hmc_context* ctx, const double* x, uint64_t n, double* sn, double* cs) {
+    if (!ctx || (n > 0 && (!x || !sn || !cs))) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
+    if (n == 0) return HMC_OK;
+    HMC_CUDA(cudaSetDevice(ctx->device));
+    double* d = nullptr;
+    uint32_t* bad = nullptr;
+    uint32_t hbad = 0;
+    cudaError_t e = cudaMalloc((void**)&d, sizeof(double) * 3 * n);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&bad, sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMemcpy(d, x, sizeof(double) * n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(bad, 0, sizeof(uint32_t));
+    if (e == cudaSuccess) e = launch_sincos(d, n, d + n, d + 2 * n, bad, nullptr);
+    if (e == cudaSuccess) e = cudaMemcpy(sn, d + n, sizeof(double) * n, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(cs, d + 2 * n, sizeof(double) * n, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(&hbad, bad, sizeof(uint32_t), cudaMemcpyDeviceToHost);
+    if (d) cudaFree(d);
+    if (bad) cudaFree(bad);
+    if (e != cudaSuccess) return fail(HMC_CUDA_ERROR, "sincos: %s", cudaGetErrorString(e));
+    if (hbad) return fail(HMC_INVALID_ARGUMENT, "an argument has |x| >= 2^20");
     return HMC_OK;
 }
 
@@ -708,6 +794,9 @@ hmc_status hmc_tune(hmc_system* s, hmc_sweep_params* p, double target, uint32_t 
         if (s->interaction == HMC_LENNARD_JONES)
             e = launch_eval_lj(s->dim, fp32, s->geom, s->arr, s->pair, db, dt, du, p->temperature, samples, dd,
                                dd + samples, dh, s->stream);
+        else if (s->polygon())
+            e = launch_eval_poly2(fp32, s->sat(), s->geom, s->arr, s->verts, s->n_vertices, s->poly_rcut2,
+                                  s->poly_rcut2_hi32, db, dt, dq, samples, dd, s->stream);
         else if (s->oriented())
             e = launch_eval_poly(fp32, s->geom, s->arr, s->verts, s->n_vertices, s->poly_rcut2, s->poly_rcut2_hi32, db,
                                  dt, dq, samples, dd, s->stream);
@@ -743,6 +832,9 @@ hmc_status hmc_overlap_check(hmc_system* s, uint64_t* n_overlaps) {
     if (st) return st;
     if (s->interaction == HMC_HARD_CONVEX_POLYHEDRON)
         HMC_CUDA(launch_overlap_poly(s->geom, s->arr, s->verts, s->n_vertices, s->poly_rcut2, (uint32_t)s->n, s->stream));
+    else if (s->polygon())
+        HMC_CUDA(launch_overlap_poly2(s->sat(), s->geom, s->arr, s->verts, s->n_vertices, s->poly_rcut2, (uint32_t)s->n,
+                                      s->stream));
     else
         HMC_CUDA(launch_overlap_sphere(s->dim, s->geom, s->arr, s->pair, (uint32_t)s->n, s->stream));
     s->prof.kernel_launches += 1;
@@ -823,6 +915,9 @@ hmc_status hmc_eval_moves(hmc_system* s, const hmc_injected_move* moves, uint64_
         if (lj)
             e = launch_eval_lj(s->dim, precision == HMC_FP32_RECHECK, s->geom, s->arr, s->pair, db, dt, du, temperature,
                                (uint32_t)n, dd, dd + n, dh, s->stream);
+        else if (s->polygon())
+            e = launch_eval_poly2(precision == HMC_FP32_RECHECK, s->sat(), s->geom, s->arr, s->verts, s->n_vertices,
+                                  s->poly_rcut2, s->poly_rcut2_hi32, db, dt, dq, (uint32_t)n, dd, s->stream);
         else if (s->oriented())
             e = launch_eval_poly(precision == HMC_FP32_RECHECK, s->geom, s->arr, s->verts, s->n_vertices, s->poly_rcut2,
                                  s->poly_rcut2_hi32, db, dt, dq, (uint32_t)n, dd, s->stream);

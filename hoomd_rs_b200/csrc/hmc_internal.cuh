@@ -13,6 +13,7 @@ namespace hmc {
 enum : uint32_t {
     kErrOutsideCheckerboard = 1u << 0,
     kErrNonFinite = 1u << 1,
+    kErrAngleRange = 1u << 2,  // a 2-D orientation angle at or beyond 2^19 rad
 };
 
 // Counters written by the kernels. Zeroed by the host before a sweep.
@@ -125,6 +126,25 @@ cudaError_t launch_overlap_poly(const Geometry& g, const Arrays& a, const double
 cudaError_t launch_tune_moves(int dim, const Geometry& g, const Arrays& a, const Launch& l, uint32_t tune_step,
                               uint32_t samples, bool rotate, uint64_t* bodies, double4* trial, double4* trial_q,
                               double* u, cudaStream_t s);
+// Hard convex polygons (hmc_poly2.cu): XenoCollide (sat = false) or separating axes (sat =
+// true); orientations are angles in .x of body_ori / sorted_q / trial_q.
+cudaError_t launch_sweep_poly2(bool fp32, bool sat, const Geometry& g, const Arrays& a, const double4* verts,
+                               uint32_t nv, double rcut2, float rcut2_hi32, const Launch& l, bool rotate,
+                               cudaStream_t s);
+cudaError_t launch_eval_poly2(bool fp32, bool sat, const Geometry& g, const Arrays& a, const double4* verts,
+                              uint32_t nv, double rcut2, float rcut2_hi32, const uint64_t* bodies,
+                              const double4* trial, const double4* trial_q, uint32_t n, uint8_t* decisions,
+                              cudaStream_t s);
+cudaError_t launch_overlap_poly2(bool sat, const Geometry& g, const Arrays& a, const double4* verts, uint32_t nv,
+                                 double rcut2, uint32_t n, cudaStream_t s);
+// The correctly rounded sin/cos of the rotation path over an array; *bad |= 1 when an
+// argument is out of range.
+cudaError_t launch_sincos(const double* x, uint64_t n, double* sn, double* cs, uint32_t* bad, cudaStream_t s);
+// 2-D orientations through the staging array: check (finite, |theta| < 2^19; smallest bad
+// index into first_bad), unpack into .x of body_ori, pack from it.
+cudaError_t launch_check_angles(const double* packed, uint64_t n, unsigned long long* first_bad, cudaStream_t s);
+cudaError_t launch_unpack_angles(const double* packed, double4* body_ori, uint64_t n, cudaStream_t s);
+cudaError_t launch_pack_angles(const double4* body_ori, double* packed, uint64_t n, cudaStream_t s);
 // State transfer through a packed staging array of n x dim doubles (the host layout):
 // first_nonfinite receives the smallest body index with a non-finite coordinate (it must hold
 // ~0 before the launch); unpack writes body positions, pack reads them.

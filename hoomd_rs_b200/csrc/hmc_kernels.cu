@@ -770,6 +770,23 @@ __global__ void k_pack_positions(const double4* __restrict__ body_pos, double* _
     }
 }
 
+__global__ void k_check_angles(const double* __restrict__ packed, uint64_t n, unsigned long long* first_bad) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const double t = packed[i];
+        if (!(fabs(t) < 524288.0)) atomicMin(first_bad, (unsigned long long)i);
+    }
+}
+
+__global__ void k_unpack_angles(const double* __restrict__ packed, double4* __restrict__ body_ori, uint64_t n) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        body_ori[i] = make_double4(packed[i], 0.0, 0.0, 0.0);
+}
+
+__global__ void k_pack_angles(const double4* __restrict__ body_ori, double* __restrict__ packed, uint64_t n) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        packed[i] = body_ori[i].x;
+}
+
 inline uint32_t stream_grid(uint64_t n) {
     uint64_t b = (n + 255) / 256;
     return (uint32_t)(b < 148ull * 16 ? (b ? b : 1) : 148ull * 16);
@@ -799,6 +816,24 @@ cudaError_t launch_pack_positions(int dim, const double4* body_pos, double* pack
         k_pack_positions<2><<<stream_grid(n), 256, 0, s>>>(body_pos, packed, n);
     else
         k_pack_positions<3><<<stream_grid(n), 256, 0, s>>>(body_pos, packed, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_check_angles(const double* packed, uint64_t n, unsigned long long* first_bad, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    k_check_angles<<<stream_grid(n), 256, 0, s>>>(packed, n, first_bad);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_unpack_angles(const double* packed, double4* body_ori, uint64_t n, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    k_unpack_angles<<<stream_grid(n), 256, 0, s>>>(packed, body_ori, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pack_angles(const double4* body_ori, double* packed, uint64_t n, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    k_pack_angles<<<stream_grid(n), 256, 0, s>>>(body_ori, packed, n);
     return cudaGetLastError();
 }
 

@@ -179,6 +179,175 @@ HMC_HD double standard_normal(Sfc64& r, const double* __restrict__ zx, const dou
     }
 }
 
+// ---- correctly rounded sin and cos ------------------------------------------------------
+// Angle -> RotationMatrix (hoomd-vector angle.rs:120-150) calls f64::sin / f64::cos, i.e.
+// the platform libm. Host and device use this deterministic method instead; it returns the
+// correctly rounded values from correctly rounded +, -, *, fma only:
+//  * Cody-Waite reduction x = k pi/2 + r, pi/2 split into 33 + 33 + 33 + 53 bits (products
+//    k*C1..k*C3 exact for |k| < 2^20), r as a double-double (error-free transforms of
+//    Dekker and Knuth);
+//  * Taylor series of sin r and cos r, |r| <= pi/4, leading terms in double-double and the
+//    rest in double (relative error below 2^-66); Ziv's rounding test against 2^-62; if it
+//    fails, the whole series in double-double (error below 2^-95) decides.
+// |x| >= 2^20 is outside the supported range (returns false).
+struct DDouble {
+    double h, l;
+};
+HMC_HD DDouble dd_two_sum(double a, double b) {
+    const double s = dadd(a, b);
+    const double bb = dsub(s, a);
+    return {s, dadd(dsub(a, dsub(s, bb)), dsub(b, bb))};
+}
+HMC_HD DDouble dd_fast_sum(double a, double b) {  // |a| >= |b|
+    const double s = dadd(a, b);
+    return {s, dsub(b, dsub(s, a))};
+}
+HMC_HD DDouble dd_mul(DDouble a, DDouble b) {
+    const double p = dmul(a.h, b.h);
+    double e = dfma(a.h, b.h, -p);
+    e = dfma(a.h, b.l, e);
+    e = dfma(a.l, b.h, e);
+    return dd_fast_sum(p, e);
+}
+HMC_HD DDouble dd_add(DDouble a, DDouble b) {
+    const DDouble s = dd_two_sum(a.h, b.h);
+    return dd_fast_sum(s.h, dadd(s.l, dadd(a.l, b.l)));
+}
+// (-1)^(k/2) / k!, k = 2..27, as double-doubles (the exact rationals rounded twice).
+HMC_HD constexpr double inv_fact_hi(int k) {
+    switch (k) {
+        case 2: return -0x1.0000000000000p-1;
+        case 3: return -0x1.5555555555555p-3;
+        case 4: return 0x1.5555555555555p-5;
+        case 5: return 0x1.1111111111111p-7;
+        case 6: return -0x1.6c16c16c16c17p-10;
+        case 7: return -0x1.a01a01a01a01ap-13;
+        case 8: return 0x1.a01a01a01a01ap-16;
+        case 9: return 0x1.71de3a556c734p-19;
+        case 10: return -0x1.27e4fb7789f5cp-22;
+        case 11: return -0x1.ae64567f544e4p-26;
+        case 12: return 0x1.1eed8eff8d898p-29;
+        case 13: return 0x1.6124613a86d09p-33;
+        case 14: return -0x1.93974a8c07c9dp-37;
+        case 15: return -0x1.ae7f3e733b81fp-41;
+        case 16: return 0x1.ae7f3e733b81fp-45;
+        case 17: return 0x1.952c77030ad4ap-49;
+        case 18: return -0x1.6827863b97d97p-53;
+        case 19: return -0x1.2f49b46814157p-57;
+        case 20: return 0x1.e542ba4020225p-62;
+        case 21: return 0x1.71b8ef6dcf572p-66;
+        case 22: return -0x1.0ce396db7f853p-70;
+        case 23: return -0x1.761b41316381ap-75;
+        case 24: return 0x1.f2cf01972f578p-80;
+        case 25: return 0x1.3f3ccdd165fa9p-84;
+        case 26: return -0x1.88e85fc6a4e5ap-89;
+        case 27: return -0x1.d1ab1c2dccea3p-94;
+        default: return 0.0;
+    }
+}
+HMC_HD constexpr double inv_fact_lo(int k) {
+    switch (k) {
+        case 2: return 0x0.0p+0;
+        case 3: return -0x1.5555555555555p-57;
+        case 4: return 0x1.5555555555555p-59;
+        case 5: return 0x1.1111111111111p-63;
+        case 6: return 0x1.f49f49f49f49fp-65;
+        case 7: return -0x1.a01a01a01a01ap-73;
+        case 8: return 0x1.a01a01a01a01ap-76;
+        case 9: return -0x1.c154f8ddc6c00p-73;
+        case 10: return -0x1.cbbc05b4fa99ap-76;
+        case 11: return 0x1.c062e06d1f209p-80;
+        case 12: return -0x1.2aec959e14c06p-83;
+        case 13: return 0x1.f28e0cc748ebep-87;
+        case 14: return -0x1.05d6f8a2efd1fp-92;
+        case 15: return -0x1.1d8656b0ee8cbp-97;
+        case 16: return 0x1.1d8656b0ee8cbp-101;
+        case 17: return 0x1.ac981465ddc6cp-103;
+        case 18: return -0x1.eec01221a8b0bp-107;
+        case 19: return -0x1.2650f61dbdcb4p-112;
+        case 20: return 0x1.ea72b4afe3c2fp-120;
+        case 21: return -0x1.d043ae40c4647p-120;
+        case 22: return 0x1.aebcdbd20331cp-124;
+        case 23: return 0x1.3423c7d91404fp-130;
+        case 24: return -0x1.9ada5fcc1ab14p-135;
+        case 25: return -0x1.58ddadf344487p-139;
+        case 26: return 0x1.71c37ebd16540p-143;
+        case 27: return -0x1.054d0c78aea14p-149;
+        default: return 0.0;
+    }
+}
+// sum_j c_(FIRST + 2j) z^j, the first NDD coefficients in double-double, the rest in double.
+template <int FIRST, int NDD>
+HMC_HD DDouble taylor_series(DDouble z) {
+    constexpr int LAST = (FIRST & 1) ? 27 : 26;
+    constexpr int SPLIT = FIRST + 2 * NDD;
+    double t = 0.0;
+#pragma unroll
+    for (int k = LAST; k >= SPLIT; k -= 2) t = dfma(t, z.h, inv_fact_hi(k));
+    DDouble p{t, 0.0};
+    if (SPLIT <= LAST) p = dd_mul(p, z);
+#pragma unroll
+    for (int k = SPLIT - 2; k >= FIRST; k -= 2) {
+        p = dd_add(DDouble{inv_fact_hi(k), inv_fact_lo(k)}, p);
+        if (k > FIRST) p = dd_mul(p, z);
+    }
+    return p;
+}
+HMC_HD double next_up_double(double x) {
+    if (x == 0.0) return 4.9406564584124654e-324;
+    const uint64_t b = as_bits(x);
+    return as_double(x > 0.0 ? b + 1 : b - 1);
+}
+// Ziv's test: the exact value lies within err of v.h + v.l; true when it rounds to v.h.
+HMC_HD bool rounds_to_head(DDouble v, double err) {
+    const double up = dmul(dsub(next_up_double(v.h), v.h), 0.5);
+    const double down = dmul(dsub(v.h, -next_up_double(-v.h)), 0.5);
+    return dadd(v.l, err) < up && dsub(v.l, err) > -down;
+}
+template <int NDD>
+HMC_HD void sincos_reduced(DDouble r, DDouble* s, DDouble* c) {
+    const DDouble z = dd_mul(r, r);
+    const DDouble ps = taylor_series<3, NDD>(z);
+    const DDouble pc = taylor_series<2, NDD>(z);
+    *s = dd_add(r, dd_mul(dd_mul(r, z), ps));
+    *c = dd_add(DDouble{1.0, 0.0}, dd_mul(z, pc));
+}
+HMC_HD bool cr_sincos(double x, double* sn, double* cs) {
+    const double ax = fabs(x);
+    if (!(ax <= 1.79769313486231570e308)) {  // inf or nan
+        *sn = *cs = dsub(x, x);
+        return true;
+    }
+    if (ax < 0x1p-27) {
+        *sn = x;
+        *cs = 1.0;
+        return true;
+    }
+    if (ax >= 0x1p20) return false;
+    const double k = rint(dmul(x, 0x1.45f306dc9c883p-1));
+    DDouble r{x, 0.0};
+    if (k != 0.0) {
+        const double t = dsub(x, dmul(k, 0x1.921fb54400000p+0));  // exact
+        r = dd_two_sum(t, -dmul(k, 0x1.0b4611a600000p-34));
+        r = dd_add(r, DDouble{-dmul(k, 0x1.3198a2e000000p-69), 0.0});
+        const double p = dmul(k, 0x1.b839a252049c1p-104);
+        r = dd_add(r, DDouble{-p, -dfma(k, 0x1.b839a252049c1p-104, -p)});
+    }
+    const int q = (int)(((long long)k) & 3);
+    DDouble s, c;
+    sincos_reduced<3>(r, &s, &c);
+    if (!rounds_to_head(s, dmul(0x1p-62, fabs(s.h))) || !rounds_to_head(c, dmul(0x1p-62, fabs(c.h))))
+        sincos_reduced<13>(r, &s, &c);
+    const double sv = s.h, cv = c.h;
+    switch (q) {
+        case 0: *sn = sv; *cs = cv; break;
+        case 1: *sn = cv; *cs = -sv; break;
+        case 2: *sn = -sv; *cs = -cv; break;
+        default: *sn = -cv; *cs = sv; break;
+    }
+    return true;
+}
+
 // ---- deterministic cube root and half-angle sin/cos -------------------------------------
 // Cube root without division: x = m 2^(3q + r) with m in [1, 2); y ~ m^(-1/3) from a
 // quadratic Chebyshev fit refined by three Newton steps y += y (1 - m y^3) / 3; then

@@ -428,7 +428,11 @@ __global__ void k_tune_moves(Geometry g, Arrays A, Launch L, uint32_t tune_step,
         const double4 q4 = A.body_ori[b];
         q = Q{q4.x, q4.y, q4.z, q4.w};
     }
-    if (rotate) {
+    if (rotate && DIM == 2) {
+        // Rotate<Angle>::propose (rotate/angle.rs:46-55): theta += Uniform(-a, a); q.s holds theta
+        const double u = dsub(as_double(0x3FF0000000000000ULL | (rng.next_u64() >> 12)), 1.0);
+        q.s = dadd(q.s, dadd(dmul(u, dsub(L.max_move, -L.max_move)), -L.max_move));
+    } else if (rotate) {
         q = versor_move(rng, L.max_move, A.zig_x, A.zig_f, q);
     } else {
         double dv[3];

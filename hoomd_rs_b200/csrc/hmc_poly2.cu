@@ -1,0 +1,426 @@
+// Hard convex polygons: PairwiseCutoff<HardShape<Convex<ConvexPolygon>>> (XenoCollide) and
+// PairwiseCutoff<HardShape<ConvexSurfaceMesh2d>> (separating axes), with
+// Translate<Cartesian<2>> and Rotate<Angle> trial moves.
+//
+// The pair test is IntersectsAtGlobal (hoomd-geometry/src/convex.rs:101-121 and
+// shape/convex_surface_mesh_2d.rs:514-536): a circumcircle rejection, pair_system_to_local
+// (hoomd-vector/src/lib.rs:878-888) with Angle rotations (hoomd-vector/src/angle.rs:120-230),
+// then XenoCollide in 2-D (hoomd-geometry/src/xenocollide.rs:92-154, :361-414) or the
+// separating-axis test (convex_surface_mesh_2d.rs:578-640). Every product, sum and fused
+// multiply-add follows the reference's expression order; sin and cos are correctly rounded
+// (cr_sincos), so the FP64 decision is the reference's on a correctly rounded libm.
+//
+// One warp per trial, as for polyhedra: all lanes compute the same trial move, then stride
+// over the stencil's candidates with an early exit by vote. FP32 + recheck: candidates whose
+// FP32 centre distance clears the circumcircles by more than the FP32 error bound are
+// skipped; every other candidate runs the FP64 test.
+#include <cuda_runtime.h>
+
+#include "hmc_device.cuh"
+
+namespace hmc {
+namespace {
+
+struct V2 {
+    double x, y;
+};
+struct M2 {
+    V2 r[2];
+};
+__device__ __forceinline__ double dot2(const V2& a, const V2& b) {  // mul_add fold from 0.0
+    return dfma(a.y, b.y, dfma(a.x, b.x, 0.0));
+}
+__device__ __forceinline__ V2 sub2(const V2& a, const V2& b) { return {dsub(a.x, b.x), dsub(a.y, b.y)}; }
+__device__ __forceinline__ V2 perp2(const V2& a) { return {-a.y, a.x}; }  // cartesian.rs:755
+__device__ __forceinline__ V2 mat2_rotate(const M2& m, const V2& v) { return {dot2(m.r[0], v), dot2(m.r[1], v)}; }
+__device__ __forceinline__ M2 transpose2(const M2& m) { return {{{m.r[0].x, m.r[1].x}, {m.r[0].y, m.r[1].y}}}; }
+
+// RotationMatrix::from(Angle) (angle.rs:120-131); false when |theta| >= 2^20.
+__device__ __forceinline__ bool mat2_from_angle(double theta, M2* m) {
+    double s, c;
+    if (!cr_sincos(theta, &s, &c)) return false;
+    *m = {{{c, -s}, {s, c}}};
+    return true;
+}
+
+// ConvexPolytope::support_mapping in 2-D: argmax of v0 n0 + v1 n1, first maximum wins.
+__device__ __forceinline__ V2 support2(const double4* __restrict__ verts, uint32_t nv, const V2& n) {
+    uint32_t arg = 0;
+    double best = -INFINITY;
+    for (uint32_t i = 0; i < nv; ++i) {
+        const double4 v = ldg4(verts + i);
+        const double x = dadd(dmul(v.x, n.x), dmul(v.y, n.y));
+        if (x > best) {
+            best = x;
+            arg = i;
+        }
+    }
+    const double4 v = ldg4(verts + arg);
+    return {v.x, v.y};
+}
+
+constexpr int kXenoMaxIter2 = 1024;  // xenocollide.rs:38
+
+// collide for N = 2 (xenocollide.rs:92-154, :361-414); the iteration cap returns overlap.
+__device__ bool collide2d(const double4* verts, uint32_t nv, const V2& vij, const M2& q) {
+    const M2 qinv = transpose2(q);
+    // composite_support_mapping (xenocollide.rs:318-328)
+    auto s = [&](const V2& n) -> V2 {
+        const V2 sb = support2(verts, nv, mat2_rotate(qinv, n));
+        V2 r = mat2_rotate(q, sb);
+        r = {dadd(r.x, vij.x), dadd(r.y, vij.y)};
+        const V2 sa = support2(verts, nv, V2{-n.x, -n.y});
+        return sub2(r, sa);
+    };
+    const double TOL = 1e-16;
+    const V2 v0 = vij;
+    const V2 v1 = s(V2{-v0.x, -v0.y});
+    V2 vp = perp2(sub2(v1, v0));
+    if (dot2(v1, vp) > 0.0) vp = {-vp.x, -vp.y};
+    const V2 v2 = s(vp);
+    V2 p0 = v1, p1 = v2;
+    for (int count = 1;; ++count) {
+        V2 nn = perp2(sub2(p1, p0));
+        if (dot2(sub2(p0, v0), nn) < 0.0) nn = {-nn.x, -nn.y};
+        if (dot2(p0, nn) >= 0.0) return true;
+        const V2 vnew = s(nn);
+        if (dot2(vnew, nn) < 0.0) return false;
+        // tolerance_check (:127-138): d = w - project(w, e), w = vnew - p0, e = p1 - p0
+        const V2 w = sub2(vnew, p0);
+        const V2 e = sub2(p1, p0);
+        const double kk = dot2(w, e);
+        const double nb = dot2(e, e);
+        const V2 pr{ddiv(dmul(e.x, kk), nb), ddiv(dmul(e.y, kk), nb)};
+        const V2 d = sub2(w, pr);
+        if (dot2(d, d) < dmul(TOL, dot2(vnew, vnew))) return true;
+        // narrow_portal (:141-154)
+        V2 vpp = perp2(sub2(vnew, v0));
+        if (dot2(sub2(p0, vnew), vpp) < 0.0) vpp = {-vpp.x, -vpp.y};
+        if (dot2(vnew, vpp) < 0.0)
+            p1 = vnew;
+        else
+            p0 = vnew;
+        if (count >= kXenoMaxIter2) return true;
+    }
+}
+
+// is_separating (convex_surface_mesh_2d.rs:625-640): every vertex of a strictly outside.
+__device__ __forceinline__ bool is_separating(const double4* verts, uint32_t nv, const V2& p, const V2& n) {
+    const double n_dot_p = dot2(n, p);
+    for (uint32_t i = 0; i < nv; ++i) {
+        const double4 v = ldg4(verts + i);
+        if (dsub(dot2(n, V2{v.x, v.y}), n_dot_p) <= 0.0) return false;
+    }
+    return true;
+}
+// b_edge_separates (:597-623) with a = b = the shape.
+__device__ __forceinline__ bool b_edge_separates(const double4* verts, uint32_t nv, const V2& v_ab, const M2& o_b) {
+    uint32_t previous = nv - 1;
+    for (uint32_t current = 0; current < nv; ++current) {
+        const double4 pc = ldg4(verts + current), pp = ldg4(verts + previous);
+        const V2 p{pc.x, pc.y};
+        const V2 edge = sub2(p, V2{pp.x, pp.y});
+        const V2 n{edge.y, -edge.x};  // -edge.perpendicular()
+        V2 pa = mat2_rotate(o_b, p);
+        pa = {dadd(pa.x, v_ab.x), dadd(pa.y, v_ab.y)};
+        const V2 na = mat2_rotate(o_b, n);
+        if (is_separating(verts, nv, pa, na)) return true;
+        previous = current;
+    }
+    return false;
+}
+// ConvexSurfaceMesh2d::intersects_at (:578-593).
+__device__ bool sat_intersects(const double4* verts, uint32_t nv, const V2& v_ij, const M2& o_j) {
+    if (b_edge_separates(verts, nv, v_ij, o_j)) return false;
+    const M2 inv = transpose2(o_j);
+    const V2 v_ji = mat2_rotate(inv, V2{-v_ij.x, -v_ij.y});
+    return !b_edge_separates(verts, nv, v_ji, inv);
+}
+
+struct PolyShape2 {
+    const double4* verts;
+    uint32_t nv;
+    double rcut2;      // (R_a + R_b)^2
+    float rcut2_hi32;  // FP32 threshold: at or above this, outside the circumcircles for certain
+};
+
+// Trial site t with angle ti against slot q's site sj (image rule) and angle: the pair test of
+// HardShape::site_pair_energy. *range_error is set when an angle is beyond the supported
+// range of cr_sincos; the pair then counts as overlapping (the move is rejected).
+template <bool SAT>
+__device__ __forceinline__ bool poly2_overlap64(const Geometry& g, const Arrays& A, const PolyShape2& sh,
+                                                const double* t, double ti, const double* sj, uint32_t q,
+                                                bool* range_error) {
+    double d[3];
+    const double d2 = ref_disp<2>(g, t, sj, d);
+    if (d2 >= sh.rcut2) return false;  // r_self.distance_squared(r_other) >= r_cut^2
+    const V2 rab{-d[0], -d[1]};  // image - t
+    const double tj = __ldg(&A.sorted_q[q].x);
+    const double inv = -ti;  // Angle::inverted
+    double sn, cs;
+    M2 m;
+    if (!cr_sincos(inv, &sn, &cs) || !mat2_from_angle(dadd(inv, tj), &m)) {
+        *range_error = true;
+        return true;
+    }
+    const V2 vij{dsub(dmul(rab.x, cs), dmul(rab.y, sn)), dadd(dmul(rab.x, sn), dmul(rab.y, cs))};  // Angle::rotate
+    return SAT ? sat_intersects(sh.verts, sh.nv, vij, m) : collide2d(sh.verts, sh.nv, vij, m);
+}
+
+__device__ __forceinline__ bool warp_any2(bool v) { return __any_sync(0xffffffffu, v); }
+
+// Overlap of the trial (t, ti) with any candidate of the 3 stencil rows around space m,
+// skipping slot self; lanes stride along each row, a vote after every stride step.
+template <bool FP32, bool SAT>
+__device__ __forceinline__ bool poly2_overlaps(const Geometry& g, const Arrays& A, const PolyShape2& sh,
+                                               const double* t, double ti, float4 t32, const uint32_t* m,
+                                               uint32_t self, uint32_t lane, PairStats& st, bool* range_error) {
+    const uint32_t sf = g.shape[1];
+    const int mf = (int)m[1];
+    for (int i0 = (g.shape[0] == 2 ? 0 : -1); i0 <= 1; ++i0) {
+        const uint32_t base = wrap_index((int)m[0] + i0, g.shape[0]) * sf;
+        uint32_t seg_lo[2], seg_hi[2];
+        uint32_t lo, hi;
+        row_span(sf, (uint32_t)mf, &lo, &hi);
+        seg_lo[0] = __ldg(A.cell_start + base + lo);
+        seg_hi[0] = __ldg(A.cell_start + base + hi);
+        seg_lo[1] = seg_hi[1] = 0;
+        int mfx[2] = {mf, mf};
+        if (sf > 2 && (mf == 0 || mf + 1 == (int)sf)) {
+            const uint32_t wlo = mf == 0 ? sf - 1u : 0u;
+            seg_lo[1] = __ldg(A.cell_start + base + wlo);
+            seg_hi[1] = __ldg(A.cell_start + base + wlo + 1u);
+            mfx[1] = mf == 0 ? (int)sf : -1;  // gives the wrapped space the cell shift -1 or +1
+        }
+        const float s0 = (float)i0 * g.w32[0];
+        for (int seg = 0; seg < 2; ++seg) {
+            for (uint32_t q0 = seg_lo[seg]; q0 < seg_hi[seg]; q0 += 32) {
+                const uint32_t q = q0 + lane;
+                bool hit = false;
+                if (q < seg_hi[seg] && q != self) {
+                    bool test = true;
+                    if (FP32) {
+                        const float4 o = __ldg(A.sorted_off + q);
+                        st.checks++;
+                        test = fp32_dist2<2>(g, t32, o, s0, 0.f, __float_as_int(o.w) - mfx[seg]) < sh.rcut2_hi32;
+                        if (test) st.rechecks++;
+                    }
+                    if (test) {
+                        double sj[3];
+                        if (FP32) {
+                            const double4 b4 = ldg4(A.sorted_b + q);
+                            sj[0] = b4.x;
+                            sj[1] = b4.y;
+                            sj[2] = 0.0;
+                            wrap_inv<2>(g.L, g.invL, sj);
+                        } else {
+                            const double4 s4 = ldg4(A.sorted_s + q);
+                            sj[0] = s4.x;
+                            sj[1] = s4.y;
+                            sj[2] = 0.0;
+                            st.checks++;
+                        }
+                        hit = poly2_overlap64<SAT>(g, A, sh, t, ti, sj, q, range_error);
+                    }
+                }
+                if (warp_any2(hit)) return true;
+            }
+        }
+    }
+    return false;
+}
+
+template <bool FP32, bool SAT>
+__global__ void __launch_bounds__(128) k_sweep_poly2(Geometry g, Arrays A, PolyShape2 sh, Launch L, uint32_t rotate) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t n_warps = (gridDim.x * blockDim.x) >> 5;
+    uint32_t n_accepted = 0;
+    PairStats st;
+    bool range_error = false;
+    for (uint32_t w = warp; w < L.n_active; w += n_warps) {
+        uint32_t m[3] = {0, 0, 0};
+        unpack_m<2>(__ldg(A.color_cells + (size_t)L.color * g.color_stride + w), m);
+        const uint32_t cell = cell_index<2>(g, m);
+        const uint32_t start = __ldg(A.cell_start + cell);
+        const uint32_t count = __ldg(A.cell_start + cell + 1) - start;
+        Sfc64 rng = make_rng(L.step, L.substep, L.seed, (uint64_t)cell);
+        const uint32_t k = start + canon_range_u32(rng, count);
+        const double4 b4 = A.sorted_b[k];
+        double x[3] = {b4.x, b4.y, 0.0};
+        double ti = A.sorted_q[k].x;
+        if (rotate) {
+            // Rotate<Angle>::propose (rotate/angle.rs:46-55): theta += Uniform(-a, a)
+            const double u = dsub(as_double(0x3FF0000000000000ULL | (rng.next_u64() >> 12)), 1.0);
+            ti = dadd(ti, dadd(dmul(u, dsub(L.max_move, -L.max_move)), -L.max_move));
+        } else {
+            double dv[3];
+            ball_sample<2>(rng, L.max_move, A.zig_x, A.zig_f, dv);
+            x[0] = dadd(x[0], dv[0]);
+            x[1] = dadd(x[1], dv[1]);
+        }
+        wrap_inv<2>(g.L, g.invL, x);  // W1 = wrap(propose(..))
+        uint32_t mt[3];
+        if (!(point_to_space<2>(g, x, mt) && cell_index<2>(g, mt) == cell)) continue;
+        double t[3] = {x[0], x[1], 0.0};
+        wrap_inv<2>(g.L, g.invL, t);
+        const float4 t32 = FP32 ? cell_offsets<2>(g, t, m) : make_float4(0.f, 0.f, 0.f, 0.f);
+        if (poly2_overlaps<FP32, SAT>(g, A, sh, t, ti, t32, m, k, lane, st, &range_error)) continue;
+        if (lane == 0) {
+            n_accepted++;
+            double sv[3] = {t[0], t[1], 0.0};
+            wrap_inv<2>(g.L, g.invL, sv);
+            const uint32_t body = A.sorted_body[k];
+            A.sorted_b[k] = make_double4(t[0], t[1], 0.0, 0.0);
+            if (!FP32) A.sorted_s[k] = make_double4(sv[0], sv[1], 0.0, 0.0);
+            A.sorted_off[k] = cell_offsets<2>(g, sv, m);
+            A.sorted_q[k] = make_double4(ti, 0.0, 0.0, 0.0);
+            A.body_pos[body] = make_double4(t[0], t[1], 0.0, 0.0);
+            A.body_ori[body] = make_double4(ti, 0.0, 0.0, 0.0);
+        }
+        __syncwarp();
+    }
+    if (range_error) atomicOr(&A.stats->error_flags, kErrAngleRange);
+    flush_stats(A.stats, st, n_accepted);
+}
+
+// Injected moves (position and angle): warp per move.
+template <bool FP32, bool SAT>
+__global__ void __launch_bounds__(128) k_eval_poly2(Geometry g, Arrays A, PolyShape2 sh, const uint64_t* bodies,
+                                                    const double4* trial, const double4* trial_q, uint32_t n,
+                                                    uint8_t* decisions) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    PairStats st;
+    bool range_error = false;
+    if (i < n) {
+        const uint32_t k = A.slot_of_body[bodies[i]];
+        const double4 w4 = trial[i];
+        double t[3] = {w4.x, w4.y, 0.0};
+        wrap_inv<2>(g.L, g.invL, t);
+        const double ti = trial_q[i].x;
+        uint32_t m[3] = {0, 0, 0};
+        uint8_t dec = 0;
+        if (point_to_space<2>(g, t, m)) {
+            const float4 t32 = FP32 ? cell_offsets<2>(g, t, m) : make_float4(0.f, 0.f, 0.f, 0.f);
+            dec = poly2_overlaps<FP32, SAT>(g, A, sh, t, ti, t32, m, k, lane, st, &range_error) ? 0 : 1;
+        } else if (lane == 0) {
+            atomicOr(&A.stats->error_flags, kErrOutsideCheckerboard);
+        }
+        if (lane == 0) decisions[i] = dec;
+    }
+    if (range_error) atomicOr(&A.stats->error_flags, kErrAngleRange);
+    flush_stats(A.stats, st, 0u);
+}
+
+// Overlapping pairs (i < j), FP64 (the overlap check of total_energy).
+template <bool SAT>
+__global__ void k_overlap_poly2(Geometry g, Arrays A, PolyShape2 sh, uint32_t n) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t found = 0;
+    bool range_error = false;
+    if (k < n) {
+        const uint32_t bi = A.sorted_body[k];
+        const double4 s4 = A.sorted_s[k];
+        const double t[3] = {s4.x, s4.y, 0.0};
+        const double ti = A.sorted_q[k].x;
+        uint32_t m[3] = {0, 0, 0};
+        uint32_t c = A.body_cell[bi];
+        m[1] = c % g.shape[1];
+        m[0] = c / g.shape[1];
+        for_each_neighbor<2>(g, A.cell_start, m, [&](uint32_t q, const float*) -> bool {
+            if (A.sorted_body[q] <= bi) return false;
+            const double4 o4 = A.sorted_s[q];
+            const double sj[3] = {o4.x, o4.y, 0.0};
+            if (poly2_overlap64<SAT>(g, A, sh, t, ti, sj, q, &range_error)) found++;
+            return false;
+        });
+    }
+    if (range_error) atomicOr(&A.stats->error_flags, kErrAngleRange);
+    const unsigned tot = __reduce_add_sync(0xffffffffu, found);
+    if ((threadIdx.x & 31) == 0 && tot) atomicAdd(&A.stats->overlaps, (unsigned long long)tot);
+}
+
+// cr_sincos over an array (the exact values the rotation path uses).
+__global__ void k_sincos(const double* x, uint64_t n, double* s, double* c, uint32_t* bad) {
+    const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double sv = 0.0, cv = 0.0;
+    if (!cr_sincos(x[i], &sv, &cv)) {
+        atomicOr(bad, 1u);
+        sv = cv = NAN;
+    }
+    s[i] = sv;
+    c[i] = cv;
+}
+
+}  // namespace
+
+cudaError_t launch_sweep_poly2(bool fp32, bool sat, const Geometry& g, const Arrays& a, const double4* verts,
+                               uint32_t nv, double rcut2, float rcut2_hi32, const Launch& l, bool rotate,
+                               cudaStream_t s) {
+    if (l.n_active == 0) return cudaSuccess;
+    static int max_blocks = 0;
+    if (max_blocks == 0) {
+        int dev = 0, sms = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        max_blocks = sms * 16;
+    }
+    PolyShape2 sh{verts, nv, rcut2, rcut2_hi32};
+    uint32_t blocks = (l.n_active + 3) / 4;
+    if (blocks > (uint32_t)max_blocks) blocks = (uint32_t)max_blocks;
+    const uint32_t rot = rotate ? 1u : 0u;
+    if (fp32) {
+        if (sat)
+            k_sweep_poly2<true, true><<<blocks, 128, 0, s>>>(g, a, sh, l, rot);
+        else
+            k_sweep_poly2<true, false><<<blocks, 128, 0, s>>>(g, a, sh, l, rot);
+    } else {
+        if (sat)
+            k_sweep_poly2<false, true><<<blocks, 128, 0, s>>>(g, a, sh, l, rot);
+        else
+            k_sweep_poly2<false, false><<<blocks, 128, 0, s>>>(g, a, sh, l, rot);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_eval_poly2(bool fp32, bool sat, const Geometry& g, const Arrays& a, const double4* verts,
+                              uint32_t nv, double rcut2, float rcut2_hi32, const uint64_t* bodies,
+                              const double4* trial, const double4* trial_q, uint32_t n, uint8_t* decisions,
+                              cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    PolyShape2 sh{verts, nv, rcut2, rcut2_hi32};
+    const uint32_t blocks = (n + 3) / 4;
+    if (fp32) {
+        if (sat)
+            k_eval_poly2<true, true><<<blocks, 128, 0, s>>>(g, a, sh, bodies, trial, trial_q, n, decisions);
+        else
+            k_eval_poly2<true, false><<<blocks, 128, 0, s>>>(g, a, sh, bodies, trial, trial_q, n, decisions);
+    } else {
+        if (sat)
+            k_eval_poly2<false, true><<<blocks, 128, 0, s>>>(g, a, sh, bodies, trial, trial_q, n, decisions);
+        else
+            k_eval_poly2<false, false><<<blocks, 128, 0, s>>>(g, a, sh, bodies, trial, trial_q, n, decisions);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_overlap_poly2(bool sat, const Geometry& g, const Arrays& a, const double4* verts, uint32_t nv,
+                                 double rcut2, uint32_t n, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    PolyShape2 sh{verts, nv, rcut2, 0.f};
+    if (sat)
+        k_overlap_poly2<true><<<(n + 127) / 128, 128, 0, s>>>(g, a, sh, n);
+    else
+        k_overlap_poly2<false><<<(n + 127) / 128, 128, 0, s>>>(g, a, sh, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sincos(const double* x, uint64_t n, double* sn, double* cs, uint32_t* bad, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    k_sincos<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(x, n, sn, cs, bad);
+    return cudaGetLastError();
+}
+
+}  // namespace hmc

@@ -65,7 +65,9 @@ typedef enum hmc_interaction {
     HMC_HARD_SPHERE = 0,            /* PairwiseCutoff(HardSphere { diameter }) */
     HMC_HARD_CONVEX_POLYGON = 1,    /* PairwiseCutoff(HardShape(Convex(ConvexPolygon))) */
     HMC_HARD_CONVEX_POLYHEDRON = 2, /* PairwiseCutoff(HardShape(Convex(ConvexPolyhedron))) */
-    HMC_LENNARD_JONES = 3           /* PairwiseCutoff(Isotropic { Shifted { LennardJones }, r_cut }) */
+    HMC_LENNARD_JONES = 3,          /* PairwiseCutoff(Isotropic { Shifted { LennardJones }, r_cut }) */
+    HMC_HARD_CONVEX_SURFACE_MESH_2D = 4 /* PairwiseCutoff(HardShape(ConvexSurfaceMesh2d)): vertices are
+                                           the counter-clockwise hull (convex_surface_mesh_2d.rs) */
 } hmc_interaction;
 
 typedef enum hmc_move {
@@ -96,7 +98,7 @@ typedef struct hmc_system_desc {
     uint32_t substep;            /* Counter substep */
     uint32_t seed;               /* Counter seed */
     uint32_t interaction;        /* hmc_interaction */
-    uint32_t n_vertices;         /* convex polytope vertex count (<= 32) */
+    uint32_t n_vertices;         /* convex polytope vertex count (<= 32; polygons >= 3) */
     const double* vertices;      /* n_vertices * dim, FP64 */
     double diameter;             /* HardSphere */
     double lj_epsilon, lj_sigma, lj_r_cut, lj_r_shift; /* Isotropic<Shifted<LennardJones>> */
@@ -130,6 +132,9 @@ typedef struct hmc_injected_move {
     double orientation[4];   /* trial versor (s, x, y, z) or angle in [0] */
     double u;                /* the Metropolis uniform in [0, 1); ignored for hard shapes */
 } hmc_injected_move;
+
+/* 2-D orientations are angles (Angle, hoomd-vector angle.rs) with |theta| < 2^19; the
+ * rotation path turns them into matrices with correctly rounded sin and cos. */
 
 /* Device-time profile of a system's kernels, collected with CUDA events on the system's
  * stream while profiling is enabled. */
@@ -208,6 +213,11 @@ hmc_status hmc_overlap_count_noalloc(const double* positions, uint64_t n_bodies,
                                      uint64_t* overlaps, void* cuda_stream);
 
 /* ---- profiling ---- */
+/* The correctly rounded sin and cos that the 2-D rotation path uses (on the context's device);
+ * no counterpart in the reference, which calls the platform libm (hoomd-vector angle.rs:120-150).
+ * HMC_INVALID_ARGUMENT when some |x[i]| >= 2^20. */
+hmc_status hmc_math_sincos(hmc_context* ctx, const double* x, uint64_t n, double* sin_out, double* cos_out);
+
 hmc_status hmc_profile_enable(hmc_system* sys, int enable);
 hmc_status hmc_profile_read(hmc_system* sys, hmc_profile* out, int reset);
 
