@@ -96,6 +96,13 @@ SIGNATURES = {
     "hmc_get_state": (C.c_int, [_vp, _dp, _dp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32)]),
     "hmc_increment_step": (C.c_int, [_vp]),
     "hmc_math_sincos": (C.c_int, [_vp, _dp, C.c_uint64, _dp, _dp]),
+    "hmc_batch_create": (C.c_int, [_vp, C.c_uint32, C.POINTER(hmc_system_desc), C.POINTER(_dp), C.POINTER(_vp)]),
+    "hmc_batch_destroy": (None, [_vp]),
+    "hmc_batch_sweep": (C.c_int, [_vp, C.POINTER(hmc_sweep_params), C.POINTER(hmc_count), C.POINTER(hmc_count)]),
+    "hmc_batch_get_state": (C.c_int, [_vp, C.c_uint32, _dp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32)]),
+    "hmc_batch_set_state": (C.c_int, [_vp, C.c_uint32, _dp, C.c_uint64, C.c_uint32]),
+    "hmc_batch_overlap_check": (C.c_int, [_vp, C.POINTER(C.c_uint64)]),
+    "hmc_batch_kernel_launches": (C.c_uint64, [_vp]),
     "hmc_sweep": (C.c_int, [_vp, C.POINTER(hmc_sweep_params), C.POINTER(hmc_count)]),
     "hmc_tune": (C.c_int, [_vp, C.POINTER(hmc_sweep_params), C.c_double, C.c_uint32, C.c_uint32]),
     "hmc_overlap_check": (C.c_int, [_vp, C.POINTER(C.c_uint64)]),
@@ -508,6 +515,86 @@ class Microstate:
         return e.value
 
 
+class Batch:
+    """Independent hard-sphere replicas swept together (hmc_batch_*): one counting sort and one
+    kernel per colour pass for all replicas. Replica k evolves exactly as a Microstate built
+    from the same (boundary, positions, diameter, seed, step, substep) would."""
+
+    def __init__(self, ctx: Context, replicas):
+        """replicas: dicts with keys boundary (Periodic), positions, diameter (default 1),
+        seed, step, substep (default 0)."""
+        lib = load_library()
+        self.n_replicas = len(replicas)
+        descs = (hmc_system_desc * self.n_replicas)()
+        self._pos = []
+        self.dim = len(replicas[0]["boundary"].edge_lengths)
+        self.sizes = []
+        for k, r in enumerate(replicas):
+            L = [float(x) for x in r["boundary"].edge_lengths]
+            pos = np.ascontiguousarray(r["positions"], dtype=np.float64).reshape(-1, len(L))
+            self._pos.append(pos)
+            self.sizes.append(pos.shape[0])
+            d = descs[k]
+            d.struct_size = C.sizeof(hmc_system_desc)
+            d.dim = len(L)
+            for a, x in enumerate(L):
+                d.edge_lengths[a] = x
+            d.n_bodies = pos.shape[0]
+            d.step, d.substep, d.seed = r.get("step", 0), r.get("substep", 0), r.get("seed", 0)
+            d.interaction = HARD_SPHERE
+            d.diameter = r.get("diameter", 1.0)
+            d.boundary_range = r["boundary"].maximum_interaction_range
+        ptrs = (_dp * self.n_replicas)(*[p.ctypes.data_as(_dp) for p in self._pos])
+        h = _vp()
+        _check(lib.hmc_batch_create(ctx._h, self.n_replicas, descs, ptrs, C.byref(h)))
+        self._h = h
+        self.ctx = ctx
+
+    def sweep(self, maxima, precision: int = FP32_RECHECK, n_sweeps: int = 1, increment_step: bool = False):
+        """ParallelSweep::apply on every replica (replica k moves up to maxima[k]); returns
+        (per-replica Counts, batch total Count)."""
+        maxima = np.broadcast_to(np.asarray(maxima, dtype=np.float64), (self.n_replicas,))
+        ps = (hmc_sweep_params * self.n_replicas)()
+        for k in range(self.n_replicas):
+            ps[k] = hmc_sweep_params(C.sizeof(hmc_sweep_params), TRANSLATE, float(maxima[k]), 1.0, precision, n_sweeps,
+                                     int(increment_step), 0)
+        cs = (hmc_count * self.n_replicas)()
+        tot = hmc_count()
+        _check(_lib.hmc_batch_sweep(self._h, ps, cs, C.byref(tot)))
+        counts = [Count(c.accepted, c.rejected, 0, 0, 0.0) for c in cs]
+        return counts, Count(tot.accepted, tot.rejected, tot.rechecks, tot.pair_checks, tot.max_fp32_error)
+
+    def state(self, k: int):
+        pos = np.empty((self.sizes[k], self.dim))
+        step = C.c_uint64()
+        sub = C.c_uint32()
+        _check(_lib.hmc_batch_get_state(self._h, k, pos.ctypes.data_as(_dp), C.byref(step), C.byref(sub)))
+        return pos, step.value, sub.value
+
+    def positions(self, k: int) -> np.ndarray:
+        return self.state(k)[0]
+
+    def set_state(self, k: int, positions, step: int, substep: int):
+        pos = np.ascontiguousarray(positions, dtype=np.float64).reshape(self.sizes[k], self.dim)
+        _check(_lib.hmc_batch_set_state(self._h, k, pos.ctypes.data_as(_dp), step, substep))
+
+    def overlap_counts(self) -> np.ndarray:
+        out = np.zeros(self.n_replicas, dtype=np.uint64)
+        _check(_lib.hmc_batch_overlap_check(self._h, out.ctypes.data_as(C.POINTER(C.c_uint64))))
+        return out
+
+    def kernel_launches(self) -> int:
+        return int(_lib.hmc_batch_kernel_launches(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.hmc_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+
 @dataclass
 class TuneOptions:
     """hoomd_mc::TuneOptions (lib.rs:394-412)."""
@@ -557,7 +644,7 @@ class ParallelSweep:
             self.local_trial.maximum_rotation = tuned
 
 
-__all__ = ["Context", "ConvexPolygon", "ConvexPolyhedron", "ConvexSurfaceMesh2d", "Count", "convex_hull_2d", "HardShape", "HardSphere", "HmcError", "Isothermal", "Isotropic",
+__all__ = ["Batch", "Context", "ConvexPolygon", "ConvexPolyhedron", "ConvexSurfaceMesh2d", "Count", "convex_hull_2d", "HardShape", "HardSphere", "HmcError", "Isothermal", "Isotropic",
            "LennardJones", "Microstate", "PairwiseCutoff", "Rotate", "Shifted", "TuneOptions",
            "ParallelSweep", "Periodic", "Translate", "load_library", "SIGNATURES", "FP64", "FP32_RECHECK",
            "TRANSLATE", "ROTATE", "HARD_SPHERE", "HARD_CONVEX_POLYGON", "HARD_CONVEX_POLYHEDRON", "LENNARD_JONES",

@@ -122,20 +122,20 @@ hmc_status dalloc(hmc_system* s, T** p, size_t count) {
 // Near contact (d ~ sigma) the FP32 d^2 is within 2*E*sqrt(dim)*d + dim*E^2 + dim*u32*d^2
 // of the exact d^2, and the reference FP64 d^2 is within 6*u64*(L+w)*sqrt(dim)*d +
 // dim*u64*d^2 of it. A factor of two covers both and the rounding of the thresholds.
-void sphere_bound(hmc_system* s) {
+void sphere_bound_for(int dim, const Geometry& geom, Pair& pair) {
     const double u32 = std::ldexp(1.0, -24), u64 = std::ldexp(1.0, -53);
     double wmax = 0, Lmax = 0;
-    for (int a = 0; a < s->dim; ++a) {
-        wmax = std::max(wmax, s->geom.width[a]);
-        Lmax = std::max(Lmax, s->geom.L[a]);
+    for (int a = 0; a < dim; ++a) {
+        wmax = std::max(wmax, geom.width[a]);
+        Lmax = std::max(Lmax, geom.L[a]);
     }
-    double sigma2 = s->pair.sigma2;
+    double sigma2 = pair.sigma2;
     double sigma = std::sqrt(sigma2);
     double E = 8.0 * u32 * wmax + 16.0 * u64 * (Lmax + wmax);
-    double rd = std::sqrt((double)s->dim);
+    double rd = std::sqrt((double)dim);
     double dmax = sigma * 1.01 + 1e-3;
-    double b32 = 2.0 * E * rd * dmax + s->dim * E * E + s->dim * u32 * dmax * dmax;
-    double b64 = 6.0 * u64 * (Lmax + wmax) * rd * dmax + s->dim * u64 * dmax * dmax;
+    double b32 = 2.0 * E * rd * dmax + dim * E * E + dim * u32 * dmax * dmax;
+    double b64 = 6.0 * u64 * (Lmax + wmax) * rd * dmax + dim * u64 * dmax * dmax;
     double B = 2.0 * (b32 + b64);
     // HMC_B200_FP32_BAND_SCALE (>= 1) widens the band of FP32 distances that are decided in
     // FP64. Decisions do not change; it makes the recheck path common enough to test.
@@ -143,9 +143,11 @@ void sphere_bound(hmc_system* s) {
         double f = std::atof(e);
         if (f > 1.0 && f < 1e12) B *= f;
     }
-    s->pair.sig2_lo32 = std::nextafter((float)(sigma2 - B), -INFINITY);
-    s->pair.sig2_hi32 = std::nextafter((float)(sigma2 + B), INFINITY);
+    pair.sig2_lo32 = std::nextafter((float)(sigma2 - B), -INFINITY);
+    pair.sig2_hi32 = std::nextafter((float)(sigma2 + B), INFINITY);
 }
+
+void sphere_bound(hmc_system* s) { sphere_bound_for(s->dim, s->geom, s->pair); }
 
 // LennardJones::energy (lennard_jones.rs:107-111), the host copy of the device formula.
 double lj_energy_host(double four_eps, double sigma, double r) {
@@ -951,5 +953,384 @@ hmc_status hmc_eval_moves(hmc_system* s, const hmc_injected_move* moves, uint64_
     }
     return HMC_OK;
 }
+
+}  // extern "C"
+
+// ---- batches of independent hard-sphere replicas ------------------------------------------
+// Every replica is a full system of its own (box, checkerboard, Counter); the batch only
+// shares the device arrays and the launches, so each replica's trajectory equals that of an
+// hmc_system built from the same description.
+struct hmc_batch {
+    hmc_context* ctx = nullptr;
+    int dim = 3;
+    uint32_t n_rep = 0;
+    uint64_t n = 0;
+    uint32_t cells = 0;
+    std::vector<Replica> rep;          // host copies; uploaded through rep_pinned
+    Replica* rep_pinned = nullptr;
+    std::vector<uint32_t> cell_base;   // [R + 1]
+    std::vector<uint32_t> body_base;   // [R + 1]
+    Arrays arr{};
+    Batch b{};
+    double* stage = nullptr;
+    unsigned long long* first_bad = nullptr;
+    cudaStream_t stream = nullptr;
+    DeviceStats* host_stats = nullptr;  // pinned
+    unsigned long long* host_rep_u64 = nullptr;  // pinned [R]: accepted or overlaps
+    unsigned int* host_nonempty = nullptr;       // pinned [R]
+    unsigned long long* host_first_bad = nullptr;
+    std::vector<void*> allocations;
+    uint64_t kernel_launches = 0;
+};
+
+namespace {
+
+template <typename T>
+hmc_status balloc(hmc_batch* bt, T** p, size_t count) {
+    *p = nullptr;
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMalloc((void**)p, sizeof(T) * count);
+    if (e != cudaSuccess)
+        return fail(e == cudaErrorMemoryAllocation ? HMC_OUT_OF_MEMORY : HMC_CUDA_ERROR, "cudaMalloc(%zu bytes): %s",
+                    sizeof(T) * count, cudaGetErrorString(e));
+    bt->allocations.push_back((void*)*p);
+    return HMC_OK;
+}
+
+hmc_status batch_upload_replicas(hmc_batch* bt) {
+    std::memcpy(bt->rep_pinned, bt->rep.data(), sizeof(Replica) * bt->n_rep);
+    HMC_CUDA(cudaMemcpyAsync((void*)bt->b.rep, bt->rep_pinned, sizeof(Replica) * bt->n_rep, cudaMemcpyHostToDevice,
+                             bt->stream));
+    return HMC_OK;
+}
+
+// update_checkerboard for every replica (its own Counter), then the batched counting sort.
+hmc_status batch_rebuild(hmc_batch* bt, bool write_s) {
+    for (Replica& r : bt->rep) {
+        Sfc64 rng = make_rng(r.step, r.substep, r.seed, UINT64_MAX);
+        for (int a = 0; a < bt->dim; ++a) {
+            double off = uniform01(rng);
+            r.g.origin[a] = -r.g.L[a] / 2.0 - off * r.g.width[a];
+        }
+    }
+    hmc_status st = batch_upload_replicas(bt);
+    if (st) return st;
+    HMC_CUDA(cudaMemsetAsync(bt->arr.stats, 0, sizeof(DeviceStats), bt->stream));
+    HMC_CUDA(launch_rebuild_batch(bt->dim, bt->b, bt->arr, (uint32_t)bt->n, write_s, bt->stream));
+    bt->kernel_launches += bt->n > 0 ? 6 : 4;
+    HMC_CUDA(cudaMemcpyAsync(bt->host_stats, bt->arr.stats, sizeof(DeviceStats), cudaMemcpyDeviceToHost, bt->stream));
+    HMC_CUDA(cudaMemcpyAsync(bt->host_nonempty, bt->b.nonempty, sizeof(unsigned int) * bt->n_rep,
+                             cudaMemcpyDeviceToHost, bt->stream));
+    HMC_CUDA(cudaStreamSynchronize(bt->stream));
+    const uint32_t f = bt->host_stats->error_flags;
+    if (f & kErrNonFinite) return fail(HMC_NAN_STATE, "a body position is not finite");
+    if (f & kErrOutsideCheckerboard) return fail(HMC_OUTSIDE_CHECKERBOARD, "a body maps to no checkerboard space");
+    return HMC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void hmc_batch_destroy(hmc_batch* bt) {
+    if (!bt) return;
+    cudaSetDevice(bt->ctx->device);
+    if (bt->stream) cudaStreamSynchronize(bt->stream);
+    for (void* p : bt->allocations) cudaFree(p);
+    if (bt->rep_pinned) cudaFreeHost(bt->rep_pinned);
+    if (bt->host_stats) cudaFreeHost(bt->host_stats);
+    if (bt->host_rep_u64) cudaFreeHost(bt->host_rep_u64);
+    if (bt->host_nonempty) cudaFreeHost(bt->host_nonempty);
+    if (bt->host_first_bad) cudaFreeHost(bt->host_first_bad);
+    if (bt->stream) cudaStreamDestroy(bt->stream);
+    cudaGetLastError();
+    hmc_context* c = bt->ctx;
+    delete bt;
+    context_release(c);
+}
+
+hmc_status hmc_batch_create(hmc_context* ctx, uint32_t n_replicas, const hmc_system_desc* descs,
+                            const double* const* positions, hmc_batch** out) {
+    if (!ctx || !descs || !positions || !out) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
+    *out = nullptr;
+    if (n_replicas == 0 || n_replicas > 65535) return fail(HMC_INVALID_ARGUMENT, "1 to 65535 replicas");
+    const uint32_t dim = descs[0].dim;
+    uint64_t n_total = 0, cells_total = 0;
+    std::vector<Replica> reps(n_replicas);
+    for (uint32_t k = 0; k < n_replicas; ++k) {
+        const hmc_system_desc* d = descs + k;
+        if (d->struct_size < sizeof(hmc_system_desc)) return fail(HMC_INVALID_ARGUMENT, "replica %u: struct_size", k);
+        if (d->dim != dim || (dim != 2 && dim != 3))
+            return fail(HMC_INVALID_ARGUMENT, "replica %u: all replicas need the same dim, 2 or 3", k);
+        if (d->interaction != HMC_HARD_SPHERE)
+            return fail(HMC_NOT_SUPPORTED, "replica %u: batches hold hard spheres", k);
+        if (!(d->diameter > 0.0)) return fail(HMC_INVALID_ARGUMENT, "replica %u: diameter must be positive", k);
+        if (d->n_bodies > 0 && !positions[k]) return fail(HMC_INVALID_ARGUMENT, "replica %u: positions is NULL", k);
+        for (uint32_t a = 0; a < dim; ++a)
+            if (!(d->edge_lengths[a] > 0.0) || !std::isfinite(d->edge_lengths[a]))
+                return fail(HMC_INVALID_ARGUMENT, "replica %u: edge length %u must be positive", k, a);
+        for (uint64_t i = 0; i < d->n_bodies * dim; ++i)
+            if (!std::isfinite(positions[k][i]))
+                return fail(HMC_NAN_STATE, "replica %u: position %llu is not finite", k, (unsigned long long)(i / dim));
+        Replica& r = reps[k];
+        std::memset(&r, 0, sizeof(Replica));
+        const double pair_range = d->diameter;
+        const double boundary_range = d->boundary_range > 0.0 ? d->boundary_range : pair_range;
+        const double body_range = d->body_interaction_range > 0.0 ? d->body_interaction_range : pair_range;
+        double min_l = d->edge_lengths[0];
+        for (uint32_t a = 0; a < dim; ++a) {
+            r.g.L[a] = d->edge_lengths[a];
+            min_l = std::min(min_l, d->edge_lengths[a]);
+        }
+        for (uint32_t a = dim; a < 3; ++a) r.g.L[a] = 1.0;
+        if (boundary_range > min_l / 2.0)
+            return fail(HMC_RANGE_TOO_LARGE, "replica %u: boundary range %g exceeds L/2", k, boundary_range);
+        if (body_range < pair_range) return fail(HMC_INVALID_ARGUMENT, "replica %u: body range below the pair range", k);
+        if (!compute_dimensions((int)dim, r.g.L, body_range, r.g.width, r.g.shape))
+            return fail(HMC_RANGE_TOO_LARGE, "replica %u: fewer than 2 spaces per axis", k);
+        uint64_t cells = 1;
+        for (uint32_t a = 0; a < dim; ++a) {
+            if (r.g.shape[a] > (dim == 3 ? 1024u : 65535u))
+                return fail(HMC_NOT_SUPPORTED, "replica %u: too many spaces on axis %u", k, a);
+            r.g.half[a] = r.g.L[a] / 2.0;
+            r.g.ghost_hi[a] = r.g.half[a] - boundary_range;
+            r.g.ghost_lo[a] = -r.g.half[a] + boundary_range;
+            r.g.w32[a] = (float)r.g.width[a];
+            r.g.invL[a] = 1.0 / r.g.L[a];
+            r.g.invW[a] = 1.0 / r.g.width[a];
+            r.g.half_shape[a] = r.g.shape[a] / 2;
+            if (r.g.shape[a] == 2) r.g.any_two = 1;
+            cells *= r.g.shape[a];
+        }
+        r.g.n_cells = (uint32_t)cells;
+        r.g.color_stride = (uint32_t)(cells >> dim);
+        r.p.sigma2 = d->diameter * d->diameter;
+        sphere_bound_for((int)dim, r.g, r.p);
+        r.cell_base = (uint32_t)cells_total;
+        r.body_base = (uint32_t)n_total;
+        r.n_bodies = (uint32_t)d->n_bodies;
+        r.step = d->step;
+        r.substep = d->substep;
+        r.seed = d->seed;
+        n_total += d->n_bodies;
+        cells_total += cells;
+        if (n_total >= (1ull << 31)) return fail(HMC_INVALID_ARGUMENT, "too many bodies");
+        if (cells_total > 16000000ull) return fail(HMC_NOT_SUPPORTED, "more than 16M spaces in the batch");
+    }
+    HMC_CUDA(cudaSetDevice(ctx->device));
+    hmc_batch* bt = new hmc_batch();
+    ctx->refs.fetch_add(1);
+    bt->ctx = ctx;
+    bt->dim = (int)dim;
+    bt->n_rep = n_replicas;
+    bt->n = n_total;
+    bt->cells = (uint32_t)cells_total;
+    bt->rep = reps;
+    auto destroy_fail = [&](hmc_status st) {
+        std::string msg = g_last_error;
+        hmc_batch_destroy(bt);
+        g_last_error = msg;
+        return st;
+    };
+    bt->cell_base.resize(n_replicas + 1);
+    bt->body_base.resize(n_replicas + 1);
+    for (uint32_t k = 0; k < n_replicas; ++k) {
+        bt->cell_base[k] = reps[k].cell_base;
+        bt->body_base[k] = reps[k].body_base;
+    }
+    bt->cell_base[n_replicas] = bt->cells;
+    bt->body_base[n_replicas] = (uint32_t)n_total;
+    cudaError_t e = cudaStreamCreateWithFlags(&bt->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMallocHost((void**)&bt->rep_pinned, sizeof(Replica) * n_replicas);
+    if (e == cudaSuccess) e = cudaMallocHost((void**)&bt->host_stats, sizeof(DeviceStats));
+    if (e == cudaSuccess) e = cudaMallocHost((void**)&bt->host_rep_u64, sizeof(unsigned long long) * n_replicas);
+    if (e == cudaSuccess) e = cudaMallocHost((void**)&bt->host_nonempty, sizeof(unsigned int) * n_replicas);
+    if (e == cudaSuccess) e = cudaMallocHost((void**)&bt->host_first_bad, sizeof(unsigned long long));
+    if (e != cudaSuccess) {
+        fail(HMC_CUDA_ERROR, "batch setup: %s", cudaGetErrorString(e));
+        return destroy_fail(HMC_CUDA_ERROR);
+    }
+    const uint64_t n = n_total;
+    const uint32_t cells = bt->cells;
+    const uint32_t scan_blocks = (cells + 2047) / 2048;
+    Arrays& A = bt->arr;
+    Replica* d_rep = nullptr;
+    uint32_t *d_cell_base = nullptr, *d_body_rep = nullptr;
+    hmc_status st;
+    if ((st = balloc(bt, &A.body_pos, n)) || (st = balloc(bt, &A.sorted_b, n)) || (st = balloc(bt, &A.sorted_s, n)) ||
+        (st = balloc(bt, &A.sorted_off, n)) || (st = balloc(bt, &A.sorted_body, n)) ||
+        (st = balloc(bt, &A.slot_of_body, n)) || (st = balloc(bt, &A.body_cell, n)) ||
+        (st = balloc(bt, &A.body_rank, n)) || (st = balloc(bt, &A.cell_count, cells)) ||
+        (st = balloc(bt, &A.cell_start, (size_t)cells + 1)) || (st = balloc(bt, &A.block_sums, (size_t)scan_blocks * 9)) ||
+        (st = balloc(bt, &A.color_cells, cells)) || (st = balloc(bt, &A.stats, 1)) ||
+        (st = balloc(bt, &d_rep, n_replicas)) || (st = balloc(bt, &d_cell_base, (size_t)n_replicas + 1)) ||
+        (st = balloc(bt, &d_body_rep, n)) || (st = balloc(bt, &bt->b.color_rep, cells)) ||
+        (st = balloc(bt, &bt->b.accepted, n_replicas)) || (st = balloc(bt, &bt->b.nonempty, n_replicas)) ||
+        (st = balloc(bt, &bt->b.overlaps, n_replicas)) || (st = balloc(bt, &bt->stage, n * dim)) ||
+        (st = balloc(bt, &bt->first_bad, 1)))
+        return destroy_fail(st);
+    A.body_ori = nullptr;
+    A.sorted_q = nullptr;
+    A.zig_x = ctx->zig;
+    A.zig_f = ctx->zig + kZigLayers + 1;
+    bt->b.rep = d_rep;
+    bt->b.cell_base = d_cell_base;
+    bt->b.body_rep = d_body_rep;
+    bt->b.n_replicas = n_replicas;
+    bt->b.n_cells = cells;
+    bt->b.color_stride = cells >> dim;
+    // Microstate::add_body (microstate.rs:777-835): each body keeps wrap(input).
+    std::vector<double4> host(n);
+    std::vector<uint32_t> host_rep(n);
+    for (uint32_t k = 0; k < n_replicas; ++k) {
+        for (uint32_t i = 0; i < reps[k].n_bodies; ++i) {
+            double pnt[3] = {0.0, 0.0, 0.0};
+            for (uint32_t a = 0; a < dim; ++a) pnt[a] = positions[k][(size_t)i * dim + a];
+            if (dim == 2)
+                wrap<2>(reps[k].g.L, pnt);
+            else
+                wrap<3>(reps[k].g.L, pnt);
+            host[reps[k].body_base + i] = make_double4(pnt[0], pnt[1], pnt[2], 0.0);
+            host_rep[reps[k].body_base + i] = k;
+        }
+    }
+    e = cudaMemcpy(A.body_pos, host.data(), sizeof(double4) * n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d_body_rep, host_rep.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(d_cell_base, bt->cell_base.data(), sizeof(uint32_t) * (n_replicas + 1), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        fail(HMC_CUDA_ERROR, "upload: %s", cudaGetErrorString(e));
+        return destroy_fail(HMC_CUDA_ERROR);
+    }
+    *out = bt;
+    return HMC_OK;
+}
+
+hmc_status hmc_batch_sweep(hmc_batch* bt, const hmc_sweep_params* params, hmc_count* counts, hmc_count* total) {
+    if (!bt || !params) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
+    const hmc_sweep_params& p0 = params[0];
+    if (p0.struct_size < sizeof(hmc_sweep_params)) return fail(HMC_INVALID_ARGUMENT, "hmc_sweep_params.struct_size");
+    if (p0.move != HMC_TRANSLATE) return fail(HMC_NOT_SUPPORTED, "hard spheres take translation moves");
+    if (p0.precision > HMC_FP32_RECHECK) return fail(HMC_INVALID_ARGUMENT, "precision");
+    for (uint32_t k = 0; k < bt->n_rep; ++k) {
+        const hmc_sweep_params& p = params[k];
+        if (p.move != p0.move || p.precision != p0.precision || p.n_sweeps != p0.n_sweeps ||
+            p.increment_step != p0.increment_step)
+            return fail(HMC_INVALID_ARGUMENT, "replica %u: move, precision, n_sweeps and increment_step must agree", k);
+        double lmax = 0.0;
+        for (int a = 0; a < bt->dim; ++a) lmax = std::max(lmax, bt->rep[k].g.L[a]);
+        if (!(p.maximum > 0.0) || !(p.maximum <= 4.0 * lmax))
+            return fail(HMC_INVALID_ARGUMENT, "replica %u: maximum must be in (0, 4 box lengths]", k);
+        bt->rep[k].max_move = p.maximum;
+    }
+    HMC_CUDA(cudaSetDevice(bt->ctx->device));
+    const bool fp32 = p0.precision == HMC_FP32_RECHECK;
+    const uint32_t colors = 1u << bt->dim;
+    if (counts) std::memset(counts, 0, sizeof(hmc_count) * bt->n_rep);
+    hmc_count tot{};
+    for (uint32_t sweep = 0; sweep < p0.n_sweeps; ++sweep) {
+        hmc_status st = batch_rebuild(bt, !fp32);
+        if (st) return st;
+        uint32_t max_rounds = 0;
+        for (uint32_t k = 0; k < bt->n_rep; ++k) {
+            Replica& r = bt->rep[k];
+            const uint32_t ne = bt->host_nonempty[k];
+            r.rounds = (r.n_bodies == 0 || ne == 0) ? 0u : (r.n_bodies + ne - 1) / ne;
+            max_rounds = std::max(max_rounds, r.rounds);
+        }
+        if ((st = batch_upload_replicas(bt))) return st;
+        HMC_CUDA(cudaMemsetAsync(bt->b.accepted, 0, sizeof(unsigned long long) * bt->n_rep, bt->stream));
+        uint32_t color_count[8];
+        for (uint32_t c = 0; c < colors; ++c) color_count[c] = bt->host_stats->color_count[c];
+        for (uint32_t round = 0; round < max_rounds; ++round)
+            for (uint32_t c = 0; c < colors; ++c) {
+                HMC_CUDA(launch_sweep_batch(bt->dim, fp32, bt->b, bt->arr, c, round, color_count[c], bt->stream));
+                bt->kernel_launches += 1;
+            }
+        HMC_CUDA(cudaMemcpyAsync(bt->host_rep_u64, bt->b.accepted, sizeof(unsigned long long) * bt->n_rep,
+                                 cudaMemcpyDeviceToHost, bt->stream));
+        HMC_CUDA(cudaMemcpyAsync(bt->host_stats, bt->arr.stats, sizeof(DeviceStats), cudaMemcpyDeviceToHost, bt->stream));
+        HMC_CUDA(cudaStreamSynchronize(bt->stream));
+        for (uint32_t k = 0; k < bt->n_rep; ++k) {
+            Replica& r = bt->rep[k];
+            const uint64_t acc = bt->host_rep_u64[k];
+            const uint64_t trials = (uint64_t)r.rounds * bt->host_nonempty[k];
+            if (counts) {
+                counts[k].accepted += acc;
+                counts[k].rejected += trials - acc;
+            }
+            tot.accepted += acc;
+            tot.rejected += trials - acc;
+            r.substep += r.rounds;  // increment_substep after every full colour set
+            if (p0.increment_step) {
+                r.step += 1;
+                r.substep = 0;
+            }
+        }
+        tot.rechecks += bt->host_stats->rechecks;
+        tot.pair_checks += bt->host_stats->pair_checks;
+        double me;
+        unsigned long long bits = bt->host_stats->max_err_bits;
+        std::memcpy(&me, &bits, 8);
+        tot.max_fp32_error = std::max(tot.max_fp32_error, me);
+    }
+    if (total) *total = tot;
+    return HMC_OK;
+}
+
+hmc_status hmc_batch_get_state(hmc_batch* bt, uint32_t replica, double* positions, uint64_t* step, uint32_t* substep) {
+    if (!bt || replica >= bt->n_rep) return fail(HMC_INVALID_ARGUMENT, "no such replica");
+    const Replica& r = bt->rep[replica];
+    if (positions && r.n_bodies) {
+        HMC_CUDA(cudaSetDevice(bt->ctx->device));
+        HMC_CUDA(launch_pack_positions(bt->dim, bt->arr.body_pos + r.body_base, bt->stage, r.n_bodies, bt->stream));
+        HMC_CUDA(cudaMemcpyAsync(positions, bt->stage, sizeof(double) * r.n_bodies * bt->dim, cudaMemcpyDeviceToHost,
+                                 bt->stream));
+        HMC_CUDA(cudaStreamSynchronize(bt->stream));
+    }
+    if (step) *step = r.step;
+    if (substep) *substep = r.substep;
+    return HMC_OK;
+}
+
+hmc_status hmc_batch_set_state(hmc_batch* bt, uint32_t replica, const double* positions, uint64_t step,
+                               uint32_t substep) {
+    if (!bt || replica >= bt->n_rep) return fail(HMC_INVALID_ARGUMENT, "no such replica");
+    Replica& r = bt->rep[replica];
+    if (r.n_bodies && !positions) return fail(HMC_INVALID_ARGUMENT, "positions is NULL");
+    if (r.n_bodies) {
+        HMC_CUDA(cudaSetDevice(bt->ctx->device));
+        const uint64_t count = (uint64_t)r.n_bodies * bt->dim;
+        HMC_CUDA(cudaMemcpyAsync(bt->stage, positions, sizeof(double) * count, cudaMemcpyHostToDevice, bt->stream));
+        HMC_CUDA(cudaMemsetAsync(bt->first_bad, 0xFF, sizeof(unsigned long long), bt->stream));
+        HMC_CUDA(launch_check_finite(bt->stage, count, (uint32_t)bt->dim, bt->first_bad, bt->stream));
+        HMC_CUDA(cudaMemcpyAsync(bt->host_first_bad, bt->first_bad, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                                 bt->stream));
+        HMC_CUDA(cudaStreamSynchronize(bt->stream));
+        if (*bt->host_first_bad != ~0ull)
+            return fail(HMC_NAN_STATE, "position %llu is not finite", (unsigned long long)*bt->host_first_bad);
+        HMC_CUDA(launch_unpack_positions(bt->dim, bt->stage, bt->arr.body_pos + r.body_base, r.n_bodies, bt->stream));
+        HMC_CUDA(cudaStreamSynchronize(bt->stream));
+    }
+    r.step = step;
+    r.substep = substep;
+    return HMC_OK;
+}
+
+hmc_status hmc_batch_overlap_check(hmc_batch* bt, uint64_t* n_overlaps) {
+    if (!bt || !n_overlaps) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
+    HMC_CUDA(cudaSetDevice(bt->ctx->device));
+    hmc_status st = batch_rebuild(bt, true);
+    if (st) return st;
+    HMC_CUDA(launch_overlap_batch(bt->dim, bt->b, bt->arr, (uint32_t)bt->n, bt->stream));
+    bt->kernel_launches += 1;
+    HMC_CUDA(cudaMemcpyAsync(bt->host_rep_u64, bt->b.overlaps, sizeof(unsigned long long) * bt->n_rep,
+                             cudaMemcpyDeviceToHost, bt->stream));
+    HMC_CUDA(cudaStreamSynchronize(bt->stream));
+    for (uint32_t k = 0; k < bt->n_rep; ++k) n_overlaps[k] = bt->host_rep_u64[k];
+    return HMC_OK;
+}
+
+uint64_t hmc_batch_kernel_launches(hmc_batch* bt) { return bt ? bt->kernel_launches : 0; }
 
 }  // extern "C"

@@ -99,10 +99,44 @@ struct Launch {
     uint32_t n_bodies;
 };
 
+// One replica of a batch of independent boxes (hmc_batch_*): its box, checkerboard, pair
+// thresholds, counter and place in the batch's concatenated arrays.
+struct Replica {
+    Geometry g;          // box and checkerboard; the origin is re-drawn every sweep
+    Pair p;              // hard-sphere thresholds
+    uint32_t cell_base;  // first space of the replica in the batch's space arrays
+    uint32_t body_base;  // first body of the replica
+    uint32_t n_bodies;
+    uint32_t rounds;     // full colour sets of the current sweep
+    uint64_t step;       // Counter at the start of the sweep
+    uint32_t substep;
+    uint32_t seed;
+    double max_move;
+};
+
+// Batch-wide tables; the Arrays of a batch span all replicas (bodies, spaces, colour lists).
+struct Batch {
+    const Replica* rep;             // [R]
+    const uint32_t* cell_base;      // [R + 1] prefix sums of the replicas' space counts
+    const uint32_t* body_rep;       // [N] replica of each body
+    uint32_t* color_rep;            // [2^d * color_stride] replica of each colour-list entry
+    unsigned long long* accepted;   // [R] per sweep
+    unsigned int* nonempty;         // [R] after a rebuild
+    unsigned long long* overlaps;   // [R] overlap check
+    uint32_t n_replicas;
+    uint32_t n_cells;               // all replicas
+    uint32_t color_stride;          // capacity of one colour's list
+};
+
 // Kernel launchers (hmc_kernels.cu). All return cudaGetLastError() after enqueueing.
 // write_s: also store the FP64 site positions S = wrap(B) in cell order (needed by the
 // plain FP64 pair test, the overlap check and injected-move evaluation).
 cudaError_t launch_rebuild(int dim, const Geometry& g, const Arrays& a, uint32_t n, bool write_s, cudaStream_t s);
+// Batches of hard-sphere replicas: the rebuild and the colour pass over all replicas at once.
+cudaError_t launch_rebuild_batch(int dim, const Batch& b, const Arrays& a, uint32_t n, bool write_s, cudaStream_t s);
+cudaError_t launch_sweep_batch(int dim, bool fp32, const Batch& b, const Arrays& a, uint32_t color, uint32_t round,
+                               uint32_t n_active, cudaStream_t s);
+cudaError_t launch_overlap_batch(int dim, const Batch& b, const Arrays& a, uint32_t n, cudaStream_t s);
 // coop selects the warp-cooperative pass (the per-lane pass otherwise).
 cudaError_t launch_sweep_sphere(int dim, bool fp32, const Geometry& g, const Arrays& a, const Pair& p,
                                 const Launch& l, bool coop, cudaStream_t s);

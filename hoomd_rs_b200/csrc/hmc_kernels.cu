@@ -64,11 +64,11 @@ __device__ __forceinline__ bool fp32_pair_overlaps(const Geometry& g, const Arra
 // on sorted S.
 template <int DIM, bool FP32>
 __device__ __forceinline__ bool sphere_overlaps_generic(const Geometry& g, const Arrays& A, const Pair& P,
-                                                        const double* t, float4 t32, const uint32_t* m, uint32_t self,
-                                                        PairStats& st) {
+                                                        const uint32_t* __restrict__ cs, const double* t, float4 t32,
+                                                        const uint32_t* m, uint32_t self, PairStats& st) {
     const uint32_t sf = g.shape[DIM - 1];
     const int mf = (int)m[DIM - 1];
-    return for_each_neighbor<DIM>(g, A.cell_start, m, [&](uint32_t q, const float* slow_shift) -> bool {
+    return for_each_neighbor<DIM>(g, cs, m, [&](uint32_t q, const float* slow_shift) -> bool {
         if (q == self) return false;
         if (FP32) {
             float4 o = __ldg(A.sorted_off + q);
@@ -152,6 +152,63 @@ __device__ __forceinline__ int sphere_overlaps_rows(const Geometry& g, const Arr
     }
 }
 
+// One trial of ParallelSweep::generate_trial_moves and update_bodies for the space with
+// multi-index m. cs is the space-range array of the system (the replica's slice in a batch);
+// slots in it index the cell-ordered arrays of A. Returns true when the move was accepted.
+template <int DIM, bool FP32>
+__device__ __forceinline__ bool sphere_trial(const Geometry& g, const Arrays& A, const Pair& P,
+                                             const uint32_t* __restrict__ cs, const uint32_t* m, uint64_t step,
+                                             uint32_t substep, uint32_t seed, double max_move, PairStats& st) {
+    const uint32_t cell = cell_index<DIM>(g, m);
+    const uint32_t sf = g.shape[DIM - 1], mf = m[DIM - 1];
+    const bool edge = sf > 2 && (mf == 0 || mf + 1 == sf);
+    // The stencil depends only on the space: start its loads before the proposal math.
+    uint32_t a0[kRows<DIM>], a1[kRows<DIM>], lo, hi;
+    row_span(sf, mf, &lo, &hi);
+    load_rows<DIM>(g, cs, m, lo, hi, a0, a1);
+    const uint32_t start = __ldg(cs + cell);
+    const uint32_t count = __ldg(cs + cell + 1) - start;
+    Sfc64 rng = make_rng(step, substep, seed, (uint64_t)cell);
+    const uint32_t k = start + canon_range_u32(rng, count);
+    double4 b4 = A.sorted_b[k];
+    double x[3] = {b4.x, b4.y, b4.z};
+    double dv[3];
+    ball_sample<DIM>(rng, max_move, A.zig_x, A.zig_f, dv);
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) x[a] = dadd(x[a], dv[a]);
+    wrap_inv<DIM>(g.L, g.invL, x);  // W1 = wrap(propose(..))
+    uint32_t mt[3];
+    bool same = point_to_space<DIM>(g, x, mt) && cell_index<DIM>(g, mt) == cell;
+    if (!same) return false;
+    double t[3] = {x[0], x[1], DIM == 3 ? x[2] : 0.0};
+    wrap_inv<DIM>(g.L, g.invL, t);  // delta_energy_one wraps the site again: T = wrap(W1)
+    float4 t32 = FP32 ? cell_offsets<DIM>(g, t, m) : make_float4(0.f, 0.f, 0.f, 0.f);
+    int res = sphere_overlaps_rows<DIM, FP32>(g, A, P, t, t32, (int)mf, k, a0, a1, st);
+    if (edge && res != kOverlap) {
+        // the wrapped space of each row; its stored fast-axis index is sf-1 (mf = 0) or 0
+        // (mf = sf-1), so a virtual mf of sf or -1 gives the cell shift -1 or +1
+        const uint32_t wlo = mf == 0 ? sf - 1u : 0u;
+        load_rows<DIM>(g, cs, m, wlo, wlo + 1u, a0, a1);
+        int r2 = sphere_overlaps_rows<DIM, FP32>(g, A, P, t, t32, mf == 0 ? (int)sf : -1, k, a0, a1, st);
+        res = r2 == kOverlap ? kOverlap : (res == kUncertain || r2 == kUncertain ? kUncertain : kClear);
+    }
+    if (res == kUncertain) {
+        PairStats st2;  // the fast path already counted its pair checks
+        res = sphere_overlaps_generic<DIM, FP32>(g, A, P, cs, t, t32, m, k, st2) ? kOverlap : kClear;
+        st.rechecks += st2.rechecks;
+        st.max_err = st2.max_err > st.max_err ? st2.max_err : st.max_err;
+    }
+    if (res == kOverlap) return false;
+    // update_body_properties: body = wrap(W1) = T, site = wrap(body)
+    double sv[3] = {t[0], t[1], t[2]};
+    wrap_inv<DIM>(g.L, g.invL, sv);
+    A.sorted_b[k] = make_double4(t[0], t[1], t[2], 0.0);
+    if (!FP32) A.sorted_s[k] = make_double4(sv[0], sv[1], sv[2], 0.0);
+    A.sorted_off[k] = cell_offsets<DIM>(g, sv, m);
+    A.body_pos[A.sorted_body[k]] = make_double4(t[0], t[1], t[2], 0.0);
+    return true;
+}
+
 // ---- the colour pass ------------------------------------------------------------------------
 // One thread per non-empty space of the colour: ParallelSweep::generate_trial_moves for that
 // space (parallel_sweep.rs:231-278) followed by update_bodies (:283-314) for an accepted move.
@@ -165,54 +222,8 @@ __global__ void __launch_bounds__(128, HMC_SWEEP_MIN_BLOCKS) k_sweep_sphere(Geom
     for (uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x; tid < L.n_active; tid += stride) {
         uint32_t m[3] = {0, 0, 0};
         unpack_m<DIM>(__ldg(A.color_cells + (size_t)L.color * g.color_stride + tid), m);
-        const uint32_t cell = cell_index<DIM>(g, m);
-        const uint32_t sf = g.shape[DIM - 1], mf = m[DIM - 1];
-        const bool edge = sf > 2 && (mf == 0 || mf + 1 == sf);
-        // The stencil depends only on the space: start its loads before the proposal math.
-        uint32_t a0[kRows<DIM>], a1[kRows<DIM>], lo, hi;
-        row_span(sf, mf, &lo, &hi);
-        load_rows<DIM>(g, A.cell_start, m, lo, hi, a0, a1);
-        const uint32_t start = __ldg(A.cell_start + cell);
-        const uint32_t count = __ldg(A.cell_start + cell + 1) - start;
-        Sfc64 rng = make_rng(L.step, L.substep, L.seed, (uint64_t)cell);
-        const uint32_t k = start + canon_range_u32(rng, count);
-        double4 b4 = A.sorted_b[k];
-        double x[3] = {b4.x, b4.y, b4.z};
-        double dv[3];
-        ball_sample<DIM>(rng, L.max_move, A.zig_x, A.zig_f, dv);
-#pragma unroll
-        for (int a = 0; a < DIM; ++a) x[a] = dadd(x[a], dv[a]);
-        wrap_inv<DIM>(g.L, g.invL, x);  // W1 = wrap(propose(..))
-        uint32_t mt[3];
-        bool same = point_to_space<DIM>(g, x, mt) && cell_index<DIM>(g, mt) == cell;
-        if (!same) continue;
-        double t[3] = {x[0], x[1], DIM == 3 ? x[2] : 0.0};
-        wrap_inv<DIM>(g.L, g.invL, t);  // delta_energy_one wraps the site again: T = wrap(W1)
-        float4 t32 = FP32 ? cell_offsets<DIM>(g, t, m) : make_float4(0.f, 0.f, 0.f, 0.f);
-        int res = sphere_overlaps_rows<DIM, FP32>(g, A, P, t, t32, (int)mf, k, a0, a1, st);
-        if (edge && res != kOverlap) {
-            // the wrapped space of each row; its stored fast-axis index is sf-1 (mf = 0) or 0
-            // (mf = sf-1), so a virtual mf of sf or -1 gives the cell shift -1 or +1
-            const uint32_t wlo = mf == 0 ? sf - 1u : 0u;
-            load_rows<DIM>(g, A.cell_start, m, wlo, wlo + 1u, a0, a1);
-            int r2 = sphere_overlaps_rows<DIM, FP32>(g, A, P, t, t32, mf == 0 ? (int)sf : -1, k, a0, a1, st);
-            res = r2 == kOverlap ? kOverlap : (res == kUncertain || r2 == kUncertain ? kUncertain : kClear);
-        }
-        if (res == kUncertain) {
-            PairStats st2;  // the fast path already counted its pair checks
-            res = sphere_overlaps_generic<DIM, FP32>(g, A, P, t, t32, m, k, st2) ? kOverlap : kClear;
-            st.rechecks += st2.rechecks;
-            st.max_err = st2.max_err > st.max_err ? st2.max_err : st.max_err;
-        }
-        if (res == kOverlap) continue;
-        n_accepted++;
-        // update_body_properties: body = wrap(W1) = T, site = wrap(body)
-        double sv[3] = {t[0], t[1], t[2]};
-        wrap_inv<DIM>(g.L, g.invL, sv);
-        A.sorted_b[k] = make_double4(t[0], t[1], t[2], 0.0);
-        if (!FP32) A.sorted_s[k] = make_double4(sv[0], sv[1], sv[2], 0.0);
-        A.sorted_off[k] = cell_offsets<DIM>(g, sv, m);
-        A.body_pos[A.sorted_body[k]] = make_double4(t[0], t[1], t[2], 0.0);
+        if (sphere_trial<DIM, FP32>(g, A, P, A.cell_start, m, L.step, L.substep, L.seed, L.max_move, st))
+            n_accepted++;
     }
     flush_stats(A.stats, st, n_accepted);
 }
@@ -397,7 +408,7 @@ __global__ void __launch_bounds__(128, HMC_SWEEP_MIN_BLOCKS) k_sweep_sphere_coop
         if (!trial || res == kFlagOverlap) continue;
         if (res & kFlagUncertain) {
             PairStats st2;  // the fast path already counted its pair checks
-            const bool ov = sphere_overlaps_generic<DIM, FP32>(g, A, P, t, t32, m, k, st2);
+            const bool ov = sphere_overlaps_generic<DIM, FP32>(g, A, P, A.cell_start, t, t32, m, k, st2);
             st.rechecks += st2.rechecks;
             st.max_err = st2.max_err > st.max_err ? st2.max_err : st.max_err;
             if (ov) continue;
@@ -727,7 +738,7 @@ __global__ void k_eval_sphere(Geometry g, Arrays A, Pair P, const uint64_t* bodi
         if (ok) {
             uint32_t self = A.slot_of_body[bodies[i]];
             float4 t32 = FP32 ? cell_offsets<DIM>(g, t, m) : make_float4(0.f, 0.f, 0.f, 0.f);
-            dec = sphere_overlaps_generic<DIM, FP32>(g, A, P, t, t32, m, self, st) ? 0 : 1;
+            dec = sphere_overlaps_generic<DIM, FP32>(g, A, P, A.cell_start, t, t32, m, self, st) ? 0 : 1;
         } else {
             atomicOr(&A.stats->error_flags, kErrOutsideCheckerboard);
         }
@@ -740,6 +751,278 @@ __global__ void k_eval_sphere(Geometry g, Arrays A, Pair P, const uint64_t* bodi
 template <typename T>
 inline uint32_t blocks_for(T n, uint32_t threads) {
     return (uint32_t)((n + threads - 1) / threads);
+}
+
+// ---- batches of replicas -------------------------------------------------------------------
+// The spaces of all replicas form one CSR (replica r's spaces start at cell_base[r]) and the
+// colour lists hold every replica's non-empty spaces of a colour, tagged with the replica.
+// Each replica keeps its own box, checkerboard and Counter, so every replica's trajectory is
+// the one its own system would produce; one launch serves all replicas.
+__device__ __forceinline__ uint32_t find_replica(const Batch& B, uint32_t c) {
+    uint32_t lo = 0, hi = B.n_replicas;  // largest r with cell_base[r] <= c
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(B.cell_base + mid) <= c)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+template <int DIM>
+__global__ void k_bin_batch(Batch B, Arrays A, uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const Replica& R = B.rep[__ldg(B.body_rep + i)];
+    const double4 b = A.body_pos[i];
+    double x[3] = {b.x, b.y, b.z};
+    uint32_t m[3] = {0, 0, 0};
+    uint32_t cell = R.cell_base;
+    const bool finite = isfinite(x[0]) && isfinite(x[1]) && (DIM == 2 || isfinite(x[2]));
+    if (!finite)
+        atomicOr(&A.stats->error_flags, kErrNonFinite);
+    else if (!point_to_space<DIM>(R.g, x, m))
+        atomicOr(&A.stats->error_flags, kErrOutsideCheckerboard);
+    else
+        cell += cell_index<DIM>(R.g, m);
+    A.body_cell[i] = cell;
+    A.body_rank[i] = atomicAdd(&A.cell_count[cell], 1u);
+}
+
+// A walk over consecutive spaces of the batch: replica, local index and multi-index.
+template <int DIM>
+struct SpaceCursor {
+    uint32_t r, local, end, m[3];
+    __device__ __forceinline__ void seek(const Batch& B, uint32_t c) {
+        r = find_replica(B, c);
+        local = c - __ldg(B.cell_base + r);
+        end = __ldg(B.cell_base + r + 1) - __ldg(B.cell_base + r);
+        uint32_t rem = local;
+        const Geometry& g = B.rep[r].g;
+#pragma unroll
+        for (int a = DIM - 1; a >= 0; --a) {
+            m[a] = rem % g.shape[a];
+            rem /= g.shape[a];
+        }
+        if (DIM == 2) m[2] = 0;
+    }
+    __device__ __forceinline__ void next(const Batch& B) {
+        if (++local == end && r + 1 < B.n_replicas) {
+            ++r;
+            local = 0;
+            end = __ldg(B.cell_base + r + 1) - __ldg(B.cell_base + r);
+            m[0] = m[1] = m[2] = 0;
+            return;
+        }
+        const Geometry& g = B.rep[r].g;
+#pragma unroll
+        for (int a = DIM - 1; a >= 0; --a) {
+            if (++m[a] < g.shape[a]) return;
+            m[a] = 0;
+        }
+    }
+};
+
+template <int DIM>
+__global__ void __launch_bounds__(kScanThreads) k_scan_reduce_batch(Batch B, Arrays A) {
+    const uint32_t base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+    uint32_t sum = 0;
+    unsigned long long lo = 0, hi = 0;
+    SpaceCursor<DIM> cur;
+    if (base < B.n_cells) cur.seek(B, base);
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        const uint32_t c = base + k;
+        const uint32_t v = c < B.n_cells ? A.cell_count[c] : 0;
+        sum += v;
+        if (v > 0) {
+            const uint32_t col = color_of<DIM>(cur.m);
+            if (col < 4)
+                lo += 1ull << (16 * col);
+            else
+                hi += 1ull << (16 * (col - 4));
+        }
+        if (c + 1 < B.n_cells) cur.next(B);
+    }
+    uint32_t total;
+    unsigned long long tlo, thi;
+    block_exclusive_scan(sum, &total);
+    block_exclusive_scan(lo, &tlo);
+    block_exclusive_scan(hi, &thi);
+    if (threadIdx.x == 0) {
+        const uint32_t nb = gridDim.x;
+        A.block_sums[blockIdx.x] = total;
+#pragma unroll
+        for (int col = 0; col < 4; ++col) {
+            A.block_sums[(1 + col) * nb + blockIdx.x] = (uint32_t)((tlo >> (16 * col)) & 0xffffu);
+            A.block_sums[(5 + col) * nb + blockIdx.x] = (uint32_t)((thi >> (16 * col)) & 0xffffu);
+        }
+    }
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(kScanThreads) k_scan_apply_batch(Batch B, Arrays A) {
+    const uint32_t nb = gridDim.x;
+    const uint32_t base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+    uint32_t v[kScanItems];
+    uint32_t sum = 0;
+    unsigned long long lo = 0, hi = 0;
+    SpaceCursor<DIM> cur;
+    if (base < B.n_cells) cur.seek(B, base);
+    SpaceCursor<DIM> first = cur;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        const uint32_t c = base + k;
+        v[k] = c < B.n_cells ? A.cell_count[c] : 0;
+        sum += v[k];
+        if (v[k] > 0) {
+            const uint32_t col = color_of<DIM>(cur.m);
+            if (col < 4)
+                lo += 1ull << (16 * col);
+            else
+                hi += 1ull << (16 * (col - 4));
+        }
+        if (c + 1 < B.n_cells) cur.next(B);
+    }
+    uint32_t total;
+    unsigned long long tlo, thi;
+    uint32_t run = block_exclusive_scan(sum, &total) + A.block_sums[blockIdx.x];
+    const unsigned long long plo = block_exclusive_scan(lo, &tlo);
+    const unsigned long long phi = block_exclusive_scan(hi, &thi);
+    uint32_t pos[8];
+#pragma unroll
+    for (int col = 0; col < 8; ++col) {
+        const uint32_t within =
+            col < 4 ? (uint32_t)((plo >> (16 * col)) & 0xffffu) : (uint32_t)((phi >> (16 * (col - 4))) & 0xffffu);
+        pos[col] = (col < (1 << DIM) ? A.block_sums[(1 + col) * nb + blockIdx.x] : 0u) + within;
+    }
+    cur = first;
+    uint32_t counted = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        const uint32_t c = base + k;
+        if (c < B.n_cells) A.cell_start[c] = run;
+        run += v[k];
+        if (c + 1 == B.n_cells) A.cell_start[B.n_cells] = run;
+        if (v[k] > 0) {
+            const uint32_t col = color_of<DIM>(cur.m);
+            const size_t e = (size_t)col * B.color_stride + pos[col];
+            A.color_cells[e] = pack_m<DIM>(cur.m);
+            B.color_rep[e] = cur.r;
+            pos[col] += 1;
+            counted += 1;
+        }
+        if (c + 1 < B.n_cells) {
+            const uint32_t r_before = cur.r;
+            cur.next(B);
+            if (cur.r != r_before) {  // the run of spaces crossed into the next replica
+                if (counted) atomicAdd(B.nonempty + r_before, counted);
+                counted = 0;
+            }
+        }
+    }
+    if (counted && base < B.n_cells) atomicAdd(B.nonempty + cur.r, counted);
+}
+
+template <int DIM, bool WRITE_S>
+__global__ void __launch_bounds__(128) k_finalize_batch(Batch B, Arrays A) {
+    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= B.n_cells) return;
+    const uint32_t s = A.cell_start[c], e = A.cell_start[c + 1];
+    if (s == e) return;
+    for (uint32_t k = s + 1; k < e; ++k) {
+        const uint32_t v = A.sorted_body[k];
+        uint32_t j = k;
+        while (j > s && A.sorted_body[j - 1] > v) {
+            A.sorted_body[j] = A.sorted_body[j - 1];
+            --j;
+        }
+        A.sorted_body[j] = v;
+    }
+    SpaceCursor<DIM> cur;
+    cur.seek(B, c);
+    const Geometry& g = B.rep[cur.r].g;
+    for (uint32_t k = s; k < e; ++k) {
+        const uint32_t i = A.sorted_body[k];
+        A.slot_of_body[i] = k;
+        const double4 b = A.body_pos[i];
+        A.sorted_b[k] = b;
+        double sv[3] = {b.x, b.y, b.z};
+        wrap_inv<DIM>(g.L, g.invL, sv);
+        if (WRITE_S) A.sorted_s[k] = make_double4(sv[0], sv[1], sv[2], 0.0);
+        A.sorted_off[k] = cell_offsets<DIM>(g, sv, cur.m);
+    }
+}
+
+// Accepted moves per replica from one warp: the lanes of each replica in the warp add up.
+__device__ __forceinline__ void add_per_replica(unsigned long long* acc, uint32_t r, bool accepted) {
+    const unsigned full = 0xffffffffu;
+    unsigned todo = full;
+    while (todo) {
+        const int leader = __ffs(todo) - 1;
+        const uint32_t rl = __shfl_sync(full, r, leader);
+        const unsigned same = __ballot_sync(full, r == rl);
+        const unsigned n = __popc(__ballot_sync(full, r == rl && accepted));
+        if ((threadIdx.x & 31) == (unsigned)leader && n) atomicAdd(acc + rl, (unsigned long long)n);
+        todo &= ~same;
+    }
+}
+
+// One colour pass over all replicas that still run round `round` of this sweep.
+template <int DIM, bool FP32>
+__global__ void __launch_bounds__(128, HMC_SWEEP_MIN_BLOCKS) k_sweep_batch(Batch B, Arrays A, uint32_t color,
+                                                                             uint32_t round, uint32_t n_active) {
+    uint32_t n_accepted = 0;
+    PairStats st;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n_active; base += stride) {
+        const uint32_t tid = base + (threadIdx.x & 31u);
+        bool accepted = false;
+        uint32_t r = 0xffffffffu;
+        if (tid < n_active) {
+            const size_t e = (size_t)color * B.color_stride + tid;
+            r = __ldg(B.color_rep + e);
+            const Replica& R = B.rep[r];
+            if (round < R.rounds) {
+                uint32_t m[3] = {0, 0, 0};
+                unpack_m<DIM>(__ldg(A.color_cells + e), m);
+                accepted = sphere_trial<DIM, FP32>(R.g, A, R.p, A.cell_start + R.cell_base, m, R.step,
+                                                   R.substep + round, R.seed, R.max_move, st);
+            }
+        }
+        n_accepted += accepted;
+        add_per_replica(B.accepted, r, accepted);
+    }
+    flush_stats(A.stats, st, n_accepted);
+}
+
+// Overlapping pairs (i < j) of every replica, FP64.
+template <int DIM>
+__global__ void k_overlap_batch(Batch B, Arrays A, uint32_t n) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const uint32_t bi = A.sorted_body[k];
+    const uint32_t r = __ldg(B.body_rep + bi);
+    const Replica& R = B.rep[r];
+    const double4 s4 = A.sorted_s[k];
+    const double t[3] = {s4.x, s4.y, s4.z};
+    uint32_t m[3] = {0, 0, 0};
+    uint32_t c = A.body_cell[bi] - R.cell_base;
+#pragma unroll
+    for (int a = DIM - 1; a >= 0; --a) {
+        m[a] = c % R.g.shape[a];
+        c /= R.g.shape[a];
+    }
+    uint32_t found = 0;
+    for_each_neighbor<DIM>(R.g, A.cell_start + R.cell_base, m, [&](uint32_t q, const float*) -> bool {
+        if (A.sorted_body[q] <= bi) return false;
+        const double4 o4 = A.sorted_s[q];
+        const double sv[3] = {o4.x, o4.y, o4.z};
+        if (ref_dist2<DIM>(R.g, t, sv) < R.p.sigma2) found++;
+        return false;
+    });
+    if (found) atomicAdd(B.overlaps + r, (unsigned long long)found);
 }
 
 // ---- state transfer ------------------------------------------------------------------
@@ -869,6 +1152,87 @@ cudaError_t launch_rebuild(int dim, const Geometry& g, const Arrays& a, uint32_t
         else
             k_finalize<3, false><<<fb, 128, 0, s>>>(g, a);
     }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_rebuild_batch(int dim, const Batch& b, const Arrays& a, uint32_t n, bool write_s, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(a.cell_count, 0, sizeof(uint32_t) * b.n_cells, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(b.nonempty, 0, sizeof(unsigned int) * b.n_replicas, s);
+    if (e != cudaSuccess) return e;
+    if (n > 0) {
+        if (dim == 2)
+            k_bin_batch<2><<<blocks_for(n, 256), 256, 0, s>>>(b, a, n);
+        else
+            k_bin_batch<3><<<blocks_for(n, 256), 256, 0, s>>>(b, a, n);
+    }
+    const uint32_t nb = blocks_for(b.n_cells, kScanTile);
+    if (dim == 2)
+        k_scan_reduce_batch<2><<<nb, kScanThreads, 0, s>>>(b, a);
+    else
+        k_scan_reduce_batch<3><<<nb, kScanThreads, 0, s>>>(b, a);
+    k_scan_block_sums<<<1, 1024, 0, s>>>(a, nb, 1u << dim);
+    if (dim == 2)
+        k_scan_apply_batch<2><<<nb, kScanThreads, 0, s>>>(b, a);
+    else
+        k_scan_apply_batch<3><<<nb, kScanThreads, 0, s>>>(b, a);
+    if (n > 0) k_scatter<<<blocks_for(n, 256), 256, 0, s>>>(a, n);
+    const uint32_t fb = blocks_for(b.n_cells, 128);
+    if (dim == 2) {
+        if (write_s)
+            k_finalize_batch<2, true><<<fb, 128, 0, s>>>(b, a);
+        else
+            k_finalize_batch<2, false><<<fb, 128, 0, s>>>(b, a);
+    } else {
+        if (write_s)
+            k_finalize_batch<3, true><<<fb, 128, 0, s>>>(b, a);
+        else
+            k_finalize_batch<3, false><<<fb, 128, 0, s>>>(b, a);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sweep_batch(int dim, bool fp32, const Batch& b, const Arrays& a, uint32_t color, uint32_t round,
+                               uint32_t n_active, cudaStream_t s) {
+    if (n_active == 0) return cudaSuccess;
+    static int max_blocks[2][2] = {{0, 0}, {0, 0}};
+    int& mb = max_blocks[dim == 3][fp32];
+    if (mb == 0) {
+        int dev = 0, sms = 0, per_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaError_t e;
+        if (dim == 2)
+            e = fp32 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_batch<2, true>, 128, 0)
+                     : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_batch<2, false>, 128, 0);
+        else
+            e = fp32 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_batch<3, true>, 128, 0)
+                     : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_batch<3, false>, 128, 0);
+        if (e != cudaSuccess) return e;
+        mb = sms * (per_sm > 0 ? per_sm : 1);
+    }
+    uint32_t grid = blocks_for(n_active, 128);
+    if (grid > (uint32_t)mb) grid = (uint32_t)mb;
+    if (dim == 2) {
+        if (fp32)
+            k_sweep_batch<2, true><<<grid, 128, 0, s>>>(b, a, color, round, n_active);
+        else
+            k_sweep_batch<2, false><<<grid, 128, 0, s>>>(b, a, color, round, n_active);
+    } else {
+        if (fp32)
+            k_sweep_batch<3, true><<<grid, 128, 0, s>>>(b, a, color, round, n_active);
+        else
+            k_sweep_batch<3, false><<<grid, 128, 0, s>>>(b, a, color, round, n_active);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_overlap_batch(int dim, const Batch& b, const Arrays& a, uint32_t n, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(b.overlaps, 0, sizeof(unsigned long long) * b.n_replicas, s);
+    if (e != cudaSuccess || n == 0) return e;
+    if (dim == 2)
+        k_overlap_batch<2><<<blocks_for(n, 128), 128, 0, s>>>(b, a, n);
+    else
+        k_overlap_batch<3><<<blocks_for(n, 128), 128, 0, s>>>(b, a, n);
     return cudaGetLastError();
 }
 

@@ -213,6 +213,30 @@ hmc_status hmc_overlap_count_noalloc(const double* positions, uint64_t n_bodies,
                                      uint64_t* overlaps, void* cuda_stream);
 
 /* ---- profiling ---- */
+/* ---- batches of independent replicas ----
+ * A batch runs many hard-sphere boxes (each its own hmc_system_desc: box, diameter, Counter,
+ * body count) through one set of launches: one counting sort and one kernel per colour pass
+ * for all replicas. Every replica's trajectory is the one hmc_system would produce from the
+ * same description. This is the replica batching of the survey's batched configuration; the
+ * reference has no counterpart (a user would loop over Microstates). */
+typedef struct hmc_batch hmc_batch;
+/* positions[k]: descs[k].n_bodies * dim doubles. All replicas: HMC_HARD_SPHERE, one dim. */
+hmc_status hmc_batch_create(hmc_context* ctx, uint32_t n_replicas, const hmc_system_desc* descs,
+                            const double* const* positions, hmc_batch** out);
+void hmc_batch_destroy(hmc_batch* batch);
+/* params: one per replica (its own maximum); move, precision, n_sweeps, increment_step must
+ * agree. counts (per replica, may be NULL) receive accepted/rejected; total (may be NULL)
+ * also receives the batch's rechecks, pair_checks and max_fp32_error. */
+hmc_status hmc_batch_sweep(hmc_batch* batch, const hmc_sweep_params* params, hmc_count* counts, hmc_count* total);
+hmc_status hmc_batch_get_state(hmc_batch* batch, uint32_t replica, double* positions, uint64_t* step,
+                               uint32_t* substep);
+hmc_status hmc_batch_set_state(hmc_batch* batch, uint32_t replica, const double* positions, uint64_t step,
+                               uint32_t substep);
+/* Overlapping pairs per replica (n_overlaps: n_replicas entries). */
+hmc_status hmc_batch_overlap_check(hmc_batch* batch, uint64_t* n_overlaps);
+/* Kernels this batch enqueued so far. */
+uint64_t hmc_batch_kernel_launches(hmc_batch* batch);
+
 /* The correctly rounded sin and cos that the 2-D rotation path uses (on the context's device);
  * no counterpart in the reference, which calls the platform libm (hoomd-vector angle.rs:120-150).
  * HMC_INVALID_ARGUMENT when some |x[i]| >= 2^20. */

@@ -1,0 +1,79 @@
+"""Batches of independent hard-sphere replicas (hmc_batch_*).
+
+Each replica keeps its own box, checkerboard and Counter, so after any number of batched
+sweeps replica k must equal, bit for bit, a single system built from the same description
+and swept with the same move size (and hence the oracle).
+"""
+import numpy as np
+import pytest
+
+import oracle
+from hoomd_rs_b200 import (FP32_RECHECK, FP64, TRANSLATE, Batch, Context, HardSphere, Microstate, PairwiseCutoff,
+                           Periodic, lattice)
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    return Context(0)
+
+
+def replicas(dim, specs):
+    out = []
+    for k, (n, phi, seed, step, kind) in enumerate(specs):
+        pos, L = lattice.hard_sphere_box(n, phi, dim, seed, lattice=kind)
+        # a valid hard-sphere start: the lattice spacing must exceed 1 + the jitter
+        assert oracle.System(dim, [L] * dim, pos).overlap_count() == 0
+        out.append({"boundary": Periodic(1.0, [L] * dim), "positions": pos, "seed": seed, "step": step})
+    return out
+
+
+# (N, packing fraction, seed, step, lattice); the last replica has two spaces per axis
+SPECS3 = [(500, 0.40, 11, 0, "fcc"), (1024, 0.48, 12, 3, "fcc"), (2000, 0.45, 13, 0, "fcc"),
+          (777, 0.50, 14, 9, "fcc"), (4096, 0.42, 15, 1, "fcc"), (8, 0.30, 16, 0, "cubic")]
+SPECS2 = [(1000, 0.60, 21, 0, "auto"), (4096, 0.70, 22, 2, "auto"), (300, 0.45, 23, 0, "auto")]
+
+
+@pytest.mark.parametrize("precision", [FP64, FP32_RECHECK])
+@pytest.mark.parametrize("dim,specs", [(3, SPECS3), (2, SPECS2)])
+def test_batch_replicas_equal_single_systems(ctx, dim, specs, precision):
+    reps = replicas(dim, specs)
+    maxima = np.linspace(0.08, 0.3, len(reps))
+    b = Batch(ctx, reps)
+    singles = [Microstate(ctx, r["boundary"], r["positions"], PairwiseCutoff(HardSphere(1.0)), seed=r["seed"],
+                          step=r["step"]) for r in reps]
+    for _ in range(5):
+        counts, total = b.sweep(maxima, precision, increment_step=True)
+        for k, m in enumerate(singles):
+            c = m.sweep(TRANSLATE, float(maxima[k]), 1.0, precision, n_sweeps=1, increment_step=True)
+            assert (counts[k].accepted, counts[k].rejected) == (c.accepted, c.rejected), k
+        assert total.accepted == sum(c.accepted for c in counts)
+    for k, m in enumerate(singles):
+        pos, step, sub = b.state(k)
+        assert np.array_equal(pos, m.positions()), k
+        assert (step, sub) == (m.step(), m.substep())
+    assert not b.overlap_counts().any()
+
+
+def test_batch_replica_equals_oracle_and_overlap_counts(ctx):
+    reps = replicas(3, SPECS3[:3])
+    b = Batch(ctx, reps)
+    r = reps[1]
+    L = r["boundary"].edge_lengths[0]
+    o = oracle.System(3, [L] * 3, r["positions"], seed=r["seed"], step=r["step"])
+    for _ in range(4):
+        b.sweep([0.2, 0.15, 0.2], FP32_RECHECK, increment_step=True)
+        o.parallel_sweep(oracle.TRANSLATE, 0.15, 1.0, 1.0)
+        o.increment_step()
+    assert np.array_equal(b.positions(1), o.state()[0])
+    # plant overlaps in replica 2 only; the oracle counts the same pairs
+    p2, step, sub = b.state(2)
+    L2 = reps[2]["boundary"].edge_lengths[0]
+    moved = p2[0] + np.array([0.5, 0.0, 0.0])
+    lam = moved / L2 - np.round(moved / L2)
+    p2[1] = np.where(lam == 0.5, -0.5, lam) * L2
+    b.set_state(2, p2, step, sub)
+    want = oracle.System(3, [L2] * 3, p2).overlap_count()
+    assert want >= 1
+    assert list(b.overlap_counts()) == [0, 0, want]
