@@ -85,6 +85,7 @@ struct hmc_system {
     unsigned long long* host_first_bad = nullptr;  // pinned mirror
     std::vector<void*> allocations;
     bool coop[2] = {true, false};  // warp-cooperative hard-sphere pass: [fp64, fp32]
+    uint32_t rounds_guess = 2;      // colour sets enqueued before the sweep's count is known
     // convex polyhedron
     double4* verts = nullptr;
     uint32_t n_vertices = 0;
@@ -210,7 +211,7 @@ hmc_status rebuild(hmc_system* s, bool write_s) {
     }
     HMC_CUDA(cudaMemsetAsync(s->arr.stats, 0, sizeof(DeviceStats), s->stream));
     HMC_CUDA(launch_rebuild(s->dim, s->geom, s->arr, (uint32_t)s->n, write_s, s->stream));
-    s->prof.kernel_launches += s->n > 0 ? 6 : 4;  // bin, 3 scan passes, scatter, finalize
+    s->prof.kernel_launches += s->n > 0 ? 7 : 3;  // bin, 3 scan passes, scatter, space sort, gather
     return HMC_OK;
 }
 
@@ -478,7 +479,7 @@ hmc_status hmc_system_create(hmc_context* ctx, const hmc_system_desc* d, const d
     if ((st = dalloc(s, &A.body_pos, n)) || (st = dalloc(s, &A.sorted_b, n)) || (st = dalloc(s, &A.sorted_s, n)) ||
         (st = dalloc(s, &A.sorted_off, n)) || (st = dalloc(s, &A.sorted_body, n)) ||
         (st = dalloc(s, &A.slot_of_body, n)) || (st = dalloc(s, &A.body_cell, n)) ||
-        (st = dalloc(s, &A.body_rank, n)) || (st = dalloc(s, &A.cell_count, cells)) ||
+        (st = dalloc(s, &A.body_rank, n)) || (st = dalloc(s, &A.body_m, n)) || (st = dalloc(s, &A.cell_count, cells)) ||
         (st = dalloc(s, &A.cell_start, cells + 1)) || (st = dalloc(s, &A.block_sums, (size_t)scan_blocks * 9)) ||
         (st = dalloc(s, &A.color_cells, cells)) ||
         (st = dalloc(s, &A.stats, 1)) || (st = dalloc(s, &s->stage, n * (uint64_t)s->dim)) ||
@@ -651,59 +652,72 @@ hmc_status hmc_sweep(hmc_system* s, const hmc_sweep_params* p, hmc_count* out) {
         hmc_status st = rebuild(s, !fp32);
         if (st) return st;
         if (s->profiling) HMC_CUDA(cudaEventRecord(s->ev[1], s->stream));
-        if ((st = read_stats(s))) return st;
-        if ((st = check_flags(s))) return st;
-        uint64_t nonempty = s->host_stats->nonempty;
-        // while count.total() < N: one trial per non-empty space per colour (:402-418)
-        uint64_t rounds = (s->n == 0) ? 0 : (s->n + nonempty - 1) / nonempty;
         Launch L{};
         L.step = s->step;
         L.seed = s->seed;
         L.max_move = p->maximum;
         L.kt = p->temperature;
         L.n_bodies = (uint32_t)s->n;
-        uint32_t color_count[8];
-        for (uint32_t c = 0; c < colors; ++c) color_count[c] = s->host_stats->color_count[c];
+        L.n_active = s->geom.color_stride;  // grid bound; the kernels read the list lengths
         if (s->profiling) HMC_CUDA(cudaEventRecord(s->ev[2], s->stream));
-        for (uint64_t r = 0; r < rounds; ++r) {
-            L.substep = s->substep;
-            for (uint32_t c = 0; c < colors; ++c) {
-                L.color = c;
-                L.n_active = color_count[c];
-                if (s->interaction == HMC_LENNARD_JONES)
-                    HMC_CUDA(launch_sweep_lj(s->dim, fp32, s->geom, s->arr, s->pair, L, s->stream));
-                else if (s->interaction == HMC_HARD_CONVEX_POLYHEDRON)
-                    HMC_CUDA(launch_sweep_poly(fp32, s->geom, s->arr, s->verts, s->n_vertices, s->poly_rcut2,
-                                               s->poly_rcut2_hi32, L, p->move == HMC_ROTATE, s->stream));
-                else if (s->polygon())
-                    HMC_CUDA(launch_sweep_poly2(fp32, s->sat(), s->geom, s->arr, s->verts, s->n_vertices, s->poly_rcut2,
-                                                s->poly_rcut2_hi32, L, p->move == HMC_ROTATE, s->stream));
-                else
-                    HMC_CUDA(launch_sweep_sphere(s->dim, fp32, s->geom, s->arr, s->pair, L, s->coop[fp32], s->stream));
-                s->prof.kernel_launches += 1;
+        // The rounds (while count.total() < N, :402-418) are known on the device after the
+        // rebuild; the host enqueues the previous sweep's number of colour sets without
+        // waiting, the kernels skip sets beyond the true count, and any missing sets follow.
+        auto enqueue = [&](uint32_t r0, uint32_t r1) -> hmc_status {
+            for (uint32_t r = r0; r < r1; ++r) {
+                L.substep = s->substep + r;  // increment_substep after every full colour set
+                L.round = r;
+                for (uint32_t c = 0; c < colors; ++c) {
+                    L.color = c;
+                    if (s->interaction == HMC_LENNARD_JONES)
+                        HMC_CUDA(launch_sweep_lj(s->dim, fp32, s->geom, s->arr, s->pair, L, s->stream));
+                    else if (s->interaction == HMC_HARD_CONVEX_POLYHEDRON)
+                        HMC_CUDA(launch_sweep_poly(fp32, s->geom, s->arr, s->verts, s->n_vertices, s->poly_rcut2,
+                                                   s->poly_rcut2_hi32, L, p->move == HMC_ROTATE, s->stream));
+                    else if (s->polygon())
+                        HMC_CUDA(launch_sweep_poly2(fp32, s->sat(), s->geom, s->arr, s->verts, s->n_vertices,
+                                                    s->poly_rcut2, s->poly_rcut2_hi32, L, p->move == HMC_ROTATE,
+                                                    s->stream));
+                    else
+                        HMC_CUDA(launch_sweep_sphere(s->dim, fp32, s->geom, s->arr, s->pair, L, s->coop[fp32],
+                                                     s->stream));
+                    s->prof.kernel_launches += 1;
+                }
             }
-            s->substep += 1;  // increment_substep after every full colour set
-        }
-        if (s->profiling) HMC_CUDA(cudaEventRecord(s->ev[3], s->stream));
+            return HMC_OK;
+        };
+        const uint32_t guess = s->n == 0 ? 0u : s->rounds_guess;
+        if ((st = enqueue(0, guess))) return st;
         if ((st = read_stats(s))) return st;
+        if ((st = check_flags(s))) return st;  // the kernels left the state untouched
+        const uint32_t rounds = s->host_stats->rounds;
+        if (rounds > guess) {
+            if ((st = enqueue(guess, rounds))) return st;
+            if ((st = read_stats(s))) return st;
+        }
+        if (rounds > 0) s->rounds_guess = rounds;
         if (s->profiling) {
+            HMC_CUDA(cudaEventRecord(s->ev[3], s->stream));
+            HMC_CUDA(cudaEventSynchronize(s->ev[3]));
             float t_rebuild = 0.f, t_sweep = 0.f;
             HMC_CUDA(cudaEventElapsedTime(&t_rebuild, s->ev[0], s->ev[1]));
             HMC_CUDA(cudaEventElapsedTime(&t_sweep, s->ev[2], s->ev[3]));
             s->prof.rebuild_ms += t_rebuild;
-            s->prof.rebuild_launches += s->n > 0 ? 6 : 4;
+            s->prof.rebuild_launches += s->n > 0 ? 7 : 3;
             s->prof.sweep_ms += t_sweep;
-            s->prof.sweep_launches += rounds * colors;
+            s->prof.sweep_launches += (uint64_t)std::max(rounds, guess) * colors;
             s->prof.sweeps += 1;
         }
+        const uint64_t nonempty = s->host_stats->nonempty;
         total.accepted += s->host_stats->accepted;
-        total.rejected += rounds * nonempty - s->host_stats->accepted;
+        total.rejected += (uint64_t)rounds * nonempty - s->host_stats->accepted;
         total.rechecks += s->host_stats->rechecks;
         total.pair_checks += s->host_stats->pair_checks;
         double me;
         unsigned long long bits = s->host_stats->max_err_bits;
         std::memcpy(&me, &bits, 8);
         total.max_fp32_error = std::max(total.max_fp32_error, me);
+        s->substep += rounds;
         if (p->increment_step) {
             s->step += 1;
             s->substep = 0;
@@ -981,6 +995,7 @@ struct hmc_batch {
     unsigned long long* host_first_bad = nullptr;
     std::vector<void*> allocations;
     uint64_t kernel_launches = 0;
+    uint32_t rounds_guess = 2;
 };
 
 namespace {
@@ -1017,9 +1032,16 @@ hmc_status batch_rebuild(hmc_batch* bt, bool write_s) {
     if (st) return st;
     HMC_CUDA(cudaMemsetAsync(bt->arr.stats, 0, sizeof(DeviceStats), bt->stream));
     HMC_CUDA(launch_rebuild_batch(bt->dim, bt->b, bt->arr, (uint32_t)bt->n, write_s, bt->stream));
-    bt->kernel_launches += bt->n > 0 ? 6 : 4;
+    bt->kernel_launches += bt->n > 0 ? 7 : 3;
+    return HMC_OK;
+}
+
+// Stats, per-replica non-empty spaces and accepted moves to the host (one synchronisation).
+hmc_status batch_read(hmc_batch* bt) {
     HMC_CUDA(cudaMemcpyAsync(bt->host_stats, bt->arr.stats, sizeof(DeviceStats), cudaMemcpyDeviceToHost, bt->stream));
     HMC_CUDA(cudaMemcpyAsync(bt->host_nonempty, bt->b.nonempty, sizeof(unsigned int) * bt->n_rep,
+                             cudaMemcpyDeviceToHost, bt->stream));
+    HMC_CUDA(cudaMemcpyAsync(bt->host_rep_u64, bt->b.accepted, sizeof(unsigned long long) * bt->n_rep,
                              cudaMemcpyDeviceToHost, bt->stream));
     HMC_CUDA(cudaStreamSynchronize(bt->stream));
     const uint32_t f = bt->host_stats->error_flags;
@@ -1160,7 +1182,7 @@ hmc_status hmc_batch_create(hmc_context* ctx, uint32_t n_replicas, const hmc_sys
     if ((st = balloc(bt, &A.body_pos, n)) || (st = balloc(bt, &A.sorted_b, n)) || (st = balloc(bt, &A.sorted_s, n)) ||
         (st = balloc(bt, &A.sorted_off, n)) || (st = balloc(bt, &A.sorted_body, n)) ||
         (st = balloc(bt, &A.slot_of_body, n)) || (st = balloc(bt, &A.body_cell, n)) ||
-        (st = balloc(bt, &A.body_rank, n)) || (st = balloc(bt, &A.cell_count, cells)) ||
+        (st = balloc(bt, &A.body_rank, n)) || (st = balloc(bt, &A.body_m, n)) || (st = balloc(bt, &A.cell_count, cells)) ||
         (st = balloc(bt, &A.cell_start, (size_t)cells + 1)) || (st = balloc(bt, &A.block_sums, (size_t)scan_blocks * 9)) ||
         (st = balloc(bt, &A.color_cells, cells)) || (st = balloc(bt, &A.stats, 1)) ||
         (st = balloc(bt, &d_rep, n_replicas)) || (st = balloc(bt, &d_cell_base, (size_t)n_replicas + 1)) ||
@@ -1231,30 +1253,32 @@ hmc_status hmc_batch_sweep(hmc_batch* bt, const hmc_sweep_params* params, hmc_co
     for (uint32_t sweep = 0; sweep < p0.n_sweeps; ++sweep) {
         hmc_status st = batch_rebuild(bt, !fp32);
         if (st) return st;
-        uint32_t max_rounds = 0;
+        HMC_CUDA(launch_batch_rounds(bt->b, const_cast<Replica*>(bt->b.rep), bt->arr.stats, bt->stream));
+        bt->kernel_launches += 1;
+        HMC_CUDA(cudaMemsetAsync(bt->b.accepted, 0, sizeof(unsigned long long) * bt->n_rep, bt->stream));
+        auto enqueue = [&](uint32_t r0, uint32_t r1) -> hmc_status {
+            for (uint32_t round = r0; round < r1; ++round)
+                for (uint32_t c = 0; c < colors; ++c) {
+                    HMC_CUDA(launch_sweep_batch(bt->dim, fp32, bt->b, bt->arr, c, round, bt->b.color_stride, bt->stream));
+                    bt->kernel_launches += 1;
+                }
+            return HMC_OK;
+        };
+        const uint32_t guess = bt->rounds_guess;
+        if ((st = enqueue(0, guess))) return st;
+        if ((st = batch_read(bt))) return st;
+        const uint32_t max_rounds = bt->host_stats->rounds;
+        if (max_rounds > guess) {
+            if ((st = enqueue(guess, max_rounds))) return st;
+            if ((st = batch_read(bt))) return st;
+        }
+        if (max_rounds > 0) bt->rounds_guess = max_rounds;
         for (uint32_t k = 0; k < bt->n_rep; ++k) {
             Replica& r = bt->rep[k];
             const uint32_t ne = bt->host_nonempty[k];
             r.rounds = (r.n_bodies == 0 || ne == 0) ? 0u : (r.n_bodies + ne - 1) / ne;
-            max_rounds = std::max(max_rounds, r.rounds);
-        }
-        if ((st = batch_upload_replicas(bt))) return st;
-        HMC_CUDA(cudaMemsetAsync(bt->b.accepted, 0, sizeof(unsigned long long) * bt->n_rep, bt->stream));
-        uint32_t color_count[8];
-        for (uint32_t c = 0; c < colors; ++c) color_count[c] = bt->host_stats->color_count[c];
-        for (uint32_t round = 0; round < max_rounds; ++round)
-            for (uint32_t c = 0; c < colors; ++c) {
-                HMC_CUDA(launch_sweep_batch(bt->dim, fp32, bt->b, bt->arr, c, round, color_count[c], bt->stream));
-                bt->kernel_launches += 1;
-            }
-        HMC_CUDA(cudaMemcpyAsync(bt->host_rep_u64, bt->b.accepted, sizeof(unsigned long long) * bt->n_rep,
-                                 cudaMemcpyDeviceToHost, bt->stream));
-        HMC_CUDA(cudaMemcpyAsync(bt->host_stats, bt->arr.stats, sizeof(DeviceStats), cudaMemcpyDeviceToHost, bt->stream));
-        HMC_CUDA(cudaStreamSynchronize(bt->stream));
-        for (uint32_t k = 0; k < bt->n_rep; ++k) {
-            Replica& r = bt->rep[k];
             const uint64_t acc = bt->host_rep_u64[k];
-            const uint64_t trials = (uint64_t)r.rounds * bt->host_nonempty[k];
+            const uint64_t trials = (uint64_t)r.rounds * ne;
             if (counts) {
                 counts[k].accepted += acc;
                 counts[k].rejected += trials - acc;
@@ -1322,6 +1346,7 @@ hmc_status hmc_batch_overlap_check(hmc_batch* bt, uint64_t* n_overlaps) {
     HMC_CUDA(cudaSetDevice(bt->ctx->device));
     hmc_status st = batch_rebuild(bt, true);
     if (st) return st;
+    if ((st = batch_read(bt))) return st;
     HMC_CUDA(launch_overlap_batch(bt->dim, bt->b, bt->arr, (uint32_t)bt->n, bt->stream));
     bt->kernel_launches += 1;
     HMC_CUDA(cudaMemcpyAsync(bt->host_rep_u64, bt->b.overlaps, sizeof(unsigned long long) * bt->n_rep,

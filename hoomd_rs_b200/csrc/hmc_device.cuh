@@ -326,6 +326,14 @@ __device__ __forceinline__ float fp32_dist2(const Geometry& g, float4 t32, float
     return dd;
 }
 
+// The length of the colour's list of non-empty spaces for this pass, or 0 when the pass is
+// beyond the sweep's rounds or the rebuild flagged an error (the state then stays untouched).
+__device__ __forceinline__ uint32_t active_count(const Arrays& A, uint32_t color, uint32_t round) {
+    const DeviceStats* st = A.stats;
+    if (st->error_flags != 0u || round >= st->rounds) return 0u;
+    return st->color_count[color];
+}
+
 __device__ __forceinline__ void flush_stats(DeviceStats* stats, const PairStats& st, uint32_t accepted) {
     const unsigned full = 0xffffffffu;
     unsigned acc = __reduce_add_sync(full, accepted);

@@ -26,6 +26,7 @@ struct DeviceStats {
     unsigned int error_flags;
     unsigned long long overlaps;      // pairs found by the overlap check
     unsigned int color_count[8];      // non-empty spaces per colour after a rebuild
+    unsigned int rounds;              // full colour sets of the sweep: ceil(N / non-empty spaces)
 };
 
 // The checkerboard (hoomd-mc/src/hypercuboid.rs) together with the periodic box.
@@ -58,6 +59,7 @@ struct Arrays {
     uint32_t* slot_of_body;  // [n] body index -> cell-order slot
     uint32_t* body_cell;     // [n]
     uint32_t* body_rank;     // [n]
+    uint32_t* body_m;        // [n] packed multi-index of each body's space (from the binning pass)
     uint32_t* cell_count;    // [cells]
     uint32_t* cell_start;    // [cells + 1]
     uint32_t* block_sums;    // scan scratch
@@ -93,7 +95,9 @@ struct Launch {
     uint32_t substep;
     uint32_t seed;
     uint32_t color;       // parity offsets: bit a of color (last axis = bit 0) is the offset on axis a
-    uint32_t n_active;    // non-empty spaces of this colour (length of its list)
+    uint32_t n_active;    // upper bound of the colour's list length (grid size); the kernels read
+                          // the length itself from DeviceStats::color_count
+    uint32_t round;       // colour set within the sweep; kernels skip it when >= DeviceStats::rounds
     double max_move;      // Translate maximum distance
     double kt;            // Isothermal temperature
     uint32_t n_bodies;
@@ -132,10 +136,12 @@ struct Batch {
 // write_s: also store the FP64 site positions S = wrap(B) in cell order (needed by the
 // plain FP64 pair test, the overlap check and injected-move evaluation).
 cudaError_t launch_rebuild(int dim, const Geometry& g, const Arrays& a, uint32_t n, bool write_s, cudaStream_t s);
+// Per-replica rounds of a batch sweep into Replica::rounds, their maximum into DeviceStats::rounds.
+cudaError_t launch_batch_rounds(const Batch& b, Replica* rep, DeviceStats* stats, cudaStream_t s);
 // Batches of hard-sphere replicas: the rebuild and the colour pass over all replicas at once.
 cudaError_t launch_rebuild_batch(int dim, const Batch& b, const Arrays& a, uint32_t n, bool write_s, cudaStream_t s);
 cudaError_t launch_sweep_batch(int dim, bool fp32, const Batch& b, const Arrays& a, uint32_t color, uint32_t round,
-                               uint32_t n_active, cudaStream_t s);
+                               uint32_t max_active, cudaStream_t s);
 cudaError_t launch_overlap_batch(int dim, const Batch& b, const Arrays& a, uint32_t n, cudaStream_t s);
 // coop selects the warp-cooperative pass (the per-lane pass otherwise).
 cudaError_t launch_sweep_sphere(int dim, bool fp32, const Geometry& g, const Arrays& a, const Pair& p,

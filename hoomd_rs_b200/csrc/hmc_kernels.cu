@@ -219,7 +219,8 @@ __global__ void __launch_bounds__(128, HMC_SWEEP_MIN_BLOCKS) k_sweep_sphere(Geom
     uint32_t n_accepted = 0;
     PairStats st;
     const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x; tid < L.n_active; tid += stride) {
+    const uint32_t n_active = active_count(A, L.color, L.round);
+    for (uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x; tid < n_active; tid += stride) {
         uint32_t m[3] = {0, 0, 0};
         unpack_m<DIM>(__ldg(A.color_cells + (size_t)L.color * g.color_stride + tid), m);
         if (sphere_trial<DIM, FP32>(g, A, P, A.cell_start, m, L.step, L.substep, L.seed, L.max_move, st))
@@ -297,14 +298,15 @@ __global__ void __launch_bounds__(128, HMC_SWEEP_MIN_BLOCKS) k_sweep_sphere_coop
     uint32_t n_accepted = 0;
     PairStats st;
     const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t base = blockIdx.x * blockDim.x + warp * 32; base < L.n_active; base += stride) {
+    const uint32_t n_active = active_count(A, L.color, L.round);
+    for (uint32_t base = blockIdx.x * blockDim.x + warp * 32; base < n_active; base += stride) {
         const uint32_t tid = base + lane;
         uint32_t m[3] = {0, 0, 0}, cell = 0, k = 0, sf = g.shape[DIM - 1], mf = 0;
         double t[3] = {0.0, 0.0, 0.0};
         float4 t32 = make_float4(0.f, 0.f, 0.f, 0.f);
         int res = kFlagOverlap;  // lanes without a trial in the cell count as decided
         bool edge = false, trial = false;
-        if (tid < L.n_active) {
+        if (tid < n_active) {
             unpack_m<DIM>(__ldg(A.color_cells + (size_t)L.color * g.color_stride + tid), m);
             cell = cell_index<DIM>(g, m);
             mf = m[DIM - 1];
@@ -443,6 +445,7 @@ __global__ void k_bin(Geometry g, Arrays A, uint32_t n) {
         cell = cell_index<DIM>(g, m);
     }
     A.body_cell[i] = cell;
+    A.body_m[i] = pack_m<DIM>(m);
     A.body_rank[i] = atomicAdd(&A.cell_count[cell], 1u);
 }
 
@@ -475,26 +478,8 @@ __device__ __forceinline__ T block_exclusive_scan(T v, T* total) {
     return warp_prefix + x - v;
 }
 
-// Each scan thread owns kScanItems consecutive spaces. Their colours (parity bits of the
-// multi-index, last axis = bit 0, as index_to_multi_index(c, [2; N]) in hypercuboid.rs)
-// are tallied as 16-bit fields of two packed u64 words (colours 0-3 and 4-7), so one
-// 64-bit block scan per word gives every colour's exclusive prefix at once.
-template <int DIM>
-__device__ __forceinline__ void first_multi_index(const Geometry& g, uint32_t c, uint32_t* m) {
-#pragma unroll
-    for (int a = DIM - 1; a >= 0; --a) {
-        m[a] = c % g.shape[a];
-        c /= g.shape[a];
-    }
-}
-template <int DIM>
-__device__ __forceinline__ void next_multi_index(const Geometry& g, uint32_t* m) {
-#pragma unroll
-    for (int a = DIM - 1; a >= 0; --a) {
-        if (++m[a] < g.shape[a]) return;
-        m[a] = 0;
-    }
-}
+// The colour of a space: the parity bits of its multi-index, last axis = bit 0, as
+// index_to_multi_index(c, [2; N]) in hypercuboid.rs orders the colours.
 template <int DIM>
 __device__ __forceinline__ uint32_t color_of(const uint32_t* m) {
     uint32_t color = 0;
@@ -503,169 +488,130 @@ __device__ __forceinline__ uint32_t color_of(const uint32_t* m) {
     return color;
 }
 
-template <int DIM>
-__global__ void __launch_bounds__(kScanThreads) k_scan_reduce(Geometry g, Arrays A) {
-    const uint32_t n_cells = g.n_cells;
-    uint32_t base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+
+// Exclusive scan of the space counts into cell_start: per-block totals, a single-block scan of
+// the totals, then each block's prefix.
+__global__ void __launch_bounds__(kScanThreads) k_count_reduce(const uint32_t* __restrict__ count, uint32_t n_cells,
+                                                               uint32_t* block_sums) {
+    const uint32_t base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
     uint32_t sum = 0;
-    unsigned long long lo = 0, hi = 0;
-    uint32_t m[3] = {0, 0, 0};
-    if (base < n_cells) first_multi_index<DIM>(g, base, m);
 #pragma unroll
-    for (int k = 0; k < kScanItems; ++k) {
-        uint32_t c = base + k;
-        uint32_t v = c < n_cells ? A.cell_count[c] : 0;
-        sum += v;
-        if (v > 0) {
-            uint32_t col = color_of<DIM>(m);
-            if (col < 4)
-                lo += 1ull << (16 * col);
-            else
-                hi += 1ull << (16 * (col - 4));
-        }
-        next_multi_index<DIM>(g, m);
-    }
-    uint32_t total;
-    unsigned long long tlo, thi;
-    block_exclusive_scan(sum, &total);
-    block_exclusive_scan(lo, &tlo);
-    block_exclusive_scan(hi, &thi);
+    for (int k = 0; k < kScanItems; ++k) sum += base + k < n_cells ? count[base + k] : 0u;
+    sum = __reduce_add_sync(0xffffffffu, sum);
+    __shared__ uint32_t warp_sums[kScanThreads / 32];
+    if ((threadIdx.x & 31) == 0) warp_sums[threadIdx.x >> 5] = sum;
+    __syncthreads();
     if (threadIdx.x == 0) {
-        const uint32_t nb = gridDim.x;
-        A.block_sums[blockIdx.x] = total;
+        uint32_t t = 0;
 #pragma unroll
-        for (int col = 0; col < 4; ++col) {
-            A.block_sums[(1 + col) * nb + blockIdx.x] = (uint32_t)((tlo >> (16 * col)) & 0xffffu);
-            A.block_sums[(5 + col) * nb + blockIdx.x] = (uint32_t)((thi >> (16 * col)) & 0xffffu);
-        }
+        for (int w = 0; w < kScanThreads / 32; ++w) t += warp_sums[w];
+        block_sums[blockIdx.x] = t;
     }
 }
 
-// Single block: exclusive scans (in place) of the block totals of the cell counts and of
-// the nine colour tallies; writes the per-colour totals and the non-empty count.
-__global__ void __launch_bounds__(1024) k_scan_block_sums(Arrays A, uint32_t n_blocks, uint32_t n_colors) {
+__global__ void __launch_bounds__(1024) k_count_block_sums(uint32_t* block_sums, uint32_t n_blocks) {
     __shared__ uint32_t warp_sums[32];
     constexpr int items = 8;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    uint32_t nonempty = 0;
-    for (uint32_t arr = 0; arr <= n_colors; ++arr) {
-        uint32_t* data = A.block_sums + (size_t)arr * n_blocks;
-        uint32_t b0 = threadIdx.x * items;
-        uint32_t v[items];
-        uint32_t sum = 0;
+    const uint32_t b0 = threadIdx.x * items;
+    uint32_t v[items];
+    uint32_t sum = 0;
 #pragma unroll
-        for (int k = 0; k < items; ++k) {
-            v[k] = b0 + k < n_blocks ? data[b0 + k] : 0;
-            sum += v[k];
-        }
-        uint32_t x = sum;
+    for (int k = 0; k < items; ++k) {
+        v[k] = b0 + k < n_blocks ? block_sums[b0 + k] : 0u;
+        sum += v[k];
+    }
+    uint32_t x = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_sums[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = warp_sums[lane];
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-            if (lane >= o) x += y;
+            const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
         }
-        if (lane == 31) warp_sums[warp] = x;
-        __syncthreads();
-        if (warp == 0) {
-            uint32_t w = warp_sums[lane];
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
-                if (lane >= o) w += y;
-            }
-            warp_sums[lane] = w;
-        }
-        __syncthreads();
-        uint32_t run = (warp > 0 ? warp_sums[warp - 1] : 0) + x - sum;
-#pragma unroll
-        for (int k = 0; k < items; ++k) {
-            if (b0 + k < n_blocks) data[b0 + k] = run;
-            run += v[k];
-        }
-        if (threadIdx.x == 0 && arr > 0) {
-            A.stats->color_count[arr - 1] = warp_sums[31];
-            nonempty += warp_sums[31];
-        }
-        __syncthreads();
+        warp_sums[lane] = w;
     }
-    if (threadIdx.x == 0) A.stats->nonempty = nonempty;
+    __syncthreads();
+    uint32_t run = (warp > 0 ? warp_sums[warp - 1] : 0u) + x - sum;
+#pragma unroll
+    for (int k = 0; k < items; ++k) {
+        if (b0 + k < n_blocks) block_sums[b0 + k] = run;
+        run += v[k];
+    }
 }
 
-template <int DIM>
-__global__ void __launch_bounds__(kScanThreads) k_scan_apply(Geometry g, Arrays A) {
-    const uint32_t n_cells = g.n_cells;
-    const uint32_t nb = gridDim.x;
-    uint32_t base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+__global__ void __launch_bounds__(kScanThreads) k_count_apply(const uint32_t* __restrict__ count, uint32_t n_cells,
+                                                              const uint32_t* __restrict__ block_sums,
+                                                              uint32_t* cell_start) {
+    const uint32_t base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
     uint32_t v[kScanItems];
     uint32_t sum = 0;
-    unsigned long long lo = 0, hi = 0;
-    uint32_t m[3] = {0, 0, 0};
-    if (base < n_cells) first_multi_index<DIM>(g, base, m);
-    uint32_t m0[3] = {m[0], m[1], m[2]};
 #pragma unroll
     for (int k = 0; k < kScanItems; ++k) {
-        uint32_t c = base + k;
-        v[k] = c < n_cells ? A.cell_count[c] : 0;
+        v[k] = base + k < n_cells ? count[base + k] : 0u;
         sum += v[k];
-        if (v[k] > 0) {
-            uint32_t col = color_of<DIM>(m);
-            if (col < 4)
-                lo += 1ull << (16 * col);
-            else
-                hi += 1ull << (16 * (col - 4));
-        }
-        next_multi_index<DIM>(g, m);
     }
     uint32_t total;
-    unsigned long long tlo, thi;
-    uint32_t run = block_exclusive_scan(sum, &total) + A.block_sums[blockIdx.x];
-    unsigned long long plo = block_exclusive_scan(lo, &tlo);
-    unsigned long long phi = block_exclusive_scan(hi, &thi);
-    uint32_t pos[8];
-#pragma unroll
-    for (int col = 0; col < 8; ++col) {
-        uint32_t within = col < 4 ? (uint32_t)((plo >> (16 * col)) & 0xffffu) : (uint32_t)((phi >> (16 * (col - 4))) & 0xffffu);
-        pos[col] = (col < (1 << DIM) ? A.block_sums[(1 + col) * nb + blockIdx.x] : 0u) + within;
-    }
-    m[0] = m0[0];
-    m[1] = m0[1];
-    m[2] = m0[2];
+    uint32_t run = block_exclusive_scan(sum, &total) + block_sums[blockIdx.x];
 #pragma unroll
     for (int k = 0; k < kScanItems; ++k) {
-        uint32_t c = base + k;
-        if (c < n_cells) A.cell_start[c] = run;
+        const uint32_t c = base + k;
+        if (c < n_cells) cell_start[c] = run;
         run += v[k];
-        if (c + 1 == n_cells) A.cell_start[n_cells] = run;
-        if (v[k] > 0) {
-            uint32_t col = color_of<DIM>(m);
-            A.color_cells[(size_t)col * g.color_stride + pos[col]] = pack_m<DIM>(m);
-            pos[col] += 1;
-        }
-        next_multi_index<DIM>(g, m);
+        if (c + 1 == n_cells) cell_start[n_cells] = run;
     }
 }
 
-__global__ void k_scatter(Arrays A, uint32_t n) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    A.sorted_body[A.cell_start[A.body_cell[i]] + A.body_rank[i]] = i;
+// Colour-list positions for one block: each lane with an entry gets a slot in its colour's
+// list. Lanes of a warp with the same colour take consecutive slots (shared-memory counters),
+// then one global atomic per colour and block reserves the block's run, so each list holds
+// runs of neighbouring spaces and the global counters see few atomics. The order within a
+// colour does not matter: its trials are independent. Call with every thread of the block.
+__device__ __forceinline__ uint32_t append_by_color(DeviceStats* stats, bool has, uint32_t col, uint32_t* s_count,
+                                                    uint32_t* s_base) {
+    const unsigned full = 0xffffffffu;
+    if (threadIdx.x < 8) s_count[threadIdx.x] = 0;
+    __syncthreads();
+    unsigned todo = __ballot_sync(full, has);
+    uint32_t pos = 0;
+    while (todo) {
+        const int leader = __ffs(todo) - 1;
+        const uint32_t cl = __shfl_sync(full, col, leader);
+        const unsigned same = __ballot_sync(full, has && col == cl);
+        uint32_t base = 0;
+        if ((int)(threadIdx.x & 31) == leader) base = atomicAdd(&s_count[cl], (unsigned)__popc(same));
+        base = __shfl_sync(full, base, leader);
+        if (has && col == cl) pos = base + __popc(same & ((1u << (threadIdx.x & 31)) - 1u));
+        todo &= ~same;
+    }
+    __syncthreads();
+    if (threadIdx.x < 8 && s_count[threadIdx.x]) s_base[threadIdx.x] = atomicAdd(&stats->color_count[threadIdx.x], s_count[threadIdx.x]);
+    __syncthreads();
+    return has ? s_base[col] + pos : 0u;
 }
 
-// One thread per space: order its bodies by index (the order in which update_checkerboard
-// pushes them, parallel_sweep.rs:194-200, which IndexedRandom::choose indexes), gather B,
-// the FP32 offsets of S = wrap(B) (and S itself when WRITE_S) and orientations into cell
-// order.
-template <int DIM, bool WRITE_S>
-__global__ void __launch_bounds__(128) k_finalize(Geometry g, Arrays A) {
+constexpr int kCellThreads = 1024;
+
+// Per space: order its bodies by index (the order update_checkerboard pushes them,
+// parallel_sweep.rs:194-200, which IndexedRandom::choose indexes), and list it under its
+// colour when it is not empty.
+template <int DIM>
+__global__ void __launch_bounds__(kCellThreads) k_cells(Geometry g, Arrays A) {
+    __shared__ uint32_t s_count[8], s_base[8], s_nonempty;
     const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool valid = c < g.n_cells;
     uint32_t s = 0, e = 0;
-    uint32_t m[3] = {0, 0, 0};
-    if (valid) {
+    if (c < g.n_cells) {
         s = A.cell_start[c];
         e = A.cell_start[c + 1];
         for (uint32_t k = s + 1; k < e; ++k) {
-            uint32_t v = A.sorted_body[k];
+            const uint32_t v = A.sorted_body[k];
             uint32_t j = k;
             while (j > s && A.sorted_body[j - 1] > v) {
                 A.sorted_body[j] = A.sorted_body[j - 1];
@@ -673,24 +619,52 @@ __global__ void __launch_bounds__(128) k_finalize(Geometry g, Arrays A) {
             }
             A.sorted_body[j] = v;
         }
-        uint32_t rem = c;
-#pragma unroll
-        for (int a = DIM - 1; a >= 0; --a) {
-            m[a] = rem % g.shape[a];
-            rem /= g.shape[a];
-        }
-        for (uint32_t k = s; k < e; ++k) {
-            uint32_t i = A.sorted_body[k];
-            A.slot_of_body[i] = k;
-            double4 b = A.body_pos[i];
-            A.sorted_b[k] = b;
-            double sv[3] = {b.x, b.y, b.z};
-            wrap_inv<DIM>(g.L, g.invL, sv);
-            if (WRITE_S) A.sorted_s[k] = make_double4(sv[0], sv[1], sv[2], 0.0);
-            A.sorted_off[k] = cell_offsets<DIM>(g, sv, m);
-            if (A.sorted_q) A.sorted_q[k] = A.body_ori[i];
-        }
     }
+    const bool has = e > s;
+    uint32_t packed = 0, col = 0;
+    if (has) {
+        packed = A.body_m[A.sorted_body[s]];
+        uint32_t m[3] = {0, 0, 0};
+        unpack_m<DIM>(packed, m);
+        col = color_of<DIM>(m);
+    }
+    if (threadIdx.x == 0) s_nonempty = 0;
+    const uint32_t pos = append_by_color(A.stats, has, col, s_count, s_base);
+    if (has) A.color_cells[(size_t)col * g.color_stride + pos] = packed;
+    const unsigned n_has = __popc(__ballot_sync(0xffffffffu, has));
+    if ((threadIdx.x & 31) == 0 && n_has) atomicAdd(&s_nonempty, n_has);
+    __syncthreads();
+    if (threadIdx.x == 0 && s_nonempty) atomicAdd(&A.stats->nonempty, s_nonempty);
+}
+
+// Per cell-order slot: gather B, S = wrap(B) (when WRITE_S), the FP32 offsets of S from its
+// space corner and the orientation; slot 0 also sets the sweep's rounds.
+template <int DIM, bool WRITE_S>
+__global__ void k_gather(Geometry g, Arrays A, uint32_t n) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    if (k == 0) {
+        const uint32_t ne = A.stats->nonempty;
+        // while count.total() < N: one trial per non-empty space per colour set (:402-418)
+        A.stats->rounds = ne == 0 ? 0u : (n + ne - 1) / ne;
+    }
+    const uint32_t i = A.sorted_body[k];
+    A.slot_of_body[i] = k;
+    const double4 b = A.body_pos[i];
+    A.sorted_b[k] = b;
+    double sv[3] = {b.x, b.y, b.z};
+    wrap_inv<DIM>(g.L, g.invL, sv);
+    if (WRITE_S) A.sorted_s[k] = make_double4(sv[0], sv[1], sv[2], 0.0);
+    uint32_t m[3] = {0, 0, 0};
+    unpack_m<DIM>(A.body_m[i], m);
+    A.sorted_off[k] = cell_offsets<DIM>(g, sv, m);
+    if (A.sorted_q) A.sorted_q[k] = A.body_ori[i];
+}
+
+__global__ void k_scatter(Arrays A, uint32_t n) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    A.sorted_body[A.cell_start[A.body_cell[i]] + A.body_rank[i]] = i;
 }
 
 // ---- overlap check (PairwiseCutoff::total_energy, pairwise_cutoff.rs:720-745) -------------
@@ -758,17 +732,6 @@ inline uint32_t blocks_for(T n, uint32_t threads) {
 // colour lists hold every replica's non-empty spaces of a colour, tagged with the replica.
 // Each replica keeps its own box, checkerboard and Counter, so every replica's trajectory is
 // the one its own system would produce; one launch serves all replicas.
-__device__ __forceinline__ uint32_t find_replica(const Batch& B, uint32_t c) {
-    uint32_t lo = 0, hi = B.n_replicas;  // largest r with cell_base[r] <= c
-    while (hi - lo > 1) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (__ldg(B.cell_base + mid) <= c)
-            lo = mid;
-        else
-            hi = mid;
-    }
-    return lo;
-}
 
 template <int DIM>
 __global__ void k_bin_batch(Batch B, Arrays A, uint32_t n) {
@@ -787,172 +750,80 @@ __global__ void k_bin_batch(Batch B, Arrays A, uint32_t n) {
     else
         cell += cell_index<DIM>(R.g, m);
     A.body_cell[i] = cell;
+    A.body_m[i] = pack_m<DIM>(m);
     A.body_rank[i] = atomicAdd(&A.cell_count[cell], 1u);
 }
 
-// A walk over consecutive spaces of the batch: replica, local index and multi-index.
-template <int DIM>
-struct SpaceCursor {
-    uint32_t r, local, end, m[3];
-    __device__ __forceinline__ void seek(const Batch& B, uint32_t c) {
-        r = find_replica(B, c);
-        local = c - __ldg(B.cell_base + r);
-        end = __ldg(B.cell_base + r + 1) - __ldg(B.cell_base + r);
-        uint32_t rem = local;
-        const Geometry& g = B.rep[r].g;
-#pragma unroll
-        for (int a = DIM - 1; a >= 0; --a) {
-            m[a] = rem % g.shape[a];
-            rem /= g.shape[a];
-        }
-        if (DIM == 2) m[2] = 0;
-    }
-    __device__ __forceinline__ void next(const Batch& B) {
-        if (++local == end && r + 1 < B.n_replicas) {
-            ++r;
-            local = 0;
-            end = __ldg(B.cell_base + r + 1) - __ldg(B.cell_base + r);
-            m[0] = m[1] = m[2] = 0;
-            return;
-        }
-        const Geometry& g = B.rep[r].g;
-#pragma unroll
-        for (int a = DIM - 1; a >= 0; --a) {
-            if (++m[a] < g.shape[a]) return;
-            m[a] = 0;
-        }
-    }
-};
+
+
+
 
 template <int DIM>
-__global__ void __launch_bounds__(kScanThreads) k_scan_reduce_batch(Batch B, Arrays A) {
-    const uint32_t base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
-    uint32_t sum = 0;
-    unsigned long long lo = 0, hi = 0;
-    SpaceCursor<DIM> cur;
-    if (base < B.n_cells) cur.seek(B, base);
-#pragma unroll
-    for (int k = 0; k < kScanItems; ++k) {
-        const uint32_t c = base + k;
-        const uint32_t v = c < B.n_cells ? A.cell_count[c] : 0;
-        sum += v;
-        if (v > 0) {
-            const uint32_t col = color_of<DIM>(cur.m);
-            if (col < 4)
-                lo += 1ull << (16 * col);
-            else
-                hi += 1ull << (16 * (col - 4));
-        }
-        if (c + 1 < B.n_cells) cur.next(B);
-    }
-    uint32_t total;
-    unsigned long long tlo, thi;
-    block_exclusive_scan(sum, &total);
-    block_exclusive_scan(lo, &tlo);
-    block_exclusive_scan(hi, &thi);
-    if (threadIdx.x == 0) {
-        const uint32_t nb = gridDim.x;
-        A.block_sums[blockIdx.x] = total;
-#pragma unroll
-        for (int col = 0; col < 4; ++col) {
-            A.block_sums[(1 + col) * nb + blockIdx.x] = (uint32_t)((tlo >> (16 * col)) & 0xffffu);
-            A.block_sums[(5 + col) * nb + blockIdx.x] = (uint32_t)((thi >> (16 * col)) & 0xffffu);
-        }
-    }
-}
-
-template <int DIM>
-__global__ void __launch_bounds__(kScanThreads) k_scan_apply_batch(Batch B, Arrays A) {
-    const uint32_t nb = gridDim.x;
-    const uint32_t base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
-    uint32_t v[kScanItems];
-    uint32_t sum = 0;
-    unsigned long long lo = 0, hi = 0;
-    SpaceCursor<DIM> cur;
-    if (base < B.n_cells) cur.seek(B, base);
-    SpaceCursor<DIM> first = cur;
-#pragma unroll
-    for (int k = 0; k < kScanItems; ++k) {
-        const uint32_t c = base + k;
-        v[k] = c < B.n_cells ? A.cell_count[c] : 0;
-        sum += v[k];
-        if (v[k] > 0) {
-            const uint32_t col = color_of<DIM>(cur.m);
-            if (col < 4)
-                lo += 1ull << (16 * col);
-            else
-                hi += 1ull << (16 * (col - 4));
-        }
-        if (c + 1 < B.n_cells) cur.next(B);
-    }
-    uint32_t total;
-    unsigned long long tlo, thi;
-    uint32_t run = block_exclusive_scan(sum, &total) + A.block_sums[blockIdx.x];
-    const unsigned long long plo = block_exclusive_scan(lo, &tlo);
-    const unsigned long long phi = block_exclusive_scan(hi, &thi);
-    uint32_t pos[8];
-#pragma unroll
-    for (int col = 0; col < 8; ++col) {
-        const uint32_t within =
-            col < 4 ? (uint32_t)((plo >> (16 * col)) & 0xffffu) : (uint32_t)((phi >> (16 * (col - 4))) & 0xffffu);
-        pos[col] = (col < (1 << DIM) ? A.block_sums[(1 + col) * nb + blockIdx.x] : 0u) + within;
-    }
-    cur = first;
-    uint32_t counted = 0;
-#pragma unroll
-    for (int k = 0; k < kScanItems; ++k) {
-        const uint32_t c = base + k;
-        if (c < B.n_cells) A.cell_start[c] = run;
-        run += v[k];
-        if (c + 1 == B.n_cells) A.cell_start[B.n_cells] = run;
-        if (v[k] > 0) {
-            const uint32_t col = color_of<DIM>(cur.m);
-            const size_t e = (size_t)col * B.color_stride + pos[col];
-            A.color_cells[e] = pack_m<DIM>(cur.m);
-            B.color_rep[e] = cur.r;
-            pos[col] += 1;
-            counted += 1;
-        }
-        if (c + 1 < B.n_cells) {
-            const uint32_t r_before = cur.r;
-            cur.next(B);
-            if (cur.r != r_before) {  // the run of spaces crossed into the next replica
-                if (counted) atomicAdd(B.nonempty + r_before, counted);
-                counted = 0;
+__global__ void __launch_bounds__(kCellThreads) k_cells_batch(Batch B, Arrays A) {
+    __shared__ uint32_t s_count[8], s_base[8], s_nonempty;
+    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t s = 0, e = 0;
+    if (c < B.n_cells) {
+        s = A.cell_start[c];
+        e = A.cell_start[c + 1];
+        for (uint32_t k = s + 1; k < e; ++k) {
+            const uint32_t v = A.sorted_body[k];
+            uint32_t j = k;
+            while (j > s && A.sorted_body[j - 1] > v) {
+                A.sorted_body[j] = A.sorted_body[j - 1];
+                --j;
             }
+            A.sorted_body[j] = v;
         }
     }
-    if (counted && base < B.n_cells) atomicAdd(B.nonempty + cur.r, counted);
+    const bool has = e > s;
+    uint32_t packed = 0, col = 0, r = 0xffffffffu;
+    if (has) {
+        const uint32_t first = A.sorted_body[s];
+        packed = A.body_m[first];
+        r = __ldg(B.body_rep + first);
+        uint32_t m[3] = {0, 0, 0};
+        unpack_m<DIM>(packed, m);
+        col = color_of<DIM>(m);
+    }
+    if (threadIdx.x == 0) s_nonempty = 0;
+    const uint32_t pos = append_by_color(A.stats, has, col, s_count, s_base);
+    if (has) {
+        const size_t entry = (size_t)col * B.color_stride + pos;
+        A.color_cells[entry] = packed;
+        B.color_rep[entry] = r;
+    }
+    const unsigned n_has = __popc(__ballot_sync(0xffffffffu, has));
+    if ((threadIdx.x & 31) == 0 && n_has) atomicAdd(&s_nonempty, n_has);
+    __syncthreads();
+    if (threadIdx.x == 0 && s_nonempty) atomicAdd(&A.stats->nonempty, s_nonempty);
+    // non-empty spaces per replica, one atomic per replica present in the warp
+    const unsigned full = 0xffffffffu;
+    unsigned todo = __ballot_sync(full, has);
+    while (todo) {
+        const int leader = __ffs(todo) - 1;
+        const uint32_t rl = __shfl_sync(full, r, leader);
+        const unsigned same = __ballot_sync(full, has && r == rl);
+        if ((int)(threadIdx.x & 31) == leader) atomicAdd(B.nonempty + rl, (unsigned)__popc(same));
+        todo &= ~same;
+    }
 }
 
 template <int DIM, bool WRITE_S>
-__global__ void __launch_bounds__(128) k_finalize_batch(Batch B, Arrays A) {
-    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= B.n_cells) return;
-    const uint32_t s = A.cell_start[c], e = A.cell_start[c + 1];
-    if (s == e) return;
-    for (uint32_t k = s + 1; k < e; ++k) {
-        const uint32_t v = A.sorted_body[k];
-        uint32_t j = k;
-        while (j > s && A.sorted_body[j - 1] > v) {
-            A.sorted_body[j] = A.sorted_body[j - 1];
-            --j;
-        }
-        A.sorted_body[j] = v;
-    }
-    SpaceCursor<DIM> cur;
-    cur.seek(B, c);
-    const Geometry& g = B.rep[cur.r].g;
-    for (uint32_t k = s; k < e; ++k) {
-        const uint32_t i = A.sorted_body[k];
-        A.slot_of_body[i] = k;
-        const double4 b = A.body_pos[i];
-        A.sorted_b[k] = b;
-        double sv[3] = {b.x, b.y, b.z};
-        wrap_inv<DIM>(g.L, g.invL, sv);
-        if (WRITE_S) A.sorted_s[k] = make_double4(sv[0], sv[1], sv[2], 0.0);
-        A.sorted_off[k] = cell_offsets<DIM>(g, sv, cur.m);
-    }
+__global__ void k_gather_batch(Batch B, Arrays A, uint32_t n) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const uint32_t i = A.sorted_body[k];
+    const Geometry& g = B.rep[__ldg(B.body_rep + i)].g;
+    A.slot_of_body[i] = k;
+    const double4 b = A.body_pos[i];
+    A.sorted_b[k] = b;
+    double sv[3] = {b.x, b.y, b.z};
+    wrap_inv<DIM>(g.L, g.invL, sv);
+    if (WRITE_S) A.sorted_s[k] = make_double4(sv[0], sv[1], sv[2], 0.0);
+    uint32_t m[3] = {0, 0, 0};
+    unpack_m<DIM>(A.body_m[i], m);
+    A.sorted_off[k] = cell_offsets<DIM>(g, sv, m);
 }
 
 // Accepted moves per replica from one warp: the lanes of each replica in the warp add up.
@@ -972,7 +843,8 @@ __device__ __forceinline__ void add_per_replica(unsigned long long* acc, uint32_
 // One colour pass over all replicas that still run round `round` of this sweep.
 template <int DIM, bool FP32>
 __global__ void __launch_bounds__(128, HMC_SWEEP_MIN_BLOCKS) k_sweep_batch(Batch B, Arrays A, uint32_t color,
-                                                                             uint32_t round, uint32_t n_active) {
+                                                                             uint32_t round) {
+    const uint32_t n_active = active_count(A, color, round);
     uint32_t n_accepted = 0;
     PairStats st;
     const uint32_t stride = gridDim.x * blockDim.x;
@@ -995,6 +867,16 @@ __global__ void __launch_bounds__(128, HMC_SWEEP_MIN_BLOCKS) k_sweep_batch(Batch
         add_per_replica(B.accepted, r, accepted);
     }
     flush_stats(A.stats, st, n_accepted);
+}
+
+// Rounds of every replica (ceil(N_r / non-empty spaces of r)) and their maximum.
+__global__ void k_batch_rounds(Batch B, Replica* rep, DeviceStats* stats) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= B.n_replicas) return;
+    const uint32_t n = rep[r].n_bodies, ne = B.nonempty[r];
+    const uint32_t rounds = (n == 0 || ne == 0) ? 0u : (n + ne - 1) / ne;
+    rep[r].rounds = rounds;
+    atomicMax(&stats->rounds, rounds);
 }
 
 // Overlapping pairs (i < j) of every replica, FP64.
@@ -1120,6 +1002,16 @@ cudaError_t launch_pack_angles(const double4* body_ori, double* packed, uint64_t
     return cudaGetLastError();
 }
 
+namespace {
+cudaError_t launch_count_scan(const Arrays& a, uint32_t n_cells, cudaStream_t s) {
+    const uint32_t nb = blocks_for(n_cells, kScanTile);
+    k_count_reduce<<<nb, kScanThreads, 0, s>>>(a.cell_count, n_cells, a.block_sums);
+    k_count_block_sums<<<1, 1024, 0, s>>>(a.block_sums, nb);
+    k_count_apply<<<nb, kScanThreads, 0, s>>>(a.cell_count, n_cells, a.block_sums, a.cell_start);
+    return cudaGetLastError();
+}
+}  // namespace
+
 cudaError_t launch_rebuild(int dim, const Geometry& g, const Arrays& a, uint32_t n, bool write_s, cudaStream_t s) {
     cudaError_t e = cudaMemsetAsync(a.cell_count, 0, sizeof(uint32_t) * g.n_cells, s);
     if (e != cudaSuccess) return e;
@@ -1129,28 +1021,22 @@ cudaError_t launch_rebuild(int dim, const Geometry& g, const Arrays& a, uint32_t
         else
             k_bin<3><<<blocks_for(n, 256), 256, 0, s>>>(g, a, n);
     }
-    uint32_t nb = blocks_for(g.n_cells, kScanTile);
-    if (dim == 2)
-        k_scan_reduce<2><<<nb, kScanThreads, 0, s>>>(g, a);
-    else
-        k_scan_reduce<3><<<nb, kScanThreads, 0, s>>>(g, a);
-    k_scan_block_sums<<<1, 1024, 0, s>>>(a, nb, 1u << dim);
-    if (dim == 2)
-        k_scan_apply<2><<<nb, kScanThreads, 0, s>>>(g, a);
-    else
-        k_scan_apply<3><<<nb, kScanThreads, 0, s>>>(g, a);
-    if (n > 0) k_scatter<<<blocks_for(n, 256), 256, 0, s>>>(a, n);
-    uint32_t fb = blocks_for(g.n_cells, 128);
+    if ((e = launch_count_scan(a, g.n_cells, s)) != cudaSuccess) return e;
+    if (n == 0) return cudaSuccess;
+    k_scatter<<<blocks_for(n, 256), 256, 0, s>>>(a, n);
+    const uint32_t cb = blocks_for(g.n_cells, kCellThreads), gb = blocks_for(n, 256);
     if (dim == 2) {
+        k_cells<2><<<cb, kCellThreads, 0, s>>>(g, a);
         if (write_s)
-            k_finalize<2, true><<<fb, 128, 0, s>>>(g, a);
+            k_gather<2, true><<<gb, 256, 0, s>>>(g, a, n);
         else
-            k_finalize<2, false><<<fb, 128, 0, s>>>(g, a);
+            k_gather<2, false><<<gb, 256, 0, s>>>(g, a, n);
     } else {
+        k_cells<3><<<cb, kCellThreads, 0, s>>>(g, a);
         if (write_s)
-            k_finalize<3, true><<<fb, 128, 0, s>>>(g, a);
+            k_gather<3, true><<<gb, 256, 0, s>>>(g, a, n);
         else
-            k_finalize<3, false><<<fb, 128, 0, s>>>(g, a);
+            k_gather<3, false><<<gb, 256, 0, s>>>(g, a, n);
     }
     return cudaGetLastError();
 }
@@ -1165,35 +1051,29 @@ cudaError_t launch_rebuild_batch(int dim, const Batch& b, const Arrays& a, uint3
         else
             k_bin_batch<3><<<blocks_for(n, 256), 256, 0, s>>>(b, a, n);
     }
-    const uint32_t nb = blocks_for(b.n_cells, kScanTile);
-    if (dim == 2)
-        k_scan_reduce_batch<2><<<nb, kScanThreads, 0, s>>>(b, a);
-    else
-        k_scan_reduce_batch<3><<<nb, kScanThreads, 0, s>>>(b, a);
-    k_scan_block_sums<<<1, 1024, 0, s>>>(a, nb, 1u << dim);
-    if (dim == 2)
-        k_scan_apply_batch<2><<<nb, kScanThreads, 0, s>>>(b, a);
-    else
-        k_scan_apply_batch<3><<<nb, kScanThreads, 0, s>>>(b, a);
-    if (n > 0) k_scatter<<<blocks_for(n, 256), 256, 0, s>>>(a, n);
-    const uint32_t fb = blocks_for(b.n_cells, 128);
+    if ((e = launch_count_scan(a, b.n_cells, s)) != cudaSuccess) return e;
+    if (n == 0) return cudaSuccess;
+    k_scatter<<<blocks_for(n, 256), 256, 0, s>>>(a, n);
+    const uint32_t cb = blocks_for(b.n_cells, kCellThreads), gb = blocks_for(n, 256);
     if (dim == 2) {
+        k_cells_batch<2><<<cb, kCellThreads, 0, s>>>(b, a);
         if (write_s)
-            k_finalize_batch<2, true><<<fb, 128, 0, s>>>(b, a);
+            k_gather_batch<2, true><<<gb, 256, 0, s>>>(b, a, n);
         else
-            k_finalize_batch<2, false><<<fb, 128, 0, s>>>(b, a);
+            k_gather_batch<2, false><<<gb, 256, 0, s>>>(b, a, n);
     } else {
+        k_cells_batch<3><<<cb, kCellThreads, 0, s>>>(b, a);
         if (write_s)
-            k_finalize_batch<3, true><<<fb, 128, 0, s>>>(b, a);
+            k_gather_batch<3, true><<<gb, 256, 0, s>>>(b, a, n);
         else
-            k_finalize_batch<3, false><<<fb, 128, 0, s>>>(b, a);
+            k_gather_batch<3, false><<<gb, 256, 0, s>>>(b, a, n);
     }
     return cudaGetLastError();
 }
 
 cudaError_t launch_sweep_batch(int dim, bool fp32, const Batch& b, const Arrays& a, uint32_t color, uint32_t round,
-                               uint32_t n_active, cudaStream_t s) {
-    if (n_active == 0) return cudaSuccess;
+                               uint32_t max_active, cudaStream_t s) {
+    if (max_active == 0) return cudaSuccess;
     static int max_blocks[2][2] = {{0, 0}, {0, 0}};
     int& mb = max_blocks[dim == 3][fp32];
     if (mb == 0) {
@@ -1210,19 +1090,24 @@ cudaError_t launch_sweep_batch(int dim, bool fp32, const Batch& b, const Arrays&
         if (e != cudaSuccess) return e;
         mb = sms * (per_sm > 0 ? per_sm : 1);
     }
-    uint32_t grid = blocks_for(n_active, 128);
+    uint32_t grid = blocks_for(max_active, 128);
     if (grid > (uint32_t)mb) grid = (uint32_t)mb;
     if (dim == 2) {
         if (fp32)
-            k_sweep_batch<2, true><<<grid, 128, 0, s>>>(b, a, color, round, n_active);
+            k_sweep_batch<2, true><<<grid, 128, 0, s>>>(b, a, color, round);
         else
-            k_sweep_batch<2, false><<<grid, 128, 0, s>>>(b, a, color, round, n_active);
+            k_sweep_batch<2, false><<<grid, 128, 0, s>>>(b, a, color, round);
     } else {
         if (fp32)
-            k_sweep_batch<3, true><<<grid, 128, 0, s>>>(b, a, color, round, n_active);
+            k_sweep_batch<3, true><<<grid, 128, 0, s>>>(b, a, color, round);
         else
-            k_sweep_batch<3, false><<<grid, 128, 0, s>>>(b, a, color, round, n_active);
+            k_sweep_batch<3, false><<<grid, 128, 0, s>>>(b, a, color, round);
     }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_rounds(const Batch& b, Replica* rep, DeviceStats* stats, cudaStream_t s) {
+    k_batch_rounds<<<blocks_for(b.n_replicas, 128), 128, 0, s>>>(b, rep, stats);
     return cudaGetLastError();
 }
 

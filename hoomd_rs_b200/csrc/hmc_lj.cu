@@ -246,7 +246,8 @@ __global__ void __launch_bounds__(128) k_sweep_lj(Geometry g, Arrays A, Pair P, 
     const uint32_t n_warps = (gridDim.x * blockDim.x) >> 5;
     uint32_t n_accepted = 0;
     PairStats pst;
-    for (uint32_t w = warp; w < L.n_active; w += n_warps) {
+    const uint32_t n_active = active_count(A, L.color, L.round);
+    for (uint32_t w = warp; w < n_active; w += n_warps) {
         uint32_t m[3] = {0, 0, 0};
         unpack_m<DIM>(__ldg(A.color_cells + (size_t)L.color * g.color_stride + w), m);
         const uint32_t cell = cell_index<DIM>(g, m);

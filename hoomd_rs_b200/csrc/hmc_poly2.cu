@@ -238,7 +238,8 @@ __global__ void __launch_bounds__(128) k_sweep_poly2(Geometry g, Arrays A, PolyS
     uint32_t n_accepted = 0;
     PairStats st;
     bool range_error = false;
-    for (uint32_t w = warp; w < L.n_active; w += n_warps) {
+    const uint32_t n_active = active_count(A, L.color, L.round);
+    for (uint32_t w = warp; w < n_active; w += n_warps) {
         uint32_t m[3] = {0, 0, 0};
         unpack_m<2>(__ldg(A.color_cells + (size_t)L.color * g.color_stride + w), m);
         const uint32_t cell = cell_index<2>(g, m);
