@@ -96,6 +96,8 @@ SIGNATURES = {
     "hmc_get_state": (C.c_int, [_vp, _dp, _dp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32)]),
     "hmc_increment_step": (C.c_int, [_vp]),
     "hmc_math_sincos": (C.c_int, [_vp, _dp, C.c_uint64, _dp, _dp]),
+    "hmc_sdf": (C.c_int, [_vp, C.c_double, C.c_uint32, C.POINTER(C.c_uint64)]),
+    "hmc_gr": (C.c_int, [_vp, C.c_double, C.c_uint32, C.POINTER(C.c_uint64)]),
     "hmc_batch_create": (C.c_int, [_vp, C.c_uint32, C.POINTER(hmc_system_desc), C.POINTER(_dp), C.POINTER(_vp)]),
     "hmc_batch_destroy": (None, [_vp]),
     "hmc_batch_sweep": (C.c_int, [_vp, C.POINTER(hmc_sweep_params), C.POINTER(hmc_count), C.POINTER(hmc_count)]),
@@ -347,6 +349,28 @@ class Translate:
         return cls(float(d))
 
 
+def sdf_pressure(counts, n: int, volume: float, dim: int, x_max: float, fit_bins: int = 12) -> float:
+    """beta P = rho (1 + s(0+) / dim) from SDF pair counts (pairs counted once, s = counts/(N dx))."""
+    counts = np.asarray(counts, dtype=np.float64)
+    dx = x_max / counts.size
+    x = (np.arange(counts.size) + 0.5) * dx
+    sx = counts / (n * dx)
+    k = min(fit_bins, counts.size)
+    s0 = np.polyval(np.polyfit(x[:k], sx[:k], 2), 0.0)
+    rho = n / volume
+    return float(rho * (1.0 + s0 / dim))
+
+
+def gr_normalise(counts, n: int, volume: float, dim: int, r_max: float) -> "tuple[np.ndarray, np.ndarray]":
+    """(r, g(r)) from pair counts (pairs counted once)."""
+    counts = np.asarray(counts, dtype=np.float64)
+    edges = np.linspace(0.0, r_max, counts.size + 1)
+    shell = (np.pi * (edges[1:] ** 2 - edges[:-1] ** 2) if dim == 2
+             else 4.0 / 3.0 * np.pi * (edges[1:] ** 3 - edges[:-1] ** 3))
+    ideal = 0.5 * n * (n - 1) / volume * shell
+    return 0.5 * (edges[1:] + edges[:-1]), counts / ideal
+
+
 class Microstate:
     """Bodies in a periodic box, resident on the GPU (one hmc_system)."""
 
@@ -457,6 +481,26 @@ class Microstate:
         p = hmc_sweep_params(C.sizeof(hmc_sweep_params), move, maximum, temperature, precision, 1, 0, 0)
         _check(_lib.hmc_tune(self._h, C.byref(p), target, samples, steps))
         return p.maximum
+
+    def sdf(self, x_max: float = 0.02, n_bins: int = 40) -> np.ndarray:
+        """Pair counts (i < j) by x = 1 - sigma/r over [0, x_max) (hard spheres)."""
+        out = np.zeros(n_bins, dtype=np.uint64)
+        _check(_lib.hmc_sdf(self._h, x_max, n_bins, out.ctypes.data_as(C.POINTER(C.c_uint64))))
+        return out
+
+    def gr_counts(self, r_max: float, n_bins: int) -> np.ndarray:
+        """Pair counts (i < j) by minimum-image distance over [0, r_max)."""
+        out = np.zeros(n_bins, dtype=np.uint64)
+        _check(_lib.hmc_gr(self._h, r_max, n_bins, out.ctypes.data_as(C.POINTER(C.c_uint64))))
+        return out
+
+    def pressure(self, x_max: float = 0.02, n_bins: int = 40, fit_bins: int = 12) -> float:
+        """beta P from the scale distribution: rho (1 + s(0+) / dim), s(x) = counts / (N dx)
+        extrapolated to x = 0 by a quadratic fit over the first fit_bins bins."""
+        return sdf_pressure(self.sdf(x_max, n_bins), self.n, self.volume(), self.dim, x_max, fit_bins)
+
+    def volume(self) -> float:
+        return float(np.prod(self.edge_lengths))
 
     def overlap_count(self) -> int:
         n = C.c_uint64()
@@ -644,7 +688,7 @@ class ParallelSweep:
             self.local_trial.maximum_rotation = tuned
 
 
-__all__ = ["Batch", "Context", "ConvexPolygon", "ConvexPolyhedron", "ConvexSurfaceMesh2d", "Count", "convex_hull_2d", "HardShape", "HardSphere", "HmcError", "Isothermal", "Isotropic",
+__all__ = ["Batch", "Context", "sdf_pressure", "gr_normalise", "ConvexPolygon", "ConvexPolyhedron", "ConvexSurfaceMesh2d", "Count", "convex_hull_2d", "HardShape", "HardSphere", "HmcError", "Isothermal", "Isotropic",
            "LennardJones", "Microstate", "PairwiseCutoff", "Rotate", "Shifted", "TuneOptions",
            "ParallelSweep", "Periodic", "Translate", "load_library", "SIGNATURES", "FP64", "FP32_RECHECK",
            "TRANSLATE", "ROTATE", "HARD_SPHERE", "HARD_CONVEX_POLYGON", "HARD_CONVEX_POLYHEDRON", "LENNARD_JONES",

@@ -860,6 +860,62 @@ hmc_status hmc_overlap_check(hmc_system* s, uint64_t* n_overlaps) {
     return HMC_OK;
 }
 
+// Pair histogram on a checkerboard at least `reach` wide (so the 3^d stencil holds every pair
+// binned); the next sweep rebuilds its own checkerboard.
+static hmc_status pair_histogram(hmc_system* s, bool sdf, double sigma, double limit, double reach, uint32_t n_bins,
+                                 uint64_t* counts) {
+    if (!counts || n_bins == 0 || n_bins > 8192) return fail(HMC_INVALID_ARGUMENT, "1 to 8192 bins");
+    if (!(limit > 0.0) || !std::isfinite(limit)) return fail(HMC_INVALID_ARGUMENT, "the histogram range must be positive");
+    HMC_CUDA(cudaSetDevice(s->ctx->device));
+    Geometry g = s->geom;
+    const double range = std::max(reach, s->body_range);
+    if (!compute_dimensions(s->dim, g.L, range, g.width, g.shape))
+        return fail(HMC_RANGE_TOO_LARGE, "a histogram reaching %g needs at least two spaces of that width per axis", range);
+    uint64_t cells = 1;
+    g.any_two = 0;
+    for (int a = 0; a < s->dim; ++a) {
+        g.w32[a] = (float)g.width[a];
+        g.invW[a] = 1.0 / g.width[a];
+        g.half_shape[a] = g.shape[a] / 2;
+        if (g.shape[a] == 2) g.any_two = 1;
+        g.origin[a] = -g.L[a] / 2.0;
+        cells *= g.shape[a];
+    }
+    g.n_cells = (uint32_t)cells;  // no more than the system's own spaces: these are wider
+    g.color_stride = (uint32_t)(cells >> s->dim);
+    HMC_CUDA(cudaMemsetAsync(s->arr.stats, 0, sizeof(DeviceStats), s->stream));
+    HMC_CUDA(launch_rebuild(s->dim, g, s->arr, (uint32_t)s->n, true, s->stream));
+    unsigned long long* d = nullptr;
+    HMC_CUDA(cudaMallocAsync((void**)&d, sizeof(unsigned long long) * n_bins, s->stream));
+    cudaError_t e = launch_pair_histogram(s->dim, sdf, g, s->arr, (uint32_t)s->n, sigma, limit, (double)n_bins / limit,
+                                          n_bins, d, s->stream);
+    std::vector<unsigned long long> h(n_bins);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), d, sizeof(unsigned long long) * n_bins, cudaMemcpyDeviceToHost, s->stream);
+    cudaFreeAsync(d, s->stream);
+    cudaError_t e2 = cudaStreamSynchronize(s->stream);
+    if (e == cudaSuccess) e = e2;
+    if (e != cudaSuccess) return fail(HMC_CUDA_ERROR, "pair histogram: %s", cudaGetErrorString(e));
+    s->prof.kernel_launches += 8;
+    hmc_status st;
+    if ((st = read_stats(s))) return st;
+    if ((st = check_flags(s))) return st;
+    for (uint32_t b = 0; b < n_bins; ++b) counts[b] = h[b];
+    return HMC_OK;
+}
+
+hmc_status hmc_sdf(hmc_system* s, double x_max, uint32_t n_bins, uint64_t* counts) {
+    if (!s) return fail(HMC_INVALID_ARGUMENT, "NULL system");
+    if (s->interaction != HMC_HARD_SPHERE) return fail(HMC_NOT_SUPPORTED, "the scale distribution is for hard spheres");
+    if (!(x_max > 0.0 && x_max < 0.5)) return fail(HMC_INVALID_ARGUMENT, "x_max must be in (0, 0.5)");
+    const double sigma = std::sqrt(s->pair.sigma2);
+    return pair_histogram(s, true, sigma, x_max, sigma / (1.0 - x_max), n_bins, counts);
+}
+
+hmc_status hmc_gr(hmc_system* s, double r_max, uint32_t n_bins, uint64_t* counts) {
+    if (!s) return fail(HMC_INVALID_ARGUMENT, "NULL system");
+    return pair_histogram(s, false, 0.0, r_max, r_max, n_bins, counts);
+}
+
 hmc_status hmc_total_energy(hmc_system* s, double* energy) {
     if (!s || !energy) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
     if (s->interaction != HMC_LENNARD_JONES) {

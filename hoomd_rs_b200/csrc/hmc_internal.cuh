@@ -185,6 +185,11 @@ cudaError_t launch_sincos(const double* x, uint64_t n, double* sn, double* cs, u
 cudaError_t launch_check_angles(const double* packed, uint64_t n, unsigned long long* first_bad, cudaStream_t s);
 cudaError_t launch_unpack_angles(const double* packed, double4* body_ori, uint64_t n, cudaStream_t s);
 cudaError_t launch_pack_angles(const double4* body_ori, double* packed, uint64_t n, cudaStream_t s);
+// Pair histograms over the current cell list (built with spaces at least `limit` wide, FP64 S):
+// SDF (x = 1 - sigma/r in [0, limit)) or g(r) (r in [0, limit)), bins of 1/inv_width.
+cudaError_t launch_pair_histogram(int dim, bool sdf, const Geometry& g, const Arrays& a, uint32_t n, double sigma,
+                                  double limit, double inv_width, uint32_t n_bins, unsigned long long* counts,
+                                  cudaStream_t s);
 // State transfer through a packed staging array of n x dim doubles (the host layout):
 // first_nonfinite receives the smallest body index with a non-finite coordinate (it must hold
 // ~0 before the launch); unpack writes body positions, pack reads them.

@@ -696,6 +696,65 @@ __global__ void k_overlap_sphere(Geometry g, Arrays A, Pair P, uint32_t n) {
     if ((threadIdx.x & 31) == 0 && tot) atomicAdd(&A.stats->overlaps, (unsigned long long)tot);
 }
 
+// ---- pair distributions: scale distribution function and g(r) ------------------------------
+// Both histogram the pairs i < j by their minimum-image distance, d = t - s - L rint((t - s)/L)
+// per axis, r^2 = sum d^2 (no hoomd-rs counterpart: these estimators are the survey's
+// equilibrium checks). SDF: x = 1 - sigma / r, bin floor(x * inv_dx) for x in [0, x_max),
+// the scale at which the pair would overlap if the box shrank by (1 - x) (spheres only).
+// g(r): bin floor(r * inv_dr) for r < r_max. The walk needs spaces at least as wide as the
+// largest distance binned; the host rebuilds the cell list with such a checkerboard first.
+template <int DIM>
+__device__ __forceinline__ double min_image_dist2(const Geometry& g, const double* t, const double* s) {
+    double p = 0.0;
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) {
+        double d = dsub(t[a], s[a]);
+        const double k = rint(ddiv(d, g.L[a]));
+        d = dsub(d, dmul(k, g.L[a]));
+        p = dadd(p, dmul(d, d));
+    }
+    return p;
+}
+
+template <int DIM, bool SDF>
+__global__ void __launch_bounds__(256) k_pair_histogram(Geometry g, Arrays A, uint32_t n, double sigma, double limit,
+                                                       double inv_width, uint32_t n_bins,
+                                                       unsigned long long* counts) {
+    extern __shared__ unsigned int s_hist[];
+    for (uint32_t b = threadIdx.x; b < n_bins; b += blockDim.x) s_hist[b] = 0;
+    __syncthreads();
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) {
+        const uint32_t bi = A.sorted_body[k];
+        const double4 s4 = A.sorted_s[k];
+        const double t[3] = {s4.x, s4.y, s4.z};
+        uint32_t m[3] = {0, 0, 0};
+        unpack_m<DIM>(A.body_m[bi], m);
+        for_each_neighbor<DIM>(g, A.cell_start, m, [&](uint32_t q, const float*) -> bool {
+            if (A.sorted_body[q] <= bi) return false;
+            const double4 o4 = A.sorted_s[q];
+            const double sv[3] = {o4.x, o4.y, o4.z};
+            const double r = dsqrt(min_image_dist2<DIM>(g, t, sv));
+            double v;
+            if (SDF) {
+                if (!(r > sigma)) return false;  // overlapping or touching pairs have no positive scale
+                v = dsub(1.0, ddiv(sigma, r));
+            } else {
+                v = r;
+            }
+            if (v < limit) {
+                const double f = floor(dmul(v, inv_width));
+                const uint32_t bin = f < (double)n_bins ? (uint32_t)f : n_bins - 1u;
+                atomicAdd(&s_hist[bin], 1u);
+            }
+            return false;
+        });
+    }
+    __syncthreads();
+    for (uint32_t b = threadIdx.x; b < n_bins; b += blockDim.x)
+        if (s_hist[b]) atomicAdd(counts + b, (unsigned long long)s_hist[b]);
+}
+
 // ---- injected moves (delta_energy_one + Metropolis for hard spheres) -----------------------
 template <int DIM, bool FP32>
 __global__ void k_eval_sphere(Geometry g, Arrays A, Pair P, const uint64_t* bodies, const double4* trial, uint32_t n,
@@ -1196,6 +1255,27 @@ cudaError_t launch_overlap_sphere(int dim, const Geometry& g, const Arrays& a, c
         k_overlap_sphere<2><<<blocks_for(n, 128), 128, 0, s>>>(g, a, p, n);
     else
         k_overlap_sphere<3><<<blocks_for(n, 128), 128, 0, s>>>(g, a, p, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pair_histogram(int dim, bool sdf, const Geometry& g, const Arrays& a, uint32_t n, double sigma,
+                                  double limit, double inv_width, uint32_t n_bins, unsigned long long* counts,
+                                  cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(counts, 0, sizeof(unsigned long long) * n_bins, s);
+    if (e != cudaSuccess || n == 0) return e;
+    const size_t smem = sizeof(unsigned int) * n_bins;
+    const uint32_t grid = blocks_for(n, 256);
+    if (dim == 2) {
+        if (sdf)
+            k_pair_histogram<2, true><<<grid, 256, smem, s>>>(g, a, n, sigma, limit, inv_width, n_bins, counts);
+        else
+            k_pair_histogram<2, false><<<grid, 256, smem, s>>>(g, a, n, sigma, limit, inv_width, n_bins, counts);
+    } else {
+        if (sdf)
+            k_pair_histogram<3, true><<<grid, 256, smem, s>>>(g, a, n, sigma, limit, inv_width, n_bins, counts);
+        else
+            k_pair_histogram<3, false><<<grid, 256, smem, s>>>(g, a, n, sigma, limit, inv_width, n_bins, counts);
+    }
     return cudaGetLastError();
 }
 

@@ -213,6 +213,16 @@ hmc_status hmc_overlap_count_noalloc(const double* positions, uint64_t n_bodies,
                                      uint64_t* overlaps, void* cuda_stream);
 
 /* ---- profiling ---- */
+/* ---- equilibrium estimators (no counterpart in the reference) ----
+ * Histograms of the pairs i < j by minimum-image distance r (FP64, per axis
+ * d = t - s - L rint((t - s)/L)). hmc_sdf: hard spheres; bins of x = 1 - sigma/r over
+ * [0, x_max), the scale distribution function: with s(x) = counts / (N dx), the pressure is
+ * beta P / rho = 1 + s(0+) / dim. hmc_gr: bins of r over [0, r_max) (r_max < L/2); normalise by
+ * the ideal-gas pair count. Both rebuild the cell list with wider spaces; the state and its
+ * counter are not changed. */
+hmc_status hmc_sdf(hmc_system* sys, double x_max, uint32_t n_bins, uint64_t* counts);
+hmc_status hmc_gr(hmc_system* sys, double r_max, uint32_t n_bins, uint64_t* counts);
+
 /* ---- batches of independent replicas ----
  * A batch runs many hard-sphere boxes (each its own hmc_system_desc: box, diameter, Counter,
  * body count) through one set of launches: one counting sort and one kernel per colour pass

@@ -100,6 +100,8 @@ def lib():
         L.oracle_serial_sweep.restype = C.c_int
         L.oracle_tune.argtypes = [C.c_void_p, C.c_uint32, C.c_double, C.c_double, C.c_double, C.c_uint32, C.c_uint32]
         L.oracle_tune.restype = C.c_double
+        L.oracle_sdf.argtypes = [C.c_void_p, C.c_double, C.c_uint32, _u64p]
+        L.oracle_gr.argtypes = [C.c_void_p, C.c_double, C.c_uint32, _u64p]
         L.oracle_overlap_count.argtypes = [C.c_void_p]
         L.oracle_overlap_count.restype = C.c_uint64
         L.oracle_total_energy.argtypes = [C.c_void_p]
@@ -346,6 +348,16 @@ class System:
 
     def tune(self, move, maximum, kt, target, samples, steps) -> float:
         return float(lib().oracle_tune(self._h, move, maximum, kt, target, samples, steps))
+
+    def sdf(self, x_max, n_bins) -> np.ndarray:
+        out = np.zeros(n_bins, dtype=np.uint64)
+        lib().oracle_sdf(self._h, x_max, n_bins, out.ctypes.data_as(_u64p))
+        return out
+
+    def gr(self, r_max, n_bins) -> np.ndarray:
+        out = np.zeros(n_bins, dtype=np.uint64)
+        lib().oracle_gr(self._h, r_max, n_bins, out.ctypes.data_as(_u64p))
+        return out
 
     def overlap_count(self) -> int:
         return int(lib().oracle_overlap_count(self._h))

@@ -1527,6 +1527,46 @@ double oracle_tune(const oracle_system* s, uint32_t move, double maximum, double
     return maximum;
 }
 
+// Pair histograms by minimum-image distance (no reference counterpart: the equilibrium
+// estimators of the device library, restated here as their checker). Pairs i < j; per axis
+// d = t - s - L rint((t - s)/L); SDF bins x = 1 - sigma/r in [0, x_max), g(r) bins r in
+// [0, r_max), bin = floor(v * n_bins / limit) (clamped to the last bin).
+static void pair_histogram(const oracle_system* s, bool sdf, double sigma, double limit, uint32_t n_bins,
+                           uint64_t* counts) {
+    for (uint32_t b = 0; b < n_bins; ++b) counts[b] = 0;
+    const double inv = (double)n_bins / limit;
+    for (uint64_t i = 0; i < s->n; ++i) {
+        for (uint64_t j = i + 1; j < s->n; ++j) {
+            double p = 0.0;
+            for (int a = 0; a < s->dim; ++a) {
+                double d = s->site[3 * i + a] - s->site[3 * j + a];
+                double k = std::nearbyint(d / s->L[a]);
+                d = d - k * s->L[a];
+                p = p + d * d;
+            }
+            double r = std::sqrt(p), v;
+            if (sdf) {
+                if (!(r > sigma)) continue;
+                v = 1.0 - sigma / r;
+            } else {
+                v = r;
+            }
+            if (v < limit) {
+                double f = std::floor(v * inv);
+                uint32_t bin = f < (double)n_bins ? (uint32_t)f : n_bins - 1;
+                counts[bin] += 1;
+            }
+        }
+    }
+}
+
+void oracle_sdf(const oracle_system* s, double x_max, uint32_t n_bins, uint64_t* counts) {
+    pair_histogram(s, true, s->diameter, x_max, n_bins, counts);
+}
+void oracle_gr(const oracle_system* s, double r_max, uint32_t n_bins, uint64_t* counts) {
+    pair_histogram(s, false, 0.0, r_max, n_bins, counts);
+}
+
 uint64_t oracle_overlap_count(const oracle_system* s) {
     // total_energy, pairwise_cutoff.rs:720-745: pairs of sites (and ghosts) with tag_i < tag_j.
     std::vector<uint32_t> cand;

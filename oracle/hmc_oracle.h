@@ -114,6 +114,10 @@ int oracle_serial_sweep(oracle_system* s, uint32_t move, double maximum, double 
 // Move-size tuning (tune_local.rs:21-89) with per-sample counter streams; returns the tuned size.
 double oracle_tune(const oracle_system* s, uint32_t move, double maximum, double kt, double target, uint32_t samples,
                    uint32_t steps);
+// Pair histograms (i < j) by minimum-image distance: scale distribution x = 1 - sigma/r over
+// [0, x_max) and g(r) over [0, r_max); brute force over all pairs (small systems).
+void oracle_sdf(const oracle_system* s, double x_max, uint32_t n_bins, uint64_t* counts);
+void oracle_gr(const oracle_system* s, double r_max, uint32_t n_bins, uint64_t* counts);
 // Number of overlapping pairs (hard) / total energy (LJ), pairs with tag_i < tag_j
 // (pairwise_cutoff.rs:720-745).
 uint64_t oracle_overlap_count(const oracle_system* s);
