@@ -97,6 +97,7 @@ SIGNATURES = {
     "hmc_increment_step": (C.c_int, [_vp]),
     "hmc_math_sincos": (C.c_int, [_vp, _dp, C.c_uint64, _dp, _dp]),
     "hmc_sdf": (C.c_int, [_vp, C.c_double, C.c_uint32, C.POINTER(C.c_uint64)]),
+    "hmc_serial_sweep": (C.c_int, [_vp, C.POINTER(hmc_sweep_params), _u8p, C.POINTER(hmc_count)]),
     "hmc_gr": (C.c_int, [_vp, C.c_double, C.c_uint32, C.POINTER(C.c_uint64)]),
     "hmc_batch_create": (C.c_int, [_vp, C.c_uint32, C.POINTER(hmc_system_desc), C.POINTER(_dp), C.POINTER(_vp)]),
     "hmc_batch_destroy": (None, [_vp]),
@@ -527,6 +528,17 @@ class Microstate:
         c = hmc_count()
         _check(_lib.hmc_sweep(self._h, C.byref(p), C.byref(c)))
         return Count(c.accepted, c.rejected, c.rechecks, c.pair_checks, c.max_fp32_error)
+
+    def serial_sweep(self, maximum: float, n_sweeps: int = 1, increment_step: bool = False, move_mask=None) -> "Count":
+        """Sweep::apply_with_filter (sweep.rs:159-224), hard spheres: bodies in index order from one
+        sequential stream; move_mask (n booleans) plays should_move_body."""
+        p = hmc_sweep_params(C.sizeof(hmc_sweep_params), TRANSLATE, maximum, 1.0, FP64, n_sweeps, int(increment_step), 0)
+        c = hmc_count()
+        mask = None
+        if move_mask is not None:
+            mask = np.ascontiguousarray(np.asarray(move_mask, dtype=bool).astype(np.uint8))
+        _check(_lib.hmc_serial_sweep(self._h, C.byref(p), None if mask is None else mask.ctypes.data_as(_u8p), C.byref(c)))
+        return Count(c.accepted, c.rejected, 0, 0, 0.0)
 
     def eval_moves(self, bodies, positions, u=None, temperature: float = 1.0, precision: int = FP64,
                    return_delta_h: bool = False, orientations=None):

@@ -86,6 +86,15 @@ struct hmc_system {
     std::vector<void*> allocations;
     bool coop[2] = {true, false};  // warp-cooperative hard-sphere pass: [fp64, fp32]
     uint32_t rounds_guess = 2;      // colour sets enqueued before the sweep's count is known
+    // serial sweep grid (allocated on first use)
+    uint32_t serial_nc[3] = {0, 0, 0};
+    double serial_w[3] = {0, 0, 0};
+    uint32_t serial_cap = 0;
+    uint32_t* serial_size = nullptr;
+    uint32_t* serial_items = nullptr;
+    uint32_t* serial_cell_of = nullptr;
+    double4* serial_site = nullptr;
+    uint8_t* serial_mask = nullptr;
     // convex polyhedron
     double4* verts = nullptr;
     uint32_t n_vertices = 0;
@@ -198,6 +207,7 @@ hmc_status check_flags(hmc_system* s) {
     if (f & kErrNonFinite) return fail(HMC_NAN_STATE, "a body position is not finite");
     if (f & kErrOutsideCheckerboard) return fail(HMC_OUTSIDE_CHECKERBOARD, "a body maps to no checkerboard space");
     if (f & kErrAngleRange) return fail(HMC_INVALID_ARGUMENT, "a 2-D orientation angle reached 2^19 rad");
+    if (f & kErrCellOverflow) return fail(HMC_CELL_OVERFLOW, "a cell of the serial sweep's grid is full");
     return HMC_OK;
 }
 
@@ -746,6 +756,70 @@ hmc_status hmc_math_sincos(hmc_context* ctx, const double* x, uint64_t n, double
     if (bad) cudaFree(bad);
     if (e != cudaSuccess) return fail(HMC_CUDA_ERROR, "sincos: %s", cudaGetErrorString(e));
     if (hbad) return fail(HMC_INVALID_ARGUMENT, "an argument has |x| >= 2^20");
+    return HMC_OK;
+}
+
+// Sweep::apply_with_filter (hoomd-mc/src/sweep.rs:159-224) for hard spheres: bodies in index
+// order, one sequential stream Counter(step, substep, seed).make_rng(), then
+// increment_substep. move_mask (n bytes, may be NULL) plays should_move_body.
+hmc_status hmc_serial_sweep(hmc_system* s, const hmc_sweep_params* p, const uint8_t* move_mask, hmc_count* out) {
+    if (!s || !p) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
+    if (p->struct_size < sizeof(hmc_sweep_params)) return fail(HMC_INVALID_ARGUMENT, "hmc_sweep_params.struct_size");
+    if (s->interaction != HMC_HARD_SPHERE) return fail(HMC_NOT_SUPPORTED, "the serial sweep is built for hard spheres");
+    if (p->move != HMC_TRANSLATE) return fail(HMC_NOT_SUPPORTED, "hard spheres take translation moves");
+    double lmax = 0.0;
+    for (int a = 0; a < s->dim; ++a) lmax = std::max(lmax, s->geom.L[a]);
+    if (!(p->maximum > 0.0) || !(p->maximum <= 4.0 * lmax))
+        return fail(HMC_INVALID_ARGUMENT, "maximum must be in (0, 4 box lengths]");
+    HMC_CUDA(cudaSetDevice(s->ctx->device));
+    if (!s->serial_size) {
+        const double sigma = std::sqrt(s->pair.sigma2);
+        uint64_t cells = 1;
+        for (int a = 0; a < s->dim; ++a) {
+            double f = std::floor(s->geom.L[a] / sigma);
+            s->serial_nc[a] = f >= 1.0 ? (uint32_t)std::min(f, 1024.0) : 1u;
+            s->serial_w[a] = s->geom.L[a] / (double)s->serial_nc[a];
+            cells *= s->serial_nc[a];
+        }
+        s->serial_cap = (uint32_t)std::min<uint64_t>(4096, 4 * (s->n / cells + 1) + 16);
+        hmc_status st;
+        if ((st = dalloc(s, &s->serial_size, cells)) || (st = dalloc(s, &s->serial_items, cells * s->serial_cap)) ||
+            (st = dalloc(s, &s->serial_cell_of, s->n)) || (st = dalloc(s, &s->serial_site, s->n)) ||
+            (st = dalloc(s, &s->serial_mask, s->n)))
+            return st;
+    }
+    uint64_t moving = s->n;
+    if (move_mask) {
+        moving = 0;
+        for (uint64_t i = 0; i < s->n; ++i) moving += move_mask[i] ? 1 : 0;
+        if (s->n) HMC_CUDA(cudaMemcpyAsync(s->serial_mask, move_mask, s->n, cudaMemcpyHostToDevice, s->stream));
+    }
+    hmc_count total{};
+    for (uint32_t sweep = 0; sweep < p->n_sweeps; ++sweep) {
+        Launch L{};
+        L.step = s->step;
+        L.substep = s->substep;
+        L.seed = s->seed;
+        L.max_move = p->maximum;
+        L.kt = p->temperature;
+        L.n_bodies = (uint32_t)s->n;
+        HMC_CUDA(cudaMemsetAsync(s->arr.stats, 0, sizeof(DeviceStats), s->stream));
+        HMC_CUDA(launch_serial_sphere(s->dim, s->geom, s->arr, s->pair, L, s->serial_nc, s->serial_w, s->serial_cap,
+                                      s->serial_size, s->serial_items, s->serial_cell_of, s->serial_site,
+                                      move_mask ? s->serial_mask : nullptr, s->stream));
+        s->prof.kernel_launches += 2;
+        hmc_status st;
+        if ((st = read_stats(s))) return st;
+        if ((st = check_flags(s))) return st;
+        total.accepted += s->host_stats->accepted;
+        total.rejected += moving - s->host_stats->accepted;
+        s->substep += 1;  // increment_substep (sweep.rs:222)
+        if (p->increment_step) {
+            s->step += 1;
+            s->substep = 0;
+        }
+    }
+    if (out) *out = total;
     return HMC_OK;
 }
 

@@ -14,6 +14,7 @@ enum : uint32_t {
     kErrOutsideCheckerboard = 1u << 0,
     kErrNonFinite = 1u << 1,
     kErrAngleRange = 1u << 2,  // a 2-D orientation angle at or beyond 2^19 rad
+    kErrCellOverflow = 1u << 3,  // a cell of the serial sweep's grid is full
 };
 
 // Counters written by the kernels. Zeroed by the host before a sweep.
@@ -190,6 +191,11 @@ cudaError_t launch_pack_angles(const double4* body_ori, double* packed, uint64_t
 cudaError_t launch_pair_histogram(int dim, bool sdf, const Geometry& g, const Arrays& a, uint32_t n, double sigma,
                                   double limit, double inv_width, uint32_t n_bins, unsigned long long* counts,
                                   cudaStream_t s);
+// Sweep::apply_with_filter for hard spheres (hmc_serial.cu): one warp, one sequential stream.
+// nc/w: the serial grid (cells per axis, widths); mask (may be null): bodies to move.
+cudaError_t launch_serial_sphere(int dim, const Geometry& g, const Arrays& a, const Pair& p, const Launch& l,
+                                 const uint32_t* nc, const double* w, uint32_t cap, uint32_t* size, uint32_t* items,
+                                 uint32_t* cell_of, double4* site, const uint8_t* mask, cudaStream_t s);
 // State transfer through a packed staging array of n x dim doubles (the host layout):
 // first_nonfinite receives the smallest body index with a non-finite coordinate (it must hold
 // ~0 before the launch); unpack writes body positions, pack reads them.

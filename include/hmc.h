@@ -176,6 +176,12 @@ hmc_status hmc_increment_step(hmc_system* sys);
 hmc_status hmc_sweep(hmc_system* sys, const hmc_sweep_params* params, hmc_count* out);
 hmc_status hmc_tune(hmc_system* sys, hmc_sweep_params* params, double target_acceptance, uint32_t samples,
                     uint32_t steps);
+/* Sweep::apply_with_filter (hoomd-mc/src/sweep.rs:159-224), hard spheres: one trial per body in
+ * index order from one sequential stream, then increment_substep. move_mask (n_bodies bytes,
+ * may be NULL) selects the bodies to move (should_move_body). The exact serial chain; the
+ * checkerboard hmc_sweep is the fast path. */
+hmc_status hmc_serial_sweep(hmc_system* sys, const hmc_sweep_params* params, const uint8_t* move_mask,
+                            hmc_count* out);
 hmc_status hmc_overlap_check(hmc_system* sys, uint64_t* n_overlaps);
 /* decisions[i] = 1 when move i would be accepted; rechecked[i] = 1 when the FP32 path had to
  * fall back to FP64 for it; delta_h[i] (may be NULL) = delta_energy_one in FP64. */

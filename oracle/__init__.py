@@ -96,6 +96,9 @@ def lib():
         L.oracle_parallel_sweep_threads.argtypes = [C.c_void_p, C.c_uint32, C.c_double, C.c_double, C.c_double,
                                                     C.c_uint32, _u64p, _u64p]
         L.oracle_parallel_sweep_threads.restype = C.c_int
+        L.oracle_serial_sweep_filter.argtypes = [C.c_void_p, C.c_uint32, C.c_double, C.c_double, _u8p, _u64p,
+                                                 _u64p]
+        L.oracle_serial_sweep_filter.restype = C.c_int
         L.oracle_serial_sweep.argtypes = [C.c_void_p, C.c_uint32, C.c_double, C.c_double, _u64p, _u64p]
         L.oracle_serial_sweep.restype = C.c_int
         L.oracle_tune.argtypes = [C.c_void_p, C.c_uint32, C.c_double, C.c_double, C.c_double, C.c_uint32, C.c_uint32]
@@ -340,10 +343,12 @@ class System:
             raise RuntimeError(f"oracle parallel sweep failed ({rc})")
         return a.value, r.value
 
-    def serial_sweep(self, move, maximum, kt):
+    def serial_sweep(self, move, maximum, kt, mask=None):
         a = C.c_uint64()
         r = C.c_uint64()
-        lib().oracle_serial_sweep(self._h, move, maximum, kt, C.byref(a), C.byref(r))
+        m = None if mask is None else np.ascontiguousarray(np.asarray(mask, dtype=bool).astype(np.uint8))
+        lib().oracle_serial_sweep_filter(self._h, move, maximum, kt, None if m is None else m.ctypes.data_as(_u8p),
+                                         C.byref(a), C.byref(r))
         return a.value, r.value
 
     def tune(self, move, maximum, kt, target, samples, steps) -> float:

@@ -1481,11 +1481,17 @@ int oracle_parallel_sweep_threads(oracle_system* s, uint32_t move, double maximu
 
 int oracle_serial_sweep(oracle_system* s, uint32_t move, double maximum, double kt, uint64_t* accepted,
                         uint64_t* rejected) {
-    // Sweep::apply_with_filter, sweep.rs:159-224 (no filter)
+    return oracle_serial_sweep_filter(s, move, maximum, kt, nullptr, accepted, rejected);
+}
+
+int oracle_serial_sweep_filter(oracle_system* s, uint32_t move, double maximum, double kt, const uint8_t* mask,
+                               uint64_t* accepted, uint64_t* rejected) {
+    // Sweep::apply_with_filter, sweep.rs:159-224; a body the filter excludes draws nothing
     Sfc64 rng = make_rng(s->step, s->substep, s->seed, 0);
     uint64_t acc = 0, rej = 0;
     int ol = s->ori_len();
     for (uint64_t b = 0; b < s->n; ++b) {
+        if (mask && !mask[b]) continue;
         double pos[3] = {0, 0, 0}, ori[4] = {0, 0, 0, 0};
         s->propose(rng, (int)move, maximum, b, pos, ori);
         wrap(s->dim, s->L, pos);

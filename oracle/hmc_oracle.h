@@ -111,6 +111,9 @@ int oracle_parallel_sweep_threads(oracle_system* s, uint32_t move, double maximu
 // Sweep::apply (sweep.rs:159-224).
 int oracle_serial_sweep(oracle_system* s, uint32_t move, double maximum, double kt,
                         uint64_t* accepted, uint64_t* rejected);
+// The same with should_move_body as a mask (n bytes; NULL moves every body).
+int oracle_serial_sweep_filter(oracle_system* s, uint32_t move, double maximum, double kt, const uint8_t* mask,
+                               uint64_t* accepted, uint64_t* rejected);
 // Move-size tuning (tune_local.rs:21-89) with per-sample counter streams; returns the tuned size.
 double oracle_tune(const oracle_system* s, uint32_t move, double maximum, double kt, double target, uint32_t samples,
                    uint32_t steps);
