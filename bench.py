@@ -247,6 +247,113 @@ def run_replicas(args, local_rank):
     b.close()
 
 
+def run_config(args, local_rank):
+    """The survey's other single-box configurations, FP32+recheck and FP64 from the same state,
+    device-timed per step like the headline, with the oracle's ParallelSweep on the host cores
+    as the CPU baseline (a bounded sample of whole sweeps). A step: one sweep (disks, LJ) or one
+    translation plus one rotation sweep (cubes)."""
+    import torch
+    import oracle
+    from hoomd_rs_b200 import (FP32_RECHECK, FP64, ROTATE, TRANSLATE, Context, ConvexPolyhedron, HardShape,
+                               HardSphere, Isotropic, LennardJones, Microstate, PairwiseCutoff, Periodic, Shifted,
+                               lattice)
+    torch.cuda.set_device(local_rank)
+    ctx = Context(local_rank)
+    kind = args.workload
+    if kind == "disks":
+        n, seed = 4096, 0x5EED0001
+        pos, L = lattice.hard_sphere_box(n, 0.70, 2, seed)
+        h, bound, dim = PairwiseCutoff(HardSphere(1.0)), Periodic(1.0, [L, L]), 2
+        moves = [(TRANSLATE, 0.1)]
+        okw = dict(diameter=1.0)
+        desc = "2-D hard disks, N=4096, area fraction 0.70, square lattice + 0.01 jitter, translation 0.1"
+        orng = 1.0
+    elif kind == "cubes":
+        n, seed = 1 << 18, 0x5EED0003
+        cube = np.array([[x, y, z] for x in (-0.5, 0.5) for y in (-0.5, 0.5) for z in (-0.5, 0.5)])
+        L = (n / 0.55) ** (1.0 / 3.0)
+        pos = lattice.cubic_lattice(n, L, 3, seed, jitter=0.0)
+        h, bound, dim = PairwiseCutoff(HardShape(ConvexPolyhedron.with_vertices(cube))), Periodic(math.sqrt(3), [L] * 3), 3
+        moves = [(TRANSLATE, 0.08), (ROTATE, 0.1)]
+        okw = dict(interaction=oracle.HARD_CONVEX_POLYHEDRON, vertices=cube)
+        desc = "hard cubes (vertices +-0.5), N=2^18, packing fraction 0.55, simple-cubic start, identity versors, " \
+               "translation 0.08 then rotation 0.1 per step"
+        orng = math.sqrt(3)
+    else:
+        n, seed = 1 << 19, 0x5EED0005
+        pos, L = lattice.lennard_jones_box(n, 0.8, 3, seed)
+        h = PairwiseCutoff(Isotropic(Shifted(LennardJones(1.0, 1.0), 2.5), 2.5))
+        bound, dim = Periodic(2.5, [L] * 3), 3
+        moves = [(TRANSLATE, 0.1)]
+        okw = dict(interaction=oracle.LENNARD_JONES, lj_epsilon=1.0, lj_sigma=1.0, lj_r_cut=2.5, lj_r_shift=2.5)
+        desc = "Lennard-Jones eps = sigma = 1, r_cut = r_shift = 2.5, N=2^19, rho 0.8, kT 1.0, FCC + 0.01 jitter, " \
+               "translation 0.1"
+        orng = 2.5
+    stream = torch.cuda.Stream()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def timed(precision):
+        m = Microstate(ctx, bound, pos, h, seed=seed)
+        m.set_stream(stream.cuda_stream)
+        for _ in range(args.warmup):
+            for mv, mx in moves:
+                m.sweep(mv, mx, 1.0, precision, n_sweeps=1, increment_step=True)
+        ms, trials, acc, rech, checks = 0.0, 0, 0, 0, 0
+        launches0 = m.profile()["kernel_launches"]
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+            for mv, mx in moves:
+                c = m.sweep(mv, mx, 1.0, precision, n_sweeps=1, increment_step=True)
+                trials += c.total()
+                acc += c.accepted
+                rech += c.rechecks
+                checks += c.pair_checks
+            e1.record(stream)
+            e1.synchronize()
+            ms += e0.elapsed_time(e1)
+        out = {"value": trials / (ms / 1e3), "ms_per_step": ms / args.steps, "acceptance": acc / max(trials, 1),
+               "recheck_fraction": rech / max(checks, 1), "launches": m.profile()["kernel_launches"] - launches0}
+        pos_end = m.positions()
+        m.close()
+        return out, pos_end
+
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    r32, p32 = timed(FP32_RECHECK)
+    clocks = sampler.stop()
+    r64, p64 = timed(FP64)
+    line = {"metric": f"trial moves/s, {kind}", "value": r32["value"], "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": r32["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "fp32 pair test + fp64 recheck (fp64 state)", "data": "synthetic",
+            "config": {"workload": desc, "n_bodies": n, "box_length": L,
+                       "l2": "flushed before every timed step (256 MiB device write)"},
+            "fp64": {"value": r64["value"], "ms_per_step": r64["ms_per_step"]},
+            "mismatches": int(np.count_nonzero(np.any(p32 != p64, axis=1))), "acceptance": r32["acceptance"],
+            "recheck_fraction": r32["recheck_fraction"], "gpu_launches": r32["launches"], "clocks": clocks}
+    if not args.no_cpu_baseline:
+        threads = host_threads()
+        o = oracle.System(dim, [L] * dim, pos, seed=seed, **okw)
+        trials, t0, sweeps = 0, time.perf_counter(), 0
+        while True:
+            for mv, mx in moves:
+                a, r = o.parallel_sweep(oracle.TRANSLATE if mv == TRANSLATE else oracle.ROTATE, mx, 1.0, orng,
+                                        threads=threads)
+                o.increment_step()
+                trials += a + r
+                sweeps += 1
+            el = time.perf_counter() - t0
+            if el >= 10.0 or sweeps >= 64:
+                break
+        line["cpu_baseline"] = {"value": trials / el, "unit": UNIT, "cores": threads, "kind": "port",
+                                "sample": f"{sweeps} ParallelSweep sweeps from the start state ({el:.1f} s, "
+                                          f"{threads} threads)"}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -254,8 +361,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="hard_spheres", choices=["hard_spheres", "replicas"],
-                    help="hard_spheres: the headline (2^20 spheres); replicas: 256 independent boxes in one batch")
+    ap.add_argument("--workload", default="hard_spheres", choices=["hard_spheres", "replicas", "disks", "cubes", "lj"],
+                    help="hard_spheres: the headline (2^20 spheres); replicas: 256 independent boxes in one batch; "
+                         "disks: 4096 hard disks; cubes: 2^18 hard cubes; lj: 2^19 Lennard-Jones sites")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", "0"))
@@ -266,6 +374,9 @@ def main():
         return
     if args.workload == "replicas":
         run_replicas(args, local_rank)
+        return
+    if args.workload in ("disks", "cubes", "lj"):
+        run_config(args, local_rank)
         return
 
     import torch
