@@ -659,7 +659,7 @@ hmc_status hmc_sweep(hmc_system* s, const hmc_sweep_params* p, hmc_count* out) {
     const uint32_t colors = 1u << s->dim;
     for (uint32_t sweep = 0; sweep < p->n_sweeps; ++sweep) {
         if (s->profiling) HMC_CUDA(cudaEventRecord(s->ev[0], s->stream));
-        hmc_status st = rebuild(s, !fp32);
+        hmc_status st = rebuild(s, !fp32 || s->oriented());  // shapes read S in both modes
         if (st) return st;
         if (s->profiling) HMC_CUDA(cudaEventRecord(s->ev[1], s->stream));
         Launch L{};

@@ -115,7 +115,7 @@ constexpr int kXenoMaxIter = 1024;  // xenocollide.rs:38
 
 // collide for N = 3 (xenocollide.rs:172-291, :361-414). The iteration caps return overlap,
 // as the reference does.
-__device__ bool collide3d(const double4* verts, uint32_t nv, const V3& vij, const Q& oij) {
+__device__ __noinline__ bool collide3d(const double4* verts, uint32_t nv, const V3& vij, const Q& oij) {
     Minkowski s;
     s.verts = verts;
     s.nv = nv;
@@ -278,20 +278,10 @@ __device__ __forceinline__ bool poly_overlaps(const Geometry& g, const Arrays& A
                             if (test) st.rechecks++;
                         }
                         if (test) {
-                            double sj[3];
-                            if (FP32) {
-                                const double4 b4 = ldg4(A.sorted_b + q);
-                                sj[0] = b4.x;
-                                sj[1] = b4.y;
-                                sj[2] = b4.z;
-                                wrap_inv<3>(g.L, g.invL, sj);
-                            } else {
-                                const double4 s4 = ldg4(A.sorted_s + q);
-                                sj[0] = s4.x;
-                                sj[1] = s4.y;
-                                sj[2] = s4.z;
-                                st.checks++;
-                            }
+                            // shapes keep S in both precision modes (the FP32 pass only prefilters)
+                            const double4 s4 = ldg4(A.sorted_s + q);
+                            const double sj[3] = {s4.x, s4.y, s4.z};
+                            if (!FP32) st.checks++;
                             hit = poly_overlap64(g, A, sh.verts, sh.nv, sh.rcut2, t, qi, sj, q);
                         }
                     }
@@ -343,7 +333,7 @@ __global__ void __launch_bounds__(128) k_sweep_poly3(Geometry g, Arrays A, PolyS
             wrap_inv<3>(g.L, g.invL, sv);
             const uint32_t body = A.sorted_body[k];
             A.sorted_b[k] = make_double4(t[0], t[1], t[2], 0.0);
-            if (!FP32) A.sorted_s[k] = make_double4(sv[0], sv[1], sv[2], 0.0);
+            A.sorted_s[k] = make_double4(sv[0], sv[1], sv[2], 0.0);
             A.sorted_off[k] = cell_offsets<3>(g, sv, m);
             A.sorted_q[k] = make_double4(qi.s, qi.x, qi.y, qi.z);
             A.body_pos[body] = make_double4(t[0], t[1], t[2], 0.0);

@@ -62,7 +62,7 @@ __device__ __forceinline__ V2 support2(const double4* __restrict__ verts, uint32
 constexpr int kXenoMaxIter2 = 1024;  // xenocollide.rs:38
 
 // collide for N = 2 (xenocollide.rs:92-154, :361-414); the iteration cap returns overlap.
-__device__ bool collide2d(const double4* verts, uint32_t nv, const V2& vij, const M2& q) {
+__device__ __noinline__ bool collide2d(const double4* verts, uint32_t nv, const V2& vij, const M2& q) {
     const M2 qinv = transpose2(q);
     // composite_support_mapping (xenocollide.rs:318-328)
     auto s = [&](const V2& n) -> V2 {
@@ -130,7 +130,7 @@ __device__ __forceinline__ bool b_edge_separates(const double4* verts, uint32_t 
     return false;
 }
 // ConvexSurfaceMesh2d::intersects_at (:578-593).
-__device__ bool sat_intersects(const double4* verts, uint32_t nv, const V2& v_ij, const M2& o_j) {
+__device__ __noinline__ bool sat_intersects(const double4* verts, uint32_t nv, const V2& v_ij, const M2& o_j) {
     if (b_edge_separates(verts, nv, v_ij, o_j)) return false;
     const M2 inv = transpose2(o_j);
     const V2 v_ji = mat2_rotate(inv, V2{-v_ij.x, -v_ij.y});
@@ -206,20 +206,10 @@ __device__ __forceinline__ bool poly2_overlaps(const Geometry& g, const Arrays& 
                         if (test) st.rechecks++;
                     }
                     if (test) {
-                        double sj[3];
-                        if (FP32) {
-                            const double4 b4 = ldg4(A.sorted_b + q);
-                            sj[0] = b4.x;
-                            sj[1] = b4.y;
-                            sj[2] = 0.0;
-                            wrap_inv<2>(g.L, g.invL, sj);
-                        } else {
-                            const double4 s4 = ldg4(A.sorted_s + q);
-                            sj[0] = s4.x;
-                            sj[1] = s4.y;
-                            sj[2] = 0.0;
-                            st.checks++;
-                        }
+                        // shapes keep S in both precision modes (the FP32 pass only prefilters)
+                        const double4 s4 = ldg4(A.sorted_s + q);
+                        const double sj[3] = {s4.x, s4.y, 0.0};
+                        if (!FP32) st.checks++;
                         hit = poly2_overlap64<SAT>(g, A, sh, t, ti, sj, q, range_error);
                     }
                 }
@@ -273,7 +263,7 @@ __global__ void __launch_bounds__(128) k_sweep_poly2(Geometry g, Arrays A, PolyS
             wrap_inv<2>(g.L, g.invL, sv);
             const uint32_t body = A.sorted_body[k];
             A.sorted_b[k] = make_double4(t[0], t[1], 0.0, 0.0);
-            if (!FP32) A.sorted_s[k] = make_double4(sv[0], sv[1], 0.0, 0.0);
+            A.sorted_s[k] = make_double4(sv[0], sv[1], 0.0, 0.0);
             A.sorted_off[k] = cell_offsets<2>(g, sv, m);
             A.sorted_q[k] = make_double4(ti, 0.0, 0.0, 0.0);
             A.body_pos[body] = make_double4(t[0], t[1], 0.0, 0.0);
