@@ -57,62 +57,67 @@ __device__ __forceinline__ void lj_pair32(const Pair& P, float r2, float& e, flo
     err = 1.1f * ((6.f * a + 3.f * b) * (dr2 * inv) + 24.f * kU32 * (a + b + fabsf(P.lj_e_shift32)));
 }
 
-// The stencil rows of space m as at most two slot ranges each (two when the row wraps around
-// the fast axis), with the slow-axis shifts of each row.
+// The stencil around space m; its rows are resolved one at a time (row_ranges) so that no
+// per-row table occupies registers across the candidate loops.
 template <int DIM>
 struct Stencil {
-    uint32_t lo[kRows<DIM>][2], hi[kRows<DIM>][2];
-    float s0[kRows<DIM>], s1[kRows<DIM>];
-    bool used[kRows<DIM>];
+    const uint32_t* cs;
+    uint32_t m[3];
 };
 
 template <int DIM>
 __device__ __forceinline__ void make_stencil(const Geometry& g, const uint32_t* __restrict__ cs, const uint32_t* m,
                                              Stencil<DIM>& st) {
-    const uint32_t sf = g.shape[DIM - 1], mf = m[DIM - 1];
-#pragma unroll
-    for (int r = 0; r < kRows<DIM>; ++r) {
-        const int i0 = DIM == 3 ? r / 3 - 1 : 0;
-        const int i1 = DIM == 3 ? r % 3 - 1 : r - 1;
-        uint32_t base;
-        bool skip;
-        if (DIM == 3) {
-            skip = (i0 == -1 && g.shape[0] == 2) || (i1 == -1 && g.shape[1] == 2);
-            base = (wrap_index((int)m[0] + i0, g.shape[0]) * g.shape[1] + wrap_index((int)m[1] + i1, g.shape[1])) * sf;
-            st.s0[r] = (float)i0 * g.w32[0];
-            st.s1[r] = (float)i1 * g.w32[1];
-        } else {
-            skip = i1 == -1 && g.shape[0] == 2;
-            base = wrap_index((int)m[0] + i1, g.shape[0]) * sf;
-            st.s0[r] = (float)i1 * g.w32[0];
-            st.s1[r] = 0.f;
-        }
-        st.used[r] = !skip;
-        uint32_t a0 = 0, a1 = 0, b0 = 0, b1 = 0;
-        if (!skip) {
-            if (sf == 2) {
-                a0 = __ldg(cs + base);
-                a1 = __ldg(cs + base + 2);
-            } else if (mf >= 1 && mf + 1 < sf) {
-                a0 = __ldg(cs + base + mf - 1);
-                a1 = __ldg(cs + base + mf + 2);
-            } else if (mf == 0) {
-                a0 = __ldg(cs + base);
-                a1 = __ldg(cs + base + 2);
-                b0 = __ldg(cs + base + sf - 1);
-                b1 = __ldg(cs + base + sf);
-            } else {
-                a0 = __ldg(cs + base + sf - 2);
-                a1 = __ldg(cs + base + sf);
-                b0 = __ldg(cs + base);
-                b1 = __ldg(cs + base + 1);
-            }
-        }
-        st.lo[r][0] = a0;
-        st.hi[r][0] = a1;
-        st.lo[r][1] = b0;
-        st.hi[r][1] = b1;
+    st.cs = cs;
+    st.m[0] = m[0];
+    st.m[1] = m[1];
+    st.m[2] = m[2];
+}
+
+// Row r of the stencil as at most two slot ranges (two when the row wraps around the fast
+// axis), with the row's slow-axis shifts; a row repeated on a two-space axis is empty.
+struct RowRanges {
+    uint32_t lo[2], hi[2];
+    float s0, s1;
+};
+template <int DIM>
+__device__ __forceinline__ RowRanges row_ranges(const Geometry& g, const Stencil<DIM>& st, int r) {
+    RowRanges rr{{0u, 0u}, {0u, 0u}, 0.f, 0.f};
+    const uint32_t sf = g.shape[DIM - 1], mf = st.m[DIM - 1];
+    const int i0 = DIM == 3 ? r / 3 - 1 : 0;
+    const int i1 = DIM == 3 ? r % 3 - 1 : r - 1;
+    uint32_t base;
+    bool skip;
+    if (DIM == 3) {
+        skip = (i0 == -1 && g.shape[0] == 2) || (i1 == -1 && g.shape[1] == 2);
+        base = (wrap_index((int)st.m[0] + i0, g.shape[0]) * g.shape[1] + wrap_index((int)st.m[1] + i1, g.shape[1])) * sf;
+        rr.s0 = (float)i0 * g.w32[0];
+        rr.s1 = (float)i1 * g.w32[1];
+    } else {
+        skip = i1 == -1 && g.shape[0] == 2;
+        base = wrap_index((int)st.m[0] + i1, g.shape[0]) * sf;
+        rr.s0 = (float)i1 * g.w32[0];
     }
+    if (skip) return rr;
+    const uint32_t* cs = st.cs;
+    if (sf == 2) {
+        rr.lo[0] = __ldg(cs + base);
+        rr.hi[0] = __ldg(cs + base + 2);
+    } else if (mf >= 1 && mf + 1 < sf) {
+        rr.lo[0] = __ldg(cs + base + mf - 1);
+        rr.hi[0] = __ldg(cs + base + mf + 2);
+    } else if (mf == 0) {
+        rr.lo[0] = __ldg(cs + base);
+        rr.hi[0] = __ldg(cs + base + 2);
+        rr.lo[1] = __ldg(cs + base + sf - 1);
+        rr.hi[1] = __ldg(cs + base + sf);
+    } else {
+        rr.lo[0] = __ldg(cs + base + sf - 2);
+        rr.hi[0] = __ldg(cs + base + sf);
+        rr.lo[1] = __ldg(cs + base);
+        rr.hi[1] = __ldg(cs + base + 1);
+    }
+    return rr;
 }
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -132,16 +137,19 @@ __device__ __forceinline__ uint32_t warp_maxu(uint32_t v) {
 }
 
 // FP64 energy of site t against the stencil of space m, skipping slot self: lane-strided over
+
+// FP64 energy of site t against the stencil of space m, skipping slot self: lane-strided over
 // the rows, then a butterfly reduction (every lane ends with the same value). S of a
 // candidate comes from sorted_s when have_s, else from wrap(sorted_b).
 template <int DIM>
 __device__ __forceinline__ double lj_energy64(const Geometry& g, const Arrays& A, const Pair& P, const double* t,
                                               const Stencil<DIM>& st, uint32_t self, bool have_s, uint32_t lane) {
     double e = 0.0;
-#pragma unroll
+#pragma unroll 1
     for (int r = 0; r < kRows<DIM>; ++r) {
+        const RowRanges rr = row_ranges<DIM>(g, st, r);
         for (int seg = 0; seg < 2; ++seg) {
-            for (uint32_t q = st.lo[r][seg] + lane; q < st.hi[r][seg]; q += 32) {
+            for (uint32_t q = rr.lo[seg] + lane; q < rr.hi[seg]; q += 32) {
                 if (q == self) continue;
                 double sv[3];
                 if (have_s) {
@@ -176,10 +184,11 @@ __device__ __forceinline__ Sums32 lj_energy32(const Geometry& g, const Arrays& A
                                                uint32_t lane) {
     Sums32 s{0.f, 0.f, 0.f, 0.f, 0u, 0u};
     const uint32_t sf = g.shape[DIM - 1];
-#pragma unroll
+#pragma unroll 1
     for (int r = 0; r < kRows<DIM>; ++r) {
+        const RowRanges rr = row_ranges<DIM>(g, st, r);
         for (int seg = 0; seg < 2; ++seg) {
-            for (uint32_t q = st.lo[r][seg] + lane; q < st.hi[r][seg]; q += 32) {
+            for (uint32_t q = rr.lo[seg] + lane; q < rr.hi[seg]; q += 32) {
                 if (q == self) continue;
                 const float4 o = __ldg(A.sorted_off + q);
                 int dm = __float_as_int(o.w) - mf;
@@ -189,8 +198,8 @@ __device__ __forceinline__ Sums32 lj_energy32(const Geometry& g, const Arrays& A
                     else if (dm < -1)
                         dm += (int)sf;
                 }
-                const float r2n = fp32_dist2<DIM>(g, t32, o, st.s0[r], st.s1[r], dm);
-                const float r2o = fp32_dist2<DIM>(g, c32, o, st.s0[r], st.s1[r], dm);
+                const float r2n = fp32_dist2<DIM>(g, t32, o, rr.s0, rr.s1, dm);
+                const float r2o = fp32_dist2<DIM>(g, c32, o, rr.s0, rr.s1, dm);
                 s.pairs += 2;
                 if (r2n < P.lj_rcut2_hi32) {
                     float e, err;
