@@ -38,6 +38,11 @@ SEED = 0x5EED0002
 TARGET_ACCEPTANCE = 0.30
 
 
+# DRAM bytes of one FP32 colour pass of this workload, read + written, from one ncu capture
+# (profiles/k_sweep_sphere_fp32_hard_spheres_2p20.md): 30.52 MB + 0.01 MB.
+SPHERE_PASS_DRAM_BYTES = 30.53e6
+
+
 def workload_config(d, extra=None):
     cfg = {"workload": "3-D hard spheres, N=2^20, packing fraction 0.50, periodic cube, FCC start + 0.01 jitter, "
                        "translation moves tuned by Tune (target 0.30, hmc_tune), one ParallelSweep per step",
@@ -507,7 +512,9 @@ def main():
         "acceptance": ra["accepted"] / max(ra["trials"], 1),
         "recheck_fraction": ra["rechecks"] / max(ra["pair_checks"], 1), "max_fp32_error": ra["max_err"],
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "kernel": "k_sweep_sphere<3,fp32>",
+                     "traffic": SPHERE_PASS_DRAM_BYTES, "kernel": "k_sweep_sphere<3,fp32>",
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one FP32 colour pass "
+                                       "(profiles/k_sweep_sphere_fp32_hard_spheres_2p20.md)",
                      "bytes_per_launch": bytes_per_launch, "launch_ms": t_launch * 1e3,
                      "peak_source": f"{peak_kind} hbm_gbs"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": N_BODIES * 3 * 8,
