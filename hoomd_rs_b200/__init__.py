@@ -31,7 +31,7 @@ LIB_PATH = os.environ.get("HMC_B200_LIB", os.path.join(_HERE, "libhmc_b200.so"))
 
 # hmc_status
 OK, INVALID_ARGUMENT, RANGE_TOO_LARGE, OVERLAP_IN_INPUT, CELL_OVERFLOW, NAN_STATE, ITERATION_CAP, TIMEOUT, \
-    CUDA_ERROR, OUT_OF_MEMORY, NOT_SUPPORTED, OUTSIDE_CHECKERBOARD = range(12)
+    CUDA_ERROR, OUT_OF_MEMORY, NOT_SUPPORTED, OUTSIDE_CHECKERBOARD, IO_ERROR = range(13)
 # hmc_interaction / hmc_move / hmc_precision
 HARD_SPHERE, HARD_CONVEX_POLYGON, HARD_CONVEX_POLYHEDRON, LENNARD_JONES, HARD_CONVEX_SURFACE_MESH_2D = range(5)
 TRANSLATE, ROTATE = range(2)
@@ -71,6 +71,20 @@ class hmc_count(C.Structure):
 class hmc_injected_move(C.Structure):
     _fields_ = [("body", C.c_uint64), ("position", C.c_double * 3), ("orientation", C.c_double * 4),
                 ("u", C.c_double)]
+
+
+class hmc_gsd_chunk(C.Structure):
+    _fields_ = [("frame", C.c_uint64), ("rows", C.c_uint64), ("location", C.c_uint64), ("columns", C.c_uint32),
+                ("id", C.c_uint16), ("type", C.c_uint8), ("flags", C.c_uint8)]
+
+
+class hmc_gsd_info(C.Structure):
+    _fields_ = [("n_frames", C.c_uint64), ("buffer_frame", C.c_uint64), ("file_length", C.c_uint64),
+                ("index_entries", C.c_uint64), ("index_allocated_entries", C.c_uint64),
+                ("namelist_allocated_entries", C.c_uint64), ("n_names", C.c_uint32), ("schema_major", C.c_uint16),
+                ("schema_minor", C.c_uint16), ("gsd_major", C.c_uint16), ("gsd_minor", C.c_uint16),
+                ("writable", C.c_int), ("maximum_write_buffer_size", C.c_uint64),
+                ("application", C.c_char * 64), ("schema", C.c_char * 64)]
 
 
 class hmc_profile(C.Structure):
@@ -113,6 +127,27 @@ SIGNATURES = {
                                  _u8p, _dp]),
     "hmc_total_energy": (C.c_int, [_vp, _dp]),
     "hmc_overlap_count_noalloc": (C.c_int, [_vp, C.c_uint64, C.c_uint32, _dp, C.c_double, C.c_double, _vp, _vp]),
+    "hmc_gsd_last_error": (C.c_int, []),
+    "hmc_gsd_create": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_uint16, C.c_uint16, C.c_int,
+                                 C.POINTER(_vp)]),
+    "hmc_gsd_open": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(_vp)]),
+    "hmc_gsd_close": (C.c_int, [_vp]),
+    "hmc_gsd_write_chunk": (C.c_int, [_vp, C.c_char_p, C.c_uint32, C.c_uint64, C.c_uint32, _vp]),
+    "hmc_gsd_write_strings": (C.c_int, [_vp, C.c_char_p, C.POINTER(C.c_char_p), C.c_uint64]),
+    "hmc_gsd_end_frame": (C.c_int, [_vp]),
+    "hmc_gsd_sync": (C.c_int, [_vp]),
+    "hmc_gsd_set_maximum_write_buffer_size": (C.c_int, [_vp, C.c_uint64]),
+    "hmc_gsd_get_info": (C.c_int, [_vp, C.POINTER(hmc_gsd_info)]),
+    "hmc_gsd_name": (C.c_int, [_vp, C.c_uint32, C.c_char_p, C.c_uint64]),
+    "hmc_gsd_find_chunk": (C.c_int, [_vp, C.c_uint64, C.c_char_p, C.POINTER(hmc_gsd_chunk), C.POINTER(C.c_int)]),
+    "hmc_gsd_read_chunk": (C.c_int, [_vp, C.c_uint64, C.c_char_p, C.c_uint32, C.c_uint32, _vp, C.c_uint64,
+                                     C.POINTER(C.c_uint64)]),
+    "hmc_gsd_create_hoomd": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.POINTER(_vp)]),
+    "hmc_gsd_append_frame": (C.c_int, [_vp, C.c_uint64]),
+    "hmc_gsd_frame_particles": (C.c_int, [_vp, C.c_char_p, C.c_uint32, C.c_uint64, C.c_uint32, _vp]),
+    "hmc_gsd_frame_end": (C.c_int, [_vp]),
+    "hmc_gsd_set_auto_sync_delay": (C.c_int, [_vp, C.c_double]),
+    "hmc_gsd_append_system": (C.c_int, [_vp, _vp]),
     "hmc_profile_enable": (C.c_int, [_vp, C.c_int]),
     "hmc_profile_read": (C.c_int, [_vp, C.POINTER(hmc_profile), C.c_int]),
 }

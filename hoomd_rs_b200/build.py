@@ -18,8 +18,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libhmc_b200.so")
-SOURCES = ["hmc_kernels.cu", "hmc_lj.cu", "hmc_poly.cu", "hmc_poly2.cu", "hmc_serial.cu", "hmc_capi.cu", "hmc_noalloc.cu"]
-HEADERS = ["hmc_math.cuh", "hmc_internal.cuh", "hmc_device.cuh"]
+SOURCES = ["hmc_kernels.cu", "hmc_lj.cu", "hmc_poly.cu", "hmc_poly2.cu", "hmc_serial.cu", "hmc_capi.cu", "hmc_gsd.cu", "hmc_noalloc.cu"]
+HEADERS = ["hmc_math.cuh", "hmc_internal.cuh", "hmc_device.cuh", "hmc_host.h"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=off,-fno-fast-math",

@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "../../include/hmc.h"
+#include "hmc_host.h"
 #include "hmc_internal.cuh"
 
 using namespace hmc;
@@ -105,6 +106,9 @@ struct hmc_system {
     }
     bool oriented() const { return interaction == HMC_HARD_CONVEX_POLYHEDRON || polygon(); }
     bool sat() const { return interaction == HMC_HARD_CONVEX_SURFACE_MESH_2D; }
+    // GSD frames: FP32 positions (n x 3) then versors (n x 4), on the device and pinned
+    float* gsd_dev = nullptr;
+    float* gsd_host = nullptr;
     // profiling
     bool profiling = false;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -233,6 +237,43 @@ hmc_status validate_positions(const hmc_system* s, const double* pos) {
 
 }  // namespace
 
+namespace hmc {
+
+hmc_status report_error(hmc_status st, const char* message) {
+    g_last_error = message;
+    return st;
+}
+
+// One FP32 frame of the state for a GSD file: one encoding kernel, one device-to-host copy.
+hmc_status system_gsd_frame(hmc_system* s, GsdFrameView* out) {
+    const uint64_t n = s->n;
+    const bool ori = s->oriented();
+    const uint64_t floats = n * (ori ? 7 : 3);
+    HMC_CUDA(cudaSetDevice(s->ctx->device));
+    if (n && !s->gsd_dev) {
+        hmc_status st = dalloc(s, &s->gsd_dev, 7 * n);
+        if (st != HMC_OK) return st;
+        HMC_CUDA(cudaMallocHost((void**)&s->gsd_host, sizeof(float) * 7 * n));
+    }
+    if (n) {
+        const int kind = !ori ? 0 : (s->dim == 3 ? 1 : 2);
+        HMC_CUDA(launch_gsd_encode(s->dim, kind, s->geom, s->arr.body_pos, s->arr.body_ori, n, s->gsd_dev,
+                                   s->gsd_dev + 3 * n, s->stream));
+        s->prof.kernel_launches += 1;
+        HMC_CUDA(cudaMemcpyAsync(s->gsd_host, s->gsd_dev, sizeof(float) * floats, cudaMemcpyDeviceToHost, s->stream));
+        HMC_CUDA(cudaStreamSynchronize(s->stream));
+    }
+    out->step = s->step;
+    out->dim = s->dim;
+    for (int a = 0; a < 3; ++a) out->L[a] = a < s->dim ? s->geom.L[a] : 0.0;
+    out->n = n;
+    out->position = s->gsd_host;
+    out->orientation = ori ? s->gsd_host + 3 * n : nullptr;
+    return HMC_OK;
+}
+
+}  // namespace hmc
+
 extern "C" {
 
 uint32_t hmc_abi_version(void) { return HMC_ABI_VERSION; }
@@ -251,6 +292,7 @@ const char* hmc_status_string(hmc_status st) {
         case HMC_OUT_OF_MEMORY: return "out of device memory";
         case HMC_NOT_SUPPORTED: return "not supported";
         case HMC_OUTSIDE_CHECKERBOARD: return "body outside the checkerboard";
+        case HMC_IO_ERROR: return "file I/O error or corrupt file";
     }
     return "unknown status";
 }
@@ -307,6 +349,7 @@ void hmc_system_destroy(hmc_system* s) {
         if (e) cudaEventDestroy(e);
     if (s->host_stats) cudaFreeHost(s->host_stats);
     if (s->host_first_bad) cudaFreeHost(s->host_first_bad);
+    if (s->gsd_host) cudaFreeHost(s->gsd_host);
     if (s->own_stream) cudaStreamDestroy(s->own_stream);
     cudaGetLastError();  // a destructor reports nothing: leave no sticky error behind
     hmc_context* c = s->ctx;

@@ -203,6 +203,10 @@ cudaError_t launch_check_finite(const double* packed, uint64_t count, uint32_t d
                                 unsigned long long* first_nonfinite, cudaStream_t s);
 cudaError_t launch_unpack_positions(int dim, const double* packed, double4* body_pos, uint64_t n, cudaStream_t s);
 cudaError_t launch_pack_positions(int dim, const double4* body_pos, double* packed, uint64_t n, cudaStream_t s);
+// GSD frame encoding: FP32 site positions (n x 3) and, for ori_kind 1 (versors, 3-D) or 2
+// (angles, 2-D), FP32 site versors (n x 4), in body order.
+cudaError_t launch_gsd_encode(int dim, int ori_kind, const Geometry& g, const double4* body_pos,
+                              const double4* body_ori, uint64_t n, float* pos, float* ori, cudaStream_t s);
 // Injected moves: positions (n x 4 doubles), result decisions and recheck flags.
 cudaError_t launch_eval_sphere(int dim, bool fp32, const Geometry& g, const Arrays& a, const Pair& p,
                                const uint64_t* bodies, const double4* trial, uint32_t n, uint8_t* decisions,

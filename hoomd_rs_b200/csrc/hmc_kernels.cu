@@ -1011,6 +1011,47 @@ __global__ void k_pack_angles(const double4* __restrict__ body_ori, double* __re
         packed[i] = body_ori[i].x;
 }
 
+// GSD frames (hoomd-microstate/src/append.rs:46-113): FP32 site positions and orientations in
+// tag (body) order. A single-site body's site is wrap(B + rotate(0)): the added vector is a zero
+// of either sign, and wrap maps a zero of either sign to +0, so the site is wrap(B) bit for bit.
+// The site versor is combine(q, identity) (quaternion.rs:408-415, 771-776) evaluated as written,
+// which keeps the reference's signs of zero components. In 2-D the site angle is theta + 0.0
+// and the written versor is from_axis_angle(z, theta) = (cos(t/2), 0 sin(t/2), 0 sin(t/2),
+// sin(t/2)) (quaternion.rs:560-567), with correctly rounded sin and cos. FP32 values are the
+// FP64 values rounded to nearest (Rust `as f32`).
+template <int DIM, int ORI>
+__global__ void k_gsd_encode(Geometry g, const double4* __restrict__ body_pos, const double4* __restrict__ body_ori,
+                             uint64_t n, float* __restrict__ pos, float* __restrict__ ori) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const double4 b = body_pos[i];
+        double s[3] = {b.x, b.y, b.z};
+        wrap_inv<DIM>(g.L, g.invL, s);
+        pos[3 * i + 0] = __double2float_rn(s[0]);
+        pos[3 * i + 1] = __double2float_rn(s[1]);
+        pos[3 * i + 2] = DIM == 3 ? __double2float_rn(s[2]) : 0.0f;
+        if (ORI == 1) {
+            const double4 q = body_ori[i];
+            const double v[3] = {q.y, q.z, q.w};
+            const double zero[3] = {0.0, 0.0, 0.0};
+            const double sc = dsub(dmul(q.x, 1.0), dot<3>(v, zero));
+            const double c[3] = {dsub(dmul(v[1], 0.0), dmul(v[2], 0.0)), dsub(dmul(v[2], 0.0), dmul(v[0], 0.0)),
+                                 dsub(dmul(v[0], 0.0), dmul(v[1], 0.0))};
+            ori[4 * i + 0] = __double2float_rn(sc);
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+                ori[4 * i + 1 + a] = __double2float_rn(dadd(dadd(dmul(0.0, q.x), dmul(v[a], 1.0)), c[a]));
+        } else if (ORI == 2) {
+            const double half = ddiv(dadd(body_ori[i].x, 0.0), 2.0);
+            double sn, cs;
+            cr_sincos(half, &sn, &cs);  // |half| < 2^18: angles are checked on upload
+            ori[4 * i + 0] = __double2float_rn(cs);
+            ori[4 * i + 1] = __double2float_rn(dmul(0.0, sn));
+            ori[4 * i + 2] = __double2float_rn(dmul(0.0, sn));
+            ori[4 * i + 3] = __double2float_rn(dmul(1.0, sn));
+        }
+    }
+}
+
 inline uint32_t stream_grid(uint64_t n) {
     uint64_t b = (n + 255) / 256;
     return (uint32_t)(b < 148ull * 16 ? (b ? b : 1) : 148ull * 16);
@@ -1058,6 +1099,24 @@ cudaError_t launch_unpack_angles(const double* packed, double4* body_ori, uint64
 cudaError_t launch_pack_angles(const double4* body_ori, double* packed, uint64_t n, cudaStream_t s) {
     if (n == 0) return cudaSuccess;
     k_pack_angles<<<stream_grid(n), 256, 0, s>>>(body_ori, packed, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gsd_encode(int dim, int ori_kind, const Geometry& g, const double4* body_pos,
+                              const double4* body_ori, uint64_t n, float* pos, float* ori, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    const uint32_t grid = stream_grid(n);
+    if (dim == 2) {
+        if (ori_kind == 2)
+            k_gsd_encode<2, 2><<<grid, 256, 0, s>>>(g, body_pos, body_ori, n, pos, ori);
+        else
+            k_gsd_encode<2, 0><<<grid, 256, 0, s>>>(g, body_pos, body_ori, n, pos, ori);
+    } else {
+        if (ori_kind == 1)
+            k_gsd_encode<3, 1><<<grid, 256, 0, s>>>(g, body_pos, body_ori, n, pos, ori);
+        else
+            k_gsd_encode<3, 0><<<grid, 256, 0, s>>>(g, body_pos, body_ori, n, pos, ori);
+    }
     return cudaGetLastError();
 }
 

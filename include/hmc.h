@@ -58,7 +58,8 @@ typedef enum hmc_status {
     HMC_CUDA_ERROR = 8,           /* a CUDA runtime call failed */
     HMC_OUT_OF_MEMORY = 9,
     HMC_NOT_SUPPORTED = 10,       /* combination not implemented */
-    HMC_OUTSIDE_CHECKERBOARD = 11 /* a body maps to no space (parallel_sweep.rs:198 panics) */
+    HMC_OUTSIDE_CHECKERBOARD = 11, /* a body maps to no space (parallel_sweep.rs:198 panics) */
+    HMC_IO_ERROR = 12              /* a GSD file could not be read or written, or is corrupt */
 } hmc_status;
 
 typedef enum hmc_interaction {
@@ -260,6 +261,136 @@ hmc_status hmc_math_sincos(hmc_context* ctx, const double* x, uint64_t n, double
 
 hmc_status hmc_profile_enable(hmc_system* sys, int enable);
 hmc_status hmc_profile_read(hmc_system* sys, hmc_profile* out, int reset);
+
+/* ---- GSD files (hoomd-gsd) ----
+ * The file layer replaces GsdFile (hoomd-gsd/src/file_layer.rs:559-2458): the same on-disk
+ * format (GSD 2.1: 256-byte header, 32-byte index entries sorted by (frame, id), a packed list
+ * of null-terminated chunk names), the same write buffering (chunks are appended to a write
+ * buffer that is flushed once it holds >= the maximum write buffer size, 1 MiB by default;
+ * names and index entries of completed frames reach the file only in sync), and the same
+ * growth of the index and the name list (doubled, copied to the end of the file). The same
+ * calls in the same order write byte-identical files.
+ *
+ * Errors: the calls return HMC_INVALID_ARGUMENT for caller errors and HMC_IO_ERROR for
+ * failed reads/writes or a corrupt file; hmc_gsd_last_error() names the kind (the variants of
+ * the reference's OpenError/DecodeError/EncodeError/ReadError/SyncError). Unlike the
+ * reference, a corrupt index entry is an error, never a panic (file_layer.rs:1326-1360). */
+
+typedef enum hmc_gsd_error {
+    HMC_GSD_OK = 0,
+    HMC_GSD_IO = 1,                   /* OpenError::IO, DecodeError::IO, SyncError::IO */
+    HMC_GSD_NAME_TOO_LONG = 2,        /* OpenError::NameTooLong: application/schema > 63 bytes */
+    HMC_GSD_NOT_WRITABLE = 3,         /* EncodeError/SyncError::NotWritable */
+    HMC_GSD_DUPLICATE_CHUNK_NAME = 4, /* EncodeError::DuplicateChunkName (or in a decoded name list) */
+    HMC_GSD_NAME_LIST_OVERFLOW = 5,   /* more than 65535 chunk names */
+    HMC_GSD_INVALID_COLUMNS = 6,      /* EncodeError/DecodeError::InvalidColumns */
+    HMC_GSD_INVALID_TYPE = 7,         /* DecodeError::InvalidType */
+    HMC_GSD_CHUNK_NOT_FOUND = 8,      /* ReadError::ChunkNotFound */
+    HMC_GSD_INCONSISTENT_LENGTH = 9,  /* hoomd AppendError::InconsistentLength */
+    HMC_GSD_INVALID_FILE_IDENTIFIER = 10,
+    HMC_GSD_UNSUPPORTED_VERSION = 11,
+    HMC_GSD_INDEX_OUT_OF_BOUNDS = 12,
+    HMC_GSD_NAME_LIST_OUT_OF_BOUNDS = 13,
+    HMC_GSD_NAME_LIST_NOT_TERMINATED = 14,
+    HMC_GSD_CORRUPT_INDEX_ENTRY = 15,
+    HMC_GSD_INVALID_STRING = 16,      /* application, schema, chunk name or string chunk not UTF-8 */
+    HMC_GSD_CHUNK_TOO_LARGE = 17      /* hoomd AppendError::ChunkTooLarge: N does not fit in u32 */
+} hmc_gsd_error;
+
+/* GSD data types (file_layer.rs DataType): the value stored in an index entry. */
+typedef enum hmc_gsd_type {
+    HMC_GSD_U8 = 1, HMC_GSD_U16 = 2, HMC_GSD_U32 = 3, HMC_GSD_U64 = 4,
+    HMC_GSD_I8 = 5, HMC_GSD_I16 = 6, HMC_GSD_I32 = 7, HMC_GSD_I64 = 8,
+    HMC_GSD_F32 = 9, HMC_GSD_F64 = 10, HMC_GSD_STRING = 11
+} hmc_gsd_type;
+
+/* One index entry (file_layer.rs IndexEntry): rows n, columns m, byte offset of the data. */
+typedef struct hmc_gsd_chunk {
+    uint64_t frame;
+    uint64_t rows;
+    uint64_t location;
+    uint32_t columns;
+    uint16_t id;
+    uint8_t type;
+    uint8_t flags;
+} hmc_gsd_chunk;
+
+typedef struct hmc_gsd hmc_gsd;
+
+/* The kind of the calling thread's last failed hmc_gsd_* call (HMC_GSD_OK after a success). */
+hmc_gsd_error hmc_gsd_last_error(void);
+
+/* GsdFile::create (exclusive = 0: truncate an existing file) and GsdFile::create_new
+ * (exclusive = 1: fail if the path exists); the file is open for writing. */
+hmc_status hmc_gsd_create(const char* path, const char* application, const char* schema, uint16_t schema_major,
+                          uint16_t schema_minor, int exclusive, hmc_gsd** out);
+/* GsdFile::open; writable = 0: Mode::Read, 1: Mode::Write (appends after the last frame). */
+hmc_status hmc_gsd_open(const char* path, int writable, hmc_gsd** out);
+/* Drop: a writable file is synchronised first (its error is returned, the handle is freed). */
+hmc_status hmc_gsd_close(hmc_gsd* file);
+
+/* write_scalars / write_arrays / write_string: rows x columns values of type `type`
+ * (columns = 1 for scalars; HMC_GSD_STRING: rows = byte length, columns = 1). */
+hmc_status hmc_gsd_write_chunk(hmc_gsd* file, const char* name, uint32_t type, uint64_t rows, uint32_t columns,
+                               const void* data);
+/* write_strings_array: rows strings padded with zeros to (longest + 1) columns of type i8. */
+hmc_status hmc_gsd_write_strings(hmc_gsd* file, const char* name, const char* const* strings, uint64_t count);
+hmc_status hmc_gsd_end_frame(hmc_gsd* file);
+hmc_status hmc_gsd_sync(hmc_gsd* file);
+hmc_status hmc_gsd_set_maximum_write_buffer_size(hmc_gsd* file, uint64_t bytes);
+
+/* File facts: frames in the file (n_frames), frames written so far including buffered ones,
+ * file length in bytes, index entries in the file, chunk names known, header fields. Any
+ * output pointer may be NULL. application/schema: buffers of >= 64 bytes. */
+typedef struct hmc_gsd_info {
+    uint64_t n_frames;
+    uint64_t buffer_frame;
+    uint64_t file_length;
+    uint64_t index_entries;
+    uint64_t index_allocated_entries;
+    uint64_t namelist_allocated_entries;
+    uint32_t n_names;
+    uint16_t schema_major, schema_minor;
+    uint16_t gsd_major, gsd_minor;
+    int writable;
+    uint64_t maximum_write_buffer_size;
+    char application[64];
+    char schema[64];
+} hmc_gsd_info;
+hmc_status hmc_gsd_get_info(hmc_gsd* file, hmc_gsd_info* out);
+/* The i-th chunk name in id order (name_id); buffer of `capacity` bytes. */
+hmc_status hmc_gsd_name(hmc_gsd* file, uint32_t id, char* buffer, uint64_t capacity);
+
+/* find_chunk: *found = 0 when the frame is not in the file or the name is unknown. */
+hmc_status hmc_gsd_find_chunk(hmc_gsd* file, uint64_t frame, const char* name, hmc_gsd_chunk* out, int* found);
+/* iter_scalars / iter_arrays / read_string: copies the chunk's bytes into `out` after checking
+ * its type (HMC_GSD_INVALID_TYPE) and columns (HMC_GSD_INVALID_COLUMNS; columns = 1 for
+ * scalars and strings). capacity: bytes available at out; *rows receives the row count. */
+hmc_status hmc_gsd_read_chunk(hmc_gsd* file, uint64_t frame, const char* name, uint32_t type, uint32_t columns,
+                              void* out, uint64_t capacity, uint64_t* rows);
+
+/* ---- HOOMD schema frames (hoomd-gsd/src/hoomd.rs) ----
+ * hmc_gsd_create_hoomd: HoomdGsdFile::create/create_new: schema "hoomd" version 1.4 and the
+ * given application (NULL: "hoomd-rs-b200"). */
+hmc_status hmc_gsd_create_hoomd(const char* path, const char* application, int exclusive, hmc_gsd** out);
+/* HoomdGsdFile::append_frame(step): writes configuration/step and opens a frame. */
+hmc_status hmc_gsd_append_frame(hmc_gsd* file, uint64_t step);
+/* Frame::particles_*: the first particles chunk of a frame writes particles/N (u32) = rows;
+ * later ones must have the same rows (HMC_GSD_INCONSISTENT_LENGTH). */
+hmc_status hmc_gsd_frame_particles(hmc_gsd* file, const char* name, uint32_t type, uint64_t rows, uint32_t columns,
+                                   const void* data);
+/* Frame::end (or drop): end_frame, then sync when the auto-sync delay (10 s by default)
+ * has passed since the last sync. */
+hmc_status hmc_gsd_frame_end(hmc_gsd* file);
+hmc_status hmc_gsd_set_auto_sync_delay(hmc_gsd* file, double seconds);
+/* AppendMicrostate::append_microstate (hoomd-microstate/src/append.rs:115-129) from the
+ * device state: configuration/step, particles/N, particles/position (FP32 site positions
+ * wrap(B), z = 0 in 2-D), particles/orientation (oriented shapes: FP32 site versors; in 2-D
+ * the versor of the rotation by theta about z), configuration/dimensions and
+ * configuration/box ([Lx, Ly, Lz or 0, 0, 0, 0]). The positions and versors are converted on
+ * the GPU and copied to the host once. The frame stays open for more chunks (log/...) until
+ * hmc_gsd_frame_end. */
+hmc_status hmc_gsd_append_system(hmc_gsd* file, hmc_system* sys);
 
 #ifdef __cplusplus
 }

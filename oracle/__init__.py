@@ -89,6 +89,7 @@ def lib():
         L.oracle_system_destroy.argtypes = [C.c_void_p]
         L.oracle_get_state.argtypes = [C.c_void_p, _dp, _dp, _u64p, _u32p]
         L.oracle_set_counter.argtypes = [C.c_void_p, C.c_uint64, C.c_uint32]
+        L.oracle_gsd_frame.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.oracle_increment_step.argtypes = [C.c_void_p]
         L.oracle_parallel_sweep.argtypes = [C.c_void_p, C.c_uint32, C.c_double, C.c_double, C.c_double,
                                             _u64p, _u64p]
@@ -330,6 +331,13 @@ class System:
 
     def set_counter(self, step, substep):
         lib().oracle_set_counter(self._h, step, substep)
+
+    def gsd_frame(self):
+        """FP32 site positions (n, 3) and versors (n, 4) or None, as a GSD frame holds them."""
+        pos = np.zeros((self.n, 3), dtype=np.float32)
+        ori = np.zeros((self.n, 4), dtype=np.float32) if self.ori_len else None
+        lib().oracle_gsd_frame(self._h, pos.ctypes.data, None if ori is None else ori.ctypes.data)
+        return pos, ori
 
     def increment_step(self):
         lib().oracle_increment_step(self._h)

@@ -1214,6 +1214,50 @@ void oracle_ziggurat_tables(double* x_out, double* f_out) {
 }
 
 void oracle_wrap(uint32_t dim, const double* L, double* point) { wrap((int)dim, L, point); }
+// AppendMicrostate::append_microstate (hoomd-microstate/src/append.rs:46-113) for single-site
+// bodies: each site is wrap(body.transform(site_local)) with the site at the body origin and the
+// identity orientation (microstate.rs:995-1010; Transform for Point: position + site position,
+// for OrientedPoint: position + rotate(site position), orientation.combine(site orientation),
+// property/oriented_point.rs:108-113), written in tag order as FP32 (Rust `as f32`). 2-D
+// orientations are written as Versor::from_axis_angle(z, theta) (append.rs:91-104,
+// quaternion.rs:560-567). pos: n x 3 floats; ori: n x 4 floats (oriented shapes only).
+void oracle_gsd_frame(const oracle_system* s, float* pos, float* ori) {
+    const double zero[3] = {0.0, 0.0, 0.0};
+    for (uint64_t i = 0; i < s->n; ++i) {
+        double p[3] = {0.0, 0.0, 0.0};
+        const double* b = &s->body[3 * i];
+        if (!s->oriented()) {
+            for (int a = 0; a < s->dim; ++a) p[a] = b[a] + zero[a];
+        } else if (s->dim == 3) {
+            const double* o = &s->orient[4 * i];
+            const Quat q{o[0], o[1], o[2], o[3]};
+            const V3 r = versor_rotate(q, zero);
+            for (int a = 0; a < 3; ++a) p[a] = b[a] + r.v[a];
+            const Quat site = qmul(q, Quat{1.0, 0.0, 0.0, 0.0});
+            ori[4 * i + 0] = (float)site.s;
+            ori[4 * i + 1] = (float)site.x;
+            ori[4 * i + 2] = (float)site.y;
+            ori[4 * i + 3] = (float)site.z;
+        } else {
+            const double theta = s->orient[i];
+            double sn, cs;
+            cr_sincos(theta, &sn, &cs);  // Angle::rotate (angle.rs:175-182)
+            const double r[2] = {zero[0] * cs - zero[1] * sn, zero[0] * sn + zero[1] * cs};
+            for (int a = 0; a < 2; ++a) p[a] = b[a] + r[a];
+            const double t = theta + 0.0;  // Angle::combine with the site's angle 0
+            double hs, hc;
+            cr_sincos(t / 2.0, &hs, &hc);
+            ori[4 * i + 0] = (float)hc;
+            ori[4 * i + 1] = (float)(0.0 * hs);
+            ori[4 * i + 2] = (float)(0.0 * hs);
+            ori[4 * i + 3] = (float)(1.0 * hs);
+        }
+        wrap(s->dim, s->L, p);
+        pos[3 * i + 0] = (float)p[0];
+        pos[3 * i + 1] = (float)p[1];
+        pos[3 * i + 2] = s->dim == 3 ? (float)p[2] : 0.0f;
+    }
+}
 uint32_t oracle_generate_ghosts(uint32_t dim, const double* L, double range, const double* point,
                                 double* out) {
     double g[7][3];

@@ -98,6 +98,9 @@ void oracle_system_destroy(oracle_system* s);
 void oracle_get_state(const oracle_system* s, double* positions, double* orientations,
                       uint64_t* step, uint32_t* substep);
 void oracle_set_counter(oracle_system* s, uint64_t step, uint32_t substep);
+// The FP32 site positions (n x 3) and site versors (n x 4, oriented shapes) that
+// AppendMicrostate writes to a GSD frame (hoomd-microstate/src/append.rs:46-113).
+void oracle_gsd_frame(const oracle_system* s, float* positions, float* orientations);
 void oracle_increment_step(oracle_system* s);
 
 // ParallelSweep::apply (parallel_sweep.rs:390-421). Returns 0, or 1 on a checkerboard error.
