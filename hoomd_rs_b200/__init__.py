@@ -33,7 +33,8 @@ LIB_PATH = os.environ.get("HMC_B200_LIB", os.path.join(_HERE, "libhmc_b200.so"))
 OK, INVALID_ARGUMENT, RANGE_TOO_LARGE, OVERLAP_IN_INPUT, CELL_OVERFLOW, NAN_STATE, ITERATION_CAP, TIMEOUT, \
     CUDA_ERROR, OUT_OF_MEMORY, NOT_SUPPORTED, OUTSIDE_CHECKERBOARD, IO_ERROR = range(13)
 # hmc_interaction / hmc_move / hmc_precision
-HARD_SPHERE, HARD_CONVEX_POLYGON, HARD_CONVEX_POLYHEDRON, LENNARD_JONES, HARD_CONVEX_SURFACE_MESH_2D = range(5)
+HARD_SPHERE, HARD_CONVEX_POLYGON, HARD_CONVEX_POLYHEDRON, LENNARD_JONES, HARD_CONVEX_SURFACE_MESH_2D, \
+    OVERLAP_PENALTY = range(6)
 TRANSLATE, ROTATE = range(2)
 FP64, FP32_RECHECK = range(2)
 
@@ -54,7 +55,9 @@ class hmc_system_desc(C.Structure):
                 ("interaction", C.c_uint32), ("n_vertices", C.c_uint32), ("vertices", C.POINTER(C.c_double)),
                 ("diameter", C.c_double), ("lj_epsilon", C.c_double), ("lj_sigma", C.c_double),
                 ("lj_r_cut", C.c_double), ("lj_r_shift", C.c_double), ("boundary_range", C.c_double),
-                ("body_interaction_range", C.c_double)]
+                ("body_interaction_range", C.c_double), ("penalty_k", C.c_double),
+                ("penalty_maximum_overlap", C.c_double), ("penalty_shoulder", C.c_double),
+                ("capacity", C.c_uint64)]
 
 
 class hmc_sweep_params(C.Structure):
@@ -71,6 +74,17 @@ class hmc_count(C.Structure):
 class hmc_injected_move(C.Structure):
     _fields_ = [("body", C.c_uint64), ("position", C.c_double * 3), ("orientation", C.c_double * 4),
                 ("u", C.c_double)]
+
+
+class hmc_quick_insert(C.Structure):
+    _fields_ = [("target", C.c_uint64), ("allowed_overlaps", C.c_uint64), ("inserted", C.c_uint64),
+                ("complete", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+class hmc_quick_compress(C.Structure):
+    _fields_ = [("target_volume", C.c_double), ("maximum_energy_per_site", C.c_double),
+                ("maximum_delta", C.c_double), ("state", C.c_uint32), ("is_final", C.c_uint32),
+                ("boundary", C.c_double * 3)]
 
 
 class hmc_gsd_chunk(C.Structure):
@@ -127,6 +141,11 @@ SIGNATURES = {
                                  _u8p, _dp]),
     "hmc_total_energy": (C.c_int, [_vp, _dp]),
     "hmc_overlap_count_noalloc": (C.c_int, [_vp, C.c_uint64, C.c_uint32, _dp, C.c_double, C.c_double, _vp, _vp]),
+    "hmc_quick_insert_apply": (C.c_int, [_vp, C.POINTER(hmc_quick_insert), C.POINTER(hmc_count)]),
+    "hmc_quick_compress_apply": (C.c_int, [_vp, C.POINTER(hmc_quick_compress)]),
+    "hmc_get_box": (C.c_int, [_vp, _dp]),
+    "hmc_set_box": (C.c_int, [_vp, _dp]),
+    "hmc_get_n_bodies": (C.c_int, [_vp, C.POINTER(C.c_uint64)]),
     "hmc_gsd_last_error": (C.c_int, []),
     "hmc_gsd_create": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_uint16, C.c_uint16, C.c_int,
                                  C.POINTER(_vp)]),
@@ -226,6 +245,23 @@ class LennardJones:
 
 
 @dataclass
+class OverlapPenalty:
+    """hoomd_interaction::univariate::OverlapPenalty (overlap_penalty.rs:42-116): inf below
+    -maximum_allowed_overlap, (k/2) r^2 + epsilon_shoulder below 0, else 0. Defaults as
+    OverlapPenalty::default()."""
+    k: float = 10000.0
+    maximum_allowed_overlap: float = 0.2
+    epsilon_shoulder: float = 100.0
+
+
+@dataclass
+class Expanded:
+    """hoomd_interaction::univariate::Expanded (expanded.rs:62-67): f(r - delta)."""
+    delta: float
+    f: OverlapPenalty
+
+
+@dataclass
 class Shifted:
     """hoomd_interaction::univariate::Shifted (shifted.rs:57-102): f(r) - f(r_shift)."""
     f: LennardJones
@@ -235,7 +271,7 @@ class Shifted:
 @dataclass
 class Isotropic:
     """hoomd_interaction::pairwise::Isotropic (isotropic.rs:88-187)."""
-    interaction: Shifted
+    interaction: object  # Shifted(LennardJones) or Expanded(OverlapPenalty)
     r_cut: float
 
     @property
@@ -412,7 +448,7 @@ class Microstate:
 
     def __init__(self, ctx: Context, boundary: Periodic, positions, hamiltonian: PairwiseCutoff, *,
                  step: int = 0, substep: int = 0, seed: int = 0, body_interaction_range: float = 0.0,
-                 orientations=None):
+                 orientations=None, capacity: int = 0):
         lib = load_library()
         L = [float(x) for x in boundary.edge_lengths]
         self.dim = len(L)
@@ -436,6 +472,15 @@ class Microstate:
             self._verts = verts  # keep alive during the call
             d.n_vertices = verts.shape[0]
             d.vertices = verts.ctypes.data_as(_dp)
+        elif isinstance(pair, Isotropic) and isinstance(pair.interaction, Expanded):
+            # the overlap-penalty sphere: Isotropic { Expanded { delta: d, OverlapPenalty }, r_cut: d }
+            if pair.interaction.delta != pair.r_cut:
+                raise HmcError(NOT_SUPPORTED, "Expanded(OverlapPenalty) needs delta == r_cut")
+            d.interaction = OVERLAP_PENALTY
+            d.diameter = pair.r_cut
+            d.penalty_k = pair.interaction.f.k
+            d.penalty_maximum_overlap = pair.interaction.f.maximum_allowed_overlap
+            d.penalty_shoulder = pair.interaction.f.epsilon_shoulder
         elif isinstance(pair, Isotropic) and isinstance(pair.interaction, Shifted):
             d.interaction = LENNARD_JONES
             d.lj_epsilon = pair.interaction.f.epsilon
@@ -446,6 +491,7 @@ class Microstate:
             raise HmcError(NOT_SUPPORTED, f"{type(pair).__name__}")
         d.boundary_range = boundary.maximum_interaction_range
         d.body_interaction_range = body_interaction_range
+        d.capacity = max(int(capacity), self.n)
         self.oriented = d.interaction in (HARD_CONVEX_POLYHEDRON, HARD_CONVEX_POLYGON, HARD_CONVEX_SURFACE_MESH_2D)
         self.ori_len = (4 if self.dim == 3 else 1) if self.oriented else 0
         ori = None
@@ -564,10 +610,12 @@ class Microstate:
         _check(_lib.hmc_sweep(self._h, C.byref(p), C.byref(c)))
         return Count(c.accepted, c.rejected, c.rechecks, c.pair_checks, c.max_fp32_error)
 
-    def serial_sweep(self, maximum: float, n_sweeps: int = 1, increment_step: bool = False, move_mask=None) -> "Count":
-        """Sweep::apply_with_filter (sweep.rs:159-224), hard spheres: bodies in index order from one
-        sequential stream; move_mask (n booleans) plays should_move_body."""
-        p = hmc_sweep_params(C.sizeof(hmc_sweep_params), TRANSLATE, maximum, 1.0, FP64, n_sweeps, int(increment_step), 0)
+    def serial_sweep(self, maximum: float, n_sweeps: int = 1, increment_step: bool = False, move_mask=None,
+                     temperature: float = 1.0) -> "Count":
+        """Sweep::apply_with_filter (sweep.rs:159-224), hard or overlap-penalty spheres: bodies in
+        index order from one sequential stream; move_mask (n booleans) plays should_move_body."""
+        p = hmc_sweep_params(C.sizeof(hmc_sweep_params), TRANSLATE, maximum, temperature, FP64, n_sweeps,
+                             int(increment_step), 0)
         c = hmc_count()
         mask = None
         if move_mask is not None:
@@ -600,10 +648,119 @@ class Microstate:
             return dec.astype(bool), rech.astype(bool), dh
         return dec.astype(bool), rech.astype(bool)
 
+    def refresh(self):
+        """Re-read the body count (QuickInsert appends bodies on the device)."""
+        n = C.c_uint64()
+        _check(_lib.hmc_get_n_bodies(self._h, C.byref(n)))
+        self.n = n.value
+
+    def box(self) -> np.ndarray:
+        L = np.zeros(3)
+        _check(_lib.hmc_get_box(self._h, L.ctypes.data_as(_dp)))
+        return L[:self.dim].copy()
+
+    def set_box(self, edge_lengths):
+        """Microstate::clone_with_boundary onto a periodic box with these edge lengths."""
+        L = np.zeros(3)
+        L[:self.dim] = edge_lengths
+        _check(_lib.hmc_set_box(self._h, L.ctypes.data_as(_dp)))
+        self.edge_lengths = [float(x) for x in L[:self.dim]]
+
+    def volume(self) -> float:
+        v = None
+        for x in self.box():
+            v = x if v is None else v * x
+        return float(v)
+
     def total_energy(self) -> float:
         e = C.c_double()
         _check(_lib.hmc_total_energy(self._h, C.byref(e)))
         return e.value
+
+
+class QuickInsert:
+    """hoomd_mc::QuickInsert (quick_insert.rs:94-280) with the distribution UniformIn over the
+    microstate's box and one site at the body origin; the microstate needs the capacity
+    (Microstate(..., capacity=N))."""
+
+    def __init__(self, target: int, allowed_overlaps: Optional[int] = None):
+        self._s = hmc_quick_insert(int(target), max(int(target) // 8, 1) if allowed_overlaps is None
+                                   else int(allowed_overlaps), 0, 0, 0)
+
+    @classmethod
+    def new(cls, target: int) -> "QuickInsert":
+        return cls(target)
+
+    @property
+    def target(self) -> int:
+        return self._s.target
+
+    @property
+    def inserted(self) -> int:
+        return self._s.inserted
+
+    def is_complete(self) -> bool:
+        return bool(self._s.complete)
+
+    def apply(self, microstate: Microstate, hamiltonian=None) -> Count:
+        c = hmc_count()
+        _check(_lib.hmc_quick_insert_apply(microstate._h, C.byref(self._s), C.byref(c)))
+        microstate.refresh()
+        return Count(c.accepted, c.rejected, 0, 0, 0.0)
+
+
+class QuickCompress:
+    """hoomd_mc::QuickCompress (quick_compress.rs:88-383)."""
+
+    STARTUP, WAITING, COMPRESSING, COMPLETE = range(4)
+
+    def __init__(self, target_volume: float):
+        self._s = hmc_quick_compress(float(target_volume), 1000.0, 0.05, self.STARTUP, 0)
+
+    @classmethod
+    def with_target_volume(cls, target_volume: float) -> "QuickCompress":
+        return cls(target_volume)
+
+    @property
+    def target_volume(self) -> float:
+        return self._s.target_volume
+
+    def set_target_volume(self, target_volume: float):
+        """set_target_volume (quick_compress.rs:215-240): Startup and Complete restart, Waiting
+        forgets that it was final, Compressing continues."""
+        if self._s.target_volume != target_volume:
+            if self._s.state in (self.STARTUP, self.COMPLETE):
+                self._s.state = self.STARTUP
+            elif self._s.state == self.WAITING:
+                self._s.is_final = 0
+        self._s.target_volume = float(target_volume)
+
+    @property
+    def maximum_energy_per_site(self) -> float:
+        return self._s.maximum_energy_per_site
+
+    @maximum_energy_per_site.setter
+    def maximum_energy_per_site(self, v: float):
+        self._s.maximum_energy_per_site = float(v)
+
+    @property
+    def maximum_delta(self) -> float:
+        return self._s.maximum_delta
+
+    @maximum_delta.setter
+    def maximum_delta(self, v: float):
+        self._s.maximum_delta = float(v)
+
+    @property
+    def state(self) -> int:
+        return self._s.state
+
+    def is_complete(self) -> bool:
+        return self._s.state == self.COMPLETE
+
+    def apply(self, microstate: Microstate, hamiltonian=None):
+        _check(_lib.hmc_quick_compress_apply(microstate._h, C.byref(self._s)))
+        microstate.edge_lengths = [float(x) for x in microstate.box()]
 
 
 class Batch:
@@ -738,5 +895,6 @@ class ParallelSweep:
 __all__ = ["Batch", "Context", "sdf_pressure", "gr_normalise", "ConvexPolygon", "ConvexPolyhedron", "ConvexSurfaceMesh2d", "Count", "convex_hull_2d", "HardShape", "HardSphere", "HmcError", "Isothermal", "Isotropic",
            "LennardJones", "Microstate", "PairwiseCutoff", "Rotate", "Shifted", "TuneOptions",
            "ParallelSweep", "Periodic", "Translate", "load_library", "SIGNATURES", "FP64", "FP32_RECHECK",
+           "QuickInsert", "QuickCompress", "OverlapPenalty", "Expanded",
            "TRANSLATE", "ROTATE", "HARD_SPHERE", "HARD_CONVEX_POLYGON", "HARD_CONVEX_POLYHEDRON", "LENNARD_JONES",
            "HARD_CONVEX_SURFACE_MESH_2D"]

@@ -109,6 +109,15 @@ struct hmc_system {
     // GSD frames: FP32 positions (n x 3) then versors (n x 4), on the device and pinned
     float* gsd_dev = nullptr;
     float* gsd_host = nullptr;
+    // bodies the per-body arrays hold (QuickInsert appends up to it)
+    uint64_t capacity = 0;
+    uint64_t cells_alloc = 0;           // spaces the checkerboard arrays hold
+    double serial_L[3] = {0, 0, 0};     // box the serial grid was laid out for
+    double4* backup = nullptr;          // [capacity] body positions kept across a box change
+    unsigned long long* qi_out = nullptr;  // [4] QuickInsert results
+    double lj_params[4] = {1, 1, 2.5, 2.5};  // epsilon, sigma, r_cut, r_shift
+    bool penalty() const { return interaction == HMC_OVERLAP_PENALTY; }
+    bool soft() const { return interaction == HMC_LENNARD_JONES || penalty(); }
     // profiling
     bool profiling = false;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -127,6 +136,15 @@ hmc_status dalloc(hmc_system* s, T** p, size_t count) {
                     sizeof(T) * count, cudaGetErrorString(e));
     s->allocations.push_back((void*)*p);
     return HMC_OK;
+}
+
+template <typename T>
+void dfree(hmc_system* s, T** p) {
+    if (!*p) return;
+    auto it = std::find(s->allocations.begin(), s->allocations.end(), (void*)*p);
+    if (it != s->allocations.end()) s->allocations.erase(it);
+    cudaFree((void*)*p);
+    *p = nullptr;
 }
 
 // The forward-error bound of the FP32 pair test for hard spheres. With u32 = 2^-24 and
@@ -200,6 +218,75 @@ void lj_setup(hmc_system* s, double eps, double sigma, double rcut, double rshif
     P.lj_band_energy = (float)(2.0 * std::max(std::fabs(e_lo), std::fabs(e_hi)) + 1e-7);
 }
 
+// Pair thresholds that depend on the box (FP32 bounds use the space widths and box lengths).
+void pair_setup(hmc_system* s) {
+    if (s->interaction == HMC_HARD_SPHERE) {
+        sphere_bound(s);
+    } else if (s->oriented()) {
+        s->pair.sigma2 = s->poly_rcut2;  // the FP32 prefilter threshold reuses the sphere bound
+        sphere_bound(s);
+        s->poly_rcut2_hi32 = s->pair.sig2_hi32;
+    } else if (s->interaction == HMC_LENNARD_JONES) {
+        lj_setup(s, s->lj_params[0], s->lj_params[1], s->lj_params[2], s->lj_params[3]);
+    }
+}
+
+// The periodic box and its checkerboard: Periodic::new's range check (boundary/periodic.rs:
+// 97-107) and HypercuboidCheckerboard::compute_dimensions (hypercuboid.rs:188-228). The
+// checkerboard arrays grow when the box needs more spaces than they hold.
+hmc_status setup_geometry(hmc_system* s, const double* L) {
+    Geometry g = s->geom;
+    for (int a = 0; a < 3; ++a) g.L[a] = a < s->dim ? L[a] : 1.0;
+    double min_l = g.L[0];
+    for (int a = 0; a < s->dim; ++a) {
+        if (!(g.L[a] > 0.0) || !std::isfinite(g.L[a])) return fail(HMC_INVALID_ARGUMENT, "edge length %d must be positive", a);
+        min_l = std::min(min_l, g.L[a]);
+    }
+    if (s->boundary_range > min_l / 2.0)
+        return fail(HMC_RANGE_TOO_LARGE, "boundary interaction range %g exceeds L/2 = %g", s->boundary_range, min_l / 2.0);
+    if (!compute_dimensions(s->dim, g.L, s->body_range, g.width, g.shape))
+        return fail(HMC_RANGE_TOO_LARGE, "body interaction range %g leaves fewer than 2 spaces per axis", s->body_range);
+    uint64_t cells = 1;
+    g.any_two = 0;
+    for (int a = 0; a < s->dim; ++a) {
+        g.half[a] = g.L[a] / 2.0;
+        g.ghost_hi[a] = g.half[a] - s->boundary_range;
+        g.ghost_lo[a] = -g.half[a] + s->boundary_range;
+        g.w32[a] = (float)g.width[a];
+        g.invL[a] = 1.0 / g.L[a];
+        g.invW[a] = 1.0 / g.width[a];
+        g.half_shape[a] = g.shape[a] / 2;
+        cells *= g.shape[a];
+    }
+    if (cells > 16000000ull)
+        return fail(HMC_NOT_SUPPORTED, "%llu checkerboard spaces exceed the supported 16M", (unsigned long long)cells);
+    // colour lists pack the multi-index: 10 bits per axis in 3-D, 16 in 2-D
+    for (int a = 0; a < s->dim; ++a) {
+        if (g.shape[a] > (s->dim == 3 ? 1024u : 65535u))
+            return fail(HMC_NOT_SUPPORTED, "%u spaces on axis %d exceed the supported %u", g.shape[a], a,
+                        s->dim == 3 ? 1024u : 65535u);
+        if (g.shape[a] == 2) g.any_two = 1;
+    }
+    g.n_cells = (uint32_t)cells;
+    g.color_stride = (uint32_t)(cells >> s->dim);
+    if (cells > s->cells_alloc) {
+        Arrays& A = s->arr;
+        dfree(s, &A.cell_count);
+        dfree(s, &A.cell_start);
+        dfree(s, &A.block_sums);
+        dfree(s, &A.color_cells);
+        const uint32_t scan_blocks = (uint32_t)((cells + 2047) / 2048);
+        hmc_status st;
+        if ((st = dalloc(s, &A.cell_count, cells)) || (st = dalloc(s, &A.cell_start, cells + 1)) ||
+            (st = dalloc(s, &A.block_sums, (size_t)scan_blocks * 9)) || (st = dalloc(s, &A.color_cells, cells)))
+            return st;
+        s->cells_alloc = cells;
+    }
+    s->geom = g;
+    pair_setup(s);
+    return HMC_OK;
+}
+
 hmc_status read_stats(hmc_system* s) {
     HMC_CUDA(cudaMemcpyAsync(s->host_stats, s->arr.stats, sizeof(DeviceStats), cudaMemcpyDeviceToHost, s->stream));
     HMC_CUDA(cudaStreamSynchronize(s->stream));
@@ -251,14 +338,14 @@ hmc_status system_gsd_frame(hmc_system* s, GsdFrameView* out) {
     const uint64_t floats = n * (ori ? 7 : 3);
     HMC_CUDA(cudaSetDevice(s->ctx->device));
     if (n && !s->gsd_dev) {
-        hmc_status st = dalloc(s, &s->gsd_dev, 7 * n);
+        hmc_status st = dalloc(s, &s->gsd_dev, 7 * s->capacity);
         if (st != HMC_OK) return st;
-        HMC_CUDA(cudaMallocHost((void**)&s->gsd_host, sizeof(float) * 7 * n));
+        HMC_CUDA(cudaMallocHost((void**)&s->gsd_host, sizeof(float) * 7 * s->capacity));
     }
     if (n) {
         const int kind = !ori ? 0 : (s->dim == 3 ? 1 : 2);
         HMC_CUDA(launch_gsd_encode(s->dim, kind, s->geom, s->arr.body_pos, s->arr.body_ori, n, s->gsd_dev,
-                                   s->gsd_dev + 3 * n, s->stream));
+                                   s->gsd_dev + 3 * n, s->stream));  // versors follow the n positions
         s->prof.kernel_launches += 1;
         HMC_CUDA(cudaMemcpyAsync(s->gsd_host, s->gsd_dev, sizeof(float) * floats, cudaMemcpyDeviceToHost, s->stream));
         HMC_CUDA(cudaStreamSynchronize(s->stream));
@@ -368,9 +455,10 @@ hmc_status hmc_system_create(hmc_context* ctx, const hmc_system_desc* d, const d
     for (uint32_t a = 0; a < d->dim; ++a)
         if (!(d->edge_lengths[a] > 0.0) || !std::isfinite(d->edge_lengths[a]))
             return fail(HMC_INVALID_ARGUMENT, "edge length %u must be positive", a);
+    if (d->capacity >= (1ull << 31)) return fail(HMC_INVALID_ARGUMENT, "capacity too large");
     if (d->interaction != HMC_HARD_SPHERE && d->interaction != HMC_LENNARD_JONES &&
         d->interaction != HMC_HARD_CONVEX_POLYHEDRON && d->interaction != HMC_HARD_CONVEX_POLYGON &&
-        d->interaction != HMC_HARD_CONVEX_SURFACE_MESH_2D)
+        d->interaction != HMC_HARD_CONVEX_SURFACE_MESH_2D && d->interaction != HMC_OVERLAP_PENALTY)
         return fail(HMC_NOT_SUPPORTED, "interaction %u is not available in this build", d->interaction);
     const bool polygon = d->interaction == HMC_HARD_CONVEX_POLYGON || d->interaction == HMC_HARD_CONVEX_SURFACE_MESH_2D;
     if (polygon) {
@@ -408,8 +496,12 @@ hmc_status hmc_system_create(hmc_context* ctx, const hmc_system_desc* d, const d
         for (uint32_t i = 0; i < 3 * d->n_vertices; ++i)
             if (!std::isfinite(d->vertices[i])) return fail(HMC_INVALID_ARGUMENT, "vertex coordinates must be finite");
     }
-    if (d->interaction == HMC_HARD_SPHERE && !(d->diameter > 0.0))
+    if ((d->interaction == HMC_HARD_SPHERE || d->interaction == HMC_OVERLAP_PENALTY) && !(d->diameter > 0.0))
         return fail(HMC_INVALID_ARGUMENT, "diameter must be positive");
+    if (d->interaction == HMC_OVERLAP_PENALTY &&
+        (!(d->penalty_k >= 0.0) || !std::isfinite(d->penalty_k) || !(d->penalty_maximum_overlap >= 0.0) ||
+         !std::isfinite(d->penalty_maximum_overlap) || !std::isfinite(d->penalty_shoulder)))
+        return fail(HMC_INVALID_ARGUMENT, "overlap penalty k and maximum overlap must be finite and >= 0");
     if (d->interaction == HMC_LENNARD_JONES &&
         (!(d->lj_sigma > 0.0) || !(d->lj_r_cut > 0.0) || !(d->lj_r_shift > 0.0) || !std::isfinite(d->lj_epsilon)))
         return fail(HMC_INVALID_ARGUMENT, "Lennard-Jones sigma, r_cut and r_shift must be positive");
@@ -436,6 +528,7 @@ hmc_status hmc_system_create(hmc_context* ctx, const hmc_system_desc* d, const d
     s->ctx = ctx;
     s->dim = (int)d->dim;
     s->n = d->n_bodies;
+    s->capacity = std::max<uint64_t>(d->n_bodies, d->capacity);
     s->step = d->step;
     s->substep = d->substep;
     s->seed = d->seed;
@@ -445,66 +538,41 @@ hmc_status hmc_system_create(hmc_context* ctx, const hmc_system_desc* d, const d
                                                                   : d->diameter;
     s->boundary_range = d->boundary_range > 0.0 ? d->boundary_range : s->pair_range;
     s->body_range = d->body_interaction_range > 0.0 ? d->body_interaction_range : s->pair_range;
-    for (int a = 0; a < 3; ++a) s->geom.L[a] = a < s->dim ? d->edge_lengths[a] : 1.0;
-    double min_l = s->geom.L[0];
-    for (int a = 0; a < s->dim; ++a) min_l = std::min(min_l, s->geom.L[a]);
     auto destroy_fail = [&](hmc_status st) {
         std::string msg = g_last_error;
         hmc_system_destroy(s);
         g_last_error = msg;
         return st;
     };
-    if (s->boundary_range > min_l / 2.0) {
-        fail(HMC_RANGE_TOO_LARGE, "boundary interaction range %g exceeds L/2 = %g", s->boundary_range, min_l / 2.0);
-        return destroy_fail(HMC_RANGE_TOO_LARGE);
-    }
     if (s->body_range < s->pair_range) {
         fail(HMC_INVALID_ARGUMENT, "body interaction range %g is below the pair range %g", s->body_range, s->pair_range);
         return destroy_fail(HMC_INVALID_ARGUMENT);
     }
-    if (!compute_dimensions(s->dim, s->geom.L, s->body_range, s->geom.width, s->geom.shape)) {
-        fail(HMC_RANGE_TOO_LARGE, "body interaction range %g leaves fewer than 2 spaces per axis", s->body_range);
-        return destroy_fail(HMC_RANGE_TOO_LARGE);
-    }
-    uint64_t cells = 1;
-    for (int a = 0; a < s->dim; ++a) {
-        s->geom.half[a] = s->geom.L[a] / 2.0;
-        s->geom.ghost_hi[a] = s->geom.half[a] - s->boundary_range;
-        s->geom.ghost_lo[a] = -s->geom.half[a] + s->boundary_range;
-        s->geom.w32[a] = (float)s->geom.width[a];
-        s->geom.invL[a] = 1.0 / s->geom.L[a];
-        s->geom.invW[a] = 1.0 / s->geom.width[a];
-        s->geom.half_shape[a] = s->geom.shape[a] / 2;
-        cells *= s->geom.shape[a];
-    }
-    if (cells > 16000000ull) {
-        fail(HMC_NOT_SUPPORTED, "%llu checkerboard spaces exceed the supported 16M", (unsigned long long)cells);
-        return destroy_fail(HMC_NOT_SUPPORTED);
-    }
-    // colour lists pack the multi-index: 10 bits per axis in 3-D, 16 in 2-D
-    for (int a = 0; a < s->dim; ++a) {
-        if (s->geom.shape[a] > (s->dim == 3 ? 1024u : 65535u)) {
-            fail(HMC_NOT_SUPPORTED, "%u spaces on axis %d exceed the supported %u", s->geom.shape[a], a,
-                 s->dim == 3 ? 1024u : 65535u);
-            return destroy_fail(HMC_NOT_SUPPORTED);
-        }
-        if (s->geom.shape[a] == 2) s->geom.any_two = 1;
-    }
-    s->geom.n_cells = (uint32_t)cells;
-    s->geom.color_stride = (uint32_t)(cells >> s->dim);
     if (d->interaction == HMC_HARD_SPHERE) {
         s->pair.sigma2 = d->diameter * d->diameter;  // diameter.powi(2)
-        sphere_bound(s);
     } else if (d->interaction == HMC_HARD_CONVEX_POLYHEDRON || polygon) {
         // circumsphere rejection (convex.rs:162-165): r_cut = R + R, compared with r_cut.powi(2)
         const double rc = bounding_radius + bounding_radius;
         s->poly_rcut2 = rc * rc;
-        s->pair.sigma2 = s->poly_rcut2;  // the FP32 prefilter threshold reuses the sphere bound
-        sphere_bound(s);
-        s->poly_rcut2_hi32 = s->pair.sig2_hi32;
         s->n_vertices = d->n_vertices;
+    } else if (d->interaction == HMC_OVERLAP_PENALTY) {
+        Pair& P = s->pair;
+        P.penalty = 1;
+        P.sigma2 = d->diameter * d->diameter;  // pairs closer than delta overlap (energy > 0)
+        P.op_rcut2 = d->diameter * d->diameter;
+        P.op_delta = d->diameter;
+        P.op_dmax = d->penalty_maximum_overlap;
+        P.op_half_k = 0.5 * d->penalty_k;
+        P.op_shoulder = d->penalty_shoulder;
     } else {
-        lj_setup(s, d->lj_epsilon, d->lj_sigma, d->lj_r_cut, d->lj_r_shift);
+        s->lj_params[0] = d->lj_epsilon;
+        s->lj_params[1] = d->lj_sigma;
+        s->lj_params[2] = d->lj_r_cut;
+        s->lj_params[3] = d->lj_r_shift;
+    }
+    {
+        hmc_status st = setup_geometry(s, d->edge_lengths);
+        if (st) return destroy_fail(st);
     }
     // The hard-sphere colour pass: per lane for FP32 (cheap pair tests), warp-cooperative for
     // FP64 (each pair test costs more than the coordination), as measured on B200;
@@ -526,17 +594,14 @@ hmc_status hmc_system_create(hmc_context* ctx, const hmc_system_desc* d, const d
         return destroy_fail(HMC_CUDA_ERROR);
     }
     uint64_t n = s->n;
+    const uint64_t cap = s->capacity;
     hmc_status st = HMC_OK;
     Arrays& A = s->arr;
-    uint32_t scan_blocks = (uint32_t)((cells + 2047) / 2048);
-    if ((st = dalloc(s, &A.body_pos, n)) || (st = dalloc(s, &A.sorted_b, n)) || (st = dalloc(s, &A.sorted_s, n)) ||
-        (st = dalloc(s, &A.sorted_off, n)) || (st = dalloc(s, &A.sorted_body, n)) ||
-        (st = dalloc(s, &A.slot_of_body, n)) || (st = dalloc(s, &A.body_cell, n)) ||
-        (st = dalloc(s, &A.body_rank, n)) || (st = dalloc(s, &A.body_m, n)) || (st = dalloc(s, &A.cell_count, cells)) ||
-        (st = dalloc(s, &A.cell_start, cells + 1)) || (st = dalloc(s, &A.block_sums, (size_t)scan_blocks * 9)) ||
-        (st = dalloc(s, &A.color_cells, cells)) ||
-        (st = dalloc(s, &A.stats, 1)) || (st = dalloc(s, &s->stage, n * (uint64_t)s->dim)) ||
-        (st = dalloc(s, &s->first_bad, 1)))
+    if ((st = dalloc(s, &A.body_pos, cap)) || (st = dalloc(s, &A.sorted_b, cap)) || (st = dalloc(s, &A.sorted_s, cap)) ||
+        (st = dalloc(s, &A.sorted_off, cap)) || (st = dalloc(s, &A.sorted_body, cap)) ||
+        (st = dalloc(s, &A.slot_of_body, cap)) || (st = dalloc(s, &A.body_cell, cap)) ||
+        (st = dalloc(s, &A.body_rank, cap)) || (st = dalloc(s, &A.body_m, cap)) || (st = dalloc(s, &A.stats, 1)) ||
+        (st = dalloc(s, &s->stage, cap * (uint64_t)s->dim)) || (st = dalloc(s, &s->first_bad, 1)))
         return destroy_fail(st);
     e = cudaMallocHost((void**)&s->host_first_bad, sizeof(unsigned long long));
     if (e != cudaSuccess) {
@@ -547,7 +612,7 @@ hmc_status hmc_system_create(hmc_context* ctx, const hmc_system_desc* d, const d
     A.body_ori = nullptr;
     A.sorted_q = nullptr;
     if (s->oriented()) {
-        if ((st = dalloc(s, &A.body_ori, n)) || (st = dalloc(s, &A.sorted_q, n)) ||
+        if ((st = dalloc(s, &A.body_ori, cap)) || (st = dalloc(s, &A.sorted_q, cap)) ||
             (st = dalloc(s, &s->verts, s->n_vertices)))
             return destroy_fail(st);
         std::vector<double4> hv(s->n_vertices);
@@ -702,7 +767,7 @@ hmc_status hmc_sweep(hmc_system* s, const hmc_sweep_params* p, hmc_count* out) {
     const uint32_t colors = 1u << s->dim;
     for (uint32_t sweep = 0; sweep < p->n_sweeps; ++sweep) {
         if (s->profiling) HMC_CUDA(cudaEventRecord(s->ev[0], s->stream));
-        hmc_status st = rebuild(s, !fp32 || s->oriented());  // shapes read S in both modes
+        hmc_status st = rebuild(s, !fp32 || s->oriented() || s->penalty());  // shapes read S in both modes
         if (st) return st;
         if (s->profiling) HMC_CUDA(cudaEventRecord(s->ev[1], s->stream));
         Launch L{};
@@ -722,8 +787,9 @@ hmc_status hmc_sweep(hmc_system* s, const hmc_sweep_params* p, hmc_count* out) {
                 L.round = r;
                 for (uint32_t c = 0; c < colors; ++c) {
                     L.color = c;
-                    if (s->interaction == HMC_LENNARD_JONES)
-                        HMC_CUDA(launch_sweep_lj(s->dim, fp32, s->geom, s->arr, s->pair, L, s->stream));
+                    if (s->soft())  // the overlap penalty has no FP32 path: FP64 in both modes
+                        HMC_CUDA(launch_sweep_lj(s->dim, fp32 && !s->penalty(), s->geom, s->arr, s->pair, L,
+                                                 s->stream));
                     else if (s->interaction == HMC_HARD_CONVEX_POLYHEDRON)
                         HMC_CUDA(launch_sweep_poly(fp32, s->geom, s->arr, s->verts, s->n_vertices, s->poly_rcut2,
                                                    s->poly_rcut2_hi32, L, p->move == HMC_ROTATE, s->stream));
@@ -805,31 +871,48 @@ hmc_status hmc_math_sincos(hmc_context* ctx, const double* x, uint64_t n, double
 // Sweep::apply_with_filter (hoomd-mc/src/sweep.rs:159-224) for hard spheres: bodies in index
 // order, one sequential stream Counter(step, substep, seed).make_rng(), then
 // increment_substep. move_mask (n bytes, may be NULL) plays should_move_body.
+// The serial grid (cells at least the pair range wide), laid out again when the box changed.
+static hmc_status serial_grid(hmc_system* s) {
+    bool same = s->serial_size != nullptr;
+    for (int a = 0; a < s->dim; ++a) same = same && s->serial_L[a] == s->geom.L[a];
+    if (same) return HMC_OK;
+    dfree(s, &s->serial_size);
+    dfree(s, &s->serial_items);
+    uint64_t cells = 1;
+    for (int a = 0; a < s->dim; ++a) {
+        double f = std::floor(s->geom.L[a] / s->pair_range);
+        s->serial_nc[a] = f >= 1.0 ? (uint32_t)std::min(f, 1024.0) : 1u;
+        s->serial_w[a] = s->geom.L[a] / (double)s->serial_nc[a];
+        s->serial_L[a] = s->geom.L[a];
+        cells *= s->serial_nc[a];
+    }
+    s->serial_cap = (uint32_t)std::min<uint64_t>(4096, 4 * (s->capacity / cells + 1) + 64);
+    hmc_status st;
+    if ((st = dalloc(s, &s->serial_size, cells)) || (st = dalloc(s, &s->serial_items, cells * s->serial_cap)))
+        return st;
+    if (!s->serial_cell_of) {
+        if ((st = dalloc(s, &s->serial_cell_of, s->capacity)) || (st = dalloc(s, &s->serial_site, s->capacity)) ||
+            (st = dalloc(s, &s->serial_mask, s->capacity)))
+            return st;
+    }
+    return HMC_OK;
+}
+
 hmc_status hmc_serial_sweep(hmc_system* s, const hmc_sweep_params* p, const uint8_t* move_mask, hmc_count* out) {
     if (!s || !p) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
     if (p->struct_size < sizeof(hmc_sweep_params)) return fail(HMC_INVALID_ARGUMENT, "hmc_sweep_params.struct_size");
-    if (s->interaction != HMC_HARD_SPHERE) return fail(HMC_NOT_SUPPORTED, "the serial sweep is built for hard spheres");
-    if (p->move != HMC_TRANSLATE) return fail(HMC_NOT_SUPPORTED, "hard spheres take translation moves");
+    if (s->interaction != HMC_HARD_SPHERE && !s->penalty())
+        return fail(HMC_NOT_SUPPORTED, "the serial sweep is built for hard and overlap-penalty spheres");
+    if (p->move != HMC_TRANSLATE) return fail(HMC_NOT_SUPPORTED, "spheres take translation moves");
+    if (!(p->temperature > 0.0)) return fail(HMC_INVALID_ARGUMENT, "temperature must be positive");
     double lmax = 0.0;
     for (int a = 0; a < s->dim; ++a) lmax = std::max(lmax, s->geom.L[a]);
     if (!(p->maximum > 0.0) || !(p->maximum <= 4.0 * lmax))
         return fail(HMC_INVALID_ARGUMENT, "maximum must be in (0, 4 box lengths]");
     HMC_CUDA(cudaSetDevice(s->ctx->device));
-    if (!s->serial_size) {
-        const double sigma = std::sqrt(s->pair.sigma2);
-        uint64_t cells = 1;
-        for (int a = 0; a < s->dim; ++a) {
-            double f = std::floor(s->geom.L[a] / sigma);
-            s->serial_nc[a] = f >= 1.0 ? (uint32_t)std::min(f, 1024.0) : 1u;
-            s->serial_w[a] = s->geom.L[a] / (double)s->serial_nc[a];
-            cells *= s->serial_nc[a];
-        }
-        s->serial_cap = (uint32_t)std::min<uint64_t>(4096, 4 * (s->n / cells + 1) + 16);
-        hmc_status st;
-        if ((st = dalloc(s, &s->serial_size, cells)) || (st = dalloc(s, &s->serial_items, cells * s->serial_cap)) ||
-            (st = dalloc(s, &s->serial_cell_of, s->n)) || (st = dalloc(s, &s->serial_site, s->n)) ||
-            (st = dalloc(s, &s->serial_mask, s->n)))
-            return st;
+    {
+        hmc_status st = serial_grid(s);
+        if (st) return st;
     }
     uint64_t moving = s->n;
     if (move_mask) {
@@ -847,7 +930,8 @@ hmc_status hmc_serial_sweep(hmc_system* s, const hmc_sweep_params* p, const uint
         L.kt = p->temperature;
         L.n_bodies = (uint32_t)s->n;
         HMC_CUDA(cudaMemsetAsync(s->arr.stats, 0, sizeof(DeviceStats), s->stream));
-        HMC_CUDA(launch_serial_sphere(s->dim, s->geom, s->arr, s->pair, L, s->serial_nc, s->serial_w, s->serial_cap,
+        HMC_CUDA(launch_serial_sphere(s->dim, s->penalty(), s->geom, s->arr, s->pair, L, s->serial_nc, s->serial_w,
+                                      s->serial_cap,
                                       s->serial_size, s->serial_items, s->serial_cell_of, s->serial_site,
                                       move_mask ? s->serial_mask : nullptr, s->stream));
         s->prof.kernel_launches += 2;
@@ -924,9 +1008,9 @@ hmc_status hmc_tune(hmc_system* s, hmc_sweep_params* p, double target, uint32_t 
         L.n_bodies = (uint32_t)s->n;
         e = launch_tune_moves(s->dim, s->geom, s->arr, L, step, samples, p->move == HMC_ROTATE, db, dt, dq, du, s->stream);
         if (e != cudaSuccess) break;
-        if (s->interaction == HMC_LENNARD_JONES)
-            e = launch_eval_lj(s->dim, fp32, s->geom, s->arr, s->pair, db, dt, du, p->temperature, samples, dd,
-                               dd + samples, dh, s->stream);
+        if (s->soft())
+            e = launch_eval_lj(s->dim, fp32 && !s->penalty(), s->geom, s->arr, s->pair, db, dt, du, p->temperature,
+                               samples, dd, dd + samples, dh, s->stream);
         else if (s->polygon())
             e = launch_eval_poly2(fp32, s->sat(), s->geom, s->arr, s->verts, s->n_vertices, s->poly_rcut2,
                                   s->poly_rcut2_hi32, db, dt, dq, samples, dd, s->stream);
@@ -960,6 +1044,7 @@ hmc_status hmc_tune(hmc_system* s, hmc_sweep_params* p, double target, uint32_t 
 hmc_status hmc_overlap_check(hmc_system* s, uint64_t* n_overlaps) {
     if (!s || !n_overlaps) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
     if (s->interaction == HMC_LENNARD_JONES) return fail(HMC_NOT_SUPPORTED, "overlap check of a soft potential");
+    // overlap penalty: pairs closer than delta (those with a positive pair energy)
     HMC_CUDA(cudaSetDevice(s->ctx->device));
     hmc_status st = rebuild(s, true);
     if (st) return st;
@@ -1035,7 +1120,7 @@ hmc_status hmc_gr(hmc_system* s, double r_max, uint32_t n_bins, uint64_t* counts
 
 hmc_status hmc_total_energy(hmc_system* s, double* energy) {
     if (!s || !energy) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
-    if (s->interaction != HMC_LENNARD_JONES) {
+    if (!s->soft()) {
         uint64_t n = 0;
         hmc_status st = hmc_overlap_check(s, &n);
         if (st) return st;
@@ -1054,11 +1139,201 @@ hmc_status hmc_total_energy(hmc_system* s, double* energy) {
     return HMC_OK;
 }
 
+hmc_status hmc_get_box(hmc_system* s, double* edge_lengths) {
+    if (!s || !edge_lengths) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
+    for (int a = 0; a < s->dim; ++a) edge_lengths[a] = s->geom.L[a];
+    return HMC_OK;
+}
+
+hmc_status hmc_get_n_bodies(hmc_system* s, uint64_t* n_bodies) {
+    if (!s || !n_bodies) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
+    *n_bodies = s->n;
+    return HMC_OK;
+}
+
+// clone_with_boundary onto the box L: the positions are kept in `backup` (restore_box puts
+// them and the old box back), mapped on the device, and the checkerboard is laid out again.
+static hmc_status restore_box(hmc_system* s, const double* L_old) {
+    if (s->n)
+        HMC_CUDA(cudaMemcpyAsync(s->arr.body_pos, s->backup, sizeof(double4) * s->n, cudaMemcpyDeviceToDevice,
+                                 s->stream));
+    return setup_geometry(s, L_old);
+}
+
+static hmc_status map_into_box(hmc_system* s, const double* L) {
+    double L_old[3] = {s->geom.L[0], s->geom.L[1], s->geom.L[2]};
+    if (!s->backup) {
+        hmc_status st = dalloc(s, &s->backup, s->capacity);
+        if (st) return st;
+    }
+    if (s->n)
+        HMC_CUDA(cudaMemcpyAsync(s->backup, s->arr.body_pos, sizeof(double4) * s->n, cudaMemcpyDeviceToDevice,
+                                 s->stream));
+    double old_half[3] = {0, 0, 0}, scale[3] = {1, 1, 1}, lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+    for (int a = 0; a < s->dim; ++a) {
+        old_half[a] = L_old[a] / 2.0;
+        scale[a] = L[a] / L_old[a];
+        lo[a] = -L[a] / 2.0;
+        hi[a] = std::nextafter(L[a] / 2.0, -INFINITY);  // f64::next_down
+    }
+    hmc_status st = setup_geometry(s, L);
+    if (st) return st;
+    const unsigned long long none = ~0ull;
+    HMC_CUDA(cudaMemcpyAsync(s->first_bad, &none, sizeof(none), cudaMemcpyHostToDevice, s->stream));
+    HMC_CUDA(launch_map_bodies(s->dim, s->geom, old_half, scale, lo, hi, s->arr.body_pos, s->n, s->first_bad,
+                               s->stream));
+    s->prof.kernel_launches += 1;
+    HMC_CUDA(cudaMemcpyAsync(s->host_first_bad, s->first_bad, sizeof(none), cudaMemcpyDeviceToHost, s->stream));
+    HMC_CUDA(cudaStreamSynchronize(s->stream));
+    if (*s->host_first_bad != none) {
+        const unsigned long long bad = *s->host_first_bad;
+        restore_box(s, L_old);
+        return fail(HMC_INVALID_ARGUMENT, "body %llu is outside the box (map_point)", bad);
+    }
+    return HMC_OK;
+}
+
+hmc_status hmc_set_box(hmc_system* s, const double* edge_lengths) {
+    if (!s || !edge_lengths) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
+    HMC_CUDA(cudaSetDevice(s->ctx->device));
+    return map_into_box(s, edge_lengths);
+}
+
+hmc_status hmc_quick_insert_apply(hmc_system* s, hmc_quick_insert* qi, hmc_count* out) {
+    if (!s || !qi) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
+    if (s->interaction != HMC_HARD_SPHERE && !s->penalty())
+        return fail(HMC_NOT_SUPPORTED, "QuickInsert places hard or overlap-penalty spheres");
+    if (qi->allowed_overlaps == 0) return fail(HMC_INVALID_ARGUMENT, "allowed_overlaps must be >= 1");
+    if (qi->inserted > qi->target) return fail(HMC_INVALID_ARGUMENT, "inserted exceeds target");
+    if (s->n + (qi->target - qi->inserted) > s->capacity)
+        return fail(HMC_INVALID_ARGUMENT, "the system holds %llu bodies; %llu more do not fit",
+                    (unsigned long long)s->capacity, (unsigned long long)(qi->target - qi->inserted));
+    hmc_count count{};
+    if (out) *out = count;
+    if (qi->complete) return HMC_OK;
+    HMC_CUDA(cudaSetDevice(s->ctx->device));
+    double energy = 0.0;
+    hmc_status st = hmc_total_energy(s, &energy);
+    if (st) return st;
+    if (energy <= 0.0 && qi->inserted >= qi->target) {
+        qi->complete = 1;
+        return HMC_OK;
+    }
+    if (energy <= 0.0) {
+        if ((st = serial_grid(s))) return st;
+        if (!s->qi_out && (st = dalloc(s, &s->qi_out, 4))) return st;
+        Launch L{};
+        L.step = s->step;
+        L.substep = s->substep;
+        L.seed = s->seed;
+        L.n_bodies = (uint32_t)s->n;
+        QuickInsertArgs q{};
+        q.n0 = (uint32_t)s->n;
+        q.capacity = (uint32_t)s->capacity;
+        q.attempts = qi->target;
+        q.to_insert = qi->target - qi->inserted;
+        q.allowed = qi->allowed_overlaps;
+        q.soft = s->penalty() ? 1u : 0u;
+        for (int a = 0; a < 3; ++a) {
+            // Uniform::new(minimal, maximal extent): low = -L/2, scale = L/2 - (-L/2)
+            const double low = a < s->dim ? -s->geom.L[a] / 2.0 : 0.0, high = a < s->dim ? s->geom.L[a] / 2.0 : 0.0;
+            q.low[a] = low;
+            q.scale[a] = high - low;
+        }
+        HMC_CUDA(cudaMemsetAsync(s->arr.stats, 0, sizeof(DeviceStats), s->stream));
+        HMC_CUDA(launch_quick_insert(s->dim, s->geom, s->arr, s->pair, L, q, s->serial_nc, s->serial_w, s->serial_cap,
+                                     s->serial_size, s->serial_items, s->serial_cell_of, s->serial_site, s->qi_out,
+                                     s->stream));
+        s->prof.kernel_launches += 2;
+        unsigned long long r[4] = {0, 0, 0, 0};
+        HMC_CUDA(cudaMemcpyAsync(r, s->qi_out, sizeof(r), cudaMemcpyDeviceToHost, s->stream));
+        if ((st = read_stats(s))) return st;
+        if ((st = check_flags(s))) return st;
+        s->n = r[3];
+        qi->inserted += r[0];
+        count.accepted = r[0];
+        count.rejected = r[2];
+    }
+    s->substep += 1;  // increment_substep (quick_insert.rs:278)
+    if (out) *out = count;
+    return HMC_OK;
+}
+
+hmc_status hmc_quick_compress_apply(hmc_system* s, hmc_quick_compress* qc) {
+    if (!s || !qc) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
+    if (!(qc->target_volume > 0.0) || !std::isfinite(qc->target_volume))
+        return fail(HMC_INVALID_ARGUMENT, "target volume must be positive");
+    if (!(qc->maximum_delta > 0.0 && qc->maximum_delta < 1.0))
+        return fail(HMC_INVALID_ARGUMENT, "maximum_delta must be in (0, 1)");
+    if (qc->state > HMC_QC_COMPLETE) return fail(HMC_INVALID_ARGUMENT, "state");
+    HMC_CUDA(cudaSetDevice(s->ctx->device));
+    Sfc64 rng = make_rng(s->step, s->substep, s->seed, 0);  // microstate.counter().make_rng()
+    s->substep += 1;
+    double L[3] = {s->geom.L[0], s->geom.L[1], s->geom.L[2]};
+    auto same_box = [&](const double* b) {
+        for (int a = 0; a < s->dim; ++a)
+            if (b[a] != L[a]) return false;
+        return true;
+    };
+    auto wait_on = [&](bool is_final, const double* b) {
+        qc->state = HMC_QC_WAITING;
+        qc->is_final = is_final ? 1u : 0u;
+        for (int a = 0; a < 3; ++a) qc->boundary[a] = a < s->dim ? b[a] : 0.0;
+    };
+    hmc_status st = HMC_OK;
+    switch (qc->state) {
+        case HMC_QC_STARTUP:
+            wait_on(false, L);
+            break;
+        case HMC_QC_COMPLETE:
+            if (!same_box(qc->boundary)) wait_on(false, L);
+            break;
+        case HMC_QC_COMPRESSING: {
+            // Uniform::new(0.0, maximum_delta).sample(rng)
+            const double u = as_double(0x3FF0000000000000ULL | (rng.next_u64() >> 12)) - 1.0;
+            const double delta = u * (qc->maximum_delta - 0.0) + 0.0;
+            double volume = L[0];
+            for (int a = 1; a < s->dim; ++a) volume = volume * L[a];  // Hypercuboid::volume
+            const double trial_volume = qc->target_volume > volume ? std::min(volume * (1.0 + delta), qc->target_volume)
+                                                                   : std::max(volume * (1.0 - delta), qc->target_volume);
+            // scale_volume: edge lengths times (V'/V)^(1/N) (cuboid.rs:483-517)
+            const double v = std::pow(trial_volume / volume, 1.0 / (double)s->dim);
+            double L_new[3] = {L[0], L[1], L[2]};
+            for (int a = 0; a < s->dim; ++a) L_new[a] = L[a] * v;
+            double e0 = 0.0, e1 = 0.0;
+            if ((st = hmc_total_energy(s, &e0))) return st;
+            if ((st = map_into_box(s, L_new))) return st;
+            if ((st = hmc_total_energy(s, &e1))) return st;
+            const double delta_energy = e1 - e0;  // delta_energy_total
+            if (delta_energy > qc->maximum_energy_per_site * (double)s->n) {
+                if ((st = restore_box(s, L))) return st;  // too strained: stay Compressing
+            } else {
+                wait_on(trial_volume == qc->target_volume, L_new);
+            }
+            break;
+        }
+        case HMC_QC_WAITING: {
+            double e = 0.0;
+            if ((st = hmc_total_energy(s, &e))) return st;
+            if (e <= 0.0) {
+                if (qc->is_final && same_box(qc->boundary)) {
+                    qc->state = HMC_QC_COMPLETE;
+                    for (int a = 0; a < 3; ++a) qc->boundary[a] = a < s->dim ? L[a] : 0.0;
+                } else {
+                    qc->state = HMC_QC_COMPRESSING;
+                }
+            }
+            break;
+        }
+    }
+    return HMC_OK;
+}
+
 hmc_status hmc_eval_moves(hmc_system* s, const hmc_injected_move* moves, uint64_t n, double temperature,
                           uint32_t precision, uint8_t* decisions, uint8_t* rechecked, double* delta_h) {
     if (!s || (n && (!moves || !decisions))) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
     if (precision > HMC_FP32_RECHECK) return fail(HMC_INVALID_ARGUMENT, "precision");
-    if (s->interaction == HMC_LENNARD_JONES && !(temperature > 0.0))
+    if (s->soft() && !(temperature > 0.0))
         return fail(HMC_INVALID_ARGUMENT, "temperature must be positive");
     if (n == 0) return HMC_OK;
     if (n >= (1ull << 31)) return fail(HMC_INVALID_ARGUMENT, "too many moves");
@@ -1080,7 +1355,7 @@ hmc_status hmc_eval_moves(hmc_system* s, const hmc_injected_move* moves, uint64_
         hq[i] = make_double4(moves[i].orientation[0], moves[i].orientation[1], moves[i].orientation[2],
                              moves[i].orientation[3]);
     }
-    const bool lj = s->interaction == HMC_LENNARD_JONES;
+    const bool lj = s->soft();
     uint64_t* db = nullptr;
     double4* dt = nullptr;
     double* du = nullptr;
@@ -1102,7 +1377,7 @@ hmc_status hmc_eval_moves(hmc_system* s, const hmc_injected_move* moves, uint64_
     if (e == cudaSuccess) e = cudaMemsetAsync(dh, 0, sizeof(double) * n, s->stream);
     if (e == cudaSuccess) {
         if (lj)
-            e = launch_eval_lj(s->dim, precision == HMC_FP32_RECHECK, s->geom, s->arr, s->pair, db, dt, du, temperature,
+            e = launch_eval_lj(s->dim, precision == HMC_FP32_RECHECK && !s->penalty(), s->geom, s->arr, s->pair, db, dt, du, temperature,
                                (uint32_t)n, dd, dd + n, dh, s->stream);
         else if (s->polygon())
             e = launch_eval_poly2(precision == HMC_FP32_RECHECK, s->sat(), s->geom, s->arr, s->verts, s->n_vertices,

@@ -88,7 +88,24 @@ struct Pair {
     float lj_rcut2_hi32;  // r_cut^2 plus the bound: at or above, outside for certain
     float lj_disp_err;    // per-axis FP32 displacement error bound E
     float lj_band_energy; // bound on |pair energy| for a pair inside the cut-off band
+    // Isotropic<Expanded<OverlapPenalty>> (overlap_penalty.rs:109-115, expanded.rs:64-66):
+    // r^2 >= r_cut^2 -> 0; x = sqrt(r^2) - delta; x < -d_max -> inf; x < 0 -> (0.5 k) x^2 + eps
+    uint32_t penalty;     // 1: the soft pair energy is the overlap penalty, else Lennard-Jones
+    double op_rcut2;      // r_cut.powi(2)
+    double op_delta;
+    double op_dmax;       // maximum_allowed_overlap
+    double op_half_k;     // 0.5 * k
+    double op_shoulder;   // epsilon_shoulder
 };
+
+// The overlap penalty's pair energy in FP64 with the reference's operation order.
+__device__ __forceinline__ double penalty_pair64(const Pair& P, double r2) {
+    if (r2 >= P.op_rcut2) return 0.0;
+    const double x = dsub(dsqrt(r2), P.op_delta);
+    if (x < -P.op_dmax) return __longlong_as_double(0x7ff0000000000000ll);
+    if (x < 0.0) return dadd(dmul(P.op_half_k, dmul(x, x)), P.op_shoulder);
+    return 0.0;
+}
 
 // One sweep launch: counter, move and colour.
 struct Launch {
@@ -191,11 +208,34 @@ cudaError_t launch_pack_angles(const double4* body_ori, double* packed, uint64_t
 cudaError_t launch_pair_histogram(int dim, bool sdf, const Geometry& g, const Arrays& a, uint32_t n, double sigma,
                                   double limit, double inv_width, uint32_t n_bins, unsigned long long* counts,
                                   cudaStream_t s);
-// Sweep::apply_with_filter for hard spheres (hmc_serial.cu): one warp, one sequential stream.
-// nc/w: the serial grid (cells per axis, widths); mask (may be null): bodies to move.
-cudaError_t launch_serial_sphere(int dim, const Geometry& g, const Arrays& a, const Pair& p, const Launch& l,
-                                 const uint32_t* nc, const double* w, uint32_t cap, uint32_t* size, uint32_t* items,
-                                 uint32_t* cell_of, double4* site, const uint8_t* mask, cudaStream_t s);
+// Sweep::apply_with_filter for hard (soft = false) or overlap-penalty spheres (hmc_serial.cu):
+// one warp, one sequential stream. nc/w: the serial grid (cells per axis, widths); mask (may be
+// null): bodies to move.
+cudaError_t launch_serial_sphere(int dim, bool soft, const Geometry& g, const Arrays& a, const Pair& p,
+                                 const Launch& l, const uint32_t* nc, const double* w, uint32_t cap, uint32_t* size,
+                                 uint32_t* items, uint32_t* cell_of, double4* site, const uint8_t* mask,
+                                 cudaStream_t s);
+// QuickInsert's insertion loop on the serial grid (one warp): bodies appended from index n0.
+struct QuickInsertArgs {
+    uint32_t n0;         // bodies before the call
+    uint32_t capacity;   // bodies the arrays hold
+    uint64_t attempts;   // draws at most (QuickInsert::target)
+    uint64_t to_insert;  // target - inserted
+    uint64_t allowed;    // allowed_overlaps
+    double low[3];       // Uniform low per axis (-L/2)
+    double scale[3];     // Uniform scale per axis
+    uint32_t soft;       // 1: overlap penalty, 0: hard spheres
+};
+cudaError_t launch_quick_insert(int dim, const Geometry& g, const Arrays& a, const Pair& p, const Launch& l,
+                                const QuickInsertArgs& q, const uint32_t* nc, const double* w, uint32_t cap,
+                                uint32_t* size, uint32_t* items, uint32_t* cell_of, double4* site,
+                                unsigned long long* out, cudaStream_t s);
+// Clone with boundary (hmc_set_box): every body x -> clamp(scale x, lo, hi) per axis, then
+// B = wrap(.) in the new box; first_outside receives the smallest body index that is not
+// inside the old box (the reference's map_point fails there).
+cudaError_t launch_map_bodies(int dim, const Geometry& g_new, const double* old_half, const double* scale,
+                              const double* lo, const double* hi, double4* body_pos, uint64_t n,
+                              unsigned long long* first_outside, cudaStream_t s);
 // State transfer through a packed staging array of n x dim doubles (the host layout):
 // first_nonfinite receives the smallest body index with a non-finite coordinate (it must hold
 // ~0 before the launch); unpack writes body positions, pack reads them.

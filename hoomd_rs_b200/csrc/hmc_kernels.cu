@@ -1052,6 +1052,37 @@ __global__ void k_gsd_encode(Geometry g, const double4* __restrict__ body_pos, c
     }
 }
 
+// Microstate::clone_with_boundary (hoomd-microstate/src/microstate.rs:1529-1565) for a
+// periodic hypercuboid: Hypercuboid::map_point (hoomd-geometry/src/shape/cuboid.rs:553-565)
+// checks -L/2 <= x < L/2 in the old box, scales by L'/L and clamps to [-L'/2, next_down(L'/2)];
+// update_body_properties then keeps B = wrap(.) in the new box.
+template <int DIM>
+__global__ void k_map_bodies(Geometry g, double3 old_half, double3 scale, double3 lo, double3 hi,
+                             double4* __restrict__ body_pos, uint64_t n, unsigned long long* first_outside) {
+    const double oh[3] = {old_half.x, old_half.y, old_half.z}, sc[3] = {scale.x, scale.y, scale.z};
+    const double l[3] = {lo.x, lo.y, lo.z}, h[3] = {hi.x, hi.y, hi.z};
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const double4 b = body_pos[i];
+        double x[3] = {b.x, b.y, b.z};
+        bool inside = true;
+#pragma unroll
+        for (int a = 0; a < DIM; ++a) inside = inside && -oh[a] <= x[a] && x[a] < oh[a];
+        if (!inside) {
+            atomicMin(first_outside, (unsigned long long)i);
+            continue;
+        }
+#pragma unroll
+        for (int a = 0; a < DIM; ++a) {
+            double y = dmul(sc[a], x[a]);
+            if (y < l[a]) y = l[a];  // f64::clamp
+            if (y > h[a]) y = h[a];
+            x[a] = y;
+        }
+        wrap_inv<DIM>(g.L, g.invL, x);
+        body_pos[i] = make_double4(x[0], x[1], DIM == 3 ? x[2] : 0.0, 0.0);
+    }
+}
+
 inline uint32_t stream_grid(uint64_t n) {
     uint64_t b = (n + 255) / 256;
     return (uint32_t)(b < 148ull * 16 ? (b ? b : 1) : 148ull * 16);
@@ -1099,6 +1130,20 @@ cudaError_t launch_unpack_angles(const double* packed, double4* body_ori, uint64
 cudaError_t launch_pack_angles(const double4* body_ori, double* packed, uint64_t n, cudaStream_t s) {
     if (n == 0) return cudaSuccess;
     k_pack_angles<<<stream_grid(n), 256, 0, s>>>(body_ori, packed, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_map_bodies(int dim, const Geometry& g_new, const double* old_half, const double* scale,
+                              const double* lo, const double* hi, double4* body_pos, uint64_t n,
+                              unsigned long long* first_outside, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    const double3 oh = make_double3(old_half[0], old_half[1], old_half[2]);
+    const double3 sc = make_double3(scale[0], scale[1], scale[2]);
+    const double3 l = make_double3(lo[0], lo[1], lo[2]), h = make_double3(hi[0], hi[1], hi[2]);
+    if (dim == 2)
+        k_map_bodies<2><<<stream_grid(n), 256, 0, s>>>(g_new, oh, sc, l, h, body_pos, n, first_outside);
+    else
+        k_map_bodies<3><<<stream_grid(n), 256, 0, s>>>(g_new, oh, sc, l, h, body_pos, n, first_outside);
     return cudaGetLastError();
 }
 

@@ -27,6 +27,7 @@ constexpr float kU32 = 5.9604645e-8f;  // 2^-24
 // (shifted.rs:92-94: f(r) - f(r_shift)), LennardJones::energy (lennard_jones.rs:107-111:
 // 4 eps ((sigma/r)^12 - (sigma/r)^6) with powi by repeated squaring).
 __device__ __forceinline__ double lj_pair64(const Pair& P, double r2) {
+    if (P.penalty) return penalty_pair64(P, r2);
     if (r2 >= P.lj_rcut2) return 0.0;
     const double r = dsqrt(r2);
     const double sr = ddiv(P.lj_sigma, r);

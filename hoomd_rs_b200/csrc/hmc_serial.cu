@@ -1,4 +1,5 @@
-// Sweep::apply_with_filter (hoomd-mc/src/sweep.rs:159-224) for hard disks and spheres: one
+// Sweep::apply_with_filter (hoomd-mc/src/sweep.rs:159-224) for hard and overlap-penalty disks
+// and spheres, and QuickInsert's insertion loop: one
 // trial per body in index order, all from ONE sequential random stream
 // Counter(step, substep, seed).make_rng() (index 0), each trial seeing every earlier accepted
 // move. The chain is sequential by definition, so one warp runs it: the 32 lanes keep the same
@@ -60,23 +61,83 @@ __global__ void k_serial_build(Geometry g, Arrays A, SerialGrid G, uint32_t n) {
         atomicOr(&A.stats->error_flags, kErrCellOverflow);
 }
 
+// This lane's stencil cell around multi-index m (radix decomposition over the distinct cells of
+// each axis); false when the lane has none.
 template <int DIM>
-__global__ void __launch_bounds__(32) k_serial_sphere(Geometry g, Arrays A, SerialGrid G, Pair P, Launch L,
-                                                      const uint8_t* __restrict__ mask) {
-    const uint32_t lane = threadIdx.x;
-    if (A.stats->error_flags) return;
-    Sfc64 rng = make_rng(L.step, L.substep, L.seed, 0);
-    // this lane's stencil cell: radix decomposition over the distinct cells of each axis
-    uint32_t len[3] = {1, 1, 1};
+__device__ __forceinline__ bool lane_cell(const SerialGrid& G, const uint32_t* m, uint32_t lane, uint32_t* cell) {
+    uint32_t len[3] = {1, 1, 1}, off[3] = {0, 0, 0}, rem = lane;
 #pragma unroll
     for (int a = 0; a < DIM; ++a) len[a] = G.nc[a] >= 3 ? 3u : G.nc[a];
-    uint32_t off[3] = {0, 0, 0}, rem = lane;
 #pragma unroll
     for (int a = DIM - 1; a >= 0; --a) {
         off[a] = rem % len[a];
         rem /= len[a];
     }
-    const bool lane_used = rem == 0;  // lane < prod(len)
+    uint32_t c[3] = {0, 0, 0};
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) c[a] = G.nc[a] >= 3 ? wrap_index((int)m[a] + (int)off[a] - 1, G.nc[a]) : off[a];
+    *cell = serial_index<DIM>(G, c);
+    return rem == 0;
+}
+
+// Soft pair energy of site t against every site of the stencil around t's cell except body
+// `self`: per-lane sums over the lane's cell, then a butterfly reduction (all lanes agree).
+template <int DIM>
+__device__ __forceinline__ double serial_energy(const Geometry& g, const SerialGrid& G, const Pair& P, const double* t,
+                                                uint32_t self, uint32_t lane) {
+    uint32_t m[3] = {0, 0, 0}, cell;
+    serial_cell<DIM>(g, G, t, m);
+    double e = 0.0;
+    if (lane_cell<DIM>(G, m, lane, &cell)) {
+        const uint32_t cnt = G.size[cell];
+        for (uint32_t k = 0; k < cnt; ++k) {
+            const uint32_t j = G.items[(size_t)cell * G.cap + k];
+            if (j == self) continue;
+            const double4 s4 = G.site[j];
+            const double sv[3] = {s4.x, s4.y, s4.z};
+            e = dadd(e, penalty_pair64(P, ref_dist2<DIM>(g, t, sv)));
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) e = dadd(e, __shfl_xor_sync(0xffffffffu, e, o));
+    return e;
+}
+
+// Move body b's site into the cell of sv (lane 0 only): the last item of the old cell takes
+// b's slot there (swap_remove), b is appended to the new cell.
+template <int DIM>
+__device__ __forceinline__ void serial_move(const Geometry& g, const SerialGrid& G, const Arrays& A, uint32_t b,
+                                            const double* sv) {
+    uint32_t ms[3] = {0, 0, 0};
+    serial_cell<DIM>(g, G, sv, ms);
+    const uint32_t nc = serial_index<DIM>(G, ms), oc = G.cell_of[b];
+    if (nc == oc) return;
+    const uint32_t osz = G.size[oc];
+    for (uint32_t k = 0; k < osz; ++k)
+        if (G.items[(size_t)oc * G.cap + k] == b) {
+            G.items[(size_t)oc * G.cap + k] = G.items[(size_t)oc * G.cap + osz - 1];
+            break;
+        }
+    G.size[oc] = osz - 1;
+    const uint32_t nsz = G.size[nc];
+    if (nsz < G.cap) {
+        G.items[(size_t)nc * G.cap + nsz] = b;
+        G.size[nc] = nsz + 1;
+    } else {
+        atomicOr(&A.stats->error_flags, kErrCellOverflow);
+    }
+    G.cell_of[b] = nc;
+}
+
+// SOFT = false: hard spheres (the trial is rejected on any overlap, no uniform is drawn).
+// SOFT = true: the overlap penalty; dH = E(trial site) - E(current site) and the Metropolis
+// test of sweep.rs:207-209 (u drawn from the stream only when 0 < dH < inf).
+template <int DIM, bool SOFT>
+__global__ void __launch_bounds__(32) k_serial_sphere(Geometry g, Arrays A, SerialGrid G, Pair P, Launch L,
+                                                      const uint8_t* __restrict__ mask) {
+    const uint32_t lane = threadIdx.x;
+    if (A.stats->error_flags) return;
+    Sfc64 rng = make_rng(L.step, L.substep, L.seed, 0);
     uint64_t accepted = 0;
     for (uint32_t b = 0; b < L.n_bodies; ++b) {
         if (mask && !mask[b]) continue;
@@ -89,25 +150,31 @@ __global__ void __launch_bounds__(32) k_serial_sphere(Geometry g, Arrays A, Seri
         wrap_inv<DIM>(g.L, g.invL, x);  // wrap(propose(..)) = W1
         double t[3] = {x[0], x[1], DIM == 3 ? x[2] : 0.0};
         wrap_inv<DIM>(g.L, g.invL, t);  // delta_energy_one wraps the site: T = wrap(W1)
-        uint32_t m[3] = {0, 0, 0};
-        serial_cell<DIM>(g, G, t, m);
-        bool overlap = false;
-        if (lane_used) {
-            uint32_t c[3] = {0, 0, 0};
-#pragma unroll
-            for (int a = 0; a < DIM; ++a)
-                c[a] = G.nc[a] >= 3 ? wrap_index((int)m[a] + (int)off[a] - 1, G.nc[a]) : off[a];
-            const uint32_t cell = serial_index<DIM>(G, c);
-            const uint32_t cnt = G.size[cell];
-            for (uint32_t k = 0; k < cnt && !overlap; ++k) {
-                const uint32_t j = G.items[(size_t)cell * G.cap + k];
-                if (j == b) continue;
-                const double4 s4 = G.site[j];
-                const double sv[3] = {s4.x, s4.y, s4.z};
-                overlap = ref_dist2<DIM>(g, t, sv) < P.sigma2;
+        if (SOFT) {
+            const double ef = serial_energy<DIM>(g, G, P, t, b, lane);
+            if (ef == __longlong_as_double(0x7ff0000000000000ll)) continue;  // early infinity
+            const double4 s4 = G.site[b];
+            const double si[3] = {s4.x, s4.y, s4.z};
+            const double dh = dsub(ef, serial_energy<DIM>(g, G, P, si, b, lane));
+            if (!(dh != __longlong_as_double(0x7ff0000000000000ll) &&
+                  (dh <= 0.0 || uniform01(rng) < exp(ddiv(-dh, L.kt)))))
+                continue;
+        } else {
+            uint32_t m[3] = {0, 0, 0}, cell;
+            serial_cell<DIM>(g, G, t, m);
+            bool overlap = false;
+            if (lane_cell<DIM>(G, m, lane, &cell)) {
+                const uint32_t cnt = G.size[cell];
+                for (uint32_t k = 0; k < cnt && !overlap; ++k) {
+                    const uint32_t j = G.items[(size_t)cell * G.cap + k];
+                    if (j == b) continue;
+                    const double4 s4 = G.site[j];
+                    const double sv[3] = {s4.x, s4.y, s4.z};
+                    overlap = ref_dist2<DIM>(g, t, sv) < P.sigma2;
+                }
             }
+            if (__any_sync(0xffffffffu, overlap)) continue;
         }
-        if (__any_sync(0xffffffffu, overlap)) continue;
         accepted++;
         if (lane == 0) {
             // update_body_properties: body = wrap(W1) = T, site = wrap(body)
@@ -115,27 +182,7 @@ __global__ void __launch_bounds__(32) k_serial_sphere(Geometry g, Arrays A, Seri
             wrap_inv<DIM>(g.L, g.invL, sv);
             A.body_pos[b] = make_double4(t[0], t[1], t[2], 0.0);
             G.site[b] = make_double4(sv[0], sv[1], sv[2], 0.0);
-            uint32_t ms[3] = {0, 0, 0};
-            serial_cell<DIM>(g, G, sv, ms);
-            const uint32_t nc = serial_index<DIM>(G, ms), oc = G.cell_of[b];
-            if (nc != oc) {
-                // remove b from its old cell (last item takes its slot), append to the new one
-                const uint32_t osz = G.size[oc];
-                for (uint32_t k = 0; k < osz; ++k)
-                    if (G.items[(size_t)oc * G.cap + k] == b) {
-                        G.items[(size_t)oc * G.cap + k] = G.items[(size_t)oc * G.cap + osz - 1];
-                        break;
-                    }
-                G.size[oc] = osz - 1;
-                const uint32_t nsz = G.size[nc];
-                if (nsz < G.cap) {
-                    G.items[(size_t)nc * G.cap + nsz] = b;
-                    G.size[nc] = nsz + 1;
-                } else {
-                    atomicOr(&A.stats->error_flags, kErrCellOverflow);
-                }
-                G.cell_of[b] = nc;
-            }
+            serial_move<DIM>(g, G, A, b, sv);
         }
         __syncwarp();
         if (A.stats->error_flags) break;
@@ -146,11 +193,99 @@ __global__ void __launch_bounds__(32) k_serial_sphere(Geometry g, Arrays A, Seri
     }
 }
 
+// QuickInsert::apply's insertion loop (hoomd-mc/src/quick_insert.rs:243-265): up to `attempts`
+// bodies drawn from UniformIn (per axis Uniform(low, low + scale), rand's UniformFloat: 52 bits
+// in [1, 2) minus 1, times scale, plus low) from one stream; a body whose insertion energy is
+// finite is appended (Microstate::add_body: B = wrap(x), S = wrap(B)); the loop stops once
+// `to_insert` bodies are in or `allowed` inserted bodies overlapped (energy > 0). The insertion
+// energy is evaluated at wrap(x) (filtered_body_energy_final, pairwise_cutoff.rs:420-450); only
+// whether it is infinite or positive matters, and with non-negative pair energies both follow
+// from single pairs, so no sum is formed. out: inserted, overlapping, rejected, final n.
+template <int DIM>
+__global__ void __launch_bounds__(32) k_quick_insert(Geometry g, Arrays A, SerialGrid G, Pair P, Launch L,
+                                                     QuickInsertArgs q, unsigned long long* out) {
+    const uint32_t lane = threadIdx.x;
+    if (A.stats->error_flags) return;
+    Sfc64 rng = make_rng(L.step, L.substep, L.seed, 0);
+    uint32_t n = q.n0;
+    uint64_t inserted = 0, overlapping = 0, rejected = 0;
+    for (uint64_t attempt = 0; attempt < q.attempts; ++attempt) {
+        double x[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int a = 0; a < DIM; ++a) {
+            const double u = dsub(as_double(0x3FF0000000000000ULL | (rng.next_u64() >> 12)), 1.0);
+            x[a] = dadd(dmul(u, q.scale[a]), q.low[a]);
+        }
+        double t[3] = {x[0], x[1], x[2]};
+        wrap_inv<DIM>(g.L, g.invL, t);
+        uint32_t m[3] = {0, 0, 0}, cell;
+        serial_cell<DIM>(g, G, t, m);
+        bool inf = false, pos = false;
+        if (lane_cell<DIM>(G, m, lane, &cell)) {
+            const uint32_t cnt = G.size[cell];
+            for (uint32_t k = 0; k < cnt && !inf; ++k) {
+                const uint32_t j = G.items[(size_t)cell * G.cap + k];
+                const double4 s4 = G.site[j];
+                const double sv[3] = {s4.x, s4.y, s4.z};
+                const double r2 = ref_dist2<DIM>(g, t, sv);
+                if (q.soft) {
+                    const double e = penalty_pair64(P, r2);
+                    inf = e == __longlong_as_double(0x7ff0000000000000ll);
+                    pos = pos || e > 0.0;
+                } else {
+                    inf = r2 < P.sigma2;
+                }
+            }
+        }
+        inf = __any_sync(0xffffffffu, inf);
+        pos = __any_sync(0xffffffffu, pos);
+        if (inf) {
+            rejected++;
+            continue;
+        }
+        if (n >= q.capacity) {
+            if (lane == 0) atomicOr(&A.stats->error_flags, kErrCellOverflow);
+            break;
+        }
+        if (lane == 0) {
+            double b[3] = {x[0], x[1], x[2]};
+            wrap_inv<DIM>(g.L, g.invL, b);
+            double sv[3] = {b[0], b[1], b[2]};
+            wrap_inv<DIM>(g.L, g.invL, sv);
+            A.body_pos[n] = make_double4(b[0], b[1], DIM == 3 ? b[2] : 0.0, 0.0);
+            G.site[n] = make_double4(sv[0], sv[1], DIM == 3 ? sv[2] : 0.0, 0.0);
+            uint32_t ms[3] = {0, 0, 0};
+            serial_cell<DIM>(g, G, sv, ms);
+            const uint32_t c = serial_index<DIM>(G, ms);
+            const uint32_t sz = G.size[c];
+            if (sz < G.cap) {
+                G.items[(size_t)c * G.cap + sz] = n;
+                G.size[c] = sz + 1;
+            } else {
+                atomicOr(&A.stats->error_flags, kErrCellOverflow);
+            }
+            G.cell_of[n] = c;
+        }
+        __syncwarp();
+        n++;
+        inserted++;
+        if (pos) overlapping++;
+        if (inserted == q.to_insert || overlapping >= q.allowed) break;
+        if (A.stats->error_flags) break;
+    }
+    if (lane == 0) {
+        out[0] = inserted;
+        out[1] = overlapping;
+        out[2] = rejected;
+        out[3] = n;
+    }
+}
+
 }  // namespace
 
-cudaError_t launch_serial_sphere(int dim, const Geometry& g, const Arrays& a, const Pair& p, const Launch& l,
-                                 const uint32_t* nc, const double* w, uint32_t cap, uint32_t* size, uint32_t* items,
-                                 uint32_t* cell_of, double4* site, const uint8_t* mask, cudaStream_t s) {
+namespace {
+SerialGrid make_grid(int dim, const uint32_t* nc, const double* w, uint32_t cap, uint32_t* size, uint32_t* items,
+                     uint32_t* cell_of, double4* site) {
     SerialGrid G{};
     uint64_t cells = 1;
     for (int k = 0; k < 3; ++k) {
@@ -164,17 +299,53 @@ cudaError_t launch_serial_sphere(int dim, const Geometry& g, const Arrays& a, co
     G.items = items;
     G.cell_of = cell_of;
     G.site = site;
-    cudaError_t e = cudaMemsetAsync(size, 0, sizeof(uint32_t) * cells, s);
-    if (e != cudaSuccess) return e;
-    const uint32_t n = l.n_bodies;
-    if (n == 0) return cudaSuccess;
-    if (dim == 2) {
+    return G;
+}
+
+cudaError_t build_grid(int dim, const Geometry& g, const Arrays& a, const SerialGrid& G, uint32_t n, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(G.size, 0, sizeof(uint32_t) * G.n_cells, s);
+    if (e != cudaSuccess || n == 0) return e;
+    if (dim == 2)
         k_serial_build<2><<<(n + 255) / 256, 256, 0, s>>>(g, a, G, n);
-        k_serial_sphere<2><<<1, 32, 0, s>>>(g, a, G, p, l, mask);
-    } else {
+    else
         k_serial_build<3><<<(n + 255) / 256, 256, 0, s>>>(g, a, G, n);
-        k_serial_sphere<3><<<1, 32, 0, s>>>(g, a, G, p, l, mask);
+    return cudaGetLastError();
+}
+}  // namespace
+
+cudaError_t launch_serial_sphere(int dim, bool soft, const Geometry& g, const Arrays& a, const Pair& p,
+                                 const Launch& l, const uint32_t* nc, const double* w, uint32_t cap, uint32_t* size,
+                                 uint32_t* items, uint32_t* cell_of, double4* site, const uint8_t* mask,
+                                 cudaStream_t s) {
+    const SerialGrid G = make_grid(dim, nc, w, cap, size, items, cell_of, site);
+    const uint32_t n = l.n_bodies;
+    cudaError_t e = build_grid(dim, g, a, G, n, s);
+    if (e != cudaSuccess || n == 0) return e;
+    if (dim == 2) {
+        if (soft)
+            k_serial_sphere<2, true><<<1, 32, 0, s>>>(g, a, G, p, l, mask);
+        else
+            k_serial_sphere<2, false><<<1, 32, 0, s>>>(g, a, G, p, l, mask);
+    } else {
+        if (soft)
+            k_serial_sphere<3, true><<<1, 32, 0, s>>>(g, a, G, p, l, mask);
+        else
+            k_serial_sphere<3, false><<<1, 32, 0, s>>>(g, a, G, p, l, mask);
     }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_quick_insert(int dim, const Geometry& g, const Arrays& a, const Pair& p, const Launch& l,
+                                const QuickInsertArgs& q, const uint32_t* nc, const double* w, uint32_t cap,
+                                uint32_t* size, uint32_t* items, uint32_t* cell_of, double4* site,
+                                unsigned long long* out, cudaStream_t s) {
+    const SerialGrid G = make_grid(dim, nc, w, cap, size, items, cell_of, site);
+    cudaError_t e = build_grid(dim, g, a, G, q.n0, s);
+    if (e != cudaSuccess) return e;
+    if (dim == 2)
+        k_quick_insert<2><<<1, 32, 0, s>>>(g, a, G, p, l, q, out);
+    else
+        k_quick_insert<3><<<1, 32, 0, s>>>(g, a, G, p, l, q, out);
     return cudaGetLastError();
 }
 

@@ -67,8 +67,13 @@ typedef enum hmc_interaction {
     HMC_HARD_CONVEX_POLYGON = 1,    /* PairwiseCutoff(HardShape(Convex(ConvexPolygon))) */
     HMC_HARD_CONVEX_POLYHEDRON = 2, /* PairwiseCutoff(HardShape(Convex(ConvexPolyhedron))) */
     HMC_LENNARD_JONES = 3,          /* PairwiseCutoff(Isotropic { Shifted { LennardJones }, r_cut }) */
-    HMC_HARD_CONVEX_SURFACE_MESH_2D = 4 /* PairwiseCutoff(HardShape(ConvexSurfaceMesh2d)): vertices are
+    HMC_HARD_CONVEX_SURFACE_MESH_2D = 4, /* PairwiseCutoff(HardShape(ConvexSurfaceMesh2d)): vertices are
                                            the counter-clockwise hull (convex_surface_mesh_2d.rs) */
+    HMC_OVERLAP_PENALTY = 5         /* PairwiseCutoff(Isotropic { Expanded { delta: diameter,
+                                       OverlapPenalty { k, maximum_allowed_overlap, epsilon_shoulder } },
+                                       r_cut: diameter }): the soft sphere that QuickInsert and
+                                       QuickCompress use (univariate/overlap_penalty.rs:42-116,
+                                       expanded.rs:62-67, benchmarks/src/mc/hard_sphere.rs:191-199) */
 } hmc_interaction;
 
 typedef enum hmc_move {
@@ -105,6 +110,11 @@ typedef struct hmc_system_desc {
     double lj_epsilon, lj_sigma, lj_r_cut, lj_r_shift; /* Isotropic<Shifted<LennardJones>> */
     double boundary_range;       /* Periodic::new maximum_interaction_range; 0 = the pair range */
     double body_interaction_range; /* ParallelSweep::new range; 0 = the pair range */
+    double penalty_k;            /* OverlapPenalty::k (default 10000) */
+    double penalty_maximum_overlap; /* OverlapPenalty::maximum_allowed_overlap (default 0.2) */
+    double penalty_shoulder;     /* OverlapPenalty::epsilon_shoulder (default 100) */
+    uint64_t capacity;           /* bodies the system can hold (>= n_bodies; 0 = n_bodies);
+                                    hmc_quick_insert_apply adds bodies up to it */
 } hmc_system_desc;
 
 typedef struct hmc_sweep_params {
@@ -261,6 +271,60 @@ hmc_status hmc_math_sincos(hmc_context* ctx, const double* x, uint64_t n, double
 
 hmc_status hmc_profile_enable(hmc_system* sys, int enable);
 hmc_status hmc_profile_read(hmc_system* sys, hmc_profile* out, int reset);
+
+/* ---- preparing states: QuickInsert and QuickCompress (hoomd-mc) ----
+ * Both hold their progress in a caller-owned struct, as the reference's QuickInsert and
+ * QuickCompress values do; the microstate is the system's device state. Hard spheres and
+ * HMC_OVERLAP_PENALTY spheres (the interaction the reference pairs them with).
+ *
+ * QuickInsert::apply (quick_insert.rs:228-280): when the total energy is <= 0 and bodies remain,
+ * up to `target` bodies are drawn from UniformIn over the box (one Uniform(-L/2, L/2) per axis,
+ * uniform_in.rs:112-130, cuboid.rs:568-596) from one stream Counter(step, substep, seed), each
+ * kept when its insertion energy (delta_energy_insert, pairwise_cutoff.rs:1000-1009) is finite;
+ * the call stops after `allowed_overlaps` kept bodies that overlap (energy > 0) or when all are
+ * in, and increments the substep. It completes (complete = 1, no substep) once every body is in
+ * and the energy is <= 0. Bodies are appended in order (new tags); the system must have the
+ * capacity. The insertions are sequential by definition: one warp runs them on the device. */
+typedef struct hmc_quick_insert {
+    uint64_t target;           /* bodies to insert */
+    uint64_t allowed_overlaps; /* QuickInsert::new: max(target / 8, 1) */
+    uint64_t inserted;         /* bodies inserted so far */
+    uint32_t complete;
+    uint32_t reserved;
+} hmc_quick_insert;
+hmc_status hmc_quick_insert_apply(hmc_system* sys, hmc_quick_insert* qi, hmc_count* out);
+
+/* QuickCompress::apply (quick_compress.rs:298-383): a state machine over Startup, Waiting,
+ * Compressing and Complete. Compressing draws delta ~ Uniform(0, maximum_delta) from
+ * Counter(step, substep, seed), scales the volume by (1 -/+ delta) towards the target (not
+ * past it), maps every body into the scaled box (Hypercuboid::map_point, cuboid.rs:553-565,
+ * then update_body_properties) and keeps the result when the total energy rose by at most
+ * maximum_energy_per_site per site. Waiting moves on once the energy is <= 0. Every call
+ * increments the substep. */
+typedef enum hmc_quick_compress_state {
+    HMC_QC_STARTUP = 0,
+    HMC_QC_WAITING = 1,
+    HMC_QC_COMPRESSING = 2,
+    HMC_QC_COMPLETE = 3
+} hmc_quick_compress_state;
+typedef struct hmc_quick_compress {
+    double target_volume;
+    double maximum_energy_per_site; /* default 1000 */
+    double maximum_delta;           /* default 0.05, in (0, 1) */
+    uint32_t state;                 /* hmc_quick_compress_state */
+    uint32_t is_final;              /* Waiting: the last accepted box had the target volume */
+    double boundary[3];             /* Waiting / Complete: the box edge lengths they refer to */
+} hmc_quick_compress;
+hmc_status hmc_quick_compress_apply(hmc_system* sys, hmc_quick_compress* qc);
+
+/* The box edge lengths. hmc_set_box replaces the box as Microstate::clone_with_boundary does
+ * (microstate.rs:1529-1565): every body is mapped into the new box (map_point), wrapped, and
+ * the checkerboard is rebuilt; HMC_RANGE_TOO_LARGE when the box is too small for the
+ * interaction range (the reference's Periodic::scale_length panics). */
+hmc_status hmc_get_box(hmc_system* sys, double* edge_lengths);
+hmc_status hmc_set_box(hmc_system* sys, const double* edge_lengths);
+/* Bodies in the system (it grows under hmc_quick_insert_apply). */
+hmc_status hmc_get_n_bodies(hmc_system* sys, uint64_t* n_bodies);
 
 /* ---- GSD files (hoomd-gsd) ----
  * The file layer replaces GsdFile (hoomd-gsd/src/file_layer.rs:559-2458): the same on-disk

@@ -21,6 +21,7 @@ HARD_CONVEX_POLYGON = 1
 HARD_CONVEX_POLYHEDRON = 2
 LENNARD_JONES = 3
 HARD_CONVEX_SURFACE_MESH_2D = 4
+OVERLAP_PENALTY = 5
 TRANSLATE = 0
 ROTATE = 1
 
@@ -90,6 +91,15 @@ def lib():
         L.oracle_get_state.argtypes = [C.c_void_p, _dp, _dp, _u64p, _u32p]
         L.oracle_set_counter.argtypes = [C.c_void_p, C.c_uint64, C.c_uint32]
         L.oracle_gsd_frame.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.oracle_set_penalty.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double]
+        L.oracle_n_bodies.argtypes = [C.c_void_p]
+        L.oracle_n_bodies.restype = C.c_uint64
+        L.oracle_get_box.argtypes = [C.c_void_p, _dp]
+        L.oracle_set_box.argtypes = [C.c_void_p, _dp]
+        L.oracle_set_box.restype = C.c_int
+        L.oracle_quick_insert.argtypes = [C.c_void_p, C.c_uint64, C.c_uint64, _u64p, _u32p, _u64p, _u64p]
+        L.oracle_quick_compress.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double, _u32p, _u32p, _dp]
+        L.oracle_quick_compress.restype = C.c_int
         L.oracle_increment_step.argtypes = [C.c_void_p]
         L.oracle_parallel_sweep.argtypes = [C.c_void_p, C.c_uint32, C.c_double, C.c_double, C.c_double,
                                             _u64p, _u64p]
@@ -293,7 +303,7 @@ class System:
 
     def __init__(self, dim, edge_lengths, positions, orientations=None, *, step=0, substep=0, seed=0,
                  interaction=HARD_SPHERE, diameter=1.0, vertices=None, lj_epsilon=1.0, lj_sigma=1.0,
-                 lj_r_cut=2.5, lj_r_shift=2.5, boundary_range=None):
+                 lj_r_cut=2.5, lj_r_shift=2.5, boundary_range=None, penalty=(10000.0, 0.2, 100.0)):
         self.dim = dim
         self.L = _f64(edge_lengths)
         pos = _f64(positions, (-1,))
@@ -303,7 +313,7 @@ class System:
         verts = None if vertices is None else _f64(vertices, (-1,))
         nv = 0 if verts is None else verts.size // dim
         if boundary_range is None:
-            if interaction == HARD_SPHERE:
+            if interaction in (HARD_SPHERE, OVERLAP_PENALTY):
                 boundary_range = diameter
             elif interaction == LENNARD_JONES:
                 boundary_range = lj_r_cut
@@ -313,7 +323,9 @@ class System:
         self._h = lib().oracle_system_create(dim, _d(self.L), self.n, _d(pos), _d(ori), step, substep, seed,
                                              interaction, diameter, _d(verts), nv, lj_epsilon, lj_sigma,
                                              lj_r_cut, lj_r_shift, boundary_range)
-        self.ori_len = 0 if interaction in (HARD_SPHERE, LENNARD_JONES) else (4 if dim == 3 else 1)
+        self.ori_len = 0 if interaction in (HARD_SPHERE, LENNARD_JONES, OVERLAP_PENALTY) else (4 if dim == 3 else 1)
+        if interaction == OVERLAP_PENALTY:
+            lib().oracle_set_penalty(self._h, *penalty)
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -331,6 +343,43 @@ class System:
 
     def set_counter(self, step, substep):
         lib().oracle_set_counter(self._h, step, substep)
+
+    @property
+    def n_bodies(self) -> int:
+        return int(lib().oracle_n_bodies(self._h))
+
+    def box(self):
+        L = np.zeros(self.dim)
+        lib().oracle_get_box(self._h, _d(L))
+        return L
+
+    def set_box(self, edge_lengths):
+        L = _f64(edge_lengths)
+        if lib().oracle_set_box(self._h, _d(L)) != 0:
+            raise ValueError("a body is outside the box")
+        self.L = L
+
+    def quick_insert(self, state: dict):
+        """QuickInsert::apply; state holds target, allowed_overlaps, inserted, complete."""
+        ins, comp = C.c_uint64(state["inserted"]), C.c_uint32(state["complete"])
+        a, r = C.c_uint64(), C.c_uint64()
+        lib().oracle_quick_insert(self._h, state["target"], state["allowed_overlaps"], C.byref(ins), C.byref(comp),
+                                  C.byref(a), C.byref(r))
+        state["inserted"], state["complete"] = ins.value, comp.value
+        self.n = self.n_bodies
+        return a.value, r.value
+
+    def quick_compress(self, state: dict):
+        """QuickCompress::apply; state holds target_volume, maximum_energy_per_site, maximum_delta,
+        state, is_final, boundary."""
+        st, fin = C.c_uint32(state["state"]), C.c_uint32(state["is_final"])
+        b = np.array(list(state["boundary"]) + [0.0] * (3 - len(state["boundary"])), dtype=np.float64)
+        rc = lib().oracle_quick_compress(self._h, state["target_volume"], state["maximum_energy_per_site"],
+                                         state["maximum_delta"], C.byref(st), C.byref(fin), _d(b))
+        if rc != 0:
+            raise ValueError("a body is outside the box")
+        state["state"], state["is_final"], state["boundary"] = st.value, fin.value, b.tolist()
+        self.L = self.box()
 
     def gsd_frame(self):
         """FP32 site positions (n, 3) and versors (n, 4) or None, as a GSD frame holds them."""

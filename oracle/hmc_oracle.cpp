@@ -997,10 +997,12 @@ struct oracle_system {
     Polytope poly;
     double eps = 1, sigma = 1, rcut = 2.5, rshift = 2.5;
     double boundary_range = 1.0;
+    double body_range = 1.0;
     double search_range = 1.0;
     Grid grid;
 
-    bool hard() const { return interaction != ORACLE_LENNARD_JONES; }
+    bool hard() const { return interaction != ORACLE_LENNARD_JONES && interaction != ORACLE_OVERLAP_PENALTY; }
+    double pk = 10000.0, pdmax = 0.2, pshoulder = 100.0;  // OverlapPenalty
     bool oriented() const {
         return interaction == ORACLE_HARD_CONVEX_POLYGON || interaction == ORACLE_HARD_CONVEX_POLYHEDRON ||
                interaction == ORACLE_HARD_CONVEX_SURFACE_MESH_2D;
@@ -1085,6 +1087,16 @@ struct oracle_system {
                 return convex_global_2d(poly, x, o[0], y, orient[j]) ? INFINITY : 0.0;
             case ORACLE_HARD_CONVEX_SURFACE_MESH_2D:
                 return sat_global_2d(poly, x, o[0], y, orient[j]) ? INFINITY : 0.0;
+            case ORACLE_OVERLAP_PENALTY: {
+                // Isotropic::site_pair_energy (isotropic.rs:147-156) of Expanded { delta: diameter,
+                // OverlapPenalty } (expanded.rs:64-66, overlap_penalty.rs:109-115), r_cut = diameter
+                const double r2 = distance_squared(x, y, dim);
+                if (r2 >= diameter * diameter) return 0.0;
+                const double r = std::sqrt(r2) - diameter;
+                if (r < -pdmax) return INFINITY;
+                if (r < 0.0) return 0.5 * pk * (r * r) + pshoulder;
+                return 0.0;
+            }
             default:
                 return shifted_lj_pair(eps, sigma, rcut, rshift, distance_squared(x, y, dim));
         }
@@ -1214,6 +1226,154 @@ void oracle_ziggurat_tables(double* x_out, double* f_out) {
 }
 
 void oracle_wrap(uint32_t dim, const double* L, double* point) { wrap((int)dim, L, point); }
+void oracle_set_penalty(oracle_system* s, double k, double maximum_allowed_overlap, double epsilon_shoulder) {
+    s->pk = k;
+    s->pdmax = maximum_allowed_overlap;
+    s->pshoulder = epsilon_shoulder;
+}
+uint64_t oracle_n_bodies(const oracle_system* s) { return s->n; }
+void oracle_get_box(const oracle_system* s, double* edge_lengths) {
+    for (int a = 0; a < s->dim; ++a) edge_lengths[a] = s->L[a];
+}
+
+// Microstate::clone_with_boundary (microstate.rs:1529-1565) with Hypercuboid::map_point
+// (cuboid.rs:553-565): inside check in the old box, scale by L'/L, clamp to
+// [-L'/2, next_down(L'/2)], then update_body_properties (body = wrap, site = wrap(body)).
+int oracle_set_box(oracle_system* s, const double* edge_lengths) {
+    std::vector<double> body = s->body;
+    for (uint64_t i = 0; i < s->n; ++i) {
+        double* x = &body[3 * i];
+        for (int a = 0; a < s->dim; ++a)
+            if (!(-s->L[a] / 2.0 <= x[a] && x[a] < s->L[a] / 2.0)) return -1;
+        for (int a = 0; a < s->dim; ++a) {
+            const double scale = edge_lengths[a] / s->L[a];
+            double y = scale * x[a];
+            const double lo = -edge_lengths[a] / 2.0, hi = std::nextafter(edge_lengths[a] / 2.0, -INFINITY);
+            if (y < lo) y = lo;
+            if (y > hi) y = hi;
+            x[a] = y;
+        }
+    }
+    for (int a = 0; a < s->dim; ++a) s->L[a] = edge_lengths[a];
+    for (uint64_t i = 0; i < s->n; ++i) {
+        double p[3] = {body[3 * i], body[3 * i + 1], body[3 * i + 2]};
+        wrap(s->dim, s->L, p);
+        for (int a = 0; a < 3; ++a) s->body[3 * i + a] = p[a];
+        wrap(s->dim, s->L, p);
+        for (int a = 0; a < 3; ++a) s->site[3 * i + a] = p[a];
+    }
+    s->build_grid();
+    return 0;
+}
+
+void oracle_quick_insert(oracle_system* s, uint64_t target, uint64_t allowed_overlaps, uint64_t* inserted,
+                         uint32_t* complete, uint64_t* accepted, uint64_t* rejected) {
+    *accepted = 0;
+    *rejected = 0;
+    if (*complete) return;
+    const double energy = oracle_total_energy(s);
+    if (energy <= 0.0 && *inserted >= target) {
+        *complete = 1;
+        return;
+    }
+    if (energy <= 0.0) {
+        Sfc64 rng = make_rng(s->step, s->substep, s->seed, 0);
+        uint64_t overlapping = 0;
+        std::vector<uint32_t> cand;
+        for (uint64_t attempt = 0; attempt < target; ++attempt) {
+            // UniformIn::sample: per axis Uniform::new(-L/2, L/2).sample(rng) (cuboid.rs:568-596)
+            double x[3] = {0.0, 0.0, 0.0};
+            for (int a = 0; a < s->dim; ++a) {
+                const double low = -s->L[a] / 2.0, high = s->L[a] / 2.0;
+                const uint64_t bits = rng.next_u64() >> 12;
+                const double u = bits_to_double(0x3FF0000000000000ULL | bits) - 1.0;
+                x[a] = u * (high - low) + low;
+            }
+            // delta_energy_insert: the site is wrap(transform(body, site)) (pairwise_cutoff.rs:420-450)
+            double t[3] = {x[0], x[1], x[2]};
+            wrap(s->dim, s->L, t);
+            const double de = s->site_energy(t, nullptr, UINT64_MAX, cand);
+            if (std::isfinite(de)) {
+                // Microstate::add_body: body = wrap(input), site = wrap(body), appended
+                double b[3] = {x[0], x[1], x[2]};
+                wrap(s->dim, s->L, b);
+                double sv[3] = {b[0], b[1], b[2]};
+                wrap(s->dim, s->L, sv);
+                for (int a = 0; a < 3; ++a) s->body.push_back(b[a]);
+                for (int a = 0; a < 3; ++a) s->site.push_back(sv[a]);
+                const uint64_t i = s->n++;
+                const uint64_t c = s->grid.cell_index(sv);
+                s->grid.cell_of.push_back(c);
+                s->grid.cells[c].push_back((uint32_t)i);
+                *accepted += 1;
+                *inserted += 1;
+                if (de > 0.0) overlapping += 1;
+                if (*inserted == target || overlapping >= allowed_overlaps) break;
+            } else {
+                *rejected += 1;
+            }
+        }
+    }
+    s->substep += 1;
+}
+
+int oracle_quick_compress(oracle_system* s, double target_volume, double maximum_energy_per_site,
+                          double maximum_delta, uint32_t* state, uint32_t* is_final, double* boundary) {
+    Sfc64 rng = make_rng(s->step, s->substep, s->seed, 0);
+    s->substep += 1;
+    double L[3] = {s->L[0], s->L[1], s->L[2]};
+    auto same = [&]() {
+        for (int a = 0; a < s->dim; ++a)
+            if (boundary[a] != L[a]) return false;
+        return true;
+    };
+    auto wait_on = [&](bool fin, const double* b) {
+        *state = 1;
+        *is_final = fin ? 1u : 0u;
+        for (int a = 0; a < 3; ++a) boundary[a] = a < s->dim ? b[a] : 0.0;
+    };
+    switch (*state) {
+        case 0:
+            wait_on(false, L);
+            break;
+        case 3:
+            if (!same()) wait_on(false, L);
+            break;
+        case 2: {
+            const uint64_t bits = rng.next_u64() >> 12;
+            const double u = bits_to_double(0x3FF0000000000000ULL | bits) - 1.0;
+            const double delta = u * (maximum_delta - 0.0) + 0.0;
+            double volume = L[0];
+            for (int a = 1; a < s->dim; ++a) volume = volume * L[a];
+            const double trial_volume = target_volume > volume ? std::min(volume * (1.0 + delta), target_volume)
+                                                               : std::max(volume * (1.0 - delta), target_volume);
+            const double v = std::pow(trial_volume / volume, 1.0 / (double)s->dim);
+            double Ln[3] = {L[0], L[1], L[2]};
+            for (int a = 0; a < s->dim; ++a) Ln[a] = L[a] * v;
+            const double e0 = oracle_total_energy(s);
+            oracle_system saved = *s;
+            if (oracle_set_box(s, Ln) != 0) return -1;
+            const double e1 = oracle_total_energy(s);
+            if (e1 - e0 > maximum_energy_per_site * (double)s->n) {
+                *s = saved;
+            } else {
+                wait_on(trial_volume == target_volume, Ln);
+            }
+            break;
+        }
+        case 1:
+            if (oracle_total_energy(s) <= 0.0) {
+                if (*is_final && same()) {
+                    *state = 3;
+                    for (int a = 0; a < 3; ++a) boundary[a] = a < s->dim ? L[a] : 0.0;
+                } else {
+                    *state = 2;
+                }
+            }
+            break;
+    }
+    return 0;
+}
 // AppendMicrostate::append_microstate (hoomd-microstate/src/append.rs:46-113) for single-site
 // bodies: each site is wrap(body.transform(site_local)) with the site at the body origin and the
 // identity orientation (microstate.rs:995-1010; Transform for Point: position + site position,
@@ -1389,6 +1549,9 @@ oracle_system* oracle_system_create(uint32_t dim, const double* L, uint64_t n, c
             break;
         case ORACLE_LENNARD_JONES:
             s->search_range = rcut;
+            break;
+        case ORACLE_OVERLAP_PENALTY:
+            s->search_range = diameter;
             break;
         default:
             s->search_range = s->poly.bounding_radius * 2.0;

@@ -81,7 +81,7 @@ double oracle_shifted_lj_pair(double epsilon, double sigma, double r_cut, double
 
 // ---- systems --------------------------------------------------------------------
 enum { ORACLE_HARD_SPHERE = 0, ORACLE_HARD_CONVEX_POLYGON = 1, ORACLE_HARD_CONVEX_POLYHEDRON = 2,
-       ORACLE_LENNARD_JONES = 3, ORACLE_HARD_CONVEX_SURFACE_MESH_2D = 4 };
+       ORACLE_LENNARD_JONES = 3, ORACLE_HARD_CONVEX_SURFACE_MESH_2D = 4, ORACLE_OVERLAP_PENALTY = 5 };
 enum { ORACLE_TRANSLATE = 0, ORACLE_ROTATE = 1 };
 
 typedef struct oracle_system oracle_system;
@@ -98,6 +98,20 @@ void oracle_system_destroy(oracle_system* s);
 void oracle_get_state(const oracle_system* s, double* positions, double* orientations,
                       uint64_t* step, uint32_t* substep);
 void oracle_set_counter(oracle_system* s, uint64_t step, uint32_t substep);
+// Isotropic<Expanded<OverlapPenalty>> parameters (interaction ORACLE_OVERLAP_PENALTY; the
+// diameter is delta and r_cut).
+void oracle_set_penalty(oracle_system* s, double k, double maximum_allowed_overlap, double epsilon_shoulder);
+uint64_t oracle_n_bodies(const oracle_system* s);
+void oracle_get_box(const oracle_system* s, double* edge_lengths);
+// Microstate::clone_with_boundary onto a new box; 0 on success, -1 if a body is outside the box.
+int oracle_set_box(oracle_system* s, const double* edge_lengths);
+// QuickInsert::apply (quick_insert.rs:228-280); the progress lives in the caller's fields.
+void oracle_quick_insert(oracle_system* s, uint64_t target, uint64_t allowed_overlaps, uint64_t* inserted,
+                         uint32_t* complete, uint64_t* accepted, uint64_t* rejected);
+// QuickCompress::apply (quick_compress.rs:298-383); state 0..3 = Startup, Waiting, Compressing,
+// Complete; boundary: the box Waiting/Complete refer to.
+int oracle_quick_compress(oracle_system* s, double target_volume, double maximum_energy_per_site,
+                          double maximum_delta, uint32_t* state, uint32_t* is_final, double* boundary);
 // The FP32 site positions (n x 3) and site versors (n x 4, oriented shapes) that
 // AppendMicrostate writes to a GSD frame (hoomd-microstate/src/append.rs:46-113).
 void oracle_gsd_frame(const oracle_system* s, float* positions, float* orientations);

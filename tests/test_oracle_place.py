@@ -1,0 +1,110 @@
+"""The oracle's restatement of state preparation: the OverlapPenalty pair energy against the
+reference's known answers (hoomd-interaction/src/univariate/overlap_penalty.rs tests), and
+QuickInsert / QuickCompress (hoomd-mc/src/quick_insert.rs, quick_compress.rs) against the
+behaviour their own tests and the benchmark placement (benchmarks/src/place.rs) rely on."""
+import math
+
+import numpy as np
+import pytest
+
+import oracle
+
+
+def pair_energy(x, k, dmax, eps, d=1.0):
+    """Energy of two overlap-penalty spheres (diameter d) at distance r = d + x along x."""
+    r = d + x
+    o = oracle.System(3, [10.0, 10.0, 10.0], [[0.0, 0.0, 0.0], [r, 0.0, 0.0]], interaction=oracle.OVERLAP_PENALTY,
+                      diameter=d, penalty=(k, dmax, eps))
+    return o.total_energy()
+
+
+def test_overlap_penalty_shoulder():
+    # overlap_penalty.rs tests::shoulder: k = 0, eps = 15, d_max = 1
+    assert pair_energy(1.0, 0.0, 1.0, 15.0) == 0.0
+    assert pair_energy(0.0, 0.0, 1.0, 15.0) == 0.0
+    assert pair_energy(-2.0 ** -53, 0.0, 1.0, 15.0) == 15.0  # 0.0_f64.next_down() after r = 1 - 2^-53
+    assert pair_energy(-0.5, 0.0, 1.0, 15.0) == 15.0
+
+
+def test_overlap_penalty_core():
+    # tests::core: k = 0, eps = 0, d_max = 0.5
+    assert pair_energy(0.5, 0.0, 0.5, 0.0) == 0.0
+    assert pair_energy(-0.5, 0.0, 0.5, 0.0) == 0.0
+    assert pair_energy(-0.5 - 2.0 ** -53, 0.0, 0.5, 0.0) == math.inf  # (-0.5).next_down()
+    assert pair_energy(-0.75, 0.0, 0.5, 0.0) == math.inf
+
+
+def test_overlap_penalty_harmonic():
+    # tests::harmonic: k = 6, eps = 0, d_max = 10; energy(-0.125) = 0.5 k 0.125^2
+    assert pair_energy(-0.125, 6.0, 10.0, 0.0, d=2.0) == 0.5 * 6.0 * 0.125 ** 2
+    assert pair_energy(0.5, 6.0, 10.0, 0.0) == 0.0
+
+
+def test_quick_insert_hard_spheres():
+    # quick_insert.rs tests::hard_spheres, in a periodic 6 x 6 box: one body at the origin,
+    # QuickInsert(target 10) applied until complete, then a serial sweep; 11 bodies, energy 0
+    o = oracle.System(2, [6.0, 6.0], [[0.0, 0.0]], diameter=1.0)
+    qi = {"target": 10, "allowed_overlaps": max(10 // 8, 1), "inserted": 0, "complete": 0}
+    for _ in range(100):
+        o.quick_insert(qi)
+        if qi["complete"]:
+            break
+    o.serial_sweep(oracle.TRANSLATE, 0.1, 1.0)
+    assert qi["inserted"] == 10 and qi["complete"] == 1
+    assert o.n_bodies == 11
+    assert o.total_energy() == 0.0
+
+
+def test_quick_insert_counts_and_substep():
+    o = oracle.System(3, [8.0, 8.0, 8.0], np.zeros((0, 3)), interaction=oracle.OVERLAP_PENALTY, diameter=1.0)
+    qi = {"target": 200, "allowed_overlaps": 25, "inserted": 0, "complete": 0}
+    a, r = o.quick_insert(qi)
+    _, _, step, sub = o.state()
+    assert (step, sub) == (0, 1)
+    assert a == qi["inserted"] == o.n_bodies > 0
+    # stops at 25 overlapping insertions or when all 200 are in
+    assert a == 200 or a < 200
+    assert o.total_energy() >= 0.0
+
+
+def _place(o, n, rho, dim, target_steps=20000):
+    """place_single_site_point_bodies (benchmarks/src/place.rs:31-110): QuickInsert then
+    QuickCompress every 20 steps, a serial translation sweep (0.1) every step."""
+    qi = {"target": n, "allowed_overlaps": max(n // 8, 1), "inserted": 0, "complete": 0}
+    qc = {"target_volume": n / rho, "maximum_energy_per_site": 1000.0, "maximum_delta": 0.05, "state": 0,
+          "is_final": 0, "boundary": [0.0, 0.0, 0.0]}
+    for _ in range(target_steps):
+        _, _, step, _ = o.state()
+        if step % 20 == 0:
+            if qi["complete"]:
+                o.quick_compress(qc)
+            else:
+                o.quick_insert(qi)
+        o.serial_sweep(oracle.TRANSLATE, 0.1, 1.0)
+        o.increment_step()
+        if qc["state"] == 3:
+            break
+    return qi, qc
+
+
+def test_place_point_bodies_2d():
+    n, rho = 64, 0.6
+    L0 = math.sqrt(n / (0.7 * rho))
+    o = oracle.System(2, [L0, L0], np.zeros((0, 2)), interaction=oracle.OVERLAP_PENALTY, diameter=1.0)
+    qi, qc = _place(o, n, rho, 2)
+    assert qi["complete"] and qc["state"] == 3
+    assert o.n_bodies == n
+    assert np.prod(o.box()) == pytest.approx(n / rho, rel=1e-12)
+    assert o.total_energy() == 0.0
+
+
+def test_set_box_maps_bodies():
+    rng = np.random.default_rng(3)
+    L = np.array([7.0, 9.0, 11.0])
+    pos = (rng.random((50, 3)) - 0.5) * L
+    o = oracle.System(3, L, pos, diameter=1.0)
+    o.set_box(L * 0.9)
+    got = o.state()[0]
+    want = np.clip(pos * (0.9 * L / L), -0.9 * L / 2, np.nextafter(0.9 * L / 2, -np.inf))
+    assert np.allclose(got, want, rtol=0, atol=1e-12)
+    assert np.all(np.abs(got) <= 0.9 * L / 2)
