@@ -87,6 +87,16 @@ class hmc_quick_compress(C.Structure):
                 ("boundary", C.c_double * 3)]
 
 
+class hmc_grand_canonical_params(C.Structure):
+    _fields_ = [("temperature", C.c_double), ("fugacity", C.c_double), ("n_trials", C.c_uint32),
+                ("reserved", C.c_uint32)]
+
+
+class hmc_insert_remove_count(C.Structure):
+    _fields_ = [("insert_accepted", C.c_uint64), ("insert_rejected", C.c_uint64), ("remove_accepted", C.c_uint64),
+                ("remove_rejected", C.c_uint64)]
+
+
 class hmc_gsd_chunk(C.Structure):
     _fields_ = [("frame", C.c_uint64), ("rows", C.c_uint64), ("location", C.c_uint64), ("columns", C.c_uint32),
                 ("id", C.c_uint16), ("type", C.c_uint8), ("flags", C.c_uint8)]
@@ -143,6 +153,8 @@ SIGNATURES = {
     "hmc_overlap_count_noalloc": (C.c_int, [_vp, C.c_uint64, C.c_uint32, _dp, C.c_double, C.c_double, _vp, _vp]),
     "hmc_quick_insert_apply": (C.c_int, [_vp, C.POINTER(hmc_quick_insert), C.POINTER(hmc_count)]),
     "hmc_quick_compress_apply": (C.c_int, [_vp, C.POINTER(hmc_quick_compress)]),
+    "hmc_grand_canonical_apply": (C.c_int, [_vp, C.POINTER(hmc_grand_canonical_params),
+                                            C.POINTER(hmc_insert_remove_count)]),
     "hmc_get_box": (C.c_int, [_vp, _dp]),
     "hmc_set_box": (C.c_int, [_vp, _dp]),
     "hmc_get_n_bodies": (C.c_int, [_vp, C.POINTER(C.c_uint64)]),
@@ -763,6 +775,35 @@ class QuickCompress:
         microstate.edge_lengths = [float(x) for x in microstate.box()]
 
 
+@dataclass
+class IsothermalIsofugacity:
+    """hoomd_simulation::macrostate::IsothermalIsofugacity: temperature and fugacity."""
+    temperature: float = 1.0
+    fugacity: float = 0.0
+
+
+@dataclass
+class InsertRemoveCount:
+    """hoomd_mc::InsertRemoveCount (grand_canonical.rs)."""
+    insert_accepted: int = 0
+    insert_rejected: int = 0
+    remove_accepted: int = 0
+    remove_rejected: int = 0
+
+
+class GrandCanonical:
+    """hoomd_mc::GrandCanonical (grand_canonical.rs:49-110) with the distribution UniformIn over
+    the microstate's box; apply(..., n_trials=k) runs k applies in sequence on the device."""
+
+    def apply(self, microstate: Microstate, hamiltonian, macrostate: IsothermalIsofugacity,
+              n_trials: int = 1) -> InsertRemoveCount:
+        p = hmc_grand_canonical_params(float(macrostate.temperature), float(macrostate.fugacity), int(n_trials), 0)
+        c = hmc_insert_remove_count()
+        _check(_lib.hmc_grand_canonical_apply(microstate._h, C.byref(p), C.byref(c)))
+        microstate.refresh()
+        return InsertRemoveCount(c.insert_accepted, c.insert_rejected, c.remove_accepted, c.remove_rejected)
+
+
 class Batch:
     """Independent hard-sphere replicas swept together (hmc_batch_*): one counting sort and one
     kernel per colour pass for all replicas. Replica k evolves exactly as a Microstate built
@@ -895,6 +936,7 @@ class ParallelSweep:
 __all__ = ["Batch", "Context", "sdf_pressure", "gr_normalise", "ConvexPolygon", "ConvexPolyhedron", "ConvexSurfaceMesh2d", "Count", "convex_hull_2d", "HardShape", "HardSphere", "HmcError", "Isothermal", "Isotropic",
            "LennardJones", "Microstate", "PairwiseCutoff", "Rotate", "Shifted", "TuneOptions",
            "ParallelSweep", "Periodic", "Translate", "load_library", "SIGNATURES", "FP64", "FP32_RECHECK",
-           "QuickInsert", "QuickCompress", "OverlapPenalty", "Expanded",
+           "QuickInsert", "QuickCompress", "OverlapPenalty", "Expanded", "GrandCanonical", "IsothermalIsofugacity",
+           "InsertRemoveCount",
            "TRANSLATE", "ROTATE", "HARD_SPHERE", "HARD_CONVEX_POLYGON", "HARD_CONVEX_POLYHEDRON", "LENNARD_JONES",
            "HARD_CONVEX_SURFACE_MESH_2D"]

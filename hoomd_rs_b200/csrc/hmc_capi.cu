@@ -116,6 +116,11 @@ struct hmc_system {
     double4* backup = nullptr;          // [capacity] body positions kept across a box change
     unsigned long long* qi_out = nullptr;  // [4] QuickInsert results
     double lj_params[4] = {1, 1, 2.5, 2.5};  // epsilon, sigma, r_cut, r_shift
+    // body tags (allocated when bodies are first inserted or removed on the device)
+    uint32_t* tags = nullptr;
+    uint32_t* tag_heap = nullptr;
+    uint32_t* tag_meta = nullptr;
+    bool tags_permuted = false;  // some body was removed: index order is not tag order
     bool penalty() const { return interaction == HMC_OVERLAP_PENALTY; }
     bool soft() const { return interaction == HMC_LENNARD_JONES || penalty(); }
     // profiling
@@ -349,6 +354,21 @@ hmc_status system_gsd_frame(hmc_system* s, GsdFrameView* out) {
         s->prof.kernel_launches += 1;
         HMC_CUDA(cudaMemcpyAsync(s->gsd_host, s->gsd_dev, sizeof(float) * floats, cudaMemcpyDeviceToHost, s->stream));
         HMC_CUDA(cudaStreamSynchronize(s->stream));
+    }
+    if (n && s->tags_permuted) {
+        // iter_sites_tag_order: rows in increasing tag order (tags are unique)
+        std::vector<uint32_t> tag(n);
+        HMC_CUDA(cudaMemcpy(tag.data(), s->tags, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost));
+        std::vector<uint32_t> order(n);
+        for (uint64_t i = 0; i < n; ++i) order[i] = (uint32_t)i;
+        std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return tag[a] < tag[b]; });
+        const int w[2] = {3, 4};
+        float* base[2] = {s->gsd_host, s->gsd_host + 3 * n};
+        for (int k = 0; k < (ori ? 2 : 1); ++k) {
+            std::vector<float> tmp(base[k], base[k] + w[k] * n);
+            for (uint64_t r = 0; r < n; ++r)
+                std::memcpy(base[k] + w[k] * r, tmp.data() + (size_t)w[k] * order[r], sizeof(float) * w[k]);
+        }
     }
     out->step = s->step;
     out->dim = s->dim;
@@ -1199,6 +1219,23 @@ hmc_status hmc_set_box(hmc_system* s, const double* edge_lengths) {
     return map_into_box(s, edge_lengths);
 }
 
+// Body tags on the device: identity for the bodies present when first needed.
+static hmc_status body_tags(hmc_system* s, BodyTags* out) {
+    if (!s->tags) {
+        hmc_status st;
+        if ((st = dalloc(s, &s->tags, s->capacity)) || (st = dalloc(s, &s->tag_heap, s->capacity)) ||
+            (st = dalloc(s, &s->tag_meta, 2)))
+            return st;
+        std::vector<uint32_t> id(std::max<uint64_t>(s->n, 1));
+        for (uint64_t i = 0; i < s->n; ++i) id[i] = (uint32_t)i;
+        if (s->n) HMC_CUDA(cudaMemcpy(s->tags, id.data(), sizeof(uint32_t) * s->n, cudaMemcpyHostToDevice));
+        const uint32_t meta[2] = {0u, (uint32_t)s->n};
+        HMC_CUDA(cudaMemcpy(s->tag_meta, meta, sizeof(meta), cudaMemcpyHostToDevice));
+    }
+    *out = BodyTags{s->tags, s->tag_heap, s->tag_meta};
+    return HMC_OK;
+}
+
 hmc_status hmc_quick_insert_apply(hmc_system* s, hmc_quick_insert* qi, hmc_count* out) {
     if (!s || !qi) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
     if (s->interaction != HMC_HARD_SPHERE && !s->penalty())
@@ -1221,7 +1258,7 @@ hmc_status hmc_quick_insert_apply(hmc_system* s, hmc_quick_insert* qi, hmc_count
     }
     if (energy <= 0.0) {
         if ((st = serial_grid(s))) return st;
-        if (!s->qi_out && (st = dalloc(s, &s->qi_out, 4))) return st;
+        if (!s->qi_out && (st = dalloc(s, &s->qi_out, 8))) return st;
         Launch L{};
         L.step = s->step;
         L.substep = s->substep;
@@ -1241,9 +1278,11 @@ hmc_status hmc_quick_insert_apply(hmc_system* s, hmc_quick_insert* qi, hmc_count
             q.scale[a] = high - low;
         }
         HMC_CUDA(cudaMemsetAsync(s->arr.stats, 0, sizeof(DeviceStats), s->stream));
-        HMC_CUDA(launch_quick_insert(s->dim, s->geom, s->arr, s->pair, L, q, s->serial_nc, s->serial_w, s->serial_cap,
-                                     s->serial_size, s->serial_items, s->serial_cell_of, s->serial_site, s->qi_out,
-                                     s->stream));
+        BodyTags tags;
+        if ((st = body_tags(s, &tags))) return st;
+        HMC_CUDA(launch_quick_insert(s->dim, s->geom, s->arr, s->pair, L, q, tags, s->serial_nc, s->serial_w,
+                                     s->serial_cap, s->serial_size, s->serial_items, s->serial_cell_of, s->serial_site,
+                                     s->qi_out, s->stream));
         s->prof.kernel_launches += 2;
         unsigned long long r[4] = {0, 0, 0, 0};
         HMC_CUDA(cudaMemcpyAsync(r, s->qi_out, sizeof(r), cudaMemcpyDeviceToHost, s->stream));
@@ -1255,6 +1294,60 @@ hmc_status hmc_quick_insert_apply(hmc_system* s, hmc_quick_insert* qi, hmc_count
         count.rejected = r[2];
     }
     s->substep += 1;  // increment_substep (quick_insert.rs:278)
+    if (out) *out = count;
+    return HMC_OK;
+}
+
+hmc_status hmc_grand_canonical_apply(hmc_system* s, const hmc_grand_canonical_params* p,
+                                     hmc_insert_remove_count* out) {
+    if (!s || !p) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
+    if (s->interaction != HMC_HARD_SPHERE && !s->penalty())
+        return fail(HMC_NOT_SUPPORTED, "GrandCanonical inserts and removes hard or overlap-penalty spheres");
+    if (!(p->temperature > 0.0)) return fail(HMC_INVALID_ARGUMENT, "temperature must be positive");
+    if (!std::isfinite(p->fugacity)) return fail(HMC_INVALID_ARGUMENT, "fugacity must be finite");
+    hmc_insert_remove_count count{};
+    if (out) *out = count;
+    if (p->n_trials == 0) return HMC_OK;
+    HMC_CUDA(cudaSetDevice(s->ctx->device));
+    hmc_status st;
+    if ((st = serial_grid(s))) return st;
+    if (!s->qi_out && (st = dalloc(s, &s->qi_out, 8))) return st;
+    BodyTags tags;
+    if ((st = body_tags(s, &tags))) return st;
+    GrandCanonicalArgs q{};
+    q.step = s->step;
+    q.substep = s->substep;
+    q.seed = s->seed;
+    q.n_trials = p->n_trials;
+    q.n0 = (uint32_t)s->n;
+    q.capacity = (uint32_t)s->capacity;
+    q.soft = s->penalty() ? 1u : 0u;
+    q.temperature = p->temperature;
+    q.fugacity = p->fugacity;
+    double volume = s->geom.L[0];
+    for (int a = 1; a < s->dim; ++a) volume = volume * s->geom.L[a];  // Hypercuboid::volume
+    q.volume = volume;
+    for (int a = 0; a < 3; ++a) {
+        const double low = a < s->dim ? -s->geom.L[a] / 2.0 : 0.0, high = a < s->dim ? s->geom.L[a] / 2.0 : 0.0;
+        q.low[a] = low;
+        q.scale[a] = high - low;
+    }
+    HMC_CUDA(cudaMemsetAsync(s->arr.stats, 0, sizeof(DeviceStats), s->stream));
+    HMC_CUDA(launch_grand_canonical(s->dim, s->geom, s->arr, s->pair, q, tags, s->serial_nc, s->serial_w, s->serial_cap,
+                                    s->serial_size, s->serial_items, s->serial_cell_of, s->serial_site, s->qi_out,
+                                    s->stream));
+    s->prof.kernel_launches += 2;
+    unsigned long long r[5] = {0, 0, 0, 0, 0};
+    HMC_CUDA(cudaMemcpyAsync(r, s->qi_out, sizeof(r), cudaMemcpyDeviceToHost, s->stream));
+    if ((st = read_stats(s))) return st;
+    if ((st = check_flags(s))) return st;
+    s->n = r[4];
+    if (r[2]) s->tags_permuted = true;
+    s->substep += p->n_trials;  // one increment_substep per apply
+    count.insert_accepted = r[0];
+    count.insert_rejected = r[1];
+    count.remove_accepted = r[2];
+    count.remove_rejected = r[3];
     if (out) *out = count;
     return HMC_OK;
 }

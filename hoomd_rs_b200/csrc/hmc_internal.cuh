@@ -226,10 +226,33 @@ struct QuickInsertArgs {
     double scale[3];     // Uniform scale per axis
     uint32_t soft;       // 1: overlap penalty, 0: hard spheres
 };
+// Body tags: tag[capacity], a min-heap of free tags heap[capacity], meta = {heap size, tag bound};
+// tag == null: tags are not tracked.
+struct BodyTags {
+    uint32_t* tag;
+    uint32_t* heap;
+    uint32_t* meta;
+};
 cudaError_t launch_quick_insert(int dim, const Geometry& g, const Arrays& a, const Pair& p, const Launch& l,
-                                const QuickInsertArgs& q, const uint32_t* nc, const double* w, uint32_t cap,
-                                uint32_t* size, uint32_t* items, uint32_t* cell_of, double4* site,
+                                const QuickInsertArgs& q, const BodyTags& tags, const uint32_t* nc, const double* w,
+                                uint32_t cap, uint32_t* size, uint32_t* items, uint32_t* cell_of, double4* site,
                                 unsigned long long* out, cudaStream_t s);
+// GrandCanonical::apply, n_trials in sequence on the serial grid (one warp).
+struct GrandCanonicalArgs {
+    uint64_t step;
+    uint32_t substep;      // of the first trial; trial i uses substep + i
+    uint32_t seed;
+    uint32_t n_trials;
+    uint32_t n0;
+    uint32_t capacity;
+    uint32_t soft;
+    double temperature, fugacity, volume;
+    double low[3], scale[3];  // UniformIn per axis
+};
+cudaError_t launch_grand_canonical(int dim, const Geometry& g, const Arrays& a, const Pair& p,
+                                   const GrandCanonicalArgs& q, const BodyTags& tags, const uint32_t* nc,
+                                   const double* w, uint32_t cap, uint32_t* size, uint32_t* items, uint32_t* cell_of,
+                                   double4* site, unsigned long long* out, cudaStream_t s);
 // Clone with boundary (hmc_set_box): every body x -> clamp(scale x, lo, hi) per axis, then
 // B = wrap(.) in the new box; first_outside receives the smallest body index that is not
 // inside the old box (the reference's map_point fails there).

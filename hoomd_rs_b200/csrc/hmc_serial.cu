@@ -41,6 +41,66 @@ __device__ __forceinline__ uint32_t serial_index(const SerialGrid& G, const uint
     return c;
 }
 
+// Body tags (the tagged container of hoomd-microstate/src/microstate.rs:60-123): a new body
+// takes the smallest free tag (a min-heap of freed tags), else the next unused one; removal
+// frees the tag and swap_removes. Lane 0 only.
+__device__ uint32_t tag_take(const BodyTags& T) {
+    uint32_t& size = T.meta[0];
+    if (size == 0) return T.meta[1]++;
+    const uint32_t top = T.heap[0];
+    const uint32_t last = T.heap[--size];
+    uint32_t i = 0;
+    for (;;) {
+        const uint32_t l = 2 * i + 1, r = l + 1;
+        uint32_t m = i;
+        uint32_t vm = last;
+        if (l < size && T.heap[l] < vm) {
+            m = l;
+            vm = T.heap[l];
+        }
+        if (r < size && T.heap[r] < vm) m = r;
+        if (m == i) break;
+        T.heap[i] = T.heap[m];
+        i = m;
+    }
+    if (size) T.heap[i] = last;
+    return top;
+}
+__device__ void tag_free(const BodyTags& T, uint32_t tag) {
+    uint32_t i = T.meta[0]++;
+    while (i > 0) {
+        const uint32_t parent = (i - 1) / 2;
+        if (T.heap[parent] <= tag) break;
+        T.heap[i] = T.heap[parent];
+        i = parent;
+    }
+    T.heap[i] = tag;
+}
+
+// Append body n at B = wrap(x), S = wrap(B) (Microstate::add_body) to the arrays and the grid.
+template <int DIM>
+__device__ void grid_append(const Geometry& g, const Arrays& A, const SerialGrid& G, const BodyTags& T, uint32_t n,
+                            const double* x) {
+    double b[3] = {x[0], x[1], x[2]};
+    wrap_inv<DIM>(g.L, g.invL, b);
+    double sv[3] = {b[0], b[1], b[2]};
+    wrap_inv<DIM>(g.L, g.invL, sv);
+    A.body_pos[n] = make_double4(b[0], b[1], DIM == 3 ? b[2] : 0.0, 0.0);
+    G.site[n] = make_double4(sv[0], sv[1], DIM == 3 ? sv[2] : 0.0, 0.0);
+    uint32_t ms[3] = {0, 0, 0};
+    serial_cell<DIM>(g, G, sv, ms);
+    const uint32_t c = serial_index<DIM>(G, ms);
+    const uint32_t sz = G.size[c];
+    if (sz < G.cap) {
+        G.items[(size_t)c * G.cap + sz] = n;
+        G.size[c] = sz + 1;
+    } else {
+        atomicOr(&A.stats->error_flags, kErrCellOverflow);
+    }
+    G.cell_of[n] = c;
+    if (T.tag) T.tag[n] = tag_take(T);
+}
+
 // Sites and cell lists from the body positions (one thread per body).
 template <int DIM>
 __global__ void k_serial_build(Geometry g, Arrays A, SerialGrid G, uint32_t n) {
@@ -203,7 +263,7 @@ __global__ void __launch_bounds__(32) k_serial_sphere(Geometry g, Arrays A, Seri
 // from single pairs, so no sum is formed. out: inserted, overlapping, rejected, final n.
 template <int DIM>
 __global__ void __launch_bounds__(32) k_quick_insert(Geometry g, Arrays A, SerialGrid G, Pair P, Launch L,
-                                                     QuickInsertArgs q, unsigned long long* out) {
+                                                     QuickInsertArgs q, BodyTags T, unsigned long long* out) {
     const uint32_t lane = threadIdx.x;
     if (A.stats->error_flags) return;
     Sfc64 rng = make_rng(L.step, L.substep, L.seed, 0);
@@ -247,25 +307,7 @@ __global__ void __launch_bounds__(32) k_quick_insert(Geometry g, Arrays A, Seria
             if (lane == 0) atomicOr(&A.stats->error_flags, kErrCellOverflow);
             break;
         }
-        if (lane == 0) {
-            double b[3] = {x[0], x[1], x[2]};
-            wrap_inv<DIM>(g.L, g.invL, b);
-            double sv[3] = {b[0], b[1], b[2]};
-            wrap_inv<DIM>(g.L, g.invL, sv);
-            A.body_pos[n] = make_double4(b[0], b[1], DIM == 3 ? b[2] : 0.0, 0.0);
-            G.site[n] = make_double4(sv[0], sv[1], DIM == 3 ? sv[2] : 0.0, 0.0);
-            uint32_t ms[3] = {0, 0, 0};
-            serial_cell<DIM>(g, G, sv, ms);
-            const uint32_t c = serial_index<DIM>(G, ms);
-            const uint32_t sz = G.size[c];
-            if (sz < G.cap) {
-                G.items[(size_t)c * G.cap + sz] = n;
-                G.size[c] = sz + 1;
-            } else {
-                atomicOr(&A.stats->error_flags, kErrCellOverflow);
-            }
-            G.cell_of[n] = c;
-        }
+        if (lane == 0) grid_append<DIM>(g, A, G, T, n, x);
         __syncwarp();
         n++;
         inserted++;
@@ -278,6 +320,128 @@ __global__ void __launch_bounds__(32) k_quick_insert(Geometry g, Arrays A, Seria
         out[1] = overlapping;
         out[2] = rejected;
         out[3] = n;
+    }
+}
+
+// Insertion energy at site t (no body excluded): the overlap penalty's sum, or 0 / infinity for
+// hard spheres.
+template <int DIM>
+__device__ __forceinline__ double insert_energy(const Geometry& g, const SerialGrid& G, const Pair& P,
+                                                const double* t, bool soft, uint32_t lane) {
+    if (soft) return serial_energy<DIM>(g, G, P, t, 0xffffffffu, lane);
+    uint32_t m[3] = {0, 0, 0}, cell;
+    serial_cell<DIM>(g, G, t, m);
+    bool overlap = false;
+    if (lane_cell<DIM>(G, m, lane, &cell)) {
+        const uint32_t cnt = G.size[cell];
+        for (uint32_t k = 0; k < cnt && !overlap; ++k) {
+            const double4 s4 = G.site[G.items[(size_t)cell * G.cap + k]];
+            const double sv[3] = {s4.x, s4.y, s4.z};
+            overlap = ref_dist2<DIM>(g, t, sv) < P.sigma2;
+        }
+    }
+    return __any_sync(0xffffffffu, overlap) ? __longlong_as_double(0x7ff0000000000000ll) : 0.0;
+}
+
+// GrandCanonical::apply (hoomd-mc/src/grand_canonical.rs:49-110), n_trials times in sequence,
+// trial i drawing from Counter(step, substep + i, seed): a fair coin (rand's bool: the sign bit
+// of next_u32) picks insertion (a UniformIn body, kept when V f exp(-dU/kT) / (N + 1) > u) or
+// removal (a body by random_range(..N), removed when N exp(-dU/kT) / (V f) > u, or always for
+// f <= 0) with swap_remove. out: insert accepted / rejected, remove accepted / rejected, final N.
+template <int DIM>
+__global__ void __launch_bounds__(32) k_grand_canonical(Geometry g, Arrays A, SerialGrid G, Pair P,
+                                                        GrandCanonicalArgs q, BodyTags T, unsigned long long* out) {
+    const uint32_t lane = threadIdx.x;
+    if (A.stats->error_flags) return;
+    uint32_t n = q.n0;
+    unsigned long long ia = 0, ir = 0, ra = 0, rr = 0;
+    const double inf = __longlong_as_double(0x7ff0000000000000ll);
+    for (uint32_t t = 0; t < q.n_trials; ++t) {
+        Sfc64 rng = make_rng(q.step, q.substep + t, q.seed, 0);
+        if (n == 0 && q.fugacity <= 0.0) continue;
+        const bool insert = (int32_t)rng.next_u32() < 0;
+        if (insert) {
+            double x[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+            for (int a = 0; a < DIM; ++a) {
+                const double u = dsub(as_double(0x3FF0000000000000ULL | (rng.next_u64() >> 12)), 1.0);
+                x[a] = dadd(dmul(u, q.scale[a]), q.low[a]);
+            }
+            double tt[3] = {x[0], x[1], x[2]};
+            wrap_inv<DIM>(g.L, g.invL, tt);
+            const double de = insert_energy<DIM>(g, G, P, tt, q.soft != 0, lane);
+            bool accept = false;
+            if (de != inf && de == de) {  // is_finite
+                const double p =
+                    ddiv(dmul(dmul(q.volume, q.fugacity), exp(ddiv(-de, q.temperature))), dadd((double)n, 1.0));
+                accept = p > uniform01(rng);
+            }
+            if (accept) {
+                if (n >= q.capacity) {
+                    if (lane == 0) atomicOr(&A.stats->error_flags, kErrCellOverflow);
+                    break;
+                }
+                if (lane == 0) grid_append<DIM>(g, A, G, T, n, x);
+                __syncwarp();
+                n++;
+                ia++;
+            } else {
+                ir++;
+            }
+        } else if (n > 0) {
+            const uint32_t idx = canon_range_u32(rng, n);
+            double e_initial = 0.0;
+            if (q.soft) {
+                const double4 s4 = G.site[idx];
+                const double si[3] = {s4.x, s4.y, s4.z};
+                e_initial = serial_energy<DIM>(g, G, P, si, idx, lane);
+            }
+            const double de = -e_initial;  // delta_energy_remove
+            const double p = q.fugacity <= 0.0
+                                 ? 1.0
+                                 : ddiv(dmul((double)n, exp(ddiv(-de, q.temperature))), dmul(q.volume, q.fugacity));
+            if (p > uniform01(rng)) {
+                if (lane == 0) {
+                    // Microstate::remove_body (microstate.rs:917-943): the last body takes idx
+                    const uint32_t last = n - 1;
+                    const uint32_t oc = G.cell_of[idx];
+                    const uint32_t osz = G.size[oc];
+                    for (uint32_t k = 0; k < osz; ++k)
+                        if (G.items[(size_t)oc * G.cap + k] == idx) {
+                            G.items[(size_t)oc * G.cap + k] = G.items[(size_t)oc * G.cap + osz - 1];
+                            break;
+                        }
+                    G.size[oc] = osz - 1;
+                    if (T.tag) tag_free(T, T.tag[idx]);
+                    if (idx != last) {
+                        const uint32_t lc = G.cell_of[last];
+                        const uint32_t lsz = G.size[lc];
+                        for (uint32_t k = 0; k < lsz; ++k)
+                            if (G.items[(size_t)lc * G.cap + k] == last) {
+                                G.items[(size_t)lc * G.cap + k] = idx;
+                                break;
+                            }
+                        A.body_pos[idx] = A.body_pos[last];
+                        G.site[idx] = G.site[last];
+                        G.cell_of[idx] = lc;
+                        if (T.tag) T.tag[idx] = T.tag[last];
+                    }
+                }
+                __syncwarp();
+                n--;
+                ra++;
+            } else {
+                rr++;
+            }
+        }
+        if (A.stats->error_flags) break;
+    }
+    if (lane == 0) {
+        out[0] = ia;
+        out[1] = ir;
+        out[2] = ra;
+        out[3] = rr;
+        out[4] = n;
     }
 }
 
@@ -336,16 +500,30 @@ cudaError_t launch_serial_sphere(int dim, bool soft, const Geometry& g, const Ar
 }
 
 cudaError_t launch_quick_insert(int dim, const Geometry& g, const Arrays& a, const Pair& p, const Launch& l,
-                                const QuickInsertArgs& q, const uint32_t* nc, const double* w, uint32_t cap,
-                                uint32_t* size, uint32_t* items, uint32_t* cell_of, double4* site,
+                                const QuickInsertArgs& q, const BodyTags& tags, const uint32_t* nc, const double* w,
+                                uint32_t cap, uint32_t* size, uint32_t* items, uint32_t* cell_of, double4* site,
                                 unsigned long long* out, cudaStream_t s) {
     const SerialGrid G = make_grid(dim, nc, w, cap, size, items, cell_of, site);
     cudaError_t e = build_grid(dim, g, a, G, q.n0, s);
     if (e != cudaSuccess) return e;
     if (dim == 2)
-        k_quick_insert<2><<<1, 32, 0, s>>>(g, a, G, p, l, q, out);
+        k_quick_insert<2><<<1, 32, 0, s>>>(g, a, G, p, l, q, tags, out);
     else
-        k_quick_insert<3><<<1, 32, 0, s>>>(g, a, G, p, l, q, out);
+        k_quick_insert<3><<<1, 32, 0, s>>>(g, a, G, p, l, q, tags, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_grand_canonical(int dim, const Geometry& g, const Arrays& a, const Pair& p,
+                                   const GrandCanonicalArgs& q, const BodyTags& tags, const uint32_t* nc,
+                                   const double* w, uint32_t cap, uint32_t* size, uint32_t* items, uint32_t* cell_of,
+                                   double4* site, unsigned long long* out, cudaStream_t s) {
+    const SerialGrid G = make_grid(dim, nc, w, cap, size, items, cell_of, site);
+    cudaError_t e = build_grid(dim, g, a, G, q.n0, s);
+    if (e != cudaSuccess) return e;
+    if (dim == 2)
+        k_grand_canonical<2><<<1, 32, 0, s>>>(g, a, G, p, q, tags, out);
+    else
+        k_grand_canonical<3><<<1, 32, 0, s>>>(g, a, G, p, q, tags, out);
     return cudaGetLastError();
 }
 

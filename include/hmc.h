@@ -317,6 +317,25 @@ typedef struct hmc_quick_compress {
 } hmc_quick_compress;
 hmc_status hmc_quick_compress_apply(hmc_system* sys, hmc_quick_compress* qc);
 
+/* GrandCanonical::apply (grand_canonical.rs:49-110), n_trials times in sequence (each a full
+ * apply that increments the substep): a fair coin picks an insertion of a UniformIn body,
+ * accepted when V f exp(-dU/kT) / (N + 1) > u, or a removal of a uniformly chosen body, accepted
+ * when N exp(-dU/kT) / (V f) > u (always when f <= 0); nothing happens when N = 0 and f <= 0.
+ * dU is delta_energy_insert / delta_energy_remove (pairwise_cutoff.rs:1000-1031). Removal is
+ * swap_remove: the last body takes the removed index, and freed tags are reused smallest
+ * first, so GSD frames (tag order) follow the reference. Hard and overlap-penalty spheres. */
+typedef struct hmc_grand_canonical_params {
+    double temperature;   /* IsothermalIsofugacity temperature (> 0) */
+    double fugacity;
+    uint32_t n_trials;
+    uint32_t reserved;
+} hmc_grand_canonical_params;
+typedef struct hmc_insert_remove_count {
+    uint64_t insert_accepted, insert_rejected, remove_accepted, remove_rejected;
+} hmc_insert_remove_count;
+hmc_status hmc_grand_canonical_apply(hmc_system* sys, const hmc_grand_canonical_params* params,
+                                     hmc_insert_remove_count* out);
+
 /* The box edge lengths. hmc_set_box replaces the box as Microstate::clone_with_boundary does
  * (microstate.rs:1529-1565): every body is mapped into the new box (map_point), wrapped, and
  * the checkerboard is rebuilt; HMC_RANGE_TOO_LARGE when the box is too small for the

@@ -100,6 +100,7 @@ def lib():
         L.oracle_quick_insert.argtypes = [C.c_void_p, C.c_uint64, C.c_uint64, _u64p, _u32p, _u64p, _u64p]
         L.oracle_quick_compress.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double, _u32p, _u32p, _dp]
         L.oracle_quick_compress.restype = C.c_int
+        L.oracle_grand_canonical.argtypes = [C.c_void_p, C.c_double, C.c_double, _u64p]
         L.oracle_increment_step.argtypes = [C.c_void_p]
         L.oracle_parallel_sweep.argtypes = [C.c_void_p, C.c_uint32, C.c_double, C.c_double, C.c_double,
                                             _u64p, _u64p]
@@ -368,6 +369,15 @@ class System:
         state["inserted"], state["complete"] = ins.value, comp.value
         self.n = self.n_bodies
         return a.value, r.value
+
+    def grand_canonical(self, temperature, fugacity, n_trials=1):
+        """GrandCanonical::apply n_trials times: (insert accepted, insert rejected, remove
+        accepted, remove rejected)."""
+        c = np.zeros(4, dtype=np.uint64)
+        for _ in range(n_trials):
+            lib().oracle_grand_canonical(self._h, temperature, fugacity, c.ctypes.data_as(_u64p))
+        self.n = self.n_bodies
+        return tuple(int(x) for x in c)
 
     def quick_compress(self, state: dict):
         """QuickCompress::apply; state holds target_volume, maximum_energy_per_site, maximum_delta,

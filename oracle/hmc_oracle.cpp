@@ -27,6 +27,7 @@
 #include <cmath>
 #include <cstring>
 #include <thread>
+#include <queue>
 #include <vector>
 
 namespace {
@@ -1000,6 +1001,61 @@ struct oracle_system {
     double body_range = 1.0;
     double search_range = 1.0;
     Grid grid;
+    // tagged container (microstate.rs:60-123): tags by index, freed tags reused smallest first
+    std::vector<uint64_t> tag;
+    uint64_t tag_bound = 0;
+    std::priority_queue<uint64_t, std::vector<uint64_t>, std::greater<uint64_t>> free_tags;
+    uint64_t take_tag() {
+        if (free_tags.empty()) return tag_bound++;
+        const uint64_t t = free_tags.top();
+        free_tags.pop();
+        return t;
+    }
+    // Microstate::add_body for a point body: body = wrap(x), site = wrap(body), appended.
+    void append_body(const double* x) {
+        double b[3] = {x[0], x[1], x[2]};
+        wrap(dim, L, b);
+        double sv[3] = {b[0], b[1], b[2]};
+        wrap(dim, L, sv);
+        for (int a = 0; a < 3; ++a) body.push_back(b[a]);
+        for (int a = 0; a < 3; ++a) site.push_back(sv[a]);
+        const uint64_t i = n++;
+        const uint64_t c = grid.cell_index(sv);
+        grid.cell_of.push_back(c);
+        grid.cells[c].push_back((uint32_t)i);
+        tag.push_back(take_tag());
+    }
+    // Microstate::remove_body (microstate.rs:917-943) for a point body: swap_remove.
+    void remove_body(uint64_t idx) {
+        const uint64_t last = n - 1;
+        auto drop = [&](uint64_t c, uint64_t v) {
+            auto& cell = grid.cells[c];
+            for (size_t k = 0; k < cell.size(); ++k)
+                if (cell[k] == v) {
+                    cell[k] = cell.back();
+                    cell.pop_back();
+                    return;
+                }
+        };
+        drop(grid.cell_of[idx], idx);
+        free_tags.push(tag[idx]);
+        if (idx != last) {
+            auto& cell = grid.cells[grid.cell_of[last]];
+            for (auto& v : cell)
+                if (v == last) v = (uint32_t)idx;
+            for (int a = 0; a < 3; ++a) {
+                body[3 * idx + a] = body[3 * last + a];
+                site[3 * idx + a] = site[3 * last + a];
+            }
+            grid.cell_of[idx] = grid.cell_of[last];
+            tag[idx] = tag[last];
+        }
+        body.resize(3 * last);
+        site.resize(3 * last);
+        grid.cell_of.resize(last);
+        tag.resize(last);
+        n = last;
+    }
 
     bool hard() const { return interaction != ORACLE_LENNARD_JONES && interaction != ORACLE_OVERLAP_PENALTY; }
     double pk = 10000.0, pdmax = 0.2, pshoulder = 100.0;  // OverlapPenalty
@@ -1294,17 +1350,7 @@ void oracle_quick_insert(oracle_system* s, uint64_t target, uint64_t allowed_ove
             wrap(s->dim, s->L, t);
             const double de = s->site_energy(t, nullptr, UINT64_MAX, cand);
             if (std::isfinite(de)) {
-                // Microstate::add_body: body = wrap(input), site = wrap(body), appended
-                double b[3] = {x[0], x[1], x[2]};
-                wrap(s->dim, s->L, b);
-                double sv[3] = {b[0], b[1], b[2]};
-                wrap(s->dim, s->L, sv);
-                for (int a = 0; a < 3; ++a) s->body.push_back(b[a]);
-                for (int a = 0; a < 3; ++a) s->site.push_back(sv[a]);
-                const uint64_t i = s->n++;
-                const uint64_t c = s->grid.cell_index(sv);
-                s->grid.cell_of.push_back(c);
-                s->grid.cells[c].push_back((uint32_t)i);
+                s->append_body(x);
                 *accepted += 1;
                 *inserted += 1;
                 if (de > 0.0) overlapping += 1;
@@ -1312,6 +1358,55 @@ void oracle_quick_insert(oracle_system* s, uint64_t target, uint64_t allowed_ove
             } else {
                 *rejected += 1;
             }
+        }
+    }
+    s->substep += 1;
+}
+
+// GrandCanonical::apply (grand_canonical.rs:49-110) for point bodies, one trial.
+void oracle_grand_canonical(oracle_system* s, double temperature, double fugacity, uint64_t* counts) {
+    const uint64_t n = s->n;
+    double volume = s->L[0];
+    for (int a = 1; a < s->dim; ++a) volume = volume * s->L[a];
+    Sfc64 rng = make_rng(s->step, s->substep, s->seed, 0);
+    if (n == 0 && fugacity <= 0.0) {
+        s->substep += 1;
+        return;
+    }
+    const bool insert = (int32_t)(uint32_t)rng.next_u64() < 0;  // rand bool: sign of next_u32
+    std::vector<uint32_t> cand;
+    if (insert) {
+        double x[3] = {0.0, 0.0, 0.0};
+        for (int a = 0; a < s->dim; ++a) {
+            const double low = -s->L[a] / 2.0, high = s->L[a] / 2.0;
+            const uint64_t bits = rng.next_u64() >> 12;
+            const double u = bits_to_double(0x3FF0000000000000ULL | bits) - 1.0;
+            x[a] = u * (high - low) + low;
+        }
+        double t[3] = {x[0], x[1], x[2]};
+        wrap(s->dim, s->L, t);
+        const double de = s->site_energy(t, nullptr, UINT64_MAX, cand);
+        if (std::isfinite(de)) {
+            const double p = (volume * fugacity * std::exp(-de / temperature)) / ((double)n + 1.0);
+            if (p > uniform01(rng)) {
+                s->append_body(x);
+                counts[0] += 1;
+            } else {
+                counts[1] += 1;
+            }
+        } else {
+            counts[1] += 1;
+        }
+    } else if (n > 0) {
+        const uint64_t idx = canon_range_u32(rng, (uint32_t)n);
+        const double ei = s->hard() ? 0.0 : s->site_energy(&s->site[3 * idx], nullptr, idx, cand);
+        const double de = -ei;
+        const double p = fugacity <= 0.0 ? 1.0 : ((double)n * std::exp(-de / temperature)) / (volume * fugacity);
+        if (p > uniform01(rng)) {
+            s->remove_body(idx);
+            counts[2] += 1;
+        } else {
+            counts[3] += 1;
         }
     }
     s->substep += 1;
@@ -1383,7 +1478,11 @@ int oracle_quick_compress(oracle_system* s, double target_volume, double maximum
 // quaternion.rs:560-567). pos: n x 3 floats; ori: n x 4 floats (oriented shapes only).
 void oracle_gsd_frame(const oracle_system* s, float* pos, float* ori) {
     const double zero[3] = {0.0, 0.0, 0.0};
-    for (uint64_t i = 0; i < s->n; ++i) {
+    std::vector<uint64_t> order(s->n);  // iter_sites_tag_order
+    for (uint64_t i = 0; i < s->n; ++i) order[i] = i;
+    std::sort(order.begin(), order.end(), [&](uint64_t a, uint64_t b) { return s->tag[a] < s->tag[b]; });
+    for (uint64_t row = 0; row < s->n; ++row) {
+        const uint64_t i = order[row];
         double p[3] = {0.0, 0.0, 0.0};
         const double* b = &s->body[3 * i];
         if (!s->oriented()) {
@@ -1394,10 +1493,10 @@ void oracle_gsd_frame(const oracle_system* s, float* pos, float* ori) {
             const V3 r = versor_rotate(q, zero);
             for (int a = 0; a < 3; ++a) p[a] = b[a] + r.v[a];
             const Quat site = qmul(q, Quat{1.0, 0.0, 0.0, 0.0});
-            ori[4 * i + 0] = (float)site.s;
-            ori[4 * i + 1] = (float)site.x;
-            ori[4 * i + 2] = (float)site.y;
-            ori[4 * i + 3] = (float)site.z;
+            ori[4 * row + 0] = (float)site.s;
+            ori[4 * row + 1] = (float)site.x;
+            ori[4 * row + 2] = (float)site.y;
+            ori[4 * row + 3] = (float)site.z;
         } else {
             const double theta = s->orient[i];
             double sn, cs;
@@ -1407,15 +1506,15 @@ void oracle_gsd_frame(const oracle_system* s, float* pos, float* ori) {
             const double t = theta + 0.0;  // Angle::combine with the site's angle 0
             double hs, hc;
             cr_sincos(t / 2.0, &hs, &hc);
-            ori[4 * i + 0] = (float)hc;
-            ori[4 * i + 1] = (float)(0.0 * hs);
-            ori[4 * i + 2] = (float)(0.0 * hs);
-            ori[4 * i + 3] = (float)(1.0 * hs);
+            ori[4 * row + 0] = (float)hc;
+            ori[4 * row + 1] = (float)(0.0 * hs);
+            ori[4 * row + 2] = (float)(0.0 * hs);
+            ori[4 * row + 3] = (float)(1.0 * hs);
         }
         wrap(s->dim, s->L, p);
-        pos[3 * i + 0] = (float)p[0];
-        pos[3 * i + 1] = (float)p[1];
-        pos[3 * i + 2] = s->dim == 3 ? (float)p[2] : 0.0f;
+        pos[3 * row + 0] = (float)p[0];
+        pos[3 * row + 1] = (float)p[1];
+        pos[3 * row + 2] = s->dim == 3 ? (float)p[2] : 0.0f;
     }
 }
 uint32_t oracle_generate_ghosts(uint32_t dim, const double* L, double range, const double* point,
@@ -1558,6 +1657,9 @@ oracle_system* oracle_system_create(uint32_t dim, const double* L, uint64_t n, c
     }
     s->body.assign(3 * n, 0.0);
     s->site.assign(3 * n, 0.0);
+    s->tag.resize(n);
+    for (uint64_t i = 0; i < n; ++i) s->tag[i] = i;
+    s->tag_bound = n;
     int ol = s->ori_len();
     s->orient.assign((size_t)ol * n, 0.0);
     // Microstate::add_body, microstate.rs:777-835: body = wrap(input), site = wrap(body).

@@ -108,6 +108,9 @@ int oracle_set_box(oracle_system* s, const double* edge_lengths);
 // QuickInsert::apply (quick_insert.rs:228-280); the progress lives in the caller's fields.
 void oracle_quick_insert(oracle_system* s, uint64_t target, uint64_t allowed_overlaps, uint64_t* inserted,
                          uint32_t* complete, uint64_t* accepted, uint64_t* rejected);
+// GrandCanonical::apply (grand_canonical.rs:49-110), one trial; counts[4] (insert accepted,
+// insert rejected, remove accepted, remove rejected) are incremented.
+void oracle_grand_canonical(oracle_system* s, double temperature, double fugacity, uint64_t* counts);
 // QuickCompress::apply (quick_compress.rs:298-383); state 0..3 = Startup, Waiting, Compressing,
 // Complete; boundary: the box Waiting/Complete refer to.
 int oracle_quick_compress(oracle_system* s, double target_volume, double maximum_energy_per_site,

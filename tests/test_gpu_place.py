@@ -178,3 +178,49 @@ def test_placement_large_reaches_target(ctx):
     assert g.volume() == pytest.approx(n / rho, rel=1e-12)
     hard = Microstate(ctx, Periodic(1.0, list(g.box())), g.positions(), PairwiseCutoff(HardSphere(1.0)))
     assert hard.overlap_count() == 0
+
+
+def test_grand_canonical_reference_case(ctx):
+    # grand_canonical.rs tests::hard_spheres_fugacity in a periodic 6 x 6 box
+    from hoomd_rs_b200 import GrandCanonical, IsothermalIsofugacity
+    g = Microstate(ctx, Periodic(1.0, [6.0, 6.0]), [[0.0, 0.0]], PairwiseCutoff(HardSphere(1.0)), capacity=64)
+    qi = QuickInsert(10)
+    for _ in range(100):
+        qi.apply(g)
+        if qi.is_complete():
+            break
+    g.serial_sweep(0.1)
+    assert qi.is_complete() and g.n == 11 and g.total_energy() == 0.0
+    gc = GrandCanonical()
+    c = gc.apply(g, None, IsothermalIsofugacity(1.0, 0.0), n_trials=100)
+    assert g.n == 0 and c.remove_accepted == 11 and c.insert_accepted == 0
+    gc.apply(g, None, IsothermalIsofugacity(1.0, 1.0), n_trials=100)
+    assert g.n > 0 and g.total_energy() == 0.0
+
+
+@pytest.mark.parametrize("soft", [False, True])
+def test_grand_canonical_bit_identical(ctx, soft, tmp_path):
+    from hoomd_rs_b200 import GrandCanonical, IsothermalIsofugacity
+    from hoomd_rs_b200.gsd import GsdFile, HoomdGsdFile
+    n, L = 600, 12.0
+    pos = lattice.cubic_lattice(n, L, 3, 4, jitter=0.01)
+    h = penalty_h() if soft else PairwiseCutoff(HardSphere(1.0))
+    g = Microstate(ctx, Periodic(1.0, [L] * 3), pos, h, seed=17, capacity=4000)
+    o = oracle.System(3, [L] * 3, pos, seed=17, interaction=oracle.OVERLAP_PENALTY if soft else oracle.HARD_SPHERE)
+    gc = GrandCanonical()
+    path = tmp_path / "gc.gsd"
+    f = HoomdGsdFile.create(path)
+    for k, (fug, trials) in enumerate([(0.05, 300), (0.5, 500), (0.0, 200), (2.0, 700), (0.2, 400)]):
+        c = gc.apply(g, None, IsothermalIsofugacity(1.0, fug), n_trials=trials)
+        oc = o.grand_canonical(1.0, fug, trials)
+        assert (c.insert_accepted, c.insert_rejected, c.remove_accepted, c.remove_rejected) == oc, k
+        same_state(g, o)
+        f.append_microstate(g).end()
+        want, _ = o.gsd_frame()  # rows in tag order
+        f.sync_all()
+        got = GsdFile.open(path).iter_arrays(k, "particles/position", np.float32, 3)
+        assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+        g.serial_sweep(0.1)
+        o.serial_sweep(oracle.TRANSLATE, 0.1, 1.0)
+        same_state(g, o)
+    f.close()

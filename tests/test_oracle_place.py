@@ -108,3 +108,34 @@ def test_set_box_maps_bodies():
     want = np.clip(pos * (0.9 * L / L), -0.9 * L / 2, np.nextafter(0.9 * L / 2, -np.inf))
     assert np.allclose(got, want, rtol=0, atol=1e-12)
     assert np.all(np.abs(got) <= 0.9 * L / 2)
+
+
+def test_grand_canonical_hard_spheres_fugacity():
+    # grand_canonical.rs tests::hard_spheres_fugacity, periodic 6 x 6: QuickInsert 10 bodies,
+    # then 100 applies at fugacity 0 remove every body; 100 at fugacity 1 insert some
+    o = oracle.System(2, [6.0, 6.0], [[0.0, 0.0]], diameter=1.0)
+    qi = {"target": 10, "allowed_overlaps": 1, "inserted": 0, "complete": 0}
+    for _ in range(100):
+        o.quick_insert(qi)
+        if qi["complete"]:
+            break
+    o.serial_sweep(oracle.TRANSLATE, 0.1, 1.0)
+    assert qi["complete"] and o.n_bodies == 11 and o.total_energy() == 0.0
+    ia, ir, ra, rr = o.grand_canonical(1.0, 0.0, 100)
+    assert o.n_bodies == 0 and ra == 11 and ia == 0
+    o.grand_canonical(1.0, 1.0, 100)
+    assert o.n_bodies > 0
+    assert o.total_energy() == 0.0
+
+
+def test_removal_reuses_smallest_tag():
+    # the tagged container: swap_remove by index, freed tags reused smallest first; GSD rows
+    # follow tags
+    o = oracle.System(2, [20.0, 20.0], [[float(i) * 2.0 - 9.0, 0.0] for i in range(6)], diameter=1.0)
+    # drive removals at fugacity 0 until two bodies are gone, then insert at high fugacity
+    while o.n_bodies > 4:
+        o.grand_canonical(1.0, 0.0, 1)
+    pos_index = o.state()[0]
+    frame, _ = o.gsd_frame()
+    assert sorted(map(tuple, frame[:, :2].astype(np.float64))) == sorted(map(tuple, pos_index.astype(np.float32)
+                                                                          .astype(np.float64)))
