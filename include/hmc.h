@@ -199,7 +199,8 @@ hmc_status hmc_overlap_check(hmc_system* sys, uint64_t* n_overlaps);
 hmc_status hmc_eval_moves(hmc_system* sys, const hmc_injected_move* moves, uint64_t n, double temperature,
                           uint32_t precision, uint8_t* decisions, uint8_t* rechecked, double* delta_h);
 /* PairwiseCutoff::total_energy (pairwise_cutoff.rs:720-745): the pair energy sum in FP64 for
- * Lennard-Jones; +infinity or 0 for hard shapes (any overlap / none). */
+ * Lennard-Jones and the overlap penalty (summed with atomics: the last bits depend on the
+ * order); +infinity or 0 for hard shapes (any overlap / none). */
 hmc_status hmc_total_energy(hmc_system* sys, double* energy);
 
 /* ---- overlap count into caller buffers, with no device allocation ----
