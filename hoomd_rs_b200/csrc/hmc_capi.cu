@@ -86,6 +86,7 @@ struct hmc_system {
     unsigned long long* host_first_bad = nullptr;  // pinned mirror
     std::vector<void*> allocations;
     bool coop[2] = {true, false};  // warp-cooperative hard-sphere pass: [fp64, fp32]
+    bool pdl = true;                // colour passes launch while the previous one finishes
     uint32_t rounds_guess = 2;      // colour sets enqueued before the sweep's count is known
     // serial sweep grid (allocated on first use)
     uint32_t serial_nc[3] = {0, 0, 0};
@@ -597,6 +598,8 @@ hmc_status hmc_system_create(hmc_context* ctx, const hmc_system_desc* d, const d
     // The hard-sphere colour pass: per lane for FP32 (cheap pair tests), warp-cooperative for
     // FP64 (each pair test costs more than the coordination), as measured on B200;
     // HMC_B200_SWEEP_KERNEL=direct or =coop forces one of them for both precisions.
+    // HMC_B200_PDL=0 launches every colour pass after the previous one has ended.
+    if (const char* pdl = std::getenv("HMC_B200_PDL")) s->pdl = std::strcmp(pdl, "0") != 0;
     if (const char* kern = std::getenv("HMC_B200_SWEEP_KERNEL")) {
         if (std::strcmp(kern, "direct") == 0) s->coop[0] = s->coop[1] = false;
         if (std::strcmp(kern, "coop") == 0) s->coop[0] = s->coop[1] = true;
@@ -807,6 +810,7 @@ hmc_status hmc_sweep(hmc_system* s, const hmc_sweep_params* p, hmc_count* out) {
                 L.round = r;
                 for (uint32_t c = 0; c < colors; ++c) {
                     L.color = c;
+                    L.overlap_previous = (r > 0 || c > 0) && s->pdl ? 1u : 0u;
                     if (s->soft())  // the overlap penalty has no FP32 path: FP64 in both modes
                         HMC_CUDA(launch_sweep_lj(s->dim, fp32 && !s->penalty(), s->geom, s->arr, s->pair, L,
                                                  s->stream));
@@ -1800,7 +1804,8 @@ hmc_status hmc_batch_sweep(hmc_batch* bt, const hmc_sweep_params* params, hmc_co
         auto enqueue = [&](uint32_t r0, uint32_t r1) -> hmc_status {
             for (uint32_t round = r0; round < r1; ++round)
                 for (uint32_t c = 0; c < colors; ++c) {
-                    HMC_CUDA(launch_sweep_batch(bt->dim, fp32, bt->b, bt->arr, c, round, bt->b.color_stride, bt->stream));
+                    HMC_CUDA(launch_sweep_batch(bt->dim, fp32, bt->b, bt->arr, c, round, bt->b.color_stride,
+                                                round > 0 || c > 0, bt->stream));
                     bt->kernel_launches += 1;
                 }
             return HMC_OK;

@@ -119,7 +119,34 @@ struct Launch {
     double max_move;      // Translate maximum distance
     double kt;            // Isothermal temperature
     uint32_t n_bodies;
+    uint32_t overlap_previous;  // 1: the previous launch on the stream is a colour pass of the
+                                // same sweep (this pass may start before it ends)
 };
+
+// Launch configuration of a colour pass: 128 threads per block; overlap = programmatic
+// dependent launch after the previous colour pass of the same sweep (the kernel waits with
+// griddepcontrol.wait before it reads neighbour sites and lets the next pass launch after).
+struct PassLaunch {
+    cudaLaunchConfig_t cfg{};
+    cudaLaunchAttribute attr[1];
+    PassLaunch(uint32_t grid, bool overlap, cudaStream_t s, uint32_t block = 128) {
+        cfg.gridDim = dim3(grid);
+        cfg.blockDim = dim3(block);
+        cfg.stream = s;
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = overlap ? 1 : 0;
+    }
+    PassLaunch(const PassLaunch&) = delete;
+};
+
+// In a colour pass: wait for the previous pass (a no-op without programmatic dependent
+// launch), and allow the next pass to launch. Everything a pass reads before the wait was
+// written before the previous pass began: the rebuild's arrays, and the bodies of the pass's
+// own colour (only the same colour, one round earlier, moved them). At most two passes overlap.
+__device__ __forceinline__ void grid_dependency_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void allow_dependent_launch() { asm volatile("griddepcontrol.launch_dependents;"); }
 
 // One replica of a batch of independent boxes (hmc_batch_*): its box, checkerboard, pair
 // thresholds, counter and place in the batch's concatenated arrays.
@@ -159,7 +186,7 @@ cudaError_t launch_batch_rounds(const Batch& b, Replica* rep, DeviceStats* stats
 // Batches of hard-sphere replicas: the rebuild and the colour pass over all replicas at once.
 cudaError_t launch_rebuild_batch(int dim, const Batch& b, const Arrays& a, uint32_t n, bool write_s, cudaStream_t s);
 cudaError_t launch_sweep_batch(int dim, bool fp32, const Batch& b, const Arrays& a, uint32_t color, uint32_t round,
-                               uint32_t max_active, cudaStream_t s);
+                               uint32_t max_active, bool overlap_previous, cudaStream_t s);
 cudaError_t launch_overlap_batch(int dim, const Batch& b, const Arrays& a, uint32_t n, cudaStream_t s);
 // coop selects the warp-cooperative pass (the per-lane pass otherwise).
 cudaError_t launch_sweep_sphere(int dim, bool fp32, const Geometry& g, const Arrays& a, const Pair& p,

@@ -152,25 +152,31 @@ __device__ __forceinline__ int sphere_overlaps_rows(const Geometry& g, const Arr
     }
 }
 
-// One trial of ParallelSweep::generate_trial_moves and update_bodies for the space with
-// multi-index m. cs is the space-range array of the system (the replica's slice in a batch);
-// slots in it index the cell-ordered arrays of A. Returns true when the move was accepted.
+// The proposal half of a trial (no neighbour data): the stencil's row ranges, the chosen body,
+// the trial site and its FP32 offsets.
+template <int DIM>
+struct SphereProposal {
+    uint32_t a0[kRows<DIM>], a1[kRows<DIM>];
+    uint32_t k;
+    double t[3];
+    float4 t32;
+};
+
 template <int DIM, bool FP32>
-__device__ __forceinline__ bool sphere_trial(const Geometry& g, const Arrays& A, const Pair& P,
-                                             const uint32_t* __restrict__ cs, const uint32_t* m, uint64_t step,
-                                             uint32_t substep, uint32_t seed, double max_move, PairStats& st) {
+__device__ __forceinline__ bool sphere_propose(const Geometry& g, const Arrays& A, const uint32_t* __restrict__ cs,
+                                               const uint32_t* m, uint64_t step, uint32_t substep, uint32_t seed,
+                                               double max_move, SphereProposal<DIM>& pr) {
     const uint32_t cell = cell_index<DIM>(g, m);
     const uint32_t sf = g.shape[DIM - 1], mf = m[DIM - 1];
-    const bool edge = sf > 2 && (mf == 0 || mf + 1 == sf);
     // The stencil depends only on the space: start its loads before the proposal math.
-    uint32_t a0[kRows<DIM>], a1[kRows<DIM>], lo, hi;
+    uint32_t lo, hi;
     row_span(sf, mf, &lo, &hi);
-    load_rows<DIM>(g, cs, m, lo, hi, a0, a1);
+    load_rows<DIM>(g, cs, m, lo, hi, pr.a0, pr.a1);
     const uint32_t start = __ldg(cs + cell);
     const uint32_t count = __ldg(cs + cell + 1) - start;
     Sfc64 rng = make_rng(step, substep, seed, (uint64_t)cell);
-    const uint32_t k = start + canon_range_u32(rng, count);
-    double4 b4 = A.sorted_b[k];
+    pr.k = start + canon_range_u32(rng, count);
+    double4 b4 = A.sorted_b[pr.k];
     double x[3] = {b4.x, b4.y, b4.z};
     double dv[3];
     ball_sample<DIM>(rng, max_move, A.zig_x, A.zig_f, dv);
@@ -178,23 +184,36 @@ __device__ __forceinline__ bool sphere_trial(const Geometry& g, const Arrays& A,
     for (int a = 0; a < DIM; ++a) x[a] = dadd(x[a], dv[a]);
     wrap_inv<DIM>(g.L, g.invL, x);  // W1 = wrap(propose(..))
     uint32_t mt[3];
-    bool same = point_to_space<DIM>(g, x, mt) && cell_index<DIM>(g, mt) == cell;
-    if (!same) return false;
-    double t[3] = {x[0], x[1], DIM == 3 ? x[2] : 0.0};
-    wrap_inv<DIM>(g.L, g.invL, t);  // delta_energy_one wraps the site again: T = wrap(W1)
-    float4 t32 = FP32 ? cell_offsets<DIM>(g, t, m) : make_float4(0.f, 0.f, 0.f, 0.f);
-    int res = sphere_overlaps_rows<DIM, FP32>(g, A, P, t, t32, (int)mf, k, a0, a1, st);
+    if (!(point_to_space<DIM>(g, x, mt) && cell_index<DIM>(g, mt) == cell)) return false;
+    pr.t[0] = x[0];
+    pr.t[1] = x[1];
+    pr.t[2] = DIM == 3 ? x[2] : 0.0;
+    wrap_inv<DIM>(g.L, g.invL, pr.t);  // delta_energy_one wraps the site again: T = wrap(W1)
+    pr.t32 = FP32 ? cell_offsets<DIM>(g, pr.t, m) : make_float4(0.f, 0.f, 0.f, 0.f);
+    return true;
+}
+
+// The decision half: the candidate walk against the current sites, then update_body_properties.
+template <int DIM, bool FP32>
+__device__ __forceinline__ bool sphere_decide(const Geometry& g, const Arrays& A, const Pair& P,
+                                              const uint32_t* __restrict__ cs, const uint32_t* m,
+                                              SphereProposal<DIM>& pr, PairStats& st) {
+    const uint32_t sf = g.shape[DIM - 1], mf = m[DIM - 1];
+    const bool edge = sf > 2 && (mf == 0 || mf + 1 == sf);
+    const uint32_t k = pr.k;
+    const double* t = pr.t;
+    int res = sphere_overlaps_rows<DIM, FP32>(g, A, P, t, pr.t32, (int)mf, k, pr.a0, pr.a1, st);
     if (edge && res != kOverlap) {
         // the wrapped space of each row; its stored fast-axis index is sf-1 (mf = 0) or 0
         // (mf = sf-1), so a virtual mf of sf or -1 gives the cell shift -1 or +1
         const uint32_t wlo = mf == 0 ? sf - 1u : 0u;
-        load_rows<DIM>(g, cs, m, wlo, wlo + 1u, a0, a1);
-        int r2 = sphere_overlaps_rows<DIM, FP32>(g, A, P, t, t32, mf == 0 ? (int)sf : -1, k, a0, a1, st);
+        load_rows<DIM>(g, cs, m, wlo, wlo + 1u, pr.a0, pr.a1);
+        int r2 = sphere_overlaps_rows<DIM, FP32>(g, A, P, t, pr.t32, mf == 0 ? (int)sf : -1, k, pr.a0, pr.a1, st);
         res = r2 == kOverlap ? kOverlap : (res == kUncertain || r2 == kUncertain ? kUncertain : kClear);
     }
     if (res == kUncertain) {
         PairStats st2;  // the fast path already counted its pair checks
-        res = sphere_overlaps_generic<DIM, FP32>(g, A, P, cs, t, t32, m, k, st2) ? kOverlap : kClear;
+        res = sphere_overlaps_generic<DIM, FP32>(g, A, P, cs, t, pr.t32, m, k, st2) ? kOverlap : kClear;
         st.rechecks += st2.rechecks;
         st.max_err = st2.max_err > st.max_err ? st2.max_err : st.max_err;
     }
@@ -207,6 +226,18 @@ __device__ __forceinline__ bool sphere_trial(const Geometry& g, const Arrays& A,
     A.sorted_off[k] = cell_offsets<DIM>(g, sv, m);
     A.body_pos[A.sorted_body[k]] = make_double4(t[0], t[1], t[2], 0.0);
     return true;
+}
+
+// One trial of ParallelSweep::generate_trial_moves and update_bodies for the space with
+// multi-index m. cs is the space-range array of the system (the replica's slice in a batch);
+// slots in it index the cell-ordered arrays of A. Returns true when the move was accepted.
+template <int DIM, bool FP32>
+__device__ __forceinline__ bool sphere_trial(const Geometry& g, const Arrays& A, const Pair& P,
+                                             const uint32_t* __restrict__ cs, const uint32_t* m, uint64_t step,
+                                             uint32_t substep, uint32_t seed, double max_move, PairStats& st) {
+    SphereProposal<DIM> pr;
+    if (!sphere_propose<DIM, FP32>(g, A, cs, m, step, substep, seed, max_move, pr)) return false;
+    return sphere_decide<DIM, FP32>(g, A, P, cs, m, pr, st);
 }
 
 // ---- the colour pass ------------------------------------------------------------------------
@@ -223,9 +254,14 @@ __global__ void __launch_bounds__(128, HMC_SWEEP_MIN_BLOCKS) k_sweep_sphere(Geom
     for (uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x; tid < n_active; tid += stride) {
         uint32_t m[3] = {0, 0, 0};
         unpack_m<DIM>(__ldg(A.color_cells + (size_t)L.color * g.color_stride + tid), m);
-        if (sphere_trial<DIM, FP32>(g, A, P, A.cell_start, m, L.step, L.substep, L.seed, L.max_move, st))
-            n_accepted++;
+        SphereProposal<DIM> pr;
+        const bool valid = sphere_propose<DIM, FP32>(g, A, A.cell_start, m, L.step, L.substep, L.seed, L.max_move, pr);
+        grid_dependency_wait();  // the previous colour's moves are visible from here on
+        allow_dependent_launch();
+        if (valid && sphere_decide<DIM, FP32>(g, A, P, A.cell_start, m, pr, st)) n_accepted++;
     }
+    grid_dependency_wait();
+    allow_dependent_launch();
     flush_stats(A.stats, st, n_accepted);
 }
 
@@ -306,12 +342,13 @@ __global__ void __launch_bounds__(128, HMC_SWEEP_MIN_BLOCKS) k_sweep_sphere_coop
         float4 t32 = make_float4(0.f, 0.f, 0.f, 0.f);
         int res = kFlagOverlap;  // lanes without a trial in the cell count as decided
         bool edge = false, trial = false;
+        uint32_t a0[R], a1[R];
         if (tid < n_active) {
             unpack_m<DIM>(__ldg(A.color_cells + (size_t)L.color * g.color_stride + tid), m);
             cell = cell_index<DIM>(g, m);
             mf = m[DIM - 1];
             edge = sf > 2 && (mf == 0 || mf + 1 == sf);
-            uint32_t a0[R], a1[R], lo, hi;
+            uint32_t lo, hi;
             row_span(sf, mf, &lo, &hi);
             load_rows<DIM>(g, A.cell_start, m, lo, hi, a0, a1);
             const uint32_t start = __ldg(A.cell_start + cell);
@@ -333,32 +370,36 @@ __global__ void __launch_bounds__(128, HMC_SWEEP_MIN_BLOCKS) k_sweep_sphere_coop
                 t[2] = DIM == 3 ? x[2] : 0.0;
                 wrap_inv<DIM>(g.L, g.invL, t);  // delta_energy_one wraps the site again: T = wrap(W1)
                 if (FP32) t32 = cell_offsets<DIM>(g, t, m);
-                res = sphere_rows_head<DIM, FP32>(g, A, P, t, t32, (int)mf, k, a0, a1, kOwnSteps, st);
-                if (res != kFlagOverlap && (res & kFlagMore || edge)) {
-                    // hand the rest to the warp: remaining row ranges, then the wrapped spaces
+            }
+        }
+        grid_dependency_wait();  // the previous colour's moves are visible from here on
+        allow_dependent_launch();
+        if (trial) {
+            res = sphere_rows_head<DIM, FP32>(g, A, P, t, t32, (int)mf, k, a0, a1, kOwnSteps, st);
+            if (res != kFlagOverlap && (res & kFlagMore || edge)) {
+                // hand the rest to the warp: remaining row ranges, then the wrapped spaces
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    s_lo[warp][lane][r] = a0[r] + kOwnSteps;
+                    s_hi[warp][lane][r] = a1[r];
+                }
+                if (edge) {
+                    const uint32_t wlo = mf == 0 ? sf - 1u : 0u;
+                    load_rows<DIM>(g, A.cell_start, m, wlo, wlo + 1u, a0, a1);
 #pragma unroll
                     for (int r = 0; r < R; ++r) {
-                        s_lo[warp][lane][r] = a0[r] + kOwnSteps;
-                        s_hi[warp][lane][r] = a1[r];
+                        s_lo[warp][lane][R + r] = a0[r];
+                        s_hi[warp][lane][R + r] = a1[r];
                     }
-                    if (edge) {
-                        const uint32_t wlo = mf == 0 ? sf - 1u : 0u;
-                        load_rows<DIM>(g, A.cell_start, m, wlo, wlo + 1u, a0, a1);
-#pragma unroll
-                        for (int r = 0; r < R; ++r) {
-                            s_lo[warp][lane][R + r] = a0[r];
-                            s_hi[warp][lane][R + r] = a1[r];
-                        }
-                        res |= kFlagMore;
-                    }
-                    if constexpr (FP32)
-                        s_site[warp][lane] = t32;
-                    else
-                        s_site[warp][lane] = make_double4(t[0], t[1], t[2], 0.0);
-                    s_mf[warp][lane][0] = (int)mf;
-                    s_mf[warp][lane][1] = mf == 0 ? (int)sf : -1;
-                    s_self[warp][lane] = k;
+                    res |= kFlagMore;
                 }
+                if constexpr (FP32)
+                    s_site[warp][lane] = t32;
+                else
+                    s_site[warp][lane] = make_double4(t[0], t[1], t[2], 0.0);
+                s_mf[warp][lane][0] = (int)mf;
+                s_mf[warp][lane][1] = mf == 0 ? (int)sf : -1;
+                s_self[warp][lane] = k;
             }
         }
         const unsigned pending = __ballot_sync(full, (res & kFlagMore) != 0);
@@ -424,6 +465,8 @@ __global__ void __launch_bounds__(128, HMC_SWEEP_MIN_BLOCKS) k_sweep_sphere_coop
         A.sorted_off[k] = cell_offsets<DIM>(g, sv, m);
         A.body_pos[A.sorted_body[k]] = make_double4(t[0], t[1], t[2], 0.0);
     }
+    grid_dependency_wait();
+    allow_dependent_launch();
     flush_stats(A.stats, st, n_accepted);
 }
 
@@ -909,22 +952,31 @@ __global__ void __launch_bounds__(128, HMC_SWEEP_MIN_BLOCKS) k_sweep_batch(Batch
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n_active; base += stride) {
         const uint32_t tid = base + (threadIdx.x & 31u);
-        bool accepted = false;
+        bool accepted = false, valid = false;
         uint32_t r = 0xffffffffu;
+        uint32_t m[3] = {0, 0, 0};
+        SphereProposal<DIM> pr;
         if (tid < n_active) {
             const size_t e = (size_t)color * B.color_stride + tid;
             r = __ldg(B.color_rep + e);
             const Replica& R = B.rep[r];
             if (round < R.rounds) {
-                uint32_t m[3] = {0, 0, 0};
                 unpack_m<DIM>(__ldg(A.color_cells + e), m);
-                accepted = sphere_trial<DIM, FP32>(R.g, A, R.p, A.cell_start + R.cell_base, m, R.step,
-                                                   R.substep + round, R.seed, R.max_move, st);
+                valid = sphere_propose<DIM, FP32>(R.g, A, A.cell_start + R.cell_base, m, R.step, R.substep + round,
+                                                  R.seed, R.max_move, pr);
             }
+        }
+        grid_dependency_wait();  // the previous colour's moves are visible from here on
+        allow_dependent_launch();
+        if (valid) {
+            const Replica& R = B.rep[r];
+            accepted = sphere_decide<DIM, FP32>(R.g, A, R.p, A.cell_start + R.cell_base, m, pr, st);
         }
         n_accepted += accepted;
         add_per_replica(B.accepted, r, accepted);
     }
+    grid_dependency_wait();
+    allow_dependent_launch();
     flush_stats(A.stats, st, n_accepted);
 }
 
@@ -1235,7 +1287,7 @@ cudaError_t launch_rebuild_batch(int dim, const Batch& b, const Arrays& a, uint3
 }
 
 cudaError_t launch_sweep_batch(int dim, bool fp32, const Batch& b, const Arrays& a, uint32_t color, uint32_t round,
-                               uint32_t max_active, cudaStream_t s) {
+                               uint32_t max_active, bool overlap_previous, cudaStream_t s) {
     if (max_active == 0) return cudaSuccess;
     static int max_blocks[2][2] = {{0, 0}, {0, 0}};
     int& mb = max_blocks[dim == 3][fp32];
@@ -1255,18 +1307,12 @@ cudaError_t launch_sweep_batch(int dim, bool fp32, const Batch& b, const Arrays&
     }
     uint32_t grid = blocks_for(max_active, 128);
     if (grid > (uint32_t)mb) grid = (uint32_t)mb;
-    if (dim == 2) {
-        if (fp32)
-            k_sweep_batch<2, true><<<grid, 128, 0, s>>>(b, a, color, round);
-        else
-            k_sweep_batch<2, false><<<grid, 128, 0, s>>>(b, a, color, round);
-    } else {
-        if (fp32)
-            k_sweep_batch<3, true><<<grid, 128, 0, s>>>(b, a, color, round);
-        else
-            k_sweep_batch<3, false><<<grid, 128, 0, s>>>(b, a, color, round);
-    }
-    return cudaGetLastError();
+    PassLaunch pl(grid, overlap_previous, s);
+    if (dim == 2)
+        return fp32 ? cudaLaunchKernelEx(&pl.cfg, k_sweep_batch<2, true>, b, a, color, round)
+                    : cudaLaunchKernelEx(&pl.cfg, k_sweep_batch<2, false>, b, a, color, round);
+    return fp32 ? cudaLaunchKernelEx(&pl.cfg, k_sweep_batch<3, true>, b, a, color, round)
+                : cudaLaunchKernelEx(&pl.cfg, k_sweep_batch<3, false>, b, a, color, round);
 }
 
 cudaError_t launch_batch_rounds(const Batch& b, Replica* rep, DeviceStats* stats, cudaStream_t s) {
@@ -1306,18 +1352,12 @@ cudaError_t launch_sweep_sphere(int dim, bool fp32, const Geometry& g, const Arr
         }
         uint32_t grid = blocks_for(l.n_active, 128);
         if (grid > (uint32_t)cb) grid = (uint32_t)cb;
-        if (dim == 2) {
-            if (fp32)
-                k_sweep_sphere_coop<2, true><<<grid, 128, 0, s>>>(g, a, p, l);
-            else
-                k_sweep_sphere_coop<2, false><<<grid, 128, 0, s>>>(g, a, p, l);
-        } else {
-            if (fp32)
-                k_sweep_sphere_coop<3, true><<<grid, 128, 0, s>>>(g, a, p, l);
-            else
-                k_sweep_sphere_coop<3, false><<<grid, 128, 0, s>>>(g, a, p, l);
-        }
-        return cudaGetLastError();
+        PassLaunch pl(grid, l.overlap_previous != 0, s);
+        if (dim == 2)
+            return fp32 ? cudaLaunchKernelEx(&pl.cfg, k_sweep_sphere_coop<2, true>, g, a, p, l)
+                        : cudaLaunchKernelEx(&pl.cfg, k_sweep_sphere_coop<2, false>, g, a, p, l);
+        return fp32 ? cudaLaunchKernelEx(&pl.cfg, k_sweep_sphere_coop<3, true>, g, a, p, l)
+                    : cudaLaunchKernelEx(&pl.cfg, k_sweep_sphere_coop<3, false>, g, a, p, l);
     }
     // Grid-stride over the colour's list with at most one resident wave of blocks.
     static int max_blocks[2][2] = {{0, 0}, {0, 0}};
@@ -1338,18 +1378,12 @@ cudaError_t launch_sweep_sphere(int dim, bool fp32, const Geometry& g, const Arr
     }
     uint32_t grid = blocks_for(l.n_active, 128);
     if (grid > (uint32_t)mb) grid = (uint32_t)mb;
-    if (dim == 2) {
-        if (fp32)
-            k_sweep_sphere<2, true><<<grid, 128, 0, s>>>(g, a, p, l);
-        else
-            k_sweep_sphere<2, false><<<grid, 128, 0, s>>>(g, a, p, l);
-    } else {
-        if (fp32)
-            k_sweep_sphere<3, true><<<grid, 128, 0, s>>>(g, a, p, l);
-        else
-            k_sweep_sphere<3, false><<<grid, 128, 0, s>>>(g, a, p, l);
-    }
-    return cudaGetLastError();
+    PassLaunch pl(grid, l.overlap_previous != 0, s);
+    if (dim == 2)
+        return fp32 ? cudaLaunchKernelEx(&pl.cfg, k_sweep_sphere<2, true>, g, a, p, l)
+                    : cudaLaunchKernelEx(&pl.cfg, k_sweep_sphere<2, false>, g, a, p, l);
+    return fp32 ? cudaLaunchKernelEx(&pl.cfg, k_sweep_sphere<3, true>, g, a, p, l)
+                : cudaLaunchKernelEx(&pl.cfg, k_sweep_sphere<3, false>, g, a, p, l);
 }
 
 cudaError_t launch_overlap_sphere(int dim, const Geometry& g, const Arrays& a, const Pair& p, uint32_t n,

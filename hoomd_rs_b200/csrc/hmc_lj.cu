@@ -279,6 +279,8 @@ __global__ void __launch_bounds__(128) k_sweep_lj(Geometry g, Arrays A, Pair P, 
         if (!(point_to_space<DIM>(g, x, mt) && cell_index<DIM>(g, mt) == cell)) continue;
         double t[3] = {x[0], x[1], DIM == 3 ? x[2] : 0.0};
         wrap_inv<DIM>(g.L, g.invL, t);
+        grid_dependency_wait();  // the previous colour's moves are visible from here on
+        allow_dependent_launch();
         int decision;
         bool drew = false;
         double u = 0.0;
@@ -325,6 +327,8 @@ __global__ void __launch_bounds__(128) k_sweep_lj(Geometry g, Arrays A, Pair P, 
         }
         __syncwarp();
     }
+    grid_dependency_wait();
+    allow_dependent_launch();
     flush_stats(A.stats, pst, n_accepted);
 }
 
@@ -441,18 +445,12 @@ cudaError_t launch_sweep_lj(int dim, bool fp32, const Geometry& g, const Arrays&
     }
     uint32_t blocks = (l.n_active + 3) / 4;  // four warps (trials) per block
     if (blocks > (uint32_t)max_blocks) blocks = (uint32_t)max_blocks;
-    if (dim == 2) {
-        if (fp32)
-            k_sweep_lj<2, true><<<blocks, 128, 0, s>>>(g, a, p, l);
-        else
-            k_sweep_lj<2, false><<<blocks, 128, 0, s>>>(g, a, p, l);
-    } else {
-        if (fp32)
-            k_sweep_lj<3, true><<<blocks, 128, 0, s>>>(g, a, p, l);
-        else
-            k_sweep_lj<3, false><<<blocks, 128, 0, s>>>(g, a, p, l);
-    }
-    return cudaGetLastError();
+    PassLaunch pl(blocks, l.overlap_previous != 0, s);
+    if (dim == 2)
+        return fp32 ? cudaLaunchKernelEx(&pl.cfg, k_sweep_lj<2, true>, g, a, p, l)
+                    : cudaLaunchKernelEx(&pl.cfg, k_sweep_lj<2, false>, g, a, p, l);
+    return fp32 ? cudaLaunchKernelEx(&pl.cfg, k_sweep_lj<3, true>, g, a, p, l)
+                : cudaLaunchKernelEx(&pl.cfg, k_sweep_lj<3, false>, g, a, p, l);
 }
 
 cudaError_t launch_eval_lj(int dim, bool fp32, const Geometry& g, const Arrays& a, const Pair& p,

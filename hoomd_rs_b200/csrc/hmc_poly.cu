@@ -326,6 +326,8 @@ __global__ void __launch_bounds__(128) k_sweep_poly3(Geometry g, Arrays A, PolyS
         double t[3] = {x[0], x[1], x[2]};
         wrap_inv<3>(g.L, g.invL, t);
         const float4 t32 = FP32 ? cell_offsets<3>(g, t, m) : make_float4(0.f, 0.f, 0.f, 0.f);
+        grid_dependency_wait();  // the previous colour's moves are visible from here on
+        allow_dependent_launch();
         if (poly_overlaps<FP32>(g, A, sh, t, qi, t32, m, k, lane, st)) continue;
         if (lane == 0) {
             n_accepted++;
@@ -341,6 +343,8 @@ __global__ void __launch_bounds__(128) k_sweep_poly3(Geometry g, Arrays A, PolyS
         }
         __syncwarp();
     }
+    grid_dependency_wait();
+    allow_dependent_launch();
     flush_stats(A.stats, st, n_accepted);
 }
 
@@ -452,11 +456,10 @@ cudaError_t launch_sweep_poly(bool fp32, const Geometry& g, const Arrays& a, con
     PolyShape sh{verts, nv, rcut2, rcut2_hi32};
     uint32_t blocks = (l.n_active + 3) / 4;
     if (blocks > (uint32_t)max_blocks) blocks = (uint32_t)max_blocks;
-    if (fp32)
-        k_sweep_poly3<true><<<blocks, 128, 0, s>>>(g, a, sh, l, rotate ? 1u : 0u);
-    else
-        k_sweep_poly3<false><<<blocks, 128, 0, s>>>(g, a, sh, l, rotate ? 1u : 0u);
-    return cudaGetLastError();
+    PassLaunch pl(blocks, l.overlap_previous != 0, s);
+    const uint32_t rot = rotate ? 1u : 0u;
+    return fp32 ? cudaLaunchKernelEx(&pl.cfg, k_sweep_poly3<true>, g, a, sh, l, rot)
+                : cudaLaunchKernelEx(&pl.cfg, k_sweep_poly3<false>, g, a, sh, l, rot);
 }
 
 cudaError_t launch_eval_poly(bool fp32, const Geometry& g, const Arrays& a, const double4* verts, uint32_t nv,

@@ -256,6 +256,8 @@ __global__ void __launch_bounds__(128) k_sweep_poly2(Geometry g, Arrays A, PolyS
         double t[3] = {x[0], x[1], 0.0};
         wrap_inv<2>(g.L, g.invL, t);
         const float4 t32 = FP32 ? cell_offsets<2>(g, t, m) : make_float4(0.f, 0.f, 0.f, 0.f);
+        grid_dependency_wait();  // the previous colour's moves are visible from here on
+        allow_dependent_launch();
         if (poly2_overlaps<FP32, SAT>(g, A, sh, t, ti, t32, m, k, lane, st, &range_error)) continue;
         if (lane == 0) {
             n_accepted++;
@@ -271,6 +273,8 @@ __global__ void __launch_bounds__(128) k_sweep_poly2(Geometry g, Arrays A, PolyS
         }
         __syncwarp();
     }
+    grid_dependency_wait();
+    allow_dependent_launch();
     if (range_error) atomicOr(&A.stats->error_flags, kErrAngleRange);
     flush_stats(A.stats, st, n_accepted);
 }
@@ -362,18 +366,12 @@ cudaError_t launch_sweep_poly2(bool fp32, bool sat, const Geometry& g, const Arr
     uint32_t blocks = (l.n_active + 3) / 4;
     if (blocks > (uint32_t)max_blocks) blocks = (uint32_t)max_blocks;
     const uint32_t rot = rotate ? 1u : 0u;
-    if (fp32) {
-        if (sat)
-            k_sweep_poly2<true, true><<<blocks, 128, 0, s>>>(g, a, sh, l, rot);
-        else
-            k_sweep_poly2<true, false><<<blocks, 128, 0, s>>>(g, a, sh, l, rot);
-    } else {
-        if (sat)
-            k_sweep_poly2<false, true><<<blocks, 128, 0, s>>>(g, a, sh, l, rot);
-        else
-            k_sweep_poly2<false, false><<<blocks, 128, 0, s>>>(g, a, sh, l, rot);
-    }
-    return cudaGetLastError();
+    PassLaunch pl(blocks, l.overlap_previous != 0, s);
+    if (fp32)
+        return sat ? cudaLaunchKernelEx(&pl.cfg, k_sweep_poly2<true, true>, g, a, sh, l, rot)
+                   : cudaLaunchKernelEx(&pl.cfg, k_sweep_poly2<true, false>, g, a, sh, l, rot);
+    return sat ? cudaLaunchKernelEx(&pl.cfg, k_sweep_poly2<false, true>, g, a, sh, l, rot)
+               : cudaLaunchKernelEx(&pl.cfg, k_sweep_poly2<false, false>, g, a, sh, l, rot);
 }
 
 cudaError_t launch_eval_poly2(bool fp32, bool sat, const Geometry& g, const Arrays& a, const double4* verts,
