@@ -811,6 +811,7 @@ hmc_status hmc_sweep(hmc_system* s, const hmc_sweep_params* p, hmc_count* out) {
                 for (uint32_t c = 0; c < colors; ++c) {
                     L.color = c;
                     L.overlap_previous = (r > 0 || c > 0) && s->pdl ? 1u : 0u;
+                    L.early_wait = r == 0 && c == 0 && s->pdl ? 1u : 0u;  // right after the rebuild
                     if (s->soft())  // the overlap penalty has no FP32 path: FP64 in both modes
                         HMC_CUDA(launch_sweep_lj(s->dim, fp32 && !s->penalty(), s->geom, s->arr, s->pair, L,
                                                  s->stream));
@@ -1805,7 +1806,7 @@ hmc_status hmc_batch_sweep(hmc_batch* bt, const hmc_sweep_params* params, hmc_co
             for (uint32_t round = r0; round < r1; ++round)
                 for (uint32_t c = 0; c < colors; ++c) {
                     HMC_CUDA(launch_sweep_batch(bt->dim, fp32, bt->b, bt->arr, c, round, bt->b.color_stride,
-                                                round > 0 || c > 0, bt->stream));
+                                                round > 0 || c > 0, round == 0 && c == 0, bt->stream));
                     bt->kernel_launches += 1;
                 }
             return HMC_OK;

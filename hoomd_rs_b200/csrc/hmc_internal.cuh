@@ -121,6 +121,8 @@ struct Launch {
     uint32_t n_bodies;
     uint32_t overlap_previous;  // 1: the previous launch on the stream is a colour pass of the
                                 // same sweep (this pass may start before it ends)
+    uint32_t early_wait;        // 1: the previous launch is the rebuild's last kernel: launch
+                                // early but wait for it before reading anything
 };
 
 // Launch configuration of a colour pass: 128 threads per block; overlap = programmatic
@@ -186,7 +188,7 @@ cudaError_t launch_batch_rounds(const Batch& b, Replica* rep, DeviceStats* stats
 // Batches of hard-sphere replicas: the rebuild and the colour pass over all replicas at once.
 cudaError_t launch_rebuild_batch(int dim, const Batch& b, const Arrays& a, uint32_t n, bool write_s, cudaStream_t s);
 cudaError_t launch_sweep_batch(int dim, bool fp32, const Batch& b, const Arrays& a, uint32_t color, uint32_t round,
-                               uint32_t max_active, bool overlap_previous, cudaStream_t s);
+                               uint32_t max_active, bool overlap_previous, bool early_wait, cudaStream_t s);
 cudaError_t launch_overlap_batch(int dim, const Batch& b, const Arrays& a, uint32_t n, cudaStream_t s);
 // coop selects the warp-cooperative pass (the per-lane pass otherwise).
 cudaError_t launch_sweep_sphere(int dim, bool fp32, const Geometry& g, const Arrays& a, const Pair& p,

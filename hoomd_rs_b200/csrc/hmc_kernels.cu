@@ -247,6 +247,7 @@ __device__ __forceinline__ bool sphere_trial(const Geometry& g, const Arrays& A,
 // invisible to every other trial of the colour, as in the reference.
 template <int DIM, bool FP32>
 __global__ void __launch_bounds__(128, HMC_SWEEP_MIN_BLOCKS) k_sweep_sphere(Geometry g, Arrays A, Pair P, Launch L) {
+    if (L.early_wait) grid_dependency_wait();  // first pass: the rebuild's arrays are read at once
     uint32_t n_accepted = 0;
     PairStats st;
     const uint32_t stride = gridDim.x * blockDim.x;
@@ -328,6 +329,7 @@ __global__ void __launch_bounds__(128, HMC_SWEEP_MIN_BLOCKS) k_sweep_sphere_coop
     __shared__ int s_mf[4][32][2];
     __shared__ uint32_t s_self[4][32];
     const unsigned full = 0xffffffffu;
+    if (L.early_wait) grid_dependency_wait();  // first pass: the rebuild's arrays are read at once
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     // this lane's range and depth for a trial with R or 2R ranges
     const uint32_t rA = lane % R, dA = lane / R, rB = lane % NR, dB = lane / NR;
@@ -473,6 +475,7 @@ __global__ void __launch_bounds__(128, HMC_SWEEP_MIN_BLOCKS) k_sweep_sphere_coop
 // ---- cell list rebuild -------------------------------------------------------------------
 template <int DIM>
 __global__ void k_bin(Geometry g, Arrays A, uint32_t n) {
+    allow_dependent_launch();  // the scan may launch; it waits for this kernel to end
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double4 b = A.body_pos[i];
@@ -536,6 +539,8 @@ __device__ __forceinline__ uint32_t color_of(const uint32_t* m) {
 // the totals, then each block's prefix.
 __global__ void __launch_bounds__(kScanThreads) k_count_reduce(const uint32_t* __restrict__ count, uint32_t n_cells,
                                                                uint32_t* block_sums) {
+    grid_dependency_wait();  // rebuild kernels run back to back: the previous one has ended here
+    allow_dependent_launch();
     const uint32_t base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
     uint32_t sum = 0;
 #pragma unroll
@@ -553,6 +558,8 @@ __global__ void __launch_bounds__(kScanThreads) k_count_reduce(const uint32_t* _
 }
 
 __global__ void __launch_bounds__(1024) k_count_block_sums(uint32_t* block_sums, uint32_t n_blocks) {
+    grid_dependency_wait();  // rebuild kernels run back to back: the previous one has ended here
+    allow_dependent_launch();
     __shared__ uint32_t warp_sums[32];
     constexpr int items = 8;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -593,6 +600,8 @@ __global__ void __launch_bounds__(1024) k_count_block_sums(uint32_t* block_sums,
 __global__ void __launch_bounds__(kScanThreads) k_count_apply(const uint32_t* __restrict__ count, uint32_t n_cells,
                                                               const uint32_t* __restrict__ block_sums,
                                                               uint32_t* cell_start) {
+    grid_dependency_wait();  // rebuild kernels run back to back: the previous one has ended here
+    allow_dependent_launch();
     const uint32_t base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
     uint32_t v[kScanItems];
     uint32_t sum = 0;
@@ -647,6 +656,8 @@ constexpr int kCellThreads = 1024;
 // colour when it is not empty.
 template <int DIM>
 __global__ void __launch_bounds__(kCellThreads) k_cells(Geometry g, Arrays A) {
+    grid_dependency_wait();  // rebuild kernels run back to back: the previous one has ended here
+    allow_dependent_launch();
     __shared__ uint32_t s_count[8], s_base[8], s_nonempty;
     const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t s = 0, e = 0;
@@ -684,6 +695,8 @@ __global__ void __launch_bounds__(kCellThreads) k_cells(Geometry g, Arrays A) {
 // space corner and the orientation; slot 0 also sets the sweep's rounds.
 template <int DIM, bool WRITE_S>
 __global__ void k_gather(Geometry g, Arrays A, uint32_t n) {
+    grid_dependency_wait();  // rebuild kernels run back to back: the previous one has ended here
+    allow_dependent_launch();
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     if (k == 0) {
@@ -705,6 +718,8 @@ __global__ void k_gather(Geometry g, Arrays A, uint32_t n) {
 }
 
 __global__ void k_scatter(Arrays A, uint32_t n) {
+    grid_dependency_wait();  // rebuild kernels run back to back: the previous one has ended here
+    allow_dependent_launch();
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     A.sorted_body[A.cell_start[A.body_cell[i]] + A.body_rank[i]] = i;
@@ -837,6 +852,7 @@ inline uint32_t blocks_for(T n, uint32_t threads) {
 
 template <int DIM>
 __global__ void k_bin_batch(Batch B, Arrays A, uint32_t n) {
+    allow_dependent_launch();  // the scan may launch; it waits for this kernel to end
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const Replica& R = B.rep[__ldg(B.body_rep + i)];
@@ -862,6 +878,8 @@ __global__ void k_bin_batch(Batch B, Arrays A, uint32_t n) {
 
 template <int DIM>
 __global__ void __launch_bounds__(kCellThreads) k_cells_batch(Batch B, Arrays A) {
+    grid_dependency_wait();  // rebuild kernels run back to back: the previous one has ended here
+    allow_dependent_launch();
     __shared__ uint32_t s_count[8], s_base[8], s_nonempty;
     const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t s = 0, e = 0;
@@ -913,6 +931,8 @@ __global__ void __launch_bounds__(kCellThreads) k_cells_batch(Batch B, Arrays A)
 
 template <int DIM, bool WRITE_S>
 __global__ void k_gather_batch(Batch B, Arrays A, uint32_t n) {
+    grid_dependency_wait();  // rebuild kernels run back to back: the previous one has ended here
+    allow_dependent_launch();
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     const uint32_t i = A.sorted_body[k];
@@ -945,7 +965,8 @@ __device__ __forceinline__ void add_per_replica(unsigned long long* acc, uint32_
 // One colour pass over all replicas that still run round `round` of this sweep.
 template <int DIM, bool FP32>
 __global__ void __launch_bounds__(128, HMC_SWEEP_MIN_BLOCKS) k_sweep_batch(Batch B, Arrays A, uint32_t color,
-                                                                             uint32_t round) {
+                                                                             uint32_t round, uint32_t early_wait) {
+    if (early_wait) grid_dependency_wait();  // first pass: the rebuild's arrays are read at once
     const uint32_t n_active = active_count(A, color, round);
     uint32_t n_accepted = 0;
     PairStats st;
@@ -1218,12 +1239,24 @@ cudaError_t launch_gsd_encode(int dim, int ori_kind, const Geometry& g, const do
 }
 
 namespace {
-cudaError_t launch_count_scan(const Arrays& a, uint32_t n_cells, cudaStream_t s) {
+// Rebuild kernels after the first launch back to back with programmatic dependent launch:
+// each waits for its predecessor at its start, so only the launch latency overlaps.
+template <typename... K, typename... A>
+cudaError_t launch_chained(void (*kernel)(K...), uint32_t grid, uint32_t block, bool chained, cudaStream_t s,
+                           A... args) {
+    PassLaunch pl(grid, chained, s, block);
+    return cudaLaunchKernelEx(&pl.cfg, kernel, args...);
+}
+
+cudaError_t launch_count_scan(const Arrays& a, uint32_t n_cells, cudaStream_t s, bool chained = true) {
     const uint32_t nb = blocks_for(n_cells, kScanTile);
-    k_count_reduce<<<nb, kScanThreads, 0, s>>>(a.cell_count, n_cells, a.block_sums);
-    k_count_block_sums<<<1, 1024, 0, s>>>(a.block_sums, nb);
-    k_count_apply<<<nb, kScanThreads, 0, s>>>(a.cell_count, n_cells, a.block_sums, a.cell_start);
-    return cudaGetLastError();
+    cudaError_t e = launch_chained(k_count_reduce, nb, kScanThreads, chained, s, (const uint32_t*)a.cell_count,
+                                   n_cells, a.block_sums);
+    if (e == cudaSuccess) e = launch_chained(k_count_block_sums, 1, 1024, true, s, a.block_sums, nb);
+    if (e == cudaSuccess)
+        e = launch_chained(k_count_apply, nb, kScanThreads, true, s, (const uint32_t*)a.cell_count, n_cells,
+                           (const uint32_t*)a.block_sums, a.cell_start);
+    return e;
 }
 }  // namespace
 
@@ -1236,24 +1269,16 @@ cudaError_t launch_rebuild(int dim, const Geometry& g, const Arrays& a, uint32_t
         else
             k_bin<3><<<blocks_for(n, 256), 256, 0, s>>>(g, a, n);
     }
-    if ((e = launch_count_scan(a, g.n_cells, s)) != cudaSuccess) return e;
+    if ((e = launch_count_scan(a, g.n_cells, s, n > 0)) != cudaSuccess) return e;
     if (n == 0) return cudaSuccess;
-    k_scatter<<<blocks_for(n, 256), 256, 0, s>>>(a, n);
+    if ((e = launch_chained(k_scatter, blocks_for(n, 256), 256, true, s, a, n)) != cudaSuccess) return e;
     const uint32_t cb = blocks_for(g.n_cells, kCellThreads), gb = blocks_for(n, 256);
     if (dim == 2) {
-        k_cells<2><<<cb, kCellThreads, 0, s>>>(g, a);
-        if (write_s)
-            k_gather<2, true><<<gb, 256, 0, s>>>(g, a, n);
-        else
-            k_gather<2, false><<<gb, 256, 0, s>>>(g, a, n);
-    } else {
-        k_cells<3><<<cb, kCellThreads, 0, s>>>(g, a);
-        if (write_s)
-            k_gather<3, true><<<gb, 256, 0, s>>>(g, a, n);
-        else
-            k_gather<3, false><<<gb, 256, 0, s>>>(g, a, n);
+        if ((e = launch_chained(k_cells<2>, cb, kCellThreads, true, s, g, a)) != cudaSuccess) return e;
+        return launch_chained(write_s ? k_gather<2, true> : k_gather<2, false>, gb, 256, true, s, g, a, n);
     }
-    return cudaGetLastError();
+    if ((e = launch_chained(k_cells<3>, cb, kCellThreads, true, s, g, a)) != cudaSuccess) return e;
+    return launch_chained(write_s ? k_gather<3, true> : k_gather<3, false>, gb, 256, true, s, g, a, n);
 }
 
 cudaError_t launch_rebuild_batch(int dim, const Batch& b, const Arrays& a, uint32_t n, bool write_s, cudaStream_t s) {
@@ -1266,28 +1291,20 @@ cudaError_t launch_rebuild_batch(int dim, const Batch& b, const Arrays& a, uint3
         else
             k_bin_batch<3><<<blocks_for(n, 256), 256, 0, s>>>(b, a, n);
     }
-    if ((e = launch_count_scan(a, b.n_cells, s)) != cudaSuccess) return e;
+    if ((e = launch_count_scan(a, b.n_cells, s, n > 0)) != cudaSuccess) return e;
     if (n == 0) return cudaSuccess;
-    k_scatter<<<blocks_for(n, 256), 256, 0, s>>>(a, n);
+    if ((e = launch_chained(k_scatter, blocks_for(n, 256), 256, true, s, a, n)) != cudaSuccess) return e;
     const uint32_t cb = blocks_for(b.n_cells, kCellThreads), gb = blocks_for(n, 256);
     if (dim == 2) {
-        k_cells_batch<2><<<cb, kCellThreads, 0, s>>>(b, a);
-        if (write_s)
-            k_gather_batch<2, true><<<gb, 256, 0, s>>>(b, a, n);
-        else
-            k_gather_batch<2, false><<<gb, 256, 0, s>>>(b, a, n);
-    } else {
-        k_cells_batch<3><<<cb, kCellThreads, 0, s>>>(b, a);
-        if (write_s)
-            k_gather_batch<3, true><<<gb, 256, 0, s>>>(b, a, n);
-        else
-            k_gather_batch<3, false><<<gb, 256, 0, s>>>(b, a, n);
+        if ((e = launch_chained(k_cells_batch<2>, cb, kCellThreads, true, s, b, a)) != cudaSuccess) return e;
+        return launch_chained(write_s ? k_gather_batch<2, true> : k_gather_batch<2, false>, gb, 256, true, s, b, a, n);
     }
-    return cudaGetLastError();
+    if ((e = launch_chained(k_cells_batch<3>, cb, kCellThreads, true, s, b, a)) != cudaSuccess) return e;
+    return launch_chained(write_s ? k_gather_batch<3, true> : k_gather_batch<3, false>, gb, 256, true, s, b, a, n);
 }
 
 cudaError_t launch_sweep_batch(int dim, bool fp32, const Batch& b, const Arrays& a, uint32_t color, uint32_t round,
-                               uint32_t max_active, bool overlap_previous, cudaStream_t s) {
+                               uint32_t max_active, bool overlap_previous, bool early_wait, cudaStream_t s) {
     if (max_active == 0) return cudaSuccess;
     static int max_blocks[2][2] = {{0, 0}, {0, 0}};
     int& mb = max_blocks[dim == 3][fp32];
@@ -1307,12 +1324,13 @@ cudaError_t launch_sweep_batch(int dim, bool fp32, const Batch& b, const Arrays&
     }
     uint32_t grid = blocks_for(max_active, 128);
     if (grid > (uint32_t)mb) grid = (uint32_t)mb;
-    PassLaunch pl(grid, overlap_previous, s);
+    PassLaunch pl(grid, overlap_previous || early_wait, s);
+    const uint32_t ew = early_wait ? 1u : 0u;
     if (dim == 2)
-        return fp32 ? cudaLaunchKernelEx(&pl.cfg, k_sweep_batch<2, true>, b, a, color, round)
-                    : cudaLaunchKernelEx(&pl.cfg, k_sweep_batch<2, false>, b, a, color, round);
-    return fp32 ? cudaLaunchKernelEx(&pl.cfg, k_sweep_batch<3, true>, b, a, color, round)
-                : cudaLaunchKernelEx(&pl.cfg, k_sweep_batch<3, false>, b, a, color, round);
+        return fp32 ? cudaLaunchKernelEx(&pl.cfg, k_sweep_batch<2, true>, b, a, color, round, ew)
+                    : cudaLaunchKernelEx(&pl.cfg, k_sweep_batch<2, false>, b, a, color, round, ew);
+    return fp32 ? cudaLaunchKernelEx(&pl.cfg, k_sweep_batch<3, true>, b, a, color, round, ew)
+                : cudaLaunchKernelEx(&pl.cfg, k_sweep_batch<3, false>, b, a, color, round, ew);
 }
 
 cudaError_t launch_batch_rounds(const Batch& b, Replica* rep, DeviceStats* stats, cudaStream_t s) {
@@ -1352,7 +1370,7 @@ cudaError_t launch_sweep_sphere(int dim, bool fp32, const Geometry& g, const Arr
         }
         uint32_t grid = blocks_for(l.n_active, 128);
         if (grid > (uint32_t)cb) grid = (uint32_t)cb;
-        PassLaunch pl(grid, l.overlap_previous != 0, s);
+        PassLaunch pl(grid, l.overlap_previous != 0 || l.early_wait != 0, s);
         if (dim == 2)
             return fp32 ? cudaLaunchKernelEx(&pl.cfg, k_sweep_sphere_coop<2, true>, g, a, p, l)
                         : cudaLaunchKernelEx(&pl.cfg, k_sweep_sphere_coop<2, false>, g, a, p, l);
@@ -1378,7 +1396,7 @@ cudaError_t launch_sweep_sphere(int dim, bool fp32, const Geometry& g, const Arr
     }
     uint32_t grid = blocks_for(l.n_active, 128);
     if (grid > (uint32_t)mb) grid = (uint32_t)mb;
-    PassLaunch pl(grid, l.overlap_previous != 0, s);
+    PassLaunch pl(grid, l.overlap_previous != 0 || l.early_wait != 0, s);
     if (dim == 2)
         return fp32 ? cudaLaunchKernelEx(&pl.cfg, k_sweep_sphere<2, true>, g, a, p, l)
                     : cudaLaunchKernelEx(&pl.cfg, k_sweep_sphere<2, false>, g, a, p, l);

@@ -251,6 +251,7 @@ __device__ __forceinline__ int decide32(const Sums32& s, double kt, Sfc64& rng, 
 
 template <int DIM, bool FP32>
 __global__ void __launch_bounds__(128) k_sweep_lj(Geometry g, Arrays A, Pair P, Launch L) {
+    if (L.early_wait) grid_dependency_wait();  // first pass: the rebuild's arrays are read at once
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t n_warps = (gridDim.x * blockDim.x) >> 5;
@@ -445,7 +446,7 @@ cudaError_t launch_sweep_lj(int dim, bool fp32, const Geometry& g, const Arrays&
     }
     uint32_t blocks = (l.n_active + 3) / 4;  // four warps (trials) per block
     if (blocks > (uint32_t)max_blocks) blocks = (uint32_t)max_blocks;
-    PassLaunch pl(blocks, l.overlap_previous != 0, s);
+    PassLaunch pl(blocks, l.overlap_previous != 0 || l.early_wait != 0, s);
     if (dim == 2)
         return fp32 ? cudaLaunchKernelEx(&pl.cfg, k_sweep_lj<2, true>, g, a, p, l)
                     : cudaLaunchKernelEx(&pl.cfg, k_sweep_lj<2, false>, g, a, p, l);

@@ -295,6 +295,7 @@ __device__ __forceinline__ bool poly_overlaps(const Geometry& g, const Arrays& A
 
 template <bool FP32>
 __global__ void __launch_bounds__(128) k_sweep_poly3(Geometry g, Arrays A, PolyShape sh, Launch L, uint32_t rotate) {
+    if (L.early_wait) grid_dependency_wait();  // first pass: the rebuild's arrays are read at once
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t n_warps = (gridDim.x * blockDim.x) >> 5;
@@ -456,7 +457,7 @@ cudaError_t launch_sweep_poly(bool fp32, const Geometry& g, const Arrays& a, con
     PolyShape sh{verts, nv, rcut2, rcut2_hi32};
     uint32_t blocks = (l.n_active + 3) / 4;
     if (blocks > (uint32_t)max_blocks) blocks = (uint32_t)max_blocks;
-    PassLaunch pl(blocks, l.overlap_previous != 0, s);
+    PassLaunch pl(blocks, l.overlap_previous != 0 || l.early_wait != 0, s);
     const uint32_t rot = rotate ? 1u : 0u;
     return fp32 ? cudaLaunchKernelEx(&pl.cfg, k_sweep_poly3<true>, g, a, sh, l, rot)
                 : cudaLaunchKernelEx(&pl.cfg, k_sweep_poly3<false>, g, a, sh, l, rot);

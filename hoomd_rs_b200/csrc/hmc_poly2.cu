@@ -222,6 +222,7 @@ __device__ __forceinline__ bool poly2_overlaps(const Geometry& g, const Arrays& 
 
 template <bool FP32, bool SAT>
 __global__ void __launch_bounds__(128) k_sweep_poly2(Geometry g, Arrays A, PolyShape2 sh, Launch L, uint32_t rotate) {
+    if (L.early_wait) grid_dependency_wait();  // first pass: the rebuild's arrays are read at once
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t n_warps = (gridDim.x * blockDim.x) >> 5;
@@ -366,7 +367,7 @@ cudaError_t launch_sweep_poly2(bool fp32, bool sat, const Geometry& g, const Arr
     uint32_t blocks = (l.n_active + 3) / 4;
     if (blocks > (uint32_t)max_blocks) blocks = (uint32_t)max_blocks;
     const uint32_t rot = rotate ? 1u : 0u;
-    PassLaunch pl(blocks, l.overlap_previous != 0, s);
+    PassLaunch pl(blocks, l.overlap_previous != 0 || l.early_wait != 0, s);
     if (fp32)
         return sat ? cudaLaunchKernelEx(&pl.cfg, k_sweep_poly2<true, true>, g, a, sh, l, rot)
                    : cudaLaunchKernelEx(&pl.cfg, k_sweep_poly2<true, false>, g, a, sh, l, rot);
