@@ -43,6 +43,21 @@ TARGET_ACCEPTANCE = 0.30
 SPHERE_PASS_DRAM_BYTES = 30.53e6
 
 
+def aggregate_over_ranks(elapsed, units, world, device):
+    """(max of `elapsed` over ranks, sum of `units` over ranks). The whole-job rate is the sum
+    of the units all ranks processed over the slowest rank's time. Every rank calls it at the
+    same point (two collectives in the same order); world == 1 needs no process group."""
+    if world <= 1:
+        return float(elapsed), int(units)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(elapsed)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    n = torch.tensor([float(units)], dtype=torch.float64, device=device)
+    dist.all_reduce(n, op=dist.ReduceOp.SUM)
+    return float(t.item()), int(n.item())
+
+
 def workload_config(d, extra=None):
     cfg = {"workload": "3-D hard spheres, N=2^20, packing fraction 0.50, periodic cube, FCC start + 0.01 jitter, "
                        "translation moves tuned by Tune (target 0.30, hmc_tune), one ParallelSweep per step",
@@ -532,15 +547,7 @@ def main():
     overlaps = a.overlap_count()
 
     # whole-job aggregate: units of all ranks over the slowest rank's device time
-    t_max = ra["ms"]
-    trials_all = ra["trials"]
-    if world > 1:
-        t = torch.tensor([ra["ms"]], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_max = float(t.item())
-        n = torch.tensor([ra["trials"]], dtype=torch.float64, device="cuda")
-        dist.all_reduce(n, op=dist.ReduceOp.SUM)
-        trials_all = int(n.item())
+    t_max, trials_all = aggregate_over_ranks(ra["ms"], ra["trials"], world, "cuda")
     value = trials_all / (t_max / 1e3)
     fp64_value = rb["trials"] / (rb["ms"] / 1e3)
 
@@ -573,11 +580,8 @@ def main():
         t_e2e += time.perf_counter() - t0
         e2e_trials += c.total()
         host_in, host_out = host_out, host_in
-    e2e_value = e2e_trials / t_e2e
-    if world > 1:
-        t = torch.tensor([t_e2e], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_value = e2e_trials * world / float(t.item())
+    t_e2e_max, e2e_trials_all = aggregate_over_ranks(t_e2e, e2e_trials, world, "cuda")
+    e2e_value = e2e_trials_all / t_e2e_max
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
