@@ -96,6 +96,15 @@ __device__ __forceinline__ bool sphere_overlaps_generic(const Geometry& g, const
 // when no pair overlaps for certain but some pair lies inside the FP32 bound; the caller
 // then decides with the generic walk, which rechecks those pairs in FP64.
 
+// The uncertain-pair fallback out of line (rare; keeps the batch pass's code small).
+template <int DIM, bool FP32>
+__device__ __noinline__ bool sphere_overlaps_generic_outlined(const Geometry& g, const Arrays& A, const Pair& P,
+                                                              const uint32_t* __restrict__ cs, const double* t,
+                                                              float4 t32, const uint32_t* m, uint32_t self,
+                                                              PairStats& st) {
+    return sphere_overlaps_generic<DIM, FP32>(g, A, P, cs, t, t32, m, self, st);
+}
+
 template <int DIM, bool FP32>
 __device__ __forceinline__ int sphere_overlaps_rows(const Geometry& g, const Arrays& A, const Pair& P,
                                                     const double* t, float4 t32, int mf, uint32_t self,
@@ -194,7 +203,7 @@ __device__ __forceinline__ bool sphere_propose(const Geometry& g, const Arrays& 
 }
 
 // The decision half: the candidate walk against the current sites, then update_body_properties.
-template <int DIM, bool FP32>
+template <int DIM, bool FP32, bool OUTLINE = false>
 __device__ __forceinline__ bool sphere_decide(const Geometry& g, const Arrays& A, const Pair& P,
                                               const uint32_t* __restrict__ cs, const uint32_t* m,
                                               SphereProposal<DIM>& pr, PairStats& st) {
@@ -213,7 +222,9 @@ __device__ __forceinline__ bool sphere_decide(const Geometry& g, const Arrays& A
     }
     if (res == kUncertain) {
         PairStats st2;  // the fast path already counted its pair checks
-        res = sphere_overlaps_generic<DIM, FP32>(g, A, P, cs, t, pr.t32, m, k, st2) ? kOverlap : kClear;
+        const bool ov = OUTLINE ? sphere_overlaps_generic_outlined<DIM, FP32>(g, A, P, cs, t, pr.t32, m, k, st2)
+                                : sphere_overlaps_generic<DIM, FP32>(g, A, P, cs, t, pr.t32, m, k, st2);
+        res = ov ? kOverlap : kClear;
         st.rechecks += st2.rechecks;
         st.max_err = st2.max_err > st.max_err ? st2.max_err : st.max_err;
     }
@@ -991,7 +1002,7 @@ __global__ void __launch_bounds__(128, HMC_SWEEP_MIN_BLOCKS) k_sweep_batch(Batch
         allow_dependent_launch();
         if (valid) {
             const Replica& R = B.rep[r];
-            accepted = sphere_decide<DIM, FP32>(R.g, A, R.p, A.cell_start + R.cell_base, m, pr, st);
+            accepted = sphere_decide<DIM, FP32, true>(R.g, A, R.p, A.cell_start + R.cell_base, m, pr, st);
         }
         n_accepted += accepted;
         add_per_replica(B.accepted, r, accepted);
