@@ -203,7 +203,9 @@ __device__ __forceinline__ bool sphere_propose(const Geometry& g, const Arrays& 
 }
 
 // The decision half: the candidate walk against the current sites, then update_body_properties.
-template <int DIM, bool FP32, bool OUTLINE = false>
+// COMPACT (the replica batch pass, whose larger code misses in the instruction cache): one
+// copy of the row walk for both segments and the rare uncertain-pair fallback out of line.
+template <int DIM, bool FP32, bool COMPACT = false>
 __device__ __forceinline__ bool sphere_decide(const Geometry& g, const Arrays& A, const Pair& P,
                                               const uint32_t* __restrict__ cs, const uint32_t* m,
                                               SphereProposal<DIM>& pr, PairStats& st) {
@@ -211,18 +213,36 @@ __device__ __forceinline__ bool sphere_decide(const Geometry& g, const Arrays& A
     const bool edge = sf > 2 && (mf == 0 || mf + 1 == sf);
     const uint32_t k = pr.k;
     const double* t = pr.t;
-    int res = sphere_overlaps_rows<DIM, FP32>(g, A, P, t, pr.t32, (int)mf, k, pr.a0, pr.a1, st);
-    if (edge && res != kOverlap) {
-        // the wrapped space of each row; its stored fast-axis index is sf-1 (mf = 0) or 0
-        // (mf = sf-1), so a virtual mf of sf or -1 gives the cell shift -1 or +1
-        const uint32_t wlo = mf == 0 ? sf - 1u : 0u;
-        load_rows<DIM>(g, cs, m, wlo, wlo + 1u, pr.a0, pr.a1);
-        int r2 = sphere_overlaps_rows<DIM, FP32>(g, A, P, t, pr.t32, mf == 0 ? (int)sf : -1, k, pr.a0, pr.a1, st);
-        res = r2 == kOverlap ? kOverlap : (res == kUncertain || r2 == kUncertain ? kUncertain : kClear);
+    // At a fast-axis end, the wrapped space of each row follows; its stored fast-axis index is
+    // sf-1 (mf = 0) or 0 (mf = sf-1), so a virtual mf of sf or -1 gives the cell shift -1 or +1.
+    int res;
+    if constexpr (COMPACT) {
+        // one copy of the row walk for both segments (smaller code)
+        res = kClear;
+        int mfx = (int)mf;
+#pragma unroll 1
+        for (int seg = 0; seg < (edge ? 2 : 1); ++seg) {
+            if (seg == 1) {
+                const uint32_t wlo = mf == 0 ? sf - 1u : 0u;
+                load_rows<DIM>(g, cs, m, wlo, wlo + 1u, pr.a0, pr.a1);
+                mfx = mf == 0 ? (int)sf : -1;
+            }
+            const int r2 = sphere_overlaps_rows<DIM, FP32>(g, A, P, t, pr.t32, mfx, k, pr.a0, pr.a1, st);
+            res = r2 == kOverlap ? kOverlap : (res == kUncertain || r2 == kUncertain ? kUncertain : kClear);
+            if (res == kOverlap) break;
+        }
+    } else {
+        res = sphere_overlaps_rows<DIM, FP32>(g, A, P, t, pr.t32, (int)mf, k, pr.a0, pr.a1, st);
+        if (edge && res != kOverlap) {
+            const uint32_t wlo = mf == 0 ? sf - 1u : 0u;
+            load_rows<DIM>(g, cs, m, wlo, wlo + 1u, pr.a0, pr.a1);
+            int r2 = sphere_overlaps_rows<DIM, FP32>(g, A, P, t, pr.t32, mf == 0 ? (int)sf : -1, k, pr.a0, pr.a1, st);
+            res = r2 == kOverlap ? kOverlap : (res == kUncertain || r2 == kUncertain ? kUncertain : kClear);
+        }
     }
     if (res == kUncertain) {
         PairStats st2;  // the fast path already counted its pair checks
-        const bool ov = OUTLINE ? sphere_overlaps_generic_outlined<DIM, FP32>(g, A, P, cs, t, pr.t32, m, k, st2)
+        const bool ov = COMPACT ? sphere_overlaps_generic_outlined<DIM, FP32>(g, A, P, cs, t, pr.t32, m, k, st2)
                                 : sphere_overlaps_generic<DIM, FP32>(g, A, P, cs, t, pr.t32, m, k, st2);
         res = ov ? kOverlap : kClear;
         st.rechecks += st2.rechecks;
