@@ -102,3 +102,17 @@ def test_delta_energy_consistent_with_total_energy(ctx):
         e1 = g.total_energy()
         g.set_state(pos, 0, 0)
         assert math.isclose(dh[0], e1 - e0, rel_tol=1e-9, abs_tol=1e-9)
+
+
+@pytest.mark.parametrize("precision", [FP64, FP32_RECHECK])
+def test_lj_overlapping_passes_equal_serialised_passes(ctx, monkeypatch, precision):
+    # colour passes launched while the previous one finishes give the serialised trajectory
+    pos, L = lattice.lennard_jones_box(1 << 16, 0.8, 3, 0x5EED0005)
+    monkeypatch.setenv("HMC_B200_PDL", "1")
+    a = Microstate(ctx, Periodic(2.5, [L] * 3), pos, lj(), seed=0x5EED0005)
+    monkeypatch.setenv("HMC_B200_PDL", "0")
+    b = Microstate(ctx, Periodic(2.5, [L] * 3), pos, lj(), seed=0x5EED0005)
+    ca = a.sweep(TRANSLATE, 0.1, 1.0, precision, n_sweeps=3, increment_step=True)
+    cb = b.sweep(TRANSLATE, 0.1, 1.0, precision, n_sweeps=3, increment_step=True)
+    assert (ca.accepted, ca.rejected) == (cb.accepted, cb.rejected)
+    assert np.array_equal(a.positions(), b.positions())

@@ -121,3 +121,22 @@ def test_planted_cube_overlap(ctx):
     pos = np.array([[0.0, 0.0, 0.0], [0.9, 0.2, 0.0], [5.0, 5.0, 5.0]])
     g, o, _ = cube_systems(ctx, 3, 0, 1, positions=pos, L=14.0)
     assert g.overlap_count() == o.overlap_count() == 1
+
+
+@pytest.mark.parametrize("precision", [FP64, FP32_RECHECK])
+def test_cube_overlapping_passes_equal_serialised_passes(ctx, monkeypatch, precision):
+    # colour passes launched while the previous one finishes give the serialised trajectory
+    n, phi = 1 << 15, 0.55
+    L = (n / phi) ** (1.0 / 3.0)
+    pos = lattice.cubic_lattice(n, L, 3, 0x5EED0003, jitter=0.0)
+    h = PairwiseCutoff(HardShape(ConvexPolyhedron.with_vertices(CUBE)))
+    monkeypatch.setenv("HMC_B200_PDL", "1")
+    a = Microstate(ctx, Periodic(math.sqrt(3.0), [L] * 3), pos, h, seed=0x5EED0003)
+    monkeypatch.setenv("HMC_B200_PDL", "0")
+    b = Microstate(ctx, Periodic(math.sqrt(3.0), [L] * 3), pos, h, seed=0x5EED0003)
+    for move, maximum in [(TRANSLATE, 0.08), (ROTATE, 0.1), (TRANSLATE, 0.08)]:
+        ca = a.sweep(move, maximum, 1.0, precision, n_sweeps=1, increment_step=True)
+        cb = b.sweep(move, maximum, 1.0, precision, n_sweeps=1, increment_step=True)
+        assert (ca.accepted, ca.rejected) == (cb.accepted, cb.rejected)
+    assert np.array_equal(a.positions(), b.positions())
+    assert np.array_equal(a.orientations(), b.orientations())

@@ -172,6 +172,23 @@ def test_full_size_fp32_recheck_equals_fp64(ctx):
     assert cb.rechecks < 1e-3 * cb.pair_checks
 
 
+@pytest.mark.parametrize("precision", [FP64, FP32_RECHECK])
+def test_overlapping_passes_equal_serialised_passes(ctx, monkeypatch, precision):
+    # 2^20 spheres: colour passes launched while the previous pass finishes (programmatic
+    # dependent launch) give the trajectory of passes launched one after another.
+    pos, L = lattice.hard_sphere_box(1 << 20, 0.50, 3, 0x5EED0002)
+    h = PairwiseCutoff(HardSphere(1.0))
+    monkeypatch.setenv("HMC_B200_PDL", "1")
+    a = Microstate(ctx, Periodic(1.0, [L] * 3), pos, h, seed=0x5EED0002)
+    monkeypatch.setenv("HMC_B200_PDL", "0")
+    b = Microstate(ctx, Periodic(1.0, [L] * 3), pos, h, seed=0x5EED0002)
+    ca = a.sweep(TRANSLATE, 0.2, 1.0, precision, n_sweeps=4, increment_step=True)
+    cb = b.sweep(TRANSLATE, 0.2, 1.0, precision, n_sweeps=4, increment_step=True)
+    assert (ca.accepted, ca.rejected) == (cb.accepted, cb.rejected)
+    assert np.array_equal(a.positions(), b.positions())
+    assert a.overlap_count() == 0
+
+
 def test_overlap_check_finds_planted_overlap(ctx):
     pos = np.array([[0.0, 0.0, 0.0], [0.5, 0.0, 0.0], [3.0, 3.0, 3.0], [-4.9, 0.0, 0.0], [4.6, 0.0, 0.0]])
     h = PairwiseCutoff(HardSphere(1.0))
