@@ -514,3 +514,24 @@ def test_upgrade_minor_version_on_write(tmp_path):
     assert struct.unpack_from("=I", path.read_bytes(), 44)[0] == 2 << 16
     GsdFile.open(path, Mode.WRITE).close()
     assert struct.unpack_from("=I", path.read_bytes(), 44)[0] == (2 << 16) | 1
+
+
+def test_large_chunks_byte_identical(tmp_path):
+    # chunks of 40 MB and 24 MB go to the file in parallel pieces; the bytes match one write
+    rng = np.random.default_rng(11)
+    path = tmp_path / "big.gsd"
+    product = GsdFile.create(path, "app", "schema", (1, 0))
+    oracle = O.Writer("app", "schema", (1, 0))
+    for frame in range(3):
+        a = rng.random((5_000_000, 1))
+        b = rng.integers(0, 1 << 30, size=(2_000_000, 3)).astype(np.uint32)
+        product.write_scalars("a", a.reshape(-1))
+        oracle.write_scalars("a", a.reshape(-1), O.F64)
+        product.write_string("note", f"frame {frame}")
+        oracle.write_string("note", f"frame {frame}")
+        product.write_arrays("b", b)
+        oracle.write_arrays("b", b, O.U32)
+        product.end_frame()
+        oracle.end_frame()
+    product.close()
+    assert path.read_bytes() == oracle.close()
