@@ -153,6 +153,17 @@ void dfree(hmc_system* s, T** p) {
     *p = nullptr;
 }
 
+// HMC_B200_FP32_BAND_SCALE (> 1) widens the FP32 error bounds (the band of FP32 distances
+// decided in FP64 for shapes, the LJ displacement error): decisions do not change, and the
+// recheck paths become common enough to test.
+double fp32_band_scale() {
+    if (const char* e = std::getenv("HMC_B200_FP32_BAND_SCALE")) {
+        const double f = std::atof(e);
+        if (f > 1.0 && f < 1e12) return f;
+    }
+    return 1.0;
+}
+
 // The forward-error bound of the FP32 pair test for hard spheres. With u32 = 2^-24 and
 // u64 = 2^-53, a stored FP32 offset differs from the exact offset of the FP64 site by at
 // most u32*w + 4*u64*(L + w); the FP32 displacement of two offsets plus a cell shift
@@ -175,12 +186,7 @@ void sphere_bound_for(int dim, const Geometry& geom, Pair& pair) {
     double b32 = 2.0 * E * rd * dmax + dim * E * E + dim * u32 * dmax * dmax;
     double b64 = 6.0 * u64 * (Lmax + wmax) * rd * dmax + dim * u64 * dmax * dmax;
     double B = 2.0 * (b32 + b64);
-    // HMC_B200_FP32_BAND_SCALE (>= 1) widens the band of FP32 distances that are decided in
-    // FP64. Decisions do not change; it makes the recheck path common enough to test.
-    if (const char* e = std::getenv("HMC_B200_FP32_BAND_SCALE")) {
-        double f = std::atof(e);
-        if (f > 1.0 && f < 1e12) B *= f;
-    }
+    B *= fp32_band_scale();
     pair.sig2_lo32 = std::nextafter((float)(sigma2 - B), -INFINITY);
     pair.sig2_hi32 = std::nextafter((float)(sigma2 + B), INFINITY);
 }
@@ -214,7 +220,7 @@ void lj_setup(hmc_system* s, double eps, double sigma, double rcut, double rshif
         Lmax = std::max(Lmax, s->geom.L[a]);
     }
     // the FP32 sigma^2 and 4 eps carry one rounding each; fold them into E generously
-    const double E = 8.0 * u32 * wmax + 16.0 * u64 * (Lmax + wmax) + 4.0 * u32 * sigma;
+    const double E = (8.0 * u32 * wmax + 16.0 * u64 * (Lmax + wmax) + 4.0 * u32 * sigma) * fp32_band_scale();
     P.lj_disp_err = (float)(E * 1.01);
     const double band = 2.0 * (3.5 * E * (rcut + E) + 3.1 * u32 * rcut * rcut);
     P.lj_rcut2_lo32 = std::nextafter((float)(P.lj_rcut2 - band), -INFINITY);

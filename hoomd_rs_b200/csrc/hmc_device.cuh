@@ -281,6 +281,86 @@ __device__ __forceinline__ bool for_each_neighbor(const Geometry& g, const uint3
     return false;
 }
 
+// The stencil around space m spread over a warp, for the kernels that give a trial one warp:
+// lane i < 2·kRows holds part i%2 of row i/2 (part 1 is the wrapped space of a row at a
+// fast-axis end, empty elsewhere) as a slot range, with the row's slow-axis shifts and the
+// exclusive prefix of the parts' lengths. The warp then takes the stencil's candidates 32 at
+// a time (flat_slot), whatever the lengths of the single rows.
+struct FlatStencil {
+    uint32_t lo, pre;  // this lane's part: first slot; candidates in the parts before it
+    uint32_t total;    // candidates in the whole stencil (the same in every lane)
+    float s0, s1;      // slow-axis shifts of this lane's row
+};
+
+// Call with all 32 lanes of the warp.
+template <int DIM>
+__device__ __forceinline__ FlatStencil flat_stencil(const Geometry& g, const uint32_t* __restrict__ cs,
+                                                    const uint32_t* m, uint32_t lane) {
+    FlatStencil fs{0u, 0u, 0u, 0.f, 0.f};
+    uint32_t len = 0;
+    if (lane < 2u * kRows<DIM>) {
+        const int r = (int)(lane >> 1);
+        const bool wrapped_part = (lane & 1u) != 0;
+        const int i0 = DIM == 3 ? r / 3 - 1 : 0;
+        const int i1 = DIM == 3 ? r % 3 - 1 : r - 1;
+        const uint32_t sf = g.shape[DIM - 1], mf = m[DIM - 1];
+        uint32_t base;
+        bool skip;
+        if (DIM == 3) {
+            skip = (i0 == -1 && g.shape[0] == 2) || (i1 == -1 && g.shape[1] == 2);
+            base = (wrap_index((int)m[0] + i0, g.shape[0]) * g.shape[1] + wrap_index((int)m[1] + i1, g.shape[1])) * sf;
+            fs.s0 = (float)i0 * g.w32[0];
+            fs.s1 = (float)i1 * g.w32[1];
+        } else {
+            skip = i1 == -1 && g.shape[0] == 2;
+            base = wrap_index((int)m[0] + i1, g.shape[0]) * sf;
+            fs.s0 = (float)i1 * g.w32[0];
+        }
+        // spaces [a, b) of the row along the fast axis
+        uint32_t a = 0, b = 0;
+        if (sf == 2) {
+            b = wrapped_part ? 0u : 2u;
+        } else if (mf >= 1 && mf + 1 < sf) {
+            if (!wrapped_part) a = mf - 1, b = mf + 2;
+        } else if (mf == 0) {
+            if (wrapped_part) a = sf - 1, b = sf;
+            else a = 0, b = 2;
+        } else {
+            if (wrapped_part) a = 0, b = 1;
+            else a = sf - 2, b = sf;
+        }
+        if (!skip && a < b) {
+            fs.lo = __ldg(cs + base + a);
+            len = __ldg(cs + base + b) - fs.lo;
+        }
+    }
+    const unsigned full = 0xffffffffu;
+    uint32_t x = len;
+#pragma unroll
+    for (uint32_t o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(full, x, o);
+        if (lane >= o) x += y;
+    }
+    fs.total = __shfl_sync(full, x, 31);
+    fs.pre = x - len;
+    return fs;
+}
+
+// Candidate j of the stencil (valid for j < total; all 32 lanes call this together): its
+// slot, and the lane holding its part. The prefixes grow with the lane (empty parts repeat
+// the next part's prefix), so the part is the last lane whose prefix is at most j.
+__device__ __forceinline__ uint32_t flat_slot(const FlatStencil& fs, uint32_t j, uint32_t& part) {
+    const unsigned full = 0xffffffffu;
+    uint32_t s = 0;
+#pragma unroll
+    for (uint32_t step = 16; step > 0; step >>= 1) {
+        const uint32_t p = __shfl_sync(full, fs.pre, s + step);
+        if (p <= j) s += step;
+    }
+    part = s;
+    return __shfl_sync(full, fs.lo, s) + (j - __shfl_sync(full, fs.pre, s));
+}
+
 // Read-only load of a double4 as two 16-byte loads through the non-coherent cache.
 __device__ __forceinline__ double4 ldg4(const double4* p) {
     const double2* q = reinterpret_cast<const double2*>(p);

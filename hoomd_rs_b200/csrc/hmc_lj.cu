@@ -3,10 +3,10 @@
 // delta_energy_one (hoomd-interaction/src/pairwise_cutoff.rs:919-941) sums the pair energy of
 // the trial site and of the current site over every other site within r_cut; the Metropolis
 // test (hoomd-mc/src/parallel_sweep.rs:267-268) accepts when dH <= 0, else draws u and accepts
-// when u < exp(-dH / kT). At the survey's LJ state (rho = 0.8, r_cut = 2.5) a space holds ~13
-// bodies, so a colour pass has few trials (~5k for 2^19 bodies) with ~360 candidates each:
-// one warp per trial, lanes striding along each stencil row (coalesced), warp reductions of
-// the sums.
+// when u < exp(-dH / kT). At rho = 0.8 with r_cut = 2.5 a space holds ~13 bodies, so a colour
+// pass has few trials (~5k for 2^19 bodies) with ~340 candidates each: one warp per trial,
+// which takes the candidates of all stencil rows 32 at a time (FlatStencil: ~11 steps instead
+// of two per row), and warp reductions of the sums.
 //
 // FP32 + recheck: the warp sums FP32 pair energies together with a rigorous bound B on
 // |dU32 - dU64| (r^2 error from the FP32 offsets, propagated through dE/dr^2; rounding of the
@@ -19,6 +19,13 @@
 
 namespace hmc {
 namespace {
+
+// Resident blocks per SM the sweep pass is compiled for: 9 caps it at 56 registers, so that a
+// colour pass of the 2^19-body LJ system (4,913 trials of one warp) runs in one wave; measured
+// 1.32e8 (FP32) and 1.83e8 (FP64) trial moves/s there, against 1.01e8 and 1.24e8 uncapped.
+#ifndef HMC_LJ_MIN_BLOCKS
+#define HMC_LJ_MIN_BLOCKS 9
+#endif
 
 constexpr float kU32 = 5.9604645e-8f;  // 2^-24
 
@@ -58,69 +65,6 @@ __device__ __forceinline__ void lj_pair32(const Pair& P, float r2, float& e, flo
     err = 1.1f * ((6.f * a + 3.f * b) * (dr2 * inv) + 24.f * kU32 * (a + b + fabsf(P.lj_e_shift32)));
 }
 
-// The stencil around space m; its rows are resolved one at a time (row_ranges) so that no
-// per-row table occupies registers across the candidate loops.
-template <int DIM>
-struct Stencil {
-    const uint32_t* cs;
-    uint32_t m[3];
-};
-
-template <int DIM>
-__device__ __forceinline__ void make_stencil(const Geometry& g, const uint32_t* __restrict__ cs, const uint32_t* m,
-                                             Stencil<DIM>& st) {
-    st.cs = cs;
-    st.m[0] = m[0];
-    st.m[1] = m[1];
-    st.m[2] = m[2];
-}
-
-// Row r of the stencil as at most two slot ranges (two when the row wraps around the fast
-// axis), with the row's slow-axis shifts; a row repeated on a two-space axis is empty.
-struct RowRanges {
-    uint32_t lo[2], hi[2];
-    float s0, s1;
-};
-template <int DIM>
-__device__ __forceinline__ RowRanges row_ranges(const Geometry& g, const Stencil<DIM>& st, int r) {
-    RowRanges rr{{0u, 0u}, {0u, 0u}, 0.f, 0.f};
-    const uint32_t sf = g.shape[DIM - 1], mf = st.m[DIM - 1];
-    const int i0 = DIM == 3 ? r / 3 - 1 : 0;
-    const int i1 = DIM == 3 ? r % 3 - 1 : r - 1;
-    uint32_t base;
-    bool skip;
-    if (DIM == 3) {
-        skip = (i0 == -1 && g.shape[0] == 2) || (i1 == -1 && g.shape[1] == 2);
-        base = (wrap_index((int)st.m[0] + i0, g.shape[0]) * g.shape[1] + wrap_index((int)st.m[1] + i1, g.shape[1])) * sf;
-        rr.s0 = (float)i0 * g.w32[0];
-        rr.s1 = (float)i1 * g.w32[1];
-    } else {
-        skip = i1 == -1 && g.shape[0] == 2;
-        base = wrap_index((int)st.m[0] + i1, g.shape[0]) * sf;
-        rr.s0 = (float)i1 * g.w32[0];
-    }
-    if (skip) return rr;
-    const uint32_t* cs = st.cs;
-    if (sf == 2) {
-        rr.lo[0] = __ldg(cs + base);
-        rr.hi[0] = __ldg(cs + base + 2);
-    } else if (mf >= 1 && mf + 1 < sf) {
-        rr.lo[0] = __ldg(cs + base + mf - 1);
-        rr.hi[0] = __ldg(cs + base + mf + 2);
-    } else if (mf == 0) {
-        rr.lo[0] = __ldg(cs + base);
-        rr.hi[0] = __ldg(cs + base + 2);
-        rr.lo[1] = __ldg(cs + base + sf - 1);
-        rr.hi[1] = __ldg(cs + base + sf);
-    } else {
-        rr.lo[0] = __ldg(cs + base + sf - 2);
-        rr.hi[0] = __ldg(cs + base + sf);
-        rr.lo[1] = __ldg(cs + base);
-        rr.hi[1] = __ldg(cs + base + 1);
-    }
-    return rr;
-}
-
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -137,39 +81,41 @@ __device__ __forceinline__ uint32_t warp_maxu(uint32_t v) {
     return v;
 }
 
-// FP64 energy of site t against the stencil of space m, skipping slot self: lane-strided over
-
-// FP64 energy of site t against the stencil of space m, skipping slot self: lane-strided over
-// the rows, then a butterfly reduction (every lane ends with the same value). S of a
-// candidate comes from sorted_s when have_s, else from wrap(sorted_b).
-template <int DIM>
-__device__ __forceinline__ double lj_energy64(const Geometry& g, const Arrays& A, const Pair& P, const double* t,
-                                              const Stencil<DIM>& st, uint32_t self, bool have_s, uint32_t lane) {
-    double e = 0.0;
+// FP64 energy of site ta (and, when TWO, of site tb in the same space) against the stencil
+// fs, skipping slot self: the warp takes the stencil's candidates 32 at a time, each lane sums
+// its own in that order, then a butterfly reduction (every lane ends with the same values).
+// S of a candidate comes from sorted_s when have_s, else from wrap(sorted_b). The two sums of
+// one call equal two calls of one sum each over the same stencil.
+template <int DIM, bool TWO>
+__device__ __forceinline__ void lj_energy64(const Geometry& g, const Arrays& A, const Pair& P, const double* ta,
+                                            const double* tb, const FlatStencil& fs, uint32_t self, bool have_s,
+                                            uint32_t lane, double& ea, double& eb) {
+    double a = 0.0, b = 0.0;
 #pragma unroll 1
-    for (int r = 0; r < kRows<DIM>; ++r) {
-        const RowRanges rr = row_ranges<DIM>(g, st, r);
-        for (int seg = 0; seg < 2; ++seg) {
-            for (uint32_t q = rr.lo[seg] + lane; q < rr.hi[seg]; q += 32) {
-                if (q == self) continue;
-                double sv[3];
-                if (have_s) {
-                    const double4 s4 = ldg4(A.sorted_s + q);
-                    sv[0] = s4.x;
-                    sv[1] = s4.y;
-                    sv[2] = s4.z;
-                } else {
-                    const double4 b4 = ldg4(A.sorted_b + q);
-                    sv[0] = b4.x;
-                    sv[1] = b4.y;
-                    sv[2] = b4.z;
-                    wrap_inv<DIM>(g.L, g.invL, sv);
-                }
-                e = dadd(e, lj_pair64(P, ref_dist2<DIM>(g, t, sv)));
+    for (uint32_t j0 = 0; j0 < fs.total; j0 += 32) {
+        const uint32_t j = j0 + lane;
+        uint32_t part;
+        const uint32_t q = flat_slot(fs, j, part);
+        if (j < fs.total && q != self) {
+            double sv[3];
+            if (have_s) {
+                const double4 s4 = ldg4(A.sorted_s + q);
+                sv[0] = s4.x;
+                sv[1] = s4.y;
+                sv[2] = s4.z;
+            } else {
+                const double4 b4 = ldg4(A.sorted_b + q);
+                sv[0] = b4.x;
+                sv[1] = b4.y;
+                sv[2] = b4.z;
+                wrap_inv<DIM>(g.L, g.invL, sv);
             }
+            a = dadd(a, lj_pair64(P, ref_dist2<DIM>(g, ta, sv)));
+            if (TWO) b = dadd(b, lj_pair64(P, ref_dist2<DIM>(g, tb, sv)));
         }
     }
-    return warp_sum(e);
+    ea = warp_sum(a);
+    eb = TWO ? warp_sum(b) : 0.0;
 }
 
 struct Sums32 {
@@ -178,46 +124,47 @@ struct Sums32 {
 };
 
 // FP32 energies of the trial site (offsets t32) and the current site (offsets c32) against
-// the stencil of their common space, with error bounds.
+// the stencil fs of their common space, with error bounds.
 template <int DIM>
 __device__ __forceinline__ Sums32 lj_energy32(const Geometry& g, const Arrays& A, const Pair& P, float4 t32,
-                                               float4 c32, int mf, const Stencil<DIM>& st, uint32_t self,
+                                               float4 c32, int mf, const FlatStencil& fs, uint32_t self,
                                                uint32_t lane) {
     Sums32 s{0.f, 0.f, 0.f, 0.f, 0u, 0u};
     const uint32_t sf = g.shape[DIM - 1];
 #pragma unroll 1
-    for (int r = 0; r < kRows<DIM>; ++r) {
-        const RowRanges rr = row_ranges<DIM>(g, st, r);
-        for (int seg = 0; seg < 2; ++seg) {
-            for (uint32_t q = rr.lo[seg] + lane; q < rr.hi[seg]; q += 32) {
-                if (q == self) continue;
-                const float4 o = __ldg(A.sorted_off + q);
-                int dm = __float_as_int(o.w) - mf;
-                if (sf >= 4) {
-                    if (dm > 1)
-                        dm -= (int)sf;
-                    else if (dm < -1)
-                        dm += (int)sf;
-                }
-                const float r2n = fp32_dist2<DIM>(g, t32, o, rr.s0, rr.s1, dm);
-                const float r2o = fp32_dist2<DIM>(g, c32, o, rr.s0, rr.s1, dm);
-                s.pairs += 2;
-                if (r2n < P.lj_rcut2_hi32) {
-                    float e, err;
-                    lj_pair32(P, r2n, e, err);
-                    s.e_new += e;
-                    s.err += err;
-                    s.mag += fabsf(e);
-                    s.terms += 1;
-                }
-                if (r2o < P.lj_rcut2_hi32) {
-                    float e, err;
-                    lj_pair32(P, r2o, e, err);
-                    s.e_old += e;
-                    s.err += err;
-                    s.mag += fabsf(e);
-                    s.terms += 1;
-                }
+    for (uint32_t j0 = 0; j0 < fs.total; j0 += 32) {
+        const uint32_t j = j0 + lane;
+        uint32_t part;
+        const uint32_t q = flat_slot(fs, j, part);
+        const float s0 = __shfl_sync(0xffffffffu, fs.s0, part);
+        const float s1 = __shfl_sync(0xffffffffu, fs.s1, part);
+        if (j < fs.total && q != self) {
+            const float4 o = __ldg(A.sorted_off + q);
+            int dm = __float_as_int(o.w) - mf;
+            if (sf >= 4) {
+                if (dm > 1)
+                    dm -= (int)sf;
+                else if (dm < -1)
+                    dm += (int)sf;
+            }
+            const float r2n = fp32_dist2<DIM>(g, t32, o, s0, s1, dm);
+            const float r2o = fp32_dist2<DIM>(g, c32, o, s0, s1, dm);
+            s.pairs += 2;
+            if (r2n < P.lj_rcut2_hi32) {
+                float e, err;
+                lj_pair32(P, r2n, e, err);
+                s.e_new += e;
+                s.err += err;
+                s.mag += fabsf(e);
+                s.terms += 1;
+            }
+            if (r2o < P.lj_rcut2_hi32) {
+                float e, err;
+                lj_pair32(P, r2o, e, err);
+                s.e_old += e;
+                s.err += err;
+                s.mag += fabsf(e);
+                s.terms += 1;
             }
         }
     }
@@ -229,10 +176,10 @@ __device__ __forceinline__ Sums32 lj_energy32(const Geometry& g, const Arrays& A
     return s;
 }
 
-// Metropolis decision from the FP32 sums: 1 accept, 0 reject, -1 needs the FP64 sums. When the
-// decision needs the uniform, *u is drawn from rng here (the FP64 path draws it at the same
-// point of the stream: only when dU > 0).
-__device__ __forceinline__ int decide32(const Sums32& s, double kt, Sfc64& rng, bool& drew, double& u) {
+// Metropolis decision from the FP32 sums: 1 accept, 0 reject, -1 needs the FP64 sums. u is the
+// uniform the reference draws only when dU > 0 (parallel_sweep.rs:267-268): the next value of
+// the trial's stream, which nothing else draws from, so the kernel draws it up front.
+__device__ __forceinline__ int decide32(const Sums32& s, double kt, double u) {
     const float d32 = s.e_new - s.e_old;
     // summation chains (per lane + 5 reduction levels + the final difference), FP64's own error
     const float b = s.err + (float)(s.terms + 7) * kU32 * s.mag * 1.01f + kU32 * fabsf(d32) + 1e-9f * (s.mag + 1.f);
@@ -240,17 +187,16 @@ __device__ __forceinline__ int decide32(const Sums32& s, double kt, Sfc64& rng, 
     const double lo = (double)d32 - (double)b, hi = (double)d32 + (double)b;
     if (hi <= 0.0) return 1;  // dU64 <= 0 for certain: accepted without a uniform
     if (lo <= 0.0) return -1;
-    u = uniform01(rng);  // dU64 > 0 for certain
-    drew = true;
-    const double t_hi = exp(-lo / kt) * (1.0 + 1e-12);
+    const double t_hi = exp(-lo / kt) * (1.0 + 1e-12);  // dU64 > 0 for certain
     const double t_lo = exp(-hi / kt) * (1.0 - 1e-12);
     if (u < t_lo) return 1;
     if (u >= t_hi) return 0;
     return -1;
 }
 
-template <int DIM, bool FP32>
-__global__ void __launch_bounds__(128) k_sweep_lj(Geometry g, Arrays A, Pair P, Launch L) {
+// The FP64 pass: one warp per trial.
+template <int DIM>
+__global__ void __launch_bounds__(128, HMC_LJ_MIN_BLOCKS) k_sweep_lj(Geometry g, Arrays A, Pair P, Launch L) {
     if (L.early_wait) grid_dependency_wait();  // first pass: the rebuild's arrays are read at once
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -262,8 +208,7 @@ __global__ void __launch_bounds__(128) k_sweep_lj(Geometry g, Arrays A, Pair P, 
         uint32_t m[3] = {0, 0, 0};
         unpack_m<DIM>(__ldg(A.color_cells + (size_t)L.color * g.color_stride + w), m);
         const uint32_t cell = cell_index<DIM>(g, m);
-        Stencil<DIM> st;
-        make_stencil<DIM>(g, A.cell_start, m, st);
+        const FlatStencil fs = flat_stencil<DIM>(g, A.cell_start, m, lane);
         const uint32_t start = __ldg(A.cell_start + cell);
         const uint32_t count = __ldg(A.cell_start + cell + 1) - start;
         // every lane draws the same stream: the trial is computed redundantly, warp-uniform
@@ -273,6 +218,7 @@ __global__ void __launch_bounds__(128) k_sweep_lj(Geometry g, Arrays A, Pair P, 
         double x[3] = {b4.x, b4.y, b4.z};
         double dv[3];
         ball_sample<DIM>(rng, L.max_move, A.zig_x, A.zig_f, dv);
+        const double u = uniform01(rng);
 #pragma unroll
         for (int a = 0; a < DIM; ++a) x[a] = dadd(x[a], dv[a]);
         wrap_inv<DIM>(g.L, g.invL, x);
@@ -282,47 +228,175 @@ __global__ void __launch_bounds__(128) k_sweep_lj(Geometry g, Arrays A, Pair P, 
         wrap_inv<DIM>(g.L, g.invL, t);
         grid_dependency_wait();  // the previous colour's moves are visible from here on
         allow_dependent_launch();
-        int decision;
-        bool drew = false;
+        const double4 s4 = ldg4(A.sorted_s + k);
+        const double si[3] = {s4.x, s4.y, s4.z};
+        double e_new, e_old;
+        lj_energy64<DIM, true>(g, A, P, t, si, fs, k, true, lane, e_new, e_old);
+        const double du = dsub(e_new, e_old);
+        if ((du <= 0.0 || u < exp(ddiv(-du, L.kt))) && lane == 0) {
+            n_accepted++;
+            double sv[3] = {t[0], t[1], t[2]};
+            wrap_inv<DIM>(g.L, g.invL, sv);
+            A.sorted_b[k] = make_double4(t[0], t[1], t[2], 0.0);
+            A.sorted_s[k] = make_double4(sv[0], sv[1], sv[2], 0.0);
+            A.sorted_off[k] = cell_offsets<DIM>(g, sv, m);
+            A.body_pos[A.sorted_body[k]] = make_double4(t[0], t[1], t[2], 0.0);
+        }
+        __syncwarp();
+    }
+    grid_dependency_wait();
+    allow_dependent_launch();
+    flush_stats(A.stats, pst, n_accepted);
+}
+
+// A trial's stencil and sites published in shared memory for the block-cooperative recheck.
+struct SharedTrial {
+    uint32_t lo[32], pre[32];  // the owner warp's FlatStencil parts
+    double t[3], si[3];        // trial site and current site
+    uint32_t total, self;
+};
+
+// Slot of candidate j of a published stencil (the FlatStencil search over shared memory).
+__device__ __forceinline__ uint32_t shared_slot(const SharedTrial& st, uint32_t j) {
+    uint32_t s = 0;
+#pragma unroll
+    for (uint32_t step = 16; step > 0; step >>= 1)
+        if (st.pre[s + step] <= j) s += step;
+    return st.lo[s] + (j - st.pre[s]);
+}
+
+constexpr uint32_t kRecheckChunks = 8;  // 32-candidate chunks per shared-memory round
+
+// The FP32 + recheck pass. One warp per trial as in the FP64 pass, the block's four warps
+// taking four trials at a time. A trial whose FP32 sums cannot decide is rechecked by the whole
+// block: each warp evaluates every fourth 32-candidate chunk of the FP64 walk into shared
+// memory, and the trial's own warp adds them per lane in chunk order, which gives the FP64
+// pass's sums bit for bit (lj_energy64: the same candidates per lane in the same order, the
+// same butterfly; an empty slot adds +0, which leaves a sum that starts at +0 unchanged). A
+// lone warp walking the stencil in FP64 would otherwise set the duration of a pass whose
+// trials all run in one wave.
+template <int DIM>
+__global__ void __launch_bounds__(128, HMC_LJ_MIN_BLOCKS) k_sweep_lj32(Geometry g, Arrays A, Pair P, Launch L) {
+    if (L.early_wait) grid_dependency_wait();  // first pass: the rebuild's arrays are read at once
+    __shared__ double s_e[kRecheckChunks][2][32];
+    __shared__ SharedTrial s_trial;
+    __shared__ uint32_t s_active;
+    const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
+    uint32_t n_accepted = 0;
+    PairStats pst;
+    if (threadIdx.x == 0) s_active = active_count(A, L.color, L.round);
+    __syncthreads();
+    const uint32_t n_active = s_active;  // block-uniform: the loop below holds barriers
+    for (uint32_t base = blockIdx.x * 4u; base < n_active; base += gridDim.x * 4u) {
+        const uint32_t w = base + wib;
+        uint32_t m[3] = {0, 0, 0};
+        uint32_t k = 0;
+        double t[3] = {0.0, 0.0, 0.0};
         double u = 0.0;
-        if (FP32) {
+        bool trial = false;
+        FlatStencil fs{0u, 0u, 0u, 0.f, 0.f};
+        if (w < n_active) {  // warp-uniform
+            unpack_m<DIM>(__ldg(A.color_cells + (size_t)L.color * g.color_stride + w), m);
+            const uint32_t cell = cell_index<DIM>(g, m);
+            fs = flat_stencil<DIM>(g, A.cell_start, m, lane);
+            const uint32_t start = __ldg(A.cell_start + cell);
+            const uint32_t count = __ldg(A.cell_start + cell + 1) - start;
+            Sfc64 rng = make_rng(L.step, L.substep, L.seed, (uint64_t)cell);
+            k = start + canon_range_u32(rng, count);
+            const double4 b4 = A.sorted_b[k];
+            double x[3] = {b4.x, b4.y, b4.z};
+            double dv[3];
+            ball_sample<DIM>(rng, L.max_move, A.zig_x, A.zig_f, dv);
+            u = uniform01(rng);
+#pragma unroll
+            for (int a = 0; a < DIM; ++a) x[a] = dadd(x[a], dv[a]);
+            wrap_inv<DIM>(g.L, g.invL, x);
+            uint32_t mt[3];
+            trial = point_to_space<DIM>(g, x, mt) && cell_index<DIM>(g, mt) == cell;
+            t[0] = x[0];
+            t[1] = x[1];
+            t[2] = DIM == 3 ? x[2] : 0.0;
+            wrap_inv<DIM>(g.L, g.invL, t);
+        }
+        grid_dependency_wait();  // the previous colour's moves are visible from here on
+        allow_dependent_launch();
+        int decision = 0;
+        float d32 = 0.f;
+        if (trial) {
             const float4 t32 = cell_offsets<DIM>(g, t, m);
             const float4 c32 = __ldg(A.sorted_off + k);
-            const Sums32 s = lj_energy32<DIM>(g, A, P, t32, c32, (int)m[DIM - 1], st, k, lane);
+            const Sums32 s = lj_energy32<DIM>(g, A, P, t32, c32, (int)m[DIM - 1], fs, k, lane);
             pst.checks += s.pairs;
-            decision = decide32(s, L.kt, rng, drew, u);
-            if (decision < 0) {
-                // FP64 recheck with the plain pass's order; the uniform, if already drawn, is
-                // the one the plain pass would draw (its draw point is the same).
-                double si[3] = {b4.x, b4.y, b4.z};
-                wrap_inv<DIM>(g.L, g.invL, si);
-                const double du = dsub(lj_energy64<DIM>(g, A, P, t, st, k, false, lane),
-                                       lj_energy64<DIM>(g, A, P, si, st, k, false, lane));
-                if (lane == 0) {
-                    pst.rechecks++;
-                    const double err = fabs((double)(s.e_new - s.e_old) - du);
-                    pst.max_err = err > pst.max_err ? err : pst.max_err;
+            decision = decide32(s, L.kt, u);
+            d32 = s.e_new - s.e_old;
+        }
+        const bool unsure = decision < 0;
+        if (__syncthreads_or(unsure)) {
+            for (uint32_t o = 0; o < 4u; ++o) {
+                const bool mine = unsure && wib == o;
+                if (mine) {
+                    s_trial.lo[lane] = fs.lo;
+                    s_trial.pre[lane] = fs.pre;
+                    if (lane == 0) {
+                        const double4 c4 = ldg4(A.sorted_b + k);
+                        double si[3] = {c4.x, c4.y, c4.z};
+                        wrap_inv<DIM>(g.L, g.invL, si);
+#pragma unroll
+                        for (int a = 0; a < 3; ++a) {
+                            s_trial.t[a] = t[a];
+                            s_trial.si[a] = si[a];
+                        }
+                        s_trial.total = fs.total;
+                        s_trial.self = k;
+                    }
                 }
-                if (du <= 0.0) {
-                    decision = 1;
-                } else {
-                    if (!drew) u = uniform01(rng);
-                    decision = u < exp(ddiv(-du, L.kt)) ? 1 : 0;
+                if (!__syncthreads_or(mine)) continue;  // also publishes s_trial
+                const uint32_t total = s_trial.total, self = s_trial.self;
+                const uint32_t n_chunks = (total + 31u) / 32u;
+                double ea = 0.0, eb = 0.0;
+                for (uint32_t c0 = 0; c0 < n_chunks; c0 += kRecheckChunks) {
+                    const uint32_t c1 = min(c0 + kRecheckChunks, n_chunks);
+                    for (uint32_t c = c0 + wib; c < c1; c += 4u) {
+                        const uint32_t j = c * 32u + lane;
+                        double en = 0.0, eo = 0.0;
+                        if (j < total) {
+                            const uint32_t q = shared_slot(s_trial, j);
+                            if (q != self) {
+                                const double4 b4 = ldg4(A.sorted_b + q);
+                                double sv[3] = {b4.x, b4.y, b4.z};
+                                wrap_inv<DIM>(g.L, g.invL, sv);
+                                en = lj_pair64(P, ref_dist2<DIM>(g, s_trial.t, sv));
+                                eo = lj_pair64(P, ref_dist2<DIM>(g, s_trial.si, sv));
+                            }
+                        }
+                        s_e[c - c0][0][lane] = en;
+                        s_e[c - c0][1][lane] = eo;
+                    }
+                    __syncthreads();
+                    if (wib == o) {
+                        for (uint32_t c = c0; c < c1; ++c) {
+                            ea = dadd(ea, s_e[c - c0][0][lane]);
+                            eb = dadd(eb, s_e[c - c0][1][lane]);
+                        }
+                    }
+                    __syncthreads();
+                }
+                if (wib == o) {
+                    const double du = dsub(warp_sum(ea), warp_sum(eb));
+                    if (lane == 0) {
+                        pst.rechecks++;
+                        const double err = fabs((double)d32 - du);
+                        pst.max_err = err > pst.max_err ? err : pst.max_err;
+                    }
+                    decision = (du <= 0.0 || u < exp(ddiv(-du, L.kt))) ? 1 : 0;
                 }
             }
-        } else {
-            const double4 s4 = ldg4(A.sorted_s + k);
-            const double si[3] = {s4.x, s4.y, s4.z};
-            const double du = dsub(lj_energy64<DIM>(g, A, P, t, st, k, true, lane),
-                                   lj_energy64<DIM>(g, A, P, si, st, k, true, lane));
-            decision = (du <= 0.0 || uniform01(rng) < exp(ddiv(-du, L.kt))) ? 1 : 0;
         }
         if (decision == 1 && lane == 0) {
             n_accepted++;
             double sv[3] = {t[0], t[1], t[2]};
             wrap_inv<DIM>(g.L, g.invL, sv);
             A.sorted_b[k] = make_double4(t[0], t[1], t[2], 0.0);
-            if (!FP32) A.sorted_s[k] = make_double4(sv[0], sv[1], sv[2], 0.0);
             A.sorted_off[k] = cell_offsets<DIM>(g, sv, m);
             A.body_pos[A.sorted_body[k]] = make_double4(t[0], t[1], t[2], 0.0);
         }
@@ -355,10 +429,12 @@ __global__ void __launch_bounds__(128) k_eval_lj(Geometry g, Arrays A, Pair P, c
         uint8_t dec = 0, rech = 0;
         double du = 0.0;
         if (ok) {
-            Stencil<DIM> stt, sti;
-            make_stencil<DIM>(g, A.cell_start, mt, stt);
-            make_stencil<DIM>(g, A.cell_start, mi, sti);
-            du = dsub(lj_energy64<DIM>(g, A, P, t, stt, k, true, lane), lj_energy64<DIM>(g, A, P, si, sti, k, true, lane));
+            const FlatStencil ft = flat_stencil<DIM>(g, A.cell_start, mt, lane);
+            const FlatStencil fi = flat_stencil<DIM>(g, A.cell_start, mi, lane);
+            double e_new, e_old, unused;
+            lj_energy64<DIM, false>(g, A, P, t, nullptr, ft, k, true, lane, e_new, unused);
+            lj_energy64<DIM, false>(g, A, P, si, nullptr, fi, k, true, lane, e_old, unused);
+            du = dsub(e_new, e_old);
             const double u = uu[i];
             bool dec64 = du <= 0.0 || u < exp(ddiv(-du, kt));
             dec = dec64 ? 1 : 0;
@@ -369,7 +445,7 @@ __global__ void __launch_bounds__(128) k_eval_lj(Geometry g, Arrays A, Pair P, c
                 if (same) {
                     const float4 t32 = cell_offsets<DIM>(g, t, mt);
                     const float4 c32 = __ldg(A.sorted_off + k);
-                    const Sums32 s = lj_energy32<DIM>(g, A, P, t32, c32, (int)mt[DIM - 1], stt, k, lane);
+                    const Sums32 s = lj_energy32<DIM>(g, A, P, t32, c32, (int)mt[DIM - 1], ft, k, lane);
                     const float d32 = s.e_new - s.e_old;
                     const float b = s.err + (float)(s.terms + 7) * kU32 * s.mag * 1.01f + kU32 * fabsf(d32) +
                                     1e-9f * (s.mag + 1.f);
@@ -448,10 +524,10 @@ cudaError_t launch_sweep_lj(int dim, bool fp32, const Geometry& g, const Arrays&
     if (blocks > (uint32_t)max_blocks) blocks = (uint32_t)max_blocks;
     PassLaunch pl(blocks, l.overlap_previous != 0 || l.early_wait != 0, s);
     if (dim == 2)
-        return fp32 ? cudaLaunchKernelEx(&pl.cfg, k_sweep_lj<2, true>, g, a, p, l)
-                    : cudaLaunchKernelEx(&pl.cfg, k_sweep_lj<2, false>, g, a, p, l);
-    return fp32 ? cudaLaunchKernelEx(&pl.cfg, k_sweep_lj<3, true>, g, a, p, l)
-                : cudaLaunchKernelEx(&pl.cfg, k_sweep_lj<3, false>, g, a, p, l);
+        return fp32 ? cudaLaunchKernelEx(&pl.cfg, k_sweep_lj32<2>, g, a, p, l)
+                    : cudaLaunchKernelEx(&pl.cfg, k_sweep_lj<2>, g, a, p, l);
+    return fp32 ? cudaLaunchKernelEx(&pl.cfg, k_sweep_lj32<3>, g, a, p, l)
+                : cudaLaunchKernelEx(&pl.cfg, k_sweep_lj<3>, g, a, p, l);
 }
 
 cudaError_t launch_eval_lj(int dim, bool fp32, const Geometry& g, const Arrays& a, const Pair& p,

@@ -8,8 +8,9 @@
 // product, sum and fused multiply-add below follows the reference's expression order, so
 // the FP64 decision is the reference's.
 //
-// One warp per trial: all lanes compute the same trial move, then stride over the stencil's
-// candidates; the first overlap found by any lane rejects the trial (early exit by vote).
+// One warp per trial: all lanes compute the same trial move, then take the stencil's
+// candidates 32 at a time across its rows; the first overlap found by any lane rejects the
+// trial (early exit by vote).
 // FP32 + recheck: a candidate whose FP32 centre distance clears the circumsphere by more
 // than the FP32 error bound is skipped; every other candidate runs the FP64 test, so the
 // decisions equal the FP64 pass.
@@ -224,71 +225,48 @@ struct PolyShape {
 
 __device__ __forceinline__ bool warp_any(bool v) { return __any_sync(0xffffffffu, v); }
 
-// Overlap of the trial (t, qi; FP32 offsets t32) with any candidate of the stencil of space m,
-// skipping slot self. Lanes stride along each row; a vote after every stride step stops the
-// warp at the first overlap. FP32: the circumsphere prefilter in FP32 under the bound.
+// Overlap of the trial (t, qi; FP32 offsets t32) with any candidate of the stencil fs,
+// skipping slot self. The warp takes the stencil's candidates 32 at a time across its rows
+// (at the bench's density one step holds the whole stencil, so the lanes that need the full
+// test run it together), and a vote after each step stops the warp at the first overlap.
+// FP32: the circumsphere prefilter in FP32 under the bound.
 template <bool FP32>
 __device__ __forceinline__ bool poly_overlaps(const Geometry& g, const Arrays& A, const PolyShape& sh, const double* t,
-                                              const Q& qi, float4 t32, const uint32_t* m, uint32_t self,
+                                              const Q& qi, float4 t32, int mf, const FlatStencil& fs, uint32_t self,
                                               uint32_t lane, PairStats& st) {
     const uint32_t sf = g.shape[2];
-    const int mf = (int)m[2];
-    for (int i0 = (g.shape[0] == 2 ? 0 : -1); i0 <= 1; ++i0) {
-        for (int i1 = (g.shape[1] == 2 ? 0 : -1); i1 <= 1; ++i1) {
-            const uint32_t base =
-                (wrap_index((int)m[0] + i0, g.shape[0]) * g.shape[1] + wrap_index((int)m[1] + i1, g.shape[1])) * sf;
-            uint32_t seg_lo[2], seg_hi[2];
-            if (sf == 2) {
-                seg_lo[0] = __ldg(A.cell_start + base);
-                seg_hi[0] = __ldg(A.cell_start + base + 2);
-                seg_lo[1] = seg_hi[1] = 0;
-            } else if (mf >= 1 && mf + 1 < (int)sf) {
-                seg_lo[0] = __ldg(A.cell_start + base + mf - 1);
-                seg_hi[0] = __ldg(A.cell_start + base + mf + 2);
-                seg_lo[1] = seg_hi[1] = 0;
-            } else if (mf == 0) {
-                seg_lo[0] = __ldg(A.cell_start + base);
-                seg_hi[0] = __ldg(A.cell_start + base + 2);
-                seg_lo[1] = __ldg(A.cell_start + base + sf - 1);
-                seg_hi[1] = __ldg(A.cell_start + base + sf);
-            } else {
-                seg_lo[0] = __ldg(A.cell_start + base + sf - 2);
-                seg_hi[0] = __ldg(A.cell_start + base + sf);
-                seg_lo[1] = __ldg(A.cell_start + base);
-                seg_hi[1] = __ldg(A.cell_start + base + 1);
-            }
-            const float s0 = (float)i0 * g.w32[0], s1 = (float)i1 * g.w32[1];
-            for (int seg = 0; seg < 2; ++seg) {
-                for (uint32_t q0 = seg_lo[seg]; q0 < seg_hi[seg]; q0 += 32) {
-                    const uint32_t q = q0 + lane;
-                    bool hit = false;
-                    if (q < seg_hi[seg] && q != self) {
-                        bool test = true;
-                        if (FP32) {
-                            const float4 o = __ldg(A.sorted_off + q);
-                            int dm = __float_as_int(o.w) - mf;
-                            if (sf >= 4) {
-                                if (dm > 1)
-                                    dm -= (int)sf;
-                                else if (dm < -1)
-                                    dm += (int)sf;
-                            }
-                            st.checks++;
-                            test = fp32_dist2<3>(g, t32, o, s0, s1, dm) < sh.rcut2_hi32;
-                            if (test) st.rechecks++;
-                        }
-                        if (test) {
-                            // shapes keep S in both precision modes (the FP32 pass only prefilters)
-                            const double4 s4 = ldg4(A.sorted_s + q);
-                            const double sj[3] = {s4.x, s4.y, s4.z};
-                            if (!FP32) st.checks++;
-                            hit = poly_overlap64(g, A, sh.verts, sh.nv, sh.rcut2, t, qi, sj, q);
-                        }
-                    }
-                    if (warp_any(hit)) return true;
+#pragma unroll 1
+    for (uint32_t j0 = 0; j0 < fs.total; j0 += 32) {
+        const uint32_t j = j0 + lane;
+        uint32_t part;
+        const uint32_t q = flat_slot(fs, j, part);
+        const float s0 = __shfl_sync(0xffffffffu, fs.s0, part);
+        const float s1 = __shfl_sync(0xffffffffu, fs.s1, part);
+        bool hit = false;
+        if (j < fs.total && q != self) {
+            bool test = true;
+            if (FP32) {
+                const float4 o = __ldg(A.sorted_off + q);
+                int dm = __float_as_int(o.w) - mf;
+                if (sf >= 4) {
+                    if (dm > 1)
+                        dm -= (int)sf;
+                    else if (dm < -1)
+                        dm += (int)sf;
                 }
+                st.checks++;
+                test = fp32_dist2<3>(g, t32, o, s0, s1, dm) < sh.rcut2_hi32;
+                if (test) st.rechecks++;
+            }
+            if (test) {
+                // shapes keep S in both precision modes (the FP32 pass only prefilters)
+                const double4 s4 = ldg4(A.sorted_s + q);
+                const double sj[3] = {s4.x, s4.y, s4.z};
+                if (!FP32) st.checks++;
+                hit = poly_overlap64(g, A, sh.verts, sh.nv, sh.rcut2, t, qi, sj, q);
             }
         }
+        if (warp_any(hit)) return true;
     }
     return false;
 }
@@ -306,6 +284,7 @@ __global__ void __launch_bounds__(128) k_sweep_poly3(Geometry g, Arrays A, PolyS
         uint32_t m[3];
         unpack_m<3>(__ldg(A.color_cells + (size_t)L.color * g.color_stride + w), m);
         const uint32_t cell = cell_index<3>(g, m);
+        const FlatStencil fs = flat_stencil<3>(g, A.cell_start, m, lane);
         const uint32_t start = __ldg(A.cell_start + cell);
         const uint32_t count = __ldg(A.cell_start + cell + 1) - start;
         Sfc64 rng = make_rng(L.step, L.substep, L.seed, (uint64_t)cell);
@@ -329,7 +308,7 @@ __global__ void __launch_bounds__(128) k_sweep_poly3(Geometry g, Arrays A, PolyS
         const float4 t32 = FP32 ? cell_offsets<3>(g, t, m) : make_float4(0.f, 0.f, 0.f, 0.f);
         grid_dependency_wait();  // the previous colour's moves are visible from here on
         allow_dependent_launch();
-        if (poly_overlaps<FP32>(g, A, sh, t, qi, t32, m, k, lane, st)) continue;
+        if (poly_overlaps<FP32>(g, A, sh, t, qi, t32, (int)m[2], fs, k, lane, st)) continue;
         if (lane == 0) {
             n_accepted++;
             double sv[3] = {t[0], t[1], t[2]};
@@ -368,7 +347,8 @@ __global__ void __launch_bounds__(128) k_eval_poly3(Geometry g, Arrays A, PolySh
         uint8_t dec = 0;
         if (point_to_space<3>(g, t, m)) {
             const float4 t32 = FP32 ? cell_offsets<3>(g, t, m) : make_float4(0.f, 0.f, 0.f, 0.f);
-            dec = poly_overlaps<FP32>(g, A, sh, t, qi, t32, m, k, lane, st) ? 0 : 1;
+            const FlatStencil fs = flat_stencil<3>(g, A.cell_start, m, lane);
+            dec = poly_overlaps<FP32>(g, A, sh, t, qi, t32, (int)m[2], fs, k, lane, st) ? 0 : 1;
         } else if (lane == 0) {
             atomicOr(&A.stats->error_flags, kErrOutsideCheckerboard);
         }

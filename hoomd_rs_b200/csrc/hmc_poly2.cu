@@ -10,8 +10,8 @@
 // multiply-add follows the reference's expression order; sin and cos are correctly rounded
 // (cr_sincos), so the FP64 decision is the reference's on a correctly rounded libm.
 //
-// One warp per trial, as for polyhedra: all lanes compute the same trial move, then stride
-// over the stencil's candidates with an early exit by vote. FP32 + recheck: candidates whose
+// One warp per trial, as for polyhedra: all lanes compute the same trial move, then take the
+// stencil's candidates 32 at a time across its rows, with an early exit by vote. FP32 + recheck: candidates whose
 // FP32 centre distance clears the circumcircles by more than the FP32 error bound are
 // skipped; every other candidate runs the FP64 test.
 #include <cuda_runtime.h>
@@ -169,53 +169,45 @@ __device__ __forceinline__ bool poly2_overlap64(const Geometry& g, const Arrays&
 
 __device__ __forceinline__ bool warp_any2(bool v) { return __any_sync(0xffffffffu, v); }
 
-// Overlap of the trial (t, ti) with any candidate of the 3 stencil rows around space m,
-// skipping slot self; lanes stride along each row, a vote after every stride step.
+// Overlap of the trial (t, ti) with any candidate of the stencil fs (the 3 rows around the
+// trial's space), skipping slot self: the warp takes the candidates 32 at a time across the
+// rows, with a vote after each step.
 template <bool FP32, bool SAT>
 __device__ __forceinline__ bool poly2_overlaps(const Geometry& g, const Arrays& A, const PolyShape2& sh,
-                                               const double* t, double ti, float4 t32, const uint32_t* m,
+                                               const double* t, double ti, float4 t32, int mf, const FlatStencil& fs,
                                                uint32_t self, uint32_t lane, PairStats& st, bool* range_error) {
     const uint32_t sf = g.shape[1];
-    const int mf = (int)m[1];
-    for (int i0 = (g.shape[0] == 2 ? 0 : -1); i0 <= 1; ++i0) {
-        const uint32_t base = wrap_index((int)m[0] + i0, g.shape[0]) * sf;
-        uint32_t seg_lo[2], seg_hi[2];
-        uint32_t lo, hi;
-        row_span(sf, (uint32_t)mf, &lo, &hi);
-        seg_lo[0] = __ldg(A.cell_start + base + lo);
-        seg_hi[0] = __ldg(A.cell_start + base + hi);
-        seg_lo[1] = seg_hi[1] = 0;
-        int mfx[2] = {mf, mf};
-        if (sf > 2 && (mf == 0 || mf + 1 == (int)sf)) {
-            const uint32_t wlo = mf == 0 ? sf - 1u : 0u;
-            seg_lo[1] = __ldg(A.cell_start + base + wlo);
-            seg_hi[1] = __ldg(A.cell_start + base + wlo + 1u);
-            mfx[1] = mf == 0 ? (int)sf : -1;  // gives the wrapped space the cell shift -1 or +1
-        }
-        const float s0 = (float)i0 * g.w32[0];
-        for (int seg = 0; seg < 2; ++seg) {
-            for (uint32_t q0 = seg_lo[seg]; q0 < seg_hi[seg]; q0 += 32) {
-                const uint32_t q = q0 + lane;
-                bool hit = false;
-                if (q < seg_hi[seg] && q != self) {
-                    bool test = true;
-                    if (FP32) {
-                        const float4 o = __ldg(A.sorted_off + q);
-                        st.checks++;
-                        test = fp32_dist2<2>(g, t32, o, s0, 0.f, __float_as_int(o.w) - mfx[seg]) < sh.rcut2_hi32;
-                        if (test) st.rechecks++;
-                    }
-                    if (test) {
-                        // shapes keep S in both precision modes (the FP32 pass only prefilters)
-                        const double4 s4 = ldg4(A.sorted_s + q);
-                        const double sj[3] = {s4.x, s4.y, 0.0};
-                        if (!FP32) st.checks++;
-                        hit = poly2_overlap64<SAT>(g, A, sh, t, ti, sj, q, range_error);
-                    }
+#pragma unroll 1
+    for (uint32_t j0 = 0; j0 < fs.total; j0 += 32) {
+        const uint32_t j = j0 + lane;
+        uint32_t part;
+        const uint32_t q = flat_slot(fs, j, part);
+        const float s0 = __shfl_sync(0xffffffffu, fs.s0, part);
+        bool hit = false;
+        if (j < fs.total && q != self) {
+            bool test = true;
+            if (FP32) {
+                const float4 o = __ldg(A.sorted_off + q);
+                int dm = __float_as_int(o.w) - mf;
+                if (sf >= 4) {  // the wrapped space of a row at a fast-axis end
+                    if (dm > 1)
+                        dm -= (int)sf;
+                    else if (dm < -1)
+                        dm += (int)sf;
                 }
-                if (warp_any2(hit)) return true;
+                st.checks++;
+                test = fp32_dist2<2>(g, t32, o, s0, 0.f, dm) < sh.rcut2_hi32;
+                if (test) st.rechecks++;
+            }
+            if (test) {
+                // shapes keep S in both precision modes (the FP32 pass only prefilters)
+                const double4 s4 = ldg4(A.sorted_s + q);
+                const double sj[3] = {s4.x, s4.y, 0.0};
+                if (!FP32) st.checks++;
+                hit = poly2_overlap64<SAT>(g, A, sh, t, ti, sj, q, range_error);
             }
         }
+        if (warp_any2(hit)) return true;
     }
     return false;
 }
@@ -234,6 +226,7 @@ __global__ void __launch_bounds__(128) k_sweep_poly2(Geometry g, Arrays A, PolyS
         uint32_t m[3] = {0, 0, 0};
         unpack_m<2>(__ldg(A.color_cells + (size_t)L.color * g.color_stride + w), m);
         const uint32_t cell = cell_index<2>(g, m);
+        const FlatStencil fs = flat_stencil<2>(g, A.cell_start, m, lane);
         const uint32_t start = __ldg(A.cell_start + cell);
         const uint32_t count = __ldg(A.cell_start + cell + 1) - start;
         Sfc64 rng = make_rng(L.step, L.substep, L.seed, (uint64_t)cell);
@@ -259,7 +252,7 @@ __global__ void __launch_bounds__(128) k_sweep_poly2(Geometry g, Arrays A, PolyS
         const float4 t32 = FP32 ? cell_offsets<2>(g, t, m) : make_float4(0.f, 0.f, 0.f, 0.f);
         grid_dependency_wait();  // the previous colour's moves are visible from here on
         allow_dependent_launch();
-        if (poly2_overlaps<FP32, SAT>(g, A, sh, t, ti, t32, m, k, lane, st, &range_error)) continue;
+        if (poly2_overlaps<FP32, SAT>(g, A, sh, t, ti, t32, (int)m[1], fs, k, lane, st, &range_error)) continue;
         if (lane == 0) {
             n_accepted++;
             double sv[3] = {t[0], t[1], 0.0};
@@ -299,7 +292,8 @@ __global__ void __launch_bounds__(128) k_eval_poly2(Geometry g, Arrays A, PolySh
         uint8_t dec = 0;
         if (point_to_space<2>(g, t, m)) {
             const float4 t32 = FP32 ? cell_offsets<2>(g, t, m) : make_float4(0.f, 0.f, 0.f, 0.f);
-            dec = poly2_overlaps<FP32, SAT>(g, A, sh, t, ti, t32, m, k, lane, st, &range_error) ? 0 : 1;
+            const FlatStencil fs = flat_stencil<2>(g, A.cell_start, m, lane);
+            dec = poly2_overlaps<FP32, SAT>(g, A, sh, t, ti, t32, (int)m[1], fs, k, lane, st, &range_error) ? 0 : 1;
         } else if (lane == 0) {
             atomicOr(&A.stats->error_flags, kErrOutsideCheckerboard);
         }

@@ -116,3 +116,24 @@ def test_lj_overlapping_passes_equal_serialised_passes(ctx, monkeypatch, precisi
     cb = b.sweep(TRANSLATE, 0.1, 1.0, precision, n_sweeps=3, increment_step=True)
     assert (ca.accepted, ca.rejected) == (cb.accepted, cb.rejected)
     assert np.array_equal(a.positions(), b.positions())
+
+
+@pytest.mark.parametrize("dim,n,rho", [(3, 1372, 0.8), (2, 900, 0.7), (2, 1 << 18, 0.7)])
+def test_lj_wide_bound_block_recheck_equals_fp64(ctx, monkeypatch, dim, n, rho):
+    # Widening the FP32 error bound 10^4 times sends most trials of the FP32 pass to the
+    # block-cooperative FP64 recheck (several per block, and in the 2^18 case more trials per
+    # colour than the grid holds); the trajectory must equal the plain FP64 pass bit for bit.
+    pos, L = lattice.lennard_jones_box(n, rho, dim, 0x5EED0012)
+    monkeypatch.setenv("HMC_B200_FP32_BAND_SCALE", "1e4")
+    a = Microstate(ctx, Periodic(2.5, [L] * dim), pos, lj(), seed=0x5EED0012)
+    monkeypatch.delenv("HMC_B200_FP32_BAND_SCALE")
+    b = Microstate(ctx, Periodic(2.5, [L] * dim), pos, lj(), seed=0x5EED0012)
+    rechecks, trials = 0, 0
+    for _ in range(3):
+        ca = a.sweep(TRANSLATE, 0.1, 1.0, FP32_RECHECK, n_sweeps=1, increment_step=True)
+        cb = b.sweep(TRANSLATE, 0.1, 1.0, FP64, n_sweeps=1, increment_step=True)
+        assert (ca.accepted, ca.rejected) == (cb.accepted, cb.rejected)
+        rechecks += ca.rechecks
+        trials += ca.total()
+    assert np.array_equal(a.positions(), b.positions())
+    assert rechecks > trials // 4, (rechecks, trials)
