@@ -268,15 +268,15 @@ def run_replicas(args, local_rank):
 
 
 def run_config(args, local_rank):
-    """The survey's other single-box configurations, FP32+recheck and FP64 from the same state,
+    """The other single-box configurations, FP32+recheck and FP64 from the same state,
     device-timed per step like the headline, with the oracle's ParallelSweep on the host cores
     as the CPU baseline (a bounded sample of whole sweeps). A step: one sweep (disks, LJ) or one
     translation plus one rotation sweep (cubes)."""
     import torch
     import oracle
-    from hoomd_rs_b200 import (FP32_RECHECK, FP64, ROTATE, TRANSLATE, Context, ConvexPolyhedron, HardShape,
-                               HardSphere, Isotropic, LennardJones, Microstate, PairwiseCutoff, Periodic, Shifted,
-                               lattice)
+    from hoomd_rs_b200 import (FP32_RECHECK, FP64, ROTATE, TRANSLATE, Context, ConvexPolygon, ConvexPolyhedron,
+                               HardShape, HardSphere, Isotropic, LennardJones, Microstate, PairwiseCutoff, Periodic,
+                               Shifted, lattice)
     torch.cuda.set_device(local_rank)
     ctx = Context(local_rank)
     kind = args.workload
@@ -299,6 +299,18 @@ def run_config(args, local_rank):
         desc = "hard cubes (vertices +-0.5), N=2^18, packing fraction 0.55, simple-cubic start, identity versors, " \
                "translation 0.08 then rotation 0.1 per step"
         orng = math.sqrt(3)
+    elif kind == "squares":
+        n, seed = 1 << 18, 0x5EED0007
+        square = np.array([[-0.5, -0.5], [0.5, -0.5], [0.5, 0.5], [-0.5, 0.5]])
+        L = math.sqrt(n / 0.6)
+        pos = lattice.cubic_lattice(n, L, 2, seed, jitter=0.0)
+        h = PairwiseCutoff(HardShape(ConvexPolygon.with_vertices(square)))
+        bound, dim = Periodic(math.sqrt(2), [L, L]), 2
+        moves = [(TRANSLATE, 0.1), (ROTATE, 0.1)]
+        okw = dict(interaction=oracle.HARD_CONVEX_POLYGON, vertices=square)
+        desc = "2-D hard squares (vertices +-0.5, XenoCollide), N=2^18, area fraction 0.60, square-lattice start, " \
+               "angles 0, translation 0.1 then rotation 0.1 per step"
+        orng = math.sqrt(2)
     else:
         n, seed = 1 << 19, 0x5EED0005
         pos, L = lattice.lennard_jones_box(n, 0.8, 3, seed)
@@ -455,7 +467,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="hard_spheres",
-                    choices=["hard_spheres", "replicas", "disks", "cubes", "lj", "gsd"],
+                    choices=["hard_spheres", "replicas", "disks", "cubes", "squares", "lj", "gsd"],
                     help="hard_spheres: the headline (2^20 spheres); replicas: 256 independent boxes in one batch; "
                          "disks: 4096 hard disks; cubes: 2^18 hard cubes; lj: 2^19 Lennard-Jones sites; "
                          "gsd: GSD frames of the 2^20-sphere state")
@@ -470,7 +482,7 @@ def main():
     if args.workload == "replicas":
         run_replicas(args, local_rank)
         return
-    if args.workload in ("disks", "cubes", "lj"):
+    if args.workload in ("disks", "cubes", "squares", "lj"):
         run_config(args, local_rank)
         return
     if args.workload == "gsd":

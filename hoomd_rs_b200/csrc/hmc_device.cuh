@@ -292,48 +292,59 @@ struct FlatStencil {
     float s0, s1;      // slow-axis shifts of this lane's row
 };
 
+// Part `wrapped_part` of stencil row r around space m (the row's spaces m[last]-1 .. m[last]+1,
+// split where the fast axis wraps): its first slot and length, and the row's slow-axis shifts.
+// A row repeated on a two-space slow axis, and the wrapped part of a row that does not wrap,
+// are empty.
+template <int DIM>
+__device__ __forceinline__ void stencil_part(const Geometry& g, const uint32_t* __restrict__ cs, const uint32_t* m,
+                                             int r, bool wrapped_part, uint32_t& lo, uint32_t& len, float& s0,
+                                             float& s1) {
+    const int i0 = DIM == 3 ? r / 3 - 1 : 0;
+    const int i1 = DIM == 3 ? r % 3 - 1 : r - 1;
+    const uint32_t sf = g.shape[DIM - 1], mf = m[DIM - 1];
+    uint32_t base;
+    bool skip;
+    if (DIM == 3) {
+        skip = (i0 == -1 && g.shape[0] == 2) || (i1 == -1 && g.shape[1] == 2);
+        base = (wrap_index((int)m[0] + i0, g.shape[0]) * g.shape[1] + wrap_index((int)m[1] + i1, g.shape[1])) * sf;
+        s0 = (float)i0 * g.w32[0];
+        s1 = (float)i1 * g.w32[1];
+    } else {
+        skip = i1 == -1 && g.shape[0] == 2;
+        base = wrap_index((int)m[0] + i1, g.shape[0]) * sf;
+        s0 = (float)i1 * g.w32[0];
+        s1 = 0.f;
+    }
+    // spaces [a, b) of the row along the fast axis
+    uint32_t a = 0, b = 0;
+    if (sf == 2) {
+        b = wrapped_part ? 0u : 2u;
+    } else if (mf >= 1 && mf + 1 < sf) {
+        if (!wrapped_part) a = mf - 1, b = mf + 2;
+    } else if (mf == 0) {
+        if (wrapped_part) a = sf - 1, b = sf;
+        else a = 0, b = 2;
+    } else {
+        if (wrapped_part) a = 0, b = 1;
+        else a = sf - 2, b = sf;
+    }
+    lo = 0;
+    len = 0;
+    if (!skip && a < b) {
+        lo = __ldg(cs + base + a);
+        len = __ldg(cs + base + b) - lo;
+    }
+}
+
 // Call with all 32 lanes of the warp.
 template <int DIM>
 __device__ __forceinline__ FlatStencil flat_stencil(const Geometry& g, const uint32_t* __restrict__ cs,
                                                     const uint32_t* m, uint32_t lane) {
     FlatStencil fs{0u, 0u, 0u, 0.f, 0.f};
     uint32_t len = 0;
-    if (lane < 2u * kRows<DIM>) {
-        const int r = (int)(lane >> 1);
-        const bool wrapped_part = (lane & 1u) != 0;
-        const int i0 = DIM == 3 ? r / 3 - 1 : 0;
-        const int i1 = DIM == 3 ? r % 3 - 1 : r - 1;
-        const uint32_t sf = g.shape[DIM - 1], mf = m[DIM - 1];
-        uint32_t base;
-        bool skip;
-        if (DIM == 3) {
-            skip = (i0 == -1 && g.shape[0] == 2) || (i1 == -1 && g.shape[1] == 2);
-            base = (wrap_index((int)m[0] + i0, g.shape[0]) * g.shape[1] + wrap_index((int)m[1] + i1, g.shape[1])) * sf;
-            fs.s0 = (float)i0 * g.w32[0];
-            fs.s1 = (float)i1 * g.w32[1];
-        } else {
-            skip = i1 == -1 && g.shape[0] == 2;
-            base = wrap_index((int)m[0] + i1, g.shape[0]) * sf;
-            fs.s0 = (float)i1 * g.w32[0];
-        }
-        // spaces [a, b) of the row along the fast axis
-        uint32_t a = 0, b = 0;
-        if (sf == 2) {
-            b = wrapped_part ? 0u : 2u;
-        } else if (mf >= 1 && mf + 1 < sf) {
-            if (!wrapped_part) a = mf - 1, b = mf + 2;
-        } else if (mf == 0) {
-            if (wrapped_part) a = sf - 1, b = sf;
-            else a = 0, b = 2;
-        } else {
-            if (wrapped_part) a = 0, b = 1;
-            else a = sf - 2, b = sf;
-        }
-        if (!skip && a < b) {
-            fs.lo = __ldg(cs + base + a);
-            len = __ldg(cs + base + b) - fs.lo;
-        }
-    }
+    if (lane < 2u * kRows<DIM>)
+        stencil_part<DIM>(g, cs, m, (int)(lane >> 1), (lane & 1u) != 0, fs.lo, len, fs.s0, fs.s1);
     const unsigned full = 0xffffffffu;
     uint32_t x = len;
 #pragma unroll

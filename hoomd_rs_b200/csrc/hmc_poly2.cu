@@ -10,16 +10,24 @@
 // multiply-add follows the reference's expression order; sin and cos are correctly rounded
 // (cr_sincos), so the FP64 decision is the reference's on a correctly rounded libm.
 //
-// One warp per trial, as for polyhedra: all lanes compute the same trial move, then take the
-// stencil's candidates 32 at a time across its rows, with an early exit by vote. FP32 + recheck: candidates whose
-// FP32 centre distance clears the circumcircles by more than the FP32 error bound are
-// skipped; every other candidate runs the FP64 test.
+// The colour pass gives a warp four trials, as for polyhedra (k_sweep_poly2); injected moves
+// take one warp per move and the stencil's candidates 32 at a time, with an early exit by
+// vote. FP32 + recheck: candidates whose FP32 centre distance clears the circumcircles by more
+// than the FP32 error bound are skipped; every other candidate runs the FP64 test.
 #include <cuda_runtime.h>
 
 #include "hmc_device.cuh"
 
 namespace hmc {
 namespace {
+
+// Resident blocks per SM the colour pass is compiled for: 6 caps it at 80 registers. On 2^18
+// hard squares at area fraction 0.60 this measured 6.1e8 (FP32 prefilter) and 6.5e8 (FP64)
+// trial moves/s, against 4.3e8 and 4.2e8 uncapped (180 registers) and 1.5e8 and 1.6e8 with one
+// warp per trial.
+#ifndef HMC_POLY2_MIN_BLOCKS
+#define HMC_POLY2_MIN_BLOCKS 6
+#endif
 
 struct V2 {
     double x, y;
@@ -212,48 +220,152 @@ __device__ __forceinline__ bool poly2_overlaps(const Geometry& g, const Arrays& 
     return false;
 }
 
+// ---- the colour pass, four trials per warp ---------------------------------------------------
+// As for polyhedra (hmc_poly.cu): each group of 8 lanes computes its trial and prefilters its
+// candidates by circumcircle, the candidates that need the full FP64 test are compacted over
+// the warp into a shared-memory list, and the warp runs those tests 32 pairs at a time, ORing
+// overlaps into a per-trial mask (a trial known to overlap lists no further candidates). The
+// decision of each trial is the OR of the same pair tests as with one warp per trial.
+constexpr int kPoly2TrialsPerWarp = 4;
+constexpr uint32_t kPair2Cap = 128;  // listed pairs per warp before the warp drains the list
+
+struct Poly2Trial {
+    double t[2];
+    double angle;
+};
+
+template <bool SAT>
+__device__ __forceinline__ void drain_pairs2(const Geometry& g, const Arrays& A, const PolyShape2& sh,
+                                             const Poly2Trial* trials, const uint32_t* pair_q, const uint8_t* pair_g,
+                                             uint32_t n_pairs, uint32_t lane, uint32_t& mask, bool* range_error) {
+    __syncwarp();
+    for (uint32_t p0 = 0; p0 < n_pairs; p0 += 32) {
+        const uint32_t p = p0 + lane;
+        uint32_t bit = 0;
+        if (p < n_pairs) {
+            const uint32_t gg = pair_g[p];
+            if (!((mask >> gg) & 1u)) {
+                const uint32_t q = pair_q[p];
+                const Poly2Trial& tr = trials[gg];
+                const double t[3] = {tr.t[0], tr.t[1], 0.0};
+                const double4 s4 = ldg4(A.sorted_s + q);
+                const double sj[3] = {s4.x, s4.y, 0.0};
+                if (poly2_overlap64<SAT>(g, A, sh, t, tr.angle, sj, q, range_error)) bit = 1u << gg;
+            }
+        }
+        mask |= __reduce_or_sync(0xffffffffu, bit);
+    }
+    __syncwarp();
+}
+
 template <bool FP32, bool SAT>
-__global__ void __launch_bounds__(128) k_sweep_poly2(Geometry g, Arrays A, PolyShape2 sh, Launch L, uint32_t rotate) {
+__global__ void __launch_bounds__(128, HMC_POLY2_MIN_BLOCKS)
+    k_sweep_poly2(Geometry g, Arrays A, PolyShape2 sh, Launch L, uint32_t rotate) {
+    constexpr uint32_t G = kPoly2TrialsPerWarp, S = 32 / G;  // trials per warp, lanes per trial
     if (L.early_wait) grid_dependency_wait();  // first pass: the rebuild's arrays are read at once
-    const uint32_t lane = threadIdx.x & 31u;
+    __shared__ Poly2Trial s_trial[4][G];
+    __shared__ uint32_t s_pair_q[4][kPair2Cap];
+    __shared__ uint8_t s_pair_g[4][kPair2Cap];
+    const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
+    const uint32_t grp = lane / S, sub = lane % S;
     const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t n_warps = (gridDim.x * blockDim.x) >> 5;
     uint32_t n_accepted = 0;
     PairStats st;
     bool range_error = false;
+    const uint32_t sf = g.shape[1];
     const uint32_t n_active = active_count(A, L.color, L.round);
-    for (uint32_t w = warp; w < n_active; w += n_warps) {
+    for (uint32_t w0 = warp * G; w0 < n_active; w0 += n_warps * G) {  // warp-uniform
+        const uint32_t w = w0 + grp;
         uint32_t m[3] = {0, 0, 0};
-        unpack_m<2>(__ldg(A.color_cells + (size_t)L.color * g.color_stride + w), m);
-        const uint32_t cell = cell_index<2>(g, m);
-        const FlatStencil fs = flat_stencil<2>(g, A.cell_start, m, lane);
-        const uint32_t start = __ldg(A.cell_start + cell);
-        const uint32_t count = __ldg(A.cell_start + cell + 1) - start;
-        Sfc64 rng = make_rng(L.step, L.substep, L.seed, (uint64_t)cell);
-        const uint32_t k = start + canon_range_u32(rng, count);
-        const double4 b4 = A.sorted_b[k];
-        double x[3] = {b4.x, b4.y, 0.0};
-        double ti = A.sorted_q[k].x;
-        if (rotate) {
-            // Rotate<Angle>::propose (rotate/angle.rs:46-55): theta += Uniform(-a, a)
-            const double u = dsub(as_double(0x3FF0000000000000ULL | (rng.next_u64() >> 12)), 1.0);
-            ti = dadd(ti, dadd(dmul(u, dsub(L.max_move, -L.max_move)), -L.max_move));
-        } else {
-            double dv[3];
-            ball_sample<2>(rng, L.max_move, A.zig_x, A.zig_f, dv);
-            x[0] = dadd(x[0], dv[0]);
-            x[1] = dadd(x[1], dv[1]);
+        uint32_t k = 0;
+        bool valid = false;
+        double t[3] = {0.0, 0.0, 0.0};
+        double ti = 0.0;
+        if (w < n_active) {  // the group's trial, computed by its S lanes alike
+            unpack_m<2>(__ldg(A.color_cells + (size_t)L.color * g.color_stride + w), m);
+            const uint32_t cell = cell_index<2>(g, m);
+            const uint32_t start = __ldg(A.cell_start + cell);
+            const uint32_t count = __ldg(A.cell_start + cell + 1) - start;
+            Sfc64 rng = make_rng(L.step, L.substep, L.seed, (uint64_t)cell);
+            k = start + canon_range_u32(rng, count);
+            const double4 b4 = A.sorted_b[k];
+            double x[3] = {b4.x, b4.y, 0.0};
+            ti = A.sorted_q[k].x;
+            if (rotate) {
+                // Rotate<Angle>::propose (rotate/angle.rs:46-55): theta += Uniform(-a, a)
+                const double u = dsub(as_double(0x3FF0000000000000ULL | (rng.next_u64() >> 12)), 1.0);
+                ti = dadd(ti, dadd(dmul(u, dsub(L.max_move, -L.max_move)), -L.max_move));
+            } else {
+                double dv[3];
+                ball_sample<2>(rng, L.max_move, A.zig_x, A.zig_f, dv);
+                x[0] = dadd(x[0], dv[0]);
+                x[1] = dadd(x[1], dv[1]);
+            }
+            wrap_inv<2>(g.L, g.invL, x);  // W1 = wrap(propose(..))
+            uint32_t mt[3];
+            valid = point_to_space<2>(g, x, mt) && cell_index<2>(g, mt) == cell;
+            t[0] = x[0];
+            t[1] = x[1];
+            wrap_inv<2>(g.L, g.invL, t);
         }
-        wrap_inv<2>(g.L, g.invL, x);  // W1 = wrap(propose(..))
-        uint32_t mt[3];
-        if (!(point_to_space<2>(g, x, mt) && cell_index<2>(g, mt) == cell)) continue;
-        double t[3] = {x[0], x[1], 0.0};
-        wrap_inv<2>(g.L, g.invL, t);
-        const float4 t32 = FP32 ? cell_offsets<2>(g, t, m) : make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4 t32 = FP32 && valid ? cell_offsets<2>(g, t, m) : make_float4(0.f, 0.f, 0.f, 0.f);
+        if (sub == 0) {
+            Poly2Trial& tr = s_trial[wib][grp];
+            tr.t[0] = t[0];
+            tr.t[1] = t[1];
+            tr.angle = ti;
+        }
         grid_dependency_wait();  // the previous colour's moves are visible from here on
         allow_dependent_launch();
-        if (poly2_overlaps<FP32, SAT>(g, A, sh, t, ti, t32, (int)m[1], fs, k, lane, st, &range_error)) continue;
-        if (lane == 0) {
+        uint32_t mask = 0, n_pairs = 0;  // warp-uniform
+#pragma unroll 1
+        for (int part = 0; part < 2 * kRows<2>; ++part) {
+            uint32_t lo = 0, len = 0;
+            float s0 = 0.f, s1 = 0.f;
+            if (valid) stencil_part<2>(g, A.cell_start, m, part >> 1, (part & 1) != 0, lo, len, s0, s1);
+            const uint32_t iters = __reduce_max_sync(0xffffffffu, (len + S - 1) / S);
+            for (uint32_t it = 0; it < iters; ++it) {
+                const uint32_t j = it * S + sub;
+                const uint32_t q = lo + j;
+                bool need = false;
+                if (j < len && q != k && !((mask >> grp) & 1u)) {
+                    st.checks++;
+                    if (FP32) {
+                        const float4 o = __ldg(A.sorted_off + q);
+                        int dm = __float_as_int(o.w) - (int)m[1];
+                        if (sf >= 4) {  // the wrapped space of a row at a fast-axis end
+                            if (dm > 1)
+                                dm -= (int)sf;
+                            else if (dm < -1)
+                                dm += (int)sf;
+                        }
+                        need = fp32_dist2<2>(g, t32, o, s0, 0.f, dm) < sh.rcut2_hi32;
+                        if (need) st.rechecks++;
+                    } else {
+                        // the circumcircle test that opens poly2_overlap64
+                        const double4 s4 = ldg4(A.sorted_s + q);
+                        const double sj[3] = {s4.x, s4.y, 0.0};
+                        double d[3];
+                        need = ref_disp<2>(g, t, sj, d) < sh.rcut2;
+                    }
+                }
+                const unsigned b = __ballot_sync(0xffffffffu, need);
+                if (need) {
+                    const uint32_t pos = n_pairs + __popc(b & ((1u << lane) - 1u));
+                    s_pair_q[wib][pos] = q;
+                    s_pair_g[wib][pos] = (uint8_t)grp;
+                }
+                n_pairs += __popc(b);
+                if (n_pairs > kPair2Cap - 32) {
+                    drain_pairs2<SAT>(g, A, sh, s_trial[wib], s_pair_q[wib], s_pair_g[wib], n_pairs, lane, mask,
+                                      &range_error);
+                    n_pairs = 0;
+                }
+            }
+        }
+        drain_pairs2<SAT>(g, A, sh, s_trial[wib], s_pair_q[wib], s_pair_g[wib], n_pairs, lane, mask, &range_error);
+        if (sub == 0 && valid && !((mask >> grp) & 1u)) {
             n_accepted++;
             double sv[3] = {t[0], t[1], 0.0};
             wrap_inv<2>(g.L, g.invL, sv);
@@ -358,7 +470,8 @@ cudaError_t launch_sweep_poly2(bool fp32, bool sat, const Geometry& g, const Arr
         max_blocks = sms * 16;
     }
     PolyShape2 sh{verts, nv, rcut2, rcut2_hi32};
-    uint32_t blocks = (l.n_active + 3) / 4;
+    const uint32_t per_block = 4u * kPoly2TrialsPerWarp;  // four warps per block
+    uint32_t blocks = (l.n_active + per_block - 1) / per_block;
     if (blocks > (uint32_t)max_blocks) blocks = (uint32_t)max_blocks;
     const uint32_t rot = rotate ? 1u : 0u;
     PassLaunch pl(blocks, l.overlap_previous != 0 || l.early_wait != 0, s);
