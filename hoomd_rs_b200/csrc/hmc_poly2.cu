@@ -21,12 +21,12 @@
 namespace hmc {
 namespace {
 
-// Resident blocks per SM the colour pass is compiled for: 6 caps it at 80 registers. On 2^18
-// hard squares at area fraction 0.60 this measured 6.1e8 (FP32 prefilter) and 6.5e8 (FP64)
-// trial moves/s, against 4.3e8 and 4.2e8 uncapped (180 registers) and 1.5e8 and 1.6e8 with one
-// warp per trial.
+// Resident blocks per SM the colour pass is compiled for: 8 caps it at 64 registers. On 2^18
+// hard squares at area fraction 0.60 this measured 6.4e8 (FP32 prefilter) and 6.7e8 (FP64)
+// trial moves/s, against 6.1e8 and 6.5e8 at 80 registers, 4.3e8 and 4.2e8 uncapped (180
+// registers) and 1.5e8 and 1.6e8 with one warp per trial.
 #ifndef HMC_POLY2_MIN_BLOCKS
-#define HMC_POLY2_MIN_BLOCKS 6
+#define HMC_POLY2_MIN_BLOCKS 8
 #endif
 
 struct V2 {
