@@ -28,6 +28,12 @@ namespace {
 #ifndef HMC_SWEEP_MIN_BLOCKS
 #define HMC_SWEEP_MIN_BLOCKS 6
 #endif
+// The replica batch pass reads its geometry from the replica table and spilled 320 bytes at
+// 80 registers; at 4 blocks per SM (128 registers) it spills nothing: 2.31e9 against 2.28e9
+// trial moves/s on 256 boxes (5 blocks: 2.24e9).
+#ifndef HMC_BATCH_MIN_BLOCKS
+#define HMC_BATCH_MIN_BLOCKS 4
+#endif
 
 constexpr int kScanThreads = 256;
 constexpr int kScanItems = 8;
@@ -995,7 +1001,7 @@ __device__ __forceinline__ void add_per_replica(unsigned long long* acc, uint32_
 
 // One colour pass over all replicas that still run round `round` of this sweep.
 template <int DIM, bool FP32>
-__global__ void __launch_bounds__(128, HMC_SWEEP_MIN_BLOCKS) k_sweep_batch(Batch B, Arrays A, uint32_t color,
+__global__ void __launch_bounds__(128, HMC_BATCH_MIN_BLOCKS) k_sweep_batch(Batch B, Arrays A, uint32_t color,
                                                                              uint32_t round, uint32_t early_wait) {
     if (early_wait) grid_dependency_wait();  // first pass: the rebuild's arrays are read at once
     const uint32_t n_active = active_count(A, color, round);
