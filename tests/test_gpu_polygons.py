@@ -141,3 +141,38 @@ def test_polygon_input_validation(ctx):
     h = PairwiseCutoff(HardShape(ConvexPolygon.with_vertices(SQUARE)))
     with pytest.raises(HmcError):
         Microstate(ctx, Periodic(1.5, [10.0, 10.0]), np.zeros((1, 2)), h, orientations=[1e6])
+
+
+ROD2 = np.array([[-1.5, -0.15], [1.5, -0.15], [1.5, 0.15], [-1.5, 0.15]])
+
+
+@pytest.mark.parametrize("precision", [FP64, FP32_RECHECK])
+@pytest.mark.parametrize("kind", ["polygon", "surface_mesh"])
+def test_rod_trajectory_with_long_pair_lists(ctx, kind, precision):
+    # Thin rectangles on a tight lattice: ~28 neighbours of a trial lie inside its circumcircle,
+    # so the four trials of a warp usually list more pairs for the full test than the warp's
+    # list holds, and the pass drains it before the stencil walk ends. The trajectory must equal
+    # the oracle's.
+    make_shape, okind = KINDS[kind]
+    shape = make_shape(ROD2)
+    nx, ny = 8, 40
+    a = np.array([3.1, 0.33])
+    L = a * np.array([nx, ny])
+    idx = np.indices([nx, ny]).reshape(2, -1).T.astype(np.float64)
+    pos = -L / 2 + (idx + 0.5) * a
+    R = shape.bounding_radius
+    ang = np.zeros(len(pos))
+    g = Microstate(ctx, Periodic(2 * R, list(L)), pos, PairwiseCutoff(HardShape(shape)), seed=0x5EED0014,
+                   orientations=ang)
+    o = oracle.System(2, list(L), pos, ang, seed=0x5EED0014, interaction=okind, vertices=shape.vertices)
+    for sweep in range(6):
+        move, maximum = (TRANSLATE, 0.05) if sweep % 2 == 0 else (ROTATE, 0.03)
+        c = g.sweep(move, maximum, 1.0, precision, n_sweeps=1, increment_step=True)
+        acc, rej = o.parallel_sweep(oracle.TRANSLATE if move == TRANSLATE else oracle.ROTATE, maximum, 1.0, 2 * R)
+        o.increment_step()
+        assert (c.accepted, c.rejected) == (acc, rej), sweep
+        assert 0 < acc < acc + rej
+    po, ao, _, _ = o.state()
+    assert np.array_equal(g.positions(), po)
+    assert np.array_equal(g.orientations(), ao.reshape(-1))
+    assert g.overlap_count() == 0 == o.overlap_count()

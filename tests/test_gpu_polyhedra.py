@@ -140,3 +140,34 @@ def test_cube_overlapping_passes_equal_serialised_passes(ctx, monkeypatch, preci
         assert (ca.accepted, ca.rejected) == (cb.accepted, cb.rejected)
     assert np.array_equal(a.positions(), b.positions())
     assert np.array_equal(a.orientations(), b.orientations())
+
+
+ROD = np.array([[x, y, z] for x in (-1.5, 1.5) for y in (-0.15, 0.15) for z in (-0.15, 0.15)])
+
+
+@pytest.mark.parametrize("precision", [FP64, FP32_RECHECK])
+def test_rod_trajectory_with_long_pair_lists(ctx, precision):
+    # Thin rods on a tight lattice: a trial has hundreds of neighbours inside its circumsphere,
+    # so the four trials of a warp list far more pairs for the full test than the warp's list
+    # holds and the pass drains it many times per trial; the two-space y and z axes make every
+    # stencil row cover its whole axis. The trajectory must equal the oracle's.
+    nx, ny = 8, 18
+    a = np.array([3.1, 0.35, 0.35])
+    L = a * np.array([nx, ny, ny])
+    idx = np.indices([nx, ny, ny]).reshape(3, -1).T.astype(np.float64)
+    pos = -L / 2 + (idx + 0.5) * a
+    R = float(np.linalg.norm(ROD[0]))
+    h = PairwiseCutoff(HardShape(ConvexPolyhedron.with_vertices(ROD)))
+    g = Microstate(ctx, Periodic(2 * R, list(L)), pos, h, seed=0x5EED0013)
+    o = oracle.System(3, list(L), pos, None, seed=0x5EED0013, interaction=oracle.HARD_CONVEX_POLYHEDRON, vertices=ROD)
+    for sweep in range(4):
+        move, maximum = (TRANSLATE, 0.04) if sweep % 2 == 0 else (ROTATE, 0.03)
+        c = g.sweep(move, maximum, 1.0, precision, n_sweeps=1, increment_step=True)
+        acc, rej = o.parallel_sweep(oracle.TRANSLATE if move == TRANSLATE else oracle.ROTATE, maximum, 1.0, 2 * R)
+        o.increment_step()
+        assert (c.accepted, c.rejected) == (acc, rej), sweep
+        assert 0 < acc < acc + rej
+    po, qo, _, _ = o.state()
+    assert np.array_equal(g.positions(), po)
+    assert np.array_equal(g.orientations(), qo)
+    assert g.overlap_count() == 0 == o.overlap_count()
