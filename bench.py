@@ -267,6 +267,94 @@ def run_replicas(args, local_rank):
     b.close()
 
 
+def run_lj_replicas(args, local_rank):
+    """64 independent Lennard-Jones boxes of 8192 bodies (rho 0.8, r_cut = r_shift = 2.5), each
+    at its own kT drawn from U[0.8, 2.0], in one hmc_batch; one step = one ParallelSweep of
+    every replica. Also timed: FP64, and the same 64 boxes swept one Microstate after another
+    (what a caller without batches would do)."""
+    import torch
+    import oracle
+    from hoomd_rs_b200 import (FP32_RECHECK, FP64, TRANSLATE, Batch, Context, Isotropic, LennardJones, Microstate,
+                               PairwiseCutoff, Periodic, Shifted, lattice)
+    torch.cuda.set_device(local_rank)
+    ctx = Context(local_rank)
+    n, n_rep, rho, r_cut, d = 8192, 64, 0.8, 2.5, 0.1
+    kts = np.random.default_rng(0x5EED0050).uniform(0.8, 2.0, n_rep)
+    h = PairwiseCutoff(Isotropic(Shifted(LennardJones(1.0, 1.0), r_cut), r_cut))
+    reps = []
+    for k in range(n_rep):
+        pos, L = lattice.lennard_jones_box(n, rho, 3, 0x5EED0050 + k)
+        reps.append({"boundary": Periodic(r_cut, [L] * 3), "positions": pos, "seed": 0x5EED0050 + k, "hamiltonian": h})
+
+    def timed_batch(precision, steps, warmup):
+        b = Batch(ctx, reps)
+        for _ in range(warmup):
+            b.sweep(d, precision, increment_step=True, temperatures=kts)
+        torch.cuda.synchronize()
+        launches0 = b.kernel_launches()
+        t0 = time.perf_counter()
+        trials = 0
+        for _ in range(steps):
+            _, tot = b.sweep(d, precision, increment_step=True, temperatures=kts)
+            trials += tot.total()
+        torch.cuda.synchronize()
+        el = time.perf_counter() - t0
+        out = (trials / el, 1e3 * el / steps, b.kernel_launches() - launches0, [b.positions(k) for k in (0, 31)])
+        b.close()
+        return out
+
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    v32, ms32, launches, p32 = timed_batch(FP32_RECHECK, args.steps, args.warmup)
+    clocks = sampler.stop()
+    v64, ms64, _, p64 = timed_batch(FP64, args.steps, args.warmup)
+    # the same replicas as separate systems, swept one after another
+    singles = [Microstate(ctx, r["boundary"], r["positions"], h, seed=r["seed"]) for r in reps]
+    for k, m in enumerate(singles):
+        m.sweep(TRANSLATE, d, float(kts[k]), FP32_RECHECK, n_sweeps=args.warmup, increment_step=True)
+    s_steps = max(1, min(args.steps, 5))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    s_trials = 0
+    for _ in range(s_steps):
+        for k, m in enumerate(singles):
+            s_trials += m.sweep(TRANSLATE, d, float(kts[k]), FP32_RECHECK, n_sweeps=1, increment_step=True).total()
+    torch.cuda.synchronize()
+    v_single = s_trials / (time.perf_counter() - t0)
+    for m in singles:
+        m.close()
+    line = {"metric": "trial moves/s, 64-replica Lennard-Jones batch", "value": v32, "unit": UNIT, "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms32, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "fp32 sums + fp64 recheck (fp64 state)", "data": "synthetic",
+            "config": {"workload": "64 Lennard-Jones boxes of 8192 bodies, rho 0.8, eps = sigma = 1, "
+                                   "r_cut = r_shift = 2.5, kT_k ~ U[0.8, 2.0], FCC + 0.01 jitter, translation 0.1, "
+                                   "one batched ParallelSweep of every replica per step", "n_bodies_total": n * n_rep,
+                       "replicas": n_rep,
+                       "timing": "host wall clock around the batched sweep calls (each ends in a device sync)"},
+            "fp64": {"value": v64, "ms_per_step": ms64},
+            "mismatches": int(sum(np.count_nonzero(np.any(a != b, axis=1)) for a, b in zip(p32, p64))),
+            "one_system_after_another": {"value": v_single, "precision": "fp32_recheck"},
+            "gpu_launches": launches, "clocks": clocks}
+    if not args.no_cpu_baseline:
+        threads = host_threads()
+        r0 = reps[0]
+        o = oracle.System(3, r0["boundary"].edge_lengths, r0["positions"], seed=r0["seed"],
+                          interaction=oracle.LENNARD_JONES, lj_epsilon=1.0, lj_sigma=1.0, lj_r_cut=r_cut,
+                          lj_r_shift=r_cut)
+        trials, t0, sweeps = 0, time.perf_counter(), 0
+        while True:
+            a_, r_ = o.parallel_sweep(oracle.TRANSLATE, d, float(kts[0]), r_cut, threads=threads)
+            o.increment_step()
+            trials += a_ + r_
+            sweeps += 1
+            el = time.perf_counter() - t0
+            if el >= 10.0 or sweeps >= 200:
+                break
+        line["cpu_baseline"] = {"value": trials / el, "unit": UNIT, "cores": threads, "kind": "port",
+                                "sample": f"{sweeps} ParallelSweep sweeps of replica 0 ({el:.1f} s, {threads} threads)"}
+    print(json.dumps(line), flush=True)
+
+
 def run_config(args, local_rank):
     """The other single-box configurations, FP32+recheck and FP64 from the same state,
     device-timed per step like the headline, with the oracle's ParallelSweep on the host cores
@@ -467,7 +555,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="hard_spheres",
-                    choices=["hard_spheres", "replicas", "disks", "cubes", "squares", "lj", "gsd"],
+                    choices=["hard_spheres", "replicas", "lj_replicas", "disks", "cubes", "squares", "lj", "gsd"],
                     help="hard_spheres: the headline (2^20 spheres); replicas: 256 independent boxes in one batch; "
                          "disks: 4096 hard disks; cubes: 2^18 hard cubes; lj: 2^19 Lennard-Jones sites; "
                          "gsd: GSD frames of the 2^20-sphere state")
@@ -481,6 +569,9 @@ def main():
         return
     if args.workload == "replicas":
         run_replicas(args, local_rank)
+        return
+    if args.workload == "lj_replicas":
+        run_lj_replicas(args, local_rank)
         return
     if args.workload in ("disks", "cubes", "squares", "lj"):
         run_config(args, local_rank)

@@ -805,13 +805,15 @@ class GrandCanonical:
 
 
 class Batch:
-    """Independent hard-sphere replicas swept together (hmc_batch_*): one counting sort and one
-    kernel per colour pass for all replicas. Replica k evolves exactly as a Microstate built
-    from the same (boundary, positions, diameter, seed, step, substep) would."""
+    """Independent replicas swept together (hmc_batch_*): one counting sort and one kernel per
+    colour pass for all replicas. Replica k evolves exactly as a Microstate built from the same
+    (boundary, positions, hamiltonian, seed, step, substep) would. All replicas hold hard spheres,
+    or all hold Lennard-Jones bodies (each replica with its own parameters and temperature)."""
 
     def __init__(self, ctx: Context, replicas):
-        """replicas: dicts with keys boundary (Periodic), positions, diameter (default 1),
-        seed, step, substep (default 0)."""
+        """replicas: dicts with keys boundary (Periodic), positions, seed, step, substep (default
+        0), and either diameter (hard spheres, default 1) or hamiltonian (PairwiseCutoff of
+        HardSphere or of Isotropic(Shifted(LennardJones)))."""
         lib = load_library()
         self.n_replicas = len(replicas)
         descs = (hmc_system_desc * self.n_replicas)()
@@ -830,8 +832,19 @@ class Batch:
                 d.edge_lengths[a] = x
             d.n_bodies = pos.shape[0]
             d.step, d.substep, d.seed = r.get("step", 0), r.get("substep", 0), r.get("seed", 0)
-            d.interaction = HARD_SPHERE
-            d.diameter = r.get("diameter", 1.0)
+            ham = r.get("hamiltonian")
+            pair = None if ham is None else ham.pair
+            if pair is None or isinstance(pair, HardSphere):
+                d.interaction = HARD_SPHERE
+                d.diameter = r.get("diameter", 1.0) if pair is None else pair.diameter
+            elif isinstance(pair, Isotropic) and isinstance(pair.interaction, Shifted):
+                d.interaction = LENNARD_JONES
+                d.lj_epsilon = pair.interaction.f.epsilon
+                d.lj_sigma = pair.interaction.f.sigma
+                d.lj_r_cut = pair.r_cut
+                d.lj_r_shift = pair.interaction.r_shift
+            else:
+                raise HmcError(NOT_SUPPORTED, f"batches of {type(pair).__name__}")
             d.boundary_range = r["boundary"].maximum_interaction_range
         ptrs = (_dp * self.n_replicas)(*[p.ctypes.data_as(_dp) for p in self._pos])
         h = _vp()
@@ -839,14 +852,16 @@ class Batch:
         self._h = h
         self.ctx = ctx
 
-    def sweep(self, maxima, precision: int = FP32_RECHECK, n_sweeps: int = 1, increment_step: bool = False):
-        """ParallelSweep::apply on every replica (replica k moves up to maxima[k]); returns
-        (per-replica Counts, batch total Count)."""
+    def sweep(self, maxima, precision: int = FP32_RECHECK, n_sweeps: int = 1, increment_step: bool = False,
+              temperatures=1.0):
+        """ParallelSweep::apply on every replica (replica k moves up to maxima[k] at kT =
+        temperatures[k]); returns (per-replica Counts, batch total Count)."""
         maxima = np.broadcast_to(np.asarray(maxima, dtype=np.float64), (self.n_replicas,))
+        kts = np.broadcast_to(np.asarray(temperatures, dtype=np.float64), (self.n_replicas,))
         ps = (hmc_sweep_params * self.n_replicas)()
         for k in range(self.n_replicas):
-            ps[k] = hmc_sweep_params(C.sizeof(hmc_sweep_params), TRANSLATE, float(maxima[k]), 1.0, precision, n_sweeps,
-                                     int(increment_step), 0)
+            ps[k] = hmc_sweep_params(C.sizeof(hmc_sweep_params), TRANSLATE, float(maxima[k]), float(kts[k]), precision,
+                                     n_sweeps, int(increment_step), 0)
         cs = (hmc_count * self.n_replicas)()
         tot = hmc_count()
         _check(_lib.hmc_batch_sweep(self._h, ps, cs, C.byref(tot)))

@@ -204,9 +204,8 @@ double lj_energy_host(double four_eps, double sigma, double r) {
 // E bounds the per-axis FP32 displacement error (as for spheres); the cut-off band is the
 // r^2 interval in which the FP32 r^2 cannot decide r^2 < r_cut^2, and band_energy bounds the
 // energy the FP64 pass may count for a pair in it.
-void lj_setup(hmc_system* s, double eps, double sigma, double rcut, double rshift) {
+void lj_setup_for(int dim, const Geometry& geom, Pair& P, double eps, double sigma, double rcut, double rshift) {
     const double u32 = std::ldexp(1.0, -24), u64 = std::ldexp(1.0, -53);
-    Pair& P = s->pair;
     P.lj_sigma = sigma;
     P.lj_four_eps = 4.0 * eps;
     P.lj_rcut2 = rcut * rcut;
@@ -215,9 +214,9 @@ void lj_setup(hmc_system* s, double eps, double sigma, double rcut, double rshif
     P.lj_four_eps32 = (float)P.lj_four_eps;
     P.lj_e_shift32 = (float)P.lj_e_shift;
     double wmax = 0, Lmax = 0;
-    for (int a = 0; a < s->dim; ++a) {
-        wmax = std::max(wmax, s->geom.width[a]);
-        Lmax = std::max(Lmax, s->geom.L[a]);
+    for (int a = 0; a < dim; ++a) {
+        wmax = std::max(wmax, geom.width[a]);
+        Lmax = std::max(Lmax, geom.L[a]);
     }
     // the FP32 sigma^2 and 4 eps carry one rounding each; fold them into E generously
     const double E = (8.0 * u32 * wmax + 16.0 * u64 * (Lmax + wmax) + 4.0 * u32 * sigma) * fp32_band_scale();
@@ -228,6 +227,10 @@ void lj_setup(hmc_system* s, double eps, double sigma, double rcut, double rshif
     double e_lo = lj_energy_host(P.lj_four_eps, sigma, std::sqrt(std::max(P.lj_rcut2 - 2.0 * band, 0.0))) - P.lj_e_shift;
     double e_hi = lj_energy_host(P.lj_four_eps, sigma, std::sqrt(P.lj_rcut2 + 2.0 * band)) - P.lj_e_shift;
     P.lj_band_energy = (float)(2.0 * std::max(std::fabs(e_lo), std::fabs(e_hi)) + 1e-7);
+}
+
+void lj_setup(hmc_system* s, double eps, double sigma, double rcut, double rshift) {
+    lj_setup_for(s->dim, s->geom, s->pair, eps, sigma, rcut, rshift);
 }
 
 // Pair thresholds that depend on the box (FP32 bounds use the space widths and box lengths).
@@ -1548,6 +1551,7 @@ struct hmc_batch {
     std::vector<void*> allocations;
     uint64_t kernel_launches = 0;
     uint32_t rounds_guess = 2;
+    uint32_t interaction = HMC_HARD_SPHERE;  // the same for every replica
 };
 
 namespace {
@@ -1629,6 +1633,8 @@ hmc_status hmc_batch_create(hmc_context* ctx, uint32_t n_replicas, const hmc_sys
     *out = nullptr;
     if (n_replicas == 0 || n_replicas > 65535) return fail(HMC_INVALID_ARGUMENT, "1 to 65535 replicas");
     const uint32_t dim = descs[0].dim;
+    const uint32_t interaction = descs[0].interaction;
+    const bool lj = interaction == HMC_LENNARD_JONES;
     uint64_t n_total = 0, cells_total = 0;
     std::vector<Replica> reps(n_replicas);
     for (uint32_t k = 0; k < n_replicas; ++k) {
@@ -1636,9 +1642,15 @@ hmc_status hmc_batch_create(hmc_context* ctx, uint32_t n_replicas, const hmc_sys
         if (d->struct_size < sizeof(hmc_system_desc)) return fail(HMC_INVALID_ARGUMENT, "replica %u: struct_size", k);
         if (d->dim != dim || (dim != 2 && dim != 3))
             return fail(HMC_INVALID_ARGUMENT, "replica %u: all replicas need the same dim, 2 or 3", k);
-        if (d->interaction != HMC_HARD_SPHERE)
-            return fail(HMC_NOT_SUPPORTED, "replica %u: batches hold hard spheres", k);
-        if (!(d->diameter > 0.0)) return fail(HMC_INVALID_ARGUMENT, "replica %u: diameter must be positive", k);
+        if (d->interaction != HMC_HARD_SPHERE && d->interaction != HMC_LENNARD_JONES)
+            return fail(HMC_NOT_SUPPORTED, "replica %u: batches hold hard spheres or Lennard-Jones bodies", k);
+        if (d->interaction != interaction)
+            return fail(HMC_INVALID_ARGUMENT, "replica %u: all replicas need the same interaction", k);
+        if (!lj && !(d->diameter > 0.0)) return fail(HMC_INVALID_ARGUMENT, "replica %u: diameter must be positive", k);
+        if (lj && (!(d->lj_sigma > 0.0) || !(d->lj_r_cut > 0.0) || !(d->lj_r_shift > 0.0) ||
+                   !std::isfinite(d->lj_epsilon) || !std::isfinite(d->lj_sigma) || !std::isfinite(d->lj_r_cut) ||
+                   !std::isfinite(d->lj_r_shift)))
+            return fail(HMC_INVALID_ARGUMENT, "replica %u: Lennard-Jones sigma, r_cut and r_shift must be positive", k);
         if (d->n_bodies > 0 && !positions[k]) return fail(HMC_INVALID_ARGUMENT, "replica %u: positions is NULL", k);
         for (uint32_t a = 0; a < dim; ++a)
             if (!(d->edge_lengths[a] > 0.0) || !std::isfinite(d->edge_lengths[a]))
@@ -1648,7 +1660,7 @@ hmc_status hmc_batch_create(hmc_context* ctx, uint32_t n_replicas, const hmc_sys
                 return fail(HMC_NAN_STATE, "replica %u: position %llu is not finite", k, (unsigned long long)(i / dim));
         Replica& r = reps[k];
         std::memset(&r, 0, sizeof(Replica));
-        const double pair_range = d->diameter;
+        const double pair_range = lj ? d->lj_r_cut : d->diameter;  // maximum_interaction_range
         const double boundary_range = d->boundary_range > 0.0 ? d->boundary_range : pair_range;
         const double body_range = d->body_interaction_range > 0.0 ? d->body_interaction_range : pair_range;
         double min_l = d->edge_lengths[0];
@@ -1678,8 +1690,13 @@ hmc_status hmc_batch_create(hmc_context* ctx, uint32_t n_replicas, const hmc_sys
         }
         r.g.n_cells = (uint32_t)cells;
         r.g.color_stride = (uint32_t)(cells >> dim);
-        r.p.sigma2 = d->diameter * d->diameter;
-        sphere_bound_for((int)dim, r.g, r.p);
+        if (lj) {
+            lj_setup_for((int)dim, r.g, r.p, d->lj_epsilon, d->lj_sigma, d->lj_r_cut, d->lj_r_shift);
+        } else {
+            r.p.sigma2 = d->diameter * d->diameter;
+            sphere_bound_for((int)dim, r.g, r.p);
+        }
+        r.kt = 1.0;
         r.cell_base = (uint32_t)cells_total;
         r.body_base = (uint32_t)n_total;
         r.n_bodies = (uint32_t)d->n_bodies;
@@ -1700,6 +1717,7 @@ hmc_status hmc_batch_create(hmc_context* ctx, uint32_t n_replicas, const hmc_sys
     bt->n = n_total;
     bt->cells = (uint32_t)cells_total;
     bt->rep = reps;
+    bt->interaction = interaction;
     auto destroy_fail = [&](hmc_status st) {
         std::string msg = g_last_error;
         hmc_batch_destroy(bt);
@@ -1784,7 +1802,7 @@ hmc_status hmc_batch_sweep(hmc_batch* bt, const hmc_sweep_params* params, hmc_co
     if (!bt || !params) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
     const hmc_sweep_params& p0 = params[0];
     if (p0.struct_size < sizeof(hmc_sweep_params)) return fail(HMC_INVALID_ARGUMENT, "hmc_sweep_params.struct_size");
-    if (p0.move != HMC_TRANSLATE) return fail(HMC_NOT_SUPPORTED, "hard spheres take translation moves");
+    if (p0.move != HMC_TRANSLATE) return fail(HMC_NOT_SUPPORTED, "batch replicas take translation moves");
     if (p0.precision > HMC_FP32_RECHECK) return fail(HMC_INVALID_ARGUMENT, "precision");
     for (uint32_t k = 0; k < bt->n_rep; ++k) {
         const hmc_sweep_params& p = params[k];
@@ -1795,7 +1813,12 @@ hmc_status hmc_batch_sweep(hmc_batch* bt, const hmc_sweep_params* params, hmc_co
         for (int a = 0; a < bt->dim; ++a) lmax = std::max(lmax, bt->rep[k].g.L[a]);
         if (!(p.maximum > 0.0) || !(p.maximum <= 4.0 * lmax))
             return fail(HMC_INVALID_ARGUMENT, "replica %u: maximum must be in (0, 4 box lengths]", k);
-        bt->rep[k].max_move = p.maximum;
+        if (!(p.temperature > 0.0) || !std::isfinite(p.temperature))
+            return fail(HMC_INVALID_ARGUMENT, "replica %u: temperature must be positive", k);
+    }
+    for (uint32_t k = 0; k < bt->n_rep; ++k) {
+        bt->rep[k].max_move = params[k].maximum;
+        bt->rep[k].kt = params[k].temperature;  // Isothermal kT of replica k (hard spheres ignore it)
     }
     HMC_CUDA(cudaSetDevice(bt->ctx->device));
     const bool fp32 = p0.precision == HMC_FP32_RECHECK;
@@ -1811,8 +1834,12 @@ hmc_status hmc_batch_sweep(hmc_batch* bt, const hmc_sweep_params* params, hmc_co
         auto enqueue = [&](uint32_t r0, uint32_t r1) -> hmc_status {
             for (uint32_t round = r0; round < r1; ++round)
                 for (uint32_t c = 0; c < colors; ++c) {
-                    HMC_CUDA(launch_sweep_batch(bt->dim, fp32, bt->b, bt->arr, c, round, bt->b.color_stride,
-                                                round > 0 || c > 0, round == 0 && c == 0, bt->stream));
+                    if (bt->interaction == HMC_LENNARD_JONES)
+                        HMC_CUDA(launch_sweep_batch_lj(bt->dim, fp32, bt->b, bt->arr, c, round, bt->b.color_stride,
+                                                       round > 0 || c > 0, round == 0 && c == 0, bt->stream));
+                    else
+                        HMC_CUDA(launch_sweep_batch(bt->dim, fp32, bt->b, bt->arr, c, round, bt->b.color_stride,
+                                                    round > 0 || c > 0, round == 0 && c == 0, bt->stream));
                     bt->kernel_launches += 1;
                 }
             return HMC_OK;
@@ -1896,6 +1923,7 @@ hmc_status hmc_batch_set_state(hmc_batch* bt, uint32_t replica, const double* po
 
 hmc_status hmc_batch_overlap_check(hmc_batch* bt, uint64_t* n_overlaps) {
     if (!bt || !n_overlaps) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
+    if (bt->interaction == HMC_LENNARD_JONES) return fail(HMC_NOT_SUPPORTED, "overlap check of a soft potential");
     HMC_CUDA(cudaSetDevice(bt->ctx->device));
     hmc_status st = batch_rebuild(bt, true);
     if (st) return st;

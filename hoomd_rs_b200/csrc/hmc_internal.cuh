@@ -154,7 +154,7 @@ __device__ __forceinline__ void allow_dependent_launch() { asm volatile("griddep
 // thresholds, counter and place in the batch's concatenated arrays.
 struct Replica {
     Geometry g;          // box and checkerboard; the origin is re-drawn every sweep
-    Pair p;              // hard-sphere thresholds
+    Pair p;              // pair parameters and FP32 thresholds (hard spheres or Lennard-Jones)
     uint32_t cell_base;  // first space of the replica in the batch's space arrays
     uint32_t body_base;  // first body of the replica
     uint32_t n_bodies;
@@ -163,6 +163,7 @@ struct Replica {
     uint32_t substep;
     uint32_t seed;
     double max_move;
+    double kt;           // Isothermal kT of the current sweep (Lennard-Jones)
 };
 
 // Batch-wide tables; the Arrays of a batch span all replicas (bodies, spaces, colour lists).
@@ -185,11 +186,14 @@ struct Batch {
 cudaError_t launch_rebuild(int dim, const Geometry& g, const Arrays& a, uint32_t n, bool write_s, cudaStream_t s);
 // Per-replica rounds of a batch sweep into Replica::rounds, their maximum into DeviceStats::rounds.
 cudaError_t launch_batch_rounds(const Batch& b, Replica* rep, DeviceStats* stats, cudaStream_t s);
-// Batches of hard-sphere replicas: the rebuild and the colour pass over all replicas at once.
+// Batches of replicas: the rebuild and the hard-sphere colour pass over all replicas at once.
 cudaError_t launch_rebuild_batch(int dim, const Batch& b, const Arrays& a, uint32_t n, bool write_s, cudaStream_t s);
 cudaError_t launch_sweep_batch(int dim, bool fp32, const Batch& b, const Arrays& a, uint32_t color, uint32_t round,
                                uint32_t max_active, bool overlap_previous, bool early_wait, cudaStream_t s);
 cudaError_t launch_overlap_batch(int dim, const Batch& b, const Arrays& a, uint32_t n, cudaStream_t s);
+// Batches of Lennard-Jones replicas: one warp per trial over every replica's colour list (hmc_lj.cu).
+cudaError_t launch_sweep_batch_lj(int dim, bool fp32, const Batch& b, const Arrays& a, uint32_t color, uint32_t round,
+                                  uint32_t max_active, bool overlap_previous, bool early_wait, cudaStream_t s);
 // coop selects the warp-cooperative pass (the per-lane pass otherwise).
 cudaError_t launch_sweep_sphere(int dim, bool fp32, const Geometry& g, const Arrays& a, const Pair& p,
                                 const Launch& l, bool coop, cudaStream_t s);

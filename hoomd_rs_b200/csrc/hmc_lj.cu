@@ -26,6 +26,12 @@ namespace {
 #ifndef HMC_LJ_MIN_BLOCKS
 #define HMC_LJ_MIN_BLOCKS 9
 #endif
+// The same for the batch passes: 7 (72 registers) still runs a colour pass of 64 replicas of
+// 8192 bodies (4,096 trials) in one wave and spills less: 1.34e8 (FP32) and 1.15e8 (FP64)
+// trial moves/s there, against 1.18e8 and 1.07e8 at 56 registers and 1.01e8 and 7.1e7 at 80.
+#ifndef HMC_LJ_BATCH_MIN_BLOCKS
+#define HMC_LJ_BATCH_MIN_BLOCKS 7
+#endif
 
 constexpr float kU32 = 5.9604645e-8f;  // 2^-24
 
@@ -407,6 +413,219 @@ __global__ void __launch_bounds__(128, HMC_LJ_MIN_BLOCKS) k_sweep_lj32(Geometry 
     flush_stats(A.stats, pst, n_accepted);
 }
 
+// One colour pass over every replica of a batch that still runs round `round` of this sweep,
+// FP64: one warp per trial as in k_sweep_lj, with the box, checkerboard, pair parameters,
+// Counter, move size and kT of the trial's replica from the replica table.
+template <int DIM>
+__global__ void __launch_bounds__(128, HMC_LJ_BATCH_MIN_BLOCKS)
+    k_sweep_batch_lj(Batch B, Arrays A, uint32_t color, uint32_t round, uint32_t early_wait) {
+    if (early_wait) grid_dependency_wait();  // first pass: the rebuild's arrays are read at once
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t n_warps = (gridDim.x * blockDim.x) >> 5;
+    uint32_t n_accepted = 0;
+    PairStats pst;
+    const uint32_t n_active = active_count(A, color, round);
+    for (uint32_t w = warp; w < n_active; w += n_warps) {
+        const size_t e = (size_t)color * B.color_stride + w;
+        const uint32_t r = __ldg(B.color_rep + e);
+        const Replica& R = B.rep[r];
+        if (round >= R.rounds) continue;  // warp-uniform
+        const Geometry& g = R.g;
+        const uint32_t* cs = A.cell_start + R.cell_base;
+        uint32_t m[3] = {0, 0, 0};
+        unpack_m<DIM>(__ldg(A.color_cells + e), m);
+        const uint32_t cell = cell_index<DIM>(g, m);
+        const FlatStencil fs = flat_stencil<DIM>(g, cs, m, lane);
+        const uint32_t start = __ldg(cs + cell);
+        const uint32_t count = __ldg(cs + cell + 1) - start;
+        Sfc64 rng = make_rng(R.step, R.substep + round, R.seed, (uint64_t)cell);
+        const uint32_t k = start + canon_range_u32(rng, count);
+        const double4 b4 = A.sorted_b[k];
+        double x[3] = {b4.x, b4.y, b4.z};
+        double dv[3];
+        ball_sample<DIM>(rng, R.max_move, A.zig_x, A.zig_f, dv);
+        const double u = uniform01(rng);
+#pragma unroll
+        for (int a = 0; a < DIM; ++a) x[a] = dadd(x[a], dv[a]);
+        wrap_inv<DIM>(g.L, g.invL, x);
+        uint32_t mt[3];
+        if (!(point_to_space<DIM>(g, x, mt) && cell_index<DIM>(g, mt) == cell)) continue;
+        double t[3] = {x[0], x[1], DIM == 3 ? x[2] : 0.0};
+        wrap_inv<DIM>(g.L, g.invL, t);
+        grid_dependency_wait();  // the previous colour's moves are visible from here on
+        allow_dependent_launch();
+        const double4 s4 = ldg4(A.sorted_s + k);
+        const double si[3] = {s4.x, s4.y, s4.z};
+        double e_new, e_old;
+        lj_energy64<DIM, true>(g, A, R.p, t, si, fs, k, true, lane, e_new, e_old);
+        const double du = dsub(e_new, e_old);
+        if ((du <= 0.0 || u < exp(ddiv(-du, R.kt))) && lane == 0) {
+            n_accepted++;
+            atomicAdd(B.accepted + r, 1ull);
+            double sv[3] = {t[0], t[1], t[2]};
+            wrap_inv<DIM>(g.L, g.invL, sv);
+            A.sorted_b[k] = make_double4(t[0], t[1], t[2], 0.0);
+            A.sorted_s[k] = make_double4(sv[0], sv[1], sv[2], 0.0);
+            A.sorted_off[k] = cell_offsets<DIM>(g, sv, m);
+            A.body_pos[A.sorted_body[k]] = make_double4(t[0], t[1], t[2], 0.0);
+        }
+        __syncwarp();
+    }
+    grid_dependency_wait();
+    allow_dependent_launch();
+    flush_stats(A.stats, pst, n_accepted);
+}
+
+// The FP32 + recheck pass over a batch: k_sweep_lj32 (four trials per block, an undecided
+// trial rechecked by the whole block in the FP64 pass's order) with each trial's geometry and
+// parameters from its replica; the owner also publishes its replica for the helping warps.
+template <int DIM>
+__global__ void __launch_bounds__(128, HMC_LJ_BATCH_MIN_BLOCKS)
+    k_sweep_batch_lj32(Batch B, Arrays A, uint32_t color, uint32_t round, uint32_t early_wait) {
+    if (early_wait) grid_dependency_wait();  // first pass: the rebuild's arrays are read at once
+    __shared__ double s_e[kRecheckChunks][2][32];
+    __shared__ SharedTrial s_trial;
+    __shared__ uint32_t s_active, s_rep;
+    const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
+    uint32_t n_accepted = 0;
+    PairStats pst;
+    if (threadIdx.x == 0) s_active = active_count(A, color, round);
+    __syncthreads();
+    const uint32_t n_active = s_active;  // block-uniform: the loop below holds barriers
+    for (uint32_t base = blockIdx.x * 4u; base < n_active; base += gridDim.x * 4u) {
+        const uint32_t w = base + wib;
+        uint32_t m[3] = {0, 0, 0};
+        uint32_t k = 0, r = 0;
+        double t[3] = {0.0, 0.0, 0.0};
+        double u = 0.0;
+        bool trial = false;
+        FlatStencil fs{0u, 0u, 0u, 0.f, 0.f};
+        if (w < n_active) {  // warp-uniform
+            const size_t e = (size_t)color * B.color_stride + w;
+            r = __ldg(B.color_rep + e);
+            const Replica& R = B.rep[r];
+            if (round < R.rounds) {
+                const Geometry& g = R.g;
+                const uint32_t* cs = A.cell_start + R.cell_base;
+                unpack_m<DIM>(__ldg(A.color_cells + e), m);
+                const uint32_t cell = cell_index<DIM>(g, m);
+                fs = flat_stencil<DIM>(g, cs, m, lane);
+                const uint32_t start = __ldg(cs + cell);
+                const uint32_t count = __ldg(cs + cell + 1) - start;
+                Sfc64 rng = make_rng(R.step, R.substep + round, R.seed, (uint64_t)cell);
+                k = start + canon_range_u32(rng, count);
+                const double4 b4 = A.sorted_b[k];
+                double x[3] = {b4.x, b4.y, b4.z};
+                double dv[3];
+                ball_sample<DIM>(rng, R.max_move, A.zig_x, A.zig_f, dv);
+                u = uniform01(rng);
+#pragma unroll
+                for (int a = 0; a < DIM; ++a) x[a] = dadd(x[a], dv[a]);
+                wrap_inv<DIM>(g.L, g.invL, x);
+                uint32_t mt[3];
+                trial = point_to_space<DIM>(g, x, mt) && cell_index<DIM>(g, mt) == cell;
+                t[0] = x[0];
+                t[1] = x[1];
+                t[2] = DIM == 3 ? x[2] : 0.0;
+                wrap_inv<DIM>(g.L, g.invL, t);
+            }
+        }
+        grid_dependency_wait();  // the previous colour's moves are visible from here on
+        allow_dependent_launch();
+        int decision = 0;
+        float d32 = 0.f;
+        if (trial) {
+            const Replica& R = B.rep[r];
+            const float4 t32 = cell_offsets<DIM>(R.g, t, m);
+            const float4 c32 = __ldg(A.sorted_off + k);
+            const Sums32 s = lj_energy32<DIM>(R.g, A, R.p, t32, c32, (int)m[DIM - 1], fs, k, lane);
+            pst.checks += s.pairs;
+            decision = decide32(s, R.kt, u);
+            d32 = s.e_new - s.e_old;
+        }
+        const bool unsure = decision < 0;
+        if (__syncthreads_or(unsure)) {
+            for (uint32_t o = 0; o < 4u; ++o) {
+                const bool mine = unsure && wib == o;
+                if (mine) {
+                    s_trial.lo[lane] = fs.lo;
+                    s_trial.pre[lane] = fs.pre;
+                    if (lane == 0) {
+                        const Geometry& g = B.rep[r].g;
+                        const double4 c4 = ldg4(A.sorted_b + k);
+                        double si[3] = {c4.x, c4.y, c4.z};
+                        wrap_inv<DIM>(g.L, g.invL, si);
+#pragma unroll
+                        for (int a = 0; a < 3; ++a) {
+                            s_trial.t[a] = t[a];
+                            s_trial.si[a] = si[a];
+                        }
+                        s_trial.total = fs.total;
+                        s_trial.self = k;
+                        s_rep = r;
+                    }
+                }
+                if (!__syncthreads_or(mine)) continue;  // also publishes s_trial and s_rep
+                const Replica& RO = B.rep[s_rep];
+                const uint32_t total = s_trial.total, self = s_trial.self;
+                const uint32_t n_chunks = (total + 31u) / 32u;
+                double ea = 0.0, eb = 0.0;
+                for (uint32_t c0 = 0; c0 < n_chunks; c0 += kRecheckChunks) {
+                    const uint32_t c1 = min(c0 + kRecheckChunks, n_chunks);
+                    for (uint32_t c = c0 + wib; c < c1; c += 4u) {
+                        const uint32_t j = c * 32u + lane;
+                        double en = 0.0, eo = 0.0;
+                        if (j < total) {
+                            const uint32_t q = shared_slot(s_trial, j);
+                            if (q != self) {
+                                const double4 b4 = ldg4(A.sorted_b + q);
+                                double sv[3] = {b4.x, b4.y, b4.z};
+                                wrap_inv<DIM>(RO.g.L, RO.g.invL, sv);
+                                en = lj_pair64(RO.p, ref_dist2<DIM>(RO.g, s_trial.t, sv));
+                                eo = lj_pair64(RO.p, ref_dist2<DIM>(RO.g, s_trial.si, sv));
+                            }
+                        }
+                        s_e[c - c0][0][lane] = en;
+                        s_e[c - c0][1][lane] = eo;
+                    }
+                    __syncthreads();
+                    if (wib == o) {
+                        for (uint32_t c = c0; c < c1; ++c) {
+                            ea = dadd(ea, s_e[c - c0][0][lane]);
+                            eb = dadd(eb, s_e[c - c0][1][lane]);
+                        }
+                    }
+                    __syncthreads();
+                }
+                if (wib == o) {
+                    const double du = dsub(warp_sum(ea), warp_sum(eb));
+                    if (lane == 0) {
+                        pst.rechecks++;
+                        const double err = fabs((double)d32 - du);
+                        pst.max_err = err > pst.max_err ? err : pst.max_err;
+                    }
+                    decision = (du <= 0.0 || u < exp(ddiv(-du, RO.kt))) ? 1 : 0;
+                }
+            }
+        }
+        if (decision == 1 && lane == 0) {
+            const Geometry& g = B.rep[r].g;
+            n_accepted++;
+            atomicAdd(B.accepted + r, 1ull);
+            double sv[3] = {t[0], t[1], t[2]};
+            wrap_inv<DIM>(g.L, g.invL, sv);
+            A.sorted_b[k] = make_double4(t[0], t[1], t[2], 0.0);
+            A.sorted_off[k] = cell_offsets<DIM>(g, sv, m);
+            A.body_pos[A.sorted_body[k]] = make_double4(t[0], t[1], t[2], 0.0);
+        }
+        __syncwarp();
+    }
+    grid_dependency_wait();
+    allow_dependent_launch();
+    flush_stats(A.stats, pst, n_accepted);
+}
+
 // Injected moves: warp per move. delta_h gets dU64 (stencils around the trial's space for the
 // final energy and around the body's space for the initial energy); the decision follows the
 // precision mode with the given uniform.
@@ -528,6 +747,27 @@ cudaError_t launch_sweep_lj(int dim, bool fp32, const Geometry& g, const Arrays&
                     : cudaLaunchKernelEx(&pl.cfg, k_sweep_lj<2>, g, a, p, l);
     return fp32 ? cudaLaunchKernelEx(&pl.cfg, k_sweep_lj32<3>, g, a, p, l)
                 : cudaLaunchKernelEx(&pl.cfg, k_sweep_lj<3>, g, a, p, l);
+}
+
+cudaError_t launch_sweep_batch_lj(int dim, bool fp32, const Batch& b, const Arrays& a, uint32_t color, uint32_t round,
+                                  uint32_t max_active, bool overlap_previous, bool early_wait, cudaStream_t s) {
+    if (max_active == 0) return cudaSuccess;
+    static int max_blocks = 0;
+    if (max_blocks == 0) {
+        int dev = 0, sms = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        max_blocks = sms * 16;
+    }
+    uint32_t blocks = (max_active + 3) / 4;  // four warps (trials) per block
+    if (blocks > (uint32_t)max_blocks) blocks = (uint32_t)max_blocks;
+    PassLaunch pl(blocks, overlap_previous || early_wait, s);
+    const uint32_t ew = early_wait ? 1u : 0u;
+    if (dim == 2)
+        return fp32 ? cudaLaunchKernelEx(&pl.cfg, k_sweep_batch_lj32<2>, b, a, color, round, ew)
+                    : cudaLaunchKernelEx(&pl.cfg, k_sweep_batch_lj<2>, b, a, color, round, ew);
+    return fp32 ? cudaLaunchKernelEx(&pl.cfg, k_sweep_batch_lj32<3>, b, a, color, round, ew)
+                : cudaLaunchKernelEx(&pl.cfg, k_sweep_batch_lj<3>, b, a, color, round, ew);
 }
 
 cudaError_t launch_eval_lj(int dim, bool fp32, const Geometry& g, const Arrays& a, const Pair& p,

@@ -242,25 +242,29 @@ hmc_status hmc_sdf(hmc_system* sys, double x_max, uint32_t n_bins, uint64_t* cou
 hmc_status hmc_gr(hmc_system* sys, double r_max, uint32_t n_bins, uint64_t* counts);
 
 /* ---- batches of independent replicas ----
- * A batch runs many hard-sphere boxes (each its own hmc_system_desc: box, diameter, Counter,
- * body count) through one set of launches: one counting sort and one kernel per colour pass
- * for all replicas. Every replica's trajectory is the one hmc_system would produce from the
- * same description. This is the replica batching of the survey's batched configuration; the
- * reference has no counterpart (a user would loop over Microstates). */
+ * A batch runs many boxes (each its own hmc_system_desc: box, pair parameters, Counter, body
+ * count) through one set of launches: one counting sort and one kernel per colour pass for all
+ * replicas. Every replica's trajectory is the one hmc_system would produce from the same
+ * description. The reference has no counterpart (a user would loop over Microstates, each
+ * with its own ParallelSweep::apply, hoomd-mc/src/parallel_sweep.rs:390-421). */
 typedef struct hmc_batch hmc_batch;
-/* positions[k]: descs[k].n_bodies * dim doubles. All replicas: HMC_HARD_SPHERE, one dim. */
+/* positions[k]: descs[k].n_bodies * dim doubles. All replicas share dim and the interaction:
+ * HMC_HARD_SPHERE, or HMC_LENNARD_JONES (each replica with its own epsilon, sigma, r_cut,
+ * r_shift). */
 hmc_status hmc_batch_create(hmc_context* ctx, uint32_t n_replicas, const hmc_system_desc* descs,
                             const double* const* positions, hmc_batch** out);
 void hmc_batch_destroy(hmc_batch* batch);
-/* params: one per replica (its own maximum); move, precision, n_sweeps, increment_step must
- * agree. counts (per replica, may be NULL) receive accepted/rejected; total (may be NULL)
- * also receives the batch's rechecks, pair_checks and max_fp32_error. */
+/* params: one per replica (its own maximum and temperature, the kT of a Lennard-Jones replica);
+ * move (HMC_TRANSLATE), precision, n_sweeps, increment_step must agree. counts (per replica,
+ * may be NULL) receive accepted/rejected; total (may be NULL) also receives the batch's
+ * rechecks, pair_checks and max_fp32_error. */
 hmc_status hmc_batch_sweep(hmc_batch* batch, const hmc_sweep_params* params, hmc_count* counts, hmc_count* total);
 hmc_status hmc_batch_get_state(hmc_batch* batch, uint32_t replica, double* positions, uint64_t* step,
                                uint32_t* substep);
 hmc_status hmc_batch_set_state(hmc_batch* batch, uint32_t replica, const double* positions, uint64_t step,
                                uint32_t substep);
-/* Overlapping pairs per replica (n_overlaps: n_replicas entries). */
+/* Overlapping pairs per replica (n_overlaps: n_replicas entries); hard spheres only
+ * (HMC_NOT_SUPPORTED for a Lennard-Jones batch). */
 hmc_status hmc_batch_overlap_check(hmc_batch* batch, uint64_t* n_overlaps);
 /* Kernels this batch enqueued so far. */
 uint64_t hmc_batch_kernel_launches(hmc_batch* batch);

@@ -77,3 +77,60 @@ def test_batch_replica_equals_oracle_and_overlap_counts(ctx):
     want = oracle.System(3, [L2] * 3, p2).overlap_count()
     assert want >= 1
     assert list(b.overlap_counts()) == [0, 0, want]
+
+
+def lj_replicas(dim, specs):
+    from hoomd_rs_b200 import Isotropic, LennardJones, Shifted
+    out = []
+    for n, rho, seed, step, r_cut in specs:
+        pos, L = lattice.lennard_jones_box(n, rho, dim, seed)
+        h = PairwiseCutoff(Isotropic(Shifted(LennardJones(1.0, 1.0), r_cut), r_cut))
+        out.append({"boundary": Periodic(r_cut, [L] * dim), "positions": pos, "seed": seed, "step": step,
+                    "hamiltonian": h})
+    return out
+
+
+# (N, density, seed, step, r_cut); different sizes, densities and cut-offs per replica
+LJ3 = [(1372, 0.8, 31, 0, 2.5), (864, 0.6, 32, 4, 2.5), (2048, 0.85, 33, 0, 2.2), (500, 0.5, 34, 1, 3.0)]
+LJ2 = [(900, 0.7, 41, 0, 2.5), (1600, 0.6, 42, 2, 2.5), (400, 0.8, 43, 0, 2.0)]
+
+
+@pytest.mark.parametrize("precision", [FP64, FP32_RECHECK])
+@pytest.mark.parametrize("dim,specs", [(3, LJ3), (2, LJ2)])
+def test_lj_batch_replicas_equal_single_systems(ctx, dim, specs, precision):
+    # Lennard-Jones replicas, each at its own temperature: replica k equals, bit for bit, a
+    # single system swept with the same move size and kT.
+    reps = lj_replicas(dim, specs)
+    maxima = np.linspace(0.08, 0.2, len(reps))
+    kts = np.linspace(0.8, 2.0, len(reps))
+    b = Batch(ctx, reps)
+    singles = [Microstate(ctx, r["boundary"], r["positions"], r["hamiltonian"], seed=r["seed"], step=r["step"])
+               for r in reps]
+    for _ in range(4):
+        counts, total = b.sweep(maxima, precision, increment_step=True, temperatures=kts)
+        for k, m in enumerate(singles):
+            c = m.sweep(TRANSLATE, float(maxima[k]), float(kts[k]), precision, n_sweeps=1, increment_step=True)
+            assert (counts[k].accepted, counts[k].rejected) == (c.accepted, c.rejected), k
+            assert 0 < c.accepted < c.total()
+    for k, m in enumerate(singles):
+        pos, step, sub = b.state(k)
+        assert np.array_equal(pos, m.positions()), k
+        assert (step, sub) == (m.step(), m.substep())
+
+
+def test_lj_batch_fp32_equals_fp64_and_rejects_overlap_check(ctx):
+    # 64 replicas of 8192 bodies at kT in [0.8, 2.0]: the FP32 + recheck batch gives the FP64
+    # batch's trajectory; the hard-sphere overlap check does not apply to a soft potential.
+    from hoomd_rs_b200 import HmcError
+    specs = [(8192, 0.8, 0x5EED0050 + k, 0, 2.5) for k in range(64)]
+    kts = np.random.default_rng(5).uniform(0.8, 2.0, 64)
+    a = Batch(ctx, lj_replicas(3, specs))
+    b = Batch(ctx, lj_replicas(3, specs))
+    for _ in range(2):
+        ca, ta = a.sweep(0.1, FP32_RECHECK, increment_step=True, temperatures=kts)
+        cb, tb = b.sweep(0.1, FP64, increment_step=True, temperatures=kts)
+        assert [(c.accepted, c.rejected) for c in ca] == [(c.accepted, c.rejected) for c in cb]
+    for k in (0, 17, 63):
+        assert np.array_equal(a.positions(k), b.positions(k))
+    with pytest.raises(HmcError):
+        a.overlap_counts()
