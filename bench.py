@@ -254,6 +254,10 @@ def run_replicas(args, local_rank):
     clocks = sampler.stop()
     over = b.overlap_counts()
     n_total = sum(n for n, _, _ in specs)
+    torch.cuda.synchronize()
+    t_sdf = time.perf_counter()
+    pressures = b.pressures(0.02, 40)
+    t_sdf = time.perf_counter() - t_sdf
     line = {"metric": "trial moves/s, 256-replica hard-sphere batch", "value": trials / el, "unit": UNIT,
             "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32 pair test + fp64 recheck",
@@ -262,7 +266,11 @@ def run_replicas(args, local_rank):
                                    "FCC starts, per-replica move sizes tuned to 0.30, one batched ParallelSweep of "
                                    "every replica per step", "n_bodies_total": n_total, "replicas": len(specs),
                        "timing": "host wall clock around the batched sweep calls (each ends in a device sync)"},
-            "overlaps_after": int(over.sum()), "gpu_launches": b.kernel_launches() - launches0, "clocks": clocks}
+            "overlaps_after": int(over.sum()), "gpu_launches": b.kernel_launches() - launches0, "clocks": clocks,
+            "sdf_pressure": {"estimator": "beta P per replica from its scale distribution (x_max 0.02, 40 bins), "
+                                          "after the timed sweeps", "min": float(pressures.min()),
+                             "median": float(np.median(pressures)), "max": float(pressures.max()),
+                             "ms_all_replicas": 1e3 * t_sdf}}
     print(json.dumps(line), flush=True)
     b.close()
 

@@ -143,6 +143,7 @@ SIGNATURES = {
     "hmc_batch_get_state": (C.c_int, [_vp, C.c_uint32, _dp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32)]),
     "hmc_batch_set_state": (C.c_int, [_vp, C.c_uint32, _dp, C.c_uint64, C.c_uint32]),
     "hmc_batch_overlap_check": (C.c_int, [_vp, C.POINTER(C.c_uint64)]),
+    "hmc_batch_sdf": (C.c_int, [_vp, C.c_double, C.c_uint32, C.POINTER(C.c_uint64)]),
     "hmc_batch_kernel_launches": (C.c_uint64, [_vp]),
     "hmc_sweep": (C.c_int, [_vp, C.POINTER(hmc_sweep_params), C.POINTER(hmc_count)]),
     "hmc_tune": (C.c_int, [_vp, C.POINTER(hmc_sweep_params), C.c_double, C.c_uint32, C.c_uint32]),
@@ -820,8 +821,10 @@ class Batch:
         self._pos = []
         self.dim = len(replicas[0]["boundary"].edge_lengths)
         self.sizes = []
+        self.edge_lengths = []
         for k, r in enumerate(replicas):
             L = [float(x) for x in r["boundary"].edge_lengths]
+            self.edge_lengths.append(L)
             pos = np.ascontiguousarray(r["positions"], dtype=np.float64).reshape(-1, len(L))
             self._pos.append(pos)
             self.sizes.append(pos.shape[0])
@@ -886,6 +889,18 @@ class Batch:
         out = np.zeros(self.n_replicas, dtype=np.uint64)
         _check(_lib.hmc_batch_overlap_check(self._h, out.ctypes.data_as(C.POINTER(C.c_uint64))))
         return out
+
+    def sdf(self, x_max: float = 0.02, n_bins: int = 40) -> np.ndarray:
+        """Scale distributions of all replicas (hard spheres): (n_replicas, n_bins) pair counts."""
+        out = np.zeros((self.n_replicas, n_bins), dtype=np.uint64)
+        _check(_lib.hmc_batch_sdf(self._h, x_max, n_bins, out.ctypes.data_as(C.POINTER(C.c_uint64))))
+        return out
+
+    def pressures(self, x_max: float = 0.02, n_bins: int = 40, fit_bins: int = 12) -> np.ndarray:
+        """beta P of every replica from its scale distribution (Microstate.pressure's estimator)."""
+        counts = self.sdf(x_max, n_bins)
+        return np.array([sdf_pressure(counts[k], self.sizes[k], float(np.prod(self.edge_lengths[k])), self.dim, x_max,
+                                      fit_bins) for k in range(self.n_replicas)])
 
     def kernel_launches(self) -> int:
         return int(_lib.hmc_batch_kernel_launches(self._h))

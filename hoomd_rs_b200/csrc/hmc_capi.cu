@@ -1552,6 +1552,7 @@ struct hmc_batch {
     uint64_t kernel_launches = 0;
     uint32_t rounds_guess = 2;
     uint32_t interaction = HMC_HARD_SPHERE;  // the same for every replica
+    std::vector<double> body_range;          // [R] ParallelSweep range of each replica
 };
 
 namespace {
@@ -1718,6 +1719,12 @@ hmc_status hmc_batch_create(hmc_context* ctx, uint32_t n_replicas, const hmc_sys
     bt->cells = (uint32_t)cells_total;
     bt->rep = reps;
     bt->interaction = interaction;
+    bt->body_range.resize(n_replicas);
+    for (uint32_t k = 0; k < n_replicas; ++k) {
+        const hmc_system_desc* d = descs + k;
+        const double pr = lj ? d->lj_r_cut : d->diameter;
+        bt->body_range[k] = d->body_interaction_range > 0.0 ? d->body_interaction_range : pr;
+    }
     auto destroy_fail = [&](hmc_status st) {
         std::string msg = g_last_error;
         hmc_batch_destroy(bt);
@@ -1918,6 +1925,81 @@ hmc_status hmc_batch_set_state(hmc_batch* bt, uint32_t replica, const double* po
     }
     r.step = step;
     r.substep = substep;
+    return HMC_OK;
+}
+
+hmc_status hmc_batch_sdf(hmc_batch* bt, double x_max, uint32_t n_bins, uint64_t* counts) {
+    if (!bt || !counts) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
+    if (bt->interaction != HMC_HARD_SPHERE) return fail(HMC_NOT_SUPPORTED, "the scale distribution is for hard spheres");
+    if (!(x_max > 0.0 && x_max < 0.5)) return fail(HMC_INVALID_ARGUMENT, "x_max must be in (0, 0.5)");
+    if (n_bins == 0 || n_bins > 8192) return fail(HMC_INVALID_ARGUMENT, "1 to 8192 bins");
+    HMC_CUDA(cudaSetDevice(bt->ctx->device));
+    // Replica by replica, hmc_sdf's histogram on a view of the batch's arrays: the replica's
+    // bodies at its offset, the (wider, so fewer) spaces of its histogram grid at the start of
+    // the batch's space arrays. The next sweep rebuilds the batch's cell order from scratch.
+    unsigned long long* d = nullptr;
+    HMC_CUDA(cudaMallocAsync((void**)&d, sizeof(unsigned long long) * n_bins, bt->stream));
+    std::vector<unsigned long long> h((size_t)n_bins * bt->n_rep);
+    hmc_status st = HMC_OK;
+    for (uint32_t k = 0; k < bt->n_rep && st == HMC_OK; ++k) {
+        const Replica& r = bt->rep[k];
+        const double sigma = std::sqrt(r.p.sigma2);
+        Geometry g = r.g;
+        const double range = std::max(sigma / (1.0 - x_max), bt->body_range[k]);
+        if (!compute_dimensions(bt->dim, g.L, range, g.width, g.shape)) {
+            st = fail(HMC_RANGE_TOO_LARGE, "replica %u: a histogram reaching %g needs two spaces per axis", k, range);
+            break;
+        }
+        uint64_t cells = 1;
+        g.any_two = 0;
+        for (int a = 0; a < bt->dim; ++a) {
+            g.w32[a] = (float)g.width[a];
+            g.invW[a] = 1.0 / g.width[a];
+            g.half_shape[a] = g.shape[a] / 2;
+            if (g.shape[a] == 2) g.any_two = 1;
+            g.origin[a] = -g.L[a] / 2.0;
+            cells *= g.shape[a];
+        }
+        g.n_cells = (uint32_t)cells;  // no more than the replica's own spaces: these are wider
+        g.color_stride = (uint32_t)(cells >> bt->dim);
+        Arrays v = bt->arr;
+        const uint32_t o = r.body_base;
+        v.body_pos += o;
+        v.sorted_b += o;
+        v.sorted_s += o;
+        v.sorted_off += o;
+        v.sorted_body += o;
+        v.slot_of_body += o;
+        v.body_cell += o;
+        v.body_rank += o;
+        v.body_m += o;
+        v.body_ori = nullptr;
+        v.sorted_q = nullptr;
+        cudaError_t e = cudaMemsetAsync(v.stats, 0, sizeof(DeviceStats), bt->stream);
+        if (e == cudaSuccess) e = launch_rebuild(bt->dim, g, v, r.n_bodies, true, bt->stream);
+        if (e == cudaSuccess)
+            e = launch_pair_histogram(bt->dim, true, g, v, r.n_bodies, sigma, x_max, (double)n_bins / x_max, n_bins, d,
+                                      bt->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(h.data() + (size_t)k * n_bins, d, sizeof(unsigned long long) * n_bins,
+                                cudaMemcpyDeviceToHost, bt->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(bt->host_stats, v.stats, sizeof(DeviceStats), cudaMemcpyDeviceToHost, bt->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(bt->stream);
+        if (e != cudaSuccess) {
+            st = fail(HMC_CUDA_ERROR, "replica %u: scale distribution: %s", k, cudaGetErrorString(e));
+            break;
+        }
+        bt->kernel_launches += 8;
+        const uint32_t f = bt->host_stats->error_flags;
+        if (f & kErrNonFinite) st = fail(HMC_NAN_STATE, "replica %u: a body position is not finite", k);
+        else if (f & kErrOutsideCheckerboard) st = fail(HMC_OUTSIDE_CHECKERBOARD, "replica %u: a body maps to no space", k);
+    }
+    cudaFreeAsync(d, bt->stream);
+    cudaError_t e2 = cudaStreamSynchronize(bt->stream);
+    if (st) return st;
+    if (e2 != cudaSuccess) return fail(HMC_CUDA_ERROR, "scale distribution: %s", cudaGetErrorString(e2));
+    for (size_t i = 0; i < h.size(); ++i) counts[i] = h[i];
     return HMC_OK;
 }
 

@@ -266,6 +266,10 @@ hmc_status hmc_batch_set_state(hmc_batch* batch, uint32_t replica, const double*
 /* Overlapping pairs per replica (n_overlaps: n_replicas entries); hard spheres only
  * (HMC_NOT_SUPPORTED for a Lennard-Jones batch). */
 hmc_status hmc_batch_overlap_check(hmc_batch* batch, uint64_t* n_overlaps);
+/* The scale distribution of every replica (hmc_sdf's pair counts by x = 1 - sigma/r over
+ * [0, x_max)): counts receives n_replicas * n_bins entries, replica by replica. Hard spheres
+ * only. The SDF pressure estimator is new (the reference has no counterpart). */
+hmc_status hmc_batch_sdf(hmc_batch* batch, double x_max, uint32_t n_bins, uint64_t* counts);
 /* Kernels this batch enqueued so far. */
 uint64_t hmc_batch_kernel_launches(hmc_batch* batch);
 

@@ -134,3 +134,26 @@ def test_lj_batch_fp32_equals_fp64_and_rejects_overlap_check(ctx):
         assert np.array_equal(a.positions(k), b.positions(k))
     with pytest.raises(HmcError):
         a.overlap_counts()
+
+
+def test_batch_sdf_equals_single_system_sdf(ctx):
+    # the scale distribution of every replica equals hmc_sdf of the same state in its own system
+    reps = replicas(3, SPECS3[:5])
+    b = Batch(ctx, reps)
+    maxima = np.linspace(0.08, 0.2, len(reps))
+    b.sweep(maxima, FP32_RECHECK, n_sweeps=3, increment_step=True)
+    counts = b.sdf(0.05, 25)
+    assert counts.shape == (len(reps), 25) and counts.sum() > 0
+    p = b.pressures(0.05, 25)
+    for k, r in enumerate(reps):
+        pos, step, sub = b.state(k)
+        m = Microstate(ctx, r["boundary"], pos, PairwiseCutoff(HardSphere(1.0)), seed=r["seed"], step=step)
+        assert np.array_equal(counts[k], m.sdf(0.05, 25)), k
+        assert p[k] == m.pressure(0.05, 25)
+    # the batch keeps sweeping correctly after the histograms reused its arrays
+    single = Microstate(ctx, reps[0]["boundary"], b.positions(0), PairwiseCutoff(HardSphere(1.0)),
+                        seed=reps[0]["seed"], step=b.state(0)[1], substep=b.state(0)[2])
+    c, _ = b.sweep(maxima, FP64, increment_step=True)
+    cs = single.sweep(TRANSLATE, float(maxima[0]), 1.0, FP64, n_sweeps=1, increment_step=True)
+    assert (c[0].accepted, c[0].rejected) == (cs.accepted, cs.rejected)
+    assert np.array_equal(b.positions(0), single.positions())
