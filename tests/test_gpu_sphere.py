@@ -234,3 +234,26 @@ def test_context_released_after_its_last_system(ctx):
     g.close()
     h = Microstate(ctx, Periodic(1.0, [L] * 3), pos, PairwiseCutoff(HardSphere(1.0)), seed=21)
     assert h.overlap_count() == 0
+
+
+def test_ten_million_injected_near_contact_moves(ctx):
+    # 10^7 injected trials of the 3-D hard-sphere state (phi = 0.50), each placed at
+    # sigma * (1 + delta) from another sphere with |delta| log-uniform down to 1e-17 (a tenth at
+    # contact): FP64 and FP32 + recheck decisions equal the oracle's on every one.
+    g, o, _ = make(ctx, 3, 32768, 0.50, seed=0x5EED0015)
+    run_both(g, o, 0.12, 2, FP64)
+    total, rechecked, accepted = 0, 0, 0
+    for chunk in range(10):
+        spread = (1e-3, 1e-6, 1e-9, 1e-12, 1e-15)[chunk % 5]
+        bodies, trial = _near_contact_moves(o, 1_000_000, seed=1000 + chunk, spread=spread)
+        want, _ = o.eval_moves(bodies, trial, None, np.zeros(len(bodies)), 1.0)
+        got64, _ = g.eval_moves(bodies, trial, precision=FP64)
+        got32, rech = g.eval_moves(bodies, trial, precision=FP32_RECHECK)
+        assert np.array_equal(got64, want), (chunk, np.flatnonzero(got64 != want)[:10])
+        assert np.array_equal(got32, want), (chunk, np.flatnonzero(got32 != want)[:10])
+        total += len(bodies)
+        rechecked += int(rech.sum())
+        accepted += int(want.sum())
+    assert total == 10_000_000
+    assert 0 < accepted < total
+    assert rechecked > 100_000
