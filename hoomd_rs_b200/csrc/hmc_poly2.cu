@@ -55,6 +55,7 @@ __device__ __forceinline__ bool mat2_from_angle(double theta, M2* m) {
 __device__ __forceinline__ V2 support2(const double4* __restrict__ verts, uint32_t nv, const V2& n) {
     uint32_t arg = 0;
     double best = -INFINITY;
+#pragma unroll 4  // vertex loads of several iterations in flight; comparisons stay in order
     for (uint32_t i = 0; i < nv; ++i) {
         const double4 v = ldg4(verts + i);
         const double x = dadd(dmul(v.x, n.x), dmul(v.y, n.y));
