@@ -157,3 +157,25 @@ def test_batch_sdf_equals_single_system_sdf(ctx):
     cs = single.sweep(TRANSLATE, float(maxima[0]), 1.0, FP64, n_sweeps=1, increment_step=True)
     assert (c[0].accepted, c[0].rejected) == (cs.accepted, cs.rejected)
     assert np.array_equal(b.positions(0), single.positions())
+
+
+def test_lj_batch_wide_bound_block_recheck_equals_fp64(ctx, monkeypatch):
+    # With the FP32 error bound widened 10^4 times most trials of the FP32 batch pass are
+    # rechecked by their whole block (several per block, from different replicas); the
+    # trajectories must equal the FP64 batch's bit for bit.
+    reps = lj_replicas(3, LJ3)
+    kts = np.linspace(0.8, 2.0, len(reps))
+    monkeypatch.setenv("HMC_B200_FP32_BAND_SCALE", "1e4")
+    a = Batch(ctx, reps)
+    monkeypatch.delenv("HMC_B200_FP32_BAND_SCALE")
+    b = Batch(ctx, reps)
+    rechecks, trials = 0, 0
+    for _ in range(3):
+        ca, ta = a.sweep(0.1, FP32_RECHECK, increment_step=True, temperatures=kts)
+        cb, tb = b.sweep(0.1, FP64, increment_step=True, temperatures=kts)
+        assert [(c.accepted, c.rejected) for c in ca] == [(c.accepted, c.rejected) for c in cb]
+        rechecks += ta.rechecks
+        trials += ta.total()
+    for k in range(len(reps)):
+        assert np.array_equal(a.positions(k), b.positions(k)), k
+    assert rechecks > trials // 4, (rechecks, trials)
