@@ -714,6 +714,10 @@ def main():
                 "d2h_bytes_per_step": N_BODIES * 3 * 8},
         "gpu_launches": ra["launches"],
         "clocks": clocks,
+        "time_split": {"unit": "ms per sweep (CUDA events inside the timed FP32 sweeps)",
+                       "cell_list_rebuild": prof["rebuild_ms"] / max(prof["sweeps"], 1),
+                       "colour_passes": prof["sweep_ms"] / max(prof["sweeps"], 1),
+                       "whole_step": t_max / args.steps},
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(start_pos, L, d, step0)

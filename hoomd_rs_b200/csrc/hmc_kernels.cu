@@ -714,9 +714,16 @@ __global__ void __launch_bounds__(kCellThreads) k_cells(Geometry g, Arrays A) {
     const bool has = e > s;
     uint32_t packed = 0, col = 0;
     if (has) {
-        packed = A.body_m[A.sorted_body[s]];
         uint32_t m[3] = {0, 0, 0};
-        unpack_m<DIM>(packed, m);
+        // the space's multi-index from its index (multi_index_to_index inverted), not from its
+        // first body: no dependent gather (rebuild 74.9 -> 73.3 us for 2^20 spheres)
+        uint32_t rem = c;
+#pragma unroll
+        for (int ax = DIM - 1; ax >= 0; --ax) {
+            m[ax] = rem % g.shape[ax];
+            rem /= g.shape[ax];
+        }
+        packed = pack_m<DIM>(m);
         col = color_of<DIM>(m);
     }
     if (threadIdx.x == 0) s_nonempty = 0;
