@@ -319,14 +319,14 @@ hmc_status check_flags(hmc_system* s) {
 
 // update_checkerboard (parallel_sweep.rs:176-201): origin shift from the counter's
 // index u64::MAX stream, then the device counting sort into cell order.
-hmc_status rebuild(hmc_system* s, bool write_s) {
+hmc_status rebuild(hmc_system* s, bool write_s, bool write_slots = true) {
     Sfc64 rng = make_rng(s->step, s->substep, s->seed, UINT64_MAX);
     for (int a = 0; a < s->dim; ++a) {
         double off = uniform01(rng);
         s->geom.origin[a] = -s->geom.L[a] / 2.0 - off * s->geom.width[a];
     }
     HMC_CUDA(cudaMemsetAsync(s->arr.stats, 0, sizeof(DeviceStats), s->stream));
-    HMC_CUDA(launch_rebuild(s->dim, s->geom, s->arr, (uint32_t)s->n, write_s, s->stream));
+    HMC_CUDA(launch_rebuild(s->dim, s->geom, s->arr, (uint32_t)s->n, write_s, s->stream, write_slots));
     s->prof.kernel_launches += s->n > 0 ? 7 : 3;  // bin, 3 scan passes, scatter, space sort, gather
     return HMC_OK;
 }
@@ -799,7 +799,8 @@ hmc_status hmc_sweep(hmc_system* s, const hmc_sweep_params* p, hmc_count* out) {
     const uint32_t colors = 1u << s->dim;
     for (uint32_t sweep = 0; sweep < p->n_sweeps; ++sweep) {
         if (s->profiling) HMC_CUDA(cudaEventRecord(s->ev[0], s->stream));
-        hmc_status st = rebuild(s, !fp32 || s->oriented() || s->penalty());  // shapes read S in both modes
+        // shapes read S in both modes; the colour passes do not read slot_of_body
+        hmc_status st = rebuild(s, !fp32 || s->oriented() || s->penalty(), false);
         if (st) return st;
         if (s->profiling) HMC_CUDA(cudaEventRecord(s->ev[1], s->stream));
         Launch L{};

@@ -183,7 +183,10 @@ struct Batch {
 // Kernel launchers (hmc_kernels.cu). All return cudaGetLastError() after enqueueing.
 // write_s: also store the FP64 site positions S = wrap(B) in cell order (needed by the
 // plain FP64 pair test, the overlap check and injected-move evaluation).
-cudaError_t launch_rebuild(int dim, const Geometry& g, const Arrays& a, uint32_t n, bool write_s, cudaStream_t s);
+// write_slots: also store each body's cell-order slot (slot_of_body), which only the
+// injected-move and tuner kernels read; a sweep's own rebuild skips it.
+cudaError_t launch_rebuild(int dim, const Geometry& g, const Arrays& a, uint32_t n, bool write_s, cudaStream_t s,
+                           bool write_slots = true);
 // Per-replica rounds of a batch sweep into Replica::rounds, their maximum into DeviceStats::rounds.
 cudaError_t launch_batch_rounds(const Batch& b, Replica* rep, DeviceStats* stats, cudaStream_t s);
 // Batches of replicas: the rebuild and the hard-sphere colour pass over all replicas at once.

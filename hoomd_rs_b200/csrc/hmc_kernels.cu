@@ -736,8 +736,9 @@ __global__ void __launch_bounds__(kCellThreads) k_cells(Geometry g, Arrays A) {
 }
 
 // Per cell-order slot: gather B, S = wrap(B) (when WRITE_S), the FP32 offsets of S from its
-// space corner and the orientation; slot 0 also sets the sweep's rounds.
-template <int DIM, bool WRITE_S>
+// space corner and the orientation, and (when WRITE_SLOTS, for the injected-move and tuner
+// kernels) the slot of each body; slot 0 also sets the sweep's rounds.
+template <int DIM, bool WRITE_S, bool WRITE_SLOTS>
 __global__ void k_gather(Geometry g, Arrays A, uint32_t n) {
     grid_dependency_wait();  // rebuild kernels run back to back: the previous one has ended here
     allow_dependent_launch();
@@ -749,7 +750,7 @@ __global__ void k_gather(Geometry g, Arrays A, uint32_t n) {
         A.stats->rounds = ne == 0 ? 0u : (n + ne - 1) / ne;
     }
     const uint32_t i = A.sorted_body[k];
-    A.slot_of_body[i] = k;
+    if (WRITE_SLOTS) A.slot_of_body[i] = k;
     const double4 b = A.body_pos[i];
     A.sorted_b[k] = b;
     double sv[3] = {b.x, b.y, b.z};
@@ -980,8 +981,7 @@ __global__ void k_gather_batch(Batch B, Arrays A, uint32_t n) {
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     const uint32_t i = A.sorted_body[k];
-    const Geometry& g = B.rep[__ldg(B.body_rep + i)].g;
-    A.slot_of_body[i] = k;
+    const Geometry& g = B.rep[__ldg(B.body_rep + i)].g;  // (no batch kernel reads slot_of_body)
     const double4 b = A.body_pos[i];
     A.sorted_b[k] = b;
     double sv[3] = {b.x, b.y, b.z};
@@ -1304,7 +1304,8 @@ cudaError_t launch_count_scan(const Arrays& a, uint32_t n_cells, cudaStream_t s,
 }
 }  // namespace
 
-cudaError_t launch_rebuild(int dim, const Geometry& g, const Arrays& a, uint32_t n, bool write_s, cudaStream_t s) {
+cudaError_t launch_rebuild(int dim, const Geometry& g, const Arrays& a, uint32_t n, bool write_s, cudaStream_t s,
+                           bool write_slots) {
     cudaError_t e = cudaMemsetAsync(a.cell_count, 0, sizeof(uint32_t) * g.n_cells, s);
     if (e != cudaSuccess) return e;
     if (n > 0) {
@@ -1319,10 +1320,14 @@ cudaError_t launch_rebuild(int dim, const Geometry& g, const Arrays& a, uint32_t
     const uint32_t cb = blocks_for(g.n_cells, kCellThreads), gb = blocks_for(n, 256);
     if (dim == 2) {
         if ((e = launch_chained(k_cells<2>, cb, kCellThreads, true, s, g, a)) != cudaSuccess) return e;
-        return launch_chained(write_s ? k_gather<2, true> : k_gather<2, false>, gb, 256, true, s, g, a, n);
+        return launch_chained(write_slots ? (write_s ? k_gather<2, true, true> : k_gather<2, false, true>)
+                                          : (write_s ? k_gather<2, true, false> : k_gather<2, false, false>),
+                              gb, 256, true, s, g, a, n);
     }
     if ((e = launch_chained(k_cells<3>, cb, kCellThreads, true, s, g, a)) != cudaSuccess) return e;
-    return launch_chained(write_s ? k_gather<3, true> : k_gather<3, false>, gb, 256, true, s, g, a, n);
+    return launch_chained(write_slots ? (write_s ? k_gather<3, true, true> : k_gather<3, false, true>)
+                                      : (write_s ? k_gather<3, true, false> : k_gather<3, false, false>),
+                          gb, 256, true, s, g, a, n);
 }
 
 cudaError_t launch_rebuild_batch(int dim, const Batch& b, const Arrays& a, uint32_t n, bool write_s, cudaStream_t s) {
