@@ -100,16 +100,7 @@ __device__ __forceinline__ bool sphere_overlaps_generic(const Geometry& g, const
 // Candidates are taken one per row per step, so the loads of all rows of a step are
 // independent and in flight together. Returns kClear, kOverlap, or (FP32 only) kUncertain
 // when no pair overlaps for certain but some pair lies inside the FP32 bound; the caller
-// then decides with the generic walk, which rechecks those pairs in FP64.
-
-// The uncertain-pair fallback out of line (rare; keeps the batch pass's code small).
-template <int DIM, bool FP32>
-__device__ __noinline__ bool sphere_overlaps_generic_outlined(const Geometry& g, const Arrays& A, const Pair& P,
-                                                              const uint32_t* __restrict__ cs, const double* t,
-                                                              float4 t32, const uint32_t* m, uint32_t self,
-                                                              PairStats& st) {
-    return sphere_overlaps_generic<DIM, FP32>(g, A, P, cs, t, t32, m, self, st);
-}
+// then settles the trial in FP64 (sphere_warp_recheck in the colour passes).
 
 template <int DIM, bool FP32>
 __device__ __forceinline__ int sphere_overlaps_rows(const Geometry& g, const Arrays& A, const Pair& P,
@@ -224,7 +215,7 @@ __device__ __forceinline__ void sphere_commit(const Geometry& g, const Arrays& A
 // Returns kOverlap (rejected) or kClear (accepted and committed); with DEFER_UNCERTAIN it returns
 // the walk's result (kUncertain included) and commits nothing. COMPACT (the replica batch pass,
 // whose larger code misses in the instruction cache): one copy of the row walk for both
-// segments and the rare uncertain-pair fallback out of line.
+// segments.
 template <int DIM, bool FP32, bool COMPACT = false, bool DEFER_UNCERTAIN = false>
 __device__ __forceinline__ int sphere_decide_res(const Geometry& g, const Arrays& A, const Pair& P,
                                                  const uint32_t* __restrict__ cs, const uint32_t* m,
@@ -263,8 +254,7 @@ __device__ __forceinline__ int sphere_decide_res(const Geometry& g, const Arrays
     if (DEFER_UNCERTAIN) return res;  // the caller settles kUncertain and commits
     if (res == kUncertain) {
         PairStats st2;  // the fast path already counted its pair checks
-        const bool ov = COMPACT ? sphere_overlaps_generic_outlined<DIM, FP32>(g, A, P, cs, t, pr.t32, m, k, st2)
-                                : sphere_overlaps_generic<DIM, FP32>(g, A, P, cs, t, pr.t32, m, k, st2);
+        const bool ov = sphere_overlaps_generic<DIM, FP32>(g, A, P, cs, t, pr.t32, m, k, st2);
         res = ov ? kOverlap : kClear;
         st.rechecks += st2.rechecks;
         st.max_err = st2.max_err > st.max_err ? st2.max_err : st.max_err;
@@ -326,18 +316,6 @@ __device__ __forceinline__ bool sphere_warp_recheck(const Geometry& g, const Arr
         if (__any_sync(full, hit)) return true;
     }
     return false;
-}
-
-// One trial of ParallelSweep::generate_trial_moves and update_bodies for the space with
-// multi-index m. cs is the space-range array of the system (the replica's slice in a batch);
-// slots in it index the cell-ordered arrays of A. Returns true when the move was accepted.
-template <int DIM, bool FP32>
-__device__ __forceinline__ bool sphere_trial(const Geometry& g, const Arrays& A, const Pair& P,
-                                             const uint32_t* __restrict__ cs, const uint32_t* m, uint64_t step,
-                                             uint32_t substep, uint32_t seed, double max_move, PairStats& st) {
-    SphereProposal<DIM> pr;
-    if (!sphere_propose<DIM, FP32>(g, A, cs, m, step, substep, seed, max_move, pr)) return false;
-    return sphere_decide<DIM, FP32>(g, A, P, cs, m, pr, st);
 }
 
 // ---- the colour pass ------------------------------------------------------------------------
