@@ -229,14 +229,13 @@ def run_replicas(args, local_rank):
     torch.cuda.set_device(local_rank)
     ctx = Context(local_rank)
     specs = replica_specs()
-    reps, maxima = [], []
+    reps = []
     for n, phi, seed in specs:
         pos, L = lattice.hard_sphere_box(n, phi, 3, seed)
-        m = Microstate(ctx, Periodic(1.0, [L] * 3), pos, PairwiseCutoff(HardSphere(1.0)), seed=seed)
-        maxima.append(m.tune(TRANSLATE, D0, 1.0, FP32_RECHECK, TARGET_ACCEPTANCE, 2000, 16))
-        m.close()
         reps.append({"boundary": Periodic(1.0, [L] * 3), "positions": pos, "seed": seed})
     b = Batch(ctx, reps)
+    # each replica's move size tuned on its own state (hmc_batch_tune = hmc_tune per replica)
+    maxima = b.tune(D0, FP32_RECHECK, TARGET_ACCEPTANCE, 2000, 16)
     stream = torch.cuda.Stream()
     for _ in range(args.warmup):
         b.sweep(maxima, FP32_RECHECK, increment_step=True)

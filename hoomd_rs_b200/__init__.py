@@ -144,6 +144,7 @@ SIGNATURES = {
     "hmc_batch_set_state": (C.c_int, [_vp, C.c_uint32, _dp, C.c_uint64, C.c_uint32]),
     "hmc_batch_overlap_check": (C.c_int, [_vp, C.POINTER(C.c_uint64)]),
     "hmc_batch_sdf": (C.c_int, [_vp, C.c_double, C.c_uint32, C.POINTER(C.c_uint64)]),
+    "hmc_batch_tune": (C.c_int, [_vp, C.POINTER(hmc_sweep_params), C.c_double, C.c_uint32, C.c_uint32]),
     "hmc_batch_kernel_launches": (C.c_uint64, [_vp]),
     "hmc_sweep": (C.c_int, [_vp, C.POINTER(hmc_sweep_params), C.POINTER(hmc_count)]),
     "hmc_tune": (C.c_int, [_vp, C.POINTER(hmc_sweep_params), C.c_double, C.c_uint32, C.c_uint32]),
@@ -889,6 +890,18 @@ class Batch:
         out = np.zeros(self.n_replicas, dtype=np.uint64)
         _check(_lib.hmc_batch_overlap_check(self._h, out.ctypes.data_as(C.POINTER(C.c_uint64))))
         return out
+
+    def tune(self, maxima, precision: int, target: float, samples: int, steps: int, temperatures=1.0) -> np.ndarray:
+        """Tune every replica's translation size towards the target acceptance (Microstate.tune on
+        each replica's state); returns the tuned maxima."""
+        maxima = np.broadcast_to(np.asarray(maxima, dtype=np.float64), (self.n_replicas,))
+        kts = np.broadcast_to(np.asarray(temperatures, dtype=np.float64), (self.n_replicas,))
+        ps = (hmc_sweep_params * self.n_replicas)()
+        for k in range(self.n_replicas):
+            ps[k] = hmc_sweep_params(C.sizeof(hmc_sweep_params), TRANSLATE, float(maxima[k]), float(kts[k]), precision,
+                                     1, 0, 0)
+        _check(_lib.hmc_batch_tune(self._h, ps, target, samples, steps))
+        return np.array([ps[k].maximum for k in range(self.n_replicas)])
 
     def sdf(self, x_max: float = 0.02, n_bins: int = 40) -> np.ndarray:
         """Scale distributions of all replicas (hard spheres): (n_replicas, n_bins) pair counts."""

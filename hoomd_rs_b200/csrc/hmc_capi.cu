@@ -1929,6 +1929,120 @@ hmc_status hmc_batch_set_state(hmc_batch* bt, uint32_t replica, const double* po
     return HMC_OK;
 }
 
+// Arrays of replica k inside the batch's arrays: its bodies at its offset, the space arrays
+// from their start (a replica's own checkerboard has no more spaces than the batch).
+static Arrays replica_view(const hmc_batch* bt, uint32_t k) {
+    Arrays v = bt->arr;
+    const uint32_t o = bt->rep[k].body_base;
+    v.body_pos += o;
+    v.sorted_b += o;
+    v.sorted_s += o;
+    v.sorted_off += o;
+    v.sorted_body += o;
+    v.slot_of_body += o;
+    v.body_cell += o;
+    v.body_rank += o;
+    v.body_m += o;
+    v.body_ori = nullptr;
+    v.sorted_q = nullptr;
+    return v;
+}
+
+hmc_status hmc_batch_tune(hmc_batch* bt, hmc_sweep_params* params, double target, uint32_t samples, uint32_t steps) {
+    if (!bt || !params) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
+    if (!(target > 0.0 && target < 1.0)) return fail(HMC_INVALID_ARGUMENT, "target acceptance must be in (0, 1)");
+    if (samples == 0 || samples >= (1u << 31)) return fail(HMC_INVALID_ARGUMENT, "samples must be in [1, 2^31)");
+    for (uint32_t k = 0; k < bt->n_rep; ++k) {
+        const hmc_sweep_params& p = params[k];
+        if (p.struct_size < sizeof(hmc_sweep_params)) return fail(HMC_INVALID_ARGUMENT, "hmc_sweep_params.struct_size");
+        if (p.move != HMC_TRANSLATE) return fail(HMC_NOT_SUPPORTED, "batch replicas take translation moves");
+        if (p.precision > HMC_FP32_RECHECK) return fail(HMC_INVALID_ARGUMENT, "precision");
+        if (!(p.maximum > 0.0) || !std::isfinite(p.maximum))
+            return fail(HMC_INVALID_ARGUMENT, "replica %u: maximum must be positive", k);
+        if (!(p.temperature > 0.0)) return fail(HMC_INVALID_ARGUMENT, "replica %u: temperature must be positive", k);
+    }
+    if (steps == 0 || bt->n == 0) return HMC_OK;
+    HMC_CUDA(cudaSetDevice(bt->ctx->device));
+    const bool lj = bt->interaction == HMC_LENNARD_JONES;
+    uint64_t* db = nullptr;
+    double4 *dt = nullptr, *dq = nullptr;
+    double *du = nullptr, *dh = nullptr;
+    uint8_t* dd = nullptr;
+    cudaError_t e = cudaMallocAsync((void**)&db, sizeof(uint64_t) * samples, bt->stream);
+    if (e == cudaSuccess) e = cudaMallocAsync((void**)&dt, sizeof(double4) * samples, bt->stream);
+    if (e == cudaSuccess) e = cudaMallocAsync((void**)&dq, sizeof(double4) * samples, bt->stream);
+    if (e == cudaSuccess) e = cudaMallocAsync((void**)&du, sizeof(double) * samples, bt->stream);
+    if (e == cudaSuccess) e = cudaMallocAsync((void**)&dh, sizeof(double) * samples, bt->stream);
+    if (e == cudaSuccess) e = cudaMallocAsync((void**)&dd, 2 * (size_t)samples, bt->stream);
+    std::vector<uint8_t> hd(samples);
+    hmc_status st = HMC_OK;
+    // Replica by replica, hmc_tune on a view of the batch's arrays: the checkerboard of the
+    // replica's Counter, the same samples and the same scaling, so replica k's maximum equals
+    // hmc_tune of the same state in its own system. The next sweep rebuilds the batch.
+    for (uint32_t k = 0; k < bt->n_rep && e == cudaSuccess && st == HMC_OK; ++k) {
+        Replica& r = bt->rep[k];
+        hmc_sweep_params& p = params[k];
+        if (r.n_bodies == 0) continue;
+        Geometry g = r.g;
+        Sfc64 rng = make_rng(r.step, r.substep, r.seed, UINT64_MAX);  // the origin of rebuild()
+        for (int a = 0; a < bt->dim; ++a) {
+            const double off = uniform01(rng);
+            g.origin[a] = -g.L[a] / 2.0 - off * g.width[a];
+        }
+        const Arrays v = replica_view(bt, k);
+        e = cudaMemsetAsync(v.stats, 0, sizeof(DeviceStats), bt->stream);
+        if (e == cudaSuccess) e = launch_rebuild(bt->dim, g, v, r.n_bodies, true, bt->stream);
+        if (e != cudaSuccess) break;
+        bt->kernel_launches += 8;
+        double lmax = 0.0;
+        for (int a = 0; a < bt->dim; ++a) lmax = std::max(lmax, g.L[a]);
+        const bool fp32 = p.precision == HMC_FP32_RECHECK;
+        for (uint32_t step = 0; step < steps && e == cudaSuccess; ++step) {
+            if (p.maximum > 4.0 * lmax) p.maximum = 4.0 * lmax;  // the samplers' bound (see hmc_sweep)
+            Launch L{};
+            L.step = r.step;
+            L.substep = r.substep;
+            L.seed = r.seed;
+            L.max_move = p.maximum;
+            L.kt = p.temperature;
+            L.n_bodies = r.n_bodies;
+            e = launch_tune_moves(bt->dim, g, v, L, step, samples, false, db, dt, dq, du, bt->stream);
+            if (e == cudaSuccess) {
+                if (lj)
+                    e = launch_eval_lj(bt->dim, fp32, g, v, r.p, db, dt, du, p.temperature, samples, dd, dd + samples,
+                                       dh, bt->stream);
+                else
+                    e = launch_eval_sphere(bt->dim, fp32, g, v, r.p, db, dt, samples, dd, dd + samples, bt->stream);
+            }
+            if (e == cudaSuccess) e = cudaMemcpyAsync(hd.data(), dd, samples, cudaMemcpyDeviceToHost, bt->stream);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(bt->stream);
+            if (e != cudaSuccess) break;
+            bt->kernel_launches += 2;
+            uint64_t acc = 0;
+            for (uint32_t j = 0; j < samples; ++j) acc += hd[j];
+            p.maximum *= ((double)acc / (double)samples + 1.5) / (target + 1.5);  // tune_by_scaling
+        }
+        if (e == cudaSuccess) e = cudaMemcpyAsync(bt->host_stats, v.stats, sizeof(DeviceStats), cudaMemcpyDeviceToHost,
+                                                  bt->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(bt->stream);
+        if (e == cudaSuccess) {
+            const uint32_t f = bt->host_stats->error_flags;
+            if (f & kErrNonFinite) st = fail(HMC_NAN_STATE, "replica %u: a body position is not finite", k);
+            else if (f & kErrOutsideCheckerboard) st = fail(HMC_OUTSIDE_CHECKERBOARD, "replica %u: a body maps to no space", k);
+        }
+    }
+    if (db) cudaFreeAsync(db, bt->stream);
+    if (dt) cudaFreeAsync(dt, bt->stream);
+    if (dq) cudaFreeAsync(dq, bt->stream);
+    if (du) cudaFreeAsync(du, bt->stream);
+    if (dh) cudaFreeAsync(dh, bt->stream);
+    if (dd) cudaFreeAsync(dd, bt->stream);
+    cudaError_t e2 = cudaStreamSynchronize(bt->stream);
+    if (e == cudaSuccess) e = e2;
+    if (e != cudaSuccess) return fail(HMC_CUDA_ERROR, "batch tune: %s", cudaGetErrorString(e));
+    return st;
+}
+
 hmc_status hmc_batch_sdf(hmc_batch* bt, double x_max, uint32_t n_bins, uint64_t* counts) {
     if (!bt || !counts) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
     if (bt->interaction != HMC_HARD_SPHERE) return fail(HMC_NOT_SUPPORTED, "the scale distribution is for hard spheres");
@@ -1963,19 +2077,7 @@ hmc_status hmc_batch_sdf(hmc_batch* bt, double x_max, uint32_t n_bins, uint64_t*
         }
         g.n_cells = (uint32_t)cells;  // no more than the replica's own spaces: these are wider
         g.color_stride = (uint32_t)(cells >> bt->dim);
-        Arrays v = bt->arr;
-        const uint32_t o = r.body_base;
-        v.body_pos += o;
-        v.sorted_b += o;
-        v.sorted_s += o;
-        v.sorted_off += o;
-        v.sorted_body += o;
-        v.slot_of_body += o;
-        v.body_cell += o;
-        v.body_rank += o;
-        v.body_m += o;
-        v.body_ori = nullptr;
-        v.sorted_q = nullptr;
+        const Arrays v = replica_view(bt, k);
         cudaError_t e = cudaMemsetAsync(v.stats, 0, sizeof(DeviceStats), bt->stream);
         if (e == cudaSuccess) e = launch_rebuild(bt->dim, g, v, r.n_bodies, true, bt->stream);
         if (e == cudaSuccess)

@@ -266,6 +266,11 @@ hmc_status hmc_batch_set_state(hmc_batch* batch, uint32_t replica, const double*
 /* Overlapping pairs per replica (n_overlaps: n_replicas entries); hard spheres only
  * (HMC_NOT_SUPPORTED for a Lennard-Jones batch). */
 hmc_status hmc_batch_overlap_check(hmc_batch* batch, uint64_t* n_overlaps);
+/* Tune::tune_with_options for every replica (hmc_tune on each replica's own state): params[k]
+ * holds replica k's start maximum, temperature and precision and receives its tuned maximum,
+ * equal to hmc_tune's on the same state (hoomd-mc/src/tune_local.rs:21-89). Translation only. */
+hmc_status hmc_batch_tune(hmc_batch* batch, hmc_sweep_params* params, double target_acceptance, uint32_t samples,
+                          uint32_t steps);
 /* The scale distribution of every replica (hmc_sdf's pair counts by x = 1 - sigma/r over
  * [0, x_max)): counts receives n_replicas * n_bins entries, replica by replica. Hard spheres
  * only. The SDF pressure estimator is new (the reference has no counterpart). */

@@ -179,3 +179,33 @@ def test_lj_batch_wide_bound_block_recheck_equals_fp64(ctx, monkeypatch):
     for k in range(len(reps)):
         assert np.array_equal(a.positions(k), b.positions(k)), k
     assert rechecks > trials // 4, (rechecks, trials)
+
+
+@pytest.mark.parametrize("precision", [FP64, FP32_RECHECK])
+def test_batch_tune_equals_single_system_tune(ctx, precision):
+    # every replica's tuned move size equals Microstate.tune on the same state, for hard-sphere
+    # and Lennard-Jones batches (per-replica start sizes and temperatures)
+    reps = replicas(3, SPECS3[:4])
+    b = Batch(ctx, reps)
+    b.sweep(0.1, precision, n_sweeps=2, increment_step=True)
+    start = np.linspace(0.05, 0.4, len(reps))
+    tuned = b.tune(start, precision, 0.3, 3000, 8)
+    for k, r in enumerate(reps):
+        pos, step, sub = b.state(k)
+        m = Microstate(ctx, r["boundary"], pos, PairwiseCutoff(HardSphere(1.0)), seed=r["seed"], step=step,
+                       substep=sub)
+        assert tuned[k] == m.tune(TRANSLATE, float(start[k]), 1.0, precision, 0.3, 3000, 8), k
+    lreps = lj_replicas(3, LJ3)
+    lb = Batch(ctx, lreps)
+    kts = np.linspace(0.8, 2.0, len(lreps))
+    ltuned = lb.tune(0.1, precision, 0.4, 2000, 6, temperatures=kts)
+    for k, r in enumerate(lreps):
+        m = Microstate(ctx, r["boundary"], r["positions"], r["hamiltonian"], seed=r["seed"], step=r["step"])
+        assert ltuned[k] == m.tune(TRANSLATE, 0.1, float(kts[k]), precision, 0.4, 2000, 6), k
+    # the batch still sweeps exactly like a single system afterwards
+    single = Microstate(ctx, reps[1]["boundary"], b.positions(1), PairwiseCutoff(HardSphere(1.0)),
+                        seed=reps[1]["seed"], step=b.state(1)[1], substep=b.state(1)[2])
+    c, _ = b.sweep(tuned, precision, increment_step=True)
+    cs = single.sweep(TRANSLATE, float(tuned[1]), 1.0, precision, n_sweeps=1, increment_step=True)
+    assert (c[1].accepted, c[1].rejected) == (cs.accepted, cs.rejected)
+    assert np.array_equal(b.positions(1), single.positions())
