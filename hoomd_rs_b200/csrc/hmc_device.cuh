@@ -337,13 +337,14 @@ __device__ __forceinline__ void stencil_part(const Geometry& g, const uint32_t* 
     }
 }
 
-// Call with all 32 lanes of the warp.
+// Call with all 32 lanes of the warp. wrapped_only: only the wrapped parts (the spaces across
+// the fast-axis end from a space at an end).
 template <int DIM>
 __device__ __forceinline__ FlatStencil flat_stencil(const Geometry& g, const uint32_t* __restrict__ cs,
-                                                    const uint32_t* m, uint32_t lane) {
+                                                    const uint32_t* m, uint32_t lane, bool wrapped_only = false) {
     FlatStencil fs{0u, 0u, 0u, 0.f, 0.f};
     uint32_t len = 0;
-    if (lane < 2u * kRows<DIM>)
+    if (lane < 2u * kRows<DIM> && (!wrapped_only || (lane & 1u)))
         stencil_part<DIM>(g, cs, m, (int)(lane >> 1), (lane & 1u) != 0, fs.lo, len, fs.s0, fs.s1);
     const unsigned full = 0xffffffffu;
     uint32_t x = len;
