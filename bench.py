@@ -39,8 +39,8 @@ TARGET_ACCEPTANCE = 0.30
 
 
 # DRAM bytes of one FP32 colour pass of this workload, read + written, from one ncu capture
-# (profiles/k_sweep_sphere_fp32_hard_spheres_2p20.md): 31.13 MB + 0.07 MB.
-SPHERE_PASS_DRAM_BYTES = 31.20e6
+# (profiles/k_sweep_sphere_fp32_hard_spheres_2p20.md): 30.51 MB + 0.07 MB.
+SPHERE_PASS_DRAM_BYTES = 30.58e6
 
 
 def aggregate_over_ranks(elapsed, units, world, device):
