@@ -327,7 +327,7 @@ hmc_status rebuild(hmc_system* s, bool write_s, bool write_slots = true) {
     }
     HMC_CUDA(cudaMemsetAsync(s->arr.stats, 0, sizeof(DeviceStats), s->stream));
     HMC_CUDA(launch_rebuild(s->dim, s->geom, s->arr, (uint32_t)s->n, write_s, s->stream, write_slots));
-    s->prof.kernel_launches += s->n > 0 ? 7 : 3;  // bin, 3 scan passes, scatter, space sort, gather
+    s->prof.kernel_launches += s->n > 0 ? 6 : 2;  // bin, 2 scan passes, scatter, space sort, gather
     return HMC_OK;
 }
 
@@ -857,7 +857,7 @@ hmc_status hmc_sweep(hmc_system* s, const hmc_sweep_params* p, hmc_count* out) {
             HMC_CUDA(cudaEventElapsedTime(&t_rebuild, s->ev[0], s->ev[1]));
             HMC_CUDA(cudaEventElapsedTime(&t_sweep, s->ev[2], s->ev[3]));
             s->prof.rebuild_ms += t_rebuild;
-            s->prof.rebuild_launches += s->n > 0 ? 7 : 3;
+            s->prof.rebuild_launches += s->n > 0 ? 6 : 2;
             s->prof.sweep_ms += t_sweep;
             s->prof.sweep_launches += (uint64_t)std::max(rounds, guess) * colors;
             s->prof.sweeps += 1;
@@ -1132,7 +1132,7 @@ static hmc_status pair_histogram(hmc_system* s, bool sdf, double sigma, double l
     cudaError_t e2 = cudaStreamSynchronize(s->stream);
     if (e == cudaSuccess) e = e2;
     if (e != cudaSuccess) return fail(HMC_CUDA_ERROR, "pair histogram: %s", cudaGetErrorString(e));
-    s->prof.kernel_launches += 8;
+    s->prof.kernel_launches += s->n > 0 ? 7 : 2;  // the rebuild and the histogram
     hmc_status st;
     if ((st = read_stats(s))) return st;
     if ((st = check_flags(s))) return st;
@@ -1590,7 +1590,7 @@ hmc_status batch_rebuild(hmc_batch* bt, bool write_s) {
     if (st) return st;
     HMC_CUDA(cudaMemsetAsync(bt->arr.stats, 0, sizeof(DeviceStats), bt->stream));
     HMC_CUDA(launch_rebuild_batch(bt->dim, bt->b, bt->arr, (uint32_t)bt->n, write_s, bt->stream));
-    bt->kernel_launches += bt->n > 0 ? 7 : 3;
+    bt->kernel_launches += bt->n > 0 ? 6 : 2;  // bin, 2 scan passes, scatter, space sort, gather
     return HMC_OK;
 }
 
@@ -1993,7 +1993,7 @@ hmc_status hmc_batch_tune(hmc_batch* bt, hmc_sweep_params* params, double target
         e = cudaMemsetAsync(v.stats, 0, sizeof(DeviceStats), bt->stream);
         if (e == cudaSuccess) e = launch_rebuild(bt->dim, g, v, r.n_bodies, true, bt->stream);
         if (e != cudaSuccess) break;
-        bt->kernel_launches += 8;
+        bt->kernel_launches += 6;  // the rebuild
         double lmax = 0.0;
         for (int a = 0; a < bt->dim; ++a) lmax = std::max(lmax, g.L[a]);
         const bool fp32 = p.precision == HMC_FP32_RECHECK;
@@ -2093,7 +2093,7 @@ hmc_status hmc_batch_sdf(hmc_batch* bt, double x_max, uint32_t n_bins, uint64_t*
             st = fail(HMC_CUDA_ERROR, "replica %u: scale distribution: %s", k, cudaGetErrorString(e));
             break;
         }
-        bt->kernel_launches += 8;
+        bt->kernel_launches += r.n_bodies > 0 ? 7 : 2;  // the rebuild and the histogram
         const uint32_t f = bt->host_stats->error_flags;
         if (f & kErrNonFinite) st = fail(HMC_NAN_STATE, "replica %u: a body position is not finite", k);
         else if (f & kErrOutsideCheckerboard) st = fail(HMC_OUTSIDE_CHECKERBOARD, "replica %u: a body maps to no space", k);

@@ -668,8 +668,8 @@ __device__ __forceinline__ uint32_t color_of(const uint32_t* m) {
 }
 
 
-// Exclusive scan of the space counts into cell_start: per-block totals, a single-block scan of
-// the totals, then each block's prefix.
+// Exclusive scan of the space counts into cell_start: per-block totals, then each block's scan
+// offset by the sum of the totals before it.
 __global__ void __launch_bounds__(kScanThreads) k_count_reduce(const uint32_t* __restrict__ count, uint32_t n_cells,
                                                                uint32_t* block_sums) {
     grid_dependency_wait();  // rebuild kernels run back to back: the previous one has ended here
@@ -690,46 +690,6 @@ __global__ void __launch_bounds__(kScanThreads) k_count_reduce(const uint32_t* _
     }
 }
 
-__global__ void __launch_bounds__(1024) k_count_block_sums(uint32_t* block_sums, uint32_t n_blocks) {
-    grid_dependency_wait();  // rebuild kernels run back to back: the previous one has ended here
-    allow_dependent_launch();
-    __shared__ uint32_t warp_sums[32];
-    constexpr int items = 8;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t b0 = threadIdx.x * items;
-    uint32_t v[items];
-    uint32_t sum = 0;
-#pragma unroll
-    for (int k = 0; k < items; ++k) {
-        v[k] = b0 + k < n_blocks ? block_sums[b0 + k] : 0u;
-        sum += v[k];
-    }
-    uint32_t x = sum;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= o) x += y;
-    }
-    if (lane == 31) warp_sums[warp] = x;
-    __syncthreads();
-    if (warp == 0) {
-        uint32_t w = warp_sums[lane];
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
-            if (lane >= o) w += y;
-        }
-        warp_sums[lane] = w;
-    }
-    __syncthreads();
-    uint32_t run = (warp > 0 ? warp_sums[warp - 1] : 0u) + x - sum;
-#pragma unroll
-    for (int k = 0; k < items; ++k) {
-        if (b0 + k < n_blocks) block_sums[b0 + k] = run;
-        run += v[k];
-    }
-}
-
 __global__ void __launch_bounds__(kScanThreads) k_count_apply(const uint32_t* __restrict__ count, uint32_t n_cells,
                                                               const uint32_t* __restrict__ block_sums,
                                                               uint32_t* cell_start) {
@@ -743,8 +703,19 @@ __global__ void __launch_bounds__(kScanThreads) k_count_apply(const uint32_t* __
         v[k] = base + k < n_cells ? count[base + k] : 0u;
         sum += v[k];
     }
+    // this block's offset: the sum of the earlier blocks' totals (at most a few hundred values,
+    // read by every block, so the separate scan of the block totals is not needed)
+    __shared__ uint32_t s_prefix[kScanThreads / 32];
+    uint32_t part = 0;
+    for (uint32_t i = threadIdx.x; i < blockIdx.x; i += kScanThreads) part += block_sums[i];
+    part = __reduce_add_sync(0xffffffffu, part);
+    if ((threadIdx.x & 31) == 0) s_prefix[threadIdx.x >> 5] = part;
+    __syncthreads();
+    uint32_t prefix = 0;
+#pragma unroll
+    for (int w = 0; w < kScanThreads / 32; ++w) prefix += s_prefix[w];
     uint32_t total;
-    uint32_t run = block_exclusive_scan(sum, &total) + block_sums[blockIdx.x];
+    uint32_t run = block_exclusive_scan(sum, &total) + prefix;
 #pragma unroll
     for (int k = 0; k < kScanItems; ++k) {
         const uint32_t c = base + k;
@@ -1429,7 +1400,6 @@ cudaError_t launch_count_scan(const Arrays& a, uint32_t n_cells, cudaStream_t s,
     const uint32_t nb = blocks_for(n_cells, kScanTile);
     cudaError_t e = launch_chained(k_count_reduce, nb, kScanThreads, chained, s, (const uint32_t*)a.cell_count,
                                    n_cells, a.block_sums);
-    if (e == cudaSuccess) e = launch_chained(k_count_block_sums, 1, 1024, true, s, a.block_sums, nb);
     if (e == cudaSuccess)
         e = launch_chained(k_count_apply, nb, kScanThreads, true, s, (const uint32_t*)a.cell_count, n_cells,
                            (const uint32_t*)a.block_sums, a.cell_start);
