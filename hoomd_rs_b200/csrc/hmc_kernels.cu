@@ -868,8 +868,8 @@ __global__ void k_overlap_sphere(Geometry g, Arrays A, Pair P, uint32_t n) {
 
 // ---- pair distributions: scale distribution function and g(r) ------------------------------
 // Both histogram the pairs i < j by their minimum-image distance, d = t - s - L rint((t - s)/L)
-// per axis, r^2 = sum d^2 (no hoomd-rs counterpart: these estimators are the survey's
-// equilibrium checks). SDF: x = 1 - sigma / r, bin floor(x * inv_dx) for x in [0, x_max),
+// per axis, r^2 = sum d^2 (no hoomd-rs counterpart: equilibrium checks of the sweep, the
+// pressure from the scale distribution and the radial distribution). SDF: x = 1 - sigma / r, bin floor(x * inv_dx) for x in [0, x_max),
 // the scale at which the pair would overlap if the box shrank by (1 - x) (spheres only).
 // g(r): bin floor(r * inv_dr) for r < r_max. The walk needs spaces at least as wide as the
 // largest distance binned; the host rebuilds the cell list with such a checkerboard first.
