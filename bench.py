@@ -38,8 +38,8 @@ SEED = 0x5EED0002
 TARGET_ACCEPTANCE = 0.30
 
 
-# DRAM bytes of one FP32 colour pass of this workload, read + written, from one ncu capture
-# (profiles/k_sweep_sphere_fp32_hard_spheres_2p20.md): 30.51 MB + 0.07 MB.
+# DRAM bytes of one FP32 colour pass of this workload, read + written, from one ncu capture of
+# the pass (dram__bytes_read.sum + dram__bytes_write.sum): 30.51 MB + 0.07 MB.
 SPHERE_PASS_DRAM_BYTES = 30.58e6
 
 
@@ -165,6 +165,26 @@ def cpu_baseline(pos, L, d, step, seconds=12.0):
                       f"{el:.1f} s, {threads} threads)"}
 
 
+def oracle_check(ctx, h, pos, L, d, step):
+    """One sampled sweep of the timed state checked against the oracle's ParallelSweep: the GPU's
+    FP32+recheck sweep and the oracle's FP64 sweep from the same state and counter must give the
+    same Count and the same positions (mismatches = bodies whose position differs)."""
+    import oracle
+    from hoomd_rs_b200 import FP32_RECHECK, TRANSLATE, Microstate, Periodic
+    g = Microstate(ctx, Periodic(1.0, [L] * 3), pos, h, seed=SEED)
+    g.set_state(pos, step, 0)
+    o = oracle.System(3, [L] * 3, pos, diameter=1.0, seed=SEED, step=step)
+    c = g.sweep(TRANSLATE, d, 1.0, FP32_RECHECK, n_sweeps=1, increment_step=True)
+    t0 = time.perf_counter()
+    a, r = o.parallel_sweep(oracle.TRANSLATE, d, 1.0, 1.0, threads=host_threads())
+    t_oracle = time.perf_counter() - t0
+    mism = int(np.count_nonzero(np.any(g.positions() != o.state()[0], axis=1)))
+    g.close()
+    return {"sweeps": 1, "count_equal": (c.accepted, c.rejected) == (a, r), "mismatches": mism,
+            "trials": a + r, "oracle_s": t_oracle,
+            "what": "one FP32+recheck sweep of the timed state against the oracle's ParallelSweep"}
+
+
 def run_reference(args, rank):
     """--impl reference: the CPU restatement of ParallelSweep (oracle/), timed on host cores."""
     if rank != 0:
@@ -174,8 +194,8 @@ def run_reference(args, rank):
     threads = host_threads()
     pos, L = lattice.hard_sphere_box(N_BODIES, PHI, 3, SEED)
     o = oracle.System(3, [L] * 3, pos, diameter=1.0, seed=SEED)
-    # the same tuner as the GPU arm (identical per-sample streams give the identical size)
-    d = o.tune(oracle.TRANSLATE, D0, 1.0, TARGET_ACCEPTANCE, TUNE_SAMPLES, TUNE_STEPS)
+    # the same tuner as the GPU arm (the reference's single stream gives the identical size)
+    d = o.tune_stream(oracle.TRANSLATE, D0, 1.0, TARGET_ACCEPTANCE, TUNE_SAMPLES, TUNE_STEPS)
     for _ in range(args.warmup):
         o.parallel_sweep(oracle.TRANSLATE, d, 1.0, 1.0, threads=threads)
         o.increment_step()
@@ -705,8 +725,7 @@ def main():
         "recheck_fraction": ra["rechecks"] / max(ra["pair_checks"], 1), "max_fp32_error": ra["max_err"],
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": SPHERE_PASS_DRAM_BYTES, "kernel": "k_sweep_sphere<3,fp32>",
-                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one FP32 colour pass "
-                                       "(profiles/k_sweep_sphere_fp32_hard_spheres_2p20.md)",
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one FP32 colour pass",
                      "bytes_per_launch": bytes_per_launch, "launch_ms": t_launch * 1e3,
                      "peak_source": f"{peak_kind} hbm_gbs"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": N_BODIES * 3 * 8,
@@ -720,6 +739,7 @@ def main():
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(start_pos, L, d, step0)
+        line["oracle_check"] = oracle_check(ctx, h, pa, L, d, a.step())
     if rank == 0:
         print(json.dumps(line), flush=True)
     a.close()

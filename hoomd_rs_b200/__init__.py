@@ -37,6 +37,8 @@ HARD_SPHERE, HARD_CONVEX_POLYGON, HARD_CONVEX_POLYHEDRON, LENNARD_JONES, HARD_CO
     OVERLAP_PENALTY = range(6)
 TRANSLATE, ROTATE = range(2)
 FP64, FP32_RECHECK = range(2)
+# hmc_sweep_params.flags of the tuners
+TUNE_PER_SAMPLE_STREAMS = 1
 
 
 class HmcError(RuntimeError):
@@ -63,12 +65,12 @@ class hmc_system_desc(C.Structure):
 class hmc_sweep_params(C.Structure):
     _fields_ = [("struct_size", C.c_uint32), ("move", C.c_uint32), ("maximum", C.c_double),
                 ("temperature", C.c_double), ("precision", C.c_uint32), ("n_sweeps", C.c_uint32),
-                ("increment_step", C.c_uint32), ("reserved", C.c_uint32)]
+                ("increment_step", C.c_uint32), ("flags", C.c_uint32)]
 
 
 class hmc_count(C.Structure):
     _fields_ = [("accepted", C.c_uint64), ("rejected", C.c_uint64), ("rechecks", C.c_uint64),
-                ("pair_checks", C.c_uint64), ("max_fp32_error", C.c_double)]
+                ("pair_checks", C.c_uint64), ("max_fp32_error", C.c_double), ("order_ambiguous", C.c_uint64)]
 
 
 class hmc_injected_move(C.Structure):
@@ -151,6 +153,8 @@ SIGNATURES = {
     "hmc_overlap_check": (C.c_int, [_vp, C.POINTER(C.c_uint64)]),
     "hmc_eval_moves": (C.c_int, [_vp, C.POINTER(hmc_injected_move), C.c_uint64, C.c_double, C.c_uint32, _u8p,
                                  _u8p, _dp]),
+    "hmc_eval_trials": (C.c_int, [_vp, C.POINTER(hmc_injected_move), C.c_uint64, C.c_double, C.c_uint32, _u8p,
+                                  _u8p]),
     "hmc_total_energy": (C.c_int, [_vp, _dp]),
     "hmc_overlap_count_noalloc": (C.c_int, [_vp, C.c_uint64, C.c_uint32, _dp, C.c_double, C.c_double, _vp, _vp]),
     "hmc_quick_insert_apply": (C.c_int, [_vp, C.POINTER(hmc_quick_insert), C.POINTER(hmc_count)]),
@@ -406,6 +410,7 @@ class Count:
     rechecks: int = 0
     pair_checks: int = 0
     max_fp32_error: float = 0.0
+    order_ambiguous: int = 0  # soft-potential decisions another summation order could change
 
     def total(self) -> int:
         return self.accepted + self.rejected
@@ -573,8 +578,11 @@ class Microstate:
         _check(_lib.hmc_increment_step(self._h))
 
     def tune(self, move: int, maximum: float, temperature: float, precision: int, target: float, samples: int,
-             steps: int) -> float:
-        p = hmc_sweep_params(C.sizeof(hmc_sweep_params), move, maximum, temperature, precision, 1, 0, 0)
+             steps: int, per_sample_streams: bool = False) -> float:
+        """Tune::tune_with_options: the reference's single-stream tuner (tune_local.rs:42-88), or
+        with per_sample_streams the faster variant that gives every sample its own stream."""
+        p = hmc_sweep_params(C.sizeof(hmc_sweep_params), move, maximum, temperature, precision, 1, 0,
+                             TUNE_PER_SAMPLE_STREAMS if per_sample_streams else 0)
         _check(_lib.hmc_tune(self._h, C.byref(p), target, samples, steps))
         return p.maximum
 
@@ -622,7 +630,7 @@ class Microstate:
                              int(increment_step), 0)
         c = hmc_count()
         _check(_lib.hmc_sweep(self._h, C.byref(p), C.byref(c)))
-        return Count(c.accepted, c.rejected, c.rechecks, c.pair_checks, c.max_fp32_error)
+        return Count(c.accepted, c.rejected, c.rechecks, c.pair_checks, c.max_fp32_error, c.order_ambiguous)
 
     def serial_sweep(self, maximum: float, n_sweeps: int = 1, increment_step: bool = False, move_mask=None,
                      temperature: float = 1.0) -> "Count":
@@ -661,6 +669,27 @@ class Microstate:
         if return_delta_h:
             return dec.astype(bool), rech.astype(bool), dh
         return dec.astype(bool), rech.astype(bool)
+
+    def eval_trials(self, bodies, positions, u=None, temperature: float = 1.0, precision: int = FP64,
+                    orientations=None):
+        """The colour pass's own decisions for injected trials (hmc_eval_trials): positions are
+        W1 = wrap(propose(..)); returns (decisions, flags) with flag bit 0 = settled in FP64 by
+        the FP32 pass, bit 1 = outside the body's checkerboard space."""
+        bodies = np.asarray(bodies, dtype=np.uint64)
+        n = len(bodies)
+        arr = np.zeros(n, dtype=[("body", np.uint64), ("position", np.float64, 3), ("orientation", np.float64, 4),
+                                 ("u", np.float64)])
+        arr["body"] = bodies
+        arr["position"][:, : self.dim] = np.asarray(positions, dtype=np.float64).reshape(n, self.dim)
+        arr["u"] = -1.0 if u is None else np.asarray(u, dtype=np.float64)
+        if orientations is not None:
+            arr["orientation"] = np.asarray(orientations, dtype=np.float64).reshape(n, 4)
+        moves = arr.ctypes.data_as(C.POINTER(hmc_injected_move))
+        dec = np.zeros(n, dtype=np.uint8)
+        flags = np.zeros(n, dtype=np.uint8)
+        _check(_lib.hmc_eval_trials(self._h, moves, n, temperature, precision, dec.ctypes.data_as(_u8p),
+                                    flags.ctypes.data_as(_u8p)))
+        return dec.astype(bool), flags
 
     def refresh(self):
         """Re-read the body count (QuickInsert appends bodies on the device)."""
@@ -870,7 +899,8 @@ class Batch:
         tot = hmc_count()
         _check(_lib.hmc_batch_sweep(self._h, ps, cs, C.byref(tot)))
         counts = [Count(c.accepted, c.rejected, 0, 0, 0.0) for c in cs]
-        return counts, Count(tot.accepted, tot.rejected, tot.rechecks, tot.pair_checks, tot.max_fp32_error)
+        return counts, Count(tot.accepted, tot.rejected, tot.rechecks, tot.pair_checks, tot.max_fp32_error,
+                             tot.order_ambiguous)
 
     def state(self, k: int):
         pos = np.empty((self.sizes[k], self.dim))
@@ -891,15 +921,17 @@ class Batch:
         _check(_lib.hmc_batch_overlap_check(self._h, out.ctypes.data_as(C.POINTER(C.c_uint64))))
         return out
 
-    def tune(self, maxima, precision: int, target: float, samples: int, steps: int, temperatures=1.0) -> np.ndarray:
+    def tune(self, maxima, precision: int, target: float, samples: int, steps: int, temperatures=1.0,
+             per_sample_streams: bool = False) -> np.ndarray:
         """Tune every replica's translation size towards the target acceptance (Microstate.tune on
         each replica's state); returns the tuned maxima."""
         maxima = np.broadcast_to(np.asarray(maxima, dtype=np.float64), (self.n_replicas,))
         kts = np.broadcast_to(np.asarray(temperatures, dtype=np.float64), (self.n_replicas,))
         ps = (hmc_sweep_params * self.n_replicas)()
+        flags = TUNE_PER_SAMPLE_STREAMS if per_sample_streams else 0
         for k in range(self.n_replicas):
             ps[k] = hmc_sweep_params(C.sizeof(hmc_sweep_params), TRANSLATE, float(maxima[k]), float(kts[k]), precision,
-                                     1, 0, 0)
+                                     1, 0, flags)
         _check(_lib.hmc_batch_tune(self._h, ps, target, samples, steps))
         return np.array([ps[k].maximum for k in range(self.n_replicas)])
 

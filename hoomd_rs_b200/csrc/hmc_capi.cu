@@ -867,6 +867,7 @@ hmc_status hmc_sweep(hmc_system* s, const hmc_sweep_params* p, hmc_count* out) {
         total.rejected += (uint64_t)rounds * nonempty - s->host_stats->accepted;
         total.rechecks += s->host_stats->rechecks;
         total.pair_checks += s->host_stats->pair_checks;
+        total.order_ambiguous += s->host_stats->ambiguous;
         double me;
         unsigned long long bits = s->host_stats->max_err_bits;
         std::memcpy(&me, &bits, 8);
@@ -1014,10 +1015,53 @@ hmc_status hmc_tune(hmc_system* s, hmc_sweep_params* p, double target, uint32_t 
     if (!(p->maximum > 0.0) || !std::isfinite(p->maximum)) return fail(HMC_INVALID_ARGUMENT, "maximum must be positive");
     if (!(p->temperature > 0.0)) return fail(HMC_INVALID_ARGUMENT, "temperature must be positive");
     if (samples == 0 || samples >= (1u << 31)) return fail(HMC_INVALID_ARGUMENT, "samples must be in [1, 2^31)");
+    if (p->flags & ~HMC_TUNE_PER_SAMPLE_STREAMS) return fail(HMC_INVALID_ARGUMENT, "unknown tune flags");
     if (s->n == 0 || steps == 0) return HMC_OK;
     HMC_CUDA(cudaSetDevice(s->ctx->device));
     hmc_status st = rebuild(s, true);
     if (st) return st;
+    if (!(p->flags & HMC_TUNE_PER_SAMPLE_STREAMS)) {
+        // the reference's single stream, one warp (tune_stream_run)
+        TuneJob job{};
+        job.g = s->geom;
+        job.a = s->arr;
+        job.p = s->pair;
+        job.step = s->step;
+        job.substep = s->substep;
+        job.seed = s->seed;
+        job.n_bodies = (uint32_t)s->n;
+        job.samples = samples;
+        job.steps = steps;
+        job.rotate = p->move == HMC_ROTATE ? 1u : 0u;
+        job.maximum = p->maximum;
+        job.kt = p->temperature;
+        job.target = target;
+        const double pi = 3.141592653589793;
+        job.cap = p->move == HMC_ROTATE ? (s->dim == 3 ? pi / 2.0 : pi) : 0.0;
+        TuneJob* dj = nullptr;
+        cudaError_t e = cudaMallocAsync((void**)&dj, sizeof(TuneJob), s->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(dj, &job, sizeof(TuneJob), cudaMemcpyHostToDevice, s->stream);
+        if (e == cudaSuccess) {
+            if (s->soft())
+                e = launch_tune_stream_lj(s->dim, dj, 1, s->stream);
+            else if (s->polygon())
+                e = launch_tune_stream_poly2(s->sat(), dj, 1, s->verts, s->n_vertices, s->poly_rcut2, s->stream);
+            else if (s->oriented())
+                e = launch_tune_stream_poly(dj, 1, s->verts, s->n_vertices, s->poly_rcut2, s->stream);
+            else
+                e = launch_tune_stream_sphere(s->dim, dj, 1, s->stream);
+            s->prof.kernel_launches += 1;
+        }
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&job, dj, sizeof(TuneJob), cudaMemcpyDeviceToHost, s->stream);
+        if (dj) cudaFreeAsync(dj, s->stream);
+        cudaError_t e2 = cudaStreamSynchronize(s->stream);
+        if (e == cudaSuccess) e = e2;
+        if (e != cudaSuccess) return fail(HMC_CUDA_ERROR, "tune: %s", cudaGetErrorString(e));
+        if ((st = read_stats(s))) return st;
+        if ((st = check_flags(s))) return st;
+        p->maximum = job.maximum;
+        return HMC_OK;
+    }
     double lmax = 0.0;
     for (int a = 0; a < s->dim; ++a) lmax = std::max(lmax, s->geom.L[a]);
     uint64_t* db = nullptr;
@@ -1524,6 +1568,79 @@ hmc_status hmc_eval_moves(hmc_system* s, const hmc_injected_move* moves, uint64_
     return HMC_OK;
 }
 
+hmc_status hmc_eval_trials(hmc_system* s, const hmc_injected_move* moves, uint64_t n, double temperature,
+                           uint32_t precision, uint8_t* decisions, uint8_t* flags) {
+    if (!s || (n && (!moves || !decisions))) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
+    if (precision > HMC_FP32_RECHECK) return fail(HMC_INVALID_ARGUMENT, "precision");
+    if (s->polygon()) return fail(HMC_NOT_SUPPORTED, "eval_trials: convex polygons");
+    if (s->soft() && !(temperature > 0.0)) return fail(HMC_INVALID_ARGUMENT, "temperature must be positive");
+    if (n == 0) return HMC_OK;
+    if (n >= (1ull << 31)) return fail(HMC_INVALID_ARGUMENT, "too many moves");
+    HMC_CUDA(cudaSetDevice(s->ctx->device));
+    for (uint64_t i = 0; i < n; ++i)
+        if (moves[i].body >= s->n) return fail(HMC_INVALID_ARGUMENT, "move %llu names body %llu of %llu",
+                                                (unsigned long long)i, (unsigned long long)moves[i].body,
+                                                (unsigned long long)s->n);
+    hmc_status st = rebuild(s, true);
+    if (st) return st;
+    std::vector<uint64_t> hb(n);
+    std::vector<double4> ht(n), hq(n);
+    std::vector<double> hu(n);
+    for (uint64_t i = 0; i < n; ++i) {
+        hb[i] = moves[i].body;
+        ht[i] = make_double4(moves[i].position[0], moves[i].position[1], s->dim == 3 ? moves[i].position[2] : 0.0, 0.0);
+        hq[i] = make_double4(moves[i].orientation[0], moves[i].orientation[1], moves[i].orientation[2],
+                             moves[i].orientation[3]);
+        hu[i] = moves[i].u;
+    }
+    const bool fp32 = precision == HMC_FP32_RECHECK;
+    uint64_t* db = nullptr;
+    double4* dt = nullptr;
+    double4* dq = nullptr;
+    double* du = nullptr;
+    uint8_t* dd = nullptr;
+    cudaError_t e = cudaMallocAsync((void**)&db, sizeof(uint64_t) * n, s->stream);
+    if (e == cudaSuccess) e = cudaMallocAsync((void**)&dt, sizeof(double4) * n, s->stream);
+    if (e == cudaSuccess) e = cudaMallocAsync((void**)&dq, sizeof(double4) * n, s->stream);
+    if (e == cudaSuccess) e = cudaMallocAsync((void**)&du, sizeof(double) * n, s->stream);
+    if (e == cudaSuccess) e = cudaMallocAsync((void**)&dd, 2 * n, s->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(db, hb.data(), sizeof(uint64_t) * n, cudaMemcpyHostToDevice, s->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dt, ht.data(), sizeof(double4) * n, cudaMemcpyHostToDevice, s->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dq, hq.data(), sizeof(double4) * n, cudaMemcpyHostToDevice, s->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(du, hu.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(dd, 0, 2 * n, s->stream);
+    if (e == cudaSuccess) {
+        Injected j;
+        j.bodies = db;
+        j.trial = dt;
+        j.trial_q = dq;
+        j.u = du;
+        j.decisions = dd;
+        j.flags = dd + n;
+        j.n = (uint32_t)n;
+        if (s->soft())
+            e = launch_trials_lj(s->dim, fp32 && !s->penalty(), s->geom, s->arr, s->pair, temperature, j, s->stream);
+        else if (s->oriented())
+            e = launch_trials_poly(fp32, s->geom, s->arr, s->verts, s->n_vertices, s->poly_rcut2, s->poly_rcut2_hi32, j,
+                                   s->stream);
+        else
+            e = launch_trials_sphere(s->dim, fp32, s->coop[fp32], s->geom, s->arr, s->pair, j, s->stream);
+        s->prof.kernel_launches++;
+    }
+    std::vector<uint8_t> hd(2 * n);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(hd.data(), dd, 2 * n, cudaMemcpyDeviceToHost, s->stream);
+    for (void* p : {(void*)db, (void*)dt, (void*)dq, (void*)du, (void*)dd})
+        if (p) cudaFreeAsync(p, s->stream);
+    cudaError_t e2 = cudaStreamSynchronize(s->stream);
+    if (e == cudaSuccess) e = e2;
+    if (e != cudaSuccess) return fail(HMC_CUDA_ERROR, "eval_trials: %s", cudaGetErrorString(e));
+    if ((st = read_stats(s))) return st;
+    if ((st = check_flags(s))) return st;
+    std::memcpy(decisions, hd.data(), n);
+    if (flags) std::memcpy(flags, hd.data() + n, n);
+    return HMC_OK;
+}
+
 }  // extern "C"
 
 // ---- batches of independent hard-sphere replicas ------------------------------------------
@@ -1881,6 +1998,7 @@ hmc_status hmc_batch_sweep(hmc_batch* bt, const hmc_sweep_params* params, hmc_co
         }
         tot.rechecks += bt->host_stats->rechecks;
         tot.pair_checks += bt->host_stats->pair_checks;
+        tot.order_ambiguous += bt->host_stats->ambiguous;
         double me;
         unsigned long long bits = bt->host_stats->max_err_bits;
         std::memcpy(&me, &bits, 8);
@@ -1961,9 +2079,84 @@ hmc_status hmc_batch_tune(hmc_batch* bt, hmc_sweep_params* params, double target
             return fail(HMC_INVALID_ARGUMENT, "replica %u: maximum must be positive", k);
         if (!(p.temperature > 0.0)) return fail(HMC_INVALID_ARGUMENT, "replica %u: temperature must be positive", k);
     }
+    for (uint32_t k = 0; k < bt->n_rep; ++k)
+        if ((params[k].flags & ~HMC_TUNE_PER_SAMPLE_STREAMS) || params[k].flags != params[0].flags)
+            return fail(HMC_INVALID_ARGUMENT, "tune flags must be known and the same for every replica");
     if (steps == 0 || bt->n == 0) return HMC_OK;
     HMC_CUDA(cudaSetDevice(bt->ctx->device));
     const bool lj = bt->interaction == HMC_LENNARD_JONES;
+    if (!(params[0].flags & HMC_TUNE_PER_SAMPLE_STREAMS)) {
+        // the reference's single stream per replica, one warp per replica in one launch: each
+        // replica's cell list is built (with its own Counter's checkerboard) into its own part of
+        // temporary space-count and space-start arrays, as hmc_tune builds a system's
+        std::vector<TuneJob> jobs;
+        std::vector<uint32_t> which;
+        uint64_t cells_total = 0;
+        for (uint32_t k = 0; k < bt->n_rep; ++k) cells_total += bt->cell_base[k + 1] - bt->cell_base[k] + 1;
+        uint32_t *cc = nullptr, *cs = nullptr;
+        TuneJob* dj = nullptr;
+        cudaError_t e = cudaMallocAsync((void**)&cc, sizeof(uint32_t) * cells_total, bt->stream);
+        if (e == cudaSuccess) e = cudaMallocAsync((void**)&cs, sizeof(uint32_t) * cells_total, bt->stream);
+        if (e == cudaSuccess) e = cudaMemsetAsync(bt->arr.stats, 0, sizeof(DeviceStats), bt->stream);
+        uint64_t off = 0;
+        for (uint32_t k = 0; k < bt->n_rep && e == cudaSuccess; ++k) {
+            const Replica& r = bt->rep[k];
+            const uint32_t cells_k = bt->cell_base[k + 1] - bt->cell_base[k];
+            const uint64_t o = off;
+            off += cells_k + 1;
+            if (r.n_bodies == 0) continue;
+            Geometry g = r.g;
+            Sfc64 rng = make_rng(r.step, r.substep, r.seed, UINT64_MAX);  // the origin of rebuild()
+            for (int a = 0; a < bt->dim; ++a) {
+                const double u0 = uniform01(rng);
+                g.origin[a] = -g.L[a] / 2.0 - u0 * g.width[a];
+            }
+            Arrays v = replica_view(bt, k);
+            v.cell_count = cc + o;
+            v.cell_start = cs + o;
+            // each rebuild appends to the colour lists from zero; the error flags of all of them
+            // (and of the tuner) accumulate
+            e = cudaMemsetAsync(&v.stats->nonempty, 0, sizeof(unsigned int), bt->stream);
+            if (e == cudaSuccess) e = cudaMemsetAsync(v.stats->color_count, 0, sizeof(unsigned int) * 8, bt->stream);
+            if (e == cudaSuccess) e = launch_rebuild(bt->dim, g, v, r.n_bodies, true, bt->stream);
+            bt->kernel_launches += 6;
+            TuneJob job{};
+            job.g = g;
+            job.a = v;
+            job.p = r.p;
+            job.step = r.step;
+            job.substep = r.substep;
+            job.seed = r.seed;
+            job.n_bodies = r.n_bodies;
+            job.samples = samples;
+            job.steps = steps;
+            job.maximum = params[k].maximum;
+            job.kt = params[k].temperature;
+            job.target = target;
+            jobs.push_back(job);
+            which.push_back(k);
+        }
+        const uint32_t nj = (uint32_t)jobs.size();
+        if (e == cudaSuccess && nj) e = cudaMallocAsync((void**)&dj, sizeof(TuneJob) * nj, bt->stream);
+        if (e == cudaSuccess && nj)
+            e = cudaMemcpyAsync(dj, jobs.data(), sizeof(TuneJob) * nj, cudaMemcpyHostToDevice, bt->stream);
+        if (e == cudaSuccess && nj) {
+            e = lj ? launch_tune_stream_lj(bt->dim, dj, nj, bt->stream)
+                   : launch_tune_stream_sphere(bt->dim, dj, nj, bt->stream);
+            bt->kernel_launches += 1;
+        }
+        if (e == cudaSuccess && nj)
+            e = cudaMemcpyAsync(jobs.data(), dj, sizeof(TuneJob) * nj, cudaMemcpyDeviceToHost, bt->stream);
+        for (void* ptr : {(void*)cc, (void*)cs, (void*)dj})
+            if (ptr) cudaFreeAsync(ptr, bt->stream);
+        cudaError_t e2 = cudaStreamSynchronize(bt->stream);
+        if (e == cudaSuccess) e = e2;
+        if (e != cudaSuccess) return fail(HMC_CUDA_ERROR, "batch tune: %s", cudaGetErrorString(e));
+        HMC_CUDA(cudaMemcpy(bt->host_stats, bt->arr.stats, sizeof(DeviceStats), cudaMemcpyDeviceToHost));
+        if (bt->host_stats->error_flags) return fail(HMC_OUTSIDE_CHECKERBOARD, "batch tune: a body maps to no space");
+        for (uint32_t j = 0; j < nj; ++j) params[which[j]].maximum = jobs[j].maximum;
+        return HMC_OK;
+    }
     uint64_t* db = nullptr;
     double4 *dt = nullptr, *dq = nullptr;
     double *du = nullptr, *dh = nullptr;

@@ -384,6 +384,7 @@ __device__ __forceinline__ double4 ldg4(const double4* p) {
 struct PairStats {
     uint32_t checks = 0;
     uint32_t rechecks = 0;
+    uint32_t ambiguous = 0;  // soft-potential decisions that the summation order could change
     double max_err = 0.0;
 };
 
@@ -426,6 +427,54 @@ __device__ __forceinline__ uint32_t active_count(const Arrays& A, uint32_t color
     return st->color_count[color];
 }
 
+// ---- the sequential-stream tuner -------------------------------------------------------------
+// tune_local_trial (hoomd-mc/src/tune_local.rs:42-88) on one warp for job J (TuneJob). Every lane
+// runs the same single stream Counter(step, substep, seed).make_rng() (index 0), so the trial is
+// computed redundantly and stays warp-uniform; only the pair work is spread over the lanes.
+// Per sample: random_range(0..n) for the body (rand's UniformUsize samples a u32 for ranges
+// that fit one: Canon's method, as IndexedRandom::choose), propose(rng, m, b, x, q) writes
+// W1 = wrap(propose(..)) and the proposed orientation, and accept(rng, b, x, q) decides the trial
+// (drawing the uniform itself when 0 < dH < infinity, as the reference does). After each round:
+// maximum *= (acceptance + 1.5) / (target + 1.5) (tune_by_scaling, lib.rs:514-524), clamped at
+// J.cap for rotations.
+template <typename Propose, typename Accept>
+__device__ __forceinline__ void tune_stream_run(TuneJob& J, Propose&& propose, Accept&& accept) {
+    Sfc64 rng = make_rng(J.step, J.substep, J.seed, 0);
+    double m = J.maximum;
+    uint32_t acc = 0;
+    for (uint32_t t = 0; t < J.steps; ++t) {
+        acc = 0;
+        for (uint32_t j = 0; j < J.samples; ++j) {
+            const uint32_t b = canon_range_u32(rng, J.n_bodies);
+            double x[3] = {0.0, 0.0, 0.0}, q[4] = {1.0, 0.0, 0.0, 0.0};
+            propose(rng, m, b, x, q);
+            if (accept(rng, b, x, q)) acc++;
+        }
+        const double ratio = ddiv((double)acc, (double)J.samples);
+        m = dmul(m, ddiv(dadd(ratio, 1.5), dadd(J.target, 1.5)));
+        if (J.cap > 0.0 && m > J.cap) m = J.cap;
+    }
+    if ((threadIdx.x & 31u) == 0) {
+        J.maximum = m;
+        J.accepted = acc;
+    }
+}
+
+// Translate<Cartesian<DIM>>::propose (translate/cartesian.rs:40-51) of body b, then wrap.
+template <int DIM>
+__device__ __forceinline__ void tune_translate(Sfc64& rng, const Geometry& g, const Arrays& A, double m, uint32_t b,
+                                               double* x) {
+    const double4 b4 = A.body_pos[b];
+    x[0] = b4.x;
+    x[1] = b4.y;
+    x[2] = DIM == 3 ? b4.z : 0.0;
+    double dv[3];
+    ball_sample<DIM>(rng, m, A.zig_x, A.zig_f, dv);
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) x[a] = dadd(x[a], dv[a]);
+    wrap_inv<DIM>(g.L, g.invL, x);
+}
+
 __device__ __forceinline__ void flush_stats(DeviceStats* stats, const PairStats& st, uint32_t accepted) {
     const unsigned full = 0xffffffffu;
     unsigned acc = __reduce_add_sync(full, accepted);
@@ -437,6 +486,7 @@ __device__ __forceinline__ void flush_stats(DeviceStats* stats, const PairStats&
         if (rech) atomicAdd(&stats->rechecks, (unsigned long long)rech);
     }
     if (st.max_err > 0.0) atomicMax(&stats->max_err_bits, (unsigned long long)__double_as_longlong(st.max_err));
+    if (st.ambiguous) atomicAdd(&stats->ambiguous, (unsigned long long)st.ambiguous);
 }
 
 

@@ -28,6 +28,8 @@ struct DeviceStats {
     unsigned long long overlaps;      // pairs found by the overlap check
     unsigned int color_count[8];      // non-empty spaces per colour after a rebuild
     unsigned int rounds;              // full colour sets of the sweep: ceil(N / non-empty spaces)
+    unsigned long long ambiguous;     // soft-potential trials whose decision the order of the
+                                      // FP64 pair-energy sum could change (order_ambiguous)
 };
 
 // The checkerboard (hoomd-mc/src/hypercuboid.rs) together with the periodic box.
@@ -123,6 +125,47 @@ struct Launch {
                                 // same sweep (this pass may start before it ends)
     uint32_t early_wait;        // 1: the previous launch is the rebuild's last kernel: launch
                                 // early but wait for it before reading anything
+};
+
+// Injected trials for the probe mode of the colour-pass kernels (hmc_eval_trials): trial i
+// moves body bodies[i] to W1 = trial[i] (the body position wrap(propose(..)) returns) with the
+// versor trial_q[i] and the Metropolis uniform u[i]. The kernel then runs the pass's own
+// decision code on it against the unchanged state and writes decisions[i] and flags[i]
+// instead of committing the move.
+struct Injected {
+    const uint64_t* bodies = nullptr;
+    const double4* trial = nullptr;
+    const double4* trial_q = nullptr;  // shapes
+    const double* u = nullptr;         // Lennard-Jones and the overlap penalty
+    uint8_t* decisions = nullptr;
+    uint8_t* flags = nullptr;
+    uint32_t n = 0;
+};
+enum : uint8_t {
+    kTrialRechecked = 1,     // the FP32 pass settled the trial with FP64 pair evaluations
+    kTrialOutsideSpace = 2,  // W1 lies outside the body's checkerboard space (the colour pass
+                             // rejects such a move before any pair test, parallel_sweep.rs:253-258)
+    kTrialAmbiguous = 4,     // another summation order of the FP64 pair energies could change the
+                             // Metropolis decision (order_ambiguous)
+};
+
+// One tuning run of tune_local_trial (hoomd-mc/src/tune_local.rs:42-88) with the reference's
+// single sequential stream: a warp per job runs `steps` rounds of `samples` trials from
+// Counter(step, substep, seed) (index 0) against the unchanged state in `a` (cell-ordered with
+// FP64 sites and body slots), scaling `maximum` after each round. A system's tuning is one job;
+// a batch's is one job per replica (a views the replica's part of the batch arrays).
+struct TuneJob {
+    Geometry g;
+    Arrays a;
+    Pair p;
+    uint64_t step;
+    uint32_t substep, seed;
+    uint32_t n_bodies, samples, steps, rotate;
+    double maximum;            // in: the start; out: the tuned maximum
+    double kt, target;
+    double cap;                // Rotate<Versor>: pi/2, Rotate<Angle>: pi; 0 = no clamp (Translate)
+    unsigned long long accepted;   // out: accepted trials of the last round
+    unsigned long long ambiguous;  // out: soft-potential decisions another summation order could change
 };
 
 // Launch configuration of a colour pass: 128 threads per block; overlap = programmatic
@@ -306,6 +349,23 @@ cudaError_t launch_pack_positions(int dim, const double4* body_pos, double* pack
 // (angles, 2-D), FP32 site versors (n x 4), in body order.
 cudaError_t launch_gsd_encode(int dim, int ori_kind, const Geometry& g, const double4* body_pos,
                               const double4* body_ori, uint64_t n, float* pos, float* ori, cudaStream_t s);
+// Injected trials through the colour-pass kernels themselves (the probe mode, Injected): the
+// hard-sphere passes (FP32: the per-lane pass, FP64: the warp-cooperative pass, or the one
+// `coop` names), the Lennard-Jones and overlap-penalty passes, the packed polyhedron pass.
+cudaError_t launch_trials_sphere(int dim, bool fp32, bool coop, const Geometry& g, const Arrays& a, const Pair& p,
+                                 const Injected& j, cudaStream_t s);
+cudaError_t launch_trials_lj(int dim, bool fp32, const Geometry& g, const Arrays& a, const Pair& p, double kt,
+                             const Injected& j, cudaStream_t s);
+cudaError_t launch_trials_poly(bool fp32, const Geometry& g, const Arrays& a, const double4* verts, uint32_t nv,
+                               double rcut2, float rcut2_hi32, const Injected& j, cudaStream_t s);
+// The sequential-stream tuner (TuneJob), one warp per job (jobs in device memory): hard spheres,
+// Lennard-Jones / overlap penalty, convex polyhedra, convex polygons (sat: separating axes).
+cudaError_t launch_tune_stream_sphere(int dim, TuneJob* jobs, uint32_t n_jobs, cudaStream_t s);
+cudaError_t launch_tune_stream_lj(int dim, TuneJob* jobs, uint32_t n_jobs, cudaStream_t s);
+cudaError_t launch_tune_stream_poly(TuneJob* jobs, uint32_t n_jobs, const double4* verts, uint32_t nv, double rcut2,
+                                    cudaStream_t s);
+cudaError_t launch_tune_stream_poly2(bool sat, TuneJob* jobs, uint32_t n_jobs, const double4* verts, uint32_t nv,
+                                     double rcut2, cudaStream_t s);
 // Injected moves: positions (n x 4 doubles), result decisions and recheck flags.
 cudaError_t launch_eval_sphere(int dim, bool fp32, const Geometry& g, const Arrays& a, const Pair& p,
                                const uint64_t* bodies, const double4* trial, uint32_t n, uint8_t* decisions,

@@ -199,6 +199,34 @@ __device__ __forceinline__ bool sphere_propose(const Geometry& g, const Arrays& 
     return true;
 }
 
+// The proposal half of injected trial i (the colour passes' probe mode): the given W1 in
+// place of the drawn one, the walk around W1's own space (the stencil of its body's space when
+// W1 stays in it, as in the sweep), self = the body's slot. A W1 outside the body's space is
+// flagged (the sweep rejects it before any pair test) and its pair decision still computed.
+template <int DIM, bool FP32>
+__device__ __forceinline__ bool sphere_inject(const Geometry& g, const Arrays& A, const uint32_t* __restrict__ cs,
+                                              const Injected& J, uint32_t i, uint32_t* m, SphereProposal<DIM>& pr,
+                                              uint8_t& flag) {
+    const uint64_t body = J.bodies[i];
+    pr.k = A.slot_of_body[body];
+    const double4 w = J.trial[i];
+    double x[3] = {w.x, w.y, DIM == 3 ? w.z : 0.0};
+    if (!point_to_space<DIM>(g, x, m)) {
+        atomicOr(&A.stats->error_flags, kErrOutsideCheckerboard);
+        return false;
+    }
+    if (cell_index<DIM>(g, m) != A.body_cell[body]) flag |= kTrialOutsideSpace;
+    uint32_t lo, hi;
+    row_span(g.shape[DIM - 1], m[DIM - 1], &lo, &hi);
+    load_rows<DIM>(g, cs, m, lo, hi, pr.a0, pr.a1);
+    pr.t[0] = x[0];
+    pr.t[1] = x[1];
+    pr.t[2] = x[2];
+    wrap_inv<DIM>(g.L, g.invL, pr.t);  // T = wrap(W1), as delta_energy_one wraps the site
+    pr.t32 = FP32 ? cell_offsets<DIM>(g, pr.t, m) : make_float4(0.f, 0.f, 0.f, 0.f);
+    return true;
+}
+
 // update_body_properties for an accepted move: body = wrap(W1) = T, site = wrap(body).
 template <int DIM, bool FP32>
 __device__ __forceinline__ void sphere_commit(const Geometry& g, const Arrays& A, const uint32_t* m, uint32_t k,
@@ -213,10 +241,12 @@ __device__ __forceinline__ void sphere_commit(const Geometry& g, const Arrays& A
 
 // The decision half: the candidate walk against the current sites, then update_body_properties.
 // Returns kOverlap (rejected) or kClear (accepted and committed); with DEFER_UNCERTAIN it returns
-// the walk's result (kUncertain included) and commits nothing. COMPACT (the replica batch pass,
+// the walk's result (kUncertain included) and commits nothing; NO_COMMIT settles the trial and
+// commits nothing (the probe mode). COMPACT (the replica batch pass,
 // whose larger code misses in the instruction cache): one copy of the row walk for both
 // segments.
-template <int DIM, bool FP32, bool COMPACT = false, bool DEFER_UNCERTAIN = false, bool DEFER_EDGE = false>
+template <int DIM, bool FP32, bool COMPACT = false, bool DEFER_UNCERTAIN = false, bool DEFER_EDGE = false,
+          bool NO_COMMIT = false>
 __device__ __forceinline__ int sphere_decide_res(const Geometry& g, const Arrays& A, const Pair& P,
                                                  const uint32_t* __restrict__ cs, const uint32_t* m,
                                                  SphereProposal<DIM>& pr, PairStats& st) {
@@ -260,7 +290,7 @@ __device__ __forceinline__ int sphere_decide_res(const Geometry& g, const Arrays
         st.max_err = st2.max_err > st.max_err ? st2.max_err : st.max_err;
     }
     if (res == kOverlap) return kOverlap;
-    sphere_commit<DIM, FP32>(g, A, m, k, t);
+    if (!NO_COMMIT) sphere_commit<DIM, FP32>(g, A, m, k, t);
     return kClear;
 }
 
@@ -326,13 +356,16 @@ __device__ __forceinline__ bool sphere_warp_recheck(const Geometry& g, const Arr
 // space (parallel_sweep.rs:231-278) followed by update_bodies (:283-314) for an accepted move.
 // Spaces of one colour are two spaces apart, so the in-place update of an accepted body is
 // invisible to every other trial of the colour, as in the reference.
-template <int DIM, bool FP32>
-__global__ void __launch_bounds__(128, HMC_SWEEP_MIN_BLOCKS) k_sweep_sphere(Geometry g, Arrays A, Pair P, Launch L) {
+// INJ: the probe mode (Injected): lane i takes injected trial i, runs the same decision code
+// and writes its decision instead of committing.
+template <int DIM, bool FP32, bool INJ = false>
+__global__ void __launch_bounds__(128, HMC_SWEEP_MIN_BLOCKS)
+    k_sweep_sphere(Geometry g, Arrays A, Pair P, Launch L, Injected J) {
     if (L.early_wait) grid_dependency_wait();  // first pass: the rebuild's arrays are read at once
     uint32_t n_accepted = 0;
     PairStats st;
     const uint32_t stride = gridDim.x * blockDim.x;
-    const uint32_t n_active = active_count(A, L.color, L.round);
+    const uint32_t n_active = INJ ? J.n : active_count(A, L.color, L.round);
     if (FP32) {
         // Warp-uniform loop: a trial left undecided by its lane's walk is settled by the whole
         // warp (sphere_warp_recheck). The per-lane generic walk it replaces is a chain of ~27
@@ -344,9 +377,14 @@ __global__ void __launch_bounds__(128, HMC_SWEEP_MIN_BLOCKS) k_sweep_sphere(Geom
             uint32_t m[3] = {0, 0, 0};
             SphereProposal<DIM> pr;
             bool valid = false;
+            uint8_t flag = 0;
             if (tid < n_active) {
-                unpack_m<DIM>(__ldg(A.color_cells + (size_t)L.color * g.color_stride + tid), m);
-                valid = sphere_propose<DIM, FP32>(g, A, A.cell_start, m, L.step, L.substep, L.seed, L.max_move, pr);
+                if constexpr (INJ) {
+                    valid = sphere_inject<DIM, FP32>(g, A, A.cell_start, J, tid, m, pr, flag);
+                } else {
+                    unpack_m<DIM>(__ldg(A.color_cells + (size_t)L.color * g.color_stride + tid), m);
+                    valid = sphere_propose<DIM, FP32>(g, A, A.cell_start, m, L.step, L.substep, L.seed, L.max_move, pr);
+                }
             }
             grid_dependency_wait();  // the previous colour's moves are visible from here on
             allow_dependent_launch();
@@ -360,7 +398,10 @@ __global__ void __launch_bounds__(128, HMC_SWEEP_MIN_BLOCKS) k_sweep_sphere(Geom
             while (todo) {
                 const int src = __ffs(todo) - 1;
                 todo &= todo - 1u;
+                const uint32_t r0 = st.rechecks;
                 const bool ov = sphere_warp_recheck<DIM>(g, A, P, A.cell_start, m, pr, src, lane, st);
+                if constexpr (INJ)
+                    if (__any_sync(0xffffffffu, st.rechecks != r0) && (int)lane == src) flag |= kTrialRechecked;
                 if ((int)lane == src) res = ov ? kOverlap : kClear;
             }
             if (kWarpEdge) {
@@ -371,11 +412,19 @@ __global__ void __launch_bounds__(128, HMC_SWEEP_MIN_BLOCKS) k_sweep_sphere(Geom
                 while (todo2) {
                     const int src = __ffs(todo2) - 1;
                     todo2 &= todo2 - 1u;
+                    const uint32_t r0 = st.rechecks;
                     const bool ov = sphere_warp_recheck<DIM, true>(g, A, P, A.cell_start, m, pr, src, lane, st);
+                    if constexpr (INJ)
+                        if (__any_sync(0xffffffffu, st.rechecks != r0) && (int)lane == src) flag |= kTrialRechecked;
                     if ((int)lane == src && ov) res = kOverlap;
                 }
             }
-            if (res == kClear) {
+            if constexpr (INJ) {
+                if (tid < n_active) {
+                    J.decisions[tid] = valid && res == kClear;
+                    J.flags[tid] = flag;
+                }
+            } else if (res == kClear) {
                 sphere_commit<DIM, FP32>(g, A, m, pr.k, pr.t);
                 n_accepted++;
             }
@@ -387,12 +436,27 @@ __global__ void __launch_bounds__(128, HMC_SWEEP_MIN_BLOCKS) k_sweep_sphere(Geom
     }
     for (uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x; tid < n_active; tid += stride) {
         uint32_t m[3] = {0, 0, 0};
-        unpack_m<DIM>(__ldg(A.color_cells + (size_t)L.color * g.color_stride + tid), m);
         SphereProposal<DIM> pr;
-        const bool valid = sphere_propose<DIM, FP32>(g, A, A.cell_start, m, L.step, L.substep, L.seed, L.max_move, pr);
+        bool valid;
+        uint8_t flag = 0;
+        if constexpr (INJ) {
+            valid = sphere_inject<DIM, FP32>(g, A, A.cell_start, J, tid, m, pr, flag);
+        } else {
+            unpack_m<DIM>(__ldg(A.color_cells + (size_t)L.color * g.color_stride + tid), m);
+            valid = sphere_propose<DIM, FP32>(g, A, A.cell_start, m, L.step, L.substep, L.seed, L.max_move, pr);
+        }
         grid_dependency_wait();  // the previous colour's moves are visible from here on
         allow_dependent_launch();
-        if (valid && sphere_decide<DIM, FP32>(g, A, P, A.cell_start, m, pr, st)) n_accepted++;
+        if constexpr (INJ) {
+            const uint32_t r0 = st.rechecks;
+            const bool clear =
+                valid && sphere_decide_res<DIM, FP32, false, false, false, true>(g, A, P, A.cell_start, m, pr, st) ==
+                             kClear;
+            J.decisions[tid] = clear;
+            J.flags[tid] = flag | (st.rechecks != r0 ? kTrialRechecked : 0);
+        } else if (valid && sphere_decide<DIM, FP32>(g, A, P, A.cell_start, m, pr, st)) {
+            n_accepted++;
+        }
     }
     grid_dependency_wait();
     allow_dependent_launch();
@@ -450,9 +514,9 @@ __device__ __forceinline__ int sphere_rows_head(const Geometry& g, const Arrays&
     return flags;
 }
 
-template <int DIM, bool FP32>
-__global__ void __launch_bounds__(128, HMC_SWEEP_MIN_BLOCKS) k_sweep_sphere_coop(Geometry g, Arrays A, Pair P,
-                                                                                  Launch L) {
+template <int DIM, bool FP32, bool INJ = false>
+__global__ void __launch_bounds__(128, HMC_SWEEP_MIN_BLOCKS)
+    k_sweep_sphere_coop(Geometry g, Arrays A, Pair P, Launch L, Injected J) {
     constexpr int R = kRows<DIM>;
     constexpr int NR = 2 * R;  // row ranges plus, at a fast-axis end, the wrapped spaces
     using Site = typename std::conditional<FP32, float4, double4>::type;
@@ -469,7 +533,7 @@ __global__ void __launch_bounds__(128, HMC_SWEEP_MIN_BLOCKS) k_sweep_sphere_coop
     uint32_t n_accepted = 0;
     PairStats st;
     const uint32_t stride = gridDim.x * blockDim.x;
-    const uint32_t n_active = active_count(A, L.color, L.round);
+    const uint32_t n_active = INJ ? J.n : active_count(A, L.color, L.round);
     for (uint32_t base = blockIdx.x * blockDim.x + warp * 32; base < n_active; base += stride) {
         const uint32_t tid = base + lane;
         uint32_t m[3] = {0, 0, 0}, cell = 0, k = 0, sf = g.shape[DIM - 1], mf = 0;
@@ -478,7 +542,31 @@ __global__ void __launch_bounds__(128, HMC_SWEEP_MIN_BLOCKS) k_sweep_sphere_coop
         int res = kFlagOverlap;  // lanes without a trial in the cell count as decided
         bool edge = false, trial = false;
         uint32_t a0[R], a1[R];
-        if (tid < n_active) {
+        uint8_t flag = 0;
+        if (INJ && tid < n_active) {
+            // the probe mode: the injected W1 and the walk around its space (sphere_inject)
+            const uint64_t body = J.bodies[tid];
+            k = A.slot_of_body[body];
+            const double4 w = J.trial[tid];
+            const double x[3] = {w.x, w.y, DIM == 3 ? w.z : 0.0};
+            if (point_to_space<DIM>(g, x, m)) {
+                cell = cell_index<DIM>(g, m);
+                if (cell != A.body_cell[body]) flag |= kTrialOutsideSpace;
+                mf = m[DIM - 1];
+                edge = sf > 2 && (mf == 0 || mf + 1 == sf);
+                uint32_t lo, hi;
+                row_span(sf, mf, &lo, &hi);
+                load_rows<DIM>(g, A.cell_start, m, lo, hi, a0, a1);
+                trial = true;
+                t[0] = x[0];
+                t[1] = x[1];
+                t[2] = x[2];
+                wrap_inv<DIM>(g.L, g.invL, t);
+                if (FP32) t32 = cell_offsets<DIM>(g, t, m);
+            } else {
+                atomicOr(&A.stats->error_flags, kErrOutsideCheckerboard);
+            }
+        } else if (tid < n_active) {
             unpack_m<DIM>(__ldg(A.color_cells + (size_t)L.color * g.color_stride + tid), m);
             cell = cell_index<DIM>(g, m);
             mf = m[DIM - 1];
@@ -583,14 +671,23 @@ __global__ void __launch_bounds__(128, HMC_SWEEP_MIN_BLOCKS) k_sweep_sphere_coop
             if (lane == src) res = ov ? kFlagOverlap : ((res & kFlagUncertain) | (un ? kFlagUncertain : 0));
         }
         __syncwarp();
-        if (!trial || res == kFlagOverlap) continue;
-        if (res & kFlagUncertain) {
+        bool clear = trial && res != kFlagOverlap;
+        if (clear && (res & kFlagUncertain)) {
             PairStats st2;  // the fast path already counted its pair checks
             const bool ov = sphere_overlaps_generic<DIM, FP32>(g, A, P, A.cell_start, t, t32, m, k, st2);
             st.rechecks += st2.rechecks;
             st.max_err = st2.max_err > st.max_err ? st2.max_err : st.max_err;
-            if (ov) continue;
+            if (st2.rechecks) flag |= kTrialRechecked;
+            if (ov) clear = false;
         }
+        if constexpr (INJ) {
+            if (tid < n_active) {
+                J.decisions[tid] = clear;
+                J.flags[tid] = flag;
+            }
+            continue;
+        }
+        if (!clear) continue;
         n_accepted++;
         // update_body_properties: body = wrap(W1) = T, site = wrap(body)
         double sv[3] = {t[0], t[1], t[2]};
@@ -949,6 +1046,45 @@ __global__ void k_eval_sphere(Geometry g, Arrays A, Pair P, const uint64_t* bodi
         rechecked[i] = st.rechecks > 0;
     }
     flush_stats(A.stats, st, 0u);
+}
+
+// The sequential-stream tuner for hard spheres (tune_stream_run): a trial is accepted when
+// its site overlaps no other site (dH = 0, no uniform drawn) and rejected otherwise (dH = inf).
+// The warp takes the stencil around the trial site's space 32 candidates at a time, FP64 pair
+// tests on the unchanged state, stopping at the first overlap.
+template <int DIM>
+__global__ void __launch_bounds__(32) k_tune_stream_sphere(TuneJob* jobs, uint32_t n_jobs) {
+    if (blockIdx.x >= n_jobs) return;
+    TuneJob& J = jobs[blockIdx.x];
+    const Geometry& g = J.g;
+    const Arrays& A = J.a;
+    const double sigma2 = J.p.sigma2;
+    const uint32_t lane = threadIdx.x & 31u;
+    tune_stream_run(
+        J, [&](Sfc64& rng, double m, uint32_t b, double* x, double*) { tune_translate<DIM>(rng, g, A, m, b, x); },
+        [&](Sfc64&, uint32_t b, const double* x, const double*) -> bool {
+            double t[3] = {x[0], x[1], x[2]};
+            wrap_inv<DIM>(g.L, g.invL, t);  // the site of the trial body
+            uint32_t m[3] = {0, 0, 0};
+            if (!point_to_space<DIM>(g, t, m)) {
+                if (lane == 0) atomicOr(&A.stats->error_flags, kErrOutsideCheckerboard);
+                return false;
+            }
+            const uint32_t self = A.slot_of_body[b];
+            const FlatStencil fs = flat_stencil<DIM>(g, A.cell_start, m, lane);
+            for (uint32_t j0 = 0; j0 < fs.total; j0 += 32) {
+                uint32_t part;
+                const uint32_t q = flat_slot(fs, j0 + lane, part);
+                bool hit = false;
+                if (j0 + lane < fs.total && q != self) {
+                    const double4 s4 = ldg4(A.sorted_s + q);
+                    const double sv[3] = {s4.x, s4.y, s4.z};
+                    hit = ref_dist2<DIM>(g, t, sv) < sigma2;
+                }
+                if (__any_sync(0xffffffffu, hit)) return false;
+            }
+            return true;
+        });
 }
 
 template <typename T>
@@ -1524,10 +1660,10 @@ cudaError_t launch_sweep_sphere(int dim, bool fp32, const Geometry& g, const Arr
         if (grid > (uint32_t)cb) grid = (uint32_t)cb;
         PassLaunch pl(grid, l.overlap_previous != 0 || l.early_wait != 0, s);
         if (dim == 2)
-            return fp32 ? cudaLaunchKernelEx(&pl.cfg, k_sweep_sphere_coop<2, true>, g, a, p, l)
-                        : cudaLaunchKernelEx(&pl.cfg, k_sweep_sphere_coop<2, false>, g, a, p, l);
-        return fp32 ? cudaLaunchKernelEx(&pl.cfg, k_sweep_sphere_coop<3, true>, g, a, p, l)
-                    : cudaLaunchKernelEx(&pl.cfg, k_sweep_sphere_coop<3, false>, g, a, p, l);
+            return fp32 ? cudaLaunchKernelEx(&pl.cfg, k_sweep_sphere_coop<2, true>, g, a, p, l, Injected{})
+                        : cudaLaunchKernelEx(&pl.cfg, k_sweep_sphere_coop<2, false>, g, a, p, l, Injected{});
+        return fp32 ? cudaLaunchKernelEx(&pl.cfg, k_sweep_sphere_coop<3, true>, g, a, p, l, Injected{})
+                    : cudaLaunchKernelEx(&pl.cfg, k_sweep_sphere_coop<3, false>, g, a, p, l, Injected{});
     }
     // Grid-stride over the colour's list with at most one resident wave of blocks.
     static int max_blocks[2][2] = {{0, 0}, {0, 0}};
@@ -1550,10 +1686,52 @@ cudaError_t launch_sweep_sphere(int dim, bool fp32, const Geometry& g, const Arr
     if (grid > (uint32_t)mb) grid = (uint32_t)mb;
     PassLaunch pl(grid, l.overlap_previous != 0 || l.early_wait != 0, s);
     if (dim == 2)
-        return fp32 ? cudaLaunchKernelEx(&pl.cfg, k_sweep_sphere<2, true>, g, a, p, l)
-                    : cudaLaunchKernelEx(&pl.cfg, k_sweep_sphere<2, false>, g, a, p, l);
-    return fp32 ? cudaLaunchKernelEx(&pl.cfg, k_sweep_sphere<3, true>, g, a, p, l)
-                : cudaLaunchKernelEx(&pl.cfg, k_sweep_sphere<3, false>, g, a, p, l);
+        return fp32 ? cudaLaunchKernelEx(&pl.cfg, k_sweep_sphere<2, true>, g, a, p, l, Injected{})
+                    : cudaLaunchKernelEx(&pl.cfg, k_sweep_sphere<2, false>, g, a, p, l, Injected{});
+    return fp32 ? cudaLaunchKernelEx(&pl.cfg, k_sweep_sphere<3, true>, g, a, p, l, Injected{})
+                : cudaLaunchKernelEx(&pl.cfg, k_sweep_sphere<3, false>, g, a, p, l, Injected{});
+}
+
+cudaError_t launch_trials_sphere(int dim, bool fp32, bool coop, const Geometry& g, const Arrays& a, const Pair& p,
+                                 const Injected& j, cudaStream_t s) {
+    if (j.n == 0) return cudaSuccess;
+    const Launch l{};
+    const uint32_t grid = blocks_for(j.n, 128);
+    if (coop) {
+        if (dim == 2) {
+            if (fp32)
+                k_sweep_sphere_coop<2, true, true><<<grid, 128, 0, s>>>(g, a, p, l, j);
+            else
+                k_sweep_sphere_coop<2, false, true><<<grid, 128, 0, s>>>(g, a, p, l, j);
+        } else {
+            if (fp32)
+                k_sweep_sphere_coop<3, true, true><<<grid, 128, 0, s>>>(g, a, p, l, j);
+            else
+                k_sweep_sphere_coop<3, false, true><<<grid, 128, 0, s>>>(g, a, p, l, j);
+        }
+    } else {
+        if (dim == 2) {
+            if (fp32)
+                k_sweep_sphere<2, true, true><<<grid, 128, 0, s>>>(g, a, p, l, j);
+            else
+                k_sweep_sphere<2, false, true><<<grid, 128, 0, s>>>(g, a, p, l, j);
+        } else {
+            if (fp32)
+                k_sweep_sphere<3, true, true><<<grid, 128, 0, s>>>(g, a, p, l, j);
+            else
+                k_sweep_sphere<3, false, true><<<grid, 128, 0, s>>>(g, a, p, l, j);
+        }
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tune_stream_sphere(int dim, TuneJob* jobs, uint32_t n_jobs, cudaStream_t s) {
+    if (n_jobs == 0) return cudaSuccess;
+    if (dim == 2)
+        k_tune_stream_sphere<2><<<n_jobs, 32, 0, s>>>(jobs, n_jobs);
+    else
+        k_tune_stream_sphere<3><<<n_jobs, 32, 0, s>>>(jobs, n_jobs);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_overlap_sphere(int dim, const Geometry& g, const Arrays& a, const Pair& p, uint32_t n,

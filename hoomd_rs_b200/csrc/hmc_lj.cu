@@ -92,11 +92,12 @@ __device__ __forceinline__ uint32_t warp_maxu(uint32_t v) {
 // its own in that order, then a butterfly reduction (every lane ends with the same values).
 // S of a candidate comes from sorted_s when have_s, else from wrap(sorted_b). The two sums of
 // one call equal two calls of one sum each over the same stencil.
+// mag receives sum |e| over both sums (for order_ambiguous).
 template <int DIM, bool TWO>
 __device__ __forceinline__ void lj_energy64(const Geometry& g, const Arrays& A, const Pair& P, const double* ta,
                                             const double* tb, const FlatStencil& fs, uint32_t self, bool have_s,
-                                            uint32_t lane, double& ea, double& eb) {
-    double a = 0.0, b = 0.0;
+                                            uint32_t lane, double& ea, double& eb, double& mag) {
+    double a = 0.0, b = 0.0, am = 0.0;
 #pragma unroll 1
     for (uint32_t j0 = 0; j0 < fs.total; j0 += 32) {
         const uint32_t j = j0 + lane;
@@ -116,12 +117,52 @@ __device__ __forceinline__ void lj_energy64(const Geometry& g, const Arrays& A, 
                 sv[2] = b4.z;
                 wrap_inv<DIM>(g.L, g.invL, sv);
             }
-            a = dadd(a, lj_pair64(P, ref_dist2<DIM>(g, ta, sv)));
-            if (TWO) b = dadd(b, lj_pair64(P, ref_dist2<DIM>(g, tb, sv)));
+            const double x = lj_pair64(P, ref_dist2<DIM>(g, ta, sv));
+            a = dadd(a, x);
+            am += fabs(x);
+            if (TWO) {
+                const double y = lj_pair64(P, ref_dist2<DIM>(g, tb, sv));
+                b = dadd(b, y);
+                am += fabs(y);
+            }
         }
     }
     ea = warp_sum(a);
     eb = TWO ? warp_sum(b) : 0.0;
+    mag = warp_sum(am);
+}
+
+// Whether another order of the same FP64 sums could change the Metropolis decision. The pair
+// energies are the same numbers in any order, and recursive summation of n terms in any order
+// (any summation tree) lies within gamma_{n-1} sum|e| of the exact sum, gamma_k = k u / (1 - k u),
+// u = 2^-53 (Higham, Accuracy and Stability of Numerical Algorithms, 2nd ed., 2002, section
+// 4.2). So dU = E_final - E_initial summed in any two orders (this pass's lanes and
+// butterfly, the reference's cell-list order) differ by at most
+// B = 2 gamma_{n-1} (sum|e_final| + sum|e_initial|) + 2 u |dU|. The decision (dU <= 0, else
+// u < exp(-dU / kT), parallel_sweep.rs:267-268) is monotone in dU: it is the same in every order
+// when dU - B and dU + B decide alike, with exp allowed 4 ulp either way (the reference calls
+// the platform libm, this pass CUDA's exp). n = the candidates of the stencil (>= the terms);
+// e0 = exp(-dU / kT) as the decision computed it. Over [dU - B, dU + B] exp(-x / kT) stays
+// within a factor exp(B / kT) <= 1 + 2 B / kT of e0 (B / kT < 1e-3), so a uniform farther than
+// e0 (4 B / kT + 1e-14) from e0 settles the trial without evaluating the ends.
+__device__ __forceinline__ double order_bound(double du, double mag, uint32_t n) {
+    const double unit = 1.1102230246251565e-16;  // 2^-53
+    const double k = (double)(n > 1u ? n - 1u : 1u);
+    const double gamma = k * unit / (1.0 - k * unit);
+    return 1.01 * (2.0 * gamma * mag + 2.0 * unit * fabs(du)) + 1e-300;
+}
+__device__ __forceinline__ bool order_ambiguous(double du, double mag, uint32_t n, double u, double kt, double e0) {
+    if (!isfinite(du) || !isfinite(mag)) return false;  // an infinite pair energy decides in any order
+    const double unit = 1.1102230246251565e-16;        // 2^-53
+    const double b = order_bound(du, mag, n);
+    const double lo = du - b, hi = du + b;
+    if (hi <= 0.0) return false;  // accepted in every order, without a uniform
+    const double rel = b / kt;
+    if (lo > 0.0 && rel < 1e-3 && fabs(u - e0) > e0 * (4.0 * rel + 1e-14)) return false;
+    const double ulp4 = 8.0 * unit;
+    const bool acc_at_lo = lo <= 0.0 || u < exp(-lo / kt) * (1.0 + ulp4);
+    const bool acc_at_hi = u < exp(-hi / kt) * (1.0 - ulp4);
+    return acc_at_lo != acc_at_hi;
 }
 
 struct Sums32 {
@@ -200,46 +241,91 @@ __device__ __forceinline__ int decide32(const Sums32& s, double kt, double u) {
     return -1;
 }
 
-// The FP64 pass: one warp per trial.
+// Injected trial w of the probe mode (Injected) in a warp-per-trial pass: the body's slot and
+// space, W1 and u from the list. The colour pass evaluates only trials that stay in their body's
+// space; the others are rejected as in the sweep (kTrialOutsideSpace).
 template <int DIM>
-__global__ void __launch_bounds__(128, HMC_LJ_MIN_BLOCKS) k_sweep_lj(Geometry g, Arrays A, Pair P, Launch L) {
+__device__ __forceinline__ void lj_inject(const Arrays& A, const Injected& J, uint32_t w, uint32_t* m, uint32_t& k,
+                                          double* x, double& u) {
+    const uint64_t body = J.bodies[w];
+    k = A.slot_of_body[body];
+    unpack_m<DIM>(A.body_m[body], m);
+    const double4 w4 = J.trial[w];
+    x[0] = w4.x;
+    x[1] = w4.y;
+    x[2] = DIM == 3 ? w4.z : 0.0;
+    u = J.u[w];
+}
+
+// The FP64 pass: one warp per trial. INJ: the probe mode (decisions instead of commits).
+template <int DIM, bool INJ = false>
+__global__ void __launch_bounds__(128, HMC_LJ_MIN_BLOCKS) k_sweep_lj(Geometry g, Arrays A, Pair P, Launch L,
+                                                                     Injected J) {
     if (L.early_wait) grid_dependency_wait();  // first pass: the rebuild's arrays are read at once
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t n_warps = (gridDim.x * blockDim.x) >> 5;
     uint32_t n_accepted = 0;
     PairStats pst;
-    const uint32_t n_active = active_count(A, L.color, L.round);
+    const uint32_t n_active = INJ ? J.n : active_count(A, L.color, L.round);
     for (uint32_t w = warp; w < n_active; w += n_warps) {
         uint32_t m[3] = {0, 0, 0};
-        unpack_m<DIM>(__ldg(A.color_cells + (size_t)L.color * g.color_stride + w), m);
+        uint32_t k = 0;
+        double x[3] = {0.0, 0.0, 0.0};
+        double u = 0.0;
+        if constexpr (INJ)
+            lj_inject<DIM>(A, J, w, m, k, x, u);
+        else
+            unpack_m<DIM>(__ldg(A.color_cells + (size_t)L.color * g.color_stride + w), m);
         const uint32_t cell = cell_index<DIM>(g, m);
         const FlatStencil fs = flat_stencil<DIM>(g, A.cell_start, m, lane);
-        const uint32_t start = __ldg(A.cell_start + cell);
-        const uint32_t count = __ldg(A.cell_start + cell + 1) - start;
-        // every lane draws the same stream: the trial is computed redundantly, warp-uniform
-        Sfc64 rng = make_rng(L.step, L.substep, L.seed, (uint64_t)cell);
-        const uint32_t k = start + canon_range_u32(rng, count);
-        const double4 b4 = A.sorted_b[k];
-        double x[3] = {b4.x, b4.y, b4.z};
-        double dv[3];
-        ball_sample<DIM>(rng, L.max_move, A.zig_x, A.zig_f, dv);
-        const double u = uniform01(rng);
+        if constexpr (!INJ) {
+            const uint32_t start = __ldg(A.cell_start + cell);
+            const uint32_t count = __ldg(A.cell_start + cell + 1) - start;
+            // every lane draws the same stream: the trial is computed redundantly, warp-uniform
+            Sfc64 rng = make_rng(L.step, L.substep, L.seed, (uint64_t)cell);
+            k = start + canon_range_u32(rng, count);
+            const double4 b4 = A.sorted_b[k];
+            x[0] = b4.x;
+            x[1] = b4.y;
+            x[2] = b4.z;
+            double dv[3];
+            ball_sample<DIM>(rng, L.max_move, A.zig_x, A.zig_f, dv);
+            u = uniform01(rng);
 #pragma unroll
-        for (int a = 0; a < DIM; ++a) x[a] = dadd(x[a], dv[a]);
-        wrap_inv<DIM>(g.L, g.invL, x);
+            for (int a = 0; a < DIM; ++a) x[a] = dadd(x[a], dv[a]);
+            wrap_inv<DIM>(g.L, g.invL, x);
+        }
         uint32_t mt[3];
-        if (!(point_to_space<DIM>(g, x, mt) && cell_index<DIM>(g, mt) == cell)) continue;
+        if (!(point_to_space<DIM>(g, x, mt) && cell_index<DIM>(g, mt) == cell)) {
+            if constexpr (INJ) {
+                if (lane == 0) {
+                    J.decisions[w] = 0;
+                    J.flags[w] = kTrialOutsideSpace;
+                }
+            }
+            continue;
+        }
         double t[3] = {x[0], x[1], DIM == 3 ? x[2] : 0.0};
         wrap_inv<DIM>(g.L, g.invL, t);
         grid_dependency_wait();  // the previous colour's moves are visible from here on
         allow_dependent_launch();
         const double4 s4 = ldg4(A.sorted_s + k);
         const double si[3] = {s4.x, s4.y, s4.z};
-        double e_new, e_old;
-        lj_energy64<DIM, true>(g, A, P, t, si, fs, k, true, lane, e_new, e_old);
+        double e_new, e_old, mag;
+        lj_energy64<DIM, true>(g, A, P, t, si, fs, k, true, lane, e_new, e_old, mag);
         const double du = dsub(e_new, e_old);
-        if ((du <= 0.0 || u < exp(ddiv(-du, L.kt))) && lane == 0) {
+        const double e0 = exp(ddiv(-du, L.kt));
+        const bool amb = order_ambiguous(du, mag, fs.total, u, L.kt, e0);
+        if constexpr (INJ) {
+            if (lane == 0) {
+                J.decisions[w] = du <= 0.0 || u < e0;
+                J.flags[w] = amb ? kTrialAmbiguous : 0;
+            }
+            continue;
+        }
+        if (amb && lane == 0) pst.ambiguous++;
+        if ((du <= 0.0 || u < e0) && lane == 0) {
             n_accepted++;
             double sv[3] = {t[0], t[1], t[2]};
             wrap_inv<DIM>(g.L, g.invL, sv);
@@ -281,8 +367,9 @@ constexpr uint32_t kRecheckChunks = 8;  // 32-candidate chunks per shared-memory
 // same butterfly; an empty slot adds +0, which leaves a sum that starts at +0 unchanged). A
 // lone warp walking the stencil in FP64 would otherwise set the duration of a pass whose
 // trials all run in one wave.
-template <int DIM>
-__global__ void __launch_bounds__(128, HMC_LJ_MIN_BLOCKS) k_sweep_lj32(Geometry g, Arrays A, Pair P, Launch L) {
+template <int DIM, bool INJ = false>
+__global__ void __launch_bounds__(128, HMC_LJ_MIN_BLOCKS) k_sweep_lj32(Geometry g, Arrays A, Pair P, Launch L,
+                                                                       Injected J) {
     if (L.early_wait) grid_dependency_wait();  // first pass: the rebuild's arrays are read at once
     __shared__ double s_e[kRecheckChunks][2][32];
     __shared__ SharedTrial s_trial;
@@ -290,7 +377,7 @@ __global__ void __launch_bounds__(128, HMC_LJ_MIN_BLOCKS) k_sweep_lj32(Geometry 
     const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
     uint32_t n_accepted = 0;
     PairStats pst;
-    if (threadIdx.x == 0) s_active = active_count(A, L.color, L.round);
+    if (threadIdx.x == 0) s_active = INJ ? J.n : active_count(A, L.color, L.round);
     __syncthreads();
     const uint32_t n_active = s_active;  // block-uniform: the loop below holds barriers
     for (uint32_t base = blockIdx.x * 4u; base < n_active; base += gridDim.x * 4u) {
@@ -301,7 +388,20 @@ __global__ void __launch_bounds__(128, HMC_LJ_MIN_BLOCKS) k_sweep_lj32(Geometry 
         double u = 0.0;
         bool trial = false;
         FlatStencil fs{0u, 0u, 0u, 0.f, 0.f};
-        if (w < n_active) {  // warp-uniform
+        bool outside = false;
+        if (INJ && w < n_active) {  // warp-uniform
+            double x[3];
+            lj_inject<DIM>(A, J, w, m, k, x, u);
+            const uint32_t cell = cell_index<DIM>(g, m);
+            fs = flat_stencil<DIM>(g, A.cell_start, m, lane);
+            uint32_t mt[3];
+            trial = point_to_space<DIM>(g, x, mt) && cell_index<DIM>(g, mt) == cell;
+            outside = !trial;
+            t[0] = x[0];
+            t[1] = x[1];
+            t[2] = x[2];
+            wrap_inv<DIM>(g.L, g.invL, t);
+        } else if (w < n_active) {  // warp-uniform
             unpack_m<DIM>(__ldg(A.color_cells + (size_t)L.color * g.color_stride + w), m);
             const uint32_t cell = cell_index<DIM>(g, m);
             fs = flat_stencil<DIM>(g, A.cell_start, m, lane);
@@ -337,6 +437,7 @@ __global__ void __launch_bounds__(128, HMC_LJ_MIN_BLOCKS) k_sweep_lj32(Geometry 
             d32 = s.e_new - s.e_old;
         }
         const bool unsure = decision < 0;
+        bool amb = false;
         if (__syncthreads_or(unsure)) {
             for (uint32_t o = 0; o < 4u; ++o) {
                 const bool mine = unsure && wib == o;
@@ -359,7 +460,7 @@ __global__ void __launch_bounds__(128, HMC_LJ_MIN_BLOCKS) k_sweep_lj32(Geometry 
                 if (!__syncthreads_or(mine)) continue;  // also publishes s_trial
                 const uint32_t total = s_trial.total, self = s_trial.self;
                 const uint32_t n_chunks = (total + 31u) / 32u;
-                double ea = 0.0, eb = 0.0;
+                double ea = 0.0, eb = 0.0, em = 0.0;
                 for (uint32_t c0 = 0; c0 < n_chunks; c0 += kRecheckChunks) {
                     const uint32_t c1 = min(c0 + kRecheckChunks, n_chunks);
                     for (uint32_t c = c0 + wib; c < c1; c += 4u) {
@@ -383,22 +484,33 @@ __global__ void __launch_bounds__(128, HMC_LJ_MIN_BLOCKS) k_sweep_lj32(Geometry 
                         for (uint32_t c = c0; c < c1; ++c) {
                             ea = dadd(ea, s_e[c - c0][0][lane]);
                             eb = dadd(eb, s_e[c - c0][1][lane]);
+                            em += fabs(s_e[c - c0][0][lane]) + fabs(s_e[c - c0][1][lane]);
                         }
                     }
                     __syncthreads();
                 }
                 if (wib == o) {
                     const double du = dsub(warp_sum(ea), warp_sum(eb));
+                    const double mag = warp_sum(em);
+                    const double e0 = exp(ddiv(-du, L.kt));
+                    amb = order_ambiguous(du, mag, total, u, L.kt, e0);
                     if (lane == 0) {
                         pst.rechecks++;
+                        pst.ambiguous += amb ? 1u : 0u;
                         const double err = fabs((double)d32 - du);
                         pst.max_err = err > pst.max_err ? err : pst.max_err;
                     }
-                    decision = (du <= 0.0 || u < exp(ddiv(-du, L.kt))) ? 1 : 0;
+                    decision = (du <= 0.0 || u < e0) ? 1 : 0;
                 }
             }
         }
-        if (decision == 1 && lane == 0) {
+        if constexpr (INJ) {
+            if (w < n_active && lane == 0) {
+                J.decisions[w] = decision == 1;
+                J.flags[w] = (outside ? kTrialOutsideSpace : 0) | (unsure ? kTrialRechecked : 0) |
+                             (amb ? kTrialAmbiguous : 0);
+            }
+        } else if (decision == 1 && lane == 0) {
             n_accepted++;
             double sv[3] = {t[0], t[1], t[2]};
             wrap_inv<DIM>(g.L, g.invL, sv);
@@ -457,10 +569,12 @@ __global__ void __launch_bounds__(128, HMC_LJ_BATCH_MIN_BLOCKS)
         allow_dependent_launch();
         const double4 s4 = ldg4(A.sorted_s + k);
         const double si[3] = {s4.x, s4.y, s4.z};
-        double e_new, e_old;
-        lj_energy64<DIM, true>(g, A, R.p, t, si, fs, k, true, lane, e_new, e_old);
+        double e_new, e_old, mag;
+        lj_energy64<DIM, true>(g, A, R.p, t, si, fs, k, true, lane, e_new, e_old, mag);
         const double du = dsub(e_new, e_old);
-        if ((du <= 0.0 || u < exp(ddiv(-du, R.kt))) && lane == 0) {
+        const double e0 = exp(ddiv(-du, R.kt));
+        if (lane == 0 && order_ambiguous(du, mag, fs.total, u, R.kt, e0)) pst.ambiguous++;
+        if ((du <= 0.0 || u < e0) && lane == 0) {
             n_accepted++;
             atomicAdd(B.accepted + r, 1ull);
             double sv[3] = {t[0], t[1], t[2]};
@@ -570,7 +684,7 @@ __global__ void __launch_bounds__(128, HMC_LJ_BATCH_MIN_BLOCKS)
                 const Replica& RO = B.rep[s_rep];
                 const uint32_t total = s_trial.total, self = s_trial.self;
                 const uint32_t n_chunks = (total + 31u) / 32u;
-                double ea = 0.0, eb = 0.0;
+                double ea = 0.0, eb = 0.0, em = 0.0;
                 for (uint32_t c0 = 0; c0 < n_chunks; c0 += kRecheckChunks) {
                     const uint32_t c1 = min(c0 + kRecheckChunks, n_chunks);
                     for (uint32_t c = c0 + wib; c < c1; c += 4u) {
@@ -594,18 +708,22 @@ __global__ void __launch_bounds__(128, HMC_LJ_BATCH_MIN_BLOCKS)
                         for (uint32_t c = c0; c < c1; ++c) {
                             ea = dadd(ea, s_e[c - c0][0][lane]);
                             eb = dadd(eb, s_e[c - c0][1][lane]);
+                            em += fabs(s_e[c - c0][0][lane]) + fabs(s_e[c - c0][1][lane]);
                         }
                     }
                     __syncthreads();
                 }
                 if (wib == o) {
                     const double du = dsub(warp_sum(ea), warp_sum(eb));
+                    const double mag = warp_sum(em);
+                    const double e0 = exp(ddiv(-du, RO.kt));
                     if (lane == 0) {
                         pst.rechecks++;
+                        pst.ambiguous += order_ambiguous(du, mag, total, u, RO.kt, e0) ? 1u : 0u;
                         const double err = fabs((double)d32 - du);
                         pst.max_err = err > pst.max_err ? err : pst.max_err;
                     }
-                    decision = (du <= 0.0 || u < exp(ddiv(-du, RO.kt))) ? 1 : 0;
+                    decision = (du <= 0.0 || u < e0) ? 1 : 0;
                 }
             }
         }
@@ -651,8 +769,9 @@ __global__ void __launch_bounds__(128) k_eval_lj(Geometry g, Arrays A, Pair P, c
             const FlatStencil ft = flat_stencil<DIM>(g, A.cell_start, mt, lane);
             const FlatStencil fi = flat_stencil<DIM>(g, A.cell_start, mi, lane);
             double e_new, e_old, unused;
-            lj_energy64<DIM, false>(g, A, P, t, nullptr, ft, k, true, lane, e_new, unused);
-            lj_energy64<DIM, false>(g, A, P, si, nullptr, fi, k, true, lane, e_old, unused);
+            double mag_new, mag_old;
+            lj_energy64<DIM, false>(g, A, P, t, nullptr, ft, k, true, lane, e_new, unused, mag_new);
+            lj_energy64<DIM, false>(g, A, P, si, nullptr, fi, k, true, lane, e_old, unused, mag_old);
             du = dsub(e_new, e_old);
             const double u = uu[i];
             bool dec64 = du <= 0.0 || u < exp(ddiv(-du, kt));
@@ -699,6 +818,56 @@ __global__ void __launch_bounds__(128) k_eval_lj(Geometry g, Arrays A, Pair P, c
     flush_stats(A.stats, pst, 0u);
 }
 
+// The sequential-stream tuner for Lennard-Jones and the overlap penalty (tune_stream_run):
+// dH = E_final - E_initial in FP64 (the warp over the stencils of the trial site's and of the
+// current site's spaces), then the reference's test: rejected at dH = inf, accepted at dH <= 0
+// without a uniform, else the stream's next uniform against exp(-dH / kT). A decision that
+// another summation order could change (order_ambiguous; also a dH <= 0 whose bound reaches
+// above 0, where another order would draw a uniform) is counted in J.ambiguous.
+template <int DIM>
+__global__ void __launch_bounds__(32) k_tune_stream_lj(TuneJob* jobs, uint32_t n_jobs) {
+    if (blockIdx.x >= n_jobs) return;
+    TuneJob& J = jobs[blockIdx.x];
+    const Geometry& g = J.g;
+    const Arrays& A = J.a;
+    const Pair& P = J.p;
+    const uint32_t lane = threadIdx.x & 31u;
+    unsigned long long ambiguous = 0;
+    tune_stream_run(
+        J, [&](Sfc64& rng, double m, uint32_t b, double* x, double*) { tune_translate<DIM>(rng, g, A, m, b, x); },
+        [&](Sfc64& rng, uint32_t b, const double* x, const double*) -> bool {
+            double t[3] = {x[0], x[1], x[2]};
+            wrap_inv<DIM>(g.L, g.invL, t);
+            const uint32_t k = A.slot_of_body[b];
+            const double4 s4 = ldg4(A.sorted_s + k);
+            const double si[3] = {s4.x, s4.y, s4.z};
+            uint32_t mt[3] = {0, 0, 0}, mi[3] = {0, 0, 0};
+            if (!(point_to_space<DIM>(g, t, mt) && point_to_space<DIM>(g, si, mi))) {
+                if (lane == 0) atomicOr(&A.stats->error_flags, kErrOutsideCheckerboard);
+                return false;
+            }
+            const FlatStencil ft = flat_stencil<DIM>(g, A.cell_start, mt, lane);
+            const FlatStencil fi = flat_stencil<DIM>(g, A.cell_start, mi, lane);
+            double e_new, e_old, unused, mag_new, mag_old;
+            lj_energy64<DIM, false>(g, A, P, t, nullptr, ft, k, true, lane, e_new, unused, mag_new);
+            if (e_new == __longlong_as_double(0x7ff0000000000000ll)) return false;  // the reference stops here
+            lj_energy64<DIM, false>(g, A, P, si, nullptr, fi, k, true, lane, e_old, unused, mag_old);
+            const double du = dsub(e_new, e_old);
+            if (!(du != __longlong_as_double(0x7ff0000000000000ll))) return false;
+            const uint32_t n = ft.total + fi.total;
+            const double mag = mag_new + mag_old;
+            if (du <= 0.0) {
+                if (isfinite(mag) && du + order_bound(du, mag, n) > 0.0) ambiguous++;
+                return true;
+            }
+            const double u = uniform01(rng);
+            const double e0 = exp(ddiv(-du, J.kt));
+            if (order_ambiguous(du, mag, n, u, J.kt, e0)) ambiguous++;
+            return u < e0;
+        });
+    if (lane == 0) J.ambiguous = ambiguous;
+}
+
 // Total pair energy, pairs (i < j) in FP64 (PairwiseCutoff::total_energy,
 // pairwise_cutoff.rs:720-745); one thread per body, atomically summed.
 template <int DIM>
@@ -743,10 +912,39 @@ cudaError_t launch_sweep_lj(int dim, bool fp32, const Geometry& g, const Arrays&
     if (blocks > (uint32_t)max_blocks) blocks = (uint32_t)max_blocks;
     PassLaunch pl(blocks, l.overlap_previous != 0 || l.early_wait != 0, s);
     if (dim == 2)
-        return fp32 ? cudaLaunchKernelEx(&pl.cfg, k_sweep_lj32<2>, g, a, p, l)
-                    : cudaLaunchKernelEx(&pl.cfg, k_sweep_lj<2>, g, a, p, l);
-    return fp32 ? cudaLaunchKernelEx(&pl.cfg, k_sweep_lj32<3>, g, a, p, l)
-                : cudaLaunchKernelEx(&pl.cfg, k_sweep_lj<3>, g, a, p, l);
+        return fp32 ? cudaLaunchKernelEx(&pl.cfg, k_sweep_lj32<2>, g, a, p, l, Injected{})
+                    : cudaLaunchKernelEx(&pl.cfg, k_sweep_lj<2>, g, a, p, l, Injected{});
+    return fp32 ? cudaLaunchKernelEx(&pl.cfg, k_sweep_lj32<3>, g, a, p, l, Injected{})
+                : cudaLaunchKernelEx(&pl.cfg, k_sweep_lj<3>, g, a, p, l, Injected{});
+}
+
+cudaError_t launch_tune_stream_lj(int dim, TuneJob* jobs, uint32_t n_jobs, cudaStream_t s) {
+    if (n_jobs == 0) return cudaSuccess;
+    if (dim == 2)
+        k_tune_stream_lj<2><<<n_jobs, 32, 0, s>>>(jobs, n_jobs);
+    else
+        k_tune_stream_lj<3><<<n_jobs, 32, 0, s>>>(jobs, n_jobs);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_trials_lj(int dim, bool fp32, const Geometry& g, const Arrays& a, const Pair& p, double kt,
+                             const Injected& j, cudaStream_t s) {
+    if (j.n == 0) return cudaSuccess;
+    Launch l{};
+    l.kt = kt;
+    const uint32_t blocks = (j.n + 3) / 4;  // four warps (trials) per block
+    if (dim == 2) {
+        if (fp32)
+            k_sweep_lj32<2, true><<<blocks, 128, 0, s>>>(g, a, p, l, j);
+        else
+            k_sweep_lj<2, true><<<blocks, 128, 0, s>>>(g, a, p, l, j);
+    } else {
+        if (fp32)
+            k_sweep_lj32<3, true><<<blocks, 128, 0, s>>>(g, a, p, l, j);
+        else
+            k_sweep_lj<3, true><<<blocks, 128, 0, s>>>(g, a, p, l, j);
+    }
+    return cudaGetLastError();
 }
 
 cudaError_t launch_sweep_batch_lj(int dim, bool fp32, const Batch& b, const Arrays& a, uint32_t color, uint32_t round,

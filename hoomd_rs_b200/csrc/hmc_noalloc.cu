@@ -18,12 +18,17 @@
 //
 // In host code the array's name is only a host-side handle, not a device address. The
 // device address comes from cudaGetSymbolAddress, taken once per device with that device
-// current, on the first call that runs on it. Make that first call before capturing any
-// stream into a CUDA graph.
+// current, on the first call that runs on it. CUDA loads a library's device code lazily by
+// default (unless CUDA_MODULE_LOADING=EAGER), so that first call is also the one that creates
+// the array on the device: it grows the device footprint once. A caller that must not grow it
+// later makes one call at start-up (n_bodies = 0 is enough), before capturing any stream into a
+// CUDA graph. The address is kept together with the identity of the device's context; after a
+// cudaDeviceReset the context is a new one and the next call looks the address up again.
 #include <cuda_runtime.h>
 
 #include <cmath>
 #include <mutex>
+#include <utility>
 
 #include "../../include/hmc.h"
 #include "hmc_math.cuh"
@@ -234,8 +239,37 @@ __global__ void k_na_count(NaGeom g, NaPtrs p, uint32_t n, unsigned long long* o
 std::mutex g_setup_mutex;
 constexpr int kMaxDevices = 64;
 unsigned char* g_scratch_ptr[kMaxDevices] = {nullptr};
+unsigned long long g_scratch_ctx[kMaxDevices] = {0};  // context the address belongs to (0: unknown)
 
 hmc_status na_fail(hmc_status st, const char*) { return st; }
+
+// The unique id of the calling thread's current context (cuCtxGetId through the runtime's
+// driver entry point; ids are never reused within a process), or 0 when it cannot be read.
+unsigned long long current_context_id() {
+    using CtxGetId = int (*)(void*, unsigned long long*);
+    static const CtxGetId fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &f, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            f = nullptr;
+        return reinterpret_cast<CtxGetId>(f);
+    }();
+    unsigned long long id = 0;
+    if (!fn || fn(nullptr, &id) != 0) return 0;
+    return id;
+}
+
+// One launch; its own status (no reliance on the thread's last-error state, which may hold an
+// unrelated earlier error).
+template <typename... K, typename... A>
+cudaError_t launch(void (*kernel)(K...), uint32_t grid, uint32_t block, cudaStream_t s, A&&... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.stream = s;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...);
+}
 
 }  // namespace
 
@@ -286,31 +320,28 @@ extern "C" hmc_status hmc_overlap_count_noalloc(const double* positions, uint64_
     unsigned char* base = nullptr;
     {
         std::lock_guard<std::mutex> lock(g_setup_mutex);
-        if (!g_scratch_ptr[device]) {
+        const unsigned long long ctx = current_context_id();
+        if (!g_scratch_ptr[device] || ctx == 0 || ctx != g_scratch_ctx[device]) {
+            // first call on this device, or its context was reset: (re)load the address
             void* ptr = nullptr;
             cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
             if (e != cudaSuccess || !ptr) return na_fail(HMC_CUDA_ERROR, "cudaGetSymbolAddress failed");
             g_scratch_ptr[device] = static_cast<unsigned char*>(ptr);
+            g_scratch_ctx[device] = current_context_id();
         }
         base = g_scratch_ptr[device];
     }
     NaPtrs p = carve(base);
     cudaStream_t s = (cudaStream_t)cuda_stream;
     const uint32_t n = (uint32_t)n_bodies;
-    k_na_zero<<<(g.n_cells + 255) / 256, 256, 0, s>>>(p, g.n_cells, overlaps);
-    if (n > 0) {
-        if (dim == 2)
-            k_na_bin<2><<<(n + 255) / 256, 256, 0, s>>>(g, p, positions, n);
-        else
-            k_na_bin<3><<<(n + 255) / 256, 256, 0, s>>>(g, p, positions, n);
-    }
-    k_na_scan<<<1, kScanThreadsNA, 0, s>>>(p, g.n_cells);
-    if (n > 0) {
-        k_na_scatter<<<(n + 255) / 256, 256, 0, s>>>(p, n);
-        if (dim == 2)
-            k_na_count<2><<<(n + 127) / 128, 128, 0, s>>>(g, p, n, overlaps);
-        else
-            k_na_count<3><<<(n + 127) / 128, 128, 0, s>>>(g, p, n, overlaps);
-    }
-    return cudaGetLastError() == cudaSuccess ? HMC_OK : na_fail(HMC_CUDA_ERROR, "kernel launch failed");
+    cudaError_t e = launch(k_na_zero, (g.n_cells + 255) / 256, 256, s, p, g.n_cells, overlaps);
+    if (e == cudaSuccess && n > 0)
+        e = dim == 2 ? launch(k_na_bin<2>, (n + 255) / 256, 256, s, g, p, positions, n)
+                     : launch(k_na_bin<3>, (n + 255) / 256, 256, s, g, p, positions, n);
+    if (e == cudaSuccess) e = launch(k_na_scan, 1, kScanThreadsNA, s, p, g.n_cells);
+    if (e == cudaSuccess && n > 0) e = launch(k_na_scatter, (n + 255) / 256, 256, s, p, n);
+    if (e == cudaSuccess && n > 0)
+        e = dim == 2 ? launch(k_na_count<2>, (n + 127) / 128, 128, s, g, p, n, overlaps)
+                     : launch(k_na_count<3>, (n + 127) / 128, 128, s, g, p, n, overlaps);
+    return e == cudaSuccess ? HMC_OK : na_fail(HMC_CUDA_ERROR, "kernel launch failed");
 }

@@ -327,9 +327,11 @@ __device__ __forceinline__ void drain_pairs(const Geometry& g, const Arrays& A, 
     __syncwarp();
 }
 
-template <bool FP32, int G>
+// INJ: the probe mode (Injected): group trial w is injected trial w, walked around the space of
+// its W1, and its decision is written instead of committed.
+template <bool FP32, int G, bool INJ = false>
 __global__ void __launch_bounds__(128, HMC_POLY_MIN_BLOCKS)
-    k_sweep_poly3_packed(Geometry g, Arrays A, PolyShape sh, Launch L, uint32_t rotate) {
+    k_sweep_poly3_packed(Geometry g, Arrays A, PolyShape sh, Launch L, uint32_t rotate, Injected J) {
     static_assert(G == 2 || G == 4 || G == 8, "G trials per warp");
     constexpr uint32_t S = 32 / G;  // lanes per trial
     if (L.early_wait) grid_dependency_wait();  // first pass: the rebuild's arrays are read at once
@@ -343,7 +345,7 @@ __global__ void __launch_bounds__(128, HMC_POLY_MIN_BLOCKS)
     uint32_t n_accepted = 0;
     PairStats st;
     const uint32_t sf = g.shape[2];
-    const uint32_t n_active = active_count(A, L.color, L.round);
+    const uint32_t n_active = INJ ? J.n : active_count(A, L.color, L.round);
     for (uint32_t w0 = warp * G; w0 < n_active; w0 += n_warps * G) {  // warp-uniform
         const uint32_t w = w0 + grp;
         uint32_t m[3] = {0, 0, 0};
@@ -351,7 +353,24 @@ __global__ void __launch_bounds__(128, HMC_POLY_MIN_BLOCKS)
         bool valid = false;
         double t[3] = {0.0, 0.0, 0.0};
         Q qi{1.0, 0.0, 0.0, 0.0};
-        if (w < n_active) {  // the group's trial, computed by its S lanes alike
+        uint8_t flag = 0;
+        if (INJ && w < n_active) {  // the injected trial (W1, versor), by the group's S lanes alike
+            const uint64_t body = J.bodies[w];
+            k = A.slot_of_body[body];
+            const double4 w4 = J.trial[w];
+            const double x[3] = {w4.x, w4.y, w4.z};
+            const double4 q4 = J.trial_q[w];
+            qi = Q{q4.x, q4.y, q4.z, q4.w};
+            valid = point_to_space<3>(g, x, m);
+            if (!valid)
+                atomicOr(&A.stats->error_flags, kErrOutsideCheckerboard);
+            else if (cell_index<3>(g, m) != A.body_cell[body])
+                flag |= kTrialOutsideSpace;
+            t[0] = x[0];
+            t[1] = x[1];
+            t[2] = x[2];
+            wrap_inv<3>(g.L, g.invL, t);
+        } else if (w < n_active) {  // the group's trial, computed by its S lanes alike
             unpack_m<3>(__ldg(A.color_cells + (size_t)L.color * g.color_stride + w), m);
             const uint32_t cell = cell_index<3>(g, m);
             const uint32_t start = __ldg(A.cell_start + cell);
@@ -436,7 +455,12 @@ __global__ void __launch_bounds__(128, HMC_POLY_MIN_BLOCKS)
             }
         }
         drain_pairs<G>(g, A, sh, s_trial[wib], s_pair_q[wib], s_pair_g[wib], n_pairs, lane, mask);
-        if (sub == 0 && valid && !((mask >> grp) & 1u)) {
+        if constexpr (INJ) {
+            if (sub == 0 && w < n_active) {
+                J.decisions[w] = valid && !((mask >> grp) & 1u);
+                J.flags[w] = flag;
+            }
+        } else if (sub == 0 && valid && !((mask >> grp) & 1u)) {
             n_accepted++;
             double sv[3] = {t[0], t[1], t[2]};
             wrap_inv<3>(g.L, g.invL, sv);
@@ -549,7 +573,59 @@ __global__ void k_tune_moves(Geometry g, Arrays A, Launch L, uint32_t tune_step,
     uu[j] = uniform01(rng);
 }
 
+// The sequential-stream tuner for hard convex polyhedra (tune_stream_run): Translate or
+// Rotate<Versor> proposals, the trial accepted when XenoCollide finds no overlap with any
+// candidate of the stencil around its site's space (FP64, the warp 32 candidates at a time).
+__global__ void __launch_bounds__(32) k_tune_stream_poly3(TuneJob* jobs, uint32_t n_jobs, PolyShape sh) {
+    if (blockIdx.x >= n_jobs) return;
+    TuneJob& J = jobs[blockIdx.x];
+    const Geometry& g = J.g;
+    const Arrays& A = J.a;
+    const uint32_t lane = threadIdx.x & 31u;
+    PairStats st;
+    tune_stream_run(
+        J,
+        [&](Sfc64& rng, double m, uint32_t b, double* x, double* q) {
+            const double4 q4 = A.body_ori[b];
+            Q qi{q4.x, q4.y, q4.z, q4.w};
+            if (J.rotate) {
+                const double4 b4 = A.body_pos[b];
+                x[0] = b4.x;
+                x[1] = b4.y;
+                x[2] = b4.z;
+                qi = versor_move(rng, m, A.zig_x, A.zig_f, qi);
+                wrap_inv<3>(g.L, g.invL, x);
+            } else {
+                tune_translate<3>(rng, g, A, m, b, x);
+            }
+            q[0] = qi.s;
+            q[1] = qi.x;
+            q[2] = qi.y;
+            q[3] = qi.z;
+        },
+        [&](Sfc64&, uint32_t b, const double* x, const double* q) -> bool {
+            double t[3] = {x[0], x[1], x[2]};
+            wrap_inv<3>(g.L, g.invL, t);
+            uint32_t m[3] = {0, 0, 0};
+            if (!point_to_space<3>(g, t, m)) {
+                if (lane == 0) atomicOr(&A.stats->error_flags, kErrOutsideCheckerboard);
+                return false;
+            }
+            const FlatStencil fs = flat_stencil<3>(g, A.cell_start, m, lane);
+            const Q qi{q[0], q[1], q[2], q[3]};
+            return !poly_overlaps<false>(g, A, sh, t, qi, make_float4(0.f, 0.f, 0.f, 0.f), (int)m[2], fs,
+                                         A.slot_of_body[b], lane, st);
+        });
+}
+
 }  // namespace
+
+cudaError_t launch_tune_stream_poly(TuneJob* jobs, uint32_t n_jobs, const double4* verts, uint32_t nv, double rcut2,
+                                    cudaStream_t s) {
+    if (n_jobs == 0) return cudaSuccess;
+    k_tune_stream_poly3<<<n_jobs, 32, 0, s>>>(jobs, n_jobs, PolyShape{verts, nv, rcut2, 0.f});
+    return cudaGetLastError();
+}
 
 cudaError_t launch_sweep_poly(bool fp32, const Geometry& g, const Arrays& a, const double4* verts, uint32_t nv,
                               double rcut2, float rcut2_hi32, const Launch& l, bool rotate, cudaStream_t s) {
@@ -567,8 +643,24 @@ cudaError_t launch_sweep_poly(bool fp32, const Geometry& g, const Arrays& a, con
     if (blocks > (uint32_t)max_blocks) blocks = (uint32_t)max_blocks;
     PassLaunch pl(blocks, l.overlap_previous != 0 || l.early_wait != 0, s);
     const uint32_t rot = rotate ? 1u : 0u;
-    return fp32 ? cudaLaunchKernelEx(&pl.cfg, k_sweep_poly3_packed<true, kPolyTrialsPerWarp>, g, a, sh, l, rot)
-                : cudaLaunchKernelEx(&pl.cfg, k_sweep_poly3_packed<false, kPolyTrialsPerWarp>, g, a, sh, l, rot);
+    return fp32 ? cudaLaunchKernelEx(&pl.cfg, k_sweep_poly3_packed<true, kPolyTrialsPerWarp>, g, a, sh, l, rot,
+                                     Injected{})
+                : cudaLaunchKernelEx(&pl.cfg, k_sweep_poly3_packed<false, kPolyTrialsPerWarp>, g, a, sh, l, rot,
+                                     Injected{});
+}
+
+cudaError_t launch_trials_poly(bool fp32, const Geometry& g, const Arrays& a, const double4* verts, uint32_t nv,
+                               double rcut2, float rcut2_hi32, const Injected& j, cudaStream_t s) {
+    if (j.n == 0) return cudaSuccess;
+    PolyShape sh{verts, nv, rcut2, rcut2_hi32};
+    const Launch l{};
+    const uint32_t per_block = 4u * kPolyTrialsPerWarp;  // four warps per block
+    const uint32_t blocks = (j.n + per_block - 1) / per_block;
+    if (fp32)
+        k_sweep_poly3_packed<true, kPolyTrialsPerWarp, true><<<blocks, 128, 0, s>>>(g, a, sh, l, 0u, j);
+    else
+        k_sweep_poly3_packed<false, kPolyTrialsPerWarp, true><<<blocks, 128, 0, s>>>(g, a, sh, l, 0u, j);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_eval_poly(bool fp32, const Geometry& g, const Arrays& a, const double4* verts, uint32_t nv,

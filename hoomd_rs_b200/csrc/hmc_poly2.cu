@@ -416,6 +416,49 @@ __global__ void __launch_bounds__(128) k_eval_poly2(Geometry g, Arrays A, PolySh
     flush_stats(A.stats, st, 0u);
 }
 
+// The sequential-stream tuner for hard convex polygons (tune_stream_run): Translate or
+// Rotate<Angle> (theta += Uniform(-a, a): 52 random bits in [1, 2) minus one, times the range,
+// plus the low end; rotate/angle.rs:46-55) proposals, the trial accepted when no candidate of the
+// stencil around its site's space overlaps it (FP64 XenoCollide or separating axes).
+template <bool SAT>
+__global__ void __launch_bounds__(32) k_tune_stream_poly2(TuneJob* jobs, uint32_t n_jobs, PolyShape2 sh) {
+    if (blockIdx.x >= n_jobs) return;
+    TuneJob& J = jobs[blockIdx.x];
+    const Geometry& g = J.g;
+    const Arrays& A = J.a;
+    const uint32_t lane = threadIdx.x & 31u;
+    PairStats st;
+    bool range_error = false;
+    tune_stream_run(
+        J,
+        [&](Sfc64& rng, double m, uint32_t b, double* x, double* q) {
+            q[0] = A.body_ori[b].x;
+            if (J.rotate) {
+                const double4 b4 = A.body_pos[b];
+                x[0] = b4.x;
+                x[1] = b4.y;
+                const double u = dsub(as_double(0x3FF0000000000000ULL | (rng.next_u64() >> 12)), 1.0);
+                q[0] = dadd(q[0], dadd(dmul(u, dsub(m, -m)), -m));
+                wrap_inv<2>(g.L, g.invL, x);
+            } else {
+                tune_translate<2>(rng, g, A, m, b, x);
+            }
+        },
+        [&](Sfc64&, uint32_t b, const double* x, const double* q) -> bool {
+            double t[3] = {x[0], x[1], 0.0};
+            wrap_inv<2>(g.L, g.invL, t);
+            uint32_t m[3] = {0, 0, 0};
+            if (!point_to_space<2>(g, t, m)) {
+                if (lane == 0) atomicOr(&A.stats->error_flags, kErrOutsideCheckerboard);
+                return false;
+            }
+            const FlatStencil fs = flat_stencil<2>(g, A.cell_start, m, lane);
+            return !poly2_overlaps<false, SAT>(g, A, sh, t, q[0], make_float4(0.f, 0.f, 0.f, 0.f), (int)m[1], fs,
+                                               A.slot_of_body[b], lane, st, &range_error);
+        });
+    if (range_error) atomicOr(&J.a.stats->error_flags, kErrAngleRange);
+}
+
 // Overlapping pairs (i < j), FP64 (the overlap check of total_energy).
 template <bool SAT>
 __global__ void k_overlap_poly2(Geometry g, Arrays A, PolyShape2 sh, uint32_t n) {
@@ -481,6 +524,17 @@ cudaError_t launch_sweep_poly2(bool fp32, bool sat, const Geometry& g, const Arr
                    : cudaLaunchKernelEx(&pl.cfg, k_sweep_poly2<true, false>, g, a, sh, l, rot);
     return sat ? cudaLaunchKernelEx(&pl.cfg, k_sweep_poly2<false, true>, g, a, sh, l, rot)
                : cudaLaunchKernelEx(&pl.cfg, k_sweep_poly2<false, false>, g, a, sh, l, rot);
+}
+
+cudaError_t launch_tune_stream_poly2(bool sat, TuneJob* jobs, uint32_t n_jobs, const double4* verts, uint32_t nv,
+                                     double rcut2, cudaStream_t s) {
+    if (n_jobs == 0) return cudaSuccess;
+    const PolyShape2 sh{verts, nv, rcut2, 0.f};
+    if (sat)
+        k_tune_stream_poly2<true><<<n_jobs, 32, 0, s>>>(jobs, n_jobs, sh);
+    else
+        k_tune_stream_poly2<false><<<n_jobs, 32, 0, s>>>(jobs, n_jobs, sh);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_eval_poly2(bool fp32, bool sat, const Geometry& g, const Arrays& a, const double4* verts,

@@ -42,7 +42,7 @@
 extern "C" {
 #endif
 
-#define HMC_ABI_VERSION 1u
+#define HMC_ABI_VERSION 2u  /* 2: hmc_count gained order_ambiguous */
 
 typedef enum hmc_status {
     HMC_OK = 0,
@@ -125,8 +125,17 @@ typedef struct hmc_sweep_params {
     uint32_t precision;       /* hmc_precision */
     uint32_t n_sweeps;        /* number of ParallelSweep::apply calls */
     uint32_t increment_step;  /* 1: Microstate::increment_step() after every apply */
-    uint32_t reserved;
+    uint32_t flags;           /* hmc_tune / hmc_batch_tune: HMC_TUNE_* bits; 0 otherwise */
 } hmc_sweep_params;
+
+/* hmc_sweep_params.flags for hmc_tune and hmc_batch_tune. By default the tuner is
+ * tune_local_trial as the reference runs it (hoomd-mc/src/tune_local.rs:42-88): every sample of
+ * every round from the one stream Counter(step, substep, seed).make_rng(), in order, on one warp
+ * (one warp per replica for a batch), so the tuned maximum equals the reference's for the same
+ * state. HMC_TUNE_PER_SAMPLE_STREAMS instead gives sample j of round t its own stream
+ * Counter(step, substep, seed).index(2^63 | t << 32 | j) and evaluates a round's samples in
+ * parallel: the same distribution, much faster, but not the reference's numbers. */
+#define HMC_TUNE_PER_SAMPLE_STREAMS 1u
 
 typedef struct hmc_count {
     uint64_t accepted;
@@ -134,6 +143,10 @@ typedef struct hmc_count {
     uint64_t rechecks;       /* FP32 pair results re-evaluated in FP64 */
     uint64_t pair_checks;    /* pair evaluations in the FP32 path */
     double max_fp32_error;   /* largest |FP32 - FP64| over rechecked pair quantities */
+    uint64_t order_ambiguous; /* Lennard-Jones and overlap-penalty trials whose FP64 dU lies so close
+                                 to the Metropolis threshold that summing the same pair energies in
+                                 another order (the reference's cell-list order) could change the
+                                 decision; 0 proves every decision equal to any order's */
 } hmc_count;
 
 /* One injected trial move for hmc_eval_moves. */
@@ -198,6 +211,21 @@ hmc_status hmc_overlap_check(hmc_system* sys, uint64_t* n_overlaps);
  * fall back to FP64 for it; delta_h[i] (may be NULL) = delta_energy_one in FP64. */
 hmc_status hmc_eval_moves(hmc_system* sys, const hmc_injected_move* moves, uint64_t n, double temperature,
                           uint32_t precision, uint8_t* decisions, uint8_t* rechecked, double* delta_h);
+/* The colour pass's own decision for injected trial moves: the kernel that hmc_sweep runs for
+ * the system's interaction and `precision` (hard spheres: the per-lane FP32 pass or the
+ * warp-cooperative FP64 pass; Lennard-Jones and the overlap penalty: the warp-per-trial passes;
+ * convex polyhedra: the packed pass) takes each move in place of a drawn trial
+ * (generate_trial_moves, parallel_sweep.rs:231-278) and writes its decision instead of
+ * committing it; the state does not change. The checkerboard is the one the next hmc_sweep lays
+ * out (update_checkerboard, parallel_sweep.rs:176-201: origin from the system's counter).
+ * decisions[i] = 1 when the pass accepts move i. flags[i] (may be NULL): bit 0 = the FP32 pass
+ * settled the move with FP64 pair evaluations; bit 1 = the move's position lies outside its
+ * body's checkerboard space, which the colour pass rejects before any pair test
+ * (parallel_sweep.rs:253-258). Lennard-Jones and penalty moves with bit 1 are not evaluated
+ * (decision 0); for hard shapes the decision is still the pair walk's around the position's own
+ * space. Convex polygons: HMC_NOT_SUPPORTED. */
+hmc_status hmc_eval_trials(hmc_system* sys, const hmc_injected_move* moves, uint64_t n, double temperature,
+                           uint32_t precision, uint8_t* decisions, uint8_t* flags);
 /* PairwiseCutoff::total_energy (pairwise_cutoff.rs:720-745): the pair energy sum in FP64 for
  * Lennard-Jones and the overlap penalty (summed with atomics: the last bits depend on the
  * order); +infinity or 0 for hard shapes (any overlap / none). */
@@ -222,8 +250,13 @@ hmc_status hmc_total_energy(hmc_system* sys, double* energy);
  * every GPU that loads the library until the process exits), so n_bodies is limited to
  * HMC_NOALLOC_MAX_BODIES (HMC_INVALID_ARGUMENT beyond). The first call on a device looks
  * up that array's device address (cudaGetSymbolAddress) with the device current; make it
- * before capturing any stream into a CUDA graph. All calls share the array: calls that
- * overlap in time on the GPU race with each other. Errors are reported by status only. */
+ * before capturing any stream into a CUDA graph. CUDA loads device code lazily by default
+ * (unless CUDA_MODULE_LOADING=EAGER), so that first call is also what creates the array on
+ * the device: the footprint grows once, then never again. A caller that must not grow it
+ * later makes one call at start-up (n_bodies = 0 is enough). The address is looked up again
+ * when the device's context changes (after cudaDeviceReset). All calls share the array:
+ * calls that overlap in time on the GPU (two streams, two threads) race with each other and
+ * give wrong counts, so serialise them. Errors are reported by status only. */
 #define HMC_NOALLOC_MAX_BODIES 65536u
 #define HMC_NOALLOC_MAX_CELLS 65536u
 hmc_status hmc_overlap_count_noalloc(const double* positions, uint64_t n_bodies, uint32_t dim,

@@ -115,6 +115,9 @@ def lib():
         L.oracle_serial_sweep.restype = C.c_int
         L.oracle_tune.argtypes = [C.c_void_p, C.c_uint32, C.c_double, C.c_double, C.c_double, C.c_uint32, C.c_uint32]
         L.oracle_tune.restype = C.c_double
+        L.oracle_tune_stream.argtypes = [C.c_void_p, C.c_uint32, C.c_double, C.c_double, C.c_double, C.c_uint32,
+                                         C.c_uint32]
+        L.oracle_tune_stream.restype = C.c_double
         L.oracle_sdf.argtypes = [C.c_void_p, C.c_double, C.c_uint32, _u64p]
         L.oracle_gr.argtypes = [C.c_void_p, C.c_double, C.c_uint32, _u64p]
         L.oracle_overlap_count.argtypes = [C.c_void_p]
@@ -307,6 +310,7 @@ class System:
                  lj_r_cut=2.5, lj_r_shift=2.5, boundary_range=None, penalty=(10000.0, 0.2, 100.0)):
         self.dim = dim
         self.L = _f64(edge_lengths)
+        self.seed = seed
         pos = _f64(positions, (-1,))
         self.n = pos.size // dim
         self.interaction = interaction
@@ -419,7 +423,12 @@ class System:
         return a.value, r.value
 
     def tune(self, move, maximum, kt, target, samples, steps) -> float:
+        """The per-sample-stream tuner (each sample its own Counter index)."""
         return float(lib().oracle_tune(self._h, move, maximum, kt, target, samples, steps))
+
+    def tune_stream(self, move, maximum, kt, target, samples, steps) -> float:
+        """tune_local_trial with the reference's one sequential stream."""
+        return float(lib().oracle_tune_stream(self._h, move, maximum, kt, target, samples, steps))
 
     def sdf(self, x_max, n_bins) -> np.ndarray:
         out = np.zeros(n_bins, dtype=np.uint64)

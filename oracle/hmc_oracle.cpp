@@ -1842,6 +1842,35 @@ double oracle_tune(const oracle_system* s, uint32_t move, double maximum, double
     return maximum;
 }
 
+// tune_local_trial (hoomd-mc/src/tune_local.rs:42-88) as the reference runs it: one stream
+// Counter(step, substep, seed).make_rng() (index 0) for every sample of every step, in order:
+// random_range(0..n) for the body, propose, wrap, delta_energy_one, and the uniform only when
+// 0 < dH < infinity. Each step scales the maximum by (a + 1.5) / (t + 1.5) (tune_by_scaling,
+// lib.rs:514-524); Rotate<Versor> clamps it at pi/2 (rotate/versor.rs:128-135), Rotate<Angle>
+// at pi (rotate/angle.rs:62-68), Translate not at all (translate.rs:90-92).
+double oracle_tune_stream(const oracle_system* s, uint32_t move, double maximum, double kt, double target,
+                          uint32_t samples, uint32_t steps) {
+    const int ol = s->ori_len();
+    Sfc64 rng = make_rng(s->step, s->substep, s->seed, 0);
+    const double pi = 3.141592653589793;
+    const double cap = move == ORACLE_TRANSLATE ? 0.0 : (s->dim == 3 ? pi / 2.0 : pi);
+    for (uint32_t t = 0; t < steps; ++t) {
+        uint64_t acc = 0;
+        for (uint32_t j = 0; j < samples; ++j) {
+            uint64_t b = canon_range_u32(rng, (uint32_t)s->n);
+            double pos[3] = {0, 0, 0}, ori[4] = {0, 0, 0, 0};
+            s->propose(rng, (int)move, maximum, b, pos, ori);
+            wrap(s->dim, s->L, pos);
+            double dh = s->delta_energy_one(b, pos, ol ? ori : nullptr);
+            if (dh != INFINITY && (dh <= 0.0 || uniform01(rng) < std::exp(-dh / kt))) acc += 1;
+        }
+        double ratio = (double)acc / (double)samples;
+        maximum *= (ratio + 1.5) / (target + 1.5);
+        if (cap > 0.0 && maximum > cap) maximum = cap;
+    }
+    return maximum;
+}
+
 // Pair histograms by minimum-image distance (no reference counterpart: the equilibrium
 // estimators of the device library, restated here as their checker). Pairs i < j; per axis
 // d = t - s - L rint((t - s)/L); SDF bins x = 1 - sigma/r in [0, x_max), g(r) bins r in
@@ -1923,19 +1952,36 @@ double oracle_delta_energy_one(const oracle_system* s, uint64_t b, const double*
     double p[3] = {position[0], position[1], s->dim == 3 ? position[2] : 0.0};
     return s->delta_energy_one(b, p, orientation);
 }
+// Each move is independent of the others (the state is read only), so the moves are split over
+// the host's threads; the results do not depend on the split.
 void oracle_eval_moves(const oracle_system* s, uint64_t n, const uint64_t* bodies, const double* positions,
                        const double* orientations, const double* u, double kt, uint8_t* decisions,
                        double* delta_h) {
-    int ol = s->ori_len();
-    for (uint64_t k = 0; k < n; ++k) {
-        double p[3] = {0, 0, 0};
-        for (int a = 0; a < s->dim; ++a) p[a] = positions[k * s->dim + a];
-        const double* o = ol ? orientations + (size_t)ol * k : nullptr;
-        double dh = s->delta_energy_one(bodies[k], p, o);
-        delta_h[k] = dh;
-        bool ok = dh != INFINITY && (dh <= 0.0 || u[k] < std::exp(-dh / kt));
-        decisions[k] = ok ? 1 : 0;
+    const int ol = s->ori_len();
+    auto run = [&](uint64_t lo, uint64_t hi) {
+        for (uint64_t k = lo; k < hi; ++k) {
+            double p[3] = {0, 0, 0};
+            for (int a = 0; a < s->dim; ++a) p[a] = positions[k * s->dim + a];
+            const double* o = ol ? orientations + (size_t)ol * k : nullptr;
+            double dh = s->delta_energy_one(bodies[k], p, o);
+            delta_h[k] = dh;
+            bool ok = dh != INFINITY && (dh <= 0.0 || u[k] < std::exp(-dh / kt));
+            decisions[k] = ok ? 1 : 0;
+        }
+    };
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const uint64_t threads = n < 4096 ? 1 : std::min<uint64_t>(hw, (n + 4095) / 4096);
+    if (threads == 1) {
+        run(0, n);
+        return;
     }
+    std::vector<std::thread> pool;
+    const uint64_t chunk = (n + threads - 1) / threads;
+    for (uint64_t w = 0; w < threads; ++w) {
+        const uint64_t lo = std::min(n, w * chunk), hi = std::min(n, lo + chunk);
+        pool.emplace_back(run, lo, hi);
+    }
+    for (auto& th : pool) th.join();
 }
 
 }  // extern "C"

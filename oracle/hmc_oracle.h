@@ -137,6 +137,9 @@ int oracle_serial_sweep_filter(oracle_system* s, uint32_t move, double maximum, 
 // Move-size tuning (tune_local.rs:21-89) with per-sample counter streams; returns the tuned size.
 double oracle_tune(const oracle_system* s, uint32_t move, double maximum, double kt, double target, uint32_t samples,
                    uint32_t steps);
+/* tune_local_trial with the reference's single sequential stream (tune_local.rs:42-88). */
+double oracle_tune_stream(const oracle_system* s, uint32_t move, double maximum, double kt, double target,
+                          uint32_t samples, uint32_t steps);
 // Pair histograms (i < j) by minimum-image distance: scale distribution x = 1 - sigma/r over
 // [0, x_max) and g(r) over [0, r_max); brute force over all pairs (small systems).
 void oracle_sdf(const oracle_system* s, double x_max, uint32_t n_bins, uint64_t* counts);

@@ -2,7 +2,7 @@
 
 Run in a checkout that holds the reference sources (glotzerlab/hoomd-rs v1.4.0):
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <path of the reference checkout>
 
 The reference is Rust and cannot be built here, so its unit tests are read as
 text: every literal that a test on the hot path asserts (SFC64 outputs, checkerboard
@@ -295,4 +295,6 @@ def main(root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <path of the reference checkout>")
+    main(sys.argv[1])

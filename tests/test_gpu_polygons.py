@@ -131,7 +131,7 @@ def test_planted_polygon_overlap_and_tune(ctx, kind):
     assert g.overlap_count() == o.overlap_count() == 1
     g2, o2, _, _ = systems(ctx, kind, SQUARE, 900, 1.02, seed=21)
     for move, om in ((TRANSLATE, oracle.TRANSLATE), (ROTATE, oracle.ROTATE)):
-        assert g2.tune(move, 0.1, 1.0, FP32_RECHECK, 0.3, 2000, 6) == o2.tune(om, 0.1, 1.0, 0.3, 2000, 6)
+        assert g2.tune(move, 0.1, 1.0, FP32_RECHECK, 0.3, 2000, 6) == o2.tune_stream(om, 0.1, 1.0, 0.3, 2000, 6)
 
 
 def test_polygon_input_validation(ctx):
