@@ -73,6 +73,11 @@ class hmc_count(C.Structure):
                 ("pair_checks", C.c_uint64), ("max_fp32_error", C.c_double), ("order_ambiguous", C.c_uint64)]
 
 
+class hmc_launch_variant(C.Structure):
+    _fields_ = [("index", C.c_uint32), ("count", C.c_uint32), ("blocks_per_sm", C.c_uint32),
+                ("trials_per_warp", C.c_uint32), ("own_steps", C.c_uint32)]
+
+
 class hmc_injected_move(C.Structure):
     _fields_ = [("body", C.c_uint64), ("position", C.c_double * 3), ("orientation", C.c_double * 4),
                 ("u", C.c_double)]
@@ -155,6 +160,14 @@ SIGNATURES = {
                                  _u8p, _dp]),
     "hmc_eval_trials": (C.c_int, [_vp, C.POINTER(hmc_injected_move), C.c_uint64, C.c_double, C.c_uint32, _u8p,
                                   _u8p]),
+    "hmc_sample_moves": (C.c_int, [_vp, C.c_uint32, C.c_uint32, C.c_double, C.c_uint64, C.c_uint32, C.c_uint32,
+                                   C.c_uint64, _dp]),
+    "hmc_get_launch_variant": (C.c_int, [_vp, C.c_uint32, C.c_uint32, C.POINTER(hmc_launch_variant)]),
+    "hmc_set_launch_variant": (C.c_int, [_vp, C.c_uint32, C.c_uint32]),
+    "hmc_autotune": (C.c_int, [_vp, C.POINTER(hmc_sweep_params), C.c_uint32, C.POINTER(hmc_launch_variant), _dp]),
+    "hmc_batch_autotune": (C.c_int, [_vp, C.POINTER(hmc_sweep_params), C.c_uint32, C.POINTER(hmc_launch_variant),
+                                     _dp]),
+    "hmc_batch_set_launch_variant": (C.c_int, [_vp, C.c_uint32, C.c_uint32]),
     "hmc_total_energy": (C.c_int, [_vp, _dp]),
     "hmc_overlap_count_noalloc": (C.c_int, [_vp, C.c_uint64, C.c_uint32, _dp, C.c_double, C.c_double, _vp, _vp]),
     "hmc_quick_insert_apply": (C.c_int, [_vp, C.POINTER(hmc_quick_insert), C.POINTER(hmc_count)]),
@@ -234,6 +247,16 @@ class Context:
         _check(_lib.hmc_math_sincos(self._h, x.ctypes.data_as(_dp), x.size, sn.ctypes.data_as(_dp),
                                     cs.ctypes.data_as(_dp)))
         return sn, cs
+
+    def sample_moves(self, dim: int, kind: int, maximum: float, n: int, step: int = 0, substep: int = 0,
+                     seed: int = 0) -> np.ndarray:
+        """n proposals of the device samplers (hmc_sample_moves), sample i from
+        Counter(step, substep, seed).index(i): kind 0 Translate displacements (n x dim), kind 1 Rotate
+        (3-D versors n x 4, 2-D angles n), kind 2 StandardNormal draws (n)."""
+        per = 1 if kind == 2 else (dim if kind == 0 else (4 if dim == 3 else 1))
+        out = np.empty(n * per)
+        _check(_lib.hmc_sample_moves(self._h, dim, kind, maximum, step, substep, seed, n, out.ctypes.data_as(_dp)))
+        return out.reshape(n, per) if per > 1 else out
 
     def close(self):
         if getattr(self, "_h", None):
@@ -632,18 +655,37 @@ class Microstate:
         _check(_lib.hmc_sweep(self._h, C.byref(p), C.byref(c)))
         return Count(c.accepted, c.rejected, c.rechecks, c.pair_checks, c.max_fp32_error, c.order_ambiguous)
 
+    def launch_variant(self, precision: int, index: Optional[int] = None) -> dict:
+        """The launch variant the next sweep runs in this precision (or variant `index`)."""
+        v = hmc_launch_variant()
+        _check(_lib.hmc_get_launch_variant(self._h, precision, 0xFFFFFFFF if index is None else index, C.byref(v)))
+        return {f: getattr(v, f) for f, _ in hmc_launch_variant._fields_}
+
+    def set_launch_variant(self, precision: int, index: Optional[int]):
+        """Force a launch variant (None: the autotuner's recorded choice for this workload, else 0)."""
+        _check(_lib.hmc_set_launch_variant(self._h, precision, 0xFFFFFFFF if index is None else index))
+
+    def autotune(self, move: int, maximum: float, temperature: float, precision: int, sweeps: int = 4):
+        """hmc_autotune: time every launch variant of this system's pass from the current state
+        (restored after), keep the fastest; returns (chosen variant, ms per sweep per variant)."""
+        p = hmc_sweep_params(C.sizeof(hmc_sweep_params), move, maximum, temperature, precision, 1, 1, 0)
+        v = hmc_launch_variant()
+        ms = np.zeros(16)
+        _check(_lib.hmc_autotune(self._h, C.byref(p), sweeps, C.byref(v), ms.ctypes.data_as(_dp)))
+        return {f: getattr(v, f) for f, _ in hmc_launch_variant._fields_}, ms[: v.count].copy()
+
     def serial_sweep(self, maximum: float, n_sweeps: int = 1, increment_step: bool = False, move_mask=None,
-                     temperature: float = 1.0) -> "Count":
-        """Sweep::apply_with_filter (sweep.rs:159-224), hard or overlap-penalty spheres: bodies in
-        index order from one sequential stream; move_mask (n booleans) plays should_move_body."""
-        p = hmc_sweep_params(C.sizeof(hmc_sweep_params), TRANSLATE, maximum, temperature, FP64, n_sweeps,
+                     temperature: float = 1.0, move: int = TRANSLATE) -> "Count":
+        """Sweep::apply_with_filter (sweep.rs:159-224), any interaction: bodies in index order from
+        one sequential stream; move_mask (n booleans) plays should_move_body; ROTATE for shapes."""
+        p = hmc_sweep_params(C.sizeof(hmc_sweep_params), move, maximum, temperature, FP64, n_sweeps,
                              int(increment_step), 0)
         c = hmc_count()
         mask = None
         if move_mask is not None:
             mask = np.ascontiguousarray(np.asarray(move_mask, dtype=bool).astype(np.uint8))
         _check(_lib.hmc_serial_sweep(self._h, C.byref(p), None if mask is None else mask.ctypes.data_as(_u8p), C.byref(c)))
-        return Count(c.accepted, c.rejected, 0, 0, 0.0)
+        return Count(c.accepted, c.rejected, 0, 0, 0.0, c.order_ambiguous)
 
     def eval_moves(self, bodies, positions, u=None, temperature: float = 1.0, precision: int = FP64,
                    return_delta_h: bool = False, orientations=None):
@@ -934,6 +976,23 @@ class Batch:
                                      1, 0, flags)
         _check(_lib.hmc_batch_tune(self._h, ps, target, samples, steps))
         return np.array([ps[k].maximum for k in range(self.n_replicas)])
+
+    def autotune(self, maxima, precision: int, sweeps: int = 3, temperatures=1.0):
+        """hmc_batch_autotune: the fastest launch variant of the replica pass, from the current
+        state (restored after); returns (chosen variant, ms per sweep per variant)."""
+        maxima = np.broadcast_to(np.asarray(maxima, dtype=np.float64), (self.n_replicas,))
+        kts = np.broadcast_to(np.asarray(temperatures, dtype=np.float64), (self.n_replicas,))
+        ps = (hmc_sweep_params * self.n_replicas)()
+        for k in range(self.n_replicas):
+            ps[k] = hmc_sweep_params(C.sizeof(hmc_sweep_params), TRANSLATE, float(maxima[k]), float(kts[k]), precision,
+                                     1, 1, 0)
+        v = hmc_launch_variant()
+        ms = np.zeros(16)
+        _check(_lib.hmc_batch_autotune(self._h, ps, sweeps, C.byref(v), ms.ctypes.data_as(_dp)))
+        return {f: getattr(v, f) for f, _ in hmc_launch_variant._fields_}, ms[: v.count].copy()
+
+    def set_launch_variant(self, precision: int, index: Optional[int]):
+        _check(_lib.hmc_batch_set_launch_variant(self._h, precision, 0xFFFFFFFF if index is None else index))
 
     def sdf(self, x_max: float = 0.02, n_bins: int = 40) -> np.ndarray:
         """Scale distributions of all replicas (hard spheres): (n_replicas, n_bins) pair counts."""

@@ -11,6 +11,9 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <vector>
 
 #include "../../include/hmc.h"
@@ -86,6 +89,7 @@ struct hmc_system {
     unsigned long long* host_first_bad = nullptr;  // pinned mirror
     std::vector<void*> allocations;
     bool coop[2] = {true, false};  // warp-cooperative hard-sphere pass: [fp64, fp32]
+    int32_t variant[2] = {-1, -1};  // launch variant per precision; -1: the cached choice or the default
     bool pdl = true;                // colour passes launch while the previous one finishes
     uint32_t rounds_guess = 2;      // colour sets enqueued before the sweep's count is known
     // serial sweep grid (allocated on first use)
@@ -315,6 +319,58 @@ hmc_status check_flags(hmc_system* s) {
     if (f & kErrAngleRange) return fail(HMC_INVALID_ARGUMENT, "a 2-D orientation angle reached 2^19 rad");
     if (f & kErrCellOverflow) return fail(HMC_CELL_OVERFLOW, "a cell of the serial sweep's grid is full");
     return HMC_OK;
+}
+
+// ---- launch variants -------------------------------------------------------------------------
+// The colour-pass kernel family a system's sweep runs in a precision, and its variant table.
+enum VariantFamily : uint32_t { kFamSphereDirect, kFamSphereCoop, kFamLj, kFamPoly3, kFamPoly2, kFamBatch, kFamBatchLj };
+
+uint32_t family_of(const hmc_system* s, bool fp32) {
+    if (s->soft()) return kFamLj;
+    if (s->interaction == HMC_HARD_CONVEX_POLYHEDRON) return kFamPoly3;
+    if (s->polygon()) return kFamPoly2;
+    return s->coop[fp32] ? kFamSphereCoop : kFamSphereDirect;
+}
+
+const LaunchShape* family_shapes(uint32_t fam, uint32_t* n) {
+    switch (fam) {
+        case kFamSphereDirect: *n = n_shapes(kSphereDirectShapes); return kSphereDirectShapes;
+        case kFamSphereCoop: *n = n_shapes(kSphereCoopShapes); return kSphereCoopShapes;
+        case kFamLj: *n = n_shapes(kLjShapes); return kLjShapes;
+        case kFamPoly3: *n = n_shapes(kPolyShapes); return kPolyShapes;
+        case kFamPoly2: *n = n_shapes(kPoly2Shapes); return kPoly2Shapes;
+        case kFamBatch: *n = n_shapes(kBatchShapes); return kBatchShapes;
+        default: *n = n_shapes(kBatchLjShapes); return kBatchLjShapes;
+    }
+}
+
+// The density band of a workload: bodies per checkerboard space in quarter octaves.
+int32_t density_band(double bodies, double spaces) {
+    if (!(bodies > 0.0) || !(spaces > 0.0)) return -1000;
+    return (int32_t)std::lround(4.0 * std::log2(bodies / spaces));
+}
+
+// Choices of hmc_autotune shared by every system and batch of the process, keyed by kernel
+// family, dimension, precision and density band.
+std::mutex g_variant_mutex;
+std::map<std::tuple<uint32_t, uint32_t, uint32_t, int32_t>, uint32_t> g_variant_cache;
+
+uint32_t cached_variant(uint32_t fam, uint32_t dim, bool fp32, int32_t band) {
+    std::lock_guard<std::mutex> lock(g_variant_mutex);
+    auto it = g_variant_cache.find(std::make_tuple(fam, dim, (uint32_t)fp32, band));
+    return it == g_variant_cache.end() ? 0u : it->second;
+}
+
+void cache_variant(uint32_t fam, uint32_t dim, bool fp32, int32_t band, uint32_t v) {
+    std::lock_guard<std::mutex> lock(g_variant_mutex);
+    g_variant_cache[std::make_tuple(fam, dim, (uint32_t)fp32, band)] = v;
+}
+
+// The variant the next sweep of system s runs in this precision.
+uint32_t variant_of(const hmc_system* s, bool fp32) {
+    if (s->variant[fp32] >= 0) return (uint32_t)s->variant[fp32];
+    return cached_variant(family_of(s, fp32), (uint32_t)s->dim, fp32,
+                          density_band((double)s->n, (double)s->geom.n_cells));
 }
 
 // update_checkerboard (parallel_sweep.rs:176-201): origin shift from the counter's
@@ -810,6 +866,7 @@ hmc_status hmc_sweep(hmc_system* s, const hmc_sweep_params* p, hmc_count* out) {
         L.kt = p->temperature;
         L.n_bodies = (uint32_t)s->n;
         L.n_active = s->geom.color_stride;  // grid bound; the kernels read the list lengths
+        const uint32_t variant = variant_of(s, fp32);
         if (s->profiling) HMC_CUDA(cudaEventRecord(s->ev[2], s->stream));
         // The rounds (while count.total() < N, :402-418) are known on the device after the
         // rebuild; the host enqueues the previous sweep's number of colour sets without
@@ -824,17 +881,18 @@ hmc_status hmc_sweep(hmc_system* s, const hmc_sweep_params* p, hmc_count* out) {
                     L.early_wait = r == 0 && c == 0 && s->pdl ? 1u : 0u;  // right after the rebuild
                     if (s->soft())  // the overlap penalty has no FP32 path: FP64 in both modes
                         HMC_CUDA(launch_sweep_lj(s->dim, fp32 && !s->penalty(), s->geom, s->arr, s->pair, L,
-                                                 s->stream));
+                                                 s->stream, variant));
                     else if (s->interaction == HMC_HARD_CONVEX_POLYHEDRON)
                         HMC_CUDA(launch_sweep_poly(fp32, s->geom, s->arr, s->verts, s->n_vertices, s->poly_rcut2,
-                                                   s->poly_rcut2_hi32, L, p->move == HMC_ROTATE, s->stream));
+                                                   s->poly_rcut2_hi32, L, p->move == HMC_ROTATE, s->stream,
+                                                   variant));
                     else if (s->polygon())
                         HMC_CUDA(launch_sweep_poly2(fp32, s->sat(), s->geom, s->arr, s->verts, s->n_vertices,
                                                     s->poly_rcut2, s->poly_rcut2_hi32, L, p->move == HMC_ROTATE,
                                                     s->stream));
                     else
                         HMC_CUDA(launch_sweep_sphere(s->dim, fp32, s->geom, s->arr, s->pair, L, s->coop[fp32],
-                                                     s->stream));
+                                                     s->stream, variant));
                     s->prof.kernel_launches += 1;
                 }
             }
@@ -882,6 +940,132 @@ hmc_status hmc_sweep(hmc_system* s, const hmc_sweep_params* p, hmc_count* out) {
     return HMC_OK;
 }
 
+static void describe_variant(uint32_t fam, uint32_t index, hmc_launch_variant* out) {
+    uint32_t n = 0;
+    const LaunchShape* t = family_shapes(fam, &n);
+    const LaunchShape& v = t[index < n ? index : 0];
+    out->index = index < n ? index : 0;
+    out->count = n;
+    out->blocks_per_sm = v.blocks_per_sm;
+    out->trials_per_warp = v.trials_per_warp;
+    out->own_steps = v.own_steps;
+}
+
+hmc_status hmc_get_launch_variant(hmc_system* s, uint32_t precision, uint32_t index, hmc_launch_variant* out) {
+    if (!s || !out) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
+    if (precision > HMC_FP32_RECHECK) return fail(HMC_INVALID_ARGUMENT, "precision");
+    const bool fp32 = precision == HMC_FP32_RECHECK;
+    const uint32_t fam = family_of(s, fp32);
+    uint32_t n = 0;
+    family_shapes(fam, &n);
+    if (index != UINT32_MAX && index >= n) return fail(HMC_INVALID_ARGUMENT, "variant %u of %u", index, n);
+    describe_variant(fam, index == UINT32_MAX ? variant_of(s, fp32) : index, out);
+    return HMC_OK;
+}
+
+hmc_status hmc_set_launch_variant(hmc_system* s, uint32_t precision, uint32_t index) {
+    if (!s) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
+    if (precision > HMC_FP32_RECHECK) return fail(HMC_INVALID_ARGUMENT, "precision");
+    const bool fp32 = precision == HMC_FP32_RECHECK;
+    uint32_t n = 0;
+    family_shapes(family_of(s, fp32), &n);
+    if (index != UINT32_MAX && index >= n) return fail(HMC_INVALID_ARGUMENT, "variant %u of %u", index, n);
+    s->variant[fp32] = index == UINT32_MAX ? -1 : (int32_t)index;
+    return HMC_OK;
+}
+
+}  // extern "C"
+
+// Times `sweeps` sweeps (after one untimed) from the state saved in `save`, restoring it first;
+// run(p) sweeps, restore() puts the saved state back. Returns the mean device time of a sweep
+// (CUDA events on the stream around the host calls, so the host's share counts too).
+template <typename Run, typename Restore>
+static hmc_status time_variant(cudaStream_t stream, const hmc_sweep_params& p, uint32_t sweeps, Run&& run,
+                               Restore&& restore, double* ms) {
+    hmc_status st;
+    if ((st = restore())) return st;
+    hmc_sweep_params one = p;
+    one.n_sweeps = 1;
+    one.increment_step = 1;
+    if ((st = run(one))) return st;  // warm-up (and the first rebuild's allocations)
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    HMC_CUDA(cudaEventCreate(&e0));
+    cudaError_t e = cudaEventCreate(&e1);
+    hmc_sweep_params many = one;
+    many.n_sweeps = sweeps;
+    if (e == cudaSuccess) e = cudaEventRecord(e0, stream);
+    if (e == cudaSuccess && !(st = run(many))) e = cudaEventRecord(e1, stream);
+    float t = 0.f;
+    if (e == cudaSuccess && !st) e = cudaEventSynchronize(e1);
+    if (e == cudaSuccess && !st) e = cudaEventElapsedTime(&t, e0, e1);
+    cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (st) return st;
+    if (e != cudaSuccess) return fail(HMC_CUDA_ERROR, "autotune timing: %s", cudaGetErrorString(e));
+    *ms = (double)t / (double)sweeps;
+    return HMC_OK;
+}
+
+extern "C" {
+
+hmc_status hmc_autotune(hmc_system* s, const hmc_sweep_params* p, uint32_t sweeps, hmc_launch_variant* chosen,
+                        double* ms_per_sweep) {
+    if (!s || !p) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
+    if (p->struct_size < sizeof(hmc_sweep_params)) return fail(HMC_INVALID_ARGUMENT, "hmc_sweep_params.struct_size");
+    if (p->precision > HMC_FP32_RECHECK) return fail(HMC_INVALID_ARGUMENT, "precision");
+    if (sweeps == 0 || sweeps > 1000) return fail(HMC_INVALID_ARGUMENT, "sweeps must be in [1, 1000]");
+    HMC_CUDA(cudaSetDevice(s->ctx->device));
+    const bool fp32 = p->precision == HMC_FP32_RECHECK;
+    const uint32_t fam = family_of(s, fp32);
+    uint32_t n_var = 0;
+    family_shapes(fam, &n_var);
+    // the state to start every variant from
+    const uint64_t n = s->n;
+    const uint64_t step0 = s->step;
+    const uint32_t substep0 = s->substep, guess0 = s->rounds_guess;
+    const int32_t own0 = s->variant[fp32];
+    double4 *bp = nullptr, *bq = nullptr;
+    cudaError_t e = cudaMallocAsync((void**)&bp, sizeof(double4) * (n ? n : 1), s->stream);
+    if (e == cudaSuccess && n)
+        e = cudaMemcpyAsync(bp, s->arr.body_pos, sizeof(double4) * n, cudaMemcpyDeviceToDevice, s->stream);
+    if (e == cudaSuccess && s->arr.body_ori) {
+        e = cudaMallocAsync((void**)&bq, sizeof(double4) * (n ? n : 1), s->stream);
+        if (e == cudaSuccess && n)
+            e = cudaMemcpyAsync(bq, s->arr.body_ori, sizeof(double4) * n, cudaMemcpyDeviceToDevice, s->stream);
+    }
+    auto restore = [&]() -> hmc_status {
+        if (n) HMC_CUDA(cudaMemcpyAsync(s->arr.body_pos, bp, sizeof(double4) * n, cudaMemcpyDeviceToDevice, s->stream));
+        if (bq && n)
+            HMC_CUDA(cudaMemcpyAsync(s->arr.body_ori, bq, sizeof(double4) * n, cudaMemcpyDeviceToDevice, s->stream));
+        s->step = step0;
+        s->substep = substep0;
+        s->rounds_guess = guess0;
+        return HMC_OK;
+    };
+    auto run = [&](const hmc_sweep_params& q) -> hmc_status { return hmc_sweep(s, &q, nullptr); };
+    hmc_status st = e == cudaSuccess ? HMC_OK : fail(HMC_CUDA_ERROR, "autotune: %s", cudaGetErrorString(e));
+    std::vector<double> ms(n_var, 0.0);
+    uint32_t best = 0;
+    for (uint32_t v = 0; v < n_var && !st; ++v) {
+        s->variant[fp32] = (int32_t)v;
+        st = time_variant(s->stream, *p, sweeps, run, restore, &ms[v]);
+        if (!st && ms[v] < ms[best]) best = v;
+    }
+    hmc_status st2 = restore();
+    if (bp) cudaFreeAsync(bp, s->stream);
+    if (bq) cudaFreeAsync(bq, s->stream);
+    cudaStreamSynchronize(s->stream);
+    if (st || st2) {
+        s->variant[fp32] = own0;
+        return st ? st : st2;
+    }
+    s->variant[fp32] = (int32_t)best;
+    cache_variant(fam, (uint32_t)s->dim, fp32, density_band((double)s->n, (double)s->geom.n_cells), best);
+    if (chosen) describe_variant(fam, best, chosen);
+    if (ms_per_sweep) std::memcpy(ms_per_sweep, ms.data(), sizeof(double) * n_var);
+    return HMC_OK;
+}
+
 hmc_status hmc_math_sincos(hmc_context* ctx, const double* x, uint64_t n, double* sn, double* cs) {
     if (!ctx || (n > 0 && (!x || !sn || !cs))) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
     if (n == 0) return HMC_OK;
@@ -901,6 +1085,25 @@ hmc_status hmc_math_sincos(hmc_context* ctx, const double* x, uint64_t n, double
     if (bad) cudaFree(bad);
     if (e != cudaSuccess) return fail(HMC_CUDA_ERROR, "sincos: %s", cudaGetErrorString(e));
     if (hbad) return fail(HMC_INVALID_ARGUMENT, "an argument has |x| >= 2^20");
+    return HMC_OK;
+}
+
+hmc_status hmc_sample_moves(hmc_context* ctx, uint32_t dim, uint32_t kind, double maximum, uint64_t step,
+                            uint32_t substep, uint32_t seed, uint64_t n, double* out) {
+    if (!ctx || (n > 0 && !out)) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
+    if (dim != 2 && dim != 3) return fail(HMC_INVALID_ARGUMENT, "dim must be 2 or 3");
+    if (kind > 2) return fail(HMC_INVALID_ARGUMENT, "kind: 0 translate, 1 rotate, 2 standard normal");
+    if (kind != 2 && !(maximum > 0.0 && std::isfinite(maximum))) return fail(HMC_INVALID_ARGUMENT, "maximum");
+    if (n == 0) return HMC_OK;
+    if (n >= (1ull << 31)) return fail(HMC_INVALID_ARGUMENT, "too many samples");
+    const uint64_t per = kind == 2 ? 1 : (kind == 0 ? dim : (dim == 3 ? 4 : 1));
+    HMC_CUDA(cudaSetDevice(ctx->device));
+    double* d = nullptr;
+    cudaError_t e = cudaMalloc((void**)&d, sizeof(double) * per * n);
+    if (e == cudaSuccess) e = launch_sample_moves((int)dim, kind, maximum, step, substep, seed, n, ctx->zig, d, nullptr);
+    if (e == cudaSuccess) e = cudaMemcpy(out, d, sizeof(double) * per * n, cudaMemcpyDeviceToHost);
+    if (d) cudaFree(d);
+    if (e != cudaSuccess) return fail(HMC_CUDA_ERROR, "sample_moves: %s", cudaGetErrorString(e));
     return HMC_OK;
 }
 
@@ -937,9 +1140,8 @@ static hmc_status serial_grid(hmc_system* s) {
 hmc_status hmc_serial_sweep(hmc_system* s, const hmc_sweep_params* p, const uint8_t* move_mask, hmc_count* out) {
     if (!s || !p) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
     if (p->struct_size < sizeof(hmc_sweep_params)) return fail(HMC_INVALID_ARGUMENT, "hmc_sweep_params.struct_size");
-    if (s->interaction != HMC_HARD_SPHERE && !s->penalty())
-        return fail(HMC_NOT_SUPPORTED, "the serial sweep is built for hard and overlap-penalty spheres");
-    if (p->move != HMC_TRANSLATE) return fail(HMC_NOT_SUPPORTED, "spheres take translation moves");
+    if (p->move != HMC_TRANSLATE && !(p->move == HMC_ROTATE && s->oriented()))
+        return fail(HMC_NOT_SUPPORTED, "rotation moves need oriented bodies (convex polyhedra or polygons)");
     if (!(p->temperature > 0.0)) return fail(HMC_INVALID_ARGUMENT, "temperature must be positive");
     double lmax = 0.0;
     for (int a = 0; a < s->dim; ++a) lmax = std::max(lmax, s->geom.L[a]);
@@ -966,16 +1168,27 @@ hmc_status hmc_serial_sweep(hmc_system* s, const hmc_sweep_params* p, const uint
         L.kt = p->temperature;
         L.n_bodies = (uint32_t)s->n;
         HMC_CUDA(cudaMemsetAsync(s->arr.stats, 0, sizeof(DeviceStats), s->stream));
-        HMC_CUDA(launch_serial_sphere(s->dim, s->penalty(), s->geom, s->arr, s->pair, L, s->serial_nc, s->serial_w,
-                                      s->serial_cap,
-                                      s->serial_size, s->serial_items, s->serial_cell_of, s->serial_site,
-                                      move_mask ? s->serial_mask : nullptr, s->stream));
+        const uint8_t* mask = move_mask ? s->serial_mask : nullptr;
+        const bool rot = p->move == HMC_ROTATE;
+        if (s->polygon())
+            HMC_CUDA(launch_serial_poly2(s->sat(), s->geom, s->arr, s->verts, s->n_vertices, s->poly_rcut2, L, rot,
+                                         s->serial_nc, s->serial_w, s->serial_cap, s->serial_size, s->serial_items,
+                                         s->serial_cell_of, s->serial_site, mask, s->stream));
+        else if (s->oriented())
+            HMC_CUDA(launch_serial_poly(s->geom, s->arr, s->verts, s->n_vertices, s->poly_rcut2, L, rot, s->serial_nc,
+                                        s->serial_w, s->serial_cap, s->serial_size, s->serial_items,
+                                        s->serial_cell_of, s->serial_site, mask, s->stream));
+        else
+            HMC_CUDA(launch_serial_sphere(s->dim, s->soft(), s->geom, s->arr, s->pair, L, s->serial_nc, s->serial_w,
+                                          s->serial_cap, s->serial_size, s->serial_items, s->serial_cell_of,
+                                          s->serial_site, mask, s->stream));
         s->prof.kernel_launches += 2;
         hmc_status st;
         if ((st = read_stats(s))) return st;
         if ((st = check_flags(s))) return st;
         total.accepted += s->host_stats->accepted;
         total.rejected += moving - s->host_stats->accepted;
+        total.order_ambiguous += s->host_stats->ambiguous;
         s->substep += 1;  // increment_substep (sweep.rs:222)
         if (p->increment_step) {
             s->step += 1;
@@ -1668,6 +1881,7 @@ struct hmc_batch {
     unsigned long long* host_first_bad = nullptr;
     std::vector<void*> allocations;
     uint64_t kernel_launches = 0;
+    int32_t variant[2] = {-1, -1};  // launch variant of the hard-sphere replica pass per precision
     uint32_t rounds_guess = 2;
     uint32_t interaction = HMC_HARD_SPHERE;  // the same for every replica
     std::vector<double> body_range;          // [R] ParallelSweep range of each replica
@@ -1923,6 +2137,17 @@ hmc_status hmc_batch_create(hmc_context* ctx, uint32_t n_replicas, const hmc_sys
     return HMC_OK;
 }
 
+static uint32_t batch_family(const hmc_batch* bt) {
+    return bt->interaction == HMC_LENNARD_JONES ? kFamBatchLj : kFamBatch;
+}
+
+// The variant the batch's next sweep runs: its own choice, else the cached one for its family,
+// dimension, precision and density band (all replicas' bodies over all their spaces), else 0.
+static uint32_t batch_variant_of(const hmc_batch* bt, bool fp32) {
+    if (bt->variant[fp32] >= 0) return (uint32_t)bt->variant[fp32];
+    return cached_variant(batch_family(bt), (uint32_t)bt->dim, fp32, density_band((double)bt->n, (double)bt->cells));
+}
+
 hmc_status hmc_batch_sweep(hmc_batch* bt, const hmc_sweep_params* params, hmc_count* counts, hmc_count* total) {
     if (!bt || !params) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
     const hmc_sweep_params& p0 = params[0];
@@ -1948,6 +2173,7 @@ hmc_status hmc_batch_sweep(hmc_batch* bt, const hmc_sweep_params* params, hmc_co
     HMC_CUDA(cudaSetDevice(bt->ctx->device));
     const bool fp32 = p0.precision == HMC_FP32_RECHECK;
     const uint32_t colors = 1u << bt->dim;
+    const uint32_t variant = batch_variant_of(bt, fp32);
     if (counts) std::memset(counts, 0, sizeof(hmc_count) * bt->n_rep);
     hmc_count tot{};
     for (uint32_t sweep = 0; sweep < p0.n_sweeps; ++sweep) {
@@ -1964,7 +2190,7 @@ hmc_status hmc_batch_sweep(hmc_batch* bt, const hmc_sweep_params* params, hmc_co
                                                        round > 0 || c > 0, round == 0 && c == 0, bt->stream));
                     else
                         HMC_CUDA(launch_sweep_batch(bt->dim, fp32, bt->b, bt->arr, c, round, bt->b.color_stride,
-                                                    round > 0 || c > 0, round == 0 && c == 0, bt->stream));
+                                                    round > 0 || c > 0, round == 0 && c == 0, bt->stream, variant));
                     bt->kernel_launches += 1;
                 }
             return HMC_OK;
@@ -2007,6 +2233,78 @@ hmc_status hmc_batch_sweep(hmc_batch* bt, const hmc_sweep_params* params, hmc_co
     if (total) *total = tot;
     return HMC_OK;
 }
+
+hmc_status hmc_batch_set_launch_variant(hmc_batch* bt, uint32_t precision, uint32_t index) {
+    if (!bt) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
+    if (precision > HMC_FP32_RECHECK) return fail(HMC_INVALID_ARGUMENT, "precision");
+    uint32_t n = 0;
+    family_shapes(batch_family(bt), &n);
+    if (index != UINT32_MAX && index >= n) return fail(HMC_INVALID_ARGUMENT, "variant %u of %u", index, n);
+    bt->variant[precision == HMC_FP32_RECHECK] = index == UINT32_MAX ? -1 : (int32_t)index;
+    return HMC_OK;
+}
+
+}  // extern "C"
+
+hmc_status hmc_batch_autotune(hmc_batch* bt, const hmc_sweep_params* params, uint32_t sweeps,
+                              hmc_launch_variant* chosen, double* ms_per_sweep) {
+    if (!bt || !params) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
+    if (params[0].precision > HMC_FP32_RECHECK) return fail(HMC_INVALID_ARGUMENT, "precision");
+    if (sweeps == 0 || sweeps > 1000) return fail(HMC_INVALID_ARGUMENT, "sweeps must be in [1, 1000]");
+    HMC_CUDA(cudaSetDevice(bt->ctx->device));
+    const bool fp32 = params[0].precision == HMC_FP32_RECHECK;
+    const uint32_t fam = batch_family(bt);
+    uint32_t n_var = 0;
+    family_shapes(fam, &n_var);
+    const uint64_t n = bt->n;
+    std::vector<std::pair<uint64_t, uint32_t>> counters(bt->n_rep);
+    for (uint32_t k = 0; k < bt->n_rep; ++k) counters[k] = {bt->rep[k].step, bt->rep[k].substep};
+    const uint32_t guess0 = bt->rounds_guess;
+    const int32_t own0 = bt->variant[fp32];
+    double4* bp = nullptr;
+    cudaError_t e = cudaMallocAsync((void**)&bp, sizeof(double4) * (n ? n : 1), bt->stream);
+    if (e == cudaSuccess && n)
+        e = cudaMemcpyAsync(bp, bt->arr.body_pos, sizeof(double4) * n, cudaMemcpyDeviceToDevice, bt->stream);
+    auto restore = [&]() -> hmc_status {
+        if (n) HMC_CUDA(cudaMemcpyAsync(bt->arr.body_pos, bp, sizeof(double4) * n, cudaMemcpyDeviceToDevice, bt->stream));
+        for (uint32_t k = 0; k < bt->n_rep; ++k) {
+            bt->rep[k].step = counters[k].first;
+            bt->rep[k].substep = counters[k].second;
+        }
+        bt->rounds_guess = guess0;
+        return HMC_OK;
+    };
+    std::vector<hmc_sweep_params> ps(params, params + bt->n_rep);
+    auto run = [&](const hmc_sweep_params& q) -> hmc_status {
+        for (auto& x : ps) {
+            x.n_sweeps = q.n_sweeps;
+            x.increment_step = q.increment_step;
+        }
+        return hmc_batch_sweep(bt, ps.data(), nullptr, nullptr);
+    };
+    hmc_status st = e == cudaSuccess ? HMC_OK : fail(HMC_CUDA_ERROR, "batch autotune: %s", cudaGetErrorString(e));
+    std::vector<double> ms(n_var, 0.0);
+    uint32_t best = 0;
+    for (uint32_t v = 0; v < n_var && !st; ++v) {
+        bt->variant[fp32] = (int32_t)v;
+        st = time_variant(bt->stream, params[0], sweeps, run, restore, &ms[v]);
+        if (!st && ms[v] < ms[best]) best = v;
+    }
+    hmc_status st2 = restore();
+    if (bp) cudaFreeAsync(bp, bt->stream);
+    cudaStreamSynchronize(bt->stream);
+    if (st || st2) {
+        bt->variant[fp32] = own0;
+        return st ? st : st2;
+    }
+    bt->variant[fp32] = (int32_t)best;
+    cache_variant(fam, (uint32_t)bt->dim, fp32, density_band((double)bt->n, (double)bt->cells), best);
+    if (chosen) describe_variant(fam, best, chosen);
+    if (ms_per_sweep) std::memcpy(ms_per_sweep, ms.data(), sizeof(double) * n_var);
+    return HMC_OK;
+}
+
+extern "C" {
 
 hmc_status hmc_batch_get_state(hmc_batch* bt, uint32_t replica, double* positions, uint64_t* step, uint32_t* substep) {
     if (!bt || replica >= bt->n_rep) return fail(HMC_INVALID_ARGUMENT, "no such replica");

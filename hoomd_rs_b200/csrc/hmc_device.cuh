@@ -427,6 +427,39 @@ __device__ __forceinline__ uint32_t active_count(const Arrays& A, uint32_t color
     return st->color_count[color];
 }
 
+// Whether another order of the same FP64 sums could change the Metropolis decision. The pair
+// energies are the same numbers in any order, and recursive summation of n terms in any order
+// (any summation tree) lies within gamma_{n-1} sum|e| of the exact sum, gamma_k = k u / (1 - k u),
+// u = 2^-53 (Higham, Accuracy and Stability of Numerical Algorithms, 2nd ed., 2002, section
+// 4.2). So dU = E_final - E_initial summed in any two orders (this pass's lanes and
+// butterfly, the reference's cell-list order) differ by at most
+// B = 2 gamma_{n-1} (sum|e_final| + sum|e_initial|) + 2 u |dU|. The decision (dU <= 0, else
+// u < exp(-dU / kT), parallel_sweep.rs:267-268) is monotone in dU: it is the same in every order
+// when dU - B and dU + B decide alike, with exp allowed 4 ulp either way (the reference calls
+// the platform libm, this pass CUDA's exp). n = the candidates of the stencil (>= the terms);
+// e0 = exp(-dU / kT) as the decision computed it. Over [dU - B, dU + B] exp(-x / kT) stays
+// within a factor exp(B / kT) <= 1 + 2 B / kT of e0 (B / kT < 1e-3), so a uniform farther than
+// e0 (4 B / kT + 1e-14) from e0 settles the trial without evaluating the ends.
+__device__ __forceinline__ double order_bound(double du, double mag, uint32_t n) {
+    const double unit = 1.1102230246251565e-16;  // 2^-53
+    const double k = (double)(n > 1u ? n - 1u : 1u);
+    const double gamma = k * unit / (1.0 - k * unit);
+    return 1.01 * (2.0 * gamma * mag + 2.0 * unit * fabs(du)) + 1e-300;
+}
+__device__ __forceinline__ bool order_ambiguous(double du, double mag, uint32_t n, double u, double kt, double e0) {
+    if (!isfinite(du) || !isfinite(mag)) return false;  // an infinite pair energy decides in any order
+    const double unit = 1.1102230246251565e-16;        // 2^-53
+    const double b = order_bound(du, mag, n);
+    const double lo = du - b, hi = du + b;
+    if (hi <= 0.0) return false;  // accepted in every order, without a uniform
+    const double rel = b / kt;
+    if (lo > 0.0 && rel < 1e-3 && fabs(u - e0) > e0 * (4.0 * rel + 1e-14)) return false;
+    const double ulp4 = 8.0 * unit;
+    const bool acc_at_lo = lo <= 0.0 || u < exp(-lo / kt) * (1.0 + ulp4);
+    const bool acc_at_hi = u < exp(-hi / kt) * (1.0 - ulp4);
+    return acc_at_lo != acc_at_hi;
+}
+
 // ---- the sequential-stream tuner -------------------------------------------------------------
 // tune_local_trial (hoomd-mc/src/tune_local.rs:42-88) on one warp for job J (TuneJob). Every lane
 // runs the same single stream Counter(step, substep, seed).make_rng() (index 0), so the trial is

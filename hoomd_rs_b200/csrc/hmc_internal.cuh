@@ -109,6 +109,19 @@ __device__ __forceinline__ double penalty_pair64(const Pair& P, double r2) {
     return 0.0;
 }
 
+// Soft pair energy in FP64 exactly as the reference evaluates it: the overlap penalty above, or
+// Isotropic::site_pair_energy (isotropic.rs:147-156: r^2 >= r_cut^2 -> 0, else energy(sqrt(r^2)))
+// of Shifted (shifted.rs:92-94: f(r) - f(r_shift)) LennardJones (lennard_jones.rs:107-111:
+// 4 eps ((sigma/r)^12 - (sigma/r)^6) with powi by repeated squaring).
+__device__ __forceinline__ double lj_pair64(const Pair& P, double r2) {
+    if (P.penalty) return penalty_pair64(P, r2);
+    if (r2 >= P.lj_rcut2) return 0.0;
+    const double r = dsqrt(r2);
+    const double sr = ddiv(P.lj_sigma, r);
+    const double s2 = dmul(sr, sr), s4 = dmul(s2, s2), s8 = dmul(s4, s4);
+    return dsub(dmul(P.lj_four_eps, dsub(dmul(s4, s8), dmul(s2, s4))), P.lj_e_shift);
+}
+
 // One sweep launch: counter, move and colour.
 struct Launch {
     uint64_t step;
@@ -167,6 +180,31 @@ struct TuneJob {
     unsigned long long accepted;   // out: accepted trials of the last round
     unsigned long long ambiguous;  // out: soft-potential decisions another summation order could change
 };
+
+// Launch variants of the colour-pass kernels (the autotuner's search space, hmc_autotune): each
+// variant is a compiled instantiation; index 0 of every table is the default. blocks_per_sm is
+// the resident-block target the kernel is compiled for (its register cap), trials_per_warp the
+// trials a warp of the packed polyhedron pass takes, own_steps the candidates per row a lane of
+// the warp-cooperative sphere pass tests before handing the rest to its warp. Every variant makes
+// the same pair tests and decisions, so the trajectory does not depend on the choice.
+struct LaunchShape {
+    uint32_t blocks_per_sm, trials_per_warp, own_steps;
+};
+constexpr LaunchShape kSphereDirectShapes[] = {{6, 1, 0}, {5, 1, 0}, {7, 1, 0}};
+constexpr LaunchShape kSphereCoopShapes[] = {{6, 1, 2}, {6, 1, 1}, {6, 1, 3}, {5, 1, 2}, {7, 1, 2}};
+constexpr LaunchShape kLjShapes[] = {{9, 1, 0}, {7, 1, 0}, {11, 1, 0}};
+constexpr LaunchShape kPolyShapes[] = {{5, 4, 0}, {5, 2, 0}, {5, 8, 0}};
+constexpr LaunchShape kBatchShapes[] = {{4, 1, 0}, {3, 1, 0}, {5, 1, 0}};
+constexpr LaunchShape kPoly2Shapes[] = {{8, 4, 0}};    // the polygon pass: one compiled shape
+constexpr LaunchShape kBatchLjShapes[] = {{7, 1, 0}};  // the Lennard-Jones replica passes: one
+template <size_t N>
+constexpr uint32_t n_shapes(const LaunchShape (&)[N]) {
+    return (uint32_t)N;
+}
+
+// Blocks in one resident wave of a 128-thread kernel on the current device (SMs x resident
+// blocks per SM), cached per kernel.
+int resident_wave(const void* kernel);
 
 // Launch configuration of a colour pass: 128 threads per block; overlap = programmatic
 // dependent launch after the previous colour pass of the same sweep (the kernel waits with
@@ -235,18 +273,19 @@ cudaError_t launch_batch_rounds(const Batch& b, Replica* rep, DeviceStats* stats
 // Batches of replicas: the rebuild and the hard-sphere colour pass over all replicas at once.
 cudaError_t launch_rebuild_batch(int dim, const Batch& b, const Arrays& a, uint32_t n, bool write_s, cudaStream_t s);
 cudaError_t launch_sweep_batch(int dim, bool fp32, const Batch& b, const Arrays& a, uint32_t color, uint32_t round,
-                               uint32_t max_active, bool overlap_previous, bool early_wait, cudaStream_t s);
+                               uint32_t max_active, bool overlap_previous, bool early_wait, cudaStream_t s,
+                               uint32_t variant = 0);
 cudaError_t launch_overlap_batch(int dim, const Batch& b, const Arrays& a, uint32_t n, cudaStream_t s);
 // Batches of Lennard-Jones replicas: one warp per trial over every replica's colour list (hmc_lj.cu).
 cudaError_t launch_sweep_batch_lj(int dim, bool fp32, const Batch& b, const Arrays& a, uint32_t color, uint32_t round,
                                   uint32_t max_active, bool overlap_previous, bool early_wait, cudaStream_t s);
 // coop selects the warp-cooperative pass (the per-lane pass otherwise).
 cudaError_t launch_sweep_sphere(int dim, bool fp32, const Geometry& g, const Arrays& a, const Pair& p,
-                                const Launch& l, bool coop, cudaStream_t s);
+                                const Launch& l, bool coop, cudaStream_t s, uint32_t variant = 0);
 cudaError_t launch_overlap_sphere(int dim, const Geometry& g, const Arrays& a, const Pair& p, uint32_t n,
                                   cudaStream_t s);
 cudaError_t launch_sweep_lj(int dim, bool fp32, const Geometry& g, const Arrays& a, const Pair& p, const Launch& l,
-                            cudaStream_t s);
+                            cudaStream_t s, uint32_t variant = 0);
 // delta_energy_one in FP64 for injected trial positions (LJ); u < 0 means no decision needed.
 cudaError_t launch_eval_lj(int dim, bool fp32, const Geometry& g, const Arrays& a, const Pair& p,
                            const uint64_t* bodies, const double4* trial, const double* u, double kt, uint32_t n,
@@ -254,7 +293,8 @@ cudaError_t launch_eval_lj(int dim, bool fp32, const Geometry& g, const Arrays& 
 cudaError_t launch_energy_lj(int dim, const Geometry& g, const Arrays& a, const Pair& p, uint32_t n, double* out,
                              cudaStream_t s);
 cudaError_t launch_sweep_poly(bool fp32, const Geometry& g, const Arrays& a, const double4* verts, uint32_t nv,
-                              double rcut2, float rcut2_hi32, const Launch& l, bool rotate, cudaStream_t s);
+                              double rcut2, float rcut2_hi32, const Launch& l, bool rotate, cudaStream_t s,
+                              uint32_t variant = 0);
 cudaError_t launch_eval_poly(bool fp32, const Geometry& g, const Arrays& a, const double4* verts, uint32_t nv,
                              double rcut2, float rcut2_hi32, const uint64_t* bodies, const double4* trial,
                              const double4* trial_q, uint32_t n, uint8_t* decisions, cudaStream_t s);
@@ -294,6 +334,16 @@ cudaError_t launch_serial_sphere(int dim, bool soft, const Geometry& g, const Ar
                                  const Launch& l, const uint32_t* nc, const double* w, uint32_t cap, uint32_t* size,
                                  uint32_t* items, uint32_t* cell_of, double4* site, const uint8_t* mask,
                                  cudaStream_t s);
+// Sweep::apply_with_filter for hard convex polyhedra (hmc_poly.cu) and polygons (hmc_poly2.cu;
+// sat: separating axes) on the serial grid, Translate or Rotate moves.
+cudaError_t launch_serial_poly(const Geometry& g, const Arrays& a, const double4* verts, uint32_t nv, double rcut2,
+                               const Launch& l, bool rotate, const uint32_t* nc, const double* w, uint32_t cap,
+                               uint32_t* size, uint32_t* items, uint32_t* cell_of, double4* site, const uint8_t* mask,
+                               cudaStream_t s);
+cudaError_t launch_serial_poly2(bool sat, const Geometry& g, const Arrays& a, const double4* verts, uint32_t nv,
+                                double rcut2, const Launch& l, bool rotate, const uint32_t* nc, const double* w,
+                                uint32_t cap, uint32_t* size, uint32_t* items, uint32_t* cell_of, double4* site,
+                                const uint8_t* mask, cudaStream_t s);
 // QuickInsert's insertion loop on the serial grid (one warp): bodies appended from index n0.
 struct QuickInsertArgs {
     uint32_t n0;         // bodies before the call
@@ -366,6 +416,10 @@ cudaError_t launch_tune_stream_poly(TuneJob* jobs, uint32_t n_jobs, const double
                                     cudaStream_t s);
 cudaError_t launch_tune_stream_poly2(bool sat, TuneJob* jobs, uint32_t n_jobs, const double4* verts, uint32_t nv,
                                      double rcut2, cudaStream_t s);
+// Sampler probe (hmc_sample_moves): n proposals from Counter(step, substep, seed).index(i) for a
+// body at the origin, identity orientation; zig: the context's tables (x then f).
+cudaError_t launch_sample_moves(int dim, uint32_t kind, double maximum, uint64_t step, uint32_t substep,
+                                uint32_t seed, uint64_t n, const double* zig, double* out, cudaStream_t s);
 // Injected moves: positions (n x 4 doubles), result decisions and recheck flags.
 cudaError_t launch_eval_sphere(int dim, bool fp32, const Geometry& g, const Arrays& a, const Pair& p,
                                const uint64_t* bodies, const double4* trial, uint32_t n, uint8_t* decisions,

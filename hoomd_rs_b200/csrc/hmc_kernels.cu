@@ -16,7 +16,9 @@
 // memory and their bodies form one contiguous range of the cell-ordered arrays.
 #include <cuda_runtime.h>
 
+#include <mutex>
 #include <type_traits>
+#include <unordered_map>
 
 #include "hmc_device.cuh"
 
@@ -358,8 +360,10 @@ __device__ __forceinline__ bool sphere_warp_recheck(const Geometry& g, const Arr
 // invisible to every other trial of the colour, as in the reference.
 // INJ: the probe mode (Injected): lane i takes injected trial i, runs the same decision code
 // and writes its decision instead of committing.
-template <int DIM, bool FP32, bool INJ = false>
-__global__ void __launch_bounds__(128, HMC_SWEEP_MIN_BLOCKS)
+// MINB: resident blocks per SM the pass is compiled for (its register cap), a launch variant
+// the autotuner chooses among.
+template <int DIM, bool FP32, bool INJ = false, int MINB = HMC_SWEEP_MIN_BLOCKS>
+__global__ void __launch_bounds__(128, MINB)
     k_sweep_sphere(Geometry g, Arrays A, Pair P, Launch L, Injected J) {
     if (L.early_wait) grid_dependency_wait();  // first pass: the rebuild's arrays are read at once
     uint32_t n_accepted = 0;
@@ -474,7 +478,7 @@ __global__ void __launch_bounds__(128, HMC_SWEEP_MIN_BLOCKS)
 #ifndef HMC_COOP_OWN_STEPS
 #define HMC_COOP_OWN_STEPS 2
 #endif
-constexpr uint32_t kOwnSteps = HMC_COOP_OWN_STEPS;
+constexpr int kOwnSteps = HMC_COOP_OWN_STEPS;
 constexpr int kFlagOverlap = 1, kFlagUncertain = 2, kFlagMore = 4;
 
 // Candidates k < k_end of every row range; returns kFlagOverlap, or kFlagUncertain and
@@ -514,8 +518,9 @@ __device__ __forceinline__ int sphere_rows_head(const Geometry& g, const Arrays&
     return flags;
 }
 
-template <int DIM, bool FP32, bool INJ = false>
-__global__ void __launch_bounds__(128, HMC_SWEEP_MIN_BLOCKS)
+// MINB (register cap) and OWN (candidates per row a lane tests itself) are launch variants.
+template <int DIM, bool FP32, bool INJ = false, int MINB = HMC_SWEEP_MIN_BLOCKS, int OWN = kOwnSteps>
+__global__ void __launch_bounds__(128, MINB)
     k_sweep_sphere_coop(Geometry g, Arrays A, Pair P, Launch L, Injected J) {
     constexpr int R = kRows<DIM>;
     constexpr int NR = 2 * R;  // row ranges plus, at a fast-axis end, the wrapped spaces
@@ -598,12 +603,12 @@ __global__ void __launch_bounds__(128, HMC_SWEEP_MIN_BLOCKS)
         grid_dependency_wait();  // the previous colour's moves are visible from here on
         allow_dependent_launch();
         if (trial) {
-            res = sphere_rows_head<DIM, FP32>(g, A, P, t, t32, (int)mf, k, a0, a1, kOwnSteps, st);
+            res = sphere_rows_head<DIM, FP32>(g, A, P, t, t32, (int)mf, k, a0, a1, (uint32_t)OWN, st);
             if (res != kFlagOverlap && (res & kFlagMore || edge)) {
                 // hand the rest to the warp: remaining row ranges, then the wrapped spaces
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
-                    s_lo[warp][lane][r] = a0[r] + kOwnSteps;
+                    s_lo[warp][lane][r] = a0[r] + (uint32_t)OWN;
                     s_hi[warp][lane][r] = a1[r];
                 }
                 if (edge) {
@@ -1210,8 +1215,8 @@ __device__ __forceinline__ void add_per_replica(unsigned long long* acc, uint32_
 }
 
 // One colour pass over all replicas that still run round `round` of this sweep.
-template <int DIM, bool FP32>
-__global__ void __launch_bounds__(128, HMC_BATCH_MIN_BLOCKS) k_sweep_batch(Batch B, Arrays A, uint32_t color,
+template <int DIM, bool FP32, int MINB = HMC_BATCH_MIN_BLOCKS>
+__global__ void __launch_bounds__(128, MINB) k_sweep_batch(Batch B, Arrays A, uint32_t color,
                                                                              uint32_t round, uint32_t early_wait) {
     if (early_wait) grid_dependency_wait();  // first pass: the rebuild's arrays are read at once
     const uint32_t n_active = active_count(A, color, round);
@@ -1592,33 +1597,23 @@ cudaError_t launch_rebuild_batch(int dim, const Batch& b, const Arrays& a, uint3
 }
 
 cudaError_t launch_sweep_batch(int dim, bool fp32, const Batch& b, const Arrays& a, uint32_t color, uint32_t round,
-                               uint32_t max_active, bool overlap_previous, bool early_wait, cudaStream_t s) {
+                               uint32_t max_active, bool overlap_previous, bool early_wait, cudaStream_t s,
+                               uint32_t variant) {
     if (max_active == 0) return cudaSuccess;
-    static int max_blocks[2][2] = {{0, 0}, {0, 0}};
-    int& mb = max_blocks[dim == 3][fp32];
-    if (mb == 0) {
-        int dev = 0, sms = 0, per_sm = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaError_t e;
-        if (dim == 2)
-            e = fp32 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_batch<2, true>, 128, 0)
-                     : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_batch<2, false>, 128, 0);
-        else
-            e = fp32 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_batch<3, true>, 128, 0)
-                     : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_batch<3, false>, 128, 0);
-        if (e != cudaSuccess) return e;
-        mb = sms * (per_sm > 0 ? per_sm : 1);
-    }
+    using BatchKernel = void (*)(Batch, Arrays, uint32_t, uint32_t, uint32_t);
+    // the compiled launch variants, in the order of kBatchShapes
+    static const BatchKernel kernels[2][2][3] = {
+        {{k_sweep_batch<2, false, 4>, k_sweep_batch<2, false, 3>, k_sweep_batch<2, false, 5>},
+         {k_sweep_batch<2, true, 4>, k_sweep_batch<2, true, 3>, k_sweep_batch<2, true, 5>}},
+        {{k_sweep_batch<3, false, 4>, k_sweep_batch<3, false, 3>, k_sweep_batch<3, false, 5>},
+         {k_sweep_batch<3, true, 4>, k_sweep_batch<3, true, 3>, k_sweep_batch<3, true, 5>}}};
+    const BatchKernel k = kernels[dim == 3][fp32][variant < 3 ? variant : 0];
     uint32_t grid = blocks_for(max_active, 128);
-    if (grid > (uint32_t)mb) grid = (uint32_t)mb;
+    const uint32_t wave = (uint32_t)resident_wave((const void*)k);
+    if (grid > wave) grid = wave;
     PassLaunch pl(grid, overlap_previous || early_wait, s);
     const uint32_t ew = early_wait ? 1u : 0u;
-    if (dim == 2)
-        return fp32 ? cudaLaunchKernelEx(&pl.cfg, k_sweep_batch<2, true>, b, a, color, round, ew)
-                    : cudaLaunchKernelEx(&pl.cfg, k_sweep_batch<2, false>, b, a, color, round, ew);
-    return fp32 ? cudaLaunchKernelEx(&pl.cfg, k_sweep_batch<3, true>, b, a, color, round, ew)
-                : cudaLaunchKernelEx(&pl.cfg, k_sweep_batch<3, false>, b, a, color, round, ew);
+    return cudaLaunchKernelEx(&pl.cfg, k, b, a, color, round, ew);
 }
 
 cudaError_t launch_batch_rounds(const Batch& b, Replica* rep, DeviceStats* stats, cudaStream_t s) {
@@ -1636,60 +1631,68 @@ cudaError_t launch_overlap_batch(int dim, const Batch& b, const Arrays& a, uint3
     return cudaGetLastError();
 }
 
+namespace {
+using SphereKernel = void (*)(Geometry, Arrays, Pair, Launch, Injected);
+
+// The compiled launch variants of the sphere passes, in the order of kSphereDirectShapes /
+// kSphereCoopShapes ([dim == 3][fp32][variant]).
+SphereKernel direct_kernel(int dim, bool fp32, uint32_t v) {
+    static const SphereKernel k[2][2][3] = {
+        {{k_sweep_sphere<2, false, false, 6>, k_sweep_sphere<2, false, false, 5>, k_sweep_sphere<2, false, false, 7>},
+         {k_sweep_sphere<2, true, false, 6>, k_sweep_sphere<2, true, false, 5>, k_sweep_sphere<2, true, false, 7>}},
+        {{k_sweep_sphere<3, false, false, 6>, k_sweep_sphere<3, false, false, 5>, k_sweep_sphere<3, false, false, 7>},
+         {k_sweep_sphere<3, true, false, 6>, k_sweep_sphere<3, true, false, 5>, k_sweep_sphere<3, true, false, 7>}}};
+    return k[dim == 3][fp32][v < 3 ? v : 0];
+}
+SphereKernel coop_kernel(int dim, bool fp32, uint32_t v) {
+    static const SphereKernel k[2][2][5] = {
+        {{k_sweep_sphere_coop<2, false, false, 6, 2>, k_sweep_sphere_coop<2, false, false, 6, 1>,
+          k_sweep_sphere_coop<2, false, false, 6, 3>, k_sweep_sphere_coop<2, false, false, 5, 2>,
+          k_sweep_sphere_coop<2, false, false, 7, 2>},
+         {k_sweep_sphere_coop<2, true, false, 6, 2>, k_sweep_sphere_coop<2, true, false, 6, 1>,
+          k_sweep_sphere_coop<2, true, false, 6, 3>, k_sweep_sphere_coop<2, true, false, 5, 2>,
+          k_sweep_sphere_coop<2, true, false, 7, 2>}},
+        {{k_sweep_sphere_coop<3, false, false, 6, 2>, k_sweep_sphere_coop<3, false, false, 6, 1>,
+          k_sweep_sphere_coop<3, false, false, 6, 3>, k_sweep_sphere_coop<3, false, false, 5, 2>,
+          k_sweep_sphere_coop<3, false, false, 7, 2>},
+         {k_sweep_sphere_coop<3, true, false, 6, 2>, k_sweep_sphere_coop<3, true, false, 6, 1>,
+          k_sweep_sphere_coop<3, true, false, 6, 3>, k_sweep_sphere_coop<3, true, false, 5, 2>,
+          k_sweep_sphere_coop<3, true, false, 7, 2>}}};
+    return k[dim == 3][fp32][v < 5 ? v : 0];
+}
+
+}  // namespace
+
+int resident_wave(const void* kernel) {
+    static std::mutex mu;
+    static std::unordered_map<const void*, int> cache;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const void* key = (const void*)((const char*)kernel + dev);  // one entry per kernel and device
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+    int sms = 0, per_sm = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 128, 0) != cudaSuccess) {
+        cudaGetLastError();
+        per_sm = 1;
+    }
+    const int wave = (sms > 0 ? sms : 1) * (per_sm > 0 ? per_sm : 1);
+    cache[key] = wave;
+    return wave;
+}
+
 cudaError_t launch_sweep_sphere(int dim, bool fp32, const Geometry& g, const Arrays& a, const Pair& p,
-                                const Launch& l, bool coop, cudaStream_t s) {
+                                const Launch& l, bool coop, cudaStream_t s, uint32_t variant) {
     if (l.n_active == 0) return cudaSuccess;  // no non-empty space of this colour
-    if (coop) {
-        static int coop_blocks[2][2] = {{0, 0}, {0, 0}};
-        int& cb = coop_blocks[dim == 3][fp32];
-        if (cb == 0) {
-            int dev = 0, sms = 0, per_sm = 0;
-            cudaGetDevice(&dev);
-            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-            cudaError_t e;
-            if (dim == 2)
-                e = fp32 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_sphere_coop<2, true>, 128, 0)
-                         : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_sphere_coop<2, false>, 128, 0);
-            else
-                e = fp32 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_sphere_coop<3, true>, 128, 0)
-                         : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_sphere_coop<3, false>, 128, 0);
-            if (e != cudaSuccess) return e;
-            cb = sms * (per_sm > 0 ? per_sm : 1);
-        }
-        uint32_t grid = blocks_for(l.n_active, 128);
-        if (grid > (uint32_t)cb) grid = (uint32_t)cb;
-        PassLaunch pl(grid, l.overlap_previous != 0 || l.early_wait != 0, s);
-        if (dim == 2)
-            return fp32 ? cudaLaunchKernelEx(&pl.cfg, k_sweep_sphere_coop<2, true>, g, a, p, l, Injected{})
-                        : cudaLaunchKernelEx(&pl.cfg, k_sweep_sphere_coop<2, false>, g, a, p, l, Injected{});
-        return fp32 ? cudaLaunchKernelEx(&pl.cfg, k_sweep_sphere_coop<3, true>, g, a, p, l, Injected{})
-                    : cudaLaunchKernelEx(&pl.cfg, k_sweep_sphere_coop<3, false>, g, a, p, l, Injected{});
-    }
-    // Grid-stride over the colour's list with at most one resident wave of blocks.
-    static int max_blocks[2][2] = {{0, 0}, {0, 0}};
-    int& mb = max_blocks[dim == 3][fp32];
-    if (mb == 0) {
-        int dev = 0, sms = 0, per_sm = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaError_t e;
-        if (dim == 2)
-            e = fp32 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_sphere<2, true>, 128, 0)
-                     : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_sphere<2, false>, 128, 0);
-        else
-            e = fp32 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_sphere<3, true>, 128, 0)
-                     : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_sphere<3, false>, 128, 0);
-        if (e != cudaSuccess) return e;
-        mb = sms * (per_sm > 0 ? per_sm : 1);
-    }
+    // grid-stride over the colour's list with at most one resident wave of blocks
+    const SphereKernel k = coop ? coop_kernel(dim, fp32, variant) : direct_kernel(dim, fp32, variant);
     uint32_t grid = blocks_for(l.n_active, 128);
-    if (grid > (uint32_t)mb) grid = (uint32_t)mb;
+    const uint32_t wave = (uint32_t)resident_wave((const void*)k);
+    if (grid > wave) grid = wave;
     PassLaunch pl(grid, l.overlap_previous != 0 || l.early_wait != 0, s);
-    if (dim == 2)
-        return fp32 ? cudaLaunchKernelEx(&pl.cfg, k_sweep_sphere<2, true>, g, a, p, l, Injected{})
-                    : cudaLaunchKernelEx(&pl.cfg, k_sweep_sphere<2, false>, g, a, p, l, Injected{});
-    return fp32 ? cudaLaunchKernelEx(&pl.cfg, k_sweep_sphere<3, true>, g, a, p, l, Injected{})
-                : cudaLaunchKernelEx(&pl.cfg, k_sweep_sphere<3, false>, g, a, p, l, Injected{});
+    return cudaLaunchKernelEx(&pl.cfg, k, g, a, p, l, Injected{});
 }
 
 cudaError_t launch_trials_sphere(int dim, bool fp32, bool coop, const Geometry& g, const Arrays& a, const Pair& p,

@@ -35,19 +35,6 @@ namespace {
 
 constexpr float kU32 = 5.9604645e-8f;  // 2^-24
 
-// Pair energy in FP64 exactly as the reference evaluates it: Isotropic::site_pair_energy
-// (isotropic.rs:147-156: r^2 >= r_cut^2 -> 0, else energy(sqrt(r^2))), Shifted::energy
-// (shifted.rs:92-94: f(r) - f(r_shift)), LennardJones::energy (lennard_jones.rs:107-111:
-// 4 eps ((sigma/r)^12 - (sigma/r)^6) with powi by repeated squaring).
-__device__ __forceinline__ double lj_pair64(const Pair& P, double r2) {
-    if (P.penalty) return penalty_pair64(P, r2);
-    if (r2 >= P.lj_rcut2) return 0.0;
-    const double r = dsqrt(r2);
-    const double sr = ddiv(P.lj_sigma, r);
-    const double s2 = dmul(sr, sr), s4 = dmul(s2, s2), s8 = dmul(s4, s4);
-    return dsub(dmul(P.lj_four_eps, dsub(dmul(s4, s8), dmul(s2, s4))), P.lj_e_shift);
-}
-
 // FP32 pair energy and a bound on its error against the exact energy of the FP64 sites, for
 // a pair with r2 below the band's upper end (the caller skips pairs outside the cut-off).
 // The r^2 error is bounded without a square root: sum |d_a| <= sqrt(3) r and
@@ -130,39 +117,6 @@ __device__ __forceinline__ void lj_energy64(const Geometry& g, const Arrays& A, 
     ea = warp_sum(a);
     eb = TWO ? warp_sum(b) : 0.0;
     mag = warp_sum(am);
-}
-
-// Whether another order of the same FP64 sums could change the Metropolis decision. The pair
-// energies are the same numbers in any order, and recursive summation of n terms in any order
-// (any summation tree) lies within gamma_{n-1} sum|e| of the exact sum, gamma_k = k u / (1 - k u),
-// u = 2^-53 (Higham, Accuracy and Stability of Numerical Algorithms, 2nd ed., 2002, section
-// 4.2). So dU = E_final - E_initial summed in any two orders (this pass's lanes and
-// butterfly, the reference's cell-list order) differ by at most
-// B = 2 gamma_{n-1} (sum|e_final| + sum|e_initial|) + 2 u |dU|. The decision (dU <= 0, else
-// u < exp(-dU / kT), parallel_sweep.rs:267-268) is monotone in dU: it is the same in every order
-// when dU - B and dU + B decide alike, with exp allowed 4 ulp either way (the reference calls
-// the platform libm, this pass CUDA's exp). n = the candidates of the stencil (>= the terms);
-// e0 = exp(-dU / kT) as the decision computed it. Over [dU - B, dU + B] exp(-x / kT) stays
-// within a factor exp(B / kT) <= 1 + 2 B / kT of e0 (B / kT < 1e-3), so a uniform farther than
-// e0 (4 B / kT + 1e-14) from e0 settles the trial without evaluating the ends.
-__device__ __forceinline__ double order_bound(double du, double mag, uint32_t n) {
-    const double unit = 1.1102230246251565e-16;  // 2^-53
-    const double k = (double)(n > 1u ? n - 1u : 1u);
-    const double gamma = k * unit / (1.0 - k * unit);
-    return 1.01 * (2.0 * gamma * mag + 2.0 * unit * fabs(du)) + 1e-300;
-}
-__device__ __forceinline__ bool order_ambiguous(double du, double mag, uint32_t n, double u, double kt, double e0) {
-    if (!isfinite(du) || !isfinite(mag)) return false;  // an infinite pair energy decides in any order
-    const double unit = 1.1102230246251565e-16;        // 2^-53
-    const double b = order_bound(du, mag, n);
-    const double lo = du - b, hi = du + b;
-    if (hi <= 0.0) return false;  // accepted in every order, without a uniform
-    const double rel = b / kt;
-    if (lo > 0.0 && rel < 1e-3 && fabs(u - e0) > e0 * (4.0 * rel + 1e-14)) return false;
-    const double ulp4 = 8.0 * unit;
-    const bool acc_at_lo = lo <= 0.0 || u < exp(-lo / kt) * (1.0 + ulp4);
-    const bool acc_at_hi = u < exp(-hi / kt) * (1.0 - ulp4);
-    return acc_at_lo != acc_at_hi;
 }
 
 struct Sums32 {
@@ -258,9 +212,8 @@ __device__ __forceinline__ void lj_inject(const Arrays& A, const Injected& J, ui
 }
 
 // The FP64 pass: one warp per trial. INJ: the probe mode (decisions instead of commits).
-template <int DIM, bool INJ = false>
-__global__ void __launch_bounds__(128, HMC_LJ_MIN_BLOCKS) k_sweep_lj(Geometry g, Arrays A, Pair P, Launch L,
-                                                                     Injected J) {
+template <int DIM, bool INJ = false, int MINB = HMC_LJ_MIN_BLOCKS>
+__global__ void __launch_bounds__(128, MINB) k_sweep_lj(Geometry g, Arrays A, Pair P, Launch L, Injected J) {
     if (L.early_wait) grid_dependency_wait();  // first pass: the rebuild's arrays are read at once
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -367,9 +320,8 @@ constexpr uint32_t kRecheckChunks = 8;  // 32-candidate chunks per shared-memory
 // same butterfly; an empty slot adds +0, which leaves a sum that starts at +0 unchanged). A
 // lone warp walking the stencil in FP64 would otherwise set the duration of a pass whose
 // trials all run in one wave.
-template <int DIM, bool INJ = false>
-__global__ void __launch_bounds__(128, HMC_LJ_MIN_BLOCKS) k_sweep_lj32(Geometry g, Arrays A, Pair P, Launch L,
-                                                                       Injected J) {
+template <int DIM, bool INJ = false, int MINB = HMC_LJ_MIN_BLOCKS>
+__global__ void __launch_bounds__(128, MINB) k_sweep_lj32(Geometry g, Arrays A, Pair P, Launch L, Injected J) {
     if (L.early_wait) grid_dependency_wait();  // first pass: the rebuild's arrays are read at once
     __shared__ double s_e[kRecheckChunks][2][32];
     __shared__ SharedTrial s_trial;
@@ -899,7 +851,7 @@ __global__ void k_energy_lj(Geometry g, Arrays A, Pair P, uint32_t n, double* ou
 }  // namespace
 
 cudaError_t launch_sweep_lj(int dim, bool fp32, const Geometry& g, const Arrays& a, const Pair& p, const Launch& l,
-                            cudaStream_t s) {
+                            cudaStream_t s, uint32_t variant) {
     if (l.n_active == 0) return cudaSuccess;
     static int max_blocks = 0;
     if (max_blocks == 0) {
@@ -911,11 +863,15 @@ cudaError_t launch_sweep_lj(int dim, bool fp32, const Geometry& g, const Arrays&
     uint32_t blocks = (l.n_active + 3) / 4;  // four warps (trials) per block
     if (blocks > (uint32_t)max_blocks) blocks = (uint32_t)max_blocks;
     PassLaunch pl(blocks, l.overlap_previous != 0 || l.early_wait != 0, s);
-    if (dim == 2)
-        return fp32 ? cudaLaunchKernelEx(&pl.cfg, k_sweep_lj32<2>, g, a, p, l, Injected{})
-                    : cudaLaunchKernelEx(&pl.cfg, k_sweep_lj<2>, g, a, p, l, Injected{});
-    return fp32 ? cudaLaunchKernelEx(&pl.cfg, k_sweep_lj32<3>, g, a, p, l, Injected{})
-                : cudaLaunchKernelEx(&pl.cfg, k_sweep_lj<3>, g, a, p, l, Injected{});
+    using LjKernel = void (*)(Geometry, Arrays, Pair, Launch, Injected);
+    // the compiled launch variants, in the order of kLjShapes ([dim == 3][fp32][variant])
+    static const LjKernel kernels[2][2][3] = {
+        {{k_sweep_lj<2, false, 9>, k_sweep_lj<2, false, 7>, k_sweep_lj<2, false, 11>},
+         {k_sweep_lj32<2, false, 9>, k_sweep_lj32<2, false, 7>, k_sweep_lj32<2, false, 11>}},
+        {{k_sweep_lj<3, false, 9>, k_sweep_lj<3, false, 7>, k_sweep_lj<3, false, 11>},
+         {k_sweep_lj32<3, false, 9>, k_sweep_lj32<3, false, 7>, k_sweep_lj32<3, false, 11>}}};
+    const LjKernel k = kernels[dim == 3][fp32][variant < 3 ? variant : 0];
+    return cudaLaunchKernelEx(&pl.cfg, k, g, a, p, l, Injected{});
 }
 
 cudaError_t launch_tune_stream_lj(int dim, TuneJob* jobs, uint32_t n_jobs, cudaStream_t s) {

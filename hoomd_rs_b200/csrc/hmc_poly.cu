@@ -17,7 +17,7 @@
 // decisions equal the FP64 pass.
 #include <cuda_runtime.h>
 
-#include "hmc_device.cuh"
+#include "hmc_serial.cuh"
 
 namespace hmc {
 namespace {
@@ -618,7 +618,122 @@ __global__ void __launch_bounds__(32) k_tune_stream_poly3(TuneJob* jobs, uint32_
         });
 }
 
+// Sweep::apply_with_filter (hoomd-mc/src/sweep.rs:159-224) for hard convex polyhedra: one trial
+// per body in index order from the one stream Counter(step, substep, seed).make_rng(), Translate
+// or Rotate<Versor>, accepted when no site of the serial grid's stencil overlaps it (dH is 0 or
+// infinite: no uniform is drawn); one warp, a lane per stencil cell, as for spheres. The pair
+// tests read each body's versor by body index.
+__global__ void __launch_bounds__(32) k_serial_poly3(Geometry g, Arrays A, SerialGrid G, PolyShape sh, Launch L,
+                                                     uint32_t rotate, const uint8_t* __restrict__ mask) {
+    const uint32_t lane = threadIdx.x;
+    if (A.stats->error_flags) return;
+    Arrays Ab = A;
+    Ab.sorted_q = A.body_ori;
+    Sfc64 rng = make_rng(L.step, L.substep, L.seed, 0);
+    uint64_t accepted = 0;
+    for (uint32_t b = 0; b < L.n_bodies; ++b) {
+        if (mask && !mask[b]) continue;
+        const double4 b4 = A.body_pos[b];
+        double x[3] = {b4.x, b4.y, b4.z};
+        const double4 q4 = A.body_ori[b];
+        Q qi{q4.x, q4.y, q4.z, q4.w};
+        if (rotate) {
+            qi = versor_move(rng, L.max_move, A.zig_x, A.zig_f, qi);
+        } else {
+            double dv[3];
+            ball_sample<3>(rng, L.max_move, A.zig_x, A.zig_f, dv);
+            for (int a = 0; a < 3; ++a) x[a] = dadd(x[a], dv[a]);
+        }
+        wrap_inv<3>(g.L, g.invL, x);  // W1 = wrap(propose(..))
+        double t[3] = {x[0], x[1], x[2]};
+        wrap_inv<3>(g.L, g.invL, t);  // the trial site T = wrap(W1)
+        uint32_t m[3] = {0, 0, 0}, cell;
+        serial_cell<3>(g, G, t, m);
+        bool overlap = false;
+        if (lane_cell<3>(G, m, lane, &cell)) {
+            const uint32_t cnt = G.size[cell];
+            for (uint32_t k = 0; k < cnt && !overlap; ++k) {
+                const uint32_t j = G.items[(size_t)cell * G.cap + k];
+                if (j == b) continue;
+                const double4 s4 = G.site[j];
+                const double sv[3] = {s4.x, s4.y, s4.z};
+                overlap = poly_overlap64(g, Ab, sh.verts, sh.nv, sh.rcut2, t, qi, sv, j);
+            }
+        }
+        if (__any_sync(0xffffffffu, overlap)) continue;
+        accepted++;
+        if (lane == 0) {
+            // update_body_properties: body = wrap(W1) = T, site = wrap(body), versor as proposed
+            double sv[3] = {t[0], t[1], t[2]};
+            wrap_inv<3>(g.L, g.invL, sv);
+            A.body_pos[b] = make_double4(t[0], t[1], t[2], 0.0);
+            A.body_ori[b] = make_double4(qi.s, qi.x, qi.y, qi.z);
+            G.site[b] = make_double4(sv[0], sv[1], sv[2], 0.0);
+            serial_move<3>(g, G, A, b, sv);
+        }
+        __syncwarp();
+        if (A.stats->error_flags) break;
+    }
+    if (lane == 0) {
+        A.stats->accepted = accepted;
+        A.stats->rechecks = 0;
+    }
+}
+
+// Proposals for a body at the origin with the identity orientation, proposal i from
+// Counter(step, substep, seed).index(i): kind 0 Translate (the displacement), kind 1 Rotate
+// (3-D: the versor; 2-D: the angle), kind 2 one StandardNormal draw.
+template <int DIM>
+__global__ void k_sample_moves(Launch L, uint32_t kind, uint64_t n, const double* zx, const double* zf, double* out) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Sfc64 rng = make_rng(L.step, L.substep, L.seed, i);
+    if (kind == 2) {
+        out[i] = standard_normal(rng, zx, zf);
+    } else if (kind == 0) {
+        double dv[3];
+        ball_sample<DIM>(rng, L.max_move, zx, zf, dv);
+        for (int a = 0; a < DIM; ++a) out[i * DIM + a] = dv[a];
+    } else if (DIM == 3) {
+        const Q q = versor_move(rng, L.max_move, zx, zf, Q{1.0, 0.0, 0.0, 0.0});
+        out[i * 4 + 0] = q.s;
+        out[i * 4 + 1] = q.x;
+        out[i * 4 + 2] = q.y;
+        out[i * 4 + 3] = q.z;
+    } else {
+        const double u = dsub(as_double(0x3FF0000000000000ULL | (rng.next_u64() >> 12)), 1.0);
+        out[i] = dadd(0.0, dadd(dmul(u, dsub(L.max_move, -L.max_move)), -L.max_move));
+    }
+}
+
 }  // namespace
+
+cudaError_t launch_sample_moves(int dim, uint32_t kind, double maximum, uint64_t step, uint32_t substep,
+                                uint32_t seed, uint64_t n, const double* zig, double* out, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    Launch l{};
+    l.step = step;
+    l.substep = substep;
+    l.seed = seed;
+    l.max_move = maximum;
+    const uint32_t blocks = (uint32_t)((n + 127) / 128);
+    if (dim == 2)
+        k_sample_moves<2><<<blocks, 128, 0, s>>>(l, kind, n, zig, zig + kZigLayers + 1, out);
+    else
+        k_sample_moves<3><<<blocks, 128, 0, s>>>(l, kind, n, zig, zig + kZigLayers + 1, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_serial_poly(const Geometry& g, const Arrays& a, const double4* verts, uint32_t nv, double rcut2,
+                               const Launch& l, bool rotate, const uint32_t* nc, const double* w, uint32_t cap,
+                               uint32_t* size, uint32_t* items, uint32_t* cell_of, double4* site, const uint8_t* mask,
+                               cudaStream_t s) {
+    const SerialGrid G = make_grid(3, nc, w, cap, size, items, cell_of, site);
+    cudaError_t e = build_grid(3, g, a, G, l.n_bodies, s);
+    if (e != cudaSuccess || l.n_bodies == 0) return e;
+    k_serial_poly3<<<1, 32, 0, s>>>(g, a, G, PolyShape{verts, nv, rcut2, 0.f}, l, rotate ? 1u : 0u, mask);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_tune_stream_poly(TuneJob* jobs, uint32_t n_jobs, const double4* verts, uint32_t nv, double rcut2,
                                     cudaStream_t s) {
@@ -628,7 +743,8 @@ cudaError_t launch_tune_stream_poly(TuneJob* jobs, uint32_t n_jobs, const double
 }
 
 cudaError_t launch_sweep_poly(bool fp32, const Geometry& g, const Arrays& a, const double4* verts, uint32_t nv,
-                              double rcut2, float rcut2_hi32, const Launch& l, bool rotate, cudaStream_t s) {
+                              double rcut2, float rcut2_hi32, const Launch& l, bool rotate, cudaStream_t s,
+                              uint32_t variant) {
     if (l.n_active == 0) return cudaSuccess;
     static int max_blocks = 0;
     if (max_blocks == 0) {
@@ -638,15 +754,18 @@ cudaError_t launch_sweep_poly(bool fp32, const Geometry& g, const Arrays& a, con
         max_blocks = sms * 16;
     }
     PolyShape sh{verts, nv, rcut2, rcut2_hi32};
-    const uint32_t per_block = 4u * kPolyTrialsPerWarp;  // four warps per block
+    const uint32_t per_block = 4u * kPolyShapes[variant < 3 ? variant : 0].trials_per_warp;  // four warps per block
     uint32_t blocks = (l.n_active + per_block - 1) / per_block;
     if (blocks > (uint32_t)max_blocks) blocks = (uint32_t)max_blocks;
     PassLaunch pl(blocks, l.overlap_previous != 0 || l.early_wait != 0, s);
     const uint32_t rot = rotate ? 1u : 0u;
-    return fp32 ? cudaLaunchKernelEx(&pl.cfg, k_sweep_poly3_packed<true, kPolyTrialsPerWarp>, g, a, sh, l, rot,
-                                     Injected{})
-                : cudaLaunchKernelEx(&pl.cfg, k_sweep_poly3_packed<false, kPolyTrialsPerWarp>, g, a, sh, l, rot,
-                                     Injected{});
+    using PolyKernel = void (*)(Geometry, Arrays, PolyShape, Launch, uint32_t, Injected);
+    // the compiled launch variants, in the order of kPolyShapes (trials per warp 4, 2, 8)
+    static const PolyKernel kernels[2][3] = {
+        {k_sweep_poly3_packed<false, 4>, k_sweep_poly3_packed<false, 2>, k_sweep_poly3_packed<false, 8>},
+        {k_sweep_poly3_packed<true, 4>, k_sweep_poly3_packed<true, 2>, k_sweep_poly3_packed<true, 8>}};
+    const uint32_t v = variant < 3 ? variant : 0;
+    return cudaLaunchKernelEx(&pl.cfg, kernels[fp32][v], g, a, sh, l, rot, Injected{});
 }
 
 cudaError_t launch_trials_poly(bool fp32, const Geometry& g, const Arrays& a, const double4* verts, uint32_t nv,

@@ -16,7 +16,7 @@
 // than the FP32 error bound are skipped; every other candidate runs the FP64 test.
 #include <cuda_runtime.h>
 
-#include "hmc_device.cuh"
+#include "hmc_serial.cuh"
 
 namespace hmc {
 namespace {
@@ -459,6 +459,71 @@ __global__ void __launch_bounds__(32) k_tune_stream_poly2(TuneJob* jobs, uint32_
     if (range_error) atomicOr(&J.a.stats->error_flags, kErrAngleRange);
 }
 
+// Sweep::apply_with_filter (hoomd-mc/src/sweep.rs:159-224) for hard convex polygons: one trial per
+// body in index order from one stream, Translate or Rotate<Angle>, accepted when no site of the
+// serial grid's stencil overlaps it (no uniform is drawn); one warp, a lane per stencil cell. The
+// pair tests read each body's angle by body index.
+template <bool SAT>
+__global__ void __launch_bounds__(32) k_serial_poly2(Geometry g, Arrays A, SerialGrid G, PolyShape2 sh, Launch L,
+                                                     uint32_t rotate, const uint8_t* __restrict__ mask) {
+    const uint32_t lane = threadIdx.x;
+    if (A.stats->error_flags) return;
+    Arrays Ab = A;
+    Ab.sorted_q = A.body_ori;
+    bool range_error = false;
+    Sfc64 rng = make_rng(L.step, L.substep, L.seed, 0);
+    uint64_t accepted = 0;
+    for (uint32_t b = 0; b < L.n_bodies; ++b) {
+        if (mask && !mask[b]) continue;
+        const double4 b4 = A.body_pos[b];
+        double x[3] = {b4.x, b4.y, 0.0};
+        double ti = A.body_ori[b].x;
+        if (rotate) {
+            // Rotate<Angle>::propose (rotate/angle.rs:46-55): theta += Uniform(-a, a)
+            const double u = dsub(as_double(0x3FF0000000000000ULL | (rng.next_u64() >> 12)), 1.0);
+            ti = dadd(ti, dadd(dmul(u, dsub(L.max_move, -L.max_move)), -L.max_move));
+        } else {
+            double dv[3];
+            ball_sample<2>(rng, L.max_move, A.zig_x, A.zig_f, dv);
+            x[0] = dadd(x[0], dv[0]);
+            x[1] = dadd(x[1], dv[1]);
+        }
+        wrap_inv<2>(g.L, g.invL, x);  // W1 = wrap(propose(..))
+        double t[3] = {x[0], x[1], 0.0};
+        wrap_inv<2>(g.L, g.invL, t);  // the trial site T = wrap(W1)
+        uint32_t m[3] = {0, 0, 0}, cell;
+        serial_cell<2>(g, G, t, m);
+        bool overlap = false;
+        if (lane_cell<2>(G, m, lane, &cell)) {
+            const uint32_t cnt = G.size[cell];
+            for (uint32_t k = 0; k < cnt && !overlap; ++k) {
+                const uint32_t j = G.items[(size_t)cell * G.cap + k];
+                if (j == b) continue;
+                const double4 s4 = G.site[j];
+                const double sv[3] = {s4.x, s4.y, 0.0};
+                overlap = poly2_overlap64<SAT>(g, Ab, sh, t, ti, sv, j, &range_error);
+            }
+        }
+        if (__any_sync(0xffffffffu, overlap)) continue;
+        accepted++;
+        if (lane == 0) {
+            double sv[3] = {t[0], t[1], 0.0};
+            wrap_inv<2>(g.L, g.invL, sv);
+            A.body_pos[b] = make_double4(t[0], t[1], 0.0, 0.0);
+            A.body_ori[b].x = ti;
+            G.site[b] = make_double4(sv[0], sv[1], 0.0, 0.0);
+            serial_move<2>(g, G, A, b, sv);
+        }
+        __syncwarp();
+        if (A.stats->error_flags) break;
+    }
+    if (range_error) atomicOr(&A.stats->error_flags, kErrAngleRange);
+    if (lane == 0) {
+        A.stats->accepted = accepted;
+        A.stats->rechecks = 0;
+    }
+}
+
 // Overlapping pairs (i < j), FP64 (the overlap check of total_energy).
 template <bool SAT>
 __global__ void k_overlap_poly2(Geometry g, Arrays A, PolyShape2 sh, uint32_t n) {
@@ -524,6 +589,21 @@ cudaError_t launch_sweep_poly2(bool fp32, bool sat, const Geometry& g, const Arr
                    : cudaLaunchKernelEx(&pl.cfg, k_sweep_poly2<true, false>, g, a, sh, l, rot);
     return sat ? cudaLaunchKernelEx(&pl.cfg, k_sweep_poly2<false, true>, g, a, sh, l, rot)
                : cudaLaunchKernelEx(&pl.cfg, k_sweep_poly2<false, false>, g, a, sh, l, rot);
+}
+
+cudaError_t launch_serial_poly2(bool sat, const Geometry& g, const Arrays& a, const double4* verts, uint32_t nv,
+                                double rcut2, const Launch& l, bool rotate, const uint32_t* nc, const double* w,
+                                uint32_t cap, uint32_t* size, uint32_t* items, uint32_t* cell_of, double4* site,
+                                const uint8_t* mask, cudaStream_t s) {
+    const SerialGrid G = make_grid(2, nc, w, cap, size, items, cell_of, site);
+    cudaError_t e = build_grid(2, g, a, G, l.n_bodies, s);
+    if (e != cudaSuccess || l.n_bodies == 0) return e;
+    const PolyShape2 sh{verts, nv, rcut2, 0.f};
+    if (sat)
+        k_serial_poly2<true><<<1, 32, 0, s>>>(g, a, G, sh, l, rotate ? 1u : 0u, mask);
+    else
+        k_serial_poly2<false><<<1, 32, 0, s>>>(g, a, G, sh, l, rotate ? 1u : 0u, mask);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_tune_stream_poly2(bool sat, TuneJob* jobs, uint32_t n_jobs, const double4* verts, uint32_t nv,

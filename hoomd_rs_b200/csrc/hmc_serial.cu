@@ -8,38 +8,10 @@
 // is the exact serial Markov chain on the device, not a fast path: the checkerboard sweep is.
 #include <cuda_runtime.h>
 
-#include "hmc_device.cuh"
+#include "hmc_serial.cuh"
 
 namespace hmc {
 namespace {
-
-struct SerialGrid {
-    uint32_t nc[3];      // cells per axis (>= 1)
-    double w[3];         // cell width L / nc (>= the diameter when nc >= 3 on that axis)
-    uint32_t n_cells;
-    uint32_t cap;        // bodies a cell holds
-    uint32_t* size;      // [n_cells]
-    uint32_t* items;     // [n_cells * cap]
-    uint32_t* cell_of;   // [n] cell of each body's site
-    double4* site;       // [n] S = wrap(B)
-};
-
-template <int DIM>
-__device__ __forceinline__ void serial_cell(const Geometry& g, const SerialGrid& G, const double* s, uint32_t* m) {
-#pragma unroll
-    for (int a = 0; a < DIM; ++a) {
-        double f = floor(ddiv(dadd(s[a], g.half[a]), G.w[a]));
-        uint32_t i = f > 0.0 ? (uint32_t)f : 0u;
-        m[a] = i < G.nc[a] ? i : G.nc[a] - 1u;
-    }
-}
-template <int DIM>
-__device__ __forceinline__ uint32_t serial_index(const SerialGrid& G, const uint32_t* m) {
-    uint32_t c = 0;
-#pragma unroll
-    for (int a = 0; a < DIM; ++a) c = c * G.nc[a] + m[a];
-    return c;
-}
 
 // Body tags (the tagged container of hoomd-microstate/src/microstate.rs:60-123): a new body
 // takes the smallest free tag (a min-heap of freed tags), else the next unused one; removal
@@ -101,92 +73,38 @@ __device__ void grid_append(const Geometry& g, const Arrays& A, const SerialGrid
     if (T.tag) T.tag[n] = tag_take(T);
 }
 
-// Sites and cell lists from the body positions (one thread per body).
-template <int DIM>
-__global__ void k_serial_build(Geometry g, Arrays A, SerialGrid G, uint32_t n) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const double4 b = A.body_pos[i];
-    double s[3] = {b.x, b.y, b.z};
-    wrap_inv<DIM>(g.L, g.invL, s);
-    G.site[i] = make_double4(s[0], s[1], s[2], 0.0);
-    uint32_t m[3] = {0, 0, 0};
-    serial_cell<DIM>(g, G, s, m);
-    const uint32_t c = serial_index<DIM>(G, m);
-    G.cell_of[i] = c;
-    const uint32_t k = atomicAdd(G.size + c, 1u);
-    if (k < G.cap)
-        G.items[(size_t)c * G.cap + k] = i;
-    else
-        atomicOr(&A.stats->error_flags, kErrCellOverflow);
-}
-
-// This lane's stencil cell around multi-index m (radix decomposition over the distinct cells of
-// each axis); false when the lane has none.
-template <int DIM>
-__device__ __forceinline__ bool lane_cell(const SerialGrid& G, const uint32_t* m, uint32_t lane, uint32_t* cell) {
-    uint32_t len[3] = {1, 1, 1}, off[3] = {0, 0, 0}, rem = lane;
-#pragma unroll
-    for (int a = 0; a < DIM; ++a) len[a] = G.nc[a] >= 3 ? 3u : G.nc[a];
-#pragma unroll
-    for (int a = DIM - 1; a >= 0; --a) {
-        off[a] = rem % len[a];
-        rem /= len[a];
-    }
-    uint32_t c[3] = {0, 0, 0};
-#pragma unroll
-    for (int a = 0; a < DIM; ++a) c[a] = G.nc[a] >= 3 ? wrap_index((int)m[a] + (int)off[a] - 1, G.nc[a]) : off[a];
-    *cell = serial_index<DIM>(G, c);
-    return rem == 0;
-}
-
-// Soft pair energy of site t against every site of the stencil around t's cell except body
-// `self`: per-lane sums over the lane's cell, then a butterfly reduction (all lanes agree).
+// Soft pair energy (Lennard-Jones or the overlap penalty) of site t against every site of the
+// stencil around t's cell except body `self`: per-lane sums over the lane's cell, then a
+// butterfly reduction (all lanes agree). mag += sum |e|, terms += the sites visited (for
+// order_ambiguous).
 template <int DIM>
 __device__ __forceinline__ double serial_energy(const Geometry& g, const SerialGrid& G, const Pair& P, const double* t,
-                                                uint32_t self, uint32_t lane) {
+                                                uint32_t self, uint32_t lane, double& mag, uint32_t& terms) {
     uint32_t m[3] = {0, 0, 0}, cell;
     serial_cell<DIM>(g, G, t, m);
-    double e = 0.0;
+    double e = 0.0, am = 0.0;
+    uint32_t cnt = 0;
     if (lane_cell<DIM>(G, m, lane, &cell)) {
-        const uint32_t cnt = G.size[cell];
+        cnt = G.size[cell];
         for (uint32_t k = 0; k < cnt; ++k) {
             const uint32_t j = G.items[(size_t)cell * G.cap + k];
             if (j == self) continue;
             const double4 s4 = G.site[j];
             const double sv[3] = {s4.x, s4.y, s4.z};
-            e = dadd(e, penalty_pair64(P, ref_dist2<DIM>(g, t, sv)));
+            const double x = lj_pair64(P, ref_dist2<DIM>(g, t, sv));
+            e = dadd(e, x);
+            am += fabs(x);
         }
     }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) e = dadd(e, __shfl_xor_sync(0xffffffffu, e, o));
-    return e;
-}
-
-// Move body b's site into the cell of sv (lane 0 only): the last item of the old cell takes
-// b's slot there (swap_remove), b is appended to the new cell.
-template <int DIM>
-__device__ __forceinline__ void serial_move(const Geometry& g, const SerialGrid& G, const Arrays& A, uint32_t b,
-                                            const double* sv) {
-    uint32_t ms[3] = {0, 0, 0};
-    serial_cell<DIM>(g, G, sv, ms);
-    const uint32_t nc = serial_index<DIM>(G, ms), oc = G.cell_of[b];
-    if (nc == oc) return;
-    const uint32_t osz = G.size[oc];
-    for (uint32_t k = 0; k < osz; ++k)
-        if (G.items[(size_t)oc * G.cap + k] == b) {
-            G.items[(size_t)oc * G.cap + k] = G.items[(size_t)oc * G.cap + osz - 1];
-            break;
-        }
-    G.size[oc] = osz - 1;
-    const uint32_t nsz = G.size[nc];
-    if (nsz < G.cap) {
-        G.items[(size_t)nc * G.cap + nsz] = b;
-        G.size[nc] = nsz + 1;
-    } else {
-        atomicOr(&A.stats->error_flags, kErrCellOverflow);
+    for (int o = 16; o > 0; o >>= 1) {
+        e = dadd(e, __shfl_xor_sync(0xffffffffu, e, o));
+        am += __shfl_xor_sync(0xffffffffu, am, o);
+        cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
     }
-    G.cell_of[b] = nc;
+    mag += am;
+    terms += cnt;
+    return e;
 }
 
 // SOFT = false: hard spheres (the trial is rejected on any overlap, no uniform is drawn).
@@ -198,7 +116,7 @@ __global__ void __launch_bounds__(32) k_serial_sphere(Geometry g, Arrays A, Seri
     const uint32_t lane = threadIdx.x;
     if (A.stats->error_flags) return;
     Sfc64 rng = make_rng(L.step, L.substep, L.seed, 0);
-    uint64_t accepted = 0;
+    uint64_t accepted = 0, ambiguous = 0;
     for (uint32_t b = 0; b < L.n_bodies; ++b) {
         if (mask && !mask[b]) continue;
         const double4 b4 = A.body_pos[b];
@@ -211,14 +129,26 @@ __global__ void __launch_bounds__(32) k_serial_sphere(Geometry g, Arrays A, Seri
         double t[3] = {x[0], x[1], DIM == 3 ? x[2] : 0.0};
         wrap_inv<DIM>(g.L, g.invL, t);  // delta_energy_one wraps the site: T = wrap(W1)
         if (SOFT) {
-            const double ef = serial_energy<DIM>(g, G, P, t, b, lane);
+            double mag = 0.0;
+            uint32_t terms = 0;
+            const double ef = serial_energy<DIM>(g, G, P, t, b, lane, mag, terms);
             if (ef == __longlong_as_double(0x7ff0000000000000ll)) continue;  // early infinity
             const double4 s4 = G.site[b];
             const double si[3] = {s4.x, s4.y, s4.z};
-            const double dh = dsub(ef, serial_energy<DIM>(g, G, P, si, b, lane));
-            if (!(dh != __longlong_as_double(0x7ff0000000000000ll) &&
-                  (dh <= 0.0 || uniform01(rng) < exp(ddiv(-dh, L.kt)))))
-                continue;
+            const double dh = dsub(ef, serial_energy<DIM>(g, G, P, si, b, lane, mag, terms));
+            if (!(dh != __longlong_as_double(0x7ff0000000000000ll))) continue;
+            bool acc;
+            if (dh <= 0.0) {
+                // another summation order could give dH > 0, draw a uniform and change the stream
+                if (isfinite(mag) && dh + order_bound(dh, mag, terms) > 0.0) ambiguous++;
+                acc = true;
+            } else {
+                const double u = uniform01(rng);
+                const double e0 = exp(ddiv(-dh, L.kt));
+                if (order_ambiguous(dh, mag, terms, u, L.kt, e0)) ambiguous++;
+                acc = u < e0;
+            }
+            if (!acc) continue;
         } else {
             uint32_t m[3] = {0, 0, 0}, cell;
             serial_cell<DIM>(g, G, t, m);
@@ -250,6 +180,7 @@ __global__ void __launch_bounds__(32) k_serial_sphere(Geometry g, Arrays A, Seri
     if (lane == 0) {
         A.stats->accepted = accepted;
         A.stats->rechecks = 0;
+        A.stats->ambiguous = ambiguous;
     }
 }
 
@@ -328,7 +259,9 @@ __global__ void __launch_bounds__(32) k_quick_insert(Geometry g, Arrays A, Seria
 template <int DIM>
 __device__ __forceinline__ double insert_energy(const Geometry& g, const SerialGrid& G, const Pair& P,
                                                 const double* t, bool soft, uint32_t lane) {
-    if (soft) return serial_energy<DIM>(g, G, P, t, 0xffffffffu, lane);
+    double mag = 0.0;
+    uint32_t terms = 0;
+    if (soft) return serial_energy<DIM>(g, G, P, t, 0xffffffffu, lane, mag, terms);
     uint32_t m[3] = {0, 0, 0}, cell;
     serial_cell<DIM>(g, G, t, m);
     bool overlap = false;
@@ -394,7 +327,9 @@ __global__ void __launch_bounds__(32) k_grand_canonical(Geometry g, Arrays A, Se
             if (q.soft) {
                 const double4 s4 = G.site[idx];
                 const double si[3] = {s4.x, s4.y, s4.z};
-                e_initial = serial_energy<DIM>(g, G, P, si, idx, lane);
+                double mag = 0.0;
+                uint32_t terms = 0;
+                e_initial = serial_energy<DIM>(g, G, P, si, idx, lane, mag, terms);
             }
             const double de = -e_initial;  // delta_energy_remove
             const double p = q.fugacity <= 0.0
@@ -448,33 +383,6 @@ __global__ void __launch_bounds__(32) k_grand_canonical(Geometry g, Arrays A, Se
 }  // namespace
 
 namespace {
-SerialGrid make_grid(int dim, const uint32_t* nc, const double* w, uint32_t cap, uint32_t* size, uint32_t* items,
-                     uint32_t* cell_of, double4* site) {
-    SerialGrid G{};
-    uint64_t cells = 1;
-    for (int k = 0; k < 3; ++k) {
-        G.nc[k] = k < dim ? nc[k] : 1u;
-        G.w[k] = k < dim ? w[k] : 1.0;
-        cells *= G.nc[k];
-    }
-    G.n_cells = (uint32_t)cells;
-    G.cap = cap;
-    G.size = size;
-    G.items = items;
-    G.cell_of = cell_of;
-    G.site = site;
-    return G;
-}
-
-cudaError_t build_grid(int dim, const Geometry& g, const Arrays& a, const SerialGrid& G, uint32_t n, cudaStream_t s) {
-    cudaError_t e = cudaMemsetAsync(G.size, 0, sizeof(uint32_t) * G.n_cells, s);
-    if (e != cudaSuccess || n == 0) return e;
-    if (dim == 2)
-        k_serial_build<2><<<(n + 255) / 256, 256, 0, s>>>(g, a, G, n);
-    else
-        k_serial_build<3><<<(n + 255) / 256, 256, 0, s>>>(g, a, G, n);
-    return cudaGetLastError();
-}
 }  // namespace
 
 cudaError_t launch_serial_sphere(int dim, bool soft, const Geometry& g, const Arrays& a, const Pair& p,

@@ -89,6 +89,7 @@ typedef enum hmc_precision {
 
 typedef struct hmc_context hmc_context;
 typedef struct hmc_system hmc_system;
+typedef struct hmc_batch hmc_batch;
 
 typedef struct hmc_device_opts {
     uint32_t struct_size; /* sizeof(hmc_device_opts) */
@@ -231,6 +232,36 @@ hmc_status hmc_eval_trials(hmc_system* sys, const hmc_injected_move* moves, uint
  * order); +infinity or 0 for hard shapes (any overlap / none). */
 hmc_status hmc_total_energy(hmc_system* sys, double* energy);
 
+/* ---- launch variants and the autotuner (no counterpart in the reference) ----
+ * Every colour-pass kernel is compiled in a few launch shapes: the resident blocks per SM it
+ * is built for (its register cap), the trials a warp takes (convex polyhedra: 4, 2 or 8) and,
+ * for the warp-cooperative FP64 sphere pass, the candidates per stencil row a lane tests before
+ * handing the rest to its warp. All make the same pair tests, so the trajectory is the same in
+ * every variant; only the speed differs, by shape and density. hmc_autotune times `sweeps`
+ * sweeps of the system in every variant of its pass (precision and move from params), each from
+ * the same saved state, keeps the fastest for this system and records it for every system and
+ * batch of the process with the same pass, dimension, precision and density band (bodies per
+ * checkerboard space, in quarter octaves); the state and counter are restored afterwards. A
+ * system without its own choice uses the recorded one for its band, else variant 0. */
+typedef struct hmc_launch_variant {
+    uint32_t index;            /* in the variant table of the system's pass for this precision */
+    uint32_t count;            /* variants in that table */
+    uint32_t blocks_per_sm;    /* resident blocks per SM the kernel is compiled for */
+    uint32_t trials_per_warp;  /* trials one warp takes at once (1: a lane or a warp per trial) */
+    uint32_t own_steps;        /* warp-cooperative sphere pass: candidates per row a lane tests */
+} hmc_launch_variant;
+/* index UINT32_MAX: the variant the next hmc_sweep in this precision runs. */
+hmc_status hmc_get_launch_variant(hmc_system* sys, uint32_t precision, uint32_t index, hmc_launch_variant* out);
+/* index UINT32_MAX: drop the system's own choice (the recorded one for its band, else 0). */
+hmc_status hmc_set_launch_variant(hmc_system* sys, uint32_t precision, uint32_t index);
+/* ms_per_sweep (may be NULL): chosen->count entries, the mean time of one sweep per variant. */
+hmc_status hmc_autotune(hmc_system* sys, const hmc_sweep_params* params, uint32_t sweeps, hmc_launch_variant* chosen,
+                        double* ms_per_sweep);
+/* The same for a batch's replica pass (params: one per replica, as hmc_batch_sweep). */
+hmc_status hmc_batch_autotune(hmc_batch* batch, const hmc_sweep_params* params, uint32_t sweeps,
+                              hmc_launch_variant* chosen, double* ms_per_sweep);
+hmc_status hmc_batch_set_launch_variant(hmc_batch* batch, uint32_t precision, uint32_t index);
+
 /* ---- overlap count into caller buffers, with no device allocation ----
  * No counterpart in the reference (hoomd-rs has no GPU path); it serves callers that must
  * not call cudaMalloc when they run the check, for example a framework that hands out all
@@ -280,7 +311,6 @@ hmc_status hmc_gr(hmc_system* sys, double r_max, uint32_t n_bins, uint64_t* coun
  * replicas. Every replica's trajectory is the one hmc_system would produce from the same
  * description. The reference has no counterpart (a user would loop over Microstates, each
  * with its own ParallelSweep::apply, hoomd-mc/src/parallel_sweep.rs:390-421). */
-typedef struct hmc_batch hmc_batch;
 /* positions[k]: descs[k].n_bodies * dim doubles. All replicas share dim and the interaction:
  * HMC_HARD_SPHERE, or HMC_LENNARD_JONES (each replica with its own epsilon, sigma, r_cut,
  * r_shift). */
@@ -315,6 +345,16 @@ uint64_t hmc_batch_kernel_launches(hmc_batch* batch);
  * no counterpart in the reference, which calls the platform libm (hoomd-vector angle.rs:120-150).
  * HMC_INVALID_ARGUMENT when some |x[i]| >= 2^20. */
 hmc_status hmc_math_sincos(hmc_context* ctx, const double* x, uint64_t n, double* sin_out, double* cos_out);
+
+/* The trial-move samplers on the device, as a probe (no counterpart in the reference, which tests
+ * its samplers statistically: translate/cartesian.rs:65-100, rotate/versor.rs:151-184,
+ * rotate/angle.rs:83-119). Sample i is drawn from Counter(step, substep, seed).index(i) for a
+ * body at the origin with the identity orientation: kind 0 = Translate<Cartesian<dim>> with
+ * maximum distance `maximum` (out: dim doubles, the displacement); kind 1 = Rotate with maximum
+ * rotation `maximum` (3-D: the proposed versor, 4 doubles s, x, y, z; 2-D: the angle, 1 double);
+ * kind 2 = one StandardNormal draw (1 double; `maximum` ignored). */
+hmc_status hmc_sample_moves(hmc_context* ctx, uint32_t dim, uint32_t kind, double maximum, uint64_t step,
+                            uint32_t substep, uint32_t seed, uint64_t n, double* out);
 
 hmc_status hmc_profile_enable(hmc_system* sys, int enable);
 hmc_status hmc_profile_read(hmc_system* sys, hmc_profile* out, int reset);

@@ -118,6 +118,9 @@ def lib():
         L.oracle_tune_stream.argtypes = [C.c_void_p, C.c_uint32, C.c_double, C.c_double, C.c_double, C.c_uint32,
                                          C.c_uint32]
         L.oracle_tune_stream.restype = C.c_double
+        L.oracle_sample_moves.argtypes = [C.c_uint32, C.c_uint32, C.c_double, C.c_uint64, C.c_uint32, C.c_uint32,
+                                          C.c_uint64, C.POINTER(C.c_double)]
+        L.oracle_sample_moves.restype = None
         L.oracle_sdf.argtypes = [C.c_void_p, C.c_double, C.c_uint32, _u64p]
         L.oracle_gr.argtypes = [C.c_void_p, C.c_double, C.c_uint32, _u64p]
         L.oracle_overlap_count.argtypes = [C.c_void_p]
@@ -169,6 +172,15 @@ def counter_ball(step, substep, seed, index, dim, radius, n):
     out = np.zeros((n, dim))
     lib().oracle_counter_ball(step, substep, seed, index, dim, radius, n, _d(out))
     return out
+
+
+def sample_moves(dim, kind, maximum, n, step=0, substep=0, seed=0) -> np.ndarray:
+    """The samplers for a body at the origin, sample i from Counter(step, substep, seed).index(i)
+    (kind 0 translate, 1 rotate, 2 standard normal), shaped like Context.sample_moves."""
+    per = 1 if kind == 2 else (dim if kind == 0 else (4 if dim == 3 else 1))
+    out = np.empty(n * per)
+    lib().oracle_sample_moves(dim, kind, maximum, step, substep, seed, n, _d(out))
+    return out.reshape(n, per) if per > 1 else out
 
 
 def cbrt(x: float) -> float:

@@ -1842,6 +1842,34 @@ double oracle_tune(const oracle_system* s, uint32_t move, double maximum, double
     return maximum;
 }
 
+// The trial-move samplers for a body at the origin with the identity orientation, sample i from
+// Counter(step, substep, seed).index(i): kind 0 Translate (ball_sample, distribution.rs:41-69),
+// kind 1 Rotate (3-D Rotate<Versor>, rotate/versor.rs:40-71, 112-123; 2-D Rotate<Angle>,
+// rotate/angle.rs:46-55), kind 2 one StandardNormal.
+void oracle_sample_moves(uint32_t dim, uint32_t kind, double maximum, uint64_t step, uint32_t substep, uint32_t seed,
+                         uint64_t n, double* out) {
+    for (uint64_t i = 0; i < n; ++i) {
+        Sfc64 rng = make_rng(step, substep, seed, i);
+        if (kind == 2) {
+            out[i] = standard_normal(rng);
+        } else if (kind == 0) {
+            double d[3] = {0, 0, 0};
+            ball_sample(rng, (int)dim, maximum, d);
+            for (uint32_t a = 0; a < dim; ++a) out[i * dim + a] = d[a];
+        } else if (dim == 3) {
+            Quat q = qmul(versor_displacement(rng, maximum), Quat{1.0, 0.0, 0.0, 0.0});
+            out[i * 4 + 0] = q.s;
+            out[i * 4 + 1] = q.x;
+            out[i * 4 + 2] = q.y;
+            out[i * 4 + 3] = q.z;
+        } else {
+            uint64_t bits = rng.next_u64() >> 12;
+            double u = bits_to_double(0x3FF0000000000000ULL | bits) - 1.0;
+            out[i] = 0.0 + (u * (maximum - (-maximum)) + (-maximum));
+        }
+    }
+}
+
 // tune_local_trial (hoomd-mc/src/tune_local.rs:42-88) as the reference runs it: one stream
 // Counter(step, substep, seed).make_rng() (index 0) for every sample of every step, in order:
 // random_range(0..n) for the body, propose, wrap, delta_energy_one, and the uniform only when

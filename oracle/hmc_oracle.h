@@ -135,6 +135,9 @@ int oracle_serial_sweep(oracle_system* s, uint32_t move, double maximum, double 
 int oracle_serial_sweep_filter(oracle_system* s, uint32_t move, double maximum, double kt, const uint8_t* mask,
                                uint64_t* accepted, uint64_t* rejected);
 // Move-size tuning (tune_local.rs:21-89) with per-sample counter streams; returns the tuned size.
+/* Sampler probe: proposals for a body at the origin (kind 0 translate, 1 rotate, 2 normal). */
+void oracle_sample_moves(uint32_t dim, uint32_t kind, double maximum, uint64_t step, uint32_t substep, uint32_t seed,
+                         uint64_t n, double* out);
 double oracle_tune(const oracle_system* s, uint32_t move, double maximum, double kt, double target, uint32_t samples,
                    uint32_t steps);
 /* tune_local_trial with the reference's single sequential stream (tune_local.rs:42-88). */
