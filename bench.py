@@ -240,15 +240,29 @@ def replica_specs(seed=REPLICA_SEED, count=REPLICAS):
     return out
 
 
+def partition_replicas(count, rank, world):
+    """The replicas rank `rank` of `world` runs: every world-th one from rank (round robin, so
+    the large and small boxes of the log-uniform draw spread evenly). No replica is exchanged;
+    the ranks only reduce timings and counts."""
+    return list(range(rank, count, world))
+
+
 def run_replicas(args, local_rank):
-    """256 independent hard-sphere boxes (one hmc_batch), each with its move size tuned by
-    Tune (target 0.30) on its own; one step = one ParallelSweep of every replica."""
+    """256 independent hard-sphere boxes (one hmc_batch per GPU: the replicas are split over
+    the ranks), each with its move size tuned by Tune (target 0.30) on its own; one step = one
+    ParallelSweep of every replica."""
     import torch
-    from hoomd_rs_b200 import (FP32_RECHECK, TRANSLATE, Batch, Context, HardSphere, Microstate, PairwiseCutoff,
-                               Periodic, lattice)
+    import torch.distributed as dist
+    from hoomd_rs_b200 import FP32_RECHECK, Batch, Context, Periodic, lattice
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     torch.cuda.set_device(local_rank)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     ctx = Context(local_rank)
-    specs = replica_specs()
+    specs_all = replica_specs()
+    mine = partition_replicas(len(specs_all), rank, world)
+    specs = [specs_all[i] for i in mine]
     reps = []
     for n, phi, seed in specs:
         pos, L = lattice.hard_sphere_box(n, phi, 3, seed)
@@ -256,42 +270,56 @@ def run_replicas(args, local_rank):
     b = Batch(ctx, reps)
     # each replica's move size tuned on its own state (hmc_batch_tune = hmc_tune per replica)
     maxima = b.tune(D0, FP32_RECHECK, TARGET_ACCEPTANCE, 2000, 16)
+    # the launch-shape autotuner for the replica pass (restores the state afterwards)
+    chosen, ms = b.autotune(maxima, FP32_RECHECK, sweeps=2)
     stream = torch.cuda.Stream()
     for _ in range(args.warmup):
         b.sweep(maxima, FP32_RECHECK, increment_step=True)
     torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
     sampler = ClockSampler(local_rank)
     sampler.start()
     launches0 = b.kernel_launches()
-    t0 = time.perf_counter()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
     trials = 0
     for _ in range(args.steps):
         _, tot = b.sweep(maxima, FP32_RECHECK, increment_step=True)
         trials += tot.total()
+    e1.record()
     torch.cuda.synchronize()
-    el = time.perf_counter() - t0
     clocks = sampler.stop()
+    t_max, trials_all = aggregate_over_ranks(e0.elapsed_time(e1) / 1e3, trials, world, "cuda")
     over = b.overlap_counts()
-    n_total = sum(n for n, _, _ in specs)
+    _, over_sum = aggregate_over_ranks(0.0, int(over.sum()), world, "cuda")
+    n_total = sum(n for n, _, _ in specs_all)
     torch.cuda.synchronize()
     t_sdf = time.perf_counter()
     pressures = b.pressures(0.02, 40)
     t_sdf = time.perf_counter() - t_sdf
-    line = {"metric": "trial moves/s, 256-replica hard-sphere batch", "value": trials / el, "unit": UNIT,
-            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32 pair test + fp64 recheck",
-            "data": "synthetic",
+    line = {"metric": "trial moves/s, 256-replica hard-sphere batch", "value": trials_all / t_max, "unit": UNIT,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+            "dtype": "fp32 pair test + fp64 recheck", "data": "synthetic",
             "config": {"workload": "256 hard-sphere boxes, N log-uniform [1024, 65536], packing fraction U[0.40, 0.54], "
                                    "FCC starts, per-replica move sizes tuned to 0.30, one batched ParallelSweep of "
-                                   "every replica per step", "n_bodies_total": n_total, "replicas": len(specs),
-                       "timing": "host wall clock around the batched sweep calls (each ends in a device sync)"},
-            "overlaps_after": int(over.sum()), "gpu_launches": b.kernel_launches() - launches0, "clocks": clocks,
+                                   "every replica per step", "n_bodies_total": n_total, "replicas": len(specs_all),
+                       "partition": f"round robin over {world} rank(s), {len(specs)} replicas on rank {rank}",
+                       "timing": "CUDA events around the batched sweep calls, max over ranks"},
+            "launch_variant": {"chosen": chosen, "ms_per_sweep": [round(float(x), 4) for x in ms]},
+            "overlaps_after": over_sum, "gpu_launches": b.kernel_launches() - launches0, "clocks": clocks,
             "sdf_pressure": {"estimator": "beta P per replica from its scale distribution (x_max 0.02, 40 bins), "
-                                          "after the timed sweeps", "min": float(pressures.min()),
+                                          "after the timed sweeps (rank 0's replicas)", "min": float(pressures.min()),
                              "median": float(np.median(pressures)), "max": float(pressures.max()),
                              "ms_all_replicas": 1e3 * t_sdf}}
-    print(json.dumps(line), flush=True)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
     b.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 def run_lj_replicas(args, local_rank):
@@ -300,16 +328,23 @@ def run_lj_replicas(args, local_rank):
     every replica. Also timed: FP64, and the same 64 boxes swept one Microstate after another
     (what a caller without batches would do)."""
     import torch
+    import torch.distributed as dist
     import oracle
     from hoomd_rs_b200 import (FP32_RECHECK, FP64, TRANSLATE, Batch, Context, Isotropic, LennardJones, Microstate,
                                PairwiseCutoff, Periodic, Shifted, lattice)
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     torch.cuda.set_device(local_rank)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     ctx = Context(local_rank)
     n, n_rep, rho, r_cut, d = 8192, 64, 0.8, 2.5, 0.1
-    kts = np.random.default_rng(0x5EED0050).uniform(0.8, 2.0, n_rep)
+    kts_all = np.random.default_rng(0x5EED0050).uniform(0.8, 2.0, n_rep)
+    mine = partition_replicas(n_rep, rank, world)  # the replicas of this rank
+    kts = kts_all[mine]
     h = PairwiseCutoff(Isotropic(Shifted(LennardJones(1.0, 1.0), r_cut), r_cut))
     reps = []
-    for k in range(n_rep):
+    for k in mine:
         pos, L = lattice.lennard_jones_box(n, rho, 3, 0x5EED0050 + k)
         reps.append({"boundary": Periodic(r_cut, [L] * 3), "positions": pos, "seed": 0x5EED0050 + k, "hamiltonian": h})
 
@@ -318,15 +353,21 @@ def run_lj_replicas(args, local_rank):
         for _ in range(warmup):
             b.sweep(d, precision, increment_step=True, temperatures=kts)
         torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
         launches0 = b.kernel_launches()
-        t0 = time.perf_counter()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
         trials = 0
         for _ in range(steps):
             _, tot = b.sweep(d, precision, increment_step=True, temperatures=kts)
             trials += tot.total()
+        e1.record()
         torch.cuda.synchronize()
-        el = time.perf_counter() - t0
-        out = (trials / el, 1e3 * el / steps, b.kernel_launches() - launches0, [b.positions(k) for k in (0, 31)])
+        el, trials_all = aggregate_over_ranks(e0.elapsed_time(e1) / 1e3, trials, world, "cuda")
+        out = (trials_all / el, 1e3 * el / steps, b.kernel_launches() - launches0,
+               [b.positions(k) for k in (0, len(reps) // 2)])
         b.close()
         return out
 
@@ -335,6 +376,20 @@ def run_lj_replicas(args, local_rank):
     v32, ms32, launches, p32 = timed_batch(FP32_RECHECK, args.steps, args.warmup)
     clocks = sampler.stop()
     v64, ms64, _, p64 = timed_batch(FP64, args.steps, args.warmup)
+    if world > 1:  # the rest (one system after another, the CPU baseline) is a one-GPU comparison
+        if rank == 0:
+            print(json.dumps({"metric": "trial moves/s, 64-replica Lennard-Jones batch", "value": v32, "unit": UNIT,
+                              "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms32,
+                              "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+                              "dtype": "fp32 sums + fp64 recheck (fp64 state)", "data": "synthetic",
+                              "config": {"workload": "64 Lennard-Jones boxes of 8192 bodies split round robin over "
+                                                     f"{world} ranks", "replicas": n_rep,
+                                         "timing": "CUDA events around the batched sweeps, max over ranks"},
+                              "fp64": {"value": v64, "ms_per_step": ms64}, "gpu_launches": launches,
+                              "clocks": clocks}), flush=True)
+        dist.barrier()
+        dist.destroy_process_group()
+        return
     # the same replicas as separate systems, swept one after another
     singles = [Microstate(ctx, r["boundary"], r["positions"], h, seed=r["seed"]) for r in reps]
     for k, m in enumerate(singles):
@@ -356,8 +411,7 @@ def run_lj_replicas(args, local_rank):
             "config": {"workload": "64 Lennard-Jones boxes of 8192 bodies, rho 0.8, eps = sigma = 1, "
                                    "r_cut = r_shift = 2.5, kT_k ~ U[0.8, 2.0], FCC + 0.01 jitter, translation 0.1, "
                                    "one batched ParallelSweep of every replica per step", "n_bodies_total": n * n_rep,
-                       "replicas": n_rep,
-                       "timing": "host wall clock around the batched sweep calls (each ends in a device sync)"},
+                       "replicas": n_rep, "timing": "CUDA events around the batched sweep calls"},
             "fp64": {"value": v64, "ms_per_step": ms64},
             "mismatches": int(sum(np.count_nonzero(np.any(a != b, axis=1)) for a, b in zip(p32, p64))),
             "one_system_after_another": {"value": v_single, "precision": "fp32_recheck"},
@@ -445,7 +499,7 @@ def run_config(args, local_rank):
         for _ in range(args.warmup):
             for mv, mx in moves:
                 m.sweep(mv, mx, 1.0, precision, n_sweeps=1, increment_step=True)
-        ms, trials, acc, rech, checks = 0.0, 0, 0, 0, 0
+        ms, trials, acc, rech, checks, amb = 0.0, 0, 0, 0, 0, 0
         launches0 = m.profile()["kernel_launches"]
         for _ in range(args.steps):
             with torch.cuda.stream(stream):
@@ -458,12 +512,14 @@ def run_config(args, local_rank):
                 trials += c.total()
                 acc += c.accepted
                 rech += c.rechecks
+                amb += c.order_ambiguous
                 checks += c.pair_checks
             e1.record(stream)
             e1.synchronize()
             ms += e0.elapsed_time(e1)
         out = {"value": trials / (ms / 1e3), "ms_per_step": ms / args.steps, "acceptance": acc / max(trials, 1),
-               "recheck_fraction": rech / max(checks, 1), "launches": m.profile()["kernel_launches"] - launches0}
+               "recheck_fraction": rech / max(checks, 1), "launches": m.profile()["kernel_launches"] - launches0,
+               "order_ambiguous": amb}
         pos_end = m.positions()
         m.close()
         return out, pos_end
@@ -480,7 +536,9 @@ def run_config(args, local_rank):
                        "l2": "flushed before every timed step (256 MiB device write)"},
             "fp64": {"value": r64["value"], "ms_per_step": r64["ms_per_step"]},
             "mismatches": int(np.count_nonzero(np.any(p32 != p64, axis=1))), "acceptance": r32["acceptance"],
-            "recheck_fraction": r32["recheck_fraction"], "gpu_launches": r32["launches"], "clocks": clocks}
+            "recheck_fraction": r32["recheck_fraction"], "gpu_launches": r32["launches"], "clocks": clocks,
+            "order_ambiguous": {"fp32_recheck": r32["order_ambiguous"], "fp64": r64["order_ambiguous"],
+                                "what": "decisions another summation order of the FP64 pair energies could change"}}
     if not args.no_cpu_baseline:
         threads = host_threads()
         o = oracle.System(dim, [L] * dim, pos, seed=seed, **okw)
@@ -624,6 +682,12 @@ def main():
     # a few sweeps away from the lattice before the copies start
     tuner.sweep(TRANSLATE, d, 1.0, FP32_RECHECK, n_sweeps=4, increment_step=True)
     start_pos, step0, _ = tuner.state()
+    # the launch-shape autotuner, per precision: it records its choice for this workload's density
+    # band, which the timed systems below pick up (it restores the tuner's state afterwards)
+    variants = {}
+    for name, prec in (("fp32_recheck", FP32_RECHECK), ("fp64", FP64)):
+        chosen, ms = tuner.autotune(TRANSLATE, d, 1.0, prec, sweeps=4)
+        variants[name] = {"chosen": chosen, "ms_per_sweep": [round(float(x), 4) for x in ms]}
     tuner.close()
 
     stream = torch.cuda.Stream()
@@ -732,6 +796,7 @@ def main():
                 "d2h_bytes_per_step": N_BODIES * 3 * 8},
         "gpu_launches": ra["launches"],
         "clocks": clocks,
+        "launch_variants": variants,
         "time_split": {"unit": "ms per sweep (CUDA events inside the timed FP32 sweeps)",
                        "cell_list_rebuild": prof["rebuild_ms"] / max(prof["sweeps"], 1),
                        "colour_passes": prof["sweep_ms"] / max(prof["sweeps"], 1),

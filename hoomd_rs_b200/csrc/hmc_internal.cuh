@@ -70,7 +70,15 @@ struct Arrays {
     DeviceStats* stats;
     const double* zig_x;     // ziggurat tables (257 each)
     const double* zig_f;
+    // A round's trial moves, one per colour-list entry (soft potentials: k_propose_lj writes them
+    // before the round's colour passes, which give each trial a warp): trial site T = wrap(W1) and
+    // the Metropolis uniform in trial_t, T's FP32 offsets in trial_o, the chosen slot in trial_k
+    // (kNoTrial when the move leaves its space or the entry is empty).
+    double4* trial_t;        // [cells]
+    float4* trial_o;         // [cells]
+    uint32_t* trial_k;       // [cells]
 };
+constexpr uint32_t kNoTrial = 0xffffffffu;
 
 // Pair interaction parameters.
 struct Pair {
@@ -286,6 +294,9 @@ cudaError_t launch_overlap_sphere(int dim, const Geometry& g, const Arrays& a, c
                                   cudaStream_t s);
 cudaError_t launch_sweep_lj(int dim, bool fp32, const Geometry& g, const Arrays& a, const Pair& p, const Launch& l,
                             cudaStream_t s, uint32_t variant = 0);
+// The trial moves of round l.round for every colour list at once (Arrays::trial_*), one thread
+// per trial; launched in stream order before the round's LJ colour passes.
+cudaError_t launch_propose_lj(int dim, bool fp32, const Geometry& g, const Arrays& a, const Launch& l, cudaStream_t s);
 // delta_energy_one in FP64 for injected trial positions (LJ); u < 0 means no decision needed.
 cudaError_t launch_eval_lj(int dim, bool fp32, const Geometry& g, const Arrays& a, const Pair& p,
                            const uint64_t* bodies, const double4* trial, const double* u, double kt, uint32_t n,

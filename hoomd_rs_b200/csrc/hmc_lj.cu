@@ -195,6 +195,50 @@ __device__ __forceinline__ int decide32(const Sums32& s, double kt, double u) {
     return -1;
 }
 
+// The trial moves of one round for all colour lists (generate_trial_moves, parallel_sweep.rs:
+// 231-278, up to the Metropolis test): thread i takes entry i of the colour lists, draws the
+// body (IndexedRandom::choose), the displacement (Ball::sample) and the uniform from
+// Counter(step, substep + round, seed).index(space), wraps (W1) and checks that W1 stays in the
+// space; the passes then give each trial a warp and read the move from here instead of having
+// every lane of the warp compute it. A trial reads only the rebuild's arrays and the bodies of its
+// own colour, which the previous colours of the round do not move.
+template <int DIM, bool FP32>
+__global__ void __launch_bounds__(128) k_propose_lj(Geometry g, Arrays A, Launch L) {
+    const DeviceStats* st = A.stats;
+    if (st->error_flags != 0u || L.round >= st->rounds) return;
+    const uint32_t colors = 1u << DIM;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < colors * g.color_stride;
+         i += gridDim.x * blockDim.x) {
+        const uint32_t c = i / g.color_stride, w = i - c * g.color_stride;
+        if (w >= st->color_count[c]) continue;
+        uint32_t m[3] = {0, 0, 0};
+        unpack_m<DIM>(__ldg(A.color_cells + i), m);
+        const uint32_t cell = cell_index<DIM>(g, m);
+        const uint32_t start = __ldg(A.cell_start + cell);
+        const uint32_t count = __ldg(A.cell_start + cell + 1) - start;
+        Sfc64 rng = make_rng(L.step, L.substep, L.seed, (uint64_t)cell);
+        const uint32_t k = start + canon_range_u32(rng, count);
+        const double4 b4 = A.sorted_b[k];
+        double x[3] = {b4.x, b4.y, b4.z};
+        double dv[3];
+        ball_sample<DIM>(rng, L.max_move, A.zig_x, A.zig_f, dv);
+        const double u = uniform01(rng);
+#pragma unroll
+        for (int a = 0; a < DIM; ++a) x[a] = dadd(x[a], dv[a]);
+        wrap_inv<DIM>(g.L, g.invL, x);  // W1 = wrap(propose(..))
+        uint32_t mt[3];
+        if (!(point_to_space<DIM>(g, x, mt) && cell_index<DIM>(g, mt) == cell)) {
+            A.trial_k[i] = kNoTrial;  // leaves its space: rejected before delta_energy_one
+            continue;
+        }
+        double t[3] = {x[0], x[1], DIM == 3 ? x[2] : 0.0};
+        wrap_inv<DIM>(g.L, g.invL, t);  // the trial site T = wrap(W1)
+        A.trial_t[i] = make_double4(t[0], t[1], t[2], u);
+        if (FP32) A.trial_o[i] = cell_offsets<DIM>(g, t, m);
+        A.trial_k[i] = k;
+    }
+}
+
 // Injected trial w of the probe mode (Injected) in a warp-per-trial pass: the body's slot and
 // space, W1 and u from the list. The colour pass evaluates only trials that stay in their body's
 // space; the others are rejected as in the sweep (kTrialOutsideSpace).
@@ -226,41 +270,37 @@ __global__ void __launch_bounds__(128, MINB) k_sweep_lj(Geometry g, Arrays A, Pa
         uint32_t k = 0;
         double x[3] = {0.0, 0.0, 0.0};
         double u = 0.0;
-        if constexpr (INJ)
+        double t[3] = {0.0, 0.0, 0.0};
+        if constexpr (INJ) {
             lj_inject<DIM>(A, J, w, m, k, x, u);
-        else
-            unpack_m<DIM>(__ldg(A.color_cells + (size_t)L.color * g.color_stride + w), m);
+        } else {
+            // the round's trial from k_propose_lj
+            const size_t e = (size_t)L.color * g.color_stride + w;
+            k = __ldg(A.trial_k + e);
+            if (k == kNoTrial) continue;  // warp-uniform: the move left its space
+            unpack_m<DIM>(__ldg(A.color_cells + e), m);
+            const double4 t4 = ldg4(A.trial_t + e);
+            t[0] = t4.x;
+            t[1] = t4.y;
+            t[2] = t4.z;
+            u = t4.w;
+        }
         const uint32_t cell = cell_index<DIM>(g, m);
         const FlatStencil fs = flat_stencil<DIM>(g, A.cell_start, m, lane);
-        if constexpr (!INJ) {
-            const uint32_t start = __ldg(A.cell_start + cell);
-            const uint32_t count = __ldg(A.cell_start + cell + 1) - start;
-            // every lane draws the same stream: the trial is computed redundantly, warp-uniform
-            Sfc64 rng = make_rng(L.step, L.substep, L.seed, (uint64_t)cell);
-            k = start + canon_range_u32(rng, count);
-            const double4 b4 = A.sorted_b[k];
-            x[0] = b4.x;
-            x[1] = b4.y;
-            x[2] = b4.z;
-            double dv[3];
-            ball_sample<DIM>(rng, L.max_move, A.zig_x, A.zig_f, dv);
-            u = uniform01(rng);
-#pragma unroll
-            for (int a = 0; a < DIM; ++a) x[a] = dadd(x[a], dv[a]);
-            wrap_inv<DIM>(g.L, g.invL, x);
-        }
-        uint32_t mt[3];
-        if (!(point_to_space<DIM>(g, x, mt) && cell_index<DIM>(g, mt) == cell)) {
-            if constexpr (INJ) {
+        if constexpr (INJ) {
+            uint32_t mt[3];
+            if (!(point_to_space<DIM>(g, x, mt) && cell_index<DIM>(g, mt) == cell)) {
                 if (lane == 0) {
                     J.decisions[w] = 0;
                     J.flags[w] = kTrialOutsideSpace;
                 }
+                continue;
             }
-            continue;
+            t[0] = x[0];
+            t[1] = x[1];
+            t[2] = DIM == 3 ? x[2] : 0.0;
+            wrap_inv<DIM>(g.L, g.invL, t);
         }
-        double t[3] = {x[0], x[1], DIM == 3 ? x[2] : 0.0};
-        wrap_inv<DIM>(g.L, g.invL, t);
         grid_dependency_wait();  // the previous colour's moves are visible from here on
         allow_dependent_launch();
         const double4 s4 = ldg4(A.sorted_s + k);
@@ -341,6 +381,7 @@ __global__ void __launch_bounds__(128, MINB) k_sweep_lj32(Geometry g, Arrays A, 
         bool trial = false;
         FlatStencil fs{0u, 0u, 0u, 0.f, 0.f};
         bool outside = false;
+        float4 t32p = make_float4(0.f, 0.f, 0.f, 0.f);
         if (INJ && w < n_active) {  // warp-uniform
             double x[3];
             lj_inject<DIM>(A, J, w, m, k, x, u);
@@ -353,35 +394,27 @@ __global__ void __launch_bounds__(128, MINB) k_sweep_lj32(Geometry g, Arrays A, 
             t[1] = x[1];
             t[2] = x[2];
             wrap_inv<DIM>(g.L, g.invL, t);
-        } else if (w < n_active) {  // warp-uniform
-            unpack_m<DIM>(__ldg(A.color_cells + (size_t)L.color * g.color_stride + w), m);
-            const uint32_t cell = cell_index<DIM>(g, m);
-            fs = flat_stencil<DIM>(g, A.cell_start, m, lane);
-            const uint32_t start = __ldg(A.cell_start + cell);
-            const uint32_t count = __ldg(A.cell_start + cell + 1) - start;
-            Sfc64 rng = make_rng(L.step, L.substep, L.seed, (uint64_t)cell);
-            k = start + canon_range_u32(rng, count);
-            const double4 b4 = A.sorted_b[k];
-            double x[3] = {b4.x, b4.y, b4.z};
-            double dv[3];
-            ball_sample<DIM>(rng, L.max_move, A.zig_x, A.zig_f, dv);
-            u = uniform01(rng);
-#pragma unroll
-            for (int a = 0; a < DIM; ++a) x[a] = dadd(x[a], dv[a]);
-            wrap_inv<DIM>(g.L, g.invL, x);
-            uint32_t mt[3];
-            trial = point_to_space<DIM>(g, x, mt) && cell_index<DIM>(g, mt) == cell;
-            t[0] = x[0];
-            t[1] = x[1];
-            t[2] = DIM == 3 ? x[2] : 0.0;
-            wrap_inv<DIM>(g.L, g.invL, t);
+        } else if (w < n_active) {  // warp-uniform: the round's trial from k_propose_lj
+            const size_t e = (size_t)L.color * g.color_stride + w;
+            k = __ldg(A.trial_k + e);
+            trial = k != kNoTrial;
+            if (trial) {
+                unpack_m<DIM>(__ldg(A.color_cells + e), m);
+                fs = flat_stencil<DIM>(g, A.cell_start, m, lane);
+                const double4 t4 = ldg4(A.trial_t + e);
+                t[0] = t4.x;
+                t[1] = t4.y;
+                t[2] = t4.z;
+                u = t4.w;
+                t32p = __ldg(A.trial_o + e);
+            }
         }
         grid_dependency_wait();  // the previous colour's moves are visible from here on
         allow_dependent_launch();
         int decision = 0;
         float d32 = 0.f;
         if (trial) {
-            const float4 t32 = cell_offsets<DIM>(g, t, m);
+            const float4 t32 = INJ ? cell_offsets<DIM>(g, t, m) : t32p;
             const float4 c32 = __ldg(A.sorted_off + k);
             const Sums32 s = lj_energy32<DIM>(g, A, P, t32, c32, (int)m[DIM - 1], fs, k, lane);
             pst.checks += s.pairs;
@@ -872,6 +905,25 @@ cudaError_t launch_sweep_lj(int dim, bool fp32, const Geometry& g, const Arrays&
          {k_sweep_lj32<3, false, 9>, k_sweep_lj32<3, false, 7>, k_sweep_lj32<3, false, 11>}}};
     const LjKernel k = kernels[dim == 3][fp32][variant < 3 ? variant : 0];
     return cudaLaunchKernelEx(&pl.cfg, k, g, a, p, l, Injected{});
+}
+
+cudaError_t launch_propose_lj(int dim, bool fp32, const Geometry& g, const Arrays& a, const Launch& l, cudaStream_t s) {
+    const uint64_t n = (uint64_t)g.color_stride << dim;
+    if (n == 0) return cudaSuccess;
+    static int max_blocks = 0;
+    if (max_blocks == 0) {
+        int dev = 0, sms = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        max_blocks = sms * 16;
+    }
+    uint32_t blocks = (uint32_t)((n + 127) / 128);
+    if (blocks > (uint32_t)max_blocks) blocks = (uint32_t)max_blocks;
+    if (dim == 2)
+        fp32 ? k_propose_lj<2, true><<<blocks, 128, 0, s>>>(g, a, l) : k_propose_lj<2, false><<<blocks, 128, 0, s>>>(g, a, l);
+    else
+        fp32 ? k_propose_lj<3, true><<<blocks, 128, 0, s>>>(g, a, l) : k_propose_lj<3, false><<<blocks, 128, 0, s>>>(g, a, l);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_tune_stream_lj(int dim, TuneJob* jobs, uint32_t n_jobs, cudaStream_t s) {

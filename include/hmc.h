@@ -201,10 +201,12 @@ hmc_status hmc_increment_step(hmc_system* sys);
 hmc_status hmc_sweep(hmc_system* sys, const hmc_sweep_params* params, hmc_count* out);
 hmc_status hmc_tune(hmc_system* sys, hmc_sweep_params* params, double target_acceptance, uint32_t samples,
                     uint32_t steps);
-/* Sweep::apply_with_filter (hoomd-mc/src/sweep.rs:159-224), hard spheres: one trial per body in
- * index order from one sequential stream, then increment_substep. move_mask (n_bodies bytes,
- * may be NULL) selects the bodies to move (should_move_body). The exact serial chain; the
- * checkerboard hmc_sweep is the fast path. */
+/* Sweep::apply_with_filter (hoomd-mc/src/sweep.rs:159-224), every interaction (hard and
+ * overlap-penalty spheres, Lennard-Jones, convex polyhedra and polygons; Translate, or Rotate for
+ * shapes): one trial per body in index order from one sequential stream, then increment_substep.
+ * move_mask (n_bodies bytes, may be NULL) selects the bodies to move (should_move_body). The exact
+ * serial chain on one warp; the checkerboard hmc_sweep is the fast path. For soft potentials
+ * out->order_ambiguous counts the decisions another summation order could change. */
 hmc_status hmc_serial_sweep(hmc_system* sys, const hmc_sweep_params* params, const uint8_t* move_mask,
                             hmc_count* out);
 hmc_status hmc_overlap_check(hmc_system* sys, uint64_t* n_overlaps);
