@@ -299,13 +299,15 @@ hmc_status setup_geometry(hmc_system* s, const double* L) {
         if ((st = dalloc(s, &A.cell_count, cells)) || (st = dalloc(s, &A.cell_start, cells + 1)) ||
             (st = dalloc(s, &A.block_sums, (size_t)scan_blocks * 9)) || (st = dalloc(s, &A.color_cells, cells)))
             return st;
-        if (s->soft()) {  // the rounds' trial moves of the warp-per-trial passes
+        if (s->soft() || s->oriented()) {  // the rounds' trial moves of the passes with lanes per trial
             dfree(s, &A.trial_t);
             dfree(s, &A.trial_o);
             dfree(s, &A.trial_k);
+            dfree(s, &A.trial_q);
             if ((st = dalloc(s, &A.trial_t, cells)) || (st = dalloc(s, &A.trial_o, cells)) ||
                 (st = dalloc(s, &A.trial_k, cells)))
                 return st;
+            if (s->interaction == HMC_HARD_CONVEX_POLYHEDRON && (st = dalloc(s, &A.trial_q, cells))) return st;
         }
         s->cells_alloc = cells;
     }
@@ -883,9 +885,16 @@ hmc_status hmc_sweep(hmc_system* s, const hmc_sweep_params* p, hmc_count* out) {
             for (uint32_t r = r0; r < r1; ++r) {
                 L.substep = s->substep + r;  // increment_substep after every full colour set
                 L.round = r;
+                // the round's trial moves, one thread each, before the passes that give a trial
+                // several lanes
                 if (s->soft()) {
-                    // the round's trial moves, one thread each, before the warp-per-trial passes
                     HMC_CUDA(launch_propose_lj(s->dim, fp32 && !s->penalty(), s->geom, s->arr, L, s->stream));
+                    s->prof.kernel_launches += 1;
+                } else if (s->interaction == HMC_HARD_CONVEX_POLYHEDRON) {
+                    HMC_CUDA(launch_propose_poly(fp32, s->geom, s->arr, L, p->move == HMC_ROTATE, s->stream));
+                    s->prof.kernel_launches += 1;
+                } else if (s->polygon()) {
+                    HMC_CUDA(launch_propose_poly2(fp32, s->geom, s->arr, L, p->move == HMC_ROTATE, s->stream));
                     s->prof.kernel_launches += 1;
                 }
                 for (uint32_t c = 0; c < colors; ++c) {
@@ -893,7 +902,7 @@ hmc_status hmc_sweep(hmc_system* s, const hmc_sweep_params* p, hmc_count* out) {
                     L.overlap_previous = (r > 0 || c > 0) && s->pdl ? 1u : 0u;
                     // the first pass after the rebuild (or after a round's proposals): launch early,
                     // wait for it before reading anything
-                    L.early_wait = (r == 0 || s->soft()) && c == 0 && s->pdl ? 1u : 0u;
+                    L.early_wait = (r == 0 || s->soft() || s->oriented()) && c == 0 && s->pdl ? 1u : 0u;
                     if (s->soft())  // the overlap penalty has no FP32 path: FP64 in both modes
                         HMC_CUDA(launch_sweep_lj(s->dim, fp32 && !s->penalty(), s->geom, s->arr, s->pair, L,
                                                  s->stream, variant));

@@ -77,6 +77,7 @@ struct Arrays {
     double4* trial_t;        // [cells]
     float4* trial_o;         // [cells]
     uint32_t* trial_k;       // [cells]
+    double4* trial_q;        // [cells] shapes: the proposed versor (2-D: the angle in .x)
 };
 constexpr uint32_t kNoTrial = 0xffffffffu;
 
@@ -295,8 +296,13 @@ cudaError_t launch_overlap_sphere(int dim, const Geometry& g, const Arrays& a, c
 cudaError_t launch_sweep_lj(int dim, bool fp32, const Geometry& g, const Arrays& a, const Pair& p, const Launch& l,
                             cudaStream_t s, uint32_t variant = 0);
 // The trial moves of round l.round for every colour list at once (Arrays::trial_*), one thread
-// per trial; launched in stream order before the round's LJ colour passes.
+// per trial; launched in stream order before the round's colour passes of the passes that give a
+// trial several lanes (LJ and the overlap penalty, convex polyhedra, convex polygons).
 cudaError_t launch_propose_lj(int dim, bool fp32, const Geometry& g, const Arrays& a, const Launch& l, cudaStream_t s);
+cudaError_t launch_propose_poly(bool fp32, const Geometry& g, const Arrays& a, const Launch& l, bool rotate,
+                                cudaStream_t s);
+cudaError_t launch_propose_poly2(bool fp32, const Geometry& g, const Arrays& a, const Launch& l, bool rotate,
+                                 cudaStream_t s);
 // delta_energy_one in FP64 for injected trial positions (LJ); u < 0 means no decision needed.
 cudaError_t launch_eval_lj(int dim, bool fp32, const Geometry& g, const Arrays& a, const Pair& p,
                            const uint64_t* bodies, const double4* trial, const double* u, double kt, uint32_t n,

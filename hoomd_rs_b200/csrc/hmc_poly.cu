@@ -327,6 +327,51 @@ __device__ __forceinline__ void drain_pairs(const Geometry& g, const Arrays& A, 
     __syncwarp();
 }
 
+// A round's trial moves of convex polyhedra for every colour list (generate_trial_moves,
+// parallel_sweep.rs:231-278, up to delta_energy_one), one thread per trial: the chosen body,
+// Translate (Ball::sample) or Rotate<Versor>, W1 = wrap(propose(..)), the space check, the trial
+// site T = wrap(W1) and its FP32 offsets; the packed pass reads them instead of computing each
+// move on the 8 lanes of its group.
+template <bool FP32>
+__global__ void __launch_bounds__(128) k_propose_poly3(Geometry g, Arrays A, Launch L, uint32_t rotate) {
+    const DeviceStats* st = A.stats;
+    if (st->error_flags != 0u || L.round >= st->rounds) return;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < 8u * g.color_stride; i += gridDim.x * blockDim.x) {
+        const uint32_t c = i / g.color_stride, w = i - c * g.color_stride;
+        if (w >= st->color_count[c]) continue;
+        uint32_t m[3] = {0, 0, 0};
+        unpack_m<3>(__ldg(A.color_cells + i), m);
+        const uint32_t cell = cell_index<3>(g, m);
+        const uint32_t start = __ldg(A.cell_start + cell);
+        const uint32_t count = __ldg(A.cell_start + cell + 1) - start;
+        Sfc64 rng = make_rng(L.step, L.substep, L.seed, (uint64_t)cell);
+        const uint32_t k = start + canon_range_u32(rng, count);
+        const double4 b4 = A.sorted_b[k];
+        double x[3] = {b4.x, b4.y, b4.z};
+        const double4 q4 = A.sorted_q[k];
+        Q qi{q4.x, q4.y, q4.z, q4.w};
+        if (rotate) {
+            qi = versor_move(rng, L.max_move, A.zig_x, A.zig_f, qi);
+        } else {
+            double dv[3];
+            ball_sample<3>(rng, L.max_move, A.zig_x, A.zig_f, dv);
+            for (int a = 0; a < 3; ++a) x[a] = dadd(x[a], dv[a]);
+        }
+        wrap_inv<3>(g.L, g.invL, x);  // W1 = wrap(propose(..))
+        uint32_t mt[3];
+        if (!(point_to_space<3>(g, x, mt) && cell_index<3>(g, mt) == cell)) {
+            A.trial_k[i] = kNoTrial;
+            continue;
+        }
+        double t[3] = {x[0], x[1], x[2]};
+        wrap_inv<3>(g.L, g.invL, t);
+        A.trial_t[i] = make_double4(t[0], t[1], t[2], 0.0);
+        A.trial_q[i] = make_double4(qi.s, qi.x, qi.y, qi.z);
+        if (FP32) A.trial_o[i] = cell_offsets<3>(g, t, m);
+        A.trial_k[i] = k;
+    }
+}
+
 // INJ: the probe mode (Injected): group trial w is injected trial w, walked around the space of
 // its W1, and its decision is written instead of committed.
 template <bool FP32, int G, bool INJ = false>
@@ -354,6 +399,7 @@ __global__ void __launch_bounds__(128, HMC_POLY_MIN_BLOCKS)
         double t[3] = {0.0, 0.0, 0.0};
         Q qi{1.0, 0.0, 0.0, 0.0};
         uint8_t flag = 0;
+        float4 t32p = make_float4(0.f, 0.f, 0.f, 0.f);
         if (INJ && w < n_active) {  // the injected trial (W1, versor), by the group's S lanes alike
             const uint64_t body = J.bodies[w];
             k = A.slot_of_body[body];
@@ -370,33 +416,22 @@ __global__ void __launch_bounds__(128, HMC_POLY_MIN_BLOCKS)
             t[1] = x[1];
             t[2] = x[2];
             wrap_inv<3>(g.L, g.invL, t);
-        } else if (w < n_active) {  // the group's trial, computed by its S lanes alike
-            unpack_m<3>(__ldg(A.color_cells + (size_t)L.color * g.color_stride + w), m);
-            const uint32_t cell = cell_index<3>(g, m);
-            const uint32_t start = __ldg(A.cell_start + cell);
-            const uint32_t count = __ldg(A.cell_start + cell + 1) - start;
-            Sfc64 rng = make_rng(L.step, L.substep, L.seed, (uint64_t)cell);
-            k = start + canon_range_u32(rng, count);
-            const double4 b4 = A.sorted_b[k];
-            double x[3] = {b4.x, b4.y, b4.z};
-            const double4 q4 = A.sorted_q[k];
-            qi = Q{q4.x, q4.y, q4.z, q4.w};
-            if (rotate) {
-                qi = versor_move(rng, L.max_move, A.zig_x, A.zig_f, qi);
-            } else {
-                double dv[3];
-                ball_sample<3>(rng, L.max_move, A.zig_x, A.zig_f, dv);
-                for (int a = 0; a < 3; ++a) x[a] = dadd(x[a], dv[a]);
+        } else if (w < n_active) {  // the group's trial from k_propose_poly3
+            const size_t e = (size_t)L.color * g.color_stride + w;
+            k = __ldg(A.trial_k + e);
+            valid = k != kNoTrial;
+            if (valid) {
+                unpack_m<3>(__ldg(A.color_cells + e), m);
+                const double4 t4 = ldg4(A.trial_t + e);
+                t[0] = t4.x;
+                t[1] = t4.y;
+                t[2] = t4.z;
+                const double4 q4 = ldg4(A.trial_q + e);
+                qi = Q{q4.x, q4.y, q4.z, q4.w};
+                if (FP32) t32p = __ldg(A.trial_o + e);
             }
-            wrap_inv<3>(g.L, g.invL, x);  // W1 = wrap(propose(..))
-            uint32_t mt[3];
-            valid = point_to_space<3>(g, x, mt) && cell_index<3>(g, mt) == cell;
-            t[0] = x[0];
-            t[1] = x[1];
-            t[2] = x[2];
-            wrap_inv<3>(g.L, g.invL, t);
         }
-        const float4 t32 = FP32 && valid ? cell_offsets<3>(g, t, m) : make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4 t32 = FP32 && valid ? (INJ ? cell_offsets<3>(g, t, m) : t32p) : make_float4(0.f, 0.f, 0.f, 0.f);
         if (sub == 0) {
             PolyTrial& tr = s_trial[wib][grp];
             tr.t[0] = t[0];
@@ -732,6 +767,20 @@ cudaError_t launch_serial_poly(const Geometry& g, const Arrays& a, const double4
     cudaError_t e = build_grid(3, g, a, G, l.n_bodies, s);
     if (e != cudaSuccess || l.n_bodies == 0) return e;
     k_serial_poly3<<<1, 32, 0, s>>>(g, a, G, PolyShape{verts, nv, rcut2, 0.f}, l, rotate ? 1u : 0u, mask);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_propose_poly(bool fp32, const Geometry& g, const Arrays& a, const Launch& l, bool rotate,
+                                cudaStream_t s) {
+    const uint64_t n = (uint64_t)g.color_stride << 3;
+    if (n == 0) return cudaSuccess;
+    const int wave = resident_wave((const void*)(fp32 ? k_propose_poly3<true> : k_propose_poly3<false>));
+    uint32_t blocks = (uint32_t)((n + 127) / 128);
+    if (blocks > (uint32_t)wave) blocks = (uint32_t)wave;
+    if (fp32)
+        k_propose_poly3<true><<<blocks, 128, 0, s>>>(g, a, l, rotate ? 1u : 0u);
+    else
+        k_propose_poly3<false><<<blocks, 128, 0, s>>>(g, a, l, rotate ? 1u : 0u);
     return cudaGetLastError();
 }
 

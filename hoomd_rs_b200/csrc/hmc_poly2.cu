@@ -283,34 +283,20 @@ __global__ void __launch_bounds__(128, HMC_POLY2_MIN_BLOCKS)
         bool valid = false;
         double t[3] = {0.0, 0.0, 0.0};
         double ti = 0.0;
-        if (w < n_active) {  // the group's trial, computed by its S lanes alike
-            unpack_m<2>(__ldg(A.color_cells + (size_t)L.color * g.color_stride + w), m);
-            const uint32_t cell = cell_index<2>(g, m);
-            const uint32_t start = __ldg(A.cell_start + cell);
-            const uint32_t count = __ldg(A.cell_start + cell + 1) - start;
-            Sfc64 rng = make_rng(L.step, L.substep, L.seed, (uint64_t)cell);
-            k = start + canon_range_u32(rng, count);
-            const double4 b4 = A.sorted_b[k];
-            double x[3] = {b4.x, b4.y, 0.0};
-            ti = A.sorted_q[k].x;
-            if (rotate) {
-                // Rotate<Angle>::propose (rotate/angle.rs:46-55): theta += Uniform(-a, a)
-                const double u = dsub(as_double(0x3FF0000000000000ULL | (rng.next_u64() >> 12)), 1.0);
-                ti = dadd(ti, dadd(dmul(u, dsub(L.max_move, -L.max_move)), -L.max_move));
-            } else {
-                double dv[3];
-                ball_sample<2>(rng, L.max_move, A.zig_x, A.zig_f, dv);
-                x[0] = dadd(x[0], dv[0]);
-                x[1] = dadd(x[1], dv[1]);
+        float4 t32 = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (w < n_active) {  // the group's trial from k_propose_poly2
+            const size_t e = (size_t)L.color * g.color_stride + w;
+            k = __ldg(A.trial_k + e);
+            valid = k != kNoTrial;
+            if (valid) {
+                unpack_m<2>(__ldg(A.color_cells + e), m);
+                const double4 t4 = ldg4(A.trial_t + e);
+                t[0] = t4.x;
+                t[1] = t4.y;
+                ti = t4.w;
+                if (FP32) t32 = __ldg(A.trial_o + e);
             }
-            wrap_inv<2>(g.L, g.invL, x);  // W1 = wrap(propose(..))
-            uint32_t mt[3];
-            valid = point_to_space<2>(g, x, mt) && cell_index<2>(g, mt) == cell;
-            t[0] = x[0];
-            t[1] = x[1];
-            wrap_inv<2>(g.L, g.invL, t);
         }
-        const float4 t32 = FP32 && valid ? cell_offsets<2>(g, t, m) : make_float4(0.f, 0.f, 0.f, 0.f);
         if (sub == 0) {
             Poly2Trial& tr = s_trial[wib][grp];
             tr.t[0] = t[0];
@@ -459,6 +445,50 @@ __global__ void __launch_bounds__(32) k_tune_stream_poly2(TuneJob* jobs, uint32_
     if (range_error) atomicOr(&J.a.stats->error_flags, kErrAngleRange);
 }
 
+// A round's trial moves of convex polygons for every colour list, one thread per trial: the
+// chosen body, Translate (Ball::sample) or Rotate<Angle> (theta += Uniform(-a, a), rotate/angle.rs:
+// 46-55), W1 = wrap(propose(..)), the space check, T = wrap(W1) with the angle in .w, and T's FP32
+// offsets; the packed pass reads them instead of computing each move on the 8 lanes of its group.
+template <bool FP32>
+__global__ void __launch_bounds__(128) k_propose_poly2(Geometry g, Arrays A, Launch L, uint32_t rotate) {
+    const DeviceStats* st = A.stats;
+    if (st->error_flags != 0u || L.round >= st->rounds) return;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < 4u * g.color_stride; i += gridDim.x * blockDim.x) {
+        const uint32_t c = i / g.color_stride, w = i - c * g.color_stride;
+        if (w >= st->color_count[c]) continue;
+        uint32_t m[3] = {0, 0, 0};
+        unpack_m<2>(__ldg(A.color_cells + i), m);
+        const uint32_t cell = cell_index<2>(g, m);
+        const uint32_t start = __ldg(A.cell_start + cell);
+        const uint32_t count = __ldg(A.cell_start + cell + 1) - start;
+        Sfc64 rng = make_rng(L.step, L.substep, L.seed, (uint64_t)cell);
+        const uint32_t k = start + canon_range_u32(rng, count);
+        const double4 b4 = A.sorted_b[k];
+        double x[3] = {b4.x, b4.y, 0.0};
+        double ti = A.sorted_q[k].x;
+        if (rotate) {
+            const double u = dsub(as_double(0x3FF0000000000000ULL | (rng.next_u64() >> 12)), 1.0);
+            ti = dadd(ti, dadd(dmul(u, dsub(L.max_move, -L.max_move)), -L.max_move));
+        } else {
+            double dv[3];
+            ball_sample<2>(rng, L.max_move, A.zig_x, A.zig_f, dv);
+            x[0] = dadd(x[0], dv[0]);
+            x[1] = dadd(x[1], dv[1]);
+        }
+        wrap_inv<2>(g.L, g.invL, x);  // W1 = wrap(propose(..))
+        uint32_t mt[3];
+        if (!(point_to_space<2>(g, x, mt) && cell_index<2>(g, mt) == cell)) {
+            A.trial_k[i] = kNoTrial;
+            continue;
+        }
+        double t[3] = {x[0], x[1], 0.0};
+        wrap_inv<2>(g.L, g.invL, t);
+        A.trial_t[i] = make_double4(t[0], t[1], 0.0, ti);
+        if (FP32) A.trial_o[i] = cell_offsets<2>(g, t, m);
+        A.trial_k[i] = k;
+    }
+}
+
 // Sweep::apply_with_filter (hoomd-mc/src/sweep.rs:159-224) for hard convex polygons: one trial per
 // body in index order from one stream, Translate or Rotate<Angle>, accepted when no site of the
 // serial grid's stencil overlaps it (no uniform is drawn); one warp, a lane per stencil cell. The
@@ -589,6 +619,20 @@ cudaError_t launch_sweep_poly2(bool fp32, bool sat, const Geometry& g, const Arr
                    : cudaLaunchKernelEx(&pl.cfg, k_sweep_poly2<true, false>, g, a, sh, l, rot);
     return sat ? cudaLaunchKernelEx(&pl.cfg, k_sweep_poly2<false, true>, g, a, sh, l, rot)
                : cudaLaunchKernelEx(&pl.cfg, k_sweep_poly2<false, false>, g, a, sh, l, rot);
+}
+
+cudaError_t launch_propose_poly2(bool fp32, const Geometry& g, const Arrays& a, const Launch& l, bool rotate,
+                                 cudaStream_t s) {
+    const uint64_t n = (uint64_t)g.color_stride << 2;
+    if (n == 0) return cudaSuccess;
+    const int wave = resident_wave((const void*)(fp32 ? k_propose_poly2<true> : k_propose_poly2<false>));
+    uint32_t blocks = (uint32_t)((n + 127) / 128);
+    if (blocks > (uint32_t)wave) blocks = (uint32_t)wave;
+    if (fp32)
+        k_propose_poly2<true><<<blocks, 128, 0, s>>>(g, a, l, rotate ? 1u : 0u);
+    else
+        k_propose_poly2<false><<<blocks, 128, 0, s>>>(g, a, l, rotate ? 1u : 0u);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_serial_poly2(bool sat, const Geometry& g, const Arrays& a, const double4* verts, uint32_t nv,
