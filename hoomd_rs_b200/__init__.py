@@ -19,6 +19,7 @@ There is no CPU fallback: if the library cannot be loaded, importing the module 
 from __future__ import annotations
 
 import ctypes as C
+import math
 import os
 from dataclasses import dataclass
 from typing import Optional, Sequence
@@ -60,6 +61,12 @@ class hmc_system_desc(C.Structure):
                 ("body_interaction_range", C.c_double), ("penalty_k", C.c_double),
                 ("penalty_maximum_overlap", C.c_double), ("penalty_shoulder", C.c_double),
                 ("capacity", C.c_uint64)]
+
+
+class hmc_shape_overlap_params(C.Structure):
+    _fields_ = [("struct_size", C.c_uint32), ("reserved", C.c_uint32), ("resolution", C.c_double),
+                ("r_cut", C.c_double), ("penalty_k", C.c_double), ("penalty_maximum_overlap", C.c_double),
+                ("penalty_shoulder", C.c_double)]
 
 
 class hmc_sweep_params(C.Structure):
@@ -177,6 +184,7 @@ SIGNATURES = {
     "hmc_get_box": (C.c_int, [_vp, _dp]),
     "hmc_set_box": (C.c_int, [_vp, _dp]),
     "hmc_get_n_bodies": (C.c_int, [_vp, C.POINTER(C.c_uint64)]),
+    "hmc_set_shape_overlap": (C.c_int, [_vp, C.POINTER(hmc_shape_overlap_params)]),
     "hmc_gsd_last_error": (C.c_int, []),
     "hmc_gsd_create": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_uint16, C.c_uint16, C.c_int,
                                  C.POINTER(_vp)]),
@@ -347,9 +355,11 @@ class ConvexPolygon:
 
     @classmethod
     def regular(cls, n: int) -> "ConvexPolygon":
-        """Regular n-gon of unit circumradius (a vertex at angle 0)."""
-        k = np.arange(n)
-        return cls(np.stack([np.cos(2 * np.pi * k / n), np.sin(2 * np.pi * k / n)], axis=1))
+        """ConvexPolygon::regular (convex_polytope.rs:137-152): vertex x at 0.5 (cos, sin) of
+        theta = 2 pi x / n. The reference sets the bounding radius to 0.5; here it is computed
+        from the vertices (0.5 up to the rounding of cos and sin)."""
+        return cls(np.array([[0.5 * math.cos(2.0 * math.pi * x / n), 0.5 * math.sin(2.0 * math.pi * x / n)]
+                             for x in range(n)]))
 
     @property
     def bounding_radius(self) -> float:
@@ -407,9 +417,40 @@ class HardShape:
 
 
 @dataclass
+class ApproximateShapeOverlap:
+    """hoomd_interaction::pairwise::ApproximateShapeOverlap (approximate_shape_overlap.rs:52-171):
+    the isotropic energy (an OverlapPenalty) at minus the approximate distance, in steps of
+    `resolution`, that shape j must move along the line of centres to stop intersecting shape i.
+    For Convex polyhedra and polygons; only for preparing states (QuickInsert, QuickCompress)."""
+    shape: object  # ConvexPolyhedron or ConvexPolygon
+    isotropic: OverlapPenalty
+    resolution: float
+
+    @classmethod
+    def new(cls, shape, isotropic: OverlapPenalty, resolution: float) -> "ApproximateShapeOverlap":
+        return cls(shape, isotropic, float(resolution))
+
+
+@dataclass
+class Anisotropic:
+    """hoomd_interaction::pairwise::Anisotropic (anisotropic.rs:88-143): the pair energy in the
+    local frame of site i, 0 at a centre distance >= r_cut."""
+    interaction: ApproximateShapeOverlap
+    r_cut: float
+
+    @property
+    def maximum_interaction_range(self) -> float:
+        return self.r_cut
+
+
+@dataclass
 class PairwiseCutoff:
     """hoomd_interaction::PairwiseCutoff (pairwise_cutoff.rs:140)."""
     pair: object
+
+    @property
+    def maximum_interaction_range(self) -> float:
+        return self.pair.maximum_interaction_range
 
 
 @dataclass
@@ -762,6 +803,29 @@ class Microstate:
         _check(_lib.hmc_total_energy(self._h, C.byref(e)))
         return e.value
 
+    def set_hamiltonian(self, hamiltonian: PairwiseCutoff):
+        """The hamiltonian the next sweeps, QuickInsert, QuickCompress and total_energy use: the
+        system's own, or for convex shapes PairwiseCutoff(Anisotropic(ApproximateShapeOverlap)),
+        the insertion hamiltonian of place_single_site_orientable_bodies (hmc_set_shape_overlap)."""
+        pair = hamiltonian.pair
+        if isinstance(pair, Anisotropic) and isinstance(pair.interaction, ApproximateShapeOverlap):
+            a = pair.interaction
+            own = self.hamiltonian.pair
+            if not (isinstance(own, HardShape) and type(own.shape) is type(a.shape)
+                    and np.array_equal(np.asarray(own.shape.vertices), np.asarray(a.shape.vertices))):
+                raise HmcError(NOT_SUPPORTED, "the approximate shape overlap needs the system's own shape")
+            prm = hmc_shape_overlap_params(C.sizeof(hmc_shape_overlap_params), 0, a.resolution, pair.r_cut,
+                                           a.isotropic.k, a.isotropic.maximum_allowed_overlap,
+                                           a.isotropic.epsilon_shoulder)
+            _check(_lib.hmc_set_shape_overlap(self._h, C.byref(prm)))
+        elif hamiltonian is self.hamiltonian or (
+                isinstance(pair, HardShape) and isinstance(self.hamiltonian.pair, HardShape)
+                and type(pair.shape) is type(self.hamiltonian.pair.shape)
+                and np.array_equal(np.asarray(pair.shape.vertices), np.asarray(self.hamiltonian.pair.shape.vertices))):
+            _check(_lib.hmc_set_shape_overlap(self._h, None))
+        else:
+            raise HmcError(NOT_SUPPORTED, f"{type(pair).__name__} on a system of {type(self.hamiltonian.pair).__name__}")
+
 
 class QuickInsert:
     """hoomd_mc::QuickInsert (quick_insert.rs:94-280) with the distribution UniformIn over the
@@ -788,6 +852,8 @@ class QuickInsert:
         return bool(self._s.complete)
 
     def apply(self, microstate: Microstate, hamiltonian=None) -> Count:
+        if hamiltonian is not None:
+            microstate.set_hamiltonian(hamiltonian)
         c = hmc_count()
         _check(_lib.hmc_quick_insert_apply(microstate._h, C.byref(self._s), C.byref(c)))
         microstate.refresh()
@@ -844,8 +910,44 @@ class QuickCompress:
         return self._s.state == self.COMPLETE
 
     def apply(self, microstate: Microstate, hamiltonian=None):
+        if hamiltonian is not None:
+            microstate.set_hamiltonian(hamiltonian)
         _check(_lib.hmc_quick_compress_apply(microstate._h, C.byref(self._s)))
         microstate.edge_lengths = [float(x) for x in microstate.box()]
+
+
+def place_single_site_orientable_bodies(ctx: "Context", n: int, number_density: float,
+                                        maximum_interaction_range: float, insert_hamiltonian: PairwiseCutoff,
+                                        hamiltonian: PairwiseCutoff, dim: int, *, seed: int = 0,
+                                        max_steps: int = 1_000_000) -> "Microstate":
+    """place_single_site_orientable_bodies (benchmarks/src/place.rs:120-219): an empty periodic
+    box at half the number density, QuickInsert of n bodies, then QuickCompress to the target
+    density (either every 10 steps), a translation (0.03) and a rotation (0.1) ParallelSweep every
+    step, all under insert_hamiltonian (PairwiseCutoff(Anisotropic(ApproximateShapeOverlap))) at
+    kT = 1. Returns the microstate under `hamiltonian` (its HardShape)."""
+    initial_box_length = (n / (0.5 * number_density)) ** (1.0 / dim)
+    final_box_volume = n / number_density
+    g = Microstate(ctx, Periodic(maximum_interaction_range, [initial_box_length] * dim), np.zeros((0, dim)),
+                   hamiltonian, seed=seed, capacity=n,
+                   body_interaction_range=insert_hamiltonian.maximum_interaction_range)
+    g.set_hamiltonian(insert_hamiltonian)
+    quick_insert = QuickInsert.new(n)
+    quick_compress = QuickCompress.with_target_volume(final_box_volume)
+    for _ in range(max_steps):
+        if quick_compress.is_complete():
+            break
+        if g.step() % 10 == 0:
+            if quick_insert.is_complete():
+                quick_compress.apply(g)
+            else:
+                quick_insert.apply(g)
+        g.sweep(TRANSLATE, 0.03, 1.0, FP64)
+        g.sweep(ROTATE, 0.1, 1.0, FP64)
+        g.increment_step()
+    else:
+        raise HmcError(ITERATION_CAP, f"QuickCompress did not complete in {max_steps} steps")
+    g.set_hamiltonian(hamiltonian)
+    return g
 
 
 @dataclass
@@ -1070,7 +1172,8 @@ class ParallelSweep:
 __all__ = ["Batch", "Context", "sdf_pressure", "gr_normalise", "ConvexPolygon", "ConvexPolyhedron", "ConvexSurfaceMesh2d", "Count", "convex_hull_2d", "HardShape", "HardSphere", "HmcError", "Isothermal", "Isotropic",
            "LennardJones", "Microstate", "PairwiseCutoff", "Rotate", "Shifted", "TuneOptions",
            "ParallelSweep", "Periodic", "Translate", "load_library", "SIGNATURES", "FP64", "FP32_RECHECK",
-           "QuickInsert", "QuickCompress", "OverlapPenalty", "Expanded", "GrandCanonical", "IsothermalIsofugacity",
+           "QuickInsert", "QuickCompress", "OverlapPenalty", "ApproximateShapeOverlap", "Anisotropic",
+           "place_single_site_orientable_bodies", "Expanded", "GrandCanonical", "IsothermalIsofugacity",
            "InsertRemoveCount",
            "TRANSLATE", "ROTATE", "HARD_SPHERE", "HARD_CONVEX_POLYGON", "HARD_CONVEX_POLYHEDRON", "LENNARD_JONES",
            "HARD_CONVEX_SURFACE_MESH_2D"]

@@ -128,6 +128,9 @@ struct hmc_system {
     bool tags_permuted = false;  // some body was removed: index order is not tag order
     bool penalty() const { return interaction == HMC_OVERLAP_PENALTY; }
     bool soft() const { return interaction == HMC_LENNARD_JONES || penalty(); }
+    // the approximate shape overlap in place of HardShape (hmc_set_shape_overlap)
+    bool shape_soft = false;
+    ShapeOverlap so{};
     // profiling
     bool profiling = false;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -328,6 +331,7 @@ hmc_status check_flags(hmc_system* s) {
     if (f & kErrOutsideCheckerboard) return fail(HMC_OUTSIDE_CHECKERBOARD, "a body maps to no checkerboard space");
     if (f & kErrAngleRange) return fail(HMC_INVALID_ARGUMENT, "a 2-D orientation angle reached 2^19 rad");
     if (f & kErrCellOverflow) return fail(HMC_CELL_OVERFLOW, "a cell of the serial sweep's grid is full");
+    if (f & kErrIterationCap) return fail(HMC_ITERATION_CAP, "an approximate separation ran past its step bound");
     return HMC_OK;
 }
 
@@ -891,10 +895,12 @@ hmc_status hmc_sweep(hmc_system* s, const hmc_sweep_params* p, hmc_count* out) {
                     HMC_CUDA(launch_propose_lj(s->dim, fp32 && !s->penalty(), s->geom, s->arr, L, s->stream));
                     s->prof.kernel_launches += 1;
                 } else if (s->interaction == HMC_HARD_CONVEX_POLYHEDRON) {
-                    HMC_CUDA(launch_propose_poly(fp32, s->geom, s->arr, L, p->move == HMC_ROTATE, s->stream));
+                    HMC_CUDA(launch_propose_poly(fp32 && !s->shape_soft, s->geom, s->arr, L, p->move == HMC_ROTATE,
+                                                 s->shape_soft, s->stream));
                     s->prof.kernel_launches += 1;
                 } else if (s->polygon()) {
-                    HMC_CUDA(launch_propose_poly2(fp32, s->geom, s->arr, L, p->move == HMC_ROTATE, s->stream));
+                    HMC_CUDA(launch_propose_poly2(fp32 && !s->shape_soft, s->geom, s->arr, L, p->move == HMC_ROTATE,
+                                                  s->shape_soft, s->stream));
                     s->prof.kernel_launches += 1;
                 }
                 for (uint32_t c = 0; c < colors; ++c) {
@@ -906,6 +912,12 @@ hmc_status hmc_sweep(hmc_system* s, const hmc_sweep_params* p, hmc_count* out) {
                     if (s->soft())  // the overlap penalty has no FP32 path: FP64 in both modes
                         HMC_CUDA(launch_sweep_lj(s->dim, fp32 && !s->penalty(), s->geom, s->arr, s->pair, L,
                                                  s->stream, variant));
+                    else if (s->shape_soft && s->dim == 3)  // FP64 in both modes
+                        HMC_CUDA(launch_sweep_poly3_soft(s->geom, s->arr, s->verts, s->n_vertices, s->so, L,
+                                                         s->stream));
+                    else if (s->shape_soft)
+                        HMC_CUDA(launch_sweep_poly2_soft(s->geom, s->arr, s->verts, s->n_vertices, s->so, L,
+                                                         s->stream));
                     else if (s->interaction == HMC_HARD_CONVEX_POLYHEDRON)
                         HMC_CUDA(launch_sweep_poly(fp32, s->geom, s->arr, s->verts, s->n_vertices, s->poly_rcut2,
                                                    s->poly_rcut2_hi32, L, p->move == HMC_ROTATE, s->stream,
@@ -1035,6 +1047,8 @@ extern "C" {
 hmc_status hmc_autotune(hmc_system* s, const hmc_sweep_params* p, uint32_t sweeps, hmc_launch_variant* chosen,
                         double* ms_per_sweep) {
     if (!s || !p) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
+    if (s->shape_soft)
+        return fail(HMC_NOT_SUPPORTED, "hmc_autotune runs under HardShape: hmc_set_shape_overlap(s, NULL) first");
     if (p->struct_size < sizeof(hmc_sweep_params)) return fail(HMC_INVALID_ARGUMENT, "hmc_sweep_params.struct_size");
     if (p->precision > HMC_FP32_RECHECK) return fail(HMC_INVALID_ARGUMENT, "precision");
     if (sweeps == 0 || sweeps > 1000) return fail(HMC_INVALID_ARGUMENT, "sweeps must be in [1, 1000]");
@@ -1163,6 +1177,8 @@ static hmc_status serial_grid(hmc_system* s) {
 
 hmc_status hmc_serial_sweep(hmc_system* s, const hmc_sweep_params* p, const uint8_t* move_mask, hmc_count* out) {
     if (!s || !p) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
+    if (s->shape_soft)
+        return fail(HMC_NOT_SUPPORTED, "hmc_serial_sweep runs under HardShape: hmc_set_shape_overlap(s, NULL) first");
     if (p->struct_size < sizeof(hmc_sweep_params)) return fail(HMC_INVALID_ARGUMENT, "hmc_sweep_params.struct_size");
     if (p->move != HMC_TRANSLATE && !(p->move == HMC_ROTATE && s->oriented()))
         return fail(HMC_NOT_SUPPORTED, "rotation moves need oriented bodies (convex polyhedra or polygons)");
@@ -1245,6 +1261,8 @@ hmc_status hmc_profile_read(hmc_system* s, hmc_profile* out, int reset) {
 // lib.rs:514-524). The state and its counters are not modified.
 hmc_status hmc_tune(hmc_system* s, hmc_sweep_params* p, double target, uint32_t samples, uint32_t steps) {
     if (!s || !p) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
+    if (s->shape_soft)
+        return fail(HMC_NOT_SUPPORTED, "hmc_tune runs under HardShape: hmc_set_shape_overlap(s, NULL) first");
     if (p->struct_size < sizeof(hmc_sweep_params)) return fail(HMC_INVALID_ARGUMENT, "hmc_sweep_params.struct_size");
     if (!(target > 0.0 && target < 1.0)) return fail(HMC_INVALID_ARGUMENT, "target acceptance must be in (0, 1)");
     if (p->move != HMC_TRANSLATE && !(p->move == HMC_ROTATE && s->oriented()))
@@ -1436,6 +1454,23 @@ hmc_status hmc_gr(hmc_system* s, double r_max, uint32_t n_bins, uint64_t* counts
 
 hmc_status hmc_total_energy(hmc_system* s, double* energy) {
     if (!s || !energy) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
+    if (s->shape_soft) {
+        HMC_CUDA(cudaSetDevice(s->ctx->device));
+        hmc_status st = rebuild(s, true);
+        if (st) return st;
+        double* d = reinterpret_cast<double*>(&s->arr.stats->overlaps);  // 8 zeroed bytes after the rebuild
+        if (s->dim == 3)
+            HMC_CUDA(launch_energy_poly3_soft(s->geom, s->arr, s->verts, s->n_vertices, s->so, (uint32_t)s->n, d,
+                                              s->stream));
+        else
+            HMC_CUDA(launch_energy_poly2_soft(s->geom, s->arr, s->verts, s->n_vertices, s->so, (uint32_t)s->n, d,
+                                              s->stream));
+        s->prof.kernel_launches += 1;
+        if ((st = read_stats(s))) return st;
+        if ((st = check_flags(s))) return st;
+        std::memcpy(energy, &s->host_stats->overlaps, sizeof(double));
+        return HMC_OK;
+    }
     if (!s->soft()) {
         uint64_t n = 0;
         hmc_status st = hmc_overlap_check(s, &n);
@@ -1509,6 +1544,43 @@ static hmc_status map_into_box(hmc_system* s, const double* L) {
     return HMC_OK;
 }
 
+hmc_status hmc_set_shape_overlap(hmc_system* s, const hmc_shape_overlap_params* p) {
+    if (!s) return fail(HMC_INVALID_ARGUMENT, "NULL system");
+    if (!p) {
+        s->shape_soft = false;
+        return HMC_OK;
+    }
+    if (p->struct_size < sizeof(hmc_shape_overlap_params))
+        return fail(HMC_INVALID_ARGUMENT, "hmc_shape_overlap_params.struct_size");
+    if (s->interaction != HMC_HARD_CONVEX_POLYHEDRON && s->interaction != HMC_HARD_CONVEX_POLYGON)
+        return fail(HMC_NOT_SUPPORTED, "the approximate shape overlap is for Convex polyhedra and polygons");
+    if (!(p->resolution > 0.0) || !std::isfinite(p->resolution))
+        return fail(HMC_INVALID_ARGUMENT, "resolution must be positive");
+    if (!(p->penalty_k >= 0.0) || !std::isfinite(p->penalty_k) || !(p->penalty_maximum_overlap >= 0.0) ||
+        !std::isfinite(p->penalty_maximum_overlap) || !std::isfinite(p->penalty_shoulder))
+        return fail(HMC_INVALID_ARGUMENT, "overlap penalty k and maximum overlap must be finite and >= 0");
+    const double range = s->pair_range;  // R + R of the shape's bounding sphere
+    const double rcut = p->r_cut > 0.0 ? p->r_cut : range;
+    // every candidate lies in the 3^d spaces around the site only up to the pair range
+    if (!(rcut <= range)) return fail(HMC_NOT_SUPPORTED, "r_cut %g beyond the shape's range %g", rcut, range);
+    // A pair closer than r_cut <= R + R separates within (R + R) / resolution steps, since
+    // |v + direction * d| = |v| + d up to rounding; the device loop stops at this bound.
+    const double steps = std::ceil(range / p->resolution) + 8.0;
+    if (!(steps <= 4194304.0))
+        return fail(HMC_INVALID_ARGUMENT, "resolution %g takes more than 2^22 steps over the range %g", p->resolution,
+                    range);
+    ShapeOverlap& so = s->so;
+    so.resolution = p->resolution;
+    so.rcut = rcut;
+    so.rr = s->poly_rcut2;
+    so.dmax = p->penalty_maximum_overlap;
+    so.half_k = 0.5 * p->penalty_k;
+    so.shoulder = p->penalty_shoulder;
+    so.max_steps = (uint32_t)steps;
+    s->shape_soft = true;
+    return HMC_OK;
+}
+
 hmc_status hmc_set_box(hmc_system* s, const double* edge_lengths) {
     if (!s || !edge_lengths) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
     HMC_CUDA(cudaSetDevice(s->ctx->device));
@@ -1534,8 +1606,10 @@ static hmc_status body_tags(hmc_system* s, BodyTags* out) {
 
 hmc_status hmc_quick_insert_apply(hmc_system* s, hmc_quick_insert* qi, hmc_count* out) {
     if (!s || !qi) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
-    if (s->interaction != HMC_HARD_SPHERE && !s->penalty())
-        return fail(HMC_NOT_SUPPORTED, "QuickInsert places hard or overlap-penalty spheres");
+    if (s->interaction != HMC_HARD_SPHERE && !s->penalty() && !s->shape_soft)
+        return fail(HMC_NOT_SUPPORTED, "QuickInsert places hard or overlap-penalty spheres, or convex shapes "
+                                       "under the approximate shape overlap");
+    if (s->sat()) return fail(HMC_NOT_SUPPORTED, "the approximate shape overlap is for Convex polygons");
     if (qi->allowed_overlaps == 0) return fail(HMC_INVALID_ARGUMENT, "allowed_overlaps must be >= 1");
     if (qi->inserted > qi->target) return fail(HMC_INVALID_ARGUMENT, "inserted exceeds target");
     if (s->n + (qi->target - qi->inserted) > s->capacity)
@@ -1576,9 +1650,20 @@ hmc_status hmc_quick_insert_apply(hmc_system* s, hmc_quick_insert* qi, hmc_count
         HMC_CUDA(cudaMemsetAsync(s->arr.stats, 0, sizeof(DeviceStats), s->stream));
         BodyTags tags;
         if ((st = body_tags(s, &tags))) return st;
-        HMC_CUDA(launch_quick_insert(s->dim, s->geom, s->arr, s->pair, L, q, tags, s->serial_nc, s->serial_w,
-                                     s->serial_cap, s->serial_size, s->serial_items, s->serial_cell_of, s->serial_site,
-                                     s->qi_out, s->stream));
+        if (s->shape_soft && s->dim == 3)
+            HMC_CUDA(launch_quick_insert_poly3(s->geom, s->arr, s->verts, s->n_vertices, s->so, L, q, tags,
+                                               s->serial_nc, s->serial_w, s->serial_cap, s->serial_size,
+                                               s->serial_items, s->serial_cell_of, s->serial_site, s->qi_out,
+                                               s->stream));
+        else if (s->shape_soft)
+            HMC_CUDA(launch_quick_insert_poly2(s->geom, s->arr, s->verts, s->n_vertices, s->so, L, q, tags,
+                                               s->serial_nc, s->serial_w, s->serial_cap, s->serial_size,
+                                               s->serial_items, s->serial_cell_of, s->serial_site, s->qi_out,
+                                               s->stream));
+        else
+            HMC_CUDA(launch_quick_insert(s->dim, s->geom, s->arr, s->pair, L, q, tags, s->serial_nc, s->serial_w,
+                                         s->serial_cap, s->serial_size, s->serial_items, s->serial_cell_of,
+                                         s->serial_site, s->qi_out, s->stream));
         s->prof.kernel_launches += 2;
         unsigned long long r[4] = {0, 0, 0, 0};
         HMC_CUDA(cudaMemcpyAsync(r, s->qi_out, sizeof(r), cudaMemcpyDeviceToHost, s->stream));
@@ -1721,6 +1806,8 @@ hmc_status hmc_quick_compress_apply(hmc_system* s, hmc_quick_compress* qc) {
 hmc_status hmc_eval_moves(hmc_system* s, const hmc_injected_move* moves, uint64_t n, double temperature,
                           uint32_t precision, uint8_t* decisions, uint8_t* rechecked, double* delta_h) {
     if (!s || (n && (!moves || !decisions))) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
+    if (s->shape_soft)
+        return fail(HMC_NOT_SUPPORTED, "hmc_eval_moves runs under HardShape: hmc_set_shape_overlap(s, NULL) first");
     if (precision > HMC_FP32_RECHECK) return fail(HMC_INVALID_ARGUMENT, "precision");
     if (s->soft() && !(temperature > 0.0))
         return fail(HMC_INVALID_ARGUMENT, "temperature must be positive");
@@ -1808,6 +1895,8 @@ hmc_status hmc_eval_moves(hmc_system* s, const hmc_injected_move* moves, uint64_
 hmc_status hmc_eval_trials(hmc_system* s, const hmc_injected_move* moves, uint64_t n, double temperature,
                            uint32_t precision, uint8_t* decisions, uint8_t* flags) {
     if (!s || (n && (!moves || !decisions))) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
+    if (s->shape_soft)
+        return fail(HMC_NOT_SUPPORTED, "hmc_eval_trials runs under HardShape: hmc_set_shape_overlap(s, NULL) first");
     if (precision > HMC_FP32_RECHECK) return fail(HMC_INVALID_ARGUMENT, "precision");
     if (s->polygon()) return fail(HMC_NOT_SUPPORTED, "eval_trials: convex polygons");
     if (s->soft() && !(temperature > 0.0)) return fail(HMC_INVALID_ARGUMENT, "temperature must be positive");

@@ -460,6 +460,22 @@ __device__ __forceinline__ bool order_ambiguous(double du, double mag, uint32_t 
     return acc_at_lo != acc_at_hi;
 }
 
+// OverlapPenalty::energy (overlap_penalty.rs:109-115) at r = -d, d an approximate separation:
+// infinite below -maximum_allowed_overlap, (0.5 k) r^2 + epsilon_shoulder below 0, else 0.
+__device__ __forceinline__ double separation_penalty(const ShapeOverlap& so, double d) {
+    const double r = -d;
+    if (r < -so.dmax) return __longlong_as_double(0x7ff0000000000000ll);
+    if (r < 0.0) return dadd(dmul(so.half_k, dmul(r, r)), so.shoulder);
+    return 0.0;
+}
+
+// Butterfly sum over the warp (every lane ends with the same value).
+__device__ __forceinline__ double warp_sum64(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
 // ---- the sequential-stream tuner -------------------------------------------------------------
 // tune_local_trial (hoomd-mc/src/tune_local.rs:42-88) on one warp for job J (TuneJob). Every lane
 // runs the same single stream Counter(step, substep, seed).make_rng() (index 0), so the trial is

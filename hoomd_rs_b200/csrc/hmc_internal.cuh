@@ -15,6 +15,7 @@ enum : uint32_t {
     kErrNonFinite = 1u << 1,
     kErrAngleRange = 1u << 2,  // a 2-D orientation angle at or beyond 2^19 rad
     kErrCellOverflow = 1u << 3,  // a cell of the serial sweep's grid is full
+    kErrIterationCap = 1u << 4,  // an approximate separation loop ran past ShapeOverlap::max_steps
 };
 
 // Counters written by the kernels. Zeroed by the host before a sweep.
@@ -299,10 +300,41 @@ cudaError_t launch_sweep_lj(int dim, bool fp32, const Geometry& g, const Arrays&
 // per trial; launched in stream order before the round's colour passes of the passes that give a
 // trial several lanes (LJ and the overlap penalty, convex polyhedra, convex polygons).
 cudaError_t launch_propose_lj(int dim, bool fp32, const Geometry& g, const Arrays& a, const Launch& l, cudaStream_t s);
+// soft: the trial also draws the Metropolis uniform after the move (trial_t.w in 3-D, .z in 2-D).
 cudaError_t launch_propose_poly(bool fp32, const Geometry& g, const Arrays& a, const Launch& l, bool rotate,
-                                cudaStream_t s);
+                                bool soft, cudaStream_t s);
 cudaError_t launch_propose_poly2(bool fp32, const Geometry& g, const Arrays& a, const Launch& l, bool rotate,
-                                 cudaStream_t s);
+                                 bool soft, cudaStream_t s);
+
+// Anisotropic { ApproximateShapeOverlap { Convex(shape), OverlapPenalty, resolution }, r_cut }
+// (hoomd-interaction/src/pairwise/anisotropic.rs:120-135, approximate_shape_overlap.rs:122-131):
+// the insertion hamiltonian that place_single_site_orientable_bodies (benchmarks/src/place.rs:
+// 120-219) prepares convex shapes with. A pair closer than r_cut costs OverlapPenalty(-d), d the
+// distance (in steps of `resolution`) the other shape moves along the line of centres until the
+// two no longer intersect (IntersectsAt::approximate_separation_distance, hoomd-geometry/src/
+// lib.rs:307-325).
+struct ShapeOverlap {
+    double resolution;
+    double rcut;      // Anisotropic::r_cut, compared with the centre distance
+    double rr;        // (R + R)^2: the bounding-sphere test of Convex::intersects_at
+    double dmax;      // OverlapPenalty::maximum_allowed_overlap
+    double half_k;    // 0.5 * OverlapPenalty::k
+    double shoulder;  // OverlapPenalty::epsilon_shoulder
+    uint32_t max_steps;  // the separation loop ends within this many steps for every pair the host
+                         // admits (|v| < r_cut); more sets kErrIterationCap
+};
+// ParallelSweep colour pass under ShapeOverlap, FP64, one warp per trial (trials from
+// launch_propose_poly / launch_propose_poly2 with soft = true).
+cudaError_t launch_sweep_poly3_soft(const Geometry& g, const Arrays& a, const double4* verts, uint32_t nv,
+                                    const ShapeOverlap& so, const Launch& l, cudaStream_t s);
+cudaError_t launch_sweep_poly2_soft(const Geometry& g, const Arrays& a, const double4* verts, uint32_t nv,
+                                    const ShapeOverlap& so, const Launch& l, cudaStream_t s);
+// PairwiseCutoff::total_energy under ShapeOverlap (pairs i < j in body order, i's frame), summed
+// into *out with atomics.
+cudaError_t launch_energy_poly3_soft(const Geometry& g, const Arrays& a, const double4* verts, uint32_t nv,
+                                     const ShapeOverlap& so, uint32_t n, double* out, cudaStream_t s);
+cudaError_t launch_energy_poly2_soft(const Geometry& g, const Arrays& a, const double4* verts, uint32_t nv,
+                                     const ShapeOverlap& so, uint32_t n, double* out, cudaStream_t s);
 // delta_energy_one in FP64 for injected trial positions (LJ); u < 0 means no decision needed.
 cudaError_t launch_eval_lj(int dim, bool fp32, const Geometry& g, const Arrays& a, const Pair& p,
                            const uint64_t* bodies, const double4* trial, const double* u, double kt, uint32_t n,
@@ -383,6 +415,18 @@ cudaError_t launch_quick_insert(int dim, const Geometry& g, const Arrays& a, con
                                 const QuickInsertArgs& q, const BodyTags& tags, const uint32_t* nc, const double* w,
                                 uint32_t cap, uint32_t* size, uint32_t* items, uint32_t* cell_of, double4* site,
                                 unsigned long long* out, cudaStream_t s);
+// The same for oriented convex shapes under ShapeOverlap: each UniformIn body also draws a uniform
+// random orientation (uniform_in.rs:158-176).
+cudaError_t launch_quick_insert_poly3(const Geometry& g, const Arrays& a, const double4* verts, uint32_t nv,
+                                      const ShapeOverlap& so, const Launch& l, const QuickInsertArgs& q,
+                                      const BodyTags& tags, const uint32_t* nc, const double* w, uint32_t cap,
+                                      uint32_t* size, uint32_t* items, uint32_t* cell_of, double4* site,
+                                      unsigned long long* out, cudaStream_t s);
+cudaError_t launch_quick_insert_poly2(const Geometry& g, const Arrays& a, const double4* verts, uint32_t nv,
+                                      const ShapeOverlap& so, const Launch& l, const QuickInsertArgs& q,
+                                      const BodyTags& tags, const uint32_t* nc, const double* w, uint32_t cap,
+                                      uint32_t* size, uint32_t* items, uint32_t* cell_of, double4* site,
+                                      unsigned long long* out, cudaStream_t s);
 // GrandCanonical::apply, n_trials in sequence on the serial grid (one warp).
 struct GrandCanonicalArgs {
     uint64_t step;

@@ -333,7 +333,8 @@ __device__ __forceinline__ void drain_pairs(const Geometry& g, const Arrays& A, 
 // site T = wrap(W1) and its FP32 offsets; the packed pass reads them instead of computing each
 // move on the 8 lanes of its group.
 template <bool FP32>
-__global__ void __launch_bounds__(128) k_propose_poly3(Geometry g, Arrays A, Launch L, uint32_t rotate) {
+__global__ void __launch_bounds__(128) k_propose_poly3(Geometry g, Arrays A, Launch L, uint32_t rotate,
+                                                       uint32_t soft) {
     const DeviceStats* st = A.stats;
     if (st->error_flags != 0u || L.round >= st->rounds) return;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < 8u * g.color_stride; i += gridDim.x * blockDim.x) {
@@ -357,6 +358,8 @@ __global__ void __launch_bounds__(128) k_propose_poly3(Geometry g, Arrays A, Lau
             ball_sample<3>(rng, L.max_move, A.zig_x, A.zig_f, dv);
             for (int a = 0; a < 3; ++a) x[a] = dadd(x[a], dv[a]);
         }
+        // soft: the Metropolis uniform, the stream's next draw after the move
+        const double u = soft ? uniform01(rng) : 0.0;
         wrap_inv<3>(g.L, g.invL, x);  // W1 = wrap(propose(..))
         uint32_t mt[3];
         if (!(point_to_space<3>(g, x, mt) && cell_index<3>(g, mt) == cell)) {
@@ -365,7 +368,7 @@ __global__ void __launch_bounds__(128) k_propose_poly3(Geometry g, Arrays A, Lau
         }
         double t[3] = {x[0], x[1], x[2]};
         wrap_inv<3>(g.L, g.invL, t);
-        A.trial_t[i] = make_double4(t[0], t[1], t[2], 0.0);
+        A.trial_t[i] = make_double4(t[0], t[1], t[2], u);
         A.trial_q[i] = make_double4(qi.s, qi.x, qi.y, qi.z);
         if (FP32) A.trial_o[i] = cell_offsets<3>(g, t, m);
         A.trial_k[i] = k;
@@ -512,6 +515,223 @@ __global__ void __launch_bounds__(128, HMC_POLY_MIN_BLOCKS)
     grid_dependency_wait();
     allow_dependent_launch();
     flush_stats(A.stats, st, n_accepted);
+}
+
+// ---- the insertion hamiltonian: approximate shape overlap -----------------------------------
+// Anisotropic::site_pair_energy (anisotropic.rs:120-135) of ApproximateShapeOverlap
+// (approximate_shape_overlap.rs:122-131) for the site t with versor qi against the site sj (image
+// rule) with versor qj: 0 at a centre distance >= r_cut, else pair_system_to_local and
+// IntersectsAt::approximate_separation_distance (hoomd-geometry/src/lib.rs:307-325): the
+// direction v / |v| (lib.rs:632-639; the last axis for v = 0, cartesian.rs:313-318) and d grown
+// by `resolution` while Convex::intersects_at (convex.rs:130-143: the bounding spheres,
+// |w|^2 <= (R + R)^2, then XenoCollide) holds at w = v + direction * d; the energy is
+// OverlapPenalty(-d).
+__device__ __forceinline__ double shape_overlap3(const Geometry& g, const PolyShape& sh, const ShapeOverlap& so,
+                                                 const double* t, const Q& qi, const double* sj, const Q& qj,
+                                                 uint32_t& capped) {
+    double d[3];
+    const double d2 = ref_disp<3>(g, t, sj, d);
+    if (dsqrt(d2) >= so.rcut) return 0.0;
+    const V3 rab{-d[0], -d[1], -d[2]};  // image - t
+    const Q ia{qi.s, -qi.x, -qi.y, -qi.z};
+    const V3 v = vrotate(ia, rab);
+    const Q oij = qmul(ia, qj);
+    const double norm = dsqrt(dot3(v, v));
+    const V3 dir = norm == 0.0 ? V3{0.0, 0.0, 1.0} : V3{ddiv(v.x, norm), ddiv(v.y, norm), ddiv(v.z, norm)};
+    double sep = 0.0;
+    for (uint32_t step = 0;; ++step) {
+        const V3 w{dadd(v.x, dmul(dir.x, sep)), dadd(v.y, dmul(dir.y, sep)), dadd(v.z, dmul(dir.z, sep))};
+        if (!(dot3(w, w) <= so.rr) || !collide3d(sh.verts, sh.nv, w, oij)) break;
+        if (step >= so.max_steps) {
+            capped = 1;
+            break;
+        }
+        sep = dadd(sep, so.resolution);
+    }
+    return separation_penalty(so, sep);
+}
+
+// ParallelSweep colour pass under the approximate shape overlap (FP64 in both precision modes):
+// one warp per trial from k_propose_poly3 (soft), the stencil's candidates 32 at a time. Each lane
+// adds the pair energies of the trial (T, q) and of the body's current site (S, q_k) against its
+// candidates; butterfly sums give E_final and E_initial (delta_energy_one, pairwise_cutoff.rs:
+// 919-941: an infinite pair makes E_final infinite and the move is rejected) and the Metropolis
+// test (parallel_sweep.rs:267-268) uses the uniform drawn after the move.
+__global__ void __launch_bounds__(128) k_sweep_poly3_soft(Geometry g, Arrays A, PolyShape sh, ShapeOverlap so,
+                                                          Launch L) {
+    if (L.early_wait) grid_dependency_wait();  // first pass: the rebuild's arrays are read at once
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t n_warps = (gridDim.x * blockDim.x) >> 5;
+    uint32_t n_accepted = 0, capped = 0;
+    PairStats pst;
+    const uint32_t n_active = active_count(A, L.color, L.round);
+    for (uint32_t w = warp; w < n_active; w += n_warps) {
+        const size_t e = (size_t)L.color * g.color_stride + w;
+        const uint32_t k = __ldg(A.trial_k + e);
+        if (k == kNoTrial) continue;  // warp-uniform: the move left its space
+        uint32_t m[3] = {0, 0, 0};
+        unpack_m<3>(__ldg(A.color_cells + e), m);
+        const double4 t4 = ldg4(A.trial_t + e);
+        const double t[3] = {t4.x, t4.y, t4.z};
+        const double u = t4.w;
+        const double4 q4 = ldg4(A.trial_q + e);
+        const Q qt{q4.x, q4.y, q4.z, q4.w};
+        const FlatStencil fs = flat_stencil<3>(g, A.cell_start, m, lane);
+        grid_dependency_wait();  // the previous colour's moves are visible from here on
+        allow_dependent_launch();
+        const double4 s4 = ldg4(A.sorted_s + k);
+        const double si[3] = {s4.x, s4.y, s4.z};
+        const double4 o4 = ldg4(A.sorted_q + k);
+        const Q qk{o4.x, o4.y, o4.z, o4.w};
+        double a = 0.0, b = 0.0, mag = 0.0;
+#pragma unroll 1
+        for (uint32_t j0 = 0; j0 < fs.total; j0 += 32) {
+            const uint32_t j = j0 + lane;
+            uint32_t part;
+            const uint32_t q = flat_slot(fs, j, part);
+            if (j < fs.total && q != k) {
+                const double4 c4 = ldg4(A.sorted_s + q);
+                const double sj[3] = {c4.x, c4.y, c4.z};
+                const double4 cq = ldg4(A.sorted_q + q);
+                const Q qj{cq.x, cq.y, cq.z, cq.w};
+                const double x = shape_overlap3(g, sh, so, t, qt, sj, qj, capped);
+                const double y = shape_overlap3(g, sh, so, si, qk, sj, qj, capped);
+                a = dadd(a, x);
+                b = dadd(b, y);
+                mag += fabs(x) + fabs(y);
+                pst.checks += 2;
+            }
+        }
+        const double e_new = warp_sum64(a), e_old = warp_sum64(b);
+        mag = warp_sum64(mag);
+        const double du = dsub(e_new, e_old);
+        const double e0 = exp(ddiv(-du, L.kt));
+        if (lane == 0 && order_ambiguous(du, mag, fs.total, u, L.kt, e0)) pst.ambiguous++;
+        if ((du <= 0.0 || u < e0) && lane == 0) {
+            n_accepted++;
+            double sv[3] = {t[0], t[1], t[2]};
+            wrap_inv<3>(g.L, g.invL, sv);
+            const uint32_t body = A.sorted_body[k];
+            A.sorted_b[k] = make_double4(t[0], t[1], t[2], 0.0);
+            A.sorted_s[k] = make_double4(sv[0], sv[1], sv[2], 0.0);
+            A.sorted_off[k] = cell_offsets<3>(g, sv, m);
+            A.sorted_q[k] = make_double4(qt.s, qt.x, qt.y, qt.z);
+            A.body_pos[body] = make_double4(t[0], t[1], t[2], 0.0);
+            A.body_ori[body] = make_double4(qt.s, qt.x, qt.y, qt.z);
+        }
+        __syncwarp();
+    }
+    if (__any_sync(0xffffffffu, capped != 0u) && lane == 0) atomicOr(&A.stats->error_flags, kErrIterationCap);
+    grid_dependency_wait();
+    allow_dependent_launch();
+    flush_stats(A.stats, pst, n_accepted);
+}
+
+// PairwiseCutoff::total_energy (pairwise_cutoff.rs:720-745) under the approximate shape overlap:
+// one thread per body i adds the pairs with the bodies j > i of its stencil in i's frame (the
+// reference's site_tag_i < site_tag_j; tags are body indices here), summed with atomics.
+__global__ void k_energy_poly3_soft(Geometry g, Arrays A, PolyShape sh, ShapeOverlap so, uint32_t n, double* out) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t capped = 0;
+    if (k < n) {
+        const uint32_t bi = A.sorted_body[k];
+        const double4 s4 = A.sorted_s[k];
+        const double t[3] = {s4.x, s4.y, s4.z};
+        const double4 o4 = A.sorted_q[k];
+        const Q qi{o4.x, o4.y, o4.z, o4.w};
+        uint32_t m[3];
+        uint32_t c = A.body_cell[bi];
+        for (int a = 2; a >= 0; --a) {
+            m[a] = c % g.shape[a];
+            c /= g.shape[a];
+        }
+        double e = 0.0;
+        for_each_neighbor<3>(g, A.cell_start, m, [&](uint32_t q, const float*) -> bool {
+            if (A.sorted_body[q] <= bi) return false;
+            const double4 c4 = A.sorted_s[q];
+            const double sj[3] = {c4.x, c4.y, c4.z};
+            const double4 cq = A.sorted_q[q];
+            e = dadd(e, shape_overlap3(g, sh, so, t, qi, sj, Q{cq.x, cq.y, cq.z, cq.w}, capped));
+            return false;
+        });
+        atomicAdd(out, e);
+    }
+    if (capped) atomicOr(&A.stats->error_flags, kErrIterationCap);
+}
+
+// QuickInsert's insertion loop (k_quick_insert in hmc_serial.cu) for convex polyhedra under the
+// approximate shape overlap, one warp: a UniformIn body draws its position per axis, then a
+// uniform random versor (StandardUniform for Versor, quaternion.rs:863-885: four standard normals,
+// scalar first, divided by sqrt(|v|^2 + s^2)); only whether the insertion energy is infinite or
+// positive matters, and single pairs decide both.
+__global__ void __launch_bounds__(32) k_quick_insert_poly3(Geometry g, Arrays A, SerialGrid G, PolyShape sh,
+                                                           ShapeOverlap so, Launch L, QuickInsertArgs q, BodyTags T,
+                                                           unsigned long long* out) {
+    const uint32_t lane = threadIdx.x;
+    if (A.stats->error_flags) return;
+    Sfc64 rng = make_rng(L.step, L.substep, L.seed, 0);
+    uint32_t n = q.n0, capped = 0;
+    uint64_t inserted = 0, overlapping = 0, rejected = 0;
+    for (uint64_t attempt = 0; attempt < q.attempts; ++attempt) {
+        double x[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const double u = dsub(as_double(0x3FF0000000000000ULL | (rng.next_u64() >> 12)), 1.0);
+            x[a] = dadd(dmul(u, q.scale[a]), q.low[a]);
+        }
+        const double sc = standard_normal(rng, A.zig_x, A.zig_f);
+        V3 vv;
+        vv.x = standard_normal(rng, A.zig_x, A.zig_f);
+        vv.y = standard_normal(rng, A.zig_x, A.zig_f);
+        vv.z = standard_normal(rng, A.zig_x, A.zig_f);
+        const double norm = dsqrt(dadd(dot3(vv, vv), dmul(sc, sc)));
+        const Q o{ddiv(sc, norm), ddiv(vv.x, norm), ddiv(vv.y, norm), ddiv(vv.z, norm)};
+        double t[3] = {x[0], x[1], x[2]};
+        wrap_inv<3>(g.L, g.invL, t);
+        uint32_t m[3] = {0, 0, 0}, cell;
+        serial_cell<3>(g, G, t, m);
+        bool inf = false, pos = false;
+        if (lane_cell<3>(G, m, lane, &cell)) {
+            const uint32_t cnt = G.size[cell];
+            for (uint32_t kk = 0; kk < cnt && !inf; ++kk) {
+                const uint32_t j = G.items[(size_t)cell * G.cap + kk];
+                const double4 s4 = G.site[j];
+                const double sv[3] = {s4.x, s4.y, s4.z};
+                const double4 oj = A.body_ori[j];
+                const double e = shape_overlap3(g, sh, so, t, o, sv, Q{oj.x, oj.y, oj.z, oj.w}, capped);
+                inf = e == __longlong_as_double(0x7ff0000000000000ll);
+                pos = pos || e > 0.0;
+            }
+        }
+        inf = __any_sync(0xffffffffu, inf);
+        pos = __any_sync(0xffffffffu, pos);
+        if (inf) {
+            rejected++;
+            continue;
+        }
+        if (n >= q.capacity) {
+            if (lane == 0) atomicOr(&A.stats->error_flags, kErrCellOverflow);
+            break;
+        }
+        if (lane == 0) {
+            grid_append<3>(g, A, G, T, n, x);
+            A.body_ori[n] = make_double4(o.s, o.x, o.y, o.z);
+        }
+        __syncwarp();
+        n++;
+        inserted++;
+        if (pos) overlapping++;
+        if (inserted == q.to_insert || overlapping >= q.allowed) break;
+        if (A.stats->error_flags) break;
+    }
+    if (__any_sync(0xffffffffu, capped != 0u) && lane == 0) atomicOr(&A.stats->error_flags, kErrIterationCap);
+    if (lane == 0) {
+        out[0] = inserted;
+        out[1] = overlapping;
+        out[2] = rejected;
+        out[3] = n;
+    }
 }
 
 // Injected moves (position and versor): warp per move, decision in the requested mode.
@@ -771,16 +991,48 @@ cudaError_t launch_serial_poly(const Geometry& g, const Arrays& a, const double4
 }
 
 cudaError_t launch_propose_poly(bool fp32, const Geometry& g, const Arrays& a, const Launch& l, bool rotate,
-                                cudaStream_t s) {
+                                bool soft, cudaStream_t s) {
     const uint64_t n = (uint64_t)g.color_stride << 3;
     if (n == 0) return cudaSuccess;
     const int wave = resident_wave((const void*)(fp32 ? k_propose_poly3<true> : k_propose_poly3<false>));
     uint32_t blocks = (uint32_t)((n + 127) / 128);
     if (blocks > (uint32_t)wave) blocks = (uint32_t)wave;
     if (fp32)
-        k_propose_poly3<true><<<blocks, 128, 0, s>>>(g, a, l, rotate ? 1u : 0u);
+        k_propose_poly3<true><<<blocks, 128, 0, s>>>(g, a, l, rotate ? 1u : 0u, soft ? 1u : 0u);
     else
-        k_propose_poly3<false><<<blocks, 128, 0, s>>>(g, a, l, rotate ? 1u : 0u);
+        k_propose_poly3<false><<<blocks, 128, 0, s>>>(g, a, l, rotate ? 1u : 0u, soft ? 1u : 0u);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sweep_poly3_soft(const Geometry& g, const Arrays& a, const double4* verts, uint32_t nv,
+                                    const ShapeOverlap& so, const Launch& l, cudaStream_t s) {
+    if (l.n_active == 0) return cudaSuccess;
+    PolyShape sh{verts, nv, so.rr, 0.f};
+    const int wave = resident_wave((const void*)k_sweep_poly3_soft);
+    uint32_t blocks = (l.n_active + 3) / 4;  // four warps (trials) per block
+    if (blocks > (uint32_t)wave) blocks = (uint32_t)wave;
+    PassLaunch pl(blocks, l.overlap_previous != 0 || l.early_wait != 0, s);
+    return cudaLaunchKernelEx(&pl.cfg, k_sweep_poly3_soft, g, a, sh, so, l);
+}
+
+cudaError_t launch_energy_poly3_soft(const Geometry& g, const Arrays& a, const double4* verts, uint32_t nv,
+                                     const ShapeOverlap& so, uint32_t n, double* out, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    PolyShape sh{verts, nv, so.rr, 0.f};
+    k_energy_poly3_soft<<<(n + 127) / 128, 128, 0, s>>>(g, a, sh, so, n, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_quick_insert_poly3(const Geometry& g, const Arrays& a, const double4* verts, uint32_t nv,
+                                      const ShapeOverlap& so, const Launch& l, const QuickInsertArgs& q,
+                                      const BodyTags& tags, const uint32_t* nc, const double* w, uint32_t cap,
+                                      uint32_t* size, uint32_t* items, uint32_t* cell_of, double4* site,
+                                      unsigned long long* out, cudaStream_t s) {
+    const SerialGrid G = make_grid(3, nc, w, cap, size, items, cell_of, site);
+    cudaError_t e = build_grid(3, g, a, G, q.n0, s);
+    if (e != cudaSuccess) return e;
+    PolyShape sh{verts, nv, so.rr, 0.f};
+    k_quick_insert_poly3<<<1, 32, 0, s>>>(g, a, G, sh, so, l, q, tags, out);
     return cudaGetLastError();
 }
 

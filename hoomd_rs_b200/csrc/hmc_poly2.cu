@@ -372,6 +372,216 @@ __global__ void __launch_bounds__(128, HMC_POLY2_MIN_BLOCKS)
     flush_stats(A.stats, st, n_accepted);
 }
 
+// ---- the insertion hamiltonian: approximate shape overlap -----------------------------------
+// Anisotropic::site_pair_energy (anisotropic.rs:120-135) of ApproximateShapeOverlap
+// (approximate_shape_overlap.rs:122-131) for the site t with angle ti against the site sj (image
+// rule) with angle tj: 0 at a centre distance >= r_cut, else pair_system_to_local (Angle::rotate
+// by -ti, o_ij = -ti + tj) and IntersectsAt::approximate_separation_distance (hoomd-geometry/src/
+// lib.rs:307-325): the direction v / |v| (the last axis for v = 0) and d grown by `resolution`
+// while Convex::intersects_at (convex.rs:87-99: the bounding circles, |w|^2 <= (R + R)^2, then
+// XenoCollide) holds at w = v + direction * d; the energy is OverlapPenalty(-d). An angle beyond
+// cr_sincos's range sets *range_error and counts as infinite.
+__device__ __forceinline__ double shape_overlap2(const Geometry& g, const PolyShape2& sh, const ShapeOverlap& so,
+                                                 const double* t, double ti, const double* sj, double tj,
+                                                 uint32_t& capped, bool* range_error) {
+    double d[3];
+    const double d2 = ref_disp<2>(g, t, sj, d);
+    if (dsqrt(d2) >= so.rcut) return 0.0;
+    const V2 rab{-d[0], -d[1]};  // image - t
+    const double inv = -ti;
+    double sn, cs;
+    M2 m;
+    if (!cr_sincos(inv, &sn, &cs) || !mat2_from_angle(dadd(inv, tj), &m)) {
+        *range_error = true;
+        return __longlong_as_double(0x7ff0000000000000ll);
+    }
+    const V2 v{dsub(dmul(rab.x, cs), dmul(rab.y, sn)), dadd(dmul(rab.x, sn), dmul(rab.y, cs))};
+    const double norm = dsqrt(dot2(v, v));
+    const V2 dir = norm == 0.0 ? V2{0.0, 1.0} : V2{ddiv(v.x, norm), ddiv(v.y, norm)};
+    double sep = 0.0;
+    for (uint32_t step = 0;; ++step) {
+        const V2 w{dadd(v.x, dmul(dir.x, sep)), dadd(v.y, dmul(dir.y, sep))};
+        if (!(dot2(w, w) <= so.rr) || !collide2d(sh.verts, sh.nv, w, m)) break;
+        if (step >= so.max_steps) {
+            capped = 1;
+            break;
+        }
+        sep = dadd(sep, so.resolution);
+    }
+    return separation_penalty(so, sep);
+}
+
+// ParallelSweep colour pass of convex polygons under the approximate shape overlap (FP64), one
+// warp per trial from k_propose_poly2 (soft: the uniform in trial_t.z, the angle in .w); the
+// sums and the Metropolis test as in k_sweep_poly3_soft.
+__global__ void __launch_bounds__(128) k_sweep_poly2_soft(Geometry g, Arrays A, PolyShape2 sh, ShapeOverlap so,
+                                                          Launch L) {
+    if (L.early_wait) grid_dependency_wait();  // first pass: the rebuild's arrays are read at once
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t n_warps = (gridDim.x * blockDim.x) >> 5;
+    uint32_t n_accepted = 0, capped = 0;
+    bool range_error = false;
+    PairStats pst;
+    const uint32_t n_active = active_count(A, L.color, L.round);
+    for (uint32_t w = warp; w < n_active; w += n_warps) {
+        const size_t e = (size_t)L.color * g.color_stride + w;
+        const uint32_t k = __ldg(A.trial_k + e);
+        if (k == kNoTrial) continue;  // warp-uniform: the move left its space
+        uint32_t m[3] = {0, 0, 0};
+        unpack_m<2>(__ldg(A.color_cells + e), m);
+        const double4 t4 = ldg4(A.trial_t + e);
+        const double t[3] = {t4.x, t4.y, 0.0};
+        const double u = t4.z, tt = t4.w;
+        const FlatStencil fs = flat_stencil<2>(g, A.cell_start, m, lane);
+        grid_dependency_wait();  // the previous colour's moves are visible from here on
+        allow_dependent_launch();
+        const double4 s4 = ldg4(A.sorted_s + k);
+        const double si[3] = {s4.x, s4.y, 0.0};
+        const double tk = __ldg(&A.sorted_q[k].x);
+        double a = 0.0, b = 0.0, mag = 0.0;
+#pragma unroll 1
+        for (uint32_t j0 = 0; j0 < fs.total; j0 += 32) {
+            const uint32_t j = j0 + lane;
+            uint32_t part;
+            const uint32_t q = flat_slot(fs, j, part);
+            if (j < fs.total && q != k) {
+                const double4 c4 = ldg4(A.sorted_s + q);
+                const double sj[3] = {c4.x, c4.y, 0.0};
+                const double tj = __ldg(&A.sorted_q[q].x);
+                const double x = shape_overlap2(g, sh, so, t, tt, sj, tj, capped, &range_error);
+                const double y = shape_overlap2(g, sh, so, si, tk, sj, tj, capped, &range_error);
+                a = dadd(a, x);
+                b = dadd(b, y);
+                mag += fabs(x) + fabs(y);
+                pst.checks += 2;
+            }
+        }
+        const double e_new = warp_sum64(a), e_old = warp_sum64(b);
+        mag = warp_sum64(mag);
+        const double du = dsub(e_new, e_old);
+        const double e0 = exp(ddiv(-du, L.kt));
+        if (lane == 0 && order_ambiguous(du, mag, fs.total, u, L.kt, e0)) pst.ambiguous++;
+        if ((du <= 0.0 || u < e0) && lane == 0) {
+            n_accepted++;
+            double sv[3] = {t[0], t[1], 0.0};
+            wrap_inv<2>(g.L, g.invL, sv);
+            const uint32_t body = A.sorted_body[k];
+            A.sorted_b[k] = make_double4(t[0], t[1], 0.0, 0.0);
+            A.sorted_s[k] = make_double4(sv[0], sv[1], 0.0, 0.0);
+            A.sorted_off[k] = cell_offsets<2>(g, sv, m);
+            A.sorted_q[k] = make_double4(tt, 0.0, 0.0, 0.0);
+            A.body_pos[body] = make_double4(t[0], t[1], 0.0, 0.0);
+            A.body_ori[body] = make_double4(tt, 0.0, 0.0, 0.0);
+        }
+        __syncwarp();
+    }
+    if (__any_sync(0xffffffffu, capped != 0u) && lane == 0) atomicOr(&A.stats->error_flags, kErrIterationCap);
+    if (range_error) atomicOr(&A.stats->error_flags, kErrAngleRange);
+    grid_dependency_wait();
+    allow_dependent_launch();
+    flush_stats(A.stats, pst, n_accepted);
+}
+
+// PairwiseCutoff::total_energy under the approximate shape overlap for polygons (as
+// k_energy_poly3_soft).
+__global__ void k_energy_poly2_soft(Geometry g, Arrays A, PolyShape2 sh, ShapeOverlap so, uint32_t n, double* out) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t capped = 0;
+    bool range_error = false;
+    if (k < n) {
+        const uint32_t bi = A.sorted_body[k];
+        const double4 s4 = A.sorted_s[k];
+        const double t[3] = {s4.x, s4.y, 0.0};
+        const double ti = A.sorted_q[k].x;
+        uint32_t m[3] = {0, 0, 0};
+        uint32_t c = A.body_cell[bi];
+        for (int a = 1; a >= 0; --a) {
+            m[a] = c % g.shape[a];
+            c /= g.shape[a];
+        }
+        double e = 0.0;
+        for_each_neighbor<2>(g, A.cell_start, m, [&](uint32_t q, const float*) -> bool {
+            if (A.sorted_body[q] <= bi) return false;
+            const double4 c4 = A.sorted_s[q];
+            const double sj[3] = {c4.x, c4.y, 0.0};
+            e = dadd(e, shape_overlap2(g, sh, so, t, ti, sj, A.sorted_q[q].x, capped, &range_error));
+            return false;
+        });
+        atomicAdd(out, e);
+    }
+    if (capped) atomicOr(&A.stats->error_flags, kErrIterationCap);
+    if (range_error) atomicOr(&A.stats->error_flags, kErrAngleRange);
+}
+
+// QuickInsert's insertion loop for convex polygons under the approximate shape overlap, one warp
+// (k_quick_insert_poly3 with the angle drawn from Uniform::new(0, 2 pi), angle.rs:268-285).
+__global__ void __launch_bounds__(32) k_quick_insert_poly2(Geometry g, Arrays A, SerialGrid G, PolyShape2 sh,
+                                                           ShapeOverlap so, Launch L, QuickInsertArgs q, BodyTags T,
+                                                           unsigned long long* out) {
+    const uint32_t lane = threadIdx.x;
+    if (A.stats->error_flags) return;
+    Sfc64 rng = make_rng(L.step, L.substep, L.seed, 0);
+    uint32_t n = q.n0, capped = 0;
+    bool range_error = false;
+    uint64_t inserted = 0, overlapping = 0, rejected = 0;
+    const double two_pi = dmul(2.0, 3.141592653589793);
+    for (uint64_t attempt = 0; attempt < q.attempts; ++attempt) {
+        double x[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int a = 0; a < 2; ++a) {
+            const double u = dsub(as_double(0x3FF0000000000000ULL | (rng.next_u64() >> 12)), 1.0);
+            x[a] = dadd(dmul(u, q.scale[a]), q.low[a]);
+        }
+        const double ua = dsub(as_double(0x3FF0000000000000ULL | (rng.next_u64() >> 12)), 1.0);
+        const double o = dadd(dmul(ua, dsub(two_pi, 0.0)), 0.0);
+        double t[3] = {x[0], x[1], 0.0};
+        wrap_inv<2>(g.L, g.invL, t);
+        uint32_t m[3] = {0, 0, 0}, cell;
+        serial_cell<2>(g, G, t, m);
+        bool inf = false, pos = false;
+        if (lane_cell<2>(G, m, lane, &cell)) {
+            const uint32_t cnt = G.size[cell];
+            for (uint32_t kk = 0; kk < cnt && !inf; ++kk) {
+                const uint32_t j = G.items[(size_t)cell * G.cap + kk];
+                const double4 s4 = G.site[j];
+                const double sv[3] = {s4.x, s4.y, 0.0};
+                const double e = shape_overlap2(g, sh, so, t, o, sv, A.body_ori[j].x, capped, &range_error);
+                inf = e == __longlong_as_double(0x7ff0000000000000ll);
+                pos = pos || e > 0.0;
+            }
+        }
+        inf = __any_sync(0xffffffffu, inf);
+        pos = __any_sync(0xffffffffu, pos);
+        if (inf) {
+            rejected++;
+            continue;
+        }
+        if (n >= q.capacity) {
+            if (lane == 0) atomicOr(&A.stats->error_flags, kErrCellOverflow);
+            break;
+        }
+        if (lane == 0) {
+            grid_append<2>(g, A, G, T, n, x);
+            A.body_ori[n] = make_double4(o, 0.0, 0.0, 0.0);
+        }
+        __syncwarp();
+        n++;
+        inserted++;
+        if (pos) overlapping++;
+        if (inserted == q.to_insert || overlapping >= q.allowed) break;
+        if (A.stats->error_flags) break;
+    }
+    if (__any_sync(0xffffffffu, capped != 0u) && lane == 0) atomicOr(&A.stats->error_flags, kErrIterationCap);
+    if (__any_sync(0xffffffffu, range_error) && lane == 0) atomicOr(&A.stats->error_flags, kErrAngleRange);
+    if (lane == 0) {
+        out[0] = inserted;
+        out[1] = overlapping;
+        out[2] = rejected;
+        out[3] = n;
+    }
+}
+
 // Injected moves (position and angle): warp per move.
 template <bool FP32, bool SAT>
 __global__ void __launch_bounds__(128) k_eval_poly2(Geometry g, Arrays A, PolyShape2 sh, const uint64_t* bodies,
@@ -450,7 +660,8 @@ __global__ void __launch_bounds__(32) k_tune_stream_poly2(TuneJob* jobs, uint32_
 // 46-55), W1 = wrap(propose(..)), the space check, T = wrap(W1) with the angle in .w, and T's FP32
 // offsets; the packed pass reads them instead of computing each move on the 8 lanes of its group.
 template <bool FP32>
-__global__ void __launch_bounds__(128) k_propose_poly2(Geometry g, Arrays A, Launch L, uint32_t rotate) {
+__global__ void __launch_bounds__(128) k_propose_poly2(Geometry g, Arrays A, Launch L, uint32_t rotate,
+                                                       uint32_t soft) {
     const DeviceStats* st = A.stats;
     if (st->error_flags != 0u || L.round >= st->rounds) return;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < 4u * g.color_stride; i += gridDim.x * blockDim.x) {
@@ -475,6 +686,8 @@ __global__ void __launch_bounds__(128) k_propose_poly2(Geometry g, Arrays A, Lau
             x[0] = dadd(x[0], dv[0]);
             x[1] = dadd(x[1], dv[1]);
         }
+        // soft: the Metropolis uniform, the stream's next draw after the move
+        const double u = soft ? uniform01(rng) : 0.0;
         wrap_inv<2>(g.L, g.invL, x);  // W1 = wrap(propose(..))
         uint32_t mt[3];
         if (!(point_to_space<2>(g, x, mt) && cell_index<2>(g, mt) == cell)) {
@@ -483,7 +696,7 @@ __global__ void __launch_bounds__(128) k_propose_poly2(Geometry g, Arrays A, Lau
         }
         double t[3] = {x[0], x[1], 0.0};
         wrap_inv<2>(g.L, g.invL, t);
-        A.trial_t[i] = make_double4(t[0], t[1], 0.0, ti);
+        A.trial_t[i] = make_double4(t[0], t[1], u, ti);
         if (FP32) A.trial_o[i] = cell_offsets<2>(g, t, m);
         A.trial_k[i] = k;
     }
@@ -622,16 +835,48 @@ cudaError_t launch_sweep_poly2(bool fp32, bool sat, const Geometry& g, const Arr
 }
 
 cudaError_t launch_propose_poly2(bool fp32, const Geometry& g, const Arrays& a, const Launch& l, bool rotate,
-                                 cudaStream_t s) {
+                                 bool soft, cudaStream_t s) {
     const uint64_t n = (uint64_t)g.color_stride << 2;
     if (n == 0) return cudaSuccess;
     const int wave = resident_wave((const void*)(fp32 ? k_propose_poly2<true> : k_propose_poly2<false>));
     uint32_t blocks = (uint32_t)((n + 127) / 128);
     if (blocks > (uint32_t)wave) blocks = (uint32_t)wave;
     if (fp32)
-        k_propose_poly2<true><<<blocks, 128, 0, s>>>(g, a, l, rotate ? 1u : 0u);
+        k_propose_poly2<true><<<blocks, 128, 0, s>>>(g, a, l, rotate ? 1u : 0u, soft ? 1u : 0u);
     else
-        k_propose_poly2<false><<<blocks, 128, 0, s>>>(g, a, l, rotate ? 1u : 0u);
+        k_propose_poly2<false><<<blocks, 128, 0, s>>>(g, a, l, rotate ? 1u : 0u, soft ? 1u : 0u);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sweep_poly2_soft(const Geometry& g, const Arrays& a, const double4* verts, uint32_t nv,
+                                    const ShapeOverlap& so, const Launch& l, cudaStream_t s) {
+    if (l.n_active == 0) return cudaSuccess;
+    PolyShape2 sh{verts, nv, so.rr, 0.f};
+    const int wave = resident_wave((const void*)k_sweep_poly2_soft);
+    uint32_t blocks = (l.n_active + 3) / 4;  // four warps (trials) per block
+    if (blocks > (uint32_t)wave) blocks = (uint32_t)wave;
+    PassLaunch pl(blocks, l.overlap_previous != 0 || l.early_wait != 0, s);
+    return cudaLaunchKernelEx(&pl.cfg, k_sweep_poly2_soft, g, a, sh, so, l);
+}
+
+cudaError_t launch_energy_poly2_soft(const Geometry& g, const Arrays& a, const double4* verts, uint32_t nv,
+                                     const ShapeOverlap& so, uint32_t n, double* out, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    PolyShape2 sh{verts, nv, so.rr, 0.f};
+    k_energy_poly2_soft<<<(n + 127) / 128, 128, 0, s>>>(g, a, sh, so, n, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_quick_insert_poly2(const Geometry& g, const Arrays& a, const double4* verts, uint32_t nv,
+                                      const ShapeOverlap& so, const Launch& l, const QuickInsertArgs& q,
+                                      const BodyTags& tags, const uint32_t* nc, const double* w, uint32_t cap,
+                                      uint32_t* size, uint32_t* items, uint32_t* cell_of, double4* site,
+                                      unsigned long long* out, cudaStream_t s) {
+    const SerialGrid G = make_grid(2, nc, w, cap, size, items, cell_of, site);
+    cudaError_t e = build_grid(2, g, a, G, q.n0, s);
+    if (e != cudaSuccess) return e;
+    PolyShape2 sh{verts, nv, so.rr, 0.f};
+    k_quick_insert_poly2<<<1, 32, 0, s>>>(g, a, G, sh, so, l, q, tags, out);
     return cudaGetLastError();
 }
 

@@ -13,66 +13,6 @@
 namespace hmc {
 namespace {
 
-// Body tags (the tagged container of hoomd-microstate/src/microstate.rs:60-123): a new body
-// takes the smallest free tag (a min-heap of freed tags), else the next unused one; removal
-// frees the tag and swap_removes. Lane 0 only.
-__device__ uint32_t tag_take(const BodyTags& T) {
-    uint32_t& size = T.meta[0];
-    if (size == 0) return T.meta[1]++;
-    const uint32_t top = T.heap[0];
-    const uint32_t last = T.heap[--size];
-    uint32_t i = 0;
-    for (;;) {
-        const uint32_t l = 2 * i + 1, r = l + 1;
-        uint32_t m = i;
-        uint32_t vm = last;
-        if (l < size && T.heap[l] < vm) {
-            m = l;
-            vm = T.heap[l];
-        }
-        if (r < size && T.heap[r] < vm) m = r;
-        if (m == i) break;
-        T.heap[i] = T.heap[m];
-        i = m;
-    }
-    if (size) T.heap[i] = last;
-    return top;
-}
-__device__ void tag_free(const BodyTags& T, uint32_t tag) {
-    uint32_t i = T.meta[0]++;
-    while (i > 0) {
-        const uint32_t parent = (i - 1) / 2;
-        if (T.heap[parent] <= tag) break;
-        T.heap[i] = T.heap[parent];
-        i = parent;
-    }
-    T.heap[i] = tag;
-}
-
-// Append body n at B = wrap(x), S = wrap(B) (Microstate::add_body) to the arrays and the grid.
-template <int DIM>
-__device__ void grid_append(const Geometry& g, const Arrays& A, const SerialGrid& G, const BodyTags& T, uint32_t n,
-                            const double* x) {
-    double b[3] = {x[0], x[1], x[2]};
-    wrap_inv<DIM>(g.L, g.invL, b);
-    double sv[3] = {b[0], b[1], b[2]};
-    wrap_inv<DIM>(g.L, g.invL, sv);
-    A.body_pos[n] = make_double4(b[0], b[1], DIM == 3 ? b[2] : 0.0, 0.0);
-    G.site[n] = make_double4(sv[0], sv[1], DIM == 3 ? sv[2] : 0.0, 0.0);
-    uint32_t ms[3] = {0, 0, 0};
-    serial_cell<DIM>(g, G, sv, ms);
-    const uint32_t c = serial_index<DIM>(G, ms);
-    const uint32_t sz = G.size[c];
-    if (sz < G.cap) {
-        G.items[(size_t)c * G.cap + sz] = n;
-        G.size[c] = sz + 1;
-    } else {
-        atomicOr(&A.stats->error_flags, kErrCellOverflow);
-    }
-    G.cell_of[n] = c;
-    if (T.tag) T.tag[n] = tag_take(T);
-}
-
 // Soft pair energy (Lennard-Jones or the overlap penalty) of site t against every site of the
 // stencil around t's cell except body `self`: per-lane sums over the lane's cell, then a
 // butterfly reduction (all lanes agree). mag += sum |e|, terms += the sites visited (for

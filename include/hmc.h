@@ -53,7 +53,8 @@ typedef enum hmc_status {
     HMC_OVERLAP_IN_INPUT = 3,     /* reserved: reported by hmc_overlap_check callers */
     HMC_CELL_OVERFLOW = 4,        /* a cell holds more bodies than a kernel supports */
     HMC_NAN_STATE = 5,            /* a non-finite coordinate was found */
-    HMC_ITERATION_CAP = 6,        /* reserved */
+    HMC_ITERATION_CAP = 6,        /* a bounded device loop reached its bound (an approximate
+                                     separation, hmc_set_shape_overlap) */
     HMC_TIMEOUT = 7,              /* reserved */
     HMC_CUDA_ERROR = 8,           /* a CUDA runtime call failed */
     HMC_OUT_OF_MEMORY = 9,
@@ -433,6 +434,32 @@ hmc_status hmc_get_box(hmc_system* sys, double* edge_lengths);
 hmc_status hmc_set_box(hmc_system* sys, const double* edge_lengths);
 /* Bodies in the system (it grows under hmc_quick_insert_apply). */
 hmc_status hmc_get_n_bodies(hmc_system* sys, uint64_t* n_bodies);
+
+/* The insertion hamiltonian of oriented convex shapes: PairwiseCutoff(Anisotropic {
+ * ApproximateShapeOverlap { Convex(shape), OverlapPenalty { k, maximum_allowed_overlap,
+ * epsilon_shoulder }, resolution }, r_cut }) (hoomd-interaction/src/pairwise/anisotropic.rs:120-135,
+ * approximate_shape_overlap.rs:122-131), which place_single_site_orientable_bodies
+ * (benchmarks/src/place.rs:120-219) prepares convex shapes with. A pair closer than r_cut costs
+ * OverlapPenalty(-d), d the distance, in steps of `resolution`, that the other shape moves along
+ * the line of centres until the two no longer intersect (IntersectsAt::
+ * approximate_separation_distance, hoomd-geometry/src/lib.rs:307-325).
+ * hmc_set_shape_overlap(sys, params) makes it the system's hamiltonian for hmc_sweep (FP64 in both
+ * precision modes; translation or rotation), hmc_quick_insert_apply (each UniformIn body also draws
+ * a uniform random orientation), hmc_quick_compress_apply and hmc_total_energy;
+ * hmc_set_shape_overlap(sys, NULL) returns to HardShape. Convex polyhedra and polygons
+ * (HMC_HARD_CONVEX_POLYHEDRON, HMC_HARD_CONVEX_POLYGON) only; r_cut (0 = 2 x the bounding radius)
+ * must not exceed 2 x the bounding radius. The serial sweep, the tuner, the autotuner and the
+ * injected-move entry points return HMC_NOT_SUPPORTED while it is set. */
+typedef struct hmc_shape_overlap_params {
+    uint32_t struct_size;           /* sizeof(hmc_shape_overlap_params) */
+    uint32_t reserved;
+    double resolution;              /* ApproximateShapeOverlap::resolution (> 0) */
+    double r_cut;                   /* Anisotropic::r_cut; 0 = 2 x the bounding radius */
+    double penalty_k;               /* OverlapPenalty::k (default 10000) */
+    double penalty_maximum_overlap; /* OverlapPenalty::maximum_allowed_overlap (default 0.2) */
+    double penalty_shoulder;        /* OverlapPenalty::epsilon_shoulder (default 100) */
+} hmc_shape_overlap_params;
+hmc_status hmc_set_shape_overlap(hmc_system* sys, const hmc_shape_overlap_params* params);
 
 /* ---- GSD files (hoomd-gsd) ----
  * The file layer replaces GsdFile (hoomd-gsd/src/file_layer.rs:559-2458): the same on-disk

@@ -22,6 +22,8 @@ HARD_CONVEX_POLYHEDRON = 2
 LENNARD_JONES = 3
 HARD_CONVEX_SURFACE_MESH_2D = 4
 OVERLAP_PENALTY = 5
+CONVEX_POLYHEDRON_PENALTY = 6  # Anisotropic { ApproximateShapeOverlap { Convex(ConvexPolyhedron), OverlapPenalty } }
+CONVEX_POLYGON_PENALTY = 7     # the same with Convex(ConvexPolygon)
 TRANSLATE = 0
 ROTATE = 1
 
@@ -92,6 +94,9 @@ def lib():
         L.oracle_set_counter.argtypes = [C.c_void_p, C.c_uint64, C.c_uint32]
         L.oracle_gsd_frame.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.oracle_set_penalty.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double]
+        L.oracle_set_shape_overlap.argtypes = [C.c_void_p, C.c_double, C.c_double]
+        L.oracle_approximate_separation.argtypes = [C.c_uint32, _dp, C.c_uint32, _dp, _dp, C.c_double]
+        L.oracle_approximate_separation.restype = C.c_double
         L.oracle_n_bodies.argtypes = [C.c_void_p]
         L.oracle_n_bodies.restype = C.c_uint64
         L.oracle_get_box.argtypes = [C.c_void_p, _dp]
@@ -273,6 +278,15 @@ def surface_mesh_intersects_at_2d(verts_a, verts_b, v_ij, theta) -> bool:
     return bool(lib().oracle_surface_mesh_intersects_at_2d(_d(a), a.shape[0], _d(b), b.shape[0], _d(v), theta))
 
 
+def approximate_separation(vertices, v_ij, o_ij, resolution) -> float:
+    """IntersectsAt::approximate_separation_distance of two equal convex polytopes; o_ij is a versor
+    (s, x, y, z) in 3-D or an angle in 2-D."""
+    verts = _f64(vertices)
+    dim = verts.shape[1]
+    return float(lib().oracle_approximate_separation(dim, _d(verts), verts.shape[0], _d(_f64(v_ij)),
+                                                     _d(_f64(np.atleast_1d(o_ij))), resolution))
+
+
 def cr_sincos(x: float):
     """Correctly rounded (sin x, cos x); raises for |x| >= 2^20."""
     s = C.c_double()
@@ -319,7 +333,8 @@ class System:
 
     def __init__(self, dim, edge_lengths, positions, orientations=None, *, step=0, substep=0, seed=0,
                  interaction=HARD_SPHERE, diameter=1.0, vertices=None, lj_epsilon=1.0, lj_sigma=1.0,
-                 lj_r_cut=2.5, lj_r_shift=2.5, boundary_range=None, penalty=(10000.0, 0.2, 100.0)):
+                 lj_r_cut=2.5, lj_r_shift=2.5, boundary_range=None, penalty=(10000.0, 0.2, 100.0),
+                 resolution=0.01, r_cut=None):
         self.dim = dim
         self.L = _f64(edge_lengths)
         self.seed = seed
@@ -341,8 +356,10 @@ class System:
                                              interaction, diameter, _d(verts), nv, lj_epsilon, lj_sigma,
                                              lj_r_cut, lj_r_shift, boundary_range)
         self.ori_len = 0 if interaction in (HARD_SPHERE, LENNARD_JONES, OVERLAP_PENALTY) else (4 if dim == 3 else 1)
-        if interaction == OVERLAP_PENALTY:
+        if interaction in (OVERLAP_PENALTY, CONVEX_POLYHEDRON_PENALTY, CONVEX_POLYGON_PENALTY):
             lib().oracle_set_penalty(self._h, *penalty)
+        if interaction in (CONVEX_POLYHEDRON_PENALTY, CONVEX_POLYGON_PENALTY):
+            lib().oracle_set_shape_overlap(self._h, resolution, boundary_range if r_cut is None else r_cut)
 
     def __del__(self):
         h = getattr(self, "_h", None)

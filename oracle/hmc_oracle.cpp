@@ -697,6 +697,69 @@ bool convex_global_2d(const Polytope& p, const double* ri, double ti, const doub
     return collide2d(p, p, vij, m);
 }
 
+// IntersectsAt::approximate_separation_distance (hoomd-geometry/src/lib.rs:307-325) for two equal
+// Convex polytopes in the local frame of the first: direction = v.to_unit() (lib.rs:632-639,
+// norm = sqrt(fma dot)), else the default unit (last axis, cartesian.rs:313-318); d grows by
+// `resolution` while Convex::intersects_at (convex.rs:87-99, :130-143) holds at v + direction * d:
+// the bounding spheres |w|^2 <= (R + R)^2 (sphere.rs:262-264), then XenoCollide.
+template <int N, class Q>
+double approximate_separation(const Polytope& p, const double* v, const Q& q, double resolution) {
+    double dir[N];
+    const double norm = std::sqrt(dot(v, v, N));
+    if (norm == 0.0) {
+        for (int a = 0; a < N; ++a) dir[a] = a == N - 1 ? 1.0 : 0.0;
+    } else {
+        for (int a = 0; a < N; ++a) dir[a] = v[a] / norm;
+    }
+    const double rr = (p.bounding_radius + p.bounding_radius) * (p.bounding_radius + p.bounding_radius);
+    double d = 0.0;
+    for (;;) {
+        double w[N];
+        for (int a = 0; a < N; ++a) w[a] = v[a] + dir[a] * d;
+        if (!(dot(w, w, N) <= rr)) break;
+        bool hit;
+        if constexpr (N == 3)
+            hit = collide3d(p, p, w, q);
+        else
+            hit = collide2d(p, p, w, q);
+        if (!hit) break;
+        d = d + resolution;
+    }
+    return d;
+}
+// OverlapPenalty::energy (overlap_penalty.rs:109-115): inf below -d_max, (0.5 k) r^2 + eps below 0.
+double overlap_penalty(double k, double dmax, double shoulder, double r) {
+    if (r < -dmax) return INFINITY;
+    if (r < 0.0) return 0.5 * k * (r * r) + shoulder;
+    return 0.0;
+}
+// Anisotropic::site_pair_energy (anisotropic.rs:120-135) of ApproximateShapeOverlap<OverlapPenalty,
+// Convex<ConvexPolyhedron>> (approximate_shape_overlap.rs:122-131): |r_j - r_i| >= r_cut -> 0, else
+// pair_system_to_local (hoomd-vector/src/lib.rs:878-888) and OverlapPenalty(-separation).
+double shape_penalty_3d(const Polytope& p, double rcut, double res, double k, double dmax, double shoulder,
+                        const double* ri, const Quat& qi, const double* rj, const Quat& qj) {
+    if (std::sqrt(distance_squared(ri, rj, 3)) >= rcut) return 0.0;
+    double rab[3] = {rj[0] - ri[0], rj[1] - ri[1], rj[2] - ri[2]};
+    const Quat qa_inv = qconj(qi);
+    const V3 vij = versor_rotate(qa_inv, rab);
+    const Quat oij = qmul(qa_inv, qj);
+    const Mat3 m = mat_from_versor(oij);
+    return overlap_penalty(k, dmax, shoulder, -approximate_separation<3>(p, vij.v, m, res));
+}
+// The same for Convex<ConvexPolygon> with Angle orientations (angle.rs:175-181, :212, :229).
+double shape_penalty_2d(const Polytope& p, double rcut, double res, double k, double dmax, double shoulder,
+                        const double* ri, double ti, const double* rj, double tj) {
+    if (std::sqrt(distance_squared(ri, rj, 2)) >= rcut) return 0.0;
+    double rab[2] = {rj[0] - ri[0], rj[1] - ri[1]};
+    const double inv = -ti;
+    double s, c;
+    cr_sincos(inv, &s, &c);
+    double vij[2] = {rab[0] * c - rab[1] * s, rab[0] * s + rab[1] * c};
+    double m[2][2];
+    mat2_from_angle(inv + tj, m);
+    return overlap_penalty(k, dmax, shoulder, -approximate_separation<2>(p, vij, m, res));
+}
+
 // ConvexSurfaceMesh2d separating-axis test (convex_surface_mesh_2d.rs:578-640): a and b
 // hold counter-clockwise hull vertices; o_b rotates b into a's frame.
 static void mat2_rotate(const double (&m)[2][2], const double* v, double* out) {  // rows dot v
@@ -1011,6 +1074,12 @@ struct oracle_system {
         free_tags.pop();
         return t;
     }
+    // Microstate::add_body: body = wrap(x), site = wrap(body), appended with orientation o
+    // (oriented bodies; the site's orientation is the body's).
+    void append_body(const double* x, const double* o) {
+        for (int k = 0; k < ori_len(); ++k) orient.push_back(o[k]);
+        append_body(x);
+    }
     // Microstate::add_body for a point body: body = wrap(x), site = wrap(body), appended.
     void append_body(const double* x) {
         double b[3] = {x[0], x[1], x[2]};
@@ -1057,11 +1126,17 @@ struct oracle_system {
         n = last;
     }
 
-    bool hard() const { return interaction != ORACLE_LENNARD_JONES && interaction != ORACLE_OVERLAP_PENALTY; }
+    bool shape_penalty() const {
+        return interaction == ORACLE_CONVEX_POLYHEDRON_PENALTY || interaction == ORACLE_CONVEX_POLYGON_PENALTY;
+    }
+    bool hard() const {
+        return interaction != ORACLE_LENNARD_JONES && interaction != ORACLE_OVERLAP_PENALTY && !shape_penalty();
+    }
     double pk = 10000.0, pdmax = 0.2, pshoulder = 100.0;  // OverlapPenalty
+    double presolution = 0.01, prcut = 1.0;              // ApproximateShapeOverlap, Anisotropic r_cut
     bool oriented() const {
         return interaction == ORACLE_HARD_CONVEX_POLYGON || interaction == ORACLE_HARD_CONVEX_POLYHEDRON ||
-               interaction == ORACLE_HARD_CONVEX_SURFACE_MESH_2D;
+               interaction == ORACLE_HARD_CONVEX_SURFACE_MESH_2D || shape_penalty();
     }
 
     void build_grid() {
@@ -1143,6 +1218,13 @@ struct oracle_system {
                 return convex_global_2d(poly, x, o[0], y, orient[j]) ? INFINITY : 0.0;
             case ORACLE_HARD_CONVEX_SURFACE_MESH_2D:
                 return sat_global_2d(poly, x, o[0], y, orient[j]) ? INFINITY : 0.0;
+            case ORACLE_CONVEX_POLYHEDRON_PENALTY: {
+                const double* oj = &orient[4 * j];
+                return shape_penalty_3d(poly, prcut, presolution, pk, pdmax, pshoulder, x, Quat{o[0], o[1], o[2], o[3]},
+                                        y, Quat{oj[0], oj[1], oj[2], oj[3]});
+            }
+            case ORACLE_CONVEX_POLYGON_PENALTY:
+                return shape_penalty_2d(poly, prcut, presolution, pk, pdmax, pshoulder, x, o[0], y, orient[j]);
             case ORACLE_OVERLAP_PENALTY: {
                 // Isotropic::site_pair_energy (isotropic.rs:147-156) of Expanded { delta: diameter,
                 // OverlapPenalty } (expanded.rs:64-66, overlap_penalty.rs:109-115), r_cut = diameter
@@ -1287,6 +1369,22 @@ void oracle_set_penalty(oracle_system* s, double k, double maximum_allowed_overl
     s->pdmax = maximum_allowed_overlap;
     s->pshoulder = epsilon_shoulder;
 }
+static Polytope make_poly(const double* verts, uint32_t nv, int dim);
+void oracle_set_shape_overlap(oracle_system* s, double resolution, double r_cut) {
+    s->presolution = resolution;
+    s->prcut = r_cut;
+    s->search_range = r_cut;
+    s->build_grid();
+}
+double oracle_approximate_separation(uint32_t dim, const double* vertices, uint32_t n_vertices, const double* v_ij,
+                                     const double* o_ij, double resolution) {
+    const Polytope p = make_poly(vertices, n_vertices, (int)dim);
+    if (dim == 3) return approximate_separation<3>(p, v_ij, mat_from_versor(Quat{o_ij[0], o_ij[1], o_ij[2], o_ij[3]}),
+                                                   resolution);
+    double m[2][2];
+    mat2_from_angle(o_ij[0], m);
+    return approximate_separation<2>(p, v_ij, m, resolution);
+}
 uint64_t oracle_n_bodies(const oracle_system* s) { return s->n; }
 void oracle_get_box(const oracle_system* s, double* edge_lengths) {
     for (int a = 0; a < s->dim; ++a) edge_lengths[a] = s->L[a];
@@ -1322,6 +1420,24 @@ int oracle_set_box(oracle_system* s, const double* edge_lengths) {
     return 0;
 }
 
+// StandardUniform orientations: Versor from four standard normals, scalar first, divided by
+// sqrt(|v|^2 + s^2) (quaternion.rs:863-885); Angle from Uniform::new(0, 2 pi) (angle.rs:268-285).
+static void uniform_orientation(Sfc64& rng, int dim, double* o) {
+    if (dim == 3) {
+        const double sc = standard_normal(rng);
+        double v[3];
+        for (int a = 0; a < 3; ++a) v[a] = standard_normal(rng);
+        const double norm = std::sqrt(dot(v, v, 3) + sc * sc);
+        o[0] = sc / norm;
+        for (int a = 0; a < 3; ++a) o[1 + a] = v[a] / norm;
+    } else {
+        const double two_pi = 2.0 * 3.141592653589793;
+        const uint64_t bits = rng.next_u64() >> 12;
+        const double u = bits_to_double(0x3FF0000000000000ULL | bits) - 1.0;
+        o[0] = u * (two_pi - 0.0) + 0.0;
+    }
+}
+
 void oracle_quick_insert(oracle_system* s, uint64_t target, uint64_t allowed_overlaps, uint64_t* inserted,
                          uint32_t* complete, uint64_t* accepted, uint64_t* rejected) {
     *accepted = 0;
@@ -1345,12 +1461,18 @@ void oracle_quick_insert(oracle_system* s, uint64_t target, uint64_t allowed_ove
                 const double u = bits_to_double(0x3FF0000000000000ULL | bits) - 1.0;
                 x[a] = u * (high - low) + low;
             }
+            // oriented bodies: then a uniform random orientation (uniform_in.rs:158-176)
+            double o[4] = {1.0, 0.0, 0.0, 0.0};
+            if (s->oriented()) uniform_orientation(rng, s->dim, o);
             // delta_energy_insert: the site is wrap(transform(body, site)) (pairwise_cutoff.rs:420-450)
             double t[3] = {x[0], x[1], x[2]};
             wrap(s->dim, s->L, t);
-            const double de = s->site_energy(t, nullptr, UINT64_MAX, cand);
+            const double de = s->site_energy(t, s->oriented() ? o : nullptr, UINT64_MAX, cand);
             if (std::isfinite(de)) {
-                s->append_body(x);
+                if (s->oriented())
+                    s->append_body(x, o);
+                else
+                    s->append_body(x);
                 *accepted += 1;
                 *inserted += 1;
                 if (de > 0.0) overlapping += 1;
@@ -1639,9 +1761,7 @@ oracle_system* oracle_system_create(uint32_t dim, const double* L, uint64_t n, c
     s->rcut = rcut;
     s->rshift = rshift;
     s->boundary_range = boundary_range;
-    if (interaction == ORACLE_HARD_CONVEX_POLYGON || interaction == ORACLE_HARD_CONVEX_POLYHEDRON ||
-        interaction == ORACLE_HARD_CONVEX_SURFACE_MESH_2D)
-        s->poly = make_poly(vertices, n_vertices, (int)dim);
+    if (s->oriented()) s->poly = make_poly(vertices, n_vertices, (int)dim);
     switch (interaction) {
         case ORACLE_HARD_SPHERE:
             s->search_range = diameter;
@@ -1654,6 +1774,7 @@ oracle_system* oracle_system_create(uint32_t dim, const double* L, uint64_t n, c
             break;
         default:
             s->search_range = s->poly.bounding_radius * 2.0;
+            s->prcut = s->search_range;
     }
     s->body.assign(3 * n, 0.0);
     s->site.assign(3 * n, 0.0);
