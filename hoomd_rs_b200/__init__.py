@@ -35,7 +35,10 @@ OK, INVALID_ARGUMENT, RANGE_TOO_LARGE, OVERLAP_IN_INPUT, CELL_OVERFLOW, NAN_STAT
     CUDA_ERROR, OUT_OF_MEMORY, NOT_SUPPORTED, OUTSIDE_CHECKERBOARD, IO_ERROR = range(13)
 # hmc_interaction / hmc_move / hmc_precision
 HARD_SPHERE, HARD_CONVEX_POLYGON, HARD_CONVEX_POLYHEDRON, LENNARD_JONES, HARD_CONVEX_SURFACE_MESH_2D, \
-    OVERLAP_PENALTY = range(6)
+    OVERLAP_PENALTY, ISOTROPIC = range(7)
+# hmc_univariate / hmc_univariate_wrap
+UV_LENNARD_JONES, UV_WEEKS_CHANDLER_ANDERSON, UV_HARMONIC, UV_HARMONIC_REPULSION, UV_BOXCAR, UV_OVERLAP_PENALTY = range(6)
+UVW_NONE, UVW_SHIFTED, UVW_EXPANDED, UVW_XPLOR = range(4)
 TRANSLATE, ROTATE = range(2)
 FP64, FP32_RECHECK = range(2)
 # hmc_sweep_params.flags of the tuners
@@ -60,7 +63,9 @@ class hmc_system_desc(C.Structure):
                 ("lj_r_cut", C.c_double), ("lj_r_shift", C.c_double), ("boundary_range", C.c_double),
                 ("body_interaction_range", C.c_double), ("penalty_k", C.c_double),
                 ("penalty_maximum_overlap", C.c_double), ("penalty_shoulder", C.c_double),
-                ("capacity", C.c_uint64)]
+                ("capacity", C.c_uint64), ("univariate", C.c_uint32), ("univariate_wrap", C.c_uint32),
+                ("univariate_params", C.c_double * 4), ("wrap_params", C.c_double * 2),
+                ("isotropic_r_cut", C.c_double)]
 
 
 class hmc_shape_overlap_params(C.Structure):
@@ -304,6 +309,46 @@ class OverlapPenalty:
 
 
 @dataclass
+class WeeksChandlerAnderson:
+    """hoomd_interaction::univariate::WeeksChandlerAnderson (weeks_chandler_anderson.rs): the
+    Lennard-Jones energy plus epsilon below 2^(1/6) sigma, else 0."""
+    epsilon: float = 1.0
+    sigma: float = 1.0
+
+
+@dataclass
+class Harmonic:
+    """hoomd_interaction::univariate::Harmonic (harmonic.rs): 0.5 k (r - r_0)^2."""
+    k: float
+    r_0: float
+
+
+@dataclass
+class HarmonicRepulsion:
+    """hoomd_interaction::univariate::HarmonicRepulsion (harmonic_repulsion.rs): 0.5 a / r_cut
+    (r - r_cut)^2 below r_cut, else 0."""
+    a: float
+    r_cut: float
+
+
+@dataclass
+class Boxcar:
+    """hoomd_interaction::univariate::Boxcar (boxcar.rs): epsilon on [left, right), else 0."""
+    epsilon: float
+    left: float
+    right: float
+
+
+@dataclass
+class Xplor:
+    """hoomd_interaction::univariate::Xplor (xplor.rs): f(r) smoothed to 0 between r_smooth and
+    r_cut."""
+    f: object
+    r_cut: float
+    r_smooth: float
+
+
+@dataclass
 class Expanded:
     """hoomd_interaction::univariate::Expanded (expanded.rs:62-67): f(r - delta)."""
     delta: float
@@ -526,6 +571,31 @@ def gr_normalise(counts, n: int, volume: float, dim: int, r_max: float) -> "tupl
     return 0.5 * (edges[1:] + edges[:-1]), counts / ideal
 
 
+def _univariate(e):
+    """(hmc_univariate, its parameters, hmc_univariate_wrap, its parameters) of a univariate energy,
+    plain or in one Shifted, Expanded or Xplor."""
+    wrap, wparams = UVW_NONE, ()
+    if isinstance(e, Shifted):
+        wrap, wparams, e = UVW_SHIFTED, (e.r_shift,), e.f
+    elif isinstance(e, Expanded):
+        wrap, wparams, e = UVW_EXPANDED, (e.delta,), e.f
+    elif isinstance(e, Xplor):
+        wrap, wparams, e = UVW_XPLOR, (e.r_cut, e.r_smooth), e.f
+    if isinstance(e, LennardJones):
+        return UV_LENNARD_JONES, (e.epsilon, e.sigma), wrap, wparams
+    if isinstance(e, WeeksChandlerAnderson):
+        return UV_WEEKS_CHANDLER_ANDERSON, (e.epsilon, e.sigma), wrap, wparams
+    if isinstance(e, Harmonic):
+        return UV_HARMONIC, (e.k, e.r_0), wrap, wparams
+    if isinstance(e, HarmonicRepulsion):
+        return UV_HARMONIC_REPULSION, (e.a, e.r_cut), wrap, wparams
+    if isinstance(e, Boxcar):
+        return UV_BOXCAR, (e.epsilon, e.left, e.right), wrap, wparams
+    if isinstance(e, OverlapPenalty):
+        return UV_OVERLAP_PENALTY, (e.k, e.maximum_allowed_overlap, e.epsilon_shoulder), wrap, wparams
+    raise HmcError(NOT_SUPPORTED, f"univariate {type(e).__name__}")
+
+
 class Microstate:
     """Bodies in a periodic box, resident on the GPU (one hmc_system)."""
 
@@ -555,21 +625,30 @@ class Microstate:
             self._verts = verts  # keep alive during the call
             d.n_vertices = verts.shape[0]
             d.vertices = verts.ctypes.data_as(_dp)
-        elif isinstance(pair, Isotropic) and isinstance(pair.interaction, Expanded):
+        elif (isinstance(pair, Isotropic) and isinstance(pair.interaction, Expanded)
+              and isinstance(pair.interaction.f, OverlapPenalty) and pair.interaction.delta == pair.r_cut):
             # the overlap-penalty sphere: Isotropic { Expanded { delta: d, OverlapPenalty }, r_cut: d }
-            if pair.interaction.delta != pair.r_cut:
-                raise HmcError(NOT_SUPPORTED, "Expanded(OverlapPenalty) needs delta == r_cut")
             d.interaction = OVERLAP_PENALTY
             d.diameter = pair.r_cut
             d.penalty_k = pair.interaction.f.k
             d.penalty_maximum_overlap = pair.interaction.f.maximum_allowed_overlap
             d.penalty_shoulder = pair.interaction.f.epsilon_shoulder
-        elif isinstance(pair, Isotropic) and isinstance(pair.interaction, Shifted):
+        elif (isinstance(pair, Isotropic) and isinstance(pair.interaction, Shifted)
+              and isinstance(pair.interaction.f, LennardJones)):
             d.interaction = LENNARD_JONES
             d.lj_epsilon = pair.interaction.f.epsilon
             d.lj_sigma = pair.interaction.f.sigma
             d.lj_r_cut = pair.r_cut
             d.lj_r_shift = pair.interaction.r_shift
+        elif isinstance(pair, Isotropic):
+            d.interaction = ISOTROPIC
+            kind, params, wrap, wparams = _univariate(pair.interaction)
+            d.univariate, d.univariate_wrap = kind, wrap
+            for k, x in enumerate(params):
+                d.univariate_params[k] = x
+            for k, x in enumerate(wparams):
+                d.wrap_params[k] = x
+            d.isotropic_r_cut = pair.r_cut
         else:
             raise HmcError(NOT_SUPPORTED, f"{type(pair).__name__}")
         d.boundary_range = boundary.maximum_interaction_range
@@ -1173,6 +1252,7 @@ __all__ = ["Batch", "Context", "sdf_pressure", "gr_normalise", "ConvexPolygon", 
            "LennardJones", "Microstate", "PairwiseCutoff", "Rotate", "Shifted", "TuneOptions",
            "ParallelSweep", "Periodic", "Translate", "load_library", "SIGNATURES", "FP64", "FP32_RECHECK",
            "QuickInsert", "QuickCompress", "OverlapPenalty", "ApproximateShapeOverlap", "Anisotropic",
+           "WeeksChandlerAnderson", "Harmonic", "HarmonicRepulsion", "Boxcar", "Xplor",
            "place_single_site_orientable_bodies", "Expanded", "GrandCanonical", "IsothermalIsofugacity",
            "InsertRemoveCount",
            "TRANSLATE", "ROTATE", "HARD_SPHERE", "HARD_CONVEX_POLYGON", "HARD_CONVEX_POLYHEDRON", "LENNARD_JONES",

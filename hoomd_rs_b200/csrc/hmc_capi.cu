@@ -127,7 +127,9 @@ struct hmc_system {
     uint32_t* tag_meta = nullptr;
     bool tags_permuted = false;  // some body was removed: index order is not tag order
     bool penalty() const { return interaction == HMC_OVERLAP_PENALTY; }
-    bool soft() const { return interaction == HMC_LENNARD_JONES || penalty(); }
+    bool soft() const { return interaction == HMC_LENNARD_JONES || penalty() || interaction == HMC_ISOTROPIC; }
+    // the soft interactions with an FP32 pass (the others run FP64 in both precision modes)
+    bool soft_fp32() const { return interaction == HMC_LENNARD_JONES; }
     // the approximate shape overlap in place of HardShape (hmc_set_shape_overlap)
     bool shape_soft = false;
     ShapeOverlap so{};
@@ -238,6 +240,31 @@ void lj_setup_for(int dim, const Geometry& geom, Pair& P, double eps, double sig
 
 void lj_setup(hmc_system* s, double eps, double sigma, double rcut, double rshift) {
     lj_setup_for(s->dim, s->geom, s->pair, eps, sigma, rcut, rshift);
+}
+
+// The univariate energy F(r) of HMC_ISOTROPIC on the host (the Shifted constant F(r_shift)), in
+// the same operations as univariate64 on the device (this file is compiled without contraction).
+double univariate_host(uint32_t kind, const double* p, double r) {
+    switch (kind) {
+        case HMC_UV_LENNARD_JONES:
+        case HMC_UV_WEEKS_CHANDLER_ANDERSON: {
+            if (kind == HMC_UV_WEEKS_CHANDLER_ANDERSON && !(r < p[2] * p[1])) return 0.0;
+            const double sr = p[1] / r;
+            const double s2 = sr * sr, s4 = s2 * s2, s8 = s4 * s4;
+            const double e = 4.0 * p[0] * (s4 * s8 - s2 * s4);
+            return kind == HMC_UV_WEEKS_CHANDLER_ANDERSON ? e + p[0] : e;
+        }
+        case HMC_UV_HARMONIC:
+            return 0.5 * p[0] * (r - p[1]) * (r - p[1]);
+        case HMC_UV_HARMONIC_REPULSION:
+            return r < p[1] ? 0.5 * p[0] / p[1] * ((r - p[1]) * (r - p[1])) : 0.0;
+        case HMC_UV_BOXCAR:
+            return r < p[1] ? 0.0 : (r < p[2] ? p[0] : 0.0);
+        default:
+            if (r < -p[1]) return INFINITY;
+            if (r < 0.0) return 0.5 * p[0] * (r * r) + p[2];
+            return 0.0;
+    }
 }
 
 // Pair thresholds that depend on the box (FP32 bounds use the space widths and box lengths).
@@ -558,8 +585,25 @@ hmc_status hmc_system_create(hmc_context* ctx, const hmc_system_desc* d, const d
     if (d->capacity >= (1ull << 31)) return fail(HMC_INVALID_ARGUMENT, "capacity too large");
     if (d->interaction != HMC_HARD_SPHERE && d->interaction != HMC_LENNARD_JONES &&
         d->interaction != HMC_HARD_CONVEX_POLYHEDRON && d->interaction != HMC_HARD_CONVEX_POLYGON &&
-        d->interaction != HMC_HARD_CONVEX_SURFACE_MESH_2D && d->interaction != HMC_OVERLAP_PENALTY)
+        d->interaction != HMC_HARD_CONVEX_SURFACE_MESH_2D && d->interaction != HMC_OVERLAP_PENALTY &&
+        d->interaction != HMC_ISOTROPIC)
         return fail(HMC_NOT_SUPPORTED, "interaction %u is not available in this build", d->interaction);
+    if (d->interaction == HMC_ISOTROPIC) {
+        if (d->univariate > HMC_UV_OVERLAP_PENALTY || d->univariate_wrap > HMC_UVW_XPLOR)
+            return fail(HMC_INVALID_ARGUMENT, "univariate %u / wrap %u", d->univariate, d->univariate_wrap);
+        for (int k = 0; k < 4; ++k)
+            if (!std::isfinite(d->univariate_params[k]))
+                return fail(HMC_INVALID_ARGUMENT, "univariate parameters must be finite");
+        for (int k = 0; k < 2; ++k)
+            if (!std::isfinite(d->wrap_params[k])) return fail(HMC_INVALID_ARGUMENT, "wrap parameters must be finite");
+        if (!(d->isotropic_r_cut > 0.0) || !std::isfinite(d->isotropic_r_cut))
+            return fail(HMC_INVALID_ARGUMENT, "Isotropic r_cut must be positive");
+        if ((d->univariate == HMC_UV_LENNARD_JONES || d->univariate == HMC_UV_WEEKS_CHANDLER_ANDERSON) &&
+            !(d->univariate_params[1] > 0.0))
+            return fail(HMC_INVALID_ARGUMENT, "sigma must be positive");
+        if (d->univariate == HMC_UV_HARMONIC_REPULSION && !(d->univariate_params[1] > 0.0))
+            return fail(HMC_INVALID_ARGUMENT, "HarmonicRepulsion r_cut must be positive");
+    }
     const bool polygon = d->interaction == HMC_HARD_CONVEX_POLYGON || d->interaction == HMC_HARD_CONVEX_SURFACE_MESH_2D;
     if (polygon) {
         if (d->dim != 2) return fail(HMC_INVALID_ARGUMENT, "convex polygons are 2-D");
@@ -633,7 +677,8 @@ hmc_status hmc_system_create(hmc_context* ctx, const hmc_system_desc* d, const d
     s->substep = d->substep;
     s->seed = d->seed;
     s->interaction = d->interaction;
-    s->pair_range = d->interaction == HMC_LENNARD_JONES ? d->lj_r_cut
+    s->pair_range = d->interaction == HMC_ISOTROPIC       ? d->isotropic_r_cut
+                    : d->interaction == HMC_LENNARD_JONES ? d->lj_r_cut
                     : (d->interaction == HMC_HARD_CONVEX_POLYHEDRON || polygon) ? bounding_radius * 2.0
                                                                   : d->diameter;
     s->boundary_range = d->boundary_range > 0.0 ? d->boundary_range : s->pair_range;
@@ -655,6 +700,17 @@ hmc_status hmc_system_create(hmc_context* ctx, const hmc_system_desc* d, const d
         const double rc = bounding_radius + bounding_radius;
         s->poly_rcut2 = rc * rc;
         s->n_vertices = d->n_vertices;
+    } else if (d->interaction == HMC_ISOTROPIC) {
+        Pair& P = s->pair;
+        P.isotropic = 1;
+        P.uv_kind = d->univariate;
+        P.uv_wrap = d->univariate_wrap;
+        for (int k = 0; k < 4; ++k) P.uv_p[k] = d->univariate_params[k];
+        for (int k = 0; k < 2; ++k) P.uv_w[k] = d->wrap_params[k];
+        // WeeksChandlerAnderson's 2.0_f64.powf(1.0 / 6.0), from the platform's pow as in the reference
+        if (P.uv_kind == HMC_UV_WEEKS_CHANDLER_ANDERSON) P.uv_p[2] = std::pow(2.0, 1.0 / 6.0);
+        P.uv_shift = P.uv_wrap == HMC_UVW_SHIFTED ? univariate_host(P.uv_kind, P.uv_p, P.uv_w[0]) : 0.0;
+        P.uv_rcut2 = d->isotropic_r_cut * d->isotropic_r_cut;
     } else if (d->interaction == HMC_OVERLAP_PENALTY) {
         Pair& P = s->pair;
         P.penalty = 1;
@@ -870,7 +926,7 @@ hmc_status hmc_sweep(hmc_system* s, const hmc_sweep_params* p, hmc_count* out) {
     for (uint32_t sweep = 0; sweep < p->n_sweeps; ++sweep) {
         if (s->profiling) HMC_CUDA(cudaEventRecord(s->ev[0], s->stream));
         // shapes read S in both modes; the colour passes do not read slot_of_body
-        hmc_status st = rebuild(s, !fp32 || s->oriented() || s->penalty(), false);
+        hmc_status st = rebuild(s, !fp32 || s->oriented() || (s->soft() && !s->soft_fp32()), false);
         if (st) return st;
         if (s->profiling) HMC_CUDA(cudaEventRecord(s->ev[1], s->stream));
         Launch L{};
@@ -892,7 +948,7 @@ hmc_status hmc_sweep(hmc_system* s, const hmc_sweep_params* p, hmc_count* out) {
                 // the round's trial moves, one thread each, before the passes that give a trial
                 // several lanes
                 if (s->soft()) {
-                    HMC_CUDA(launch_propose_lj(s->dim, fp32 && !s->penalty(), s->geom, s->arr, L, s->stream));
+                    HMC_CUDA(launch_propose_lj(s->dim, fp32 && s->soft_fp32(), s->geom, s->arr, L, s->stream));
                     s->prof.kernel_launches += 1;
                 } else if (s->interaction == HMC_HARD_CONVEX_POLYHEDRON) {
                     HMC_CUDA(launch_propose_poly(fp32 && !s->shape_soft, s->geom, s->arr, L, p->move == HMC_ROTATE,
@@ -910,7 +966,7 @@ hmc_status hmc_sweep(hmc_system* s, const hmc_sweep_params* p, hmc_count* out) {
                     // wait for it before reading anything
                     L.early_wait = (r == 0 || s->soft() || s->oriented()) && c == 0 && s->pdl ? 1u : 0u;
                     if (s->soft())  // the overlap penalty has no FP32 path: FP64 in both modes
-                        HMC_CUDA(launch_sweep_lj(s->dim, fp32 && !s->penalty(), s->geom, s->arr, s->pair, L,
+                        HMC_CUDA(launch_sweep_lj(s->dim, fp32 && s->soft_fp32(), s->geom, s->arr, s->pair, L,
                                                  s->stream, variant));
                     else if (s->shape_soft && s->dim == 3)  // FP64 in both modes
                         HMC_CUDA(launch_sweep_poly3_soft(s->geom, s->arr, s->verts, s->n_vertices, s->so, L,
@@ -1343,7 +1399,7 @@ hmc_status hmc_tune(hmc_system* s, hmc_sweep_params* p, double target, uint32_t 
         e = launch_tune_moves(s->dim, s->geom, s->arr, L, step, samples, p->move == HMC_ROTATE, db, dt, dq, du, s->stream);
         if (e != cudaSuccess) break;
         if (s->soft())
-            e = launch_eval_lj(s->dim, fp32 && !s->penalty(), s->geom, s->arr, s->pair, db, dt, du, p->temperature,
+            e = launch_eval_lj(s->dim, fp32 && s->soft_fp32(), s->geom, s->arr, s->pair, db, dt, du, p->temperature,
                                samples, dd, dd + samples, dh, s->stream);
         else if (s->polygon())
             e = launch_eval_poly2(fp32, s->sat(), s->geom, s->arr, s->verts, s->n_vertices, s->poly_rcut2,
@@ -1377,7 +1433,8 @@ hmc_status hmc_tune(hmc_system* s, hmc_sweep_params* p, double target, uint32_t 
 
 hmc_status hmc_overlap_check(hmc_system* s, uint64_t* n_overlaps) {
     if (!s || !n_overlaps) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
-    if (s->interaction == HMC_LENNARD_JONES) return fail(HMC_NOT_SUPPORTED, "overlap check of a soft potential");
+    if (s->interaction == HMC_LENNARD_JONES || s->interaction == HMC_ISOTROPIC)
+        return fail(HMC_NOT_SUPPORTED, "overlap check of a soft potential");
     // overlap penalty: pairs closer than delta (those with a positive pair energy)
     HMC_CUDA(cudaSetDevice(s->ctx->device));
     hmc_status st = rebuild(s, true);
@@ -1853,7 +1910,7 @@ hmc_status hmc_eval_moves(hmc_system* s, const hmc_injected_move* moves, uint64_
     if (e == cudaSuccess) e = cudaMemsetAsync(dh, 0, sizeof(double) * n, s->stream);
     if (e == cudaSuccess) {
         if (lj)
-            e = launch_eval_lj(s->dim, precision == HMC_FP32_RECHECK && !s->penalty(), s->geom, s->arr, s->pair, db, dt, du, temperature,
+            e = launch_eval_lj(s->dim, precision == HMC_FP32_RECHECK && s->soft_fp32(), s->geom, s->arr, s->pair, db, dt, du, temperature,
                                (uint32_t)n, dd, dd + n, dh, s->stream);
         else if (s->polygon())
             e = launch_eval_poly2(precision == HMC_FP32_RECHECK, s->sat(), s->geom, s->arr, s->verts, s->n_vertices,
@@ -1945,7 +2002,7 @@ hmc_status hmc_eval_trials(hmc_system* s, const hmc_injected_move* moves, uint64
         j.flags = dd + n;
         j.n = (uint32_t)n;
         if (s->soft())
-            e = launch_trials_lj(s->dim, fp32 && !s->penalty(), s->geom, s->arr, s->pair, temperature, j, s->stream);
+            e = launch_trials_lj(s->dim, fp32 && s->soft_fp32(), s->geom, s->arr, s->pair, temperature, j, s->stream);
         else if (s->oriented())
             e = launch_trials_poly(fp32, s->geom, s->arr, s->verts, s->n_vertices, s->poly_rcut2, s->poly_rcut2_hi32, j,
                                    s->stream);

@@ -108,7 +108,78 @@ struct Pair {
     double op_dmax;       // maximum_allowed_overlap
     double op_half_k;     // 0.5 * k
     double op_shoulder;   // epsilon_shoulder
+    // Isotropic { W(F), r_cut } for the univariates of hmc_univariate (hmc.h): isotropic = 1
+    uint32_t isotropic;
+    uint32_t uv_kind, uv_wrap;  // hmc_univariate, hmc_univariate_wrap
+    double uv_p[4];             // F's parameters (WeeksChandlerAnderson: p[2] = 2^(1/6), the host's pow)
+    double uv_w[2];             // W's parameters: Shifted {r_shift}, Expanded {delta}, Xplor {r_cut, r_smooth}
+    double uv_shift;            // Shifted: F(r_shift), evaluated once on the host with the same arithmetic
+    double uv_rcut2;            // Isotropic::r_cut.powi(2)
 };
+
+// The univariate energies of hoomd-interaction/src/univariate/*.rs in FP64 with the reference's
+// order of operations: LennardJones<12, 6> (lennard_jones.rs:107-111, powi by repeated squaring),
+// WeeksChandlerAnderson (LJ + epsilon below 2^(1/6) sigma), Harmonic (0.5 k (r - r_0) (r - r_0)),
+// HarmonicRepulsion (0.5 a / r_cut (r - r_cut)^2 below r_cut), Boxcar (epsilon on [left, right)),
+// OverlapPenalty (overlap_penalty.rs:109-115).
+enum : uint32_t { kUvLennardJones = 0, kUvWca = 1, kUvHarmonic = 2, kUvHarmonicRepulsion = 3, kUvBoxcar = 4,
+                  kUvOverlapPenalty = 5 };
+enum : uint32_t { kUvwNone = 0, kUvwShifted = 1, kUvwExpanded = 2, kUvwXplor = 3 };
+__device__ __forceinline__ double univariate64(uint32_t kind, const double* p, double r) {
+    switch (kind) {
+        case kUvLennardJones:
+        case kUvWca: {
+            if (kind == kUvWca && !(r < dmul(p[2], p[1]))) return 0.0;
+            const double sr = ddiv(p[1], r);
+            const double s2 = dmul(sr, sr), s4 = dmul(s2, s2), s8 = dmul(s4, s4);
+            const double e = dmul(dmul(4.0, p[0]), dsub(dmul(s4, s8), dmul(s2, s4)));
+            return kind == kUvWca ? dadd(e, p[0]) : e;
+        }
+        case kUvHarmonic: {
+            const double d = dsub(r, p[1]);
+            return dmul(dmul(dmul(0.5, p[0]), d), d);
+        }
+        case kUvHarmonicRepulsion: {
+            if (!(r < p[1])) return 0.0;
+            const double d = dsub(r, p[1]);
+            return dmul(ddiv(dmul(0.5, p[0]), p[1]), dmul(d, d));
+        }
+        case kUvBoxcar:
+            return r < p[1] ? 0.0 : (r < p[2] ? p[0] : 0.0);
+        default:
+            if (r < -p[1]) return __longlong_as_double(0x7ff0000000000000ll);
+            if (r < 0.0) return dadd(dmul(dmul(0.5, p[0]), dmul(r, r)), p[2]);
+            return 0.0;
+    }
+}
+// Isotropic::site_pair_energy (isotropic.rs:147-156) of W(F): Shifted (shifted.rs:92-94),
+// Expanded (expanded.rs:64-66) or Xplor (xplor.rs: s(r) F(r), s the smoothing polynomial between
+// r_smooth and r_cut).
+__device__ __forceinline__ double isotropic_pair64(const Pair& P, double r2) {
+    if (r2 >= P.uv_rcut2) return 0.0;
+    double r = dsqrt(r2);
+    switch (P.uv_wrap) {
+        case kUvwShifted:
+            return dsub(univariate64(P.uv_kind, P.uv_p, r), P.uv_shift);
+        case kUvwExpanded:
+            return univariate64(P.uv_kind, P.uv_p, dsub(r, P.uv_w[0]));
+        case kUvwXplor: {
+            double sm;
+            if (r < P.uv_w[1]) {
+                sm = 1.0;
+            } else if (r > P.uv_w[0]) {
+                sm = 0.0;
+            } else {
+                const double r_sq = dmul(r, r), rc_sq = dmul(P.uv_w[0], P.uv_w[0]), rs_sq = dmul(P.uv_w[1], P.uv_w[1]);
+                const double a = dsub(rc_sq, r_sq), d = dsub(rc_sq, rs_sq);
+                sm = ddiv(dmul(dmul(a, a), dsub(dadd(rc_sq, dmul(2.0, r_sq)), dmul(3.0, rs_sq))), dmul(dmul(d, d), d));
+            }
+            return dmul(sm, univariate64(P.uv_kind, P.uv_p, r));
+        }
+        default:
+            return univariate64(P.uv_kind, P.uv_p, r);
+    }
+}
 
 // The overlap penalty's pair energy in FP64 with the reference's operation order.
 __device__ __forceinline__ double penalty_pair64(const Pair& P, double r2) {
@@ -124,6 +195,7 @@ __device__ __forceinline__ double penalty_pair64(const Pair& P, double r2) {
 // of Shifted (shifted.rs:92-94: f(r) - f(r_shift)) LennardJones (lennard_jones.rs:107-111:
 // 4 eps ((sigma/r)^12 - (sigma/r)^6) with powi by repeated squaring).
 __device__ __forceinline__ double lj_pair64(const Pair& P, double r2) {
+    if (P.isotropic) return isotropic_pair64(P, r2);
     if (P.penalty) return penalty_pair64(P, r2);
     if (r2 >= P.lj_rcut2) return 0.0;
     const double r = dsqrt(r2);

@@ -42,7 +42,8 @@
 extern "C" {
 #endif
 
-#define HMC_ABI_VERSION 2u  /* 2: hmc_count gained order_ambiguous */
+#define HMC_ABI_VERSION 3u  /* 2: hmc_count gained order_ambiguous; 3: HMC_ISOTROPIC and its
+                               hmc_system_desc fields, hmc_set_shape_overlap */
 
 typedef enum hmc_status {
     HMC_OK = 0,
@@ -70,12 +71,34 @@ typedef enum hmc_interaction {
     HMC_LENNARD_JONES = 3,          /* PairwiseCutoff(Isotropic { Shifted { LennardJones }, r_cut }) */
     HMC_HARD_CONVEX_SURFACE_MESH_2D = 4, /* PairwiseCutoff(HardShape(ConvexSurfaceMesh2d)): vertices are
                                            the counter-clockwise hull (convex_surface_mesh_2d.rs) */
-    HMC_OVERLAP_PENALTY = 5         /* PairwiseCutoff(Isotropic { Expanded { delta: diameter,
+    HMC_OVERLAP_PENALTY = 5,        /* PairwiseCutoff(Isotropic { Expanded { delta: diameter,
                                        OverlapPenalty { k, maximum_allowed_overlap, epsilon_shoulder } },
                                        r_cut: diameter }): the soft sphere that QuickInsert and
                                        QuickCompress use (univariate/overlap_penalty.rs:42-116,
                                        expanded.rs:62-67, benchmarks/src/mc/hard_sphere.rs:191-199) */
+    HMC_ISOTROPIC = 6               /* PairwiseCutoff(Isotropic { W(F), r_cut }) for a univariate F
+                                       (hmc_system_desc.univariate, hmc_univariate) in a wrapper W
+                                       (univariate_wrap, hmc_univariate_wrap), isotropic.rs:88-187;
+                                       FP64 in both precision modes */
 } hmc_interaction;
+
+/* The univariate energies of HMC_ISOTROPIC (hoomd-interaction/src/univariate/), with their
+ * parameters in hmc_system_desc.univariate_params in this order. */
+typedef enum hmc_univariate {
+    HMC_UV_LENNARD_JONES = 0,          /* {epsilon, sigma}: LennardJones<12, 6> */
+    HMC_UV_WEEKS_CHANDLER_ANDERSON = 1, /* {epsilon, sigma} */
+    HMC_UV_HARMONIC = 2,               /* {k, r_0} */
+    HMC_UV_HARMONIC_REPULSION = 3,     /* {a, r_cut} */
+    HMC_UV_BOXCAR = 4,                 /* {epsilon, left, right} */
+    HMC_UV_OVERLAP_PENALTY = 5         /* {k, maximum_allowed_overlap, epsilon_shoulder} */
+} hmc_univariate;
+/* The wrapper around the univariate, with its parameters in hmc_system_desc.wrap_params. */
+typedef enum hmc_univariate_wrap {
+    HMC_UVW_NONE = 0,
+    HMC_UVW_SHIFTED = 1,  /* {r_shift}: Shifted, F(r) - F(r_shift) */
+    HMC_UVW_EXPANDED = 2, /* {delta}: Expanded, F(r - delta) */
+    HMC_UVW_XPLOR = 3     /* {r_cut, r_smooth}: Xplor, s(r) F(r) */
+} hmc_univariate_wrap;
 
 typedef enum hmc_move {
     HMC_TRANSLATE = 0, /* Translate::with_maximum_distance(maximum) */
@@ -117,6 +140,11 @@ typedef struct hmc_system_desc {
     double penalty_shoulder;     /* OverlapPenalty::epsilon_shoulder (default 100) */
     uint64_t capacity;           /* bodies the system can hold (>= n_bodies; 0 = n_bodies);
                                     hmc_quick_insert_apply adds bodies up to it */
+    uint32_t univariate;         /* HMC_ISOTROPIC: hmc_univariate */
+    uint32_t univariate_wrap;    /* HMC_ISOTROPIC: hmc_univariate_wrap */
+    double univariate_params[4]; /* HMC_ISOTROPIC: the univariate's parameters */
+    double wrap_params[2];       /* HMC_ISOTROPIC: the wrapper's parameters */
+    double isotropic_r_cut;      /* HMC_ISOTROPIC: Isotropic::r_cut (the pair range) */
 } hmc_system_desc;
 
 typedef struct hmc_sweep_params {

@@ -24,6 +24,9 @@ HARD_CONVEX_SURFACE_MESH_2D = 4
 OVERLAP_PENALTY = 5
 CONVEX_POLYHEDRON_PENALTY = 6  # Anisotropic { ApproximateShapeOverlap { Convex(ConvexPolyhedron), OverlapPenalty } }
 CONVEX_POLYGON_PENALTY = 7     # the same with Convex(ConvexPolygon)
+ISOTROPIC = 8                  # Isotropic { W(F), r_cut }: F and W below
+UV_LENNARD_JONES, UV_WEEKS_CHANDLER_ANDERSON, UV_HARMONIC, UV_HARMONIC_REPULSION, UV_BOXCAR, UV_OVERLAP_PENALTY = range(6)
+UVW_NONE, UVW_SHIFTED, UVW_EXPANDED, UVW_XPLOR = range(4)
 TRANSLATE = 0
 ROTATE = 1
 
@@ -95,6 +98,9 @@ def lib():
         L.oracle_gsd_frame.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.oracle_set_penalty.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double]
         L.oracle_set_shape_overlap.argtypes = [C.c_void_p, C.c_double, C.c_double]
+        L.oracle_set_isotropic.argtypes = [C.c_void_p, C.c_uint32, _dp, C.c_uint32, _dp, C.c_double]
+        L.oracle_univariate_energy.argtypes = [C.c_uint32, _dp, C.c_uint32, _dp, C.c_double]
+        L.oracle_univariate_energy.restype = C.c_double
         L.oracle_approximate_separation.argtypes = [C.c_uint32, _dp, C.c_uint32, _dp, _dp, C.c_double]
         L.oracle_approximate_separation.restype = C.c_double
         L.oracle_n_bodies.argtypes = [C.c_void_p]
@@ -287,6 +293,17 @@ def approximate_separation(vertices, v_ij, o_ij, resolution) -> float:
                                                      _d(_f64(np.atleast_1d(o_ij))), resolution))
 
 
+def _params(p, n):
+    a = np.zeros(n)
+    a[:len(p)] = p
+    return a
+
+
+def univariate_energy(kind, params, r, wrap=UVW_NONE, wrap_params=()) -> float:
+    """W(F).energy(r) for a univariate F (UV_*) with parameters `params` and a wrapper W (UVW_*)."""
+    return float(lib().oracle_univariate_energy(kind, _d(_params(params, 4)), wrap, _d(_params(wrap_params, 2)), r))
+
+
 def cr_sincos(x: float):
     """Correctly rounded (sin x, cos x); raises for |x| >= 2^20."""
     s = C.c_double()
@@ -334,7 +351,7 @@ class System:
     def __init__(self, dim, edge_lengths, positions, orientations=None, *, step=0, substep=0, seed=0,
                  interaction=HARD_SPHERE, diameter=1.0, vertices=None, lj_epsilon=1.0, lj_sigma=1.0,
                  lj_r_cut=2.5, lj_r_shift=2.5, boundary_range=None, penalty=(10000.0, 0.2, 100.0),
-                 resolution=0.01, r_cut=None):
+                 resolution=0.01, r_cut=None, isotropic=None):
         self.dim = dim
         self.L = _f64(edge_lengths)
         self.seed = seed
@@ -344,6 +361,8 @@ class System:
         ori = None if orientations is None else _f64(orientations, (-1,))
         verts = None if vertices is None else _f64(vertices, (-1,))
         nv = 0 if verts is None else verts.size // dim
+        if boundary_range is None and interaction == ISOTROPIC:
+            boundary_range = isotropic["r_cut"]
         if boundary_range is None:
             if interaction in (HARD_SPHERE, OVERLAP_PENALTY):
                 boundary_range = diameter
@@ -355,7 +374,13 @@ class System:
         self._h = lib().oracle_system_create(dim, _d(self.L), self.n, _d(pos), _d(ori), step, substep, seed,
                                              interaction, diameter, _d(verts), nv, lj_epsilon, lj_sigma,
                                              lj_r_cut, lj_r_shift, boundary_range)
-        self.ori_len = 0 if interaction in (HARD_SPHERE, LENNARD_JONES, OVERLAP_PENALTY) else (4 if dim == 3 else 1)
+        self.ori_len = 0 if interaction in (HARD_SPHERE, LENNARD_JONES, OVERLAP_PENALTY, ISOTROPIC) else \
+            (4 if dim == 3 else 1)
+        if interaction == ISOTROPIC:
+            # isotropic = {"kind", "params", "wrap", "wrap_params", "r_cut"}
+            lib().oracle_set_isotropic(self._h, isotropic["kind"], _d(_params(isotropic["params"], 4)),
+                                       isotropic.get("wrap", UVW_NONE), _d(_params(isotropic.get("wrap_params", ()), 2)),
+                                       isotropic["r_cut"])
         if interaction in (OVERLAP_PENALTY, CONVEX_POLYHEDRON_PENALTY, CONVEX_POLYGON_PENALTY):
             lib().oracle_set_penalty(self._h, *penalty)
         if interaction in (CONVEX_POLYHEDRON_PENALTY, CONVEX_POLYGON_PENALTY):

@@ -837,6 +837,61 @@ double shifted_lj_pair(double eps, double sigma, double rcut, double rshift, dou
     return lj_energy(eps, sigma, r) - lj_energy(eps, sigma, rshift);
 }
 
+// The univariate energies Isotropic accepts (hoomd-interaction/src/univariate/*.rs), each with
+// the reference's order of operations, and the wrappers around them.
+enum { UV_LENNARD_JONES = 0, UV_WEEKS_CHANDLER_ANDERSON = 1, UV_HARMONIC = 2, UV_HARMONIC_REPULSION = 3,
+       UV_BOXCAR = 4, UV_OVERLAP_PENALTY = 5 };
+enum { UVW_NONE = 0, UVW_SHIFTED = 1, UVW_EXPANDED = 2, UVW_XPLOR = 3 };
+struct Univariate {
+    int kind = UV_LENNARD_JONES, wrap = UVW_NONE;
+    double p[4] = {0, 0, 0, 0};  // the univariate's parameters
+    double w[2] = {0, 0};        // Shifted: r_shift; Expanded: delta; Xplor: r_cut, r_smooth
+    double rcut = 1.0;           // Isotropic::r_cut
+    double f(double r) const {
+        switch (kind) {
+            case UV_LENNARD_JONES:  // lennard_jones.rs:107-111
+                return lj_energy(p[0], p[1], r);
+            case UV_WEEKS_CHANDLER_ANDERSON:  // weeks_chandler_anderson.rs: r < 2^(1/6) sigma (p[2] = 2^(1/6))
+                return r < p[2] * p[1] ? lj_energy(p[0], p[1], r) + p[0] : 0.0;
+            case UV_HARMONIC:  // harmonic.rs: 0.5 k (r - r_0) (r - r_0)
+                return 0.5 * p[0] * (r - p[1]) * (r - p[1]);
+            case UV_HARMONIC_REPULSION:  // harmonic_repulsion.rs: 0.5 a / r_cut (r - r_cut)^2 below r_cut
+                return r < p[1] ? 0.5 * p[0] / p[1] * ((r - p[1]) * (r - p[1])) : 0.0;
+            case UV_BOXCAR:  // boxcar.rs: epsilon on [left, right)
+                return r < p[1] ? 0.0 : (r < p[2] ? p[0] : 0.0);
+            default:  // overlap_penalty.rs:109-115
+                if (r < -p[1]) return INFINITY;
+                if (r < 0.0) return 0.5 * p[0] * (r * r) + p[2];
+                return 0.0;
+        }
+    }
+    // Xplor::s (xplor.rs): 1 below r_smooth, 0 beyond r_cut, the smoothing polynomial between.
+    double xplor_s(double r) const {
+        if (r < w[1]) return 1.0;
+        if (r > w[0]) return 0.0;
+        const double r_sq = r * r, rc_sq = w[0] * w[0], rs_sq = w[1] * w[1];
+        const double a = rc_sq - r_sq, d = rc_sq - rs_sq;
+        return a * a * (rc_sq + 2.0 * r_sq - 3.0 * rs_sq) / (d * d * d);
+    }
+    double energy(double r) const {
+        switch (wrap) {
+            case UVW_SHIFTED:  // shifted.rs:92-94
+                return f(r) - f(w[0]);
+            case UVW_EXPANDED:  // expanded.rs:64-66
+                return f(r - w[0]);
+            case UVW_XPLOR:
+                return xplor_s(r) * f(r);
+            default:
+                return f(r);
+        }
+    }
+    // Isotropic::site_pair_energy (isotropic.rs:147-156)
+    double pair(double r2) const {
+        if (r2 >= rcut * rcut) return 0.0;
+        return energy(std::sqrt(r2));
+    }
+};
+
 // ============================================================================
 // hoomd-microstate: periodic hypercuboid boundary
 // ============================================================================
@@ -1130,10 +1185,12 @@ struct oracle_system {
         return interaction == ORACLE_CONVEX_POLYHEDRON_PENALTY || interaction == ORACLE_CONVEX_POLYGON_PENALTY;
     }
     bool hard() const {
-        return interaction != ORACLE_LENNARD_JONES && interaction != ORACLE_OVERLAP_PENALTY && !shape_penalty();
+        return interaction != ORACLE_LENNARD_JONES && interaction != ORACLE_OVERLAP_PENALTY &&
+               interaction != ORACLE_ISOTROPIC && !shape_penalty();
     }
     double pk = 10000.0, pdmax = 0.2, pshoulder = 100.0;  // OverlapPenalty
     double presolution = 0.01, prcut = 1.0;              // ApproximateShapeOverlap, Anisotropic r_cut
+    Univariate uv;                                       // ORACLE_ISOTROPIC
     bool oriented() const {
         return interaction == ORACLE_HARD_CONVEX_POLYGON || interaction == ORACLE_HARD_CONVEX_POLYHEDRON ||
                interaction == ORACLE_HARD_CONVEX_SURFACE_MESH_2D || shape_penalty();
@@ -1225,6 +1282,8 @@ struct oracle_system {
             }
             case ORACLE_CONVEX_POLYGON_PENALTY:
                 return shape_penalty_2d(poly, prcut, presolution, pk, pdmax, pshoulder, x, o[0], y, orient[j]);
+            case ORACLE_ISOTROPIC:
+                return uv.pair(distance_squared(x, y, dim));
             case ORACLE_OVERLAP_PENALTY: {
                 // Isotropic::site_pair_energy (isotropic.rs:147-156) of Expanded { delta: diameter,
                 // OverlapPenalty } (expanded.rs:64-66, overlap_penalty.rs:109-115), r_cut = diameter
@@ -1370,6 +1429,28 @@ void oracle_set_penalty(oracle_system* s, double k, double maximum_allowed_overl
     s->pshoulder = epsilon_shoulder;
 }
 static Polytope make_poly(const double* verts, uint32_t nv, int dim);
+void oracle_set_isotropic(oracle_system* s, uint32_t kind, const double* params, uint32_t wrap,
+                          const double* wrap_params, double r_cut) {
+    Univariate& u = s->uv;
+    u.kind = (int)kind;
+    u.wrap = (int)wrap;
+    for (int k = 0; k < 4; ++k) u.p[k] = params[k];
+    for (int k = 0; k < 2; ++k) u.w[k] = wrap_params[k];
+    if (kind == UV_WEEKS_CHANDLER_ANDERSON) u.p[2] = std::pow(2.0, 1.0 / 6.0);
+    u.rcut = r_cut;
+    s->search_range = r_cut;
+    s->build_grid();
+}
+double oracle_univariate_energy(uint32_t kind, const double* params, uint32_t wrap, const double* wrap_params,
+                                double r) {
+    Univariate u;
+    u.kind = (int)kind;
+    u.wrap = (int)wrap;
+    for (int k = 0; k < 4; ++k) u.p[k] = params[k];
+    for (int k = 0; k < 2; ++k) u.w[k] = wrap_params[k];
+    if (kind == UV_WEEKS_CHANDLER_ANDERSON) u.p[2] = std::pow(2.0, 1.0 / 6.0);
+    return u.energy(r);
+}
 void oracle_set_shape_overlap(oracle_system* s, double resolution, double r_cut) {
     s->presolution = resolution;
     s->prcut = r_cut;
@@ -1771,6 +1852,9 @@ oracle_system* oracle_system_create(uint32_t dim, const double* L, uint64_t n, c
             break;
         case ORACLE_OVERLAP_PENALTY:
             s->search_range = diameter;
+            break;
+        case ORACLE_ISOTROPIC:  // r_cut, set again by oracle_set_isotropic
+            s->search_range = boundary_range;
             break;
         default:
             s->search_range = s->poly.bounding_radius * 2.0;

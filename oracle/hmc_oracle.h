@@ -82,7 +82,7 @@ double oracle_shifted_lj_pair(double epsilon, double sigma, double r_cut, double
 // ---- systems --------------------------------------------------------------------
 enum { ORACLE_HARD_SPHERE = 0, ORACLE_HARD_CONVEX_POLYGON = 1, ORACLE_HARD_CONVEX_POLYHEDRON = 2,
        ORACLE_LENNARD_JONES = 3, ORACLE_HARD_CONVEX_SURFACE_MESH_2D = 4, ORACLE_OVERLAP_PENALTY = 5,
-       ORACLE_CONVEX_POLYHEDRON_PENALTY = 6, ORACLE_CONVEX_POLYGON_PENALTY = 7 };
+       ORACLE_CONVEX_POLYHEDRON_PENALTY = 6, ORACLE_CONVEX_POLYGON_PENALTY = 7, ORACLE_ISOTROPIC = 8 };
 enum { ORACLE_TRANSLATE = 0, ORACLE_ROTATE = 1 };
 
 typedef struct oracle_system oracle_system;
@@ -106,6 +106,15 @@ void oracle_set_penalty(oracle_system* s, double k, double maximum_allowed_overl
 // (interactions ORACLE_CONVEX_POLYHEDRON_PENALTY and ORACLE_CONVEX_POLYGON_PENALTY; the penalty's
 // parameters come from oracle_set_penalty). r_cut is also the checkerboard's search range.
 void oracle_set_shape_overlap(oracle_system* s, double resolution, double r_cut);
+// Isotropic { W(F), r_cut } (interaction ORACLE_ISOTROPIC): F = kind (0 LennardJones {eps, sigma},
+// 1 WeeksChandlerAnderson {eps, sigma}, 2 Harmonic {k, r_0}, 3 HarmonicRepulsion {a, r_cut},
+// 4 Boxcar {eps, left, right}, 5 OverlapPenalty {k, d_max, eps}), W = wrap (0 none, 1 Shifted
+// {r_shift}, 2 Expanded {delta}, 3 Xplor {r_cut, r_smooth}); r_cut is also the search range.
+void oracle_set_isotropic(oracle_system* s, uint32_t kind, const double* params, uint32_t wrap,
+                          const double* wrap_params, double r_cut);
+// W(F).energy(r) for the same kinds.
+double oracle_univariate_energy(uint32_t kind, const double* params, uint32_t wrap, const double* wrap_params,
+                                double r);
 // IntersectsAt::approximate_separation_distance of two equal convex polytopes (n_vertices x dim
 // vertices): v_ij in the first shape's frame, o_ij a versor (s, x, y, z) or an angle.
 double oracle_approximate_separation(uint32_t dim, const double* vertices, uint32_t n_vertices, const double* v_ij,

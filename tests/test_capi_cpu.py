@@ -43,7 +43,7 @@ def test_library_loads_without_gpu_and_binds(lib_path):
 
     lib = h.load_library(lib_path)
     assert set(h.SIGNATURES) == set(declared_functions())
-    assert lib.hmc_abi_version() == 2
+    assert lib.hmc_abi_version() == 3
     assert lib.hmc_status_string(h.RANGE_TOO_LARGE).decode().startswith("interaction range")
 
 
