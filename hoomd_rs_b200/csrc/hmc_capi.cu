@@ -702,7 +702,7 @@ hmc_status hmc_system_create(hmc_context* ctx, const hmc_system_desc* d, const d
         s->n_vertices = d->n_vertices;
     } else if (d->interaction == HMC_ISOTROPIC) {
         Pair& P = s->pair;
-        P.isotropic = 1;
+        P.penalty = 2;
         P.uv_kind = d->univariate;
         P.uv_wrap = d->univariate_wrap;
         for (int k = 0; k < 4; ++k) P.uv_p[k] = d->univariate_params[k];
@@ -966,8 +966,8 @@ hmc_status hmc_sweep(hmc_system* s, const hmc_sweep_params* p, hmc_count* out) {
                     // wait for it before reading anything
                     L.early_wait = (r == 0 || s->soft() || s->oriented()) && c == 0 && s->pdl ? 1u : 0u;
                     if (s->soft())  // the overlap penalty has no FP32 path: FP64 in both modes
-                        HMC_CUDA(launch_sweep_lj(s->dim, fp32 && s->soft_fp32(), s->geom, s->arr, s->pair, L,
-                                                 s->stream, variant));
+                        HMC_CUDA(launch_sweep_lj(s->dim, fp32 && s->soft_fp32(), !s->soft_fp32(), s->geom, s->arr,
+                                                 s->pair, L, s->stream, variant));
                     else if (s->shape_soft && s->dim == 3)  // FP64 in both modes
                         HMC_CUDA(launch_sweep_poly3_soft(s->geom, s->arr, s->verts, s->n_vertices, s->so, L,
                                                          s->stream));

@@ -102,14 +102,13 @@ struct Pair {
     float lj_band_energy; // bound on |pair energy| for a pair inside the cut-off band
     // Isotropic<Expanded<OverlapPenalty>> (overlap_penalty.rs:109-115, expanded.rs:64-66):
     // r^2 >= r_cut^2 -> 0; x = sqrt(r^2) - delta; x < -d_max -> inf; x < 0 -> (0.5 k) x^2 + eps
-    uint32_t penalty;     // 1: the soft pair energy is the overlap penalty, else Lennard-Jones
+    uint32_t penalty;     // the soft pair energy: 0 Lennard-Jones, 1 the overlap penalty, 2 Isotropic (below)
     double op_rcut2;      // r_cut.powi(2)
     double op_delta;
     double op_dmax;       // maximum_allowed_overlap
     double op_half_k;     // 0.5 * k
     double op_shoulder;   // epsilon_shoulder
-    // Isotropic { W(F), r_cut } for the univariates of hmc_univariate (hmc.h): isotropic = 1
-    uint32_t isotropic;
+    // Isotropic { W(F), r_cut } for the univariates of hmc_univariate (hmc.h): penalty = 2
     uint32_t uv_kind, uv_wrap;  // hmc_univariate, hmc_univariate_wrap
     double uv_p[4];             // F's parameters (WeeksChandlerAnderson: p[2] = 2^(1/6), the host's pow)
     double uv_w[2];             // W's parameters: Shifted {r_shift}, Expanded {delta}, Xplor {r_cut, r_smooth}
@@ -194,14 +193,22 @@ __device__ __forceinline__ double penalty_pair64(const Pair& P, double r2) {
 // Isotropic::site_pair_energy (isotropic.rs:147-156: r^2 >= r_cut^2 -> 0, else energy(sqrt(r^2)))
 // of Shifted (shifted.rs:92-94: f(r) - f(r_shift)) LennardJones (lennard_jones.rs:107-111:
 // 4 eps ((sigma/r)^12 - (sigma/r)^6) with powi by repeated squaring).
-__device__ __forceinline__ double lj_pair64(const Pair& P, double r2) {
-    if (P.isotropic) return isotropic_pair64(P, r2);
-    if (P.penalty) return penalty_pair64(P, r2);
+__device__ __forceinline__ double lj_only64(const Pair& P, double r2) {
     if (r2 >= P.lj_rcut2) return 0.0;
     const double r = dsqrt(r2);
     const double sr = ddiv(P.lj_sigma, r);
     const double s2 = dmul(sr, sr), s4 = dmul(s2, s2), s8 = dmul(s4, s4);
     return dsub(dmul(P.lj_four_eps, dsub(dmul(s4, s8), dmul(s2, s4))), P.lj_e_shift);
+}
+__device__ __forceinline__ double lj_pair64(const Pair& P, double r2) {
+    if (P.penalty) return P.penalty == 1u ? penalty_pair64(P, r2) : isotropic_pair64(P, r2);
+    return lj_only64(P, r2);
+}
+// GENERIC = false: the kernel serves Shifted Lennard-Jones only (its FP32 passes and batches), so
+// the other energies stay out of its code and registers.
+template <bool GENERIC>
+__device__ __forceinline__ double soft_pair64(const Pair& P, double r2) {
+    return GENERIC ? lj_pair64(P, r2) : lj_only64(P, r2);
 }
 
 // One sweep launch: counter, move and colour.
@@ -366,7 +373,9 @@ cudaError_t launch_sweep_sphere(int dim, bool fp32, const Geometry& g, const Arr
                                 const Launch& l, bool coop, cudaStream_t s, uint32_t variant = 0);
 cudaError_t launch_overlap_sphere(int dim, const Geometry& g, const Arrays& a, const Pair& p, uint32_t n,
                                   cudaStream_t s);
-cudaError_t launch_sweep_lj(int dim, bool fp32, const Geometry& g, const Arrays& a, const Pair& p, const Launch& l,
+// generic: the system's energy is not Shifted Lennard-Jones (the overlap penalty, Isotropic).
+cudaError_t launch_sweep_lj(int dim, bool fp32, bool generic, const Geometry& g, const Arrays& a, const Pair& p,
+                            const Launch& l,
                             cudaStream_t s, uint32_t variant = 0);
 // The trial moves of round l.round for every colour list at once (Arrays::trial_*), one thread
 // per trial; launched in stream order before the round's colour passes of the passes that give a

@@ -80,7 +80,7 @@ __device__ __forceinline__ uint32_t warp_maxu(uint32_t v) {
 // S of a candidate comes from sorted_s when have_s, else from wrap(sorted_b). The two sums of
 // one call equal two calls of one sum each over the same stencil.
 // mag receives sum |e| over both sums (for order_ambiguous).
-template <int DIM, bool TWO>
+template <int DIM, bool TWO, bool GENERIC = true>
 __device__ __forceinline__ void lj_energy64(const Geometry& g, const Arrays& A, const Pair& P, const double* ta,
                                             const double* tb, const FlatStencil& fs, uint32_t self, bool have_s,
                                             uint32_t lane, double& ea, double& eb, double& mag) {
@@ -104,11 +104,11 @@ __device__ __forceinline__ void lj_energy64(const Geometry& g, const Arrays& A, 
                 sv[2] = b4.z;
                 wrap_inv<DIM>(g.L, g.invL, sv);
             }
-            const double x = lj_pair64(P, ref_dist2<DIM>(g, ta, sv));
+            const double x = soft_pair64<GENERIC>(P, ref_dist2<DIM>(g, ta, sv));
             a = dadd(a, x);
             am += fabs(x);
             if (TWO) {
-                const double y = lj_pair64(P, ref_dist2<DIM>(g, tb, sv));
+                const double y = soft_pair64<GENERIC>(P, ref_dist2<DIM>(g, tb, sv));
                 b = dadd(b, y);
                 am += fabs(y);
             }
@@ -256,7 +256,7 @@ __device__ __forceinline__ void lj_inject(const Arrays& A, const Injected& J, ui
 }
 
 // The FP64 pass: one warp per trial. INJ: the probe mode (decisions instead of commits).
-template <int DIM, bool INJ = false, int MINB = HMC_LJ_MIN_BLOCKS>
+template <int DIM, bool INJ = false, int MINB = HMC_LJ_MIN_BLOCKS, bool GENERIC = true>
 __global__ void __launch_bounds__(128, MINB) k_sweep_lj(Geometry g, Arrays A, Pair P, Launch L, Injected J) {
     if (L.early_wait) grid_dependency_wait();  // first pass: the rebuild's arrays are read at once
     const uint32_t lane = threadIdx.x & 31u;
@@ -306,7 +306,7 @@ __global__ void __launch_bounds__(128, MINB) k_sweep_lj(Geometry g, Arrays A, Pa
         const double4 s4 = ldg4(A.sorted_s + k);
         const double si[3] = {s4.x, s4.y, s4.z};
         double e_new, e_old, mag;
-        lj_energy64<DIM, true>(g, A, P, t, si, fs, k, true, lane, e_new, e_old, mag);
+        lj_energy64<DIM, true, GENERIC>(g, A, P, t, si, fs, k, true, lane, e_new, e_old, mag);
         const double du = dsub(e_new, e_old);
         const double e0 = exp(ddiv(-du, L.kt));
         const bool amb = order_ambiguous(du, mag, fs.total, u, L.kt, e0);
@@ -457,8 +457,8 @@ __global__ void __launch_bounds__(128, MINB) k_sweep_lj32(Geometry g, Arrays A, 
                                 const double4 b4 = ldg4(A.sorted_b + q);
                                 double sv[3] = {b4.x, b4.y, b4.z};
                                 wrap_inv<DIM>(g.L, g.invL, sv);
-                                en = lj_pair64(P, ref_dist2<DIM>(g, s_trial.t, sv));
-                                eo = lj_pair64(P, ref_dist2<DIM>(g, s_trial.si, sv));
+                                en = lj_only64(P, ref_dist2<DIM>(g, s_trial.t, sv));
+                                eo = lj_only64(P, ref_dist2<DIM>(g, s_trial.si, sv));
                             }
                         }
                         s_e[c - c0][0][lane] = en;
@@ -555,7 +555,7 @@ __global__ void __launch_bounds__(128, HMC_LJ_BATCH_MIN_BLOCKS)
         const double4 s4 = ldg4(A.sorted_s + k);
         const double si[3] = {s4.x, s4.y, s4.z};
         double e_new, e_old, mag;
-        lj_energy64<DIM, true>(g, A, R.p, t, si, fs, k, true, lane, e_new, e_old, mag);
+        lj_energy64<DIM, true, false>(g, A, R.p, t, si, fs, k, true, lane, e_new, e_old, mag);
         const double du = dsub(e_new, e_old);
         const double e0 = exp(ddiv(-du, R.kt));
         if (lane == 0 && order_ambiguous(du, mag, fs.total, u, R.kt, e0)) pst.ambiguous++;
@@ -681,8 +681,8 @@ __global__ void __launch_bounds__(128, HMC_LJ_BATCH_MIN_BLOCKS)
                                 const double4 b4 = ldg4(A.sorted_b + q);
                                 double sv[3] = {b4.x, b4.y, b4.z};
                                 wrap_inv<DIM>(RO.g.L, RO.g.invL, sv);
-                                en = lj_pair64(RO.p, ref_dist2<DIM>(RO.g, s_trial.t, sv));
-                                eo = lj_pair64(RO.p, ref_dist2<DIM>(RO.g, s_trial.si, sv));
+                                en = lj_only64(RO.p, ref_dist2<DIM>(RO.g, s_trial.t, sv));
+                                eo = lj_only64(RO.p, ref_dist2<DIM>(RO.g, s_trial.si, sv));
                             }
                         }
                         s_e[c - c0][0][lane] = en;
@@ -883,8 +883,8 @@ __global__ void k_energy_lj(Geometry g, Arrays A, Pair P, uint32_t n, double* ou
 
 }  // namespace
 
-cudaError_t launch_sweep_lj(int dim, bool fp32, const Geometry& g, const Arrays& a, const Pair& p, const Launch& l,
-                            cudaStream_t s, uint32_t variant) {
+cudaError_t launch_sweep_lj(int dim, bool fp32, bool generic, const Geometry& g, const Arrays& a, const Pair& p,
+                            const Launch& l, cudaStream_t s, uint32_t variant) {
     if (l.n_active == 0) return cudaSuccess;
     static int max_blocks = 0;
     if (max_blocks == 0) {
@@ -899,11 +899,16 @@ cudaError_t launch_sweep_lj(int dim, bool fp32, const Geometry& g, const Arrays&
     using LjKernel = void (*)(Geometry, Arrays, Pair, Launch, Injected);
     // the compiled launch variants, in the order of kLjShapes ([dim == 3][fp32][variant])
     static const LjKernel kernels[2][2][3] = {
-        {{k_sweep_lj<2, false, 9>, k_sweep_lj<2, false, 7>, k_sweep_lj<2, false, 11>},
+        {{k_sweep_lj<2, false, 9, false>, k_sweep_lj<2, false, 7, false>, k_sweep_lj<2, false, 11, false>},
          {k_sweep_lj32<2, false, 9>, k_sweep_lj32<2, false, 7>, k_sweep_lj32<2, false, 11>}},
-        {{k_sweep_lj<3, false, 9>, k_sweep_lj<3, false, 7>, k_sweep_lj<3, false, 11>},
+        {{k_sweep_lj<3, false, 9, false>, k_sweep_lj<3, false, 7, false>, k_sweep_lj<3, false, 11, false>},
          {k_sweep_lj32<3, false, 9>, k_sweep_lj32<3, false, 7>, k_sweep_lj32<3, false, 11>}}};
-    const LjKernel k = kernels[dim == 3][fp32][variant < 3 ? variant : 0];
+    // the overlap penalty and Isotropic: the FP64 pass with the dispatching pair energy
+    static const LjKernel generic_kernels[2][3] = {
+        {k_sweep_lj<2, false, 9, true>, k_sweep_lj<2, false, 7, true>, k_sweep_lj<2, false, 11, true>},
+        {k_sweep_lj<3, false, 9, true>, k_sweep_lj<3, false, 7, true>, k_sweep_lj<3, false, 11, true>}};
+    const LjKernel k = generic ? generic_kernels[dim == 3][variant < 3 ? variant : 0]
+                               : kernels[dim == 3][fp32][variant < 3 ? variant : 0];
     return cudaLaunchKernelEx(&pl.cfg, k, g, a, p, l, Injected{});
 }
 
