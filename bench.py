@@ -39,8 +39,8 @@ TARGET_ACCEPTANCE = 0.30
 
 
 # DRAM bytes of one FP32 colour pass of this workload, read + written, from one ncu capture of
-# the pass (dram__bytes_read.sum + dram__bytes_write.sum): 30.51 MB + 0.07 MB.
-SPHERE_PASS_DRAM_BYTES = 30.58e6
+# the pass (dram__bytes_read.sum + dram__bytes_write.sum): 30.72 MB + 0.04 MB.
+SPHERE_PASS_DRAM_BYTES = 30.76e6
 
 
 def aggregate_over_ranks(elapsed, units, world, device):
