@@ -125,53 +125,20 @@ struct Sums32 {
 };
 
 // FP32 energies of the trial site (offsets t32) and the current site (offsets c32) against
-// the stencil fs of their common space, with error bounds. The lanes take the stencil's
-// candidates 32 at a time, but only ~1 in 7 lies inside the cut-off band; instead of evaluating
-// the pair energy where a lane has one (a handful of lanes active), each step lists the in-band
-// r^2 of the step in the warp's buffer buf (kLjBuf floats of shared memory; old-site entries
-// carry the sign bit) and the warp evaluates the listed pairs 32 at a time. The sums are FP32
-// with a bound on their error for any order (terms per lane + the 5 reduction levels), so the
-// order of the listed pairs does not matter; the FP64 recheck keeps its own fixed order.
-constexpr uint32_t kLjBuf = 96;  // < 32 listed + 64 from one step
+// the stencil fs of their common space, with error bounds.
 template <int DIM>
 __device__ __forceinline__ Sums32 lj_energy32(const Geometry& g, const Arrays& A, const Pair& P, float4 t32,
                                                float4 c32, int mf, const FlatStencil& fs, uint32_t self,
-                                               uint32_t lane, float* buf) {
+                                               uint32_t lane) {
     Sums32 s{0.f, 0.f, 0.f, 0.f, 0u, 0u};
-    const unsigned full = 0xffffffffu;
     const uint32_t sf = g.shape[DIM - 1];
-    uint32_t n_buf = 0;  // warp-uniform
-    uint32_t my_terms = 0;
-    // the first 32 listed pairs, one per lane; the rest move down
-    auto drain = [&](uint32_t count) {
-        __syncwarp();
-        if (lane < count) {
-            const float x = buf[lane];
-            float e, err;
-            lj_pair32(P, fabsf(x), e, err);
-            if (signbit(x))
-                s.e_old += e;
-            else
-                s.e_new += e;
-            s.err += err;
-            s.mag += fabsf(e);
-            my_terms += 1;
-        }
-        __syncwarp();
-        const uint32_t rest = n_buf > 32u ? n_buf - 32u : 0u;
-        for (uint32_t k2 = lane; k2 < rest; k2 += 32u) buf[k2] = buf[32u + k2];
-        n_buf = rest;
-        __syncwarp();
-    };
 #pragma unroll 1
     for (uint32_t j0 = 0; j0 < fs.total; j0 += 32) {
         const uint32_t j = j0 + lane;
         uint32_t part;
         const uint32_t q = flat_slot(fs, j, part);
-        const float s0 = __shfl_sync(full, fs.s0, part);
-        const float s1 = __shfl_sync(full, fs.s1, part);
-        bool in_n = false, in_o = false;
-        float r2n = 0.f, r2o = 0.f;
+        const float s0 = __shfl_sync(0xffffffffu, fs.s0, part);
+        const float s1 = __shfl_sync(0xffffffffu, fs.s1, part);
         if (j < fs.total && q != self) {
             const float4 o = __ldg(A.sorted_off + q);
             int dm = __float_as_int(o.w) - mf;
@@ -181,21 +148,27 @@ __device__ __forceinline__ Sums32 lj_energy32(const Geometry& g, const Arrays& A
                 else if (dm < -1)
                     dm += (int)sf;
             }
-            r2n = fp32_dist2<DIM>(g, t32, o, s0, s1, dm);
-            r2o = fp32_dist2<DIM>(g, c32, o, s0, s1, dm);
+            const float r2n = fp32_dist2<DIM>(g, t32, o, s0, s1, dm);
+            const float r2o = fp32_dist2<DIM>(g, c32, o, s0, s1, dm);
             s.pairs += 2;
-            in_n = r2n < P.lj_rcut2_hi32;
-            in_o = r2o < P.lj_rcut2_hi32;
+            if (r2n < P.lj_rcut2_hi32) {
+                float e, err;
+                lj_pair32(P, r2n, e, err);
+                s.e_new += e;
+                s.err += err;
+                s.mag += fabsf(e);
+                s.terms += 1;
+            }
+            if (r2o < P.lj_rcut2_hi32) {
+                float e, err;
+                lj_pair32(P, r2o, e, err);
+                s.e_old += e;
+                s.err += err;
+                s.mag += fabsf(e);
+                s.terms += 1;
+            }
         }
-        const unsigned bn = __ballot_sync(full, in_n), bo = __ballot_sync(full, in_o);
-        const unsigned below = (1u << lane) - 1u;
-        if (in_n) buf[n_buf + __popc(bn & below)] = r2n;
-        if (in_o) buf[n_buf + __popc(bn) + __popc(bo & below)] = __int_as_float(__float_as_int(r2o) | (int)0x80000000);
-        n_buf += __popc(bn) + __popc(bo);
-        while (n_buf >= 32u) drain(32u);
     }
-    if (n_buf) drain(n_buf);
-    s.terms = my_terms;
     s.e_new = warp_sumf(s.e_new);
     s.e_old = warp_sumf(s.e_old);
     s.err = warp_sumf(s.err);
@@ -393,7 +366,6 @@ __global__ void __launch_bounds__(128, MINB) k_sweep_lj32(Geometry g, Arrays A, 
     __shared__ double s_e[kRecheckChunks][2][32];
     __shared__ SharedTrial s_trial;
     __shared__ uint32_t s_active;
-    __shared__ float s_r2[4][kLjBuf];
     const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
     uint32_t n_accepted = 0;
     PairStats pst;
@@ -444,7 +416,7 @@ __global__ void __launch_bounds__(128, MINB) k_sweep_lj32(Geometry g, Arrays A, 
         if (trial) {
             const float4 t32 = INJ ? cell_offsets<DIM>(g, t, m) : t32p;
             const float4 c32 = __ldg(A.sorted_off + k);
-            const Sums32 s = lj_energy32<DIM>(g, A, P, t32, c32, (int)m[DIM - 1], fs, k, lane, s_r2[wib]);
+            const Sums32 s = lj_energy32<DIM>(g, A, P, t32, c32, (int)m[DIM - 1], fs, k, lane);
             pst.checks += s.pairs;
             decision = decide32(s, L.kt, u);
             d32 = s.e_new - s.e_old;
@@ -614,7 +586,6 @@ __global__ void __launch_bounds__(128, HMC_LJ_BATCH_MIN_BLOCKS)
     __shared__ double s_e[kRecheckChunks][2][32];
     __shared__ SharedTrial s_trial;
     __shared__ uint32_t s_active, s_rep;
-    __shared__ float s_r2[4][kLjBuf];
     const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
     uint32_t n_accepted = 0;
     PairStats pst;
@@ -667,7 +638,7 @@ __global__ void __launch_bounds__(128, HMC_LJ_BATCH_MIN_BLOCKS)
             const Replica& R = B.rep[r];
             const float4 t32 = cell_offsets<DIM>(R.g, t, m);
             const float4 c32 = __ldg(A.sorted_off + k);
-            const Sums32 s = lj_energy32<DIM>(R.g, A, R.p, t32, c32, (int)m[DIM - 1], fs, k, lane, s_r2[wib]);
+            const Sums32 s = lj_energy32<DIM>(R.g, A, R.p, t32, c32, (int)m[DIM - 1], fs, k, lane);
             pst.checks += s.pairs;
             decision = decide32(s, R.kt, u);
             d32 = s.e_new - s.e_old;
@@ -765,7 +736,6 @@ template <int DIM, bool FP32>
 __global__ void __launch_bounds__(128) k_eval_lj(Geometry g, Arrays A, Pair P, const uint64_t* bodies,
                                                  const double4* trial, const double* uu, double kt, uint32_t n,
                                                  uint8_t* decisions, uint8_t* rechecked, double* delta_h) {
-    __shared__ float s_r2[4][kLjBuf];  // launched with 128 threads
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     PairStats pst;
@@ -798,8 +768,7 @@ __global__ void __launch_bounds__(128) k_eval_lj(Geometry g, Arrays A, Pair P, c
                 if (same) {
                     const float4 t32 = cell_offsets<DIM>(g, t, mt);
                     const float4 c32 = __ldg(A.sorted_off + k);
-                    const Sums32 s = lj_energy32<DIM>(g, A, P, t32, c32, (int)mt[DIM - 1], ft, k, lane,
-                                                      s_r2[threadIdx.x >> 5]);
+                    const Sums32 s = lj_energy32<DIM>(g, A, P, t32, c32, (int)mt[DIM - 1], ft, k, lane);
                     const float d32 = s.e_new - s.e_old;
                     const float b = s.err + (float)(s.terms + 7) * kU32 * s.mag * 1.01f + kU32 * fabsf(d32) +
                                     1e-9f * (s.mag + 1.f);
