@@ -79,7 +79,7 @@ def sphere_trials(pos, L, n_moves, seed, spread):
 
 
 @pytest.mark.parametrize("dim,n,phi,total,chunk", [(3, 32768, 0.50, 10_000_000, 1_000_000),
-                                                   (2, 4096, 0.70, 2_000_000, 500_000)])
+                                                   (2, 4096, 0.70, 10_000_000, 1_000_000)])
 def test_sphere_trials_through_the_colour_passes(ctx, dim, n, phi, total, chunk):
     pos0, L = lattice.hard_sphere_box(n, phi, dim, 0x5EED0015)
     h = PairwiseCutoff(HardSphere(1.0))
