@@ -972,8 +972,8 @@ hmc_status hmc_sweep(hmc_system* s, const hmc_sweep_params* p, hmc_count* out) {
                         HMC_CUDA(launch_sweep_poly3_soft(s->geom, s->arr, s->verts, s->n_vertices, s->so, L,
                                                          s->stream));
                     else if (s->shape_soft)
-                        HMC_CUDA(launch_sweep_poly2_soft(s->geom, s->arr, s->verts, s->n_vertices, s->so, L,
-                                                         s->stream));
+                        HMC_CUDA(launch_sweep_poly2_soft(s->sat(), s->geom, s->arr, s->verts, s->n_vertices, s->so,
+                                                         L, s->stream));
                     else if (s->interaction == HMC_HARD_CONVEX_POLYHEDRON)
                         HMC_CUDA(launch_sweep_poly(fp32, s->geom, s->arr, s->verts, s->n_vertices, s->poly_rcut2,
                                                    s->poly_rcut2_hi32, L, p->move == HMC_ROTATE, s->stream,
@@ -1520,8 +1520,8 @@ hmc_status hmc_total_energy(hmc_system* s, double* energy) {
             HMC_CUDA(launch_energy_poly3_soft(s->geom, s->arr, s->verts, s->n_vertices, s->so, (uint32_t)s->n, d,
                                               s->stream));
         else
-            HMC_CUDA(launch_energy_poly2_soft(s->geom, s->arr, s->verts, s->n_vertices, s->so, (uint32_t)s->n, d,
-                                              s->stream));
+            HMC_CUDA(launch_energy_poly2_soft(s->sat(), s->geom, s->arr, s->verts, s->n_vertices, s->so,
+                                              (uint32_t)s->n, d, s->stream));
         s->prof.kernel_launches += 1;
         if ((st = read_stats(s))) return st;
         if ((st = check_flags(s))) return st;
@@ -1609,8 +1609,8 @@ hmc_status hmc_set_shape_overlap(hmc_system* s, const hmc_shape_overlap_params* 
     }
     if (p->struct_size < sizeof(hmc_shape_overlap_params))
         return fail(HMC_INVALID_ARGUMENT, "hmc_shape_overlap_params.struct_size");
-    if (s->interaction != HMC_HARD_CONVEX_POLYHEDRON && s->interaction != HMC_HARD_CONVEX_POLYGON)
-        return fail(HMC_NOT_SUPPORTED, "the approximate shape overlap is for Convex polyhedra and polygons");
+    if (!s->oriented())
+        return fail(HMC_NOT_SUPPORTED, "the approximate shape overlap is for convex polyhedra and polygons");
     if (!(p->resolution > 0.0) || !std::isfinite(p->resolution))
         return fail(HMC_INVALID_ARGUMENT, "resolution must be positive");
     if (!(p->penalty_k >= 0.0) || !std::isfinite(p->penalty_k) || !(p->penalty_maximum_overlap >= 0.0) ||
@@ -1666,7 +1666,6 @@ hmc_status hmc_quick_insert_apply(hmc_system* s, hmc_quick_insert* qi, hmc_count
     if (s->interaction != HMC_HARD_SPHERE && !s->penalty() && !s->shape_soft)
         return fail(HMC_NOT_SUPPORTED, "QuickInsert places hard or overlap-penalty spheres, or convex shapes "
                                        "under the approximate shape overlap");
-    if (s->sat()) return fail(HMC_NOT_SUPPORTED, "the approximate shape overlap is for Convex polygons");
     if (qi->allowed_overlaps == 0) return fail(HMC_INVALID_ARGUMENT, "allowed_overlaps must be >= 1");
     if (qi->inserted > qi->target) return fail(HMC_INVALID_ARGUMENT, "inserted exceeds target");
     if (s->n + (qi->target - qi->inserted) > s->capacity)
@@ -1713,7 +1712,7 @@ hmc_status hmc_quick_insert_apply(hmc_system* s, hmc_quick_insert* qi, hmc_count
                                                s->serial_items, s->serial_cell_of, s->serial_site, s->qi_out,
                                                s->stream));
         else if (s->shape_soft)
-            HMC_CUDA(launch_quick_insert_poly2(s->geom, s->arr, s->verts, s->n_vertices, s->so, L, q, tags,
+            HMC_CUDA(launch_quick_insert_poly2(s->sat(), s->geom, s->arr, s->verts, s->n_vertices, s->so, L, q, tags,
                                                s->serial_nc, s->serial_w, s->serial_cap, s->serial_size,
                                                s->serial_items, s->serial_cell_of, s->serial_site, s->qi_out,
                                                s->stream));

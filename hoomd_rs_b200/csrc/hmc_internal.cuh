@@ -408,13 +408,13 @@ struct ShapeOverlap {
 // launch_propose_poly / launch_propose_poly2 with soft = true).
 cudaError_t launch_sweep_poly3_soft(const Geometry& g, const Arrays& a, const double4* verts, uint32_t nv,
                                     const ShapeOverlap& so, const Launch& l, cudaStream_t s);
-cudaError_t launch_sweep_poly2_soft(const Geometry& g, const Arrays& a, const double4* verts, uint32_t nv,
+cudaError_t launch_sweep_poly2_soft(bool sat, const Geometry& g, const Arrays& a, const double4* verts, uint32_t nv,
                                     const ShapeOverlap& so, const Launch& l, cudaStream_t s);
 // PairwiseCutoff::total_energy under ShapeOverlap (pairs i < j in body order, i's frame), summed
 // into *out with atomics.
 cudaError_t launch_energy_poly3_soft(const Geometry& g, const Arrays& a, const double4* verts, uint32_t nv,
                                      const ShapeOverlap& so, uint32_t n, double* out, cudaStream_t s);
-cudaError_t launch_energy_poly2_soft(const Geometry& g, const Arrays& a, const double4* verts, uint32_t nv,
+cudaError_t launch_energy_poly2_soft(bool sat, const Geometry& g, const Arrays& a, const double4* verts, uint32_t nv,
                                      const ShapeOverlap& so, uint32_t n, double* out, cudaStream_t s);
 // delta_energy_one in FP64 for injected trial positions (LJ); u < 0 means no decision needed.
 cudaError_t launch_eval_lj(int dim, bool fp32, const Geometry& g, const Arrays& a, const Pair& p,
@@ -503,7 +503,7 @@ cudaError_t launch_quick_insert_poly3(const Geometry& g, const Arrays& a, const 
                                       const BodyTags& tags, const uint32_t* nc, const double* w, uint32_t cap,
                                       uint32_t* size, uint32_t* items, uint32_t* cell_of, double4* site,
                                       unsigned long long* out, cudaStream_t s);
-cudaError_t launch_quick_insert_poly2(const Geometry& g, const Arrays& a, const double4* verts, uint32_t nv,
+cudaError_t launch_quick_insert_poly2(bool sat, const Geometry& g, const Arrays& a, const double4* verts, uint32_t nv,
                                       const ShapeOverlap& so, const Launch& l, const QuickInsertArgs& q,
                                       const BodyTags& tags, const uint32_t* nc, const double* w, uint32_t cap,
                                       uint32_t* size, uint32_t* items, uint32_t* cell_of, double4* site,

@@ -381,6 +381,9 @@ __global__ void __launch_bounds__(128, HMC_POLY2_MIN_BLOCKS)
 // while Convex::intersects_at (convex.rs:87-99: the bounding circles, |w|^2 <= (R + R)^2, then
 // XenoCollide) holds at w = v + direction * d; the energy is OverlapPenalty(-d). An angle beyond
 // cr_sincos's range sets *range_error and counts as infinite.
+// SAT: ConvexSurfaceMesh2d, whose intersects_at (convex_surface_mesh_2d.rs:538-595) is the
+// separating-axis test alone, without the bounding circles.
+template <bool SAT>
 __device__ __forceinline__ double shape_overlap2(const Geometry& g, const PolyShape2& sh, const ShapeOverlap& so,
                                                  const double* t, double ti, const double* sj, double tj,
                                                  uint32_t& capped, bool* range_error) {
@@ -401,7 +404,8 @@ __device__ __forceinline__ double shape_overlap2(const Geometry& g, const PolySh
     double sep = 0.0;
     for (uint32_t step = 0;; ++step) {
         const V2 w{dadd(v.x, dmul(dir.x, sep)), dadd(v.y, dmul(dir.y, sep))};
-        if (!(dot2(w, w) <= so.rr) || !collide2d(sh.verts, sh.nv, w, m)) break;
+        if (SAT ? !sat_intersects(sh.verts, sh.nv, w, m) : (!(dot2(w, w) <= so.rr) || !collide2d(sh.verts, sh.nv, w, m)))
+            break;
         if (step >= so.max_steps) {
             capped = 1;
             break;
@@ -414,6 +418,7 @@ __device__ __forceinline__ double shape_overlap2(const Geometry& g, const PolySh
 // ParallelSweep colour pass of convex polygons under the approximate shape overlap (FP64), one
 // warp per trial from k_propose_poly2 (soft: the uniform in trial_t.z, the angle in .w); the
 // sums and the Metropolis test as in k_sweep_poly3_soft.
+template <bool SAT>
 __global__ void __launch_bounds__(128) k_sweep_poly2_soft(Geometry g, Arrays A, PolyShape2 sh, ShapeOverlap so,
                                                           Launch L) {
     if (L.early_wait) grid_dependency_wait();  // first pass: the rebuild's arrays are read at once
@@ -449,8 +454,8 @@ __global__ void __launch_bounds__(128) k_sweep_poly2_soft(Geometry g, Arrays A, 
                 const double4 c4 = ldg4(A.sorted_s + q);
                 const double sj[3] = {c4.x, c4.y, 0.0};
                 const double tj = __ldg(&A.sorted_q[q].x);
-                const double x = shape_overlap2(g, sh, so, t, tt, sj, tj, capped, &range_error);
-                const double y = shape_overlap2(g, sh, so, si, tk, sj, tj, capped, &range_error);
+                const double x = shape_overlap2<SAT>(g, sh, so, t, tt, sj, tj, capped, &range_error);
+                const double y = shape_overlap2<SAT>(g, sh, so, si, tk, sj, tj, capped, &range_error);
                 a = dadd(a, x);
                 b = dadd(b, y);
                 mag += fabs(x) + fabs(y);
@@ -485,6 +490,7 @@ __global__ void __launch_bounds__(128) k_sweep_poly2_soft(Geometry g, Arrays A, 
 
 // PairwiseCutoff::total_energy under the approximate shape overlap for polygons (as
 // k_energy_poly3_soft).
+template <bool SAT>
 __global__ void k_energy_poly2_soft(Geometry g, Arrays A, PolyShape2 sh, ShapeOverlap so, uint32_t n, double* out) {
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t capped = 0;
@@ -505,7 +511,7 @@ __global__ void k_energy_poly2_soft(Geometry g, Arrays A, PolyShape2 sh, ShapeOv
             if (A.sorted_body[q] <= bi) return false;
             const double4 c4 = A.sorted_s[q];
             const double sj[3] = {c4.x, c4.y, 0.0};
-            e = dadd(e, shape_overlap2(g, sh, so, t, ti, sj, A.sorted_q[q].x, capped, &range_error));
+            e = dadd(e, shape_overlap2<SAT>(g, sh, so, t, ti, sj, A.sorted_q[q].x, capped, &range_error));
             return false;
         });
         atomicAdd(out, e);
@@ -516,6 +522,7 @@ __global__ void k_energy_poly2_soft(Geometry g, Arrays A, PolyShape2 sh, ShapeOv
 
 // QuickInsert's insertion loop for convex polygons under the approximate shape overlap, one warp
 // (k_quick_insert_poly3 with the angle drawn from Uniform::new(0, 2 pi), angle.rs:268-285).
+template <bool SAT>
 __global__ void __launch_bounds__(32) k_quick_insert_poly2(Geometry g, Arrays A, SerialGrid G, PolyShape2 sh,
                                                            ShapeOverlap so, Launch L, QuickInsertArgs q, BodyTags T,
                                                            unsigned long long* out) {
@@ -546,7 +553,7 @@ __global__ void __launch_bounds__(32) k_quick_insert_poly2(Geometry g, Arrays A,
                 const uint32_t j = G.items[(size_t)cell * G.cap + kk];
                 const double4 s4 = G.site[j];
                 const double sv[3] = {s4.x, s4.y, 0.0};
-                const double e = shape_overlap2(g, sh, so, t, o, sv, A.body_ori[j].x, capped, &range_error);
+                const double e = shape_overlap2<SAT>(g, sh, so, t, o, sv, A.body_ori[j].x, capped, &range_error);
                 inf = e == __longlong_as_double(0x7ff0000000000000ll);
                 pos = pos || e > 0.0;
             }
@@ -848,26 +855,31 @@ cudaError_t launch_propose_poly2(bool fp32, const Geometry& g, const Arrays& a, 
     return cudaGetLastError();
 }
 
-cudaError_t launch_sweep_poly2_soft(const Geometry& g, const Arrays& a, const double4* verts, uint32_t nv,
+cudaError_t launch_sweep_poly2_soft(bool sat, const Geometry& g, const Arrays& a, const double4* verts, uint32_t nv,
                                     const ShapeOverlap& so, const Launch& l, cudaStream_t s) {
     if (l.n_active == 0) return cudaSuccess;
     PolyShape2 sh{verts, nv, so.rr, 0.f};
-    const int wave = resident_wave((const void*)k_sweep_poly2_soft);
+    using SoftKernel = void (*)(Geometry, Arrays, PolyShape2, ShapeOverlap, Launch);
+    const SoftKernel k = sat ? k_sweep_poly2_soft<true> : k_sweep_poly2_soft<false>;
+    const int wave = resident_wave((const void*)k);
     uint32_t blocks = (l.n_active + 3) / 4;  // four warps (trials) per block
     if (blocks > (uint32_t)wave) blocks = (uint32_t)wave;
     PassLaunch pl(blocks, l.overlap_previous != 0 || l.early_wait != 0, s);
-    return cudaLaunchKernelEx(&pl.cfg, k_sweep_poly2_soft, g, a, sh, so, l);
+    return cudaLaunchKernelEx(&pl.cfg, k, g, a, sh, so, l);
 }
 
-cudaError_t launch_energy_poly2_soft(const Geometry& g, const Arrays& a, const double4* verts, uint32_t nv,
+cudaError_t launch_energy_poly2_soft(bool sat, const Geometry& g, const Arrays& a, const double4* verts, uint32_t nv,
                                      const ShapeOverlap& so, uint32_t n, double* out, cudaStream_t s) {
     if (n == 0) return cudaSuccess;
     PolyShape2 sh{verts, nv, so.rr, 0.f};
-    k_energy_poly2_soft<<<(n + 127) / 128, 128, 0, s>>>(g, a, sh, so, n, out);
+    if (sat)
+        k_energy_poly2_soft<true><<<(n + 127) / 128, 128, 0, s>>>(g, a, sh, so, n, out);
+    else
+        k_energy_poly2_soft<false><<<(n + 127) / 128, 128, 0, s>>>(g, a, sh, so, n, out);
     return cudaGetLastError();
 }
 
-cudaError_t launch_quick_insert_poly2(const Geometry& g, const Arrays& a, const double4* verts, uint32_t nv,
+cudaError_t launch_quick_insert_poly2(bool sat, const Geometry& g, const Arrays& a, const double4* verts, uint32_t nv,
                                       const ShapeOverlap& so, const Launch& l, const QuickInsertArgs& q,
                                       const BodyTags& tags, const uint32_t* nc, const double* w, uint32_t cap,
                                       uint32_t* size, uint32_t* items, uint32_t* cell_of, double4* site,
@@ -876,7 +888,10 @@ cudaError_t launch_quick_insert_poly2(const Geometry& g, const Arrays& a, const 
     cudaError_t e = build_grid(2, g, a, G, q.n0, s);
     if (e != cudaSuccess) return e;
     PolyShape2 sh{verts, nv, so.rr, 0.f};
-    k_quick_insert_poly2<<<1, 32, 0, s>>>(g, a, G, sh, so, l, q, tags, out);
+    if (sat)
+        k_quick_insert_poly2<true><<<1, 32, 0, s>>>(g, a, G, sh, so, l, q, tags, out);
+    else
+        k_quick_insert_poly2<false><<<1, 32, 0, s>>>(g, a, G, sh, so, l, q, tags, out);
     return cudaGetLastError();
 }
 

@@ -475,7 +475,8 @@ hmc_status hmc_get_n_bodies(hmc_system* sys, uint64_t* n_bodies);
  * precision modes; translation or rotation), hmc_quick_insert_apply (each UniformIn body also draws
  * a uniform random orientation), hmc_quick_compress_apply and hmc_total_energy;
  * hmc_set_shape_overlap(sys, NULL) returns to HardShape. Convex polyhedra and polygons
- * (HMC_HARD_CONVEX_POLYHEDRON, HMC_HARD_CONVEX_POLYGON) only; r_cut (0 = 2 x the bounding radius)
+ * (HMC_HARD_CONVEX_POLYHEDRON, HMC_HARD_CONVEX_POLYGON: the bounding spheres, then XenoCollide;
+ * HMC_HARD_CONVEX_SURFACE_MESH_2D: the separating-axis test alone); r_cut (0 = 2 x the bounding radius)
  * must not exceed 2 x the bounding radius. The serial sweep, the tuner, the autotuner and the
  * injected-move entry points return HMC_NOT_SUPPORTED while it is set. */
 typedef struct hmc_shape_overlap_params {

@@ -25,6 +25,7 @@ OVERLAP_PENALTY = 5
 CONVEX_POLYHEDRON_PENALTY = 6  # Anisotropic { ApproximateShapeOverlap { Convex(ConvexPolyhedron), OverlapPenalty } }
 CONVEX_POLYGON_PENALTY = 7     # the same with Convex(ConvexPolygon)
 ISOTROPIC = 8                  # Isotropic { W(F), r_cut }: F and W below
+SURFACE_MESH_2D_PENALTY = 9    # ApproximateShapeOverlap with ConvexSurfaceMesh2d (separating axes)
 UV_LENNARD_JONES, UV_WEEKS_CHANDLER_ANDERSON, UV_HARMONIC, UV_HARMONIC_REPULSION, UV_BOXCAR, UV_OVERLAP_PENALTY = range(6)
 UVW_NONE, UVW_SHIFTED, UVW_EXPANDED, UVW_XPLOR = range(4)
 TRANSLATE = 0
@@ -101,7 +102,7 @@ def lib():
         L.oracle_set_isotropic.argtypes = [C.c_void_p, C.c_uint32, _dp, C.c_uint32, _dp, C.c_double]
         L.oracle_univariate_energy.argtypes = [C.c_uint32, _dp, C.c_uint32, _dp, C.c_double]
         L.oracle_univariate_energy.restype = C.c_double
-        L.oracle_approximate_separation.argtypes = [C.c_uint32, _dp, C.c_uint32, _dp, _dp, C.c_double]
+        L.oracle_approximate_separation.argtypes = [C.c_uint32, _dp, C.c_uint32, _dp, _dp, C.c_double, C.c_uint32]
         L.oracle_approximate_separation.restype = C.c_double
         L.oracle_n_bodies.argtypes = [C.c_void_p]
         L.oracle_n_bodies.restype = C.c_uint64
@@ -284,13 +285,13 @@ def surface_mesh_intersects_at_2d(verts_a, verts_b, v_ij, theta) -> bool:
     return bool(lib().oracle_surface_mesh_intersects_at_2d(_d(a), a.shape[0], _d(b), b.shape[0], _d(v), theta))
 
 
-def approximate_separation(vertices, v_ij, o_ij, resolution) -> float:
+def approximate_separation(vertices, v_ij, o_ij, resolution, sat=False) -> float:
     """IntersectsAt::approximate_separation_distance of two equal convex polytopes; o_ij is a versor
-    (s, x, y, z) in 3-D or an angle in 2-D."""
+    (s, x, y, z) in 3-D or an angle in 2-D; sat: ConvexSurfaceMesh2d polygons."""
     verts = _f64(vertices)
     dim = verts.shape[1]
     return float(lib().oracle_approximate_separation(dim, _d(verts), verts.shape[0], _d(_f64(v_ij)),
-                                                     _d(_f64(np.atleast_1d(o_ij))), resolution))
+                                                     _d(_f64(np.atleast_1d(o_ij))), resolution, int(sat)))
 
 
 def _params(p, n):
@@ -381,9 +382,9 @@ class System:
             lib().oracle_set_isotropic(self._h, isotropic["kind"], _d(_params(isotropic["params"], 4)),
                                        isotropic.get("wrap", UVW_NONE), _d(_params(isotropic.get("wrap_params", ()), 2)),
                                        isotropic["r_cut"])
-        if interaction in (OVERLAP_PENALTY, CONVEX_POLYHEDRON_PENALTY, CONVEX_POLYGON_PENALTY):
+        if interaction in (OVERLAP_PENALTY, CONVEX_POLYHEDRON_PENALTY, CONVEX_POLYGON_PENALTY, SURFACE_MESH_2D_PENALTY):
             lib().oracle_set_penalty(self._h, *penalty)
-        if interaction in (CONVEX_POLYHEDRON_PENALTY, CONVEX_POLYGON_PENALTY):
+        if interaction in (CONVEX_POLYHEDRON_PENALTY, CONVEX_POLYGON_PENALTY, SURFACE_MESH_2D_PENALTY):
             lib().oracle_set_shape_overlap(self._h, resolution, boundary_range if r_cut is None else r_cut)
 
     def __del__(self):

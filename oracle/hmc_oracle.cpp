@@ -697,69 +697,6 @@ bool convex_global_2d(const Polytope& p, const double* ri, double ti, const doub
     return collide2d(p, p, vij, m);
 }
 
-// IntersectsAt::approximate_separation_distance (hoomd-geometry/src/lib.rs:307-325) for two equal
-// Convex polytopes in the local frame of the first: direction = v.to_unit() (lib.rs:632-639,
-// norm = sqrt(fma dot)), else the default unit (last axis, cartesian.rs:313-318); d grows by
-// `resolution` while Convex::intersects_at (convex.rs:87-99, :130-143) holds at v + direction * d:
-// the bounding spheres |w|^2 <= (R + R)^2 (sphere.rs:262-264), then XenoCollide.
-template <int N, class Q>
-double approximate_separation(const Polytope& p, const double* v, const Q& q, double resolution) {
-    double dir[N];
-    const double norm = std::sqrt(dot(v, v, N));
-    if (norm == 0.0) {
-        for (int a = 0; a < N; ++a) dir[a] = a == N - 1 ? 1.0 : 0.0;
-    } else {
-        for (int a = 0; a < N; ++a) dir[a] = v[a] / norm;
-    }
-    const double rr = (p.bounding_radius + p.bounding_radius) * (p.bounding_radius + p.bounding_radius);
-    double d = 0.0;
-    for (;;) {
-        double w[N];
-        for (int a = 0; a < N; ++a) w[a] = v[a] + dir[a] * d;
-        if (!(dot(w, w, N) <= rr)) break;
-        bool hit;
-        if constexpr (N == 3)
-            hit = collide3d(p, p, w, q);
-        else
-            hit = collide2d(p, p, w, q);
-        if (!hit) break;
-        d = d + resolution;
-    }
-    return d;
-}
-// OverlapPenalty::energy (overlap_penalty.rs:109-115): inf below -d_max, (0.5 k) r^2 + eps below 0.
-double overlap_penalty(double k, double dmax, double shoulder, double r) {
-    if (r < -dmax) return INFINITY;
-    if (r < 0.0) return 0.5 * k * (r * r) + shoulder;
-    return 0.0;
-}
-// Anisotropic::site_pair_energy (anisotropic.rs:120-135) of ApproximateShapeOverlap<OverlapPenalty,
-// Convex<ConvexPolyhedron>> (approximate_shape_overlap.rs:122-131): |r_j - r_i| >= r_cut -> 0, else
-// pair_system_to_local (hoomd-vector/src/lib.rs:878-888) and OverlapPenalty(-separation).
-double shape_penalty_3d(const Polytope& p, double rcut, double res, double k, double dmax, double shoulder,
-                        const double* ri, const Quat& qi, const double* rj, const Quat& qj) {
-    if (std::sqrt(distance_squared(ri, rj, 3)) >= rcut) return 0.0;
-    double rab[3] = {rj[0] - ri[0], rj[1] - ri[1], rj[2] - ri[2]};
-    const Quat qa_inv = qconj(qi);
-    const V3 vij = versor_rotate(qa_inv, rab);
-    const Quat oij = qmul(qa_inv, qj);
-    const Mat3 m = mat_from_versor(oij);
-    return overlap_penalty(k, dmax, shoulder, -approximate_separation<3>(p, vij.v, m, res));
-}
-// The same for Convex<ConvexPolygon> with Angle orientations (angle.rs:175-181, :212, :229).
-double shape_penalty_2d(const Polytope& p, double rcut, double res, double k, double dmax, double shoulder,
-                        const double* ri, double ti, const double* rj, double tj) {
-    if (std::sqrt(distance_squared(ri, rj, 2)) >= rcut) return 0.0;
-    double rab[2] = {rj[0] - ri[0], rj[1] - ri[1]};
-    const double inv = -ti;
-    double s, c;
-    cr_sincos(inv, &s, &c);
-    double vij[2] = {rab[0] * c - rab[1] * s, rab[0] * s + rab[1] * c};
-    double m[2][2];
-    mat2_from_angle(inv + tj, m);
-    return overlap_penalty(k, dmax, shoulder, -approximate_separation<2>(p, vij, m, res));
-}
-
 // ConvexSurfaceMesh2d separating-axis test (convex_surface_mesh_2d.rs:578-640): a and b
 // hold counter-clockwise hull vertices; o_b rotates b into a's frame.
 static void mat2_rotate(const double (&m)[2][2], const double* v, double* out) {  // rows dot v
@@ -809,6 +746,75 @@ bool sat_global_2d(const Polytope& p, const double* ri, double ti, const double*
     double m[2][2];
     mat2_from_angle(inv + tj, m);
     return sat_intersects_at(p, p, vij, m);
+}
+
+// IntersectsAt::approximate_separation_distance (hoomd-geometry/src/lib.rs:307-325) for two equal
+// Convex polytopes in the local frame of the first: direction = v.to_unit() (lib.rs:632-639,
+// norm = sqrt(fma dot)), else the default unit (last axis, cartesian.rs:313-318); d grows by
+// `resolution` while Convex::intersects_at (convex.rs:87-99, :130-143) holds at v + direction * d:
+// the bounding spheres |w|^2 <= (R + R)^2 (sphere.rs:262-264), then XenoCollide.
+// SAT: ConvexSurfaceMesh2d, whose intersects_at (convex_surface_mesh_2d.rs:538-595) is the
+// separating-axis test alone, without the bounding circles.
+template <int N, class Q, bool SAT = false>
+double approximate_separation(const Polytope& p, const double* v, const Q& q, double resolution) {
+    double dir[N];
+    const double norm = std::sqrt(dot(v, v, N));
+    if (norm == 0.0) {
+        for (int a = 0; a < N; ++a) dir[a] = a == N - 1 ? 1.0 : 0.0;
+    } else {
+        for (int a = 0; a < N; ++a) dir[a] = v[a] / norm;
+    }
+    const double rr = (p.bounding_radius + p.bounding_radius) * (p.bounding_radius + p.bounding_radius);
+    double d = 0.0;
+    for (;;) {
+        double w[N];
+        for (int a = 0; a < N; ++a) w[a] = v[a] + dir[a] * d;
+        if (!SAT && !(dot(w, w, N) <= rr)) break;
+        bool hit;
+        if constexpr (N == 3)
+            hit = collide3d(p, p, w, q);
+        else if constexpr (SAT)
+            hit = sat_intersects_at(p, p, w, q);
+        else
+            hit = collide2d(p, p, w, q);
+        if (!hit) break;
+        d = d + resolution;
+    }
+    return d;
+}
+// OverlapPenalty::energy (overlap_penalty.rs:109-115): inf below -d_max, (0.5 k) r^2 + eps below 0.
+double overlap_penalty(double k, double dmax, double shoulder, double r) {
+    if (r < -dmax) return INFINITY;
+    if (r < 0.0) return 0.5 * k * (r * r) + shoulder;
+    return 0.0;
+}
+// Anisotropic::site_pair_energy (anisotropic.rs:120-135) of ApproximateShapeOverlap<OverlapPenalty,
+// Convex<ConvexPolyhedron>> (approximate_shape_overlap.rs:122-131): |r_j - r_i| >= r_cut -> 0, else
+// pair_system_to_local (hoomd-vector/src/lib.rs:878-888) and OverlapPenalty(-separation).
+double shape_penalty_3d(const Polytope& p, double rcut, double res, double k, double dmax, double shoulder,
+                        const double* ri, const Quat& qi, const double* rj, const Quat& qj) {
+    if (std::sqrt(distance_squared(ri, rj, 3)) >= rcut) return 0.0;
+    double rab[3] = {rj[0] - ri[0], rj[1] - ri[1], rj[2] - ri[2]};
+    const Quat qa_inv = qconj(qi);
+    const V3 vij = versor_rotate(qa_inv, rab);
+    const Quat oij = qmul(qa_inv, qj);
+    const Mat3 m = mat_from_versor(oij);
+    return overlap_penalty(k, dmax, shoulder, -approximate_separation<3>(p, vij.v, m, res));
+}
+// The same for Convex<ConvexPolygon> (SAT: ConvexSurfaceMesh2d) with Angle orientations
+// (angle.rs:175-181, :212, :229).
+template <bool SAT = false>
+double shape_penalty_2d(const Polytope& p, double rcut, double res, double k, double dmax, double shoulder,
+                        const double* ri, double ti, const double* rj, double tj) {
+    if (std::sqrt(distance_squared(ri, rj, 2)) >= rcut) return 0.0;
+    double rab[2] = {rj[0] - ri[0], rj[1] - ri[1]};
+    const double inv = -ti;
+    double s, c;
+    cr_sincos(inv, &s, &c);
+    double vij[2] = {rab[0] * c - rab[1] * s, rab[0] * s + rab[1] * c};
+    double m[2][2];
+    mat2_from_angle(inv + tj, m);
+    return overlap_penalty(k, dmax, shoulder, -approximate_separation<2, double[2][2], SAT>(p, vij, m, res));
 }
 
 // ============================================================================
@@ -1182,7 +1188,8 @@ struct oracle_system {
     }
 
     bool shape_penalty() const {
-        return interaction == ORACLE_CONVEX_POLYHEDRON_PENALTY || interaction == ORACLE_CONVEX_POLYGON_PENALTY;
+        return interaction == ORACLE_CONVEX_POLYHEDRON_PENALTY || interaction == ORACLE_CONVEX_POLYGON_PENALTY ||
+               interaction == ORACLE_SURFACE_MESH_2D_PENALTY;
     }
     bool hard() const {
         return interaction != ORACLE_LENNARD_JONES && interaction != ORACLE_OVERLAP_PENALTY &&
@@ -1282,6 +1289,8 @@ struct oracle_system {
             }
             case ORACLE_CONVEX_POLYGON_PENALTY:
                 return shape_penalty_2d(poly, prcut, presolution, pk, pdmax, pshoulder, x, o[0], y, orient[j]);
+            case ORACLE_SURFACE_MESH_2D_PENALTY:
+                return shape_penalty_2d<true>(poly, prcut, presolution, pk, pdmax, pshoulder, x, o[0], y, orient[j]);
             case ORACLE_ISOTROPIC:
                 return uv.pair(distance_squared(x, y, dim));
             case ORACLE_OVERLAP_PENALTY: {
@@ -1458,12 +1467,13 @@ void oracle_set_shape_overlap(oracle_system* s, double resolution, double r_cut)
     s->build_grid();
 }
 double oracle_approximate_separation(uint32_t dim, const double* vertices, uint32_t n_vertices, const double* v_ij,
-                                     const double* o_ij, double resolution) {
+                                     const double* o_ij, double resolution, uint32_t sat) {
     const Polytope p = make_poly(vertices, n_vertices, (int)dim);
     if (dim == 3) return approximate_separation<3>(p, v_ij, mat_from_versor(Quat{o_ij[0], o_ij[1], o_ij[2], o_ij[3]}),
                                                    resolution);
     double m[2][2];
     mat2_from_angle(o_ij[0], m);
+    if (sat) return approximate_separation<2, double[2][2], true>(p, v_ij, m, resolution);
     return approximate_separation<2>(p, v_ij, m, resolution);
 }
 uint64_t oracle_n_bodies(const oracle_system* s) { return s->n; }

@@ -82,7 +82,8 @@ double oracle_shifted_lj_pair(double epsilon, double sigma, double r_cut, double
 // ---- systems --------------------------------------------------------------------
 enum { ORACLE_HARD_SPHERE = 0, ORACLE_HARD_CONVEX_POLYGON = 1, ORACLE_HARD_CONVEX_POLYHEDRON = 2,
        ORACLE_LENNARD_JONES = 3, ORACLE_HARD_CONVEX_SURFACE_MESH_2D = 4, ORACLE_OVERLAP_PENALTY = 5,
-       ORACLE_CONVEX_POLYHEDRON_PENALTY = 6, ORACLE_CONVEX_POLYGON_PENALTY = 7, ORACLE_ISOTROPIC = 8 };
+       ORACLE_CONVEX_POLYHEDRON_PENALTY = 6, ORACLE_CONVEX_POLYGON_PENALTY = 7, ORACLE_ISOTROPIC = 8,
+       ORACLE_SURFACE_MESH_2D_PENALTY = 9 };
 enum { ORACLE_TRANSLATE = 0, ORACLE_ROTATE = 1 };
 
 typedef struct oracle_system oracle_system;
@@ -102,8 +103,8 @@ void oracle_set_counter(oracle_system* s, uint64_t step, uint32_t substep);
 // Isotropic<Expanded<OverlapPenalty>> parameters (interaction ORACLE_OVERLAP_PENALTY; the
 // diameter is delta and r_cut).
 void oracle_set_penalty(oracle_system* s, double k, double maximum_allowed_overlap, double epsilon_shoulder);
-// Anisotropic { ApproximateShapeOverlap { Convex(shape), OverlapPenalty, resolution }, r_cut }
-// (interactions ORACLE_CONVEX_POLYHEDRON_PENALTY and ORACLE_CONVEX_POLYGON_PENALTY; the penalty's
+// Anisotropic { ApproximateShapeOverlap { shape, OverlapPenalty, resolution }, r_cut } (interactions
+// ORACLE_CONVEX_POLYHEDRON_PENALTY, ORACLE_CONVEX_POLYGON_PENALTY, ORACLE_SURFACE_MESH_2D_PENALTY; the penalty's
 // parameters come from oracle_set_penalty). r_cut is also the checkerboard's search range.
 void oracle_set_shape_overlap(oracle_system* s, double resolution, double r_cut);
 // Isotropic { W(F), r_cut } (interaction ORACLE_ISOTROPIC): F = kind (0 LennardJones {eps, sigma},
@@ -116,9 +117,10 @@ void oracle_set_isotropic(oracle_system* s, uint32_t kind, const double* params,
 double oracle_univariate_energy(uint32_t kind, const double* params, uint32_t wrap, const double* wrap_params,
                                 double r);
 // IntersectsAt::approximate_separation_distance of two equal convex polytopes (n_vertices x dim
-// vertices): v_ij in the first shape's frame, o_ij a versor (s, x, y, z) or an angle.
+// vertices): v_ij in the first shape's frame, o_ij a versor (s, x, y, z) or an angle; sat: the
+// polygons are ConvexSurfaceMesh2d (the separating-axis test) instead of Convex (XenoCollide).
 double oracle_approximate_separation(uint32_t dim, const double* vertices, uint32_t n_vertices, const double* v_ij,
-                                     const double* o_ij, double resolution);
+                                     const double* o_ij, double resolution, uint32_t sat);
 uint64_t oracle_n_bodies(const oracle_system* s);
 void oracle_get_box(const oracle_system* s, double* edge_lengths);
 // Microstate::clone_with_boundary onto a new box; 0 on success, -1 if a body is outside the box.

@@ -185,10 +185,80 @@ def test_entry_points_and_errors(ctx):
                                                                   1e-9), math.sqrt(3.0)))
     with pytest.raises(HmcError):
         g.set_hamiltonian(fine)
-    # separating-axis polygons have no approximate shape overlap
-    sq = np.array([[-0.5, -0.5], [0.5, -0.5], [0.5, 0.5], [-0.5, 0.5]])
-    mesh = ConvexSurfaceMesh2d.from_point_set(sq)
-    m = Microstate(ctx, Periodic(math.sqrt(2.0), [6.0, 6.0]), [[0.0, 0.0]], PairwiseCutoff(HardShape(mesh)))
+    # the shape of the insertion hamiltonian must be the system's own
+    other = ConvexPolyhedron.with_vertices(1.1 * CUBE)
     with pytest.raises(HmcError):
-        m.set_hamiltonian(PairwiseCutoff(Anisotropic(ApproximateShapeOverlap.new(mesh, OverlapPenalty(), 0.01),
-                                                     math.sqrt(2.0))))
+        g.set_hamiltonian(PairwiseCutoff(Anisotropic(ApproximateShapeOverlap.new(other, OverlapPenalty(), 0.01),
+                                                     math.sqrt(3.0))))
+
+
+def hexagon_mesh():
+    return ConvexSurfaceMesh2d.from_point_set(ConvexPolygon.regular(6).vertices)
+
+
+def test_mesh_pair_energies_equal_the_oracle(ctx):
+    # ConvexSurfaceMesh2d: the separating-axis test without bounding circles in intersects_at
+    mesh = hexagon_mesh()
+    hard, soft = hamiltonians(mesh)
+    r_cut = hard.maximum_interaction_range
+    rng = np.random.default_rng(5)
+    for _ in range(60):
+        d = rng.normal(size=2)
+        d *= rng.uniform(0.3, 1.05) / np.linalg.norm(d)
+        th = rng.uniform(0.0, 2.0 * math.pi, 2)
+        pos = [[0.0, 0.0], list(d)]
+        g = Microstate(ctx, Periodic(r_cut, [8.0, 8.0]), pos, hard, orientations=th)
+        g.set_hamiltonian(soft)
+        o = oracle.System(2, [8.0, 8.0], pos, th, interaction=oracle.SURFACE_MESH_2D_PENALTY, vertices=mesh.vertices,
+                          r_cut=r_cut)
+        assert g.total_energy() == o.total_energy()
+        g.close()
+
+
+def test_mesh_placement_loop_bit_identical(ctx):
+    mesh = hexagon_mesh()
+    n, rho = 24, 0.9
+    hard, soft = hamiltonians(mesh)
+    L0 = (n / (0.5 * rho)) ** 0.5
+    r = hard.maximum_interaction_range
+    g = Microstate(ctx, Periodic(r, [L0, L0]), np.zeros((0, 2)), hard, seed=0x5EED0042, capacity=n)
+    g.set_hamiltonian(soft)
+    o = oracle.System(2, [L0, L0], np.zeros((0, 2)), np.zeros(0), seed=0x5EED0042,
+                      interaction=oracle.SURFACE_MESH_2D_PENALTY, vertices=mesh.vertices)
+    qi, qc = QuickInsert.new(n), QuickCompress.with_target_volume(n / rho)
+    oqi = {"target": n, "allowed_overlaps": max(n // 8, 1), "inserted": 0, "complete": 0}
+    oqc = {"target_volume": n / rho, "maximum_energy_per_site": 1000.0, "maximum_delta": 0.05, "state": 0,
+           "is_final": 0, "boundary": [0.0, 0.0, 0.0]}
+    for step in range(20000):
+        if qc.is_complete():
+            break
+        if step % 10 == 0:
+            if qi.is_complete():
+                qc.apply(g)
+                o.quick_compress(oqc)
+            else:
+                qi.apply(g)
+                o.quick_insert(oqi)
+        for mv, omv, m in ((TRANSLATE, oracle.TRANSLATE, 0.03), (ROTATE, oracle.ROTATE, 0.1)):
+            c = g.sweep(mv, m, 1.0, FP64)
+            a, rj = o.parallel_sweep(omv, m, 1.0, o.boundary_range)
+            assert c.order_ambiguous == 0
+            assert (c.accepted, c.rejected) == (a, rj), step
+        g.increment_step()
+        o.increment_step()
+    assert qc.is_complete() and oqc["state"] == 3
+    same_state(g, o)
+    g.set_hamiltonian(hard)
+    assert g.overlap_count() == 0
+
+
+def test_place_hexagons_benchmark_density(ctx):
+    # benchmarks/src/mc/regular_polygon.rs:187-244: ConvexSurfaceMesh2d hexagons placed at packing
+    # fraction 0.68 under the approximate shape overlap (1024 here); no hard overlap after
+    mesh = hexagon_mesh()
+    hard, soft = hamiltonians(mesh)
+    area = 1.5 * math.sqrt(3.0) * 0.25  # regular hexagon of circumradius 0.5
+    n = 1024
+    g = place_single_site_orientable_bodies(ctx, n, 0.68 / area, hard.maximum_interaction_range, soft, hard, 2,
+                                            seed=12)
+    assert g.n == n and g.overlap_count() == 0
