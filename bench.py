@@ -443,12 +443,14 @@ def run_config(args, local_rank):
     translation plus one rotation sweep (cubes)."""
     import torch
     import oracle
-    from hoomd_rs_b200 import (FP32_RECHECK, FP64, ROTATE, TRANSLATE, Context, ConvexPolygon, ConvexPolyhedron,
-                               HardShape, HardSphere, Isotropic, LennardJones, Microstate, PairwiseCutoff, Periodic,
-                               Shifted, lattice)
+    from hoomd_rs_b200 import (FP32_RECHECK, FP64, ROTATE, TRANSLATE, Anisotropic, ApproximateShapeOverlap, Context,
+                               ConvexPolygon, ConvexPolyhedron, ConvexSurfaceMesh2d, HardShape, HardSphere, Isotropic,
+                               LennardJones, Microstate, OverlapPenalty, PairwiseCutoff, Periodic, Shifted, lattice,
+                               place_single_site_orientable_bodies)
     torch.cuda.set_device(local_rank)
     ctx = Context(local_rank)
     kind = args.workload
+    ori, extra = None, {}
     if kind == "disks":
         n, seed = 4096, 0x5EED0001
         pos, L = lattice.hard_sphere_box(n, 0.70, 2, seed)
@@ -468,6 +470,31 @@ def run_config(args, local_rank):
         desc = "hard cubes (vertices +-0.5), N=2^18, packing fraction 0.55, simple-cubic start, identity versors, " \
                "translation 0.08 then rotation 0.1 per step"
         orng = math.sqrt(3)
+    elif kind == "hexagons":
+        # benchmarks/src/mc/regular_polygon.rs:187-244: ConvexSurfaceMesh2d hexagons (circumradius 0.5) at
+        # packing fraction 0.68, placed by place_single_site_orientable_bodies on the device, then one
+        # translation (0.2) and one rotation (2 pi / 6) ParallelSweep per step
+        n, seed = 1 << 16, 0x5EED0008
+        mesh = ConvexSurfaceMesh2d.from_point_set(ConvexPolygon.regular(6).vertices)
+        h = PairwiseCutoff(HardShape(mesh))
+        r = h.maximum_interaction_range
+        insert = PairwiseCutoff(Anisotropic(ApproximateShapeOverlap.new(mesh, OverlapPenalty(), 0.01), r))
+        rho = 0.68 / (1.5 * math.sqrt(3.0) * 0.25)
+        t0 = time.perf_counter()
+        g = place_single_site_orientable_bodies(ctx, n, rho, r, insert, h, 2, seed=seed)
+        g.sweep(TRANSLATE, 0.2, 1.0, FP64, n_sweeps=20, increment_step=True)  # a short relaxation
+        placed_s = time.perf_counter() - t0
+        pos, ori, L = g.positions(), g.orientations(), float(g.box()[0])
+        assert g.overlap_count() == 0
+        g.close()
+        bound, dim = Periodic(r, [L, L]), 2
+        moves = [(TRANSLATE, 0.2), (ROTATE, 2.0 * math.pi / 6.0)]
+        okw = dict(interaction=oracle.HARD_CONVEX_SURFACE_MESH_2D, vertices=mesh.vertices)
+        desc = "2-D hexagons (ConvexSurfaceMesh2d, circumradius 0.5, separating axes), N=2^16, packing fraction " \
+               "0.68, placed on the device by QuickInsert/QuickCompress under the approximate shape overlap, " \
+               "then 20 translation sweeps; translation 0.2 then rotation 2 pi/6 per step"
+        orng = r
+        extra = {"placement_s": placed_s}
     elif kind == "squares":
         n, seed = 1 << 18, 0x5EED0007
         square = np.array([[-0.5, -0.5], [0.5, -0.5], [0.5, 0.5], [-0.5, 0.5]])
@@ -494,7 +521,7 @@ def run_config(args, local_rank):
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
     def timed(precision):
-        m = Microstate(ctx, bound, pos, h, seed=seed)
+        m = Microstate(ctx, bound, pos, h, seed=seed, orientations=ori)
         m.set_stream(stream.cuda_stream)
         for _ in range(args.warmup):
             for mv, mx in moves:
@@ -533,7 +560,7 @@ def run_config(args, local_rank):
             "warmup": args.warmup, "ms_per_step": r32["ms_per_step"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "fp32 pair test + fp64 recheck (fp64 state)", "data": "synthetic",
             "config": {"workload": desc, "n_bodies": n, "box_length": L,
-                       "l2": "flushed before every timed step (256 MiB device write)"},
+                       "l2": "flushed before every timed step (256 MiB device write)", **extra},
             "fp64": {"value": r64["value"], "ms_per_step": r64["ms_per_step"]},
             "mismatches": int(np.count_nonzero(np.any(p32 != p64, axis=1))), "acceptance": r32["acceptance"],
             "recheck_fraction": r32["recheck_fraction"], "gpu_launches": r32["launches"], "clocks": clocks,
@@ -541,7 +568,7 @@ def run_config(args, local_rank):
                                 "what": "decisions another summation order of the FP64 pair energies could change"}}
     if not args.no_cpu_baseline:
         threads = host_threads()
-        o = oracle.System(dim, [L] * dim, pos, seed=seed, **okw)
+        o = oracle.System(dim, [L] * dim, pos, ori, seed=seed, **okw)
         trials, t0, sweeps = 0, time.perf_counter(), 0
         while True:
             for mv, mx in moves:
@@ -640,9 +667,11 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="hard_spheres",
-                    choices=["hard_spheres", "replicas", "lj_replicas", "disks", "cubes", "squares", "lj", "gsd"],
+                    choices=["hard_spheres", "replicas", "lj_replicas", "disks", "cubes", "squares", "hexagons", "lj",
+                             "gsd"],
                     help="hard_spheres: the headline (2^20 spheres); replicas: 256 independent boxes in one batch; "
-                         "disks: 4096 hard disks; cubes: 2^18 hard cubes; lj: 2^19 Lennard-Jones sites; "
+                         "disks: 4096 hard disks; cubes: 2^18 hard cubes; hexagons: 2^16 hexagons placed on the "
+                         "device; lj: 2^19 Lennard-Jones sites; "
                          "gsd: GSD frames of the 2^20-sphere state")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -658,7 +687,7 @@ def main():
     if args.workload == "lj_replicas":
         run_lj_replicas(args, local_rank)
         return
-    if args.workload in ("disks", "cubes", "squares", "lj"):
+    if args.workload in ("disks", "cubes", "squares", "hexagons", "lj"):
         run_config(args, local_rank)
         return
     if args.workload == "gsd":
