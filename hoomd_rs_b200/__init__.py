@@ -37,7 +37,8 @@ OK, INVALID_ARGUMENT, RANGE_TOO_LARGE, OVERLAP_IN_INPUT, CELL_OVERFLOW, NAN_STAT
 HARD_SPHERE, HARD_CONVEX_POLYGON, HARD_CONVEX_POLYHEDRON, LENNARD_JONES, HARD_CONVEX_SURFACE_MESH_2D, \
     OVERLAP_PENALTY, ISOTROPIC = range(7)
 # hmc_univariate / hmc_univariate_wrap
-UV_LENNARD_JONES, UV_WEEKS_CHANDLER_ANDERSON, UV_HARMONIC, UV_HARMONIC_REPULSION, UV_BOXCAR, UV_OVERLAP_PENALTY = range(6)
+UV_LENNARD_JONES, UV_WEEKS_CHANDLER_ANDERSON, UV_HARMONIC, UV_HARMONIC_REPULSION, UV_BOXCAR, UV_OVERLAP_PENALTY, \
+    UV_LENNARD_JONES_GAUSS = range(7)
 UVW_NONE, UVW_SHIFTED, UVW_EXPANDED, UVW_XPLOR = range(4)
 TRANSLATE, ROTATE = range(2)
 FP64, FP32_RECHECK = range(2)
@@ -340,6 +341,16 @@ class Boxcar:
 
 
 @dataclass
+class LennardJonesGauss:
+    """hoomd_interaction::univariate::LennardJonesGauss (lennard_jones_gauss.rs): r_inv^12 - 2 r_inv^6
+    - epsilon exp(-(r / scale - r_0)^2 / (2 sigma_squared)), r_inv = scale / r."""
+    epsilon: float
+    sigma_squared: float
+    r_0: float
+    scale: float = 1.0
+
+
+@dataclass
 class Xplor:
     """hoomd_interaction::univariate::Xplor (xplor.rs): f(r) smoothed to 0 between r_smooth and
     r_cut."""
@@ -593,6 +604,8 @@ def _univariate(e):
         return UV_BOXCAR, (e.epsilon, e.left, e.right), wrap, wparams
     if isinstance(e, OverlapPenalty):
         return UV_OVERLAP_PENALTY, (e.k, e.maximum_allowed_overlap, e.epsilon_shoulder), wrap, wparams
+    if isinstance(e, LennardJonesGauss):
+        return UV_LENNARD_JONES_GAUSS, (e.epsilon, e.sigma_squared, e.r_0, e.scale), wrap, wparams
     raise HmcError(NOT_SUPPORTED, f"univariate {type(e).__name__}")
 
 
@@ -1252,7 +1265,7 @@ __all__ = ["Batch", "Context", "sdf_pressure", "gr_normalise", "ConvexPolygon", 
            "LennardJones", "Microstate", "PairwiseCutoff", "Rotate", "Shifted", "TuneOptions",
            "ParallelSweep", "Periodic", "Translate", "load_library", "SIGNATURES", "FP64", "FP32_RECHECK",
            "QuickInsert", "QuickCompress", "OverlapPenalty", "ApproximateShapeOverlap", "Anisotropic",
-           "WeeksChandlerAnderson", "Harmonic", "HarmonicRepulsion", "Boxcar", "Xplor",
+           "WeeksChandlerAnderson", "Harmonic", "HarmonicRepulsion", "Boxcar", "Xplor", "LennardJonesGauss",
            "place_single_site_orientable_bodies", "Expanded", "GrandCanonical", "IsothermalIsofugacity",
            "InsertRemoveCount",
            "TRANSLATE", "ROTATE", "HARD_SPHERE", "HARD_CONVEX_POLYGON", "HARD_CONVEX_POLYHEDRON", "LENNARD_JONES",

@@ -260,6 +260,13 @@ double univariate_host(uint32_t kind, const double* p, double r) {
             return r < p[1] ? 0.5 * p[0] / p[1] * ((r - p[1]) * (r - p[1])) : 0.0;
         case HMC_UV_BOXCAR:
             return r < p[1] ? 0.0 : (r < p[2] ? p[0] : 0.0);
+        case HMC_UV_LENNARD_JONES_GAUSS: {
+            const double ri = p[3] / r;
+            const double x = r / p[3] - p[2];
+            const double arg = -(x * x) / (2.0 * p[1]);
+            const double s2 = ri * ri, s4 = s2 * s2, s8 = s4 * s4;
+            return s4 * s8 - 2.0 * (s2 * s4) - p[0] * std::exp(arg);
+        }
         default:
             if (r < -p[1]) return INFINITY;
             if (r < 0.0) return 0.5 * p[0] * (r * r) + p[2];
@@ -589,7 +596,7 @@ hmc_status hmc_system_create(hmc_context* ctx, const hmc_system_desc* d, const d
         d->interaction != HMC_ISOTROPIC)
         return fail(HMC_NOT_SUPPORTED, "interaction %u is not available in this build", d->interaction);
     if (d->interaction == HMC_ISOTROPIC) {
-        if (d->univariate > HMC_UV_OVERLAP_PENALTY || d->univariate_wrap > HMC_UVW_XPLOR)
+        if (d->univariate > HMC_UV_LENNARD_JONES_GAUSS || d->univariate_wrap > HMC_UVW_XPLOR)
             return fail(HMC_INVALID_ARGUMENT, "univariate %u / wrap %u", d->univariate, d->univariate_wrap);
         for (int k = 0; k < 4; ++k)
             if (!std::isfinite(d->univariate_params[k]))
@@ -603,6 +610,9 @@ hmc_status hmc_system_create(hmc_context* ctx, const hmc_system_desc* d, const d
             return fail(HMC_INVALID_ARGUMENT, "sigma must be positive");
         if (d->univariate == HMC_UV_HARMONIC_REPULSION && !(d->univariate_params[1] > 0.0))
             return fail(HMC_INVALID_ARGUMENT, "HarmonicRepulsion r_cut must be positive");
+        if (d->univariate == HMC_UV_LENNARD_JONES_GAUSS &&
+            (!(d->univariate_params[1] > 0.0) || !(d->univariate_params[3] > 0.0)))
+            return fail(HMC_INVALID_ARGUMENT, "LennardJonesGauss sigma_squared and scale must be positive");
     }
     const bool polygon = d->interaction == HMC_HARD_CONVEX_POLYGON || d->interaction == HMC_HARD_CONVEX_SURFACE_MESH_2D;
     if (polygon) {

@@ -122,7 +122,7 @@ struct Pair {
 // HarmonicRepulsion (0.5 a / r_cut (r - r_cut)^2 below r_cut), Boxcar (epsilon on [left, right)),
 // OverlapPenalty (overlap_penalty.rs:109-115).
 enum : uint32_t { kUvLennardJones = 0, kUvWca = 1, kUvHarmonic = 2, kUvHarmonicRepulsion = 3, kUvBoxcar = 4,
-                  kUvOverlapPenalty = 5 };
+                  kUvOverlapPenalty = 5, kUvLjGauss = 6 };
 enum : uint32_t { kUvwNone = 0, kUvwShifted = 1, kUvwExpanded = 2, kUvwXplor = 3 };
 __device__ __forceinline__ double univariate64(uint32_t kind, const double* p, double r) {
     switch (kind) {
@@ -145,6 +145,13 @@ __device__ __forceinline__ double univariate64(uint32_t kind, const double* p, d
         }
         case kUvBoxcar:
             return r < p[1] ? 0.0 : (r < p[2] ? p[0] : 0.0);
+        case kUvLjGauss: {  // lennard_jones_gauss.rs: r_inv^12 - 2 r_inv^6 - eps exp(-(r / scale - r_0)^2 / (2 s^2))
+            const double ri = ddiv(p[3], r);
+            const double x = dsub(ddiv(r, p[3]), p[2]);
+            const double arg = ddiv(-dmul(x, x), dmul(2.0, p[1]));
+            const double s2 = dmul(ri, ri), s4 = dmul(s2, s2), s8 = dmul(s4, s4);
+            return dsub(dsub(dmul(s4, s8), dmul(2.0, dmul(s2, s4))), dmul(p[0], exp(arg)));
+        }
         default:
             if (r < -p[1]) return __longlong_as_double(0x7ff0000000000000ll);
             if (r < 0.0) return dadd(dmul(dmul(0.5, p[0]), dmul(r, r)), p[2]);
@@ -199,6 +206,13 @@ __device__ __forceinline__ double lj_only64(const Pair& P, double r2) {
     const double sr = ddiv(P.lj_sigma, r);
     const double s2 = dmul(sr, sr), s4 = dmul(s2, s2), s8 = dmul(s4, s4);
     return dsub(dmul(P.lj_four_eps, dsub(dmul(s4, s8), dmul(s2, s4))), P.lj_e_shift);
+}
+// The magnitude a soft pair energy adds to the order bound: |e|, and for LennardJonesGauss
+// 16 |epsilon| more (its exp is the device's, within a few ulp of the platform's, on the pair's
+// energy and on a Shifted constant; exp of a non-positive argument is at most 1).
+__device__ __forceinline__ double soft_pair_mag(const Pair& P, double r2, double e) {
+    if (P.penalty == 2u && P.uv_kind == kUvLjGauss && r2 < P.uv_rcut2) return fabs(e) + 16.0 * fabs(P.uv_p[0]);
+    return fabs(e);
 }
 __device__ __forceinline__ double lj_pair64(const Pair& P, double r2) {
     if (P.penalty) return P.penalty == 1u ? penalty_pair64(P, r2) : isotropic_pair64(P, r2);

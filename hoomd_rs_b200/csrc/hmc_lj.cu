@@ -104,13 +104,15 @@ __device__ __forceinline__ void lj_energy64(const Geometry& g, const Arrays& A, 
                 sv[2] = b4.z;
                 wrap_inv<DIM>(g.L, g.invL, sv);
             }
-            const double x = soft_pair64<GENERIC>(P, ref_dist2<DIM>(g, ta, sv));
+            const double ra = ref_dist2<DIM>(g, ta, sv);
+            const double x = soft_pair64<GENERIC>(P, ra);
             a = dadd(a, x);
-            am += fabs(x);
+            am += GENERIC ? soft_pair_mag(P, ra, x) : fabs(x);
             if (TWO) {
-                const double y = soft_pair64<GENERIC>(P, ref_dist2<DIM>(g, tb, sv));
+                const double rb = ref_dist2<DIM>(g, tb, sv);
+                const double y = soft_pair64<GENERIC>(P, rb);
                 b = dadd(b, y);
-                am += fabs(y);
+                am += GENERIC ? soft_pair_mag(P, rb, y) : fabs(y);
             }
         }
     }

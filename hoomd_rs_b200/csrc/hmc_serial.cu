@@ -31,9 +31,10 @@ __device__ __forceinline__ double serial_energy(const Geometry& g, const SerialG
             if (j == self) continue;
             const double4 s4 = G.site[j];
             const double sv[3] = {s4.x, s4.y, s4.z};
-            const double x = lj_pair64(P, ref_dist2<DIM>(g, t, sv));
+            const double r2 = ref_dist2<DIM>(g, t, sv);
+            const double x = lj_pair64(P, r2);
             e = dadd(e, x);
-            am += fabs(x);
+            am += soft_pair_mag(P, r2, x);
         }
     }
 #pragma unroll

@@ -90,7 +90,9 @@ typedef enum hmc_univariate {
     HMC_UV_HARMONIC = 2,               /* {k, r_0} */
     HMC_UV_HARMONIC_REPULSION = 3,     /* {a, r_cut} */
     HMC_UV_BOXCAR = 4,                 /* {epsilon, left, right} */
-    HMC_UV_OVERLAP_PENALTY = 5         /* {k, maximum_allowed_overlap, epsilon_shoulder} */
+    HMC_UV_OVERLAP_PENALTY = 5,        /* {k, maximum_allowed_overlap, epsilon_shoulder} */
+    HMC_UV_LENNARD_JONES_GAUSS = 6     /* {epsilon, sigma_squared, r_0, scale}: exp is the device's, within
+                                          a few ulp of the platform's, and the order bound covers it */
 } hmc_univariate;
 /* The wrapper around the univariate, with its parameters in hmc_system_desc.wrap_params. */
 typedef enum hmc_univariate_wrap {

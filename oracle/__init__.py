@@ -26,7 +26,8 @@ CONVEX_POLYHEDRON_PENALTY = 6  # Anisotropic { ApproximateShapeOverlap { Convex(
 CONVEX_POLYGON_PENALTY = 7     # the same with Convex(ConvexPolygon)
 ISOTROPIC = 8                  # Isotropic { W(F), r_cut }: F and W below
 SURFACE_MESH_2D_PENALTY = 9    # ApproximateShapeOverlap with ConvexSurfaceMesh2d (separating axes)
-UV_LENNARD_JONES, UV_WEEKS_CHANDLER_ANDERSON, UV_HARMONIC, UV_HARMONIC_REPULSION, UV_BOXCAR, UV_OVERLAP_PENALTY = range(6)
+UV_LENNARD_JONES, UV_WEEKS_CHANDLER_ANDERSON, UV_HARMONIC, UV_HARMONIC_REPULSION, UV_BOXCAR, UV_OVERLAP_PENALTY, \
+    UV_LENNARD_JONES_GAUSS = range(7)
 UVW_NONE, UVW_SHIFTED, UVW_EXPANDED, UVW_XPLOR = range(4)
 TRANSLATE = 0
 ROTATE = 1

@@ -846,7 +846,7 @@ double shifted_lj_pair(double eps, double sigma, double rcut, double rshift, dou
 // The univariate energies Isotropic accepts (hoomd-interaction/src/univariate/*.rs), each with
 // the reference's order of operations, and the wrappers around them.
 enum { UV_LENNARD_JONES = 0, UV_WEEKS_CHANDLER_ANDERSON = 1, UV_HARMONIC = 2, UV_HARMONIC_REPULSION = 3,
-       UV_BOXCAR = 4, UV_OVERLAP_PENALTY = 5 };
+       UV_BOXCAR = 4, UV_OVERLAP_PENALTY = 5, UV_LENNARD_JONES_GAUSS = 6 };
 enum { UVW_NONE = 0, UVW_SHIFTED = 1, UVW_EXPANDED = 2, UVW_XPLOR = 3 };
 struct Univariate {
     int kind = UV_LENNARD_JONES, wrap = UVW_NONE;
@@ -865,6 +865,11 @@ struct Univariate {
                 return r < p[1] ? 0.5 * p[0] / p[1] * ((r - p[1]) * (r - p[1])) : 0.0;
             case UV_BOXCAR:  // boxcar.rs: epsilon on [left, right)
                 return r < p[1] ? 0.0 : (r < p[2] ? p[0] : 0.0);
+            case UV_LENNARD_JONES_GAUSS: {  // lennard_jones_gauss.rs: {eps, sigma^2, r_0, scale}
+                const double r_inv = p[3] / r;
+                const double arg = -((r / p[3] - p[2]) * (r / p[3] - p[2])) / (2.0 * p[1]);
+                return powi(r_inv, 12) - 2.0 * powi(r_inv, 6) - p[0] * std::exp(arg);
+            }
             default:  // overlap_penalty.rs:109-115
                 if (r < -p[1]) return INFINITY;
                 if (r < 0.0) return 0.5 * p[0] * (r * r) + p[2];

@@ -12,8 +12,8 @@ import pytest
 
 import oracle
 from hoomd_rs_b200 import (FP32_RECHECK, FP64, TRANSLATE, Boxcar, Context, Expanded, Harmonic, HarmonicRepulsion,
-                           Isotropic, LennardJones, Microstate, OverlapPenalty, PairwiseCutoff, Periodic, Shifted,
-                           WeeksChandlerAnderson, Xplor, lattice)
+                           Isotropic, LennardJones, LennardJonesGauss, Microstate, OverlapPenalty, PairwiseCutoff,
+                           Periodic, Shifted, WeeksChandlerAnderson, Xplor, lattice)
 
 pytestmark = pytest.mark.gpu
 
@@ -42,7 +42,12 @@ CASES = {
                            "wrap_params": [0.2]}, 1.5),
     "penalty": (OverlapPenalty(100.0, 0.3, 2.0), {"kind": oracle.UV_OVERLAP_PENALTY, "params": [100.0, 0.3, 2.0]},
                 1.0),
+    "lj_gauss": (Shifted(LennardJonesGauss(1.5, 0.02, 1.5, 1.0), 2.0),
+                 {"kind": oracle.UV_LENNARD_JONES_GAUSS, "params": [1.5, 0.02, 1.5, 1.0], "wrap": oracle.UVW_SHIFTED,
+                  "wrap_params": [2.0]}, 2.0),
 }
+# the potentials whose pair energy uses exp: the device's, within a few ulp of the platform's
+EXP = {"lj_gauss"}
 
 
 def systems(ctx, name, dim, pos, L, seed):
@@ -65,7 +70,10 @@ def test_pair_energies_equal_the_oracle(ctx, name):
         pos = [[0.0, 0.0, 0.0], [float(r), 0.0, 0.0]]
         g, o = systems(ctx, name, 3, pos, 10.0, 1)
         got, want = g.total_energy(), o.total_energy()
-        assert got == want or (math.isnan(got) and math.isnan(want)), (name, r, got, want)
+        if name in EXP:
+            assert math.isclose(got, want, rel_tol=1e-14, abs_tol=1e-14 * 1.5), (name, r, got, want)
+        else:
+            assert got == want or (math.isnan(got) and math.isnan(want)), (name, r, got, want)
         g.close()
 
 
@@ -74,6 +82,7 @@ def test_pair_energies_equal_the_oracle(ctx, name):
                                                   ("harmonic_repulsion", 2, 800, 0.9, 0.5, 0.15),
                                                   ("xplor_lj", 3, 1372, 0.8, 1.0, 0.1),
                                                   ("boxcar", 3, 800, 0.5, 1.0, 0.2),
+                                                  ("lj_gauss", 3, 1000, 0.7, 1.0, 0.1),
                                                   ("expanded_harmonic", 3, 600, 0.3, 1.0, 0.2)])
 def test_trajectory_matches_oracle(ctx, name, dim, n, rho, kt, d, precision):
     pos, L = start(dim, n, rho, 0x5EED0051)

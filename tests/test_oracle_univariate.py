@@ -1,7 +1,8 @@
 """The oracle's univariate energies for Isotropic (hoomd-interaction/src/univariate/) against the
 reference's own tests of them, with their tolerances: weeks_chandler_anderson.rs
 special_points_12_6, harmonic.rs zero_energy_point / general_case, harmonic_repulsion.rs
-outside_rcut / general_case, boxcar.rs general_case and xplor.rs special_points_12_6; and
+outside_rcut / general_case, boxcar.rs general_case, xplor.rs special_points_12_6 and
+lennard_jones_gauss.rs select_points_first_set / select_points_second_set; and
 Isotropic's cut-off (isotropic.rs:147-156) through two-body systems."""
 import math
 
@@ -101,3 +102,13 @@ def test_isotropic_cut_off_and_sum():
     assert o.total_energy() == pytest.approx(want, rel=1e-15)
     # the pair at exactly r_cut contributes nothing
     assert e(oracle.UV_HARMONIC_REPULSION, [3.0, 1.5], 1.5) == 0.0
+
+
+@pytest.mark.parametrize("params,r,want", [([2.0, 0.5, 3.0, 1.0], 1.5, -0.378_674_092_892_274),
+                                           ([2.0, 0.5, 3.0, 1.0], 3.2, -1.923_440_656_092_139),
+                                           ([10.0, 0.1, 5.0, 1.0], 1.5, -0.167_875_643_768_546),
+                                           ([10.0, 0.1, 5.0, 1.0], 3.2, -0.001_862_699_147_576_425)])
+def test_lennard_jones_gauss_select_points(params, r, want):
+    # lennard_jones_gauss.rs: assert_relative_eq!(energy, want, epsilon = 1e-12)
+    got = e(oracle.UV_LENNARD_JONES_GAUSS, params, r)
+    assert abs(got - want) <= 1e-12 or abs(got - want) <= EPS * max(abs(got), abs(want))
