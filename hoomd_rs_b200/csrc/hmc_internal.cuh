@@ -297,7 +297,7 @@ constexpr LaunchShape kSphereDirectShapes[] = {{6, 1, 0}, {5, 1, 0}, {7, 1, 0}};
 constexpr LaunchShape kSphereCoopShapes[] = {{6, 1, 2}, {6, 1, 1}, {6, 1, 3}, {5, 1, 2}, {7, 1, 2}};
 constexpr LaunchShape kLjShapes[] = {{9, 1, 0}, {7, 1, 0}, {11, 1, 0}};
 constexpr LaunchShape kPolyShapes[] = {{5, 4, 0}, {5, 2, 0}, {5, 8, 0}};
-constexpr LaunchShape kBatchShapes[] = {{4, 1, 0}, {3, 1, 0}, {5, 1, 0}, {6, 1, 0}};
+constexpr LaunchShape kBatchShapes[] = {{4, 1, 0}, {3, 1, 0}, {5, 1, 0}, {6, 1, 0}, {7, 1, 0}, {8, 1, 0}};
 constexpr LaunchShape kPoly2Shapes[] = {{8, 4, 0}};    // the polygon pass: one compiled shape
 constexpr LaunchShape kBatchLjShapes[] = {{7, 1, 0}};  // the Lennard-Jones replica passes: one
 template <size_t N>

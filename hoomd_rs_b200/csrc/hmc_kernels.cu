@@ -1602,14 +1602,16 @@ cudaError_t launch_sweep_batch(int dim, bool fp32, const Batch& b, const Arrays&
     if (max_active == 0) return cudaSuccess;
     using BatchKernel = void (*)(Batch, Arrays, uint32_t, uint32_t, uint32_t);
     // the compiled launch variants, in the order of kBatchShapes
-    static const BatchKernel kernels[2][2][4] = {
+    static const BatchKernel kernels[2][2][6] = {
         {{k_sweep_batch<2, false, 4>, k_sweep_batch<2, false, 3>, k_sweep_batch<2, false, 5>,
-          k_sweep_batch<2, false, 6>},
-         {k_sweep_batch<2, true, 4>, k_sweep_batch<2, true, 3>, k_sweep_batch<2, true, 5>, k_sweep_batch<2, true, 6>}},
+          k_sweep_batch<2, false, 6>, k_sweep_batch<2, false, 7>, k_sweep_batch<2, false, 8>},
+         {k_sweep_batch<2, true, 4>, k_sweep_batch<2, true, 3>, k_sweep_batch<2, true, 5>, k_sweep_batch<2, true, 6>,
+          k_sweep_batch<2, true, 7>, k_sweep_batch<2, true, 8>}},
         {{k_sweep_batch<3, false, 4>, k_sweep_batch<3, false, 3>, k_sweep_batch<3, false, 5>,
-          k_sweep_batch<3, false, 6>},
-         {k_sweep_batch<3, true, 4>, k_sweep_batch<3, true, 3>, k_sweep_batch<3, true, 5>, k_sweep_batch<3, true, 6>}}};
-    const BatchKernel k = kernels[dim == 3][fp32][variant < 4 ? variant : 0];
+          k_sweep_batch<3, false, 6>, k_sweep_batch<3, false, 7>, k_sweep_batch<3, false, 8>},
+         {k_sweep_batch<3, true, 4>, k_sweep_batch<3, true, 3>, k_sweep_batch<3, true, 5>, k_sweep_batch<3, true, 6>,
+          k_sweep_batch<3, true, 7>, k_sweep_batch<3, true, 8>}}};
+    const BatchKernel k = kernels[dim == 3][fp32][variant < 6 ? variant : 0];
     uint32_t grid = blocks_for(max_active, 128);
     const uint32_t wave = (uint32_t)resident_wave((const void*)k);
     if (grid > wave) grid = wave;

@@ -110,7 +110,7 @@ def test_batch_variants_and_autotune(ctx):
     ref = Batch(ctx, reps)
     ref.set_launch_variant(FP32_RECHECK, 0)
     want, _ = ref.sweep(maxima, FP32_RECHECK, n_sweeps=2, increment_step=True)
-    for v in (1, 2, 3):
+    for v in (1, 2, 3, 4, 5):
         b = Batch(ctx, reps)
         b.set_launch_variant(FP32_RECHECK, v)
         got, _ = b.sweep(maxima, FP32_RECHECK, n_sweeps=2, increment_step=True)
@@ -120,7 +120,7 @@ def test_batch_variants_and_autotune(ctx):
     b = Batch(ctx, reps)
     before = [b.state(k) for k in range(len(reps))]
     chosen, ms = b.autotune(maxima, FP32_RECHECK, sweeps=2)
-    assert len(ms) == chosen["count"] == 4 and ms[chosen["index"]] == ms.min()
+    assert len(ms) == chosen["count"] == 6 and ms[chosen["index"]] == ms.min()
     for k in range(len(reps)):
         pos, step, sub = b.state(k)
         assert np.array_equal(pos, before[k][0]) and (step, sub) == before[k][1:]
