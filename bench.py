@@ -348,10 +348,14 @@ def run_lj_replicas(args, local_rank):
         pos, L = lattice.lennard_jones_box(n, rho, 3, 0x5EED0050 + k)
         reps.append({"boundary": Periodic(r_cut, [L] * 3), "positions": pos, "seed": 0x5EED0050 + k, "hamiltonian": h})
 
+    tuned = {}
+
     def timed_batch(precision, steps, warmup):
         b = Batch(ctx, reps)
         for _ in range(warmup):
             b.sweep(d, precision, increment_step=True, temperatures=kts)
+        # the launch-shape autotuner for the replica pass (restores the state afterwards)
+        tuned[precision] = b.autotune(d, precision, sweeps=2, temperatures=kts)
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
@@ -415,6 +419,9 @@ def run_lj_replicas(args, local_rank):
             "fp64": {"value": v64, "ms_per_step": ms64},
             "mismatches": int(sum(np.count_nonzero(np.any(a != b, axis=1)) for a, b in zip(p32, p64))),
             "one_system_after_another": {"value": v_single, "precision": "fp32_recheck"},
+            "launch_variants": {("fp32_recheck" if p == FP32_RECHECK else "fp64"):
+                                {"chosen": c, "ms_per_sweep": [round(float(x), 4) for x in m]}
+                                for p, (c, m) in tuned.items()},
             "gpu_launches": launches, "clocks": clocks}
     if not args.no_cpu_baseline:
         threads = host_threads()

@@ -2366,7 +2366,8 @@ hmc_status hmc_batch_sweep(hmc_batch* bt, const hmc_sweep_params* params, hmc_co
                 for (uint32_t c = 0; c < colors; ++c) {
                     if (bt->interaction == HMC_LENNARD_JONES)
                         HMC_CUDA(launch_sweep_batch_lj(bt->dim, fp32, bt->b, bt->arr, c, round, bt->b.color_stride,
-                                                       round > 0 || c > 0, round == 0 && c == 0, bt->stream));
+                                                       round > 0 || c > 0, round == 0 && c == 0, bt->stream,
+                                                       variant));
                     else
                         HMC_CUDA(launch_sweep_batch(bt->dim, fp32, bt->b, bt->arr, c, round, bt->b.color_stride,
                                                     round > 0 || c > 0, round == 0 && c == 0, bt->stream, variant));

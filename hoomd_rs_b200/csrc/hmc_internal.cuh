@@ -299,7 +299,7 @@ constexpr LaunchShape kLjShapes[] = {{9, 1, 0}, {7, 1, 0}, {11, 1, 0}};
 constexpr LaunchShape kPolyShapes[] = {{5, 4, 0}, {5, 2, 0}, {5, 8, 0}};
 constexpr LaunchShape kBatchShapes[] = {{4, 1, 0}, {3, 1, 0}, {5, 1, 0}, {6, 1, 0}, {7, 1, 0}, {8, 1, 0}};
 constexpr LaunchShape kPoly2Shapes[] = {{8, 4, 0}};    // the polygon pass: one compiled shape
-constexpr LaunchShape kBatchLjShapes[] = {{7, 1, 0}};  // the Lennard-Jones replica passes: one
+constexpr LaunchShape kBatchLjShapes[] = {{7, 1, 0}, {9, 1, 0}, {5, 1, 0}};  // the Lennard-Jones replica passes
 template <size_t N>
 constexpr uint32_t n_shapes(const LaunchShape (&)[N]) {
     return (uint32_t)N;
@@ -381,7 +381,8 @@ cudaError_t launch_sweep_batch(int dim, bool fp32, const Batch& b, const Arrays&
 cudaError_t launch_overlap_batch(int dim, const Batch& b, const Arrays& a, uint32_t n, cudaStream_t s);
 // Batches of Lennard-Jones replicas: one warp per trial over every replica's colour list (hmc_lj.cu).
 cudaError_t launch_sweep_batch_lj(int dim, bool fp32, const Batch& b, const Arrays& a, uint32_t color, uint32_t round,
-                                  uint32_t max_active, bool overlap_previous, bool early_wait, cudaStream_t s);
+                                  uint32_t max_active, bool overlap_previous, bool early_wait, cudaStream_t s,
+                                  uint32_t variant = 0);
 // coop selects the warp-cooperative pass (the per-lane pass otherwise).
 cudaError_t launch_sweep_sphere(int dim, bool fp32, const Geometry& g, const Arrays& a, const Pair& p,
                                 const Launch& l, bool coop, cudaStream_t s, uint32_t variant = 0);

@@ -515,8 +515,8 @@ __global__ void __launch_bounds__(128, MINB) k_sweep_lj32(Geometry g, Arrays A, 
 // One colour pass over every replica of a batch that still runs round `round` of this sweep,
 // FP64: one warp per trial as in k_sweep_lj, with the box, checkerboard, pair parameters,
 // Counter, move size and kT of the trial's replica from the replica table.
-template <int DIM>
-__global__ void __launch_bounds__(128, HMC_LJ_BATCH_MIN_BLOCKS)
+template <int DIM, int MINB = HMC_LJ_BATCH_MIN_BLOCKS>
+__global__ void __launch_bounds__(128, MINB)
     k_sweep_batch_lj(Batch B, Arrays A, uint32_t color, uint32_t round, uint32_t early_wait) {
     if (early_wait) grid_dependency_wait();  // first pass: the rebuild's arrays are read at once
     const uint32_t lane = threadIdx.x & 31u;
@@ -581,8 +581,8 @@ __global__ void __launch_bounds__(128, HMC_LJ_BATCH_MIN_BLOCKS)
 // The FP32 + recheck pass over a batch: k_sweep_lj32 (four trials per block, an undecided
 // trial rechecked by the whole block in the FP64 pass's order) with each trial's geometry and
 // parameters from its replica; the owner also publishes its replica for the helping warps.
-template <int DIM>
-__global__ void __launch_bounds__(128, HMC_LJ_BATCH_MIN_BLOCKS)
+template <int DIM, int MINB = HMC_LJ_BATCH_MIN_BLOCKS>
+__global__ void __launch_bounds__(128, MINB)
     k_sweep_batch_lj32(Batch B, Arrays A, uint32_t color, uint32_t round, uint32_t early_wait) {
     if (early_wait) grid_dependency_wait();  // first pass: the rebuild's arrays are read at once
     __shared__ double s_e[kRecheckChunks][2][32];
@@ -963,7 +963,8 @@ cudaError_t launch_trials_lj(int dim, bool fp32, const Geometry& g, const Arrays
 }
 
 cudaError_t launch_sweep_batch_lj(int dim, bool fp32, const Batch& b, const Arrays& a, uint32_t color, uint32_t round,
-                                  uint32_t max_active, bool overlap_previous, bool early_wait, cudaStream_t s) {
+                                  uint32_t max_active, bool overlap_previous, bool early_wait, cudaStream_t s,
+                                  uint32_t variant) {
     if (max_active == 0) return cudaSuccess;
     static int max_blocks = 0;
     if (max_blocks == 0) {
@@ -976,11 +977,14 @@ cudaError_t launch_sweep_batch_lj(int dim, bool fp32, const Batch& b, const Arra
     if (blocks > (uint32_t)max_blocks) blocks = (uint32_t)max_blocks;
     PassLaunch pl(blocks, overlap_previous || early_wait, s);
     const uint32_t ew = early_wait ? 1u : 0u;
-    if (dim == 2)
-        return fp32 ? cudaLaunchKernelEx(&pl.cfg, k_sweep_batch_lj32<2>, b, a, color, round, ew)
-                    : cudaLaunchKernelEx(&pl.cfg, k_sweep_batch_lj<2>, b, a, color, round, ew);
-    return fp32 ? cudaLaunchKernelEx(&pl.cfg, k_sweep_batch_lj32<3>, b, a, color, round, ew)
-                : cudaLaunchKernelEx(&pl.cfg, k_sweep_batch_lj<3>, b, a, color, round, ew);
+    using BatchLjKernel = void (*)(Batch, Arrays, uint32_t, uint32_t, uint32_t);
+    // the compiled launch variants, in the order of kBatchLjShapes ([dim == 3][fp32][variant])
+    static const BatchLjKernel kernels[2][2][3] = {
+        {{k_sweep_batch_lj<2, 7>, k_sweep_batch_lj<2, 9>, k_sweep_batch_lj<2, 5>},
+         {k_sweep_batch_lj32<2, 7>, k_sweep_batch_lj32<2, 9>, k_sweep_batch_lj32<2, 5>}},
+        {{k_sweep_batch_lj<3, 7>, k_sweep_batch_lj<3, 9>, k_sweep_batch_lj<3, 5>},
+         {k_sweep_batch_lj32<3, 7>, k_sweep_batch_lj32<3, 9>, k_sweep_batch_lj32<3, 5>}}};
+    return cudaLaunchKernelEx(&pl.cfg, kernels[dim == 3][fp32][variant < 3 ? variant : 0], b, a, color, round, ew);
 }
 
 cudaError_t launch_eval_lj(int dim, bool fp32, const Geometry& g, const Arrays& a, const Pair& p,

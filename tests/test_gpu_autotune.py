@@ -124,3 +124,24 @@ def test_batch_variants_and_autotune(ctx):
     for k in range(len(reps)):
         pos, step, sub = b.state(k)
         assert np.array_equal(pos, before[k][0]) and (step, sub) == before[k][1:]
+
+
+def test_lj_batch_variants_give_the_same_trajectory(ctx):
+    # the Lennard-Jones replica pass in every compiled launch shape, both precision modes
+    h = PairwiseCutoff(Isotropic(Shifted(LennardJones(1.0, 1.0), 2.5), 2.5))
+    reps = []
+    for k in range(6):
+        pos, L = lattice.lennard_jones_box(2048, 0.8, 3, 400 + k)
+        reps.append({"boundary": Periodic(2.5, [L] * 3), "positions": pos, "seed": 400 + k, "hamiltonian": h})
+    kts = np.linspace(0.8, 2.0, len(reps))
+    for precision in (FP64, FP32_RECHECK):
+        ref = Batch(ctx, reps)
+        ref.set_launch_variant(precision, 0)
+        want, _ = ref.sweep(0.1, precision, n_sweeps=2, increment_step=True, temperatures=kts)
+        for v in (1, 2):
+            b = Batch(ctx, reps)
+            b.set_launch_variant(precision, v)
+            got, _ = b.sweep(0.1, precision, n_sweeps=2, increment_step=True, temperatures=kts)
+            assert [(c.accepted, c.rejected) for c in got] == [(c.accepted, c.rejected) for c in want], (precision, v)
+            for k in range(len(reps)):
+                assert np.array_equal(b.positions(k), ref.positions(k)), (precision, v, k)
