@@ -86,6 +86,10 @@ class hmc_count(C.Structure):
                 ("pair_checks", C.c_uint64), ("max_fp32_error", C.c_double), ("order_ambiguous", C.c_uint64)]
 
 
+_SWEEP_PARAMS_DTYPE = np.dtype(hmc_sweep_params)
+_COUNT_DTYPE = np.dtype(hmc_count)
+
+
 class hmc_launch_variant(C.Structure):
     _fields_ = [("index", C.c_uint32), ("count", C.c_uint32), ("blocks_per_sm", C.c_uint32),
                 ("trials_per_warp", C.c_uint32), ("own_steps", C.c_uint32)]
@@ -1125,16 +1129,21 @@ class Batch:
               temperatures=1.0):
         """ParallelSweep::apply on every replica (replica k moves up to maxima[k] at kT =
         temperatures[k]); returns (per-replica Counts, batch total Count)."""
-        maxima = np.broadcast_to(np.asarray(maxima, dtype=np.float64), (self.n_replicas,))
-        kts = np.broadcast_to(np.asarray(temperatures, dtype=np.float64), (self.n_replicas,))
-        ps = (hmc_sweep_params * self.n_replicas)()
-        for k in range(self.n_replicas):
-            ps[k] = hmc_sweep_params(C.sizeof(hmc_sweep_params), TRANSLATE, float(maxima[k]), float(kts[k]), precision,
-                                     n_sweeps, int(increment_step), 0)
-        cs = (hmc_count * self.n_replicas)()
+        # the per-replica parameters and counts as arrays of the C structs, filled without a Python
+        # loop over the replicas (the batch's step would otherwise wait for it)
+        ps = np.zeros(self.n_replicas, dtype=_SWEEP_PARAMS_DTYPE)
+        ps["struct_size"] = C.sizeof(hmc_sweep_params)
+        ps["move"] = TRANSLATE
+        ps["maximum"] = maxima
+        ps["temperature"] = temperatures
+        ps["precision"] = precision
+        ps["n_sweeps"] = n_sweeps
+        ps["increment_step"] = int(increment_step)
+        cs = np.zeros(self.n_replicas, dtype=_COUNT_DTYPE)
         tot = hmc_count()
-        _check(_lib.hmc_batch_sweep(self._h, ps, cs, C.byref(tot)))
-        counts = [Count(c.accepted, c.rejected, 0, 0, 0.0) for c in cs]
+        _check(_lib.hmc_batch_sweep(self._h, ps.ctypes.data_as(C.POINTER(hmc_sweep_params)),
+                                    cs.ctypes.data_as(C.POINTER(hmc_count)), C.byref(tot)))
+        counts = [Count(int(a), int(r), 0, 0, 0.0) for a, r in zip(cs["accepted"].tolist(), cs["rejected"].tolist())]
         return counts, Count(tot.accepted, tot.rejected, tot.rechecks, tot.pair_checks, tot.max_fp32_error,
                              tot.order_ambiguous)
 
