@@ -1012,6 +1012,35 @@ class QuickCompress:
         microstate.edge_lengths = [float(x) for x in microstate.box()]
 
 
+def place_single_site_point_bodies(ctx: "Context", n: int, number_density: float, maximum_interaction_range: float,
+                                   overlap_penalty_hamiltonian: PairwiseCutoff, dim: int, *, seed: int = 0,
+                                   max_steps: int = 1_000_000) -> "Microstate":
+    """place_single_site_point_bodies (benchmarks/src/place.rs:31-110): an empty periodic box at
+    0.7 times the number density, QuickInsert of n bodies, then QuickCompress to the target
+    density (either every 20 steps), and a serial translation Sweep (0.1, kT = 1) every step, all
+    under the overlap-penalty hamiltonian. Returns that microstate; its positions start a system of
+    the hard hamiltonian."""
+    initial_box_length = (n / (0.7 * number_density)) ** (1.0 / dim)
+    final_box_volume = n / number_density
+    g = Microstate(ctx, Periodic(maximum_interaction_range, [initial_box_length] * dim), np.zeros((0, dim)),
+                   overlap_penalty_hamiltonian, seed=seed, capacity=n)
+    quick_insert = QuickInsert.new(n)
+    quick_compress = QuickCompress.with_target_volume(final_box_volume)
+    for _ in range(max_steps):
+        if quick_compress.is_complete():
+            break
+        if g.step() % 20 == 0:
+            if quick_insert.is_complete():
+                quick_compress.apply(g)
+            else:
+                quick_insert.apply(g)
+        g.serial_sweep(0.1)
+        g.increment_step()
+    else:
+        raise HmcError(ITERATION_CAP, f"QuickCompress did not complete in {max_steps} steps")
+    return g
+
+
 def place_single_site_orientable_bodies(ctx: "Context", n: int, number_density: float,
                                         maximum_interaction_range: float, insert_hamiltonian: PairwiseCutoff,
                                         hamiltonian: PairwiseCutoff, dim: int, *, seed: int = 0,
@@ -1275,7 +1304,7 @@ __all__ = ["Batch", "Context", "sdf_pressure", "gr_normalise", "ConvexPolygon", 
            "ParallelSweep", "Periodic", "Translate", "load_library", "SIGNATURES", "FP64", "FP32_RECHECK",
            "QuickInsert", "QuickCompress", "OverlapPenalty", "ApproximateShapeOverlap", "Anisotropic",
            "WeeksChandlerAnderson", "Harmonic", "HarmonicRepulsion", "Boxcar", "Xplor", "LennardJonesGauss",
-           "place_single_site_orientable_bodies", "Expanded", "GrandCanonical", "IsothermalIsofugacity",
+           "place_single_site_orientable_bodies", "place_single_site_point_bodies", "Expanded", "GrandCanonical", "IsothermalIsofugacity",
            "InsertRemoveCount",
            "TRANSLATE", "ROTATE", "HARD_SPHERE", "HARD_CONVEX_POLYGON", "HARD_CONVEX_POLYHEDRON", "LENNARD_JONES",
            "HARD_CONVEX_SURFACE_MESH_2D"]

@@ -11,7 +11,8 @@ import pytest
 
 import oracle
 from hoomd_rs_b200 import (FP32_RECHECK, FP64, TRANSLATE, Context, Expanded, HardSphere, HmcError, Isotropic,
-                           Microstate, OverlapPenalty, PairwiseCutoff, Periodic, QuickCompress, QuickInsert, lattice)
+                           Microstate, OverlapPenalty, PairwiseCutoff, Periodic, QuickCompress, QuickInsert, lattice,
+                           place_single_site_point_bodies)
 
 pytestmark = pytest.mark.gpu
 
@@ -224,3 +225,22 @@ def test_grand_canonical_bit_identical(ctx, soft, tmp_path):
         o.serial_sweep(oracle.TRANSLATE, 0.1, 1.0)
         same_state(g, o)
     f.close()
+
+
+def test_place_single_site_point_bodies_equals_the_oracle(ctx):
+    # the library's place.rs:31-110 loop against the same loop on the oracle
+    n, rho, dim = 300, 0.8, 2
+    g = place_single_site_point_bodies(ctx, n, rho, 1.0, penalty_h(), dim, seed=0x5EED0043)
+    L0 = (n / (0.7 * rho)) ** (1.0 / dim)
+    o = oracle.System(dim, [L0] * dim, np.zeros((0, dim)), seed=0x5EED0043, interaction=oracle.OVERLAP_PENALTY,
+                      diameter=1.0)
+    oqi = {"target": n, "allowed_overlaps": max(n // 8, 1), "inserted": 0, "complete": 0}
+    oqc = {"target_volume": n / rho, "maximum_energy_per_site": 1000.0, "maximum_delta": 0.05, "state": 0,
+           "is_final": 0, "boundary": [0.0, 0.0, 0.0]}
+    while oqc["state"] != 3:
+        if o.state()[2] % 20 == 0:
+            (o.quick_compress if oqi["complete"] else o.quick_insert)(oqc if oqi["complete"] else oqi)
+        o.serial_sweep(oracle.TRANSLATE, 0.1, 1.0)
+        o.increment_step()
+    same_state(g, o)
+    assert g.total_energy() == 0.0 == o.total_energy()
