@@ -195,6 +195,7 @@ SIGNATURES = {
     "hmc_set_box": (C.c_int, [_vp, _dp]),
     "hmc_get_n_bodies": (C.c_int, [_vp, C.POINTER(C.c_uint64)]),
     "hmc_set_shape_overlap": (C.c_int, [_vp, C.POINTER(hmc_shape_overlap_params)]),
+    "hmc_set_cooperative_pass": (C.c_int, [_vp, C.c_uint32, C.c_uint32]),
     "hmc_gsd_last_error": (C.c_int, []),
     "hmc_gsd_create": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_uint16, C.c_uint16, C.c_int,
                                  C.POINTER(_vp)]),
@@ -801,6 +802,11 @@ class Microstate:
     def set_launch_variant(self, precision: int, index: Optional[int]):
         """Force a launch variant (None: the autotuner's recorded choice for this workload, else 0)."""
         _check(_lib.hmc_set_launch_variant(self._h, precision, 0xFFFFFFFF if index is None else index))
+
+    def set_cooperative_pass(self, precision: int, cooperative: bool):
+        """Hard spheres: the warp-cooperative colour pass (the FP64 default) or one lane per trial
+        (the FP32 default) for this precision; the trajectory is the same."""
+        _check(_lib.hmc_set_cooperative_pass(self._h, precision, int(cooperative)))
 
     def autotune(self, move: int, maximum: float, temperature: float, precision: int, sweeps: int = 4):
         """hmc_autotune: time every launch variant of this system's pass from the current state

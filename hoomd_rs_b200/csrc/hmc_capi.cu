@@ -1065,6 +1065,16 @@ hmc_status hmc_get_launch_variant(hmc_system* s, uint32_t precision, uint32_t in
     return HMC_OK;
 }
 
+hmc_status hmc_set_cooperative_pass(hmc_system* s, uint32_t precision, uint32_t cooperative) {
+    if (!s) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
+    if (precision > HMC_FP32_RECHECK) return fail(HMC_INVALID_ARGUMENT, "precision");
+    if (s->interaction != HMC_HARD_SPHERE) return fail(HMC_NOT_SUPPORTED, "the cooperative pass is for hard spheres");
+    const bool fp32 = precision == HMC_FP32_RECHECK;
+    if (s->coop[fp32] != (cooperative != 0)) s->variant[fp32] = -1;  // the other pass has its own variants
+    s->coop[fp32] = cooperative != 0;
+    return HMC_OK;
+}
+
 hmc_status hmc_set_launch_variant(hmc_system* s, uint32_t precision, uint32_t index) {
     if (!s) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
     if (precision > HMC_FP32_RECHECK) return fail(HMC_INVALID_ARGUMENT, "precision");

@@ -287,6 +287,11 @@ typedef struct hmc_launch_variant {
 hmc_status hmc_get_launch_variant(hmc_system* sys, uint32_t precision, uint32_t index, hmc_launch_variant* out);
 /* index UINT32_MAX: drop the system's own choice (the recorded one for its band, else 0). */
 hmc_status hmc_set_launch_variant(hmc_system* sys, uint32_t precision, uint32_t index);
+/* Hard spheres and disks: which colour pass a precision runs, one lane per trial (cooperative = 0,
+ * the FP32 default) or the warp-cooperative pass (1, the FP64 default). Both make the same pair
+ * tests, so the trajectory does not depend on the choice; the launch variants are those of the
+ * chosen pass. HMC_NOT_SUPPORTED for other interactions. */
+hmc_status hmc_set_cooperative_pass(hmc_system* sys, uint32_t precision, uint32_t cooperative);
 /* ms_per_sweep (may be NULL): chosen->count entries, the mean time of one sweep per variant. */
 hmc_status hmc_autotune(hmc_system* sys, const hmc_sweep_params* params, uint32_t sweeps, hmc_launch_variant* chosen,
                         double* ms_per_sweep);

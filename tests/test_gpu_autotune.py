@@ -145,3 +145,17 @@ def test_lj_batch_variants_give_the_same_trajectory(ctx):
             assert [(c.accepted, c.rejected) for c in got] == [(c.accepted, c.rejected) for c in want], (precision, v)
             for k in range(len(reps)):
                 assert np.array_equal(b.positions(k), ref.positions(k)), (precision, v, k)
+
+
+@pytest.mark.parametrize("dim,n,phi", [(3, 32768, 0.5), (2, 4096, 0.7)])
+def test_cooperative_and_one_lane_passes_give_the_same_trajectory(ctx, dim, n, phi):
+    make = spheres(ctx, dim, n, phi, seed=0x5EED0025)
+    for precision in (FP64, FP32_RECHECK):
+        runs = []
+        for coop in (False, True):
+            g = make()
+            g.set_cooperative_pass(precision, coop)
+            runs.append((run(g, [(TRANSLATE, 0.2 if dim == 3 else 0.1)] * 3, precision), g.positions()))
+            g.close()
+        assert runs[0][0] == runs[1][0], precision
+        assert np.array_equal(runs[0][1], runs[1][1]), precision
