@@ -272,26 +272,42 @@ def run_replicas(args, local_rank):
     maxima = b.tune(D0, FP32_RECHECK, TARGET_ACCEPTANCE, 2000, 16)
     # the launch-shape autotuner for the replica pass (restores the state afterwards)
     chosen, ms = b.autotune(maxima, FP32_RECHECK, sweeps=2)
-    stream = torch.cuda.Stream()
-    for _ in range(args.warmup):
-        b.sweep(maxima, FP32_RECHECK, increment_step=True)
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
+
+    def timed(captured):
+        # captured: every sweep one CUDA-graph launch, all steps in one call with one wait at the
+        # end; else one call per step, each launching its kernels and waiting for its counts
+        b.set_captured_sweeps(captured)
+        for _ in range(args.warmup):
+            b.sweep(maxima, FP32_RECHECK, increment_step=True)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        launches0 = b.kernel_launches()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        trials = 0
+        if captured:
+            _, tot = b.sweep(maxima, FP32_RECHECK, n_sweeps=args.steps, increment_step=True)
+            trials = tot.total()
+        else:
+            for _ in range(args.steps):
+                _, tot = b.sweep(maxima, FP32_RECHECK, increment_step=True)
+                trials += tot.total()
+        e1.record()
+        torch.cuda.synchronize()
+        t, tr = aggregate_over_ranks(e0.elapsed_time(e1) / 1e3, trials, world, "cuda")
+        return t, tr, b.kernel_launches() - launches0
+
+    # captured first (the same sweeps after the start as the single-box headline times), then
+    # launched, then captured again: the state moves on from the lattice start, so the two
+    # captured runs bracket the launched one
     sampler = ClockSampler(local_rank)
     sampler.start()
-    launches0 = b.kernel_launches()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record()
-    trials = 0
-    for _ in range(args.steps):
-        _, tot = b.sweep(maxima, FP32_RECHECK, increment_step=True)
-        trials += tot.total()
-    e1.record()
-    torch.cuda.synchronize()
+    t_max, trials_all, launches = timed(True)
+    t_launched, trials_launched, _ = timed(False)
+    t_again, trials_again, _ = timed(True)
     clocks = sampler.stop()
-    t_max, trials_all = aggregate_over_ranks(e0.elapsed_time(e1) / 1e3, trials, world, "cuda")
     over = b.overlap_counts()
     _, over_sum = aggregate_over_ranks(0.0, int(over.sum()), world, "cuda")
     n_total = sum(n for n, _, _ in specs_all)
@@ -307,9 +323,17 @@ def run_replicas(args, local_rank):
                                    "FCC starts, per-replica move sizes tuned to 0.30, one batched ParallelSweep of "
                                    "every replica per step", "n_bodies_total": n_total, "replicas": len(specs_all),
                        "partition": f"round robin over {world} rank(s), {len(specs)} replicas on rank {rank}",
-                       "timing": "CUDA events around the batched sweep calls, max over ranks"},
+                       "timing": "CUDA events around the batched sweep calls, max over ranks",
+                       "sweeps": "captured: each sweep one CUDA-graph launch (rounds loop, origins, counts and "
+                                 "Counters on the device), the timed steps in one call",
+                       "l2": "not flushed: the batch's body arrays (about 4e6 bodies) exceed L2"},
+            "launched": {"value": trials_launched / t_launched, "ms_per_step": 1e3 * t_launched / args.steps,
+                         "what": "one hmc_batch_sweep call per step, kernels launched one by one; timed after "
+                                 "the captured steps"},
+            "captured_after": {"value": trials_again / t_again, "ms_per_step": 1e3 * t_again / args.steps,
+                               "what": "captured again, after the launched steps"},
             "launch_variant": {"chosen": chosen, "ms_per_sweep": [round(float(x), 4) for x in ms]},
-            "overlaps_after": over_sum, "gpu_launches": b.kernel_launches() - launches0, "clocks": clocks,
+            "overlaps_after": over_sum, "gpu_launches": launches, "clocks": clocks,
             "sdf_pressure": {"estimator": "beta P per replica from its scale distribution (x_max 0.02, 40 bins), "
                                           "after the timed sweeps (rank 0's replicas)", "min": float(pressures.min()),
                              "median": float(np.median(pressures)), "max": float(pressures.max()),
@@ -356,6 +380,9 @@ def run_lj_replicas(args, local_rank):
             b.sweep(d, precision, increment_step=True, temperatures=kts)
         # the launch-shape autotuner for the replica pass (restores the state afterwards)
         tuned[precision] = b.autotune(d, precision, sweeps=2, temperatures=kts)
+        # every sweep one CUDA-graph launch, the timed steps in one call with one wait at the end
+        b.set_captured_sweeps(True)
+        b.sweep(d, precision, increment_step=True, temperatures=kts)  # builds the graph
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
@@ -363,10 +390,8 @@ def run_lj_replicas(args, local_rank):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record()
-        trials = 0
-        for _ in range(steps):
-            _, tot = b.sweep(d, precision, increment_step=True, temperatures=kts)
-            trials += tot.total()
+        _, tot = b.sweep(d, precision, n_sweeps=steps, increment_step=True, temperatures=kts)
+        trials = tot.total()
         e1.record()
         torch.cuda.synchronize()
         el, trials_all = aggregate_over_ranks(e0.elapsed_time(e1) / 1e3, trials, world, "cuda")
@@ -415,7 +440,10 @@ def run_lj_replicas(args, local_rank):
             "config": {"workload": "64 Lennard-Jones boxes of 8192 bodies, rho 0.8, eps = sigma = 1, "
                                    "r_cut = r_shift = 2.5, kT_k ~ U[0.8, 2.0], FCC + 0.01 jitter, translation 0.1, "
                                    "one batched ParallelSweep of every replica per step", "n_bodies_total": n * n_rep,
-                       "replicas": n_rep, "timing": "CUDA events around the batched sweep calls"},
+                       "replicas": n_rep, "timing": "CUDA events around the batched sweep calls",
+                       "sweeps": "captured: each sweep one CUDA-graph launch, the timed steps in one call",
+                       "l2": "not flushed between sweeps (the timed steps run in one call); the batch's arrays "
+                             "(524288 bodies, about 70 MB) fit in L2"},
             "fp64": {"value": v64, "ms_per_step": ms64},
             "mismatches": int(sum(np.count_nonzero(np.any(a != b, axis=1)) for a, b in zip(p32, p64))),
             "one_system_after_another": {"value": v_single, "precision": "fp32_recheck"},

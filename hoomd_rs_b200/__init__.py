@@ -185,6 +185,7 @@ SIGNATURES = {
     "hmc_batch_autotune": (C.c_int, [_vp, C.POINTER(hmc_sweep_params), C.c_uint32, C.POINTER(hmc_launch_variant),
                                      _dp]),
     "hmc_batch_set_launch_variant": (C.c_int, [_vp, C.c_uint32, C.c_uint32]),
+    "hmc_batch_set_captured_sweeps": (C.c_int, [_vp, C.c_uint32]),
     "hmc_total_energy": (C.c_int, [_vp, _dp]),
     "hmc_overlap_count_noalloc": (C.c_int, [_vp, C.c_uint64, C.c_uint32, _dp, C.c_double, C.c_double, _vp, _vp]),
     "hmc_quick_insert_apply": (C.c_int, [_vp, C.POINTER(hmc_quick_insert), C.POINTER(hmc_count)]),
@@ -1231,6 +1232,11 @@ class Batch:
 
     def set_launch_variant(self, precision: int, index: Optional[int]):
         _check(_lib.hmc_batch_set_launch_variant(self._h, precision, 0xFFFFFFFF if index is None else index))
+
+    def set_captured_sweeps(self, enable: bool = True):
+        """hmc_batch_set_captured_sweeps: each sweep as one CUDA-graph launch, the sweeps of a call
+        back to back with one wait at the end (same trajectory as the launched sweeps)."""
+        _check(_lib.hmc_batch_set_captured_sweeps(self._h, 1 if enable else 0))
 
     def sdf(self, x_max: float = 0.02, n_bins: int = 40) -> np.ndarray:
         """Scale distributions of all replicas (hard spheres): (n_replicas, n_bins) pair counts."""

@@ -2074,6 +2074,18 @@ struct hmc_batch {
     uint32_t rounds_guess = 2;
     uint32_t interaction = HMC_HARD_SPHERE;  // the same for every replica
     std::vector<double> body_range;          // [R] ParallelSweep range of each replica
+    // captured sweeps (hmc_batch_set_captured_sweeps): one sweep as a CUDA graph, built for a
+    // precision, launch variant and increment_step (graph_key), launched once per sweep
+    bool captured = false;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    uint32_t graph_key = UINT32_MAX;
+    cudaStream_t body_stream = nullptr;             // captures the rounds loop's body
+    uint32_t* round_dev = nullptr;                  // the colour set the captured passes run
+    unsigned long long* rep_counts = nullptr;       // [2R] accepted, rejected per replica
+    BatchSweepTotals* totals = nullptr;
+    unsigned long long* host_rep_counts = nullptr;  // pinned [2R]
+    BatchSweepTotals* host_totals = nullptr;        // pinned
 };
 
 namespace {
@@ -2128,6 +2140,156 @@ hmc_status batch_read(hmc_batch* bt) {
     return HMC_OK;
 }
 
+// The colour passes of one set of a batch sweep, every colour, on stream s.
+hmc_status batch_enqueue_colours(hmc_batch* bt, bool fp32, uint32_t round, bool first, uint32_t variant,
+                                 cudaStream_t s) {
+    const uint32_t colors = 1u << bt->dim;
+    for (uint32_t c = 0; c < colors; ++c) {
+        const bool overlap = !first || c > 0, early = first && c == 0;
+        if (bt->interaction == HMC_LENNARD_JONES)
+            HMC_CUDA(launch_sweep_batch_lj(bt->dim, fp32, bt->b, bt->arr, c, round, bt->b.color_stride, overlap, early,
+                                           s, variant));
+        else
+            HMC_CUDA(launch_sweep_batch(bt->dim, fp32, bt->b, bt->arr, c, round, bt->b.color_stride, overlap, early, s,
+                                        variant));
+    }
+    return HMC_OK;
+}
+
+void batch_drop_graph(hmc_batch* bt) {
+    if (bt->graph_exec) cudaGraphExecDestroy(bt->graph_exec);
+    if (bt->graph) cudaGraphDestroy(bt->graph);
+    bt->graph_exec = nullptr;
+    bt->graph = nullptr;
+    bt->graph_key = UINT32_MAX;
+}
+
+// One batch sweep as a CUDA graph, built by stream capture: every replica's origin from its
+// Counter (k_batch_origins), the batched rebuild, the per-replica rounds, a while node whose body
+// is one colour set (the passes read the set from round_dev; k_batch_round_next advances it and
+// sets the condition), and the bookkeeping (k_batch_sweep_end). The graph reads and writes device
+// memory only, so the sweeps of a call are launched back to back and the host waits once.
+hmc_status batch_build_graph(hmc_batch* bt, bool fp32, uint32_t variant, bool increment_step) {
+    batch_drop_graph(bt);
+    if (!bt->body_stream) HMC_CUDA(cudaStreamCreateWithFlags(&bt->body_stream, cudaStreamNonBlocking));
+    cudaGraph_t g = nullptr;
+    HMC_CUDA(cudaGraphCreate(&g, 0));
+    bt->graph = g;
+    cudaGraphConditionalHandle h;
+    HMC_CUDA(cudaGraphConditionalHandleCreate(&h, g, 0, 0));
+    cudaStream_t cs = bt->stream;
+    Replica* rep = const_cast<Replica*>(bt->b.rep);
+    // an error inside a capture leaves the stream capturing: end it before returning
+    auto capture = [&](cudaStream_t st, auto&& body) -> hmc_status {
+        hmc_status r = body();
+        cudaGraph_t out = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(st, &out);
+        if (r != HMC_OK) return r;
+        if (e != cudaSuccess) return fail(HMC_CUDA_ERROR, "captured sweep: %s", cudaGetErrorString(e));
+        return HMC_OK;
+    };
+    HMC_CUDA(cudaStreamBeginCaptureToGraph(cs, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    hmc_status st = capture(cs, [&]() -> hmc_status {
+        HMC_CUDA(cudaMemsetAsync(bt->arr.stats, 0, sizeof(DeviceStats), cs));
+        HMC_CUDA(launch_batch_origins(bt->dim, bt->b, rep, cs));
+        HMC_CUDA(launch_rebuild_batch(bt->dim, bt->b, bt->arr, (uint32_t)bt->n, !fp32, cs));
+        HMC_CUDA(launch_batch_rounds(bt->b, rep, bt->arr.stats, cs));
+        HMC_CUDA(cudaMemsetAsync(bt->b.accepted, 0, sizeof(unsigned long long) * bt->n_rep, cs));
+        HMC_CUDA(launch_batch_round_first(h, bt->arr.stats, bt->round_dev, bt->totals, cs));
+        // the rounds loop
+        cudaStreamCaptureStatus cst;
+        cudaGraph_t cg = nullptr;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t n_deps = 0;
+        HMC_CUDA(cudaStreamGetCaptureInfo(cs, &cst, nullptr, &cg, &deps, &n_deps));
+        cudaGraphNodeParams cp{};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t loop;
+        HMC_CUDA(cudaGraphAddNode(&loop, cg, deps, n_deps, &cp));
+        HMC_CUDA(cudaStreamUpdateCaptureDependencies(cs, &loop, 1, cudaStreamSetCaptureDependencies));
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        HMC_CUDA(cudaStreamBeginCaptureToGraph(bt->body_stream, body, nullptr, nullptr, 0,
+                                               cudaStreamCaptureModeThreadLocal));
+        hmc_status sb = capture(bt->body_stream, [&]() -> hmc_status {
+            hmc_status r = batch_enqueue_colours(bt, fp32, kRoundFromDevice, true, variant, bt->body_stream);
+            if (r) return r;
+            HMC_CUDA(launch_batch_round_next(h, bt->arr.stats, bt->round_dev, bt->body_stream));
+            return HMC_OK;
+        });
+        if (sb) return sb;
+        HMC_CUDA(launch_batch_sweep_end(bt->b, rep, bt->arr.stats, bt->rep_counts, bt->totals, increment_step, cs));
+        return HMC_OK;
+    });
+    if (st) {
+        batch_drop_graph(bt);
+        return st;
+    }
+    cudaGraphExec_t x = nullptr;
+    const cudaError_t e = cudaGraphInstantiate(&x, g, 0);
+    if (e != cudaSuccess) {
+        batch_drop_graph(bt);
+        return fail(HMC_CUDA_ERROR, "captured sweep: cudaGraphInstantiate: %s", cudaGetErrorString(e));
+    }
+    bt->graph_exec = x;
+    bt->graph_key = (fp32 ? 1u : 0u) | (increment_step ? 2u : 0u) | (variant << 2);
+    return HMC_OK;
+}
+
+// n_sweeps batch sweeps through the captured graph: the replica table up, one graph launch per
+// sweep, then the counts, the statistics and the replica table (Counters, rounds) down with one
+// wait. Decisions, counts and Counters equal the launched sweep's.
+hmc_status batch_sweep_captured(hmc_batch* bt, const hmc_sweep_params& p0, bool fp32, uint32_t variant,
+                                hmc_count* counts, hmc_count* total) {
+    const uint32_t key = (fp32 ? 1u : 0u) | (p0.increment_step ? 2u : 0u) | (variant << 2);
+    if (!bt->graph_exec || bt->graph_key != key) {
+        hmc_status st = batch_build_graph(bt, fp32, variant, p0.increment_step != 0);
+        if (st) return st;
+    }
+    hmc_status st = batch_upload_replicas(bt);
+    if (st) return st;
+    HMC_CUDA(cudaMemsetAsync(bt->rep_counts, 0, sizeof(unsigned long long) * 2 * bt->n_rep, bt->stream));
+    HMC_CUDA(cudaMemsetAsync(bt->totals, 0, sizeof(BatchSweepTotals), bt->stream));
+    for (uint32_t sweep = 0; sweep < p0.n_sweeps; ++sweep) HMC_CUDA(cudaGraphLaunch(bt->graph_exec, bt->stream));
+    HMC_CUDA(cudaMemcpyAsync(bt->host_totals, bt->totals, sizeof(BatchSweepTotals), cudaMemcpyDeviceToHost,
+                             bt->stream));
+    HMC_CUDA(cudaMemcpyAsync(bt->host_rep_counts, bt->rep_counts, sizeof(unsigned long long) * 2 * bt->n_rep,
+                             cudaMemcpyDeviceToHost, bt->stream));
+    HMC_CUDA(cudaMemcpyAsync(bt->rep_pinned, bt->b.rep, sizeof(Replica) * bt->n_rep, cudaMemcpyDeviceToHost,
+                             bt->stream));
+    HMC_CUDA(cudaStreamSynchronize(bt->stream));
+    std::memcpy(bt->rep.data(), bt->rep_pinned, sizeof(Replica) * bt->n_rep);
+    const BatchSweepTotals& t = *bt->host_totals;
+    // kernels: origins, the rebuild's six, rounds, the first test and the end per sweep; the
+    // colour passes and the step per colour set
+    const uint64_t per_sweep = bt->n > 0 ? 10 : 6;
+    bt->kernel_launches += per_sweep * p0.n_sweeps + t.colour_sets * ((1u << bt->dim) + 1);
+    const uint32_t f = t.error_flags;
+    if (f & kErrNonFinite) return fail(HMC_NAN_STATE, "a body position is not finite");
+    if (f & kErrOutsideCheckerboard) return fail(HMC_OUTSIDE_CHECKERBOARD, "a body maps to no checkerboard space");
+    hmc_count tot{};
+    for (uint32_t k = 0; k < bt->n_rep; ++k) {
+        const uint64_t acc = bt->host_rep_counts[2 * k], rej = bt->host_rep_counts[2 * k + 1];
+        if (counts) {
+            counts[k].accepted += acc;
+            counts[k].rejected += rej;
+        }
+        tot.accepted += acc;
+        tot.rejected += rej;
+    }
+    tot.rechecks = t.rechecks;
+    tot.pair_checks = t.pair_checks;
+    tot.order_ambiguous = t.ambiguous;
+    double me;
+    unsigned long long bits = t.max_err_bits;
+    std::memcpy(&me, &bits, 8);
+    tot.max_fp32_error = me;
+    if (total) *total = tot;
+    return HMC_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -2142,6 +2304,11 @@ void hmc_batch_destroy(hmc_batch* bt) {
     if (bt->host_rep_u64) cudaFreeHost(bt->host_rep_u64);
     if (bt->host_nonempty) cudaFreeHost(bt->host_nonempty);
     if (bt->host_first_bad) cudaFreeHost(bt->host_first_bad);
+    if (bt->host_rep_counts) cudaFreeHost(bt->host_rep_counts);
+    if (bt->host_totals) cudaFreeHost(bt->host_totals);
+    if (bt->graph_exec) cudaGraphExecDestroy(bt->graph_exec);
+    if (bt->graph) cudaGraphDestroy(bt->graph);
+    if (bt->body_stream) cudaStreamDestroy(bt->body_stream);
     if (bt->stream) cudaStreamDestroy(bt->stream);
     cudaGetLastError();
     hmc_context* c = bt->ctx;
@@ -2266,6 +2433,9 @@ hmc_status hmc_batch_create(hmc_context* ctx, uint32_t n_replicas, const hmc_sys
     if (e == cudaSuccess) e = cudaMallocHost((void**)&bt->host_rep_u64, sizeof(unsigned long long) * n_replicas);
     if (e == cudaSuccess) e = cudaMallocHost((void**)&bt->host_nonempty, sizeof(unsigned int) * n_replicas);
     if (e == cudaSuccess) e = cudaMallocHost((void**)&bt->host_first_bad, sizeof(unsigned long long));
+    if (e == cudaSuccess)
+        e = cudaMallocHost((void**)&bt->host_rep_counts, sizeof(unsigned long long) * 2 * (size_t)n_replicas);
+    if (e == cudaSuccess) e = cudaMallocHost((void**)&bt->host_totals, sizeof(BatchSweepTotals));
     if (e != cudaSuccess) {
         fail(HMC_CUDA_ERROR, "batch setup: %s", cudaGetErrorString(e));
         return destroy_fail(HMC_CUDA_ERROR);
@@ -2287,8 +2457,10 @@ hmc_status hmc_batch_create(hmc_context* ctx, uint32_t n_replicas, const hmc_sys
         (st = balloc(bt, &d_body_rep, n)) || (st = balloc(bt, &bt->b.color_rep, cells)) ||
         (st = balloc(bt, &bt->b.accepted, n_replicas)) || (st = balloc(bt, &bt->b.nonempty, n_replicas)) ||
         (st = balloc(bt, &bt->b.overlaps, n_replicas)) || (st = balloc(bt, &bt->stage, n * dim)) ||
-        (st = balloc(bt, &bt->first_bad, 1)))
+        (st = balloc(bt, &bt->first_bad, 1)) || (st = balloc(bt, &bt->round_dev, 1)) ||
+        (st = balloc(bt, &bt->rep_counts, 2 * (size_t)n_replicas)) || (st = balloc(bt, &bt->totals, 1)))
         return destroy_fail(st);
+    bt->b.round_dev = bt->round_dev;
     A.body_ori = nullptr;
     A.sorted_q = nullptr;
     A.zig_x = ctx->zig;
@@ -2364,6 +2536,7 @@ hmc_status hmc_batch_sweep(hmc_batch* bt, const hmc_sweep_params* params, hmc_co
     const uint32_t colors = 1u << bt->dim;
     const uint32_t variant = batch_variant_of(bt, fp32);
     if (counts) std::memset(counts, 0, sizeof(hmc_count) * bt->n_rep);
+    if (bt->captured) return batch_sweep_captured(bt, p0, fp32, variant, counts, total);
     hmc_count tot{};
     for (uint32_t sweep = 0; sweep < p0.n_sweeps; ++sweep) {
         hmc_status st = batch_rebuild(bt, !fp32);
@@ -2421,6 +2594,12 @@ hmc_status hmc_batch_sweep(hmc_batch* bt, const hmc_sweep_params* params, hmc_co
         tot.max_fp32_error = std::max(tot.max_fp32_error, me);
     }
     if (total) *total = tot;
+    return HMC_OK;
+}
+
+hmc_status hmc_batch_set_captured_sweeps(hmc_batch* bt, uint32_t enable) {
+    if (!bt) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
+    bt->captured = enable != 0;
     return HMC_OK;
 }
 

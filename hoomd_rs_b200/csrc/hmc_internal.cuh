@@ -359,9 +359,27 @@ struct Batch {
     unsigned long long* accepted;   // [R] per sweep
     unsigned int* nonempty;         // [R] after a rebuild
     unsigned long long* overlaps;   // [R] overlap check
+    const uint32_t* round_dev;      // the colour set a pass launched with kRoundFromDevice runs
     uint32_t n_replicas;
     uint32_t n_cells;               // all replicas
     uint32_t color_stride;          // capacity of one colour's list
+};
+// The round argument of a batch pass that reads its colour set from Batch::round_dev (the passes
+// of a captured sweep, whose rounds loop runs on the device).
+constexpr uint32_t kRoundFromDevice = 0xffffffffu;
+
+// What the sweeps of one captured-sweep call add up on the device: per replica the accepted and
+// rejected moves (rep_counts[2 r], [2 r + 1]), and for the batch the sums of the per-sweep
+// statistics, the error flags of every sweep, and the sweeps that ran.
+struct BatchSweepTotals {
+    unsigned long long rechecks;
+    unsigned long long pair_checks;
+    unsigned long long ambiguous;
+    unsigned long long max_err_bits;
+    unsigned long long sweeps;
+    unsigned long long colour_sets;  // the colour sets (rounds) run, summed over the sweeps
+    unsigned int error_flags;
+    unsigned int pad;
 };
 
 // Kernel launchers (hmc_kernels.cu). All return cudaGetLastError() after enqueueing.
@@ -373,6 +391,17 @@ cudaError_t launch_rebuild(int dim, const Geometry& g, const Arrays& a, uint32_t
                            bool write_slots = true);
 // Per-replica rounds of a batch sweep into Replica::rounds, their maximum into DeviceStats::rounds.
 cudaError_t launch_batch_rounds(const Batch& b, Replica* rep, DeviceStats* stats, cudaStream_t s);
+// The device side of a captured batch sweep: every replica's checkerboard origin from its own
+// Counter (update_checkerboard); the rounds loop's first test and its step to the next colour
+// set (a while node's condition); each replica's counts and Counter after the sweep.
+cudaError_t launch_batch_origins(int dim, const Batch& b, Replica* rep, cudaStream_t s);
+cudaError_t launch_batch_round_first(cudaGraphConditionalHandle h, const DeviceStats* stats, uint32_t* round_dev,
+                                     const BatchSweepTotals* totals, cudaStream_t s);
+cudaError_t launch_batch_round_next(cudaGraphConditionalHandle h, const DeviceStats* stats, uint32_t* round_dev,
+                                    cudaStream_t s);
+cudaError_t launch_batch_sweep_end(const Batch& b, Replica* rep, const DeviceStats* stats,
+                                   unsigned long long* rep_counts, BatchSweepTotals* totals, bool increment_step,
+                                   cudaStream_t s);
 // Batches of replicas: the rebuild and the hard-sphere colour pass over all replicas at once.
 cudaError_t launch_rebuild_batch(int dim, const Batch& b, const Arrays& a, uint32_t n, bool write_s, cudaStream_t s);
 cudaError_t launch_sweep_batch(int dim, bool fp32, const Batch& b, const Arrays& a, uint32_t color, uint32_t round,

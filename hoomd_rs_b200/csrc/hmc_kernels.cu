@@ -1219,6 +1219,7 @@ template <int DIM, bool FP32, int MINB = HMC_BATCH_MIN_BLOCKS>
 __global__ void __launch_bounds__(128, MINB) k_sweep_batch(Batch B, Arrays A, uint32_t color,
                                                                              uint32_t round, uint32_t early_wait) {
     if (early_wait) grid_dependency_wait();  // first pass: the rebuild's arrays are read at once
+    if (round == kRoundFromDevice) round = *B.round_dev;  // a captured sweep's rounds loop
     const uint32_t n_active = active_count(A, color, round);
     uint32_t n_accepted = 0;
     PairStats st;
@@ -1288,6 +1289,70 @@ __global__ void __launch_bounds__(128, MINB) k_sweep_batch(Batch B, Arrays A, ui
     grid_dependency_wait();
     allow_dependent_launch();
     flush_stats(A.stats, st, n_accepted);
+}
+
+// update_checkerboard's origin shift (parallel_sweep.rs:176-190) for every replica from its own
+// Counter's index u64::MAX stream: the host's computation, on the device.
+template <int DIM>
+__global__ void k_batch_origins(Batch B, Replica* rep) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= B.n_replicas) return;
+    Replica& R = rep[r];
+    Sfc64 rng = make_rng(R.step, R.substep, R.seed, UINT64_MAX);
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) {
+        const double off = uniform01(rng);
+        R.g.origin[a] = dsub(-R.g.L[a] / 2.0, dmul(off, R.g.width[a]));
+    }
+}
+
+// The first test of a captured sweep's rounds loop: colour set 0 runs when some replica has a
+// round and no earlier sweep of the call (nor this sweep's rebuild) flagged an error.
+__global__ void k_batch_round_first(cudaGraphConditionalHandle h, const DeviceStats* stats, uint32_t* round_dev,
+                                    const BatchSweepTotals* totals) {
+    *round_dev = 0;
+    cudaGraphSetConditional(h, stats->rounds > 0u && stats->error_flags == 0u && totals->error_flags == 0u);
+}
+
+// The end of one colour set of a captured sweep: the next runs while the sweep has rounds left.
+__global__ void k_batch_round_next(cudaGraphConditionalHandle h, const DeviceStats* stats, uint32_t* round_dev) {
+    const uint32_t next = *round_dev + 1u;
+    *round_dev = next;
+    cudaGraphSetConditional(h, next < stats->rounds);
+}
+
+// The host's bookkeeping after a batch sweep, on the device: per replica its trials
+// (rounds x non-empty spaces) split into accepted and rejected, and its Counter
+// (increment_substep per colour set, then increment_step); for the batch the sweep's statistics.
+// A sweep whose rebuild flagged an error (or that follows one) ran no pass and changes nothing
+// but the flags.
+__global__ void k_batch_sweep_end(Batch B, Replica* rep, const DeviceStats* stats, unsigned long long* rep_counts,
+                                  BatchSweepTotals* totals, uint32_t increment_step) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    // (thread 0 adds only this sweep's flags, which every thread reads itself)
+    const bool failed = stats->error_flags != 0u || totals->error_flags != 0u;
+    if (r == 0) {
+        totals->error_flags |= stats->error_flags;
+        if (!failed) {
+            totals->rechecks += stats->rechecks;
+            totals->pair_checks += stats->pair_checks;
+            totals->ambiguous += stats->ambiguous;
+            if (stats->max_err_bits > totals->max_err_bits) totals->max_err_bits = stats->max_err_bits;
+            totals->sweeps += 1;
+            totals->colour_sets += stats->rounds;
+        }
+    }
+    if (failed || r >= B.n_replicas) return;
+    Replica& R = rep[r];
+    const unsigned long long acc = B.accepted[r];
+    const unsigned long long trials = (unsigned long long)R.rounds * B.nonempty[r];
+    rep_counts[2 * r] += acc;
+    rep_counts[2 * r + 1] += trials - acc;
+    R.substep += R.rounds;
+    if (increment_step) {
+        R.step += 1;
+        R.substep = 0;
+    }
 }
 
 // Rounds of every replica (ceil(N_r / non-empty spaces of r)) and their maximum.
@@ -1622,6 +1687,34 @@ cudaError_t launch_sweep_batch(int dim, bool fp32, const Batch& b, const Arrays&
 
 cudaError_t launch_batch_rounds(const Batch& b, Replica* rep, DeviceStats* stats, cudaStream_t s) {
     k_batch_rounds<<<blocks_for(b.n_replicas, 128), 128, 0, s>>>(b, rep, stats);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_origins(int dim, const Batch& b, Replica* rep, cudaStream_t s) {
+    if (dim == 2)
+        k_batch_origins<2><<<blocks_for(b.n_replicas, 128), 128, 0, s>>>(b, rep);
+    else
+        k_batch_origins<3><<<blocks_for(b.n_replicas, 128), 128, 0, s>>>(b, rep);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_round_first(cudaGraphConditionalHandle h, const DeviceStats* stats, uint32_t* round_dev,
+                                     const BatchSweepTotals* totals, cudaStream_t s) {
+    k_batch_round_first<<<1, 1, 0, s>>>(h, stats, round_dev, totals);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_round_next(cudaGraphConditionalHandle h, const DeviceStats* stats, uint32_t* round_dev,
+                                    cudaStream_t s) {
+    k_batch_round_next<<<1, 1, 0, s>>>(h, stats, round_dev);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_sweep_end(const Batch& b, Replica* rep, const DeviceStats* stats,
+                                   unsigned long long* rep_counts, BatchSweepTotals* totals, bool increment_step,
+                                   cudaStream_t s) {
+    k_batch_sweep_end<<<blocks_for(b.n_replicas, 128), 128, 0, s>>>(b, rep, stats, rep_counts, totals,
+                                                                      increment_step ? 1u : 0u);
     return cudaGetLastError();
 }
 

@@ -519,6 +519,7 @@ template <int DIM, int MINB = HMC_LJ_BATCH_MIN_BLOCKS>
 __global__ void __launch_bounds__(128, MINB)
     k_sweep_batch_lj(Batch B, Arrays A, uint32_t color, uint32_t round, uint32_t early_wait) {
     if (early_wait) grid_dependency_wait();  // first pass: the rebuild's arrays are read at once
+    if (round == kRoundFromDevice) round = *B.round_dev;  // a captured sweep's rounds loop
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t n_warps = (gridDim.x * blockDim.x) >> 5;
@@ -585,6 +586,7 @@ template <int DIM, int MINB = HMC_LJ_BATCH_MIN_BLOCKS>
 __global__ void __launch_bounds__(128, MINB)
     k_sweep_batch_lj32(Batch B, Arrays A, uint32_t color, uint32_t round, uint32_t early_wait) {
     if (early_wait) grid_dependency_wait();  // first pass: the rebuild's arrays are read at once
+    if (round == kRoundFromDevice) round = *B.round_dev;  // a captured sweep's rounds loop
     __shared__ double s_e[kRecheckChunks][2][32];
     __shared__ SharedTrial s_trial;
     __shared__ uint32_t s_active, s_rep;

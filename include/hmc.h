@@ -360,6 +360,14 @@ void hmc_batch_destroy(hmc_batch* batch);
  * may be NULL) receive accepted/rejected; total (may be NULL) also receives the batch's
  * rechecks, pair_checks and max_fp32_error. */
 hmc_status hmc_batch_sweep(hmc_batch* batch, const hmc_sweep_params* params, hmc_count* counts, hmc_count* total);
+/* enable = 1: hmc_batch_sweep runs each sweep as one launch of a CUDA graph (built on first use
+ * for the precision, launch variant and increment_step, rebuilt when they change): the origins of
+ * the replicas' checkerboards, the rebuild, the rounds (a while node over the colour sets) and the
+ * per-replica counts and Counters all stay on the device, so the n_sweeps sweeps of one call are
+ * launched back to back and the host waits once, at the end. Decisions, counts and Counters are
+ * the launched sweep's (enable = 0, the default). A sweep whose rebuild flags an error runs no
+ * colour pass, nor do the later sweeps of the call; the call then returns the error. */
+hmc_status hmc_batch_set_captured_sweeps(hmc_batch* batch, uint32_t enable);
 hmc_status hmc_batch_get_state(hmc_batch* batch, uint32_t replica, double* positions, uint64_t* step,
                                uint32_t* substep);
 hmc_status hmc_batch_set_state(hmc_batch* batch, uint32_t replica, const double* positions, uint64_t step,
