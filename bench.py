@@ -38,9 +38,13 @@ SEED = 0x5EED0002
 TARGET_ACCEPTANCE = 0.30
 
 
-# DRAM bytes of one FP32 colour pass of this workload, read + written, from one ncu capture of
-# the pass (dram__bytes_read.sum + dram__bytes_write.sum): 30.72 MB + 0.04 MB.
-SPHERE_PASS_DRAM_BYTES = 30.76e6
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of the FP32 colour passes of this
+# workload from ncu. As the passes run, caches kept (--cache-control none): 88-97 MB over the 16
+# passes of a sweep, a mean of 5.7 MB per pass (the first pass after the rebuild about 27 MB, the
+# others 4.1-4.7 MB from L2 misses). One pass with the caches flushed first (ncu's default):
+# 30.72 MB read + 0.04 MB written.
+SPHERE_PASS_DRAM_BYTES = 5.7e6
+SPHERE_PASS_DRAM_BYTES_COLD = 30.76e6
 
 
 def aggregate_over_ranks(elapsed, units, world, device):
@@ -864,7 +868,9 @@ def main():
         "recheck_fraction": ra["rechecks"] / max(ra["pair_checks"], 1), "max_fp32_error": ra["max_err"],
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": SPHERE_PASS_DRAM_BYTES, "kernel": "k_sweep_sphere<3,fp32>",
-                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one FP32 colour pass",
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per FP32 colour pass, "
+                                       "mean over the 16 passes of a sweep as they run (--cache-control none)",
+                     "traffic_cold": SPHERE_PASS_DRAM_BYTES_COLD,
                      "bytes_per_launch": bytes_per_launch, "launch_ms": t_launch * 1e3,
                      "peak_source": f"{peak_kind} hbm_gbs"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": N_BODIES * 3 * 8,
