@@ -565,6 +565,8 @@ def run_config(args, local_rank):
         for _ in range(args.warmup):
             for mv, mx in moves:
                 m.sweep(mv, mx, 1.0, precision, n_sweeps=1, increment_step=True)
+        # the launch-shape autotuner on the first move (restores the state afterwards)
+        chosen, ms_var = m.autotune(moves[0][0], moves[0][1], 1.0, precision, sweeps=2)
         ms, trials, acc, rech, checks, amb = 0.0, 0, 0, 0, 0, 0
         launches0 = m.profile()["kernel_launches"]
         for _ in range(args.steps):
@@ -585,7 +587,8 @@ def run_config(args, local_rank):
             ms += e0.elapsed_time(e1)
         out = {"value": trials / (ms / 1e3), "ms_per_step": ms / args.steps, "acceptance": acc / max(trials, 1),
                "recheck_fraction": rech / max(checks, 1), "launches": m.profile()["kernel_launches"] - launches0,
-               "order_ambiguous": amb}
+               "order_ambiguous": amb,
+               "launch_variant": {"chosen": chosen, "ms_per_sweep": [round(float(x), 4) for x in ms_var]}}
         pos_end = m.positions()
         m.close()
         return out, pos_end
@@ -604,7 +607,8 @@ def run_config(args, local_rank):
             "mismatches": int(np.count_nonzero(np.any(p32 != p64, axis=1))), "acceptance": r32["acceptance"],
             "recheck_fraction": r32["recheck_fraction"], "gpu_launches": r32["launches"], "clocks": clocks,
             "order_ambiguous": {"fp32_recheck": r32["order_ambiguous"], "fp64": r64["order_ambiguous"],
-                                "what": "decisions another summation order of the FP64 pair energies could change"}}
+                                "what": "decisions another summation order of the FP64 pair energies could change"},
+            "launch_variants": {"fp32_recheck": r32["launch_variant"], "fp64": r64["launch_variant"]}}
     if not args.no_cpu_baseline:
         threads = host_threads()
         o = oracle.System(dim, [L] * dim, pos, ori, seed=seed, **okw)

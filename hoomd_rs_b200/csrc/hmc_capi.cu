@@ -947,6 +947,7 @@ hmc_status hmc_sweep(hmc_system* s, const hmc_sweep_params* p, hmc_count* out) {
         L.n_bodies = (uint32_t)s->n;
         L.n_active = s->geom.color_stride;  // grid bound; the kernels read the list lengths
         const uint32_t variant = variant_of(s, fp32);
+        const bool poly2_fp32 = fp32 && variant == 0;  // polygon variant 1: the FP64 pass in both modes
         if (s->profiling) HMC_CUDA(cudaEventRecord(s->ev[2], s->stream));
         // The rounds (while count.total() < N, :402-418) are known on the device after the
         // rebuild; the host enqueues the previous sweep's number of colour sets without
@@ -965,8 +966,8 @@ hmc_status hmc_sweep(hmc_system* s, const hmc_sweep_params* p, hmc_count* out) {
                                                  s->shape_soft, s->stream));
                     s->prof.kernel_launches += 1;
                 } else if (s->polygon()) {
-                    HMC_CUDA(launch_propose_poly2(fp32 && !s->shape_soft, s->geom, s->arr, L, p->move == HMC_ROTATE,
-                                                  s->shape_soft, s->stream));
+                    HMC_CUDA(launch_propose_poly2(poly2_fp32 && !s->shape_soft, s->geom, s->arr, L,
+                                                  p->move == HMC_ROTATE, s->shape_soft, s->stream));
                     s->prof.kernel_launches += 1;
                 }
                 for (uint32_t c = 0; c < colors; ++c) {
@@ -989,7 +990,7 @@ hmc_status hmc_sweep(hmc_system* s, const hmc_sweep_params* p, hmc_count* out) {
                                                    s->poly_rcut2_hi32, L, p->move == HMC_ROTATE, s->stream,
                                                    variant));
                     else if (s->polygon())
-                        HMC_CUDA(launch_sweep_poly2(fp32, s->sat(), s->geom, s->arr, s->verts, s->n_vertices,
+                        HMC_CUDA(launch_sweep_poly2(poly2_fp32, s->sat(), s->geom, s->arr, s->verts, s->n_vertices,
                                                     s->poly_rcut2, s->poly_rcut2_hi32, L, p->move == HMC_ROTATE,
                                                     s->stream));
                     else

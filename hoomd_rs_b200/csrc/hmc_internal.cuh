@@ -298,7 +298,10 @@ constexpr LaunchShape kSphereCoopShapes[] = {{6, 1, 2}, {6, 1, 1}, {6, 1, 3}, {5
 constexpr LaunchShape kLjShapes[] = {{9, 1, 0}, {7, 1, 0}, {11, 1, 0}};
 constexpr LaunchShape kPolyShapes[] = {{5, 4, 0}, {5, 2, 0}, {5, 8, 0}};
 constexpr LaunchShape kBatchShapes[] = {{4, 1, 0}, {3, 1, 0}, {5, 1, 0}, {6, 1, 0}, {7, 1, 0}, {8, 1, 0}};
-constexpr LaunchShape kPoly2Shapes[] = {{8, 4, 0}};    // the polygon pass: one compiled shape
+// The polygon pass: one compiled shape; in the FP32 mode, variant 1 runs the FP64 pass instead
+// of the FP32 prefilter (the same decisions; the prefilter saves little where the FP64
+// circumsphere test is cheap against the separating-axis or XenoCollide test behind it).
+constexpr LaunchShape kPoly2Shapes[] = {{8, 4, 0}, {8, 4, 0}};
 constexpr LaunchShape kBatchLjShapes[] = {{7, 1, 0}, {9, 1, 0}, {5, 1, 0}};  // the Lennard-Jones replica passes
 template <size_t N>
 constexpr uint32_t n_shapes(const LaunchShape (&)[N]) {

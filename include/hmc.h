@@ -269,8 +269,9 @@ hmc_status hmc_total_energy(hmc_system* sys, double* energy);
  * Every colour-pass kernel is compiled in a few launch shapes: the resident blocks per SM it
  * is built for (its register cap), the trials a warp takes (convex polyhedra: 4, 2 or 8) and,
  * for the warp-cooperative FP64 sphere pass, the candidates per stencil row a lane tests before
- * handing the rest to its warp. All make the same pair tests, so the trajectory is the same in
- * every variant; only the speed differs, by shape and density. hmc_autotune times `sweeps`
+ * handing the rest to its warp; for convex polygons in HMC_FP32_RECHECK, variant 1 runs the FP64
+ * pass instead of the FP32 prefilter. All take the same decisions, so the trajectory is the same
+ * in every variant; only the speed differs, by shape and density. hmc_autotune times `sweeps`
  * sweeps of the system in every variant of its pass (precision and move from params), each from
  * the same saved state, keeps the fastest for this system and records it for every system and
  * batch of the process with the same pass, dimension, precision and density band (bodies per

@@ -43,6 +43,16 @@ def cubes(ctx, n=4096, phi=0.55, seed=0x5EED0023):
     return lambda: Microstate(ctx, Periodic(math.sqrt(3.0), [L] * 3), pos, h, seed=seed)
 
 
+def squares(ctx, n=4096, seed=0x5EED0024):
+    from hoomd_rs_b200 import ConvexPolygon
+    sq = np.array([[-0.5, -0.5], [0.5, -0.5], [0.5, 0.5], [-0.5, 0.5]])
+    L = math.sqrt(n / 0.6)
+    pos = lattice.cubic_lattice(n, L, 2, seed, jitter=0.0)
+    ang = np.random.default_rng(seed).uniform(-0.2, 0.2, n)
+    h = PairwiseCutoff(HardShape(ConvexPolygon.with_vertices(sq)))
+    return lambda: Microstate(ctx, Periodic(math.sqrt(2.0), [L, L]), pos, h, seed=seed, orientations=ang)
+
+
 def run(g, moves, precision, kt=1.0):
     counts = []
     for move, maximum in moves:
@@ -52,19 +62,20 @@ def run(g, moves, precision, kt=1.0):
 
 
 @pytest.mark.parametrize("precision", [FP64, FP32_RECHECK])
-@pytest.mark.parametrize("kind", ["spheres3", "disks", "lj", "cubes"])
+@pytest.mark.parametrize("kind", ["spheres3", "disks", "lj", "cubes", "squares"])
 def test_every_variant_gives_the_same_trajectory(ctx, kind, precision):
     make, moves = {
         "spheres3": (spheres(ctx), [(TRANSLATE, 0.2)] * 3),
         "disks": (spheres(ctx, 2, 4096, 0.7), [(TRANSLATE, 0.1)] * 4),
         "lj": (lj(ctx), [(TRANSLATE, 0.1)] * 3),
         "cubes": (cubes(ctx), [(TRANSLATE, 0.08), (ROTATE, 0.1), (TRANSLATE, 0.08)]),
+        "squares": (squares(ctx), [(TRANSLATE, 0.1), (ROTATE, 0.1), (TRANSLATE, 0.1)]),
     }[kind]
     ref = make()
     count = ref.launch_variant(precision)["count"]
     ref.set_launch_variant(precision, 0)
     want = run(ref, moves, precision)
-    pos, ori = ref.positions(), (ref.orientations() if kind == "cubes" else None)
+    pos, ori = ref.positions(), (ref.orientations() if kind in ("cubes", "squares") else None)
     for v in range(1, count):
         g = make()
         g.set_launch_variant(precision, v)
