@@ -103,3 +103,19 @@ def test_captured_sweeps_count_their_kernels(ctx):
     launched = b.kernel_launches() - k0
     assert launched >= 2 * 10 + 2 * 9
     assert (launched - 20) % 9 == 0
+
+
+@pytest.mark.parametrize("precision", [FP64, FP32_RECHECK])
+def test_one_replica_batch_captured_equals_single_system(ctx, precision):
+    # a single system run as a one-replica batch with captured sweeps: the same trajectory as
+    # the Microstate's own sweeps (2-D disks at area fraction 0.70, 40 sweeps in one call)
+    from hoomd_rs_b200 import TRANSLATE, HardSphere, Microstate, PairwiseCutoff, Periodic, lattice
+    pos, L = lattice.hard_sphere_box(4096, 0.70, 2, 0x5EED0061)
+    b = Batch(ctx, [{"boundary": Periodic(1.0, [L, L]), "positions": pos, "seed": 0x5EED0061}])
+    b.set_captured_sweeps(True)
+    m = Microstate(ctx, Periodic(1.0, [L, L]), pos, PairwiseCutoff(HardSphere(1.0)), seed=0x5EED0061)
+    counts, total = b.sweep(0.1, precision, n_sweeps=40, increment_step=True)
+    c = m.sweep(TRANSLATE, 0.1, 1.0, precision, n_sweeps=40, increment_step=True)
+    assert (counts[0].accepted, counts[0].rejected) == (c.accepted, c.rejected)
+    assert np.array_equal(b.positions(0), m.positions())
+    assert b.state(0)[1:] == (m.step(), m.substep())
