@@ -758,8 +758,10 @@ def main():
     # band, which the timed systems below pick up (it restores the tuner's state afterwards)
     variants = {}
     for name, prec in (("fp32_recheck", FP32_RECHECK), ("fp64", FP64)):
+        # both passes (a lane or a warp per trial) and their variants; the fastest is recorded
         chosen, ms = tuner.autotune(TRANSLATE, d, 1.0, prec, sweeps=4)
-        variants[name] = {"chosen": chosen, "ms_per_sweep": [round(float(x), 4) for x in ms]}
+        variants[name] = {"chosen": chosen, "cooperative_pass": tuner.cooperative_pass(prec),
+                          "ms_per_sweep": [round(float(x), 4) for x in ms]}
     tuner.close()
 
     stream = torch.cuda.Stream()

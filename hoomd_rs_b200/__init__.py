@@ -197,6 +197,7 @@ SIGNATURES = {
     "hmc_get_n_bodies": (C.c_int, [_vp, C.POINTER(C.c_uint64)]),
     "hmc_set_shape_overlap": (C.c_int, [_vp, C.POINTER(hmc_shape_overlap_params)]),
     "hmc_set_cooperative_pass": (C.c_int, [_vp, C.c_uint32, C.c_uint32]),
+    "hmc_get_cooperative_pass": (C.c_int, [_vp, C.c_uint32, C.POINTER(C.c_uint32)]),
     "hmc_gsd_last_error": (C.c_int, []),
     "hmc_gsd_create": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_uint16, C.c_uint16, C.c_int,
                                  C.POINTER(_vp)]),
@@ -808,6 +809,12 @@ class Microstate:
         """Hard spheres: the warp-cooperative colour pass (the FP64 default) or one lane per trial
         (the FP32 default) for this precision; the trajectory is the same."""
         _check(_lib.hmc_set_cooperative_pass(self._h, precision, int(cooperative)))
+
+    def cooperative_pass(self, precision: int) -> bool:
+        """Hard spheres: whether the next sweep in this precision runs the warp-cooperative pass."""
+        v = C.c_uint32()
+        _check(_lib.hmc_get_cooperative_pass(self._h, precision, C.byref(v)))
+        return bool(v.value)
 
     def autotune(self, move: int, maximum: float, temperature: float, precision: int, sweeps: int = 4):
         """hmc_autotune: time every launch variant of this system's pass from the current state

@@ -89,6 +89,7 @@ struct hmc_system {
     unsigned long long* host_first_bad = nullptr;  // pinned mirror
     std::vector<void*> allocations;
     bool coop[2] = {true, false};  // warp-cooperative hard-sphere pass: [fp64, fp32]
+    bool coop_set[2] = {false, false};  // coop chosen for this system (else the recorded choice)
     int32_t variant[2] = {-1, -1};  // launch variant per precision; -1: the cached choice or the default
     bool pdl = true;                // colour passes launch while the previous one finishes
     uint32_t rounds_guess = 2;      // colour sets enqueued before the sweep's count is known
@@ -373,11 +374,13 @@ hmc_status check_flags(hmc_system* s) {
 // The colour-pass kernel family a system's sweep runs in a precision, and its variant table.
 enum VariantFamily : uint32_t { kFamSphereDirect, kFamSphereCoop, kFamLj, kFamPoly3, kFamPoly2, kFamBatch, kFamBatchLj };
 
+bool coop_of(const hmc_system* s, bool fp32);
+
 uint32_t family_of(const hmc_system* s, bool fp32) {
     if (s->soft()) return kFamLj;
     if (s->interaction == HMC_HARD_CONVEX_POLYHEDRON) return kFamPoly3;
     if (s->polygon()) return kFamPoly2;
-    return s->coop[fp32] ? kFamSphereCoop : kFamSphereDirect;
+    return coop_of(s, fp32) ? kFamSphereCoop : kFamSphereDirect;
 }
 
 const LaunchShape* family_shapes(uint32_t fam, uint32_t* n) {
@@ -412,6 +415,25 @@ uint32_t cached_variant(uint32_t fam, uint32_t dim, bool fp32, int32_t band) {
 void cache_variant(uint32_t fam, uint32_t dim, bool fp32, int32_t band, uint32_t v) {
     std::lock_guard<std::mutex> lock(g_variant_mutex);
     g_variant_cache[std::make_tuple(fam, dim, (uint32_t)fp32, band)] = v;
+}
+
+// Hard-sphere pass choices of hmc_autotune (true: the warp-cooperative pass), keyed by
+// dimension, precision and density band; guarded by g_variant_mutex.
+std::map<std::tuple<uint32_t, uint32_t, int32_t>, bool> g_pass_cache;
+
+// Whether the next hard-sphere sweep of system s in this precision runs the warp-cooperative
+// pass: the system's own choice, else the recorded one for its band, else the default.
+bool coop_of(const hmc_system* s, bool fp32) {
+    if (s->coop_set[fp32] || s->interaction != HMC_HARD_SPHERE) return s->coop[fp32];
+    std::lock_guard<std::mutex> lock(g_variant_mutex);
+    auto it = g_pass_cache.find(std::make_tuple((uint32_t)s->dim, (uint32_t)fp32,
+                                                density_band((double)s->n, (double)s->geom.n_cells)));
+    return it == g_pass_cache.end() ? s->coop[fp32] : it->second;
+}
+
+void cache_pass(uint32_t dim, bool fp32, int32_t band, bool coop) {
+    std::lock_guard<std::mutex> lock(g_variant_mutex);
+    g_pass_cache[std::make_tuple(dim, (uint32_t)fp32, band)] = coop;
 }
 
 // The variant the next sweep of system s runs in this precision.
@@ -746,8 +768,11 @@ hmc_status hmc_system_create(hmc_context* ctx, const hmc_system_desc* d, const d
     // HMC_B200_PDL=0 launches every colour pass after the previous one has ended.
     if (const char* pdl = std::getenv("HMC_B200_PDL")) s->pdl = std::strcmp(pdl, "0") != 0;
     if (const char* kern = std::getenv("HMC_B200_SWEEP_KERNEL")) {
-        if (std::strcmp(kern, "direct") == 0) s->coop[0] = s->coop[1] = false;
-        if (std::strcmp(kern, "coop") == 0) s->coop[0] = s->coop[1] = true;
+        const bool direct = std::strcmp(kern, "direct") == 0, coop = std::strcmp(kern, "coop") == 0;
+        if (direct || coop) {
+            s->coop[0] = s->coop[1] = coop;
+            s->coop_set[0] = s->coop_set[1] = true;
+        }
     }
 
     cudaError_t e = cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking);
@@ -947,6 +972,7 @@ hmc_status hmc_sweep(hmc_system* s, const hmc_sweep_params* p, hmc_count* out) {
         L.n_bodies = (uint32_t)s->n;
         L.n_active = s->geom.color_stride;  // grid bound; the kernels read the list lengths
         const uint32_t variant = variant_of(s, fp32);
+        const bool coop = coop_of(s, fp32);
         const bool poly2_fp32 = fp32 && variant == 0;  // polygon variant 1: the FP64 pass in both modes
         if (s->profiling) HMC_CUDA(cudaEventRecord(s->ev[2], s->stream));
         // The rounds (while count.total() < N, :402-418) are known on the device after the
@@ -994,8 +1020,8 @@ hmc_status hmc_sweep(hmc_system* s, const hmc_sweep_params* p, hmc_count* out) {
                                                     s->poly_rcut2, s->poly_rcut2_hi32, L, p->move == HMC_ROTATE,
                                                     s->stream));
                     else
-                        HMC_CUDA(launch_sweep_sphere(s->dim, fp32, s->geom, s->arr, s->pair, L, s->coop[fp32],
-                                                     s->stream, variant));
+                        HMC_CUDA(launch_sweep_sphere(s->dim, fp32, s->geom, s->arr, s->pair, L, coop, s->stream,
+                                                     variant));
                     s->prof.kernel_launches += 1;
                 }
             }
@@ -1071,8 +1097,17 @@ hmc_status hmc_set_cooperative_pass(hmc_system* s, uint32_t precision, uint32_t 
     if (precision > HMC_FP32_RECHECK) return fail(HMC_INVALID_ARGUMENT, "precision");
     if (s->interaction != HMC_HARD_SPHERE) return fail(HMC_NOT_SUPPORTED, "the cooperative pass is for hard spheres");
     const bool fp32 = precision == HMC_FP32_RECHECK;
-    if (s->coop[fp32] != (cooperative != 0)) s->variant[fp32] = -1;  // the other pass has its own variants
+    if (coop_of(s, fp32) != (cooperative != 0)) s->variant[fp32] = -1;  // the other pass has its own variants
     s->coop[fp32] = cooperative != 0;
+    s->coop_set[fp32] = true;
+    return HMC_OK;
+}
+
+hmc_status hmc_get_cooperative_pass(hmc_system* s, uint32_t precision, uint32_t* cooperative) {
+    if (!s || !cooperative) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
+    if (precision > HMC_FP32_RECHECK) return fail(HMC_INVALID_ARGUMENT, "precision");
+    if (s->interaction != HMC_HARD_SPHERE) return fail(HMC_NOT_SUPPORTED, "the cooperative pass is for hard spheres");
+    *cooperative = coop_of(s, precision == HMC_FP32_RECHECK) ? 1u : 0u;
     return HMC_OK;
 }
 
@@ -1131,9 +1166,10 @@ hmc_status hmc_autotune(hmc_system* s, const hmc_sweep_params* p, uint32_t sweep
     if (sweeps == 0 || sweeps > 1000) return fail(HMC_INVALID_ARGUMENT, "sweeps must be in [1, 1000]");
     HMC_CUDA(cudaSetDevice(s->ctx->device));
     const bool fp32 = p->precision == HMC_FP32_RECHECK;
-    const uint32_t fam = family_of(s, fp32);
-    uint32_t n_var = 0;
-    family_shapes(fam, &n_var);
+    // hard spheres without a pass chosen for the system: both passes (a lane or a warp per
+    // trial) and each one's variants, the current pass first
+    const bool coop0 = coop_of(s, fp32), coop_set0 = s->coop_set[fp32], coop_own0 = s->coop[fp32];
+    const bool both = s->interaction == HMC_HARD_SPHERE && !coop_set0;
     // the state to start every variant from
     const uint64_t n = s->n;
     const uint64_t step0 = s->step;
@@ -1159,12 +1195,32 @@ hmc_status hmc_autotune(hmc_system* s, const hmc_sweep_params* p, uint32_t sweep
     };
     auto run = [&](const hmc_sweep_params& q) -> hmc_status { return hmc_sweep(s, &q, nullptr); };
     hmc_status st = e == cudaSuccess ? HMC_OK : fail(HMC_CUDA_ERROR, "autotune: %s", cudaGetErrorString(e));
-    std::vector<double> ms(n_var, 0.0);
-    uint32_t best = 0;
-    for (uint32_t v = 0; v < n_var && !st; ++v) {
-        s->variant[fp32] = (int32_t)v;
-        st = time_variant(s->stream, *p, sweeps, run, restore, &ms[v]);
-        if (!st && ms[v] < ms[best]) best = v;
+    std::vector<double> ms, best_ms;
+    uint32_t best = 0, best_fam = family_of(s, fp32);
+    bool best_coop = coop0, have = false;
+    double best_t = 0.0;
+    for (int k = 0; k < (both ? 2 : 1) && !st; ++k) {
+        const bool coop = k == 0 ? coop0 : !coop0;
+        if (both) {
+            s->coop[fp32] = coop;
+            s->coop_set[fp32] = true;
+        }
+        const uint32_t fam = family_of(s, fp32);
+        uint32_t n_var = 0;
+        family_shapes(fam, &n_var);
+        ms.assign(n_var, 0.0);
+        for (uint32_t v = 0; v < n_var && !st; ++v) {
+            s->variant[fp32] = (int32_t)v;
+            st = time_variant(s->stream, *p, sweeps, run, restore, &ms[v]);
+            if (!st && (!have || ms[v] < best_t)) {
+                have = true;
+                best_t = ms[v];
+                best = v;
+                best_fam = fam;
+                best_coop = coop;
+            }
+        }
+        if (!st && best_fam == fam && best_coop == coop) best_ms = ms;  // the chosen pass's times
     }
     hmc_status st2 = restore();
     if (bp) cudaFreeAsync(bp, s->stream);
@@ -1172,12 +1228,20 @@ hmc_status hmc_autotune(hmc_system* s, const hmc_sweep_params* p, uint32_t sweep
     cudaStreamSynchronize(s->stream);
     if (st || st2) {
         s->variant[fp32] = own0;
+        s->coop[fp32] = coop_own0;
+        s->coop_set[fp32] = coop_set0;
         return st ? st : st2;
     }
+    const int32_t band = density_band((double)s->n, (double)s->geom.n_cells);
+    if (both) {  // the pass chosen becomes the system's own, and the recorded one for its band
+        s->coop[fp32] = best_coop;
+        s->coop_set[fp32] = true;
+        cache_pass((uint32_t)s->dim, fp32, band, best_coop);
+    }
     s->variant[fp32] = (int32_t)best;
-    cache_variant(fam, (uint32_t)s->dim, fp32, density_band((double)s->n, (double)s->geom.n_cells), best);
-    if (chosen) describe_variant(fam, best, chosen);
-    if (ms_per_sweep) std::memcpy(ms_per_sweep, ms.data(), sizeof(double) * n_var);
+    cache_variant(best_fam, (uint32_t)s->dim, fp32, band, best);
+    if (chosen) describe_variant(best_fam, best, chosen);
+    if (ms_per_sweep) std::memcpy(ms_per_sweep, best_ms.data(), sizeof(double) * best_ms.size());
     return HMC_OK;
 }
 
@@ -2027,7 +2091,7 @@ hmc_status hmc_eval_trials(hmc_system* s, const hmc_injected_move* moves, uint64
             e = launch_trials_poly(fp32, s->geom, s->arr, s->verts, s->n_vertices, s->poly_rcut2, s->poly_rcut2_hi32, j,
                                    s->stream);
         else
-            e = launch_trials_sphere(s->dim, fp32, s->coop[fp32], s->geom, s->arr, s->pair, j, s->stream);
+            e = launch_trials_sphere(s->dim, fp32, coop_of(s, fp32), s->geom, s->arr, s->pair, j, s->stream);
         s->prof.kernel_launches++;
     }
     std::vector<uint8_t> hd(2 * n);

@@ -291,9 +291,15 @@ hmc_status hmc_set_launch_variant(hmc_system* sys, uint32_t precision, uint32_t 
 /* Hard spheres and disks: which colour pass a precision runs, one lane per trial (cooperative = 0,
  * the FP32 default) or the warp-cooperative pass (1, the FP64 default). Both make the same pair
  * tests, so the trajectory does not depend on the choice; the launch variants are those of the
- * chosen pass. HMC_NOT_SUPPORTED for other interactions. */
+ * chosen pass. A system without its own choice runs the one hmc_autotune recorded for its
+ * dimension, precision and density band, else the default. HMC_NOT_SUPPORTED for other
+ * interactions. */
 hmc_status hmc_set_cooperative_pass(hmc_system* sys, uint32_t precision, uint32_t cooperative);
-/* ms_per_sweep (may be NULL): chosen->count entries, the mean time of one sweep per variant. */
+hmc_status hmc_get_cooperative_pass(hmc_system* sys, uint32_t precision, uint32_t* cooperative);
+/* Hard spheres and disks without a pass set by hmc_set_cooperative_pass: hmc_autotune times the
+ * variants of both passes and keeps the fastest pass and variant (and records both).
+ * ms_per_sweep (may be NULL): chosen->count entries, the mean time of one sweep per variant of
+ * the chosen pass. */
 hmc_status hmc_autotune(hmc_system* sys, const hmc_sweep_params* params, uint32_t sweeps, hmc_launch_variant* chosen,
                         double* ms_per_sweep);
 /* The same for a batch's replica pass (params: one per replica, as hmc_batch_sweep). */

@@ -106,7 +106,9 @@ def test_autotune_restores_state_and_records_its_choice(ctx, precision):
     c2 = twin.sweep(TRANSLATE, 0.2, 1.0, precision, n_sweeps=2, increment_step=True)
     assert (c1.accepted, c1.rejected) == (c2.accepted, c2.rejected)
     assert np.array_equal(g.positions(), twin.positions())
-    # the recorded choice applies to another system of the same workload (same density band)
+    # the recorded choice (pass and variant) applies to another system of the same workload
+    # (same density band)
+    assert twin.cooperative_pass(precision) == g.cooperative_pass(precision)
     assert twin.launch_variant(precision)["index"] == chosen["index"]
 
 
