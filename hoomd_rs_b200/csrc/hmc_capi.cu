@@ -1029,16 +1029,19 @@ hmc_status hmc_sweep(hmc_system* s, const hmc_sweep_params* p, hmc_count* out) {
         };
         const uint32_t guess = s->n == 0 ? 0u : s->rounds_guess;
         if ((st = enqueue(0, guess))) return st;
+        // the passes' end is recorded before the host waits for the counts, so that profiling adds
+        // no host round trip to the sweep
+        if (s->profiling) HMC_CUDA(cudaEventRecord(s->ev[3], s->stream));
         if ((st = read_stats(s))) return st;
         if ((st = check_flags(s))) return st;  // the kernels left the state untouched
         const uint32_t rounds = s->host_stats->rounds;
         if (rounds > guess) {
             if ((st = enqueue(guess, rounds))) return st;
+            if (s->profiling) HMC_CUDA(cudaEventRecord(s->ev[3], s->stream));
             if ((st = read_stats(s))) return st;
         }
         if (rounds > 0) s->rounds_guess = rounds;
         if (s->profiling) {
-            HMC_CUDA(cudaEventRecord(s->ev[3], s->stream));
             HMC_CUDA(cudaEventSynchronize(s->ev[3]));
             float t_rebuild = 0.f, t_sweep = 0.f;
             HMC_CUDA(cudaEventElapsedTime(&t_rebuild, s->ev[0], s->ev[1]));
