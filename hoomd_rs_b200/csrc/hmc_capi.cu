@@ -315,8 +315,9 @@ hmc_status setup_geometry(hmc_system* s, const double* L) {
         g.half_shape[a] = g.shape[a] / 2;
         cells *= g.shape[a];
     }
-    if (cells > 16000000ull)
-        return fail(HMC_NOT_SUPPORTED, "%llu checkerboard spaces exceed the supported 16M", (unsigned long long)cells);
+    // 32-bit space indices and slot offsets; the packed multi-index caps the axes below
+    if (cells > (1ull << 31))
+        return fail(HMC_NOT_SUPPORTED, "%llu checkerboard spaces exceed the supported 2^31", (unsigned long long)cells);
     // colour lists pack the multi-index: 10 bits per axis in 3-D, 16 in 2-D
     for (int a = 0; a < s->dim; ++a) {
         if (g.shape[a] > (s->dim == 3 ? 1024u : 65535u))
@@ -453,7 +454,8 @@ hmc_status rebuild(hmc_system* s, bool write_s, bool write_slots = true) {
     }
     HMC_CUDA(cudaMemsetAsync(s->arr.stats, 0, sizeof(DeviceStats), s->stream));
     HMC_CUDA(launch_rebuild(s->dim, s->geom, s->arr, (uint32_t)s->n, write_s, s->stream, write_slots));
-    s->prof.kernel_launches += s->n > 0 ? 6 : 2;  // bin, 2 scan passes, scatter, space sort, gather
+    // bin, 2 scan passes (3 for grids of more than 2048 scan blocks), scatter, space sort, gather
+    s->prof.kernel_launches += (s->n > 0 ? 6 : 2) + ((s->geom.n_cells + 2047u) / 2048u > 2048u ? 1 : 0);
     return HMC_OK;
 }
 

@@ -792,9 +792,53 @@ __global__ void __launch_bounds__(kScanThreads) k_count_reduce(const uint32_t* _
     }
 }
 
+// Blocks of the count scan up to which each block of k_count_apply sums the earlier blocks'
+// totals itself; beyond, k_scan_block_sums scans the totals first (the per-block sums would cost
+// O(blocks^2) reads).
+constexpr uint32_t kScanDirectBlocks = 2048;
+
+// Exclusive scan of the per-block totals, in place, by one block of 1024 threads.
+__global__ void __launch_bounds__(1024) k_scan_block_sums(uint32_t* block_sums, uint32_t nb) {
+    grid_dependency_wait();  // rebuild kernels run back to back: the previous one has ended here
+    allow_dependent_launch();
+    __shared__ uint32_t s_warp[32];
+    __shared__ uint32_t s_carry;
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) s_carry = 0;
+    __syncthreads();
+    for (uint32_t base = 0; base < nb; base += 1024) {
+        const uint32_t i = base + threadIdx.x;
+        const uint32_t v = i < nb ? block_sums[i] : 0u;
+        uint32_t x = v;
+#pragma unroll
+        for (uint32_t o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) s_warp[warp] = x;
+        __syncthreads();
+        if (warp == 0) {
+            uint32_t w = s_warp[lane];
+#pragma unroll
+            for (uint32_t o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+                if (lane >= o) w += y;
+            }
+            s_warp[lane] = w;  // inclusive over the warps
+        }
+        __syncthreads();
+        const uint32_t carry = s_carry;
+        const uint32_t excl = carry + (warp > 0 ? s_warp[warp - 1] : 0u) + x - v;
+        if (i < nb) block_sums[i] = excl;
+        __syncthreads();  // every thread has read s_carry and s_warp
+        if (threadIdx.x == 0) s_carry = carry + s_warp[31];
+        __syncthreads();
+    }
+}
+
 __global__ void __launch_bounds__(kScanThreads) k_count_apply(const uint32_t* __restrict__ count, uint32_t n_cells,
                                                               const uint32_t* __restrict__ block_sums,
-                                                              uint32_t* cell_start) {
+                                                              uint32_t* cell_start, uint32_t scanned) {
     grid_dependency_wait();  // rebuild kernels run back to back: the previous one has ended here
     allow_dependent_launch();
     const uint32_t base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
@@ -805,17 +849,21 @@ __global__ void __launch_bounds__(kScanThreads) k_count_apply(const uint32_t* __
         v[k] = base + k < n_cells ? count[base + k] : 0u;
         sum += v[k];
     }
-    // this block's offset: the sum of the earlier blocks' totals (at most a few hundred values,
-    // read by every block, so the separate scan of the block totals is not needed)
+    // this block's offset: the scanned totals (scanned), else the sum of the earlier blocks'
+    // totals, read by every block (at most kScanDirectBlocks values)
     __shared__ uint32_t s_prefix[kScanThreads / 32];
-    uint32_t part = 0;
-    for (uint32_t i = threadIdx.x; i < blockIdx.x; i += kScanThreads) part += block_sums[i];
-    part = __reduce_add_sync(0xffffffffu, part);
-    if ((threadIdx.x & 31) == 0) s_prefix[threadIdx.x >> 5] = part;
-    __syncthreads();
     uint32_t prefix = 0;
+    if (scanned) {
+        prefix = block_sums[blockIdx.x];
+    } else {
+        uint32_t part = 0;
+        for (uint32_t i = threadIdx.x; i < blockIdx.x; i += kScanThreads) part += block_sums[i];
+        part = __reduce_add_sync(0xffffffffu, part);
+        if ((threadIdx.x & 31) == 0) s_prefix[threadIdx.x >> 5] = part;
+        __syncthreads();
 #pragma unroll
-    for (int w = 0; w < kScanThreads / 32; ++w) prefix += s_prefix[w];
+        for (int w = 0; w < kScanThreads / 32; ++w) prefix += s_prefix[w];
+    }
     uint32_t total;
     uint32_t run = block_exclusive_scan(sum, &total) + prefix;
 #pragma unroll
@@ -1606,9 +1654,11 @@ cudaError_t launch_count_scan(const Arrays& a, uint32_t n_cells, cudaStream_t s,
     const uint32_t nb = blocks_for(n_cells, kScanTile);
     cudaError_t e = launch_chained(k_count_reduce, nb, kScanThreads, chained, s, (const uint32_t*)a.cell_count,
                                    n_cells, a.block_sums);
+    const uint32_t scanned = nb > kScanDirectBlocks ? 1u : 0u;
+    if (e == cudaSuccess && scanned) e = launch_chained(k_scan_block_sums, 1, 1024, true, s, a.block_sums, nb);
     if (e == cudaSuccess)
         e = launch_chained(k_count_apply, nb, kScanThreads, true, s, (const uint32_t*)a.cell_count, n_cells,
-                           (const uint32_t*)a.block_sums, a.cell_start);
+                           (const uint32_t*)a.block_sums, a.cell_start, scanned);
     return e;
 }
 }  // namespace
