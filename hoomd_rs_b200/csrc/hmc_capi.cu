@@ -2465,7 +2465,7 @@ hmc_status hmc_batch_create(hmc_context* ctx, uint32_t n_replicas, const hmc_sys
         n_total += d->n_bodies;
         cells_total += cells;
         if (n_total >= (1ull << 31)) return fail(HMC_INVALID_ARGUMENT, "too many bodies");
-        if (cells_total > 16000000ull) return fail(HMC_NOT_SUPPORTED, "more than 16M spaces in the batch");
+        if (cells_total > (1ull << 31)) return fail(HMC_NOT_SUPPORTED, "more than 2^31 spaces in the batch");
     }
     HMC_CUDA(cudaSetDevice(ctx->device));
     hmc_batch* bt = new hmc_batch();

@@ -209,3 +209,21 @@ def test_batch_tune_equals_single_system_tune(ctx, precision):
     cs = single.sweep(TRANSLATE, float(tuned[1]), 1.0, precision, n_sweeps=1, increment_step=True)
     assert (c[1].accepted, c[1].rejected) == (cs.accepted, cs.rejected)
     assert np.array_equal(b.positions(1), single.positions())
+
+
+def test_batch_of_many_spaces_equals_single_systems(ctx):
+    # 64 replicas of 65536 spheres: 5.45 M spaces in the batch, whose space counts are scanned in
+    # three kernels (more than 2048 blocks of 2048 spaces); replicas 0 and 63 against single systems
+    specs = [(65536, 0.40, 0x5EED0080 + k, 0, "fcc") for k in range(64)]
+    reps = replicas(3, specs)
+    b = Batch(ctx, reps)
+    picks = (0, 63)
+    singles = {k: Microstate(ctx, reps[k]["boundary"], reps[k]["positions"], PairwiseCutoff(HardSphere(1.0)),
+                             seed=reps[k]["seed"]) for k in picks}
+    for _ in range(2):
+        counts, _ = b.sweep(0.3, FP32_RECHECK, increment_step=True)
+        for k, m in singles.items():
+            c = m.sweep(TRANSLATE, 0.3, 1.0, FP32_RECHECK, n_sweeps=1, increment_step=True)
+            assert (counts[k].accepted, counts[k].rejected) == (c.accepted, c.rejected), k
+    for k, m in singles.items():
+        assert np.array_equal(b.positions(k), m.positions()), k
