@@ -598,6 +598,27 @@ def run_config(args, local_rank):
     r32, p32 = timed(FP32_RECHECK)
     clocks = sampler.stop()
     r64, p64 = timed(FP64)
+    side = {}
+    if kind == "disks":
+        # the configuration's 1000 sweeps as one call: the sweeps are enqueued back to back (the
+        # host waits once per 64) instead of one call and one wait per sweep
+        runs = {}
+        for name, prec in (("fp32_recheck", FP32_RECHECK), ("fp64", FP64)):
+            m = Microstate(ctx, bound, pos, h, seed=seed, orientations=ori)
+            m.set_stream(stream.cuda_stream)
+            m.sweep(TRANSLATE, moves[0][1], 1.0, prec, n_sweeps=args.warmup, increment_step=True)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            c = m.sweep(TRANSLATE, moves[0][1], 1.0, prec, n_sweeps=1000, increment_step=True)
+            el = time.perf_counter() - t0
+            runs[name] = {"value": c.total() / el, "ms_per_sweep": 1e3 * el / 1000, "positions": m.positions()}
+            m.close()
+        side["sweeps_1000_one_call"] = {
+            **{k: {"value": v["value"], "ms_per_sweep": v["ms_per_sweep"]} for k, v in runs.items()},
+            "mismatches": int(np.count_nonzero(np.any(runs["fp32_recheck"]["positions"] != runs["fp64"]["positions"],
+                                                      axis=1))),
+            "what": "1000 sweeps in one Microstate.sweep call, wall clock around the call (L2 not flushed: the "
+                    "4096-disk state stays in L2)"}
     line = {"metric": f"trial moves/s, {kind}", "value": r32["value"], "unit": UNIT, "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": r32["ms_per_step"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "fp32 pair test + fp64 recheck (fp64 state)", "data": "synthetic",
@@ -608,7 +629,7 @@ def run_config(args, local_rank):
             "recheck_fraction": r32["recheck_fraction"], "gpu_launches": r32["launches"], "clocks": clocks,
             "order_ambiguous": {"fp32_recheck": r32["order_ambiguous"], "fp64": r64["order_ambiguous"],
                                 "what": "decisions another summation order of the FP64 pair energies could change"},
-            "launch_variants": {"fp32_recheck": r32["launch_variant"], "fp64": r64["launch_variant"]}}
+            "launch_variants": {"fp32_recheck": r32["launch_variant"], "fp64": r64["launch_variant"]}, **side}
     if not args.no_cpu_baseline:
         threads = host_threads()
         o = oracle.System(dim, [L] * dim, pos, ori, seed=seed, **okw)

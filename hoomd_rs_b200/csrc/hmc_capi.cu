@@ -90,6 +90,8 @@ struct hmc_system {
     std::vector<void*> allocations;
     bool coop[2] = {true, false};  // warp-cooperative hard-sphere pass: [fp64, fp32]
     bool coop_set[2] = {false, false};  // coop chosen for this system (else the recorded choice)
+    DeviceStats* host_slots = nullptr;  // pinned: per-sweep statistics of a pipelined call
+    uint32_t slots_cap = 0;
     int32_t variant[2] = {-1, -1};  // launch variant per precision; -1: the cached choice or the default
     bool pdl = true;                // colour passes launch while the previous one finishes
     uint32_t rounds_guess = 2;      // colour sets enqueued before the sweep's count is known
@@ -594,6 +596,7 @@ void hmc_system_destroy(hmc_system* s) {
         if (e) cudaEventDestroy(e);
     if (s->host_stats) cudaFreeHost(s->host_stats);
     if (s->host_first_bad) cudaFreeHost(s->host_first_bad);
+    if (s->host_slots) cudaFreeHost(s->host_slots);
     if (s->gsd_host) cudaFreeHost(s->gsd_host);
     if (s->own_stream) cudaStreamDestroy(s->own_stream);
     cudaGetLastError();  // a destructor reports nothing: leave no sticky error behind
@@ -796,6 +799,7 @@ hmc_status hmc_system_create(hmc_context* ctx, const hmc_system_desc* d, const d
         (st = dalloc(s, &A.sorted_off, cap)) || (st = dalloc(s, &A.sorted_body, cap)) ||
         (st = dalloc(s, &A.slot_of_body, cap)) || (st = dalloc(s, &A.body_cell, cap)) ||
         (st = dalloc(s, &A.body_rank, cap)) || (st = dalloc(s, &A.body_m, cap)) || (st = dalloc(s, &A.stats, 1)) ||
+        (st = dalloc(s, &A.abort_word, 1)) ||
         (st = dalloc(s, &s->stage, cap * (uint64_t)s->dim)) || (st = dalloc(s, &s->first_bad, 1)))
         return destroy_fail(st);
     e = cudaMallocHost((void**)&s->host_first_bad, sizeof(unsigned long long));
@@ -803,6 +807,11 @@ hmc_status hmc_system_create(hmc_context* ctx, const hmc_system_desc* d, const d
         s->host_first_bad = nullptr;
         fail(HMC_OUT_OF_MEMORY, "cudaMallocHost: %s", cudaGetErrorString(e));
         return destroy_fail(HMC_OUT_OF_MEMORY);
+    }
+    e = cudaMemset(A.abort_word, 0, sizeof(uint32_t));
+    if (e != cudaSuccess) {
+        fail(HMC_CUDA_ERROR, "cudaMemset: %s", cudaGetErrorString(e));
+        return destroy_fail(HMC_CUDA_ERROR);
     }
     A.body_ori = nullptr;
     A.sorted_q = nullptr;
@@ -943,6 +952,185 @@ hmc_status hmc_increment_step(hmc_system* s) {
     return HMC_OK;
 }
 
+// How the sweeps of one call run: precision, launch variant and, for hard spheres, the pass.
+struct SweepPlan {
+    bool fp32, coop, poly2_fp32;
+    uint32_t variant;
+};
+
+static SweepPlan sweep_plan(const hmc_system* s, const hmc_sweep_params* p) {
+    SweepPlan sp{};
+    sp.fp32 = p->precision == HMC_FP32_RECHECK;
+    sp.variant = variant_of(s, sp.fp32);
+    sp.coop = coop_of(s, sp.fp32);
+    sp.poly2_fp32 = sp.fp32 && sp.variant == 0;  // polygon variant 1: the FP64 pass in both modes
+    return sp;
+}
+
+// The cell-list rebuild of the current sweep; shapes read S in both modes, and the colour passes
+// do not read slot_of_body.
+static hmc_status sweep_rebuild(hmc_system* s, const SweepPlan& sp) {
+    return rebuild(s, !sp.fp32 || s->oriented() || (s->soft() && !s->soft_fp32()), false);
+}
+
+static Launch sweep_launch(const hmc_system* s, const hmc_sweep_params* p) {
+    Launch L{};
+    L.step = s->step;
+    L.seed = s->seed;
+    L.max_move = p->maximum;
+    L.kt = p->temperature;
+    L.n_bodies = (uint32_t)s->n;
+    L.n_active = s->geom.color_stride;  // grid bound; the kernels read the list lengths
+    return L;
+}
+
+// Colour sets r0 .. r1-1 of the current sweep: per set the round's trial moves where a trial has
+// several lanes (one thread each), then the 2^d colour passes.
+static hmc_status enqueue_sets(hmc_system* s, const hmc_sweep_params* p, const SweepPlan& sp, Launch& L, uint32_t r0,
+                               uint32_t r1) {
+    const bool fp32 = sp.fp32;
+    const uint32_t colors = 1u << s->dim;
+    for (uint32_t r = r0; r < r1; ++r) {
+        L.substep = s->substep + r;  // increment_substep after every full colour set
+        L.round = r;
+        if (s->soft()) {
+            HMC_CUDA(launch_propose_lj(s->dim, fp32 && s->soft_fp32(), s->geom, s->arr, L, s->stream));
+            s->prof.kernel_launches += 1;
+        } else if (s->interaction == HMC_HARD_CONVEX_POLYHEDRON) {
+            HMC_CUDA(launch_propose_poly(fp32 && !s->shape_soft, s->geom, s->arr, L, p->move == HMC_ROTATE,
+                                         s->shape_soft, s->stream));
+            s->prof.kernel_launches += 1;
+        } else if (s->polygon()) {
+            HMC_CUDA(launch_propose_poly2(sp.poly2_fp32 && !s->shape_soft, s->geom, s->arr, L, p->move == HMC_ROTATE,
+                                          s->shape_soft, s->stream));
+            s->prof.kernel_launches += 1;
+        }
+        for (uint32_t c = 0; c < colors; ++c) {
+            L.color = c;
+            L.overlap_previous = (r > 0 || c > 0) && s->pdl ? 1u : 0u;
+            // the first pass after the rebuild (or after a round's proposals): launch early, wait
+            // for it before reading anything
+            L.early_wait = (r == 0 || s->soft() || s->oriented()) && c == 0 && s->pdl ? 1u : 0u;
+            if (s->soft())  // the overlap penalty has no FP32 path: FP64 in both modes
+                HMC_CUDA(launch_sweep_lj(s->dim, fp32 && s->soft_fp32(), !s->soft_fp32(), s->geom, s->arr, s->pair, L,
+                                         s->stream, sp.variant));
+            else if (s->shape_soft && s->dim == 3)  // FP64 in both modes
+                HMC_CUDA(launch_sweep_poly3_soft(s->geom, s->arr, s->verts, s->n_vertices, s->so, L, s->stream));
+            else if (s->shape_soft)
+                HMC_CUDA(launch_sweep_poly2_soft(s->sat(), s->geom, s->arr, s->verts, s->n_vertices, s->so, L,
+                                                 s->stream));
+            else if (s->interaction == HMC_HARD_CONVEX_POLYHEDRON)
+                HMC_CUDA(launch_sweep_poly(fp32, s->geom, s->arr, s->verts, s->n_vertices, s->poly_rcut2,
+                                           s->poly_rcut2_hi32, L, p->move == HMC_ROTATE, s->stream, sp.variant));
+            else if (s->polygon())
+                HMC_CUDA(launch_sweep_poly2(sp.poly2_fp32, s->sat(), s->geom, s->arr, s->verts, s->n_vertices,
+                                            s->poly_rcut2, s->poly_rcut2_hi32, L, p->move == HMC_ROTATE, s->stream));
+            else
+                HMC_CUDA(launch_sweep_sphere(s->dim, fp32, s->geom, s->arr, s->pair, L, sp.coop, s->stream,
+                                             sp.variant));
+            s->prof.kernel_launches += 1;
+        }
+    }
+    return HMC_OK;
+}
+
+// A finished sweep into the call's Count and the system's Counter.
+static void account_sweep(hmc_system* s, const hmc_sweep_params* p, const DeviceStats& d, hmc_count& total) {
+    const uint32_t rounds = d.rounds;
+    if (rounds > 0) s->rounds_guess = rounds;
+    total.accepted += d.accepted;
+    total.rejected += (uint64_t)rounds * d.nonempty - d.accepted;
+    total.rechecks += d.rechecks;
+    total.pair_checks += d.pair_checks;
+    total.order_ambiguous += d.ambiguous;
+    double me;
+    unsigned long long bits = d.max_err_bits;
+    std::memcpy(&me, &bits, 8);
+    total.max_fp32_error = std::max(total.max_fp32_error, me);
+    s->substep += rounds;
+    if (p->increment_step) {
+        s->step += 1;
+        s->substep = 0;
+    }
+}
+
+// Sweeps that increment the step, run without waiting for each one's count: every Counter of the
+// call is known in advance (step + j, substep 0), so the host enqueues up to kPipelineSweeps
+// sweeps back to back, each with the previous sweep's number of colour sets and its statistics
+// copied to a pinned slot. After each sweep k_sweep_guard raises the abort word when the sweep
+// needed more colour sets (or flagged an error); every later sweep then finds kErrAborted in its
+// statistics (k_bin puts it there) and runs no colour pass. The host waits once, reads the slots,
+// completes a sweep that needed more sets (the same origin gives the same spaces, since bodies
+// do not leave their spaces within a sweep) and enqueues the sweeps after it again.
+constexpr uint32_t kPipelineSweeps = 64;
+
+static hmc_status sweep_pipelined(hmc_system* s, const hmc_sweep_params* p, hmc_count& total) {
+    if (s->slots_cap < kPipelineSweeps) {
+        if (s->host_slots) cudaFreeHost(s->host_slots);
+        s->host_slots = nullptr;
+        s->slots_cap = 0;
+        HMC_CUDA(cudaMallocHost((void**)&s->host_slots, sizeof(DeviceStats) * kPipelineSweeps));
+        s->slots_cap = kPipelineSweeps;
+    }
+    const SweepPlan sp = sweep_plan(s, p);
+    uint32_t done = 0;
+    while (done < p->n_sweeps) {
+        const uint32_t chunk = std::min(p->n_sweeps - done, kPipelineSweeps);
+        const uint32_t guess = std::max(1u, s->rounds_guess);
+        const uint64_t step0 = s->step;
+        const uint32_t substep0 = s->substep;
+        hmc_status st = HMC_OK;
+        for (uint32_t j = 0; j < chunk && !st; ++j) {
+            s->step = step0 + j;
+            s->substep = j == 0 ? substep0 : 0u;
+            if ((st = sweep_rebuild(s, sp))) break;
+            Launch L = sweep_launch(s, p);
+            if ((st = enqueue_sets(s, p, sp, L, 0, guess))) break;
+            cudaError_t e = launch_sweep_guard(s->arr.stats, guess, s->arr.abort_word, s->stream);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(s->host_slots + j, s->arr.stats, sizeof(DeviceStats), cudaMemcpyDeviceToHost,
+                                    s->stream);
+            if (e != cudaSuccess) st = fail(HMC_CUDA_ERROR, "pipelined sweep: %s", cudaGetErrorString(e));
+            s->prof.kernel_launches += 1;
+        }
+        s->step = step0;
+        s->substep = substep0;
+        HMC_CUDA(cudaStreamSynchronize(s->stream));
+        if (st) {
+            cudaMemsetAsync(s->arr.abort_word, 0, sizeof(uint32_t), s->stream);
+            return st;
+        }
+        for (uint32_t j = 0; j < chunk; ++j) {
+            DeviceStats d = s->host_slots[j];
+            if (d.error_flags & kErrAborted) break;  // a sweep before it stopped the chunk
+            const bool short_sets = d.rounds > guess;
+            if (short_sets || d.error_flags) HMC_CUDA(cudaMemsetAsync(s->arr.abort_word, 0, sizeof(uint32_t), s->stream));
+            if (d.error_flags) {
+                *s->host_stats = d;
+                HMC_CUDA(cudaStreamSynchronize(s->stream));
+                return check_flags(s);  // the colour passes left the state untouched
+            }
+            if (short_sets) {  // this sweep's missing colour sets, then the sweeps after it again
+                if ((st = sweep_rebuild(s, sp))) return st;
+                Launch L = sweep_launch(s, p);
+                if ((st = enqueue_sets(s, p, sp, L, guess, d.rounds))) return st;
+                if ((st = read_stats(s))) return st;
+                if ((st = check_flags(s))) return st;
+                const DeviceStats& x = *s->host_stats;
+                d.accepted += x.accepted;
+                d.rechecks += x.rechecks;
+                d.pair_checks += x.pair_checks;
+                d.ambiguous += x.ambiguous;
+                d.max_err_bits = std::max(d.max_err_bits, x.max_err_bits);
+            }
+            account_sweep(s, p, d, total);
+            done += 1;
+            if (short_sets) break;
+        }
+    }
+    return HMC_OK;
+}
+
 hmc_status hmc_sweep(hmc_system* s, const hmc_sweep_params* p, hmc_count* out) {
     if (!s || !p) return fail(HMC_INVALID_ARGUMENT, "NULL argument");
     if (p->struct_size < sizeof(hmc_sweep_params)) return fail(HMC_INVALID_ARGUMENT, "hmc_sweep_params.struct_size");
@@ -958,79 +1146,26 @@ hmc_status hmc_sweep(hmc_system* s, const hmc_sweep_params* p, hmc_count* out) {
     if (p->precision > HMC_FP32_RECHECK) return fail(HMC_INVALID_ARGUMENT, "precision");
     HMC_CUDA(cudaSetDevice(s->ctx->device));
     hmc_count total{};
-    const bool fp32 = p->precision == HMC_FP32_RECHECK;
+    if (p->increment_step && p->n_sweeps > 1 && s->n > 0 && !s->profiling) {
+        hmc_status st = sweep_pipelined(s, p, total);
+        if (st) return st;
+        if (out) *out = total;
+        return HMC_OK;
+    }
+    const SweepPlan sp = sweep_plan(s, p);
     const uint32_t colors = 1u << s->dim;
     for (uint32_t sweep = 0; sweep < p->n_sweeps; ++sweep) {
         if (s->profiling) HMC_CUDA(cudaEventRecord(s->ev[0], s->stream));
-        // shapes read S in both modes; the colour passes do not read slot_of_body
-        hmc_status st = rebuild(s, !fp32 || s->oriented() || (s->soft() && !s->soft_fp32()), false);
+        hmc_status st = sweep_rebuild(s, sp);
         if (st) return st;
         if (s->profiling) HMC_CUDA(cudaEventRecord(s->ev[1], s->stream));
-        Launch L{};
-        L.step = s->step;
-        L.seed = s->seed;
-        L.max_move = p->maximum;
-        L.kt = p->temperature;
-        L.n_bodies = (uint32_t)s->n;
-        L.n_active = s->geom.color_stride;  // grid bound; the kernels read the list lengths
-        const uint32_t variant = variant_of(s, fp32);
-        const bool coop = coop_of(s, fp32);
-        const bool poly2_fp32 = fp32 && variant == 0;  // polygon variant 1: the FP64 pass in both modes
+        Launch L = sweep_launch(s, p);
         if (s->profiling) HMC_CUDA(cudaEventRecord(s->ev[2], s->stream));
         // The rounds (while count.total() < N, :402-418) are known on the device after the
         // rebuild; the host enqueues the previous sweep's number of colour sets without
         // waiting, the kernels skip sets beyond the true count, and any missing sets follow.
-        auto enqueue = [&](uint32_t r0, uint32_t r1) -> hmc_status {
-            for (uint32_t r = r0; r < r1; ++r) {
-                L.substep = s->substep + r;  // increment_substep after every full colour set
-                L.round = r;
-                // the round's trial moves, one thread each, before the passes that give a trial
-                // several lanes
-                if (s->soft()) {
-                    HMC_CUDA(launch_propose_lj(s->dim, fp32 && s->soft_fp32(), s->geom, s->arr, L, s->stream));
-                    s->prof.kernel_launches += 1;
-                } else if (s->interaction == HMC_HARD_CONVEX_POLYHEDRON) {
-                    HMC_CUDA(launch_propose_poly(fp32 && !s->shape_soft, s->geom, s->arr, L, p->move == HMC_ROTATE,
-                                                 s->shape_soft, s->stream));
-                    s->prof.kernel_launches += 1;
-                } else if (s->polygon()) {
-                    HMC_CUDA(launch_propose_poly2(poly2_fp32 && !s->shape_soft, s->geom, s->arr, L,
-                                                  p->move == HMC_ROTATE, s->shape_soft, s->stream));
-                    s->prof.kernel_launches += 1;
-                }
-                for (uint32_t c = 0; c < colors; ++c) {
-                    L.color = c;
-                    L.overlap_previous = (r > 0 || c > 0) && s->pdl ? 1u : 0u;
-                    // the first pass after the rebuild (or after a round's proposals): launch early,
-                    // wait for it before reading anything
-                    L.early_wait = (r == 0 || s->soft() || s->oriented()) && c == 0 && s->pdl ? 1u : 0u;
-                    if (s->soft())  // the overlap penalty has no FP32 path: FP64 in both modes
-                        HMC_CUDA(launch_sweep_lj(s->dim, fp32 && s->soft_fp32(), !s->soft_fp32(), s->geom, s->arr,
-                                                 s->pair, L, s->stream, variant));
-                    else if (s->shape_soft && s->dim == 3)  // FP64 in both modes
-                        HMC_CUDA(launch_sweep_poly3_soft(s->geom, s->arr, s->verts, s->n_vertices, s->so, L,
-                                                         s->stream));
-                    else if (s->shape_soft)
-                        HMC_CUDA(launch_sweep_poly2_soft(s->sat(), s->geom, s->arr, s->verts, s->n_vertices, s->so,
-                                                         L, s->stream));
-                    else if (s->interaction == HMC_HARD_CONVEX_POLYHEDRON)
-                        HMC_CUDA(launch_sweep_poly(fp32, s->geom, s->arr, s->verts, s->n_vertices, s->poly_rcut2,
-                                                   s->poly_rcut2_hi32, L, p->move == HMC_ROTATE, s->stream,
-                                                   variant));
-                    else if (s->polygon())
-                        HMC_CUDA(launch_sweep_poly2(poly2_fp32, s->sat(), s->geom, s->arr, s->verts, s->n_vertices,
-                                                    s->poly_rcut2, s->poly_rcut2_hi32, L, p->move == HMC_ROTATE,
-                                                    s->stream));
-                    else
-                        HMC_CUDA(launch_sweep_sphere(s->dim, fp32, s->geom, s->arr, s->pair, L, coop, s->stream,
-                                                     variant));
-                    s->prof.kernel_launches += 1;
-                }
-            }
-            return HMC_OK;
-        };
         const uint32_t guess = s->n == 0 ? 0u : s->rounds_guess;
-        if ((st = enqueue(0, guess))) return st;
+        if ((st = enqueue_sets(s, p, sp, L, 0, guess))) return st;
         // the passes' end is recorded before the host waits for the counts, so that profiling adds
         // no host round trip to the sweep
         if (s->profiling) HMC_CUDA(cudaEventRecord(s->ev[3], s->stream));
@@ -1038,11 +1173,10 @@ hmc_status hmc_sweep(hmc_system* s, const hmc_sweep_params* p, hmc_count* out) {
         if ((st = check_flags(s))) return st;  // the kernels left the state untouched
         const uint32_t rounds = s->host_stats->rounds;
         if (rounds > guess) {
-            if ((st = enqueue(guess, rounds))) return st;
+            if ((st = enqueue_sets(s, p, sp, L, guess, rounds))) return st;
             if (s->profiling) HMC_CUDA(cudaEventRecord(s->ev[3], s->stream));
             if ((st = read_stats(s))) return st;
         }
-        if (rounds > 0) s->rounds_guess = rounds;
         if (s->profiling) {
             HMC_CUDA(cudaEventSynchronize(s->ev[3]));
             float t_rebuild = 0.f, t_sweep = 0.f;
@@ -1054,21 +1188,7 @@ hmc_status hmc_sweep(hmc_system* s, const hmc_sweep_params* p, hmc_count* out) {
             s->prof.sweep_launches += (uint64_t)std::max(rounds, guess) * colors;
             s->prof.sweeps += 1;
         }
-        const uint64_t nonempty = s->host_stats->nonempty;
-        total.accepted += s->host_stats->accepted;
-        total.rejected += (uint64_t)rounds * nonempty - s->host_stats->accepted;
-        total.rechecks += s->host_stats->rechecks;
-        total.pair_checks += s->host_stats->pair_checks;
-        total.order_ambiguous += s->host_stats->ambiguous;
-        double me;
-        unsigned long long bits = s->host_stats->max_err_bits;
-        std::memcpy(&me, &bits, 8);
-        total.max_fp32_error = std::max(total.max_fp32_error, me);
-        s->substep += rounds;
-        if (p->increment_step) {
-            s->step += 1;
-            s->substep = 0;
-        }
+        account_sweep(s, p, *s->host_stats, total);
     }
     if (out) *out = total;
     return HMC_OK;

@@ -16,6 +16,7 @@ enum : uint32_t {
     kErrAngleRange = 1u << 2,  // a 2-D orientation angle at or beyond 2^19 rad
     kErrCellOverflow = 1u << 3,  // a cell of the serial sweep's grid is full
     kErrIterationCap = 1u << 4,  // an approximate separation loop ran past ShapeOverlap::max_steps
+    kErrAborted = 1u << 5,       // a sweep of a pipelined call after one that stopped the call
 };
 
 // Counters written by the kernels. Zeroed by the host before a sweep.
@@ -69,6 +70,7 @@ struct Arrays {
     uint32_t* block_sums;    // scan scratch
     uint32_t* color_cells;   // [cells] per-colour lists of non-empty spaces, packed multi-indices
     DeviceStats* stats;
+    uint32_t* abort_word;    // pipelined sweeps: nonzero once a sweep stopped the call (may be null)
     const double* zig_x;     // ziggurat tables (257 each)
     const double* zig_f;
     // A round's trial moves, one per colour-list entry (soft potentials: k_propose_lj writes them
@@ -392,6 +394,9 @@ struct BatchSweepTotals {
 // injected-move and tuner kernels read; a sweep's own rebuild skips it.
 cudaError_t launch_rebuild(int dim, const Geometry& g, const Arrays& a, uint32_t n, bool write_s, cudaStream_t s,
                            bool write_slots = true);
+// After a sweep of a pipelined call: raise the abort word when the sweep needed more colour sets
+// than the `enqueued` ones or flagged an error.
+cudaError_t launch_sweep_guard(const DeviceStats* stats, uint32_t enqueued, uint32_t* abort_word, cudaStream_t s);
 // Per-replica rounds of a batch sweep into Replica::rounds, their maximum into DeviceStats::rounds.
 cudaError_t launch_batch_rounds(const Batch& b, Replica* rep, DeviceStats* stats, cudaStream_t s);
 // The device side of a captured batch sweep: every replica's checkerboard origin from its own

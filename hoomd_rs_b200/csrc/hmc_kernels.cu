@@ -713,6 +713,8 @@ __global__ void k_bin(Geometry g, Arrays A, uint32_t n) {
     allow_dependent_launch();  // the scan may launch; it waits for this kernel to end
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    // a pipelined call stopped by an earlier sweep: this sweep's colour passes do nothing
+    if (i == 0 && A.abort_word && *A.abort_word != 0u) atomicOr(&A.stats->error_flags, kErrAborted);
     double4 b = A.body_pos[i];
     double x[3] = {b.x, b.y, b.z};
     uint32_t m[3] = {0, 0, 0};
@@ -1733,6 +1735,16 @@ cudaError_t launch_sweep_batch(int dim, bool fp32, const Batch& b, const Arrays&
     PassLaunch pl(grid, overlap_previous || early_wait, s);
     const uint32_t ew = early_wait ? 1u : 0u;
     return cudaLaunchKernelEx(&pl.cfg, k, b, a, color, round, ew);
+}
+
+__global__ void k_sweep_guard(const DeviceStats* stats, uint32_t enqueued, uint32_t* abort_word) {
+    if (*abort_word == 0u && (stats->rounds > enqueued || (stats->error_flags & ~kErrAborted) != 0u))
+        *abort_word = 1u;
+}
+
+cudaError_t launch_sweep_guard(const DeviceStats* stats, uint32_t enqueued, uint32_t* abort_word, cudaStream_t s) {
+    k_sweep_guard<<<1, 1, 0, s>>>(stats, enqueued, abort_word);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_batch_rounds(const Batch& b, Replica* rep, DeviceStats* stats, cudaStream_t s) {

@@ -228,7 +228,13 @@ hmc_status hmc_get_state(hmc_system* sys, double* positions, double* orientation
 /* Microstate::increment_step (hoomd-microstate/src/microstate.rs:412-415): step += 1, substep = 0. */
 hmc_status hmc_increment_step(hmc_system* sys);
 
-/* ---- the sweep ---- */
+/* ---- the sweep ----
+ * n_sweeps ParallelSweep::apply calls; out receives their summed Count. With n_sweeps > 1 and
+ * increment_step (and profiling off) the sweeps are enqueued back to back and the host waits
+ * once per 64 sweeps rather than once per sweep; a sweep that needs more colour sets than were
+ * enqueued stops the ones after it on the device, is completed, and they are enqueued again, so
+ * the trajectory, Count and Counter are those of one call per sweep. On an error the sweeps
+ * before the failing one stay applied and counted in the system's Counter; out is not written. */
 hmc_status hmc_sweep(hmc_system* sys, const hmc_sweep_params* params, hmc_count* out);
 hmc_status hmc_tune(hmc_system* sys, hmc_sweep_params* params, double target_acceptance, uint32_t samples,
                     uint32_t steps);
