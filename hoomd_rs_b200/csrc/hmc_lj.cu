@@ -127,31 +127,41 @@ struct Sums32 {
 };
 
 // FP32 energies of the trial site (offsets t32) and the current site (offsets c32) against
-// the stencil fs of their common space, with error bounds.
-template <int DIM>
+// the stencil fs of their common space, with error bounds. Each lane takes U candidates per
+// step (loads issued together); the order of a lane's terms does not enter the bound.
+template <int DIM, int U = 1>
 __device__ __forceinline__ Sums32 lj_energy32(const Geometry& g, const Arrays& A, const Pair& P, float4 t32,
                                                float4 c32, int mf, const FlatStencil& fs, uint32_t self,
                                                uint32_t lane) {
     Sums32 s{0.f, 0.f, 0.f, 0.f, 0u, 0u};
     const uint32_t sf = g.shape[DIM - 1];
 #pragma unroll 1
-    for (uint32_t j0 = 0; j0 < fs.total; j0 += 32) {
-        const uint32_t j = j0 + lane;
-        uint32_t part;
-        const uint32_t q = flat_slot(fs, j, part);
-        const float s0 = __shfl_sync(0xffffffffu, fs.s0, part);
-        const float s1 = __shfl_sync(0xffffffffu, fs.s1, part);
-        if (j < fs.total && q != self) {
-            const float4 o = __ldg(A.sorted_off + q);
-            int dm = __float_as_int(o.w) - mf;
+    for (uint32_t j0 = 0; j0 < fs.total; j0 += 32u * U) {
+        float4 o[U];
+        float s0[U], s1[U];
+        bool ok[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const uint32_t j = j0 + 32u * u + lane;
+            uint32_t part;
+            const uint32_t q = flat_slot(fs, j, part);
+            s0[u] = __shfl_sync(0xffffffffu, fs.s0, part);
+            s1[u] = __shfl_sync(0xffffffffu, fs.s1, part);
+            ok[u] = j < fs.total && q != self;
+            o[u] = ok[u] ? __ldg(A.sorted_off + q) : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if (!ok[u]) continue;
+            int dm = __float_as_int(o[u].w) - mf;
             if (sf >= 4) {
                 if (dm > 1)
                     dm -= (int)sf;
                 else if (dm < -1)
                     dm += (int)sf;
             }
-            const float r2n = fp32_dist2<DIM>(g, t32, o, s0, s1, dm);
-            const float r2o = fp32_dist2<DIM>(g, c32, o, s0, s1, dm);
+            const float r2n = fp32_dist2<DIM>(g, t32, o[u], s0[u], s1[u], dm);
+            const float r2o = fp32_dist2<DIM>(g, c32, o[u], s0[u], s1[u], dm);
             s.pairs += 2;
             if (r2n < P.lj_rcut2_hi32) {
                 float e, err;
@@ -362,7 +372,7 @@ constexpr uint32_t kRecheckChunks = 8;  // 32-candidate chunks per shared-memory
 // same butterfly; an empty slot adds +0, which leaves a sum that starts at +0 unchanged). A
 // lone warp walking the stencil in FP64 would otherwise set the duration of a pass whose
 // trials all run in one wave.
-template <int DIM, bool INJ = false, int MINB = HMC_LJ_MIN_BLOCKS>
+template <int DIM, bool INJ = false, int MINB = HMC_LJ_MIN_BLOCKS, int U = 1>
 __global__ void __launch_bounds__(128, MINB) k_sweep_lj32(Geometry g, Arrays A, Pair P, Launch L, Injected J) {
     if (L.early_wait) grid_dependency_wait();  // first pass: the rebuild's arrays are read at once
     __shared__ double s_e[kRecheckChunks][2][32];
@@ -418,7 +428,7 @@ __global__ void __launch_bounds__(128, MINB) k_sweep_lj32(Geometry g, Arrays A, 
         if (trial) {
             const float4 t32 = INJ ? cell_offsets<DIM>(g, t, m) : t32p;
             const float4 c32 = __ldg(A.sorted_off + k);
-            const Sums32 s = lj_energy32<DIM>(g, A, P, t32, c32, (int)m[DIM - 1], fs, k, lane);
+            const Sums32 s = lj_energy32<DIM, U>(g, A, P, t32, c32, (int)m[DIM - 1], fs, k, lane);
             pst.checks += s.pairs;
             decision = decide32(s, L.kt, u);
             d32 = s.e_new - s.e_old;
@@ -902,17 +912,25 @@ cudaError_t launch_sweep_lj(int dim, bool fp32, bool generic, const Geometry& g,
     PassLaunch pl(blocks, l.overlap_previous != 0 || l.early_wait != 0, s);
     using LjKernel = void (*)(Geometry, Arrays, Pair, Launch, Injected);
     // the compiled launch variants, in the order of kLjShapes ([dim == 3][fp32][variant])
-    static const LjKernel kernels[2][2][3] = {
-        {{k_sweep_lj<2, false, 9, false>, k_sweep_lj<2, false, 7, false>, k_sweep_lj<2, false, 11, false>},
-         {k_sweep_lj32<2, false, 9>, k_sweep_lj32<2, false, 7>, k_sweep_lj32<2, false, 11>}},
-        {{k_sweep_lj<3, false, 9, false>, k_sweep_lj<3, false, 7, false>, k_sweep_lj<3, false, 11, false>},
-         {k_sweep_lj32<3, false, 9>, k_sweep_lj32<3, false, 7>, k_sweep_lj32<3, false, 11>}}};
+    // (variants 3 and 4 take two candidates per lane and step in the FP32 pass; the FP64 passes
+    // have one form, so there they repeat variants 1 and 0)
+    static const LjKernel kernels[2][2][5] = {
+        {{k_sweep_lj<2, false, 9, false>, k_sweep_lj<2, false, 7, false>, k_sweep_lj<2, false, 11, false>,
+          k_sweep_lj<2, false, 7, false>, k_sweep_lj<2, false, 9, false>},
+         {k_sweep_lj32<2, false, 9>, k_sweep_lj32<2, false, 7>, k_sweep_lj32<2, false, 11>,
+          k_sweep_lj32<2, false, 7, 2>, k_sweep_lj32<2, false, 9, 2>}},
+        {{k_sweep_lj<3, false, 9, false>, k_sweep_lj<3, false, 7, false>, k_sweep_lj<3, false, 11, false>,
+          k_sweep_lj<3, false, 7, false>, k_sweep_lj<3, false, 9, false>},
+         {k_sweep_lj32<3, false, 9>, k_sweep_lj32<3, false, 7>, k_sweep_lj32<3, false, 11>,
+          k_sweep_lj32<3, false, 7, 2>, k_sweep_lj32<3, false, 9, 2>}}};
     // the overlap penalty and Isotropic: the FP64 pass with the dispatching pair energy
-    static const LjKernel generic_kernels[2][3] = {
-        {k_sweep_lj<2, false, 9, true>, k_sweep_lj<2, false, 7, true>, k_sweep_lj<2, false, 11, true>},
-        {k_sweep_lj<3, false, 9, true>, k_sweep_lj<3, false, 7, true>, k_sweep_lj<3, false, 11, true>}};
-    const LjKernel k = generic ? generic_kernels[dim == 3][variant < 3 ? variant : 0]
-                               : kernels[dim == 3][fp32][variant < 3 ? variant : 0];
+    static const LjKernel generic_kernels[2][5] = {
+        {k_sweep_lj<2, false, 9, true>, k_sweep_lj<2, false, 7, true>, k_sweep_lj<2, false, 11, true>,
+         k_sweep_lj<2, false, 7, true>, k_sweep_lj<2, false, 9, true>},
+        {k_sweep_lj<3, false, 9, true>, k_sweep_lj<3, false, 7, true>, k_sweep_lj<3, false, 11, true>,
+         k_sweep_lj<3, false, 7, true>, k_sweep_lj<3, false, 9, true>}};
+    const LjKernel k = generic ? generic_kernels[dim == 3][variant < 5 ? variant : 0]
+                               : kernels[dim == 3][fp32][variant < 5 ? variant : 0];
     return cudaLaunchKernelEx(&pl.cfg, k, g, a, p, l, Injected{});
 }
 
