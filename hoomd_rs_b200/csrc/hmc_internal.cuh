@@ -297,7 +297,7 @@ struct LaunchShape {
 };
 constexpr LaunchShape kSphereDirectShapes[] = {{6, 1, 0}, {5, 1, 0}, {7, 1, 0}};
 constexpr LaunchShape kSphereCoopShapes[] = {{6, 1, 2}, {6, 1, 1}, {6, 1, 3}, {5, 1, 2}, {7, 1, 2}};
-// Lennard-Jones and Isotropic passes; own_steps 2: the FP32 pass takes two candidates per lane and step
+// Lennard-Jones and Isotropic passes; own_steps 2: two candidates per lane and step
 constexpr LaunchShape kLjShapes[] = {{9, 1, 0}, {7, 1, 0}, {11, 1, 0}, {7, 1, 2}, {9, 1, 2}};
 constexpr LaunchShape kPolyShapes[] = {{5, 4, 0}, {5, 2, 0}, {5, 8, 0}};
 constexpr LaunchShape kBatchShapes[] = {{4, 1, 0}, {3, 1, 0}, {5, 1, 0}, {6, 1, 0}, {7, 1, 0}, {8, 1, 0}};

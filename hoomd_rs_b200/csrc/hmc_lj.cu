@@ -80,30 +80,30 @@ __device__ __forceinline__ uint32_t warp_maxu(uint32_t v) {
 // S of a candidate comes from sorted_s when have_s, else from wrap(sorted_b). The two sums of
 // one call equal two calls of one sum each over the same stencil.
 // mag receives sum |e| over both sums (for order_ambiguous).
-template <int DIM, bool TWO, bool GENERIC = true>
+// U: candidates a lane loads per step (U = 2 keeps two loads in flight); a lane still adds its
+// terms in increasing candidate order, so the sums are the same bits for every U.
+template <int DIM, bool TWO, bool GENERIC = true, int U = 1>
 __device__ __forceinline__ void lj_energy64(const Geometry& g, const Arrays& A, const Pair& P, const double* ta,
                                             const double* tb, const FlatStencil& fs, uint32_t self, bool have_s,
                                             uint32_t lane, double& ea, double& eb, double& mag) {
     double a = 0.0, b = 0.0, am = 0.0;
 #pragma unroll 1
-    for (uint32_t j0 = 0; j0 < fs.total; j0 += 32) {
-        const uint32_t j = j0 + lane;
-        uint32_t part;
-        const uint32_t q = flat_slot(fs, j, part);
-        if (j < fs.total && q != self) {
-            double sv[3];
-            if (have_s) {
-                const double4 s4 = ldg4(A.sorted_s + q);
-                sv[0] = s4.x;
-                sv[1] = s4.y;
-                sv[2] = s4.z;
-            } else {
-                const double4 b4 = ldg4(A.sorted_b + q);
-                sv[0] = b4.x;
-                sv[1] = b4.y;
-                sv[2] = b4.z;
-                wrap_inv<DIM>(g.L, g.invL, sv);
-            }
+    for (uint32_t j0 = 0; j0 < fs.total; j0 += 32u * U) {
+        double4 v[U];
+        bool ok[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const uint32_t j = j0 + 32u * u + lane;
+            uint32_t part;
+            const uint32_t q = flat_slot(fs, j, part);
+            ok[u] = j < fs.total && q != self;
+            v[u] = ok[u] ? ldg4((have_s ? A.sorted_s : A.sorted_b) + q) : make_double4(0.0, 0.0, 0.0, 0.0);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if (!ok[u]) continue;
+            double sv[3] = {v[u].x, v[u].y, v[u].z};
+            if (!have_s) wrap_inv<DIM>(g.L, g.invL, sv);
             const double ra = ref_dist2<DIM>(g, ta, sv);
             const double x = soft_pair64<GENERIC>(P, ra);
             a = dadd(a, x);
@@ -268,7 +268,7 @@ __device__ __forceinline__ void lj_inject(const Arrays& A, const Injected& J, ui
 }
 
 // The FP64 pass: one warp per trial. INJ: the probe mode (decisions instead of commits).
-template <int DIM, bool INJ = false, int MINB = HMC_LJ_MIN_BLOCKS, bool GENERIC = true>
+template <int DIM, bool INJ = false, int MINB = HMC_LJ_MIN_BLOCKS, bool GENERIC = true, int U = 1>
 __global__ void __launch_bounds__(128, MINB) k_sweep_lj(Geometry g, Arrays A, Pair P, Launch L, Injected J) {
     if (L.early_wait) grid_dependency_wait();  // first pass: the rebuild's arrays are read at once
     const uint32_t lane = threadIdx.x & 31u;
@@ -318,7 +318,7 @@ __global__ void __launch_bounds__(128, MINB) k_sweep_lj(Geometry g, Arrays A, Pa
         const double4 s4 = ldg4(A.sorted_s + k);
         const double si[3] = {s4.x, s4.y, s4.z};
         double e_new, e_old, mag;
-        lj_energy64<DIM, true, GENERIC>(g, A, P, t, si, fs, k, true, lane, e_new, e_old, mag);
+        lj_energy64<DIM, true, GENERIC, U>(g, A, P, t, si, fs, k, true, lane, e_new, e_old, mag);
         const double du = dsub(e_new, e_old);
         const double e0 = exp(ddiv(-du, L.kt));
         const bool amb = order_ambiguous(du, mag, fs.total, u, L.kt, e0);
@@ -912,23 +912,22 @@ cudaError_t launch_sweep_lj(int dim, bool fp32, bool generic, const Geometry& g,
     PassLaunch pl(blocks, l.overlap_previous != 0 || l.early_wait != 0, s);
     using LjKernel = void (*)(Geometry, Arrays, Pair, Launch, Injected);
     // the compiled launch variants, in the order of kLjShapes ([dim == 3][fp32][variant])
-    // (variants 3 and 4 take two candidates per lane and step in the FP32 pass; the FP64 passes
-    // have one form, so there they repeat variants 1 and 0)
+    // (variants 3 and 4 take two candidates per lane and step)
     static const LjKernel kernels[2][2][5] = {
         {{k_sweep_lj<2, false, 9, false>, k_sweep_lj<2, false, 7, false>, k_sweep_lj<2, false, 11, false>,
-          k_sweep_lj<2, false, 7, false>, k_sweep_lj<2, false, 9, false>},
+          k_sweep_lj<2, false, 7, false, 2>, k_sweep_lj<2, false, 9, false, 2>},
          {k_sweep_lj32<2, false, 9>, k_sweep_lj32<2, false, 7>, k_sweep_lj32<2, false, 11>,
           k_sweep_lj32<2, false, 7, 2>, k_sweep_lj32<2, false, 9, 2>}},
         {{k_sweep_lj<3, false, 9, false>, k_sweep_lj<3, false, 7, false>, k_sweep_lj<3, false, 11, false>,
-          k_sweep_lj<3, false, 7, false>, k_sweep_lj<3, false, 9, false>},
+          k_sweep_lj<3, false, 7, false, 2>, k_sweep_lj<3, false, 9, false, 2>},
          {k_sweep_lj32<3, false, 9>, k_sweep_lj32<3, false, 7>, k_sweep_lj32<3, false, 11>,
           k_sweep_lj32<3, false, 7, 2>, k_sweep_lj32<3, false, 9, 2>}}};
     // the overlap penalty and Isotropic: the FP64 pass with the dispatching pair energy
     static const LjKernel generic_kernels[2][5] = {
         {k_sweep_lj<2, false, 9, true>, k_sweep_lj<2, false, 7, true>, k_sweep_lj<2, false, 11, true>,
-         k_sweep_lj<2, false, 7, true>, k_sweep_lj<2, false, 9, true>},
+         k_sweep_lj<2, false, 7, true, 2>, k_sweep_lj<2, false, 9, true, 2>},
         {k_sweep_lj<3, false, 9, true>, k_sweep_lj<3, false, 7, true>, k_sweep_lj<3, false, 11, true>,
-         k_sweep_lj<3, false, 7, true>, k_sweep_lj<3, false, 9, true>}};
+         k_sweep_lj<3, false, 7, true, 2>, k_sweep_lj<3, false, 9, true, 2>}};
     const LjKernel k = generic ? generic_kernels[dim == 3][variant < 5 ? variant : 0]
                                : kernels[dim == 3][fp32][variant < 5 ? variant : 0];
     return cudaLaunchKernelEx(&pl.cfg, k, g, a, p, l, Injected{});

@@ -289,7 +289,8 @@ typedef struct hmc_launch_variant {
     uint32_t blocks_per_sm;    /* resident blocks per SM the kernel is compiled for */
     uint32_t trials_per_warp;  /* trials one warp takes at once (1: a lane or a warp per trial) */
     uint32_t own_steps;        /* warp-cooperative sphere pass: candidates per row a lane tests;
-                                  FP32 Lennard-Jones pass: 2 = two candidates per lane and step */
+                                  Lennard-Jones / Isotropic passes: 2 = two candidates per lane
+                                  and step */
 } hmc_launch_variant;
 /* index UINT32_MAX: the variant the next hmc_sweep in this precision runs. */
 hmc_status hmc_get_launch_variant(hmc_system* sys, uint32_t precision, uint32_t index, hmc_launch_variant* out);
