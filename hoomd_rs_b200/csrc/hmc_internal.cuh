@@ -305,7 +305,8 @@ constexpr LaunchShape kBatchShapes[] = {{4, 1, 0}, {3, 1, 0}, {5, 1, 0}, {6, 1, 
 // of the FP32 prefilter (the same decisions; the prefilter saves little where the FP64
 // circumsphere test is cheap against the separating-axis or XenoCollide test behind it).
 constexpr LaunchShape kPoly2Shapes[] = {{8, 4, 0}, {8, 4, 0}};
-constexpr LaunchShape kBatchLjShapes[] = {{7, 1, 0}, {9, 1, 0}, {5, 1, 0}};  // the Lennard-Jones replica passes
+// the Lennard-Jones replica passes; own_steps 2: two candidates per lane and step
+constexpr LaunchShape kBatchLjShapes[] = {{7, 1, 0}, {9, 1, 0}, {5, 1, 0}, {7, 1, 2}, {9, 1, 2}};
 template <size_t N>
 constexpr uint32_t n_shapes(const LaunchShape (&)[N]) {
     return (uint32_t)N;

@@ -525,7 +525,7 @@ __global__ void __launch_bounds__(128, MINB) k_sweep_lj32(Geometry g, Arrays A, 
 // One colour pass over every replica of a batch that still runs round `round` of this sweep,
 // FP64: one warp per trial as in k_sweep_lj, with the box, checkerboard, pair parameters,
 // Counter, move size and kT of the trial's replica from the replica table.
-template <int DIM, int MINB = HMC_LJ_BATCH_MIN_BLOCKS>
+template <int DIM, int MINB = HMC_LJ_BATCH_MIN_BLOCKS, int U = 1>
 __global__ void __launch_bounds__(128, MINB)
     k_sweep_batch_lj(Batch B, Arrays A, uint32_t color, uint32_t round, uint32_t early_wait) {
     if (early_wait) grid_dependency_wait();  // first pass: the rebuild's arrays are read at once
@@ -568,7 +568,7 @@ __global__ void __launch_bounds__(128, MINB)
         const double4 s4 = ldg4(A.sorted_s + k);
         const double si[3] = {s4.x, s4.y, s4.z};
         double e_new, e_old, mag;
-        lj_energy64<DIM, true, false>(g, A, R.p, t, si, fs, k, true, lane, e_new, e_old, mag);
+        lj_energy64<DIM, true, false, U>(g, A, R.p, t, si, fs, k, true, lane, e_new, e_old, mag);
         const double du = dsub(e_new, e_old);
         const double e0 = exp(ddiv(-du, R.kt));
         if (lane == 0 && order_ambiguous(du, mag, fs.total, u, R.kt, e0)) pst.ambiguous++;
@@ -592,7 +592,7 @@ __global__ void __launch_bounds__(128, MINB)
 // The FP32 + recheck pass over a batch: k_sweep_lj32 (four trials per block, an undecided
 // trial rechecked by the whole block in the FP64 pass's order) with each trial's geometry and
 // parameters from its replica; the owner also publishes its replica for the helping warps.
-template <int DIM, int MINB = HMC_LJ_BATCH_MIN_BLOCKS>
+template <int DIM, int MINB = HMC_LJ_BATCH_MIN_BLOCKS, int U = 1>
 __global__ void __launch_bounds__(128, MINB)
     k_sweep_batch_lj32(Batch B, Arrays A, uint32_t color, uint32_t round, uint32_t early_wait) {
     if (early_wait) grid_dependency_wait();  // first pass: the rebuild's arrays are read at once
@@ -652,7 +652,7 @@ __global__ void __launch_bounds__(128, MINB)
             const Replica& R = B.rep[r];
             const float4 t32 = cell_offsets<DIM>(R.g, t, m);
             const float4 c32 = __ldg(A.sorted_off + k);
-            const Sums32 s = lj_energy32<DIM>(R.g, A, R.p, t32, c32, (int)m[DIM - 1], fs, k, lane);
+            const Sums32 s = lj_energy32<DIM, U>(R.g, A, R.p, t32, c32, (int)m[DIM - 1], fs, k, lane);
             pst.checks += s.pairs;
             decision = decide32(s, R.kt, u);
             d32 = s.e_new - s.e_old;
@@ -998,12 +998,17 @@ cudaError_t launch_sweep_batch_lj(int dim, bool fp32, const Batch& b, const Arra
     const uint32_t ew = early_wait ? 1u : 0u;
     using BatchLjKernel = void (*)(Batch, Arrays, uint32_t, uint32_t, uint32_t);
     // the compiled launch variants, in the order of kBatchLjShapes ([dim == 3][fp32][variant])
-    static const BatchLjKernel kernels[2][2][3] = {
-        {{k_sweep_batch_lj<2, 7>, k_sweep_batch_lj<2, 9>, k_sweep_batch_lj<2, 5>},
-         {k_sweep_batch_lj32<2, 7>, k_sweep_batch_lj32<2, 9>, k_sweep_batch_lj32<2, 5>}},
-        {{k_sweep_batch_lj<3, 7>, k_sweep_batch_lj<3, 9>, k_sweep_batch_lj<3, 5>},
-         {k_sweep_batch_lj32<3, 7>, k_sweep_batch_lj32<3, 9>, k_sweep_batch_lj32<3, 5>}}};
-    return cudaLaunchKernelEx(&pl.cfg, kernels[dim == 3][fp32][variant < 3 ? variant : 0], b, a, color, round, ew);
+    // (variants 3 and 4 take two candidates per lane and step)
+    static const BatchLjKernel kernels[2][2][5] = {
+        {{k_sweep_batch_lj<2, 7>, k_sweep_batch_lj<2, 9>, k_sweep_batch_lj<2, 5>, k_sweep_batch_lj<2, 7, 2>,
+          k_sweep_batch_lj<2, 9, 2>},
+         {k_sweep_batch_lj32<2, 7>, k_sweep_batch_lj32<2, 9>, k_sweep_batch_lj32<2, 5>, k_sweep_batch_lj32<2, 7, 2>,
+          k_sweep_batch_lj32<2, 9, 2>}},
+        {{k_sweep_batch_lj<3, 7>, k_sweep_batch_lj<3, 9>, k_sweep_batch_lj<3, 5>, k_sweep_batch_lj<3, 7, 2>,
+          k_sweep_batch_lj<3, 9, 2>},
+         {k_sweep_batch_lj32<3, 7>, k_sweep_batch_lj32<3, 9>, k_sweep_batch_lj32<3, 5>, k_sweep_batch_lj32<3, 7, 2>,
+          k_sweep_batch_lj32<3, 9, 2>}}};
+    return cudaLaunchKernelEx(&pl.cfg, kernels[dim == 3][fp32][variant < 5 ? variant : 0], b, a, color, round, ew);
 }
 
 cudaError_t launch_eval_lj(int dim, bool fp32, const Geometry& g, const Arrays& a, const Pair& p,
