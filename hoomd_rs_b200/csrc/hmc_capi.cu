@@ -446,6 +446,12 @@ uint32_t variant_of(const hmc_system* s, bool fp32) {
                           density_band((double)s->n, (double)s->geom.n_cells));
 }
 
+// Kernels of one cell-list rebuild: bin, 2 scan passes (3 for grids of more than 2048 scan
+// blocks), scatter, space sort, gather.
+uint32_t rebuild_kernels(const hmc_system* s) {
+    return (s->n > 0 ? 6u : 2u) + ((s->geom.n_cells + 2047u) / 2048u > 2048u ? 1u : 0u);
+}
+
 // update_checkerboard (parallel_sweep.rs:176-201): origin shift from the counter's
 // index u64::MAX stream, then the device counting sort into cell order.
 hmc_status rebuild(hmc_system* s, bool write_s, bool write_slots = true) {
@@ -456,8 +462,7 @@ hmc_status rebuild(hmc_system* s, bool write_s, bool write_slots = true) {
     }
     HMC_CUDA(cudaMemsetAsync(s->arr.stats, 0, sizeof(DeviceStats), s->stream));
     HMC_CUDA(launch_rebuild(s->dim, s->geom, s->arr, (uint32_t)s->n, write_s, s->stream, write_slots));
-    // bin, 2 scan passes (3 for grids of more than 2048 scan blocks), scatter, space sort, gather
-    s->prof.kernel_launches += (s->n > 0 ? 6 : 2) + ((s->geom.n_cells + 2047u) / 2048u > 2048u ? 1 : 0);
+    s->prof.kernel_launches += rebuild_kernels(s);
     return HMC_OK;
 }
 
@@ -1183,7 +1188,7 @@ hmc_status hmc_sweep(hmc_system* s, const hmc_sweep_params* p, hmc_count* out) {
             HMC_CUDA(cudaEventElapsedTime(&t_rebuild, s->ev[0], s->ev[1]));
             HMC_CUDA(cudaEventElapsedTime(&t_sweep, s->ev[2], s->ev[3]));
             s->prof.rebuild_ms += t_rebuild;
-            s->prof.rebuild_launches += s->n > 0 ? 6 : 2;
+            s->prof.rebuild_launches += rebuild_kernels(s);
             s->prof.sweep_ms += t_sweep;
             s->prof.sweep_launches += (uint64_t)std::max(rounds, guess) * colors;
             s->prof.sweeps += 1;
