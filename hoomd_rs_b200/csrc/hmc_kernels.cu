@@ -1728,6 +1728,7 @@ cudaError_t launch_sweep_batch(int dim, bool fp32, const Batch& b, const Arrays&
           k_sweep_batch<3, false, 6>, k_sweep_batch<3, false, 7>, k_sweep_batch<3, false, 8>},
          {k_sweep_batch<3, true, 4>, k_sweep_batch<3, true, 3>, k_sweep_batch<3, true, 5>, k_sweep_batch<3, true, 6>,
           k_sweep_batch<3, true, 7>, k_sweep_batch<3, true, 8>}}};
+    static_assert(n_shapes(kBatchShapes) == 6, "one compiled kernel per batch variant");
     const BatchKernel k = kernels[dim == 3][fp32][variant < 6 ? variant : 0];
     uint32_t grid = blocks_for(max_active, 128);
     const uint32_t wave = (uint32_t)resident_wave((const void*)k);
@@ -1801,6 +1802,7 @@ SphereKernel direct_kernel(int dim, bool fp32, uint32_t v) {
          {k_sweep_sphere<2, true, false, 6>, k_sweep_sphere<2, true, false, 5>, k_sweep_sphere<2, true, false, 7>}},
         {{k_sweep_sphere<3, false, false, 6>, k_sweep_sphere<3, false, false, 5>, k_sweep_sphere<3, false, false, 7>},
          {k_sweep_sphere<3, true, false, 6>, k_sweep_sphere<3, true, false, 5>, k_sweep_sphere<3, true, false, 7>}}};
+    static_assert(n_shapes(kSphereDirectShapes) == 3, "one compiled kernel per direct sphere variant");
     return k[dim == 3][fp32][v < 3 ? v : 0];
 }
 SphereKernel coop_kernel(int dim, bool fp32, uint32_t v) {
@@ -1817,6 +1819,7 @@ SphereKernel coop_kernel(int dim, bool fp32, uint32_t v) {
          {k_sweep_sphere_coop<3, true, false, 6, 2>, k_sweep_sphere_coop<3, true, false, 6, 1>,
           k_sweep_sphere_coop<3, true, false, 6, 3>, k_sweep_sphere_coop<3, true, false, 5, 2>,
           k_sweep_sphere_coop<3, true, false, 7, 2>}}};
+    static_assert(n_shapes(kSphereCoopShapes) == 5, "one compiled kernel per cooperative sphere variant");
     return k[dim == 3][fp32][v < 5 ? v : 0];
 }
 

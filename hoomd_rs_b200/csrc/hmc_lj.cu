@@ -928,6 +928,7 @@ cudaError_t launch_sweep_lj(int dim, bool fp32, bool generic, const Geometry& g,
          k_sweep_lj<2, false, 7, true, 2>, k_sweep_lj<2, false, 9, true, 2>},
         {k_sweep_lj<3, false, 9, true>, k_sweep_lj<3, false, 7, true>, k_sweep_lj<3, false, 11, true>,
          k_sweep_lj<3, false, 7, true, 2>, k_sweep_lj<3, false, 9, true, 2>}};
+    static_assert(n_shapes(kLjShapes) == 5, "one compiled kernel per Lennard-Jones variant");
     const LjKernel k = generic ? generic_kernels[dim == 3][variant < 5 ? variant : 0]
                                : kernels[dim == 3][fp32][variant < 5 ? variant : 0];
     return cudaLaunchKernelEx(&pl.cfg, k, g, a, p, l, Injected{});
@@ -1008,6 +1009,7 @@ cudaError_t launch_sweep_batch_lj(int dim, bool fp32, const Batch& b, const Arra
           k_sweep_batch_lj<3, 9, 2>},
          {k_sweep_batch_lj32<3, 7>, k_sweep_batch_lj32<3, 9>, k_sweep_batch_lj32<3, 5>, k_sweep_batch_lj32<3, 7, 2>,
           k_sweep_batch_lj32<3, 9, 2>}}};
+    static_assert(n_shapes(kBatchLjShapes) == 5, "one compiled kernel per Lennard-Jones batch variant");
     return cudaLaunchKernelEx(&pl.cfg, kernels[dim == 3][fp32][variant < 5 ? variant : 0], b, a, color, round, ew);
 }
 

@@ -1065,6 +1065,7 @@ cudaError_t launch_sweep_poly(bool fp32, const Geometry& g, const Arrays& a, con
     static const PolyKernel kernels[2][3] = {
         {k_sweep_poly3_packed<false, 4>, k_sweep_poly3_packed<false, 2>, k_sweep_poly3_packed<false, 8>},
         {k_sweep_poly3_packed<true, 4>, k_sweep_poly3_packed<true, 2>, k_sweep_poly3_packed<true, 8>}};
+    static_assert(n_shapes(kPolyShapes) == 3, "one compiled kernel per polyhedron variant");
     const uint32_t v = variant < 3 ? variant : 0;
     return cudaLaunchKernelEx(&pl.cfg, kernels[fp32][v], g, a, sh, l, rot, Injected{});
 }
