@@ -227,3 +227,30 @@ def test_batch_of_many_spaces_equals_single_systems(ctx):
             assert (counts[k].accepted, counts[k].rejected) == (c.accepted, c.rejected), k
     for k, m in singles.items():
         assert np.array_equal(b.positions(k), m.positions()), k
+
+
+@pytest.mark.parametrize("captured", [False, True])
+@pytest.mark.parametrize("precision", [FP64, FP32_RECHECK])
+def test_batch_with_replicas_of_more_colour_sets(ctx, precision, captured):
+    # replicas whose checkerboard spaces are 2 or 3 diameters wide hold several bodies per space
+    # and run more colour sets per sweep than the others (which run two): the later sets take
+    # only their spaces (the late lists); every replica equals its single system
+    specs = [(2000, 0.45, 61, 1.0), (3000, 0.50, 62, 2.0), (1500, 0.40, 63, 1.0), (2500, 0.48, 64, 3.0),
+             (800, 0.35, 65, 1.0)]
+    reps = []
+    for n, phi, seed, rng in specs:
+        pos, L = lattice.hard_sphere_box(n, phi, 3, seed)
+        reps.append({"boundary": Periodic(rng, [L] * 3), "positions": pos, "seed": seed})
+    b = Batch(ctx, reps)
+    b.set_captured_sweeps(captured)
+    singles = [Microstate(ctx, r["boundary"], r["positions"], PairwiseCutoff(HardSphere(1.0)), seed=r["seed"])
+               for r in reps]
+    for _ in range(3):
+        counts, _ = b.sweep(0.2, precision, increment_step=True)
+        for k, m in enumerate(singles):
+            c = m.sweep(TRANSLATE, 0.2, 1.0, precision, n_sweeps=1, increment_step=True)
+            assert (counts[k].accepted, counts[k].rejected) == (c.accepted, c.rejected), k
+            assert c.total() >= specs[k][0]  # full colour sets until at least N trials
+    for k, m in enumerate(singles):
+        assert np.array_equal(b.positions(k), m.positions()), k
+        assert m.substep() == 0 and b.state(k)[1:] == (m.step(), m.substep())
