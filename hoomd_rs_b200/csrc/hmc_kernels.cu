@@ -1665,30 +1665,36 @@ cudaError_t launch_count_scan(const Arrays& a, uint32_t n_cells, cudaStream_t s,
 }
 }  // namespace
 
+// Threads per block of the rebuild's per-body kernels (k_bin, k_scatter, k_gather).
+#ifndef HMC_BODY_THREADS
+#define HMC_BODY_THREADS 256
+#endif
+constexpr uint32_t kBodyThreads = HMC_BODY_THREADS;
+
 cudaError_t launch_rebuild(int dim, const Geometry& g, const Arrays& a, uint32_t n, bool write_s, cudaStream_t s,
                            bool write_slots) {
     cudaError_t e = cudaMemsetAsync(a.cell_count, 0, sizeof(uint32_t) * g.n_cells, s);
     if (e != cudaSuccess) return e;
     if (n > 0) {
         if (dim == 2)
-            k_bin<2><<<blocks_for(n, 256), 256, 0, s>>>(g, a, n);
+            k_bin<2><<<blocks_for(n, kBodyThreads), kBodyThreads, 0, s>>>(g, a, n);
         else
-            k_bin<3><<<blocks_for(n, 256), 256, 0, s>>>(g, a, n);
+            k_bin<3><<<blocks_for(n, kBodyThreads), kBodyThreads, 0, s>>>(g, a, n);
     }
     if ((e = launch_count_scan(a, g.n_cells, s, n > 0)) != cudaSuccess) return e;
     if (n == 0) return cudaSuccess;
-    if ((e = launch_chained(k_scatter, blocks_for(n, 256), 256, true, s, a, n)) != cudaSuccess) return e;
-    const uint32_t cb = blocks_for(g.n_cells, kCellThreads), gb = blocks_for(n, 256);
+    if ((e = launch_chained(k_scatter, blocks_for(n, kBodyThreads), kBodyThreads, true, s, a, n)) != cudaSuccess) return e;
+    const uint32_t cb = blocks_for(g.n_cells, kCellThreads), gb = blocks_for(n, kBodyThreads);
     if (dim == 2) {
         if ((e = launch_chained(k_cells<2>, cb, kCellThreads, true, s, g, a)) != cudaSuccess) return e;
         return launch_chained(write_slots ? (write_s ? k_gather<2, true, true> : k_gather<2, false, true>)
                                           : (write_s ? k_gather<2, true, false> : k_gather<2, false, false>),
-                              gb, 256, true, s, g, a, n);
+                              gb, kBodyThreads, true, s, g, a, n);
     }
     if ((e = launch_chained(k_cells<3>, cb, kCellThreads, true, s, g, a)) != cudaSuccess) return e;
     return launch_chained(write_slots ? (write_s ? k_gather<3, true, true> : k_gather<3, false, true>)
                                       : (write_s ? k_gather<3, true, false> : k_gather<3, false, false>),
-                          gb, 256, true, s, g, a, n);
+                          gb, kBodyThreads, true, s, g, a, n);
 }
 
 cudaError_t launch_rebuild_batch(int dim, const Batch& b, const Arrays& a, uint32_t n, bool write_s, cudaStream_t s) {
